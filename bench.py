@@ -1,0 +1,315 @@
+"""Benchmark of the batched destiny tick on B200: bit-exact ship-ticks/s of the flight-mode park.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--worlds W] [--ships S]
+
+A step is one tick of every world. The workload is the flight-mode park's benchmark shape: `--worlds` (65,536)
+worlds of `--ships` (4) ships drawn by exact_ballpark_b200.workloads.flight_worlds (config 0's distributions, each
+world its own seed), dynamical orientation on, the new orbit law. Each rank ticks its own worlds (seed = rank + 1):
+replicas, weak scaling, no collective on the data path; the timing is the max over ranks.
+
+Timed: W untimed warm-up ticks, then K ticks, each launched as one CUDA-graph replay of the tiled (ragged,
+persistent) schedule and timed with CUDA events on the launching stream; L2 is flushed (a 256 MiB write, untimed)
+before each step. Beside it the plain schedule (two launches, records in scratch) is timed the same way, and `e2e`
+times the same step through the public API from host buffers: every step a pinned host->device copy of the ships'
+speed fractions applied by set_speed_fraction (the values they hold, so the flight is unchanged), the tick, and a
+device->host copy of every position. `cpu_baseline` is the C++ oracle (a scalar port of the reference's algorithm)
+on the host's cores over a bounded sample. `--impl reference` times that CPU port on the whole workload instead (the
+reference's own implementation is Python; the port is its compiled restatement), rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "bit-exact ship-ticks/s on 1 B200 (ragged batch vs plain)"
+UNIT = "ship-ticks/s"
+# Algorithmic bytes a ship-tick reads and writes in the minimal (this package's) layout, dynamical orientation on:
+# reads 229 B (pos, vel, goto, last_g 4 x 24; mass, time factor, warp length 3 x 8; radius, max_vel, agility, speed
+# fraction, follow range, max_ang_vel, rot_agility 7 x 4; ids, stamp, follow id, owner id, clock 5 x 8; mode,
+# follow_ptr 2 x 4; 5 flag bytes; rotation 16, angular velocity 12), writes 274 B (pos, vel, old_pos, old_vel, goto,
+# last_g 6 x 24; warp length 8, speed fraction and follow range 2 x 4, mode 4, stamp, follow id, owner id, clock
+# 4 x 8, follow_ptr 4, 2 flag bytes; rotation and old rotation 2 x 16, angular velocity, old angular velocity,
+# torque 3 x 12, roll 4).
+BYTES_PER_SHIP_TICK = 229 + 274
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _peaks() -> tuple:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms during the timed region (SM clock, throttle reasons)."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if self.proc is None or self.path is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        Path(self.path).unlink(missing_ok=True)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for k, name in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_sample(worlds: int, ships: int, seconds: float = 12.0) -> dict:
+    """The CPU oracle over a bounded sample of the workload on every host core: ship-ticks/s."""
+    from exact_ballpark_b200.workloads import flight_worlds
+    from oracle.park import OraclePark
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    w = flight_worlds(1, worlds, ships)
+    p = OraclePark(len(w.rows), dynamical_orientation=True, use_new_orbit=True)
+    p.load(w.rows)
+    w.apply(p)
+    p.evolve(threads=threads)
+    t0 = time.perf_counter()
+    k = 0
+    while time.perf_counter() - t0 < seconds:
+        p.evolve(threads=threads)
+        k += 1
+    dt = time.perf_counter() - t0
+    return {"value": len(w.rows) * k / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{worlds} worlds x {ships} ships, {k} ticks from tick 1 ({dt:.1f} s), C++ oracle "
+                      f"(oracle/flight.cpp), {threads} threads over disjoint worlds"}
+
+
+def run_reference(args, rank: int) -> None:
+    """The reference arm: the CPU port of the reference's algorithm on the whole workload, host cores, rank 0."""
+    if rank != 0:
+        return
+    from exact_ballpark_b200.workloads import flight_worlds
+    from oracle.park import OraclePark
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    w = flight_worlds(1, args.worlds, args.ships)
+    p = OraclePark(len(w.rows), dynamical_orientation=True, use_new_orbit=True)
+    p.load(w.rows)
+    w.apply(p)
+    for _ in range(args.warmup):
+        p.evolve(threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        p.evolve(threads=threads)
+    dt = time.perf_counter() - t0
+    value = len(w.rows) * args.steps / dt
+    sample = (f"{args.worlds} worlds x {args.ships} ships, {args.steps} ticks after {args.warmup}; the reference's "
+              f"algorithm as the C++ oracle (its implementation is Python), {threads} host threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32",
+            "data": "synthetic (seeded)", "config": _config(args, "CPU port of the reference algorithm"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _config(args, schedule: str) -> dict:
+    return {"workload": (f"flight-mode park, dynamical orientation on, new orbit law: {args.worlds} worlds x "
+                         f"{args.ships} ships (follow / orbit / warp), per-rank"),
+            "worlds_per_rank": args.worlds, "ships_per_world": args.ships, "schedule": schedule,
+            "parallelism": f"replicas x{args.gpus}", "l2": "flushed between timed steps (256 MiB write, untimed)"}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--worlds", type=int, default=65536)
+    ap.add_argument("--ships", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if world_size > 1:
+            import torch.distributed as dist
+            dist.init_process_group("gloo", init_method="env://")
+        run_reference(args, rank)
+        if world_size > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+
+    from exact_ballpark_b200 import ModesGraph, VecModesPark, tick_plain
+    from exact_ballpark_b200.workloads import flight_worlds
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world_size > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+
+    w = flight_worlds(rank + 1, args.worlds, args.ships)
+    n = len(w.rows)
+    park = VecModesPark(n, device=dev, dynamical_orientation=True, use_new_orbit=True)
+    park.load(w.rows)
+    w.apply(park)
+    plain = VecModesPark(n, device=dev, dynamical_orientation=True, use_new_orbit=True)
+    plain.load(w.rows)
+    w.apply(plain)
+    graph = ModesGraph(park)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(step, k: int) -> float:
+        total = 0.0
+        for _ in range(k):
+            flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step()
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        graph.tick()
+        tick_plain(plain)
+    barrier()
+    with Clocks(local) as clk:
+        barrier()
+        ms_tiled = timed(graph.tick, args.steps)
+        barrier()
+        ms_plain = timed(lambda: tick_plain(plain), args.steps)
+        barrier()
+    clocks = clk.summary()
+    ms_tiled, ms_plain = max_over_ranks(ms_tiled), max_over_ranks(ms_plain)
+    per_tiled, per_plain = ms_tiled / args.steps, ms_plain / args.steps
+
+    # e2e through the public API from host buffers
+    every = torch.ones(n, dtype=torch.bool, device=dev)
+    sf_host = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    sf_host.copy_(park.speed_fraction.cpu())
+    pos_host = torch.empty(n, 3, dtype=torch.float64, pin_memory=True)
+    sf_dev = torch.empty(n, dtype=torch.float64, device=dev)
+
+    def e2e_step():
+        sf_dev.copy_(sf_host, non_blocking=True)
+        park.set_speed_fraction(every, sf_dev)
+        graph.tick()
+        pos_host.copy_(park.pos, non_blocking=True)
+
+    for _ in range(3):
+        e2e_step()
+    barrier()
+    ms_e2e = max_over_ranks(timed(e2e_step, args.steps))
+    h2d, d2h = n * 8, n * 24
+
+    total_ships = n * world_size
+    value = total_ships * args.steps / (ms_tiled / 1e3)
+    peak, peak_kind = _peaks()
+    achieved = BYTES_PER_SHIP_TICK * n / (per_tiled / 1e3) / 1e9
+    traffic = None
+    tp = ROOT / "profiles" / "flight_tiled_traffic.json"
+    if tp.exists():
+        try:
+            t = json.loads(tp.read_text())
+            traffic = float(t["dram_bytes_per_ship_tick"]) * n
+        except Exception:
+            traffic = None
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": per_tiled, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64/f32", "data": "synthetic (seeded)",
+            "config": _config(args, "tiled: worlds packed in tiles, one block a tile, records in shared memory, one "
+                                    "launch, CUDA graph"),
+            "plain": {"value": total_ships * args.steps / (ms_plain / 1e3), "ms_per_step": per_plain,
+                      "schedule": "plain: records pass + tick, two launches, records in scratch"},
+            "speedup_tiled_vs_plain": per_plain / per_tiled,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "note": (f"algorithmic {BYTES_PER_SHIP_TICK} B/ship-tick x {n} ships per launch over the "
+                                  "tiled launch's CUDA-event time; the tick is FP64/FP32 issue- and latency-bound "
+                                  "(divides, square roots, libm, divergent torque searches), not HBM-bound")},
+            "e2e": {"value": total_ships * args.steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
+            "gpu_launches": 3 * args.steps, "clocks": clocks}
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(4096, args.ships)
+    if dist is not None:
+        del graph
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,60 @@
+"""The package's native library (libebb.so, built in-tree from csrc/ by exact_ballpark_b200.build), loaded once a
+process through ctypes, its entry points typed from include/ebb.h. There is no fallback: a missing or stale library
+raises."""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libebb.so"
+ABI = 1
+
+_lib = None
+
+
+class FlightState(ctypes.Structure):
+    """include/ebb.h's EbbFlightState, field for field."""
+    _fields_ = ([("n", ctypes.c_int64), ("friction", ctypes.c_double), ("dt", ctypes.c_double),
+                 ("ffriction", ctypes.c_float), ("fdt", ctypes.c_float), ("new_orbit", ctypes.c_int32),
+                 ("dynamical", ctypes.c_int32)]
+                + [(k, ctypes.c_void_p) for k in (
+                    "pos", "vel", "old_pos", "old_vel", "goto_pt", "last_g", "mass", "time_factor", "last_collision",
+                    "radius", "max_vel", "agility", "speed_fraction", "follow_range", "max_ang_vel", "rot_agility",
+                    "rot_roll", "rot", "old_rot", "ang_vel", "old_ang_vel", "torque", "ids", "effect_stamp",
+                    "follow_id", "owner_id", "clock", "mode", "follow_ptr", "free_", "moribund", "massive",
+                    "interactive", "sensor")])
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library (loaded and checked on first use)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`"
+                           " (the package has no CPU or library fallback)")
+    L = ctypes.CDLL(str(LIB_PATH))
+    if L.ebb_abi() != ABI:
+        raise RuntimeError(f"{LIB_PATH}: ABI {L.ebb_abi()} is not {ABI}; rebuild it")
+    p, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+    L.ebb_error_string.restype = ctypes.c_char_p
+    L.ebb_error_string.argtypes = [i32]
+    L.ebb_flight_scratch_bytes.restype = i64
+    L.ebb_flight_scratch_bytes.argtypes = [i64]
+    L.ebb_flight_tick.argtypes = [ctypes.POINTER(FlightState), p, i64, p, i32]
+    L.ebb_flight_tick_tiled.argtypes = [ctypes.POINTER(FlightState), p, i64, i32, p, p, i32, i32]
+    L.ebb_flight_snap.argtypes = [ctypes.POINTER(FlightState), p, i32, p, i32]
+    L.ebb_flight_decay.argtypes = [ctypes.POINTER(FlightState), p, ctypes.c_double, p, i32]
+    L.ebb_libm.argtypes = [i32, i64, p, p, p, p, i32]
+    L.ebb_kernel_info.argtypes = [i32] + [ctypes.POINTER(i32)] * 5
+    _lib = L
+    return L
+
+
+def check(rc: int, fn: str) -> None:
+    """Raise RuntimeError for a nonzero return code of entry point `fn`."""
+    if rc:
+        msg = lib().ebb_error_string(rc).decode()
+        raise RuntimeError(f"{fn} failed ({rc}: {msg})")

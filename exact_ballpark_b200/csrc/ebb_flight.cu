@@ -1,0 +1,501 @@
+// SPDX-License-Identifier: MIT
+// The flight-mode tick on sm_100a: the kernels behind include/ebb.h's ebb_flight_* entry points.
+//
+// A tick of Destiny's Ballpark::Evolve (modes.py:702-745) runs every world's live ships in ascending id: phase 1 (the
+// behaviours) reads other ships of the world as they stand at that moment, then phase 3 (the end-of-tick states) and
+// phase 4 (the commit). A ship's behaviour reads another ship only through three facts: its start-of-tick position,
+// its velocity after its own turn (STOP's vertical damping, once a release before its turn is known), and whether it
+// starts warp proper at its turn (then its followers are released: before their own turn when its id is lower, after
+// it otherwise). So a tick is two passes: the records pass writes those facts for every ship, then every ship runs
+// its whole tick independently, reading other ships only through the records, bit for bit the sequential order.
+//
+// Two schedules of the same per-ship code (ebb_flight.cuh):
+// - plain: the records pass and the tick as two launches over all rows, the records in caller scratch (global);
+// - tiled: worlds packed into tiles of whole worlds, one thread block a tile, a persistent grid; the records live in
+//   shared memory and both passes run in one launch (one __syncthreads between them), so a tick reads and writes
+//   each ship's state once and never touches scratch.
+#include <cuda_runtime.h>
+
+#include "../../include/ebb.h"
+#include "ebb_flight.cuh"
+
+namespace ebb {
+namespace flight {
+
+// ---- SoA access ----
+__device__ __forceinline__ D3 ld3(const double* p, int64_t i, int64_t n) { return D3{p[i], p[n + i], p[2 * n + i]}; }
+__device__ __forceinline__ void st3(double* p, int64_t i, int64_t n, D3 v) {
+    p[i] = v.x;
+    p[n + i] = v.y;
+    p[2 * n + i] = v.z;
+}
+__device__ __forceinline__ F3 ldf3(const float* p, int64_t i, int64_t n) { return F3{p[i], p[n + i], p[2 * n + i]}; }
+__device__ __forceinline__ void stf3(float* p, int64_t i, int64_t n, F3 v) {
+    p[i] = v.x;
+    p[n + i] = v.y;
+    p[2 * n + i] = v.z;
+}
+__device__ __forceinline__ F4 ldf4(const float* p, int64_t i, int64_t n) {
+    return F4{p[i], p[n + i], p[2 * n + i], p[3 * n + i]};
+}
+__device__ __forceinline__ void stf4(float* p, int64_t i, int64_t n, F4 v) {
+    p[i] = v.x;
+    p[n + i] = v.y;
+    p[2 * n + i] = v.z;
+    p[3 * n + i] = v.w;
+}
+
+__device__ __forceinline__ Cfg cfg_of(const EbbFlightState& s) {
+    return Cfg{s.friction, s.dt, s.ffriction, s.fdt, s.new_orbit, s.dynamical};
+}
+
+// Starts warp proper at its own turn this tick: free, live, aligning, aligned (its start state: nothing changes an
+// aligning ship's own state before its turn)
+__device__ __forceinline__ bool activates(const EbbFlightState& s, int64_t i) {
+    if (!s.free_[i] || s.moribund[i] || s.mode[i] != WARP || s.effect_stamp[i] >= 0) return false;
+    return aligned_for_warp(ld3(s.goto_pt, i, s.n), ld3(s.pos, i, s.n), ld3(s.vel, i, s.n), s.max_vel[i],
+                            s.effect_stamp[i]);
+}
+
+// A follower's membership in row t's set (StopAllFollowers' test, Ballpark.cpp:5433-5450): its follow_ptr is t and
+// its follow id t's id
+__device__ __forceinline__ bool member_of(const EbbFlightState& s, int64_t t, int64_t follow_id) {
+    return t >= 0 && t < s.n && s.ids[t] == follow_id;
+}
+
+// The records of row i: whether it starts warp proper, and its vertical velocity after its own turn
+__device__ __forceinline__ void records_of(const EbbFlightState& s, int64_t i, bool* act, double* vy_after) {
+    *act = activates(s, i);
+    double vy = s.vel[s.n + i];
+    if (s.free_[i] && !s.moribund[i] && !s.dynamical) {
+        int32_t m = s.mode[i];
+        const int64_t t = s.follow_ptr[i];
+        if (member_of(s, t, s.follow_id[i]) && s.ids[t] < s.ids[i] && activates(s, t)) {
+            Ship f;                                                   // released before its own turn
+            f.mode = m;
+            f.interactive = s.interactive[i] != 0;
+            f.vel = ld3(s.vel, i, s.n);
+            f.pos = ld3(s.pos, i, s.n);
+            m = release(f, false);
+        }
+        if (m == STOP) vy = dmul(dsub(vy, dmul(STOP_DECAY, vy)), STOP_DAMP);
+    }
+    *vy_after = vy;
+}
+
+// What a ship's tick reads of another ship: the records and its id and radius
+struct View {
+    D3 pos, vel;
+    double vy_after;
+    int64_t id;
+    float radius;
+    bool act, valid;
+};
+
+// One ship's whole tick in place (phase 1, 3, 4, PetrifyTroll, the clock); `tgt` is its follow_ptr's view (valid
+// false when it has none), `act_self` its own record
+__device__ __forceinline__ void tick_ship(const EbbFlightState& s, int64_t i, const View& tgt, bool act_self) {
+    const int64_t n = s.n;
+    const Cfg c = cfg_of(s);
+    Ship b;
+    b.pos = ld3(s.pos, i, n);
+    b.vel = ld3(s.vel, i, n);
+    b.gp = ld3(s.goto_pt, i, n);
+    b.last_g = ld3(s.last_g, i, n);
+    b.mass = s.mass[i];
+    b.tf = s.time_factor[i];
+    b.last_collision = s.last_collision[i];
+    b.radius = s.radius[i];
+    b.max_vel = s.max_vel[i];
+    b.agility = s.agility[i];
+    b.sf = s.speed_fraction[i];
+    b.follow_range = s.follow_range[i];
+    b.id = s.ids[i];
+    b.mode = s.mode[i];
+    b.effect_stamp = s.effect_stamp[i];
+    b.follow_id = s.follow_id[i];
+    b.owner_id = s.owner_id[i];
+    b.follow_ptr = s.follow_ptr[i];
+    b.clock = s.clock[i];
+    b.massive = s.massive[i] != 0;
+    b.interactive = s.interactive[i] != 0;
+    b.sensor = s.sensor[i] != 0;
+    const bool live = s.free_[i] && !s.moribund[i];
+    // ---- phase 1: the release when the target starts warp proper (before or after this ship's turn), the
+    // behaviour, dynamical orientation
+    bool release_after = false;
+    if (tgt.valid && tgt.id == b.follow_id && tgt.act) {
+        if (tgt.id < b.id) release(b, true);
+        else release_after = true;
+    }
+    F3 torque = F3{0.0f, 0.0f, 0.0f};
+    float roll = 0.0f;
+    F4 r0 = q_identity(), rot1 = r0;
+    F3 w0 = F3{0.0f, 0.0f, 0.0f}, w1 = w0;
+    if (live) {
+        D3 a = D3{0.0, 0.0, 0.0};
+        if (s.dynamical) {
+            r0 = ldf4(s.rot, i, n);
+            w0 = ldf3(s.ang_vel, i, n);
+        }
+        if (b.mode == WARP) {                                         // EvolveWarp (modes.py:379)
+            if (b.effect_stamp >= 0) {
+                a = D3{0.0, 0.0, 0.0};
+            } else if (act_self) {
+                start_warp(b);
+            } else {
+                b.effect_stamp -= 1;
+                a = goto_thrust(b, b.gp, c);
+            }
+        } else if (b.mode == GOTO) {
+            a = goto_thrust(b, b.gp, c);
+        } else if ((b.mode == FOLLOW || b.mode == ORBIT) && !tgt.valid) {
+            a = D3{0.0, 0.0, 0.0};                                    // no target row: the park never leaves one so
+        } else if (b.mode == FOLLOW) {
+            a = follow_thrust(b, tgt.pos, tgt.radius, c);
+        } else if (b.mode == ORBIT) {
+            if (c.new_orbit) {
+                D3 tv = tgt.vel;
+                if (tgt.id < b.id) tv.y = tgt.vy_after;               // the target's turn came first
+                a = new_orbit_thrust(b, tgt.pos, tv, tgt.radius, c, r0);
+            } else {
+                a = old_orbit_thrust(b, tgt.pos, tgt.radius, c);
+            }
+        } else if (b.mode == STOP) {
+            if (!c.dynamical) b.vel.y = dmul(dsub(b.vel.y, dmul(STOP_DECAY, b.vel.y)), STOP_DAMP);
+        }                                                             // BOID, MINIBALL, FIELD, RIGID, TROLL: none
+        if (c.dynamical) a = orient(b, a, s.max_ang_vel[i], s.rot_agility[i], r0, w0, c, &torque, &roll, &rot1, &w1);
+        b.last_g = a;
+    }
+    if (release_after) release(b, true);
+    // ---- phases 3 and 4
+    if (live) {
+        if (b.massive) b.last_collision = -1.0;                       // the gradient without neighbours
+        D3 p = b.pos, v = b.vel;
+        const D3 a = D3{dadd(b.last_g.x, 0.0), dadd(b.last_g.y, 0.0), dadd(b.last_g.z, 0.0)};   // mLastG + mLastC
+        const double m = dmul(b.mass, tod(b.agility));
+        if (b.mode == WARP && b.effect_stamp >= 0) {
+            if (warp_path(b, &p, &v, dmul(i2d(b.clock - b.effect_stamp), c.dt))) {
+                b.massive = true;                                     // dropped out: massive and sensing again, Stop
+                b.sensor = true;
+                b.mode = STOP;
+                b.pos = p;                                            // TRV-714: the drop-out point is the old state
+                b.vel = v;
+                integrate(&p, &v, a, m, c.friction, b.tf, c.dt);
+            }
+        } else {
+            integrate(&p, &v, a, m, c.friction, b.tf, c.dt);
+        }
+        st3(s.old_pos, i, n, b.pos);
+        st3(s.old_vel, i, n, b.vel);
+        b.pos = p;
+        b.vel = v;
+        if (c.dynamical) {                                            // the commit: the new values where finite
+            const bool rot_ok = ffinite(q_lensq(rot1));
+            const bool w_ok = ffinite(f3_dot(w1, w1));
+            stf4(s.rot, i, n, rot_ok ? rot1 : r0);
+            stf4(s.old_rot, i, n, rot_ok ? r0 : rot1);
+            stf3(s.ang_vel, i, n, w_ok ? w1 : w0);
+            stf3(s.old_ang_vel, i, n, w_ok ? w0 : w1);
+            stf3(s.torque, i, n, torque);
+            s.rot_roll[i] = roll;
+        }
+        if (b.mode == TROLL && !(b.effect_stamp > b.clock)) {
+            // PetrifyTroll (full.py:1800) of a troll due: fixed, at rest (velocity and old velocity), mLastG cleared,
+            // non-interactive, RIGID; only this ship's fields, which no other ship reads this tick
+            b.vel = D3{0.0, 0.0, 0.0};
+            st3(s.old_vel, i, n, b.vel);
+            b.last_g = D3{0.0, 0.0, 0.0};
+            s.free_[i] = 0;
+            s.interactive[i] = 0;
+            b.mode = RIGID;
+        }
+    }
+    st3(s.pos, i, n, b.pos);
+    st3(s.vel, i, n, b.vel);
+    st3(s.goto_pt, i, n, b.gp);
+    st3(s.last_g, i, n, b.last_g);
+    s.last_collision[i] = b.last_collision;
+    s.speed_fraction[i] = b.sf;
+    s.follow_range[i] = b.follow_range;
+    s.mode[i] = b.mode;
+    s.effect_stamp[i] = b.effect_stamp;
+    s.follow_id[i] = b.follow_id;
+    s.owner_id[i] = b.owner_id;
+    s.follow_ptr[i] = b.follow_ptr;
+    s.clock[i] = b.clock + 1;
+    s.massive[i] = b.massive ? 1 : 0;
+    s.sensor[i] = b.sensor ? 1 : 0;
+}
+
+// ================================================================================================ plain schedule
+
+struct Records {
+    double *pos, *vel, *vy;                                           // [3][n], [3][n], [n]
+    uint8_t* act;                                                     // [n]
+};
+
+__host__ __device__ inline int64_t align256(int64_t b) { return (b + 255) & ~(int64_t)255; }
+
+__host__ __device__ inline Records records_in(void* scratch, int64_t n) {
+    char* p = (char*)scratch;
+    Records r;
+    r.pos = (double*)p;
+    p += align256(3 * n * 8);
+    r.vel = (double*)p;
+    p += align256(3 * n * 8);
+    r.vy = (double*)p;
+    p += align256(n * 8);
+    r.act = (uint8_t*)p;
+    return r;
+}
+
+__host__ __device__ inline int64_t records_bytes(int64_t n) {
+    return align256(3 * n * 8) * 2 + align256(n * 8) + align256(n);
+}
+
+__global__ void __launch_bounds__(256) records_kernel(EbbFlightState s, Records r) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n) return;
+    bool act;
+    double vy;
+    records_of(s, i, &act, &vy);
+    r.act[i] = act ? 1 : 0;
+    r.vy[i] = vy;
+    st3(r.pos, i, s.n, ld3(s.pos, i, s.n));
+    st3(r.vel, i, s.n, ld3(s.vel, i, s.n));
+}
+
+__global__ void __launch_bounds__(256) tick_kernel(EbbFlightState s, Records r) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n) return;
+    View tgt;
+    const int64_t t = s.follow_ptr[i];
+    tgt.valid = t >= 0 && t < s.n;
+    if (tgt.valid) {
+        tgt.pos = ld3(r.pos, t, s.n);
+        tgt.vel = ld3(r.vel, t, s.n);
+        tgt.vy_after = r.vy[t];
+        tgt.id = s.ids[t];
+        tgt.radius = s.radius[t];
+        tgt.act = r.act[t] != 0;
+    } else {
+        tgt.act = false;
+        tgt.id = 0;
+    }
+    tick_ship(s, i, tgt, r.act[i] != 0);
+}
+
+// ================================================================================================ tiled schedule
+
+// The tiled tick's shared records: one slot a row of the tile
+struct SlotRec {
+    double px, py, pz, vx, vy, vz, vy_after;
+    int64_t id;
+    float radius;
+    int32_t act;
+};
+
+__global__ void __launch_bounds__(1024) tiled_kernel(EbbFlightState s, const int64_t* __restrict__ tile_rows,
+                                                     int64_t tiles, int32_t* status) {
+    extern __shared__ SlotRec rec[];
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int64_t r0 = tile_rows[tile], r1 = tile_rows[tile + 1];
+        const int64_t i = r0 + threadIdx.x;
+        const bool mine = i < r1;
+        bool act = false;
+        if (mine) {                                                   // the records pass, into shared memory
+            double vy_after;
+            records_of(s, i, &act, &vy_after);
+            SlotRec& q = rec[threadIdx.x];
+            const D3 p = ld3(s.pos, i, s.n), v = ld3(s.vel, i, s.n);
+            q.px = p.x;
+            q.py = p.y;
+            q.pz = p.z;
+            q.vx = v.x;
+            q.vy = v.y;
+            q.vz = v.z;
+            q.vy_after = vy_after;
+            q.id = s.ids[i];
+            q.radius = s.radius[i];
+            q.act = act ? 1 : 0;
+        }
+        __syncthreads();
+        if (mine) {
+            View tgt;
+            const int64_t t = s.follow_ptr[i];
+            tgt.valid = t >= r0 && t < r1;
+            if (!tgt.valid && t >= 0 && t < s.n) atomicOr(status, 1);    // a target outside its world's tile
+            if (tgt.valid) {
+                const SlotRec& q = rec[t - r0];
+                tgt.pos = D3{q.px, q.py, q.pz};
+                tgt.vel = D3{q.vx, q.vy, q.vz};
+                tgt.vy_after = q.vy_after;
+                tgt.id = q.id;
+                tgt.radius = q.radius;
+                tgt.act = q.act != 0;
+            } else {
+                tgt.act = false;
+                tgt.id = 0;
+            }
+            tick_ship(s, i, tgt, act);
+        }
+        __syncthreads();                                              // the slots are the next tile's
+    }
+}
+
+// ================================================================================================ set-up kernels
+
+__global__ void snap_kernel(EbbFlightState s, const uint8_t* __restrict__ mask, int fresh) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n || !mask[i]) return;
+    const int64_t n = s.n;
+    if (fresh) {                                                      // a new ball: mOldRot = rot x RotationQ(w, -dt|w|)
+        const F4 rot = q_identity();
+        const F3 w = ldf3(s.ang_vel, i, n);
+        const F4 back = q_axis_angle(w, tof(dmul(dneg((double)s.fdt), tod(f3_len(w)))));
+        stf4(s.rot, i, n, rot);
+        stf4(s.old_rot, i, n, q_mul(rot, back));
+    }
+    const D3 v = ld3(s.vel, i, n);
+    if (!(d3_lensq(v) > 1e-12)) return;
+    const F4 r = snap_rotation(v);
+    stf4(s.rot, i, n, r);
+    stf4(s.old_rot, i, n, r);
+    stf3(s.ang_vel, i, n, F3{0.0f, 0.0f, 0.0f});
+    stf3(s.old_ang_vel, i, n, F3{0.0f, 0.0f, 0.0f});
+}
+
+__global__ void decay_kernel(EbbFlightState s, const uint8_t* __restrict__ mask, double neg_kdt) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n || !mask[i]) return;
+    const double m = dmul(s.mass[i], tod(s.agility[i]));
+    s.time_factor[i] = (m <= 0.0) ? 0.0 : lm::exp(ddiv(neg_kdt, m));
+}
+
+__global__ void libm_kernel(int func, int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                            double* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double a = x[i];
+    double sn, cs;
+    switch (func) {
+        case 0: out[i] = lm::sin(a); break;
+        case 1: out[i] = lm::cos(a); break;
+        case 2: out[i] = lm::log(a); break;
+        case 3: out[i] = lm::exp(a); break;
+        case 4: lm::sincos(a, &sn, &cs); out[i] = sn; break;
+        case 5: lm::sincos(a, &sn, &cs); out[i] = cs; break;
+        case 6: out[i] = lm::pow(a, y[i]); break;
+        case 10: out[i] = tod(lm::expf(tof(a))); break;
+        case 11: out[i] = tod(lm::logf(tof(a))); break;
+        case 12: out[i] = tod(lm::sinf(tof(a))); break;
+        case 13: out[i] = tod(lm::cosf(tof(a))); break;
+        case 14: out[i] = tod(lm::acosf(tof(a))); break;
+        case 15: out[i] = tod(lm::atanf(tof(a))); break;
+        case 16: out[i] = tod(lm::atan2f(tof(y[i]), tof(a))); break;
+        default: out[i] = dnan(); break;
+    }
+}
+
+}  // namespace flight
+}  // namespace ebb
+
+// ==================================================================================================== the C ABI
+
+namespace {
+int launched() {
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : (int)e;
+}
+bool block_ok(int block, int max_block) { return block > 0 && block <= max_block && block % 32 == 0; }
+unsigned grid_of(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
+}  // namespace
+
+extern "C" {
+
+int ebb_abi(void) { return EBB_ABI_VERSION; }
+
+const char* ebb_error_string(int code) {
+    if (code == EBB_EINVAL) return "refused: invalid arguments (block size, scratch, tiles)";
+    return cudaGetErrorString((cudaError_t)code);
+}
+
+int64_t ebb_flight_scratch_bytes(int64_t n) { return n <= 0 ? 0 : ebb::flight::records_bytes(n); }
+
+int ebb_flight_tick(const EbbFlightState* s, void* scratch, int64_t scratch_bytes, void* stream, int block) {
+    if (s == nullptr) return EBB_EINVAL;
+    if (s->n <= 0) return 0;
+    if (!block_ok(block, 256) || scratch == nullptr || ((uintptr_t)scratch & 255) != 0 ||
+        scratch_bytes < ebb_flight_scratch_bytes(s->n))
+        return EBB_EINVAL;
+    const ebb::flight::Records r = ebb::flight::records_in(scratch, s->n);
+    const cudaStream_t st = (cudaStream_t)stream;
+    ebb::flight::records_kernel<<<grid_of(s->n, block), block, 0, st>>>(*s, r);
+    int rc = launched();
+    if (rc) return rc;
+    ebb::flight::tick_kernel<<<grid_of(s->n, block), block, 0, st>>>(*s, r);
+    return launched();
+}
+
+int ebb_flight_tick_tiled(const EbbFlightState* s, const int64_t* tile_rows, int64_t tiles, int tile_cap,
+                          int32_t* status, void* stream, int block, int grid) {
+    if (s == nullptr) return EBB_EINVAL;
+    if (s->n <= 0 || tiles <= 0) return 0;
+    if (!block_ok(block, 1024) || tile_cap <= 0 || tile_cap > block || tile_rows == nullptr || status == nullptr ||
+        grid <= 0)
+        return EBB_EINVAL;
+    const size_t smem = (size_t)block * sizeof(ebb::flight::SlotRec);
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(ebb::flight::tiled_kernel,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
+    ebb::flight::tiled_kernel<<<(unsigned)grid, block, smem, (cudaStream_t)stream>>>(*s, tile_rows, tiles, status);
+    return launched();
+}
+
+int ebb_flight_snap(const EbbFlightState* s, const uint8_t* mask, int fresh, void* stream, int block) {
+    if (s == nullptr || mask == nullptr) return EBB_EINVAL;
+    if (s->n <= 0) return 0;
+    if (!block_ok(block, 1024)) return EBB_EINVAL;
+    ebb::flight::snap_kernel<<<grid_of(s->n, block), block, 0, (cudaStream_t)stream>>>(*s, mask, fresh);
+    return launched();
+}
+
+int ebb_flight_decay(const EbbFlightState* s, const uint8_t* mask, double neg_kdt, void* stream, int block) {
+    if (s == nullptr || mask == nullptr) return EBB_EINVAL;
+    if (s->n <= 0) return 0;
+    if (!block_ok(block, 1024)) return EBB_EINVAL;
+    ebb::flight::decay_kernel<<<grid_of(s->n, block), block, 0, (cudaStream_t)stream>>>(*s, mask, neg_kdt);
+    return launched();
+}
+
+int ebb_libm(int func, int64_t n, const double* x, const double* y, double* out, void* stream, int block) {
+    if (n <= 0) return 0;
+    if (!block_ok(block, 1024) || x == nullptr || out == nullptr) return EBB_EINVAL;
+    if (!((func >= 0 && func <= 6) || (func >= 10 && func <= 16))) return EBB_EINVAL;
+    if ((func == 6 || func == 16) && y == nullptr) return EBB_EINVAL;
+    ebb::flight::libm_kernel<<<grid_of(n, block), block, 0, (cudaStream_t)stream>>>(func, n, x, y, out);
+    return launched();
+}
+
+int ebb_kernel_info(int which, int* regs, int* local_bytes, int* binary_version, int* ptx_version, int* max_threads) {
+    cudaFuncAttributes fa;
+    cudaError_t e;
+    switch (which) {
+        case 0: e = cudaFuncGetAttributes(&fa, ebb::flight::tick_kernel); break;
+        case 1: e = cudaFuncGetAttributes(&fa, ebb::flight::records_kernel); break;
+        case 2: e = cudaFuncGetAttributes(&fa, ebb::flight::tiled_kernel); break;
+        default: return EBB_EINVAL;
+    }
+    if (e != cudaSuccess) return (int)e;
+    *regs = fa.numRegs;
+    *local_bytes = (int)fa.localSizeBytes;
+    *binary_version = fa.binaryVersion;
+    *ptx_version = fa.ptxVersion;
+    *max_threads = fa.maxThreadsPerBlock;
+    return 0;
+}
+
+}  // extern "C"

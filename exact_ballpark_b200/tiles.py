@@ -1,0 +1,81 @@
+"""Packing worlds into tiles for the tiled (ragged, persistent) tick, and the plan's autotuned shape.
+
+A tile is a run of whole worlds, at most `cap` rows, handled by one thread block of `block` threads (one thread a
+row, the records of the tile in shared memory). Worlds of any size pack with no padding between them: the tile
+table is the row offsets of the tiles (tile_rows[t] .. tile_rows[t + 1]). The grid is persistent: `grid` blocks take
+the tiles in turn (grid = tiles is one block a tile).
+
+`plan_tiles` needs each world's rows contiguous (a world's rows one run, every world one run); otherwise it returns
+None and the park ticks with the plain schedule. The shape (cap, block, grid) is chosen by `autotune`, which times
+the candidates on the park itself and keeps the fastest (exact_ballpark_b200.autotune).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import torch
+
+DEFAULT_CAP = 128
+
+
+@dataclass
+class TilePlan:
+    tile_rows: list            # tiles + 1 row offsets
+    cap: int                   # rows a tile holds at most
+    block: int                 # threads a block (>= cap, a multiple of 32)
+    grid: int                  # blocks of the persistent grid
+    max_world: int             # the largest world's rows
+    _dev: dict = field(default_factory=dict, repr=False)
+
+    @property
+    def tiles(self) -> int:
+        return len(self.tile_rows) - 1
+
+    def tile_rows_on(self, dev) -> torch.Tensor:
+        key = str(dev)
+        if key not in self._dev:
+            self._dev[key] = torch.tensor(self.tile_rows, dtype=torch.int64, device=dev)
+        return self._dev[key]
+
+
+def world_runs(world: torch.Tensor) -> list | None:
+    """The row offsets of the worlds' runs ([0, ..., n]) when every world is one contiguous run, else None."""
+    w = world.detach().to("cpu", torch.int64)
+    n = int(w.numel())
+    if n == 0:
+        return [0]
+    change = torch.nonzero(w[1:] != w[:-1]).reshape(-1) + 1
+    starts = [0] + change.tolist()
+    if len(starts) != int(torch.unique(w).numel()):
+        return None
+    return starts + [n]
+
+
+def pack(runs: list, cap: int) -> list:
+    """Greedy packing of consecutive world runs into tiles of at most cap rows (a world never split; every world at
+    most cap rows)."""
+    out = [runs[0]]
+    for k in range(1, len(runs)):
+        if runs[k] - out[-1] > cap:                  # world k-1 does not fit: the tile closes before it
+            out.append(runs[k - 1])
+    if out[-1] != runs[-1]:
+        out.append(runs[-1])
+    return out
+
+
+def plan_tiles(world: torch.Tensor, cap: int = DEFAULT_CAP, block: int | None = None, grid: int | None = None):
+    """The tile plan for a park's world column, or None when its worlds are not contiguous runs or a world is larger
+    than 1024 rows."""
+    runs = world_runs(world)
+    if runs is None or len(runs) < 2:
+        return None
+    max_world = max(b - a for a, b in zip(runs[:-1], runs[1:]))
+    if max_world > 1024:
+        return None
+    cap = max(cap, max_world)
+    tile_rows = pack(runs, cap)
+    blk = block or ((cap + 31) // 32) * 32
+    if blk < cap:
+        raise ValueError(f"block {blk} < cap {cap}")
+    return TilePlan(tile_rows, cap, blk, grid or (len(tile_rows) - 1), max_world)

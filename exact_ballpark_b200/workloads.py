@@ -1,0 +1,94 @@
+"""Seeded synthetic worlds for the flight-mode park: the batched destiny tick's benchmark and parity workloads.
+
+`flight_worlds` builds W independent worlds of S ships each, every world from its own seed (base seed + world
+index), in the shape the flight-mode benchmark is quoted on: positions uniform in a +-50 km cube, at rest; maximum
+velocity log-uniform in [100, 3000] m/s; mass log-uniform in [1e6, 1e9] kg; agility uniform in [0.1, 5]; radius
+uniform in [20, 500] m; each ship FOLLOW, ORBIT or WARP uniformly at random. A follower or orbiter targets a uniform
+other ship of its world at a range uniform in [500, 30,000] m; a warper aims at a point 10^U(8, 11) m away in a
+uniform direction, with the thunker's minimum range (20 km) and a warp factor uniform in [3000, 10000] (the
+reference's flight benchmark's span). Half the ships are interactive (an interactive orbiter flies on when its
+target warps off). Dynamical orientation's turning values are Destiny's defaults.
+
+The worlds are plain data (`rows`, and the commands as row masks and values), applied through the park's public
+API (`apply`), so the same world can be run by any implementation of that API.
+"""
+
+from __future__ import annotations
+
+import math
+import random
+from dataclasses import dataclass
+
+import torch
+
+FOLLOW, ORBIT, WARP = 1, 4, 3          # Destiny's DSTBALL_FOLLOW, DSTBALL_ORBIT, DSTBALL_WARP
+
+
+@dataclass
+class FlightWorlds:
+    rows: list                          # load() rows, world-major, ships in id order
+    follow_mask: list
+    orbit_mask: list
+    warp_mask: list
+    target: list                        # the target's row (followers and orbiters), -1 otherwise
+    range_: list
+    point: list                         # the warp point ([x, y, z]), zeros otherwise
+    warp_factor: list
+    worlds: int
+    ships: int
+
+    def apply(self, park) -> None:
+        """The initial commands, through the park's API: FollowBall, Orbit and WarpTo on their rows."""
+        dev = park.dev
+        b = lambda xs: torch.tensor(xs, dtype=torch.bool, device=dev)
+        target = torch.tensor(self.target, dtype=torch.int64, device=dev)
+        rng = torch.tensor(self.range_, dtype=torch.float64, device=dev)
+        point = torch.tensor(self.point, dtype=torch.float64, device=dev)
+        wf = torch.tensor(self.warp_factor, dtype=torch.int64, device=dev)
+        park.follow(b(self.follow_mask), target, rng)
+        park.orbit(b(self.orbit_mask), target, rng)
+        park.warp_to(b(self.warp_mask), point, torch.full_like(rng, 20000.0), wf)
+
+
+def _unit(r: random.Random) -> list:
+    while True:
+        v = [r.gauss(0.0, 1.0) for _ in range(3)]
+        n = math.sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+        if n > 1e-9:
+            return [c / n for c in v]
+
+
+def flight_worlds(seed: int, worlds: int, ships: int = 4) -> FlightWorlds:
+    """W worlds of S ships (module docstring); world w is drawn from random.Random(seed * 1_000_003 + w)."""
+    rows, fm, om, wm, tgt, rg, pt, wf = [], [], [], [], [], [], [], []
+    for w in range(worlds):
+        r = random.Random(seed * 1_000_003 + w)
+        base = w * ships
+        for j in range(ships):
+            rows.append({
+                "id": base + j + 1, "world": w, "time": 0,
+                "mass": 10.0 ** r.uniform(6.0, 9.0), "radius": r.uniform(20.0, 500.0),
+                "max_vel": 10.0 ** r.uniform(2.0, math.log10(3000.0)),
+                "pos": [r.uniform(-5e4, 5e4) for _ in range(3)], "vel": [0.0, 0.0, 0.0],
+                "agility": r.uniform(0.1, 5.0), "speed_fraction": 1.0, "free": True, "massive": False,
+                "interactive": r.random() < 0.5,
+            })
+            mode = r.choice((FOLLOW, ORBIT, WARP)) if ships > 1 else WARP
+            fm.append(mode == FOLLOW)
+            om.append(mode == ORBIT)
+            wm.append(mode == WARP)
+            if mode in (FOLLOW, ORBIT):
+                other = r.randrange(ships - 1)
+                tgt.append(base + (other if other < j else other + 1))
+                rg.append(r.uniform(500.0, 30000.0))
+                pt.append([0.0, 0.0, 0.0])
+                wf.append(0)
+            else:
+                d = 10.0 ** r.uniform(8.0, 11.0)
+                u = _unit(r)
+                p = rows[-1]["pos"]
+                tgt.append(-1)
+                rg.append(0.0)
+                pt.append([p[0] + u[0] * d, p[1] + u[1] * d, p[2] + u[2] * d])
+                wf.append(r.randint(3000, 10000))
+    return FlightWorlds(rows, fm, om, wm, tgt, rg, pt, wf, worlds, ships)

@@ -1,0 +1,94 @@
+/* exact-ballpark-b200: the C ABI of the batched destiny tick on sm_100a.
+ *
+ * Plain C: pointers and sizes, no torch types. Every entry point launches on the caller's CUDA stream, allocates
+ * nothing and never synchronises the host, so a caller may capture it in a CUDA graph. Return codes: 0 success;
+ * EBB_EINVAL (-1) for refused arguments (nothing launched); a positive value is a cudaError_t from the launch
+ * (ebb_error_string names it). Device-side domain problems are reported through the status word some calls take.
+ *
+ * The flight-mode park's state is structure-of-arrays in device memory: a vector field is 3 (or 4) consecutive
+ * planes of n values (x plane, y plane, z plane); Destiny's float members are stored as float, its doubles as
+ * double. The reference keeps the same state as [n, 3] float64 tensors (exact_ballpark/vec_modes_cuda.py:280-290).
+ */
+#ifndef EBB_H
+#define EBB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EBB_ABI_VERSION 1
+#define EBB_EINVAL (-1)
+
+/* The flight-mode park (one row a ship; rows grouped in worlds by the caller), field for field the state the
+ * reference's xbpm_tick reads and writes (exact_ballpark/vec_modes_cuda.cu:83-96), laid out as above. */
+typedef struct EbbFlightState {
+    int64_t n;
+    double friction, dt;          /* k and the tick in seconds */
+    float ffriction, fdt;         /* the same as C floats */
+    int32_t new_orbit;            /* Destiny's process-global useNewOrbit */
+    int32_t dynamical;            /* dynamical orientation on */
+    double *pos, *vel, *old_pos, *old_vel, *goto_pt, *last_g;   /* [3][n] */
+    double *mass, *time_factor, *last_collision;               /* [n] */
+    float *radius, *max_vel, *agility, *speed_fraction, *follow_range, *max_ang_vel, *rot_agility, *rot_roll;
+    float *rot, *old_rot;                                      /* [4][n] x, y, z, w */
+    float *ang_vel, *old_ang_vel, *torque;                     /* [3][n] */
+    int64_t *ids, *effect_stamp, *follow_id, *owner_id, *clock;
+    int32_t *mode, *follow_ptr;                                /* follow_ptr: the target's row, -1 for none */
+    uint8_t *free_, *moribund, *massive, *interactive, *sensor;
+} EbbFlightState;
+
+/* The ABI version (EBB_ABI_VERSION). Replaces xbpm_abi / xbpo_abi (exact_ballpark/vec_modes_cuda.cu:750,
+ * vec_orient_cuda.cu:499). */
+int ebb_abi(void);
+
+/* A cudaError_t's name, for a positive return code. Replaces xbpo_error_string (vec_orient_cuda.cu:503). */
+const char* ebb_error_string(int code);
+
+/* Bytes of device scratch ebb_flight_tick needs for n rows (the prepass's records). */
+int64_t ebb_flight_scratch_bytes(int64_t n);
+
+/* One tick of every world of the park in place: the prepass (each ship's start-of-tick position and velocity, its
+ * vertical velocity after its own turn, whether it starts warp proper) into `scratch`, then each ship's tick (phase 1,
+ * phase 3, phase 4, PetrifyTroll, its world's clock), one thread a ship. `scratch` holds at least
+ * ebb_flight_scratch_bytes(n) bytes of device memory, 256-byte aligned; block is a multiple of 32 up to 1024.
+ * Replaces xbpm_tick (exact_ballpark/vec_modes_cuda.cu:754), which exact_ballpark.vec_modes_cuda.tick calls
+ * (vec_modes_cuda.py:322). */
+int ebb_flight_tick(const EbbFlightState* s, void* scratch, int64_t scratch_bytes, void* stream, int block);
+
+/* The same tick with the worlds packed into tiles, one thread block a tile, the prepass's records in shared memory
+ * (no scratch, one launch): tile_rows[0..tiles] are row offsets, each tile a run of whole worlds of at most
+ * `tile_cap` rows, rows of a world contiguous; block >= tile_cap. status[0] is set nonzero if a follow_ptr leaves
+ * its tile (the ship is then ticked without its target, as a missing target). The grid is persistent: `grid` blocks
+ * take tiles in turn. The worlds-per-tile packing and block are the autotuner's choice
+ * (exact_ballpark_b200.tiles). No counterpart in the reference (its tick is two launches, xbpm_tick). */
+int ebb_flight_tick_tiled(const EbbFlightState* s, const int64_t* tile_rows, int64_t tiles, int tile_cap,
+                          int32_t* status, void* stream, int block, int grid);
+
+/* SnapOrientation of the rows in mask[n] (nonzero bytes): the rotation turned to the velocity and rolled upright,
+ * the old rotation the same, the angular velocities zeroed (at a speed of 1e-6 m/s or less nothing changes). With
+ * `fresh`, first the state of a new ball: rotation identity, old rotation rot x RotationQuaternion(angVel,
+ * -dt |angVel|), angular velocities kept. Replaces VecOrientPark._snap_orientation and the load's mOldRot
+ * (exact_ballpark/vec_orient.py:556, vec_modes.py:256-264). */
+int ebb_flight_snap(const EbbFlightState* s, const uint8_t* mask, int fresh, void* stream, int block);
+
+/* SetBallTimeFactor for the rows in mask[n]: time_factor = 0 if mass x agility <= 0, else exp(neg_kdt / (mass x
+ * agility)) with glibc's exp, neg_kdt = -friction x dt. Replaces VecOrientPark._decay (vec_orient.py:376). */
+int ebb_flight_decay(const EbbFlightState* s, const uint8_t* mask, double neg_kdt, void* stream, int block);
+
+/* glibc 2.34 aarch64's function `func` elementwise on the device, for the tests: 0 sin, 1 cos, 2 log, 3 exp,
+ * 4 sincos's sine, 5 sincos's cosine, 6 pow(x, y); 10 expf, 11 logf, 12 sinf, 13 cosf, 14 acosf, 15 atanf,
+ * 16 atan2f(y, x) (floats held in doubles). Replaces xbpm_dlibm and xbpo_libm (vec_modes_cuda.cu:779,
+ * vec_orient_cuda.cu:520). */
+int ebb_libm(int func, int64_t n, const double* x, const double* y, double* out, void* stream, int block);
+
+/* A kernel's resources as loaded on the current device: which 0 the plain tick, 1 the prepass, 2 the tiled tick.
+ * Replaces xbpm_info (vec_modes_cuda.cu:766). */
+int ebb_kernel_info(int which, int* regs, int* local_bytes, int* binary_version, int* ptx_version, int* max_threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EBB_H */

@@ -1,0 +1,233 @@
+"""Generates the golden fixtures under tests/golden/ from the reference itself (run where the reference is checked
+out; nothing on a GPU box runs this):
+
+    EXACT_BALLPARK_REF=<checkout of exact-ballpark> python tests/golden/make_golden.py [--only libm|traces]
+
+1. libm.npz: inputs and outputs of glibc 2.34 aarch64's functions as the reference transcribes them (dlibm.sin,
+   cos, sincos, log; vec_exp.exp; vec_libm.expf, logf, sinf, cosf, acosf, atanf, atan2f, pow), on seeded random
+   arguments over each function's branches plus the edge cases (zeros, infinities, NaN, subnormals, the branch
+   bounds, sincos's odd point +-0x1.ad1fb54442d18p+0).
+2. trace_*.json.gz / .npz: the flight-mode park's scenarios as golden traces (tests/golden/trace.py), recorded on
+   the reference's batched park (VecModesPark, CPU tick):
+   - mc{1,2}: the reference's own mode_cases scenarios (tests/mode_cases.py; seed 1 development, 2 held out),
+     driven by its own modes_batch.batched_modes: FOLLOW, ORBIT under both laws, WARP and its transitions,
+     EntityWarpIn, the guards, mixed worlds (no dynamical orientation);
+   - fc{1,2}: the reference's flight_cases scenarios (tests/flight_cases.py) driven by modes_batch.batched_full:
+     the modes with dynamical orientation on and off and every setter in flight;
+   - w0_*: flight_worlds(seed, 64 worlds x 4 ships), 200 ticks, dynamical orientation on, each orbit law, and one
+     run without dynamical orientation.
+   Before recording, a sample of each scenario family is checked against the reference's scalar transcriptions
+   (ModeBallpark, FullBallpark) with the reference's own comparison (modes_batch.differences): the batched CPU park
+   the traces come from is bit-exact to the scalar reference on it.
+"""
+
+from __future__ import annotations
+
+import argparse
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE))
+sys.path.insert(0, str(HERE.parent.parent))
+
+import refshim  # noqa: E402
+
+refshim.install()
+
+import torch  # noqa: E402
+
+import trace as tr  # noqa: E402
+
+torch.set_num_threads(8)
+
+
+# ============================================================================================ libm vectors
+
+def make_libm(rng: np.random.Generator, n: int = 3000) -> None:
+    from exact_ballpark import dlibm, vec_exp, vec_libm as L
+
+    H = float.fromhex
+    f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)
+    dbl_edges = [0.0, -0.0, 1.0, -1.0, 0.5, 2.0, 1e-310, -1e-310, 5e-324, 1e-300, 1e300, -1e300, np.inf, -np.inf,
+                 np.nan, H("0x1.ad1fb54442d18p+0"), -H("0x1.ad1fb54442d18p+0"), H("0x1.921fb54442d18p+0"),
+                 0.855469, 2.426265, 105414350.0, 105414351.0, 1e9, 1e15, 1e22, 1e100, 2 ** -27, 2 ** -26,
+                 0.126, 0.12599999999999997, 65535.999, 0.001, 0.9375, 1.0625, 0.93749999, 1.06445312]
+    big = rng.uniform(-1, 1, n) * np.exp(rng.uniform(-60, 250, n))
+    dx = np.concatenate([rng.uniform(-4, 4, n), rng.uniform(-7e4, 7e4, n), big, np.array(dbl_edges)])
+    out = {}
+    out["sin_x"] = dx
+    out["sin_y"] = np.array([dlibm.sin(float(v)) for v in dx])
+    out["cos_y"] = np.array([dlibm.cos(float(v)) for v in dx])
+    sc = [dlibm.sincos(float(v)) for v in dx]
+    out["sincos_s"] = np.array([s for s, _ in sc])
+    out["sincos_c"] = np.array([c for _, c in sc])
+    lx = np.concatenate([rng.uniform(0.9, 1.1, n), np.exp(rng.uniform(-700, 700, n)), rng.uniform(0, 10, n),
+                         np.array([0.0, -0.0, 1.0, -1.0, 1e-310, 5e-324, np.inf, -np.inf, np.nan, 0.001,
+                                   H("0x1.e000000000000p-1"), H("0x1.0900000000000p+0"), 0.9375 - 1e-17])])
+    out["log_x"] = lx
+    out["log_y"] = np.array([dlibm.log(float(v)) if v > 0 or np.isnan(v) else
+                             (-np.inf if v == 0 else np.nan) for v in lx])
+    ex = np.concatenate([rng.uniform(-30, 10, n), rng.uniform(-746, 710, n), rng.uniform(-1e-16, 1e-16, 50),
+                         np.array([0.0, -0.0, 709.78, 709.79, 710.0, -745.13, -745.14, -708.4, -708.39, -720.0,
+                                   512.0, -512.0, 1024.0, -1024.0, np.inf, -np.inf, np.nan, 1e-20, -1e-20])])
+    out["exp_x"] = ex
+    out["exp_y"] = vec_exp.exp(torch.tensor(ex)).numpy()
+    fx = f32(np.concatenate([rng.uniform(-10, 10, n), rng.uniform(-130, 130, n), rng.uniform(-1.05, 1.05, n),
+                             rng.uniform(-1, 1, n) * np.exp(rng.uniform(-100, 88, n)), rng.uniform(-1e9, 1e9, n // 4)]))
+    fedges = f32([0.0, -0.0, 1.0, -1.0, 0.5, -0.5, np.inf, -np.inf, np.nan, 88.72, 88.73, -103.28, -103.97, -104.0,
+                  1e-40, -1e-40, 1e-45, 120.0, 119.99, 0.7853981, 2 ** -12, 2 ** -26, 2 ** -29, 2 ** 25, 0.4375,
+                  0.6875, 1.1875, 2.4375, 3e38, 1.17549435e-38])
+    fx = np.concatenate([fx, fedges])
+    T = torch.tensor(fx)
+    out["f_x"] = fx
+    out["expf_y"] = L.expf(T).numpy()
+    out["sinf_y"] = L.sinf(T).numpy()
+    out["cosf_y"] = L.cosf(T).numpy()
+    out["atanf_y"] = L.atanf(T).numpy()
+    ax = np.abs(fx)
+    out["logf_x"] = np.concatenate([ax, f32([-1.0, -0.0, -np.inf])])
+    out["logf_y"] = L.logf(torch.tensor(out["logf_x"])).numpy()
+    cx = f32(np.concatenate([rng.uniform(-1, 1, 2 * n), rng.uniform(-1.1, 1.1, n),
+                             np.array([0.0, -0.0, 1.0, -1.0, 0.5, -0.5, 2 ** -26, -2 ** -26, 1.0000001, np.nan,
+                                       np.inf, 0.49999997, -0.49999997])]))
+    out["acosf_x"] = cx
+    out["acosf_y"] = L.acosf(torch.tensor(cx)).numpy()
+    yy = f32(np.concatenate([rng.uniform(-10, 10, len(fx) - 16), np.array([0.0, -0.0, np.inf, -np.inf, 1.0, -1.0,
+                                                                           0.0, np.nan, 1e30, -1e-30, 5.0, -5.0,
+                                                                           np.inf, -np.inf, 0.0, -0.0])]))
+    out["atan2f_y"] = yy
+    out["atan2f_out"] = L.atan2f(torch.tensor(yy), T).numpy()
+    px = np.concatenate([rng.uniform(0, 1, n), rng.uniform(0.9, 1.1, n), rng.uniform(0, 1e3, n),
+                         -rng.uniform(0, 10, 200),
+                         np.array([0.0, -0.0, 1.0, -1.0, np.inf, -np.inf, np.nan, 1e-310, 2.0, 0.5, -2.0, -0.5,
+                                   10.0, 0.999999, 1e300, 1e-300])])
+    py = np.concatenate([rng.integers(0, 100, n).astype(float), rng.uniform(-1e4, 1e4, n), rng.uniform(-300, 300, n),
+                         rng.integers(-7, 7, 200).astype(float),
+                         np.array([3.0, -3.0, 2.0, np.inf, 0.5, 1e30, 0.0, 1.0, 1e-30, -1e-30, 3.0, -3.0, 1e19,
+                                   -1e19, 2.0, 0.5])])
+    out["pow_x"], out["pow_y"] = px, py
+    out["pow_out"] = L.pow(torch.tensor(px), torch.tensor(py)).numpy()
+    np.savez_compressed(HERE / "libm.npz", **out)
+    print("libm.npz", {k: v.shape for k, v in out.items()})
+
+
+# ============================================================================================ traces
+
+def _recorded(fn, *args, **kw) -> list:
+    """Run one of modes_batch's drivers with the reference's VecModesPark replaced by a recording subclass; the
+    parks it made (one per group), in order."""
+    import modes_batch as mb
+    from exact_ballpark.vec_modes import VecModesPark
+
+    made = []
+    Rec = tr.recording(VecModesPark)
+
+    class Collect(Rec):
+        def __init__(self, *a, **k):
+            super().__init__(*a, **k)
+            made.append(self)
+
+    old = mb.VecModesPark
+    mb.VecModesPark = Collect
+    try:
+        fn(*args, **kw)
+    finally:
+        mb.VecModesPark = old
+    return made
+
+
+def _check_scalar(kind: str, cs: list) -> None:
+    """The batched CPU park against the reference's scalar transcription on the scenarios cs (the reference's own
+    comparison); raises on any difference."""
+    import modes_batch as mb
+    t = time.time()
+    if kind == "modes":
+        want = mb.reference_modes(cs)
+        got = mb.batched_modes(cs, device="cpu")
+        bad = mb.differences(want, got, mb.FIELDS_MODES)
+    else:
+        want = mb.reference_full(cs)
+        got = mb.batched_full(cs, device="cpu")
+        bad = mb.differences(want, got, mb.FIELDS_FULL)
+    if bad:
+        raise RuntimeError(f"the batched CPU park differs from the scalar reference: {bad[:10]}")
+    print(f"  scalar check ({kind}, {len(cs)} scenarios): 0 differences, {time.time() - t:.0f} s")
+
+
+def _sample(cs: list, per_kind: int) -> list:
+    seen, out = {}, []
+    for c in cs:
+        k = (c["kind"], bool(c.get("do", False)), bool(c["new_orbit"]))
+        if seen.get(k, 0) < per_kind:
+            seen[k] = seen.get(k, 0) + 1
+            out.append(c)
+    return out
+
+
+def _save_parks(prefix: str, parks: list) -> None:
+    name = f"trace_{prefix}"
+    tr.save([p.trace for p in parks], HERE / name, [tr.snapshot(p) for p in parks])
+    print(f"  {name}: {len(parks)} parks, {sum(p.n for p in parks)} rows, "
+          f"{sum(len(p.trace['digests']) for p in parks)} ticks")
+
+
+def make_traces(sample: int) -> None:
+    import flight_cases as flc
+    import mode_cases as mc
+    import modes_batch as mb
+
+    for seed in (1, 2):
+        t = time.time()
+        cs = mc.cases(seed)
+        if sample:
+            _check_scalar("modes", _sample(cs, sample))
+        parks = _recorded(mb.batched_modes, cs, device="cpu")
+        _save_parks(f"mc{seed}", parks)
+        print(f"mode_cases({seed}): {len(cs)} scenarios, {time.time() - t:.0f} s")
+    for seed in (1, 2):
+        t = time.time()
+        cs = flc.cases(seed)
+        if sample:
+            _check_scalar("full", _sample(cs, max(1, sample // 2)))
+        parks = _recorded(mb.batched_full, cs, device="cpu")
+        _save_parks(f"fc{seed}", parks)
+        print(f"flight_cases({seed}): {len(cs)} scenarios, {time.time() - t:.0f} s")
+
+
+def make_workload_traces() -> None:
+    from exact_ballpark.vec_modes import VecModesPark
+    from exact_ballpark_b200.workloads import flight_worlds
+
+    Rec = tr.recording(VecModesPark)
+    for name, seed, do, new in (("w0_do_new", 1, True, True), ("w0_do_old", 2, True, False),
+                                ("w0_nodo_new", 3, False, True)):
+        t = time.time()
+        w = flight_worlds(seed, 64, 4)
+        park = Rec(len(w.rows), device="cpu", dynamical_orientation=do, use_new_orbit=new)
+        park.load(w.rows)
+        w.apply(park)
+        for _ in range(200):
+            park.evolve()
+        tr.save([park.trace], HERE / f"trace_{name}", [tr.snapshot(park)])
+        print(f"  trace_{name}: n={park.n} 200 ticks, {time.time() - t:.0f} s")
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", choices=("libm", "traces", "workload"), default=None)
+    ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
+    a = ap.parse_args()
+    if a.only in (None, "libm"):
+        make_libm(np.random.default_rng(20261203))
+    if a.only in (None, "workload"):
+        make_workload_traces()
+    if a.only in (None, "traces"):
+        make_traces(a.sample)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,45 @@
+"""The C ABI without a GPU: libebb.so loads, exports every entry point include/ebb.h declares, reports its ABI
+version, and refuses bad arguments before launching anything."""
+
+import ctypes
+import re
+
+from exact_ballpark_b200 import _native
+from golden_util import GOLDEN
+
+HEADER = GOLDEN.parent.parent / "include" / "ebb.h"
+
+
+def declared() -> list:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ebb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_the_library_exports_every_declared_entry_point():
+    lib = _native.lib()
+    names = declared()
+    assert len(names) >= 8
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_abi_version_and_scratch_size():
+    lib = _native.lib()
+    assert lib.ebb_abi() == _native.ABI == 1
+    assert lib.ebb_flight_scratch_bytes(0) == 0
+    b = lib.ebb_flight_scratch_bytes(1000)
+    assert b >= 1000 * (8 * 7 + 1) and b % 256 == 0
+
+
+def test_refused_arguments_launch_nothing():
+    lib = _native.lib()
+    s = _native.FlightState()
+    s.n = 16
+    assert lib.ebb_flight_tick(ctypes.byref(s), None, 0, None, 128) == -1          # no scratch
+    assert lib.ebb_flight_tick(ctypes.byref(s), ctypes.c_void_p(256), 1 << 20, None, 100) == -1   # block % 32
+    assert lib.ebb_flight_tick_tiled(ctypes.byref(s), None, 1, 128, None, None, 128, 1) == -1
+    assert lib.ebb_libm(99, 4, ctypes.c_void_p(256), None, ctypes.c_void_p(512), None, 128) == -1
+    assert lib.ebb_error_string(-1).decode().startswith("refused")
+    s.n = 0
+    assert lib.ebb_flight_tick(ctypes.byref(s), None, 0, None, 128) == 0             # nothing to do
