@@ -56,7 +56,7 @@ def _peaks() -> tuple:
 
 
 class Clocks:
-    """nvidia-smi sampled every 200 ms during the timed region (SM clock, throttle reasons)."""
+    """nvidia-smi sampled every 100 ms during the timed region (SM clock, throttle reasons)."""
 
     def __init__(self, index: int):
         self.index = index
@@ -71,7 +71,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -108,8 +108,9 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def cpu_sample(worlds: int, ships: int, seconds: float = 12.0) -> dict:
-    """The CPU oracle over a bounded sample of the workload on every host core: ship-ticks/s."""
+def cpu_sample(worlds: int, ships: int, warmup: int, steps: int) -> dict:
+    """The CPU oracle on every host core over the same tick window as the GPU run (ticks warmup+1 .. warmup+steps of
+    the same workload), on `worlds` worlds: ship-ticks/s."""
     from exact_ballpark_b200.workloads import flight_worlds
     from oracle.park import OraclePark
     threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
@@ -117,16 +118,16 @@ def cpu_sample(worlds: int, ships: int, seconds: float = 12.0) -> dict:
     p = OraclePark(len(w.rows), dynamical_orientation=True, use_new_orbit=True)
     p.load(w.rows)
     w.apply(p)
-    p.evolve(threads=threads)
-    t0 = time.perf_counter()
-    k = 0
-    while time.perf_counter() - t0 < seconds:
+    for _ in range(warmup):
         p.evolve(threads=threads)
-        k += 1
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        p.evolve(threads=threads)
     dt = time.perf_counter() - t0
-    return {"value": len(w.rows) * k / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{worlds} worlds x {ships} ships, {k} ticks from tick 1 ({dt:.1f} s), C++ oracle "
-                      f"(oracle/flight.cpp), {threads} threads over disjoint worlds"}
+    return {"value": len(w.rows) * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{worlds} worlds x {ships} ships (seed 1), ticks {warmup + 1}..{warmup + steps} "
+                      f"({dt:.1f} s wall, {dt * threads:.0f} core-s), C++ oracle (oracle/flight.cpp), "
+                      f"{threads} threads over disjoint worlds"}
 
 
 def run_reference(args, rank: int) -> None:
@@ -168,7 +169,7 @@ def _config(args, schedule: str) -> dict:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--worlds", type=int, default=65536)
@@ -303,7 +304,7 @@ def main() -> None:
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
             "gpu_launches": 3 * args.steps, "clocks": clocks}
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_sample(4096, args.ships)
+        line["cpu_baseline"] = cpu_sample(args.worlds, args.ships, args.warmup, args.steps)
     if dist is not None:
         del graph
         dist.destroy_process_group()
