@@ -194,6 +194,7 @@ def main() -> None:
     import torch
 
     from exact_ballpark_b200 import ModesGraph, VecModesPark, tick_plain
+    from exact_ballpark_b200.autotune import autotune
     from exact_ballpark_b200.workloads import flight_worlds
 
     torch.cuda.set_device(local)
@@ -214,7 +215,6 @@ def main() -> None:
     plain = VecModesPark(n, device=dev, dynamical_orientation=True, use_new_orbit=True)
     plain.load(w.rows)
     w.apply(plain)
-    graph = ModesGraph(park)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
@@ -242,9 +242,13 @@ def main() -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    for _ in range(args.warmup):
-        graph.tick()
+    for _ in range(args.warmup):                                     # warm-up ticks (they also warm the cost hint)
+        park.evolve()
         tick_plain(plain)
+        plain.current_time += 1
+    tuning = autotune(park)                                          # the tiled plan, the park's state unchanged
+    plan = park.plan
+    graph = ModesGraph(park)
     barrier()
     with Clocks(local) as clk:
         barrier()
@@ -290,8 +294,10 @@ def main() -> None:
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_tiled, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64/f32", "data": "synthetic (seeded)",
-            "config": _config(args, "tiled: worlds packed in tiles, one block a tile, records in shared memory, one "
-                                    "launch, CUDA graph"),
+            "config": dict(_config(args, "tiled: worlds packed in tiles, one block a tile, records in shared memory, "
+                                         "ships in cost order, one launch, CUDA graph"),
+                           plan={"tile_rows_max": plan.cap, "block": plan.block, "grid": plan.grid, "tiles": plan.tiles,
+                                 "candidates_timed": len(tuning)}),
             "plain": {"value": total_ships * args.steps / (ms_plain / 1e3), "ms_per_step": per_plain,
                       "schedule": "plain: records pass + tick, two launches, records in scratch"},
             "speedup_tiled_vs_plain": per_plain / per_tiled,

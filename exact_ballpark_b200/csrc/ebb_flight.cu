@@ -94,7 +94,8 @@ struct View {
 
 // One ship's whole tick in place (phase 1, 3, 4, PetrifyTroll, the clock); `tgt` is its follow_ptr's view (valid
 // false when it has none), `act_self` its own record
-__device__ __forceinline__ void tick_ship(const EbbFlightState& s, int64_t i, const View& tgt, bool act_self) {
+__device__ __forceinline__ void tick_ship(const EbbFlightState& s, int64_t i, const View& tgt, bool act_self,
+                                          const float* ndt_tab) {
     const int64_t n = s.n;
     const Cfg c = cfg_of(s);
     Ship b;
@@ -164,7 +165,12 @@ __device__ __forceinline__ void tick_ship(const EbbFlightState& s, int64_t i, co
         } else if (b.mode == STOP) {
             if (!c.dynamical) b.vel.y = dmul(dsub(b.vel.y, dmul(STOP_DECAY, b.vel.y)), STOP_DAMP);
         }                                                             // BOID, MINIBALL, FIELD, RIGID, TROLL: none
-        if (c.dynamical) a = orient(b, a, s.max_ang_vel[i], s.rot_agility[i], r0, w0, c, &torque, &roll, &rot1, &w1);
+        if (c.dynamical) {
+            int iters = 0;
+            a = orient(b, a, s.max_ang_vel[i], s.rot_agility[i], r0, w0, c, ndt_tab, &torque, &roll, &rot1, &w1,
+                       &iters);
+            if (s.cost != nullptr) s.cost[i] = (uint8_t)(iters >= 1020 ? 255 : (iters + 3) / 4);
+        }
         b.last_g = a;
     }
     if (release_after) release(b, true);
@@ -267,6 +273,9 @@ __global__ void __launch_bounds__(256) records_kernel(EbbFlightState s, Records 
 }
 
 __global__ void __launch_bounds__(256) tick_kernel(EbbFlightState s, Records r) {
+    __shared__ float ndt_tab[TORQUE_STEPS];
+    fill_ndt(ndt_tab, s.dt);
+    __syncthreads();
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
     View tgt;
@@ -283,7 +292,7 @@ __global__ void __launch_bounds__(256) tick_kernel(EbbFlightState s, Records r) 
         tgt.act = false;
         tgt.id = 0;
     }
-    tick_ship(s, i, tgt, r.act[i] != 0);
+    tick_ship(s, i, tgt, r.act[i] != 0, ndt_tab);
 }
 
 // ================================================================================================ tiled schedule
@@ -296,18 +305,32 @@ struct SlotRec {
     int32_t act;
 };
 
-__global__ void __launch_bounds__(1024) tiled_kernel(EbbFlightState s, const int64_t* __restrict__ tile_rows,
-                                                     int64_t tiles, int32_t* status) {
-    extern __shared__ SlotRec rec[];
+constexpr int COST_BUCKETS = 16;
+
+// One tile at a time (a run of whole worlds, rows [r0, r1)): the records pass into shared memory, then the ships'
+// ticks in the order of their last tick's search cost (the `cost` hint: ships of similar cost share a warp, so the
+// torque searches diverge less), each thread taking ships j = t, t + blockDim, ... of that order. The order decides
+// only which thread runs which ship: every ship's tick is the same computation whatever its thread.
+__global__ void __launch_bounds__(256, 2) tiled_kernel(EbbFlightState s, const int64_t* __restrict__ tile_rows,
+                                                       int64_t tiles, int32_t* status) {
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ float ndt_tab[TORQUE_STEPS];
+    __shared__ int bucket_count[COST_BUCKETS], bucket_next[COST_BUCKETS];
+    fill_ndt(ndt_tab, s.dt);
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int64_t r0 = tile_rows[tile], r1 = tile_rows[tile + 1];
-        const int64_t i = r0 + threadIdx.x;
-        const bool mine = i < r1;
-        bool act = false;
-        if (mine) {                                                   // the records pass, into shared memory
+        const int m = (int)(r1 - r0);
+        SlotRec* rec = (SlotRec*)smem_raw;
+        uint16_t* order = (uint16_t*)(rec + m);
+        uint8_t* bucket = (uint8_t*)(order + m);
+        if (threadIdx.x < COST_BUCKETS) bucket_count[threadIdx.x] = 0;
+        __syncthreads();
+        for (int j = threadIdx.x; j < m; j += blockDim.x) {           // the records pass, into shared memory
+            const int64_t i = r0 + j;
+            bool act;
             double vy_after;
             records_of(s, i, &act, &vy_after);
-            SlotRec& q = rec[threadIdx.x];
+            SlotRec& q = rec[j];
             const D3 p = ld3(s.pos, i, s.n), v = ld3(s.vel, i, s.n);
             q.px = p.x;
             q.py = p.y;
@@ -319,9 +342,24 @@ __global__ void __launch_bounds__(1024) tiled_kernel(EbbFlightState s, const int
             q.id = s.ids[i];
             q.radius = s.radius[i];
             q.act = act ? 1 : 0;
+            const int b = s.cost != nullptr ? (s.cost[i] >> 4) : 0;
+            bucket[j] = (uint8_t)b;
+            atomicAdd(&bucket_count[b], 1);
         }
         __syncthreads();
-        if (mine) {
+        if (threadIdx.x == 0) {                                       // each bucket's first slot in the order
+            int acc = 0;
+            for (int b = 0; b < COST_BUCKETS; ++b) {
+                bucket_next[b] = acc;
+                acc += bucket_count[b];
+            }
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < m; j += blockDim.x) order[atomicAdd(&bucket_next[bucket[j]], 1)] = (uint16_t)j;
+        __syncthreads();
+        for (int k = threadIdx.x; k < m; k += blockDim.x) {
+            const int j = order[k];
+            const int64_t i = r0 + j;
             View tgt;
             const int64_t t = s.follow_ptr[i];
             tgt.valid = t >= r0 && t < r1;
@@ -338,10 +376,14 @@ __global__ void __launch_bounds__(1024) tiled_kernel(EbbFlightState s, const int
                 tgt.act = false;
                 tgt.id = 0;
             }
-            tick_ship(s, i, tgt, act);
+            tick_ship(s, i, tgt, rec[j].act != 0, ndt_tab);
         }
         __syncthreads();                                              // the slots are the next tile's
     }
+}
+
+__host__ __device__ inline size_t tiled_smem_bytes(int cap) {
+    return ((size_t)cap * (sizeof(SlotRec) + sizeof(uint16_t) + 1) + 15) & ~(size_t)15;
 }
 
 // ================================================================================================ set-up kernels
@@ -442,10 +484,10 @@ int ebb_flight_tick_tiled(const EbbFlightState* s, const int64_t* tile_rows, int
                           int32_t* status, void* stream, int block, int grid) {
     if (s == nullptr) return EBB_EINVAL;
     if (s->n <= 0 || tiles <= 0) return 0;
-    if (!block_ok(block, 1024) || tile_cap <= 0 || tile_cap > block || tile_rows == nullptr || status == nullptr ||
+    if (!block_ok(block, 256) || tile_cap <= 0 || tile_cap > 4096 || tile_rows == nullptr || status == nullptr ||
         grid <= 0)
         return EBB_EINVAL;
-    const size_t smem = (size_t)block * sizeof(ebb::flight::SlotRec);
+    const size_t smem = ebb::flight::tiled_smem_bytes(tile_cap);
     if (smem > 48 * 1024) {
         const cudaError_t e = cudaFuncSetAttribute(ebb::flight::tiled_kernel,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

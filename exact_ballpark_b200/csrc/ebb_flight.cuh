@@ -388,10 +388,51 @@ struct Turn {
     float max_ang_vel, t_scale, tf, tau_s;     // tf = expf(-dt t_scale); tau_s = 1 / t_scale
     double dt;
     float fdt;
+    const float* ndt_tab;                      // float(n dt) for n = 0 .. TORQUE_STEPS - 1 (shared memory)
+    int iters;                                 // the searches' steps this tick (a scheduling hint, not state)
 };
 
 // float(n dt)
 __device__ __forceinline__ float ndt(int n, double dt) { return tof(dmul((double)n, dt)); }
+
+// The table float(n dt), n = 0 .. TORQUE_STEPS - 1, that a block's searches read (filled by the block's threads)
+__device__ __forceinline__ void fill_ndt(float* tab, double dt) {
+    for (int k = threadIdx.x; k < TORQUE_STEPS; k += blockDim.x) tab[k] = ndt(k, dt);
+}
+
+// The least float y with fsqrt(y) >= m, for m > 0: then fsqrt(x) < m exactly when x < y (fsqrt is correctly rounded,
+// so monotonic; x a sum of squares, never negative). Found from m m by unit steps, at most a few. False (the test
+// stays fsqrt(x) < m) if it does not settle within 64 steps.
+__device__ __forceinline__ bool sqrt_threshold(float m, float* out) {
+    float y = fmul(m, m);
+    if (!(y == y)) {                                                  // m NaN: no x passes either way
+        *out = y;
+        return true;
+    }
+    if (fsqrt(y) >= m) {
+        for (int k = 0; k < 64; ++k) {
+            if (y == 0.0f) {
+                *out = y;
+                return true;
+            }
+            const float below = ffrom(fbits(y) - 1u);
+            if (!(fsqrt(below) >= m)) {
+                *out = y;
+                return true;
+            }
+            y = below;
+        }
+        return false;
+    }
+    for (int k = 0; k < 64; ++k) {
+        y = ffrom(fbits(y) + 1u);
+        if (fsqrt(y) >= m) {
+            *out = y;
+            return true;
+        }
+    }
+    return false;
+}
 
 // CalculateN2Alpha2 (full.py:2124-2150): the braking ticks n2, kappa2 = tf^n2 (pow), and the braking factor
 // t_scale kappa2 / (1 - kappa2) the torque is -omega times (when the turning rate is above 1e-10)
@@ -426,7 +467,7 @@ __device__ __forceinline__ void search_terms(const Search& q, float kappa1, floa
 }
 
 // GotoTorqueBreaks (full.py:2155): the heading torque toward `direction`
-__device__ __noinline__ F3 heading_torque(const Turn& t, F3 direction, F4 rot, F3 w) {
+__device__ __noinline__ F3 heading_torque(Turn& t, F3 direction, F4 rot, F3 w) {
     const F3 zero = F3{0.0f, 0.0f, 0.0f};
     const float max_alpha = fmul(t.max_ang_vel, t.t_scale);
     if (max_alpha <= 0.0f) return zero;
@@ -449,6 +490,8 @@ __device__ __noinline__ F3 heading_torque(const Turn& t, F3 direction, F4 rot, F
     int n1 = 0;
     F3 alpha1 = zero;
     float kappa1 = 1.0f;
+    float limit2;                                                     // |alpha1| < max_alpha as a squared test
+    const bool squared = sqrt_threshold(max_alpha, &limit2);
     for (int round = 0; round < TORQUE_ROUNDS; ++round) {
         q.n2dt = ndt(q.n2, t.dt);
         q.one_k2 = fsub(1.0f, q.kappa2);
@@ -464,10 +507,11 @@ __device__ __noinline__ F3 heading_torque(const Turn& t, F3 direction, F4 rot, F
         for (n1 = 1; n1 < TORQUE_STEPS; ++n1) {
             kappa1 = fmul(kappa1, t.tf);
             float num, den;
-            search_terms(q, kappa1, ndt(n1, t.dt), &num, &den);
+            search_terms(q, kappa1, t.ndt_tab[n1], &num, &den);
             alpha1 = f3_div(f3_sub(target, f3_mul(omega0, num)), den);
-            if (f3_len(alpha1) < max_alpha) break;
+            if (squared ? (f3_dot(alpha1, alpha1) < limit2) : (f3_len(alpha1) < max_alpha)) break;
         }
+        t.iters += n1;
         const F3 omega1 = f3_add(f3_mul(alpha1, fmul(q.tau, fsub(1.0f, kappa1))), f3_mul(omega0, kappa1));
         const int n2_old = q.n2;
         alpha2 = zero;
@@ -481,7 +525,7 @@ __device__ __noinline__ F3 heading_torque(const Turn& t, F3 direction, F4 rot, F
 
 // GotoRollBreaks (full.py:2224): the roll torque, rolling into strong turns, otherwise upright (its division is a
 // true division where the vector search multiplies by the reciprocal)
-__device__ __noinline__ float roll_torque(const Turn& t, F3 heading_torque, F4 rot, F3 w) {
+__device__ __noinline__ float roll_torque(Turn& t, F3 heading_torque, F4 rot, F3 w) {
     const float max_alpha = fmul(t.t_scale, t.max_ang_vel);
     if (max_alpha <= 0.0f) return 0.0f;
     const M3 mat = m_of_q(q_conj(rot));
@@ -524,10 +568,11 @@ __device__ __noinline__ float roll_torque(const Turn& t, F3 heading_torque, F4 r
         for (n1 = 1; n1 < TORQUE_STEPS; ++n1) {
             kappa1 = fmul(kappa1, t.tf);
             float num, den;
-            search_terms(q, kappa1, ndt(n1, t.dt), &num, &den);
+            search_terms(q, kappa1, t.ndt_tab[n1], &num, &den);
             alpha1 = fdiv(fsub(desired, fmul(omega_roll, num)), den);
             if (fabs_(alpha1) < max_alpha) break;
         }
+        t.iters += n1;
         const float omega1 = fadd(fmul(fmul(alpha1, q.tau), fsub(1.0f, kappa1)), fmul(omega_roll, kappa1));
         const int n2_old = q.n2;
         alpha2 = 0.0f;
@@ -580,7 +625,8 @@ __device__ __noinline__ void apply_torque(F4 rotation, F3 w, F3 torque, float ro
 // 90 degrees or more); below it the thrust is kept, a ship in warp proper turns toward its exit point. Out: the
 // torque, the roll, and ApplyTorque's rotation and angular velocity (the commit's: same inputs).
 __device__ __noinline__ D3 orient(const Ship& s, D3 a, float max_ang_vel, float rot_agility, F4 r0, F3 w0,
-                                  const Cfg& c, F3* torque_out, float* roll_out, F4* rot_out, F3* w_out) {
+                                  const Cfg& c, const float* ndt_tab, F3* torque_out, float* roll_out, F4* rot_out,
+                                  F3* w_out, int* iters) {
     const float accel = tof(d3_len(a));
     const float fmass = tof(s.mass);
     const float fmag = fmul(fmass, s.agility);
@@ -594,6 +640,8 @@ __device__ __noinline__ D3 orient(const Ship& s, D3 a, float max_ang_vel, float 
     t.tau_s = fdiv(1.0f, t.t_scale);
     t.dt = c.dt;
     t.fdt = c.fdt;
+    t.ndt_tab = ndt_tab;
+    t.iters = 0;
     const F3 a32 = f3_of(a);
     F3 torque = F3{0.0f, 0.0f, 0.0f};
     if (thrust) torque = heading_torque(t, a32, r0, w0);
@@ -603,6 +651,7 @@ __device__ __noinline__ D3 orient(const Ship& s, D3 a, float max_ang_vel, float 
     apply_torque(r0, w0, torque, roll, tau, c.fdt, rot_out, w_out);
     *torque_out = torque;
     *roll_out = roll;
+    *iters = t.iters;
     if (!thrust) return a;
     const F3 heading = m_apply(F3{0.0f, 0.0f, 1.0f}, m_of_q(*rot_out));
     const float cosangle = fmin_(1.0f, fdiv(f3_dot(heading, a32), accel));

@@ -1,9 +1,9 @@
 """Packing worlds into tiles for the tiled (ragged, persistent) tick, and the plan's autotuned shape.
 
-A tile is a run of whole worlds, at most `cap` rows, handled by one thread block of `block` threads (one thread a
-row, the records of the tile in shared memory). Worlds of any size pack with no padding between them: the tile
-table is the row offsets of the tiles (tile_rows[t] .. tile_rows[t + 1]). The grid is persistent: `grid` blocks take
-the tiles in turn (grid = tiles is one block a tile).
+A tile is a run of whole worlds, at most `cap` rows, handled by one thread block of `block` threads (the records of
+the tile in shared memory, the block's threads taking the tile's ships in the order of their last search cost).
+Worlds of any size pack with no padding between them: the tile table is the row offsets of the tiles (tile_rows[t] ..
+tile_rows[t + 1]). The grid is persistent: `grid` blocks take the tiles in turn (grid = tiles is one block a tile).
 
 `plan_tiles` needs each world's rows contiguous (a world's rows one run, every world one run); otherwise it returns
 None and the park ticks with the plain schedule. The shape (cap, block, grid) is chosen by `autotune`, which times
@@ -16,7 +16,9 @@ from dataclasses import dataclass, field
 
 import torch
 
-DEFAULT_CAP = 128
+DEFAULT_CAP = 512
+DEFAULT_BLOCK = 256
+MAX_CAP = 4096
 
 
 @dataclass
@@ -66,16 +68,16 @@ def pack(runs: list, cap: int) -> list:
 
 def plan_tiles(world: torch.Tensor, cap: int = DEFAULT_CAP, block: int | None = None, grid: int | None = None):
     """The tile plan for a park's world column, or None when its worlds are not contiguous runs or a world is larger
-    than 1024 rows."""
+    than MAX_CAP rows."""
     runs = world_runs(world)
     if runs is None or len(runs) < 2:
         return None
     max_world = max(b - a for a, b in zip(runs[:-1], runs[1:]))
-    if max_world > 1024:
+    if max_world > MAX_CAP:
         return None
-    cap = max(cap, max_world)
+    cap = min(max(cap, max_world), MAX_CAP)
     tile_rows = pack(runs, cap)
-    blk = block or ((cap + 31) // 32) * 32
-    if blk < cap:
-        raise ValueError(f"block {blk} < cap {cap}")
+    blk = block or DEFAULT_BLOCK
+    if blk % 32 or not 32 <= blk <= 256:
+        raise ValueError(f"block {blk}: a multiple of 32 up to 256")
     return TilePlan(tile_rows, cap, blk, grid or (len(tile_rows) - 1), max_world)

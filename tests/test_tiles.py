@@ -23,6 +23,6 @@ def test_pack_keeps_worlds_whole_and_tiles_within_cap():
 def test_plan_grows_the_cap_to_the_largest_world():
     w = torch.repeat_interleave(torch.arange(4), torch.tensor([3, 200, 5, 7]))
     p = plan_tiles(w, cap=128)
-    assert p.cap >= 200 and p.block % 32 == 0 and p.block >= p.cap
+    assert p.cap >= 200 and p.block % 32 == 0 and p.block <= 256
     assert p.tile_rows[-1] == 215
     assert plan_tiles(torch.tensor([0, 1, 0])) is None
