@@ -18,6 +18,7 @@
 
 #include "../../include/ebb.h"
 #include "ebb_flight.cuh"
+#include "ebb_orient.cuh"
 
 namespace ebb {
 namespace flight {
@@ -92,12 +93,8 @@ struct View {
     bool act, valid;
 };
 
-// One ship's whole tick in place (phase 1, 3, 4, PetrifyTroll, the clock); `tgt` is its follow_ptr's view (valid
-// false when it has none), `act_self` its own record
-__device__ __forceinline__ void tick_ship(const EbbFlightState& s, int64_t i, const View& tgt, bool act_self,
-                                          const float* ndt_tab) {
+__device__ __forceinline__ Ship load_ship(const EbbFlightState& s, int64_t i) {
     const int64_t n = s.n;
-    const Cfg c = cfg_of(s);
     Ship b;
     b.pos = ld3(s.pos, i, n);
     b.vel = ld3(s.vel, i, n);
@@ -121,24 +118,44 @@ __device__ __forceinline__ void tick_ship(const EbbFlightState& s, int64_t i, co
     b.massive = s.massive[i] != 0;
     b.interactive = s.interactive[i] != 0;
     b.sensor = s.sensor[i] != 0;
+    return b;
+}
+
+// The fields a tick's phase 1 may change (the velocity's STOP damping, a release, a warp's start), stored in place
+// between the phases: no other ship reads them this tick (they read the records)
+__device__ __forceinline__ void store_phase1(const EbbFlightState& s, int64_t i, const Ship& b) {
+    const int64_t n = s.n;
+    st3(s.vel, i, n, b.vel);
+    st3(s.goto_pt, i, n, b.gp);
+    s.last_collision[i] = b.last_collision;
+    s.speed_fraction[i] = b.sf;
+    s.follow_range[i] = b.follow_range;
+    s.mode[i] = b.mode;
+    s.effect_stamp[i] = b.effect_stamp;
+    s.follow_id[i] = b.follow_id;
+    s.owner_id[i] = b.owner_id;
+    s.follow_ptr[i] = b.follow_ptr;
+    s.massive[i] = b.massive ? 1 : 0;
+    s.sensor[i] = b.sensor ? 1 : 0;
+}
+
+// A ship's tick, first part: the release when its target starts warp proper before its own turn, and the behaviour
+// (modes.py:359-377): the thrust, into the orientation step's lane (with dynamical orientation) or as it stands
+__device__ __forceinline__ void tick_begin(const EbbFlightState& s, int64_t i, const View& tgt, bool act_self,
+                                           DoLane& d, bool* release_after) {
+    const int64_t n = s.n;
+    const Cfg c = cfg_of(s);
+    Ship b = load_ship(s, i);
     const bool live = s.free_[i] && !s.moribund[i];
-    // ---- phase 1: the release when the target starts warp proper (before or after this ship's turn), the
-    // behaviour, dynamical orientation
-    bool release_after = false;
+    *release_after = false;
     if (tgt.valid && tgt.id == b.follow_id && tgt.act) {
         if (tgt.id < b.id) release(b, true);
-        else release_after = true;
+        else *release_after = true;
     }
-    F3 torque = F3{0.0f, 0.0f, 0.0f};
-    float roll = 0.0f;
-    F4 r0 = q_identity(), rot1 = r0;
-    F3 w0 = F3{0.0f, 0.0f, 0.0f}, w1 = w0;
+    D3 a = D3{0.0, 0.0, 0.0};
+    F4 r0 = q_identity();
     if (live) {
-        D3 a = D3{0.0, 0.0, 0.0};
-        if (s.dynamical) {
-            r0 = ldf4(s.rot, i, n);
-            w0 = ldf3(s.ang_vel, i, n);
-        }
+        if (s.dynamical) r0 = ldf4(s.rot, i, n);
         if (b.mode == WARP) {                                         // EvolveWarp (modes.py:379)
             if (b.effect_stamp >= 0) {
                 a = D3{0.0, 0.0, 0.0};
@@ -165,16 +182,36 @@ __device__ __forceinline__ void tick_ship(const EbbFlightState& s, int64_t i, co
         } else if (b.mode == STOP) {
             if (!c.dynamical) b.vel.y = dmul(dsub(b.vel.y, dmul(STOP_DECAY, b.vel.y)), STOP_DAMP);
         }                                                             // BOID, MINIBALL, FIELD, RIGID, TROLL: none
-        if (c.dynamical) {
-            int iters = 0;
-            a = orient(b, a, s.max_ang_vel[i], s.rot_agility[i], r0, w0, c, ndt_tab, &torque, &roll, &rot1, &w1,
-                       &iters);
-            if (s.cost != nullptr) s.cost[i] = (uint8_t)(iters >= 1020 ? 255 : (iters + 3) / 4);
-        }
-        b.last_g = a;
     }
+    store_phase1(s, i, b);
+    d.on = live && s.dynamical;
+    d.a = a;
+    if (d.on) {
+        d.fmass = tof(b.mass);
+        d.agility = b.agility;
+        d.sf = b.sf;
+        d.max_vel = b.max_vel;
+        d.max_ang_vel = s.max_ang_vel[i];
+        d.rot_agility = s.rot_agility[i];
+        d.warping = b.mode == WARP && b.effect_stamp >= 0;
+        d.to_exit = f3_of(d3_sub(b.gp, b.pos));
+        d.r0 = r0;
+        d.w0 = ldf3(s.ang_vel, i, n);
+    } else {
+        d.r0 = q_identity();
+        d.w0 = F3{0.0f, 0.0f, 0.0f};
+    }
+}
+
+// A ship's tick, last part: the thrust (mLastG), the release after its own turn, phase 3 (the warp path or the
+// integrator), phase 4 (the commit, the rotation where finite), PetrifyTroll, its world's clock
+__device__ __forceinline__ void tick_end(const EbbFlightState& s, int64_t i, const DoLane& d, bool release_after) {
+    const int64_t n = s.n;
+    const Cfg c = cfg_of(s);
+    Ship b = load_ship(s, i);
+    const bool live = s.free_[i] && !s.moribund[i];
+    if (live) b.last_g = d.a;
     if (release_after) release(b, true);
-    // ---- phases 3 and 4
     if (live) {
         if (b.massive) b.last_collision = -1.0;                       // the gradient without neighbours
         D3 p = b.pos, v = b.vel;
@@ -197,14 +234,15 @@ __device__ __forceinline__ void tick_ship(const EbbFlightState& s, int64_t i, co
         b.pos = p;
         b.vel = v;
         if (c.dynamical) {                                            // the commit: the new values where finite
-            const bool rot_ok = ffinite(q_lensq(rot1));
-            const bool w_ok = ffinite(f3_dot(w1, w1));
-            stf4(s.rot, i, n, rot_ok ? rot1 : r0);
-            stf4(s.old_rot, i, n, rot_ok ? r0 : rot1);
-            stf3(s.ang_vel, i, n, w_ok ? w1 : w0);
-            stf3(s.old_ang_vel, i, n, w_ok ? w0 : w1);
-            stf3(s.torque, i, n, torque);
-            s.rot_roll[i] = roll;
+            const bool rot_ok = ffinite(q_lensq(d.rot1));
+            const bool w_ok = ffinite(f3_dot(d.w1, d.w1));
+            stf4(s.rot, i, n, rot_ok ? d.rot1 : d.r0);
+            stf4(s.old_rot, i, n, rot_ok ? d.r0 : d.rot1);
+            stf3(s.ang_vel, i, n, w_ok ? d.w1 : d.w0);
+            stf3(s.old_ang_vel, i, n, w_ok ? d.w0 : d.w1);
+            stf3(s.torque, i, n, d.torque);
+            s.rot_roll[i] = d.roll;
+            if (s.cost != nullptr) s.cost[i] = (uint8_t)(d.iters >= 1020 ? 255 : (d.iters + 3) / 4);
         }
         if (b.mode == TROLL && !(b.effect_stamp > b.clock)) {
             // PetrifyTroll (full.py:1800) of a troll due: fixed, at rest (velocity and old velocity), mLastG cleared,
@@ -272,27 +310,37 @@ __global__ void __launch_bounds__(256) records_kernel(EbbFlightState s, Records 
     st3(r.vel, i, s.n, ld3(s.vel, i, s.n));
 }
 
+// The plain tick: one thread a row, every warp's 32 rows through the warp's orientation step together (rows past n
+// pass through it)
 __global__ void __launch_bounds__(256) tick_kernel(EbbFlightState s, Records r) {
     __shared__ float ndt_tab[TORQUE_STEPS];
+    __shared__ float ktab[(256 / 32) * KTAB_FLOATS];
     fill_ndt(ndt_tab, s.dt);
     __syncthreads();
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.n) return;
-    View tgt;
-    const int64_t t = s.follow_ptr[i];
-    tgt.valid = t >= 0 && t < s.n;
-    if (tgt.valid) {
-        tgt.pos = ld3(r.pos, t, s.n);
-        tgt.vel = ld3(r.vel, t, s.n);
-        tgt.vy_after = r.vy[t];
-        tgt.id = s.ids[t];
-        tgt.radius = s.radius[t];
-        tgt.act = r.act[t] != 0;
-    } else {
-        tgt.act = false;
-        tgt.id = 0;
+    const bool mine = i < s.n;
+    DoLane d;
+    d.on = false;
+    bool release_after = false;
+    if (mine) {
+        View tgt;
+        const int64_t t = s.follow_ptr[i];
+        tgt.valid = t >= 0 && t < s.n;
+        if (tgt.valid) {
+            tgt.pos = ld3(r.pos, t, s.n);
+            tgt.vel = ld3(r.vel, t, s.n);
+            tgt.vy_after = r.vy[t];
+            tgt.id = s.ids[t];
+            tgt.radius = s.radius[t];
+            tgt.act = r.act[t] != 0;
+        } else {
+            tgt.act = false;
+            tgt.id = 0;
+        }
+        tick_begin(s, i, tgt, r.act[i] != 0, d, &release_after);
     }
-    tick_ship(s, i, tgt, r.act[i] != 0, ndt_tab);
+    orient_warp(d, cfg_of(s), ndt_tab, ktab + (threadIdx.x >> 5) * KTAB_FLOATS);
+    if (mine) tick_end(s, i, d, release_after);
 }
 
 // ================================================================================================ tiled schedule
@@ -311,8 +359,12 @@ constexpr int COST_BUCKETS = 16;
 // ticks in the order of their last tick's search cost (the `cost` hint: ships of similar cost share a warp, so the
 // torque searches diverge less), each thread taking ships j = t, t + blockDim, ... of that order. The order decides
 // only which thread runs which ship: every ship's tick is the same computation whatever its thread.
+__host__ __device__ inline size_t tiled_records_bytes(int cap) {
+    return ((size_t)cap * (sizeof(SlotRec) + sizeof(uint16_t) + 1) + 15) & ~(size_t)15;
+}
+
 __global__ void __launch_bounds__(256, 2) tiled_kernel(EbbFlightState s, const int64_t* __restrict__ tile_rows,
-                                                       int64_t tiles, int32_t* status) {
+                                                       int64_t tiles, int cap, int32_t* status) {
     extern __shared__ unsigned char smem_raw[];
     __shared__ float ndt_tab[TORQUE_STEPS];
     __shared__ int bucket_count[COST_BUCKETS], bucket_next[COST_BUCKETS];
@@ -357,33 +409,44 @@ __global__ void __launch_bounds__(256, 2) tiled_kernel(EbbFlightState s, const i
         __syncthreads();
         for (int j = threadIdx.x; j < m; j += blockDim.x) order[atomicAdd(&bucket_next[bucket[j]], 1)] = (uint16_t)j;
         __syncthreads();
-        for (int k = threadIdx.x; k < m; k += blockDim.x) {
-            const int j = order[k];
-            const int64_t i = r0 + j;
-            View tgt;
-            const int64_t t = s.follow_ptr[i];
-            tgt.valid = t >= r0 && t < r1;
-            if (!tgt.valid && t >= 0 && t < s.n) atomicOr(status, 1);    // a target outside its world's tile
-            if (tgt.valid) {
-                const SlotRec& q = rec[t - r0];
-                tgt.pos = D3{q.px, q.py, q.pz};
-                tgt.vel = D3{q.vx, q.vy, q.vz};
-                tgt.vy_after = q.vy_after;
-                tgt.id = q.id;
-                tgt.radius = q.radius;
-                tgt.act = q.act != 0;
-            } else {
-                tgt.act = false;
-                tgt.id = 0;
+        float* ktab = (float*)(smem_raw + tiled_records_bytes(cap)) + (threadIdx.x >> 5) * KTAB_FLOATS;
+        for (int base = threadIdx.x & ~31; base < m; base += blockDim.x) {   // warp-uniform: each warp's 32 ships
+            const int k = base + (threadIdx.x & 31);
+            const bool mine = k < m;
+            DoLane d;
+            d.on = false;
+            bool release_after = false;
+            int64_t i = r0;
+            if (mine) {
+                const int j = order[k];
+                i = r0 + j;
+                View tgt;
+                const int64_t t = s.follow_ptr[i];
+                tgt.valid = t >= r0 && t < r1;
+                if (!tgt.valid && t >= 0 && t < s.n) atomicOr(status, 1);    // a target outside its world's tile
+                if (tgt.valid) {
+                    const SlotRec& q = rec[t - r0];
+                    tgt.pos = D3{q.px, q.py, q.pz};
+                    tgt.vel = D3{q.vx, q.vy, q.vz};
+                    tgt.vy_after = q.vy_after;
+                    tgt.id = q.id;
+                    tgt.radius = q.radius;
+                    tgt.act = q.act != 0;
+                } else {
+                    tgt.act = false;
+                    tgt.id = 0;
+                }
+                tick_begin(s, i, tgt, rec[j].act != 0, d, &release_after);
             }
-            tick_ship(s, i, tgt, rec[j].act != 0, ndt_tab);
+            orient_warp(d, cfg_of(s), ndt_tab, ktab);
+            if (mine) tick_end(s, i, d, release_after);
         }
         __syncthreads();                                              // the slots are the next tile's
     }
 }
 
-__host__ __device__ inline size_t tiled_smem_bytes(int cap) {
-    return ((size_t)cap * (sizeof(SlotRec) + sizeof(uint16_t) + 1) + 15) & ~(size_t)15;
+__host__ __device__ inline size_t tiled_smem_bytes(int cap, int block) {
+    return tiled_records_bytes(cap) + (size_t)(block / 32) * KTAB_FLOATS * sizeof(float);
 }
 
 // ================================================================================================ set-up kernels
@@ -487,13 +550,14 @@ int ebb_flight_tick_tiled(const EbbFlightState* s, const int64_t* tile_rows, int
     if (!block_ok(block, 256) || tile_cap <= 0 || tile_cap > 4096 || tile_rows == nullptr || status == nullptr ||
         grid <= 0)
         return EBB_EINVAL;
-    const size_t smem = ebb::flight::tiled_smem_bytes(tile_cap);
+    const size_t smem = ebb::flight::tiled_smem_bytes(tile_cap, block);
     if (smem > 48 * 1024) {
         const cudaError_t e = cudaFuncSetAttribute(ebb::flight::tiled_kernel,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
     }
-    ebb::flight::tiled_kernel<<<(unsigned)grid, block, smem, (cudaStream_t)stream>>>(*s, tile_rows, tiles, status);
+    ebb::flight::tiled_kernel<<<(unsigned)grid, block, smem, (cudaStream_t)stream>>>(*s, tile_rows, tiles, tile_cap,
+                                                                                     status);
     return launched();
 }
 

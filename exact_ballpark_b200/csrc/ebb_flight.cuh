@@ -434,13 +434,33 @@ __device__ __forceinline__ bool sqrt_threshold(float m, float* out) {
     return false;
 }
 
+// The ship's last two pow(tf, n2) results (tf is fixed for its tick, so a repeated n2 repeats the result exactly)
+struct PowCache {
+    int n2[2];
+    float kappa2[2];
+};
+__device__ __forceinline__ void pow_cache_clear(PowCache& c) {
+    c.n2[0] = c.n2[1] = INT32_MIN;
+    c.kappa2[0] = c.kappa2[1] = 0.0f;
+}
+
 // CalculateN2Alpha2 (full.py:2124-2150): the braking ticks n2, kappa2 = tf^n2 (pow), and the braking factor
 // t_scale kappa2 / (1 - kappa2) the torque is -omega times (when the turning rate is above 1e-10)
-__device__ __noinline__ bool braking(const Turn& t, float len_omega, int* n2, float* kappa2, float* g) {
+__device__ __noinline__ bool braking(const Turn& t, float len_omega, int* n2, float* kappa2, float* g, PowCache& pc) {
     if (tod(len_omega) > 1e-10) {
         const float factor = fdiv(t.max_ang_vel, len_omega);
         *n2 = to_i32(tod(fceil(fdiv(lm::logf(fdiv(factor, fadd(1.0f, factor))), fmul(fneg(t.fdt), t.t_scale)))));
-        *kappa2 = tof(lm::pow(tod(t.tf), (double)*n2));
+        if (*n2 == pc.n2[0]) {
+            *kappa2 = pc.kappa2[0];
+        } else if (*n2 == pc.n2[1]) {
+            *kappa2 = pc.kappa2[1];
+        } else {
+            *kappa2 = tof(lm::pow(tod(t.tf), (double)*n2));
+            pc.n2[1] = pc.n2[0];
+            pc.kappa2[1] = pc.kappa2[0];
+            pc.n2[0] = *n2;
+            pc.kappa2[0] = *kappa2;
+        }
         *g = fdiv(fmul(t.t_scale, *kappa2), fsub(1.0f, *kappa2));
         return true;
     }
@@ -464,124 +484,6 @@ __device__ __forceinline__ void search_terms(const Search& q, float kappa1, floa
         *num = fsub(q.tau, fdiv(fmul(fmul(kappa1, q.kappa2), q.n2dt), q.one_k2));
         *den = fmul(q.tau, fsub(n1dt, fdiv(fmul(fmul(q.n2dt, q.kappa2), fsub(1.0f, kappa1)), q.one_k2)));
     }
-}
-
-// GotoTorqueBreaks (full.py:2155): the heading torque toward `direction`
-__device__ __noinline__ F3 heading_torque(Turn& t, F3 direction, F4 rot, F3 w) {
-    const F3 zero = F3{0.0f, 0.0f, 0.0f};
-    const float max_alpha = fmul(t.max_ang_vel, t.t_scale);
-    if (max_alpha <= 0.0f) return zero;
-    const float len_dir = f3_len(direction);
-    if (len_dir == 0.0f) return zero;
-    const F3 heading = f3_unit(m_apply(F3{0.0f, 0.0f, 1.0f}, m_of_q(rot)));
-    F3 target = f3_div(f3_cross(heading, direction), len_dir);
-    const float rot_len = f3_len(target);
-    const float rot_angle = lm::acosf(fmax_(-1.0f, fmin_(1.0f, fdiv(f3_dot(direction, heading), len_dir))));
-    if (tod(rot_len) > 1e-12) target = f3_mul(target, fdiv(rot_angle, rot_len));
-    else if (rot_angle > 1.0f) target = F3{fneg(rot_angle), 0.0f, 0.0f};
-    const F3 omega0 = f3_sub(w, f3_mul(heading, f3_dot(heading, w)));
-    const float len_omega0 = f3_len(omega0);
-    if (dmul(tod(len_omega0), t.dt) < 1e-4 && tod(rot_angle) < 1e-4) return zero;
-    Search q;
-    q.tau = t.tau_s;
-    float g;
-    F3 alpha2 = zero;
-    if (braking(t, len_omega0, &q.n2, &q.kappa2, &g)) alpha2 = f3_mul(F3{fneg(omega0.x), fneg(omega0.y), fneg(omega0.z)}, g);
-    int n1 = 0;
-    F3 alpha1 = zero;
-    float kappa1 = 1.0f;
-    float limit2;                                                     // |alpha1| < max_alpha as a squared test
-    const bool squared = sqrt_threshold(max_alpha, &limit2);
-    for (int round = 0; round < TORQUE_ROUNDS; ++round) {
-        q.n2dt = ndt(q.n2, t.dt);
-        q.one_k2 = fsub(1.0f, q.kappa2);
-        if (q.n2 > 0) {
-            const F3 theta2 = f3_add(f3_mul(f3_mul(alpha2, q.tau), fsub(q.n2dt, fmul(q.tau, q.one_k2))),
-                                     f3_mul(f3_mul(omega0, q.tau), q.one_k2));
-            if (tod(f3_len(f3_sub(target, theta2))) < 1e-3) {    // braking alone gets there
-                n1 = 0;
-                break;
-            }
-        }
-        kappa1 = 1.0f;
-        for (n1 = 1; n1 < TORQUE_STEPS; ++n1) {
-            kappa1 = fmul(kappa1, t.tf);
-            float num, den;
-            search_terms(q, kappa1, t.ndt_tab[n1], &num, &den);
-            alpha1 = f3_div(f3_sub(target, f3_mul(omega0, num)), den);
-            if (squared ? (f3_dot(alpha1, alpha1) < limit2) : (f3_len(alpha1) < max_alpha)) break;
-        }
-        t.iters += n1;
-        const F3 omega1 = f3_add(f3_mul(alpha1, fmul(q.tau, fsub(1.0f, kappa1))), f3_mul(omega0, kappa1));
-        const int n2_old = q.n2;
-        alpha2 = zero;
-        if (braking(t, f3_len(omega1), &q.n2, &q.kappa2, &g)) alpha2 = f3_mul(F3{fneg(omega1.x), fneg(omega1.y), fneg(omega1.z)}, g);
-        if (q.n2 == n2_old) break;
-    }
-    if (n1 > 0) return n1 > 1 ? f3_mul(f3_unit(alpha1), max_alpha) : alpha1;
-    if (q.n2 > 0) return alpha2;
-    return zero;
-}
-
-// GotoRollBreaks (full.py:2224): the roll torque, rolling into strong turns, otherwise upright (its division is a
-// true division where the vector search multiplies by the reciprocal)
-__device__ __noinline__ float roll_torque(Turn& t, F3 heading_torque, F4 rot, F3 w) {
-    const float max_alpha = fmul(t.t_scale, t.max_ang_vel);
-    if (max_alpha <= 0.0f) return 0.0f;
-    const M3 mat = m_of_q(q_conj(rot));
-    const F3 ship_omega = m_apply(w, mat);
-    const float omega_roll = ship_omega.z;
-    const float len_torque = f3_len(heading_torque);
-    float turn_roll = 0.0f, weight = 0.0f;
-    if (tod(len_torque) > dmul(0.05, tod(max_alpha))) {
-        const F3 ship_torque = m_apply(heading_torque, mat);
-        const F3 flat = F3{ship_omega.x, ship_omega.y, 0.0f};
-        if (f3_dot(flat, ship_torque) >= 0.0f || f3_len(flat) < fmul(tof(0.01), t.max_ang_vel)) {
-            turn_roll = lm::atan2f(fneg(ship_torque.y), fneg(ship_torque.x));
-            weight = fdiv(len_torque, t.t_scale);
-            if (weight > 1.0f) weight = 1.0f;
-        }
-    }
-    const F3 up = m_apply(F3{0.0f, 1.0f, 0.0f}, mat);
-    const float up_roll = up.z < tof(0.95) ? lm::atan2f(fneg(up.x), up.y) : 0.0f;
-    const float desired = weight < tof(0.05) ? up_roll : fmul(weight, turn_roll);
-    if (tod(fabs_(omega_roll)) < 1e-4 && tod(fabs_(desired)) < 1e-4) return 0.0f;
-    Search q;
-    q.tau = t.tau_s;
-    float g;
-    float alpha2 = 0.0f;
-    if (braking(t, fabs_(omega_roll), &q.n2, &q.kappa2, &g)) alpha2 = fmul(fneg(omega_roll), g);
-    int n1 = 0;
-    float alpha1 = 0.0f, kappa1 = 1.0f;
-    for (int round = 0; round < TORQUE_ROUNDS; ++round) {
-        q.n2dt = ndt(q.n2, t.dt);
-        q.one_k2 = fsub(1.0f, q.kappa2);
-        if (q.n2 > 0) {
-            const float theta2 = fadd(fmul(fmul(q.tau, alpha2), fsub(q.n2dt, fmul(q.tau, q.one_k2))),
-                                      fmul(fmul(q.tau, omega_roll), q.one_k2));
-            if (tod(fabs_(fsub(desired, theta2))) < 1e-3) {
-                n1 = 0;
-                break;
-            }
-        }
-        kappa1 = 1.0f;
-        for (n1 = 1; n1 < TORQUE_STEPS; ++n1) {
-            kappa1 = fmul(kappa1, t.tf);
-            float num, den;
-            search_terms(q, kappa1, t.ndt_tab[n1], &num, &den);
-            alpha1 = fdiv(fsub(desired, fmul(omega_roll, num)), den);
-            if (fabs_(alpha1) < max_alpha) break;
-        }
-        t.iters += n1;
-        const float omega1 = fadd(fmul(fmul(alpha1, q.tau), fsub(1.0f, kappa1)), fmul(omega_roll, kappa1));
-        const int n2_old = q.n2;
-        alpha2 = 0.0f;
-        if (braking(t, fabs_(omega1), &q.n2, &q.kappa2, &g)) alpha2 = fmul(fneg(omega1), g);
-        if (q.n2 == n2_old) break;
-    }
-    if (n1 > 0) return n1 > 1 ? fmul(alpha1 >= 0.0f ? 1.0f : -1.0f, max_alpha) : alpha1;
-    if (q.n2 > 0) return alpha2;
-    return 0.0f;
 }
 
 // RotationQuaternion(axis, angle): sinf and cosf of the half angle around the normalised axis
@@ -618,45 +520,6 @@ __device__ __noinline__ void apply_torque(F4 rotation, F3 w, F3 torque, float ro
     if (norm > 0.0f) rotation = q_scale_inv(rotation, norm);
     *rot_out = rotation;
     *w_out = wn;
-}
-
-// EvolveBehaviorForBall's dynamical-orientation branch (full.py:2459): above 1 % of the maximum acceleration the
-// torque and roll are searched and the thrust laid along the heading a tick on, scaled by cos^2 of its angle (zero at
-// 90 degrees or more); below it the thrust is kept, a ship in warp proper turns toward its exit point. Out: the
-// torque, the roll, and ApplyTorque's rotation and angular velocity (the commit's: same inputs).
-__device__ __noinline__ D3 orient(const Ship& s, D3 a, float max_ang_vel, float rot_agility, F4 r0, F3 w0,
-                                  const Cfg& c, const float* ndt_tab, F3* torque_out, float* roll_out, F4* rot_out,
-                                  F3* w_out, int* iters) {
-    const float accel = tof(d3_len(a));
-    const float fmass = tof(s.mass);
-    const float fmag = fmul(fmass, s.agility);
-    const float max_accel = fdiv(fmul(fmul(c.ffriction, s.sf), s.max_vel), fmag);
-    const bool thrust = tod(accel) > dmul(DO_THRUST, tod(max_accel));
-    Turn t;
-    t.max_ang_vel = max_ang_vel;
-    const float inertia = fmul(fmag, rot_agility);
-    t.t_scale = fdiv(c.ffriction, inertia);
-    t.tf = lm::expf(fmul(fneg(c.fdt), t.t_scale));
-    t.tau_s = fdiv(1.0f, t.t_scale);
-    t.dt = c.dt;
-    t.fdt = c.fdt;
-    t.ndt_tab = ndt_tab;
-    t.iters = 0;
-    const F3 a32 = f3_of(a);
-    F3 torque = F3{0.0f, 0.0f, 0.0f};
-    if (thrust) torque = heading_torque(t, a32, r0, w0);
-    else if (s.mode == WARP && s.effect_stamp >= 0) torque = heading_torque(t, f3_of(d3_sub(s.gp, s.pos)), r0, w0);
-    const float roll = roll_torque(t, torque, r0, w0);
-    const float tau = fdiv(inertia, c.ffriction);
-    apply_torque(r0, w0, torque, roll, tau, c.fdt, rot_out, w_out);
-    *torque_out = torque;
-    *roll_out = roll;
-    *iters = t.iters;
-    if (!thrust) return a;
-    const F3 heading = m_apply(F3{0.0f, 0.0f, 1.0f}, m_of_q(*rot_out));
-    const float cosangle = fmin_(1.0f, fdiv(f3_dot(heading, a32), accel));
-    if (cosangle <= 0.0f) return D3{0.0, 0.0, 0.0};
-    return d3_of(f3_mul(heading, fmul(fmul(cosangle, cosangle), accel)));
 }
 
 // Ball::SnapOrientation (full.py:2092): turned to the velocity and rolled upright (the caller clears the turning)
