@@ -81,7 +81,7 @@ __device__ __forceinline__ D3 goto_thrust(const Ship& s, D3 target, const Cfg& c
 }
 
 // EvolveFollow (modes.py:428): the point at followRange + both radii from the target, on the line from it
-__device__ __noinline__ D3 follow_thrust(Ship& s, D3 tpos, float tradius, const Cfg& c) {
+__device__ __forceinline__ D3 follow_thrust(Ship& s, D3 tpos, float tradius, const Cfg& c) {
     const D3 delta = d3_sub(s.pos, tpos);
     const double dist = d3_len(delta);
     const double r = dadd(dadd(tod(s.follow_range), tod(s.radius)), tod(tradius));
@@ -99,18 +99,17 @@ __device__ __noinline__ D3 follow_thrust(Ship& s, D3 tpos, float tradius, const 
 __device__ __forceinline__ double trunc7(double x) { return ddiv(i2d(to_i64(dmul(x, TRUNC7))), TRUNC7); }
 
 // DefaultOrbitalNormal (modes.py:480): the precessing w, truncated to 7 decimals, not normalised
-__device__ __noinline__ D3 precessing_normal(const Ship& s) {
-    const double t = i2d(s.clock);
+__device__ __noinline__ D3 precessing_w(int64_t clock, int64_t id) {
+    const double t = i2d(clock);
     const double phi1 = dmul(t, ORBITAL_PRECESSION);
-    const double phi2 = dadd(i2d(s.id & 0xFFFFLL), dmul(t, ORBITAL_PRECESSION));
-    double s1, c1, s2, c2;
-    lm::sincos(phi1, &s1, &c1);
-    lm::sincos(phi2, &s2, &c2);
-    return D3{trunc7(dmul(c1, c2)), trunc7(s2), trunc7(dmul(s1, c2))};
+    const double phi2 = dadd(i2d(id & 0xFFFFLL), dmul(t, ORBITAL_PRECESSION));
+    const lm::SinCos a = lm::sincos_v(phi1), b = lm::sincos_v(phi2);
+    return D3{trunc7(dmul(a.c, b.c)), trunc7(b.s), trunc7(dmul(a.s, b.c))};
 }
+__device__ __forceinline__ D3 precessing_normal(const Ship& s) { return precessing_w(s.clock, s.id); }
 
 // EvolveOldStyleOrbit (modes.py:444)
-__device__ __noinline__ D3 old_orbit_thrust(Ship& s, D3 tpos, float tradius, const Cfg& c) {
+__device__ __forceinline__ D3 old_orbit_thrust(Ship& s, D3 tpos, float tradius, const Cfg& c) {
     const double cruise = dmul(tod(s.sf), tod(s.max_vel));
     const double max_thrust = ddiv(dmul(c.friction, cruise), dmul(s.mass, tod(s.agility)));
     const double r = dadd(dadd(tod(s.follow_range), tod(s.radius)), tod(tradius));
@@ -152,7 +151,7 @@ __device__ __forceinline__ D3 brake_thrust(const Ship& s, D3 target, const Cfg& 
 }
 
 // GotoThrustFollow (modes.py:557) with weight 1: reach the point and match the velocity, capped
-__device__ __noinline__ D3 match_thrust(const Ship& s, D3 target, D3 tv, const Cfg& c) {
+__device__ __forceinline__ D3 match_thrust(const Ship& s, D3 target, D3 tv, const Cfg& c) {
     const double sf = tod(s.sf), mv = tod(s.max_vel);
     if (d3_len(tv) < dmul(dmul(SLOW_TARGET, mv), sf)) {
         if (c.new_orbit && s.mode == ORBIT) return brake_thrust(s, target, c);
@@ -182,7 +181,7 @@ __device__ __noinline__ D3 match_thrust(const Ship& s, D3 target, D3 tv, const C
 // EvolveNewStyleOrbit (modes.py:509) with GetOrbitalNormal (modes.py:488; with dynamical orientation the heading's
 // fallback, full.py:2385): a logarithmic spiral toward the orbit radius. tvel is the target's velocity as this ship
 // sees it at its own turn; rot its rotation at the start of the tick.
-__device__ __noinline__ D3 new_orbit_thrust(Ship& s, D3 tpos, D3 tvel, float tradius, const Cfg& c, F4 rot) {
+__device__ __forceinline__ D3 new_orbit_thrust(Ship& s, D3 tpos, D3 tvel, float tradius, const Cfg& c, F4 rot) {
     const double cruise = dmul(tod(s.sf), tod(s.max_vel));
     const double tau = ddiv(dmul(s.mass, tod(s.agility)), c.friction);
     const double max_thrust = ddiv(cruise, tau);
@@ -217,8 +216,8 @@ __device__ __noinline__ D3 new_orbit_thrust(Ship& s, D3 tpos, D3 tvel, float tra
     D3 gp, gv;
     if (dabs(angle) < ANGLE_ZERO) {                                  // the circle
         const double t = ddiv(est_d, dist);
-        double st, ct;
-        lm::sincos(t, &st, &ct);
+        const lm::SinCos sc = lm::sincos_v(t);
+        const double st = sc.s, ct = sc.c;
         const double cp = dmul(dist, dsub(1.0, ct)), sp = dmul(dist, st), cv = dmul(ct, est_v), sv = dmul(st, est_v);
         gp = D3{dadd(dmul(to.x, cp), dmul(radial.x, sp)), dadd(dmul(to.y, cp), dmul(radial.y, sp)),
                 dadd(dmul(to.z, cp), dmul(radial.z, sp))};
@@ -231,8 +230,8 @@ __device__ __noinline__ D3 new_orbit_thrust(Ship& s, D3 tpos, D3 tvel, float tra
         else if (dabs(factor) > ANGLE_ZERO) t = ddiv(lm::log(dadd(1.0, factor)), angle);
         else t = ddiv(factor, angle);
         const double dexp = dmul(dist, lm::exp(dmul(angle, t)));
-        double st, ct;
-        lm::sincos(t, &st, &ct);
+        const lm::SinCos sc = lm::sincos_v(t);
+        const double st = sc.s, ct = sc.c;
         const double cp = dsub(dist, dmul(dexp, ct)), sp = dmul(dexp, st);
         gp = D3{dadd(dmul(to.x, cp), dmul(radial.x, sp)), dadd(dmul(to.y, cp), dmul(radial.y, sp)),
                 dadd(dmul(to.z, cp), dmul(radial.z, sp))};
@@ -272,7 +271,7 @@ __device__ __forceinline__ void start_warp(Ship& s) {
 
 // WarpDistance with SetupWarpConstants (modes.py:606-666): the position and velocity t seconds into warp proper on
 // the line to the exit point; true when the ship drops out (slow enough, or past the deceleration)
-__device__ __noinline__ bool warp_path(const Ship& s, D3* pp, D3* vp, double t) {
+__device__ __forceinline__ bool warp_path(const Ship& s, D3* pp, D3* vp, double t) {
     const double wf = i2d(s.owner_id);
     const double wd = s.last_collision;
     double speed_max = dmul(dmul(wf, WARP_AU_PER_S), AU);
@@ -444,18 +443,26 @@ __device__ __forceinline__ void pow_cache_clear(PowCache& c) {
     c.kappa2[0] = c.kappa2[1] = 0.0f;
 }
 
+// CalculateN2Alpha2's braking ticks (full.py:2128): n2 = ceil(log(factor / (1 + factor)) / (-dt t_scale)) as an int
+__device__ __noinline__ int braking_ticks(float max_ang_vel, float len_omega, float fdt, float t_scale) {
+    const float factor = fdiv(max_ang_vel, len_omega);
+    return to_i32(tod(fceil(fdiv(lm::logf(fdiv(factor, fadd(1.0f, factor))), fmul(fneg(fdt), t_scale)))));
+}
+// kappa2 = tf^n2 (glibc's pow, rounded to float)
+__device__ __noinline__ float braking_kappa(float tf, int n2) { return tof(lm::pow(tod(tf), (double)n2)); }
+
 // CalculateN2Alpha2 (full.py:2124-2150): the braking ticks n2, kappa2 = tf^n2 (pow), and the braking factor
 // t_scale kappa2 / (1 - kappa2) the torque is -omega times (when the turning rate is above 1e-10)
-__device__ __noinline__ bool braking(const Turn& t, float len_omega, int* n2, float* kappa2, float* g, PowCache& pc) {
+__device__ __forceinline__ bool braking(const Turn& t, float len_omega, int* n2, float* kappa2, float* g,
+                                        PowCache& pc) {
     if (tod(len_omega) > 1e-10) {
-        const float factor = fdiv(t.max_ang_vel, len_omega);
-        *n2 = to_i32(tod(fceil(fdiv(lm::logf(fdiv(factor, fadd(1.0f, factor))), fmul(fneg(t.fdt), t.t_scale)))));
+        *n2 = braking_ticks(t.max_ang_vel, len_omega, t.fdt, t.t_scale);
         if (*n2 == pc.n2[0]) {
             *kappa2 = pc.kappa2[0];
         } else if (*n2 == pc.n2[1]) {
             *kappa2 = pc.kappa2[1];
         } else {
-            *kappa2 = tof(lm::pow(tod(t.tf), (double)*n2));
+            *kappa2 = braking_kappa(t.tf, *n2);
             pc.n2[1] = pc.n2[0];
             pc.kappa2[1] = pc.kappa2[0];
             pc.n2[0] = *n2;
@@ -494,9 +501,13 @@ __device__ __noinline__ F4 q_axis_angle(F3 axis, float angle) {
     return F4{fmul(s, u.x), fmul(s, u.y), fmul(s, u.z), lm::cosf(h)};
 }
 
+struct Turned {
+    F4 rot;
+    F3 w;
+};
+
 // ApplyTorque over one tick (full.py:2292, fraction 1): heading and roll apart; the rotation and angular velocity
-__device__ __noinline__ void apply_torque(F4 rotation, F3 w, F3 torque, float roll, float tau, float fdt, F4* rot_out,
-                                          F3* w_out) {
+__device__ __forceinline__ Turned apply_torque(F4 rotation, F3 w, F3 torque, float roll, float tau, float fdt) {
     const float tf = lm::expf(fdiv(fneg(fdt), tau));
     const F3 heading = m_apply(F3{0.0f, 0.0f, 1.0f}, m_of_q(rotation));
     const float omega_roll = f3_dot(w, heading);
@@ -518,8 +529,7 @@ __device__ __noinline__ void apply_torque(F4 rotation, F3 w, F3 torque, float ro
     rotation = q_mul(rotation, q_axis_angle(heading_rotated, rot_roll));
     const float norm = fsqrt(q_lensq(rotation));
     if (norm > 0.0f) rotation = q_scale_inv(rotation, norm);
-    *rot_out = rotation;
-    *w_out = wn;
+    return Turned{rotation, wn};
 }
 
 // Ball::SnapOrientation (full.py:2092): turned to the velocity and rolled upright (the caller clears the turning)

@@ -227,8 +227,14 @@ EBB_HD double do_cos(double x, double dx) {
     return dadd(c.cs, cor);
 }
 
+// x = n pi/2 + a + da
+struct Reduced {
+    int n;
+    double a, da;
+};
+
 // reduce_sincos: x = n pi/2 + a + da in four fused steps, n the low bits of round(x 2/pi)
-EBB_HD int reduce_sincos(double x, double* a, double* da) {
+EBB_HD Reduced reduce_sincos(double x) {
     const double t = dfma(x, DL_HPINV, DL_TOINT);
     const double xn = dsub(t, DL_TOINT);
     const double y = dfma(dneg(xn), DL_MP2, dfma(dneg(xn), DL_MP1, x));
@@ -236,13 +242,14 @@ EBB_HD int reduce_sincos(double x, double* a, double* da) {
     const double b = dfma(dneg(xn), DL_PP4, t2);
     double db = dfma(dneg(xn), DL_PP3, dsub(y, t2));
     db = dadd(db, dfma(dneg(xn), DL_PP4, dsub(t2, b)));
-    *a = b;
-    *da = db;
-    return (int)(dbits(t) & 3);
+    return Reduced{(int)(dbits(t) & 3), b, db};
 }
 
 // one half of __branred: xh 2/pi from six 24-bit pieces of 2/pi, the integer part split off
-EBB_HD void branred_half(double xh, double* sum_out, double* b_out, double* bb_out) {
+struct BranredHalf {
+    double sum, b, bb;
+};
+EBB_HD BranredHalf branred_half(double xh) {
     const uint32_t e = (uint32_t)(dbits(xh) >> 52) & 0x7ff;
     int k = 0;
     if (e > (uint32_t)DL_BR_EXP_LIMIT && e >= (uint32_t)DL_BR_EXP_BIAS) k = (int)((e - (uint32_t)DL_BR_EXP_BIAS) / 24);
@@ -269,20 +276,17 @@ EBB_HD void branred_half(double xh, double* sum_out, double* b_out, double* bb_o
     total = dsub(total, s);
     const double b = dadd(bb, t);
     bb = dadd(dsub(t, b), bb);
-    *sum_out = total;
-    *b_out = b;
-    *bb_out = bb;
+    return BranredHalf{total, b, bb};
 }
 
 // __branred: x = n pi/2 + a + da for huge x (scaled by 2^-600 and split in two)
-EBB_HDNI int branred(double x, double* a, double* da) {
+EBB_HDNI Reduced branred(double x) {
     x = dmul(x, DL_BR_TM600);
     const double t0 = dmul(x, DL_BR_SPLIT);
     const double x1 = dsub(t0, dsub(t0, x));
     const double x2 = dsub(x, x1);
-    double sum1, b1, bb1, sum2, b2, bb2;
-    branred_half(x1, &sum1, &b1, &bb1);
-    branred_half(x2, &sum2, &b2, &bb2);
+    const BranredHalf h1 = branred_half(x1), h2 = branred_half(x2);
+    const double sum1 = h1.sum, b1 = h1.b, bb1 = h1.bb, sum2 = h2.sum, b2 = h2.b, bb2 = h2.bb;
     double total = dadd(sum1, sum2);
     double b = dadd(b1, b2);
     double bb = (dabs(b1) > dabs(b2)) ? dadd(dsub(b1, b), b2) : dadd(dsub(b2, b), b1);
@@ -302,9 +306,7 @@ EBB_HDNI int branred(double x, double* a, double* da) {
     const double bl = dadd(dadd(dadd(dsub(dmul(t1, DL_BR_MP1), bh), dmul(t1, DL_BR_MP2)), dmul(t2, DL_BR_MP1)),
                            dadd(dadd(dmul(t2, DL_BR_MP2), dmul(s, DL_BR_HP1)), dmul(t, DL_BR_HP0)));
     const double ss = dadd(bh, bl);
-    *a = ss;
-    *da = dadd(dsub(bh, ss), bl);
-    return (int)(to_i64(total) & 3);
+    return Reduced{(int)(to_i64(total) & 3), ss, dadd(dsub(bh, ss), bl)};
 }
 
 // do_sincos: do_cos for odd n, else do_sin; negated when n & 2
@@ -318,12 +320,11 @@ EBB_HDNI double sin(double x) {
     if (k < (uint32_t)DL_K_TINY_SIN) return x;
     if (k < (uint32_t)DL_K_DO_SIN) return do_sin(x, 0.0);
     if (k < (uint32_t)DL_K_MID) return dcopysign(do_cos(dsub(DL_HP0, dabs(x)), DL_HP1), x);
-    double a, da;
-    int n;
-    if (k < (uint32_t)DL_K_REDUCE) n = reduce_sincos(x, &a, &da);
-    else if (k < (uint32_t)DL_K_HUGE) n = branred(x, &a, &da);
+    Reduced r;
+    if (k < (uint32_t)DL_K_REDUCE) r = reduce_sincos(x);
+    else if (k < (uint32_t)DL_K_HUGE) r = branred(x);
     else return dnan();
-    return sincos_n(a, da, n);
+    return sincos_n(r.a, r.da, r.n);
 }
 
 EBB_HDNI double cos(double x) {
@@ -335,47 +336,39 @@ EBB_HDNI double cos(double x) {
         const double a = dadd(y, DL_HP1);
         return do_sin(a, dadd(dsub(y, a), DL_HP1));
     }
-    double a, da;
-    int n;
-    if (k < (uint32_t)DL_K_REDUCE) n = reduce_sincos(x, &a, &da);
-    else if (k < (uint32_t)DL_K_HUGE) n = branred(x, &a, &da);
+    Reduced r;
+    if (k < (uint32_t)DL_K_REDUCE) r = reduce_sincos(x);
+    else if (k < (uint32_t)DL_K_HUGE) r = branred(x);
     else return dnan();
-    return sincos_n(a, da, n + 1);
+    return sincos_n(r.a, r.da, r.n + 1);
 }
+
+struct SinCos {
+    double s, c;
+};
 
 // sincos as Destiny's compiled code takes a sine and a cosine of one argument: __sin's and __cos's branches, except
 // that between 0.855469 and 2.426265 the sine is do_cos after the two-sum of hp0 - |x| and hp1
-EBB_HDNI void sincos(double x, double* s_out, double* c_out) {
+EBB_HDNI SinCos sincos_v(double x) {
     const uint32_t k = (uint32_t)(dbits(x) >> 32) & 0x7fffffffu;
-    if (k < (uint32_t)DL_K_TINY_COS) {
-        *s_out = x;
-        *c_out = 1.0;
-        return;
-    }
-    if (k < (uint32_t)DL_K_DO_SIN) {
-        *s_out = do_sin(x, 0.0);
-        *c_out = do_cos(x, 0.0);
-        return;
-    }
+    if (k < (uint32_t)DL_K_TINY_COS) return SinCos{x, 1.0};
+    if (k < (uint32_t)DL_K_DO_SIN) return SinCos{do_sin(x, 0.0), do_cos(x, 0.0)};
     if (k < (uint32_t)DL_K_MID) {
         const double y = dsub(DL_HP0, dabs(x));
         const double a = dadd(y, DL_HP1);
         const double da = dadd(dsub(y, a), DL_HP1);
-        *s_out = dcopysign(do_cos(a, da), x);
-        *c_out = do_sin(a, da);
-        return;
+        return SinCos{dcopysign(do_cos(a, da), x), do_sin(a, da)};
     }
-    double a, da;
-    int n;
-    if (k < (uint32_t)DL_K_REDUCE) n = reduce_sincos(x, &a, &da);
-    else if (k < (uint32_t)DL_K_HUGE) n = branred(x, &a, &da);
-    else {
-        *s_out = dnan();
-        *c_out = dnan();
-        return;
-    }
-    *s_out = sincos_n(a, da, n);
-    *c_out = sincos_n(a, da, n + 1);
+    Reduced r;
+    if (k < (uint32_t)DL_K_REDUCE) r = reduce_sincos(x);
+    else if (k < (uint32_t)DL_K_HUGE) r = branred(x);
+    else return SinCos{dnan(), dnan()};
+    return SinCos{sincos_n(r.a, r.da, r.n), sincos_n(r.a, r.da, r.n + 1)};
+}
+EBB_HD void sincos(double x, double* s_out, double* c_out) {
+    const SinCos v = sincos_v(x);
+    *s_out = v.s;
+    *c_out = v.c;
 }
 
 // ======================================================================================== expf, logf
@@ -458,7 +451,11 @@ EBB_HD double sinf_cos_poly(double x2) {
 }
 
 // reduce_large (sincosf.h): x 4/pi in 62-bit fixed point from __inv_pio4
-EBB_HD double sinf_reduce_large(uint32_t xi, int* np) {
+struct ReducedF {
+    int n;
+    double x;
+};
+EBB_HD ReducedF sinf_reduce_large(uint32_t xi) {
     const uint32_t idx = (xi >> 26) & 15;
     const int shift = (xi >> 23) & 7;
     const uint32_t m = ((xi & 0x7fffffu) | 0x800000u) << shift;
@@ -469,8 +466,7 @@ EBB_HD double sinf_reduce_large(uint32_t xi, int* np) {
     res0 += res1;
     const uint64_t n = (res0 + (1ULL << 61)) >> 62;
     res0 -= n << 62;
-    *np = (int)n;
-    return dmul(i2d((int64_t)res0), FL_PI63);
+    return ReducedF{(int)n, dmul(i2d((int64_t)res0), FL_PI63)};
 }
 
 // glibc's sinf (cosine = false) and cosf (cosine = true): the polynomial at x below pi/4 (x or 1 below 2^-12);
@@ -495,7 +491,9 @@ EBB_HD float sincosf_one(float y, bool cosine) {
         n = (int)(int64_t)kd;
         q = n;
     } else {
-        xr = sinf_reduce_large(ix, &n);
+        const ReducedF rl = sinf_reduce_large(ix);
+        xr = rl.x;
+        n = rl.n;
         q = n + (int)(ix >> 31);
     }
     const double s = SIGN[q & 3];
@@ -658,8 +656,11 @@ EBB_HD int pow_checkint(uint64_t iy) {
     return 2;
 }
 
+struct HiLo {
+    double hi, lo;
+};
 // log_inline: log x as hi + lo, every step as compiled
-EBB_HD double pow_log_inline(uint64_t ix, double* tail) {
+EBB_HD HiLo pow_log_inline(uint64_t ix) {
     const uint64_t tmp = ix - FL_POW_OFF;
     const uint32_t i = (uint32_t)(tmp >> 45) & 127;
     const double kd = i2d(((int64_t)tmp) >> 52);
@@ -690,8 +691,7 @@ EBB_HD double pow_log_inline(uint64_t ix, double* tail) {
     s = dadd(s, lo4);
     const double lo = dfma(ar3, poly, s);
     const double y = dadd(hi, lo);
-    *tail = dadd(dsub(hi, y), lo);
-    return y;
+    return HiLo{y, dadd(dsub(hi, y), lo)};
 }
 
 // exp_inline: sign x exp(ehi + elo), the sign through the scale's sign bit
@@ -783,8 +783,8 @@ EBB_HDNI double pow(double x, double y) {
             ix -= 52ULL << 52;
         }
     }
-    double lo;
-    const double hi = pow_log_inline(ix, &lo);
+    const HiLo hl = pow_log_inline(ix);
+    const double hi = hl.hi, lo = hl.lo;
     const double ehi = dmul(y, hi);
     const double elo = dfma(y, lo, dfma(y, hi, dneg(ehi)));
     return pow_exp_inline(ehi, elo, negative);

@@ -53,7 +53,7 @@ __device__ __forceinline__ float candidate_kappa(const float* krow, int b, int l
 // The heading search's round for one ship (the loop of full.py:2189-2201), all lanes: the first n1 in 1 .. 99 whose
 // alpha1 = (target - omega0 num) / den is within max_alpha (n1 = 100 with the 99th candidate when none is), and its
 // alpha1 and kappa1, returned to every lane
-__device__ __noinline__ void warp_search_v(const float* krow, const float* ndt_tab, F3 target, F3 omega0,
+__device__ __forceinline__ void warp_search_v(const float* krow, const float* ndt_tab, F3 target, F3 omega0,
                                            const Search& q, float tf, float max_alpha, float limit2, bool squared,
                                            int lane, int* n1_out, F3* a1_out, float* k1_out) {
     float kbase = 1.0f;
@@ -84,7 +84,7 @@ __device__ __noinline__ void warp_search_v(const float* krow, const float* ndt_t
 }
 
 // The roll search's round for one ship (full.py:2264-2276): a true division, |alpha1| against max_alpha
-__device__ __noinline__ void warp_search_f(const float* krow, const float* ndt_tab, float desired, float omega_roll,
+__device__ __forceinline__ void warp_search_f(const float* krow, const float* ndt_tab, float desired, float omega_roll,
                                            const Search& q, float tf, float max_alpha, int lane, int* n1_out,
                                            float* a1_out, float* k1_out) {
     float kbase = 1.0f;
@@ -115,7 +115,7 @@ __device__ __noinline__ void warp_search_f(const float* krow, const float* ndt_t
 
 // The warp's orientation step: every lane calls it together (lanes whose ship is off pass through). `ktab` is the
 // warp's KTAB_FLOATS floats of shared memory; `ndt_tab` the block's table float(n dt).
-__device__ __noinline__ void orient_warp(DoLane& d, const Cfg& c, const float* ndt_tab, float* ktab) {
+__device__ __forceinline__ void orient_warp(DoLane& d, const Cfg& c, const float* ndt_tab, float* ktab) {
     const int lane = threadIdx.x & 31;
     const F3 zero = F3{0.0f, 0.0f, 0.0f};
     d.torque = zero;
@@ -326,7 +326,9 @@ __device__ __noinline__ void orient_warp(DoLane& d, const Cfg& c, const float* n
     // ---- ApplyTorque (the tick's rotation, the commit's too) and the thrust along the heading a tick on
     if (d.on) {
         const float tau = fdiv(inertia, c.ffriction);
-        apply_torque(d.r0, d.w0, d.torque, d.roll, tau, c.fdt, &d.rot1, &d.w1);
+        const Turned tr = apply_torque(d.r0, d.w0, d.torque, d.roll, tau, c.fdt);
+        d.rot1 = tr.rot;
+        d.w1 = tr.w;
         if (thrust) {
             const F3 heading = m_apply(F3{0.0f, 0.0f, 1.0f}, m_of_q(d.rot1));
             const float cosangle = fmin_(1.0f, fdiv(f3_dot(heading, a32), accel));
