@@ -24,7 +24,7 @@ class FlightState(ctypes.Structure):
                     "radius", "max_vel", "agility", "speed_fraction", "follow_range", "max_ang_vel", "rot_agility",
                     "rot_roll", "rot", "old_rot", "ang_vel", "old_ang_vel", "torque", "ids", "effect_stamp",
                     "follow_id", "owner_id", "clock", "mode", "follow_ptr", "free_", "moribund", "massive",
-                    "interactive", "sensor", "cost")])
+                    "interactive", "sensor")])
 
 
 def lib() -> ctypes.CDLL:

@@ -1,8 +1,8 @@
-"""The tiled schedule's autotuner: tile size (rows a tile holds, so worlds a block takes), threads a block (so ships
-a warp holds at once, the block's threads taking the tile's ships in cost order), and the persistent grid (blocks
-resident for the whole launch). Each candidate is timed on the park itself with CUDA events (median of a few ticks,
+"""The tiled schedule's autotuner: tile size (rows a tile holds, so worlds a block takes), threads a block (warps a
+block runs; each warp takes 32 of the tile's ships at a time through the warp-cooperative orientation step), and the
+persistent grid (blocks resident for the whole launch, or one block a tile). Each candidate is timed on the park itself with CUDA events (median of a few ticks,
 after one warm-up); the park's state is saved before and restored after, so tuning changes nothing a caller sees.
-The winner becomes the park's plan."""
+The winner becomes the park's plan. Worlds larger than a candidate's tile size raise it to the largest world."""
 
 from __future__ import annotations
 
@@ -15,11 +15,11 @@ from .tiles import plan_tiles
 
 def candidates(sm_count: int) -> list:
     out = []
-    for cap in (128, 256, 512, 1024, 2048):
-        for block in (128, 256):
+    for cap in (32, 64, 128, 256, 512):
+        for block in (32, 64, 128, 256):
             if block > cap:
                 continue
-            for per_sm in (None, 2, 4, 8):
+            for per_sm in (None, 8, 16):
                 out.append((cap, block, None if per_sm is None else per_sm * sm_count))
     return out
 
@@ -33,7 +33,7 @@ def autotune(park, ticks: int = 3, cands: list | None = None, verbose: bool = Fa
         raise ValueError("the park's worlds are not contiguous rows: nothing to tune")
     dev = park.dev
     sm = torch.cuda.get_device_properties(dev).multi_processor_count
-    names = park.row_tensors() + ["_cost"]
+    names = park.row_tensors()
     saved = {k: getattr(park, k).clone() for k in names}
     stream = torch.cuda.current_stream(dev)
     results = {}

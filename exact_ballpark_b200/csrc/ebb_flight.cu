@@ -242,7 +242,6 @@ __device__ __forceinline__ void tick_end(const EbbFlightState& s, int64_t i, con
             stf3(s.old_ang_vel, i, n, w_ok ? d.w0 : d.w1);
             stf3(s.torque, i, n, d.torque);
             s.rot_roll[i] = d.roll;
-            if (s.cost != nullptr) s.cost[i] = (uint8_t)(d.iters >= 1020 ? 255 : (d.iters + 3) / 4);
         }
         if (b.mode == TROLL && !(b.effect_stamp > b.clock)) {
             // PetrifyTroll (full.py:1800) of a troll due: fixed, at rest (velocity and old velocity), mLastG cleared,
@@ -312,7 +311,7 @@ __global__ void __launch_bounds__(256) records_kernel(EbbFlightState s, Records 
 
 // The plain tick: one thread a row, every warp's 32 rows through the warp's orientation step together (rows past n
 // pass through it)
-__global__ void __launch_bounds__(256) tick_kernel(EbbFlightState s, Records r) {
+__global__ void __launch_bounds__(256, 1) tick_kernel(EbbFlightState s, Records r) {
     __shared__ float ndt_tab[TORQUE_STEPS];
     __shared__ float ktab[(256 / 32) * KTAB_FLOATS];
     fill_ndt(ndt_tab, s.dt);
@@ -353,30 +352,24 @@ struct SlotRec {
     int32_t act;
 };
 
-constexpr int COST_BUCKETS = 16;
-
-// One tile at a time (a run of whole worlds, rows [r0, r1)): the records pass into shared memory, then the ships'
-// ticks in the order of their last tick's search cost (the `cost` hint: ships of similar cost share a warp, so the
-// torque searches diverge less), each thread taking ships j = t, t + blockDim, ... of that order. The order decides
-// only which thread runs which ship: every ship's tick is the same computation whatever its thread.
 __host__ __device__ inline size_t tiled_records_bytes(int cap) {
-    return ((size_t)cap * (sizeof(SlotRec) + sizeof(uint16_t) + 1) + 15) & ~(size_t)15;
+    return ((size_t)cap * sizeof(SlotRec) + 15) & ~(size_t)15;
 }
 
-__global__ void __launch_bounds__(256, 2) tiled_kernel(EbbFlightState s, const int64_t* __restrict__ tile_rows,
-                                                       int64_t tiles, int cap, int32_t* status) {
-    extern __shared__ unsigned char smem_raw[];
+// One tile at a time (a run of whole worlds, rows [r0, r1)): the records pass into shared memory, then the tile's
+// ships' ticks, each warp taking 32 ships at a time through the warp's orientation step. With one tile a block (grid
+// = tiles) the block ends with its tile; a persistent grid (grid < tiles) syncs before reusing the records.
+__global__ void __launch_bounds__(256, 1) tiled_kernel(EbbFlightState s, const int64_t* __restrict__ tile_rows,
+                                                    int64_t tiles, int cap, int32_t* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ float ndt_tab[TORQUE_STEPS];
-    __shared__ int bucket_count[COST_BUCKETS], bucket_next[COST_BUCKETS];
+    SlotRec* rec = (SlotRec*)smem_raw;
+    float* ktab = (float*)(smem_raw + tiled_records_bytes(cap)) + (threadIdx.x >> 5) * KTAB_FLOATS;
     fill_ndt(ndt_tab, s.dt);
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int64_t r0 = tile_rows[tile], r1 = tile_rows[tile + 1];
         const int m = (int)(r1 - r0);
-        SlotRec* rec = (SlotRec*)smem_raw;
-        uint16_t* order = (uint16_t*)(rec + m);
-        uint8_t* bucket = (uint8_t*)(order + m);
-        if (threadIdx.x < COST_BUCKETS) bucket_count[threadIdx.x] = 0;
-        __syncthreads();
+        if (tile != blockIdx.x) __syncthreads();                     // the previous tile's records are done with
         for (int j = threadIdx.x; j < m; j += blockDim.x) {           // the records pass, into shared memory
             const int64_t i = r0 + j;
             bool act;
@@ -394,32 +387,16 @@ __global__ void __launch_bounds__(256, 2) tiled_kernel(EbbFlightState s, const i
             q.id = s.ids[i];
             q.radius = s.radius[i];
             q.act = act ? 1 : 0;
-            const int b = s.cost != nullptr ? (s.cost[i] >> 4) : 0;
-            bucket[j] = (uint8_t)b;
-            atomicAdd(&bucket_count[b], 1);
         }
         __syncthreads();
-        if (threadIdx.x == 0) {                                       // each bucket's first slot in the order
-            int acc = 0;
-            for (int b = 0; b < COST_BUCKETS; ++b) {
-                bucket_next[b] = acc;
-                acc += bucket_count[b];
-            }
-        }
-        __syncthreads();
-        for (int j = threadIdx.x; j < m; j += blockDim.x) order[atomicAdd(&bucket_next[bucket[j]], 1)] = (uint16_t)j;
-        __syncthreads();
-        float* ktab = (float*)(smem_raw + tiled_records_bytes(cap)) + (threadIdx.x >> 5) * KTAB_FLOATS;
         for (int base = threadIdx.x & ~31; base < m; base += blockDim.x) {   // warp-uniform: each warp's 32 ships
-            const int k = base + (threadIdx.x & 31);
-            const bool mine = k < m;
+            const int j = base + (threadIdx.x & 31);
+            const bool mine = j < m;
             DoLane d;
             d.on = false;
             bool release_after = false;
-            int64_t i = r0;
+            const int64_t i = r0 + j;
             if (mine) {
-                const int j = order[k];
-                i = r0 + j;
                 View tgt;
                 const int64_t t = s.follow_ptr[i];
                 tgt.valid = t >= r0 && t < r1;
@@ -441,7 +418,6 @@ __global__ void __launch_bounds__(256, 2) tiled_kernel(EbbFlightState s, const i
             orient_warp(d, cfg_of(s), ndt_tab, ktab);
             if (mine) tick_end(s, i, d, release_after);
         }
-        __syncthreads();                                              // the slots are the next tile's
     }
 }
 

@@ -388,7 +388,6 @@ struct Turn {
     double dt;
     float fdt;
     const float* ndt_tab;                      // float(n dt) for n = 0 .. TORQUE_STEPS - 1 (shared memory)
-    int iters;                                 // the searches' steps this tick (a scheduling hint, not state)
 };
 
 // float(n dt)

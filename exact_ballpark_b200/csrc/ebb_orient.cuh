@@ -35,7 +35,6 @@ struct DoLane {
     float roll;
     F4 rot1;
     F3 w1;
-    int iters;               // out: the candidate steps the serial loops would have taken (the cost hint)
 };
 
 __device__ __forceinline__ float wbc(float v, int src) { return __shfl_sync(FULL_WARP, v, src); }
@@ -122,7 +121,6 @@ __device__ __forceinline__ void orient_warp(DoLane& d, const Cfg& c, const float
     d.roll = 0.0f;
     d.rot1 = d.r0;
     d.w1 = d.w0;
-    d.iters = 0;
     PowCache pc;
     pow_cache_clear(pc);
     Turn t;
@@ -220,7 +218,6 @@ __device__ __forceinline__ void orient_warp(DoLane& d, const Cfg& c, const float
                 h_n1 = n1;
                 h_alpha1 = a1;
                 h_kappa1 = k1;
-                d.iters += n1;
             }
         }
         if (h_active) {
@@ -307,7 +304,6 @@ __device__ __forceinline__ void orient_warp(DoLane& d, const Cfg& c, const float
                 r_n1 = n1;
                 r_alpha1 = a1;
                 r_kappa1 = k1;
-                d.iters += n1;
             }
         }
         if (r_active) {

@@ -134,7 +134,6 @@ class VecModesPark:
         self._follow_ptr.fill_(-1)
         self._mode.fill_(STOP)
         self.bubble.fill_(-1)
-        self._cost = torch.zeros(n, dtype=torch.uint8, device=dev)   # the tiled schedule's ordering hint
         self._scratch = None
         self.plan: TilePlan | None = None
         self._status = torch.zeros(1, dtype=I32, device=dev)
@@ -162,7 +161,6 @@ class VecModesPark:
             s.new_orbit, s.dynamical = int(self.use_new_orbit), int(self.dynamical_orientation)
             for name, _, _ in _STORAGE:
                 setattr(s, _STATE_FIELD.get(name, name), getattr(self, "_" + name).data_ptr())
-            s.cost = self._cost.data_ptr()
             self._state = s
         return self._state
 

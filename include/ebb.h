@@ -37,8 +37,6 @@ typedef struct EbbFlightState {
     int64_t *ids, *effect_stamp, *follow_id, *owner_id, *clock;
     int32_t *mode, *follow_ptr;                                /* follow_ptr: the target's row, -1 for none */
     uint8_t *free_, *moribund, *massive, *interactive, *sensor;
-    uint8_t* cost;                /* optional (may be NULL): each ship's last torque-search cost, written by the tick
-                                     and read by the tiled schedule to order a tile's ships; never part of the state */
 } EbbFlightState;
 
 /* The ABI version (EBB_ABI_VERSION). Replaces xbpm_abi / xbpo_abi (exact_ballpark/vec_modes_cuda.cu:750,
@@ -62,10 +60,10 @@ int ebb_flight_tick(const EbbFlightState* s, void* scratch, int64_t scratch_byte
 /* The same tick with the worlds packed into tiles, one thread block a tile, the prepass's records in shared memory
  * (no scratch, one launch): tile_rows[0..tiles] are row offsets, each tile a run of whole worlds of at most
  * `tile_cap` rows (<= 4096), rows of a world contiguous; `block` threads (a multiple of 32, <= 256) take the tile's
- * ships in the order of the cost hint (s->cost, when given). status[0] is set nonzero if a follow_ptr leaves its tile
- * (the ship is then ticked without its target, as a missing target). The grid is persistent: `grid` blocks take tiles
- * in turn. The tile size, block and grid are the autotuner's choice (exact_ballpark_b200.tiles). No counterpart in
- * the reference (its tick is two launches, xbpm_tick). */
+ * ships 32 to a warp. status[0] is set nonzero if a follow_ptr leaves its tile (the ship is then ticked without its
+ * target, as a missing target). The grid is persistent: `grid` blocks take tiles in turn. The tile size, block and
+ * grid are the autotuner's choice (exact_ballpark_b200.autotune). No counterpart in the reference (its tick is two
+ * launches, xbpm_tick). */
 int ebb_flight_tick_tiled(const EbbFlightState* s, const int64_t* tile_rows, int64_t tiles, int tile_cap,
                           int32_t* status, void* stream, int block, int grid);
 
