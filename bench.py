@@ -242,9 +242,9 @@ def main() -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    for _ in range(args.warmup):                                     # warm-up ticks (they also warm the cost hint)
+    for _ in range(args.warmup):                                     # warm-up ticks
         park.evolve()
-        tick_plain(plain)
+        tick_plain(plain, 256)
         plain.current_time += 1
     tuning = autotune(park)                                          # the tiled plan, the park's state unchanged
     plan = park.plan
@@ -254,7 +254,7 @@ def main() -> None:
         barrier()
         ms_tiled = timed(graph.tick, args.steps)
         barrier()
-        ms_plain = timed(lambda: tick_plain(plain), args.steps)
+        ms_plain = timed(lambda: tick_plain(plain, 256), args.steps)
         barrier()
     clocks = clk.summary()
     ms_tiled, ms_plain = max_over_ranks(ms_tiled), max_over_ranks(ms_plain)
@@ -295,11 +295,11 @@ def main() -> None:
             "warmup": args.warmup, "ms_per_step": per_tiled, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64/f32", "data": "synthetic (seeded)",
             "config": dict(_config(args, "tiled: worlds packed in tiles, one block a tile, records in shared memory, "
-                                         "ships in cost order, one launch, CUDA graph"),
+                                         "warp-cooperative torque searches, one launch, CUDA graph"),
                            plan={"tile_rows_max": plan.cap, "block": plan.block, "grid": plan.grid, "tiles": plan.tiles,
                                  "candidates_timed": len(tuning)}),
             "plain": {"value": total_ships * args.steps / (ms_plain / 1e3), "ms_per_step": per_plain,
-                      "schedule": "plain: records pass + tick, two launches, records in scratch"},
+                      "schedule": "plain: records pass + tick, two launches, records in scratch, 256-thread blocks"},
             "speedup_tiled_vs_plain": per_plain / per_tiled,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,

@@ -15,12 +15,9 @@ from .tiles import plan_tiles
 
 def candidates(sm_count: int) -> list:
     out = []
-    for cap in (32, 64, 128, 256, 512):
-        for block in (32, 64, 128, 256):
-            if block > cap:
-                continue
-            for per_sm in (None, 8, 16):
-                out.append((cap, block, None if per_sm is None else per_sm * sm_count))
+    for cap, block in ((128, 128), (256, 128), (256, 256), (384, 256), (512, 256)):
+        for per_sm in (None, 3, 6):
+            out.append((cap, block, None if per_sm is None else per_sm * sm_count))
     return out
 
 

@@ -20,6 +20,15 @@
 #include "ebb_flight.cuh"
 #include "ebb_orient.cuh"
 
+// Resident blocks a multiprocessor is asked to fit (the register budget the compiler gets), per schedule
+// (3: 80 registers a thread, 24 warps a multiprocessor; measured fastest for both schedules on B200)
+#ifndef EBB_TICK_MIN_BLOCKS
+#define EBB_TICK_MIN_BLOCKS 3
+#endif
+#ifndef EBB_TILED_MIN_BLOCKS
+#define EBB_TILED_MIN_BLOCKS 3
+#endif
+
 namespace ebb {
 namespace flight {
 
@@ -311,7 +320,7 @@ __global__ void __launch_bounds__(256) records_kernel(EbbFlightState s, Records 
 
 // The plain tick: one thread a row, every warp's 32 rows through the warp's orientation step together (rows past n
 // pass through it)
-__global__ void __launch_bounds__(256, 1) tick_kernel(EbbFlightState s, Records r) {
+__global__ void __launch_bounds__(256, EBB_TICK_MIN_BLOCKS) tick_kernel(EbbFlightState s, Records r) {
     __shared__ float ndt_tab[TORQUE_STEPS];
     __shared__ float ktab[(256 / 32) * KTAB_FLOATS];
     fill_ndt(ndt_tab, s.dt);
@@ -359,7 +368,7 @@ __host__ __device__ inline size_t tiled_records_bytes(int cap) {
 // One tile at a time (a run of whole worlds, rows [r0, r1)): the records pass into shared memory, then the tile's
 // ships' ticks, each warp taking 32 ships at a time through the warp's orientation step. With one tile a block (grid
 // = tiles) the block ends with its tile; a persistent grid (grid < tiles) syncs before reusing the records.
-__global__ void __launch_bounds__(256, 1) tiled_kernel(EbbFlightState s, const int64_t* __restrict__ tile_rows,
+__global__ void __launch_bounds__(256, EBB_TILED_MIN_BLOCKS) tiled_kernel(EbbFlightState s, const int64_t* __restrict__ tile_rows,
                                                     int64_t tiles, int cap, int32_t* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ float ndt_tab[TORQUE_STEPS];

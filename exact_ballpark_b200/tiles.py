@@ -16,7 +16,7 @@ from dataclasses import dataclass, field
 
 import torch
 
-DEFAULT_CAP = 512
+DEFAULT_CAP = 256
 DEFAULT_BLOCK = 256
 MAX_CAP = 4096
 
