@@ -44,6 +44,7 @@ def lib() -> ctypes.CDLL:
     L.ebb_flight_scratch_bytes.restype = i64
     L.ebb_flight_scratch_bytes.argtypes = [i64]
     L.ebb_flight_tick.argtypes = [ctypes.POINTER(FlightState), p, i64, p, i32]
+    L.ebb_flight_tick_noalloc.argtypes = [ctypes.POINTER(FlightState), p, i32]
     L.ebb_flight_tick_tiled.argtypes = [ctypes.POINTER(FlightState), p, i64, i32, p, p, i32, i32]
     L.ebb_flight_snap.argtypes = [ctypes.POINTER(FlightState), p, i32, p, i32]
     L.ebb_flight_decay.argtypes = [ctypes.POINTER(FlightState), p, ctypes.c_double, p, i32]

@@ -16,6 +16,8 @@
 //   each ship's state once and never touches scratch.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "../../include/ebb.h"
 #include "ebb_flight.cuh"
 #include "ebb_orient.cuh"
@@ -287,7 +289,7 @@ struct Records {
     uint8_t* act;                                                     // [n]
 };
 
-__host__ __device__ inline int64_t align256(int64_t b) { return (b + 255) & ~(int64_t)255; }
+__host__ __device__ constexpr int64_t align256(int64_t b) { return (b + 255) & ~(int64_t)255; }
 
 __host__ __device__ inline Records records_in(void* scratch, int64_t n) {
     char* p = (char*)scratch;
@@ -302,9 +304,14 @@ __host__ __device__ inline Records records_in(void* scratch, int64_t n) {
     return r;
 }
 
-__host__ __device__ inline int64_t records_bytes(int64_t n) {
+__host__ __device__ constexpr int64_t records_bytes(int64_t n) {
     return align256(3 * n * 8) * 2 + align256(n * 8) + align256(n);
 }
+
+// The records of ebb_flight_tick_noalloc, for callers that cannot allocate device memory: a fixed array in the
+// library's own device memory, sized for EBB_NOALLOC_MAX_ROWS rows (records_bytes of that count, about 14.4 MB).
+// Every device that loads the library holds it until the process exits, and every call on a device shares it.
+__device__ __align__(256) static unsigned char noalloc_records[records_bytes(EBB_NOALLOC_MAX_ROWS)];
 
 __global__ void __launch_bounds__(256) records_kernel(EbbFlightState s, Records r) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -508,6 +515,7 @@ int ebb_abi(void) { return EBB_ABI_VERSION; }
 
 const char* ebb_error_string(int code) {
     if (code == EBB_EINVAL) return "refused: invalid arguments (block size, scratch, tiles)";
+    if (code == EBB_ETOOBIG) return "refused: more rows than the allocation-free tick holds (EBB_NOALLOC_MAX_ROWS)";
     return cudaGetErrorString((cudaError_t)code);
 }
 
@@ -520,6 +528,38 @@ int ebb_flight_tick(const EbbFlightState* s, void* scratch, int64_t scratch_byte
         scratch_bytes < ebb_flight_scratch_bytes(s->n))
         return EBB_EINVAL;
     const ebb::flight::Records r = ebb::flight::records_in(scratch, s->n);
+    const cudaStream_t st = (cudaStream_t)stream;
+    ebb::flight::records_kernel<<<grid_of(s->n, block), block, 0, st>>>(*s, r);
+    int rc = launched();
+    if (rc) return rc;
+    ebb::flight::tick_kernel<<<grid_of(s->n, block), block, 0, st>>>(*s, r);
+    return launched();
+}
+
+// ebb_flight_tick_noalloc's set-up: the device address of noalloc_records, one a device. In host code the array's
+// name stands for a host-side shadow, not device memory, so the kernels get the address cudaGetSymbolAddress gives
+// with the device current; it is looked up on the first call on each device and kept.
+static std::atomic<uintptr_t> noalloc_address[EBB_NOALLOC_MAX_DEVICES];
+
+int ebb_flight_tick_noalloc(const EbbFlightState* s, void* stream, int block) {
+    if (s == nullptr) return EBB_EINVAL;
+    if (s->n <= 0) return 0;
+    if (s->n > EBB_NOALLOC_MAX_ROWS) return EBB_ETOOBIG;
+    if (!block_ok(block, 256)) return EBB_EINVAL;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (int)e;
+    if (dev < 0 || dev >= EBB_NOALLOC_MAX_DEVICES) return EBB_EINVAL;
+    uintptr_t addr = noalloc_address[dev].load(std::memory_order_acquire);
+    if (addr == 0) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, ebb::flight::noalloc_records);
+        if (e != cudaSuccess) return (int)e;
+        addr = (uintptr_t)p;
+        noalloc_address[dev].store(addr, std::memory_order_release);
+    }
+    // Every record a tick reads (rows below n) is written by the records pass first: nothing needs clearing.
+    const ebb::flight::Records r = ebb::flight::records_in((void*)addr, s->n);
     const cudaStream_t st = (cudaStream_t)stream;
     ebb::flight::records_kernel<<<grid_of(s->n, block), block, 0, st>>>(*s, r);
     int rc = launched();

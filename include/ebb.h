@@ -20,6 +20,11 @@ extern "C" {
 
 #define EBB_ABI_VERSION 1
 #define EBB_EINVAL (-1)
+#define EBB_ETOOBIG (-2)
+
+/* The allocation-free tick's limits: rows its fixed records buffer holds, and devices it keeps an address for. */
+#define EBB_NOALLOC_MAX_ROWS 262144
+#define EBB_NOALLOC_MAX_DEVICES 64
 
 /* The flight-mode park (one row a ship; rows grouped in worlds by the caller), field for field the state the
  * reference's xbpm_tick reads and writes (exact_ballpark/vec_modes_cuda.cu:83-96), laid out as above. */
@@ -56,6 +61,17 @@ int64_t ebb_flight_scratch_bytes(int64_t n);
  * Replaces xbpm_tick (exact_ballpark/vec_modes_cuda.cu:754), which exact_ballpark.vec_modes_cuda.tick calls
  * (vec_modes_cuda.py:322). */
 int ebb_flight_tick(const EbbFlightState* s, void* scratch, int64_t scratch_bytes, void* stream, int block);
+
+/* ebb_flight_tick without caller scratch, for callers that cannot allocate device memory: an engine whose own
+ * allocator owns the GPU's memory and hands none out, a loop that must not allocate once it runs, or a binding from a
+ * language with no CUDA allocator at hand. The records go to a fixed buffer inside the library (EBB_NOALLOC_MAX_ROWS
+ * rows, about 14.4 MB of device memory on every device that loads the library, held until the process exits), so
+ * parks of more rows are refused with EBB_ETOOBIG, nothing launched. The same kernels and results as ebb_flight_tick.
+ * The first call on a device looks up the buffer's device address (cudaGetSymbolAddress, with that device current);
+ * make that first call before any stream capture. All calls on a device share the buffer: calls that may overlap on
+ * the GPU (other streams, other threads) race on it and must be ordered by the caller. Each call writes every record
+ * it reads, so the buffer needs no clearing. No counterpart in the reference. */
+int ebb_flight_tick_noalloc(const EbbFlightState* s, void* stream, int block);
 
 /* The same tick with the worlds packed into tiles, one thread block a tile, the prepass's records in shared memory
  * (no scratch, one launch): tile_rows[0..tiles] are row offsets, each tile a run of whole worlds of at most
