@@ -4,6 +4,6 @@ The drop-in API is exact_ballpark.vec_modes / vec_modes_cuda's: `VecModesPark`, 
 `kernel_info`. The tick runs in the native library libebb.so (csrc/, C ABI in include/ebb.h).
 """
 
-from .modes import (VecModesPark, ModesGraph, kernel_info, libm, tick, tick_plain, tick_tiled)  # noqa: F401
+from .modes import (VecModesPark, ModesGraph, kernel_info, libm, tick, tick_plain, tick_tiled, tick_worlds)  # noqa: F401
 
-__all__ = ["VecModesPark", "ModesGraph", "kernel_info", "libm", "tick", "tick_plain", "tick_tiled"]
+__all__ = ["VecModesPark", "ModesGraph", "kernel_info", "libm", "tick", "tick_plain", "tick_tiled", "tick_worlds"]

@@ -441,6 +441,222 @@ __host__ __device__ inline size_t tiled_smem_bytes(int cap, int block) {
     return tiled_records_bytes(cap) + (size_t)(block / 32) * KTAB_FLOATS * sizeof(float);
 }
 
+// ================================================================================================ listed worlds
+
+// The listed-worlds tick's shared records: one slot a row of the tile, with the slot's world (its index in the tile)
+struct ListRec {
+    double px, py, pz, vx, vy, vz, vy_after;
+    int64_t id;
+    float radius;
+    int32_t act;
+    int32_t world;
+    int32_t pad;
+};
+
+__host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+// Shared memory of a listed-worlds tile of `cap` rows and at most `cap` worlds: the records, each world's first row
+// (int64) and first slot (int32, plus the end), then the warps' kappa tables
+__host__ __device__ inline size_t listed_tables_bytes(int cap) {
+    return align16((size_t)cap * sizeof(ListRec)) + align16((size_t)cap * 8) + align16((size_t)(cap + 1) * 4);
+}
+__host__ __device__ inline size_t listed_smem_bytes(int cap, int block) {
+    return listed_tables_bytes(cap) + (size_t)(block / 32) * KTAB_FLOATS * sizeof(float);
+}
+
+// One tick of a list of worlds anywhere in the park: world w is rows [worlds[2w], worlds[2w + 1]), a tile is the
+// worlds [tile_worlds[t], tile_worlds[t + 1]) (at most cap rows), and each tile's rows are gathered into shared-memory
+// slots world after world. Rows in no listed world are not read or written; rows with active[i] == 0 (when `active`
+// is given) are not ticked, though their records are made for the rest of their world (OnTick's per-world mask, in
+// the kernel). status: bit 1 a follow pointer leaving its world (the ship ticks without its target), bit 2 a malformed
+// tile (rows outside the park, more than cap rows or worlds: skipped).
+__global__ void __launch_bounds__(256, EBB_TILED_MIN_BLOCKS)
+    worlds_kernel(EbbFlightState s, const int64_t* __restrict__ worlds, const int64_t* __restrict__ tile_worlds,
+                  int64_t tiles, int cap, const uint8_t* __restrict__ active, int32_t* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ float ndt_tab[TORQUE_STEPS];
+    __shared__ int tile_rows;
+    ListRec* rec = (ListRec*)smem_raw;
+    int64_t* wrow = (int64_t*)(smem_raw + align16((size_t)cap * sizeof(ListRec)));
+    int32_t* wslot = (int32_t*)(smem_raw + align16((size_t)cap * sizeof(ListRec)) + align16((size_t)cap * 8));
+    float* ktab = (float*)(smem_raw + listed_tables_bytes(cap)) + (threadIdx.x >> 5) * KTAB_FLOATS;
+    fill_ndt(ndt_tab, s.dt);
+    const int lane = threadIdx.x & 31;
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        if (tile != blockIdx.x) __syncthreads();                     // the previous tile's tables are done with
+        const int64_t w0 = tile_worlds[tile], nw64 = tile_worlds[tile + 1] - w0;
+        if (nw64 <= 0 || nw64 > cap) {                                // block-uniform
+            if (nw64 != 0 && threadIdx.x == 0) atomicOr(status, 2);
+            continue;
+        }
+        const int nw = (int)nw64;
+        if (threadIdx.x < 32) {                                       // warp 0: the worlds' slot offsets (a scan)
+            int carry = 0;
+            bool bad = false;
+            for (int k0 = 0; k0 < nw; k0 += 32) {
+                const int k = k0 + lane;
+                int64_t b = 0, len = 0;
+                if (k < nw) {
+                    b = worlds[2 * (w0 + k)];
+                    len = worlds[2 * (w0 + k) + 1] - b;
+                    if (b < 0 || len < 0 || len > cap || b + len > s.n) {
+                        bad = true;
+                        len = 0;
+                    }
+                }
+                int c = (int)len;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, c, o);
+                    if (lane >= o) c += y;
+                }
+                if (k < nw) {
+                    wrow[k] = b;
+                    wslot[k] = carry + c - (int)len;
+                }
+                carry += __shfl_sync(0xffffffffu, c, 31);
+                if (carry > cap) bad = true;
+            }
+            bad = __any_sync(0xffffffffu, bad);
+            if (lane == 0) {
+                wslot[nw] = carry;
+                tile_rows = bad ? -1 : carry;
+            }
+        }
+        __syncthreads();
+        const int m = tile_rows;
+        if (m < 0) {                                                  // block-uniform
+            if (threadIdx.x == 0) atomicOr(status, 2);
+            continue;
+        }
+        for (int j = threadIdx.x; j < m; j += blockDim.x) {           // the records pass, into shared memory
+            int lo = 0, hi = nw - 1;                                  // the slot's world: the last k with wslot[k] <= j
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (wslot[mid] <= j) lo = mid;
+                else hi = mid - 1;
+            }
+            const int64_t i = wrow[lo] + (j - wslot[lo]);
+            bool act;
+            double vy_after;
+            records_of(s, i, &act, &vy_after);
+            ListRec& q = rec[j];
+            const D3 p = ld3(s.pos, i, s.n), v = ld3(s.vel, i, s.n);
+            q.px = p.x;
+            q.py = p.y;
+            q.pz = p.z;
+            q.vx = v.x;
+            q.vy = v.y;
+            q.vz = v.z;
+            q.vy_after = vy_after;
+            q.id = s.ids[i];
+            q.radius = s.radius[i];
+            q.act = act ? 1 : 0;
+            q.world = lo;
+        }
+        __syncthreads();
+        for (int base = threadIdx.x & ~31; base < m; base += blockDim.x) {   // warp-uniform: each warp's 32 slots
+            const int j = base + lane;
+            bool mine = j < m;
+            int64_t i = 0;
+            int e = 0;
+            if (mine) {
+                e = rec[j].world;
+                i = wrow[e] + (j - wslot[e]);
+                if (active != nullptr && active[i] == 0) mine = false;
+            }
+            DoLane d;
+            d.on = false;
+            bool release_after = false;
+            if (mine) {
+                View tgt;
+                const int64_t t = s.follow_ptr[i];
+                const int64_t b = wrow[e], len = wslot[e + 1] - wslot[e];
+                tgt.valid = t >= b && t < b + len;
+                if (!tgt.valid && t >= 0 && t < s.n) atomicOr(status, 1);    // a target outside its world
+                if (tgt.valid) {
+                    const ListRec& q = rec[wslot[e] + (int)(t - b)];
+                    tgt.pos = D3{q.px, q.py, q.pz};
+                    tgt.vel = D3{q.vx, q.vy, q.vz};
+                    tgt.vy_after = q.vy_after;
+                    tgt.id = q.id;
+                    tgt.radius = q.radius;
+                    tgt.act = q.act != 0;
+                } else {
+                    tgt.act = false;
+                    tgt.id = 0;
+                }
+                tick_begin(s, i, tgt, rec[j].act != 0, d, &release_after);
+            }
+            orient_warp(d, cfg_of(s), ndt_tab, ktab);
+            if (mine) tick_end(s, i, d, release_after);
+        }
+    }
+}
+
+// ================================================================================================ moving worlds
+
+// Rows copied from one park to another (a world admitted into a resident park, or taken out of it): every field of
+// src row src_rows[k] into dst row dst_rows[k]. A follow pointer moves with its row (a world moves as one run, so its
+// target moves by the same number of rows); one that would leave dst becomes -1 (status bit 4), as do rows outside
+// either park (skipped).
+__global__ void move_kernel(EbbFlightState dst, EbbFlightState src, const int64_t* __restrict__ src_rows,
+                            const int64_t* __restrict__ dst_rows, int64_t m, int32_t* status) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const int64_t a = src_rows[k], b = dst_rows[k];
+    if (a < 0 || a >= src.n || b < 0 || b >= dst.n) {
+        atomicOr(status, 4);
+        return;
+    }
+    const int64_t sn = src.n, dn = dst.n;
+#define EBB_MOVE(f, planes)                                                                                      \
+    for (int p = 0; p < (planes); ++p) dst.f[p * dn + b] = src.f[p * sn + a];
+    EBB_MOVE(pos, 3)
+    EBB_MOVE(vel, 3)
+    EBB_MOVE(old_pos, 3)
+    EBB_MOVE(old_vel, 3)
+    EBB_MOVE(goto_pt, 3)
+    EBB_MOVE(last_g, 3)
+    EBB_MOVE(mass, 1)
+    EBB_MOVE(time_factor, 1)
+    EBB_MOVE(last_collision, 1)
+    EBB_MOVE(radius, 1)
+    EBB_MOVE(max_vel, 1)
+    EBB_MOVE(agility, 1)
+    EBB_MOVE(speed_fraction, 1)
+    EBB_MOVE(follow_range, 1)
+    EBB_MOVE(max_ang_vel, 1)
+    EBB_MOVE(rot_agility, 1)
+    EBB_MOVE(rot_roll, 1)
+    EBB_MOVE(rot, 4)
+    EBB_MOVE(old_rot, 4)
+    EBB_MOVE(ang_vel, 3)
+    EBB_MOVE(old_ang_vel, 3)
+    EBB_MOVE(torque, 3)
+    EBB_MOVE(ids, 1)
+    EBB_MOVE(effect_stamp, 1)
+    EBB_MOVE(follow_id, 1)
+    EBB_MOVE(owner_id, 1)
+    EBB_MOVE(clock, 1)
+    EBB_MOVE(mode, 1)
+    EBB_MOVE(free_, 1)
+    EBB_MOVE(moribund, 1)
+    EBB_MOVE(massive, 1)
+    EBB_MOVE(interactive, 1)
+    EBB_MOVE(sensor, 1)
+#undef EBB_MOVE
+    const int32_t fp = src.follow_ptr[a];
+    int64_t q = fp;
+    if (fp >= 0) {
+        q = (int64_t)fp + (b - a);
+        if (q < 0 || q >= dn || q > INT32_MAX) {
+            atomicOr(status, 4);
+            q = -1;
+        }
+    }
+    dst.follow_ptr[b] = (int32_t)q;
+}
+
 // ================================================================================================ set-up kernels
 
 __global__ void snap_kernel(EbbFlightState s, const uint8_t* __restrict__ mask, int fresh) {
@@ -586,6 +802,34 @@ int ebb_flight_tick_tiled(const EbbFlightState* s, const int64_t* tile_rows, int
     return launched();
 }
 
+int ebb_flight_tick_worlds(const EbbFlightState* s, const int64_t* worlds, const int64_t* tile_worlds, int64_t tiles,
+                           int tile_cap, const uint8_t* active, int32_t* status, void* stream, int block, int grid) {
+    if (s == nullptr) return EBB_EINVAL;
+    if (s->n <= 0 || tiles <= 0) return 0;
+    if (!block_ok(block, 256) || tile_cap <= 0 || tile_cap > EBB_WORLDS_MAX_TILE || worlds == nullptr ||
+        tile_worlds == nullptr || status == nullptr || grid <= 0)
+        return EBB_EINVAL;
+    const size_t smem = ebb::flight::listed_smem_bytes(tile_cap, block);
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(ebb::flight::worlds_kernel,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
+    ebb::flight::worlds_kernel<<<(unsigned)grid, block, smem, (cudaStream_t)stream>>>(*s, worlds, tile_worlds, tiles,
+                                                                                      tile_cap, active, status);
+    return launched();
+}
+
+int ebb_flight_move(const EbbFlightState* dst, const EbbFlightState* src, const int64_t* src_rows,
+                    const int64_t* dst_rows, int64_t m, int32_t* status, void* stream, int block) {
+    if (dst == nullptr || src == nullptr) return EBB_EINVAL;
+    if (m <= 0) return 0;
+    if (!block_ok(block, 1024) || src_rows == nullptr || dst_rows == nullptr || status == nullptr) return EBB_EINVAL;
+    ebb::flight::move_kernel<<<grid_of(m, block), block, 0, (cudaStream_t)stream>>>(*dst, *src, src_rows, dst_rows, m,
+                                                                                    status);
+    return launched();
+}
+
 int ebb_flight_snap(const EbbFlightState* s, const uint8_t* mask, int fresh, void* stream, int block) {
     if (s == nullptr || mask == nullptr) return EBB_EINVAL;
     if (s->n <= 0) return 0;
@@ -618,6 +862,8 @@ int ebb_kernel_info(int which, int* regs, int* local_bytes, int* binary_version,
         case 0: e = cudaFuncGetAttributes(&fa, ebb::flight::tick_kernel); break;
         case 1: e = cudaFuncGetAttributes(&fa, ebb::flight::records_kernel); break;
         case 2: e = cudaFuncGetAttributes(&fa, ebb::flight::tiled_kernel); break;
+        case 3: e = cudaFuncGetAttributes(&fa, ebb::flight::worlds_kernel); break;
+        case 4: e = cudaFuncGetAttributes(&fa, ebb::flight::move_kernel); break;
         default: return EBB_EINVAL;
     }
     if (e != cudaSuccess) return (int)e;

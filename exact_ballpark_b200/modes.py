@@ -513,9 +513,14 @@ class VecModesPark:
 
     def evolve(self, lib=None, active: torch.Tensor | None = None) -> None:
         """One tick of every world, in place, on the device, no host synchronisation. `active` [n] (OnTick's
-        per-world mask): only those rows tick, every other row keeps its state bit for bit."""
+        per-world mask): only those rows tick, every other row keeps its state bit for bit (inside the listed-worlds
+        kernel when the worlds are contiguous rows, else by a save and put-back around the tick)."""
         if active is not None:
-            masked_tick(self, active, lambda: tick(self, self.block))
+            act = torch.as_tensor(active).to(device=self.dev, dtype=BOOL).reshape(self.n).contiguous()
+            if _worlds_plan_ok(self):
+                tick_worlds(self, act)
+            else:
+                masked_tick(self, act, lambda: tick(self, self.block))
         else:
             tick(self, self.block)
         self.current_time += 1
@@ -551,6 +556,30 @@ def tick_tiled(park: VecModesPark, plan: TilePlan | None = None) -> None:
     _native.check(rc, "ebb_flight_tick_tiled")
 
 
+WORLDS_MAX_TILE = 1024          # include/ebb.h: EBB_WORLDS_MAX_TILE
+
+
+def _worlds_plan_ok(park: VecModesPark) -> bool:
+    return park.plan is not None and park.plan.cap <= WORLDS_MAX_TILE and len(park.plan.world_rows) > 1
+
+
+def tick_worlds(park: VecModesPark, active: torch.Tensor | None = None, plan: TilePlan | None = None) -> None:
+    """The listed-worlds schedule over the park's own worlds (its tile plan as a world list), with OnTick's row mask
+    `active` (a contiguous bool tensor [n], or None for every row) applied inside the kernel."""
+    plan = plan or park.plan
+    if plan is None:
+        raise ValueError("the park's worlds are not contiguous rows: no tile plan")
+    if not park.n:
+        return
+    worlds, tile_worlds = plan.worlds_on(park.dev)
+    act = 0 if active is None else active.data_ptr()
+    with torch.cuda.device(park.dev):
+        rc = _native.lib().ebb_flight_tick_worlds(ctypes.byref(park.state()), worlds.data_ptr(), tile_worlds.data_ptr(),
+                                                  plan.tiles, plan.cap, act, park._status.data_ptr(), park._stream(),
+                                                  plan.block, plan.grid)
+    _native.check(rc, "ebb_flight_tick_worlds")
+
+
 def tick(park: VecModesPark, block: int = 128, lib=None) -> None:
     """One tick in place on torch's current stream (the drop-in for exact_ballpark.vec_modes_cuda.tick): the tiled
     schedule when the park's worlds are contiguous rows, the plain one otherwise."""
@@ -576,7 +605,7 @@ def masked_tick(park: VecModesPark, active: torch.Tensor, run) -> None:
 def kernel_info(device=None) -> dict:
     """The kernels as loaded on a device: registers, local memory, binary and PTX versions."""
     out = {}
-    for which, name in ((0, "tick"), (1, "records"), (2, "tiled")):
+    for which, name in ((0, "tick"), (1, "records"), (2, "tiled"), (3, "worlds"), (4, "move")):
         vals = [ctypes.c_int() for _ in range(5)]
         with torch.cuda.device(torch.device(device or "cuda")):
             rc = _native.lib().ebb_kernel_info(which, *[ctypes.byref(v) for v in vals])
@@ -618,12 +647,18 @@ class ModesGraph:
         else:
             park.plan.tile_rows_on(park.dev)
         names = park.row_tensors()
-        self.saved = {k: torch.empty_like(getattr(park, k)) for k in names} if masked else {}
+        self.in_kernel = masked and _worlds_plan_ok(park)            # OnTick's mask inside the listed-worlds kernel
+        if self.in_kernel:
+            park.plan.worlds_on(park.dev)
+        self.saved = {k: torch.empty_like(getattr(park, k)) for k in names} if masked and not self.in_kernel else {}
         keep = {k: getattr(park, k).clone() for k in names}      # the warm-up tick is undone
         side = torch.cuda.Stream(device=park.dev)
         side.wait_stream(torch.cuda.current_stream(park.dev))
         with torch.cuda.stream(side):                                # a warm-up launch of every kernel
-            tick(park, self.block)
+            if self.in_kernel:
+                tick_worlds(park, self.mask)
+            else:
+                tick(park, self.block)
             for k, v in keep.items():
                 getattr(park, k).copy_(v)
         torch.cuda.current_stream(park.dev).wait_stream(side)
@@ -631,11 +666,14 @@ class ModesGraph:
         del keep
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph):
-            if masked:
-                self._save()
-            tick(park, self.block)
-            if masked:
-                self._put_back()
+            if self.in_kernel:
+                tick_worlds(park, self.mask)
+            else:
+                if masked:
+                    self._save()
+                tick(park, self.block)
+                if masked:
+                    self._put_back()
 
     def _save(self) -> None:
         for k, b in self.saved.items():

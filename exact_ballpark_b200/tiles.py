@@ -28,11 +28,27 @@ class TilePlan:
     block: int                 # threads a block (>= cap, a multiple of 32)
     grid: int                  # blocks of the persistent grid
     max_world: int             # the largest world's rows
+    world_rows: list = field(default_factory=list)   # the worlds' row offsets ([0, ..., n]), when known
     _dev: dict = field(default_factory=dict, repr=False)
 
     @property
     def tiles(self) -> int:
         return len(self.tile_rows) - 1
+
+    def worlds_on(self, dev) -> tuple:
+        """The same plan as a list of worlds (the listed-worlds tick's form): world w is rows [worlds[2w],
+        worlds[2w + 1]), tile t the worlds [tile_worlds[t], tile_worlds[t + 1]); device tensors, made once."""
+        key = "worlds:" + str(dev)
+        if key not in self._dev:
+            runs = self.world_rows
+            if len(runs) < 2:
+                raise ValueError("the plan was made without its world offsets")
+            pairs = [x for a, b in zip(runs[:-1], runs[1:]) for x in (a, b)]
+            index = {r: k for k, r in enumerate(runs)}
+            tile_worlds = [index[r] for r in self.tile_rows]
+            self._dev[key] = (torch.tensor(pairs, dtype=torch.int64, device=dev),
+                              torch.tensor(tile_worlds, dtype=torch.int64, device=dev))
+        return self._dev[key]
 
     def tile_rows_on(self, dev) -> torch.Tensor:
         key = str(dev)
@@ -80,4 +96,4 @@ def plan_tiles(world: torch.Tensor, cap: int = DEFAULT_CAP, block: int | None = 
     blk = block or DEFAULT_BLOCK
     if blk % 32 or not 32 <= blk <= 256:
         raise ValueError(f"block {blk}: a multiple of 32 up to 256")
-    return TilePlan(tile_rows, cap, blk, grid or (len(tile_rows) - 1), max_world)
+    return TilePlan(tile_rows, cap, blk, grid or (len(tile_rows) - 1), max_world, runs)

@@ -49,6 +49,41 @@ class FlightWorlds:
         park.orbit(b(self.orbit_mask), target, rng)
         park.warp_to(b(self.warp_mask), point, torch.full_like(rng, 20000.0), wf)
 
+    @property
+    def sizes(self) -> list:
+        """Each world's rows, in order."""
+        out = []
+        for r in self.rows:
+            if not out or r["world"] != last:
+                out.append(0)
+                last = r["world"]
+            out[-1] += 1
+        return out
+
+    @staticmethod
+    def concat(parts: list) -> "FlightWorlds":
+        """Several FlightWorlds as one: worlds renumbered in order, targets moved with their rows. Each world loads
+        and takes its commands as it does alone (a park's load and commands act on each world's own rows)."""
+        rows, fm, om, wm, tgt, rg, pt, wf = [], [], [], [], [], [], [], []
+        world = 0
+        for part in parts:
+            base = len(rows)
+            first = part.rows[0]["world"] if part.rows else 0
+            for r in part.rows:
+                q = dict(r)
+                q["world"] = world + (r["world"] - first)
+                rows.append(q)
+            world += part.worlds
+            fm += part.follow_mask
+            om += part.orbit_mask
+            wm += part.warp_mask
+            tgt += [t + base if t >= 0 else -1 for t in part.target]
+            rg += part.range_
+            pt += part.point
+            wf += part.warp_factor
+        ships = max((p.ships for p in parts), default=0)
+        return FlightWorlds(rows, fm, om, wm, tgt, rg, pt, wf, world, ships)
+
 
 def _unit(r: random.Random) -> list:
     while True:
@@ -92,3 +127,8 @@ def flight_worlds(seed: int, worlds: int, ships: int = 4) -> FlightWorlds:
                 pt.append([p[0] + u[0] * d, p[1] + u[1] * d, p[2] + u[2] * d])
                 wf.append(r.randint(3000, 10000))
     return FlightWorlds(rows, fm, om, wm, tgt, rg, pt, wf, worlds, ships)
+
+
+def ragged_ships(r: random.Random, max_ships: int) -> int:
+    """A world's ship count, log-uniform in [1, max_ships] (floor of 10^U(0, log10 max_ships))."""
+    return max(1, min(max_ships, int(10.0 ** r.uniform(0.0, math.log10(max_ships)))))

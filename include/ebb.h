@@ -83,6 +83,29 @@ int ebb_flight_tick_noalloc(const EbbFlightState* s, void* stream, int block);
 int ebb_flight_tick_tiled(const EbbFlightState* s, const int64_t* tile_rows, int64_t tiles, int tile_cap,
                           int32_t* status, void* stream, int block, int grid);
 
+/* Rows a tile of ebb_flight_tick_worlds holds at most. */
+#define EBB_WORLDS_MAX_TILE 1024
+
+/* One tick of a list of worlds, each a contiguous run of rows anywhere in the park (a serving loop's resident
+ * episodes, or the worlds with a tick under OnTick's mask): world w is rows [worlds[2w], worlds[2w + 1]), worlds never
+ * overlap; tile t is the worlds [tile_worlds[t], tile_worlds[t + 1]), at most `tile_cap` rows (<= EBB_WORLDS_MAX_TILE)
+ * and `tile_cap` worlds, gathered into one thread block's shared memory with their records; `grid` persistent blocks
+ * take the `tiles` tiles in turn. Rows of no listed world are neither read nor written. With `active` [n] non-null,
+ * rows whose byte is 0 keep their state bit for bit and the others tick as in the unmasked tick (OnTick's mask inside
+ * the kernel, in place of a save and put-back of every row). status[0] bits: 1 a follow pointer leaving its world
+ * (ticked without its target), 2 a malformed tile (skipped). Replaces the masked tick of
+ * exact_ballpark.vec_orient.masked_tick (vec_orient.py:217) over xbpm_tick (vec_modes_cuda.cu:754); the listing
+ * of worlds has no counterpart in the reference. */
+int ebb_flight_tick_worlds(const EbbFlightState* s, const int64_t* worlds, const int64_t* tile_worlds, int64_t tiles,
+                           int tile_cap, const uint8_t* active, int32_t* status, void* stream, int block, int grid);
+
+/* Rows copied between two parks, every field: src row src_rows[k] into dst row dst_rows[k], k < m (device arrays).
+ * A follow pointer moves with its row, so a world moved as one run keeps its targets; a pointer that would leave dst
+ * becomes -1, and rows outside either park are skipped (status[0] bit 4 for both). Admission and retirement of a
+ * serving loop's episodes. No counterpart in the reference (its parks are loaded whole). */
+int ebb_flight_move(const EbbFlightState* dst, const EbbFlightState* src, const int64_t* src_rows,
+                    const int64_t* dst_rows, int64_t m, int32_t* status, void* stream, int block);
+
 /* SnapOrientation of the rows in mask[n] (nonzero bytes): the rotation turned to the velocity and rolled upright,
  * the old rotation the same, the angular velocities zeroed (at a speed of 1e-6 m/s or less nothing changes). With
  * `fresh`, first the state of a new ball: rotation identity, old rotation rot x RotationQuaternion(angVel,
@@ -100,7 +123,8 @@ int ebb_flight_decay(const EbbFlightState* s, const uint8_t* mask, double neg_kd
  * vec_orient_cuda.cu:520). */
 int ebb_libm(int func, int64_t n, const double* x, const double* y, double* out, void* stream, int block);
 
-/* A kernel's resources as loaded on the current device: which 0 the plain tick, 1 the prepass, 2 the tiled tick.
+/* A kernel's resources as loaded on the current device: which 0 the plain tick, 1 the prepass, 2 the tiled tick,
+ * 3 the listed-worlds tick, 4 the row move.
  * Replaces xbpm_info (vec_modes_cuda.cu:766). */
 int ebb_kernel_info(int which, int* regs, int* local_bytes, int* binary_version, int* ptx_version, int* max_threads);
 
