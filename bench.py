@@ -14,7 +14,9 @@ times the same step through the public API from host buffers: every step a pinne
 speed fractions applied by set_speed_fraction (the values they hold, so the flight is unchanged), the tick, and a
 device->host copy of every position. `cpu_baseline` is the C++ oracle (a scalar port of the reference's algorithm)
 on the host's cores over a bounded sample. `--impl reference` times that CPU port on the whole workload instead (the
-reference's own implementation is Python; the port is its compiled restatement), rank 0 only.
+reference's own implementation is Python; the port is its compiled restatement), rank 0 only. `serve` runs the
+serving loop (continuous batching of arriving episodes, state resident under a byte budget): an open loop at the
+configured arrival rate, with p50/p99 step latency, and a saturated closed loop (bench.serve_runs).
 """
 
 from __future__ import annotations
@@ -32,7 +34,7 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "bit-exact ship-ticks/s on 1 B200 (ragged batch vs plain)"
+METRIC = "bit-exact ship-ticks/s on 1 B200 (ragged batch vs plain); serve p50/p99 latency"
 UNIT = "ship-ticks/s"
 # Algorithmic bytes a ship-tick reads and writes in the minimal (this package's) layout, dynamical orientation on:
 # reads 229 B (pos, vel, goto, last_g 4 x 24; mass, time factor, warp length 3 x 8; radius, max_vel, agility, speed
@@ -71,14 +73,26 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        self._wait_lines(1, 5.0)                 # sampling has started before the timed region
         return self
+
+    def _wait_lines(self, k: int, limit: float) -> int:
+        until = time.perf_counter() + limit
+        n = 0
+        while self.proc is not None and time.perf_counter() < until:
+            n = len(Path(self.path).read_text().splitlines())
+            if n >= k or self.proc.poll() is not None:
+                break
+            time.sleep(0.01)
+        return n
 
     def __exit__(self, *exc):
         if self.proc is not None:
+            self._wait_lines(self._wait_lines(0, 0.0) + 1, 1.0)   # one more sample after the timed region
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -159,6 +173,46 @@ def run_reference(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def serve_runs(args, dev) -> dict:
+    """The serving loop (exact_ballpark_b200.serving) on this GPU: an open loop of episodes arriving as a Poisson
+    process (--serve-rate a second, 1-256 ships log-uniform, 10-10,000 ticks log-uniform, flight-mode worlds), state
+    admitted under an --serve-budget-gb budget, for --serve-seconds of arrivals; then a saturated closed loop (every
+    episode waiting from the start, a 262,144-row budget, two steps in flight) for --serve-steps steps after
+    untimed warm-up steps (at least --serve-warmup, and until 90 % of the budget's rows are live). p50/p99 of each step's latency (host wall time from the step's
+    start to its tick's completion; with two steps in flight, to when the loop saw it complete), ship-ticks/s over the
+    wall time, and the tick launches' own device rate."""
+    import torch
+
+    from exact_ballpark_b200.serving import Server, episode_stream, serve
+    out = {}
+    count = int(args.serve_rate * args.serve_seconds)
+    eps = episode_stream(11, count, rate=args.serve_rate)
+    with Server(budget_bytes=args.serve_budget_gb * 1e9, device=dev, keep=False) as srv:
+        s = serve(srv, eps, realtime=True, max_steps=None if args.serve_all else args.serve_max_steps)
+        out["open_loop"] = dict(s, rate_per_s=args.serve_rate, episodes=count, budget_rows=srv.capacity,
+                                arrivals_s=args.serve_seconds)
+    del srv
+    torch.cuda.empty_cache()
+    eps = episode_stream(12, 16000, rate=0.0)
+    with Server(rows=262144, device=dev, keep=False, depth=2) as srv:
+        for ep in eps:
+            srv.submit(ep)
+        until = time.perf_counter() + 120.0                                 # fill the budget, untimed
+        warm = 0
+        while time.perf_counter() < until and (warm < args.serve_warmup or srv.live_rows < 0.9 * srv.capacity):
+            if srv.step():
+                warm += 1
+            else:
+                time.sleep(0.0001)
+        srv.reset_stats()
+        s = serve(srv, [], realtime=False, max_steps=args.serve_steps)
+        out["saturated"] = dict(s, budget_rows=srv.capacity, episodes_offered=len(eps), depth=2,
+                                warmup_steps=warm)
+    del srv
+    torch.cuda.empty_cache()
+    return out
+
+
 def _config(args, schedule: str) -> dict:
     return {"workload": (f"flight-mode park, dynamical orientation on, new orbit law: {args.worlds} worlds x "
                          f"{args.ships} ships (follow / orbit / warp), per-rank"),
@@ -169,12 +223,20 @@ def _config(args, schedule: str) -> dict:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--worlds", type=int, default=65536)
     ap.add_argument("--ships", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--serve-seconds", type=float, default=6.0)
+    ap.add_argument("--serve-budget-gb", type=float, default=80.0)
+    ap.add_argument("--serve-max-steps", type=int, default=20000)
+    ap.add_argument("--serve-all", action="store_true")
+    ap.add_argument("--serve-steps", type=int, default=3000)
+    ap.add_argument("--serve-warmup", type=int, default=200)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -309,6 +371,9 @@ def main() -> None:
             "e2e": {"value": total_ships * args.steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
             "gpu_launches": 3 * args.steps, "clocks": clocks}
+    if not args.no_serve:
+        line["serve"] = serve_runs(args, dev)
+        line["serve"]["plain_ship_ticks_per_s"] = line["plain"]["value"] / world_size
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(args.worlds, args.ships, args.warmup, args.steps)
     if dist is not None:

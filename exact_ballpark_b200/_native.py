@@ -47,6 +47,8 @@ def lib() -> ctypes.CDLL:
     L.ebb_flight_tick_noalloc.argtypes = [ctypes.POINTER(FlightState), p, i32]
     L.ebb_flight_tick_tiled.argtypes = [ctypes.POINTER(FlightState), p, i64, i32, p, p, i32, i32]
     L.ebb_flight_tick_worlds.argtypes = [ctypes.POINTER(FlightState), p, p, i64, i32, p, p, p, i32, i32]
+    L.ebb_plan_worlds.restype = i64
+    L.ebb_plan_worlds.argtypes = [p, p, i64, i32, p, p]
     L.ebb_flight_move.argtypes = [ctypes.POINTER(FlightState), ctypes.POINTER(FlightState), p, p, i64, p, p, i32]
     L.ebb_flight_snap.argtypes = [ctypes.POINTER(FlightState), p, i32, p, i32]
     L.ebb_flight_decay.argtypes = [ctypes.POINTER(FlightState), p, ctypes.c_double, p, i32]

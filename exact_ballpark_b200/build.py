@@ -16,7 +16,7 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libebb.so"
-SOURCES = ("ebb_flight.cu",)
+SOURCES = ("ebb_flight.cu", "ebb_plan.cpp")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
               "-prec-div=true", "-prec-sqrt=true", "-ftz=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
               "-Xptxas", "-v", "-shared"]
@@ -37,7 +37,7 @@ def _stale(target: Path, deps) -> bool:
 
 
 def build_native(force: bool = False, verbose: bool = False) -> Path:
-    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "ebb.h"]
+    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "ebb.h"]
     if not force and not _stale(LIB, deps):
         return LIB
     tmp = LIB.with_suffix(".so.tmp")

@@ -372,9 +372,68 @@ __host__ __device__ inline size_t tiled_records_bytes(int cap) {
     return ((size_t)cap * sizeof(SlotRec) + 15) & ~(size_t)15;
 }
 
-// One tile at a time (a run of whole worlds, rows [r0, r1)): the records pass into shared memory, then the tile's
-// ships' ticks, each warp taking 32 ships at a time through the warp's orientation step. With one tile a block (grid
-// = tiles) the block ends with its tile; a persistent grid (grid < tiles) syncs before reusing the records.
+// One tile (a run of whole worlds, rows [r0, r1)): the records pass into shared memory, then the tile's ships' ticks,
+// each warp taking 32 ships at a time through the warp's orientation step. ONE_ROUND: the tile has at most as many
+// rows as the block has threads, so each thread ticks at most one ship.
+template <bool ONE_ROUND>
+__device__ __forceinline__ void tiled_tile(const EbbFlightState& s, int64_t r0, int64_t r1, SlotRec* rec,
+                                           const float* ndt_tab, float* ktab, int32_t* status) {
+    const int m = (int)(r1 - r0);
+    for (int j = threadIdx.x; j < m; j += blockDim.x) {               // the records pass, into shared memory
+        const int64_t i = r0 + j;
+        bool act;
+        double vy_after;
+        records_of(s, i, &act, &vy_after);
+        SlotRec& q = rec[j];
+        const D3 p = ld3(s.pos, i, s.n), v = ld3(s.vel, i, s.n);
+        q.px = p.x;
+        q.py = p.y;
+        q.pz = p.z;
+        q.vx = v.x;
+        q.vy = v.y;
+        q.vz = v.z;
+        q.vy_after = vy_after;
+        q.id = s.ids[i];
+        q.radius = s.radius[i];
+        q.act = act ? 1 : 0;
+    }
+    __syncthreads();
+    for (int base = threadIdx.x & ~31; base < m; base += blockDim.x) {   // warp-uniform: each warp's 32 ships
+        const int j = base + (threadIdx.x & 31);
+        const bool mine = j < m;
+        DoLane d;
+        d.on = false;
+        bool release_after = false;
+        const int64_t i = r0 + j;
+        if (mine) {
+            View tgt;
+            const int64_t t = s.follow_ptr[i];
+            tgt.valid = t >= r0 && t < r1;
+            if (!tgt.valid && t >= 0 && t < s.n) atomicOr(status, 1);    // a target outside its world's tile
+            if (tgt.valid) {
+                const SlotRec& q = rec[t - r0];
+                tgt.pos = D3{q.px, q.py, q.pz};
+                tgt.vel = D3{q.vx, q.vy, q.vz};
+                tgt.vy_after = q.vy_after;
+                tgt.id = q.id;
+                tgt.radius = q.radius;
+                tgt.act = q.act != 0;
+            } else {
+                tgt.act = false;
+                tgt.id = 0;
+            }
+            tick_begin(s, i, tgt, rec[j].act != 0, d, &release_after);
+        }
+        orient_warp(d, cfg_of(s), ndt_tab, ktab);
+        if (mine) tick_end(s, i, d, release_after);
+        if (ONE_ROUND) break;
+    }
+}
+
+// The tiled tick. SINGLE: one tile a block (grid >= tiles), each of at most `block` rows, so a thread ticks one ship
+// and exits: no state lives across tiles or rounds, which halves the register spills of the general form. Otherwise a
+// persistent grid takes the tiles in turn, syncing before it reuses the records.
+template <bool SINGLE>
 __global__ void __launch_bounds__(256, EBB_TILED_MIN_BLOCKS) tiled_kernel(EbbFlightState s, const int64_t* __restrict__ tile_rows,
                                                     int64_t tiles, int cap, int32_t* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -382,58 +441,14 @@ __global__ void __launch_bounds__(256, EBB_TILED_MIN_BLOCKS) tiled_kernel(EbbFli
     SlotRec* rec = (SlotRec*)smem_raw;
     float* ktab = (float*)(smem_raw + tiled_records_bytes(cap)) + (threadIdx.x >> 5) * KTAB_FLOATS;
     fill_ndt(ndt_tab, s.dt);
+    if (SINGLE) {
+        if (blockIdx.x < tiles)
+            tiled_tile<true>(s, tile_rows[blockIdx.x], tile_rows[blockIdx.x + 1], rec, ndt_tab, ktab, status);
+        return;
+    }
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const int64_t r0 = tile_rows[tile], r1 = tile_rows[tile + 1];
-        const int m = (int)(r1 - r0);
-        if (tile != blockIdx.x) __syncthreads();                     // the previous tile's records are done with
-        for (int j = threadIdx.x; j < m; j += blockDim.x) {           // the records pass, into shared memory
-            const int64_t i = r0 + j;
-            bool act;
-            double vy_after;
-            records_of(s, i, &act, &vy_after);
-            SlotRec& q = rec[j];
-            const D3 p = ld3(s.pos, i, s.n), v = ld3(s.vel, i, s.n);
-            q.px = p.x;
-            q.py = p.y;
-            q.pz = p.z;
-            q.vx = v.x;
-            q.vy = v.y;
-            q.vz = v.z;
-            q.vy_after = vy_after;
-            q.id = s.ids[i];
-            q.radius = s.radius[i];
-            q.act = act ? 1 : 0;
-        }
-        __syncthreads();
-        for (int base = threadIdx.x & ~31; base < m; base += blockDim.x) {   // warp-uniform: each warp's 32 ships
-            const int j = base + (threadIdx.x & 31);
-            const bool mine = j < m;
-            DoLane d;
-            d.on = false;
-            bool release_after = false;
-            const int64_t i = r0 + j;
-            if (mine) {
-                View tgt;
-                const int64_t t = s.follow_ptr[i];
-                tgt.valid = t >= r0 && t < r1;
-                if (!tgt.valid && t >= 0 && t < s.n) atomicOr(status, 1);    // a target outside its world's tile
-                if (tgt.valid) {
-                    const SlotRec& q = rec[t - r0];
-                    tgt.pos = D3{q.px, q.py, q.pz};
-                    tgt.vel = D3{q.vx, q.vy, q.vz};
-                    tgt.vy_after = q.vy_after;
-                    tgt.id = q.id;
-                    tgt.radius = q.radius;
-                    tgt.act = q.act != 0;
-                } else {
-                    tgt.act = false;
-                    tgt.id = 0;
-                }
-                tick_begin(s, i, tgt, rec[j].act != 0, d, &release_after);
-            }
-            orient_warp(d, cfg_of(s), ndt_tab, ktab);
-            if (mine) tick_end(s, i, d, release_after);
-        }
+        __syncthreads();                                              // the table, and the previous tile's records
+        tiled_tile<false>(s, tile_rows[tile], tile_rows[tile + 1], rec, ndt_tab, ktab, status);
     }
 }
 
@@ -464,12 +479,130 @@ __host__ __device__ inline size_t listed_smem_bytes(int cap, int block) {
     return listed_tables_bytes(cap) + (size_t)(block / 32) * KTAB_FLOATS * sizeof(float);
 }
 
-// One tick of a list of worlds anywhere in the park: world w is rows [worlds[2w], worlds[2w + 1]), a tile is the
-// worlds [tile_worlds[t], tile_worlds[t + 1]) (at most cap rows), and each tile's rows are gathered into shared-memory
-// slots world after world. Rows in no listed world are not read or written; rows with active[i] == 0 (when `active`
-// is given) are not ticked, though their records are made for the rest of their world (OnTick's per-world mask, in
-// the kernel). status: bit 1 a follow pointer leaving its world (the ship ticks without its target), bit 2 a malformed
-// tile (rows outside the park, more than cap rows or worlds: skipped).
+// One tile of a list of worlds: world w is rows [worlds[2w], worlds[2w + 1]), the tile the worlds [w0, w0 + nw),
+// gathered into shared-memory slots world after world (warp 0 scans their row counts into slot offsets), then the
+// records pass and the ships' ticks as in the tiled tick. Rows with active[i] == 0 (when `active` is given) are not
+// ticked, though their records are made for the rest of their world. A malformed tile is skipped (status bit 2).
+template <bool ONE_ROUND>
+__device__ __forceinline__ void listed_tile(const EbbFlightState& s, const int64_t* __restrict__ worlds, int64_t w0,
+                                            int64_t nw64, int cap, const uint8_t* __restrict__ active,
+                                            int32_t* status, ListRec* rec, int64_t* wrow, int32_t* wslot,
+                                            int* tile_rows, const float* ndt_tab, float* ktab) {
+    const int lane = threadIdx.x & 31;
+    if (nw64 <= 0 || nw64 > cap) {                                    // block-uniform
+        if (nw64 != 0 && threadIdx.x == 0) atomicOr(status, 2);
+        return;
+    }
+    const int nw = (int)nw64;
+    if (threadIdx.x < 32) {                                           // warp 0: the worlds' slot offsets (a scan)
+        int carry = 0;
+        bool bad = false;
+        for (int k0 = 0; k0 < nw; k0 += 32) {
+            const int k = k0 + lane;
+            int64_t b = 0, len = 0;
+            if (k < nw) {
+                b = worlds[2 * (w0 + k)];
+                len = worlds[2 * (w0 + k) + 1] - b;
+                if (b < 0 || len < 0 || len > cap || b + len > s.n) {
+                    bad = true;
+                    len = 0;
+                }
+            }
+            int c = (int)len;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, c, o);
+                if (lane >= o) c += y;
+            }
+            if (k < nw) {
+                wrow[k] = b;
+                wslot[k] = carry + c - (int)len;
+            }
+            carry += __shfl_sync(0xffffffffu, c, 31);
+            if (carry > cap) bad = true;
+        }
+        bad = __any_sync(0xffffffffu, bad);
+        if (lane == 0) {
+            wslot[nw] = carry;
+            *tile_rows = bad ? -1 : carry;
+        }
+    }
+    __syncthreads();
+    const int m = *tile_rows;
+    if (m < 0) {                                                      // block-uniform
+        if (threadIdx.x == 0) atomicOr(status, 2);
+        return;
+    }
+    for (int j = threadIdx.x; j < m; j += blockDim.x) {               // the records pass, into shared memory
+        int lo = 0, hi = nw - 1;                                      // the slot's world: the last k with wslot[k] <= j
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (wslot[mid] <= j) lo = mid;
+            else hi = mid - 1;
+        }
+        const int64_t i = wrow[lo] + (j - wslot[lo]);
+        bool act;
+        double vy_after;
+        records_of(s, i, &act, &vy_after);
+        ListRec& q = rec[j];
+        const D3 p = ld3(s.pos, i, s.n), v = ld3(s.vel, i, s.n);
+        q.px = p.x;
+        q.py = p.y;
+        q.pz = p.z;
+        q.vx = v.x;
+        q.vy = v.y;
+        q.vz = v.z;
+        q.vy_after = vy_after;
+        q.id = s.ids[i];
+        q.radius = s.radius[i];
+        q.act = act ? 1 : 0;
+        q.world = lo;
+    }
+    __syncthreads();
+    for (int base = threadIdx.x & ~31; base < m; base += blockDim.x) {   // warp-uniform: each warp's 32 slots
+        const int j = base + lane;
+        bool mine = j < m;
+        int64_t i = 0;
+        int e = 0;
+        if (mine) {
+            e = rec[j].world;
+            i = wrow[e] + (j - wslot[e]);
+            if (active != nullptr && active[i] == 0) mine = false;
+        }
+        DoLane d;
+        d.on = false;
+        bool release_after = false;
+        if (mine) {
+            View tgt;
+            const int64_t t = s.follow_ptr[i];
+            const int64_t b = wrow[e], len = wslot[e + 1] - wslot[e];
+            tgt.valid = t >= b && t < b + len;
+            if (!tgt.valid && t >= 0 && t < s.n) atomicOr(status, 1);    // a target outside its world
+            if (tgt.valid) {
+                const ListRec& q = rec[wslot[e] + (int)(t - b)];
+                tgt.pos = D3{q.px, q.py, q.pz};
+                tgt.vel = D3{q.vx, q.vy, q.vz};
+                tgt.vy_after = q.vy_after;
+                tgt.id = q.id;
+                tgt.radius = q.radius;
+                tgt.act = q.act != 0;
+            } else {
+                tgt.act = false;
+                tgt.id = 0;
+            }
+            tick_begin(s, i, tgt, rec[j].act != 0, d, &release_after);
+        }
+        orient_warp(d, cfg_of(s), ndt_tab, ktab);
+        if (mine) tick_end(s, i, d, release_after);
+        if (ONE_ROUND) break;
+    }
+}
+
+// One tick of a list of worlds anywhere in the park: a tile is the worlds [tile_worlds[t], tile_worlds[t + 1]) (at
+// most cap rows). Rows in no listed world are not read or written; rows with active[i] == 0 keep their state (OnTick's
+// per-world mask, in the kernel). status: bit 1 a follow pointer leaving its world (the ship ticks without its
+// target), bit 2 a malformed tile (rows outside the park, more than cap rows or worlds: skipped). SINGLE: one tile a
+// block of at most `block` rows (no state across tiles or rounds), else a persistent grid.
+template <bool SINGLE>
 __global__ void __launch_bounds__(256, EBB_TILED_MIN_BLOCKS)
     worlds_kernel(EbbFlightState s, const int64_t* __restrict__ worlds, const int64_t* __restrict__ tile_worlds,
                   int64_t tiles, int cap, const uint8_t* __restrict__ active, int32_t* status) {
@@ -481,115 +614,19 @@ __global__ void __launch_bounds__(256, EBB_TILED_MIN_BLOCKS)
     int32_t* wslot = (int32_t*)(smem_raw + align16((size_t)cap * sizeof(ListRec)) + align16((size_t)cap * 8));
     float* ktab = (float*)(smem_raw + listed_tables_bytes(cap)) + (threadIdx.x >> 5) * KTAB_FLOATS;
     fill_ndt(ndt_tab, s.dt);
-    const int lane = threadIdx.x & 31;
+    if (SINGLE) {
+        if (blockIdx.x < tiles) {
+            const int64_t w0 = tile_worlds[blockIdx.x];
+            listed_tile<true>(s, worlds, w0, tile_worlds[blockIdx.x + 1] - w0, cap, active, status, rec, wrow, wslot,
+                              &tile_rows, ndt_tab, ktab);
+        }
+        return;
+    }
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        if (tile != blockIdx.x) __syncthreads();                     // the previous tile's tables are done with
-        const int64_t w0 = tile_worlds[tile], nw64 = tile_worlds[tile + 1] - w0;
-        if (nw64 <= 0 || nw64 > cap) {                                // block-uniform
-            if (nw64 != 0 && threadIdx.x == 0) atomicOr(status, 2);
-            continue;
-        }
-        const int nw = (int)nw64;
-        if (threadIdx.x < 32) {                                       // warp 0: the worlds' slot offsets (a scan)
-            int carry = 0;
-            bool bad = false;
-            for (int k0 = 0; k0 < nw; k0 += 32) {
-                const int k = k0 + lane;
-                int64_t b = 0, len = 0;
-                if (k < nw) {
-                    b = worlds[2 * (w0 + k)];
-                    len = worlds[2 * (w0 + k) + 1] - b;
-                    if (b < 0 || len < 0 || len > cap || b + len > s.n) {
-                        bad = true;
-                        len = 0;
-                    }
-                }
-                int c = (int)len;
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, c, o);
-                    if (lane >= o) c += y;
-                }
-                if (k < nw) {
-                    wrow[k] = b;
-                    wslot[k] = carry + c - (int)len;
-                }
-                carry += __shfl_sync(0xffffffffu, c, 31);
-                if (carry > cap) bad = true;
-            }
-            bad = __any_sync(0xffffffffu, bad);
-            if (lane == 0) {
-                wslot[nw] = carry;
-                tile_rows = bad ? -1 : carry;
-            }
-        }
-        __syncthreads();
-        const int m = tile_rows;
-        if (m < 0) {                                                  // block-uniform
-            if (threadIdx.x == 0) atomicOr(status, 2);
-            continue;
-        }
-        for (int j = threadIdx.x; j < m; j += blockDim.x) {           // the records pass, into shared memory
-            int lo = 0, hi = nw - 1;                                  // the slot's world: the last k with wslot[k] <= j
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (wslot[mid] <= j) lo = mid;
-                else hi = mid - 1;
-            }
-            const int64_t i = wrow[lo] + (j - wslot[lo]);
-            bool act;
-            double vy_after;
-            records_of(s, i, &act, &vy_after);
-            ListRec& q = rec[j];
-            const D3 p = ld3(s.pos, i, s.n), v = ld3(s.vel, i, s.n);
-            q.px = p.x;
-            q.py = p.y;
-            q.pz = p.z;
-            q.vx = v.x;
-            q.vy = v.y;
-            q.vz = v.z;
-            q.vy_after = vy_after;
-            q.id = s.ids[i];
-            q.radius = s.radius[i];
-            q.act = act ? 1 : 0;
-            q.world = lo;
-        }
-        __syncthreads();
-        for (int base = threadIdx.x & ~31; base < m; base += blockDim.x) {   // warp-uniform: each warp's 32 slots
-            const int j = base + lane;
-            bool mine = j < m;
-            int64_t i = 0;
-            int e = 0;
-            if (mine) {
-                e = rec[j].world;
-                i = wrow[e] + (j - wslot[e]);
-                if (active != nullptr && active[i] == 0) mine = false;
-            }
-            DoLane d;
-            d.on = false;
-            bool release_after = false;
-            if (mine) {
-                View tgt;
-                const int64_t t = s.follow_ptr[i];
-                const int64_t b = wrow[e], len = wslot[e + 1] - wslot[e];
-                tgt.valid = t >= b && t < b + len;
-                if (!tgt.valid && t >= 0 && t < s.n) atomicOr(status, 1);    // a target outside its world
-                if (tgt.valid) {
-                    const ListRec& q = rec[wslot[e] + (int)(t - b)];
-                    tgt.pos = D3{q.px, q.py, q.pz};
-                    tgt.vel = D3{q.vx, q.vy, q.vz};
-                    tgt.vy_after = q.vy_after;
-                    tgt.id = q.id;
-                    tgt.radius = q.radius;
-                    tgt.act = q.act != 0;
-                } else {
-                    tgt.act = false;
-                    tgt.id = 0;
-                }
-                tick_begin(s, i, tgt, rec[j].act != 0, d, &release_after);
-            }
-            orient_warp(d, cfg_of(s), ndt_tab, ktab);
-            if (mine) tick_end(s, i, d, release_after);
-        }
+        __syncthreads();                                              // the previous tile's tables are done with
+        const int64_t w0 = tile_worlds[tile];
+        listed_tile<false>(s, worlds, w0, tile_worlds[tile + 1] - w0, cap, active, status, rec, wrow, wslot,
+                           &tile_rows, ndt_tab, ktab);
     }
 }
 
@@ -792,13 +829,13 @@ int ebb_flight_tick_tiled(const EbbFlightState* s, const int64_t* tile_rows, int
         grid <= 0)
         return EBB_EINVAL;
     const size_t smem = ebb::flight::tiled_smem_bytes(tile_cap, block);
+    auto kernel = (tile_cap <= block && grid >= tiles) ? ebb::flight::tiled_kernel<true>
+                                                         : ebb::flight::tiled_kernel<false>;
     if (smem > 48 * 1024) {
-        const cudaError_t e = cudaFuncSetAttribute(ebb::flight::tiled_kernel,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
     }
-    ebb::flight::tiled_kernel<<<(unsigned)grid, block, smem, (cudaStream_t)stream>>>(*s, tile_rows, tiles, tile_cap,
-                                                                                     status);
+    kernel<<<(unsigned)grid, block, smem, (cudaStream_t)stream>>>(*s, tile_rows, tiles, tile_cap, status);
     return launched();
 }
 
@@ -810,13 +847,14 @@ int ebb_flight_tick_worlds(const EbbFlightState* s, const int64_t* worlds, const
         tile_worlds == nullptr || status == nullptr || grid <= 0)
         return EBB_EINVAL;
     const size_t smem = ebb::flight::listed_smem_bytes(tile_cap, block);
+    auto kernel = (tile_cap <= block && grid >= tiles) ? ebb::flight::worlds_kernel<true>
+                                                         : ebb::flight::worlds_kernel<false>;
     if (smem > 48 * 1024) {
-        const cudaError_t e = cudaFuncSetAttribute(ebb::flight::worlds_kernel,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
     }
-    ebb::flight::worlds_kernel<<<(unsigned)grid, block, smem, (cudaStream_t)stream>>>(*s, worlds, tile_worlds, tiles,
-                                                                                      tile_cap, active, status);
+    kernel<<<(unsigned)grid, block, smem, (cudaStream_t)stream>>>(*s, worlds, tile_worlds, tiles, tile_cap, active,
+                                                                  status);
     return launched();
 }
 
@@ -861,8 +899,10 @@ int ebb_kernel_info(int which, int* regs, int* local_bytes, int* binary_version,
     switch (which) {
         case 0: e = cudaFuncGetAttributes(&fa, ebb::flight::tick_kernel); break;
         case 1: e = cudaFuncGetAttributes(&fa, ebb::flight::records_kernel); break;
-        case 2: e = cudaFuncGetAttributes(&fa, ebb::flight::tiled_kernel); break;
-        case 3: e = cudaFuncGetAttributes(&fa, ebb::flight::worlds_kernel); break;
+        case 2: e = cudaFuncGetAttributes(&fa, ebb::flight::tiled_kernel<true>); break;
+        case 3: e = cudaFuncGetAttributes(&fa, ebb::flight::worlds_kernel<true>); break;
+        case 5: e = cudaFuncGetAttributes(&fa, ebb::flight::tiled_kernel<false>); break;
+        case 6: e = cudaFuncGetAttributes(&fa, ebb::flight::worlds_kernel<false>); break;
         case 4: e = cudaFuncGetAttributes(&fa, ebb::flight::move_kernel); break;
         default: return EBB_EINVAL;
     }

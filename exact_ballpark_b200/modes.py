@@ -27,6 +27,7 @@ from __future__ import annotations
 
 import ctypes
 
+import numpy as np
 import torch
 
 from . import _native
@@ -55,6 +56,30 @@ _STORAGE = (
     ("interactive", BOOL, 0), ("sensor", BOOL, 0))
 _HOST_ONLY = (("world", I64), ("cloaked", I64), ("bubble", I64), ("refiled", I64))
 _STATE_FIELD = {"goto": "goto_pt", "free": "free_"}
+
+
+# load()'s row keys: (key, numpy dtype, default (None: required)); pos and vel are 3-vectors
+ROW_COLUMNS = (("id", np.int64, None), ("world", np.int64, 0), ("time", np.int64, 0), ("mass", np.float64, None),
+               ("radius", np.float64, None), ("max_vel", np.float64, None), ("agility", np.float64, None),
+               ("speed_fraction", np.float64, None), ("free", np.bool_, True), ("massive", np.bool_, False),
+               ("interactive", np.bool_, False), ("moribund", np.bool_, False), ("cloaked", np.int64, 0),
+               ("bubble", np.int64, -1), ("mode", np.int64, STOP), ("max_ang_vel", np.float64, 1.0),
+               ("rot_agility", np.float64, 0.9))
+
+
+def rows_to_columns(rows: list) -> dict:
+    """load()'s rows as columns (numpy arrays), the reference's defaults filled in: what load_columns takes."""
+    conv = {np.int64: int, np.float64: float, np.bool_: bool}
+    cols = {}
+    for key, dt, default in ROW_COLUMNS:
+        c = conv[dt]
+        if default is None:
+            cols[key] = np.array([c(r[key]) for r in rows], dtype=dt)
+        else:
+            cols[key] = np.array([c(r.get(key, default)) for r in rows], dtype=dt)
+    for key in ("pos", "vel"):
+        cols[key] = np.array([[float(v) for v in r[key]] for r in rows], dtype=np.float64).reshape(len(rows), 3)
+    return cols
 
 
 def f32(x: torch.Tensor) -> torch.Tensor:
@@ -192,27 +217,32 @@ class VecModesPark:
         Ball::Ball's defaults; with dynamical orientation the turning values and the rotation snapped to the
         velocity. Keys as the reference's: id, world, time, mass, radius, max_vel, pos, vel, agility,
         speed_fraction, free, massive, interactive, cloaked, bubble, moribund, mode, max_ang_vel, rot_agility."""
-        n = len(rows)
+        if len(rows) != self.n:
+            raise ValueError(f"{len(rows)} rows for a park of {self.n}")
+        self.load_columns(rows_to_columns(rows))
+
+    def load_columns(self, cols: dict) -> None:
+        """`load` with the rows given as columns (numpy arrays, rows_to_columns' keys and dtypes): the same balls."""
+        n = len(cols["id"])
         if n != self.n:
             raise ValueError(f"{n} rows for a park of {self.n}")
-        for r in rows:
-            if r.get("mode", STOP) not in LOADABLE:
-                raise ValueError(f"a ball starts in STOP or an inert mode, not {r.get('mode')}")
-        cpu = lambda xs, dt=F64: torch.tensor(xs, dtype=dt)
-        col = lambda key, d=None: cpu([float(r[key] if d is None else r.get(key, d)) for r in rows])
-        mass = col("mass")
-        mass = torch.where(mass < 0.0, 0.0, mass)
-        radius = f32(col("radius"))
-        radius = torch.where(radius < 0.0, 0.0, radius)
-        max_vel = f32(col("max_vel"))
-        max_vel = torch.where(max_vel < 0.0, 0.0, max_vel)
-        agility = f32(col("agility"))
-        agility = torch.where(agility <= 0.0, 1.0, agility)
-        sf = f32(col("speed_fraction"))
-        sf = torch.where(sf < 0.0, 0.0, sf)
-        pos = cpu([[float(c) for c in r["pos"]] for r in rows]).reshape(n, 3)
-        vel = cpu([[float(c) for c in r["vel"]] for r in rows]).reshape(n, 3)
+        mode = np.asarray(cols["mode"])
+        if not np.isin(mode, LOADABLE).all():
+            raise ValueError(f"a ball starts in STOP or an inert mode, not {int(mode[~np.isin(mode, LOADABLE)][0])}")
         dev = self.dev
+        cpu = lambda key, dt=F64: torch.from_numpy(np.ascontiguousarray(cols[key])).to(dt)
+        mass = cpu("mass")
+        mass = torch.where(mass < 0.0, 0.0, mass)
+        radius = f32(cpu("radius"))
+        radius = torch.where(radius < 0.0, 0.0, radius)
+        max_vel = f32(cpu("max_vel"))
+        max_vel = torch.where(max_vel < 0.0, 0.0, max_vel)
+        agility = f32(cpu("agility"))
+        agility = torch.where(agility <= 0.0, 1.0, agility)
+        sf = f32(cpu("speed_fraction"))
+        sf = torch.where(sf < 0.0, 0.0, sf)
+        pos = cpu("pos").reshape(n, 3)
+        vel = cpu("vel").reshape(n, 3)
         self._mass.copy_(mass)
         self._radius.copy_(radius)
         self._max_vel.copy_(max_vel)
@@ -230,24 +260,23 @@ class VecModesPark:
         for t in (self._ang_vel, self._old_ang_vel, self._torque, self._rot_roll):
             t.zero_()
         if self.dynamical_orientation:
-            mav = f32(col("max_ang_vel", 1.0))
-            rag = f32(col("rot_agility", 0.9))
+            mav = f32(cpu("max_ang_vel"))
+            rag = f32(cpu("rot_agility"))
             self._max_ang_vel.copy_(torch.where(mav < 0.0, 0.0, mav))
             self._rot_agility.copy_(torch.where(rag <= 0.0, 1.0, rag))
         else:
             self._max_ang_vel.fill_(1.0)
             self._rot_agility.fill_(0.9)
-        self._ids.copy_(cpu([int(r["id"]) for r in rows], I64))
-        self.world.copy_(cpu([int(r.get("world", 0)) for r in rows], I64))
-        self._clock.copy_(cpu([int(r.get("time", 0)) for r in rows], I64))
-        self._mode.copy_(cpu([int(r.get("mode", STOP)) for r in rows], I32))
-        b = lambda key, d: cpu([bool(r.get(key, d)) for r in rows], BOOL)
-        self._free.copy_(b("free", True))
-        self._massive.copy_(b("massive", False))
-        self._interactive.copy_(b("interactive", False))
-        self._moribund.copy_(b("moribund", False))
-        self.cloaked.copy_(cpu([int(r.get("cloaked", 0)) for r in rows], I64))
-        self.bubble.copy_(cpu([int(r.get("bubble", -1)) for r in rows], I64))
+        self._ids.copy_(cpu("id", I64))
+        self.world.copy_(cpu("world", I64))
+        self._clock.copy_(cpu("time", I64))
+        self._mode.copy_(cpu("mode", I32))
+        self._free.copy_(cpu("free", BOOL))
+        self._massive.copy_(cpu("massive", BOOL))
+        self._interactive.copy_(cpu("interactive", BOOL))
+        self._moribund.copy_(cpu("moribund", BOOL))
+        self.cloaked.copy_(cpu("cloaked", I64))
+        self.bubble.copy_(cpu("bubble", I64))
         self._sensor.zero_()
         self._effect_stamp.zero_()
         self._follow_id.zero_()

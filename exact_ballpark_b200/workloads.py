@@ -19,6 +19,7 @@ import math
 import random
 from dataclasses import dataclass
 
+import numpy as np
 import torch
 
 FOLLOW, ORBIT, WARP = 1, 4, 3          # Destiny's DSTBALL_FOLLOW, DSTBALL_ORBIT, DSTBALL_WARP
@@ -39,15 +40,20 @@ class FlightWorlds:
 
     def apply(self, park) -> None:
         """The initial commands, through the park's API: FollowBall, Orbit and WarpTo on their rows."""
-        dev = park.dev
-        b = lambda xs: torch.tensor(xs, dtype=torch.bool, device=dev)
-        target = torch.tensor(self.target, dtype=torch.int64, device=dev)
-        rng = torch.tensor(self.range_, dtype=torch.float64, device=dev)
-        point = torch.tensor(self.point, dtype=torch.float64, device=dev)
-        wf = torch.tensor(self.warp_factor, dtype=torch.int64, device=dev)
-        park.follow(b(self.follow_mask), target, rng)
-        park.orbit(b(self.orbit_mask), target, rng)
-        park.warp_to(b(self.warp_mask), point, torch.full_like(rng, 20000.0), wf)
+        self.packed().apply(park)
+
+    def packed(self) -> "PackedWorlds":
+        """The same worlds as numpy columns (made once): what a park's load_columns and the commands take."""
+        if getattr(self, "_packed", None) is None:
+            from .modes import rows_to_columns
+            n = len(self.rows)
+            self._packed = PackedWorlds(
+                rows_to_columns(self.rows), np.array(self.follow_mask, dtype=bool).reshape(n),
+                np.array(self.orbit_mask, dtype=bool).reshape(n), np.array(self.warp_mask, dtype=bool).reshape(n),
+                np.array(self.target, dtype=np.int64).reshape(n), np.array(self.range_, dtype=np.float64).reshape(n),
+                np.array(self.point, dtype=np.float64).reshape(n, 3),
+                np.array(self.warp_factor, dtype=np.int64).reshape(n), self.worlds)
+        return self._packed
 
     @property
     def sizes(self) -> list:
@@ -83,6 +89,54 @@ class FlightWorlds:
             wf += part.warp_factor
         ships = max((p.ships for p in parts), default=0)
         return FlightWorlds(rows, fm, om, wm, tgt, rg, pt, wf, world, ships)
+
+
+@dataclass
+class PackedWorlds:
+    """Worlds as columns: the load columns (exact_ballpark_b200.modes.rows_to_columns) and the initial commands as
+    arrays, one entry a row. `concat` joins several (worlds renumbered, targets moved with their rows) with numpy
+    alone, and `load` + `apply` give a park the same state as FlightWorlds.rows and FlightWorlds.apply."""
+    cols: dict
+    follow_mask: np.ndarray
+    orbit_mask: np.ndarray
+    warp_mask: np.ndarray
+    target: np.ndarray
+    range_: np.ndarray
+    point: np.ndarray
+    warp_factor: np.ndarray
+    worlds: int
+
+    @property
+    def n(self) -> int:
+        return len(self.target)
+
+    def load(self, park) -> None:
+        park.load_columns(self.cols)
+
+    def apply(self, park) -> None:
+        dev = park.dev
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        rng = t(self.range_)
+        park.follow(t(self.follow_mask), t(self.target), rng)
+        park.orbit(t(self.orbit_mask), t(self.target), rng)
+        park.warp_to(t(self.warp_mask), t(self.point), torch.full_like(rng, 20000.0), t(self.warp_factor))
+
+    @staticmethod
+    def concat(parts: list) -> "PackedWorlds":
+        sizes = [p.n for p in parts]
+        base = np.concatenate(([0], np.cumsum(sizes)[:-1])).astype(np.int64)
+        wbase = np.concatenate(([0], np.cumsum([p.worlds for p in parts])[:-1])).astype(np.int64)
+        cols = {}
+        for key in parts[0].cols:
+            if key == "world":
+                cols[key] = np.concatenate([p.cols[key] - (p.cols[key][0] if p.n else 0) + wb
+                                            for p, wb in zip(parts, wbase)])
+            else:
+                cols[key] = np.concatenate([p.cols[key] for p in parts])
+        target = np.concatenate([np.where(p.target >= 0, p.target + b, -1) for p, b in zip(parts, base)])
+        cat = lambda k: np.concatenate([getattr(p, k) for p in parts])
+        return PackedWorlds(cols, cat("follow_mask"), cat("orbit_mask"), cat("warp_mask"), target, cat("range_"),
+                            cat("point"), cat("warp_factor"), int(sum(p.worlds for p in parts)))
 
 
 def _unit(r: random.Random) -> list:

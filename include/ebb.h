@@ -99,6 +99,14 @@ int ebb_flight_tick_tiled(const EbbFlightState* s, const int64_t* tile_rows, int
 int ebb_flight_tick_worlds(const EbbFlightState* s, const int64_t* worlds, const int64_t* tile_worlds, int64_t tiles,
                            int tile_cap, const uint8_t* active, int32_t* status, void* stream, int block, int grid);
 
+/* Host-side planning for ebb_flight_tick_worlds: packs `count` worlds (rows [starts[k], starts[k] + lens[k]), each of
+ * at most tile_cap rows; empty ones left out) into tiles of at most tile_cap rows, best-fit decreasing (the tiles
+ * need not be runs of adjacent worlds), each tile's worlds in row order. Writes worlds[2 x listed] and
+ * tile_worlds[tiles + 1] (caller arrays of 2 x count and count + 1 entries) and returns the number of tiles, or
+ * EBB_EINVAL. No device work. No counterpart in the reference. */
+int64_t ebb_plan_worlds(const int64_t* starts, const int64_t* lens, int64_t count, int tile_cap, int64_t* worlds,
+                        int64_t* tile_worlds);
+
 /* Rows copied between two parks, every field: src row src_rows[k] into dst row dst_rows[k], k < m (device arrays).
  * A follow pointer moves with its row, so a world moved as one run keeps its targets; a pointer that would leave dst
  * becomes -1, and rows outside either park are skipped (status[0] bit 4 for both). Admission and retirement of a

@@ -47,17 +47,26 @@ def _same_states(a: dict, b: dict, where: str) -> None:
             raise AssertionError(f"{where}: {f} differs in {len(rows)} rows, first {rows[:5]}")
 
 
-def test_the_listed_worlds_tick_equals_the_tiled_tick():
-    from exact_ballpark_b200 import tick_tiled, tick_worlds
+@pytest.mark.parametrize("cap,block,grid", [(256, 256, None), (128, 256, None), (512, 128, None), (256, 128, 7),
+                                            (128, 128, 5)])
+def test_the_listed_worlds_tick_equals_the_tiled_and_plain_ticks(cap, block, grid):
+    """Both forms of each tiled kernel: one tile a block of at most `block` rows, and the persistent grid with
+    several rounds of ships a tile."""
+    from exact_ballpark_b200 import tick_plain, tick_tiled, tick_worlds
+    from exact_ballpark_b200.tiles import plan_tiles
     w = _ragged(3, 600, 64)
-    a, b = _loaded(w), _loaded(w)
-    assert a.plan is not None
+    a, b, c = _loaded(w), _loaded(w), _loaded(w)
+    plan = plan_tiles(a.world, cap=cap, block=block, grid=grid)
+    assert plan is not None
     for _ in range(30):
-        tick_tiled(a)
-        tick_worlds(b)
+        tick_tiled(a, plan)
+        tick_worlds(b, None, plan)
+        tick_plain(c)
     torch.cuda.synchronize()
-    _same_states(_state(a), _state(b), "after 30 ticks")
-    assert int(b._status.item()) == 0
+    sc = _state(c)
+    _same_states(_state(a), sc, "tiled after 30 ticks")
+    _same_states(_state(b), sc, "listed worlds after 30 ticks")
+    assert int(a._status.item()) == 0 and int(b._status.item()) == 0
 
 
 @pytest.mark.parametrize("per_world", [True, False])
@@ -123,7 +132,10 @@ def test_moving_rows_keeps_every_field_and_moves_targets():
 def _served(episodes, rows: int, **kw):
     from exact_ballpark_b200.serving import Server, serve
     srv = Server(rows=rows, max_ships=max(e.ships for e in episodes), **kw)
-    summary = serve(srv, episodes, realtime=False)
+    try:
+        summary = serve(srv, episodes, realtime=False)
+    finally:
+        srv.close()
     return srv, summary
 
 
@@ -145,7 +157,7 @@ def test_each_served_episode_equals_the_episode_alone():
     holes that later ones fill, and every tick runs a different mix."""
     from exact_ballpark_b200.serving import episode_stream
     eps = episode_stream(17, 30, rate=0.0, max_ships=48, min_ticks=2, max_ticks=60)
-    srv, summary = _served(eps, rows=200, tile_cap=128)
+    srv, summary = _served(eps, rows=200, tile_cap=128, stage_rows=64)
     assert summary["admitted"] == summary["retired"] == len(eps)
     assert summary["steps"] > max(e.ticks for e in eps)
     assert len(srv.results) == len(eps)
@@ -181,7 +193,10 @@ def test_open_loop_arrivals_are_served_and_timed():
     from exact_ballpark_b200.serving import Server, serve
     eps = episode_stream(29, 60, rate=5000.0, max_ships=64, min_ticks=5, max_ticks=50)
     srv = Server(rows=4096, max_ships=64, tile_cap=256)
-    summary = serve(srv, eps, realtime=True)
+    try:
+        summary = serve(srv, eps, realtime=True)
+    finally:
+        srv.close()
     assert summary["admitted"] == summary["retired"] == 60
     assert summary["p99_ms"] >= summary["p50_ms"] > 0
     for ep in eps[:10]:

@@ -82,10 +82,13 @@ def test_the_tile_plan_lists_every_world_once_within_the_tile_size():
             assert (np.diff(tile_worlds) > 0).all() or e == 0
             pairs = worlds.reshape(-1, 2)
             assert sorted(map(tuple, pairs.tolist())) == sorted(zip(starts.tolist(), (starts + lens).tolist()))
-            assert (np.diff(pairs[:, 0]) > 0).all() if e > 1 else True       # row order
+            total = int(lens.sum())
             for a, b in zip(tile_worlds[:-1], tile_worlds[1:]):
                 rows = int((pairs[a:b, 1] - pairs[a:b, 0]).sum())
                 assert rows <= cap and b - a <= cap
+                assert (np.diff(pairs[a:b, 0]) > 0).all()                    # each tile's worlds in row order
+            tiles = len(tile_worlds) - 1
+            assert tiles <= max(1, 2 * -(-total // cap))                      # best fit: at most twice the least
 
 
 def test_a_world_bigger_than_a_tile_is_refused():
