@@ -186,3 +186,72 @@ def flight_worlds(seed: int, worlds: int, ships: int = 4) -> FlightWorlds:
 def ragged_ships(r: random.Random, max_ships: int) -> int:
     """A world's ship count, log-uniform in [1, max_ships] (floor of 10^U(0, log10 max_ships))."""
     return max(1, min(max_ships, int(10.0 ** r.uniform(0.0, math.log10(max_ships)))))
+
+
+# ============================================================================ collisions with static spheres
+
+@dataclass
+class CollideWorlds:
+    """Worlds for the collision park (exact_ballpark_b200.collide.VecCollidePark): `worlds` (each a list of the
+    load's ball dicts) and the ships' GOTO aims, {step: [(world, ball id, point)]} (step 1 is before the first tick)."""
+    worlds: list
+    aims: dict
+    ships: int
+    spheres: int
+    statics: int
+
+    def apply(self, park, step: int) -> None:
+        """The aims of `step` through the park's API: one GotoPoint call with every aimed ship's point."""
+        todo = self.aims.get(step)
+        if not todo:
+            return
+        mask = torch.zeros(park.W, park.N, dtype=torch.bool)
+        point = torch.zeros(park.W, park.N, 3, dtype=torch.float64)
+        ids = park.id.detach().cpu()
+        for w, bid, p in todo:
+            j = int((ids[w] == bid).nonzero()[0, 0])
+            mask[w, j] = True
+            point[w, j] = torch.tensor(p, dtype=torch.float64)
+        park.goto_point(mask.to(park.dev), point.to(park.dev))
+
+
+def collide_worlds(seed: int, worlds: int, ships: int = 4, spheres: int = 4, statics: int = 8, ticks: int = 500,
+                   reaim: int = 25) -> CollideWorlds:
+    """W worlds of `ships` ships, `spheres` free massive spheres and `statics` fixed spheres, everything in a +-20 km
+    cube, each world from random.Random(seed * 1_000_003 + w). Ships as the flight-mode benchmark draws them (mass
+    log-uniform 1e6-1e9 kg, radius 20-500 m, max velocity log-uniform 100-3000 m/s, agility 0.1-5); spheres of radius
+    log-uniform 10 m-5 km, mass log-uniform 1e6-1e10 kg (the free ones; a fixed sphere is immovable whatever its
+    mass); free balls start with a velocity of uniform direction and a speed uniform up to their maximum. Every ship
+    flies GOTO at a sphere's centre, re-aimed at another random sphere every `reaim` ticks (the aims are harness
+    choices), so that overlaps and gradient pushes occur every tick."""
+    out, aims = [], {}
+    lg = math.log10
+    for w in range(worlds):
+        r = random.Random(seed * 1_000_003 + w)
+        balls = []
+        bid = 0
+        for kind, count in (("ship", ships), ("sphere", spheres), ("static", statics)):
+            for _ in range(count):
+                bid += 1
+                free = kind != "static"
+                if kind == "ship":
+                    mass, radius = 10.0 ** r.uniform(6.0, 9.0), r.uniform(20.0, 500.0)
+                    max_vel, agility = 10.0 ** r.uniform(2.0, lg(3000.0)), r.uniform(0.1, 5.0)
+                else:
+                    mass, radius = 10.0 ** r.uniform(6.0, 10.0), 10.0 ** r.uniform(1.0, lg(5000.0))
+                    max_vel, agility = 10.0 ** r.uniform(2.0, lg(3000.0)), 1.0
+                pos = [r.uniform(-2e4, 2e4) for _ in range(3)]
+                vel = [0.0, 0.0, 0.0]
+                if free:
+                    u = _unit(r)
+                    sp = r.uniform(0.0, max_vel)
+                    vel = [c * sp for c in u]
+                balls.append({"id": bid, "mass": mass, "radius": radius, "max_vel": max_vel, "agility": agility,
+                              "speed_fraction": 1.0, "pos": pos, "vel": vel, "free": free, "massive": True})
+        out.append(balls)
+        targets = [b for b in balls if b["id"] > ships]
+        for step in range(1, ticks + 1, reaim):
+            for s in range(ships):
+                t = r.choice(targets)
+                aims.setdefault(step, []).append((w, s + 1, list(t["pos"])))
+    return CollideWorlds(out, aims, ships, spheres, statics)

@@ -1,7 +1,7 @@
 """Generates the golden fixtures under tests/golden/ from the reference itself (run where the reference is checked
 out; nothing on a GPU box runs this):
 
-    EXACT_BALLPARK_REF=<checkout of exact-ballpark> python tests/golden/make_golden.py [--only libm|traces]
+    EXACT_BALLPARK_REF=<checkout of exact-ballpark> python tests/golden/make_golden.py [--only libm|traces|collide]
 
 1. libm.npz: inputs and outputs of glibc 2.34 aarch64's functions as the reference transcribes them (dlibm.sin,
    cos, sincos, log; vec_exp.exp; vec_libm.expf, logf, sinf, cosf, acosf, atanf, atan2f, pow), on seeded random
@@ -216,9 +216,52 @@ def make_workload_traces() -> None:
         print(f"  trace_{name}: n={park.n} 200 ticks, {time.time() - t:.0f} s")
 
 
+def make_collide_traces(sample: int) -> None:
+    """The collision park's traces: the reference's collide_cases scenarios (seed 1 development, 2 held out; the
+    gradient method, a client's view) driven by its own collide_cases.batched, and the collision benchmark's worlds
+    (workloads.collide_worlds: 64 worlds of 4 ships, 4 free spheres and 8 fixed spheres, 100 ticks). Before
+    recording, each seed's scenarios are checked against the scalar SpaceBallpark (collide_cases.reference_rows)
+    with the reference's own comparison (collide_cases.differences)."""
+    import collide_cases as cc
+    import collide_trace as ct
+    from exact_ballpark.vec_collide import VecCollidePark
+    from exact_ballpark_b200.workloads import collide_worlds
+
+    Rec = ct.recording(VecCollidePark)
+    for seed in (1, 2):
+        t = time.time()
+        cs = cc.cases(seed)
+        if sample:
+            sub = cs[:max(1, sample) * 20]
+            want, undefined = cc.reference_rows(sub)
+            got = cc.batched(sub, "cpu")
+            bad = cc.differences(want, {k: v for k, v in got.items() if k[0] not in undefined})
+            if bad:
+                raise RuntimeError(f"the batched CPU collision park differs from the scalar reference: {bad[:10]}")
+            print(f"  scalar check (collide seed {seed}, {len(sub)} scenarios): 0 differences")
+        parks = []
+
+        def make(*a, **k):
+            parks.append(Rec(*a, **k))
+            return parks[-1]
+        cc.batched(cs, "cpu", park_cls=make)
+        ct.save([p.trace for p in parks], HERE / f"collide_cc{seed}")
+        ticks = sum(len(p.trace["field_digests"]) for p in parks)
+        print(f"  collide_cc{seed}: {len(cs)} scenarios in {len(parks)} parks, {ticks} ticks, {time.time() - t:.0f} s")
+    t = time.time()
+    w = collide_worlds(1, 64, ticks=100)
+    park = Rec(64, 16, friction=1.0e6, tick_interval_ms=1000, device="cpu")
+    park.load(w.worlds)
+    for step in range(1, 101):
+        w.apply(park, step)
+        park.evolve()
+    ct.save([park.trace], HERE / "collide_w0")
+    print(f"  collide_w0: 64 worlds x 16 balls, 100 ticks, {time.time() - t:.0f} s")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=("libm", "traces", "workload"), default=None)
+    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide"), default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
     a = ap.parse_args()
     if a.only in (None, "libm"):
@@ -227,6 +270,8 @@ def main() -> None:
         make_workload_traces()
     if a.only in (None, "traces"):
         make_traces(a.sample)
+    if a.only in (None, "collide"):
+        make_collide_traces(a.sample)
 
 
 if __name__ == "__main__":
