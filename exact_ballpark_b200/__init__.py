@@ -1,9 +1,13 @@
-"""exact-ballpark-b200: the batched destiny tick (exact-ballpark's flight-mode park) on NVIDIA B200, bit-exact.
+"""exact-ballpark-b200: exact-ballpark's batched destiny tick on NVIDIA B200, bit-exact.
 
-The drop-in API is exact_ballpark.vec_modes / vec_modes_cuda's: `VecModesPark`, `tick`, `ModesGraph`,
-`kernel_info`. The tick runs in the native library libebb.so (csrc/, C ABI in include/ebb.h).
+The drop-in APIs are the reference's: exact_ballpark.vec_modes / vec_modes_cuda's flight-mode park (`VecModesPark`,
+`tick`, `ModesGraph`, `kernel_info`) and exact_ballpark.vec_collide's collision park (`VecCollidePark`, gradient method
+on spheres; `CollideGraph`). The ticks run in the native library libebb.so (csrc/, C ABI in include/ebb.h).
 """
 
-from .modes import (VecModesPark, ModesGraph, kernel_info, libm, tick, tick_plain, tick_tiled, tick_worlds)  # noqa: F401
+from .collide import CollideGraph, VecCollidePark  # noqa: F401
+from .modes import (ModesGraph, VecModesPark, kernel_info, libm, tick, tick_plain, tick_tiled,  # noqa: F401
+                    tick_worlds)
 
-__all__ = ["VecModesPark", "ModesGraph", "kernel_info", "libm", "tick", "tick_plain", "tick_tiled", "tick_worlds"]
+__all__ = ["VecModesPark", "ModesGraph", "kernel_info", "libm", "tick", "tick_plain", "tick_tiled", "tick_worlds",
+           "VecCollidePark", "CollideGraph"]

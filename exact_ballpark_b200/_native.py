@@ -10,6 +10,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libebb.so"
 ABI = 1
+COLLIDE_MAX_SLOTS = 64          # include/ebb.h: EBB_COLLIDE_MAX_SLOTS
 
 _lib = None
 
@@ -50,6 +51,8 @@ def lib() -> ctypes.CDLL:
     L.ebb_plan_worlds.restype = i64
     L.ebb_plan_worlds.argtypes = [p, p, i64, i32, p, p]
     L.ebb_flight_move.argtypes = [ctypes.POINTER(FlightState), ctypes.POINTER(FlightState), p, p, i64, p, p, i32]
+    L.ebb_collide_tick.argtypes = [p, p, p, p]
+    L.ebb_collide_load.argtypes = [p, p, p]
     L.ebb_flight_snap.argtypes = [ctypes.POINTER(FlightState), p, i32, p, i32]
     L.ebb_flight_decay.argtypes = [ctypes.POINTER(FlightState), p, ctypes.c_double, p, i32]
     L.ebb_libm.argtypes = [i32, i64, p, p, p, p, i32]

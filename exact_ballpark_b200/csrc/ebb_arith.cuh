@@ -17,7 +17,7 @@
 
 #ifdef __CUDACC__
 #define EBB_HD __host__ __device__ __forceinline__
-#define EBB_HDNI __host__ __device__ __noinline__
+#define EBB_HDNI inline __host__ __device__ __noinline__
 #else
 #define EBB_HD inline
 #define EBB_HDNI inline

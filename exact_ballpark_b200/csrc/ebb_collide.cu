@@ -1,0 +1,467 @@
+// SPDX-License-Identifier: MIT
+// The collision park's tick on sm_100a: the gradient method on spheres, behind include/ebb.h's ebb_collide_* entry
+// points.
+//
+// A tick of Destiny's Evolve with collisions (TIME-706/707; exact_ballpark/vec_collide.py, evolve :990): every free
+// ball's behaviour (GOTO's thrust or STOP's damping; mLastC and the collision list cleared), then for every free
+// massive ball Gradient (space.py:1650): Potential (space.py:1663) with each collision candidate in the order
+// Partition::GetNearbyBalls walks them, recursing on overlaps; then the commit of every free ball (integrated with
+// mLastG + mLastC) and the re-filing in the partition of the balls that moved at least sqrt(0.1) m.
+//
+// One fused kernel: a thread block holds whole worlds (256 / N of them, one thread a slot), so the phases meet at
+// block barriers: behaviours, each ball's end-of-tick prediction into shared memory (depth 0 of every Potential
+// reads it), the gradient (one thread a responder: its candidates, their walk-order keys, the active ones sorted, then
+// Potential on each in turn with the recursion unrolled by depth), then the commit and filing. A ball's gradient reads
+// the others' start-of-tick state only, as Destiny's does (the end states are committed after every Gradient).
+//
+// Exactness: every double operation a single correctly rounded IEEE operation in the reference's order (ebb_arith),
+// glibc's exp (ebb_libm) for integrations over part of a tick, aarch64's int64 conversion for the partition keys.
+#include <cuda_runtime.h>
+
+#include "../../include/ebb.h"
+#include "ebb_arith.cuh"
+#include "ebb_libm.cuh"
+
+namespace ebb {
+namespace collide {
+
+constexpr int NUM_LEVELS = 8;
+constexpr double BIG_BOX = 7864320.0;                 // (1 << 2 NUM_LEVELS) x 480 m x 0.25 (space.py:71)
+constexpr int64_t CODE_BASE = 65;                      // a post-order digit: 0..63 a child box, 64 past the box's level
+constexpr int64_t NOT_A_CANDIDATE = int64_t(1) << 62;
+constexpr double LIGHT_BALL_RATIO = 25.0;
+constexpr double RESPONSE_SCALE = 0.85;
+constexpr double STOP_DAMP = 0.9345794392523364485981308411215;
+constexpr double FIXED_MASS = 1.0e34;
+constexpr int64_t GOTO = 0, STOP = 2;
+
+struct V {
+    double x, y, z;
+};
+__device__ __forceinline__ V vsub(V a, V b) { return V{dsub(a.x, b.x), dsub(a.y, b.y), dsub(a.z, b.z)}; }
+__device__ __forceinline__ V vadd(V a, V b) { return V{dadd(a.x, b.x), dadd(a.y, b.y), dadd(a.z, b.z)}; }
+__device__ __forceinline__ V vmul(V a, double c) { return V{dmul(a.x, c), dmul(a.y, c), dmul(a.z, c)}; }
+__device__ __forceinline__ double vdot(V a, V b) { return dadd(dadd(dmul(a.x, b.x), dmul(a.y, b.y)), dmul(a.z, b.z)); }
+// Vector3d::Normalize: times the reciprocal of the length; a zero vector as it is
+__device__ __forceinline__ V vnorm(V v) {
+    const double n = dsqrt(vdot(v, v));
+    if (n == 0.0) return v;
+    return vmul(v, ddiv(1.0, n));
+}
+__device__ __forceinline__ V ldv(const double* p, int64_t i) { return V{p[3 * i], p[3 * i + 1], p[3 * i + 2]}; }
+__device__ __forceinline__ void stv(double* p, int64_t i, V v) {
+    p[3 * i] = v.x;
+    p[3 * i + 1] = v.y;
+    p[3 * i + 2] = v.z;
+}
+
+// The partition's level widths (exact: BIG_BOX / 4^level) and grid sizes (1 << (2 level + 23))
+__device__ __forceinline__ double level_width(int l) { return ddiv(BIG_BOX, i2d(int64_t(1) << (2 * l))); }
+__device__ __forceinline__ int64_t level_grid(int l) { return int64_t(1) << (2 * l + 23); }
+
+// Ballpark::Integrate (space.py:1609; vec_collide.py:903-932): nothing for t = 0, the cached factor for t = dt, else
+// glibc's exp of (-k / m) t; the Taylor form when k < 1e-10 m t
+__device__ __forceinline__ void integrate(V& p, V& v, V a, double m, double k, double tf, double t, double dt) {
+    if (t == 0.0) return;
+    if (t != dt) tf = lm::exp(dmul(ddiv(dneg(k), m), t));
+    const double k2 = dmul(k, k), ook2 = ddiv(1.0, k2), ook = ddiv(1.0, k);
+    const double pa[3] = {p.x, p.y, p.z}, va[3] = {v.x, v.y, v.z}, aa[3] = {a.x, a.y, a.z};
+    double pn[3], vn[3];
+    if (k < dmul(dmul(1e-10, m), t)) {
+        const double inv_m = ddiv(1.0, m), kt = dmul(dneg(k), t);
+        for (int q = 0; q < 3; ++q) {
+            const double in = dadd(dmul(aa[q], t), dmul(dmul(dmul(va[q], k), inv_m), t));
+            pn[q] = dmul(dadd(dmul(m, dadd(dmul(aa[q], kt), dmul(k, in))), dmul(pa[q], k2)), ook2);
+        }
+    } else {
+        const double tf1 = dsub(tf, 1.0);
+        for (int q = 0; q < 3; ++q) {
+            const double in = dsub(dadd(dmul(aa[q], t), va[q]), dmul(tf, va[q]));
+            pn[q] = dmul(dadd(dmul(m, dadd(dmul(dmul(m, aa[q]), tf1), dmul(k, in))), dmul(pa[q], k2)), ook2);
+        }
+    }
+    for (int q = 0; q < 3; ++q) {
+        const double ma = dmul(m, aa[q]);
+        vn[q] = dmul(dsub(ma, dmul(dsub(ma, dmul(va[q], k)), tf)), ook);
+    }
+    p = V{pn[0], pn[1], pn[2]};
+    v = V{vn[0], vn[1], vn[2]};
+}
+
+// CollideTwoSpheres (Collision.cpp:108; space.py:1631): 0 if already touching, the earlier root in [0, 1], else -1
+__device__ __forceinline__ double collide_two_spheres(V p0, V p1, V q0, V q1, double cr) {
+    const V p0q0 = vsub(p0, q0);
+    const double p0q0_2 = vdot(p0q0, p0q0), cr2 = dmul(cr, cr);
+    if (p0q0_2 <= cr2) return 0.0;
+    const V dpq = vsub(vsub(p1, p0), vsub(q1, q0));
+    const double a = vdot(dpq, dpq), b = dmul(2.0, vdot(p0q0, dpq)), c = dsub(p0q0_2, cr2);
+    if (a == 0.0 && b == 0.0) return -1.0;
+    const double det = dsub(dmul(b, b), dmul(dmul(4.0, a), c));
+    if (det < 0.0) return -1.0;
+    const double s2 = ddiv(dmul(dsub(dneg(b), dsqrt(det)), 0.5), a);
+    return (s2 >= 0.0 && s2 <= 1.0) ? s2 : -1.0;
+}
+
+// A responder's running state through its Gradient: mLastC, mLastCollision, the collision list and the impact record
+struct Acc {
+    V last_c;
+    double last_collision;
+    int64_t hits_n, imp_n;
+};
+
+struct World {
+    const EbbCollideState* s;
+    int64_t base;                 // the world's first slot
+    const V* ends;                // each slot's end-of-tick prediction (shared memory)
+};
+
+// Potential (Ballpark.cpp:2789; space.py:1663) of responder slot b with slot o at recursion depth D, the positions
+// as the recursion has pushed them; its updates of mLastC, mLastCollision, the collision list and the impact record
+template <int D>
+__device__ __forceinline__ void potential(const World& W, int b, int o, V me_pos, V o_pos, Acc& acc) {
+    const EbbCollideState& s = *W.s;
+    const int64_t ib = W.base + b, io = W.base + o;
+    const double k = s.friction, dt = s.dt;
+    const double cr = dadd(s.radius[ib], s.radius[io]);
+    const double m1 = dmul(s.mass[ib], s.agility[ib]);                     // the responder is free
+    const bool free2 = s.free_[io] != 0;
+    const double m2 = free2 ? dmul(s.mass[io], s.agility[io]) : FIXED_MASS;
+    const V v1 = ldv(s.vel, ib), v2 = ldv(s.vel, io), g1 = ldv(s.last_g, ib), g2 = ldv(s.last_g, io);
+    const double tf1 = s.time_factor[ib], tf2 = s.time_factor[io];
+    V p1, q1;
+    if (D == 0) {
+        p1 = W.ends[b];
+        q1 = W.ends[o];
+    } else {
+        V t1 = v1, t2 = v2;
+        p1 = me_pos;
+        q1 = o_pos;
+        integrate(p1, t1, g1, m1, k, tf1, dt, dt);
+        integrate(q1, t2, g2, m2, k, tf2, dt, dt);
+    }
+    const double sv = collide_two_spheres(me_pos, p1, o_pos, q1, cr);
+    if (sv == -1.0) return;
+    V a1;
+    if (sv > 0.0) {                                                   // COL-707, COL-708: the impact
+        V pp = me_pos, vp = v1, qq = o_pos, vq = v2;
+        integrate(pp, vp, g1, m1, k, tf1, dmul(sv, dt), dt);
+        integrate(qq, vq, g2, m2, k, tf2, dmul(sv, dt), dt);
+        const V normal = vnorm(vsub(qq, pp));
+        const double u1 = vdot(vp, normal), u2 = vdot(vq, normal);
+        if (!free2) {
+            vp = vsub(vp, vmul(normal, dmul(2.0, u1)));
+        } else {
+            const double mm1 = s.mass[ib], mm2 = s.mass[io];
+            const double u1p = ddiv(dadd(dsub(dmul(mm1, u1), dmul(mm2, u1)), dmul(dmul(2.0, mm2), u2)), dadd(mm1, mm2));
+            vp = vadd(vp, vmul(normal, dsub(u1p, u1)));
+        }
+        integrate(pp, vp, g1, m1, k, tf1, dmul(dsub(1.0, sv), dt), dt);
+        const double inv_m = ddiv(1.0, m1), inv_t = ddiv(1.0, dsub(tf1, 1.0));
+        const double ga[3] = {g1.x, g1.y, g1.z}, va[3] = {v1.x, v1.y, v1.z}, wa[3] = {vp.x, vp.y, vp.z};
+        double r[3];
+        for (int q = 0; q < 3; ++q) {
+            const double x = dadd(dsub(dadd(dmul(ga[q], dneg(m1)), dmul(ga[q], dmul(tf1, m1))), dmul(dmul(va[q], tf1), k)),
+                                  dmul(wa[q], k));
+            r[q] = dmul(dmul(dneg(x), inv_m), inv_t);
+        }
+        a1 = V{r[0], r[1], r[2]};
+        if (D == 0) {                                                 // the impact record, in candidate order
+            const int64_t at = ib * s.impact_cap + (acc.imp_n < s.impact_cap ? acc.imp_n : s.impact_cap - 1);
+            s.imp_slot[at] = o;
+            s.imp_s[at] = sv;
+            s.imp_closing[at] = dsub(u1, u2);
+            ++acc.imp_n;
+        }
+    } else {                                                          // COL-709, COL-710: already overlapping
+        const V p0q0 = vsub(o_pos, me_pos);
+        const double p0q0_2 = vdot(p0q0, p0q0);
+        V normal;
+        if (p0q0_2 == 0.0) normal = (s.id[ib] > s.id[io]) ? V{1.0, 0.0, 0.0} : V{-1.0, 0.0, 0.0};
+        else normal = vnorm(p0q0);
+        const double dist = dadd(dsub(cr, dsqrt(p0q0_2)), 1.0);
+        const double msum = dadd(m1, m2);
+        const double d1 = dmul(ddiv(m2, msum), dist);
+        [[maybe_unused]] const double d2 = dmul(ddiv(m1, msum), dist);
+        if constexpr (D < 2) {                                       // COL-710: two free balls pushed apart first
+            if (free2) {
+                potential<D + 1>(W, b, o, vsub(me_pos, vmul(normal, d1)), vadd(o_pos, vmul(normal, d2)), acc);
+                if (ddiv(m2, m1) > LIGHT_BALL_RATIO) acc.last_c = vmul(vnorm(acc.last_c), dist);
+                const V dv = vsub(v1, v2);
+                if (vdot(dv, dv) > 0.0001) return;
+            }
+        }
+        const double normal_comp = vdot(g1, normal);
+        const double tmp = ddiv(1.0, dadd(m1, dmul(dt, k)));
+        const double c = ddiv(dneg(d1), dmul(dmul(dt, tmp), m1));
+        a1 = vsub(vmul(vsub(vmul(normal, c), v1), ddiv(1.0, dt)), vmul(normal, normal_comp));
+    }
+    if (sv >= acc.last_collision) {                                  // COL-711: the later impact, the stronger at a tie
+        const V lc = vmul(a1, RESPONSE_SCALE);
+        if (sv == acc.last_collision) {
+            if (vdot(lc, lc) > vdot(acc.last_c, acc.last_c)) acc.last_c = lc;
+        } else {
+            acc.last_c = lc;
+            acc.last_collision = sv;
+        }
+    }
+    s.hits[ib * s.hit_cap + (acc.hits_n < s.hit_cap ? acc.hits_n : s.hit_cap - 1)] = s.id[io];
+    ++acc.hits_n;
+}
+
+// Whether a box of ball n is one of ball b's boxes, an ancestor of one or below one (vec_collide.py:809): per axis,
+// some option of the finer ball shifted to the coarser level equals some option of the coarser
+__device__ __forceinline__ bool related(const EbbCollideState& s, int64_t ib, int64_t in) {
+    const int64_t Lb = s.level[ib], Ln = s.level[in];
+    const int64_t sh = 2 * (Lb > Ln ? Lb - Ln : Ln - Lb);
+    const bool coarse = Ln <= Lb;
+    for (int q = 0; q < 3; ++q) {
+        const int64_t kb = s.key[3 * ib + q], mb = s.mod[3 * ib + q], kn = s.key[3 * in + q], mn = s.mod[3 * in + q];
+        const int64_t lo_b = kb + (mb < 0 ? mb : 0), hi_b = kb + (mb > 0 ? mb : 0);
+        const int64_t lo_n = kn + (mn < 0 ? mn : 0), hi_n = kn + (mn > 0 ? mn : 0);
+        const int64_t xl = (coarse ? lo_b : lo_n) >> sh, xh = (coarse ? hi_b : hi_n) >> sh;
+        const int64_t yl = coarse ? lo_n : lo_b, yh = coarse ? hi_n : hi_b;
+        if (!(xl == yl || xl == yh || xh == yl || xh == yh)) return false;
+    }
+    return true;
+}
+
+// The position of ball n's first box in ball b's GetNearbyBalls walk, as a sort key (vec_collide.py:825): the index of
+// the first of b's boxes (by key) that n's box relates to, the part (0 an ancestor, 1 below, 2 the box itself) and
+// within it the ancestor's distance or the box's post-order code (path digits from b's level; 64 past n's level)
+__device__ __forceinline__ int64_t order_key(const EbbCollideState& s, int64_t ib, int64_t in) {
+    const int64_t Lb = s.level[ib], Ln = s.level[in];
+    int64_t Kn[3], Mn[3], cb[3], lo_b[3], hi_b[3];
+    for (int q = 0; q < 3; ++q) {
+        const int64_t kb = s.key[3 * ib + q], mb = s.mod[3 * ib + q];
+        Kn[q] = s.key[3 * in + q];
+        Mn[q] = s.mod[3 * in + q];
+        cb[q] = 1 + (mb != 0);
+        lo_b[q] = kb + (mb < 0 ? mb : 0);
+        hi_b[q] = kb + (mb > 0 ? mb : 0);
+    }
+    int64_t span = 1;
+    for (int l = 0; l < NUM_LEVELS - 1; ++l) span *= CODE_BASE;
+    if (Ln <= Lb) {
+        const int64_t s_up = 2 * (Lb - Ln);
+        int64_t idx[3];
+        for (int q = 0; q < 3; ++q) {
+            const int64_t v = lo_b[q] >> s_up;
+            idx[q] = ((v == Kn[q]) || (Mn[q] != 0 && v == Kn[q] + Mn[q])) ? 0 : 1;
+        }
+        const int64_t seg = (idx[0] * cb[1] + idx[1]) * cb[2] + idx[2];
+        return Ln < Lb ? (seg * 3) * span + (Lb - Ln) : (seg * 3 + 2) * span;
+    }
+    const int64_t s_dn = 2 * (Ln - Lb);
+    int64_t best = NOT_A_CANDIDATE;
+    for (int c = 0; c < 8; ++c) {
+        const int64_t bit[3] = {(c >> 2) & 1, (c >> 1) & 1, c & 1};
+        bool ok = true;
+        int64_t box[3], jx[3];
+        for (int q = 0; q < 3; ++q) {
+            if (bit[q] != 0 && Mn[q] == 0) ok = false;
+            box[q] = Kn[q] + Mn[q] * bit[q];
+            const int64_t anc = box[q] >> s_dn;
+            const bool in0 = anc == lo_b[q], in1 = anc == hi_b[q] && cb[q] == 2;
+            if (!(in0 || in1)) ok = false;
+            jx[q] = in0 ? 0 : 1;
+        }
+        if (!ok) continue;
+        const int64_t seg = (jx[0] * cb[1] + jx[1]) * cb[2] + jx[2];
+        int64_t code = 0, power = span;
+        for (int lvl = 1; lvl < NUM_LEVELS; ++lvl) {
+            power /= CODE_BASE;
+            const int64_t shift = 2 * (Ln - lvl) > 0 ? 2 * (Ln - lvl) : 0;
+            int64_t digit = ((box[0] >> shift) & 3) * 16 + ((box[1] >> shift) & 3) * 4 + ((box[2] >> shift) & 3);
+            if (lvl > Ln) digit = CODE_BASE - 1;
+            if (lvl <= Lb) digit = 0;
+            code += digit * power;
+        }
+        const int64_t key = (seg * 3 + 1) * span + code;
+        if (key < best) best = key;
+    }
+    return best;
+}
+
+// Ball::InsertInBoxes' outcome (vec_collide.py:767-798): the level of the inflated radius, the key of the box holding
+// the centre, the side (-1, 0, +1) an axis where the inflated sphere reaches the next box. Returns whether the
+// reference's park would refuse the filing (a key at the grid's edge, or a ball wider than a top box).
+__device__ __forceinline__ bool file_slot(const EbbCollideState& s, int64_t i) {
+    const V p = ldv(s.pos, i), v = ldv(s.vel, i);
+    const double k = s.friction;
+    double infl = s.radius[i];
+    if (s.free_[i]) {
+        const double m = dmul(s.mass[i], s.agility[i]);
+        const double a = ddiv(dmul(dmul(k, s.speed_fraction[i]), s.max_vel[i]), m);
+        const double speed = dsqrt(vdot(v, v));
+        const double ma = dmul(m, a);
+        const double mps = ddiv(dsub(ma, dmul(dsub(ma, dmul(speed, k)), s.time_factor[i])), k);
+        infl = dadd(s.radius[i], dmul(s.dt, mps));
+    }
+    int level = -1;
+    for (int l = 0; l < NUM_LEVELS; ++l)
+        if (!(dmul(3.0, infl) > level_width(l))) ++level;
+    if (level < 0) level = 0;
+    const double w = level_width(level);
+    const int64_t grid = level_grid(level);
+    const double half = dmul(dmul(0.5, w), i2d(grid)), center = dmul(dmul(w, i2d(grid)), 0.5), fac = ddiv(1.0, w);
+    const double pa[3] = {p.x, p.y, p.z};
+    bool bad = level == 0 && dmul(s.radius[i], 2.0) > level_width(0);
+    s.level[i] = level;
+    for (int q = 0; q < 3; ++q) {
+        int64_t kq = to_i64(dmul(dadd(pa[q], half), fac));
+        kq = kq < 0 ? 0 : (kq >= grid ? grid - 1 : kq);
+        const double lo = dsub(dmul(i2d(kq), w), center), hi = dsub(dmul(i2d(kq + 1), w), center);
+        const bool down = dsub(dadd(lo, infl), pa[q]) > 0.0, up = dsub(dsub(hi, infl), pa[q]) < 0.0;
+        const int64_t mq = down ? -1 : (up ? 1 : 0);
+        s.key[3 * i + q] = kq;
+        s.mod[3 * i + q] = mq;
+        if (kq <= 0 || kq >= grid - 1 || kq + mq < 0 || kq + mq >= grid) bad = true;
+    }
+    return bad;
+}
+
+constexpr int MAX_SLOTS = EBB_COLLIDE_MAX_SLOTS;
+
+__global__ void __launch_bounds__(256) tick_kernel(EbbCollideState s, const uint8_t* __restrict__ active,
+                                                   int32_t* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* ends = (V*)smem_raw;
+    const int N = (int)s.slots, wpb = blockDim.x / N;
+    const int lw = threadIdx.x / N, j = threadIdx.x - lw * N;
+    const int64_t w = (int64_t)blockIdx.x * wpb + lw;
+    const bool mine = lw < wpb && w < s.worlds && (active == nullptr || active[w] != 0);
+    const int64_t base = w * N, i = base + j;
+    const bool live = mine && s.exists[i] && s.free_[i];
+    const double k = s.friction, dt = s.dt;
+    // (1) the behaviours: mLastG, STOP's damping, mLastC and the collision list cleared
+    if (live) {
+        V g = V{0.0, 0.0, 0.0};
+        if (s.mode[i] == GOTO) {
+            const V a = vsub(ldv(s.goto_pt, i), ldv(s.pos, i));
+            const double length2 = vdot(a, a);
+            const double sf = s.speed_fraction[i], mv = s.max_vel[i];
+            const double dist = dmul(dmul(sf, mv), dt);
+            const double max_thrust = ddiv(dmul(dmul(k, sf), mv), dmul(s.mass[i], s.agility[i]));
+            const V unit = vnorm(a);
+            const double dd = dmul(dist, dist);
+            double scale = max_thrust;
+            if (length2 < dd) {
+                const double coff = ddiv(length2, dd);
+                scale = dmul(dmul(max_thrust, coff), coff);
+            }
+            g = vmul(unit, scale);
+        }
+        stv(s.last_g, i, g);
+        if (s.mode[i] == STOP) {
+            const double vy = s.vel[3 * i + 1];
+            s.vel[3 * i + 1] = dmul(dsub(vy, dmul(0.07, vy)), STOP_DAMP);
+        }
+        stv(s.last_c, i, V{0.0, 0.0, 0.0});
+        for (int64_t q = 0; q < s.hit_cap; ++q) s.hits[i * s.hit_cap + q] = -1;
+        s.hits_n[i] = 0;
+        for (int64_t q = 0; q < s.impact_cap; ++q) s.imp_slot[i * s.impact_cap + q] = -1;
+        s.imp_n[i] = 0;
+    }
+    __syncthreads();
+    // (2) every ball's end of the tick as depth 0 of Potential predicts it (a fixed ball with mass 1e34)
+    if (mine && s.exists[i]) {
+        V p = ldv(s.pos, i), v = ldv(s.vel, i);
+        const double m = s.free_[i] ? dmul(s.mass[i], s.agility[i]) : FIXED_MASS;
+        integrate(p, v, ldv(s.last_g, i), m, k, s.time_factor[i], dt, dt);
+        ends[threadIdx.x] = p;
+    }
+    __syncthreads();
+    // (3) the gradient: each free massive ball against its candidates in GetNearbyBalls' order
+    if (live && s.massive[i]) {
+        const World W{&s, base, ends + lw * N};
+        const double cr0 = s.radius[i];
+        const V pb = ldv(s.pos, i), eb = W.ends[j];
+        int64_t okey[MAX_SLOTS];
+        int8_t oslot[MAX_SLOTS];
+        int nact = 0;
+        for (int o = 0; o < N; ++o) {
+            const int64_t io = base + o;
+            if (o == j || !s.exists[io] || !s.massive[io] || s.cloaked[io]) continue;
+            if (s.junk[io] && !s.junk[i]) continue;
+            if (!related(s, i, io)) continue;
+            if (collide_two_spheres(pb, eb, ldv(s.pos, io), W.ends[o], dadd(cr0, s.radius[io])) == -1.0) continue;
+            const int64_t key = order_key(s, i, io), id = s.id[io];
+            int at = nact++;                                          // insertion by (key, id)
+            while (at > 0 && (okey[at - 1] > key || (okey[at - 1] == key && s.id[base + oslot[at - 1]] > id))) {
+                okey[at] = okey[at - 1];
+                oslot[at] = oslot[at - 1];
+                --at;
+            }
+            okey[at] = key;
+            oslot[at] = (int8_t)o;
+        }
+        Acc acc{V{0.0, 0.0, 0.0}, -1.0, 0, 0};
+        for (int q = 0; q < nact; ++q) {
+            const int o = oslot[q];
+            potential<0>(W, j, o, pb, ldv(s.pos, base + o), acc);
+        }
+        stv(s.last_c, i, acc.last_c);
+        s.last_collision[i] = acc.last_collision;
+        s.hits_n[i] = acc.hits_n;
+        s.imp_n[i] = acc.imp_n;
+    }
+    __syncthreads();
+    // (4) the commit, then the re-filing of the balls that moved at least sqrt(0.1) m
+    if (live) {
+        V p = ldv(s.pos, i), v = ldv(s.vel, i);
+        const V old = p, oldv = v;
+        integrate(p, v, vadd(ldv(s.last_g, i), ldv(s.last_c, i)), dmul(s.mass[i], s.agility[i]), k, s.time_factor[i],
+                  dt, dt);
+        stv(s.old_pos, i, old);
+        stv(s.old_vel, i, oldv);
+        stv(s.pos, i, p);
+        stv(s.vel, i, v);
+        const V d = vsub(p, old);
+        if (!(vdot(d, d) < 0.1) && file_slot(s, i)) atomicOr(status, 2);
+    }
+}
+
+// The load's last steps for every existing slot: the decay factor (exp(-k dt / m), 0 for m <= 0) and the first filing
+__global__ void load_kernel(EbbCollideState s, int32_t* status) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.worlds * s.slots || !s.exists[i]) return;
+    const double m = dmul(s.mass[i], s.agility[i]);
+    s.time_factor[i] = m > 0.0 ? lm::exp(ddiv(dmul(dneg(s.friction), s.dt), m)) : 0.0;
+    if (file_slot(s, i)) atomicOr(status, 1);
+}
+
+}  // namespace collide
+}  // namespace ebb
+
+namespace {
+int launched() {
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : (int)e;
+}
+bool shape_ok(const EbbCollideState* s) {
+    return s != nullptr && s->worlds >= 0 && s->slots >= 1 && s->slots <= EBB_COLLIDE_MAX_SLOTS &&
+           s->hit_cap == (s->slots > 1 ? 3 * (s->slots - 1) : 1) && s->impact_cap == (s->slots > 1 ? s->slots - 1 : 1);
+}
+}  // namespace
+
+extern "C" {
+
+int ebb_collide_tick(const EbbCollideState* s, const uint8_t* active, int32_t* status, void* stream) {
+    if (!shape_ok(s) || status == nullptr) return EBB_EINVAL;
+    if (s->worlds == 0) return 0;
+    const int N = (int)s->slots, wpb = 256 / N > 0 ? 256 / N : 1, threads = wpb * N;
+    const unsigned grid = (unsigned)((s->worlds + wpb - 1) / wpb);
+    const size_t smem = (size_t)threads * sizeof(ebb::collide::V);
+    ebb::collide::tick_kernel<<<grid, threads, smem, (cudaStream_t)stream>>>(*s, active, status);
+    return launched();
+}
+
+int ebb_collide_load(const EbbCollideState* s, int32_t* status, void* stream) {
+    if (!shape_ok(s) || status == nullptr) return EBB_EINVAL;
+    const int64_t n = s->worlds * s->slots;
+    if (n == 0) return 0;
+    ebb::collide::load_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*s, status);
+    return launched();
+}
+
+}  // extern "C"

@@ -207,12 +207,15 @@ class CollideWorlds:
             return
         mask = torch.zeros(park.W, park.N, dtype=torch.bool)
         point = torch.zeros(park.W, park.N, 3, dtype=torch.float64)
-        ids = park.id.detach().cpu()
+        ids = torch.as_tensor(park.id).detach().cpu()
         for w, bid, p in todo:
             j = int((ids[w] == bid).nonzero()[0, 0])
             mask[w, j] = True
             point[w, j] = torch.tensor(p, dtype=torch.float64)
-        park.goto_point(mask.to(park.dev), point.to(park.dev))
+        if isinstance(park.id, torch.Tensor):
+            park.goto_point(mask.to(park.dev), point.to(park.dev))
+        else:                                    # a numpy park (the CPU oracle)
+            park.goto_point(mask.numpy(), point.numpy())
 
 
 def collide_worlds(seed: int, worlds: int, ships: int = 4, spheres: int = 4, statics: int = 8, ticks: int = 500,

@@ -44,6 +44,24 @@ typedef struct EbbFlightState {
     uint8_t *free_, *moribund, *massive, *interactive, *sensor;
 } EbbFlightState;
 
+/* The collision park (the gradient method on spheres): W worlds of N ball slots, world w is slots [w N, (w + 1) N),
+ * each world's balls in its first slots in ascending id (an empty slot has exists = 0). The layout is the
+ * reference's [W, N] tensors, row-major: a vector field is [W N][3] (x, y, z of a slot together), the collision list
+ * [W N][hit_cap] (hit_cap = 3 (N - 1), at least 1), the impact record [W N][impact_cap] (impact_cap = N - 1, at least
+ * 1). Field for field the state of exact_ballpark.vec_collide.VecCollidePark (vec_collide.py:470-512). */
+#define EBB_COLLIDE_MAX_SLOTS 64
+typedef struct EbbCollideState {
+    int64_t worlds, slots, hit_cap, impact_cap;
+    double friction, dt;
+    double *pos, *vel, *old_pos, *old_vel, *goto_pt, *last_g, *last_c;                 /* [W N][3] */
+    double *mass, *radius, *max_vel, *agility, *speed_fraction, *time_factor, *last_collision;   /* [W N] */
+    int64_t *id, *mode, *level, *key, *mod;                                            /* key, mod [W N][3] */
+    uint8_t *exists, *free_, *massive, *junk, *cloaked;
+    int64_t *hits, *hits_n;                                                            /* [W N][hit_cap], [W N] */
+    int64_t *imp_slot, *imp_n;                                                         /* [W N][impact_cap], [W N] */
+    double *imp_s, *imp_closing;                                                       /* [W N][impact_cap] */
+} EbbCollideState;
+
 /* The ABI version (EBB_ABI_VERSION). Replaces xbpm_abi / xbpo_abi (exact_ballpark/vec_modes_cuda.cu:750,
  * vec_orient_cuda.cu:499). */
 int ebb_abi(void);
@@ -113,6 +131,21 @@ int64_t ebb_plan_worlds(const int64_t* starts, const int64_t* lens, int64_t coun
  * serving loop's episodes. No counterpart in the reference (its parks are loaded whole). */
 int ebb_flight_move(const EbbFlightState* dst, const EbbFlightState* src, const int64_t* src_rows,
                     const int64_t* dst_rows, int64_t m, int32_t* status, void* stream, int block);
+
+/* One tick of the collision park in place (TIME-706/707): the free balls' behaviours (GOTO's thrust, STOP's
+ * damping), Gradient for every free massive ball (Potential with each collision candidate in Partition::
+ * GetNearbyBalls' order, the overlap recursion, the impact and overlap responses, the later impact kept), the commit and
+ * the re-filing of the balls that moved. `active` [W] (nullable): only those worlds tick. One launch, one thread block
+ * a group of whole worlds (N <= EBB_COLLIDE_MAX_SLOTS). status[0] bit 2: a re-filing at the grid's edge. Replaces
+ * VecCollidePark.evolve's gradient path (exact_ballpark/vec_collide.py:990) and its kernels xbpc_tick / xbpc_gradient
+ * (vec_collide_cuda.cu:1312-1530). */
+int ebb_collide_tick(const EbbCollideState* s, const uint8_t* active, int32_t* status, void* stream);
+
+/* The load's device steps for every existing slot (the host has written AddBall's clamped values): the decay factor
+ * exp(-k dt / m) with glibc's exp (0 for m <= 0) and the first filing. status[0] bit 1: a filing the reference refuses
+ * (a key at the grid's edge, or a ball wider than a top box). Replaces VecCollidePark.load's time factor and
+ * _filing / _check_filing (vec_collide.py:550-667, 776-807). */
+int ebb_collide_load(const EbbCollideState* s, int32_t* status, void* stream);
 
 /* SnapOrientation of the rows in mask[n] (nonzero bytes): the rotation turned to the velocity and rolled upright,
  * the old rotation the same, the angular velocities zeroed (at a speed of 1e-6 m/s or less nothing changes). With
