@@ -213,6 +213,67 @@ def serve_runs(args, dev) -> dict:
     return out
 
 
+# Algorithmic bytes of one world-tick of the collision park (4 ships, 4 free spheres, 8 fixed spheres): a free ball
+# reads 235 B (position, velocity, goto point 3 x 24; mode, mass, agility, speed fraction, max velocity, decay factor,
+# radius, id, level 8 x 8; key, side 2 x 24; 5 flags) and writes 740 B (mLastG, mLastC, old position and velocity,
+# position, velocity 6 x 24 plus the damped vertical velocity 8; the collision list 45 x 8 and its count 8, the impact
+# record's slots 15 x 8 and its count 8, mLastCollision 8; level 8, key and side 2 x 24 when re-filed); a fixed ball
+# is read as a candidate, 150 B (position, velocity, mLastG 3 x 24; decay factor, mass, agility, radius, id, level
+# 6 x 8; key, side counted once with the free balls' 0; 5 flags, rounded up).
+COLLIDE_BYTES_PER_WORLD_TICK = 8 * (235 + 740) + 8 * 150
+
+
+def collide_runs(args, dev) -> dict:
+    """The collision park (exact_ballpark_b200.collide, the gradient method on spheres) at the collision
+    benchmark's shape: --collide-worlds worlds of 4 ships, 4 free spheres and 8 fixed spheres
+    (workloads.collide_worlds: +-20 km, radii log-uniform 10 m - 5 km, ships GOTO at spheres, re-aimed every 25 ticks
+    between timed ticks), warm-up ticks, then --collide-steps ticks each one CUDA-graph replay of the one-launch tick,
+    timed with CUDA events (L2 flushed before each). Ship-ticks count the 4 ships a world, as the reference's
+    collision benchmark does; world-ticks and ball-ticks beside them."""
+    import torch
+
+    from exact_ballpark_b200.collide import CollideGraph, VecCollidePark
+    from exact_ballpark_b200.workloads import collide_worlds
+    W = args.collide_worlds
+    ticks = args.warmup + args.collide_steps
+    w = collide_worlds(21, W, ticks=ticks)
+    park = VecCollidePark(W, 16, device=dev)
+    park.load(w.worlds)
+    graph = CollideGraph(park)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    total = 0.0
+    contacts = 0
+    for step in range(1, ticks + 1):
+        w.apply(park, step)
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        graph.tick()
+        b.record(stream)
+        b.synchronize()
+        if step > args.warmup:
+            total += a.elapsed_time(b)
+            contacts += int(park.hits_n.sum().item())
+    park.check()
+    per = total / args.collide_steps
+    peak, kind = _peaks()
+    achieved = COLLIDE_BYTES_PER_WORLD_TICK * W / (per / 1e3) / 1e9
+    return {"workload": f"collision park, gradient method on spheres: {W} worlds x (4 ships + 4 free spheres + 8 "
+                        "fixed spheres), ships GOTO at spheres re-aimed every 25 ticks",
+            "value": 4 * W / (per / 1e3), "unit": "ship-ticks/s", "world_ticks_per_s": W / (per / 1e3),
+            "ball_ticks_per_s": 16 * W / (per / 1e3), "ms_per_step": per, "steps": args.collide_steps,
+            "warmup": args.warmup, "contacts_per_tick": contacts / args.collide_steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": kind, "traffic": None,
+                         "note": f"algorithmic {COLLIDE_BYTES_PER_WORLD_TICK} B/world-tick x {W} worlds over the "
+                                 "tick's CUDA-event time; the tick is FP64 latency-bound (divides, square roots, "
+                                 "the candidates' sort), not HBM-bound"},
+            "reference_published": {"value": 141e6, "unit": "ship-ticks/s", "hardware": "GH200",
+                                    "config": "ships=4, spheres=4, statics=0, kernel, 65,536 worlds "
+                                              "(docs/benchmarks.md)"}}
+
+
 def _config(args, schedule: str) -> dict:
     return {"workload": (f"flight-mode park, dynamical orientation on, new orbit law: {args.worlds} worlds x "
                          f"{args.ships} ships (follow / orbit / warp), per-rank"),
@@ -230,6 +291,9 @@ def main() -> None:
     ap.add_argument("--ships", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-collide", action="store_true")
+    ap.add_argument("--collide-worlds", type=int, default=65536)
+    ap.add_argument("--collide-steps", type=int, default=50)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-seconds", type=float, default=6.0)
     ap.add_argument("--serve-budget-gb", type=float, default=80.0)
@@ -371,6 +435,8 @@ def main() -> None:
             "e2e": {"value": total_ships * args.steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
             "gpu_launches": 3 * args.steps, "clocks": clocks}
+    if not args.no_collide:
+        line["collide"] = collide_runs(args, dev)
     if not args.no_serve:
         line["serve"] = serve_runs(args, dev)
         line["serve"]["plain_ship_ticks_per_s"] = line["plain"]["value"] / world_size
