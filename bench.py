@@ -259,13 +259,20 @@ def collide_runs(args, dev) -> dict:
     per = total / args.collide_steps
     peak, kind = _peaks()
     achieved = COLLIDE_BYTES_PER_WORLD_TICK * W / (per / 1e3) / 1e9
+    traffic = None
+    tp = ROOT / "profiles" / "collide_tick_traffic.json"
+    if tp.exists():
+        try:
+            traffic = float(json.loads(tp.read_text())["dram_bytes_per_world_tick"]) * W
+        except Exception:
+            traffic = None
     return {"workload": f"collision park, gradient method on spheres: {W} worlds x (4 ships + 4 free spheres + 8 "
                         "fixed spheres), ships GOTO at spheres re-aimed every 25 ticks",
             "value": 4 * W / (per / 1e3), "unit": "ship-ticks/s", "world_ticks_per_s": W / (per / 1e3),
             "ball_ticks_per_s": 16 * W / (per / 1e3), "ms_per_step": per, "steps": args.collide_steps,
             "warmup": args.warmup, "contacts_per_tick": contacts / args.collide_steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": kind, "traffic": None,
+                         "peak_kind": kind, "traffic": traffic,
                          "note": f"algorithmic {COLLIDE_BYTES_PER_WORLD_TICK} B/world-tick x {W} worlds over the "
                                  "tick's CUDA-event time; the tick is FP64 latency-bound (divides, square roots, "
                                  "the candidates' sort), not HBM-bound"},
