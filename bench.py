@@ -223,6 +223,53 @@ def serve_runs(args, dev) -> dict:
 COLLIDE_BYTES_PER_WORLD_TICK = 8 * (235 + 740) + 8 * 150
 
 
+def ragged_runs(args, dev) -> dict:
+    """The ragged batch against the plain schedule on the same GPU: --ragged-worlds flight-mode worlds of 1-128 ships
+    (log-uniform, the ragged benchmark's world sizes; workloads.ragged_flight_worlds), dynamical orientation on, packed
+    with no padding. The same --ragged-steps ticks from the same state (saved and restored) through each schedule:
+    plain (two launches, records in scratch), tiled (worlds packed greedily in row order, one tile a block) and listed
+    worlds packed best fit (ebb_plan_worlds: any worlds in a tile, one tile a block), each tick timed with CUDA events
+    after an L2 flush."""
+    import torch
+
+    from exact_ballpark_b200 import VecModesPark, tick_plain, tick_tiled, tick_worlds
+    from exact_ballpark_b200.tiles import plan_best_fit, plan_tiles
+    from exact_ballpark_b200.workloads import ragged_flight_worlds
+    w = ragged_flight_worlds(31, args.ragged_worlds)
+    n = len(w.rows)
+    park = VecModesPark(n, device=dev, dynamical_orientation=True, use_new_orbit=True)
+    w.packed().load(park)
+    w.apply(park)
+    for _ in range(args.warmup):
+        tick_plain(park, 256)
+    greedy = plan_tiles(park.world, cap=256, block=256)
+    best = plan_best_fit(park.world, cap=256, block=256)
+    saved = {k: getattr(park, k).clone() for k in park.row_tensors()}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    out = {"workload": f"ragged flight-mode batch: {args.ragged_worlds} worlds of 1-128 ships (log-uniform), {n} "
+                       "ships, dynamical orientation on, new orbit law", "ships": n, "worlds": args.ragged_worlds,
+           "steps": args.ragged_steps, "tiles_greedy": greedy.tiles, "tiles_best_fit": best.tiles}
+    for name, run in (("plain", lambda: tick_plain(park, 256)), ("tiled_greedy", lambda: tick_tiled(park, greedy)),
+                      ("worlds_best_fit", lambda: tick_worlds(park, None, best))):
+        for k, v in saved.items():
+            getattr(park, k).copy_(v)
+        total = 0.0
+        for _ in range(args.ragged_steps):
+            flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            run()
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        per = total / args.ragged_steps
+        out[name] = {"ms_per_step": per, "value": n / (per / 1e3), "unit": "ship-ticks/s"}
+    out["speedup_best_fit_vs_plain"] = out["plain"]["ms_per_step"] / out["worlds_best_fit"]["ms_per_step"]
+    out["speedup_greedy_vs_plain"] = out["plain"]["ms_per_step"] / out["tiled_greedy"]["ms_per_step"]
+    return out
+
+
 def collide_runs(args, dev) -> dict:
     """The collision park (exact_ballpark_b200.collide, the gradient method on spheres) at the collision
     benchmark's shape: --collide-worlds worlds of 4 ships, 4 free spheres and 8 fixed spheres
@@ -299,6 +346,9 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-collide", action="store_true")
+    ap.add_argument("--no-ragged", action="store_true")
+    ap.add_argument("--ragged-worlds", type=int, default=10000)
+    ap.add_argument("--ragged-steps", type=int, default=30)
     ap.add_argument("--collide-worlds", type=int, default=65536)
     ap.add_argument("--collide-steps", type=int, default=50)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
@@ -442,6 +492,8 @@ def main() -> None:
             "e2e": {"value": total_ships * args.steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
             "gpu_launches": 3 * args.steps, "clocks": clocks}
+    if not args.no_ragged:
+        line["ragged"] = ragged_runs(args, dev)
     if not args.no_collide:
         line["collide"] = collide_runs(args, dev)
     if not args.no_serve:

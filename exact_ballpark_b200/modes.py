@@ -592,9 +592,10 @@ def _worlds_plan_ok(park: VecModesPark) -> bool:
     return park.plan is not None and park.plan.cap <= WORLDS_MAX_TILE and len(park.plan.world_rows) > 1
 
 
-def tick_worlds(park: VecModesPark, active: torch.Tensor | None = None, plan: TilePlan | None = None) -> None:
-    """The listed-worlds schedule over the park's own worlds (its tile plan as a world list), with OnTick's row mask
-    `active` (a contiguous bool tensor [n], or None for every row) applied inside the kernel."""
+def tick_worlds(park: VecModesPark, active: torch.Tensor | None = None, plan=None) -> None:
+    """The listed-worlds schedule over the park's own worlds (its tile plan as a world list, or a best-fit
+    tiles.WorldsPlan), with OnTick's row mask `active` (a contiguous bool tensor [n], or None for every row) applied
+    inside the kernel."""
     plan = plan or park.plan
     if plan is None:
         raise ValueError("the park's worlds are not contiguous rows: no tile plan")

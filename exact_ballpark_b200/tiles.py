@@ -97,3 +97,49 @@ def plan_tiles(world: torch.Tensor, cap: int = DEFAULT_CAP, block: int | None = 
     if blk % 32 or not 32 <= blk <= 256:
         raise ValueError(f"block {blk}: a multiple of 32 up to 256")
     return TilePlan(tile_rows, cap, blk, grid or (len(tile_rows) - 1), max_world, runs)
+
+
+@dataclass
+class WorldsPlan:
+    """A plan for the listed-worlds tick over a park's own worlds, packed best fit (include/ebb.h: ebb_plan_worlds):
+    tiles of at most `cap` rows made of any whole worlds, not only neighbours, so small worlds fill the tiles that
+    large ones leave room in. `worlds` [2W] row runs and `tile_worlds` [T + 1] as the kernel takes them."""
+    worlds: list
+    tile_worlds: list
+    cap: int
+    block: int
+    grid: int
+    _dev: dict = field(default_factory=dict, repr=False)
+
+    @property
+    def tiles(self) -> int:
+        return len(self.tile_worlds) - 1
+
+    def worlds_on(self, dev) -> tuple:
+        key = str(dev)
+        if key not in self._dev:
+            self._dev[key] = (torch.tensor(self.worlds, dtype=torch.int64, device=dev),
+                              torch.tensor(self.tile_worlds, dtype=torch.int64, device=dev))
+        return self._dev[key]
+
+
+def plan_best_fit(world: torch.Tensor, cap: int = DEFAULT_CAP, block: int | None = None) -> WorldsPlan | None:
+    """The best-fit plan of a park's world column (each world one contiguous run of at most cap rows), one tile a
+    block; None when the worlds are not contiguous runs or one is larger than cap."""
+    import numpy as np
+
+    from . import _native
+    runs = world_runs(world)
+    if runs is None or len(runs) < 2:
+        return None
+    r = np.asarray(runs, dtype=np.int64)
+    starts, lens = np.ascontiguousarray(r[:-1]), np.ascontiguousarray(np.diff(r))
+    if int(lens.max()) > cap:
+        return None
+    worlds = np.empty(2 * len(starts), dtype=np.int64)
+    tile_worlds = np.empty(len(starts) + 1, dtype=np.int64)
+    tiles = _native.lib().ebb_plan_worlds(starts.ctypes.data, lens.ctypes.data, len(starts), int(cap),
+                                          worlds.ctypes.data, tile_worlds.ctypes.data)
+    _native.check(int(tiles) if tiles < 0 else 0, "ebb_plan_worlds")
+    blk = block or DEFAULT_BLOCK
+    return WorldsPlan(worlds.tolist(), tile_worlds[:tiles + 1].tolist(), int(cap), blk, int(tiles))

@@ -183,6 +183,14 @@ def flight_worlds(seed: int, worlds: int, ships: int = 4) -> FlightWorlds:
     return FlightWorlds(rows, fm, om, wm, tgt, rg, pt, wf, worlds, ships)
 
 
+def ragged_flight_worlds(seed: int, worlds: int, max_ships: int = 128) -> FlightWorlds:
+    """W flight-mode worlds of ragged size (ship counts log-uniform in [1, max_ships], the ragged benchmark's shape;
+    world w drawn as flight_worlds(seed * 1_000_003 + w, 1, size)), concatenated with ids restarting in each world."""
+    r = random.Random(seed)
+    return FlightWorlds.concat([flight_worlds(seed * 1_000_003 + w, 1, ragged_ships(r, max_ships))
+                                for w in range(worlds)])
+
+
 def ragged_ships(r: random.Random, max_ships: int) -> int:
     """A world's ship count, log-uniform in [1, max_ships] (floor of 10^U(0, log10 max_ships))."""
     return max(1, min(max_ships, int(10.0 ** r.uniform(0.0, math.log10(max_ships)))))

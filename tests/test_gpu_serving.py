@@ -204,3 +204,19 @@ def test_open_loop_arrivals_are_served_and_timed():
         start = srv.results[ep.eid].start
         res["follow_ptr"] = np.where(res["follow_ptr"] >= 0, res["follow_ptr"] - start, -1)
         _same_states(res, _alone(ep), f"episode {ep.eid}")
+
+
+def test_a_best_fit_plan_ticks_as_the_plain_schedule():
+    """Tiles of any whole worlds (not only neighbours), packed best fit by ebb_plan_worlds."""
+    from exact_ballpark_b200 import tick_plain, tick_worlds
+    from exact_ballpark_b200.tiles import plan_best_fit
+    w = _ragged(8, 700, 128)
+    a, c = _loaded(w), _loaded(w)
+    plan = plan_best_fit(a.world, cap=256, block=256)
+    assert plan is not None and plan.tiles < len(w.rows) // 128
+    for _ in range(25):
+        tick_worlds(a, None, plan)
+        tick_plain(c)
+    torch.cuda.synchronize()
+    _same_states(_state(a), _state(c), "best fit after 25 ticks")
+    assert int(a._status.item()) == 0
