@@ -27,7 +27,9 @@ class _Collide(ctypes.Structure):
                     "pos", "vel", "old_pos", "old_vel", "goto", "last_g", "last_c", "mass", "radius", "max_vel",
                     "agility", "speed_fraction", "time_factor", "last_collision", "id", "mode", "level", "key", "mod",
                     "exists", "free", "massive", "junk", "cloaked", "hits", "hits_n", "imp_slot", "imp_n", "imp_s",
-                    "imp_closing")])
+                    "imp_closing")]
+                + [("S", ctypes.c_int64), ("B", ctypes.c_int64)]
+                + [(k, ctypes.c_void_p) for k in ("s_exists", "s_geo", "s_int", "s_keys")])
 
 
 def _normalized(v: np.ndarray) -> np.ndarray:
@@ -41,13 +43,14 @@ class OracleCollidePark:
     """W worlds of N ball slots on the CPU (module docstring): each world's balls in the first slots, ascending id."""
 
     def __init__(self, worlds: int, slots: int, friction: float = 1.0e6, tick_interval_ms: int = 1000, device="cpu",
-                 **_):
-        self.W, self.N = int(worlds), int(slots)
+                 statics: int = 0, **_):
+        self.W, self.N, self.S = int(worlds), int(slots), int(statics)
         self.dev = "cpu"
         self.friction, self.dt = float(friction), tick_interval_ms * 0.001
         self.current_time = 0
         W, N = self.W, self.N
-        self.C, self.I = max(1, 3 * (N - 1)), max(1, N - 1)
+        self.C, self.I = max(1, 3 * (N - 1)) + self.S, max(1, N - 1)
+        self._statics(1)
         z = lambda *s: np.zeros((W, N) + s)
         self.pos, self.vel, self.old_pos, self.old_vel = z(3), z(3), z(3), z(3)
         self.goto, self.last_g, self.last_c = z(3), z(3), z(3)
@@ -70,10 +73,21 @@ class OracleCollidePark:
         lib().oracle_collide_tick.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         lib().oracle_collide_filing.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
 
+    def _statics(self, boxes: int) -> None:
+        W, S = self.W, max(self.S, 1)
+        self.B = max(1, int(boxes))
+        self.s_exists = np.zeros((W, S), dtype=bool)
+        self.s_geo = np.zeros((W, S, 175))
+        self.s_int = np.zeros((W, S, 5), dtype=np.int64)
+        self.s_keys = np.zeros((W, S, self.B, 3), dtype=np.int64)
+
     def _state(self) -> _Collide:
         s = _Collide()
         s.W, s.N, s.C, s.I, s.k, s.dt = self.W, self.N, self.C, self.I, self.friction, self.dt
+        s.S, s.B = self.S, self.B
         for name, _ in _Collide._fields_[6:]:
+            if name in ("S", "B"):
+                continue
             a = getattr(self, name)
             if not a.flags["C_CONTIGUOUS"]:
                 a = np.ascontiguousarray(a)
@@ -81,12 +95,23 @@ class OracleCollidePark:
             setattr(s, name, a.ctypes.data)
         return s
 
-    def load(self, worlds: list) -> None:
+    def load(self, worlds: list, statics: list | None = None) -> None:
         """AddBall for each world's balls (vec_collide.py:550): ascending id in the slots, the float members rounded
-        to floats, AddBall's clamps, the decay factor, STOP, the first filing."""
+        to floats, AddBall's clamps, the decay factor, STOP, the first filing; then each world's static collidables
+        (vec_collide.py:1329; their records from exact_ballpark_b200.statics, which the tests pin to the reference's
+        own records)."""
         if len(worlds) != self.W:
             raise ValueError(f"{len(worlds)} worlds for a park of {self.W}")
-        self.__init__(self.W, self.N, self.friction, int(round(self.dt * 1000)))
+        self.__init__(self.W, self.N, self.friction, int(round(self.dt * 1000)), statics=self.S)
+        if statics is not None:
+            from exact_ballpark_b200.statics import static_record
+            recs = [[static_record(x) for x in items] for items in statics]
+            self._statics(max([len(r[2]) for rs in recs for r in rs], default=1))
+            for w, rs in enumerate(recs):
+                for j, (g, i, k) in enumerate(rs):
+                    self.s_geo[w, j], self.s_int[w, j], self.s_exists[w, j] = g, i, True
+                    for b, key in enumerate(k):
+                        self.s_keys[w, j, b] = key
         m_all = np.zeros((self.W, self.N))
         for w, balls in enumerate(worlds):
             if len(balls) > self.N:

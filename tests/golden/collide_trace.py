@@ -47,7 +47,10 @@ def _ball_json(b: dict) -> dict:
 
 
 def _unhex(x):
-    return float.fromhex(x) if isinstance(x, str) else x
+    """A float written by float.hex() back to its value; any other string (a static collidable's kind) as it is."""
+    if isinstance(x, str) and (x.lstrip("-").startswith("0x") or x in ("inf", "-inf", "nan")):
+        return float.fromhex(x)
+    return x
 
 
 def recording(park_cls):
@@ -58,15 +61,21 @@ def recording(park_cls):
         def __init__(self, worlds, slots, *args, **kw):
             super().__init__(worlds, slots, *args, **kw)
             self._depth = 0
-            self.trace = {"W": int(worlds), "N": int(slots), "friction": float(self.friction),
-                          "tick_interval_ms": int(round(self.dt * 1000)), "worlds": None, "events": [],
-                          "field_digests": []}
+            self.trace = {"W": int(worlds), "N": int(slots), "S": int(kw.get("statics", 0)),
+                          "friction": float(self.friction), "tick_interval_ms": int(round(self.dt * 1000)),
+                          "worlds": None, "statics": None, "events": [], "field_digests": []}
 
         def load(self, worlds, statics=None):
-            if statics is not None:
-                raise ValueError("static collidables are not recorded")
             self.trace["worlds"] = [[_ball_json(b) for b in w] for w in worlds]
-            super().load(worlds)
+            if statics is not None:
+                self.trace["statics"] = [[_ball_json(x) for x in w] for w in statics]
+                super().load(worlds, statics)
+                self.trace["filing"] = {"s_geo": self.s_geo.cpu().numpy().copy(),
+                                        "s_int": self.s_int.cpu().numpy().copy(),
+                                        "s_keys": self.s_keys.cpu().numpy().copy(),
+                                        "s_exists": self.s_exists.cpu().numpy().copy()}
+            else:
+                super().load(worlds)
 
         def evolve(self, *a, **k):
             if a or k:
@@ -102,11 +111,14 @@ def recording(park_cls):
 
 
 def save(traces: list, path: Path) -> None:
-    bodies = [{k: v for k, v in t.items() if k != "field_digests"} for t in traces]
+    bodies = [{k: v for k, v in t.items() if k not in ("field_digests", "filing")} for t in traces]
     with gzip.open(str(path) + ".json.gz", "wt") as f:
         json.dump({"groups": bodies}, f)
     arrays = {f"g{i}_field_digests": np.array(t["field_digests"], dtype=np.uint64).reshape(-1, len(FIELDS))
               for i, t in enumerate(traces)}
+    for i, t in enumerate(traces):
+        for k, v in (t.get("filing") or {}).items():
+            arrays[f"g{i}_{k}"] = v
     np.savez_compressed(str(path) + ".npz", **arrays)
 
 
@@ -118,13 +130,19 @@ def load(path: Path) -> list:
         g["worlds"] = [[{k: ([_unhex(c) for c in v] if isinstance(v, list) else _unhex(v)) for k, v in b.items()}
                         for b in w] for w in g["worlds"]]
         g["field_digests"] = z[f"g{i}_field_digests"]
+        g["statics"] = [[{k: ([_unhex(c) for c in v] if isinstance(v, list) else _unhex(v)) for k, v in x.items()}
+                         for x in w] for w in g["statics"]] if g.get("statics") else None
+        g["filing"] = {k: z[f"g{i}_{k}"] for k in ("s_geo", "s_int", "s_keys", "s_exists") if f"g{i}_{k}" in z.files}
     return groups
 
 
 def replay(g: dict, park, on_tick) -> None:
     """Drive `park` (already constructed with g's W, N and tick) through the trace: the load, then every event;
     on_tick(k, park) after tick k."""
-    park.load(g["worlds"])
+    if g.get("statics"):
+        park.load(g["worlds"], g["statics"])
+    else:
+        park.load(g["worlds"])
     dev = park.dev
     k = 0
     for ev in g["events"]:

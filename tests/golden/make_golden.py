@@ -248,6 +248,32 @@ def make_collide_traces(sample: int) -> None:
         ct.save([p.trace for p in parks], HERE / f"collide_cc{seed}")
         ticks = sum(len(p.trace["field_digests"]) for p in parks)
         print(f"  collide_cc{seed}: {len(cs)} scenarios in {len(parks)} parks, {ticks} ticks, {time.time() - t:.0f} s")
+    import exact_ballpark.vec_collide as VC
+    import static_cases as stc
+    for seed in (1, 2):
+        t = time.time()
+        cs = stc.cases(seed, n=200)
+        if sample:
+            want, _, _, undefined = stc.reference(cs)
+            got = stc.batched(cs, "cpu")
+            bad = stc.differences(want, {k: v for k, v in got.items() if k[0] not in undefined})
+            if bad:
+                raise RuntimeError(f"the batched CPU statics park differs from the scalar reference: {bad[:10]}")
+            print(f"  scalar check (statics seed {seed}, {len(cs)} scenarios): 0 differences")
+        parks = []
+        real = VC.VecCollidePark
+
+        def make_s(*a, **k):
+            parks.append(Rec(*a, **k))
+            return parks[-1]
+        VC.VecCollidePark = make_s
+        try:
+            stc.batched(cs, "cpu")
+        finally:
+            VC.VecCollidePark = real
+        ct.save([p.trace for p in parks], HERE / f"collide_st{seed}")
+        ticks = sum(len(p.trace["field_digests"]) for p in parks)
+        print(f"  collide_st{seed}: {len(cs)} scenarios in {len(parks)} parks, {ticks} ticks, {time.time() - t:.0f} s")
     t = time.time()
     w = collide_worlds(1, 64, ticks=100)
     park = Rec(64, 16, friction=1.0e6, tick_interval_ms=1000, device="cpu")

@@ -3,15 +3,19 @@ on the reference's batched collision park (tests/golden/collide_trace.py): the r
 (seed 1 development, seed 2 held out: approaching, glancing, overlapping and coincident balls, light balls, fixed
 spheres as walls and fields, several contacts in a tick, near misses, chains, fast balls, balls on partition box faces,
 space junk, cloaked and non-massive neighbours, racers with throttle and stop commands; ticks of 0.25 to 2 s, several
-frictions) and the collision benchmark's worlds (64 worlds of 4 ships, 4 free and 8 fixed spheres, 100 ticks). Every
-field's digest after every tick, bit for bit; a planted fault is caught."""
+frictions), its static_cases scenarios (capsules and oriented boxes: ships through, at and along them, grazing, inside,
+at rest beside, backing into them; faces, edges and corners of aligned, rotated, skewed and flat boxes; a box wider than
+a top box; fields and clusters with racers; several static collidables touched in one tick) and the collision
+benchmark's worlds (64 worlds of 4 ships, 4 free and 8 fixed spheres, 100 ticks). Every field's digest after every
+tick, bit for bit; a planted fault is caught. The static collidables' records (exact_ballpark_b200.statics) against the
+reference park's own records, double for double."""
 
 import numpy as np
 import pytest
 
 import collide_trace as ct
 
-TRACES = ("collide_cc1", "collide_cc2", "collide_w0")
+TRACES = ("collide_cc1", "collide_cc2", "collide_w0", "collide_st1", "collide_st2")
 
 
 def _replay(g, park, plant=None) -> list:
@@ -33,7 +37,8 @@ def test_the_oracle_replays_the_golden_collision_trace(name):
     groups = ct.load(ct.GOLDEN / name)
     failures = []
     for gi, g in enumerate(groups):
-        p = OracleCollidePark(g["W"], g["N"], friction=g["friction"], tick_interval_ms=g["tick_interval_ms"])
+        p = OracleCollidePark(g["W"], g["N"], friction=g["friction"], tick_interval_ms=g["tick_interval_ms"],
+                              statics=g.get("S", 0))
         bad = _replay(g, p)
         if bad:
             failures.append((gi, bad[0]))
@@ -54,3 +59,19 @@ def test_the_benchmark_worlds_collide_and_a_planted_fault_is_caught():
     p = OracleCollidePark(g["W"], g["N"], friction=g["friction"], tick_interval_ms=g["tick_interval_ms"])
     bad = _replay(g, p, plant=plant)
     assert bad and bad[0][0] == 10 and "vel" in bad[0][1]
+
+
+@pytest.mark.parametrize("name", ["collide_st1", "collide_st2"])
+def test_the_static_records_are_the_references(name):
+    from exact_ballpark_b200.statics import static_record
+    n = 0
+    for g in ct.load(ct.GOLDEN / name):
+        f = g["filing"]
+        for w, items in enumerate(g["statics"]):
+            for j, item in enumerate(items):
+                geo, ints, keys = static_record(item)
+                assert (np.asarray(geo).view(np.uint64) == f["s_geo"][w, j].view(np.uint64)).all()
+                assert list(ints) == f["s_int"][w, j].tolist()
+                assert [list(k) for k in keys] == f["s_keys"][w, j][:ints[4]].tolist()
+                n += 1
+    assert n > 250
