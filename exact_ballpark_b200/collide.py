@@ -1,4 +1,5 @@
-"""The collision park on a B200: a drop-in for exact_ballpark.vec_collide.VecCollidePark's gradient method on spheres.
+"""The collision park on a B200: a drop-in for exact_ballpark.vec_collide.VecCollidePark's gradient method (spheres free
+and fixed, and static collidables: capsules and oriented boxes).
 
 The public API is the reference park's (exact_ballpark/vec_collide.py:432-700, 990): the constructor (W worlds of N
 ball slots, friction, tick), `load(worlds)` (each world a list of AddBall's arguments), the commands goto_point,
@@ -11,9 +12,9 @@ every free ball's behaviour, Gradient for every free massive ball with its candi
 order, the commit and the re-filing. Nothing waits for the host and nothing is pruned on the host, so the tick can be
 captured in a CUDA graph; every contact a ball has is handled (no contact_slots overflow). There is no CPU tick.
 
-Not here (the constructor or the load refuses them): the iterative collision method, static collidables (capsules and
-oriented boxes), minis and force fields, global balls, the master's bubbles, the `rows` lever (every slot is a row),
-turning collisions off; balls filed at the partition grid's edge or wider than a top box (the reference refuses them).
+Not here (the constructor or the load refuses them): the iterative collision method, minis and force fields, global
+balls, the master's bubbles, the `rows` lever (every slot is a row), turning collisions off; balls filed at the
+partition grid's edge or wider than a top box and static collidables at its edge (the reference refuses them).
 """
 
 from __future__ import annotations
@@ -25,6 +26,7 @@ import numpy as np
 import torch
 
 from . import _native
+from .statics import G_SIZE, I_SIZE, static_record
 
 F64, I64, BOOL = torch.float64, torch.int64, torch.bool
 GOTO, STOP = 0, 2
@@ -38,7 +40,9 @@ class CollideState(ctypes.Structure):
                     "pos", "vel", "old_pos", "old_vel", "goto_pt", "last_g", "last_c", "mass", "radius", "max_vel",
                     "agility", "speed_fraction", "time_factor", "last_collision", "id", "mode", "level", "key", "mod",
                     "exists", "free_", "massive", "junk", "cloaked", "hits", "hits_n", "imp_slot", "imp_n", "imp_s",
-                    "imp_closing")])
+                    "imp_closing")]
+                + [("statics", ctypes.c_int64), ("boxes", ctypes.c_int64)]
+                + [(k, ctypes.c_void_p) for k in ("s_exists", "s_geo", "s_int", "s_keys")])
 
 
 _STATE_NAME = {"goto_pt": "goto", "free_": "free"}
@@ -74,19 +78,21 @@ class VecCollidePark:
             raise ValueError("the B200 collision park ticks on a CUDA device only (there is no CPU tick)")
         if dev.index is None:
             dev = torch.device("cuda", torch.cuda.current_device())
-        if iterative or not collisions or statics or minis or fields or global_balls:
-            raise ValueError("this park runs the gradient method on spheres: no iterative method, static "
-                             "collidables, minis, force fields or global balls, and collisions on")
+        if iterative or not collisions or minis or fields or global_balls:
+            raise ValueError("this park runs the gradient method: no iterative method, minis, force fields or global "
+                             "balls, and collisions on")
+        if not 0 <= int(statics) <= _native.COLLIDE_MAX_STATICS:
+            raise ValueError(f"statics: 0 to {_native.COLLIDE_MAX_STATICS} slots a world")
         if rows is not None and int(rows) != int(slots):
             raise ValueError("every slot is a row here (the rows lever is not taken)")
         if not 1 <= int(slots) <= _native.COLLIDE_MAX_SLOTS:
             raise ValueError(f"slots: 1 to {_native.COLLIDE_MAX_SLOTS}")
-        self.W, self.N, self.R, self.dev = int(worlds), int(slots), int(slots), dev
+        self.W, self.N, self.R, self.S, self.dev = int(worlds), int(slots), int(slots), int(statics), dev
         self.friction, self.dt = float(friction), tick_interval_ms * 0.001
         self.contact_slots, self.impact_slots = contact_slots, impact_slots     # accepted: nothing overflows here
         self.current_time = 0
         W, N = self.W, self.N
-        self.C, self.I = max(1, 3 * (N - 1)), max(1, N - 1)
+        self.C, self.I = max(1, 3 * (N - 1)) + self.S, max(1, N - 1)
         z = lambda *s: torch.zeros((W, N) + s, dtype=F64, device=dev)
         for k in _VEC:
             setattr(self, k, z(3))
@@ -107,6 +113,17 @@ class VecCollidePark:
         self.imp_closing = torch.zeros(W, N, self.I, dtype=F64, device=dev)
         self.imp_n = torch.zeros(W, N, dtype=I64, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._empty_statics(1)
+        self._state = None
+
+    def _empty_statics(self, boxes: int) -> None:
+        """The static collidable slots, none filled: records [W, S] (exact_ballpark_b200.statics) and box keys."""
+        W, S = (self.W, self.S) if self.S else (1, 1)       # a park without static slots holds one empty record
+        self.B = max(1, int(boxes))
+        self.s_exists = torch.zeros(W, S, dtype=BOOL, device=self.dev)
+        self.s_geo = torch.zeros(W, S, G_SIZE, dtype=F64, device=self.dev)
+        self.s_int = torch.zeros(W, S, I_SIZE, dtype=I64, device=self.dev)
+        self.s_keys = torch.zeros(W, S, self.B, 3, dtype=I64, device=self.dev)
         self._state = None
 
     def state(self) -> CollideState:
@@ -115,7 +132,10 @@ class VecCollidePark:
             s = CollideState()
             s.worlds, s.slots, s.hit_cap, s.impact_cap = self.W, self.N, self.C, self.I
             s.friction, s.dt = self.friction, self.dt
+            s.statics, s.boxes = self.S, self.B
             for name, _ in CollideState._fields_[6:]:
+                if name in ("statics", "boxes"):
+                    continue
                 t = getattr(self, _STATE_NAME.get(name, name))
                 if not t.is_contiguous():
                     raise RuntimeError(f"{name} is not contiguous")
@@ -127,11 +147,13 @@ class VecCollidePark:
         return torch.cuda.current_stream(self.dev).cuda_stream
 
     # ---- loading (vec_collide.py:550) ----
-    def load(self, worlds: list) -> None:
+    def load(self, worlds: list, statics: list | None = None) -> None:
         """Each world a list of balls (AddBall's arguments: id, mass, radius, max_vel, agility, speed_fraction, pos,
         vel, free, massive, and optionally junk and cloaked): the balls in ascending id in the world's first slots,
         AddBall's float members and clamps, every ball in STOP with its goto point at the origin; on the device the
-        decay factors and the first filing."""
+        decay factors and the first filing. `statics` (a park made with static slots): each world's capsules and
+        oriented boxes as AddCapsule and AddOrientedBox take them ({"kind": "capsule", "id", "parent", "a", "b",
+        "radius"} or {"kind": "box", "id", "parent", "corner", "lx", "ly", "lz"}), their records made on the host."""
         if len(worlds) != self.W:
             raise ValueError(f"{len(worlds)} worlds for a park of {self.W}")
         W, N = self.W, self.N
@@ -190,12 +212,45 @@ class VecCollidePark:
         self.imp_closing.zero_()
         self.imp_n.zero_()
         self.status.zero_()
+        self._load_statics(statics)
         with torch.cuda.device(self.dev):
             rc = _native.lib().ebb_collide_load(ctypes.byref(self.state()), self.status.data_ptr(), self._stream())
         _native.check(rc, "ebb_collide_load")
         if int(self.status.item()) & 1:
             raise ValueError("a ball at the partition's edge or wider than a top box: not in this module")
         self.current_time = 0
+
+    def _load_statics(self, statics: list | None) -> None:
+        """The worlds' static collidables into the static slots (vec_collide.py:1329): records and filings made once
+        on the host (exact_ballpark_b200.statics.static_record); refused beyond the park's slots."""
+        if statics is None:
+            self._empty_statics(1)
+            return
+        if len(statics) != self.W:
+            raise ValueError(f"{len(statics)} worlds of static collidables for a park of {self.W}")
+        recs = []
+        for w, items in enumerate(statics):
+            if len(items) > self.S:
+                raise ValueError(f"world {w} has {len(items)} static collidables for the park's {self.S} slots")
+            ids = [int(x["id"]) for x in items]
+            if len(set(ids)) != len(ids):
+                raise ValueError(f"world {w}: static collidable ids must be distinct")
+            recs.append([static_record(x) for x in items])
+        self._empty_statics(max([len(r[2]) for rs in recs for r in rs], default=1))
+        W, S = self.s_exists.shape
+        geo = np.zeros((W, S, G_SIZE))
+        ints = np.zeros((W, S, I_SIZE), dtype=np.int64)
+        keys = np.zeros((W, S, self.B, 3), dtype=np.int64)
+        exists = np.zeros((W, S), dtype=bool)
+        for w, rs in enumerate(recs):
+            for j, (g, i, k) in enumerate(rs):
+                geo[w, j], ints[w, j], exists[w, j] = g, i, True
+                if k:
+                    keys[w, j, :len(k)] = k
+        self.s_geo.copy_(torch.from_numpy(geo))
+        self.s_int.copy_(torch.from_numpy(ints))
+        self.s_keys.copy_(torch.from_numpy(keys))
+        self.s_exists.copy_(torch.from_numpy(exists))
 
     # ---- commands (vec_collide.py:669-697) ----
     def goto_point(self, mask: torch.Tensor, point: torch.Tensor) -> None:

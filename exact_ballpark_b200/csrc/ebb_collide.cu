@@ -320,6 +320,359 @@ __device__ __forceinline__ bool file_slot(const EbbCollideState& s, int64_t i) {
     return bad;
 }
 
+
+// ================================================================== static collidables (COL-712)
+// Capsule::CollideWithBall / OrientedBox::CollideWithBall and ReactToCollision (Capsule.cpp, OrientedBox.cpp,
+// BoxShape.cpp; vec_collide.py:1435-1737): a responder against a capsule or an oriented box from the tick's start, its
+// straight path predicted with mLastG. A record is 175 doubles laid out as the reference's park keeps it.
+constexpr int G_A = 0, G_B = 3, G_AB = 6, G_RAD = 9, G_CENTER = 10, G_LO = 13, G_HI = 16, G_AXES = 19, G_UNIT = 28;
+constexpr int G_HALF = 37, G_LENSQ = 40, G_CORNERS = 43, G_RECT = 67, G_RNORM = 139, G_TNORM = 157, G_SIZE = 175;
+constexpr int I_KIND = 0, I_ID = 1, I_PARENT = 2, I_LEVEL = 3, I_NBOX = 4, I_SIZE = 5;
+constexpr double DBL_MAX_ = 1.7976931348623157e308, STATIC_TINY = 1e-10, STATIC_FLOOR = 1e-5, EJECT_MARGIN = 1.0;
+__constant__ int CONNECTED_SIDES[8][3] = {{1, 2, 5}, {1, 3, 5}, {1, 2, 4}, {0, 2, 5}, {1, 3, 4}, {0, 2, 4},
+                                          {0, 3, 5}, {0, 3, 4}};    // BoxShape.cpp:189, a corner's three sides
+__constant__ int SIDE_MAPPING[3][2] = {{2, 3}, {5, 4}, {1, 0}};     // BoxShape.cpp:137, an axis's two sides
+
+__device__ __forceinline__ V gv(const double* g, int at) { return V{g[at], g[at + 1], g[at + 2]}; }
+__device__ __forceinline__ V vcross(V u, V v) {
+    return V{dsub(dmul(u.y, v.z), dmul(u.z, v.y)), dsub(dmul(u.z, v.x), dmul(u.x, v.z)),
+             dsub(dmul(u.x, v.y), dmul(u.y, v.x))};
+}
+
+// Capsule::HandleCollisionNonIteratively: the time of impact (-1: none), the normal before normalising, and whether
+// the end velocity is parallel to the axis (the caps alone, the reaction from the tick's end)
+__device__ __forceinline__ double capsule_contact(V p0, V p1, V vp1, double brad, const double* g, V* nrm,
+                                                  bool* parallel) {
+    const V ca = gv(g, G_A), cb = gv(g, G_B), ab = gv(g, G_AB);
+    const double rad = dadd(brad, g[G_RAD]);
+    const V ao = vsub(p0, ca);
+    const double abab = vdot(ab, ab);
+    const double m = ddiv(vdot(ab, vp1), abab), n = ddiv(vdot(ab, ao), abab);
+    const V q = vsub(vp1, vmul(ab, m)), r = vsub(ao, vmul(ab, n));
+    const double a = vdot(q, q), bq = dmul(2.0, vdot(q, r)), rad_sq = dmul(rad, rad);
+    const double cq = dsub(vdot(r, r), rad_sq);
+    const double sa = collide_two_spheres(p0, p1, ca, ca, rad), sb = collide_two_spheres(p0, p1, cb, cb, rad);
+    const V na = vsub(p0, ca), nb = vsub(p0, cb), zero = V{0.0, 0.0, 0.0};
+    if (a == 0.0) {
+        *parallel = true;
+        const bool take_a = sa != -1.0;
+        double toi = take_a ? sa : -1.0;
+        const bool take_b = sb != -1.0 && (toi == -1.0 || sb < toi);
+        if (take_b) toi = sb;
+        *nrm = take_b ? nb : (take_a ? na : zero);
+        return toi;
+    }
+    *parallel = false;
+    const double det = dsub(dmul(bq, bq), dmul(dmul(4.0, a), cq));
+    if (det < 0.0) {
+        *nrm = zero;
+        return -1.0;
+    }
+    const double root = dsqrt(det), nbq = dneg(bq);
+    const double s1 = ddiv(dmul(dadd(nbq, root), 0.5), a), s2 = ddiv(dmul(dsub(nbq, root), 0.5), a);
+    double sv = (s1 >= 0.0 && s1 <= 1.0) ? s1 : -1.0;
+    const bool second = s2 >= 0.0 && s2 <= 1.0 && s2 < s1;
+    if (second) sv = s2;
+    const double t = ddiv(vdot(ao, ab), abab);
+    const V dist = vsub(p0, vadd(ca, vmul(ab, t)));
+    if (!second && sv == -1.0 && t >= 0.0 && t <= 1.0 && vdot(dist, dist) < rad_sq) {
+        *nrm = dist;
+        return 0.0;
+    }
+    const V mid_n = vsub(ao, vmul(ab, t));
+    const double mid_t = vdot(mid_n, mid_n) < rad_sq ? 0.0 : sv;
+    double toi = -1.0;
+    V out = zero;
+    const double tk[2] = {dadd(dmul(s1, m), n), dadd(dmul(s2, m), n)};
+    const V far[2] = {p0, p1};
+    for (int k = 0; k < 2; ++k) {
+        const bool low = tk[k] < 0.0, high = tk[k] > 1.0;
+        if (low && sa != -1.0 && (toi == -1.0 || sa < toi)) {
+            toi = sa;
+            out = na;
+        } else if (!low && high && sb != -1.0 && (toi == -1.0 || sb < toi)) {
+            toi = sb;
+            out = vsub(far[k], cb);
+        } else if (!low && !high && sv != -1.0 && (toi == -1.0 || sv < toi)) {
+            toi = mid_t;
+            out = mid_n;
+        }
+    }
+    *nrm = out;
+    return toi;
+}
+
+// Triangle::ClosestPoint, its regions in order
+__device__ __forceinline__ V triangle_closest(V A, V B, V C, V P) {
+    const V ab = vsub(B, A), ac = vsub(C, A), ap = vsub(P, A);
+    const double d1 = vdot(ab, ap), d2 = vdot(ac, ap);
+    if (d1 <= 0.0 && d2 <= 0.0) return A;
+    const V bp = vsub(P, B);
+    const double d3 = vdot(ab, bp), d4 = vdot(ac, bp);
+    if (d3 >= 0.0 && d4 <= d3) return B;
+    const double vc = dsub(dmul(d1, d4), dmul(d3, d2));
+    if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) return vadd(A, vmul(ab, ddiv(d1, dsub(d1, d3))));
+    const V cp = vsub(P, C);
+    const double d5 = vdot(ab, cp), d6 = vdot(ac, cp);
+    if (d6 > 0.0 && d5 <= d6) return C;
+    const double vb = dsub(dmul(d5, d2), dmul(d1, d6));
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) return vadd(A, vmul(ac, ddiv(d2, dsub(d2, d6))));
+    const double va = dsub(dmul(d3, d6), dmul(d5, d4));
+    const double e43 = dsub(d4, d3), e56 = dsub(d5, d6);
+    if (va <= 0.0 && e43 >= 0.0 && e56 >= 0.0) return vadd(B, vmul(vsub(C, B), ddiv(e43, dadd(e43, e56))));
+    const double denom = ddiv(1.0, dadd(dadd(va, vb), vc));
+    return vadd(vadd(A, vmul(ab, dmul(vb, denom))), vmul(ac, dmul(vc, denom)));
+}
+
+// RectangleShape::CollideWithSphere on one side: whether it is struck, the normal, the time
+__device__ __forceinline__ bool rect_contact(V p, double radius, V vel, int side, const double* g, V* nrm, double* tt) {
+    const double* rc = g + G_RECT + 12 * side;
+    const V a = gv(rc, 0), b = gv(rc, 3), c = gv(rc, 6), d = gv(rc, 9);
+    const V m = vcross(vsub(c, p), vsub(a, p));
+    const bool abc = vdot(vel, m) <= 0.0;
+    const V TA = a, TB = abc ? b : c, TC = abc ? c : d;
+    const V n = abc ? gv(g, G_RNORM + 3 * side) : gv(g, G_TNORM + 3 * side);
+    const V p0 = vsub(p, vmul(n, radius));
+    const V p0p1 = vsub(vadd(p0, vel), p0);
+    const double ndab = vdot(n, p0p1);
+    const double t = ddiv(dsub(vdot(TA, n), vdot(n, p0)), ndab);
+    const bool plane = ndab != 0.0 && t >= 0.0 && t <= 1.0;
+    const V point = vadd(p0, vmul(p0p1, t));
+    const V v0 = vsub(TC, TA), v1 = vsub(TB, TA), v2 = vsub(point, TA);
+    const double dot00 = vdot(v0, v0), dot01 = vdot(v0, v1), dot02 = vdot(v0, v2), dot11 = vdot(v1, v1),
+                 dot12 = vdot(v1, v2);
+    const double inv = ddiv(1.0, dsub(dmul(dot00, dot11), dmul(dot01, dot01)));
+    const double u = dmul(dsub(dmul(dot11, dot02), dmul(dot01, dot12)), inv);
+    const double v = dmul(dsub(dmul(dot00, dot12), dmul(dot01, dot02)), inv);
+    const bool within = u >= 0.0 && v >= 0.0 && dadd(u, v) < 1.0;
+    const V q0 = triangle_closest(TA, TB, TC, point);
+    const V direction = vsub(vsub(q0, vel), q0);
+    const V nd = vnorm(direction);
+    const V mm = vsub(q0, p);
+    const double bb = vdot(mm, nd), cc = dsub(vdot(mm, mm), dmul(radius, radius));
+    const double disc = dsub(dmul(bb, bb), cc);
+    const double tq = dsub(dneg(bb), dsqrt(disc < 0.0 ? 0.0 : disc));
+    const double ts = tq < 0.0 ? 0.0 : ddiv(tq, dsqrt(vdot(direction, direction)));
+    const bool swept = !(cc > 0.0 && bb > 0.0) && !(disc < 0.0) && !(ts > 1.0);
+    *nrm = within ? n : vnorm(vsub(p, vadd(q0, vmul(direction, ts))));
+    *tt = within ? t : ts;
+    return plane && (within || swept);
+}
+
+__device__ __forceinline__ double fmax5(double x) { return x < STATIC_FLOOR ? STATIC_FLOOR : x; }
+
+// OrientedBox::CollideWithBall with BoxShape::CollideWithSphere: the time of impact (-1: none) and the normal
+__device__ __forceinline__ double box_contact(V p0, V p1, double brad, const double* g, V* nrm) {
+    const double r = brad;
+    const double p0a[3] = {p0.x, p0.y, p0.z}, p1a[3] = {p1.x, p1.y, p1.z};
+    bool excl = false;                                                // AABB::CanExclude
+    for (int q = 0; q < 3; ++q) {
+        const double lo = g[G_LO + q], hi = g[G_HI + q];
+        excl = excl || (dsub(p0a[q], r) > hi && dsub(p1a[q], r) > hi) || (dadd(p0a[q], r) < lo && dadd(p1a[q], r) < lo);
+    }
+    const V vel = vsub(p1, p0), p = p0;
+    const double radius = brad;
+    V dd = vsub(gv(g, G_CORNERS), p);                                 // ClosestCorner: the first nearest
+    double min_d = vdot(dd, dd);
+    int closest = 0;
+    for (int i = 1; i < 8; ++i) {
+        dd = vsub(gv(g, G_CORNERS + 3 * i), p);
+        const double di = vdot(dd, dd);
+        if (di < min_d) {
+            min_d = di;
+            closest = i;
+        }
+    }
+    bool alive = true;
+    double shortest = -1.0;
+    int half = 0;
+    for (int i = 0; i < 3; ++i) {
+        const int side = CONNECTED_SIDES[closest][i];
+        const V n_s = gv(g, G_RNORM + 3 * side);
+        const V point = vsub(p, vmul(n_s, radius));
+        const double hs = vdot(n_s, vsub(gv(g, G_RECT + 12 * side), point));
+        const bool ok = hs >= 0.0;
+        if (alive && ok && (hs < shortest || shortest == -1.0)) {
+            shortest = hs;
+            half = side;
+        }
+        alive = alive && ok;
+    }
+    V q = gv(g, G_CENTER);                                            // BoxShape::ClosestPoint
+    const V d = vsub(p, q);
+    for (int i = 0; i < 3; ++i) {
+        const V u = gv(g, G_UNIT + 3 * i);
+        const double hl = g[G_HALF + i];
+        double dist = vdot(d, u);
+        dist = dist > hl ? hl : (dist < dneg(hl) ? dneg(hl) : dist);
+        q = vadd(q, vmul(u, dist));
+    }
+    const V normal = vsub(p, q);
+    const double n_len = dsqrt(vdot(normal, normal)), speed = dsqrt(vdot(vel, vel));
+    const bool inside = alive && n_len < radius;
+    V n_in = V{0.0, 0.0, 0.0};
+    if (inside) {
+        if (n_len < STATIC_TINY) {
+            const V n_half = gv(g, G_RNORM + 3 * half);
+            if (speed < STATIC_TINY) {
+                n_in = vmul(n_half, fmax5(shortest));
+            } else {
+                const V o = vsub(p, gv(g, G_CENTER));                 // BoxShape::RayIntersect, the slabs
+                double tmin[3], tmax[3];
+                int rev[3];
+                for (int i = 0; i < 3; ++i) {
+                    const V arm = gv(g, G_AXES + 3 * i);
+                    const double als = g[G_LENSQ + i], a_o = vdot(arm, o), a_r = vdot(arm, vel);
+                    const bool neg = a_r < 0.0, pos = a_r > 0.0;
+                    tmin[i] = neg ? ddiv(dsub(dmul(0.5, als), a_o), a_r)
+                                  : (pos ? ddiv(dsub(dmul(-0.5, als), a_o), a_r) : dneg(DBL_MAX_));
+                    tmax[i] = neg ? ddiv(dsub(dmul(-0.5, als), a_o), a_r)
+                                  : (pos ? ddiv(dsub(dmul(0.5, als), a_o), a_r) : DBL_MAX_);
+                    rev[i] = neg ? 1 : 0;
+                }
+                int i_min = 0;
+                double v_min = tmin[0], v_max = tmax[0];
+                for (int i = 1; i < 3; ++i) {
+                    if (v_min < tmin[i]) {
+                        i_min = i;
+                        v_min = tmin[i];
+                    }
+                    if (tmax[i] < v_max) v_max = tmax[i];
+                }
+                if (v_min < v_max) {
+                    const int rv = rev[i_min];
+                    n_in = dabs(v_min) < dabs(v_max)
+                               ? vmul(gv(g, G_RNORM + 3 * SIDE_MAPPING[i_min][rv]), fmax5(dmul(dabs(v_min), speed)))
+                               : vmul(gv(g, G_RNORM + 3 * SIDE_MAPPING[i_min][1 - rv]), fmax5(dmul(dabs(v_max), speed)));
+                } else {
+                    n_in = vmul(n_half, shortest);
+                }
+            }
+        } else {
+            n_in = vmul(vnorm(normal), dabs(dsub(radius, n_len)));
+        }
+    }
+    bool hit = false;
+    V out = V{0.0, 0.0, 0.0};
+    double time = 0.0;
+    for (int i = 0; i < 3; ++i) {                                     // else the sides' triangles, the first struck
+        V n_i;
+        double t_i;
+        const bool h = rect_contact(p, radius, vel, CONNECTED_SIDES[closest][i], g, &n_i, &t_i);
+        if (!hit && h) {
+            out = n_i;
+            time = t_i;
+        }
+        hit = hit || h;
+    }
+    hit = !excl && (inside || hit);
+    if (inside) {
+        out = n_in;
+        time = 0.0;
+    }
+    *nrm = out;
+    return hit ? time : -1.0;
+}
+
+// The position of a static collidable's first box in responder ib's walk (its boxes all at its one level), as the
+// balls' key: the ball's box (by key) it relates to first, the part (ancestor, below, the box itself) and the
+// ancestor's distance or the box's post-order code
+__device__ __forceinline__ int64_t static_order_key(const EbbCollideState& s, int64_t ib, const int64_t* ints,
+                                                    const int64_t* keys) {
+    const int64_t Lb = s.level[ib], Ln = ints[I_LEVEL];
+    int64_t cb[3], lo_b[3], hi_b[3];
+    for (int q = 0; q < 3; ++q) {
+        const int64_t kb = s.key[3 * ib + q], mb = s.mod[3 * ib + q];
+        cb[q] = 1 + (mb != 0);
+        lo_b[q] = kb + (mb < 0 ? mb : 0);
+        hi_b[q] = kb + (mb > 0 ? mb : 0);
+    }
+    int64_t span = 1;
+    for (int l = 0; l < NUM_LEVELS - 1; ++l) span *= CODE_BASE;
+    const int64_t s_up = Lb > Ln ? 2 * (Lb - Ln) : 0, s_dn = Ln > Lb ? 2 * (Ln - Lb) : 0;
+    int64_t best = NOT_A_CANDIDATE;
+    for (int64_t bx = 0; bx < ints[I_NBOX]; ++bx) {
+        const int64_t* Kn = keys + 3 * bx;
+        int64_t code = 0, power = span;
+        for (int lvl = 1; lvl < NUM_LEVELS; ++lvl) {
+            power /= CODE_BASE;
+            const int64_t shift = 2 * (Ln - lvl) > 0 ? 2 * (Ln - lvl) : 0;
+            int64_t digit = ((Kn[0] >> shift) & 3) * 16 + ((Kn[1] >> shift) & 3) * 4 + ((Kn[2] >> shift) & 3);
+            if (Ln < lvl) digit = CODE_BASE - 1;
+            if (Lb >= lvl) digit = 0;
+            code += digit * power;
+        }
+        for (int c = 0; c < 8; ++c) {
+            const int64_t bit[3] = {(c >> 2) & 1, (c >> 1) & 1, c & 1};
+            bool valid = true, up = true, same = true, down = true;
+            for (int q = 0; q < 3; ++q) {
+                if (bit[q] != 0 && cb[q] != 2) valid = false;
+                const int64_t box = bit[q] ? hi_b[q] : lo_b[q];
+                if ((box >> s_up) != Kn[q]) up = false;
+                if (box != Kn[q]) same = false;
+                if (box != (Kn[q] >> s_dn)) down = false;
+            }
+            if (!valid) continue;
+            const int64_t seg = (bit[0] * cb[1] + bit[1]) * cb[2] + bit[2];
+            int64_t k = NOT_A_CANDIDATE;
+            if (Ln < Lb) {
+                if (up) k = (seg * 3) * span + (Lb - Ln);
+            } else if (Ln == Lb) {
+                if (same) k = (seg * 3 + 2) * span;
+            } else if (down) {
+                k = (seg * 3 + 1) * span + code;
+            }
+            if (k < best) best = k;
+        }
+    }
+    return best;
+}
+
+// CollideWithBall then ReactToCollision (Capsule.cpp:365-437, OrientedBox.cpp:44-106) of responder ib with one static
+// collidable: whether the reaction is called (not for no contact, nor for a capsule when mLastG points out of it at an
+// impact within the tick), its time and 0.85 of its acceleration (the reflection off it, or the ejection by the
+// overlap plus a metre)
+__device__ __forceinline__ bool static_values(const EbbCollideState& s, int64_t ib, V pe, V ve, const double* g,
+                                              int64_t kind, double* toi_out, V* lc) {
+    const double k = s.friction, dt = s.dt;
+    const double m1 = dmul(s.mass[ib], s.agility[ib]), tf = s.time_factor[ib], brad = s.radius[ib];
+    const V p0 = ldv(s.pos, ib), v0 = ldv(s.vel, ib), gg = ldv(s.last_g, ib);
+    const bool cap = kind == 0;
+    V normal;
+    bool parallel = false;
+    const double toi = cap ? capsule_contact(p0, pe, ve, brad, g, &normal, &parallel) : box_contact(p0, pe, brad, g, &normal);
+    if (toi == -1.0) return false;
+    const double cl = dsqrt(vdot(normal, normal));
+    const V nn = vnorm(normal);
+    const double nc = vdot(gg, nn);
+    if (cap && toi > 0.0 && nc > 0.0) return false;
+    V a;
+    if (toi > 0.0) {
+        const bool end = cap && parallel;
+        V pos = end ? pe : p0, vel = end ? ve : v0;
+        integrate(pos, vel, gg, m1, k, tf, dmul(toi, dt), dt);
+        V vb = vsub(vel, vmul(nn, dmul(2.0, vdot(vel, nn))));
+        integrate(pos, vb, gg, m1, k, tf, dmul(dsub(1.0, toi), dt), dt);
+        const double ga[3] = {gg.x, gg.y, gg.z}, va[3] = {v0.x, v0.y, v0.z}, wa[3] = {vb.x, vb.y, vb.z};
+        const double inv_m = ddiv(1.0, m1), inv_t = ddiv(1.0, dsub(tf, 1.0));
+        double rr[3];
+        for (int q = 0; q < 3; ++q) {
+            const double x = dadd(dsub(dadd(dmul(ga[q], dneg(m1)), dmul(ga[q], dmul(tf, m1))), dmul(dmul(va[q], tf), k)),
+                                  dmul(wa[q], k));
+            rr[q] = dmul(dmul(dneg(x), inv_m), inv_t);
+        }
+        a = V{rr[0], rr[1], rr[2]};
+    } else {
+        const double dist = cap ? dadd(dsub(dadd(g[G_RAD], brad), cl), EJECT_MARGIN) : dadd(cl, EJECT_MARGIN);
+        const double tmp = ddiv(1.0, dadd(m1, dmul(dt, k)));
+        const double c = ddiv(dist, dmul(dmul(dt, tmp), m1));
+        a = vsub(vmul(vsub(vmul(nn, c), v0), ddiv(1.0, dt)), vmul(nn, nc));
+    }
+    *toi_out = toi;
+    *lc = vmul(a, RESPONSE_SCALE);
+    return true;
+}
+
 constexpr int MAX_SLOTS = EBB_COLLIDE_MAX_SLOTS;
 
 // Threads a block (whole worlds of N slots each) and resident blocks a multiprocessor is asked to fit (the register
@@ -411,6 +764,46 @@ __global__ void __launch_bounds__(EBB_COLLIDE_THREADS, EBB_COLLIDE_MIN_BLOCKS) t
             const int o = oslot[q];
             potential<0>(W, j, o, pb, ldv(s.pos, base + o), acc);
         }
+        if (s.statics > 0) {                                          // then the static collidables (COL-712)
+            V pe = pb, ve = ldv(s.vel, i);
+            integrate(pe, ve, ldv(s.last_g, i), dmul(s.mass[i], s.agility[i]), k, s.time_factor[i], dt, dt);
+            int nst = 0;                                                  // the reacting ones in the walk's order:
+            for (int q = 0; q < s.statics && q < MAX_SLOTS; ++q) {        // first box, parent id, id, slot
+                const int64_t at = w * s.statics + q;
+                if (!s.s_exists[at]) continue;
+                const int64_t* ints = s.s_int + at * I_SIZE;
+                const int64_t key = static_order_key(s, i, ints, s.s_keys + at * s.boxes * 3);
+                if (key >= NOT_A_CANDIDATE) continue;
+                double toi;
+                V lc;
+                if (!static_values(s, i, pe, ve, s.s_geo + at * G_SIZE, ints[I_KIND], &toi, &lc)) continue;
+                int pos = nst++;
+                while (pos > 0) {
+                    const int64_t* pi = s.s_int + (w * s.statics + oslot[pos - 1]) * I_SIZE;
+                    const bool after = okey[pos - 1] > key ||
+                                       (okey[pos - 1] == key && (pi[I_PARENT] > ints[I_PARENT] ||
+                                                                 (pi[I_PARENT] == ints[I_PARENT] && pi[I_ID] > ints[I_ID])));
+                    if (!after) break;
+                    okey[pos] = okey[pos - 1];
+                    oslot[pos] = oslot[pos - 1];
+                    --pos;
+                }
+                okey[pos] = key;
+                oslot[pos] = (int8_t)q;
+            }
+            for (int q = 0; q < nst; ++q) {
+                const int64_t at = w * s.statics + oslot[q];
+                const int64_t* ints = s.s_int + at * I_SIZE;
+                double toi;
+                V lc;
+                static_values(s, i, pe, ve, s.s_geo + at * G_SIZE, ints[I_KIND], &toi, &lc);
+                const bool eq = toi == acc.last_collision;              // the stronger at a tie, no later-impact test
+                if (!eq || vdot(lc, lc) > vdot(acc.last_c, acc.last_c)) acc.last_c = lc;
+                if (!eq) acc.last_collision = toi;
+                s.hits[i * s.hit_cap + (acc.hits_n < s.hit_cap ? acc.hits_n : s.hit_cap - 1)] = ints[I_ID];
+                ++acc.hits_n;
+            }
+        }
         stv(s.last_c, i, acc.last_c);
         s.last_collision[i] = acc.last_collision;
         s.hits_n[i] = acc.hits_n;
@@ -450,8 +843,11 @@ int launched() {
     return e == cudaSuccess ? 0 : (int)e;
 }
 bool shape_ok(const EbbCollideState* s) {
-    return s != nullptr && s->worlds >= 0 && s->slots >= 1 && s->slots <= EBB_COLLIDE_MAX_SLOTS &&
-           s->hit_cap == (s->slots > 1 ? 3 * (s->slots - 1) : 1) && s->impact_cap == (s->slots > 1 ? s->slots - 1 : 1);
+    return s != nullptr && s->worlds >= 0 && s->slots >= 1 && s->slots <= EBB_COLLIDE_MAX_SLOTS && s->statics >= 0 &&
+           s->statics <= EBB_COLLIDE_MAX_STATICS && s->boxes >= 1 &&
+           s->hit_cap == (s->slots > 1 ? 3 * (s->slots - 1) : 1) + s->statics &&
+           s->impact_cap == (s->slots > 1 ? s->slots - 1 : 1) &&
+           (s->statics == 0 || (s->s_exists && s->s_geo && s->s_int && s->s_keys));
 }
 }  // namespace
 

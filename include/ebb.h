@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define EBB_ABI_VERSION 1
+#define EBB_ABI_VERSION 2
 #define EBB_EINVAL (-1)
 #define EBB_ETOOBIG (-2)
 
@@ -50,6 +50,7 @@ typedef struct EbbFlightState {
  * [W N][hit_cap] (hit_cap = 3 (N - 1), at least 1), the impact record [W N][impact_cap] (impact_cap = N - 1, at least
  * 1). Field for field the state of exact_ballpark.vec_collide.VecCollidePark (vec_collide.py:470-512). */
 #define EBB_COLLIDE_MAX_SLOTS 64
+#define EBB_COLLIDE_MAX_STATICS 64
 typedef struct EbbCollideState {
     int64_t worlds, slots, hit_cap, impact_cap;
     double friction, dt;
@@ -60,6 +61,13 @@ typedef struct EbbCollideState {
     int64_t *hits, *hits_n;                                                            /* [W N][hit_cap], [W N] */
     int64_t *imp_slot, *imp_n;                                                         /* [W N][impact_cap], [W N] */
     double *imp_s, *imp_closing;                                                       /* [W N][impact_cap] */
+    /* static collidables (capsules, oriented boxes): S slots a world (0: none; at most EBB_COLLIDE_MAX_STATICS), each
+     * a record of 175 doubles and 5 integers (kind, id, parent id, level, boxes) and up to B box keys, made once at the
+     * load (exact_ballpark_b200.statics; vec_collide.py:261); hit_cap then counts S more entries */
+    int64_t statics, boxes;
+    uint8_t* s_exists;                                                                 /* [W S] */
+    double* s_geo;                                                                     /* [W S][175] */
+    int64_t *s_int, *s_keys;                                                           /* [W S][5], [W S][B][3] */
 } EbbCollideState;
 
 /* The ABI version (EBB_ABI_VERSION). Replaces xbpm_abi / xbpo_abi (exact_ballpark/vec_modes_cuda.cu:750,
@@ -134,7 +142,8 @@ int ebb_flight_move(const EbbFlightState* dst, const EbbFlightState* src, const 
 
 /* One tick of the collision park in place (TIME-706/707): the free balls' behaviours (GOTO's thrust, STOP's
  * damping), Gradient for every free massive ball (Potential with each collision candidate in Partition::
- * GetNearbyBalls' order, the overlap recursion, the impact and overlap responses, the later impact kept), the commit and
+ * GetNearbyBalls' order, the overlap recursion, the impact and overlap responses, the later impact kept; then its
+ * static collidables in the walk's order, CollideWithBall and ReactToCollision, COL-712), the commit and
  * the re-filing of the balls that moved. `active` [W] (nullable): only those worlds tick. One launch, one thread block
  * a group of whole worlds (N <= EBB_COLLIDE_MAX_SLOTS). status[0] bit 2: a re-filing at the grid's edge. Replaces
  * VecCollidePark.evolve's gradient path (exact_ballpark/vec_collide.py:990) and its kernels xbpc_tick / xbpc_gradient

@@ -1,7 +1,8 @@
 """The collision park on the GPU, through the C ABI (ebb_collide_load, ebb_collide_tick):
 
-- against the golden traces recorded on the reference's collision park (its collide_cases scenarios, seeds 1 and 2,
-  and the collision benchmark's worlds): every field's digest after every tick, bit for bit;
+- against the golden traces recorded on the reference's collision park (its collide_cases scenarios, seeds 1 and 2, its
+  static_cases scenarios with capsules and oriented boxes, seeds 1 and 2, and the collision benchmark's worlds): every
+  field's digest after every tick, bit for bit;
 - against the CPU oracle beyond the fixtures (the benchmark's worlds at other seeds, 1024 worlds, 150 ticks with the
   ships re-aimed): every field after every 25th tick;
 - a CUDA graph's replays against eager ticks, and inactive worlds (evolve(active)) keeping their state.
@@ -17,13 +18,14 @@ from golden_util import bit_equal
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 
-@pytest.mark.parametrize("name", ["collide_cc1", "collide_cc2", "collide_w0"])
+@pytest.mark.parametrize("name", ["collide_cc1", "collide_cc2", "collide_w0", "collide_st1", "collide_st2"])
 def test_the_gpu_collision_park_replays_the_golden_trace(name):
     from exact_ballpark_b200 import VecCollidePark
     groups = ct.load(ct.GOLDEN / name)
     failures = []
     for gi, g in enumerate(groups):
-        p = VecCollidePark(g["W"], g["N"], friction=g["friction"], tick_interval_ms=g["tick_interval_ms"])
+        p = VecCollidePark(g["W"], g["N"], friction=g["friction"], tick_interval_ms=g["tick_interval_ms"],
+                           statics=g.get("S", 0))
         bad = []
 
         def on_tick(k, park):
