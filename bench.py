@@ -270,7 +270,7 @@ def ragged_runs(args, dev) -> dict:
     return out
 
 
-def collide_runs(args, dev) -> dict:
+def collide_runs(args, dev, statics: bool = False) -> dict:
     """The collision park (exact_ballpark_b200.collide, the gradient method on spheres) at the collision
     benchmark's shape: --collide-worlds worlds of 4 ships, 4 free spheres and 8 fixed spheres
     (workloads.collide_worlds: +-20 km, radii log-uniform 10 m - 5 km, ships GOTO at spheres, re-aimed every 25 ticks
@@ -280,12 +280,17 @@ def collide_runs(args, dev) -> dict:
     import torch
 
     from exact_ballpark_b200.collide import CollideGraph, VecCollidePark
-    from exact_ballpark_b200.workloads import collide_worlds
+    from exact_ballpark_b200.workloads import collide_statics_worlds, collide_worlds
     W = args.collide_worlds
     ticks = args.warmup + args.collide_steps
-    w = collide_worlds(21, W, ticks=ticks)
-    park = VecCollidePark(W, 16, device=dev)
-    park.load(w.worlds)
+    if statics:
+        w = collide_statics_worlds(22, W, ticks=ticks)
+        park = VecCollidePark(W, 8, device=dev, statics=8)
+        park.load(w.worlds, w.collidables)
+    else:
+        w = collide_worlds(21, W, ticks=ticks)
+        park = VecCollidePark(W, 16, device=dev)
+        park.load(w.worlds)
     graph = CollideGraph(park)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -313,6 +318,15 @@ def collide_runs(args, dev) -> dict:
             traffic = float(json.loads(tp.read_text())["dram_bytes_per_world_tick"]) * W
         except Exception:
             traffic = None
+    if statics:
+        return {"workload": f"collision park with static collidables: {W} worlds x (4 ships + 4 fixed spheres + 4 "
+                            "capsules + 4 oriented boxes), ships GOTO at them re-aimed every 25 ticks",
+                "value": 4 * W / (per / 1e3), "unit": "ship-ticks/s", "world_ticks_per_s": W / (per / 1e3),
+                "ms_per_step": per, "steps": args.collide_steps, "warmup": args.warmup,
+                "contacts_per_tick": contacts / args.collide_steps,
+                "reference_published": {"value": 54.3e6, "unit": "ship-ticks/s", "hardware": "GH200",
+                                        "config": "contact_slots=8, ships=4, spheres=4, statics=8, kernel, 65,536 "
+                                                  "worlds (docs/benchmarks.md)"}}
     return {"workload": f"collision park, gradient method on spheres: {W} worlds x (4 ships + 4 free spheres + 8 "
                         "fixed spheres), ships GOTO at spheres re-aimed every 25 ticks",
             "value": 4 * W / (per / 1e3), "unit": "ship-ticks/s", "world_ticks_per_s": W / (per / 1e3),
@@ -496,6 +510,7 @@ def main() -> None:
         line["ragged"] = ragged_runs(args, dev)
     if not args.no_collide:
         line["collide"] = collide_runs(args, dev)
+        line["collide_statics"] = collide_runs(args, dev, statics=True)
     if not args.no_serve:
         line["serve"] = serve_runs(args, dev)
         line["serve"]["plain_ship_ticks_per_s"] = line["plain"]["value"] / world_size

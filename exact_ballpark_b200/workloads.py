@@ -201,12 +201,14 @@ def ragged_ships(r: random.Random, max_ships: int) -> int:
 @dataclass
 class CollideWorlds:
     """Worlds for the collision park (exact_ballpark_b200.collide.VecCollidePark): `worlds` (each a list of the
-    load's ball dicts) and the ships' GOTO aims, {step: [(world, ball id, point)]} (step 1 is before the first tick)."""
+    load's ball dicts), `collidables` (each world's capsules and oriented boxes, or None) and the ships' GOTO aims,
+    {step: [(world, ball id, point)]} (step 1 is before the first tick)."""
     worlds: list
     aims: dict
     ships: int
     spheres: int
     statics: int
+    collidables: list | None = None
 
     def apply(self, park, step: int) -> None:
         """The aims of `step` through the park's API: one GotoPoint call with every aimed ship's point."""
@@ -266,3 +268,77 @@ def collide_worlds(seed: int, worlds: int, ships: int = 4, spheres: int = 4, sta
                 t = r.choice(targets)
                 aims.setdefault(step, []).append((w, s + 1, list(t["pos"])))
     return CollideWorlds(out, aims, ships, spheres, statics)
+
+
+def _frame(r: random.Random) -> tuple:
+    """Three orthonormal directions, uniformly oriented (Gram-Schmidt of two random unit vectors)."""
+    u = _unit(r)
+    while True:
+        v = _unit(r)
+        d = sum(u[i] * v[i] for i in range(3))
+        w = [v[i] - d * u[i] for i in range(3)]
+        n = math.sqrt(sum(c * c for c in w))
+        if n > 1e-3:
+            w = [c / n for c in w]
+            break
+    x = [u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]]
+    return u, w, x
+
+
+def collide_statics_worlds(seed: int, worlds: int, ships: int = 4, spheres: int = 4, statics: int = 8,
+                           ticks: int = 500, reaim: int = 25) -> CollideWorlds:
+    """The collision benchmark's static-collidable shape: W worlds of `ships` ships and `spheres` fixed spheres (the
+    balls), and `statics` static collidables, half capsules and half oriented boxes, in a +-20 km cube, world w from
+    random.Random(seed * 1_000_003 + w). Ships as collide_worlds draws them; fixed spheres of radius log-uniform
+    10 m - 5 km; a capsule of radius log-uniform 30-500 m along a uniform direction, 100 m - 2 km long; a box of
+    edges log-uniform 100 m - 5 km on a uniformly oriented frame. Every ship flies GOTO at a static collidable's
+    centre or a sphere's, re-aimed every `reaim` ticks (harness choices, as in collide_worlds)."""
+    out, coll, aims = [], [], {}
+    lg = math.log10
+    for w in range(worlds):
+        r = random.Random(seed * 1_000_003 + w)
+        balls, items, centres = [], [], []
+        bid = 0
+        for kind, count in (("ship", ships), ("sphere", spheres)):
+            for _ in range(count):
+                bid += 1
+                if kind == "ship":
+                    mass, radius = 10.0 ** r.uniform(6.0, 9.0), r.uniform(20.0, 500.0)
+                    max_vel, agility = 10.0 ** r.uniform(2.0, lg(3000.0)), r.uniform(0.1, 5.0)
+                else:
+                    mass, radius, max_vel, agility = 10.0 ** r.uniform(6.0, 10.0), 10.0 ** r.uniform(1.0, lg(5000.0)), \
+                        0.0, 1.0
+                pos = [r.uniform(-2e4, 2e4) for _ in range(3)]
+                vel = [0.0, 0.0, 0.0]
+                if kind == "ship":
+                    u = _unit(r)
+                    sp = r.uniform(0.0, max_vel)
+                    vel = [c * sp for c in u]
+                else:
+                    centres.append(pos)
+                balls.append({"id": bid, "mass": mass, "radius": radius, "max_vel": max_vel, "agility": agility,
+                              "speed_fraction": 1.0, "pos": pos, "vel": vel, "free": kind == "ship", "massive": True})
+        for k in range(statics):
+            sid = 1000 + k
+            c = [r.uniform(-1.8e4, 1.8e4) for _ in range(3)]
+            if k % 2 == 0:
+                u = _unit(r)
+                half = r.uniform(100.0, 2000.0) / 2.0
+                a = [c[i] - u[i] * half for i in range(3)]
+                b = [c[i] + u[i] * half for i in range(3)]
+                items.append({"kind": "capsule", "id": sid, "parent": 0, "a": a, "b": b,
+                              "radius": 10.0 ** r.uniform(lg(30.0), lg(500.0))})
+            else:
+                f = _frame(r)
+                e = [10.0 ** r.uniform(2.0, lg(5000.0)) for _ in range(3)]
+                edges = [[f[j][i] * e[j] for i in range(3)] for j in range(3)]
+                corner = [c[i] - (edges[0][i] + edges[1][i] + edges[2][i]) / 2.0 for i in range(3)]
+                items.append({"kind": "box", "id": sid, "parent": 0, "corner": corner, "lx": edges[0],
+                              "ly": edges[1], "lz": edges[2]})
+            centres.append(c)
+        out.append(balls)
+        coll.append(items)
+        for step in range(1, ticks + 1, reaim):
+            for s in range(ships):
+                aims.setdefault(step, []).append((w, s + 1, list(r.choice(centres))))
+    return CollideWorlds(out, aims, ships, spheres, statics, coll)

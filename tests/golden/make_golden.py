@@ -283,6 +283,16 @@ def make_collide_traces(sample: int) -> None:
         park.evolve()
     ct.save([park.trace], HERE / "collide_w0")
     print(f"  collide_w0: 64 worlds x 16 balls, 100 ticks, {time.time() - t:.0f} s")
+    from exact_ballpark_b200.workloads import collide_statics_worlds
+    t = time.time()
+    w = collide_statics_worlds(1, 64, ticks=100)
+    park = Rec(64, 8, friction=1.0e6, tick_interval_ms=1000, device="cpu", statics=8)
+    park.load(w.worlds, w.collidables)
+    for step in range(1, 101):
+        w.apply(park, step)
+        park.evolve()
+    ct.save([park.trace], HERE / "collide_s0")
+    print(f"  collide_s0: 64 worlds x (8 balls + 8 static collidables), 100 ticks, {time.time() - t:.0f} s")
 
 
 def main() -> None:

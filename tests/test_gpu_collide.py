@@ -18,7 +18,8 @@ from golden_util import bit_equal
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 
-@pytest.mark.parametrize("name", ["collide_cc1", "collide_cc2", "collide_w0", "collide_st1", "collide_st2"])
+@pytest.mark.parametrize("name", ["collide_cc1", "collide_cc2", "collide_w0", "collide_st1", "collide_st2",
+                                  "collide_s0"])
 def test_the_gpu_collision_park_replays_the_golden_trace(name):
     from exact_ballpark_b200 import VecCollidePark
     groups = ct.load(ct.GOLDEN / name)
