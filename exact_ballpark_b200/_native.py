@@ -54,6 +54,8 @@ def lib() -> ctypes.CDLL:
     L.ebb_flight_move.argtypes = [ctypes.POINTER(FlightState), ctypes.POINTER(FlightState), p, p, i64, p, p, i32]
     L.ebb_collide_tick.argtypes = [p, p, p, p]
     L.ebb_collide_load.argtypes = [p, p, p]
+    L.ebb_glibc_srand.argtypes = [p, i64, p, p]
+    L.ebb_glibc_rand.argtypes = [p, i64, i64, p, p]
     L.ebb_flight_snap.argtypes = [ctypes.POINTER(FlightState), p, i32, p, i32]
     L.ebb_flight_decay.argtypes = [ctypes.POINTER(FlightState), p, ctypes.c_double, p, i32]
     L.ebb_libm.argtypes = [i32, i64, p, p, p, p, i32]

@@ -470,6 +470,10 @@ __device__ __forceinline__ double box_contact(V p0, V p1, double brad, const dou
         const double lo = g[G_LO + q], hi = g[G_HI + q];
         excl = excl || (dsub(p0a[q], r) > hi && dsub(p1a[q], r) > hi) || (dadd(p0a[q], r) < lo && dadd(p1a[q], r) < lo);
     }
+    if (excl) {                                                       // the AABB excludes the move: no contact,
+        *nrm = V{0.0, 0.0, 0.0};                                      // whatever the tests below would find
+        return -1.0;
+    }
     const V vel = vsub(p1, p0), p = p0;
     const double radius = brad;
     V dd = vsub(gv(g, G_CORNERS), p);                                 // ClosestCorner: the first nearest
@@ -565,7 +569,7 @@ __device__ __forceinline__ double box_contact(V p0, V p1, double brad, const dou
         }
         hit = hit || h;
     }
-    hit = !excl && (inside || hit);
+    hit = inside || hit;
     if (inside) {
         out = n_in;
         time = 0.0;

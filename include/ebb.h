@@ -156,6 +156,15 @@ int ebb_collide_tick(const EbbCollideState* s, const uint8_t* active, int32_t* s
  * _filing / _check_filing (vec_collide.py:550-667, 776-807). */
 int ebb_collide_load(const EbbCollideState* s, int32_t* status, void* stream);
 
+/* glibc 2.34's rand() after srand(seed) (random_r, TYPE_3), one generator a world: a world's state is EBB_RAND_WORDS
+ * int32 (the 31-word table, then the front and rear indices). ebb_glibc_srand seeds worlds[W] states from seeds[W]
+ * (srandom_r, its 310 discarded draws included); ebb_glibc_rand draws `draws` values a world into out[W][draws],
+ * advancing the states. destiny's floatrand (Ball.cpp:19) is rand() / 2147483647.0. Replaces GlibcRandom and
+ * glibc_srand (exact_ballpark/glibc_rand.py:14, vec_space.py:148) and vec_space.cu's glibc_rand. */
+#define EBB_RAND_WORDS 33
+int ebb_glibc_srand(const int64_t* seeds, int64_t worlds, int32_t* state, void* stream);
+int ebb_glibc_rand(int32_t* state, int64_t worlds, int64_t draws, int32_t* out, void* stream);
+
 /* SnapOrientation of the rows in mask[n] (nonzero bytes): the rotation turned to the velocity and rolled upright,
  * the old rotation the same, the angular velocities zeroed (at a speed of 1e-6 m/s or less nothing changes). With
  * `fresh`, first the state of a new ball: rotation identity, old rotation rot x RotationQuaternion(angVel,

@@ -295,9 +295,27 @@ def make_collide_traces(sample: int) -> None:
     print(f"  collide_s0: 64 worlds x (8 balls + 8 static collidables), 100 ticks, {time.time() - t:.0f} s")
 
 
+def make_rand() -> None:
+    """rand.npz: glibc's rand() after srand(seed) from the reference's own generator (exact_ballpark.space's
+    GlibcRandom, glibc_rand.py), 2000 draws for each of 40 seeds (edge seeds included: 0, 1, 2^31 - 1, 2^31, 2^32 - 1,
+    2^32, a negative one), and the state after srand."""
+    from exact_ballpark.space import GlibcRandom
+    r = np.random.default_rng(7)
+    seeds = [0, 1, 2, 2 ** 31 - 1, 2 ** 31, 2 ** 32 - 1, 2 ** 32, -5, 123456789] + \
+        [int(x) for x in r.integers(0, 2 ** 40, 31)]
+    draws = np.zeros((len(seeds), 2000), dtype=np.int64)
+    states = np.zeros((len(seeds), 33), dtype=np.int64)
+    for i, sd in enumerate(seeds):
+        g = GlibcRandom(sd)
+        states[i] = list(g.s) + [g.f, g.r]
+        draws[i] = [g.next() for _ in range(2000)]
+    np.savez_compressed(HERE / "rand.npz", seeds=np.array(seeds, dtype=np.int64), draws=draws, states=states)
+    print(f"  rand.npz: {len(seeds)} seeds x 2000 draws")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide"), default=None)
+    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand"), default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
     a = ap.parse_args()
     if a.only in (None, "libm"):
@@ -308,6 +326,8 @@ def main() -> None:
         make_traces(a.sample)
     if a.only in (None, "collide"):
         make_collide_traces(a.sample)
+    if a.only in (None, "rand"):
+        make_rand()
 
 
 if __name__ == "__main__":
