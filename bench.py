@@ -144,6 +144,18 @@ def cpu_sample(worlds: int, ships: int, warmup: int, steps: int) -> dict:
                       f"{threads} threads over disjoint worlds"}
 
 
+def reduce_max(x: float, dist, device) -> float:
+    """The largest x over the ranks of the process group (one all-reduce; x itself without a group): the timing of a
+    multi-GPU run is its slowest rank's. `device`: where the group's backend reduces (a CUDA device for NCCL, the CPU
+    for gloo)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args, rank: int) -> None:
     """The reference arm: the CPU port of the reference's algorithm on the whole workload, host cores, rank 0."""
     if rank != 0:
@@ -433,11 +445,7 @@ def main() -> None:
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, dev)
 
     for _ in range(args.warmup):                                     # warm-up ticks
         park.evolve()
