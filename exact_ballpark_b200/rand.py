@@ -34,5 +34,7 @@ def rand(state: torch.Tensor, draws: int) -> torch.Tensor:
 
 
 def floatrand(state: torch.Tensor, draws: int = 1) -> torch.Tensor:
-    """destiny's floatrand (Ball.cpp:19): rand() / RAND_MAX as a double, [W, draws]."""
-    return rand(state, draws).to(torch.float64) / RAND_MAX
+    """destiny's floatrand (Ball.cpp:19): rand() / RAND_MAX as a double, [W, draws] (a tensor divisor: torch on CUDA
+    divides by a Python number through its reciprocal, which is not the IEEE quotient)."""
+    r = rand(state, draws).to(torch.float64)
+    return r / torch.tensor(RAND_MAX, dtype=torch.float64, device=r.device)
