@@ -9,7 +9,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libebb.so"
-ABI = 2
+ABI = 3
 COLLIDE_MAX_SLOTS = 64          # include/ebb.h: EBB_COLLIDE_MAX_SLOTS
 COLLIDE_MAX_STATICS = 64        # include/ebb.h: EBB_COLLIDE_MAX_STATICS
 
@@ -27,6 +27,16 @@ class FlightState(ctypes.Structure):
                     "rot_roll", "rot", "old_rot", "ang_vel", "old_ang_vel", "torque", "ids", "effect_stamp",
                     "follow_id", "owner_id", "clock", "mode", "follow_ptr", "free_", "moribund", "massive",
                     "interactive", "sensor")])
+
+
+class CombatState(ctypes.Structure):
+    """include/ebb.h's EbbCombatState, field for field."""
+    _fields_ = ([("flight", FlightState)]
+                + [(k, ctypes.c_void_p) for k in (
+                    "exists", "formation_id", "formation_slots", "owner_ptr", "hits_n", "ev_n", "ev_self", "bubble",
+                    "cloaked", "flags", "formations", "formation_len")]
+                + [("n_formations", ctypes.c_int64), ("max_slots", ctypes.c_int64), ("tick_ms", ctypes.c_int64),
+                   ("do_missiles_off", ctypes.c_int32), ("master", ctypes.c_int32)])
 
 
 def lib() -> ctypes.CDLL:
@@ -54,6 +64,7 @@ def lib() -> ctypes.CDLL:
     L.ebb_flight_move.argtypes = [ctypes.POINTER(FlightState), ctypes.POINTER(FlightState), p, p, i64, p, p, i32]
     L.ebb_collide_tick.argtypes = [p, p, p, p]
     L.ebb_collide_load.argtypes = [p, p, p]
+    L.ebb_combat_tick.argtypes = [ctypes.POINTER(CombatState), p, i64, p, p, i32]
     L.ebb_glibc_srand.argtypes = [p, i64, p, p]
     L.ebb_glibc_rand.argtypes = [p, i64, i64, p, p]
     L.ebb_flight_snap.argtypes = [ctypes.POINTER(FlightState), p, i32, p, i32]

@@ -99,7 +99,7 @@ __device__ __forceinline__ D3 follow_thrust(Ship& s, D3 tpos, float tradius, con
 __device__ __forceinline__ double trunc7(double x) { return ddiv(i2d(to_i64(dmul(x, TRUNC7))), TRUNC7); }
 
 // DefaultOrbitalNormal (modes.py:480): the precessing w, truncated to 7 decimals, not normalised
-__device__ __noinline__ D3 precessing_w(int64_t clock, int64_t id) {
+inline __device__ __noinline__ D3 precessing_w(int64_t clock, int64_t id) {
     const double t = i2d(clock);
     const double phi1 = dmul(t, ORBITAL_PRECESSION);
     const double phi2 = dadd(i2d(id & 0xFFFFLL), dmul(t, ORBITAL_PRECESSION));
@@ -443,12 +443,12 @@ __device__ __forceinline__ void pow_cache_clear(PowCache& c) {
 }
 
 // CalculateN2Alpha2's braking ticks (full.py:2128): n2 = ceil(log(factor / (1 + factor)) / (-dt t_scale)) as an int
-__device__ __noinline__ int braking_ticks(float max_ang_vel, float len_omega, float fdt, float t_scale) {
+inline __device__ __noinline__ int braking_ticks(float max_ang_vel, float len_omega, float fdt, float t_scale) {
     const float factor = fdiv(max_ang_vel, len_omega);
     return to_i32(tod(fceil(fdiv(lm::logf(fdiv(factor, fadd(1.0f, factor))), fmul(fneg(fdt), t_scale)))));
 }
 // kappa2 = tf^n2 (glibc's pow, rounded to float)
-__device__ __noinline__ float braking_kappa(float tf, int n2) { return tof(lm::pow(tod(tf), (double)n2)); }
+inline __device__ __noinline__ float braking_kappa(float tf, int n2) { return tof(lm::pow(tod(tf), (double)n2)); }
 
 // CalculateN2Alpha2 (full.py:2124-2150): the braking ticks n2, kappa2 = tf^n2 (pow), and the braking factor
 // t_scale kappa2 / (1 - kappa2) the torque is -omega times (when the turning rate is above 1e-10)
@@ -493,7 +493,7 @@ __device__ __forceinline__ void search_terms(const Search& q, float kappa1, floa
 }
 
 // RotationQuaternion(axis, angle): sinf and cosf of the half angle around the normalised axis
-__device__ __noinline__ F4 q_axis_angle(F3 axis, float angle) {
+inline __device__ __noinline__ F4 q_axis_angle(F3 axis, float angle) {
     const F3 u = f3_unit(axis);
     const float h = fdiv(angle, 2.0f);
     const float s = lm::sinf(h);
@@ -532,7 +532,7 @@ __device__ __forceinline__ Turned apply_torque(F4 rotation, F3 w, F3 torque, flo
 }
 
 // Ball::SnapOrientation (full.py:2092): turned to the velocity and rolled upright (the caller clears the turning)
-__device__ __noinline__ F4 snap_rotation(D3 vel) {
+inline __device__ __noinline__ F4 snap_rotation(D3 vel) {
     const F3 d = f3_of(vel);
     const float len_dir = f3_len(d);
     if (tod(len_dir) < 1e-12) return q_identity();

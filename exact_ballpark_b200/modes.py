@@ -292,8 +292,12 @@ class VecModesPark:
         self.plan = plan_tiles(self.world)
 
     # ---- the follower bookkeeping: Stop(Ball*) (vec_modes.py:289) ----
+    def _following(self) -> torch.Tensor:
+        """The rows in a follow mode whose Stop clears the follow fields (FOLLOW, ORBIT here)."""
+        return (self._mode == FOLLOW) | (self._mode == ORBIT)
+
     def _stop_rows(self, mask: torch.Tensor) -> None:
-        follower = mask & ((self._mode == FOLLOW) | (self._mode == ORBIT))
+        follower = mask & self._following()
         self._effect_stamp.masked_fill_(follower, 0)
         self._follow_ptr.masked_fill_(follower, -1)
         self._follow_id.masked_fill_(follower, 0)

@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define EBB_ABI_VERSION 2
+#define EBB_ABI_VERSION 3
 #define EBB_EINVAL (-1)
 #define EBB_ETOOBIG (-2)
 
@@ -69,6 +69,24 @@ typedef struct EbbCollideState {
     double* s_geo;                                                                     /* [W S][175] */
     int64_t *s_int, *s_keys;                                                           /* [W S][5], [W S][B][3] */
 } EbbCollideState;
+
+/* The combat park (missiles, formations, cloaking; exact_ballpark.vec_combat.VecCombatPark, vec_combat_cuda.cu:53-74):
+ * the flight park's rows and, per row, whether it holds a ball (an empty row is moribund and inert until AddBall),
+ * the leader's formation (char semantics, -1 none) and slot bits, a missile's owner row (-1 none), the tick's
+ * contact and dispatch counts, and the bubble and cloak the commands keep; the formation table [formations][max
+ * slots][3] with each formation's length. Dynamical orientation is required (flight.dynamical = 1). */
+typedef struct EbbCombatState {
+    EbbFlightState flight;
+    uint8_t* exists;
+    int64_t *formation_id, *formation_slots, *owner_ptr;
+    int64_t *hits_n, *ev_n;                    /* out: contacts with the target this tick; target collisions dispatched */
+    uint8_t* ev_self;                          /* out: the master's self-collision dispatched */
+    int64_t *bubble, *cloaked, *flags;
+    const double* formations;
+    const int64_t* formation_len;
+    int64_t n_formations, max_slots, tick_ms;
+    int32_t do_missiles_off, master;
+} EbbCombatState;
 
 /* The ABI version (EBB_ABI_VERSION). Replaces xbpm_abi / xbpo_abi (exact_ballpark/vec_modes_cuda.cu:750,
  * vec_orient_cuda.cu:499). */
@@ -156,6 +174,17 @@ int ebb_collide_tick(const EbbCollideState* s, const uint8_t* active, int32_t* s
  * _filing / _check_filing (vec_collide.py:550-667, 776-807). */
 int ebb_collide_load(const EbbCollideState* s, int32_t* status, void* stream);
 
+/* One tick of the combat park in place, in tiles of whole worlds (tile_rows[tiles + 1], each tile at most `block`
+ * rows, one block a tile): the records pass, phase 1 for every ball (the releases by a target starting warp proper,
+ * each mode's thrust with MISSILE and FORMATION, dynamical orientation unless disabled for missiles), each massive
+ * normal missile's contacts with its target (Potential's recursion, counted), then phases 3 and 4 (the warp path or
+ * the integrator, the rotation a tick on or a disabled missile's snap, the commit, the dispatch counts, PetrifyTroll,
+ * the clock), block barriers between the steps. status[0] bit 0: a follow target outside its tile; bit 1: a tile
+ * wider than the block. Replaces xbpc_tick (exact_ballpark/vec_combat_cuda.cu:731-800: its prepass, phase-1, contact
+ * and commit launches), which exact_ballpark.vec_combat_cuda.tick calls (vec_combat_cuda.py:289). */
+int ebb_combat_tick(const EbbCombatState* s, const int64_t* tile_rows, int64_t tiles, int32_t* status, void* stream,
+                    int block);
+
 /* glibc 2.34's rand() after srand(seed) (random_r, TYPE_3), one generator a world: a world's state is EBB_RAND_WORDS
  * int32 (the 31-word table, then the front and rear indices). ebb_glibc_srand seeds worlds[W] states from seeds[W]
  * (srandom_r, its 310 discarded draws included); ebb_glibc_rand draws `draws` values a world into out[W][draws],
@@ -183,7 +212,7 @@ int ebb_flight_decay(const EbbFlightState* s, const uint8_t* mask, double neg_kd
 int ebb_libm(int func, int64_t n, const double* x, const double* y, double* out, void* stream, int block);
 
 /* A kernel's resources as loaded on the current device: which 0 the plain tick, 1 the prepass, 2 the tiled tick,
- * 3 the listed-worlds tick, 4 the row move.
+ * 3 the listed-worlds tick, 4 the row move, 7 the combat tick.
  * Replaces xbpm_info (vec_modes_cuda.cu:766). */
 int ebb_kernel_info(int which, int* regs, int* local_bytes, int* binary_version, int* ptx_version, int* max_threads);
 

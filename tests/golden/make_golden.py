@@ -313,9 +313,69 @@ def make_rand() -> None:
     print(f"  rand.npz: {len(seeds)} seeds x 2000 draws")
 
 
+# ============================================================================================ combat
+
+def _combat_batches(seed: int) -> list:
+    """The reference's combat scenarios of a seed (tests/destiny_combat_cases.py, 12 batches of 12 worlds, as its own
+    tests run them), the batches with dynamical orientation, each world checked on the scalar FullBallpark first: the
+    worlds outside the reference's domain (Destiny's result undefined, or balls in two bubbles) left out."""
+    import destiny_combat_cases as dc
+    out = []
+    for cfg in dc.batches(seed, 12, 12):
+        if not cfg["do"]:
+            continue
+        refs = [dc.reference(cfg, w) for w in cfg["worlds"]]
+        keep = [w for w, r in zip(cfg["worlds"], refs) if dc.in_domain(r)]
+        out.append(({**cfg, "worlds": keep}, [r for r in refs if dc.in_domain(r)]))
+    return out
+
+
+def make_combat() -> None:
+    """combat_{1,2}: the reference's combat scenarios (seed 1 development, 2 held out), batches with dynamical
+    orientation (its missile exclusion on and off, master and client, every tick length and orbit law), recorded on
+    the reference's VecCombatPark (its tick on tensors, CPU) by tests/golden/combat_trace.py's driver. Each batch is
+    first run by the reference's own harness (destiny_combat_cases.batched) and compared with the scalar FullBallpark
+    by its own comparison (destiny_combat_cases.differences): 0 differences, or the generator stops. Worlds the batch
+    flags (outside its domain) are left out; the driver's run then gives the same events, answers and final state as
+    the reference's harness."""
+    import combat_trace as ct
+    import destiny_combat_cases as dc
+    import exact_ballpark.vec_combat as vc
+    for seed in (1, 2):
+        t = time.time()
+        batches = []
+        for cfg, refs in _combat_batches(seed):
+            outs, park = dc.batched(cfg, "cpu", path="torch")
+            flags = park.world_flags()
+            keep = [k for k in range(len(cfg["worlds"])) if not flags[k]]
+            for k in keep:
+                bad = dc.differences(refs[k], outs[k])
+                if bad:
+                    raise RuntimeError(f"seed {seed}: the reference's batch differs from FullBallpark: {bad[:4]}")
+            cfg = {**cfg, "worlds": [cfg["worlds"][k] for k in keep]}
+            outs, park = dc.batched(cfg, "cpu", path="torch")
+            if any(park.world_flags()):
+                raise RuntimeError("a world flagged once its neighbours were left out")
+            digests = []
+            p, where = ct.make_park(vc.VecCombatPark, cfg, dc.FORMATIONS, "cpu")
+            got = ct.drive(p, cfg, where, lambda s, q: digests.append(ct.field_digests(q)))
+            want_e = [(wl, *e) for wl, o in enumerate(outs) for e in o["E"]]
+            if sorted(got["E"]) != sorted(want_e) or got["A"] != [o["A"] for o in outs]:
+                raise RuntimeError("the driver's run differs from the reference harness's (events or answers)")
+            for f in ct.FIELDS + ("exists",):
+                a, b = ct.canonical(getattr(p, f)), ct.canonical(getattr(park, f))
+                if a.shape != b.shape or not (a.view(np.uint64) == b.view(np.uint64)).all():
+                    raise RuntimeError(f"the driver's final {f} differs from the reference harness's")
+            batches.append({"cfg": cfg, "digests": np.array(digests, dtype=np.uint64), "events": got["E"],
+                            "answers": got["A"]})
+        ct.save(HERE / f"combat_{seed}", dc.FORMATIONS, batches)
+        print(f"  combat_{seed}: {len(batches)} batches, {sum(len(b['cfg']['worlds']) for b in batches)} worlds, "
+              f"{sum(len(b['events']) for b in batches)} events, {time.time() - t:.0f} s")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand"), default=None)
+    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat"), default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
     a = ap.parse_args()
     if a.only in (None, "libm"):
@@ -328,6 +388,8 @@ def main() -> None:
         make_collide_traces(a.sample)
     if a.only in (None, "rand"):
         make_rand()
+    if a.only in (None, "combat"):
+        make_combat()
 
 
 if __name__ == "__main__":
