@@ -354,6 +354,86 @@ def collide_runs(args, dev, statics: bool = False) -> dict:
                                               "(docs/benchmarks.md)"}}
 
 
+# The combat park's algorithmic bytes a row-tick: the flight row's (BYTES_PER_SHIP_TICK) and the combat state it
+# reads (exists 1, formation id 8, owner row 8, bubble 8, cloak 8) and writes (contacts 8, dispatch count 8, the
+# self-collision byte 1)
+COMBAT_BYTES_PER_ROW_TICK = BYTES_PER_SHIP_TICK + (1 + 8 + 8 + 8 + 8) + (8 + 8 + 1)
+
+
+def combat_cpu_sample(worlds: int, warmup: int, steps: int) -> dict:
+    """The CPU oracle of the combat park (oracle/combat_park.py, the C++ sequential tick) on every host core, on
+    `worlds` worlds of the benchmark's workload over `steps` ticks after `warmup`: ship-ticks/s (4 ships a world)."""
+    from exact_ballpark_b200.workloads import combat_worlds
+    from oracle.combat_park import OracleCombatPark
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    w = combat_worlds(31, worlds)
+    p = OracleCombatPark(len(w.rows), dynamical_orientation=True, use_new_orbit=True)
+    p.load(w.rows)
+    w.apply(p)
+    for _ in range(warmup):
+        p.evolve(threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        p.evolve(threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": w.ships * worlds * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{worlds} worlds x (4 ships + 4 missiles) (seed 31), ticks {warmup + 1}..{warmup + steps} "
+                      f"({dt:.1f} s wall), C++ oracle (oracle/flight.cpp's combat tick), {threads} threads over "
+                      "disjoint worlds"}
+
+
+def combat_runs(args, dev) -> dict:
+    """The combat park (exact_ballpark_b200.combat, missiles and formations) at the reference's combat benchmark
+    shape: --combat-worlds worlds of 4 ships and 4 missiles (workloads.combat_worlds: the ships following, orbiting
+    or flying to points, half the worlds with a formation; each missile added at a random launcher and launched aimed
+    and massive at another ship), warm-up ticks, then --combat-steps ticks each one CUDA-graph replay of the tick (the
+    domain watch and the one-launch tick), timed with CUDA events (L2 flushed before each). Ship-ticks count the 4
+    ships a world (missiles excluded), as the reference's benchmark does."""
+    import torch
+
+    from exact_ballpark_b200.combat import CombatGraph, VecCombatPark
+    from exact_ballpark_b200.workloads import combat_worlds
+    W = args.combat_worlds
+    w = combat_worlds(31, W)
+    n = len(w.rows)
+    park = VecCombatPark(n, device=dev, dynamical_orientation=True, use_new_orbit=True, block=128)
+    park.load(w.rows)
+    w.apply(park)
+    graph = CombatGraph(park)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    total, events = 0.0, 0
+    for step in range(1, args.warmup + args.combat_steps + 1):
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        graph.tick()
+        b.record(stream)
+        b.synchronize()
+        if step > args.warmup:
+            total += a.elapsed_time(b)
+            events += len(park.events())
+    park.check()
+    per = total / args.combat_steps
+    peak, kind = _peaks()
+    achieved = COMBAT_BYTES_PER_ROW_TICK * n / (per / 1e3) / 1e9
+    out = {"workload": f"combat park: {W} worlds x (4 ships + 4 missiles launched aimed and massive), ships "
+                       "follow / orbit / goto, half the worlds with a formation, dynamical orientation on",
+           "value": 4 * W / (per / 1e3), "unit": "ship-ticks/s", "world_ticks_per_s": W / (per / 1e3),
+           "row_ticks_per_s": n / (per / 1e3), "ms_per_step": per, "steps": args.combat_steps,
+           "warmup": args.warmup, "events_per_tick": events / args.combat_steps,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_kind": kind, "traffic": None,
+                        "note": f"algorithmic {COMBAT_BYTES_PER_ROW_TICK} B/row-tick x {n} rows over the tick's "
+                                "CUDA-event time (a graph replay: the watch's few small kernels and the tick); "
+                                "issue- and latency-bound like the flight tick"},
+           "reference_published": {"value": 92.7e6, "unit": "ship-ticks/s", "hardware": "GH200",
+                                   "config": "do=1, missiles=4, ships=4, graph, 65,536 worlds (docs/benchmarks.md)"}}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = combat_cpu_sample(256, 3, 20)
+    return out
+
+
 def _config(args, schedule: str) -> dict:
     return {"workload": (f"flight-mode park, dynamical orientation on, new orbit law: {args.worlds} worlds x "
                          f"{args.ships} ships (follow / orbit / warp), per-rank"),
@@ -377,6 +457,9 @@ def main() -> None:
     ap.add_argument("--ragged-steps", type=int, default=30)
     ap.add_argument("--collide-worlds", type=int, default=65536)
     ap.add_argument("--collide-steps", type=int, default=50)
+    ap.add_argument("--no-combat", action="store_true")
+    ap.add_argument("--combat-worlds", type=int, default=65536)
+    ap.add_argument("--combat-steps", type=int, default=50)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-seconds", type=float, default=6.0)
     ap.add_argument("--serve-budget-gb", type=float, default=80.0)
@@ -519,6 +602,8 @@ def main() -> None:
     if not args.no_collide:
         line["collide"] = collide_runs(args, dev)
         line["collide_statics"] = collide_runs(args, dev, statics=True)
+    if not args.no_combat:
+        line["combat"] = combat_runs(args, dev)
     if not args.no_serve:
         line["serve"] = serve_runs(args, dev)
         line["serve"]["plain_ship_ticks_per_s"] = line["plain"]["value"] / world_size

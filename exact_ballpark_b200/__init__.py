@@ -7,9 +7,9 @@ cloaking). The ticks run in the native library libebb.so (csrc/, C ABI in includ
 """
 
 from .collide import CollideGraph, VecCollidePark  # noqa: F401
-from .combat import VecCombatPark  # noqa: F401
+from .combat import CombatGraph, VecCombatPark  # noqa: F401
 from .modes import (ModesGraph, VecModesPark, kernel_info, libm, tick, tick_plain, tick_tiled,  # noqa: F401
                     tick_worlds)
 
 __all__ = ["VecModesPark", "ModesGraph", "kernel_info", "libm", "tick", "tick_plain", "tick_tiled", "tick_worlds",
-           "VecCollidePark", "CollideGraph", "VecCombatPark"]
+           "VecCollidePark", "CollideGraph", "VecCombatPark", "CombatGraph"]

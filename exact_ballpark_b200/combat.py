@@ -562,3 +562,39 @@ def tick(park: VecCombatPark, block: int | None = None) -> None:
         rc = _native.lib().ebb_combat_tick(ctypes.byref(park.combat_state()), tr.data_ptr(), plan.tiles,
                                            park._status.data_ptr(), park._stream(), plan.block)
     _native.check(rc, "ebb_combat_tick")
+
+
+class CombatGraph:
+    """The combat park's tick (`evolve`: the domain watch and the one-launch tick) captured as a CUDA graph on the
+    park's own buffers (the drop-in for exact_ballpark.vec_combat_cuda.CombatGraph): each `tick()` is one replay; a
+    LoadFormations since the capture (a new table) is captured anew first."""
+
+    def __init__(self, park: VecCombatPark):
+        self.park = park
+        self._capture()
+
+    def _capture(self) -> None:
+        park = self.park
+        names = [n for n in vars(park) if isinstance(getattr(park, n), torch.Tensor)]
+        keep = {n: getattr(park, n).clone() for n in names}
+        side = torch.cuda.Stream(device=park.dev)
+        side.wait_stream(torch.cuda.current_stream(park.dev))
+        with torch.cuda.stream(side):                             # a warm-up tick, undone
+            park.evolve()
+            for n, v in keep.items():
+                getattr(park, n).copy_(v)
+        torch.cuda.current_stream(park.dev).wait_stream(side)
+        torch.cuda.synchronize(park.dev)
+        park.current_time -= 1
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            park.evolve()
+        park.current_time -= 1
+        self._tables = (park.formation_table, park.formation_lengths)
+
+    def tick(self) -> None:
+        park = self.park
+        if park.formation_table is not self._tables[0] or park.formation_lengths is not self._tables[1]:
+            self._capture()
+        self.graph.replay()
+        park.current_time += 1

@@ -342,3 +342,113 @@ def collide_statics_worlds(seed: int, worlds: int, ships: int = 4, spheres: int 
             for s in range(ships):
                 aims.setdefault(step, []).append((w, s + 1, list(r.choice(centres))))
     return CollideWorlds(out, aims, ships, spheres, statics, coll)
+
+
+# ============================================================================ the combat park
+
+GOTO, FORMATION_MODE = 0, 12
+COMBAT_FORMATIONS = [[[0.0, 0.0, -1.0], [1.0, 0.0, -1.0], [-1.0, 0.0, -1.0], [0.0, 1.0, -2.0]],
+                     [[3.0, 0.0, 0.0], [-3.0, 0.0, 0.0], [0.0, 3.0, 0.0]]]
+
+
+@dataclass
+class CombatWorlds:
+    """Worlds for the combat park (exact_ballpark_b200.combat.VecCombatPark): each world its ships (ids 1 .. S) and
+    its missile rows (ids 101 .., empty until the set-up adds them), as `load` rows; the set-up's commands as row
+    arrays, applied through the park's public API by `apply` (so any implementation of it runs the same worlds):
+    the ships' modes (FOLLOW, ORBIT or GOTO; in half the worlds ship 1 leads formation 0 or 1 with ship 2 in a slot),
+    then each missile added at its launcher and launched (aimed, massive) at another ship of its world."""
+    rows: list
+    worlds: int
+    ships: int
+    missiles: int
+    follow: np.ndarray
+    orbit: np.ndarray
+    goto: np.ndarray
+    target: np.ndarray              # a follower's or orbiter's target row
+    range_: np.ndarray
+    point: np.ndarray
+    leader: np.ndarray              # rows that lead a formation, with its index in `formation`
+    formation: np.ndarray
+    member: np.ndarray              # rows that follow their world's leader (its id in `leader_id`) in slot `slot`
+    leader_id: np.ndarray
+    slot: np.ndarray
+    missile: np.ndarray             # the missile rows
+    missile_balls: list             # their AddBall dicts, in row order
+    launch_target: np.ndarray       # target and owner ids (per row)
+    launch_owner: np.ndarray
+
+    def apply(self, park) -> None:
+        dev = park.dev
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        park.load_formations(COMBAT_FORMATIONS)
+        park.follow(t(self.follow), t(self.target), t(self.range_))
+        park.orbit(t(self.orbit), t(self.target), t(self.range_))
+        park.goto_point(t(self.goto), t(self.point))
+        park.set_ball_formation(t(self.leader), t(self.formation))
+        park.formation_follow(t(self.member), t(self.leader_id), t(self.slot))
+        park.add_balls(t(self.missile), self.missile_balls)
+        one = torch.ones(len(self.rows), dtype=torch.int64, device=dev)
+        park.launch_missile(t(self.missile), t(self.launch_target), t(self.launch_owner), one, one)
+
+
+def combat_worlds(seed: int, worlds: int, ships: int = 4, missiles: int = 4) -> CombatWorlds:
+    """W combat worlds (CombatWorlds); world w drawn from random.Random(seed * 1_000_003 + w): ships as the flight
+    benchmark's (positions in a +-20 km cube, at rest, maximum velocity log-uniform in [100, 3000] m/s, mass
+    log-uniform in [1e6, 1e9] kg, agility uniform in [0.1, 5], radius uniform in [20, 500] m, non-massive), each
+    FOLLOW or ORBIT of another ship at 500 - 30,000 m or GOTO a point in the cube; missiles of mass 10^U(3, 5) kg,
+    radius U(1, 6) m, maximum velocity U(3000, 8000) m/s, agility U(0.01, 0.2), each launched by a random ship at a
+    random other one."""
+    n = worlds * (ships + missiles)
+    rows = []
+    follow, orbit, goto = (np.zeros(n, dtype=bool) for _ in range(3))
+    target = np.full(n, -1, dtype=np.int64)
+    range_ = np.zeros(n)
+    point = np.zeros((n, 3))
+    leader, member, missile = (np.zeros(n, dtype=bool) for _ in range(3))
+    formation, leader_id, slot = (np.zeros(n, dtype=np.int64) for _ in range(3))
+    launch_target, launch_owner = np.zeros(n, dtype=np.int64), np.zeros(n, dtype=np.int64)
+    balls = []
+    for w in range(worlds):
+        r = random.Random(seed * 1_000_003 + w)
+        base = len(rows)
+        for j in range(ships):
+            rows.append({"id": j + 1, "world": w, "time": 0, "mass": 10.0 ** r.uniform(6.0, 9.0),
+                         "radius": r.uniform(20.0, 500.0), "max_vel": 10.0 ** r.uniform(2.0, math.log10(3000.0)),
+                         "pos": [r.uniform(-2e4, 2e4) for _ in range(3)], "vel": [0.0, 0.0, 0.0],
+                         "agility": r.uniform(0.1, 5.0), "speed_fraction": 1.0, "free": True, "massive": False,
+                         "interactive": j == 0 or r.random() < 0.5})
+            k = base + j
+            mode = r.choice((FOLLOW, ORBIT, GOTO)) if ships > 1 else GOTO
+            if mode == GOTO:
+                goto[k] = True
+                point[k] = [r.uniform(-2e4, 2e4) for _ in range(3)]
+            else:
+                other = r.randrange(ships - 1)
+                target[k] = base + (other if other < j else other + 1)
+                range_[k] = r.uniform(500.0, 30000.0)
+                (follow if mode == FOLLOW else orbit)[k] = True
+        if ships > 1 and r.random() < 0.5:                 # ship 1 leads a formation, ship 2 flies in a slot
+            leader[base] = True
+            formation[base] = r.randrange(len(COMBAT_FORMATIONS))
+            member[base + 1] = True
+            leader_id[base + 1] = 1
+            slot[base + 1] = r.randrange(len(COMBAT_FORMATIONS[formation[base]]))
+        for m in range(missiles):
+            k = len(rows)
+            owner = r.randrange(ships)
+            other = r.randrange(ships - 1) if ships > 1 else 0
+            tgt = (other if other < owner else other + 1) if ships > 1 else owner
+            ball = {"id": 101 + m, "mass": 10.0 ** r.uniform(3.0, 5.0), "radius": r.uniform(1.0, 6.0),
+                    "max_vel": r.uniform(3000.0, 8000.0), "free": True, "massive": False, "interactive": False,
+                    "pos": [0.0, 0.0, 0.0], "vel": [0.0, 0.0, 0.0], "agility": r.uniform(0.01, 0.2),
+                    "speed_fraction": 1.0, "max_ang_vel": r.uniform(0.5, 3.0), "rot_agility": r.uniform(0.2, 1.0)}
+            rows.append({"id": 101 + m, "world": w, "time": 0, "exists": False, "mass": 1.0, "radius": 1.0,
+                         "max_vel": 1.0, "pos": [0.0, 0.0, 0.0], "vel": [0.0, 0.0, 0.0], "agility": 1.0,
+                         "speed_fraction": 1.0})
+            missile[k] = True
+            balls.append(ball)
+            launch_target[k] = tgt + 1
+            launch_owner[k] = owner + 1
+    return CombatWorlds(rows, worlds, ships, missiles, follow, orbit, goto, target, range_, point, leader, formation,
+                        member, leader_id, slot, missile, balls, launch_target, launch_owner)

@@ -11,6 +11,13 @@
 // integers int64, flags bytes). The follower set of a ball is the rows whose follow_ptr is its row and whose follow
 // id is its id (vec_modes.py:37-47).
 //
+// With the combat park's state (exact_ballpark/vec_combat.py, full.py's missiles and formations) the same tick also
+// runs MISSILE (EvolveMissile, full.py:2337) and FORMATION (EvolveFormation, full.py:2359), the release of a missile
+// (non-massive, GotoDirection along its velocity) or a formation member (Stop, its slot freed on the master), each
+// massive normal missile's Potential with its target after every behaviour (counted: its response is not kept),
+// dynamical orientation disabled for missiles when asked (the old rotation kept, snapped to the velocity at the
+// commit), and the commit's dispatch counts (DoCollision with the target, the master's self-collision).
+//
 // Arithmetic: plain C++ double and float operations (built with -ffp-contract=off: each one IEEE-rounded, nothing
 // fused), glibc 2.34 aarch64's libm through ebb_libm.cuh's host build (pinned separately to the reference's
 // transcriptions by tests/test_libm_oracle.py).
@@ -27,14 +34,29 @@ namespace {
 namespace lm = ebb::lm;
 
 // Destiny's modes (IDstConstants.h; modes.py:65-67)
-constexpr int64_t GOTO = 0, FOLLOW = 1, STOP = 2, WARP = 3, ORBIT = 4, MISSILE = 5, TROLL = 8, RIGID = 11;
+constexpr int64_t GOTO = 0, FOLLOW = 1, STOP = 2, WARP = 3, ORBIT = 4, MISSILE = 5, MUSHROOM = 6, TROLL = 8;
+constexpr int64_t MINIBALL = 9, RIGID = 11, FORMATION = 12;
 constexpr double STOP_DAMP = 0.9345794392523364485981308411215;   // ref.py:48
 constexpr double AU = .1495978707e12;                              // modes.py:72
 constexpr double ORBITAL_PRECESSION = 0.001;                       // modes.py:73
 constexpr double WARP_AU_PER_S = 0.001, WARP_ACC = 1.0 / 1000, WARP_DEC = 1.0 / 3000;   // modes.py:74-76
 constexpr int64_t MAX_ALIGN_TICKS = 180;                           // modes.py:77
 
+// The combat park's state beside the flight fields (vec_combat.py:151-170): which rows hold a ball, a leader's
+// formation and slot bits, a missile's owner row, the tick's counts, the bubbles and cloaks, the formation table
+struct Combat {
+    uint8_t* exists;
+    int64_t *formation_id, *formation_slots, *owner_ptr, *hits_n, *ev_n;
+    uint8_t* ev_self;
+    int64_t *bubble, *cloaked, *flags;
+    const double* formations;
+    const int64_t* formation_len;
+    int64_t n_formations, max_slots, tick_ms;
+    int32_t do_missiles_off, master;
+};
+
 struct Park {
+    Combat* c = nullptr;
     int64_t n;
     double friction, dt;
     float ffriction, fdt;
@@ -297,6 +319,8 @@ void apply_torque(F4 rotation, F3 angvel, F3 torque, float roll, float tau, floa
     *w_out = w;
 }
 
+void snap_one(const double* v, double* rot, double* old_rot, double* w, double* old_w);
+
 // ============================================================================================= the tick
 
 struct Tick {
@@ -333,15 +357,38 @@ struct Tick {
     // Stop(Ball*) (modes.py:206)
     void stop_ball(int64_t i) {
         const int64_t m = p.mode[i];
-        if (m == FOLLOW || m == ORBIT || m == MISSILE || m == 12) {
+        if (p.c && p.c->master && m == FORMATION) free_slot(i);
+        if (m == FOLLOW || m == ORBIT || m == MISSILE || m == FORMATION) {
             p.effect_stamp[i] = 0;
             p.follow_ptr[i] = -1;
             p.follow_id[i] = 0;
             p.owner_id[i] = 0;
             p.follow_range[i] = 0.0;
+            if (p.c) p.c->owner_ptr[i] = -1;
         }
         p.mode[i] = STOP;
     }
+    // On the master, Stop(Ball*) of a FORMATION member frees its slot in the leader (Ballpark.cpp:4629-4633;
+    // Ball::FreeFormationSlot((size_t) mEffectStamp), Ball.cpp:2324): nothing without a loaded formation or past its
+    // end; a negative formation index or a slot of 16 or more flagged
+    void free_slot(int64_t i) {
+        const int64_t t = p.follow_ptr[i];
+        if (t < 0 || t >= p.n) return;
+        const int64_t fid = p.c->formation_id[t];
+        if (fid == -1 || fid > p.c->n_formations - 1) return;
+        if (fid < 0) {
+            p.c->flags[i] |= 2;
+            return;
+        }
+        const uint64_t len = (uint64_t)p.c->formation_len[fid], slot = (uint64_t)p.effect_stamp[i];
+        if (slot > len - 1) return;
+        if (slot >= 16) {
+            p.c->flags[i] |= 2;
+            return;
+        }
+        p.c->formation_slots[t] &= ~(int64_t)(1ULL << slot);
+    }
+    bool disabled(int64_t i) const { return p.c && p.c->do_missiles_off && p.mode[i] == MISSILE; }
     // GotoDirection(Ball*) (modes.py:252) with GotoPoint(Ball*) (modes.py:238)
     void goto_direction(int64_t i, V d) {
         if (!finite3(d)) return;
@@ -358,6 +405,7 @@ struct Tick {
     void stop_all_followers(int64_t w, const std::vector<int64_t>& rows) {
         for (int64_t f : rows) {
             if (p.follow_ptr[f] != w || p.follow_id[f] != p.ids[w]) continue;
+            if (p.c && !p.c->exists[f]) continue;
             if (p.mode[f] == MISSILE || (p.interactive[f] && p.mode[f] == ORBIT)) {
                 if (p.mode[f] == MISSILE) p.massive[f] = 0;
                 goto_direction(f, ld(p.vel, f));
@@ -582,6 +630,101 @@ struct Tick {
         const F3 h = f3mul(heading, cosangle * cosangle * accel);
         return V{h.x, h.y, h.z};
     }
+    // EvolveMissile (full.py:2337; Ballpark.cpp:972): straight on toward mGoto while (time - launch) x tick is at most
+    // 800 ms, then the lead point (the target's position plus its velocity times dist / maxVel, offset along the line
+    // from it by followRange + both radii) at full thrust, never tapered
+    V evolve_missile(int64_t i, int64_t o) {
+        if ((p.clock[i] - p.effect_stamp[i]) * p.c->tick_ms <= 800) return goto_thrust(i, ld(p.goto_, i));
+        const V op = ld(p.pos, o), ov = ld(p.vel, o);
+        const V delta = sub(ld(p.pos, i), op);
+        const double dist = length(delta);
+        const double ct = dist / p.max_vel[i];
+        V target = V{op.x + ov.x * ct, op.y + ov.y * ct, op.z + ov.z * ct};
+        const double r = p.follow_range[i] + p.radius[i] + p.radius[o];
+        if (dist == 0.0) {
+            target = V{op.x + 1.0 * r, op.y + 0.0 * r, op.z + 0.0 * r};
+        } else {
+            const double inv = 1.0 / dist;
+            target = V{target.x + delta.x * r * inv, target.y + delta.y * r * inv, target.z + delta.z * r * inv};
+        }
+        st(p.goto_, i, target);
+        const double max_thrust = p.friction * p.speed_fraction[i] * p.max_vel[i] / (p.mass[i] * p.agility[i]);
+        return scl(normalized(sub(target, ld(p.pos, i))), max_thrust);
+    }
+    // EvolveFormation (full.py:2359; Ballpark.cpp:1023): the leader's slot offset scaled to both radii plus its
+    // length, turned by the leader's rotation as floats, at the leader's position; GotoThrust toward it
+    V evolve_formation(int64_t i, int64_t o) {
+        const int64_t fid = p.c->formation_id[o];
+        if (fid < 0 || fid > p.c->n_formations - 1) return V{0, 0, 0};
+        const int64_t slot = (int64_t)(int8_t)(uint8_t)(p.effect_stamp[i] & 0xFF);
+        if (slot > p.c->formation_len[fid] - 1 || slot < 0) return V{0, 0, 0};
+        const double* f = p.c->formations + (fid * p.c->max_slots + slot) * 3;
+        const V offset = V{f[0], f[1], f[2]};
+        double len = length(offset);
+        if (len == 0.0) len = 1.0;
+        const double k = p.radius[i] + p.radius[o] + len;
+        const double inv = 1.0 / len;
+        const F3 vec = F3{(float)(offset.x * k * inv), (float)(offset.y * k * inv), (float)(offset.z * k * inv)};
+        const F3 rv = tcoord(vec, mrot(rot_of(o)));
+        const V op = ld(p.pos, o);
+        const V g = V{op.x + (double)rv.x, op.y + (double)rv.y, op.z + (double)rv.z};
+        st(p.goto_, i, g);
+        return goto_thrust(i, g);
+    }
+    // CollideTwoSpheres (Collision.cpp:108): 0 if touching, the earlier root in [0, 1], else -1
+    static double spheres(V p0, V p1, V q0, V q1, double cr) {
+        const V d = sub(p0, q0);
+        const double d2 = lensq(d);
+        if (d2 <= cr * cr) return 0.0;
+        const V e = V{(p1.x - p0.x) - (q1.x - q0.x), (p1.y - p0.y) - (q1.y - q0.y), (p1.z - p0.z) - (q1.z - q0.z)};
+        const double a = lensq(e);
+        const double b = 2.0 * (d.x * e.x + d.y * e.y + d.z * e.z);
+        const double c = d2 - cr * cr;
+        if (a == 0.0 && b == 0.0) return -1.0;
+        double det = b * b - 4.0 * a * c;
+        if (det < 0.0) return -1.0;
+        det = std::sqrt(det);
+        const double s2 = ((-b - det) * 0.5) / a;
+        return (s2 >= 0.0 && s2 <= 1.0) ? s2 : -1.0;
+    }
+    // Potential(missile, target, depth) (Ballpark.cpp:2789; space.py's _potential): the target ids appended
+    int64_t potential(int64_t i, int64_t t, V pi, V pt, int depth) {
+        const double m1 = p.mass[i] * p.agility[i];
+        const bool other_free = p.free_[t] != 0;
+        const double m2 = other_free ? p.mass[t] * p.agility[t] : 1.0e34;
+        V p1 = pi, v1 = ld(p.vel, i), q1 = pt, w1 = ld(p.vel, t);
+        integrate(&p1, &v1, ld(p.last_g, i), m1, p.time_factor[i]);
+        integrate(&q1, &w1, ld(p.last_g, t), m2, p.time_factor[t]);
+        const double cr = p.radius[i] + p.radius[t];
+        const double s = spheres(pi, p1, pt, q1, cr);
+        if (s == -1.0) return 0;
+        if (s > 0.0) return 1;
+        if (!other_free || depth >= 2) return 1;
+        const V d = sub(pt, pi);
+        const double d2 = lensq(d);
+        const V normal = d2 == 0.0 ? V{p.ids[i] > p.ids[t] ? 1.0 : -1.0, 0.0, 0.0} : normalized(d);
+        const double dist = (cr - std::sqrt(d2)) + 1.0;
+        const double d1 = m2 / (m1 + m2) * dist, dd2 = m1 / (m1 + m2) * dist;
+        const V pp = V{pi.x - normal.x * d1, pi.y - normal.y * d1, pi.z - normal.z * d1};
+        const V qq = V{pt.x + normal.x * dd2, pt.y + normal.y * dd2, pt.z + normal.z * dd2};
+        const int64_t inner = potential(i, t, pp, qq, depth + 1);
+        const V rel = sub(ld(p.vel, i), ld(p.vel, t));
+        if (lensq(rel) > 0.0001) return inner;
+        return inner + 1;
+    }
+    // The gradient of a massive normal missile: its one candidate is its target in its bubble, less Gradient's skips
+    int64_t missile_contacts(int64_t i) {
+        const int64_t t = p.follow_ptr[i];
+        if (!(live(i) && p.massive[i] && p.mode[i] == MISSILE && p.owner_id[i] >= 0 && t >= 0 && t < p.n &&
+              p.c->bubble[i] == p.c->bubble[t]))
+            return 0;
+        const int64_t mt = p.mode[t], own = p.owner_id[i];
+        if (p.ids[t] == own || (mt == MINIBALL && p.owner_id[t] == own) ||
+            ((mt == MISSILE || mt == MUSHROOM) && p.ids[i] == p.owner_id[t]) ||
+            (mt == MISSILE && p.ids[i] == p.follow_id[t]))
+            return 0;
+        return potential(i, t, ld(p.pos, i), ld(p.pos, t), 0);
+    }
     // EvolveBehaviorForBall (modes.py:359, full.py:2416)
     void behaviour(int64_t i, const std::vector<int64_t>& rows) {
         st(p.last_g, i, V{0, 0, 0});
@@ -600,16 +743,20 @@ struct Tick {
             }
         } else if (m == GOTO) {
             a = goto_thrust(i, ld(p.goto_, i));
-        } else if ((m == FOLLOW || m == ORBIT) && !has_target) {
+        } else if ((m == FOLLOW || m == ORBIT || m == MISSILE || m == FORMATION) && !has_target) {
             a = V{0, 0, 0};
         } else if (m == FOLLOW) {
             a = evolve_follow(i, o);
         } else if (m == ORBIT) {
             a = p.new_orbit ? evolve_new_orbit(i, o) : evolve_old_orbit(i, o);
+        } else if (m == MISSILE) {
+            a = evolve_missile(i, o);
+        } else if (m == FORMATION) {
+            a = evolve_formation(i, o);
         } else if (m == STOP) {
             if (!p.dynamical) p.vel[3 * i + 1] = (p.vel[3 * i + 1] - 0.07 * p.vel[3 * i + 1]) * STOP_DAMP;
         }
-        if (p.dynamical) a = orient(i, a);
+        if (p.dynamical && !disabled(i)) a = orient(i, a);
         st(p.last_g, i, a);
     }
     // Ballpark::Integrate over one tick (ref.py:354)
@@ -683,6 +830,8 @@ struct Tick {
         // (1) behaviours, ascending id
         for (int64_t i : rows)
             if (live(i)) behaviour(i, rows);
+        if (p.c)                                // the missiles' contacts with their targets, after every behaviour
+            for (int64_t i : rows) p.c->hits_n[i] = missile_contacts(i);
         // (3) end-of-tick states into temporaries, and the rotation a tick on
         const size_t k = rows.size();
         std::vector<V> np(k), nv(k);
@@ -710,7 +859,11 @@ struct Tick {
             }
             np[j] = pv;
             nv[j] = vv;
-            if (p.dynamical) {
+            if (p.dynamical && disabled(i)) {  // phase 3 leaves a disabled missile's mOldRot as it was
+                nrot[j] = F4{ff(p.old_rot, 4 * i), ff(p.old_rot, 4 * i + 1), ff(p.old_rot, 4 * i + 2),
+                             ff(p.old_rot, 4 * i + 3)};
+                nw[j] = F3{ff(p.old_ang_vel, 3 * i), ff(p.old_ang_vel, 3 * i + 1), ff(p.old_ang_vel, 3 * i + 2)};
+            } else if (p.dynamical) {
                 const F3 tq = F3{ff(p.torque, 3 * i), ff(p.torque, 3 * i + 1), ff(p.torque, 3 * i + 2)};
                 apply_torque(rot_of(i), w_of(i), tq, ff(p.rot_roll, i), tau(i), p.fdt, &nrot[j], &nw[j]);
             }
@@ -718,7 +871,12 @@ struct Tick {
         // (4) the commit; PetrifyTroll of the trolls due; the clock
         for (size_t j = 0; j < k; ++j) {
             const int64_t i = rows[j];
+            if (p.c) {
+                p.c->ev_n[i] = 0;
+                p.c->ev_self[i] = 0;
+            }
             if (live(i)) {
+                const V before = ld(p.pos, i);
                 st(p.old_pos, i, ld(p.pos, i));
                 st(p.old_vel, i, ld(p.vel, i));
                 st(p.pos, i, np[j]);
@@ -741,6 +899,20 @@ struct Tick {
                     for (int c = 0; c < 3; ++c) {
                         p.ang_vel[3 * i + c] = ww[c];
                         p.old_ang_vel[3 * i + c] = ow[c];
+                    }
+                    if (disabled(i))            // SnapOrientation of a disabled missile (phase 4)
+                        snap_one(p.vel + 3 * i, p.rot + 4 * i, p.old_rot + 4 * i, p.ang_vel + 3 * i,
+                                 p.old_ang_vel + 3 * i);
+                }
+                if (p.c && p.mode[i] == MISSILE && !(lensq(sub(ld(p.pos, i), before)) < 0.1)) {
+                    // DispatchCollisions (Ballpark.cpp:600-639): the target ids, then on the master a collision with
+                    // itself when its owner is gone, cloaked or in another bubble
+                    p.c->ev_n[i] = p.c->hits_n[i];
+                    if (p.c->master) {
+                        const int64_t o = p.c->owner_ptr[i];
+                        const bool gone = o < 0 || o >= p.n || !p.c->exists[o];
+                        p.c->ev_self[i] = (gone || (p.c->bubble[o] != p.c->bubble[i] && p.c->bubble[i] != -1) ||
+                                           p.c->cloaked[o] != 0) ? 1 : 0;
                     }
                 }
                 if (p.mode[i] == TROLL && !(p.effect_stamp[i] > p.clock[i])) {   // TrollReady, PetrifyTroll
@@ -808,7 +980,43 @@ struct OracleFlight {
 };
 
 // One tick of every world in place, the worlds shared among `threads` host threads. Returns 0.
+// The combat park's extra state (the Combat structure above, field for field).
+struct OracleCombat {
+    uint8_t* exists;
+    int64_t *formation_id, *formation_slots, *owner_ptr, *hits_n, *ev_n;
+    uint8_t* ev_self;
+    int64_t *bubble, *cloaked, *flags;
+    const double* formations;
+    const int64_t* formation_len;
+    int64_t n_formations, max_slots, tick_ms;
+    int32_t do_missiles_off, master;
+};
+
+// One tick of every world of a combat park in place (dynamical orientation on), `threads` host threads. Returns 0.
+int oracle_combat_tick_mt(const OracleFlight* s, const OracleCombat* c, int threads);
+
+static Park park_of(const OracleFlight* s);
+
 int oracle_flight_tick_mt(const OracleFlight* s, int threads) {
+    Park p = park_of(s);
+    Tick(p).run(threads);
+    return 0;
+}
+
+int oracle_combat_tick_mt(const OracleFlight* s, const OracleCombat* c, int threads) {
+    Park p = park_of(s);
+    Combat cx;
+    cx.exists = c->exists; cx.formation_id = c->formation_id; cx.formation_slots = c->formation_slots;
+    cx.owner_ptr = c->owner_ptr; cx.hits_n = c->hits_n; cx.ev_n = c->ev_n; cx.ev_self = c->ev_self;
+    cx.bubble = c->bubble; cx.cloaked = c->cloaked; cx.flags = c->flags; cx.formations = c->formations;
+    cx.formation_len = c->formation_len; cx.n_formations = c->n_formations; cx.max_slots = c->max_slots;
+    cx.tick_ms = c->tick_ms; cx.do_missiles_off = c->do_missiles_off; cx.master = c->master;
+    p.c = &cx;
+    Tick(p).run(threads);
+    return 0;
+}
+
+static Park park_of(const OracleFlight* s) {
     Park p;
     p.n = s->n;
     p.friction = s->friction;
@@ -826,12 +1034,12 @@ int oracle_flight_tick_mt(const OracleFlight* s, int threads) {
     p.effect_stamp = s->effect_stamp; p.follow_id = s->follow_id; p.owner_id = s->owner_id;
     p.follow_ptr = s->follow_ptr; p.clock = s->clock; p.free_ = s->free_; p.moribund = s->moribund;
     p.massive = s->massive; p.interactive = s->interactive; p.sensor = s->sensor;
-    Tick(p).run(threads);
-    return 0;
+    return p;
 }
 
 // One tick of every world in place, on the calling thread. Returns 0.
 int oracle_flight_tick(const OracleFlight* s) { return oracle_flight_tick_mt(s, 1); }
+
 
 }  // extern "C"
 

@@ -37,6 +37,7 @@ def lib():
         _lib.oracle_libm.argtypes = [ctypes.c_int, i64, p, p, p]
         _lib.oracle_flight_tick.argtypes = [p]
         _lib.oracle_flight_tick_mt.argtypes = [p, ctypes.c_int]
+        _lib.oracle_combat_tick_mt.argtypes = [p, p, ctypes.c_int]
         _lib.oracle_snap.argtypes = [i64, p, p, p, p, p, p]
         _lib.oracle_q_rot_mul.argtypes = [i64, p, p, p, p]
     return _lib
@@ -202,8 +203,11 @@ class OraclePark:
     def _a(x) -> np.ndarray:
         return np.asarray(x.cpu() if hasattr(x, "cpu") else x)
 
+    def _following(self) -> np.ndarray:
+        return (self.mode == FOLLOW) | (self.mode == ORBIT)
+
     def _stop_rows(self, mask: np.ndarray) -> None:
-        follower = mask & ((self.mode == FOLLOW) | (self.mode == ORBIT))
+        follower = mask & self._following()
         self.effect_stamp = np.where(follower, 0, self.effect_stamp)
         self.follow_ptr = np.where(follower, -1, self.follow_ptr)
         self.follow_id = np.where(follower, 0, self.follow_id)

@@ -96,6 +96,11 @@ def make_park(park_cls, cfg: dict, formations: list, device, **extra):
 
 # ---- the driver ----
 
+def _t(x, dev) -> torch.Tensor:
+    """A park's per-row array as a tensor (the oracle's parks hold numpy arrays)."""
+    return x if isinstance(x, torch.Tensor) else torch.as_tensor(np.asarray(x), device=dev)
+
+
 def _one_kind(p, op: str, group: dict, where: dict, n: int, answers: list, dev) -> None:
     """The records `group` {world: record} of one kind, as one masked command (or, for the slot calls, one call a
     world in world order)."""
@@ -149,7 +154,7 @@ def _one_kind(p, op: str, group: dict, where: dict, n: int, answers: list, dev) 
     m = torch.tensor(mask, dtype=BOOL, device=dev)
     A, B, C, D = (torch.tensor(ints[k], dtype=I64, device=dev) for k in range(4))
     V = torch.tensor(vec, dtype=F64, device=dev)
-    live = m & p.exists
+    live = m & _t(p.exists, dev)
     if op == "goto":
         p.goto_point(live, V)
     elif op == "dir":
@@ -161,7 +166,7 @@ def _one_kind(p, op: str, group: dict, where: dict, n: int, answers: list, dev) 
     elif op == "vel":
         p.set_velocity(live, V)
     elif op == "massive":
-        p.massive = torch.where(live, A != 0, p.massive)
+        p.massive = torch.where(live, A != 0, _t(p.massive, dev))
     elif op == "launch":
         p.launch_missile(m, A, B, C, D)
     elif op == "mfollow":
@@ -185,7 +190,7 @@ def drive(p, cfg: dict, where: dict, on_step=None, tick=None) -> dict:
     collider)]}. on_step(step, park) after each step's records and tick; tick(park) replaces p.evolve()."""
     W = len(cfg["worlds"])
     n = p.n
-    dev = p.exists.device
+    dev = p.dev
     answers = [[] for _ in range(W)]
     events = []
     by_step = [defaultdict(list) for _ in range(W)]

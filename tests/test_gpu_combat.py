@@ -26,3 +26,44 @@ def test_the_gpu_combat_park_replays_the_golden_batches(seed):
         if bad:
             failures.append((bi, bad[:2]))
     assert not failures, f"{len(failures)} of {len(batches)} batches differ, first {failures[:2]}"
+
+
+def test_the_gpu_combat_park_matches_the_oracle_on_the_benchmark_worlds():
+    """The combat benchmark's worlds (workloads.combat_worlds: 4 ships and 4 missiles launched aimed and massive, ships
+    following, orbiting, flying to points, in formation) at 512 worlds, 60 ticks: every field of every row holding a
+    ball after every 10th tick and every tick's events, GPU against the CPU oracle; then a CUDA graph's replays
+    against eager ticks, bit for bit."""
+    from exact_ballpark_b200 import CombatGraph, VecCombatPark
+    from exact_ballpark_b200.workloads import combat_worlds
+    from oracle.combat_park import OracleCombatPark
+    w = combat_worlds(7, 512)
+    n = len(w.rows)
+    g = VecCombatPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    o = OracleCombatPark(n, dynamical_orientation=True, use_new_orbit=True)
+    for p in (g, o):
+        p.load(w.rows)
+        w.apply(p)
+    events = 0
+    for k in range(1, 61):
+        g.evolve()
+        o.evolve()
+        ge, oe = g.events(), o.events()
+        assert ge == oe, f"tick {k}: events differ"
+        events += len(ge)
+        if k % 10 == 0:
+            want, got = ct.field_digests(o), ct.field_digests(g)
+            assert not ct.first_mismatch(want, got), f"tick {k}: {ct.first_mismatch(want, got)}"
+    g.check()
+    assert events > 1000
+    h = VecCombatPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    h.load(w.rows)
+    w.apply(h)
+    e = VecCombatPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    e.load(w.rows)
+    w.apply(e)
+    graph = CombatGraph(h)
+    for k in range(20):
+        graph.tick()
+        e.evolve()
+        assert h.events() == e.events()
+    assert not ct.first_mismatch(ct.field_digests(e), ct.field_digests(h))
