@@ -39,6 +39,13 @@ class CombatState(ctypes.Structure):
                    ("do_missiles_off", ctypes.c_int32), ("master", ctypes.c_int32)])
 
 
+class ComposedState(ctypes.Structure):
+    """include/ebb.h's EbbComposedState, field for field."""
+    _fields_ = ([("combat", CombatState)]
+                + [(k, ctypes.c_void_p) for k in ("world", "last_c", "level", "key", "mod", "hits")]
+                + [("hit_cap", ctypes.c_int64)])
+
+
 def lib() -> ctypes.CDLL:
     """The loaded library (loaded and checked on first use)."""
     global _lib
@@ -65,6 +72,8 @@ def lib() -> ctypes.CDLL:
     L.ebb_collide_tick.argtypes = [p, p, p, p]
     L.ebb_collide_load.argtypes = [p, p, p]
     L.ebb_combat_tick.argtypes = [ctypes.POINTER(CombatState), p, i64, p, p, i32]
+    L.ebb_composed_tick.argtypes = [ctypes.POINTER(ComposedState), p, i64, p, p, i32]
+    L.ebb_composed_file.argtypes = [ctypes.POINTER(ComposedState), p, p, p, p, p]
     L.ebb_glibc_srand.argtypes = [p, i64, p, p]
     L.ebb_glibc_rand.argtypes = [p, i64, i64, p, p]
     L.ebb_flight_snap.argtypes = [ctypes.POINTER(FlightState), p, i32, p, i32]

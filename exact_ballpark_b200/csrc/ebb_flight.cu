@@ -641,6 +641,7 @@ __global__ void libm_kernel(int func, int64_t n, const double* __restrict__ x, c
 namespace ebb {
 namespace combat {
 cudaError_t kernel_attributes(cudaFuncAttributes* fa);   // ebb_combat.cu
+cudaError_t composed_attributes(cudaFuncAttributes* fa);
 }
 }  // namespace ebb
 
@@ -796,6 +797,7 @@ int ebb_kernel_info(int which, int* regs, int* local_bytes, int* binary_version,
         case 6: e = cudaFuncGetAttributes(&fa, ebb::flight::worlds_kernel<false>); break;
         case 4: e = cudaFuncGetAttributes(&fa, ebb::flight::move_kernel); break;
         case 7: e = ebb::combat::kernel_attributes(&fa); break;
+        case 8: e = ebb::combat::composed_attributes(&fa); break;
         default: return EBB_EINVAL;
     }
     if (e != cudaSuccess) return (int)e;

@@ -392,14 +392,16 @@ class CombatWorlds:
         park.launch_missile(t(self.missile), t(self.launch_target), t(self.launch_owner), one, one)
 
 
-def combat_worlds(seed: int, worlds: int, ships: int = 4, missiles: int = 4) -> CombatWorlds:
+def combat_worlds(seed: int, worlds: int, ships: int = 4, missiles: int = 4, spheres: int = 0,
+                  massive: bool = False, cube: float = 2e4) -> CombatWorlds:
     """W combat worlds (CombatWorlds); world w drawn from random.Random(seed * 1_000_003 + w): ships as the flight
     benchmark's (positions in a +-20 km cube, at rest, maximum velocity log-uniform in [100, 3000] m/s, mass
     log-uniform in [1e6, 1e9] kg, agility uniform in [0.1, 5], radius uniform in [20, 500] m, non-massive), each
     FOLLOW or ORBIT of another ship at 500 - 30,000 m or GOTO a point in the cube; missiles of mass 10^U(3, 5) kg,
     radius U(1, 6) m, maximum velocity U(3000, 8000) m/s, agility U(0.01, 0.2), each launched by a random ship at a
-    random other one."""
-    n = worlds * (ships + missiles)
+    random other one. For the composed park: `massive` ships, `spheres` fixed massive spheres a world (ids after the
+    ships; radius log-uniform in [10, 5000] m, mass log-uniform in [1e8, 1e11] kg) and a smaller `cube`."""
+    n = worlds * (ships + spheres + missiles)
     rows = []
     follow, orbit, goto = (np.zeros(n, dtype=bool) for _ in range(3))
     target = np.full(n, -1, dtype=np.int64)
@@ -415,14 +417,14 @@ def combat_worlds(seed: int, worlds: int, ships: int = 4, missiles: int = 4) -> 
         for j in range(ships):
             rows.append({"id": j + 1, "world": w, "time": 0, "mass": 10.0 ** r.uniform(6.0, 9.0),
                          "radius": r.uniform(20.0, 500.0), "max_vel": 10.0 ** r.uniform(2.0, math.log10(3000.0)),
-                         "pos": [r.uniform(-2e4, 2e4) for _ in range(3)], "vel": [0.0, 0.0, 0.0],
-                         "agility": r.uniform(0.1, 5.0), "speed_fraction": 1.0, "free": True, "massive": False,
+                         "pos": [r.uniform(-cube, cube) for _ in range(3)], "vel": [0.0, 0.0, 0.0],
+                         "agility": r.uniform(0.1, 5.0), "speed_fraction": 1.0, "free": True, "massive": massive,
                          "interactive": j == 0 or r.random() < 0.5})
             k = base + j
             mode = r.choice((FOLLOW, ORBIT, GOTO)) if ships > 1 else GOTO
             if mode == GOTO:
                 goto[k] = True
-                point[k] = [r.uniform(-2e4, 2e4) for _ in range(3)]
+                point[k] = [r.uniform(-cube, cube) for _ in range(3)]
             else:
                 other = r.randrange(ships - 1)
                 target[k] = base + (other if other < j else other + 1)
@@ -434,6 +436,11 @@ def combat_worlds(seed: int, worlds: int, ships: int = 4, missiles: int = 4) -> 
             member[base + 1] = True
             leader_id[base + 1] = 1
             slot[base + 1] = r.randrange(len(COMBAT_FORMATIONS[formation[base]]))
+        for q in range(spheres):
+            rows.append({"id": ships + q + 1, "world": w, "time": 0, "mass": 10.0 ** r.uniform(8.0, 11.0),
+                         "radius": 10.0 ** r.uniform(1.0, math.log10(5000.0)), "max_vel": 0.0,
+                         "pos": [r.uniform(-cube, cube) for _ in range(3)], "vel": [0.0, 0.0, 0.0], "agility": 1.0,
+                         "speed_fraction": 0.0, "free": False, "massive": True, "interactive": False})
         for m in range(missiles):
             k = len(rows)
             owner = r.randrange(ships)
@@ -452,3 +459,9 @@ def combat_worlds(seed: int, worlds: int, ships: int = 4, missiles: int = 4) -> 
             launch_owner[k] = owner + 1
     return CombatWorlds(rows, worlds, ships, missiles, follow, orbit, goto, target, range_, point, leader, formation,
                         member, leader_id, slot, missile, balls, launch_target, launch_owner)
+
+
+def composed_worlds(seed: int, worlds: int, ships: int = 6, missiles: int = 2, spheres: int = 1) -> CombatWorlds:
+    """The composed benchmark's worlds (its shape: 6 ships, 2 missiles and 1 sphere a world): combat_worlds with
+    massive ships in a +-5 km cube and fixed massive spheres among them, so ships, spheres and missiles meet."""
+    return combat_worlds(seed, worlds, ships, missiles, spheres, massive=True, cube=5e3)

@@ -88,6 +88,21 @@ typedef struct EbbCombatState {
     int32_t do_missiles_off, master;
 } EbbCombatState;
 
+/* The composed park (exact_ballpark.vec_composed.VecComposedPark: the combat park with the gradient method's collisions
+ * between every massive ball, missiles included): the combat state and, per row, its world label (a world's rows are
+ * contiguous), the collision acceleration mLastC [3][n], the partition's filing (level [n], key and adjacent side
+ * [3][n]) and the collision list [n][hit_cap] (hit_cap = 3 (S - 1) + 1 for worlds of at most S rows: three appends a
+ * candidate and the master's self-collision). */
+#define EBB_COMPOSED_FLAG_WARP_MASSIVE 64
+#define EBB_COMPOSED_FLAG_PARTITION 128
+typedef struct EbbComposedState {
+    EbbCombatState combat;
+    const int64_t* world;
+    double* last_c;
+    int64_t *level, *key, *mod, *hits;
+    int64_t hit_cap;
+} EbbComposedState;
+
 /* The ABI version (EBB_ABI_VERSION). Replaces xbpm_abi / xbpo_abi (exact_ballpark/vec_modes_cuda.cu:750,
  * vec_orient_cuda.cu:499). */
 int ebb_abi(void);
@@ -185,6 +200,24 @@ int ebb_collide_load(const EbbCollideState* s, int32_t* status, void* stream);
 int ebb_combat_tick(const EbbCombatState* s, const int64_t* tile_rows, int64_t tiles, int32_t* status, void* stream,
                     int block);
 
+/* One tick of the composed park in place, in tiles of whole worlds as ebb_combat_tick: the records pass, phase 1 (the
+ * live balls' collision lists cleared), the warp paths with the drop-outs (re-filed at rest), the gradient for every
+ * live massive ball in its world (GetNearbyBalls' candidates in the partition's walk order with a normal missile's
+ * target its one candidate, Potential's recursion, COL-711's missile exception, the later-impact rule, the collision
+ * list), then phases 3 and 4 with mLastG + mLastC, the re-filing of the balls that moved, the dispatch and the
+ * master's self-collision appended; flags FLAG_WARP_MASSIVE and FLAG_PARTITION on the rows. Replaces
+ * xbpp_tick (exact_ballpark/vec_composed_cuda.cu:421-509: its thirteen launches), which
+ * exact_ballpark.vec_composed_cuda.tick calls. */
+int ebb_composed_tick(const EbbComposedState* s, const int64_t* tile_rows, int64_t tiles, int32_t* status,
+                      void* stream, int block);
+
+/* Ball::InsertInBoxes' outcome (level, key, adjacent side) for the rows in `mask` ([n] bytes), from each row's state
+ * or the given position, velocity ([3][n] planes) and speed fraction ([n] floats), any of them null for the row's
+ * own; a filing the reference refuses (a key at the grid's edge, a ball wider than a top box) raises
+ * EBB_COMPOSED_FLAG_PARTITION on the row. Replaces VecComposedPark._file (vec_composed.py:330-345). */
+int ebb_composed_file(const EbbComposedState* s, const uint8_t* mask, const double* pos, const double* vel,
+                      const float* sf, void* stream);
+
 /* glibc 2.34's rand() after srand(seed) (random_r, TYPE_3), one generator a world: a world's state is EBB_RAND_WORDS
  * int32 (the 31-word table, then the front and rear indices). ebb_glibc_srand seeds worlds[W] states from seeds[W]
  * (srandom_r, its 310 discarded draws included); ebb_glibc_rand draws `draws` values a world into out[W][draws],
@@ -212,7 +245,7 @@ int ebb_flight_decay(const EbbFlightState* s, const uint8_t* mask, double neg_kd
 int ebb_libm(int func, int64_t n, const double* x, const double* y, double* out, void* stream, int block);
 
 /* A kernel's resources as loaded on the current device: which 0 the plain tick, 1 the prepass, 2 the tiled tick,
- * 3 the listed-worlds tick, 4 the row move, 7 the combat tick.
+ * 3 the listed-worlds tick, 4 the row move, 7 the combat tick, 8 the composed tick.
  * Replaces xbpm_info (vec_modes_cuda.cu:766). */
 int ebb_kernel_info(int which, int* regs, int* local_bytes, int* binary_version, int* ptx_version, int* max_threads);
 

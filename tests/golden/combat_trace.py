@@ -49,12 +49,27 @@ def canonical(t) -> np.ndarray:
     return np.ascontiguousarray(a.to(torch.int64).numpy())
 
 
-def field_digests(park) -> np.ndarray:
-    """[len(FIELDS) + 1] uint64: each field's digest over the rows holding a ball, then `exists` over every row."""
+COMPOSED_FIELDS = FIELDS + ("last_c", "level", "key", "mod", "hits_n", "collisions")
+LIST_WIDTH = 192                    # a collision list as a digest holds it: its entries, then -1 up to this width
+
+
+def _field(park, f: str) -> np.ndarray:
+    if f != "collisions":
+        return canonical(getattr(park, f))
+    hits, n = canonical(park.hits), canonical(park.hits_n)
+    out = np.full((hits.shape[0], LIST_WIDTH), -1, dtype=np.int64)
+    for r in np.nonzero(n)[0].tolist():
+        out[r, :n[r]] = hits[r, :n[r]]
+    return out
+
+
+def field_digests(park, fields: tuple = FIELDS) -> np.ndarray:
+    """[len(fields) + 1] uint64: each field's digest over the rows holding a ball, then `exists` over every row (the
+    collision list as its entries, padded with -1 to LIST_WIDTH)."""
     exists = canonical(park.exists).astype(bool)
-    out = np.zeros(len(FIELDS) + 1, dtype=np.uint64)
-    for i, f in enumerate(FIELDS):
-        a = canonical(getattr(park, f))[exists]
+    out = np.zeros(len(fields) + 1, dtype=np.uint64)
+    for i, f in enumerate(fields):
+        a = _field(park, f)[exists]
         h = hashlib.sha256(f.encode() + str(a.shape).encode() + a.tobytes()).digest()
         out[i] = np.frombuffer(h[:8], dtype=np.uint64)[0]
     e = exists.astype(np.int64)
@@ -62,8 +77,8 @@ def field_digests(park) -> np.ndarray:
     return out
 
 
-def first_mismatch(want: np.ndarray, got: np.ndarray) -> list:
-    names = FIELDS + ("exists",)
+def first_mismatch(want: np.ndarray, got: np.ndarray, fields: tuple = FIELDS) -> list:
+    names = fields + ("exists",)
     return [names[i] for i in range(len(names)) if want[i] != got[i]]
 
 
@@ -151,6 +166,12 @@ def _one_kind(p, op: str, group: dict, where: dict, n: int, answers: list, dev) 
             ints[:, r] = args[1:5]
         elif op in ("mfollow", "formfollow"):
             ints[0, r], ints[1, r] = args[1], args[2]
+        elif op in ("follow", "orbit"):
+            ints[0, r], one[r] = where.get((wi, args[1]), -1), args[2]
+        elif op == "warpin":
+            vec[r], ints[0, r] = args[1:4], args[4]
+        elif op in ("radius", "maxvel", "sf", "mass"):
+            one[r] = args[1]
     m = torch.tensor(mask, dtype=BOOL, device=dev)
     A, B, C, D = (torch.tensor(ints[k], dtype=I64, device=dev) for k in range(4))
     V = torch.tensor(vec, dtype=F64, device=dev)
@@ -181,6 +202,22 @@ def _one_kind(p, op: str, group: dict, where: dict, n: int, answers: list, dev) 
         p.set_ball_formation(m, A)
     elif op == "formfollow":
         p.formation_follow(m, A, B)
+    elif op in ("follow", "orbit", "warpin", "radius", "maxvel", "sf", "mass"):
+        X1 = torch.tensor(one, dtype=F64, device=dev)
+        if op == "follow":
+            p.follow(live, A, X1)
+        elif op == "orbit":
+            p.orbit(live, A, X1)
+        elif op == "warpin":
+            p.entity_warp_in(live, V, A)
+        elif op == "radius":
+            p.set_radius(live, X1)
+        elif op == "maxvel":
+            p.set_max_velocity(live, X1)
+        elif op == "sf":
+            p.set_speed_fraction(live, X1)
+        else:
+            p.set_mass(live, X1)
     else:
         raise ValueError(f"unknown record {op!r}")
 
@@ -247,12 +284,12 @@ def load(path: Path) -> tuple:
     return body["formations"], out
 
 
-def replay(p, batch: dict, where: dict, tick=None) -> list:
+def replay(p, batch: dict, where: dict, tick=None, fields: tuple = FIELDS) -> list:
     """Drive a recorded batch on park p; the differences: [(step, fields)] for digests, then events and answers."""
     bad = []
 
     def on_step(s, q):
-        mm = first_mismatch(batch["digests"][s], field_digests(q))
+        mm = first_mismatch(batch["digests"][s], field_digests(q, fields), fields)
         if mm:
             bad.append((s, mm))
     got = drive(p, batch["cfg"], where, on_step, tick)

@@ -373,9 +373,60 @@ def make_combat() -> None:
               f"{sum(len(b['events']) for b in batches)} events, {time.time() - t:.0f} s")
 
 
+def make_composed() -> None:
+    """composed_{1,2}: the reference's composed-park scenarios (tests/park_cases.py: ship clusters with fixed spheres,
+    GOTO, FOLLOW and ORBIT at short range, warps into and out of the cluster with their drop-outs, the setters,
+    cloaks, formations, missiles launched at the ships; seed 1 development, 2 held out; 16 batches of 16 worlds as its
+    own tests run them), the batches with dynamical orientation, recorded on the reference's VecComposedPark (its
+    tick on tensors, CPU) by tests/golden/combat_trace.py's driver with the composed fields (the collision
+    acceleration, the filing, the collision list). Each batch is first run by the reference's own harness
+    (park_cases.batched) and compared with the scalar FullBallpark by its own comparison: 0 differences, or the
+    generator stops. Worlds outside the reference's domain or flagged by the batch are left out."""
+    import combat_trace as ct
+    import destiny_combat_cases as dc
+    import park_cases as pc
+    import exact_ballpark.vec_composed as vp
+    for seed in (1, 2):
+        t = time.time()
+        batches = []
+        for cfg in pc.batches(seed, 16, 16):
+            if not cfg["do"]:
+                continue
+            refs = [pc.reference(cfg, w) for w in cfg["worlds"]]
+            outs, park = pc.batched(cfg, "cpu")
+            flags = park.world_flags()
+            keep = [k for k in range(len(cfg["worlds"])) if dc.in_domain(refs[k]) and not flags[k]]
+            for k in keep:
+                bad = pc.differences(refs[k], outs[k])
+                if bad:
+                    raise RuntimeError(f"seed {seed}: the reference's batch differs from FullBallpark: {bad[:4]}")
+            if not keep:
+                continue
+            cfg = {**cfg, "worlds": [cfg["worlds"][k] for k in keep]}
+            outs, park = pc.batched(cfg, "cpu")
+            if any(park.world_flags()):
+                raise RuntimeError("a world flagged once its neighbours were left out")
+            digests = []
+            p, where = ct.make_park(vp.VecComposedPark, cfg, pc.FORMATIONS, "cpu")
+            got = ct.drive(p, cfg, where, lambda s, q: digests.append(ct.field_digests(q, ct.COMPOSED_FIELDS)))
+            want_e = [(wl, *e) for wl, o in enumerate(outs) for e in o["E"]]
+            if sorted(got["E"]) != sorted(want_e) or got["A"] != [o["A"] for o in outs]:
+                raise RuntimeError("the driver's run differs from the reference harness's (events or answers)")
+            for f in ct.COMPOSED_FIELDS + ("exists",):
+                a, b = ct._field(p, f), ct._field(park, f)
+                if a.shape != b.shape or not (a.view(np.uint64) == b.view(np.uint64)).all():
+                    raise RuntimeError(f"the driver's final {f} differs from the reference harness's")
+            batches.append({"cfg": cfg, "digests": np.array(digests, dtype=np.uint64), "events": got["E"],
+                            "answers": got["A"]})
+            print(f"    batch: {len(keep)} worlds, {len(got['E'])} events, {time.time() - t:.0f} s", flush=True)
+        ct.save(HERE / f"composed_{seed}", pc.FORMATIONS, batches)
+        print(f"  composed_{seed}: {len(batches)} batches, {sum(len(b['cfg']['worlds']) for b in batches)} worlds, "
+              f"{sum(len(b['events']) for b in batches)} events, {time.time() - t:.0f} s", flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat"), default=None)
+    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed"), default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
     a = ap.parse_args()
     if a.only in (None, "libm"):
@@ -390,6 +441,8 @@ def main() -> None:
         make_rand()
     if a.only in (None, "combat"):
         make_combat()
+    if a.only in (None, "composed"):
+        make_composed()
 
 
 if __name__ == "__main__":
