@@ -358,16 +358,24 @@ def collide_runs(args, dev, statics: bool = False) -> dict:
 # reads (exists 1, formation id 8, owner row 8, bubble 8, cloak 8) and writes (contacts 8, dispatch count 8, the
 # self-collision byte 1)
 COMBAT_BYTES_PER_ROW_TICK = BYTES_PER_SHIP_TICK + (1 + 8 + 8 + 8 + 8) + (8 + 8 + 1)
+# The composed park's on top: the collision acceleration (24 written, 24 read by the commit), the filing (level and
+# key, side 8 + 48 read; written again by the commit's re-filing: counted once) and the collision list's length
+COMPOSED_EXTRA_BYTES_PER_ROW_TICK = 24 + 24 + 56 + 8
 
 
-def combat_cpu_sample(worlds: int, warmup: int, steps: int) -> dict:
-    """The CPU oracle of the combat park (oracle/combat_park.py, the C++ sequential tick) on every host core, on
-    `worlds` worlds of the benchmark's workload over `steps` ticks after `warmup`: ship-ticks/s (4 ships a world)."""
-    from exact_ballpark_b200.workloads import combat_worlds
-    from oracle.combat_park import OracleCombatPark
+def combat_cpu_sample(worlds: int, warmup: int, steps: int, composed: bool = False) -> dict:
+    """The CPU oracle of the combat park (oracle/combat_park.py, the C++ sequential tick) or of the composed park
+    (oracle/composed_park.py: each massive ball's Gradient at its turn) on every host core, on `worlds` worlds of the
+    benchmark's workload over `steps` ticks after `warmup`: ship-ticks/s."""
+    from exact_ballpark_b200.workloads import combat_worlds, composed_worlds
     threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-    w = combat_worlds(31, worlds)
-    p = OracleCombatPark(len(w.rows), dynamical_orientation=True, use_new_orbit=True)
+    if composed:
+        from oracle.composed_park import OracleComposedPark as Park
+        w = composed_worlds(41, worlds)
+    else:
+        from oracle.combat_park import OracleCombatPark as Park
+        w = combat_worlds(31, worlds)
+    p = Park(len(w.rows), dynamical_orientation=True, use_new_orbit=True)
     p.load(w.rows)
     w.apply(p)
     for _ in range(warmup):
@@ -376,33 +384,37 @@ def combat_cpu_sample(worlds: int, warmup: int, steps: int) -> dict:
     for _ in range(steps):
         p.evolve(threads=threads)
     dt = time.perf_counter() - t0
+    shape = "6 ships + 1 sphere + 2 missiles (seed 41)" if composed else "4 ships + 4 missiles (seed 31)"
     return {"value": w.ships * worlds * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{worlds} worlds x (4 ships + 4 missiles) (seed 31), ticks {warmup + 1}..{warmup + steps} "
-                      f"({dt:.1f} s wall), C++ oracle (oracle/flight.cpp's combat tick), {threads} threads over "
-                      "disjoint worlds"}
+            "sample": f"{worlds} worlds x ({shape}), ticks {warmup + 1}..{warmup + steps} ({dt:.1f} s wall), C++ "
+                      f"oracle (oracle/flight.cpp's {'composed' if composed else 'combat'} tick), {threads} threads "
+                      "over disjoint worlds"}
 
 
-def combat_runs(args, dev) -> dict:
-    """The combat park (exact_ballpark_b200.combat, missiles and formations) at the reference's combat benchmark
-    shape: --combat-worlds worlds of 4 ships and 4 missiles (workloads.combat_worlds: the ships following, orbiting
-    or flying to points, half the worlds with a formation; each missile added at a random launcher and launched aimed
-    and massive at another ship), warm-up ticks, then --combat-steps ticks each one CUDA-graph replay of the tick (the
-    domain watch and the one-launch tick), timed with CUDA events (L2 flushed before each). Ship-ticks count the 4
-    ships a world (missiles excluded), as the reference's benchmark does."""
+def combat_runs(args, dev, composed: bool = False) -> dict:
+    """The combat park (exact_ballpark_b200.combat) at the reference's combat benchmark shape, or the composed park
+    (exact_ballpark_b200.composed, combat with collisions) at its composed benchmark shape: --combat-worlds worlds of
+    4 ships and 4 missiles (workloads.combat_worlds: the ships following, orbiting or flying to points, half the
+    worlds with a formation; each missile added at a random launcher and launched aimed and massive at another ship),
+    or of 6 massive ships, 1 fixed sphere and 2 missiles within 5 km (workloads.composed_worlds); warm-up ticks, then
+    --combat-steps ticks each one CUDA-graph replay of the tick, timed with CUDA events (L2 flushed before each).
+    Ship-ticks count the ships (missiles and spheres excluded), as the reference's benchmarks do."""
     import torch
 
     from exact_ballpark_b200.combat import CombatGraph, VecCombatPark
-    from exact_ballpark_b200.workloads import combat_worlds
+    from exact_ballpark_b200.composed import VecComposedPark
+    from exact_ballpark_b200.workloads import combat_worlds, composed_worlds
     W = args.combat_worlds
-    w = combat_worlds(31, W)
+    w = composed_worlds(41, W) if composed else combat_worlds(31, W)
     n = len(w.rows)
-    park = VecCombatPark(n, device=dev, dynamical_orientation=True, use_new_orbit=True, block=128)
+    cls = VecComposedPark if composed else VecCombatPark
+    park = cls(n, device=dev, dynamical_orientation=True, use_new_orbit=True, block=128)
     park.load(w.rows)
     w.apply(park)
     graph = CombatGraph(park)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
-    total, events = 0.0, 0
+    total, events, contacts = 0.0, 0, 0
     for step in range(1, args.warmup + args.combat_steps + 1):
         flush.fill_(1)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -413,24 +425,34 @@ def combat_runs(args, dev) -> dict:
         if step > args.warmup:
             total += a.elapsed_time(b)
             events += len(park.events())
+            contacts += int(park.hits_n.sum().item())
     park.check()
     per = total / args.combat_steps
     peak, kind = _peaks()
-    achieved = COMBAT_BYTES_PER_ROW_TICK * n / (per / 1e3) / 1e9
-    out = {"workload": f"combat park: {W} worlds x (4 ships + 4 missiles launched aimed and massive), ships "
-                       "follow / orbit / goto, half the worlds with a formation, dynamical orientation on",
-           "value": 4 * W / (per / 1e3), "unit": "ship-ticks/s", "world_ticks_per_s": W / (per / 1e3),
-           "row_ticks_per_s": n / (per / 1e3), "ms_per_step": per, "steps": args.combat_steps,
-           "warmup": args.warmup, "events_per_tick": events / args.combat_steps,
+    row_bytes = COMBAT_BYTES_PER_ROW_TICK + (COMPOSED_EXTRA_BYTES_PER_ROW_TICK if composed else 0)
+    achieved = row_bytes * n / (per / 1e3) / 1e9
+    if composed:
+        workload = (f"composed park: {W} worlds x (6 massive ships + 1 fixed sphere + 2 missiles launched aimed and "
+                    "massive) within 5 km, the gradient method's collisions between every massive ball, ships follow / "
+                    "orbit / goto, half the worlds with a formation, dynamical orientation on")
+        published = {"value": 89e6, "unit": "ship-ticks/s", "hardware": "GH200",
+                     "config": "do=1, missiles=2, ships=6, spheres=1, graph, 65,536 worlds (docs/benchmarks.md)"}
+    else:
+        workload = (f"combat park: {W} worlds x (4 ships + 4 missiles launched aimed and massive), ships follow / "
+                    "orbit / goto, half the worlds with a formation, dynamical orientation on")
+        published = {"value": 92.7e6, "unit": "ship-ticks/s", "hardware": "GH200",
+                     "config": "do=1, missiles=4, ships=4, graph, 65,536 worlds (docs/benchmarks.md)"}
+    out = {"workload": workload, "value": w.ships * W / (per / 1e3), "unit": "ship-ticks/s",
+           "world_ticks_per_s": W / (per / 1e3), "row_ticks_per_s": n / (per / 1e3), "ms_per_step": per,
+           "steps": args.combat_steps, "warmup": args.warmup, "events_per_tick": events / args.combat_steps,
+           "contacts_per_tick": contacts / args.combat_steps,
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                         "peak_kind": kind, "traffic": None,
-                        "note": f"algorithmic {COMBAT_BYTES_PER_ROW_TICK} B/row-tick x {n} rows over the tick's "
-                                "CUDA-event time (a graph replay: the watch's few small kernels and the tick); "
-                                "issue- and latency-bound like the flight tick"},
-           "reference_published": {"value": 92.7e6, "unit": "ship-ticks/s", "hardware": "GH200",
-                                   "config": "do=1, missiles=4, ships=4, graph, 65,536 worlds (docs/benchmarks.md)"}}
+                        "note": f"algorithmic {row_bytes} B/row-tick x {n} rows over the tick's CUDA-event time (a "
+                                "graph replay); issue- and latency-bound like the flight tick"},
+           "reference_published": published}
     if not args.no_cpu_baseline:
-        out["cpu_baseline"] = combat_cpu_sample(256, 3, 20)
+        out["cpu_baseline"] = combat_cpu_sample(256, 3, 20, composed)
     return out
 
 
@@ -604,6 +626,7 @@ def main() -> None:
         line["collide_statics"] = collide_runs(args, dev, statics=True)
     if not args.no_combat:
         line["combat"] = combat_runs(args, dev)
+        line["composed"] = combat_runs(args, dev, composed=True)
     if not args.no_serve:
         line["serve"] = serve_runs(args, dev)
         line["serve"]["plain_ship_ticks_per_s"] = line["plain"]["value"] / world_size

@@ -55,8 +55,17 @@ struct Combat {
     int32_t do_missiles_off, master;
 };
 
+// The composed park's state beside the combat state (vec_composed.py:189-205): each row's collision acceleration
+// mLastC [n][3], its filing in the partition (level [n], key and side [n][3]) and its collision list [n][hit_cap]
+struct Composed {
+    double* last_c;
+    int64_t *level, *key, *mod, *hits;
+    int64_t hit_cap;
+};
+
 struct Park {
     Combat* c = nullptr;
+    Composed* x = nullptr;
     int64_t n;
     double friction, dt;
     float ffriction, fdt;
@@ -725,6 +734,230 @@ struct Tick {
             return 0;
         return potential(i, t, ld(p.pos, i), ld(p.pos, t), 0);
     }
+    // ---- the composed park: the partition's filing and the gradient (vec_composed.py; space.py:1631-1760) ----
+    static constexpr int NUM_LEVELS = 8;
+    static double level_width(int l) { return 7864320.0 / (double)(int64_t(1) << (2 * l)); }
+    static int64_t level_grid(int l) { return int64_t(1) << (2 * l + 23); }
+    // Ball::InsertInBoxes' level, key and side for row i at (pos, vel) with speed fraction sf (vec_collide.py:767-807);
+    // a filing the reference refuses flags the row (FLAG_PARTITION)
+    void file(int64_t i, V pos, V vel, double sf) {
+        const double k = p.friction;
+        double infl = p.radius[i];
+        if (p.free_[i]) {
+            const double m = p.mass[i] * p.agility[i];
+            const double a = k * sf * p.max_vel[i] / m;
+            const double speed = std::sqrt(lensq(vel));
+            const double ma = m * a;
+            infl = p.radius[i] + p.dt * ((ma - (ma - speed * k) * p.time_factor[i]) / k);
+        }
+        int level = -1;
+        for (int l = 0; l < NUM_LEVELS; ++l)
+            if (!(3.0 * infl > level_width(l))) ++level;
+        if (level < 0) level = 0;
+        const double w = level_width(level);
+        const int64_t grid = level_grid(level);
+        const double half = 0.5 * w * (double)grid, center = w * (double)grid * 0.5, fac = 1.0 / w;
+        const double pa[3] = {pos.x, pos.y, pos.z};
+        bool bad = level == 0 && p.radius[i] * 2.0 > level_width(0);
+        p.x->level[i] = level;
+        for (int q = 0; q < 3; ++q) {
+            int64_t kq = to_i64((pa[q] + half) * fac);
+            kq = kq < 0 ? 0 : (kq >= grid ? grid - 1 : kq);
+            const double lo = (double)kq * w - center, hi = (double)(kq + 1) * w - center;
+            const int64_t mq = (lo + infl) - pa[q] > 0.0 ? -1 : ((hi - infl) - pa[q] < 0.0 ? 1 : 0);
+            p.x->key[3 * i + q] = kq;
+            p.x->mod[3 * i + q] = mq;
+            if (kq <= 0 || kq >= grid - 1 || kq + mq < 0 || kq + mq >= grid) bad = true;
+        }
+        if (bad) p.c->flags[i] |= 128;
+    }
+    // Whether a box of ball n is one of ball b's boxes, an ancestor of one or below one (vec_collide.py:809)
+    bool related(int64_t b, int64_t n) const {
+        const int64_t Lb = p.x->level[b], Ln = p.x->level[n];
+        const int64_t sh = 2 * (Lb > Ln ? Lb - Ln : Ln - Lb);
+        for (int q = 0; q < 3; ++q) {
+            const int64_t kb = p.x->key[3 * b + q], mb = p.x->mod[3 * b + q];
+            const int64_t kn = p.x->key[3 * n + q], mn = p.x->mod[3 * n + q];
+            const int64_t bo[2] = {kb + std::min<int64_t>(mb, 0), kb + std::max<int64_t>(mb, 0)};
+            const int64_t no[2] = {kn + std::min<int64_t>(mn, 0), kn + std::max<int64_t>(mn, 0)};
+            const int64_t* fine = Ln <= Lb ? bo : no;
+            const int64_t* coarse = Ln <= Lb ? no : bo;
+            bool any = false;
+            for (int u = 0; u < 2; ++u)
+                for (int w = 0; w < 2; ++w) any = any || (fine[u] >> sh) == coarse[w];
+            if (!any) return false;
+        }
+        return true;
+    }
+    // Ball n's first box's place in ball b's GetNearbyBalls walk (vec_collide.py:825): b's box (by key order) that
+    // n's box relates to first, the part (an ancestor, below, the box itself) and the ancestor's distance or the box's
+    // post-order code below b's level
+    int64_t walk_key(int64_t b, int64_t n) const {
+        const int64_t Lb = p.x->level[b], Ln = p.x->level[n];
+        constexpr int64_t BASE = 65;
+        int64_t span = 1;
+        for (int l = 0; l < NUM_LEVELS - 1; ++l) span *= BASE;
+        int64_t lo_b[3], hi_b[3], cb[3], Kn[3], Mn[3];
+        for (int q = 0; q < 3; ++q) {
+            const int64_t kb = p.x->key[3 * b + q], mb = p.x->mod[3 * b + q];
+            lo_b[q] = kb + std::min<int64_t>(mb, 0);
+            hi_b[q] = kb + std::max<int64_t>(mb, 0);
+            cb[q] = mb != 0 ? 2 : 1;
+            Kn[q] = p.x->key[3 * n + q];
+            Mn[q] = p.x->mod[3 * n + q];
+        }
+        if (Ln <= Lb) {
+            const int64_t up = 2 * (Lb - Ln);
+            int64_t seg = 0;
+            for (int q = 0; q < 3; ++q) {
+                const int64_t v = lo_b[q] >> up;
+                const int64_t idx = (v == Kn[q] || (Mn[q] != 0 && v == Kn[q] + Mn[q])) ? 0 : 1;
+                seg = q == 0 ? idx : seg * cb[q] + idx;
+            }
+            return Ln < Lb ? seg * 3 * span + (Lb - Ln) : (seg * 3 + 2) * span;
+        }
+        const int64_t dn = 2 * (Ln - Lb);
+        int64_t best = int64_t(1) << 62;
+        for (int c = 0; c < 8; ++c) {
+            int64_t box[3], jx[3];
+            bool ok = true;
+            for (int q = 0; q < 3; ++q) {
+                const int64_t bit = (c >> (2 - q)) & 1;
+                if (bit && Mn[q] == 0) ok = false;
+                box[q] = Kn[q] + Mn[q] * bit;
+                const int64_t anc = box[q] >> dn;
+                const bool in0 = anc == lo_b[q], in1 = cb[q] == 2 && anc == hi_b[q];
+                if (!in0 && !in1) ok = false;
+                jx[q] = in0 ? 0 : 1;
+            }
+            if (!ok) continue;
+            const int64_t seg = (jx[0] * cb[1] + jx[1]) * cb[2] + jx[2];
+            int64_t code = 0, power = span;
+            for (int lvl = 1; lvl < NUM_LEVELS; ++lvl) {
+                power /= BASE;
+                const int64_t sh = std::max<int64_t>(2 * (Ln - lvl), 0);
+                int64_t digit = ((box[0] >> sh) & 3) * 16 + ((box[1] >> sh) & 3) * 4 + ((box[2] >> sh) & 3);
+                if (lvl > Ln) digit = BASE - 1;
+                if (lvl <= Lb) digit = 0;
+                code += digit * power;
+            }
+            best = std::min(best, (seg * 3 + 1) * span + code);
+        }
+        return best;
+    }
+    struct Acc {
+        V last_c;
+        double last_collision;
+        int64_t hits_n;
+    };
+    double gmass(int64_t i) const { return p.free_[i] ? p.mass[i] * p.agility[i] : 1.0e34; }
+    // Potential(b, o, depth) (space.py:1663; Ballpark.cpp:2789) at the positions the recursion pushed, with the
+    // composed park's end: a missile's response to its own target not kept (COL-711), the id appended either way
+    void potential_c(int64_t b, int64_t o, V pb, V po, int depth, bool exempt, Acc& acc) {
+        const double k = p.friction, dt = p.dt;
+        const double cr = p.radius[b] + p.radius[o];
+        const double m1 = gmass(b), m2 = gmass(o);
+        const bool free2 = p.free_[o] != 0;
+        const V v1 = ld(p.vel, b), v2 = ld(p.vel, o), g1 = ld(p.last_g, b), g2 = ld(p.last_g, o);
+        const double tf1 = p.time_factor[b], tf2 = p.time_factor[o];
+        V p1 = pb, w1 = v1, q1 = po, w2 = v2;
+        integrate_for(&p1, &w1, g1, m1, tf1, dt);
+        integrate_for(&q1, &w2, g2, m2, tf2, dt);
+        const double sv = spheres(pb, p1, po, q1, cr);
+        if (sv == -1.0) return;
+        V a1;
+        if (sv > 0.0) {                         // the impact: both to the time of impact, the reflection, the rest
+            V pp = pb, vp = v1, qq = po, vq = v2;
+            integrate_for(&pp, &vp, g1, m1, tf1, sv * dt);
+            integrate_for(&qq, &vq, g2, m2, tf2, sv * dt);
+            const V normal = normalized(sub(qq, pp));
+            const double u1 = vp.x * normal.x + vp.y * normal.y + vp.z * normal.z;
+            const double u2 = vq.x * normal.x + vq.y * normal.y + vq.z * normal.z;
+            if (!free2) {
+                vp = sub(vp, scl(normal, 2.0 * u1));
+            } else {
+                const double mm1 = p.mass[b], mm2 = p.mass[o];
+                const double u1p = (mm1 * u1 - mm2 * u1 + 2.0 * mm2 * u2) / (mm1 + mm2);
+                vp = add(vp, scl(normal, u1p - u1));
+            }
+            integrate_for(&pp, &vp, g1, m1, tf1, (1.0 - sv) * dt);
+            const double inv_m = 1.0 / m1, inv_t = 1.0 / (tf1 - 1.0);
+            const double ga[3] = {g1.x, g1.y, g1.z}, va[3] = {v1.x, v1.y, v1.z}, wa[3] = {vp.x, vp.y, vp.z};
+            double r[3];
+            for (int q = 0; q < 3; ++q) r[q] = -(ga[q] * -m1 + ga[q] * (tf1 * m1) - va[q] * tf1 * k + wa[q] * k) * inv_m * inv_t;
+            a1 = V{r[0], r[1], r[2]};
+        } else {                                // already overlapping: pushed apart, the recursion, the response
+            const V d = sub(po, pb);
+            const double d2 = lensq(d);
+            const V normal = d2 == 0.0 ? V{p.ids[b] > p.ids[o] ? 1.0 : -1.0, 0.0, 0.0} : normalized(d);
+            const double dist = (cr - std::sqrt(d2)) + 1.0;
+            const double d1 = m2 / (m1 + m2) * dist, dd2 = m1 / (m1 + m2) * dist;
+            if (depth < 2 && free2) {
+                potential_c(b, o, sub(pb, scl(normal, d1)), add(po, scl(normal, dd2)), depth + 1, exempt, acc);
+                if (m2 / m1 > 25.0) acc.last_c = scl(normalized(acc.last_c), dist);
+                if (lensq(sub(v1, v2)) > 0.0001) return;
+            }
+            const double normal_comp = g1.x * normal.x + g1.y * normal.y + g1.z * normal.z;
+            const double tmp = 1.0 / (m1 + dt * k);
+            const double c = -d1 / (dt * tmp * m1);
+            a1 = sub(scl(sub(scl(normal, c), v1), 1.0 / dt), scl(normal, normal_comp));
+        }
+        if (!exempt && sv >= acc.last_collision) {
+            const V lc = scl(a1, 0.85);
+            if (sv == acc.last_collision) {
+                if (lensq(lc) > lensq(acc.last_c)) acc.last_c = lc;
+            } else {
+                acc.last_c = lc;
+                acc.last_collision = sv;
+            }
+        }
+        p.x->hits[b * p.x->hit_cap + std::min(acc.hits_n, p.x->hit_cap - 1)] = p.ids[o];
+        ++acc.hits_n;
+    }
+    // Gradient of responder b at its turn (Ballpark.cpp:2745): the others as they stand now (a warper that dropped out
+    // at an earlier turn is massive again, at its drop-out point), GetNearbyBalls' candidates less Gradient's skips,
+    // those Potential's depth 0 does not rule out, in the walk's order then id (a normal missile: its target only)
+    void gradient(int64_t b, const std::vector<int64_t>& rows) {
+        const bool ex_b = p.c->exists[b] && !p.moribund[b];
+        const bool missile_b = ex_b && p.mode[b] == MISSILE, defender = missile_b && p.owner_id[b] < 0;
+        const double k = p.friction;
+        V eb = ld(p.pos, b), wb = ld(p.vel, b);
+        integrate_for(&eb, &wb, ld(p.last_g, b), gmass(b), p.time_factor[b], p.dt);
+        std::vector<std::pair<std::pair<int64_t, int64_t>, int64_t>> cand;
+        for (int64_t o : rows) {
+            if (o == b) continue;
+            const bool ex = p.c->exists[o] && !p.moribund[o];
+            const bool missile_o = ex && p.mode[o] == MISSILE;
+            bool pair, first = false;
+            if (missile_b && !defender) {
+                pair = o == p.follow_ptr[b] && ex && p.c->bubble[o] == p.c->bubble[b];
+                first = pair;
+            } else {
+                const bool nearby = ex && p.massive[o] && p.c->cloaked[o] == 0 && related(b, o);
+                pair = defender ? nearby : nearby && !missile_o;
+            }
+            if (!pair) continue;
+            const int64_t mo = p.mode[o];
+            if ((missile_b && (p.ids[o] == p.owner_id[b] || (mo == MINIBALL && p.owner_id[o] == p.owner_id[b]))) ||
+                ((mo == MISSILE || mo == MUSHROOM) && p.ids[b] == p.owner_id[o]) ||
+                (mo == MISSILE && p.ids[b] == p.follow_id[o]))
+                continue;
+            V eo = ld(p.pos, o), wo = ld(p.vel, o);
+            integrate_for(&eo, &wo, ld(p.last_g, o), gmass(o), p.time_factor[o], p.dt);
+            if (spheres(ld(p.pos, b), eb, ld(p.pos, o), eo, p.radius[b] + p.radius[o]) == -1.0) continue;
+            cand.push_back({{first ? 0 : walk_key(b, o), p.ids[o]}, o});
+        }
+        std::sort(cand.begin(), cand.end());
+        Acc acc{V{0, 0, 0}, -1.0, 0};
+        for (const auto& c : cand) {
+            const int64_t o = c.second;
+            potential_c(b, o, ld(p.pos, b), ld(p.pos, o), 0, missile_b && p.ids[o] == p.follow_id[b], acc);
+        }
+        (void)k;
+        st(p.x->last_c, b, acc.last_c);
+        p.last_collision[b] = acc.last_collision;
+        p.c->hits_n[b] = acc.hits_n;
+    }
     // EvolveBehaviorForBall (modes.py:359, full.py:2416)
     void behaviour(int64_t i, const std::vector<int64_t>& rows) {
         st(p.last_g, i, V{0, 0, 0});
@@ -760,9 +993,12 @@ struct Tick {
         st(p.last_g, i, a);
     }
     // Ballpark::Integrate over one tick (ref.py:354)
-    void integrate(V* pp, V* vp, V a, double m, double tfac) {
-        const double k = p.friction, t = p.dt;
+    void integrate(V* pp, V* vp, V a, double m, double tfac) { integrate_for(pp, vp, a, m, tfac, p.dt); }
+    // Ballpark::Integrate over t seconds: the cached decay factor for a whole tick, else glibc's exp(-k t / m)
+    void integrate_for(V* pp, V* vp, V a, double m, double tfac, double t) {
+        const double k = p.friction;
         if (t == 0.0) return;
+        if (t != p.dt) tfac = lm::exp(-k / m * t);
         const double k2 = k * k, ook2 = 1.0 / k2, ook = 1.0 / k;
         const V pv = *pp, v = *vp;
         V pn;
@@ -828,9 +1064,16 @@ struct Tick {
 
     void world(const std::vector<int64_t>& rows) {
         // (1) behaviours, ascending id
+        if (p.x)                                // the composed park: the live balls' responses and lists cleared
+            for (int64_t i : rows)
+                if (live(i)) {
+                    st(p.x->last_c, i, V{0, 0, 0});
+                    for (int64_t q = 0; q < p.x->hit_cap; ++q) p.x->hits[i * p.x->hit_cap + q] = -1;
+                    p.c->hits_n[i] = 0;
+                }
         for (int64_t i : rows)
             if (live(i)) behaviour(i, rows);
-        if (p.c)                                // the missiles' contacts with their targets, after every behaviour
+        if (p.c && !p.x)                        // the missiles' contacts with their targets, after every behaviour
             for (int64_t i : rows) p.c->hits_n[i] = missile_contacts(i);
         // (3) end-of-tick states into temporaries, and the rotation a tick on
         const size_t k = rows.size();
@@ -840,10 +1083,15 @@ struct Tick {
         for (size_t j = 0; j < k; ++j) {
             const int64_t i = rows[j];
             if (!live(i)) continue;
-            if (p.massive[i]) p.last_collision[i] = -1.0;
+            if (p.x) {                          // the gradient at its turn (a massive ball), then its end state
+                if (p.massive[i]) gradient(i, rows);
+            } else if (p.massive[i]) {
+                p.last_collision[i] = -1.0;
+            }
             V pv = ld(p.pos, i), vv = ld(p.vel, i);
             const V lg = ld(p.last_g, i);
-            const V a = V{lg.x + 0.0, lg.y + 0.0, lg.z + 0.0};
+            const V lc = p.x ? ld(p.x->last_c, i) : V{0.0, 0.0, 0.0};
+            const V a = V{lg.x + lc.x, lg.y + lc.y, lg.z + lc.z};
             if (warping(i)) {
                 const bool drop = warp_distance(i, &pv, &vv, (double)(p.clock[i] - p.effect_stamp[i]) * p.dt);
                 if (drop) {                     // massive and sensing again, Stop (a warper follows nothing)
@@ -852,6 +1100,7 @@ struct Tick {
                     stop_ball(i);
                     st(p.pos, i, pv);           // TRV-714: the drop-out point becomes the old state
                     st(p.vel, i, vv);
+                    if (p.x && !(lensq(vv) >= 0.1)) file(i, pv, vv, p.speed_fraction[i]);   // re-filed at rest
                     integrate(&pv, &vv, a, p.mass[i] * p.agility[i], p.time_factor[i]);
                 }
             } else {
@@ -904,7 +1153,9 @@ struct Tick {
                         snap_one(p.vel + 3 * i, p.rot + 4 * i, p.old_rot + 4 * i, p.ang_vel + 3 * i,
                                  p.old_ang_vel + 3 * i);
                 }
-                if (p.c && p.mode[i] == MISSILE && !(lensq(sub(ld(p.pos, i), before)) < 0.1)) {
+                const bool moved = !(lensq(sub(ld(p.pos, i), before)) < 0.1);
+                if (p.x && moved) file(i, ld(p.pos, i), ld(p.vel, i), p.speed_fraction[i]);   // re-filed
+                if (p.c && p.mode[i] == MISSILE && moved) {
                     // DispatchCollisions (Ballpark.cpp:600-639): the target ids, then on the master a collision with
                     // itself when its owner is gone, cloaked or in another bubble
                     p.c->ev_n[i] = p.c->hits_n[i];
@@ -913,6 +1164,10 @@ struct Tick {
                         const bool gone = o < 0 || o >= p.n || !p.c->exists[o];
                         p.c->ev_self[i] = (gone || (p.c->bubble[o] != p.c->bubble[i] && p.c->bubble[i] != -1) ||
                                            p.c->cloaked[o] != 0) ? 1 : 0;
+                    }
+                    if (p.x && p.c->ev_self[i]) {   // the master's self-collision joins the missile's list
+                        p.x->hits[i * p.x->hit_cap + std::min(p.c->hits_n[i], p.x->hit_cap - 1)] = p.ids[i];
+                        p.c->hits_n[i] += 1;
                     }
                 }
                 if (p.mode[i] == TROLL && !(p.effect_stamp[i] > p.clock[i])) {   // TrollReady, PetrifyTroll
@@ -995,6 +1250,21 @@ struct OracleCombat {
 // One tick of every world of a combat park in place (dynamical orientation on), `threads` host threads. Returns 0.
 int oracle_combat_tick_mt(const OracleFlight* s, const OracleCombat* c, int threads);
 
+// The composed park's extra state (the Composed structure above, field for field).
+struct OracleComposed {
+    double* last_c;
+    int64_t *level, *key, *mod, *hits;
+    int64_t hit_cap;
+};
+
+// One tick of every world of a composed park in place (dynamical orientation on), `threads` host threads. Returns 0.
+int oracle_composed_tick_mt(const OracleFlight* s, const OracleCombat* c, const OracleComposed* x, int threads);
+
+// The filing of the rows with mask[i] != 0 from their state or the given pos, vel ([n][3]) and sf ([n]) (null for the
+// row's own). Returns 0.
+int oracle_composed_file(const OracleFlight* s, const OracleCombat* c, const OracleComposed* x, const uint8_t* mask,
+                         const double* pos, const double* vel, const double* sf);
+
 static Park park_of(const OracleFlight* s);
 
 int oracle_flight_tick_mt(const OracleFlight* s, int threads) {
@@ -1003,17 +1273,50 @@ int oracle_flight_tick_mt(const OracleFlight* s, int threads) {
     return 0;
 }
 
+static Combat combat_of(const OracleCombat* c);
+
 int oracle_combat_tick_mt(const OracleFlight* s, const OracleCombat* c, int threads) {
     Park p = park_of(s);
+    Combat cx = combat_of(c);
+    p.c = &cx;
+    Tick(p).run(threads);
+    return 0;
+}
+
+int oracle_composed_tick_mt(const OracleFlight* s, const OracleCombat* c, const OracleComposed* x, int threads) {
+    Park p = park_of(s);
+    Combat cx = combat_of(c);
+    Composed xx{x->last_c, x->level, x->key, x->mod, x->hits, x->hit_cap};
+    p.c = &cx;
+    p.x = &xx;
+    Tick(p).run(threads);
+    return 0;
+}
+
+int oracle_composed_file(const OracleFlight* s, const OracleCombat* c, const OracleComposed* x, const uint8_t* mask,
+                         const double* pos, const double* vel, const double* sf) {
+    Park p = park_of(s);
+    Combat cx = combat_of(c);
+    Composed xx{x->last_c, x->level, x->key, x->mod, x->hits, x->hit_cap};
+    p.c = &cx;
+    p.x = &xx;
+    Tick t(p);
+    for (int64_t i = 0; i < p.n; ++i) {
+        if (!mask[i]) continue;
+        const V pv = ld(pos ? pos : p.pos, i), vv = ld(vel ? vel : p.vel, i);
+        t.file(i, pv, vv, sf ? sf[i] : p.speed_fraction[i]);
+    }
+    return 0;
+}
+
+static Combat combat_of(const OracleCombat* c) {
     Combat cx;
     cx.exists = c->exists; cx.formation_id = c->formation_id; cx.formation_slots = c->formation_slots;
     cx.owner_ptr = c->owner_ptr; cx.hits_n = c->hits_n; cx.ev_n = c->ev_n; cx.ev_self = c->ev_self;
     cx.bubble = c->bubble; cx.cloaked = c->cloaked; cx.flags = c->flags; cx.formations = c->formations;
     cx.formation_len = c->formation_len; cx.n_formations = c->n_formations; cx.max_slots = c->max_slots;
     cx.tick_ms = c->tick_ms; cx.do_missiles_off = c->do_missiles_off; cx.master = c->master;
-    p.c = &cx;
-    Tick(p).run(threads);
-    return 0;
+    return cx;
 }
 
 static Park park_of(const OracleFlight* s) {

@@ -38,6 +38,8 @@ def lib():
         _lib.oracle_flight_tick.argtypes = [p]
         _lib.oracle_flight_tick_mt.argtypes = [p, ctypes.c_int]
         _lib.oracle_combat_tick_mt.argtypes = [p, p, ctypes.c_int]
+        _lib.oracle_composed_tick_mt.argtypes = [p, p, p, ctypes.c_int]
+        _lib.oracle_composed_file.argtypes = [p, p, p, p, p, p, p]
         _lib.oracle_snap.argtypes = [i64, p, p, p, p, p, p]
         _lib.oracle_q_rot_mul.argtypes = [i64, p, p, p, p]
     return _lib

@@ -38,3 +38,20 @@ def test_a_planted_fault_in_the_oracle_is_caught():
             q.pos[r, 0] = np.nextafter(q.pos[r, 0], np.inf)
     bad = ct.replay(p, b, where, tick=tick)
     assert bad and bad[0][0] == 4 and "pos" in bad[0][1]
+
+
+@pytest.mark.parametrize("seed", [1, 2], ids=["development", "held_out"])
+def test_the_oracle_replays_the_golden_composed_batches(seed):
+    """The composed park's oracle (the sequential tick: each massive ball's Gradient at its own turn) against the
+    golden batches recorded on the reference's composed park: every field with the collision acceleration, the
+    filing and the collision list, every step; the events and the slot answers."""
+    from oracle.composed_park import OracleComposedPark
+    formations, batches = ct.load(ct.GOLDEN / f"composed_{seed}")
+    failures = []
+    for bi, b in enumerate(batches):
+        p, where = ct.make_park(OracleComposedPark, b["cfg"], formations, "cpu")
+        bad = ct.replay(p, b, where, fields=ct.COMPOSED_FIELDS)
+        if bad:
+            failures.append((bi, bad[:2]))
+    assert not failures, f"{len(failures)} of {len(batches)} batches differ, first {failures[:2]}"
+    assert sum(len(b["events"]) for b in batches) > 400

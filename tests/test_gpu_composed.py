@@ -27,3 +27,46 @@ def test_the_gpu_composed_park_replays_the_golden_batches(seed):
         if bad:
             failures.append((bi, bad[:2]))
     assert not failures, f"{len(failures)} of {len(batches)} batches differ, first {failures[:2]}"
+
+
+def test_the_gpu_composed_park_matches_the_oracle_on_the_benchmark_worlds():
+    """The composed benchmark's worlds (workloads.composed_worlds: 6 massive ships, 1 fixed sphere and 2 missiles
+    launched aimed and massive a world, within 5 km) at 512 worlds, 60 ticks: every composed field of every row
+    holding a ball after every 10th tick and every tick's events, GPU against the sequential CPU oracle; then a CUDA
+    graph's replays against eager ticks, bit for bit."""
+    from exact_ballpark_b200 import CombatGraph, VecComposedPark
+    from exact_ballpark_b200.workloads import composed_worlds
+    from oracle.composed_park import OracleComposedPark
+    w = composed_worlds(9, 512)
+    n = len(w.rows)
+    g = VecComposedPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    o = OracleComposedPark(n, dynamical_orientation=True, use_new_orbit=True)
+    for p in (g, o):
+        p.load(w.rows)
+        w.apply(p)
+    events = contacts = 0
+    for k in range(1, 61):
+        g.evolve()
+        o.evolve()
+        ge, oe = g.events(), o.events()
+        assert ge == oe, f"tick {k}: events differ"
+        events += len(ge)
+        contacts += int(o.hits_n.sum())
+        if k % 10 == 0:
+            want, got = ct.field_digests(o, ct.COMPOSED_FIELDS), ct.field_digests(g, ct.COMPOSED_FIELDS)
+            assert not ct.first_mismatch(want, got, ct.COMPOSED_FIELDS), \
+                f"tick {k}: {ct.first_mismatch(want, got, ct.COMPOSED_FIELDS)}"
+    g.check()
+    assert events > 100 and contacts > 1000
+    h = VecComposedPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    e = VecComposedPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    for p in (h, e):
+        p.load(w.rows)
+        w.apply(p)
+    graph = CombatGraph(h)
+    for _ in range(20):
+        graph.tick()
+        e.evolve()
+        assert h.events() == e.events()
+    assert not ct.first_mismatch(ct.field_digests(e, ct.COMPOSED_FIELDS), ct.field_digests(h, ct.COMPOSED_FIELDS),
+                                 ct.COMPOSED_FIELDS)
