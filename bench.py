@@ -480,6 +480,9 @@ def main() -> None:
     ap.add_argument("--collide-worlds", type=int, default=65536)
     ap.add_argument("--collide-steps", type=int, default=50)
     ap.add_argument("--no-combat", action="store_true")
+    ap.add_argument("--only", choices=("ragged", "collide", "collide_statics", "combat", "composed", "serve"),
+                    default=None, help="run one section alone on one GPU and print it (for profiling); the default "
+                                       "run prints the headline line with every section")
     ap.add_argument("--combat-worlds", type=int, default=65536)
     ap.add_argument("--combat-steps", type=int, default=50)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
@@ -513,6 +516,13 @@ def main() -> None:
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.only is not None:
+        run = {"ragged": lambda: ragged_runs(args, dev), "collide": lambda: collide_runs(args, dev),
+               "collide_statics": lambda: collide_runs(args, dev, statics=True),
+               "combat": lambda: combat_runs(args, dev), "composed": lambda: combat_runs(args, dev, composed=True),
+               "serve": lambda: serve_runs(args, dev)}[args.only]
+        print(json.dumps({"metric": METRIC, "section": args.only, args.only: run()}), flush=True)
+        return
     dist = None
     if world_size > 1:
         import datetime
