@@ -9,7 +9,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libebb.so"
-ABI = 3
+ABI = 4
 COLLIDE_MAX_SLOTS = 64          # include/ebb.h: EBB_COLLIDE_MAX_SLOTS
 COLLIDE_MAX_STATICS = 64        # include/ebb.h: EBB_COLLIDE_MAX_STATICS
 
@@ -36,7 +36,7 @@ class CombatState(ctypes.Structure):
                     "exists", "formation_id", "formation_slots", "owner_ptr", "hits_n", "ev_n", "ev_self", "bubble",
                     "cloaked", "flags", "formations", "formation_len")]
                 + [("n_formations", ctypes.c_int64), ("max_slots", ctypes.c_int64), ("tick_ms", ctypes.c_int64),
-                   ("do_missiles_off", ctypes.c_int32), ("master", ctypes.c_int32)])
+                   ("do_missiles_off", ctypes.c_int32), ("master", ctypes.c_int32), ("active", ctypes.c_void_p)])
 
 
 class ComposedState(ctypes.Structure):

@@ -15,7 +15,7 @@ comparisons and selections; floats as float32 operations); the tick is one launc
 (ebb_combat_tick: tiles of whole worlds, one thread block a tile, the records in shared memory, block barriers between
 phase 1, the missiles' contacts and the commit). Dynamical orientation is required: the yaw, pitch and roll path the
 reference keeps without it (glibc's double atan2, asin and sin on the host every tick) is not built. Not built
-either: mushrooms (AddMushroom, BringOutTheDeads) and the masked tick (OnTick's mask).
+either: mushrooms (AddMushroom, BringOutTheDeads). OnTick's per-world mask runs inside the kernel.
 """
 
 from __future__ import annotations
@@ -474,19 +474,40 @@ class VecCombatPark(VecModesPark):
 
     def evolve(self, lib=None, active: torch.Tensor | None = None) -> None:
         """One tick of every world in place (ebb_combat_tick: one launch), the domain watched at its start and end;
-        no host synchronisation."""
-        if active is not None:
-            raise NotImplementedError("OnTick's mask is not built for the combat park")
+        no host synchronisation. `active` [n] (OnTick's per-world mask, a world's rows alike): only those worlds
+        tick, inside the kernel; every other row keeps every field (the reference's tick-and-put-back, exact since a
+        world's tick reads its own rows only), and `events()` then reports the rows that ticked."""
+        act = self._world_mask(active)
         self.watch()
-        tick(self)
+        tick(self, act)
         self.watch()
+        self._ticked = (self.current_time, act)
         self.current_time += 1
+
+    def _world_mask(self, active) -> torch.Tensor | None:
+        """OnTick's mask as bytes on the device, refused unless a world's rows are alike (one host synchronisation)."""
+        if active is None:
+            return None
+        act = torch.as_tensor(active).to(device=self.dev, dtype=BOOL).reshape(self.n)
+        rw = self.rows_of_world
+        v = act[rw.clamp(min=0)] | (rw < 0)
+        w = act[rw.clamp(min=0)] & (rw >= 0)
+        if bool((v.all(dim=1) != w.any(dim=1)).any()):
+            raise ValueError("OnTick's mask: a world's rows tick together")
+        return act.to(torch.uint8).contiguous()
+
+    def _ticked_rows(self, sel: torch.Tensor) -> torch.Tensor:
+        """sel, less the rows outside the last tick's mask when that tick was a masked one."""
+        last = getattr(self, "_ticked", None)
+        if last is not None and last[0] == self.current_time - 1 and last[1] is not None:
+            return sel & (last[1] != 0)
+        return sel
 
     def events(self) -> list:
         """The tick's DoCollision events (COL-719) in Destiny's order, from the dispatch's counts: per world (its label,
         in first-appearance order), the missiles by ascending id, each with its target's id ev_n times, then itself on
         the master when orphaned: (world label, time, missile id, collider id). One host synchronisation."""
-        sel = (self._ev_n > 0) | self._ev_self
+        sel = self._ticked_rows((self._ev_n > 0) | self._ev_self)
         rows = sel.nonzero().flatten().tolist()
         if not rows:
             return []
@@ -547,7 +568,7 @@ class VecCombatPark(VecModesPark):
         return super().row_tensors() + ["_" + name for name, _ in _COMBAT_STORAGE]
 
 
-def tick(park: VecCombatPark, block: int | None = None) -> None:
+def tick(park: VecCombatPark, active: torch.Tensor | None = None) -> None:
     """One tick of a VecCombatPark in place on torch's current stream (the drop-in for
     exact_ballpark.vec_combat_cuda.tick): one launch, tiles of whole worlds; no allocation, no host synchronisation."""
     plan = park.plan
@@ -558,9 +579,11 @@ def tick(park: VecCombatPark, block: int | None = None) -> None:
     if plan.cap > plan.block:
         raise ValueError(f"a world of {plan.max_world} rows is wider than the block ({plan.block} threads)")
     tr = plan.tile_rows_on(park.dev)
+    c = park.combat_state()
+    c.active = None if active is None else active.data_ptr()
     with torch.cuda.device(park.dev):
-        rc = _native.lib().ebb_combat_tick(ctypes.byref(park.combat_state()), tr.data_ptr(), plan.tiles,
-                                           park._status.data_ptr(), park._stream(), plan.block)
+        rc = _native.lib().ebb_combat_tick(ctypes.byref(c), tr.data_ptr(), plan.tiles, park._status.data_ptr(),
+                                           park._stream(), plan.block)
     _native.check(rc, "ebb_combat_tick")
 
 

@@ -194,15 +194,21 @@ class VecComposedPark(VecCombatPark):
 
     def evolve(self, lib=None, active: torch.Tensor | None = None) -> None:
         """One tick in place, no host synchronisation: with collisions the composed tick (one launch); without them
-        the combat park's tick and the collision lists made from its counts."""
-        if active is not None:
-            raise NotImplementedError("OnTick's mask is not built for the composed park")
+        the combat park's tick and the collision lists made from its counts. `active`: OnTick's per-world mask, inside
+        the kernel (the combat park's `evolve`)."""
         if not self.collisions:
             follow = self._follow_id.clone()
-            super().evolve()
+            hits, hits_n = self._hits.clone(), self._hits_n.clone()
+            super().evolve(active=active)
             self._lists_from_counts(follow)
+            if active is not None:                                    # the lists of the worlds that did not tick
+                act = torch.as_tensor(active).to(device=self.dev, dtype=BOOL).reshape(self.n)
+                self._hits.copy_(torch.where(act[:, None], self._hits, hits))
+                self._hits_n.copy_(torch.where(act, self._hits_n, hits_n))
             return
-        tick(self)
+        act = self._world_mask(active)
+        tick(self, act)
+        self._ticked = (self.current_time, act)
         self.current_time += 1
 
     def _lists_from_counts(self, follow: torch.Tensor) -> None:
@@ -226,7 +232,7 @@ class VecComposedPark(VecCombatPark):
         """The tick's DoCollision events in Destiny's order: per world (label order) the missiles that dispatched by
         ascending id, each with its collision list in order, then itself on the master when orphaned: (world label,
         time, missile id, collider id). One host synchronisation."""
-        sel = (self._ev_n > 0) | self._ev_self
+        sel = self._ticked_rows((self._ev_n > 0) | self._ev_self)
         rows = sel.nonzero().flatten().tolist()
         if not rows:
             return []
@@ -254,11 +260,13 @@ class VecComposedPark(VecCombatPark):
             raise RuntimeError(f"a world wider than {MAX_WORLD_ROWS} rows reached the composed tick")
         super().check()
 
+    ROW_MAJOR = ("_hits",)                  # per-row tensors laid out [n, ...] (the others are [k, n] planes)
+
     def row_tensors(self) -> list:
         return super().row_tensors() + ["_last_c", "_level", "_key", "_mod", "_hits"]
 
 
-def tick(park: VecComposedPark) -> None:
+def tick(park: VecComposedPark, active: torch.Tensor | None = None) -> None:
     """One tick of a VecComposedPark with collisions in place on torch's current stream (the drop-in for
     exact_ballpark.vec_composed_cuda.tick): one launch; no allocation, no host synchronisation."""
     plan = park.plan
@@ -269,7 +277,9 @@ def tick(park: VecComposedPark) -> None:
     if plan.cap > plan.block:
         raise ValueError(f"a world of {plan.max_world} rows is wider than the block ({plan.block} threads)")
     tr = plan.tile_rows_on(park.dev)
+    x = park.composed_state()
+    x.combat.active = None if active is None else active.data_ptr()
     with torch.cuda.device(park.dev):
-        rc = _native.lib().ebb_composed_tick(ctypes.byref(park.composed_state()), tr.data_ptr(), plan.tiles,
-                                             park._status.data_ptr(), park._stream(), plan.block)
+        rc = _native.lib().ebb_composed_tick(ctypes.byref(x), tr.data_ptr(), plan.tiles, park._status.data_ptr(),
+                                             park._stream(), plan.block)
     _native.check(rc, "ebb_composed_tick")

@@ -945,8 +945,8 @@ __global__ void __launch_bounds__(256, EBB_COMBAT_MIN_BLOCKS) tick_kernel(EbbCom
     fill_ndt(ndt_tab, c.flight.dt);
     const int m = (int)(r1 - r0);
     const int j = threadIdx.x;
-    const bool mine = j < m;
     const int64_t i = r0 + j;
+    const bool mine = j < m && (c.active == nullptr || c.active[i] != 0);   // OnTick: a world's rows alike
     if (mine) record(c, i, rec[j]);
     __syncthreads();
     DoLane d;
@@ -963,6 +963,7 @@ __global__ void __launch_bounds__(256, EBB_COMBAT_MIN_BLOCKS) tick_kernel(EbbCom
     if (COLLIDE) {
         GBall* gv = (GBall*)smem_raw;
         if (mine) stage(x, i, r0, r1, gv[j]);
+        else if (j < m) gv[j].world = INT64_MIN;                      // a world outside OnTick's mask: no view
         __syncthreads();
         if (mine && c.flight.free_[i] && !c.flight.moribund[i] && (gv[j].flags & G_MASSIVE)) {
             int w0 = j, w1 = j + 1;                                   // the world's rows in the tile

@@ -630,9 +630,10 @@ def masked_tick(park: VecModesPark, active: torch.Tensor, run) -> None:
     names = park.row_tensors()
     before = {k: getattr(park, k).clone() for k in names}
     run()
+    row_major = getattr(park, "ROW_MAJOR", ())
     for k, old in before.items():
         cur = getattr(park, k)
-        sel = act if cur.dim() == 1 else act[None, :]
+        sel = act if cur.dim() == 1 else (act[:, None] if k in row_major else act[None, :])
         cur.copy_(torch.where(sel, cur, old))
 
 

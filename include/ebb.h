@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define EBB_ABI_VERSION 3
+#define EBB_ABI_VERSION 4
 #define EBB_EINVAL (-1)
 #define EBB_ETOOBIG (-2)
 
@@ -86,6 +86,7 @@ typedef struct EbbCombatState {
     const int64_t* formation_len;
     int64_t n_formations, max_slots, tick_ms;
     int32_t do_missiles_off, master;
+    const uint8_t* active;                     /* OnTick's per-world mask ([n] bytes, a world's rows alike), or null */
 } EbbCombatState;
 
 /* The composed park (exact_ballpark.vec_composed.VecComposedPark: the combat park with the gradient method's collisions

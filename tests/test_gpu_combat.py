@@ -67,3 +67,36 @@ def test_the_gpu_combat_park_matches_the_oracle_on_the_benchmark_worlds():
         e.evolve()
         assert h.events() == e.events()
     assert not ct.first_mismatch(ct.field_digests(e), ct.field_digests(h))
+
+
+def _masked_against_put_back(park_cls, worlds_fn, fields):
+    """OnTick's per-world mask inside the kernel against the reference's semantics (tick every world, then give the
+    rows outside the mask back their state): 30 ticks, a different half of the worlds each tick, every field and the
+    ticked worlds' events."""
+    import torch
+    from exact_ballpark_b200.modes import masked_tick
+    w = worlds_fn()
+    n = len(w.rows)
+    a = park_cls(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    b = park_cls(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    for p in (a, b):
+        p.load(w.rows)
+        w.apply(p)
+    world = a.world
+    g = torch.Generator(device="cpu").manual_seed(5)
+    for k in range(30):
+        on = torch.rand(int(world.max()) + 1, generator=g) < 0.5
+        act = on.to(world.device)[world]
+        a.evolve(active=act)
+        got = a.events()
+        want = []
+        masked_tick(b, act, lambda: (b.evolve(), want.extend(e for e in b.events() if bool(on[e[0]]))))
+        assert got == want, f"tick {k}: events differ"
+        assert not ct.first_mismatch(ct.field_digests(b, fields), ct.field_digests(a, fields), fields), \
+            f"tick {k}: {ct.first_mismatch(ct.field_digests(b, fields), ct.field_digests(a, fields), fields)}"
+
+
+def test_the_combat_parks_masked_tick_is_the_put_back():
+    from exact_ballpark_b200 import VecCombatPark
+    from exact_ballpark_b200.workloads import combat_worlds
+    _masked_against_put_back(VecCombatPark, lambda: combat_worlds(13, 256), ct.FIELDS)

@@ -70,3 +70,10 @@ def test_the_gpu_composed_park_matches_the_oracle_on_the_benchmark_worlds():
         assert h.events() == e.events()
     assert not ct.first_mismatch(ct.field_digests(e, ct.COMPOSED_FIELDS), ct.field_digests(h, ct.COMPOSED_FIELDS),
                                  ct.COMPOSED_FIELDS)
+
+
+def test_the_composed_parks_masked_tick_is_the_put_back():
+    from exact_ballpark_b200 import VecComposedPark
+    from exact_ballpark_b200.workloads import composed_worlds
+    from test_gpu_combat import _masked_against_put_back
+    _masked_against_put_back(VecComposedPark, lambda: composed_worlds(13, 256), ct.COMPOSED_FIELDS)
