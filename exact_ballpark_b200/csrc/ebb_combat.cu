@@ -38,6 +38,11 @@
 #ifndef EBB_COMBAT_MIN_BLOCKS
 #define EBB_COMBAT_MIN_BLOCKS 3
 #endif
+// How the tick's large one-call steps (a responder's Gradient, the commit) are compiled: inlined into the kernel, or
+// out of line with their own register allocation
+#ifndef EBB_COMBAT_STEP
+#define EBB_COMBAT_STEP __forceinline__
+#endif
 
 namespace ebb {
 namespace combat {
@@ -679,12 +684,12 @@ constexpr int MAX_WORLD_ROWS = 64;                  // a world's rows at most in
 // Gradient (Ballpark.cpp:2745) of responder j (a live massive ball) over its world's rows [w0, w1) of the tile's view:
 // the composed candidates (vec_composed.py:_pair_mask) that Potential's depth 0 does not rule out, in the partition's
 // walk order (then id; a normal missile's target first), each through Potential
-__device__ __forceinline__ void gradient(const EbbComposedState& x, int64_t ib, int j, int w0, int w1, const GBall* gv) {
+__device__ EBB_COMBAT_STEP void gradient(const EbbComposedState& x, int64_t ib, int j, int w0, int w1, const GBall* gv) {
     const GBall& B = gv[j];
     const bool missile_b = (B.flags & G_EXISTS) && B.mode == MISSILE;
     const bool defender = missile_b && B.owner < 0;
     int64_t okey[MAX_WORLD_ROWS];
-    int8_t oslot[MAX_WORLD_ROWS];
+    uint8_t oslot[MAX_WORLD_ROWS];                                    // tile rows: below the block's 256 threads
     int nact = 0;
     for (int o = w0; o < w1; ++o) {
         if (o == j) continue;
@@ -716,7 +721,7 @@ __device__ __forceinline__ void gradient(const EbbComposedState& x, int64_t ib, 
             --at;
         }
         okey[at] = key;
-        oslot[at] = (int8_t)o;
+        oslot[at] = (uint8_t)o;
     }
     Acc acc{D3{0.0, 0.0, 0.0}, -1.0, 0};
     for (int q = 0; q < nact; ++q) {
@@ -798,7 +803,7 @@ __device__ __forceinline__ void stage(const EbbComposedState& x, int64_t i, int6
 // drop-out at rest re-filed there and every ball that moved at least sqrt(0.1) m re-filed after the commit, the
 // master's self-collision appended to the missile's collision list)
 template <bool COLLIDE>
-__device__ __forceinline__ void commit(const EbbComposedState& x, int64_t i, const DoLane& d, int64_t hits) {
+__device__ EBB_COMBAT_STEP void commit(const EbbComposedState& x, int64_t i, const DoLane& d, int64_t hits) {
     const EbbCombatState& c = x.combat;
     const EbbFlightState& s = c.flight;
     const int64_t n = s.n;

@@ -28,7 +28,8 @@ def test_the_gpu_combat_park_replays_the_golden_batches(seed):
     assert not failures, f"{len(failures)} of {len(batches)} batches differ, first {failures[:2]}"
 
 
-def test_the_gpu_combat_park_matches_the_oracle_on_the_benchmark_worlds():
+@pytest.mark.parametrize("block", [128, 256])
+def test_the_gpu_combat_park_matches_the_oracle_on_the_benchmark_worlds(block):
     """The combat benchmark's worlds (workloads.combat_worlds: 4 ships and 4 missiles launched aimed and massive, ships
     following, orbiting, flying to points, in formation) at 512 worlds, 60 ticks: every field of every row holding a
     ball after every 10th tick and every tick's events, GPU against the CPU oracle; then a CUDA graph's replays
@@ -38,7 +39,7 @@ def test_the_gpu_combat_park_matches_the_oracle_on_the_benchmark_worlds():
     from oracle.combat_park import OracleCombatPark
     w = combat_worlds(7, 512)
     n = len(w.rows)
-    g = VecCombatPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    g = VecCombatPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True, block=block)
     o = OracleCombatPark(n, dynamical_orientation=True, use_new_orbit=True)
     for p in (g, o):
         p.load(w.rows)
@@ -55,10 +56,10 @@ def test_the_gpu_combat_park_matches_the_oracle_on_the_benchmark_worlds():
             assert not ct.first_mismatch(want, got), f"tick {k}: {ct.first_mismatch(want, got)}"
     g.check()
     assert events > 1000
-    h = VecCombatPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    h = VecCombatPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True, block=block)
     h.load(w.rows)
     w.apply(h)
-    e = VecCombatPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    e = VecCombatPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True, block=block)
     e.load(w.rows)
     w.apply(e)
     graph = CombatGraph(h)

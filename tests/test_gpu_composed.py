@@ -29,7 +29,8 @@ def test_the_gpu_composed_park_replays_the_golden_batches(seed):
     assert not failures, f"{len(failures)} of {len(batches)} batches differ, first {failures[:2]}"
 
 
-def test_the_gpu_composed_park_matches_the_oracle_on_the_benchmark_worlds():
+@pytest.mark.parametrize("block", [128, 256])
+def test_the_gpu_composed_park_matches_the_oracle_on_the_benchmark_worlds(block):
     """The composed benchmark's worlds (workloads.composed_worlds: 6 massive ships, 1 fixed sphere and 2 missiles
     launched aimed and massive a world, within 5 km) at 512 worlds, 60 ticks: every composed field of every row
     holding a ball after every 10th tick and every tick's events, GPU against the sequential CPU oracle; then a CUDA
@@ -39,7 +40,7 @@ def test_the_gpu_composed_park_matches_the_oracle_on_the_benchmark_worlds():
     from oracle.composed_park import OracleComposedPark
     w = composed_worlds(9, 512)
     n = len(w.rows)
-    g = VecComposedPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    g = VecComposedPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True, block=block)
     o = OracleComposedPark(n, dynamical_orientation=True, use_new_orbit=True)
     for p in (g, o):
         p.load(w.rows)
@@ -58,8 +59,8 @@ def test_the_gpu_composed_park_matches_the_oracle_on_the_benchmark_worlds():
                 f"tick {k}: {ct.first_mismatch(want, got, ct.COMPOSED_FIELDS)}"
     g.check()
     assert events > 100 and contacts > 1000
-    h = VecComposedPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
-    e = VecComposedPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True)
+    h = VecComposedPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True, block=block)
+    e = VecComposedPark(n, device="cuda", dynamical_orientation=True, use_new_orbit=True, block=block)
     for p in (h, e):
         p.load(w.rows)
         w.apply(p)
