@@ -408,7 +408,7 @@ def combat_runs(args, dev, composed: bool = False) -> dict:
     w = composed_worlds(41, W) if composed else combat_worlds(31, W)
     n = len(w.rows)
     cls = VecComposedPark if composed else VecCombatPark
-    park = cls(n, device=dev, dynamical_orientation=True, use_new_orbit=True, block=128)
+    park = cls(n, device=dev, dynamical_orientation=True, use_new_orbit=True, block=256)
     park.load(w.rows)
     w.apply(park)
     graph = CombatGraph(park)

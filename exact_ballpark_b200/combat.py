@@ -81,7 +81,7 @@ class VecCombatPark(VecModesPark):
     AddBall and RemoveBall mid-run (the module's docstring)."""
 
     def __init__(self, n: int, friction: float = 1.0e6, tick_interval_ms: int = 1000, device="cuda",
-                 dynamical_orientation: bool = True, use_new_orbit: bool = False, block: int = 128,
+                 dynamical_orientation: bool = True, use_new_orbit: bool = False, block: int = 256,
                  master: bool = False, disable_do_for_missiles: bool = False, ypr: str = "host"):
         if not dynamical_orientation:
             raise ValueError("the B200 combat park needs dynamical orientation (the yaw, pitch and roll path is not "

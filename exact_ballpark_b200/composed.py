@@ -46,7 +46,7 @@ class VecComposedPark(VecCombatPark):
     """VecCombatPark with the gradient method's collisions between every massive ball (the module's docstring)."""
 
     def __init__(self, n: int, friction: float = 1.0e6, tick_interval_ms: int = 1000, device="cuda",
-                 dynamical_orientation: bool = True, use_new_orbit: bool = False, block: int = 128,
+                 dynamical_orientation: bool = True, use_new_orbit: bool = False, block: int = 256,
                  master: bool = False, disable_do_for_missiles: bool = False, collisions: bool = True):
         super().__init__(n, friction, tick_interval_ms, device, dynamical_orientation, use_new_orbit, block, master,
                          disable_do_for_missiles)

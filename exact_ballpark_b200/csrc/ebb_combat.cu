@@ -35,13 +35,15 @@
 #include "ebb_orient.cuh"
 #include "ebb_rows.cuh"
 
+// Resident blocks a multiprocessor is asked to fit (the register budget the compiler gets), per tick: the combat tick
+// at 80 registers (3 blocks of 256 threads), the composed tick at 128 with its Gradient and commit out of line (2
+// blocks): measured fastest on B200 at 65,536 worlds (1.21 and 1.65 ms a tick, against 1.54 and 2.84 ms with the
+// composed tick at 80 registers, everything inlined and 128-thread blocks)
 #ifndef EBB_COMBAT_MIN_BLOCKS
 #define EBB_COMBAT_MIN_BLOCKS 3
 #endif
-// How the tick's large one-call steps (a responder's Gradient, the commit) are compiled: inlined into the kernel, or
-// out of line with their own register allocation
-#ifndef EBB_COMBAT_STEP
-#define EBB_COMBAT_STEP __forceinline__
+#ifndef EBB_COMPOSED_MIN_BLOCKS
+#define EBB_COMPOSED_MIN_BLOCKS 2
 #endif
 
 namespace ebb {
@@ -684,7 +686,7 @@ constexpr int MAX_WORLD_ROWS = 64;                  // a world's rows at most in
 // Gradient (Ballpark.cpp:2745) of responder j (a live massive ball) over its world's rows [w0, w1) of the tile's view:
 // the composed candidates (vec_composed.py:_pair_mask) that Potential's depth 0 does not rule out, in the partition's
 // walk order (then id; a normal missile's target first), each through Potential
-__device__ EBB_COMBAT_STEP void gradient(const EbbComposedState& x, int64_t ib, int j, int w0, int w1, const GBall* gv) {
+__device__ __noinline__ void gradient(const EbbComposedState& x, int64_t ib, int j, int w0, int w1, const GBall* gv) {
     const GBall& B = gv[j];
     const bool missile_b = (B.flags & G_EXISTS) && B.mode == MISSILE;
     const bool defender = missile_b && B.owner < 0;
@@ -803,7 +805,7 @@ __device__ __forceinline__ void stage(const EbbComposedState& x, int64_t i, int6
 // drop-out at rest re-filed there and every ball that moved at least sqrt(0.1) m re-filed after the commit, the
 // master's self-collision appended to the missile's collision list)
 template <bool COLLIDE>
-__device__ EBB_COMBAT_STEP void commit(const EbbComposedState& x, int64_t i, const DoLane& d, int64_t hits) {
+__device__ __forceinline__ void commit(const EbbComposedState& x, int64_t i, const DoLane& d, int64_t hits) {
     const EbbCombatState& c = x.combat;
     const EbbFlightState& s = c.flight;
     const int64_t n = s.n;
@@ -915,6 +917,11 @@ __device__ EBB_COMBAT_STEP void commit(const EbbComposedState& x, int64_t i, con
     c.ev_self[i] = ev_self;
 }
 
+// The composed tick's commit, out of line (its own register allocation)
+__device__ __noinline__ void commit_composed(const EbbComposedState& x, int64_t i, const DoLane& d, int64_t hits) {
+    commit<true>(x, i, d, hits);
+}
+
 // The composed park's phase-1 clearing of a live ball's collision response and list (vec_composed.py:_clear_contacts)
 __device__ __forceinline__ void clear_contacts(const EbbComposedState& x, int64_t i) {
     const int64_t n = x.combat.flight.n;
@@ -933,7 +940,7 @@ __host__ __device__ inline size_t tick_smem_bytes(int block, bool collide) {
 // COLLIDE: the composed park's; the gradient's view of the tile reuses the records' and the orientation tables' shared
 // memory (both done with at the barrier after phase 1).
 template <bool COLLIDE>
-__global__ void __launch_bounds__(256, EBB_COMBAT_MIN_BLOCKS) tick_kernel(EbbComposedState x,
+__global__ void __launch_bounds__(256, COLLIDE ? EBB_COMPOSED_MIN_BLOCKS : EBB_COMBAT_MIN_BLOCKS) tick_kernel(EbbComposedState x,
                                                                           const int64_t* __restrict__ tile_rows,
                                                                           int64_t tiles, int32_t* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -986,7 +993,10 @@ __global__ void __launch_bounds__(256, EBB_COMBAT_MIN_BLOCKS) tick_kernel(EbbCom
         }
         __syncthreads();
     }
-    if (mine) commit<COLLIDE>(x, i, d, hits);
+    if (mine) {
+        if constexpr (COLLIDE) commit_composed(x, i, d, hits);
+        else commit<false>(x, i, d, hits);
+    }
 }
 
 // The composed park's filing of the rows in a mask (the commands' re-filings), one thread a row
