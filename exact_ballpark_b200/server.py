@@ -1,0 +1,403 @@
+"""The server layer over the flight-mode park on a B200: a drop-in for exact_ballpark.vec_server's VecServer and
+ModesAdapter (exact_ballpark/vec_server.py:197-1080): Destiny's net/server layer batched for many worlds, each world one
+bubble with its pilots.
+
+Per tick, as Destiny's test helper drives the layer: `push` queues an Actions call for every masked world (TIME-709,
+TIME-710: stamped, and dropped when it equals the world's last queued call — same kind, ball, target, floats by value
+(a NaN equals nothing), ints and the local argument exactly); `pre_tick` moves the stamp, flushes the queue and applies
+every queued call but CloakBall through the park in queue order (the j-th calls of every world together, each world's
+in its own order), updates the bubble's additions (BubbleUpdater: a user ball seen for the first time gets every
+uncloaked ball of its bubble), then walks the history: CloakBall applied there and its event sent to the bubble it
+was queued in, UncloakBall's event to its own character with an AddBallsToPark to every other interactive pilot, a
+local SetBallPosition sent nowhere, every other event to the bubble, or to the ball's character while it is cloaked;
+`evolve` is the park's tick (a world whose bubble is dead at an evolve is refused by `check`); `post_tick` sets, per
+pilot, whether it gets the bubble's narrowcast and a character update (ParkUpdateBatcher.send_batch). `batch` holds the
+tick's update batch as tensors: the stamps, the queued calls, their routes, the uncloaks' recipients, the additions
+and the flags, with the park's fields where the streams would be written (`stream_fields`).
+
+Every park write is the park's own command or setter (exact_ballpark_b200.modes, on the device); the layer adds only
+index work (masks, gathers, comparisons) and the cloak's float sum radius + range as float32, as the C++ does.
+
+Not built: the encoding of the batches into Destiny's tuples and streams (`decode`), the pending queries and the undo,
+OnTick's intervals, the kernel path (one launch for the pre-tick), the other parks' adapters, bubbles other than one a
+world.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import torch
+
+from .modes import WARP
+
+F64, F32, I64, BOOL = torch.float64, torch.float32, torch.int64, torch.bool
+
+# the queued actions by the event the server sends (the index is the kind's code; 0 no action)
+KINDS = ("", "GotoPoint", "GotoDirection", "Stop", "FollowBall", "Orbit", "WarpTo", "EntityWarpIn", "SetSpeedFraction",
+         "SetMaxSpeed", "SetBallMass", "SetBallAgility", "SetBallRadius", "SetBallVelocity", "SetBallMassive",
+         "SetBallInteractive", "SetBallPosition", "CloakBall", "UncloakBall", "SetMaxAngularSpeed",
+         "SetBallAngularVelocity", "SetBallRotation", "SetBallAngularAgility", "SetMaxAngularVelocity",
+         "LaunchMissile", "SetBallTroll", "SetBallFree", "AddBallsToPark", "BallNotGlobal")
+CODE = {name: k for k, name in enumerate(KINDS) if name}
+DYNAMICAL_ONLY = frozenset(CODE[k] for k in ("SetBallAngularVelocity", "SetMaxAngularVelocity", "SetBallRotation",
+                                             "SetBallAngularAgility", "SetMaxAngularSpeed"))
+NONE, BUBBLE, CHARACTER = 0, 1, 2                   # where an event goes
+DSTNORMALCLOAK = 1
+CLOAK, UNCLOAK, SETPOS, INTERACTIVE = CODE["CloakBall"], CODE["UncloakBall"], CODE["SetBallPosition"], \
+    CODE["SetBallInteractive"]
+FOLLOWS = (CODE["FollowBall"], CODE["Orbit"])
+TROLL = CODE["SetBallTroll"]
+# applied by the parks with missiles, and by the partition layer's server: not by the flight park
+NOT_APPLIED = frozenset(CODE[k] for k in ("LaunchMissile", "AddBallsToPark", "BallNotGlobal"))
+
+
+def _char(x: torch.Tensor) -> torch.Tensor:
+    return ((x.to(I64) + 128) & 0xFF) - 128
+
+
+class ModesAdapter:
+    """The flight-mode park (exact_ballpark_b200.VecModesPark) as the server layer sees it: its rows grouped by world
+    label (first appearance order; a world's rows in the order its balls were added, the bubble's dictionary order),
+    the Destiny ids, the flags the layer routes by, and each kind applied through the park's command or setter."""
+
+    master = True
+
+    def __init__(self, park, master: bool = True):
+        self.park, self.R, self.dev, self.master = park, park.n, park.dev, bool(master)
+        self.ids = park.ids
+        self.exists = torch.ones(self.R, dtype=BOOL, device=self.dev)
+        labels = park.world.tolist()
+        order, groups = [], {}
+        for r, w in enumerate(labels):
+            if w not in groups:
+                groups[w] = []
+                order.append(w)
+            groups[w].append(r)
+        self.labels, self.W = order, len(order)
+        width = max((len(g) for g in groups.values()), default=0)
+        table = [g + [-1] * (width - len(g)) for g in (groups[w] for w in order)]
+        self.rows_of_world = torch.tensor(table, dtype=I64, device=self.dev).reshape(self.W, width)
+        index = {w: k for k, w in enumerate(order)}
+        self.world = torch.tensor([index[w] for w in labels], dtype=I64, device=self.dev)
+        safe = self.rows_of_world.clamp(min=0)
+        self.ids_of_world = torch.where(self.rows_of_world >= 0, self.ids[safe], 0)
+        self.arange = torch.arange(self.R, device=self.dev)
+        do = park.dynamical_orientation
+        self.kinds = frozenset(k for k in range(1, len(KINDS))
+                               if (do or k not in DYNAMICAL_ONLY) and k not in NOT_APPLIED)
+
+    interactive = property(lambda s: s.park.interactive, lambda s, v: setattr(s.park, "interactive", v))
+    massive = property(lambda s: s.park.massive, lambda s, v: setattr(s.park, "massive", v))
+
+    @property
+    def cloaked(self) -> torch.Tensor:
+        return self.park.cloaked
+
+    @cloaked.setter
+    def cloaked(self, v) -> None:
+        self.park.cloaked.copy_(torch.as_tensor(v, device=self.dev))
+
+    def lookup(self, ball: torch.Tensor) -> torch.Tensor:
+        """Each world's row of the ball whose Destiny id is ball[w], or -1."""
+        hit = self.ids_of_world == ball.to(I64)[:, None]
+        first = hit.to(I64).argmax(dim=1)
+        return torch.where(hit.any(dim=1), self.rows_of_world.gather(1, first[:, None])[:, 0], -1)
+
+    def any_in_world(self, flag: torch.Tensor) -> torch.Tensor:
+        safe = self.rows_of_world.clamp(min=0)
+        return (flag[safe] & (self.rows_of_world >= 0)).any(dim=1)
+
+    def radius(self) -> torch.Tensor:
+        return self.park.radius
+
+    def clock(self) -> torch.Tensor:
+        """Each world's mCurrentTime (its rows share one clock)."""
+        return self.park.clock[self.rows_of_world[:, 0]]
+
+    def warping(self) -> torch.Tensor:
+        return (self.park.mode == WARP) & (self.park.effect_stamp >= 0)
+
+    def cloak(self, m: torch.Tensor, mode: torch.Tensor, rng: torch.Tensor) -> None:
+        """CloakBall (Ballpark.cpp:5223): refused unless the signed char mode is positive; on the master a normal cloak
+        adds a proximity sensor (unless float(radius) + float(range) < 0); the followers released; cloaked with the
+        mode's byte, non-massive."""
+        mode = _char(mode)
+        ok = m & self.exists & (mode > 0)
+        if self.master:
+            rng32 = rng.to(F64).to(F32).to(F64)
+            sense = ok & (mode == DSTNORMALCLOAK) & ~((self.radius() + rng32).to(F32) < 0.0)
+            self.park.sensor = self.park.sensor | sense
+        self.park._release_followers(ok)
+        self.cloaked = torch.where(ok, mode & 0xFF, self.cloaked)
+        self.massive = torch.where(ok, False, self.massive)
+
+    def uncloak(self, m: torch.Tensor) -> None:
+        """UncloakBall (Ballpark.cpp:5257): a normal cloak's sensor removed (master); uncloaked; massive again unless
+        in warp proper."""
+        ok = m & self.exists
+        if self.master:
+            self.park.sensor = self.park.sensor & ~(ok & (self.cloaked == DSTNORMALCLOAK))
+        self.cloaked = torch.where(ok, 0, self.cloaked)
+        self.massive = torch.where(ok & ~self.warping(), True, self.massive)
+
+    def apply(self, kind: int, m: torch.Tensor, trow: torch.Tensor, f: torch.Tensor, n: torch.Tensor) -> None:
+        """One kind on the rows in m, each row's arguments: the park's own command or setter."""
+        p, name = self.park, KINDS[kind]
+        xyz = f[:, :3].contiguous()
+        one = f[:, 0].contiguous()
+        if name == "GotoPoint":
+            p.goto_point(m, xyz)
+        elif name == "GotoDirection":
+            p.goto_direction(m, xyz)
+        elif name == "Stop":
+            p.stop(m)
+        elif name == "FollowBall":
+            p.follow(m, trow, one)
+        elif name == "Orbit":
+            p.orbit(m, trow, one)
+        elif name == "WarpTo":
+            p.warp_to(m, xyz, f[:, 3].contiguous(), n)
+        elif name == "EntityWarpIn":
+            p.entity_warp_in(m, xyz, n)
+        elif name == "SetSpeedFraction":
+            p.set_speed_fraction(m, one)
+        elif name == "SetMaxSpeed":
+            p.set_max_velocity(m, one)
+        elif name == "SetBallMass":
+            p.set_mass(m, one)
+        elif name == "SetBallAgility":
+            p.set_agility(m, one)
+        elif name == "SetBallRadius":
+            p.set_radius(m, one)
+        elif name == "SetBallVelocity":
+            p.set_velocity(m, xyz)
+        elif name == "SetBallMassive":
+            p.massive = torch.where(m, n != 0, p.massive)
+        elif name == "SetBallInteractive":
+            p.interactive = torch.where(m, n != 0, p.interactive)
+        elif name == "SetBallPosition":                 # the new and old position
+            p.pos = torch.where(m[:, None], xyz, p.pos)
+            p.old_pos = torch.where(m[:, None], xyz, p.old_pos)
+        elif name == "UncloakBall":
+            self.uncloak(m)
+        elif name == "SetMaxAngularSpeed":
+            p.set_max_angular_speed(m, one)
+        elif name == "SetBallAngularVelocity":
+            p.set_angular_velocity(m, xyz)
+        elif name == "SetBallRotation":
+            p.set_rotation(m, f)
+        elif name == "SetBallAngularAgility":
+            p.set_rot_agility(m, one)
+        elif name == "SetMaxAngularVelocity":
+            pass                                        # the park has no such method: never applied
+        elif name == "SetBallTroll":
+            p.set_ball_troll(m, n)
+        elif name == "SetBallFree":                     # a flag != 0 frees
+            p.set_free(m, n)
+        else:
+            raise ValueError(f"{name} is not applied by the flight park's server layer")
+
+    def evolve(self) -> None:
+        self.park.evolve()
+
+    def stream_fields(self) -> dict:
+        """The fields WriteBallToStream writes (Thunkers.cpp:3180-3377), every row, on the host."""
+        p = self.park
+        out = {k: getattr(p, k).detach().cpu() for k in ("ids", "mode", "radius", "pos", "free", "massive",
+                                                          "interactive", "mass", "cloaked", "max_vel", "vel",
+                                                          "agility", "speed_fraction", "goto", "follow_id",
+                                                          "follow_range", "effect_stamp", "last_collision",
+                                                          "owner_id", "rot", "max_ang_vel", "ang_vel",
+                                                          "rot_agility")}
+        out["dynamical"] = bool(p.dynamical_orientation)
+        return out
+
+
+@dataclass
+class Slot:
+    """One push: one Actions call for every masked world."""
+    kind: int
+    ok: torch.Tensor                    # [W] queued
+    ball: torch.Tensor                  # [W] Destiny id
+    row: torch.Tensor                   # [W] the ball's row, or -1
+    target: torch.Tensor                # [W] the target's id (FollowBall, Orbit)
+    trow: torch.Tensor                  # [W] the target's row, or -1
+    f: torch.Tensor                     # [W, 4] the float arguments
+    n: torch.Tensor                     # [W] the int argument
+    loc: torch.Tensor                   # [W] SetBallPosition: is local; CloakBall: its bubble (0, or -1)
+
+
+@dataclass
+class Batch:
+    """One tick's update batches, every world (the fields of exact_ballpark.vec_server.Batch)."""
+    stamp: torch.Tensor
+    clock: torch.Tensor
+    slots: list
+    route: torch.Tensor                 # [W, J] NONE, BUBBLE or CHARACTER
+    notices: list = field(default_factory=list)     # (slot j, recipients [R], the park's fields there or None)
+    additions: tuple | None = None      # (fresh [R], listed [R], the park's fields or None)
+    gets_bubble: torch.Tensor | None = None
+    has_character: torch.Tensor | None = None
+    ticked: torch.Tensor | None = None
+
+
+class VecServer:
+    """The server layer over an adapter (the module's docstring)."""
+
+    def __init__(self, adapter: ModesAdapter, pilots=None):
+        self.a = A = adapter
+        self.W, self.R, self.dev = A.W, A.R, A.dev
+        self.pilot = (torch.full((self.R,), -1, dtype=I64, device=self.dev) if pilots is None
+                      else torch.as_tensor(pilots, dtype=I64).to(self.dev))
+        clock = A.clock()
+        self.stamp_for_system = torch.where(clock == 0, 0, clock + 1)     # Actions' first stamp
+        self.settled = torch.zeros(self.R, dtype=BOOL, device=self.dev)   # the old bubble is the bubble
+        self.dead = torch.zeros(self.W, dtype=BOOL, device=self.dev)
+        self._bubble_time = torch.full((self.W,), -1, dtype=I64, device=self.dev)
+        self._fresh = torch.zeros(self.R, dtype=BOOL, device=self.dev)
+        self._listed = torch.zeros(self.R, dtype=BOOL, device=self.dev)
+        self._seen_first = False
+        self.slots: list = []
+        self._reset_last()
+        self.batch: Batch | None = None
+
+    def _reset_last(self) -> None:
+        W, d = self.W, self.dev
+        self.last = {"kind": torch.zeros(W, dtype=I64, device=d), "ball": torch.zeros(W, dtype=I64, device=d),
+                     "target": torch.zeros(W, dtype=I64, device=d), "f": torch.zeros(W, 4, dtype=F64, device=d),
+                     "n": torch.zeros(W, dtype=I64, device=d), "loc": torch.zeros(W, dtype=I64, device=d)}
+
+    def push(self, kind, mask, ball, target=None, f=None, n=None, loc=None) -> Slot:
+        """An Actions call (a kind's code or event name) for every world in mask [W]: ball [W] ids, target [W] ids
+        (FollowBall, Orbit), f [W, k<=4] floats, n [W] the int argument, loc [W] SetBallPosition's is_local_ball.
+        CloakBall captures the ball's bubble (0, or -1 before its old bubble is its bubble) and is not queued for a
+        ball not in the park; a call equal to the world's last queued call is dropped."""
+        k = CODE[kind] if isinstance(kind, str) else int(kind)
+        if k not in self.a.kinds:
+            raise ValueError(f"{KINDS[k] or kind} is not applied by this park")
+        W, d = self.W, self.dev
+        z = lambda dt: torch.zeros(W, dtype=dt, device=d)                    # noqa: E731
+        mask = torch.as_tensor(mask).to(device=d, dtype=BOOL)
+        ball = torch.as_tensor(ball).to(device=d, dtype=I64)
+        target = z(I64) if target is None else torch.as_tensor(target).to(device=d, dtype=I64)
+        ff = torch.zeros(W, 4, dtype=F64, device=d)
+        if f is not None:
+            f = torch.as_tensor(f).to(device=d, dtype=F64).reshape(W, -1)
+            ff[:, :f.shape[1]] = f
+        n = z(I64) if n is None else torch.as_tensor(n).to(device=d, dtype=I64)
+        loc = z(I64) if loc is None else torch.as_tensor(loc).to(device=d, dtype=I64)
+        row = self.a.lookup(ball)
+        trow = self.a.lookup(target) if k in FOLLOWS else z(I64) - 1
+        if k == CLOAK:
+            loc = torch.where(self.settled[row.clamp(min=0)], 0, -1)
+            mask = mask & (row >= 0)
+        last = self.last
+        dup = ((last["kind"] == k) & (last["ball"] == ball) & (last["target"] == target)
+               & (last["f"] == ff).all(dim=1) & (last["n"] == n) & (last["loc"] == loc))
+        ok = mask & ~dup
+        for key, val in (("kind", torch.full((W,), k, dtype=I64, device=d)), ("ball", ball), ("target", target),
+                         ("n", n), ("loc", loc)):
+            last[key] = torch.where(ok, val, last[key])
+        last["f"] = torch.where(ok[:, None], ff, last["f"])
+        slot = Slot(k, ok, ball, row, target, trow, ff, n, loc)
+        self.slots.append(slot)
+        return slot
+
+    def _rows(self, slot: Slot) -> tuple:
+        """The call as per-row masks and arguments: a row is commanded iff its world's call is queued for it."""
+        A = self.a
+        w = A.world
+        m = slot.ok[w] & (slot.row[w] == A.arange)
+        return m, slot.trow[w], slot.f[w], slot.n[w]
+
+    def pre_tick(self, snapshot: bool | None = None, mask=None) -> None:
+        """The Ticker's tick (TIME-712): the stamp moves, the queue is flushed and applied (CloakBall after the bubble
+        update), the events routed. `snapshot`: record the park's fields where the streams would be written (by
+        default when an uncloak, a SetBallInteractive, a SetBallTroll or the first pre-tick can send one)."""
+        if mask is not None:
+            raise NotImplementedError("OnTick's mask is not built for the server layer")
+        A = self.a
+        clock = A.clock().clone()
+        stamp = self.stamp_for_system
+        self.stamp_for_system = clock + 1
+        slots, self.slots = self.slots, []
+        self._reset_last()
+        kinds = {s.kind for s in slots}
+        if snapshot is None:
+            snapshot = (UNCLOAK in kinds) or (INTERACTIVE in kinds) or (TROLL in kinds) or not self._seen_first
+        for s in slots:                                     # every queued call but CloakBall, in queue order
+            if s.kind != CLOAK:
+                A.apply(s.kind, *self._rows(s))
+        # BubbleUpdater: the additions once per park time (a second pre-tick at the same time reuses the lists)
+        user = A.interactive & A.exists
+        fresh = user & ~self.settled
+        listed = A.exists & (A.cloaked == 0)
+        fresh = fresh & A.any_in_world(listed)[A.world]
+        again = (clock == self._bubble_time)[A.world]
+        fresh = torch.where(again, self._fresh, fresh)
+        listed = torch.where(again, self._listed, listed)
+        self.settled = torch.where(again, self.settled, self.settled | user)
+        self._bubble_time, self._fresh, self._listed = clock, fresh, listed
+        additions = (fresh, listed, A.stream_fields() if snapshot else None)
+        self._seen_first = True
+        live = A.any_in_world(A.interactive & A.exists)
+        route = torch.zeros(self.W, len(slots), dtype=torch.int8, device=self.dev)
+        notices = []
+        for j, s in enumerate(slots):                       # the history
+            valid = s.ok & (s.row >= 0)
+            safe = s.row.clamp(min=0)
+            if s.kind == CLOAK:                             # to the bubble it was queued in; then applied
+                r = torch.where(s.ok & (s.loc == 0), BUBBLE, NONE)
+                m, _, f, n = self._rows(s)
+                A.cloak(m, n, f[:, 0])
+            elif s.kind == UNCLOAK:                         # to its own character; AddBallsToPark to the others
+                own = valid & A.interactive[safe] & (self.pilot[safe] >= 0) & live
+                r = torch.where(own, CHARACTER, NONE)
+                rec = ((valid & live)[A.world] & A.interactive & A.exists & (A.arange != s.row[A.world])
+                       & (self.pilot >= 0))
+                notices.append((j, rec, A.stream_fields() if snapshot else None))
+            elif s.kind == SETPOS:                          # a local ball's move is sent nowhere
+                go = valid & (s.loc == 0) & live
+                r = torch.where(go, torch.where(A.cloaked[safe] == 0, BUBBLE,
+                                                torch.where(self.pilot[safe] >= 0, CHARACTER, NONE)), NONE)
+            else:
+                go = valid & live & (s.ball > 0)
+                r = torch.where(go, torch.where(A.cloaked[safe] == 0, BUBBLE,
+                                                torch.where(self.pilot[safe] >= 0, CHARACTER, NONE)), NONE)
+            route[:, j] = r.to(torch.int8)
+        self.batch = Batch(stamp=stamp, clock=clock, slots=slots, route=route, notices=notices, additions=additions)
+
+    def evolve(self, mask=None) -> None:
+        """The park's tick; a world whose bubble is dead is recorded (refused by `check`)."""
+        if mask is not None:
+            raise NotImplementedError("OnTick's mask is not built for the server layer")
+        A = self.a
+        self.dead = self.dead | ~A.any_in_world(A.interactive & A.exists)
+        A.evolve()
+
+    def post_tick(self, mask=None) -> None:
+        """send_batch: per row (its pilot), whether it gets the bubble's narrowcast and a character update."""
+        A, b = self.a, self.batch
+        bubble = ((b.route == BUBBLE).any(dim=1) if b.route.shape[1]
+                  else torch.zeros(self.W, dtype=BOOL, device=self.dev))
+        has = torch.zeros(self.R, dtype=BOOL, device=self.dev)
+        for j, s in enumerate(b.slots):
+            has = has | (s.ok[A.world] & (s.row[A.world] == A.arange) & (b.route[:, j] == CHARACTER)[A.world])
+        for _, rec, _ in b.notices:
+            has = has | rec
+        has = has | b.additions[0]
+        pilot = self.pilot >= 0
+        b.has_character = has & pilot
+        b.gets_bubble = bubble[A.world] & A.interactive & A.exists & pilot
+
+    def tick(self) -> None:
+        self.pre_tick()
+        self.evolve()
+        self.post_tick()
+
+    def check(self) -> None:
+        if bool(self.dead.any()):
+            bad = torch.nonzero(self.dead).flatten().tolist()
+            raise RuntimeError(f"worlds {bad[:8]} had no interactive ball at an evolve: on the master their balls "
+                               "would not be evolved (TIME-714), which the batched park does not model")

@@ -424,9 +424,43 @@ def make_composed() -> None:
               f"{sum(len(b['events']) for b in batches)} events, {time.time() - t:.0f} s", flush=True)
 
 
+def make_server() -> None:
+    """server_{modes,modes_do}: the reference's server-layer scenarios over the flight-mode park (tests/server_cases.py:
+    40 worlds of one bubble with their pilots, 14 ticks of Actions calls each: conflicting commands, duplicates dropped
+    and kept, cloaks and uncloaks in both orders, local and non-local SetBallPosition, follows and orbits of a
+    cloaking ship, warps and warp-ins with followers, every setter, refused values; seeds 1 and 2; without and with
+    dynamical orientation), recorded on the reference's VecServer (torch path, over its VecModesPark on the CPU) by
+    tests/golden/server_trace.py's driver. Each scenario set is first run by the reference's own comparison against
+    its scalar server layer (server_cases.run: every ball's state and every client's update list): 0 differences."""
+    import server_cases as S
+    import server_trace as st
+    import exact_ballpark.vec_server as VS
+    from exact_ballpark.vec_modes import VecModesPark
+    for do in (False, True):
+        t = time.time()
+        runs = []
+        for seed in (1, 2):
+            cs = S.cases(seed, 40, "modes", do=do, ticks=14)
+            res = S.run(cs, "modes", "cpu", do=do, evolve=True)
+            if res["rows"] or res["sends"] or not res["compared"]:
+                raise RuntimeError(f"seed {seed}: the reference's server layer differs from its scalar one")
+            parks, batches = [], []
+
+            def on_tick(tk, server):
+                parks.append(tr.field_digests(server.a.park))
+                batches.append(st.batch_digests(server))
+            server, _ = st.build(VS, VecModesPark, cs, do, "cpu")
+            st.drive(server, cs, True, "cpu", on_tick)
+            runs.append({"cases": cs, "do": do, "evolve": True, "park": np.array(parks, dtype=np.uint64),
+                         "batch": batches})
+        name = "server_modes_do" if do else "server_modes"
+        st.save(HERE / name, runs)
+        print(f"  {name}: {len(runs)} runs of {len(runs[0]['cases'])} worlds, {time.time() - t:.0f} s", flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed"), default=None)
+    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed", "server"), default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
     a = ap.parse_args()
     if a.only in (None, "libm"):
@@ -443,6 +477,8 @@ def main() -> None:
         make_combat()
     if a.only in (None, "composed"):
         make_composed()
+    if a.only in (None, "server"):
+        make_server()
 
 
 if __name__ == "__main__":

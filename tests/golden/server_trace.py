@@ -1,0 +1,194 @@
+"""Golden traces of the server layer over the flight-mode park: the reference's server scenarios (worlds of one bubble
+with their pilots and each tick's Actions calls, as its server scenario generator states them), the driver that runs
+them through any server layer with the reference's API (push, pre_tick, evolve, post_tick, batch), and each tick's
+digests: the park's state and the update batch (the stamps, each queued call's flags and rows, the routes, the
+uncloaks' recipients and the bubble's additions with the park's fields at each of them, and who gets the bubble's
+narrowcast and a character update).
+
+`make_golden.py` records traces by driving the reference's own batched server layer (exact_ballpark.vec_server's
+VecServer, its torch path, over its VecModesPark on the CPU), which the reference holds bit for bit to its scalar
+server layer (exact_ballpark.server over FullBallpark) on these very scenarios; the tests replay them on this
+package's server layer.
+"""
+
+from __future__ import annotations
+
+import gzip
+import hashlib
+import json
+from collections import defaultdict
+from pathlib import Path
+
+import numpy as np
+import torch
+
+import trace as tr
+
+GOLDEN = Path(__file__).resolve().parent
+PARK_FIELDS = tr.FIELDS
+STREAM_FIELDS = ("ids", "mode", "radius", "pos", "free", "massive", "interactive", "mass", "cloaked", "max_vel", "vel",
+                 "agility", "speed_fraction", "goto", "follow_id", "follow_range", "effect_stamp", "last_collision",
+                 "owner_id", "rot", "max_ang_vel", "ang_vel", "rot_agility")
+ACTION_KINDS = {"go_to_point": "GotoPoint", "go_to_direction": "GotoDirection", "stop": "Stop",
+                "follow_ball": "FollowBall", "orbit": "Orbit", "warp_to": "WarpTo", "entity_warp_in": "EntityWarpIn",
+                "set_speed_fraction": "SetSpeedFraction", "set_max_speed": "SetMaxSpeed",
+                "set_ball_mass": "SetBallMass", "set_ball_agility": "SetBallAgility",
+                "set_ball_radius": "SetBallRadius", "set_ball_velocity": "SetBallVelocity",
+                "set_ball_massive": "SetBallMassive", "set_ball_interactive": "SetBallInteractive",
+                "set_ball_position": "SetBallPosition", "cloak_ball": "CloakBall", "uncloak_ball": "UncloakBall",
+                "set_max_angular_speed": "SetMaxAngularSpeed", "set_ball_angular_velocity": "SetBallAngularVelocity",
+                "set_ball_rotation": "SetBallRotation", "set_ball_angular_agility": "SetBallAngularAgility",
+                "set_max_angular_velocity": "SetMaxAngularVelocity"}
+
+
+def _h(name: str, a) -> np.uint64:
+    x = tr.canonical(a)
+    d = hashlib.sha256(name.encode() + str(x.shape).encode() + x.tobytes()).digest()
+    return np.frombuffer(d[:8], dtype=np.uint64)[0]
+
+
+def _fields_digest(fields) -> np.uint64:
+    if fields is None:
+        return np.uint64(0)
+    parts = [_h(k, fields[k]) for k in STREAM_FIELDS]
+    d = hashlib.sha256(np.array(parts, dtype=np.uint64).tobytes() + bytes([int(bool(fields["dynamical"]))])).digest()
+    return np.frombuffer(d[:8], dtype=np.uint64)[0]
+
+
+def batch_digests(server) -> np.ndarray:
+    """The last tick's update batch as digests (uint64): the stamps and clocks, the routes, each queued call's kind,
+    queued flag, row, target row and local argument, each uncloak's recipients and the park's fields there, the
+    bubble's additions (fresh, listed, fields), and the narrowcast and character flags."""
+    b = server.batch
+    out = [_h("stamp", b.stamp), _h("clock", b.clock), _h("route", b.route.to(torch.int64))]
+    for j, s in enumerate(b.slots):
+        out += [np.uint64(s.kind), _h(f"ok{j}", s.ok), _h(f"row{j}", s.row), _h(f"trow{j}", s.trow),
+                _h(f"loc{j}", s.loc)]
+    for j, rec, fields in b.notices:
+        out += [np.uint64(j), _h("notice", rec), _fields_digest(fields)]
+    fresh, listed, fields = b.additions
+    out += [_h("fresh", fresh), _h("listed", listed), _fields_digest(fields), _h("gets_bubble", b.gets_bubble),
+            _h("has_character", b.has_character)]
+    return np.array(out, dtype=np.uint64)
+
+
+# ---- the batch's park and server ----
+
+def build(server_mod, park_cls, cs: list, do: bool, device, friction: float = 1.0e6, tick_ms: int = 1000):
+    """The server layer (server_mod's VecServer over its ModesAdapter) over a flight park of the worlds cs:
+    (server, {(world, ball id): row})."""
+    rows = [(w, b) for w in cs for b in w["balls"]]
+    p = park_cls(len(rows), friction=friction, tick_interval_ms=tick_ms, device=device, dynamical_orientation=do)
+    p.load([{"id": b["id"], "world": w["id"], "time": 0, "mass": b["mass"], "radius": b["radius"],
+             "max_vel": b["max_vel"], "pos": b["pos"], "vel": b["vel"], "agility": b["agility"],
+             "speed_fraction": b["sf"], "free": True, "massive": b["massive"], "interactive": b["interactive"],
+             "cloaked": 0, "bubble": 0, "moribund": False, "max_ang_vel": b["max_ang_vel"],
+             "rot_agility": b["rot_agility"]} for w, b in rows])
+    a = server_mod.ModesAdapter(p)
+    index = {(w["id"], b["id"]): i for i, (w, b) in enumerate(rows)}
+    pilots = [-1] * a.R
+    for w in cs:
+        for bid, pp in w["pilots"].items():
+            pilots[index[(w["id"], int(bid))]] = pp
+    return server_mod.VecServer(a, pilots), index
+
+
+def pushes(cs: list, t: int, device) -> list:
+    """Tick t's calls of every world as pushes: the j-th calls of one kind of all worlds together, each world's calls
+    in its own order: [(kind, mask, ball, target, f, n, loc)]."""
+    W = len(cs)
+    out = []
+    width = max((len(w["ticks"][t]) for w in cs), default=0)
+    for j in range(width):
+        by_kind = defaultdict(list)
+        for wi, w in enumerate(cs):
+            calls = w["ticks"][t]
+            if j < len(calls):
+                by_kind[ACTION_KINDS[calls[j][0]]].append((wi, calls[j][1]))
+        for kind, items in by_kind.items():
+            mask = torch.zeros(W, dtype=torch.bool)
+            ball, target, n, loc = (torch.zeros(W, dtype=torch.int64) for _ in range(4))
+            f = torch.zeros(W, 4, dtype=torch.float64)
+            for wi, args in items:
+                mask[wi] = True
+                ball[wi] = int(args[0])
+                rest = list(args[1:])
+                if kind in ("FollowBall", "Orbit"):
+                    target[wi], f[wi, 0] = int(rest[0]), float(rest[1])
+                elif kind == "WarpTo":
+                    f[wi, :4] = torch.tensor([float(x) for x in rest[:4]], dtype=torch.float64)
+                    n[wi] = int(rest[4])
+                elif kind == "EntityWarpIn":
+                    f[wi, :3] = torch.tensor([float(x) for x in rest[:3]], dtype=torch.float64)
+                    n[wi] = int(rest[3])
+                elif kind in ("SetBallMassive", "SetBallInteractive"):
+                    n[wi] = int(rest[0])
+                elif kind == "SetBallPosition":
+                    f[wi, :3] = torch.tensor([float(x) for x in rest[:3]], dtype=torch.float64)
+                    loc[wi] = 1 if rest[3] is True else 0
+                elif kind == "CloakBall":
+                    n[wi], f[wi, 0] = int(rest[0]), float(rest[1])
+                elif rest:
+                    f[wi, :len(rest)] = torch.tensor([float(x) for x in rest], dtype=torch.float64)
+            out.append((kind, *(x.to(device) for x in (mask, ball, target, f, n, loc))))
+    return out
+
+
+def drive(server, cs: list, evolve: bool, device, on_tick=None) -> None:
+    """Each tick: the worlds' calls pushed, the pre-tick, the park's tick (unless `evolve` is false), the post-tick;
+    on_tick(t, server) after each."""
+    for t in range(len(cs[0]["ticks"])):
+        for kind, mask, ball, target, f, n, loc in pushes(cs, t, device):
+            server.push(kind, mask, ball, target, f, n, loc)
+        server.pre_tick()
+        if evolve:
+            server.evolve()
+        server.post_tick()
+        if on_tick is not None:
+            on_tick(t, server)
+
+
+# ---- the golden bundle ----
+
+def save(path: Path, runs: list) -> None:
+    """runs: [{"cases", "do", "evolve", "park" [T, F] uint64, "batch": [T arrays]}]."""
+    body = [{"cases": r["cases"], "do": r["do"], "evolve": r["evolve"]} for r in runs]
+    with gzip.open(str(path) + ".json.gz", "wt") as f:
+        json.dump(body, f)
+    arrays = {}
+    for i, r in enumerate(runs):
+        arrays[f"r{i}_park"] = r["park"]
+        for t, b in enumerate(r["batch"]):
+            arrays[f"r{i}_batch{t}"] = b
+    np.savez_compressed(str(path) + ".npz", **arrays)
+
+
+def load(path: Path) -> list:
+    with gzip.open(str(path) + ".json.gz", "rt") as f:
+        body = json.load(f)
+    z = np.load(str(path) + ".npz")
+    for i, r in enumerate(body):
+        r["park"] = z[f"r{i}_park"]
+        r["batch"] = [z[f"r{i}_batch{t}"] for t in range(len(r["park"]))]
+        for w in r["cases"]:
+            w["pilots"] = {int(k): v for k, v in w["pilots"].items()}
+            w["ticks"] = [[(c[0], tuple(c[1])) for c in calls] for calls in w["ticks"]]
+    return body
+
+
+def replay(server_mod, park_cls, run: dict, device) -> list:
+    """A recorded run on server_mod's layer over park_cls: the differences [(tick, 'park', fields) or (tick, 'batch')]."""
+    server, _ = build(server_mod, park_cls, run["cases"], run["do"], device)
+    bad = []
+
+    def on_tick(t, s):
+        got = tr.field_digests(s.a.park)
+        mm = [PARK_FIELDS[k] for k in range(len(PARK_FIELDS)) if got[k] != run["park"][t][k]]
+        if mm:
+            bad.append((t, "park", mm))
+        b = batch_digests(s)
+        want = run["batch"][t]
+        if b.shape != want.shape or not (b == want).all():
+            bad.append((t, "batch"))
+    drive(server, run["cases"], run["evolve"], device, on_tick)
+    return bad
