@@ -9,7 +9,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libebb.so"
-ABI = 4
+ABI = 5
 COLLIDE_MAX_SLOTS = 64          # include/ebb.h: EBB_COLLIDE_MAX_SLOTS
 COLLIDE_MAX_STATICS = 64        # include/ebb.h: EBB_COLLIDE_MAX_STATICS
 
@@ -46,6 +46,23 @@ class ComposedState(ctypes.Structure):
                 + [("hit_cap", ctypes.c_int64)])
 
 
+class ServerState(ctypes.Structure):
+    """include/ebb.h's EbbServerState, field for field."""
+    _fields_ = ([("flight", FlightState), ("worlds", ctypes.c_int64), ("width", ctypes.c_int64)]
+                + [(k, ctypes.c_void_p) for k in ("world_rows", "world_ids", "pilot", "exists", "label", "cloaked",
+                                                  "bubble", "refiled", "stamp_for_system", "bubble_time", "dead",
+                                                  "settled", "fresh", "listed")]
+                + [("neg_kdt", ctypes.c_double), ("master", ctypes.c_int32)])
+
+
+class ServerQueue(ctypes.Structure):
+    """include/ebb.h's EbbServerQueue, field for field."""
+    _fields_ = ([("slots", ctypes.c_int64)]
+                + [(k, ctypes.c_void_p) for k in ("kinds", "mask", "ball", "target", "n", "loc_in", "f", "ok", "row",
+                                                  "trow", "loc", "route", "notice", "stamp", "clock", "has_character",
+                                                  "gets_bubble")])
+
+
 def lib() -> ctypes.CDLL:
     """The loaded library (loaded and checked on first use)."""
     global _lib
@@ -74,6 +91,7 @@ def lib() -> ctypes.CDLL:
     L.ebb_combat_tick.argtypes = [ctypes.POINTER(CombatState), p, i64, p, p, i32]
     L.ebb_composed_tick.argtypes = [ctypes.POINTER(ComposedState), p, i64, p, p, i32]
     L.ebb_composed_file.argtypes = [ctypes.POINTER(ComposedState), p, p, p, p, p]
+    L.ebb_server_tick.argtypes = [ctypes.POINTER(ServerState), ctypes.POINTER(ServerQueue), i32, i64, i64, p, i32]
     L.ebb_glibc_srand.argtypes = [p, i64, p, p]
     L.ebb_glibc_rand.argtypes = [p, i64, i64, p, p]
     L.ebb_flight_snap.argtypes = [ctypes.POINTER(FlightState), p, i32, p, i32]

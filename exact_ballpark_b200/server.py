@@ -15,21 +15,27 @@ pilot, whether it gets the bubble's narrowcast and a character update (ParkUpdat
 tick's update batch as tensors: the stamps, the queued calls, their routes, the uncloaks' recipients, the additions
 and the flags, with the park's fields where the streams would be written (`stream_fields`).
 
-Every park write is the park's own command or setter (exact_ballpark_b200.modes, on the device); the layer adds only
+Two paths with one result, bit for bit. kernel="torch": every park write is the park's own command or setter
+(exact_ballpark_b200.modes, on the device) over all worlds at once, one queued call after another; the layer adds only
 index work (masks, gathers, comparisons) and the cloak's float sum radius + range as float32, as the C++ does.
+kernel="cuda": the native library's server kernel (ebb_server_tick), one thread a world walking its own queue, every
+command restated for one row; one launch for the whole pre-tick (or one per history segment when the park's fields are
+recorded for the streams), one for the dead-bubble test before the park's tick and one for the send flags after it.
+`ServerGraph` captures a kernel-path tick with a fixed schedule of pushes as one CUDA graph.
 
 Not built: the encoding of the batches into Destiny's tuples and streams (`decode`), the pending queries and the undo,
-OnTick's intervals, the kernel path (one launch for the pre-tick), the other parks' adapters, bubbles other than one a
-world.
+OnTick's intervals, the other parks' adapters, bubbles other than one a world.
 """
 
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass, field
 
 import torch
 
-from .modes import WARP
+from . import _native
+from .modes import WARP, tick as _park_tick
 
 F64, F32, I64, BOOL = torch.float64, torch.float32, torch.int64, torch.bool
 
@@ -243,11 +249,14 @@ class Batch:
 
 
 class VecServer:
-    """The server layer over an adapter (the module's docstring)."""
+    """The server layer over an adapter (the module's docstring): kernel "torch" or "cuda"."""
 
-    def __init__(self, adapter: ModesAdapter, pilots=None):
+    def __init__(self, adapter: ModesAdapter, pilots=None, kernel: str = "torch", block: int = 128):
+        if kernel not in ("torch", "cuda"):
+            raise ValueError(f"kernel {kernel!r}: 'torch' or 'cuda'")
         self.a = A = adapter
         self.W, self.R, self.dev = A.W, A.R, A.dev
+        self.kernel, self.block = kernel, int(block)
         self.pilot = (torch.full((self.R,), -1, dtype=I64, device=self.dev) if pilots is None
                       else torch.as_tensor(pilots, dtype=I64).to(self.dev))
         clock = A.clock()
@@ -261,6 +270,11 @@ class VecServer:
         self.slots: list = []
         self._reset_last()
         self.batch: Batch | None = None
+        self._q = None
+        if kernel == "cuda":
+            if self.dev.type != "cuda":
+                raise ValueError("the server kernel runs on a CUDA device")
+            self._state = self._server_state()
 
     def _reset_last(self) -> None:
         W, d = self.W, self.dev
@@ -268,11 +282,61 @@ class VecServer:
                      "target": torch.zeros(W, dtype=I64, device=d), "f": torch.zeros(W, 4, dtype=F64, device=d),
                      "n": torch.zeros(W, dtype=I64, device=d), "loc": torch.zeros(W, dtype=I64, device=d)}
 
+    # ---- the kernel's state and queue (include/ebb.h: EbbServerState, EbbServerQueue) ----
+    def _server_state(self) -> _native.ServerState:
+        A, p = self.a, self.a.park
+        self._const = {"world_rows": A.rows_of_world.contiguous(), "world_ids": A.ids_of_world.contiguous(),
+                       "pilot": self.pilot.contiguous(), "exists": A.exists.contiguous()}
+        st = _native.ServerState()
+        st.flight = p.state()
+        st.worlds, st.width = self.W, A.rows_of_world.shape[1]
+        for k, t in self._const.items():
+            setattr(st, k, t.data_ptr())
+        for k, t in (("label", p.world), ("cloaked", p.cloaked), ("bubble", p.bubble), ("refiled", p.refiled),
+                     ("stamp_for_system", self.stamp_for_system), ("bubble_time", self._bubble_time),
+                     ("dead", self.dead), ("settled", self.settled), ("fresh", self._fresh),
+                     ("listed", self._listed)):
+            if not t.is_contiguous() or t.device != self.dev:
+                raise ValueError(f"the server kernel writes {k} in place: a contiguous tensor on {self.dev}")
+            setattr(st, k, t.data_ptr())
+        st.neg_kdt = -p.friction * p.dt
+        st.master = int(A.master)
+        return st
+
+    def _queue(self, kinds: list, cols: dict | None = None) -> dict:
+        """The queue's tensors for kinds [J]: the pushes' columns ([J, W] stacks, given or zeros) and the outputs."""
+        J, W, R, d = len(kinds), self.W, self.R, self.dev
+        z = lambda *shape, dt=I64: torch.zeros(*shape, dtype=dt, device=d)          # noqa: E731
+        q = {"kinds": torch.tensor(kinds, dtype=torch.int32).to(d), "mask": z(J, W, dt=BOOL), "ball": z(J, W),
+             "target": z(J, W), "f": z(J, W, 4, dt=F64), "n": z(J, W), "loc_in": z(J, W),
+             "ok": z(J, W, dt=BOOL), "row": z(J, W), "trow": z(J, W), "loc": z(J, W),
+             "route": z(W, J, dt=torch.int8), "notice": z(J, R, dt=BOOL), "stamp": z(W), "clock": z(W),
+             "has_character": z(R, dt=BOOL), "gets_bubble": z(R, dt=BOOL)}
+        if cols is not None:
+            for k, v in cols.items():
+                q[k].copy_(v)
+        qs = _native.ServerQueue()
+        qs.slots = J
+        for k in ("kinds", "mask", "ball", "target", "n", "loc_in", "f", "ok", "row", "trow", "loc", "route",
+                  "notice", "stamp", "clock", "has_character", "gets_bubble"):
+            setattr(qs, k, q[k].data_ptr())
+        q["struct"] = qs
+        return q
+
+    def _launch(self, q: dict, phase: int, j0: int = 0, j1: int = 0) -> None:
+        with torch.cuda.device(self.dev):
+            stream = torch.cuda.current_stream(self.dev).cuda_stream
+            rc = _native.lib().ebb_server_tick(ctypes.byref(self._state), ctypes.byref(q["struct"]), int(phase),
+                                               int(j0), int(j1), stream, self.block)
+        _native.check(rc, "ebb_server_tick")
+
+    # ---- the queue ----
     def push(self, kind, mask, ball, target=None, f=None, n=None, loc=None) -> Slot:
         """An Actions call (a kind's code or event name) for every world in mask [W]: ball [W] ids, target [W] ids
         (FollowBall, Orbit), f [W, k<=4] floats, n [W] the int argument, loc [W] SetBallPosition's is_local_ball.
         CloakBall captures the ball's bubble (0, or -1 before its old bubble is its bubble) and is not queued for a
-        ball not in the park; a call equal to the world's last queued call is dropped."""
+        ball not in the park; a call equal to the world's last queued call is dropped. On the kernel path the call is
+        recorded as given and tested in the pre-tick's launch (its flags and rows filled in there)."""
         k = CODE[kind] if isinstance(kind, str) else int(kind)
         if k not in self.a.kinds:
             raise ValueError(f"{KINDS[k] or kind} is not applied by this park")
@@ -287,6 +351,11 @@ class VecServer:
             ff[:, :f.shape[1]] = f
         n = z(I64) if n is None else torch.as_tensor(n).to(device=d, dtype=I64)
         loc = z(I64) if loc is None else torch.as_tensor(loc).to(device=d, dtype=I64)
+        if self.kernel == "cuda":
+            slot = Slot(k, None, ball, None, target, None, ff, n, loc)
+            slot.mask = mask
+            self.slots.append(slot)
+            return slot
         row = self.a.lookup(ball)
         trow = self.a.lookup(target) if k in FOLLOWS else z(I64) - 1
         if k == CLOAK:
@@ -311,21 +380,28 @@ class VecServer:
         m = slot.ok[w] & (slot.row[w] == A.arange)
         return m, slot.trow[w], slot.f[w], slot.n[w]
 
+    def _snapshot(self, kinds, snapshot):
+        if snapshot is None:
+            snapshot = (UNCLOAK in kinds) or (INTERACTIVE in kinds) or (TROLL in kinds) or not self._seen_first
+        self._seen_first = True
+        return snapshot
+
+    # ---- the tick ----
     def pre_tick(self, snapshot: bool | None = None, mask=None) -> None:
         """The Ticker's tick (TIME-712): the stamp moves, the queue is flushed and applied (CloakBall after the bubble
         update), the events routed. `snapshot`: record the park's fields where the streams would be written (by
         default when an uncloak, a SetBallInteractive, a SetBallTroll or the first pre-tick can send one)."""
         if mask is not None:
             raise NotImplementedError("OnTick's mask is not built for the server layer")
+        if self.kernel == "cuda":
+            return self._pre_tick_kernel(snapshot)
         A = self.a
         clock = A.clock().clone()
         stamp = self.stamp_for_system
         self.stamp_for_system = clock + 1
         slots, self.slots = self.slots, []
         self._reset_last()
-        kinds = {s.kind for s in slots}
-        if snapshot is None:
-            snapshot = (UNCLOAK in kinds) or (INTERACTIVE in kinds) or (TROLL in kinds) or not self._seen_first
+        snapshot = self._snapshot({s.kind for s in slots}, snapshot)
         for s in slots:                                     # every queued call but CloakBall, in queue order
             if s.kind != CLOAK:
                 A.apply(s.kind, *self._rows(s))
@@ -340,7 +416,6 @@ class VecServer:
         self.settled = torch.where(again, self.settled, self.settled | user)
         self._bubble_time, self._fresh, self._listed = clock, fresh, listed
         additions = (fresh, listed, A.stream_fields() if snapshot else None)
-        self._seen_first = True
         live = A.any_in_world(A.interactive & A.exists)
         route = torch.zeros(self.W, len(slots), dtype=torch.int8, device=self.dev)
         notices = []
@@ -368,16 +443,63 @@ class VecServer:
             route[:, j] = r.to(torch.int8)
         self.batch = Batch(stamp=stamp, clock=clock, slots=slots, route=route, notices=notices, additions=additions)
 
+    def _pre_tick_kernel(self, snapshot) -> None:
+        """The pre-tick as the kernel: one launch, or, with the park's fields recorded, the queue and bubble update,
+        then the history split at each UncloakBall (the fields its notices send are read there)."""
+        A = self.a
+        slots, self.slots = self.slots, []
+        kinds = [s.kind for s in slots]
+        J = len(slots)
+        snapshot = self._snapshot(set(kinds), snapshot)
+        cols = None
+        if J:
+            cols = {"mask": torch.stack([s.mask for s in slots]), "ball": torch.stack([s.ball for s in slots]),
+                    "target": torch.stack([s.target for s in slots]), "f": torch.stack([s.f for s in slots]),
+                    "n": torch.stack([s.n for s in slots]), "loc_in": torch.stack([s.loc for s in slots])}
+        q = self._queue(kinds, cols)
+        notices, fields = [], None
+        if not snapshot:
+            self._launch(q, 0)
+            notices = [(j, q["notice"][j], None) for j, k in enumerate(kinds) if k == UNCLOAK]
+        else:
+            self._launch(q, 1)
+            fields = A.stream_fields()
+            j0 = 0
+            for j in [j for j, k in enumerate(kinds) if k == UNCLOAK]:
+                self._launch(q, 2, j0, j)
+                notices.append((j, q["notice"][j], A.stream_fields()))
+                j0 = j
+            self._launch(q, 2, j0, J)
+        self._finish(q, slots, notices, fields)
+
+    def _finish(self, q: dict, slots: list, notices: list, fields, live: bool = False) -> None:
+        """The Batch over the queue's tensors; the additions copied (an eager tick) or the live lists (a graph's)."""
+        for j, s in enumerate(slots):                       # the slots as the torch path holds them
+            s.ok, s.row, s.trow, s.loc = q["ok"][j], q["row"][j], q["trow"][j], q["loc"][j]
+        self._q = q
+        lists = (self._fresh, self._listed) if live else (self._fresh.clone(), self._listed.clone())
+        self.batch = Batch(stamp=q["stamp"], clock=q["clock"], slots=slots, route=q["route"], notices=notices,
+                           additions=(*lists, fields),
+                           gets_bubble=q["gets_bubble"], has_character=q["has_character"])
+
     def evolve(self, mask=None) -> None:
         """The park's tick; a world whose bubble is dead is recorded (refused by `check`)."""
         if mask is not None:
             raise NotImplementedError("OnTick's mask is not built for the server layer")
         A = self.a
-        self.dead = self.dead | ~A.any_in_world(A.interactive & A.exists)
+        if self.kernel == "cuda":
+            self._launch(self._q if self._q is not None else self._queue([]), 4)
+        else:
+            self.dead = self.dead | ~A.any_in_world(A.interactive & A.exists)
         A.evolve()
 
     def post_tick(self, mask=None) -> None:
         """send_batch: per row (its pilot), whether it gets the bubble's narrowcast and a character update."""
+        if mask is not None:
+            raise NotImplementedError("OnTick's mask is not built for the server layer")
+        if self.kernel == "cuda":                           # the flags' phase, in place in the batch
+            self._launch(self._q, 3)
+            return
         A, b = self.a, self.batch
         bubble = ((b.route == BUBBLE).any(dim=1) if b.route.shape[1]
                   else torch.zeros(self.W, dtype=BOOL, device=self.dev))
@@ -401,3 +523,72 @@ class VecServer:
             bad = torch.nonzero(self.dead).flatten().tolist()
             raise RuntimeError(f"worlds {bad[:8]} had no interactive ball at an evolve: on the master their balls "
                                "would not be evolved (TIME-714), which the batched park does not model")
+
+
+class ServerGraph:
+    """A kernel-path VecServer's tick with a fixed schedule of pushes, captured once as a CUDA graph (the drop-in for
+    exact_ballpark.vec_server.ServerGraph, vec_server.py:1200): before each replay the caller writes each push's
+    arguments into `inputs[j]` (mask, ball, target, f, n, loc: views of the queue's [J, W] buffers) and `tick()`
+    replays the pre-tick (one launch), the dead-bubble test, the park's tick and the send flags, and returns the graph's
+    Batch (its tensors refilled in place; no park fields recorded). Every state tensor is written in place by its
+    kernel, so nothing is re-bound between replays and eager setters between ticks are seen by the next replay."""
+
+    def __init__(self, server: VecServer, schedule: list):
+        if server.kernel != "cuda":
+            raise ValueError("a ServerGraph captures the kernel path (VecServer(..., kernel='cuda'))")
+        if server.slots:
+            raise ValueError("pushes are queued: tick them eagerly first")
+        self.server = srv = server
+        self.schedule = [CODE[k] if isinstance(k, str) else int(k) for k in schedule]
+        for k in self.schedule:
+            if k not in srv.a.kinds:
+                raise ValueError(f"{KINDS[k]} is not applied by this park")
+        p, d = srv.a.park, srv.dev
+        self.q = q = srv._queue(self.schedule)
+        self.inputs = [{"mask": q["mask"][j], "ball": q["ball"][j], "target": q["target"][j], "f": q["f"][j],
+                        "n": q["n"][j], "loc": q["loc_in"][j]} for j in range(len(self.schedule))]
+        if p.plan is None:
+            p.scratch()
+        else:
+            p.plan.tile_rows_on(d)
+        keep = [(t, t.clone()) for t in self._state_tensors()]
+        side = torch.cuda.Stream(device=d)                 # a warm-up of every launch, undone
+        side.wait_stream(torch.cuda.current_stream(d))
+        with torch.cuda.stream(side):
+            self._body()
+        torch.cuda.current_stream(d).wait_stream(side)
+        torch.cuda.synchronize(d)
+        for t, v in keep:
+            t.copy_(v)
+        del keep
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._body()
+        srv._seen_first = True
+        slots = [Slot(k, None, q["ball"][j], None, q["target"][j], None, q["f"][j], q["n"][j], q["loc_in"][j])
+                 for j, k in enumerate(self.schedule)]
+        notices = [(j, q["notice"][j], None) for j, k in enumerate(self.schedule) if k == UNCLOAK]
+        srv._finish(q, slots, notices, None, live=True)
+        self.out = srv.batch
+
+    def _state_tensors(self) -> list:
+        srv, p = self.server, self.server.a.park
+        return ([getattr(p, k) for k in p.row_tensors()] + [p.cloaked, p.bubble]
+                + [srv.stamp_for_system, srv._bubble_time, srv.dead, srv.settled, srv._fresh, srv._listed]
+                + [self.q[k] for k in ("ok", "row", "trow", "loc", "route", "notice", "stamp", "clock",
+                                       "has_character", "gets_bubble")])
+
+    def _body(self) -> None:
+        srv, p = self.server, self.server.a.park
+        srv._launch(self.q, 0)
+        srv._launch(self.q, 4)
+        _park_tick(p, p.block)
+        srv._launch(self.q, 3)
+
+    def tick(self) -> Batch:
+        if self.server.slots:
+            raise RuntimeError("eager pushes before a graph tick: the graph's tick pushes its own schedule")
+        self.graph.replay()
+        self.server.a.park.current_time += 1
+        self.server.batch = self.out
+        return self.out

@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define EBB_ABI_VERSION 4
+#define EBB_ABI_VERSION 5
 #define EBB_EINVAL (-1)
 #define EBB_ETOOBIG (-2)
 
@@ -103,6 +103,57 @@ typedef struct EbbComposedState {
     int64_t *level, *key, *mod, *hits;
     int64_t hit_cap;
 } EbbComposedState;
+
+/* The server layer over the flight park (exact_ballpark.vec_server.VecServer with its ModesAdapter): W worlds of one
+ * bubble, each world's rows listed in the order its balls were added ([W][width], -1 padded) with their Destiny ids
+ * (0 padded); per row its pilot (-1 none), the adapter's exists byte and the park's host-side columns (world label,
+ * cloak, bubble, the re-filing count); the layer's own state per world (the next stamp, the bubble update's park time,
+ * a dead bubble seen at an evolve) and per row (the old bubble settled, the last additions' fresh and listed flags).
+ * A queued call's kind is its event's code, the index of the event's name in the reference's KINDS table
+ * (vec_server.py:118-123). */
+enum {
+    EBB_KIND_GOTO_POINT = 1, EBB_KIND_GOTO_DIRECTION, EBB_KIND_STOP, EBB_KIND_FOLLOW_BALL, EBB_KIND_ORBIT,
+    EBB_KIND_WARP_TO, EBB_KIND_ENTITY_WARP_IN, EBB_KIND_SET_SPEED_FRACTION, EBB_KIND_SET_MAX_SPEED, EBB_KIND_SET_MASS,
+    EBB_KIND_SET_AGILITY, EBB_KIND_SET_RADIUS, EBB_KIND_SET_VELOCITY, EBB_KIND_SET_MASSIVE, EBB_KIND_SET_INTERACTIVE,
+    EBB_KIND_SET_POSITION, EBB_KIND_CLOAK, EBB_KIND_UNCLOAK, EBB_KIND_SET_MAX_ANGULAR_SPEED,
+    EBB_KIND_SET_ANGULAR_VELOCITY, EBB_KIND_SET_ROTATION, EBB_KIND_SET_ANGULAR_AGILITY,
+    EBB_KIND_SET_MAX_ANGULAR_VELOCITY, EBB_KIND_LAUNCH_MISSILE, EBB_KIND_SET_TROLL, EBB_KIND_SET_FREE
+};
+enum { EBB_ROUTE_NONE = 0, EBB_ROUTE_BUBBLE = 1, EBB_ROUTE_CHARACTER = 2 };
+#define EBB_SERVER_MAX_SLOTS 256
+typedef struct EbbServerState {
+    EbbFlightState flight;
+    int64_t worlds, width;
+    const int64_t *world_rows, *world_ids;     /* [W][width] */
+    const int64_t* pilot;                      /* [n] */
+    const uint8_t* exists;                     /* [n] */
+    const int64_t* label;                      /* [n] the park's world label */
+    int64_t *cloaked, *bubble, *refiled;       /* [n] */
+    int64_t *stamp_for_system, *bubble_time;   /* [W] */
+    uint8_t* dead;                             /* [W] */
+    uint8_t *settled, *fresh, *listed;         /* [n] */
+    double neg_kdt;                            /* -friction x dt: the decay factor's numerator */
+    int32_t master;
+} EbbServerState;
+
+/* One tick's queue: J slots (the pushes, in order), each a kind [J] and per world its pushed byte, ball id, target id,
+ * float arguments (4), int argument and SetBallPosition's local flag ([J][W], f [J][W][4]); out: per slot and world the
+ * queued flag, the ball's and target's rows (-1 none) and the local argument or CloakBall's bubble (0, or -1 before
+ * the ball's old bubble is its bubble) ([J][W]); the routes [W][J]; the uncloaks' AddBallsToPark recipients [J][n]
+ * (rows of other slots untouched); the world's stamp and park time [W]; the send flags [n]. */
+typedef struct EbbServerQueue {
+    int64_t slots;
+    const int32_t* kinds;
+    const uint8_t* mask;
+    const int64_t *ball, *target, *n, *loc_in;
+    const double* f;
+    uint8_t* ok;
+    int64_t *row, *trow, *loc;
+    int8_t* route;
+    uint8_t* notice;
+    int64_t *stamp, *clock;
+    uint8_t *has_character, *gets_bubble;
+} EbbServerQueue;
 
 /* The ABI version (EBB_ABI_VERSION). Replaces xbpm_abi / xbpo_abi (exact_ballpark/vec_modes_cuda.cu:750,
  * vec_orient_cuda.cu:499). */
@@ -218,6 +269,18 @@ int ebb_composed_tick(const EbbComposedState* s, const int64_t* tile_rows, int64
  * EBB_COMPOSED_FLAG_PARTITION on the row. Replaces VecComposedPark._file (vec_composed.py:330-345). */
 int ebb_composed_file(const EbbComposedState* s, const uint8_t* mask, const double* pos, const double* vel,
                       const float* sf, void* stream);
+
+/* The server layer's pre- and post-tick over the flight park, one thread a world, the park written in place. phase 0:
+ * all of 1 and 2 over every slot; 1: the stamps, the queue in order (the duplicate test against the world's last queued
+ * call, the rows, CloakBall's bubble, every call but CloakBall applied by the park's own command or setter), then the
+ * bubble update; 2: the history over slots [j0, j1) (routes, CloakBall applied, the uncloaks' recipients), so that the
+ * host can read the park between segments; 3: the send flags (after the park's tick); 4: a bubble without an
+ * interactive ball recorded as dead (before the park's tick). Returns -1 for a bad argument (J outside
+ * [0, EBB_SERVER_MAX_SLOTS], a bad phase, range or block), else a cudaError_t. Replaces xbpv_pre_tick
+ * (exact_ballpark/vec_server_cuda.cu:615), which exact_ballpark.vec_server_cuda.launch calls (vec_server_cuda.py:307),
+ * and VecServer.evolve's dead-bubble test (vec_server.py:1021). */
+int ebb_server_tick(const EbbServerState* s, const EbbServerQueue* q, int phase, int64_t j0, int64_t j1, void* stream,
+                    int block);
 
 /* glibc 2.34's rand() after srand(seed) (random_r, TYPE_3), one generator a world: a world's state is EBB_RAND_WORDS
  * int32 (the 31-word table, then the front and rear indices). ebb_glibc_srand seeds worlds[W] states from seeds[W]

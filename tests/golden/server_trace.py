@@ -74,9 +74,10 @@ def batch_digests(server) -> np.ndarray:
 
 # ---- the batch's park and server ----
 
-def build(server_mod, park_cls, cs: list, do: bool, device, friction: float = 1.0e6, tick_ms: int = 1000):
-    """The server layer (server_mod's VecServer over its ModesAdapter) over a flight park of the worlds cs:
-    (server, {(world, ball id): row})."""
+def build(server_mod, park_cls, cs: list, do: bool, device, friction: float = 1.0e6, tick_ms: int = 1000,
+          kernel: str | None = None):
+    """The server layer (server_mod's VecServer over its ModesAdapter; `kernel` its path, when given) over a flight
+    park of the worlds cs: (server, {(world, ball id): row})."""
     rows = [(w, b) for w in cs for b in w["balls"]]
     p = park_cls(len(rows), friction=friction, tick_interval_ms=tick_ms, device=device, dynamical_orientation=do)
     p.load([{"id": b["id"], "world": w["id"], "time": 0, "mass": b["mass"], "radius": b["radius"],
@@ -90,7 +91,9 @@ def build(server_mod, park_cls, cs: list, do: bool, device, friction: float = 1.
     for w in cs:
         for bid, pp in w["pilots"].items():
             pilots[index[(w["id"], int(bid))]] = pp
-    return server_mod.VecServer(a, pilots), index
+    if kernel is None:
+        return server_mod.VecServer(a, pilots), index
+    return server_mod.VecServer(a, pilots, kernel=kernel), index
 
 
 def pushes(cs: list, t: int, device) -> list:
@@ -176,9 +179,9 @@ def load(path: Path) -> list:
     return body
 
 
-def replay(server_mod, park_cls, run: dict, device) -> list:
+def replay(server_mod, park_cls, run: dict, device, kernel: str | None = None) -> list:
     """A recorded run on server_mod's layer over park_cls: the differences [(tick, 'park', fields) or (tick, 'batch')]."""
-    server, _ = build(server_mod, park_cls, run["cases"], run["do"], device)
+    server, _ = build(server_mod, park_cls, run["cases"], run["do"], device, kernel=kernel)
     bad = []
 
     def on_tick(t, s):

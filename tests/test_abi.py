@@ -26,7 +26,7 @@ def test_the_library_exports_every_declared_entry_point():
 
 def test_abi_version_and_scratch_size():
     lib = _native.lib()
-    assert lib.ebb_abi() == _native.ABI == 4
+    assert lib.ebb_abi() == _native.ABI == 5
     assert lib.ebb_flight_scratch_bytes(0) == 0
     b = lib.ebb_flight_scratch_bytes(1000)
     assert b >= 1000 * (8 * 7 + 1) and b % 256 == 0
@@ -43,3 +43,22 @@ def test_refused_arguments_launch_nothing():
     assert lib.ebb_error_string(-1).decode().startswith("refused")
     s.n = 0
     assert lib.ebb_flight_tick(ctypes.byref(s), None, 0, None, 128) == 0             # nothing to do
+
+
+def test_the_server_tick_refuses_bad_arguments_before_launching():
+    lib = _native.lib()
+    s, q = _native.ServerState(), _native.ServerQueue()
+    s.worlds = 0
+    call = lambda phase, j0=0, j1=0, block=128: lib.ebb_server_tick(ctypes.byref(s), ctypes.byref(q), phase, j0,  # noqa: E731
+                                                                     j1, None, block)
+    assert call(0) == 0                                   # no worlds: nothing to do
+    assert call(5) == -1 and call(-1) == -1               # no such phase
+    assert call(0, block=100) == -1 and call(0, block=256) == -1
+    q.slots = 257
+    assert call(0) == -1                                  # more than EBB_SERVER_MAX_SLOTS
+    q.slots = 4
+    assert call(2, 3, 2) == -1 and call(2, 0, 5) == -1    # a history range outside the queue
+    s.worlds, s.width = 8, 4
+    assert call(0) == -1                                  # no world table
+    assert ctypes.sizeof(_native.ServerState) == ctypes.sizeof(_native.FlightState) + 16 + 14 * 8 + 16
+    assert ctypes.sizeof(_native.ServerQueue) == 8 + 17 * 8

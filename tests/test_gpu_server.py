@@ -5,14 +5,20 @@ ticks of Actions calls: conflicting commands, duplicates dropped and kept, cloak
 non-local SetBallPosition, follows and orbits of a cloaking ship, warps and warp-ins, every setter, refused values).
 After every tick: every park field's digest and the update batch's digest (stamps, queued flags and rows, routes, the
 uncloaks' recipients and the park's fields there, the bubble's additions, the narrowcast and character flags), bit for
-bit. The CPU tests hold the queue's duplicate rule and the world lookup on a stand-in park."""
+bit, on both paths (the park's commands over all worlds; the server kernel, one thread a world). Then the kernel
+against the torch path on random queues over 1,536 worlds (every kind the flight park applies, refused and edge
+values, duplicates, misses), and a ServerGraph's replays against eager kernel ticks. The CPU tests hold the queue's
+duplicate rule and the world lookup on a stand-in park."""
 
+import random
 from types import SimpleNamespace
 
+import numpy as np
 import pytest
 import torch
 
 import server_trace as st
+import trace as tr
 
 
 def _golden(name):
@@ -23,11 +29,145 @@ def _golden(name):
 @pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")
 @pytest.mark.parametrize("name", ["server_modes", "server_modes_do"], ids=["euler", "dynamical"])
 @pytest.mark.parametrize("run", [0, 1], ids=["development", "held_out"])
-def test_the_server_layer_replays_the_golden_ticks(name, run):
+@pytest.mark.parametrize("kernel", ["torch", "cuda"])
+def test_the_server_layer_replays_the_golden_ticks(name, run, kernel):
     from exact_ballpark_b200 import VecModesPark, server
     r = _golden(name)[run]
-    bad = st.replay(server, VecModesPark, r, "cuda")
+    bad = st.replay(server, VecModesPark, r, "cuda", kernel=kernel)
     assert not bad, f"{len(bad)} differences, first {bad[:3]}"
+
+
+# ---- random queues: the kernel against the torch path ----
+
+def _random_worlds(seed: int, W: int, do: bool) -> list:
+    """W worlds of 1 to 6 balls (ids 1 to 40, distinct in a world), mostly interactive, about half piloted."""
+    r = random.Random(seed)
+    cs = []
+    for w in range(W):
+        ids = r.sample(range(1, 41), r.randint(1, 6))
+        centre = [r.uniform(-1e5, 1e5) for _ in range(3)]
+        balls = [{"id": i, "mass": 10 ** r.uniform(5, 8), "radius": r.uniform(10, 300), "max_vel": r.uniform(50, 500),
+                  "pos": [c + r.uniform(-5e3, 5e3) for c in centre], "vel": [r.uniform(-50, 50) for _ in range(3)],
+                  "agility": r.uniform(0.2, 2.0), "sf": r.choice([0.0, 0.5, 1.0]), "massive": r.random() < 0.5,
+                  "interactive": r.random() < 0.8, "max_ang_vel": r.uniform(0.1, 1.0), "rot_agility": r.uniform(0.1, 1)}
+                 for i in ids]
+        pilots = {b["id"]: k for k, b in enumerate(balls) if r.random() < 0.5}
+        cs.append({"id": 1000 + 7 * w, "balls": balls, "pilots": pilots, "ticks": []})
+    return cs
+
+
+def _value(r: random.Random, lo: float, hi: float) -> float:
+    x = r.random()
+    if x < 0.03:
+        return float("nan")
+    if x < 0.05:
+        return float("inf")
+    if x < 0.15:
+        return -r.uniform(lo, hi)
+    if x < 0.2:
+        return 0.0
+    return r.uniform(lo, hi)
+
+
+def _random_pushes(r: random.Random, cs: list, kinds: list, dev) -> list:
+    """One tick's pushes: 0 to 14 calls of random kinds, worlds masked at random, arguments with edge values; a push
+    repeated as it was now and then (the duplicate rule)."""
+    W = len(cs)
+    out = []
+    for _ in range(r.randint(0, 14)):
+        if out and r.random() < 0.2:
+            out.append(out[-1])
+            continue
+        kind = r.choice(kinds)
+        mask = torch.tensor([r.random() < 0.7 for _ in range(W)])
+        pick = lambda w: r.choice([b["id"] for b in cs[w]["balls"]]) if r.random() < 0.93 else r.choice([0, 99])  # noqa: E731
+        ball = torch.tensor([pick(w) for w in range(W)], dtype=torch.int64)
+        target = torch.tensor([pick(w) for w in range(W)], dtype=torch.int64)
+        if kind in ("GotoPoint", "WarpTo", "EntityWarpIn", "SetBallPosition"):
+            f = [[_value(r, 1e3, 1e7) for _ in range(3)] + [_value(r, 0, 1e5)] for _ in range(W)]
+        elif kind in ("GotoDirection", "SetBallVelocity", "SetBallAngularVelocity", "SetBallRotation"):
+            f = [[_value(r, 0, 2) for _ in range(4)] for _ in range(W)]
+        else:
+            f = [[_value(r, 0, 1.5) if kind in ("SetSpeedFraction", "SetBallAgility") else _value(r, 0, 1e6)]
+                 + [0.0] * 3 for _ in range(W)]
+        n = torch.tensor([r.choice([-3, 0, 1, 2, 3, 5, 257, 300]) for _ in range(W)], dtype=torch.int64)
+        loc = torch.tensor([r.choice([0, 0, 1]) for _ in range(W)], dtype=torch.int64)
+        out.append((kind, *(x.to(dev) for x in (mask, ball, target, torch.tensor(f, dtype=torch.float64), n, loc))))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")
+@pytest.mark.parametrize("do", [False, True], ids=["euler", "dynamical"])
+def test_the_server_kernel_matches_the_torch_path_on_random_queues(do):
+    from exact_ballpark_b200 import VecModesPark, server
+    cs = _random_worlds(5 + int(do), 1536, do)
+    a, _ = st.build(server, VecModesPark, cs, do, "cuda", kernel="torch")
+    b, _ = st.build(server, VecModesPark, cs, do, "cuda", kernel="cuda")
+    kinds = sorted(server.KINDS[k] for k in a.a.kinds)
+    assert len(kinds) == (25 if do else 20)
+    r = random.Random(11)
+    routed = 0
+    for t in range(24):
+        pushes = _random_pushes(r, cs, kinds, "cuda")
+        for p in pushes:
+            a.push(*p)
+            b.push(*p)
+        for s in (a, b):
+            s.pre_tick()
+            s.evolve()
+            s.post_tick()
+        fa, fb = tr.field_digests(a.a.park), tr.field_digests(b.a.park)
+        bad = [st.PARK_FIELDS[k] for k in range(len(fa)) if fa[k] != fb[k]]
+        assert not bad, f"tick {t}: park fields {bad} differ"
+        da, db = st.batch_digests(a), st.batch_digests(b)
+        assert da.shape == db.shape and (da == db).all(), f"tick {t}: the update batches differ"
+        routed += int((a.batch.route != 0).sum())
+        assert torch.equal(a.dead, b.dead)
+    assert routed > 10000
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")
+def test_a_server_graph_replays_eager_kernel_ticks():
+    from exact_ballpark_b200 import VecModesPark, server
+    cs = _random_worlds(9, 1024, True)
+    sched = ["GotoDirection", "SetSpeedFraction", "FollowBall", "SetMaxSpeed", "Orbit", "GotoDirection",
+             "CloakBall", "SetSpeedFraction"]
+    g = torch.Generator().manual_seed(3)
+    W = len(cs)
+    ins = []
+    for k in sched:
+        ids = torch.tensor([w["balls"][int(torch.randint(len(w["balls"]), (1,), generator=g))]["id"] for w in cs])
+        tgt = torch.tensor([w["balls"][0]["id"] for w in cs])
+        f = torch.rand(W, 4, generator=g, dtype=torch.float64) * 2 - 1
+        ins.append({"mask": torch.rand(W, generator=g) < 0.8, "ball": ids, "target": tgt, "f": f,
+                    "n": torch.ones(W, dtype=torch.int64), "loc": torch.zeros(W, dtype=torch.int64)})
+    eager, _ = st.build(server, VecModesPark, cs, True, "cuda", kernel="cuda")
+    graphed, _ = st.build(server, VecModesPark, cs, True, "cuda", kernel="cuda")
+    for s in (eager, graphed):                             # the first tick (its additions' fields) eagerly
+        s.pre_tick()
+        s.evolve()
+        s.post_tick()
+    gr = server.ServerGraph(graphed, sched)
+    for j, inp in enumerate(ins):
+        for key, v in inp.items():
+            gr.inputs[j][key].copy_(v.to("cuda"))
+    for t in range(12):
+        for k, inp in zip(sched, ins):
+            eager.push(k, *(inp[key].to("cuda") for key in ("mask", "ball", "target", "f", "n", "loc")))
+        eager.pre_tick(snapshot=False)
+        eager.evolve()
+        eager.post_tick()
+        out = gr.tick()
+        fa, fb = tr.field_digests(eager.a.park), tr.field_digests(graphed.a.park)
+        assert np.array_equal(fa, fb), f"tick {t}: park fields differ"
+        assert graphed.a.park.current_time == eager.a.park.current_time
+        for key in ("has_character", "gets_bubble"):
+            assert torch.equal(getattr(out, key), getattr(eager.batch, key)), (t, key)
+        assert torch.equal(out.route, eager.batch.route) and torch.equal(out.stamp, eager.batch.stamp)
+        for j in range(len(sched)):
+            assert torch.equal(out.slots[j].ok, eager.batch.slots[j].ok), (t, j)
 
 
 def test_the_server_goldens_hold_every_action_kind():
@@ -66,7 +206,7 @@ def test_push_drops_a_call_equal_to_the_worlds_last_and_keeps_the_rest():
     from exact_ballpark_b200 import server
     A = _StandIn()
     s = server.VecServer.__new__(server.VecServer)
-    s.a, s.W, s.R, s.dev = A, A.W, A.R, A.dev
+    s.a, s.W, s.R, s.dev, s.kernel = A, A.W, A.R, A.dev, "torch"
     s.settled = torch.tensor([True, False, False, True, True, True])
     s.slots = []
     s._reset_last()
@@ -90,3 +230,11 @@ def test_push_drops_a_call_equal_to_the_worlds_last_and_keeps_the_rest():
         s.push("LaunchMissile", both, torch.tensor([10, 20]))
     assert len(s.slots) == 7
     assert SimpleNamespace(**s.last).kind.tolist() == [server.CODE["FollowBall"]] * 2
+
+
+def test_the_kernel_path_wants_a_cuda_device_and_a_known_path():
+    from exact_ballpark_b200 import server
+    with pytest.raises(ValueError):
+        server.VecServer(_StandIn(), kernel="triton")
+    with pytest.raises(ValueError):
+        server.VecServer(_StandIn(), kernel="cuda")
