@@ -456,6 +456,134 @@ def combat_runs(args, dev, composed: bool = False) -> dict:
     return out
 
 
+# Algorithmic bytes of one world's pre-tick on the server kernel at the server benchmark's shape (4 piloted ships, the
+# 8 pushes GotoDirection and SetSpeedFraction a ship): per queued call the pushed columns read (mask 1, ball, target,
+# n, local flag 4 x 8, floats 32) and the outputs written (queued 1, row, target row, local 3 x 8, route 1) and read
+# again by the history and the flags (34); per world the stamps (next stamp read and written, stamp and park time
+# written, the first row's clock read: 40), the bubble update's park time (16) and the world's rows and ids (2 x 32);
+# per ship the command fields (position read, goto point written 2 x 24; mode read and written 8; speed fraction read
+# and written twice 12), the bubble update (interactive, exists, settled 3, cloaked 8, fresh, listed and settled
+# written 3) and the route and flags (pilot 8, the two flags 2).
+SERVER_BYTES_PER_WORLD_TICK = 8 * (1 + 32 + 32 + 26 + 34) + 40 + 16 + 64 + 4 * (48 + 8 + 12 + 14 + 10)
+# (the dead-bubble test fused into the same launch reads interactive and exists again: L1 hits, not counted)
+
+
+def server_runs(args, dev) -> dict:
+    """The server layer (exact_ballpark_b200.server) over the flight park at the reference's server benchmark shape
+    (benchmarks/server_speed.py): --server-worlds worlds of 4 ships, each flown by a pilot that sends GotoDirection
+    and SetSpeedFraction every tick (8 Actions calls a world a tick, directions and speed fractions drawn once,
+    seeded), the flight park without dynamical orientation; a ServerGraph (the server kernel's pre-tick with the
+    dead-bubble test, the park's tick, the send flags) replayed --server-steps times after warm-up, timed with CUDA
+    events (L2 flushed before each). Then the same three launches eagerly, each timed alone (the shares and the server
+    kernel's roofline), and the end-to-end tick: the pushes' floats copied in from pinned host memory, the replay, the
+    two send flags of every row copied back."""
+    import random
+
+    import torch
+
+    from exact_ballpark_b200 import VecModesPark, server
+    from exact_ballpark_b200.modes import tick as park_tick
+    K, W = 4, args.server_worlds
+    r = random.Random(7)
+    rows = []
+    for i in range(W * K):
+        if i % K == 0:
+            centre = [r.uniform(-1e5, 1e5) for _ in range(3)]
+        rows.append({"id": i % K + 1, "world": i // K, "time": 0, "mass": 10 ** r.uniform(6.0, 8.0),
+                     "radius": r.uniform(20.0, 80.0), "max_vel": r.uniform(100.0, 400.0),
+                     "pos": [c + r.uniform(-4e3, 4e3) for c in centre], "vel": [0.0, 0.0, 0.0],
+                     "agility": r.uniform(0.3, 1.5), "speed_fraction": 1.0, "free": True, "massive": False,
+                     "interactive": True, "cloaked": 0, "bubble": 0, "moribund": False})
+    n = len(rows)
+    park = VecModesPark(n, device=dev)
+    park.load(rows)
+    srv = server.VecServer(server.ModesAdapter(park), [x["id"] - 1 for x in rows], kernel="cuda")
+    srv.pre_tick()                                                   # the first tick (its additions) eagerly
+    srv.evolve()
+    srv.post_tick()
+    sched = [k for _ in range(K) for k in ("GotoDirection", "SetSpeedFraction")]
+    g = server.ServerGraph(srv, sched)
+    gen = torch.Generator().manual_seed(11)
+    for k in range(K):
+        d, sf = torch.rand(W, 3, generator=gen, dtype=torch.float64) * 2 - 1, torch.rand(W, generator=gen,
+                                                                                         dtype=torch.float64)
+        for j, f in ((2 * k, d), (2 * k + 1, sf[:, None])):
+            g.inputs[j]["mask"].fill_(True)
+            g.inputs[j]["ball"].fill_(k + 1)
+            g.inputs[j]["f"][:, :f.shape[1]].copy_(f.to(dev))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        g.tick()
+    total = 0.0
+    for _ in range(args.server_steps):
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        g.tick()
+        b.record(stream)
+        b.synchronize()
+        total += a.elapsed_time(b)
+    per = total / args.server_steps
+    routed = int((g.out.route == server.BUBBLE).sum().item())
+    flags = int(g.out.gets_bubble.sum().item())
+    # the same four launches eagerly, each timed alone
+    parts = {"pre_tick": lambda: srv._launch(g.q, 5), "park_tick": lambda: park_tick(park, park.block),
+             "send_flags": lambda: srv._launch(g.q, 3)}
+    times = {k: 0.0 for k in parts}
+    for _ in range(args.server_steps):
+        flush.fill_(1)
+        for k, f in parts.items():
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            f()
+            b.record(stream)
+            b.synchronize()
+            times[k] += a.elapsed_time(b)
+        park.current_time += 1
+    ms = {k: v / args.server_steps for k, v in times.items()}
+    # end to end: the pushes' floats in from pinned host memory, the two flags of every row back
+    f_host = torch.empty_like(g.q["f"], device="cpu").pin_memory()
+    f_host.copy_(g.q["f"])
+    flags_host = [torch.empty(n, dtype=torch.bool).pin_memory() for _ in range(2)]
+    e2e = 0.0
+    for step in range(args.warmup + args.server_steps):
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        g.q["f"].copy_(f_host, non_blocking=True)
+        out = g.tick()
+        flags_host[0].copy_(out.has_character, non_blocking=True)
+        flags_host[1].copy_(out.gets_bubble, non_blocking=True)
+        b.record(stream)
+        b.synchronize()
+        if step >= args.warmup:
+            e2e += a.elapsed_time(b)
+    e2e /= args.server_steps
+    srv.check()
+    peak, kind = _peaks()
+    achieved = SERVER_BYTES_PER_WORLD_TICK * W / (ms["pre_tick"] / 1e3) / 1e9
+    return {"workload": (f"server layer over the flight park: {W} worlds x 4 piloted ships, 8 Actions calls a world a "
+                         "tick (GotoDirection + SetSpeedFraction a ship), dynamical orientation off; ServerGraph "
+                         "(server kernel pre-tick with the dead-bubble test, park tick, send flags)"),
+            "value": n / (per / 1e3), "unit": "ship-ticks/s", "world_ticks_per_s": W / (per / 1e3),
+            "ms_per_step": per, "steps": args.server_steps, "warmup": args.warmup,
+            "launch_ms": ms, "launch_share": {k: v / sum(ms.values()) for k, v in ms.items()},
+            "routed_to_bubble_last_tick": routed, "narrowcast_rows_last_tick": flags,
+            "roofline": {"bound": "hbm", "kernel": "server_kernel (pre-tick and dead-bubble test, phase 5)",
+                         "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind, "traffic": None,
+                         "note": f"algorithmic {SERVER_BYTES_PER_WORLD_TICK} B/world x {W} worlds over the pre-tick "
+                                 "launch's own CUDA-event time (eager, L2 flushed); one thread a world walking its "
+                                 "queue: latency-bound"},
+            "e2e": {"value": n / (e2e / 1e3), "unit": "ship-ticks/s", "ms_per_step": e2e,
+                    "h2d_bytes_per_step": g.q["f"].numel() * 8, "d2h_bytes_per_step": 2 * n},
+            "gpu_launches_per_step": 3,
+            "reference_published": {"value": 716e6, "unit": "ship-ticks/s", "hardware": "GH200",
+                                    "config": "layer=server, mode=server_k_graph, park=modes, 65,536 worlds x 4 "
+                                              "(docs/benchmarks.md)"}}
+
+
 def _config(args, schedule: str) -> dict:
     return {"workload": (f"flight-mode park, dynamical orientation on, new orbit law: {args.worlds} worlds x "
                          f"{args.ships} ships (follow / orbit / warp), per-rank"),
@@ -480,11 +608,14 @@ def main() -> None:
     ap.add_argument("--collide-worlds", type=int, default=65536)
     ap.add_argument("--collide-steps", type=int, default=50)
     ap.add_argument("--no-combat", action="store_true")
-    ap.add_argument("--only", choices=("ragged", "collide", "collide_statics", "combat", "composed", "serve"),
+    ap.add_argument("--only", choices=("ragged", "collide", "collide_statics", "combat", "composed", "serve", "server"),
                     default=None, help="run one section alone on one GPU and print it (for profiling); the default "
                                        "run prints the headline line with every section")
     ap.add_argument("--combat-worlds", type=int, default=65536)
     ap.add_argument("--combat-steps", type=int, default=50)
+    ap.add_argument("--no-server", action="store_true")
+    ap.add_argument("--server-worlds", type=int, default=65536)
+    ap.add_argument("--server-steps", type=int, default=100)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-seconds", type=float, default=6.0)
     ap.add_argument("--serve-budget-gb", type=float, default=80.0)
@@ -520,7 +651,7 @@ def main() -> None:
         run = {"ragged": lambda: ragged_runs(args, dev), "collide": lambda: collide_runs(args, dev),
                "collide_statics": lambda: collide_runs(args, dev, statics=True),
                "combat": lambda: combat_runs(args, dev), "composed": lambda: combat_runs(args, dev, composed=True),
-               "serve": lambda: serve_runs(args, dev)}[args.only]
+               "serve": lambda: serve_runs(args, dev), "server": lambda: server_runs(args, dev)}[args.only]
         print(json.dumps({"metric": METRIC, "section": args.only, args.only: run()}), flush=True)
         return
     dist = None
@@ -637,6 +768,8 @@ def main() -> None:
     if not args.no_combat:
         line["combat"] = combat_runs(args, dev)
         line["composed"] = combat_runs(args, dev, composed=True)
+    if not args.no_server:
+        line["server"] = server_runs(args, dev)
     if not args.no_serve:
         line["serve"] = serve_runs(args, dev)
         line["serve"]["plain_ship_ticks_per_s"] = line["plain"]["value"] / world_size

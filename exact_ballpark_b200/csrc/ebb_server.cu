@@ -287,32 +287,57 @@ struct World {
     }
 };
 
-__device__ void queue_and_apply(const World& x, const EbbServerQueue& q) {
+// The queue pass: each push's rows, CloakBall's bubble and the duplicate test, nothing written to the park (so the
+// loads of later slots need not wait for earlier slots' commands); the world's ids held in registers for the lookups.
+constexpr int IDS_IN_REGISTERS = 8;
+
+__device__ void queue(const World& x, const EbbServerQueue& q) {
     const EbbServerState& s = x.s;
-    const int64_t W = s.worlds, w = x.w;
-    const int64_t clock = x.p.clock[x.rows[0]];
-    q.clock[w] = clock;
-    q.stamp[w] = s.stamp_for_system[w];
-    s.stamp_for_system[w] = clock + 1;
+    const int64_t W = s.worlds, w = x.w, J = q.slots;
+    const int32_t* __restrict__ kinds = q.kinds;
+    const uint8_t* __restrict__ mask = q.mask;
+    const int64_t* __restrict__ balls = q.ball;
+    const int64_t* __restrict__ targets = q.target;
+    const int64_t* __restrict__ ns = q.n;
+    const int64_t* __restrict__ locs = q.loc_in;
+    const double* __restrict__ fs = q.f;
+    uint8_t* __restrict__ oks = q.ok;
+    int64_t* __restrict__ rows_out = q.row;
+    int64_t* __restrict__ trows_out = q.trow;
+    int64_t* __restrict__ locs_out = q.loc;
+    int64_t ids[IDS_IN_REGISTERS], rows[IDS_IN_REGISTERS];
+#pragma unroll
+    for (int k = 0; k < IDS_IN_REGISTERS; ++k) {
+        ids[k] = k < s.width ? x.ids[k] : 0;
+        rows[k] = k < s.width ? x.rows[k] : -1;
+    }
+    auto lookup = [&](int64_t id) -> int64_t {
+        if (s.width > IDS_IN_REGISTERS) return x.lookup(id);
+        int64_t found = -1;
+#pragma unroll
+        for (int k = IDS_IN_REGISTERS - 1; k >= 0; --k)       // the first match wins
+            if (k < s.width && ids[k] == id) found = rows[k];
+        return found;
+    };
     int32_t lk = 0;                                       // the world's last queued call (none yet: all zero)
     int64_t lb = 0, lt = 0, ln = 0, ll = 0;
-    double lf[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int64_t j = 0; j < q.slots; ++j) {
+    double lf0 = 0.0, lf1 = 0.0, lf2 = 0.0, lf3 = 0.0;
+#pragma unroll 2
+    for (int64_t j = 0; j < J; ++j) {
         const int64_t a = j * W + w;
-        const int32_t kind = q.kinds[j];
-        const int64_t ball = q.ball[a], target = q.target[a], n = q.n[a];
-        double f[4];
-        for (int c = 0; c < 4; ++c) f[c] = q.f[a * 4 + c];
-        const int64_t row = x.lookup(ball);
-        const int64_t trow = (kind == EBB_KIND_FOLLOW_BALL || kind == EBB_KIND_ORBIT) ? x.lookup(target) : -1;
-        bool pushed = q.mask[a] != 0;
-        int64_t loc = q.loc_in[a];
+        const int32_t kind = kinds[j];
+        const int64_t ball = balls[a], target = targets[a], n = ns[a];
+        const double f0 = fs[a * 4], f1 = fs[a * 4 + 1], f2 = fs[a * 4 + 2], f3 = fs[a * 4 + 3];
+        const int64_t row = lookup(ball);
+        const int64_t trow = (kind == EBB_KIND_FOLLOW_BALL || kind == EBB_KIND_ORBIT) ? lookup(target) : -1;
+        bool pushed = mask[a] != 0;
+        int64_t loc = locs[a];
         if (kind == EBB_KIND_CLOAK) {                     // the bubble it is queued in (row 0's flag for a miss)
             loc = s.settled[row < 0 ? 0 : row] ? 0 : -1;
             pushed = pushed && row >= 0;
         }
-        const bool dup = lk == kind && lb == ball && lt == target && lf[0] == f[0] && lf[1] == f[1] &&
-                         lf[2] == f[2] && lf[3] == f[3] && ln == n && ll == loc;
+        const bool dup = lk == kind && lb == ball && lt == target && lf0 == f0 && lf1 == f1 && lf2 == f2 &&
+                         lf3 == f3 && ln == n && ll == loc;
         const bool ok = pushed && !dup;
         if (ok) {
             lk = kind;
@@ -320,13 +345,33 @@ __device__ void queue_and_apply(const World& x, const EbbServerQueue& q) {
             lt = target;
             ln = n;
             ll = loc;
-            for (int c = 0; c < 4; ++c) lf[c] = f[c];
+            lf0 = f0;
+            lf1 = f1;
+            lf2 = f2;
+            lf3 = f3;
         }
-        q.ok[a] = ok;
-        q.row[a] = row;
-        q.trow[a] = trow;
-        q.loc[a] = loc;
-        if (ok && row >= 0 && kind != EBB_KIND_CLOAK) x.apply(kind, row, trow, f, n);
+        oks[a] = ok;
+        rows_out[a] = row;
+        trows_out[a] = trow;
+        locs_out[a] = loc;
+    }
+}
+
+__device__ void queue_and_apply(const World& x, const EbbServerQueue& q) {
+    const EbbServerState& s = x.s;
+    const int64_t W = s.worlds, w = x.w;
+    const int64_t clock = x.p.clock[x.rows[0]];
+    q.clock[w] = clock;
+    q.stamp[w] = s.stamp_for_system[w];
+    s.stamp_for_system[w] = clock + 1;
+    queue(x, q);
+    for (int64_t j = 0; j < q.slots; ++j) {               // every queued call but CloakBall, in queue order
+        const int64_t a = j * W + w;
+        const int32_t kind = q.kinds[j];
+        const int64_t row = q.row[a];
+        if (!q.ok[a] || row < 0 || kind == EBB_KIND_CLOAK) continue;
+        const double f[4] = {q.f[a * 4], q.f[a * 4 + 1], q.f[a * 4 + 2], q.f[a * 4 + 3]};
+        x.apply(kind, row, q.trow[a], f, q.n[a]);
     }
     // the bubble update, once per park time
     if (clock == s.bubble_time[w]) return;
@@ -380,15 +425,33 @@ __device__ void flags(const World& x, const EbbServerQueue& q) {
     const EbbServerState& s = x.s;
     const int64_t W = s.worlds, w = x.w, R = x.p.n, J = q.slots;
     bool bubble = false;
-    for (int64_t j = 0; j < J; ++j) bubble = bubble || q.route[w * J + j] == EBB_ROUTE_BUBBLE;
+    uint32_t character = 0;                               // the world's rows (by position) routed to their character
+    bool uncloaks = false;
+    for (int64_t j = 0; j < J; ++j) {
+        const int8_t route = q.route[w * J + j];
+        bubble = bubble || route == EBB_ROUTE_BUBBLE;
+        uncloaks = uncloaks || q.kinds[j] == EBB_KIND_UNCLOAK;
+        if (route != EBB_ROUTE_CHARACTER) continue;
+        const int64_t a = j * W + w;
+        if (!q.ok[a]) continue;
+        const int64_t row = q.row[a];
+        for (int64_t k = 0; k < s.width && k < 32; ++k)
+            if (x.rows[k] == row) character |= 1u << k;
+    }
     for (int64_t k = 0; k < s.width; ++k) {
         const int64_t r = x.rows[k];
         if (r < 0) continue;
         bool has = s.fresh[r] != 0;
-        for (int64_t j = 0; j < J && !has; ++j) {
-            const int64_t a = j * W + w;
-            has = (q.ok[a] && q.row[a] == r && q.route[w * J + j] == EBB_ROUTE_CHARACTER) || q.notice[j * R + r];
+        if (k < 32) {
+            has = has || ((character >> k) & 1u);
+        } else {                                          // a world wider than the mask: the slots again
+            for (int64_t j = 0; j < J && !has; ++j) {
+                const int64_t a = j * W + w;
+                has = q.ok[a] && q.row[a] == r && q.route[w * J + j] == EBB_ROUTE_CHARACTER;
+            }
         }
+        for (int64_t j = 0; j < J && uncloaks && !has; ++j)
+            has = q.kinds[j] == EBB_KIND_UNCLOAK && q.notice[j * R + r];
         const bool pilot = s.pilot[r] >= 0;
         q.has_character[r] = has && pilot;
         q.gets_bubble[r] = bubble && x.p.interactive[r] && s.exists[r] && pilot;
@@ -411,6 +474,11 @@ __global__ void __launch_bounds__(128) server_kernel(EbbServerState s, EbbServer
         case 4:
             if (!x.any_interactive()) s.dead[w] = 1;
             break;
+        case 5:                                           // phase 0, then the park's tick's dead-bubble test
+            queue_and_apply(x, q);
+            history(x, q, 0, q.slots);
+            if (!x.any_interactive()) s.dead[w] = 1;
+            break;
         default: break;
     }
 }
@@ -424,7 +492,7 @@ extern "C" {
 
 int ebb_server_tick(const EbbServerState* s, const EbbServerQueue* q, int phase, int64_t j0, int64_t j1, void* stream,
                     int block) {
-    if (s == nullptr || q == nullptr || phase < 0 || phase > 4) return EBB_EINVAL;
+    if (s == nullptr || q == nullptr || phase < 0 || phase > 5) return EBB_EINVAL;
     if (q->slots < 0 || q->slots > EBB_SERVER_MAX_SLOTS || block <= 0 || block > 128 || block % 32 != 0)
         return EBB_EINVAL;
     if (phase == 2 && (j0 < 0 || j1 < j0 || j1 > q->slots)) return EBB_EINVAL;

@@ -20,7 +20,8 @@ Two paths with one result, bit for bit. kernel="torch": every park write is the 
 index work (masks, gathers, comparisons) and the cloak's float sum radius + range as float32, as the C++ does.
 kernel="cuda": the native library's server kernel (ebb_server_tick), one thread a world walking its own queue, every
 command restated for one row; one launch for the whole pre-tick (or one per history segment when the park's fields are
-recorded for the streams), one for the dead-bubble test before the park's tick and one for the send flags after it.
+recorded for the streams), one for the dead-bubble test before the park's tick (fused into the pre-tick's launch in a
+graph, where nothing comes between them) and one for the send flags after it.
 `ServerGraph` captures a kernel-path tick with a fixed schedule of pushes as one CUDA graph.
 
 Not built: the encoding of the batches into Destiny's tuples and streams (`decode`), the pending queries and the undo,
@@ -529,7 +530,7 @@ class ServerGraph:
     """A kernel-path VecServer's tick with a fixed schedule of pushes, captured once as a CUDA graph (the drop-in for
     exact_ballpark.vec_server.ServerGraph, vec_server.py:1200): before each replay the caller writes each push's
     arguments into `inputs[j]` (mask, ball, target, f, n, loc: views of the queue's [J, W] buffers) and `tick()`
-    replays the pre-tick (one launch), the dead-bubble test, the park's tick and the send flags, and returns the graph's
+    replays the pre-tick with the dead-bubble test (one launch), the park's tick and the send flags, and returns the graph's
     Batch (its tensors refilled in place; no park fields recorded). Every state tensor is written in place by its
     kernel, so nothing is re-bound between replays and eager setters between ticks are seen by the next replay."""
 
@@ -580,8 +581,7 @@ class ServerGraph:
 
     def _body(self) -> None:
         srv, p = self.server, self.server.a.park
-        srv._launch(self.q, 0)
-        srv._launch(self.q, 4)
+        srv._launch(self.q, 5)                             # the pre-tick and the dead-bubble test, one launch
         _park_tick(p, p.block)
         srv._launch(self.q, 3)
 

@@ -166,6 +166,7 @@ def test_a_server_graph_replays_eager_kernel_ticks():
         for key in ("has_character", "gets_bubble"):
             assert torch.equal(getattr(out, key), getattr(eager.batch, key)), (t, key)
         assert torch.equal(out.route, eager.batch.route) and torch.equal(out.stamp, eager.batch.stamp)
+        assert torch.equal(graphed.dead, eager.dead)
         for j in range(len(sched)):
             assert torch.equal(out.slots[j].ok, eager.batch.slots[j].ok), (t, j)
 
