@@ -330,15 +330,21 @@ __device__ void queue(const World& x, const EbbServerQueue& q) {
         const double f0 = fs[a * 4], f1 = fs[a * 4 + 1], f2 = fs[a * 4 + 2], f3 = fs[a * 4 + 3];
         const int64_t row = lookup(ball);
         const int64_t trow = (kind == EBB_KIND_FOLLOW_BALL || kind == EBB_KIND_ORBIT) ? lookup(target) : -1;
-        bool pushed = mask[a] != 0;
+        const uint8_t byte = mask[a];
         int64_t loc = locs[a];
-        if (kind == EBB_KIND_CLOAK) {                     // the bubble it is queued in (row 0's flag for a miss)
-            loc = s.settled[row < 0 ? 0 : row] ? 0 : -1;
-            pushed = pushed && row >= 0;
+        bool ok;
+        if (byte & 2) {                                   // tested already by an undo: bit 0 is its queued flag
+            ok = (byte & 1) != 0;
+        } else {
+            bool pushed = (byte & 1) != 0;
+            if (kind == EBB_KIND_CLOAK) {                 // the bubble it is queued in (row 0's flag for a miss)
+                loc = s.settled[row < 0 ? 0 : row] ? 0 : -1;
+                pushed = pushed && row >= 0;
+            }
+            const bool dup = lk == kind && lb == ball && lt == target && lf0 == f0 && lf1 == f1 && lf2 == f2 &&
+                             lf3 == f3 && ln == n && ll == loc;
+            ok = pushed && !dup;
         }
-        const bool dup = lk == kind && lb == ball && lt == target && lf0 == f0 && lf1 == f1 && lf2 == f2 &&
-                         lf3 == f3 && ln == n && ll == loc;
-        const bool ok = pushed && !dup;
         if (ok) {
             lk = kind;
             lb = ball;

@@ -24,8 +24,10 @@ recorded for the streams), one for the dead-bubble test before the park's tick (
 graph, where nothing comes between them) and one for the send flags after it.
 `ServerGraph` captures a kernel-path tick with a fixed schedule of pushes as one CUDA graph.
 
-Not built: the encoding of the batches into Destiny's tuples and streams (`decode`), the pending queries and the undo,
-OnTick's intervals, the other parks' adapters, bubbles other than one a world.
+The pending queries and the undo of a pending cloak (Actions, _actions.py:686-766) answer from the queue on both paths.
+
+Not built: the encoding of the batches into Destiny's tuples and streams (`decode`), OnTick's intervals, the other
+parks' adapters, bubbles other than one a world.
 """
 
 from __future__ import annotations
@@ -308,7 +310,7 @@ class VecServer:
         """The queue's tensors for kinds [J]: the pushes' columns ([J, W] stacks, given or zeros) and the outputs."""
         J, W, R, d = len(kinds), self.W, self.R, self.dev
         z = lambda *shape, dt=I64: torch.zeros(*shape, dtype=dt, device=d)          # noqa: E731
-        q = {"kinds": torch.tensor(kinds, dtype=torch.int32).to(d), "mask": z(J, W, dt=BOOL), "ball": z(J, W),
+        q = {"kinds": torch.tensor(kinds, dtype=torch.int32).to(d), "mask": z(J, W, dt=torch.uint8), "ball": z(J, W),
              "target": z(J, W), "f": z(J, W, 4, dt=F64), "n": z(J, W), "loc_in": z(J, W),
              "ok": z(J, W, dt=BOOL), "row": z(J, W), "trow": z(J, W), "loc": z(J, W),
              "route": z(W, J, dt=torch.int8), "notice": z(J, R, dt=BOOL), "stamp": z(W), "clock": z(W),
@@ -373,6 +375,144 @@ class VecServer:
         slot = Slot(k, ok, ball, row, target, trow, ff, n, loc)
         self.slots.append(slot)
         return slot
+
+    # ---- the pending queries and the undo of a pending cloak (_actions.py:686-766) ----
+    #
+    # Destiny's game code asks the queue between ticks what is pending and may undo a pending cloak. On the torch path
+    # each call was tested at its push; on the kernel path the calls are tested here, in queue order, as the kernel
+    # would test them, and an undo hands the kernel the tested calls (`resolved`: bit 1 of the kernel's mask byte,
+    # bit 0 then the queued flag and `loc` CloakBall's tested bubble) so that it does not test them again.
+
+    def _deferred(self) -> bool:
+        return self.kernel == "cuda"
+
+    def _zero_last(self) -> dict:
+        W, d = self.W, self.dev
+        return {"kind": torch.zeros(W, dtype=I64, device=d), "ball": torch.zeros(W, dtype=I64, device=d),
+                "target": torch.zeros(W, dtype=I64, device=d), "f": torch.zeros(W, 4, dtype=F64, device=d),
+                "n": torch.zeros(W, dtype=I64, device=d), "loc": torch.zeros(W, dtype=I64, device=d)}
+
+    @staticmethod
+    def _become_last(last: dict, s: Slot, queued: torch.Tensor, loc: torch.Tensor) -> None:
+        for key, val in (("kind", torch.full_like(last["kind"], s.kind)), ("ball", s.ball), ("target", s.target),
+                         ("n", s.n), ("loc", loc)):
+            last[key] = torch.where(queued, val, last[key])
+        last["f"] = torch.where(queued[:, None], s.f, last["f"])
+
+    def _test_pending(self, commit: bool = False) -> list:
+        """The kernel path's pending calls tested as the kernel tests them (the resolved prefix taken as it is): each
+        call's queued flag [W]; `commit` makes every call resolved."""
+        last = self._zero_last()
+        out = []
+        for s in self.slots:
+            if getattr(s, "resolved", False):
+                queued, loc = s.mask, s.loc
+            else:
+                row = self.a.lookup(s.ball)
+                queued, loc = s.mask, s.loc
+                if s.kind == CLOAK:
+                    loc = torch.where(self.settled[row.clamp(min=0)], 0, -1)
+                    queued = queued & (row >= 0)
+                dup = ((last["kind"] == s.kind) & (last["ball"] == s.ball) & (last["target"] == s.target)
+                       & (last["f"] == s.f).all(dim=1) & (last["n"] == s.n) & (last["loc"] == loc))
+                queued = queued & ~dup
+            self._become_last(last, s, queued, loc)
+            out.append(queued)
+            if commit:
+                s.mask, s.loc, s.resolved = queued, loc, True
+        return out
+
+    def _queued(self) -> list:
+        return self._test_pending() if self._deferred() else [s.ok for s in self.slots]
+
+    def _last_pending(self, kind: int, mask, ball) -> tuple:
+        """Actions._get_pending_actions for one kind in every world of mask: (found [W], the last such call's slot
+        index [W], -1 for none)."""
+        mask = torch.as_tensor(mask).to(device=self.dev, dtype=BOOL)
+        ball = torch.as_tensor(ball).to(device=self.dev, dtype=I64)
+        found = torch.zeros(self.W, dtype=BOOL, device=self.dev)
+        at = torch.full((self.W,), -1, dtype=I64, device=self.dev)
+        for j, (s, queued) in enumerate(zip(self.slots, self._queued())):
+            if s.kind == kind:
+                hit = mask & queued & (s.ball == ball)
+                found = found | hit
+                at = torch.where(hit, j, at)
+        return found, at
+
+    def _pending_value(self, at: torch.Tensor, attr: str, col: int | None = None) -> torch.Tensor:
+        if not self.slots:
+            return torch.zeros(self.W, dtype=F64 if col is not None else I64, device=self.dev)
+        vals = torch.stack([getattr(s, attr) if col is None else getattr(s, attr)[:, col] for s in self.slots])
+        return vals.gather(0, at.clamp(min=0)[None, :])[0]
+
+    def _pending_else_current(self, kind: int, mask, ball, attr: str, col, current: torch.Tensor) -> tuple:
+        """The last pending call's argument as pushed, else the ball's current value, else nothing: (value, known)."""
+        found, at = self._last_pending(kind, mask, ball)
+        row = self.a.lookup(torch.as_tensor(ball).to(device=self.dev, dtype=I64))
+        pending = self._pending_value(at, attr, col)
+        now = current[row.clamp(min=0)].to(pending.dtype)
+        value = torch.where(found, pending, torch.where(row >= 0, now, torch.zeros_like(pending)))
+        known = torch.as_tensor(mask).to(device=self.dev, dtype=BOOL) & (found | (row >= 0))
+        return value, known
+
+    def has_pending_cloak(self, mask, ball) -> torch.Tensor:
+        """Actions.has_pending_cloak, every world of mask: [W] bool."""
+        return self._last_pending(CLOAK, mask, ball)[0]
+
+    def has_pending_uncloak(self, mask, ball) -> torch.Tensor:
+        """Actions.has_pending_uncloak, every world of mask: [W] bool."""
+        return self._last_pending(UNCLOAK, mask, ball)[0]
+
+    def get_pending_cloak_mode(self, mask, ball) -> tuple:
+        """Actions.get_pending_cloak_mode: the last pending CloakBall's mode as pushed, else the ball's cloak byte, else
+        None: (value [W] int64, known [W] bool)."""
+        return self._pending_else_current(CLOAK, mask, ball, "n", None, self.a.cloaked)
+
+    def get_pending_interactive_state(self, mask, ball) -> tuple:
+        """Actions.get_pending_interactive_state: the last pending SetBallInteractive's flag, else the ball's, else
+        None: (value [W] bool, known [W] bool)."""
+        value, known = self._pending_else_current(INTERACTIVE, mask, ball, "n", None, self.a.interactive.to(I64))
+        return value != 0, known
+
+    def get_pending_speed_fraction(self, mask, ball) -> tuple:
+        """Actions.get_pending_speed_fraction: the last pending SetSpeedFraction's value as pushed, else the ball's
+        speed fraction, else None: (value [W] float64, known [W] bool)."""
+        return self._pending_else_current(CODE["SetSpeedFraction"], mask, ball, "f", 0, self.a.park.speed_fraction)
+
+    def _pending_free(self, mask, ball, value: int) -> tuple:
+        found, at = self._last_pending(CODE["SetBallFree"], mask, ball)
+        return found & (self._pending_value(at, "n") == value), found
+
+    def has_pending_set_free(self, mask, ball) -> tuple:
+        """Actions.has_pending_set_free: whether the last pending SetBallFree's flag is 1: (answer, pending) [W]; where
+        nothing is pending Destiny answers the int 0 (`pending` False)."""
+        return self._pending_free(mask, ball, 1)
+
+    def has_pending_set_not_free(self, mask, ball) -> tuple:
+        """Actions.has_pending_set_not_free: whether the last pending SetBallFree's flag is 0: (answer, pending)."""
+        return self._pending_free(mask, ball, 0)
+
+    def undo_pending_cloak(self, mask, ball) -> None:
+        """Actions.undo_pending_cloak, every world of mask: every pending CloakBall of the ball taken out of the
+        world's queue; the calls pushed later are tested against the queue's last call as it then stands."""
+        mask = torch.as_tensor(mask).to(device=self.dev, dtype=BOOL)
+        ball = torch.as_tensor(ball).to(device=self.dev, dtype=I64)
+        deferred = self._deferred()
+        if deferred:
+            self._test_pending(commit=True)
+        for s in self.slots:
+            if s.kind != CLOAK:
+                continue
+            out = mask & (s.ball == ball)
+            if deferred:
+                s.mask = s.mask & ~out
+            else:
+                s.ok = s.ok & ~out
+        if not deferred:                                  # the torch path's queue: its last call again
+            last = self._zero_last()
+            for s in self.slots:
+                self._become_last(last, s, s.ok, s.loc)
+            self.last = last
 
     def _rows(self, slot: Slot) -> tuple:
         """The call as per-row masks and arguments: a row is commanded iff its world's call is queued for it."""
@@ -454,7 +594,9 @@ class VecServer:
         snapshot = self._snapshot(set(kinds), snapshot)
         cols = None
         if J:
-            cols = {"mask": torch.stack([s.mask for s in slots]), "ball": torch.stack([s.ball for s in slots]),
+            cols = {"mask": torch.stack([s.mask.to(torch.uint8) | (2 if getattr(s, "resolved", False) else 0)
+                                         for s in slots]),
+                    "ball": torch.stack([s.ball for s in slots]),
                     "target": torch.stack([s.target for s in slots]), "f": torch.stack([s.f for s in slots]),
                     "n": torch.stack([s.n for s in slots]), "loc_in": torch.stack([s.loc for s in slots])}
         q = self._queue(kinds, cols)
@@ -546,7 +688,7 @@ class ServerGraph:
                 raise ValueError(f"{KINDS[k]} is not applied by this park")
         p, d = srv.a.park, srv.dev
         self.q = q = srv._queue(self.schedule)
-        self.inputs = [{"mask": q["mask"][j], "ball": q["ball"][j], "target": q["target"][j], "f": q["f"][j],
+        self.inputs = [{"mask": q["mask"][j].view(BOOL), "ball": q["ball"][j], "target": q["target"][j], "f": q["f"][j],
                         "n": q["n"][j], "loc": q["loc_in"][j]} for j in range(len(self.schedule))]
         if p.plan is None:
             p.scratch()

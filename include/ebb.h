@@ -136,7 +136,9 @@ typedef struct EbbServerState {
     int32_t master;
 } EbbServerState;
 
-/* One tick's queue: J slots (the pushes, in order), each a kind [J] and per world its pushed byte, ball id, target id,
+/* One tick's queue: J slots (the pushes, in order), each a kind [J] and per world its pushed byte (bit 0 pushed; bit
+ * 1 the call already tested by an undo of a pending cloak, bit 0 then its queued flag and the local argument
+ * CloakBall's tested bubble: no duplicate test again; the tested calls are a prefix of the queue), ball id, target id,
  * float arguments (4), int argument and SetBallPosition's local flag ([J][W], f [J][W][4]); out: per slot and world the
  * queued flag, the ball's and target's rows (-1 none) and the local argument or CloakBall's bubble (0, or -1 before
  * the ball's old bubble is its bubble) ([J][W]); the routes [W][J]; the uncloaks' AddBallsToPark recipients [J][n]

@@ -458,9 +458,47 @@ def make_server() -> None:
         print(f"  {name}: {len(runs)} runs of {len(runs[0]['cases'])} worlds, {time.time() - t:.0f} s", flush=True)
 
 
+def make_server_pending() -> None:
+    """server_pending: the reference's pending-query scenarios over the flight-mode park (tests/server_pending_cases.py's
+    augment over tests/server_cases.py's worlds: 40 worlds of one bubble, 12 ticks, the game's queries of every kind at
+    any place among the calls, undos of a pending cloak, a cloak pushed twice then undone, undone then pushed again with
+    another mode, the prune's edge X, CloakBall, X, undo; seeds 101 and held-out 117), recorded on the reference's
+    VecServer (torch path, over its VecModesPark on the CPU) by server_trace's driver with every answer's digest. Each
+    scenario set is first run by the reference's own comparison against its scalar server layer (every answer, every
+    client's update list, every ship's state): 0 differences."""
+    import server_cases as S
+    import server_pending_cases as P
+    import server_trace as st
+    import exact_ballpark.vec_server as VS
+    from exact_ballpark.vec_modes import VecModesPark
+    t0 = time.time()
+    runs = []
+    for seed in (101, 117):
+        cs = P.augment(S.cases(seed, 40, "modes", ticks=12), "server", f"modes-{seed}", P.MODES["server"]["modes"])
+        server, index = S.build(cs, "modes", "cpu")
+        res = P.run(cs, "modes", "cpu", server, index, [S.ScalarWorld(w) for w in cs])
+        if res["answers"] or res["sends"] or res["rows"] or res["flagged"]:
+            raise RuntimeError(f"seed {seed}: the reference's server layer differs from its scalar one")
+        cs = P.augment(S.cases(seed, 40, "modes", ticks=12), "server", f"modes-{seed}", P.MODES["server"]["modes"])
+        parks, batches, answers = [], [], []
+
+        def on_tick(tk, server, ans):
+            parks.append(tr.field_digests(server.a.park))
+            batches.append(st.batch_digests(server))
+            answers.append(ans)
+        server, _ = st.build(VS, VecModesPark, cs, False, "cpu")
+        st.drive_pending(server, cs, "cpu", on_tick)
+        runs.append({"cases": cs, "do": False, "evolve": True, "park": np.array(parks, dtype=np.uint64),
+                     "batch": batches, "answers": answers})
+        print(f"  seed {seed}: {res['volumes']['answers']} answers, {res['volumes']['undos']} undos", flush=True)
+    st.save(HERE / "server_pending", runs)
+    print(f"  server_pending: {len(runs)} runs of 40 worlds, {time.time() - t0:.0f} s", flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed", "server"), default=None)
+    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending"),
+                    default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
     a = ap.parse_args()
     if a.only in (None, "libm"):
@@ -479,6 +517,8 @@ def main() -> None:
         make_composed()
     if a.only in (None, "server"):
         make_server()
+    if a.only in (None, "server_pending"):
+        make_server_pending()
 
 
 if __name__ == "__main__":

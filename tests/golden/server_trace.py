@@ -96,10 +96,41 @@ def build(server_mod, park_cls, cs: list, do: bool, device, friction: float = 1.
     return server_mod.VecServer(a, pilots, kernel=kernel), index
 
 
+def _group(by_kind: dict, W: int, device) -> list:
+    """One push a kind for the calls {kind: [(world index, args)]}: [(kind, mask, ball, target, f, n, loc)]."""
+    out = []
+    for kind, items in by_kind.items():
+        mask = torch.zeros(W, dtype=torch.bool)
+        ball, target, n, loc = (torch.zeros(W, dtype=torch.int64) for _ in range(4))
+        f = torch.zeros(W, 4, dtype=torch.float64)
+        for wi, args in items:
+            mask[wi] = True
+            ball[wi] = int(args[0])
+            rest = list(args[1:])
+            if kind in ("FollowBall", "Orbit"):
+                target[wi], f[wi, 0] = int(rest[0]), float(rest[1])
+            elif kind == "WarpTo":
+                f[wi, :4] = torch.tensor([float(x) for x in rest[:4]], dtype=torch.float64)
+                n[wi] = int(rest[4])
+            elif kind == "EntityWarpIn":
+                f[wi, :3] = torch.tensor([float(x) for x in rest[:3]], dtype=torch.float64)
+                n[wi] = int(rest[3])
+            elif kind in ("SetBallMassive", "SetBallInteractive"):
+                n[wi] = int(rest[0])
+            elif kind == "SetBallPosition":
+                f[wi, :3] = torch.tensor([float(x) for x in rest[:3]], dtype=torch.float64)
+                loc[wi] = 1 if rest[3] is True else 0
+            elif kind == "CloakBall":
+                n[wi], f[wi, 0] = int(rest[0]), float(rest[1])
+            elif rest:
+                f[wi, :len(rest)] = torch.tensor([float(x) for x in rest], dtype=torch.float64)
+        out.append((kind, *(x.to(device) for x in (mask, ball, target, f, n, loc))))
+    return out
+
+
 def pushes(cs: list, t: int, device) -> list:
     """Tick t's calls of every world as pushes: the j-th calls of one kind of all worlds together, each world's calls
     in its own order: [(kind, mask, ball, target, f, n, loc)]."""
-    W = len(cs)
     out = []
     width = max((len(w["ticks"][t]) for w in cs), default=0)
     for j in range(width):
@@ -108,33 +139,74 @@ def pushes(cs: list, t: int, device) -> list:
             calls = w["ticks"][t]
             if j < len(calls):
                 by_kind[ACTION_KINDS[calls[j][0]]].append((wi, calls[j][1]))
-        for kind, items in by_kind.items():
-            mask = torch.zeros(W, dtype=torch.bool)
-            ball, target, n, loc = (torch.zeros(W, dtype=torch.int64) for _ in range(4))
-            f = torch.zeros(W, 4, dtype=torch.float64)
-            for wi, args in items:
-                mask[wi] = True
-                ball[wi] = int(args[0])
-                rest = list(args[1:])
-                if kind in ("FollowBall", "Orbit"):
-                    target[wi], f[wi, 0] = int(rest[0]), float(rest[1])
-                elif kind == "WarpTo":
-                    f[wi, :4] = torch.tensor([float(x) for x in rest[:4]], dtype=torch.float64)
-                    n[wi] = int(rest[4])
-                elif kind == "EntityWarpIn":
-                    f[wi, :3] = torch.tensor([float(x) for x in rest[:3]], dtype=torch.float64)
-                    n[wi] = int(rest[3])
-                elif kind in ("SetBallMassive", "SetBallInteractive"):
-                    n[wi] = int(rest[0])
-                elif kind == "SetBallPosition":
-                    f[wi, :3] = torch.tensor([float(x) for x in rest[:3]], dtype=torch.float64)
-                    loc[wi] = 1 if rest[3] is True else 0
-                elif kind == "CloakBall":
-                    n[wi], f[wi, 0] = int(rest[0]), float(rest[1])
-                elif rest:
-                    f[wi, :len(rest)] = torch.tensor([float(x) for x in rest], dtype=torch.float64)
-            out.append((kind, *(x.to(device) for x in (mask, ball, target, f, n, loc))))
+        out += _group(by_kind, len(cs), device)
     return out
+
+
+# the game's queries of the Actions queue and the undo of a pending cloak, between the calls
+QUERIES = ("has_pending_cloak", "has_pending_uncloak", "get_pending_cloak_mode", "get_pending_interactive_state",
+           "get_pending_speed_fraction")
+UNDO = "undo_pending_cloak"
+
+
+def steps(cs: list, t: int, device) -> list:
+    """Tick t of every world with queries and undos among its calls: for each position j, the calls at j as pushes
+    (one a kind), then the queries and undos at j (one a name): ("push", ...), ("query", name, mask, ball),
+    ("undo", mask, ball)."""
+    W = len(cs)
+    out = []
+    width = max((len(w["ticks"][t]) for w in cs), default=0)
+    for j in range(width):
+        by_kind, asks = defaultdict(list), defaultdict(list)
+        for wi, w in enumerate(cs):
+            calls = w["ticks"][t]
+            if j >= len(calls):
+                continue
+            name, args = calls[j]
+            if name in QUERIES or name == UNDO:
+                asks[name].append((wi, int(args[0])))
+            else:
+                by_kind[ACTION_KINDS[name]].append((wi, args))
+        out += [("push", *p) for p in _group(by_kind, W, device)]
+        for name, items in asks.items():
+            mask = torch.zeros(W, dtype=torch.bool)
+            ball = torch.zeros(W, dtype=torch.int64)
+            for wi, b in items:
+                mask[wi], ball[wi] = True, b
+            mask, ball = mask.to(device), ball.to(device)
+            out.append(("undo", mask, ball) if name == UNDO else ("query", name, mask, ball))
+    return out
+
+
+def answer_digest(name: str, res, mask: torch.Tensor) -> np.uint64:
+    """A query's answer over every world as one digest: the flag (has_*), or the value where known and the known
+    flags (get_*)."""
+    if name.startswith("has_"):
+        parts = [_h(name, res & mask)]
+    else:
+        value, known = res
+        parts = [_h(name + ":v", torch.where(known, value, torch.zeros_like(value))), _h(name + ":k", known)]
+    d = hashlib.sha256(np.array(parts, dtype=np.uint64).tobytes()).digest()
+    return np.frombuffer(d[:8], dtype=np.uint64)[0]
+
+
+def drive_pending(server, cs: list, device, on_tick) -> None:
+    """Each tick: the steps in order (pushes, queries, undos), the pre-tick, the park's tick, the post-tick;
+    on_tick(t, server, [the answers' digests])."""
+    for t in range(len(cs[0]["ticks"])):
+        answers = []
+        for st in steps(cs, t, device):
+            if st[0] == "push":
+                server.push(*st[1:])
+            elif st[0] == "undo":
+                server.undo_pending_cloak(st[1], st[2])
+            else:
+                name, mask, ball = st[1:]
+                answers.append(answer_digest(name, getattr(server, name)(mask, ball), mask))
+        server.pre_tick()
+        server.evolve()
+        server.post_tick()
+        on_tick(t, server, np.array(answers, dtype=np.uint64))
 
 
 def drive(server, cs: list, evolve: bool, device, on_tick=None) -> None:
@@ -154,8 +226,9 @@ def drive(server, cs: list, evolve: bool, device, on_tick=None) -> None:
 # ---- the golden bundle ----
 
 def save(path: Path, runs: list) -> None:
-    """runs: [{"cases", "do", "evolve", "park" [T, F] uint64, "batch": [T arrays]}]."""
-    body = [{"cases": r["cases"], "do": r["do"], "evolve": r["evolve"]} for r in runs]
+    """runs: [{"cases", "do", "evolve", "park" [T, F] uint64, "batch": [T arrays], and for runs with queries
+    "answers": [T arrays]}]."""
+    body = [{"cases": r["cases"], "do": r["do"], "evolve": r["evolve"], "pending": "answers" in r} for r in runs]
     with gzip.open(str(path) + ".json.gz", "wt") as f:
         json.dump(body, f)
     arrays = {}
@@ -163,6 +236,8 @@ def save(path: Path, runs: list) -> None:
         arrays[f"r{i}_park"] = r["park"]
         for t, b in enumerate(r["batch"]):
             arrays[f"r{i}_batch{t}"] = b
+        for t, a in enumerate(r.get("answers", [])):
+            arrays[f"r{i}_answers{t}"] = a
     np.savez_compressed(str(path) + ".npz", **arrays)
 
 
@@ -173,6 +248,8 @@ def load(path: Path) -> list:
     for i, r in enumerate(body):
         r["park"] = z[f"r{i}_park"]
         r["batch"] = [z[f"r{i}_batch{t}"] for t in range(len(r["park"]))]
+        if r.get("pending"):
+            r["answers"] = [z[f"r{i}_answers{t}"] for t in range(len(r["park"]))]
         for w in r["cases"]:
             w["pilots"] = {int(k): v for k, v in w["pilots"].items()}
             w["ticks"] = [[(c[0], tuple(c[1])) for c in calls] for calls in w["ticks"]]
@@ -180,11 +257,12 @@ def load(path: Path) -> list:
 
 
 def replay(server_mod, park_cls, run: dict, device, kernel: str | None = None) -> list:
-    """A recorded run on server_mod's layer over park_cls: the differences [(tick, 'park', fields) or (tick, 'batch')]."""
+    """A recorded run on server_mod's layer over park_cls: the differences [(tick, 'park', fields), (tick, 'batch') or
+    (tick, 'answers')]."""
     server, _ = build(server_mod, park_cls, run["cases"], run["do"], device, kernel=kernel)
     bad = []
 
-    def on_tick(t, s):
+    def check(t, s):
         got = tr.field_digests(s.a.park)
         mm = [PARK_FIELDS[k] for k in range(len(PARK_FIELDS)) if got[k] != run["park"][t][k]]
         if mm:
@@ -193,5 +271,14 @@ def replay(server_mod, park_cls, run: dict, device, kernel: str | None = None) -
         want = run["batch"][t]
         if b.shape != want.shape or not (b == want).all():
             bad.append((t, "batch"))
-    drive(server, run["cases"], run["evolve"], device, on_tick)
+
+    if run.get("pending"):
+        def on_tick(t, s, answers):
+            check(t, s)
+            want = run["answers"][t]
+            if answers.shape != want.shape or not (answers == want).all():
+                bad.append((t, "answers"))
+        drive_pending(server, run["cases"], device, on_tick)
+    else:
+        drive(server, run["cases"], run["evolve"], device, check)
     return bad

@@ -37,6 +37,19 @@ def test_the_server_layer_replays_the_golden_ticks(name, run, kernel):
     assert not bad, f"{len(bad)} differences, first {bad[:3]}"
 
 
+@pytest.mark.gpu
+@pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")
+@pytest.mark.parametrize("run", [0, 1], ids=["development", "held_out"])
+@pytest.mark.parametrize("kernel", ["torch", "cuda"])
+def test_the_pending_queries_and_undos_replay_the_golden_ticks(run, kernel):
+    """The reference's pending-query scenarios (queries of every kind among the calls, undos of a pending cloak, the
+    prune's edge): every answer, the park and the update batch after every tick, on both paths."""
+    from exact_ballpark_b200 import VecModesPark, server
+    r = _golden("server_pending")[run]
+    bad = st.replay(server, VecModesPark, r, "cuda", kernel=kernel)
+    assert not bad, f"{len(bad)} differences, first {bad[:3]}"
+
+
 # ---- random queues: the kernel against the torch path ----
 
 def _random_worlds(seed: int, W: int, do: bool) -> list:
@@ -171,6 +184,17 @@ def test_a_server_graph_replays_eager_kernel_ticks():
             assert torch.equal(out.slots[j].ok, eager.batch.slots[j].ok), (t, j)
 
 
+def test_the_pending_goldens_hold_queries_and_undos():
+    runs = _golden("server_pending")
+    assert len(runs) == 2
+    for r in runs:
+        names = [c[0] for w in r["cases"] for t in w["ticks"] for c in t]
+        assert names.count(st.UNDO) >= 300
+        for q in st.QUERIES:
+            assert names.count(q) >= 50, q
+        assert len(r["answers"]) == len(r["park"]) and sum(len(a) for a in r["answers"]) > 100
+
+
 def test_the_server_goldens_hold_every_action_kind():
     from exact_ballpark_b200 import server
     for name in ("server_modes", "server_modes_do"):
@@ -231,6 +255,48 @@ def test_push_drops_a_call_equal_to_the_worlds_last_and_keeps_the_rest():
         s.push("LaunchMissile", both, torch.tensor([10, 20]))
     assert len(s.slots) == 7
     assert SimpleNamespace(**s.last).kind.tolist() == [server.CODE["FollowBall"]] * 2
+
+
+def _standin_server(kernel: str):
+    from exact_ballpark_b200 import server
+    A = _StandIn()
+    s = server.VecServer.__new__(server.VecServer)
+    s.a, s.W, s.R, s.dev, s.kernel = A, A.W, A.R, A.dev, kernel
+    s.settled = torch.tensor([True, True, True, True, True, True])
+    A.cloaked = torch.tensor([0, 0, 0, 0, 0, 2])
+    s.slots = []
+    s._reset_last()
+    return s
+
+
+@pytest.mark.parametrize("kernel", ["torch", "cuda"])
+def test_an_undo_prunes_the_pending_cloaks_and_the_calls_around_them_stand(kernel):
+    """X, CloakBall, X, undo: both X stay queued (the second was tested against the cloak); a cloak pushed twice is
+    queued once and the undo takes it out; the pending mode falls back to the ball's cloak byte. On the kernel path the
+    calls are tested at the query, as the kernel tests them, and the undo marks them tested."""
+    s = _standin_server(kernel)
+    both = torch.tensor([True, True])
+    x = ("SetSpeedFraction", both, torch.tensor([11, 21]), None, torch.tensor([[0.5], [0.5]]))
+    cloak = ("CloakBall", both, torch.tensor([10, 22]), None, torch.tensor([[900.0], [900.0]]), torch.tensor([1, 3]))
+    s.push(*x)
+    s.push(*cloak)
+    s.push(*cloak)                                   # the same cloak again: a duplicate
+    s.push(*x)
+    assert [q.tolist() for q in s._queued()] == [[True, True], [True, True], [False, False], [True, True]]
+    assert s.has_pending_cloak(both, torch.tensor([10, 22])).tolist() == [True, True]
+    mode, known = s.get_pending_cloak_mode(both, torch.tensor([10, 22]))
+    assert mode.tolist() == [1, 3] and known.tolist() == [True, True]
+    s.undo_pending_cloak(torch.tensor([True, False]), torch.tensor([10, 22]))
+    assert s.has_pending_cloak(both, torch.tensor([10, 22])).tolist() == [False, True]
+    mode, known = s.get_pending_cloak_mode(both, torch.tensor([10, 22]))
+    assert mode.tolist() == [0, 3] and known.tolist() == [True, True]
+    mode, known = s.get_pending_cloak_mode(both, torch.tensor([99, 23]))
+    assert known.tolist() == [False, False]
+    assert [q.tolist() for q in s._queued()] == [[True, True], [False, True], [False, False], [True, True]]
+    s.push(*x)                                       # now equal to the world's last queued call: dropped
+    assert s._queued()[-1].tolist() == [False, False]
+    if kernel == "cuda":
+        assert all(getattr(q, "resolved", False) for q in s.slots[:4]) and not getattr(s.slots[4], "resolved", False)
 
 
 def test_the_kernel_path_wants_a_cuda_device_and_a_known_path():
