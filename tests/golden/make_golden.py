@@ -495,9 +495,44 @@ def make_server_pending() -> None:
     print(f"  server_pending: {len(runs)} runs of 40 worlds, {time.time() - t0:.0f} s", flush=True)
 
 
+def make_server_ontick() -> None:
+    """server_ontick: the reference's OnTick scenarios over the flight-mode park (tests/server_ontick_cases.py's
+    server_cases: 32 worlds, 14 OnTick calls, each world's own simulation clock: calls too early, a world's first call,
+    one interval, remainders carried, several intervals, the master's resynchronisation, the last call pushed again
+    across a kept queue; seed 1 development and 31 held out, dynamical orientation off and on), recorded on the
+    reference's VecServer (torch path, over its VecModesPark on the CPU) by server_trace's driver: after every call the
+    park's fields, each world's clocks and every round's worlds and update batch. Each scenario set is first run by
+    the reference's own comparison against its scalar server layer under OnTick (every send, every ship's fields,
+    the clocks): 0 differences."""
+    import server_ontick_cases as O
+    import server_trace as st
+    import exact_ballpark.vec_server as VS
+    from exact_ballpark.vec_modes import VecModesPark
+    t0 = time.time()
+    runs = []
+    for do in (False, True):
+        for seed in (1, 31):
+            res = O.run(O.server_cases(seed, 32, "modes", do, 14), "modes", "cpu", do=do)
+            if res["sends"] or res["rows"] or res["clocks"]:
+                raise RuntimeError(f"seed {seed}: the reference's OnTick differs from its scalar one")
+            cs = O.server_cases(seed, 32, "modes", do, 14)
+            parks, calls = [], []
+
+            def on_call(tk, server, batches):
+                parks.append(tr.field_digests(server.a.park))
+                calls.append(st.ontick_digests(server, batches))
+            server, _ = st.build(VS, VecModesPark, cs, do, "cpu")
+            st.drive_ontick(server, cs, "cpu", on_call)
+            runs.append({"cases": cs, "do": do, "evolve": True, "ontick": True,
+                         "park": np.array(parks, dtype=np.uint64), "batch": calls})
+            print(f"  do={do} seed {seed}: {res['coverage']}, {len(res['out'])} worlds left the domain", flush=True)
+    st.save(HERE / "server_ontick", runs)
+    print(f"  server_ontick: {len(runs)} runs, {time.time() - t0:.0f} s", flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending"),
+    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending", "server_ontick"),
                     default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
     a = ap.parse_args()
@@ -519,6 +554,8 @@ def main() -> None:
         make_server()
     if a.only in (None, "server_pending"):
         make_server_pending()
+    if a.only in (None, "server_ontick"):
+        make_server_ontick()
 
 
 if __name__ == "__main__":

@@ -55,11 +55,11 @@ def _fields_digest(fields) -> np.uint64:
     return np.frombuffer(d[:8], dtype=np.uint64)[0]
 
 
-def batch_digests(server) -> np.ndarray:
-    """The last tick's update batch as digests (uint64): the stamps and clocks, the routes, each queued call's kind,
-    queued flag, row, target row and local argument, each uncloak's recipients and the park's fields there, the
-    bubble's additions (fresh, listed, fields), and the narrowcast and character flags."""
-    b = server.batch
+def batch_digests(server, b=None) -> np.ndarray:
+    """The last tick's update batch (or the batch b) as digests (uint64): the stamps and clocks, the routes, each
+    queued call's kind, queued flag, row, target row and local argument, each uncloak's recipients and the park's
+    fields there, the bubble's additions (fresh, listed, fields), and the narrowcast and character flags."""
+    b = server.batch if b is None else b
     out = [_h("stamp", b.stamp), _h("clock", b.clock), _h("route", b.route.to(torch.int64))]
     for j, s in enumerate(b.slots):
         out += [np.uint64(s.kind), _h(f"ok{j}", s.ok), _h(f"row{j}", s.row), _h(f"trow{j}", s.trow),
@@ -223,12 +223,34 @@ def drive(server, cs: list, evolve: bool, device, on_tick=None) -> None:
             on_tick(t, server)
 
 
+def ontick_digests(server, batches: list) -> np.ndarray:
+    """One OnTick call as digests: each world's time, first-time flag and park time, the number of rounds run, and
+    each round's worlds and update batch."""
+    out = [_h("time", server.time), _h("first_time", server.first_time), _h("clock", server.a.clock()),
+           np.uint64(len(batches))]
+    for b in batches:
+        out.append(_h("ticked", b.ticked))
+        out += list(batch_digests(server, b))
+    return np.array(out, dtype=np.uint64)
+
+
+def drive_ontick(server, cs: list, device, on_tick) -> None:
+    """Each call: the worlds' calls pushed, then OnTick at each world's own simulation time (w["clock"][t]);
+    on_tick(t, server, batches)."""
+    for t in range(len(cs[0]["clock"])):
+        for kind, mask, ball, target, f, n, loc in pushes(cs, t, device):
+            server.push(kind, mask, ball, target, f, n, loc)
+        sim = torch.tensor([w["clock"][t] for w in cs], dtype=torch.int64)
+        on_tick(t, server, server.on_tick(sim))
+
+
 # ---- the golden bundle ----
 
 def save(path: Path, runs: list) -> None:
     """runs: [{"cases", "do", "evolve", "park" [T, F] uint64, "batch": [T arrays], and for runs with queries
     "answers": [T arrays]}]."""
-    body = [{"cases": r["cases"], "do": r["do"], "evolve": r["evolve"], "pending": "answers" in r} for r in runs]
+    body = [{"cases": r["cases"], "do": r["do"], "evolve": r["evolve"], "pending": "answers" in r,
+             "ontick": bool(r.get("ontick"))} for r in runs]
     with gzip.open(str(path) + ".json.gz", "wt") as f:
         json.dump(body, f)
     arrays = {}
@@ -272,7 +294,18 @@ def replay(server_mod, park_cls, run: dict, device, kernel: str | None = None) -
         if b.shape != want.shape or not (b == want).all():
             bad.append((t, "batch"))
 
-    if run.get("pending"):
+    if run.get("ontick"):
+        def on_call(t, s, batches):
+            got = tr.field_digests(s.a.park)
+            mm = [PARK_FIELDS[k] for k in range(len(PARK_FIELDS)) if got[k] != run["park"][t][k]]
+            if mm:
+                bad.append((t, "park", mm))
+            d = ontick_digests(s, batches)
+            want = run["batch"][t]
+            if d.shape != want.shape or not (d == want).all():
+                bad.append((t, "batches"))
+        drive_ontick(server, run["cases"], device, on_call)
+    elif run.get("pending"):
         def on_tick(t, s, answers):
             check(t, s)
             want = run["answers"][t]

@@ -50,6 +50,21 @@ def test_the_pending_queries_and_undos_replay_the_golden_ticks(run, kernel):
     assert not bad, f"{len(bad)} differences, first {bad[:3]}"
 
 
+@pytest.mark.gpu
+@pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")
+@pytest.mark.parametrize("run", [0, 1, 2, 3], ids=["euler-development", "euler-held_out", "dynamical-development",
+                                                   "dynamical-held_out"])
+@pytest.mark.parametrize("kernel", ["torch", "cuda"])
+def test_on_tick_replays_the_golden_calls(run, kernel):
+    """The reference's OnTick scenarios (each world's own clock: calls too early, first calls, remainders, the
+    master's resynchronisation, masked rounds, kept queues): after every call the park, each world's clocks and every
+    round's worlds and update batch, on both paths."""
+    from exact_ballpark_b200 import VecModesPark, server
+    r = _golden("server_ontick")[run]
+    bad = st.replay(server, VecModesPark, r, "cuda", kernel=kernel)
+    assert not bad, f"{len(bad)} differences, first {bad[:3]}"
+
+
 # ---- random queues: the kernel against the torch path ----
 
 def _random_worlds(seed: int, W: int, do: bool) -> list:
@@ -184,6 +199,17 @@ def test_a_server_graph_replays_eager_kernel_ticks():
             assert torch.equal(out.slots[j].ok, eager.batch.slots[j].ok), (t, j)
 
 
+def test_the_on_tick_goldens_hold_masked_rounds_and_kept_queues():
+    runs = _golden("server_ontick")
+    assert len(runs) == 4 and all(r["ontick"] for r in runs)
+    for r in runs:
+        T = len(r["cases"][0]["clock"])
+        assert r["park"].shape[0] == T and len(r["batch"]) == T
+        rounds = [int(d[3]) for d in r["batch"]]
+        assert sum(rounds) > 20 and 0 in rounds              # calls with no round, calls with several
+        assert max(rounds) > 1
+
+
 def test_the_pending_goldens_hold_queries_and_undos():
     runs = _golden("server_pending")
     assert len(runs) == 2
@@ -297,6 +323,29 @@ def test_an_undo_prunes_the_pending_cloaks_and_the_calls_around_them_stand(kerne
     assert s._queued()[-1].tolist() == [False, False]
     if kernel == "cuda":
         assert all(getattr(q, "resolved", False) for q in s.slots[:4]) and not getattr(s.slots[4], "resolved", False)
+
+
+def test_a_masked_split_keeps_the_same_queue_on_both_paths():
+    """OnTick's queue split: a world without a tick keeps its queued calls (a duplicate dropped), in order, and the
+    ticking worlds' calls go to the pre-tick, alike on the torch path (tested at each push) and the kernel path (tested
+    at the split, as the kernel tests them)."""
+    both = torch.tensor([True, True])
+    on = torch.tensor([True, False])
+    kept = {}
+    for kernel in ("torch", "cuda"):
+        s = _standin_server(kernel)
+        s.push("SetSpeedFraction", both, torch.tensor([11, 21]), f=torch.tensor([[0.5], [0.5]]))
+        s.push("SetSpeedFraction", both, torch.tensor([11, 21]), f=torch.tensor([[0.5], [0.5]]))   # duplicates
+        s.push("CloakBall", torch.tensor([False, True]), torch.tensor([10, 22]), n=torch.tensor([1, 1]),
+               f=torch.tensor([[9.0], [9.0]]))
+        if kernel == "cuda":
+            s._test_pending(commit=True)
+        flag = "ok" if kernel == "torch" else "mask"
+        going = s._split_queue(on, flag)
+        kept[kernel] = [(q.kind, getattr(q, flag).tolist(), q.loc.tolist()) for q in s.slots]
+        assert [getattr(q, flag).tolist() for q in going] == [[True, False], [False, False], [False, False]]
+    assert kept["torch"] == kept["cuda"]
+    assert [k[1] for k in kept["torch"]] == [[False, True], [False, True]]
 
 
 def test_the_kernel_path_wants_a_cuda_device_and_a_known_path():
