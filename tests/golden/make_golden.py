@@ -430,8 +430,9 @@ def make_server() -> None:
     and kept, cloaks and uncloaks in both orders, local and non-local SetBallPosition, follows and orbits of a
     cloaking ship, warps and warp-ins with followers, every setter, refused values; seeds 1 and 2; without and with
     dynamical orientation), recorded on the reference's VecServer (torch path, over its VecModesPark on the CPU) by
-    tests/golden/server_trace.py's driver. Each scenario set is first run by the reference's own comparison against
-    its scalar server layer (server_cases.run: every ball's state and every client's update list): 0 differences."""
+    tests/golden/server_trace.py's driver, with the digest of what every client is sent (the reference's decode). Each
+    scenario set is first run by the reference's own comparison against its scalar server layer (server_cases.run:
+    every ball's state and every client's update list): 0 differences."""
     import server_cases as S
     import server_trace as st
     import exact_ballpark.vec_server as VS
@@ -444,18 +445,51 @@ def make_server() -> None:
             res = S.run(cs, "modes", "cpu", do=do, evolve=True)
             if res["rows"] or res["sends"] or not res["compared"]:
                 raise RuntimeError(f"seed {seed}: the reference's server layer differs from its scalar one")
-            parks, batches = [], []
+            parks, batches, sends = [], [], []
 
             def on_tick(tk, server):
                 parks.append(tr.field_digests(server.a.park))
                 batches.append(st.batch_digests(server))
+                sends.append(st.decode_digest(VS.decode(server)))
             server, _ = st.build(VS, VecModesPark, cs, do, "cpu")
             st.drive(server, cs, True, "cpu", on_tick)
             runs.append({"cases": cs, "do": do, "evolve": True, "park": np.array(parks, dtype=np.uint64),
-                         "batch": batches})
+                         "batch": batches, "decode": sends})
         name = "server_modes_do" if do else "server_modes"
         st.save(HERE / name, runs)
         print(f"  {name}: {len(runs)} runs of {len(runs[0]['cases'])} worlds, {time.time() - t:.0f} s", flush=True)
+
+
+def make_server_collide() -> None:
+    """server_collide: the reference's server scenarios over the collision park (tests/server_cases.py with park
+    "collide": 40 worlds of 2 to 5 massive balls within 3 km that meet, GotoPoint, GotoDirection, Stop, the speed
+    fraction, SetBallMassive, SetBallInteractive, the cloaks; seeds 1 and 2, 14 ticks), recorded on the reference's
+    VecServer over its CollideAdapter (torch path, its VecCollidePark on the CPU) by server_trace's driver: the park's
+    fields (collide_trace's), the update batch and what every client is sent, after every tick. Each scenario set is
+    first run by the reference's own comparison against its scalar server layer: 0 differences."""
+    import server_cases as S
+    import server_trace as st
+    import exact_ballpark.vec_server as VS
+    from exact_ballpark.vec_collide import VecCollidePark
+    t0 = time.time()
+    runs = []
+    for seed in (1, 2):
+        cs = S.cases(seed, 40, "collide", ticks=14)
+        res = S.run(cs, "collide", "cpu", evolve=True)
+        if res["rows"] or res["sends"] or not res["compared"]:
+            raise RuntimeError(f"seed {seed}: the reference's server layer differs from its scalar one")
+        parks, batches, sends = [], [], []
+
+        def on_tick(tk, server):
+            parks.append(st.park_digests("collide", server.a.park))
+            batches.append(st.batch_digests(server))
+            sends.append(st.decode_digest(VS.decode(server)))
+        server, _ = st.build(VS, VecCollidePark, cs, False, "cpu", park="collide")
+        st.drive(server, cs, True, "cpu", on_tick)
+        runs.append({"cases": cs, "do": False, "evolve": True, "park": np.array(parks, dtype=np.uint64),
+                     "batch": batches, "decode": sends, "park_kind": "collide"})
+    st.save(HERE / "server_collide", runs)
+    print(f"  server_collide: {len(runs)} runs of 40 worlds, {time.time() - t0:.0f} s", flush=True)
 
 
 def make_server_pending() -> None:
@@ -480,16 +514,17 @@ def make_server_pending() -> None:
         if res["answers"] or res["sends"] or res["rows"] or res["flagged"]:
             raise RuntimeError(f"seed {seed}: the reference's server layer differs from its scalar one")
         cs = P.augment(S.cases(seed, 40, "modes", ticks=12), "server", f"modes-{seed}", P.MODES["server"]["modes"])
-        parks, batches, answers = [], [], []
+        parks, batches, answers, sends = [], [], [], []
 
         def on_tick(tk, server, ans):
             parks.append(tr.field_digests(server.a.park))
             batches.append(st.batch_digests(server))
             answers.append(ans)
+            sends.append(st.decode_digest(VS.decode(server)))
         server, _ = st.build(VS, VecModesPark, cs, False, "cpu")
         st.drive_pending(server, cs, "cpu", on_tick)
         runs.append({"cases": cs, "do": False, "evolve": True, "park": np.array(parks, dtype=np.uint64),
-                     "batch": batches, "answers": answers})
+                     "batch": batches, "answers": answers, "decode": sends})
         print(f"  seed {seed}: {res['volumes']['answers']} answers, {res['volumes']['undos']} undos", flush=True)
     st.save(HERE / "server_pending", runs)
     print(f"  server_pending: {len(runs)} runs of 40 worlds, {time.time() - t0:.0f} s", flush=True)
@@ -516,15 +551,16 @@ def make_server_ontick() -> None:
             if res["sends"] or res["rows"] or res["clocks"]:
                 raise RuntimeError(f"seed {seed}: the reference's OnTick differs from its scalar one")
             cs = O.server_cases(seed, 32, "modes", do, 14)
-            parks, calls = [], []
+            parks, calls, sends = [], [], []
 
             def on_call(tk, server, batches):
                 parks.append(tr.field_digests(server.a.park))
                 calls.append(st.ontick_digests(server, batches))
+                sends.append(st.decode_digest([VS.decode(server, b) for b in batches]))
             server, _ = st.build(VS, VecModesPark, cs, do, "cpu")
             st.drive_ontick(server, cs, "cpu", on_call)
             runs.append({"cases": cs, "do": do, "evolve": True, "ontick": True,
-                         "park": np.array(parks, dtype=np.uint64), "batch": calls})
+                         "park": np.array(parks, dtype=np.uint64), "batch": calls, "decode": sends})
             print(f"  do={do} seed {seed}: {res['coverage']}, {len(res['out'])} worlds left the domain", flush=True)
     st.save(HERE / "server_ontick", runs)
     print(f"  server_ontick: {len(runs)} runs, {time.time() - t0:.0f} s", flush=True)
@@ -532,7 +568,8 @@ def make_server_ontick() -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending", "server_ontick"),
+    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending", "server_ontick",
+                                       "server_collide"),
                     default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
     a = ap.parse_args()
@@ -556,6 +593,8 @@ def main() -> None:
         make_server_pending()
     if a.only in (None, "server_ontick"):
         make_server_ontick()
+    if a.only in (None, "server_collide"):
+        make_server_collide()
 
 
 if __name__ == "__main__":

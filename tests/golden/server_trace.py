@@ -22,6 +22,7 @@ from pathlib import Path
 import numpy as np
 import torch
 
+import collide_trace as ct
 import trace as tr
 
 GOLDEN = Path(__file__).resolve().parent
@@ -50,7 +51,7 @@ def _h(name: str, a) -> np.uint64:
 def _fields_digest(fields) -> np.uint64:
     if fields is None:
         return np.uint64(0)
-    parts = [_h(k, fields[k]) for k in STREAM_FIELDS]
+    parts = [_h(k, fields[k]) for k in STREAM_FIELDS if k in fields]      # (a collision park has no rotation)
     d = hashlib.sha256(np.array(parts, dtype=np.uint64).tobytes() + bytes([int(bool(fields["dynamical"]))])).digest()
     return np.frombuffer(d[:8], dtype=np.uint64)[0]
 
@@ -74,10 +75,38 @@ def batch_digests(server, b=None) -> np.ndarray:
 
 # ---- the batch's park and server ----
 
+def park_digests(park_kind: str, park) -> np.ndarray:
+    return (ct.field_digests(park) if park_kind == "collide" else tr.field_digests(park))
+
+
+def park_fields(park_kind: str) -> tuple:
+    return ct.FIELDS if park_kind == "collide" else PARK_FIELDS
+
+
 def build(server_mod, park_cls, cs: list, do: bool, device, friction: float = 1.0e6, tick_ms: int = 1000,
-          kernel: str | None = None):
-    """The server layer (server_mod's VecServer over its ModesAdapter; `kernel` its path, when given) over a flight
-    park of the worlds cs: (server, {(world, ball id): row})."""
+          kernel: str | None = None, park: str = "modes"):
+    """The server layer (server_mod's VecServer over its ModesAdapter, or its CollideAdapter for park "collide";
+    `kernel` its path, when given) over a park of the worlds cs: (server, {(world, ball id): row})."""
+    if park == "collide":                                # W worlds of N slots, a world's balls in ascending id
+        slots = max(len(w["balls"]) for w in cs)
+        p = park_cls(len(cs), slots, friction=friction, tick_interval_ms=tick_ms, device=device)
+        p.load([[{"id": b["id"], "mass": b["mass"], "radius": b["radius"], "max_vel": b["max_vel"],
+                  "agility": b["agility"], "speed_fraction": b["sf"], "pos": b["pos"], "vel": b["vel"], "free": True,
+                  "massive": b["massive"]} for b in w["balls"]] for w in cs])
+        index, inter = {}, []
+        for wi, w in enumerate(cs):
+            by_id = {b["id"]: b for b in w["balls"]}
+            flags = [False] * slots
+            for k, bid in enumerate(sorted(by_id)):
+                index[(w["id"], bid)] = wi * slots + k
+                flags[k] = by_id[bid]["interactive"]
+            inter += flags
+        a = server_mod.CollideAdapter(p, interactive=inter)
+        pilots = [-1] * a.R
+        for w in cs:
+            for bid, pp in w["pilots"].items():
+                pilots[index[(w["id"], int(bid))]] = pp
+        return server_mod.VecServer(a, pilots), index
     rows = [(w, b) for w in cs for b in w["balls"]]
     p = park_cls(len(rows), friction=friction, tick_interval_ms=tick_ms, device=device, dynamical_orientation=do)
     p.load([{"id": b["id"], "world": w["id"], "time": 0, "mass": b["mass"], "radius": b["radius"],
@@ -244,13 +273,42 @@ def drive_ontick(server, cs: list, device, on_tick) -> None:
         on_tick(t, server, server.on_tick(sim))
 
 
+def canon(x):
+    """A decoded value as compared: floats by their bits, ints and bools apart, bytes, a marshalled payload by its
+    value (either layer's Marshalled), sequences by type and item."""
+    if isinstance(x, bool):
+        return ("b", x)
+    if isinstance(x, int):
+        return ("i", int(x))
+    if isinstance(x, float):
+        return ("f", "nan" if x != x else x.hex())
+    if isinstance(x, (bytes, bytearray)):
+        return ("B", bytes(x).hex())
+    if type(x).__name__ == "Marshalled":
+        return ("M", canon(x.value))
+    if isinstance(x, (list, tuple)):
+        return (type(x).__name__, tuple(canon(v) for v in x))
+    if isinstance(x, dict):
+        return ("d", tuple((canon(k), canon(v)) for k, v in x.items()))
+    if isinstance(x, str):
+        return ("s", x)
+    raise TypeError(type(x))
+
+
+def decode_digest(decoded) -> np.uint64:
+    """What every client of every world is sent (a decode's result, or a list of them) as one digest."""
+    d = hashlib.sha256(repr(canon(decoded)).encode()).digest()
+    return np.frombuffer(d[:8], dtype=np.uint64)[0]
+
+
 # ---- the golden bundle ----
 
 def save(path: Path, runs: list) -> None:
     """runs: [{"cases", "do", "evolve", "park" [T, F] uint64, "batch": [T arrays], and for runs with queries
     "answers": [T arrays]}]."""
     body = [{"cases": r["cases"], "do": r["do"], "evolve": r["evolve"], "pending": "answers" in r,
-             "ontick": bool(r.get("ontick"))} for r in runs]
+             "ontick": bool(r.get("ontick")), "decoded": "decode" in r, "park_kind": r.get("park_kind", "modes")}
+            for r in runs]
     with gzip.open(str(path) + ".json.gz", "wt") as f:
         json.dump(body, f)
     arrays = {}
@@ -260,6 +318,8 @@ def save(path: Path, runs: list) -> None:
             arrays[f"r{i}_batch{t}"] = b
         for t, a in enumerate(r.get("answers", [])):
             arrays[f"r{i}_answers{t}"] = a
+        if "decode" in r:
+            arrays[f"r{i}_decode"] = np.array(r["decode"], dtype=np.uint64)
     np.savez_compressed(str(path) + ".npz", **arrays)
 
 
@@ -272,6 +332,8 @@ def load(path: Path) -> list:
         r["batch"] = [z[f"r{i}_batch{t}"] for t in range(len(r["park"]))]
         if r.get("pending"):
             r["answers"] = [z[f"r{i}_answers{t}"] for t in range(len(r["park"]))]
+        if r.get("decoded"):
+            r["decode"] = z[f"r{i}_decode"]
         for w in r["cases"]:
             w["pilots"] = {int(k): v for k, v in w["pilots"].items()}
             w["ticks"] = [[(c[0], tuple(c[1])) for c in calls] for calls in w["ticks"]]
@@ -279,14 +341,21 @@ def load(path: Path) -> list:
 
 
 def replay(server_mod, park_cls, run: dict, device, kernel: str | None = None) -> list:
-    """A recorded run on server_mod's layer over park_cls: the differences [(tick, 'park', fields), (tick, 'batch') or
-    (tick, 'answers')]."""
-    server, _ = build(server_mod, park_cls, run["cases"], run["do"], device, kernel=kernel)
+    """A recorded run on server_mod's layer over park_cls: the differences [(tick, 'park', fields), (tick, 'batch'),
+    (tick, 'answers') or (tick, 'sends')]."""
+    kind = run.get("park_kind", "modes")
+    server, _ = build(server_mod, park_cls, run["cases"], run["do"], device, kernel=kernel, park=kind)
+    names = park_fields(kind)
     bad = []
 
+    def sends(t, decoded):
+        if "decode" in run and decode_digest(decoded) != run["decode"][t]:
+            bad.append((t, "sends"))
+
     def check(t, s):
-        got = tr.field_digests(s.a.park)
-        mm = [PARK_FIELDS[k] for k in range(len(PARK_FIELDS)) if got[k] != run["park"][t][k]]
+        sends(t, server_mod.decode(s))
+        got = park_digests(kind, s.a.park)
+        mm = [names[k] for k in range(len(names)) if got[k] != run["park"][t][k]]
         if mm:
             bad.append((t, "park", mm))
         b = batch_digests(s)
@@ -296,6 +365,7 @@ def replay(server_mod, park_cls, run: dict, device, kernel: str | None = None) -
 
     if run.get("ontick"):
         def on_call(t, s, batches):
+            sends(t, [server_mod.decode(s, b) for b in batches])
             got = tr.field_digests(s.a.park)
             mm = [PARK_FIELDS[k] for k in range(len(PARK_FIELDS)) if got[k] != run["park"][t][k]]
             if mm:

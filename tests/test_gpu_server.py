@@ -65,6 +65,18 @@ def test_on_tick_replays_the_golden_calls(run, kernel):
     assert not bad, f"{len(bad)} differences, first {bad[:3]}"
 
 
+@pytest.mark.gpu
+@pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")
+@pytest.mark.parametrize("run", [0, 1], ids=["development", "held_out"])
+def test_the_server_layer_over_the_collision_park_replays_the_golden_ticks(run):
+    """The reference's server scenarios over the collision park (massive balls within 3 km that meet, cloaks,
+    SetBallMassive, SetBallInteractive): the park's every field, the batch and every client's sends, every tick."""
+    from exact_ballpark_b200 import VecCollidePark, server
+    r = _golden("server_collide")[run]
+    bad = st.replay(server, VecCollidePark, r, "cuda")
+    assert not bad, f"{len(bad)} differences, first {bad[:3]}"
+
+
 # ---- random queues: the kernel against the torch path ----
 
 def _random_worlds(seed: int, W: int, do: bool) -> list:
@@ -197,6 +209,14 @@ def test_a_server_graph_replays_eager_kernel_ticks():
         assert torch.equal(graphed.dead, eager.dead)
         for j in range(len(sched)):
             assert torch.equal(out.slots[j].ok, eager.batch.slots[j].ok), (t, j)
+
+
+def test_every_server_golden_carries_the_clients_sends():
+    for name in ("server_modes", "server_modes_do", "server_pending", "server_ontick", "server_collide"):
+        for r in _golden(name):
+            assert r["decoded"] and len(r["decode"]) == len(r["park"])
+    kinds = {c[0] for r in _golden("server_collide") for w in r["cases"] for t in w["ticks"] for c in t}
+    assert {"cloak_ball", "uncloak_ball", "set_ball_massive", "go_to_point", "stop"} <= kinds
 
 
 def test_the_on_tick_goldens_hold_masked_rounds_and_kept_queues():
@@ -346,6 +366,47 @@ def test_a_masked_split_keeps_the_same_queue_on_both_paths():
         assert [getattr(q, flag).tolist() for q in going] == [[True, False], [False, False], [False, False]]
     assert kept["torch"] == kept["cuda"]
     assert [k[1] for k in kept["torch"]] == [[False, True], [False, True]]
+
+
+def _fields(mode: int, free: bool = True, dynamical: bool = False) -> dict:
+    f = {"ids": torch.tensor([7]), "mode": torch.tensor([mode]), "radius": torch.tensor([12.5]),
+         "pos": torch.tensor([[1.0, -2.0, 3.5]], dtype=torch.float64), "free": torch.tensor([free]),
+         "massive": torch.tensor([True]), "interactive": torch.tensor([False]), "mass": torch.tensor([1e6]),
+         "cloaked": torch.tensor([200]), "max_vel": torch.tensor([150.0]),
+         "vel": torch.tensor([[4.0, 5.0, 6.0]], dtype=torch.float64), "agility": torch.tensor([0.75]),
+         "speed_fraction": torch.tensor([0.5]), "goto": torch.tensor([[9.0, 8.0, 7.0]], dtype=torch.float64),
+         "follow_id": torch.tensor([42]), "follow_range": torch.tensor([250.0]),
+         "effect_stamp": torch.tensor([(1 << 32) + 5]), "last_collision": torch.tensor([3.25]),
+         "owner_id": torch.tensor([3000]), "rot": torch.tensor([[0.0, 0.0, 0.0, 1.0]]),
+         "max_ang_vel": torch.tensor([1.0]), "ang_vel": torch.tensor([[0.0, 0.5, 0.0]]),
+         "rot_agility": torch.tensor([0.9]), "dynamical": dynamical}
+    return f
+
+
+def test_a_ball_stream_has_write_ball_to_streams_layout():
+    import struct
+
+    from exact_ballpark_b200 import server
+    blob = server.ball_stream(_fields(3), [0], 12)                       # a free ball in WARP
+    tag, time = struct.unpack_from("<Bi", blob, 0)
+    head = struct.unpack_from("<qBf3dB", blob, 5)
+    assert (tag, time) == (1, 12) and head == (7, 3, 12.5, 1.0, -2.0, 3.5, 0x01 | 0x04)
+    o = 5 + struct.calcsize("<qBf3dB")
+    assert struct.unpack_from("<dbqii", blob, o) == (1e6, 200 - 256, -1, -1, -1)     # the cloak as a signed char
+    o += struct.calcsize("<dbqii")
+    assert struct.unpack_from("<f3dff", blob, o) == (150.0, 4.0, 5.0, 6.0, 0.75, 0.5)
+    o += struct.calcsize("<f3dff")
+    assert struct.unpack_from("<b", blob, o) == (-1,)                               # no formation
+    o += 1
+    assert struct.unpack_from("<3didqq", blob, o) == (9.0, 8.0, 7.0, 5, 3.25, 42, 3000)
+    assert len(blob) == o + struct.calcsize("<3didqq")
+    held = server.ball_stream(_fields(2, free=False), [0], 12)            # STOP, not free: no motion block, no tail
+    assert len(held) == 5 + struct.calcsize("<qBf3dB") + struct.calcsize("<dbqii") + 1
+    rigid = server.ball_stream(_fields(11, free=False), [0], 12)          # RIGID: no mass block either
+    assert len(rigid) == 5 + struct.calcsize("<qBf3dB") + 1
+    turning = server.ball_stream(_fields(0, dynamical=True), [0], -1)     # GOTO with the orientation block
+    assert struct.unpack_from("<Bi", turning, 0) == (1, -1)
+    assert len(turning) == len(blob) - struct.calcsize("<3didqq") + struct.calcsize("<4ff3ff") + 24
 
 
 def test_the_kernel_path_wants_a_cuda_device_and_a_known_path():
