@@ -456,6 +456,49 @@ def combat_runs(args, dev, composed: bool = False) -> dict:
     return out
 
 
+def pipelined(dev, steps: int, send, run, fetch) -> float:
+    """Milliseconds for `steps` end-to-end steps through the public API, double-buffered over two streams: step t+1's
+    inputs are copied in and step t-1's results copied out on a copy stream while step t's tick runs. send(t, s)
+    copies step t's inputs from pinned host memory into device slot s = t % 2 (on the copy stream); run(t, s) takes
+    slot s into the tick, runs it and copies its results into device slot s (on the compute stream); fetch(t, s)
+    copies result slot s to pinned host memory (on the copy stream). Every step still moves its own bytes each way;
+    the CUDA events bracket all the steps, both streams joined at the end."""
+    import torch
+    comp = torch.cuda.current_stream(dev)
+    side = torch.cuda.Stream(device=dev)
+    sent = [torch.cuda.Event() for _ in range(2)]          # slot s's inputs are on the device
+    taken = [torch.cuda.Event() for _ in range(2)]         # slot s's inputs are in the tick, slot s's results out
+    fetched = [torch.cuda.Event() for _ in range(2)]       # slot s's results are on the host
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    start.record(comp)
+    side.wait_stream(comp)
+    with torch.cuda.stream(side):
+        send(0, 0)
+        sent[0].record(side)
+    for t in range(steps):
+        s = t % 2
+        if t + 1 < steps:
+            with torch.cuda.stream(side):
+                if t >= 1:
+                    side.wait_event(taken[1 - s])         # the tick of step t - 1 has its inputs
+                send(t + 1, 1 - s)
+                sent[1 - s].record(side)
+        comp.wait_event(sent[s])
+        if t >= 2:
+            comp.wait_event(fetched[s])                   # step t - 2's results are on the host
+        run(t, s)
+        taken[s].record(comp)
+        with torch.cuda.stream(side):
+            side.wait_event(taken[s])
+            fetch(t, s)
+            fetched[s].record(side)
+    comp.wait_stream(side)
+    end.record(comp)
+    end.synchronize()
+    return start.elapsed_time(end)
+
+
 # Algorithmic bytes of one world's pre-tick on the server kernel at the server benchmark's shape (4 piloted ships, the
 # 8 pushes GotoDirection and SetSpeedFraction a ship): per queued call the pushed columns read (mask 1, ball, target,
 # n, local flag 4 x 8, floats 32) and the outputs written (queued 1, row, target row, local 3 x 8, route 1) and read
@@ -542,24 +585,27 @@ def server_runs(args, dev) -> dict:
             times[k] += a.elapsed_time(b)
         park.current_time += 1
     ms = {k: v / args.server_steps for k, v in times.items()}
-    # end to end: the pushes' floats in from pinned host memory, the two flags of every row back
+    # end to end: the pushes' floats in from pinned host memory, the two flags of every row back, double-buffered
     f_host = torch.empty_like(g.q["f"], device="cpu").pin_memory()
     f_host.copy_(g.q["f"])
-    flags_host = [torch.empty(n, dtype=torch.bool).pin_memory() for _ in range(2)]
-    e2e = 0.0
-    for step in range(args.warmup + args.server_steps):
-        flush.fill_(1)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        g.q["f"].copy_(f_host, non_blocking=True)
+    f_slot = [torch.empty_like(g.q["f"]) for _ in range(2)]
+    flags_slot = [torch.empty(2, n, dtype=torch.bool, device=dev) for _ in range(2)]
+    flags_host = [torch.empty(2, n, dtype=torch.bool).pin_memory() for _ in range(2)]
+
+    def send(t, s):
+        f_slot[s].copy_(f_host, non_blocking=True)
+
+    def run(t, s):
+        g.q["f"].copy_(f_slot[s])
         out = g.tick()
-        flags_host[0].copy_(out.has_character, non_blocking=True)
-        flags_host[1].copy_(out.gets_bubble, non_blocking=True)
-        b.record(stream)
-        b.synchronize()
-        if step >= args.warmup:
-            e2e += a.elapsed_time(b)
-    e2e /= args.server_steps
+        flags_slot[s][0].copy_(out.has_character)
+        flags_slot[s][1].copy_(out.gets_bubble)
+
+    def fetch(t, s):
+        flags_host[s].copy_(flags_slot[s], non_blocking=True)
+
+    pipelined(dev, args.warmup, send, run, fetch)
+    e2e = pipelined(dev, args.server_steps, send, run, fetch) / args.server_steps
     srv.check()
     peak, kind = _peaks()
     achieved = SERVER_BYTES_PER_WORLD_TICK * W / (ms["pre_tick"] / 1e3) / 1e9
@@ -577,7 +623,9 @@ def server_runs(args, dev) -> dict:
                                  "launch's own CUDA-event time (eager, L2 flushed); one thread a world walking its "
                                  "queue: latency-bound"},
             "e2e": {"value": n / (e2e / 1e3), "unit": "ship-ticks/s", "ms_per_step": e2e,
-                    "h2d_bytes_per_step": g.q["f"].numel() * 8, "d2h_bytes_per_step": 2 * n},
+                    "h2d_bytes_per_step": g.q["f"].numel() * 8, "d2h_bytes_per_step": 2 * n,
+                    "pipeline": "double-buffered: step t+1's floats in and step t-1's flags out on a copy stream "
+                                "during step t's tick; timed over all steps; inputs larger than L2, no flush"},
             "gpu_launches_per_step": 3,
             "reference_published": {"value": 716e6, "unit": "ship-ticks/s", "hardware": "GH200",
                                     "config": "layer=server, mode=server_k_graph, park=modes, 65,536 worlds x 4 "
@@ -711,23 +759,29 @@ def main() -> None:
     ms_tiled, ms_plain = max_over_ranks(ms_tiled), max_over_ranks(ms_plain)
     per_tiled, per_plain = ms_tiled / args.steps, ms_plain / args.steps
 
-    # e2e through the public API from host buffers
+    # e2e through the public API from host buffers: each step's speed fractions in, each step's positions out,
+    # double-buffered over a copy stream
     every = torch.ones(n, dtype=torch.bool, device=dev)
     sf_host = torch.empty(n, dtype=torch.float64, pin_memory=True)
     sf_host.copy_(park.speed_fraction.cpu())
-    pos_host = torch.empty(n, 3, dtype=torch.float64, pin_memory=True)
-    sf_dev = torch.empty(n, dtype=torch.float64, device=dev)
+    sf_slot = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(2)]
+    pos_slot = [torch.empty(3, n, dtype=torch.float64, device=dev) for _ in range(2)]
+    pos_host = [torch.empty(3, n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
 
-    def e2e_step():
-        sf_dev.copy_(sf_host, non_blocking=True)
-        park.set_speed_fraction(every, sf_dev)
+    def send(t, s):
+        sf_slot[s].copy_(sf_host, non_blocking=True)
+
+    def run(t, s):
+        park.set_speed_fraction(every, sf_slot[s])
         graph.tick()
-        pos_host.copy_(park.pos, non_blocking=True)
+        pos_slot[s].copy_(park._pos)                                 # the positions as stored: x, y, z planes
 
-    for _ in range(3):
-        e2e_step()
+    def fetch(t, s):
+        pos_host[s].copy_(pos_slot[s], non_blocking=True)
+
+    pipelined(dev, 3, send, run, fetch)
     barrier()
-    ms_e2e = max_over_ranks(timed(e2e_step, args.steps))
+    ms_e2e = max_over_ranks(pipelined(dev, args.steps, send, run, fetch))
     h2d, d2h = n * 8, n * 24
 
     total_ships = n * world_size
@@ -758,7 +812,10 @@ def main() -> None:
                                   "tiled launch's CUDA-event time; the tick is FP64/FP32 issue- and latency-bound "
                                   "(divides, square roots, libm, divergent torque searches), not HBM-bound")},
             "e2e": {"value": total_ships * args.steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps,
+                    "pipeline": "double-buffered: step t+1's speed fractions in and step t-1's positions out on a "
+                                "copy stream during step t's tick (SetSpeedFraction, the graph's tick); timed over "
+                                "all steps; the park's state (131 MB) larger than L2, no flush"},
             "gpu_launches": 3 * args.steps, "clocks": clocks}
     if not args.no_ragged:
         line["ragged"] = ragged_runs(args, dev)
