@@ -409,6 +409,101 @@ def test_a_ball_stream_has_write_ball_to_streams_layout():
     assert len(turning) == len(blob) - struct.calcsize("<3didqq") + struct.calcsize("<4ff3ff") + 24
 
 
+class _ClockPark:
+    """A stand-in park with what the torch path reads: per-row clocks that its tick moves, flags, no motion."""
+
+    def __init__(self, worlds: int, per: int, interactive=True):
+        from exact_ballpark_b200 import server
+        self.n, self.dev, self.dt = worlds * per, torch.device("cpu"), 1.0
+        self.ids = torch.tensor([k + 1 for _ in range(worlds) for k in range(per)])
+        self.world = torch.arange(self.n) // per
+        self.clock = torch.zeros(self.n, dtype=torch.int64)
+        self.interactive = torch.full((self.n,), bool(interactive))
+        self.cloaked = torch.zeros(self.n, dtype=torch.int64)
+        self.massive = torch.zeros(self.n, dtype=torch.bool)
+        self.ticks = []
+        self.kinds = frozenset({server.CODE["SetSpeedFraction"], server.CODE["Stop"]})
+
+    def evolve(self, active=None):
+        act = torch.ones(self.n, dtype=torch.bool) if active is None else active
+        self.clock += act.to(torch.int64)
+        self.ticks.append(act.clone())
+
+
+def _clock_server(worlds: int = 4, per: int = 2, pilots=None):
+    from exact_ballpark_b200 import server
+    park = _ClockPark(worlds, per)
+    a = server.ModesAdapter.__new__(server.ModesAdapter)
+    a.park, a.R, a.dev, a.master, a.ids = park, park.n, park.dev, True, park.ids
+    a.exists = torch.ones(park.n, dtype=torch.bool)
+    a._index_worlds(park.world.tolist())
+    a.kinds = park.kinds
+    a.apply = lambda kind, m, trow, f, n: None
+    a.stream_fields = lambda: {"ids": park.ids.clone()}
+    return server.VecServer(a, pilots if pilots is not None else list(range(park.n))), park
+
+
+def test_on_tick_runs_each_worlds_whole_intervals_and_carries_the_rest():
+    """OnTick's arithmetic (Ballpark.cpp:219-330): too early, a first call (one evolve, no pre-tick), whole
+    intervals under a mask, the remainder carried, the master's backlog of more than five intervals cut to one."""
+    s, park = _clock_server()
+    I = 10_000_000                                          # a 1 s interval in 100 ns units
+    assert s.on_tick(torch.tensor([0, I - 1, I, 3 * I + 7])) == []      # first calls evolve once: worlds 2 and 3
+    assert s.tick_counts == {"worlds too early": 2, "first calls": 2, "resynchronisations": 0, "intervals run": 0,
+                             "remainders carried": 0}
+    assert park.ticks[-1].tolist() == [False, False, False, False, True, True, True, True]
+    assert s.time.tolist() == [0, 0, I, 3 * I + 7] and s.first_time.tolist() == [True, True, False, False]
+    batches = s.on_tick(torch.tensor([I, I - 1, 3 * I + 5, 5 * I + 6]))   # world 0's first call; 2 runs 2, 3 runs 1
+    assert [b.ticked.tolist() for b in batches] == [[False, False, True, True], [False, False, True, False]]
+    assert s.time.tolist() == [I, 0, 3 * I, 4 * I + 7]                   # world 3 carries 2 I - 1
+    assert s.tick_counts["remainders carried"] == 2
+    assert park.clock.tolist() == [1, 1, 0, 0, 3, 3, 2, 2]
+    batches = s.on_tick(torch.tensor([2 * I, I, 3 * I, 14 * I + 8]))      # world 3: ten intervals behind: one
+    assert s.tick_counts["resynchronisations"] == 1
+    assert s.time.tolist() == [2 * I, I, 3 * I, 14 * I + 8]
+    assert [b.ticked.tolist() for b in batches] == [[True, False, False, True]]
+
+
+def test_a_masked_tick_keeps_the_queue_and_the_stamp_of_a_world_without_a_tick():
+    s, park = _clock_server(worlds=2, per=2)
+    both = torch.tensor([True, True])
+    s.push("SetSpeedFraction", both, torch.tensor([1, 2]), f=torch.tensor([[0.5], [0.5]]))
+    on = torch.tensor([True, False])
+    s.pre_tick(mask=on)
+    s.evolve(mask=on)
+    s.post_tick(mask=on)
+    assert s.batch.slots[0].ok.tolist() == [True, False] and s.batch.ticked.tolist() == [True, False]
+    assert [q.ok.tolist() for q in s.slots] == [[False, True]]           # world 1's call kept
+    assert s.stamp_for_system.tolist() == [1, 0]
+    assert s.batch.has_character.tolist()[2:] == [False, False]          # a world without a tick sends nothing
+    s.push("SetSpeedFraction", both, torch.tensor([1, 2]), f=torch.tensor([[0.5], [0.5]]))
+    assert s.slots[-1].ok.tolist() == [True, False]                      # world 1: the same call is still its last
+    s.pre_tick()
+    assert [q.ok.tolist() for q in s.batch.slots] == [[False, True], [True, False]]
+
+
+def test_decode_sends_each_pilot_its_updates_in_destinys_order():
+    """One world, two piloted balls: a call routed to the bubble goes to both pilots' narrowcast; the first pre-tick's
+    additions (none listed without a cloak change here: the fields stand in) are a PackagedAction in the singlecast."""
+    from exact_ballpark_b200 import server
+    s, park = _clock_server(worlds=1, per=2, pilots=[0, 1])
+    s.push("SetSpeedFraction", torch.tensor([True]), torch.tensor([2]), f=torch.tensor([[0.25]]))
+    s.pre_tick(snapshot=False)
+    s.evolve()
+    s.post_tick()
+    b = s.batch
+    assert b.route.tolist() == [[server.BUBBLE]]
+    assert b.gets_bubble.tolist() == [True, True] and b.has_character.tolist() == [True, True]
+    with pytest.raises(ValueError):                       # the additions' streams were not recorded
+        server.decode(s)
+    b.additions = (torch.zeros(2, dtype=torch.bool), b.additions[1], None)
+    b.has_character = torch.zeros(2, dtype=torch.bool)
+    sent = server.decode(s)
+    event = (0, ("SetSpeedFraction", (2, 0.25)))
+    assert sent == [{10000: [("narrow", "DoDestinyUpdate", [event], False, server.ClientUpdateCountThisTick.ONE)],
+                     10001: [("narrow", "DoDestinyUpdate", [event], False, server.ClientUpdateCountThisTick.ONE)]}]
+
+
 def test_the_kernel_path_wants_a_cuda_device_and_a_known_path():
     from exact_ballpark_b200 import server
     with pytest.raises(ValueError):
