@@ -30,7 +30,8 @@ OnTick's per-world intervals (`on_tick`, the masks of `pre_tick`, `evolve` and `
 `decode` turns a batch into what Destiny's network sends each client: its singlecast and the bubble's narrowcast, with
 the events, the AddBallsToPark streams in WriteBallToStream's layout and the packaged additions.
 
-`CollideAdapter` puts the layer over the collision park (torch path).
+`CollideAdapter` puts the layer over the collision park (torch path). `ClientView` keeps what each pilot's client
+holds, `down` ticks behind the server.
 
 Not built: the orientation and combat parks' adapters, bubbles other than one a world.
 """
@@ -983,6 +984,56 @@ class ServerGraph:
         self.server.a.park.current_time += 1
         self.server.batch = self.out
         return self.out
+
+
+# ================================================================================ what each client holds
+
+class ClientView:
+    """What each pilot's client holds after each tick (vec_server.py:1292-1340): the server's state `down` ticks back (a
+    client applies each update at its stamp, so its park settles `down` ticks behind the server's), kept as a ring of
+    the last `down` + 1 recorded states of the observed fields; another pilot's cloaked ship is absent from a client's
+    park (its CloakBall removed it there), the client's own ship is present, and a client's park holds its own world
+    only. `record(time)` after each server tick; `view()` the state each client holds and its park time."""
+
+    def __init__(self, server: VecServer, down: int, fields: tuple = ("pos", "vel", "mode")):
+        if down < 0:
+            raise ValueError("down: whole ticks, at least 0")
+        self.server, self.down, self.fields = server, int(down), tuple(fields)
+        self.depth = self.down + 1
+        self.ring: dict = {}
+        self.times = torch.full((self.depth,), -1, dtype=I64)
+        self.k = 0
+
+    def _field(self, name: str) -> torch.Tensor:
+        a = self.server.a
+        if name == "cloaked":
+            return a.cloaked
+        t = getattr(a.park, name)
+        return t.reshape(a.R, *t.shape[2:]) if isinstance(a, CollideAdapter) else t
+
+    def record(self, time: int) -> None:
+        """Keep the server's state at park time `time` (the time the park has reached)."""
+        slot = self.k % self.depth
+        for name in self.fields + ("cloaked",):
+            t = self._field(name)
+            if name not in self.ring:
+                self.ring[name] = torch.zeros((self.depth, *t.shape), dtype=t.dtype, device=t.device)
+            self.ring[name][slot].copy_(t)
+        self.times[slot] = int(time)
+        self.k += 1
+
+    def view(self) -> tuple:
+        """(time, {field: [R, ...]}, present [R, R]: row r is in the park of the pilot whose ship is row c), the state
+        `down` ticks before the latest recorded one; time -1 (and nothing) until that state was recorded."""
+        if self.k <= self.down:
+            return -1, {}, None
+        slot = (self.k - 1 - self.down) % self.depth
+        out = {name: self.ring[name][slot] for name in self.fields}
+        cloaked = self.ring["cloaked"][slot]
+        a = self.server.a
+        own_world = a.world[:, None] == a.world[None, :]
+        mine = torch.eye(a.R, dtype=BOOL, device=cloaked.device)
+        return int(self.times[slot]), out, own_world & ((cloaked == 0)[:, None] | mine)
 
 
 # ================================================================================ the batches as Destiny sends them

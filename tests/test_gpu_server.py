@@ -504,6 +504,31 @@ def test_decode_sends_each_pilot_its_updates_in_destinys_order():
                      10001: [("narrow", "DoDestinyUpdate", [event], False, server.ClientUpdateCountThisTick.ONE)]}]
 
 
+def test_a_client_view_lags_down_ticks_and_hides_the_other_pilots_cloaked_ships():
+    from exact_ballpark_b200 import server
+    s, park = _clock_server(worlds=2, per=2)
+    park.pos = torch.zeros(4, 3, dtype=torch.float64)
+    view = server.ClientView(s, down=2, fields=("pos", "clock"))
+    with pytest.raises(ValueError):
+        server.ClientView(s, down=-1)
+    for t in range(1, 6):
+        park.pos[:, 0] = float(t)
+        park.cloaked.copy_(torch.tensor([0, 1, 0, 0]) if t >= 3 else torch.zeros(4, dtype=torch.int64))
+        s.evolve()
+        view.record(t)
+        time, fields, present = view.view()
+        if t <= 2:
+            assert time == -1 and fields == {} and present is None
+            continue
+        assert time == t - 2
+        assert fields["pos"][:, 0].tolist() == [float(t - 2)] * 4
+        assert fields["clock"].tolist() == [t - 2] * 4
+        hidden = t - 2 >= 3                                   # row 1 cloaked in the state the clients hold
+        assert present[1].tolist() == [not hidden, True, False, False]      # its own pilot still holds it
+        assert present[0].tolist() == [True, True, False, False]
+        assert present[2].tolist() == [False, False, True, True]
+
+
 def test_the_kernel_path_wants_a_cuda_device_and_a_known_path():
     from exact_ballpark_b200 import server
     with pytest.raises(ValueError):
