@@ -232,9 +232,10 @@ class ModesAdapter(_Worlds):
         self.park.evolve(active=None if worlds is None else worlds[self.world])
 
     def stream_fields(self) -> dict:
-        """The fields WriteBallToStream writes (Thunkers.cpp:3180-3377), every row, on the host."""
+        """The fields WriteBallToStream writes (Thunkers.cpp:3180-3377), every row, copied to the host (a snapshot: later
+        writes to the park do not reach it)."""
         p = self.park
-        out = {k: getattr(p, k).detach().cpu() for k in ("ids", "mode", "radius", "pos", "free", "massive",
+        out = {k: getattr(p, k).detach().to("cpu", copy=True) for k in ("ids", "mode", "radius", "pos", "free", "massive",
                                                           "interactive", "mass", "cloaked", "max_vel", "vel",
                                                           "agility", "speed_fraction", "goto", "follow_id",
                                                           "follow_range", "effect_stamp", "last_collision",
@@ -339,12 +340,13 @@ class CollideAdapter(_Worlds):
 
     def stream_fields(self) -> dict:
         p, R = self.park, self.R
-        flat = lambda t: t.detach().reshape(R, *t.shape[2:]).cpu()           # noqa: E731
+        host = lambda t: t.detach().to("cpu", copy=True)                     # noqa: E731  (a snapshot)
         zero = torch.zeros(R, dtype=I64)
-        out = {k: flat(getattr(p, k)) for k in ("mode", "radius", "pos", "free", "mass", "max_vel", "vel", "agility",
-                                                 "speed_fraction", "goto", "last_collision")}
-        out.update(ids=self.ids.cpu(), massive=self.massive.cpu(), interactive=self.interactive.cpu(),
-                   cloaked=self.cloaked.cpu(), follow_id=zero, owner_id=zero, effect_stamp=zero,
+        out = {k: host(getattr(p, k).reshape(R, *getattr(p, k).shape[2:]))
+               for k in ("mode", "radius", "pos", "free", "mass", "max_vel", "vel", "agility", "speed_fraction", "goto",
+                         "last_collision")}
+        out.update(ids=host(self.ids), massive=host(self.massive), interactive=host(self.interactive),
+                   cloaked=host(self.cloaked), follow_id=zero, owner_id=zero, effect_stamp=zero,
                    follow_range=torch.zeros(R, dtype=F64), dynamical=False)
         return out
 
