@@ -511,6 +511,73 @@ SERVER_BYTES_PER_WORLD_TICK = 8 * (1 + 32 + 32 + 26 + 34) + 40 + 16 + 64 + 4 * (
 # (the dead-bubble test fused into the same launch reads interactive and exists again: L1 hits, not counted)
 
 
+def server_worlds(W: int, seed: int = 7) -> list:
+    """The server benchmark's worlds (benchmarks/server_speed.py's shape): W worlds of 4 ships near a centre, every ship
+    interactive and piloted, at rest, speed fraction 1, seeded."""
+    import random
+    r = random.Random(seed)
+    rows = []
+    for i in range(W * 4):
+        if i % 4 == 0:
+            centre = [r.uniform(-1e5, 1e5) for _ in range(3)]
+        rows.append({"id": i % 4 + 1, "world": i // 4, "time": 0, "mass": 10 ** r.uniform(6.0, 8.0),
+                     "radius": r.uniform(20.0, 80.0), "max_vel": r.uniform(100.0, 400.0),
+                     "pos": [c + r.uniform(-4e3, 4e3) for c in centre], "vel": [0.0, 0.0, 0.0],
+                     "agility": r.uniform(0.3, 1.5), "speed_fraction": 1.0, "free": True, "massive": False,
+                     "interactive": True, "cloaked": 0, "bubble": 0, "moribund": False})
+    return rows
+
+
+def server_pushes(W: int, dev) -> list:
+    """Per ship k of a world: (kind, mask, ball id, floats) for GotoDirection and SetSpeedFraction, drawn once."""
+    import torch
+    gen = torch.Generator().manual_seed(11)
+    out = []
+    for k in range(4):
+        d = torch.rand(W, 3, generator=gen, dtype=torch.float64) * 2 - 1
+        sf = torch.rand(W, generator=gen, dtype=torch.float64)[:, None]
+        mask = torch.ones(W, dtype=torch.bool, device=dev)
+        ball = torch.full((W,), k + 1, dtype=torch.int64, device=dev)
+        out += [("GotoDirection", mask, ball, d.to(dev)), ("SetSpeedFraction", mask, ball, sf.to(dev))]
+    return out
+
+
+def server_cpu_sample(worlds: int, warmup: int, steps: int) -> dict:
+    """The server layer's algorithm on the host (its torch path, the reference's organisation, over the C++ oracle's
+    flight park: oracle/server_view.py) on `worlds` worlds of the benchmark's shape: the 8 pushes, the pre-tick, the
+    park's tick and the send flags each tick; ship-ticks/s."""
+    import torch
+
+    from exact_ballpark_b200 import server
+    from oracle.park import OraclePark
+    from oracle.server_view import OracleParkView
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    torch.set_num_threads(threads)
+    rows = server_worlds(worlds)
+    park = OracleParkView(OraclePark(len(rows)), threads=threads)
+    park.load(rows)
+    srv = server.VecServer(server.ModesAdapter(park), [x["id"] - 1 for x in rows])
+    pushes = server_pushes(worlds, "cpu")
+
+    def tick():
+        for kind, mask, ball, f in pushes:
+            srv.push(kind, mask, ball, f=f)
+        srv.pre_tick(snapshot=False)
+        srv.evolve()
+        srv.post_tick()
+    srv.tick()
+    for _ in range(warmup):
+        tick()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        tick()
+    dt = time.perf_counter() - t0
+    return {"value": len(rows) * steps / dt, "unit": "ship-ticks/s", "cores": threads, "kind": "port",
+            "sample": f"{worlds} worlds x 4 piloted ships, 8 calls a world a tick, ticks {warmup + 2}..{warmup + steps + 1} "
+                      f"({dt:.1f} s wall): the server layer's torch path on the host ({threads} torch threads) over the "
+                      f"C++ oracle's flight park (its tick on {threads} threads over disjoint worlds)"}
+
+
 def server_runs(args, dev) -> dict:
     """The server layer (exact_ballpark_b200.server) over the flight park at the reference's server benchmark shape
     (benchmarks/server_speed.py): --server-worlds worlds of 4 ships, each flown by a pilot that sends GotoDirection
@@ -520,23 +587,12 @@ def server_runs(args, dev) -> dict:
     events (L2 flushed before each). Then the same three launches eagerly, each timed alone (the shares and the server
     kernel's roofline), and the end-to-end tick: the pushes' floats copied in from pinned host memory, the replay, the
     two send flags of every row copied back."""
-    import random
-
     import torch
 
     from exact_ballpark_b200 import VecModesPark, server
     from exact_ballpark_b200.modes import tick as park_tick
     K, W = 4, args.server_worlds
-    r = random.Random(7)
-    rows = []
-    for i in range(W * K):
-        if i % K == 0:
-            centre = [r.uniform(-1e5, 1e5) for _ in range(3)]
-        rows.append({"id": i % K + 1, "world": i // K, "time": 0, "mass": 10 ** r.uniform(6.0, 8.0),
-                     "radius": r.uniform(20.0, 80.0), "max_vel": r.uniform(100.0, 400.0),
-                     "pos": [c + r.uniform(-4e3, 4e3) for c in centre], "vel": [0.0, 0.0, 0.0],
-                     "agility": r.uniform(0.3, 1.5), "speed_fraction": 1.0, "free": True, "massive": False,
-                     "interactive": True, "cloaked": 0, "bubble": 0, "moribund": False})
+    rows = server_worlds(W)
     n = len(rows)
     park = VecModesPark(n, device=dev)
     park.load(rows)
@@ -546,14 +602,10 @@ def server_runs(args, dev) -> dict:
     srv.post_tick()
     sched = [k for _ in range(K) for k in ("GotoDirection", "SetSpeedFraction")]
     g = server.ServerGraph(srv, sched)
-    gen = torch.Generator().manual_seed(11)
-    for k in range(K):
-        d, sf = torch.rand(W, 3, generator=gen, dtype=torch.float64) * 2 - 1, torch.rand(W, generator=gen,
-                                                                                         dtype=torch.float64)
-        for j, f in ((2 * k, d), (2 * k + 1, sf[:, None])):
-            g.inputs[j]["mask"].fill_(True)
-            g.inputs[j]["ball"].fill_(k + 1)
-            g.inputs[j]["f"][:, :f.shape[1]].copy_(f.to(dev))
+    for j, (kind, mask, ball, f) in enumerate(server_pushes(W, dev)):
+        g.inputs[j]["mask"].copy_(mask)
+        g.inputs[j]["ball"].copy_(ball)
+        g.inputs[j]["f"][:, :f.shape[1]].copy_(f)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
     for _ in range(args.warmup):
@@ -629,7 +681,8 @@ def server_runs(args, dev) -> dict:
             "gpu_launches_per_step": 3,
             "reference_published": {"value": 716e6, "unit": "ship-ticks/s", "hardware": "GH200",
                                     "config": "layer=server, mode=server_k_graph, park=modes, 65,536 worlds x 4 "
-                                              "(docs/benchmarks.md)"}}
+                                              "(docs/benchmarks.md)"},
+            **({} if args.no_cpu_baseline else {"cpu_baseline": server_cpu_sample(16384, 3, 100)})}
 
 
 def _config(args, schedule: str) -> dict:

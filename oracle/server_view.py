@@ -21,8 +21,9 @@ from .park import ORBIT
 class OracleParkView:
     """An OraclePark whose arrays read as CPU tensors (module docstring)."""
 
-    def __init__(self, park):
+    def __init__(self, park, threads: int = 1):
         object.__setattr__(self, "_park", park)
+        object.__setattr__(self, "_threads", int(threads))
 
     def __getattr__(self, name):
         v = getattr(self._park, name)
@@ -50,12 +51,12 @@ class OracleParkView:
     def evolve(self, lib=None, active=None) -> None:
         p = self._park
         if active is None:
-            p.evolve()
+            p.evolve(threads=self._threads)
             return
         act = np.asarray(active.cpu() if torch.is_tensor(active) else active, dtype=bool).reshape(p.n)
         names = [k for k, v in vars(p).items() if isinstance(v, np.ndarray) and v.shape[:1] == (p.n,)]
         before = {k: getattr(p, k).copy() for k in names}
-        p.evolve()
+        p.evolve(threads=self._threads)
         for k, old in before.items():
             cur = getattr(p, k)
             sel = act.reshape((p.n,) + (1,) * (cur.ndim - 1))
