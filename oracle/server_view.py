@@ -6,8 +6,9 @@ reference's server goldens check the layer's logic without a GPU. Only tests/ us
 
 Two things the oracle's flight park does not carry are stated here from the reference park's API: StopAllFollowers of a set of
 rows (`_release_followers`, vec_modes.py:388: a member's Stop, an interactive orbiter sent along its velocity) and
-OnTick's per-world mask on the tick (`evolve(active=...)`: every row ticked, then the rows outside the mask given back
-their state, as the reference's masked tick does, vec_orient.py:217).
+OnTick's per-world mask on the flight park's tick (`evolve(active=...)`: every row ticked, then the rows outside the
+mask given back their state, as the reference's masked tick does, vec_orient.py:217; the collision oracle masks its
+worlds itself).
 """
 
 from __future__ import annotations
@@ -52,6 +53,10 @@ class OracleParkView:
         p = self._park
         if active is None:
             p.evolve(threads=self._threads)
+            return
+        if hasattr(p, "W"):                                 # the collision oracle masks its worlds itself
+            p.evolve(active=np.asarray(active.cpu() if torch.is_tensor(active) else active, dtype=bool),
+                     threads=self._threads)
             return
         act = np.asarray(active.cpu() if torch.is_tensor(active) else active, dtype=bool).reshape(p.n)
         names = [k for k, v in vars(p).items() if isinstance(v, np.ndarray) and v.shape[:1] == (p.n,)]

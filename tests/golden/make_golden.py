@@ -566,10 +566,40 @@ def make_server_ontick() -> None:
     print(f"  server_ontick: {len(runs)} runs, {time.time() - t0:.0f} s", flush=True)
 
 
+def make_server_collide_more() -> None:
+    """server_collide_ontick: the reference's OnTick scenarios over the collision park (tests/server_ontick_cases.py's
+    server_cases with park "collide", seed 1: 32 worlds, 14 calls), recorded on the reference's VecServer over its
+    CollideAdapter (torch path, its VecCollidePark on the CPU) by server_trace's driver, after the set is first run by
+    the reference's own comparison against its scalar server layer under OnTick: 0 differences. (Its pending queries
+    do not run over the collision park: the reference reads the park's [W, N] speed fraction by row.)"""
+    import server_ontick_cases as O
+    import server_trace as st
+    import exact_ballpark.vec_server as VS
+    from exact_ballpark.vec_collide import VecCollidePark
+    t0 = time.time()
+    seed = 1
+    res = O.run(O.server_cases(seed, 32, "collide", False, 14), "collide", "cpu")
+    if res["sends"] or res["rows"] or res["clocks"]:
+        raise RuntimeError("the reference's collision server layer differs from its scalar one (OnTick)")
+    cs = O.server_cases(seed, 32, "collide", False, 14)
+    parks, calls, sends = [], [], []
+
+    def on_call(tk, server, batches):
+        parks.append(st.park_digests("collide", server.a.park))
+        calls.append(st.ontick_digests(server, batches))
+        sends.append(st.decode_digest([VS.decode(server, b) for b in batches]))
+    server, _ = st.build(VS, VecCollidePark, cs, False, "cpu", park="collide")
+    st.drive_ontick(server, cs, "cpu", on_call)
+    st.save(HERE / "server_collide_ontick", [{"cases": cs, "do": False, "evolve": True, "ontick": True,
+                                              "park_kind": "collide", "park": np.array(parks, dtype=np.uint64),
+                                              "batch": calls, "decode": sends}])
+    print(f"  server_collide_ontick: {res['coverage']}, {time.time() - t0:.0f} s", flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending", "server_ontick",
-                                       "server_collide"),
+                                       "server_collide", "server_collide_more"),
                     default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
     a = ap.parse_args()
@@ -595,6 +625,8 @@ def main() -> None:
         make_server_ontick()
     if a.only in (None, "server_collide"):
         make_server_collide()
+    if a.only in (None, "server_collide_more"):
+        make_server_collide_more()
 
 
 if __name__ == "__main__":

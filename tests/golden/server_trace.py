@@ -366,8 +366,8 @@ def replay(server_mod, park_cls, run: dict, device, kernel: str | None = None) -
     if run.get("ontick"):
         def on_call(t, s, batches):
             sends(t, [server_mod.decode(s, b) for b in batches])
-            got = tr.field_digests(s.a.park)
-            mm = [PARK_FIELDS[k] for k in range(len(PARK_FIELDS)) if got[k] != run["park"][t][k]]
+            got = park_digests(kind, s.a.park)
+            mm = [names[k] for k in range(len(names)) if got[k] != run["park"][t][k]]
             if mm:
                 bad.append((t, "park", mm))
             d = ontick_digests(s, batches)

@@ -67,12 +67,14 @@ def test_on_tick_replays_the_golden_calls(run, kernel):
 
 @pytest.mark.gpu
 @pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")
-@pytest.mark.parametrize("run", [0, 1], ids=["development", "held_out"])
-def test_the_server_layer_over_the_collision_park_replays_the_golden_ticks(run):
+@pytest.mark.parametrize("name,run", [("server_collide", 0), ("server_collide", 1), ("server_collide_ontick", 0)],
+                         ids=["development", "held_out", "on_tick"])
+def test_the_server_layer_over_the_collision_park_replays_the_golden_ticks(name, run):
     """The reference's server scenarios over the collision park (massive balls within 3 km that meet, cloaks,
-    SetBallMassive, SetBallInteractive): the park's every field, the batch and every client's sends, every tick."""
+    SetBallMassive, SetBallInteractive) and its OnTick scenarios there: the park's every field, the batch and every
+    client's sends, every tick or call."""
     from exact_ballpark_b200 import VecCollidePark, server
-    r = _golden("server_collide")[run]
+    r = _golden(name)[run]
     bad = st.replay(server, VecCollidePark, r, "cuda")
     assert not bad, f"{len(bad)} differences, first {bad[:3]}"
 
@@ -212,7 +214,8 @@ def test_a_server_graph_replays_eager_kernel_ticks():
 
 
 def test_every_server_golden_carries_the_clients_sends():
-    for name in ("server_modes", "server_modes_do", "server_pending", "server_ontick", "server_collide"):
+    for name in ("server_modes", "server_modes_do", "server_pending", "server_ontick", "server_collide",
+                 "server_collide_ontick"):
         for r in _golden(name):
             assert r["decoded"] and len(r["decode"]) == len(r["park"])
     kinds = {c[0] for r in _golden("server_collide") for w in r["cases"] for t in w["ticks"] for c in t}

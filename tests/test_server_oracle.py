@@ -33,9 +33,9 @@ def _oracle_collide_park(worlds, slots, friction=1.0e6, tick_interval_ms=1000, d
     return OracleParkView(OracleCollidePark(worlds, slots, friction=friction, tick_interval_ms=tick_interval_ms))
 
 
-@pytest.mark.parametrize("run", [0, 1])
-def test_the_collision_parks_layer_over_the_oracle_replays_the_golden_ticks(run):
+@pytest.mark.parametrize("name,run", [("server_collide", 0), ("server_collide", 1), ("server_collide_ontick", 0)])
+def test_the_collision_parks_layer_over_the_oracle_replays_the_golden_ticks(name, run):
     from exact_ballpark_b200 import server
-    r = st.load(st.GOLDEN / "server_collide")[run]
+    r = st.load(st.GOLDEN / name)[run]
     bad = st.replay(server, _oracle_collide_park, r, "cpu")
     assert not bad, f"{len(bad)} differences, first {bad[:3]}"
