@@ -756,6 +756,8 @@ def main() -> None:
         print(json.dumps({"metric": METRIC, "section": args.only, args.only: run()}), flush=True)
         return
     dist = None
+    if rank != 0 or world_size > 1:                                   # the sections' CPU baselines: rank 0 at N = 1
+        args.no_cpu_baseline = True
     if world_size > 1:
         import datetime
 
