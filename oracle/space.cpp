@@ -1,0 +1,573 @@
+// TEST INFRASTRUCTURE, NOT THE PRODUCT. The master's partition and bubble partition of one world, restated as a plain
+// sequential C++ program from the reference's scalar transcription (exact_ballpark/space.py: Partition's GetBox,
+// CheckBox and the BoxAllocator, space.py:596-676; Ball::InsertInBoxes and DeleteFromBoxes, :683-818; NearbyBubbles,
+// Traverse, AddToBubble, InitializeBubbles, CopyBubbles, InDeadBubble, :896-1056; AddBall, the re-filing setters and
+// RemoveBall, :1097-1319). A world is driven by a list of operations and its state is printed after each one, as a text
+// the tests compare with the reference's own state on the same operations (tests/golden/space_trace.py).
+//
+// Boxes are made on demand with their parents and released when empty; a released box's memory is kept (up to 256
+// boxes, BoxAllocator's free list) or deleted, and Destiny reads a released box in one path (a ball that was its
+// box's only occupant): every box ever made is kept here, so that read sees the stale values, and a read of a deleted
+// box sets `undefined` (Destiny's result is undefined there). Balls, bubbles and the bubble dictionaries keep the
+// reference's insertion orders. Sensors, collisions, queries, modes and the tick are not in this slice.
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <set>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace space_oracle {
+
+constexpr int NUM_LEVELS = 8;
+constexpr double GRID_UNIT = 480.0;
+constexpr int BOX_KEEP = 256;                              // BoxAllocator's kept boxes
+
+double level_width(int i) { return double(int64_t(1) << (2 * NUM_LEVELS)) * GRID_UNIT * 0.25 / double(int64_t(1) << (2 * i)); }
+int64_t level_grid(int i) { return int64_t(1) << (2 * i - 2 * NUM_LEVELS + 39); }
+
+using Key = std::array<int64_t, 3>;
+
+int64_t to_int64(double x) {                               // int64_t(x) as aarch64 converts: NaN 0, saturating
+    if (x != x) return 0;
+    if (x >= 9223372036854775808.0) return INT64_MAX;
+    if (x < -9223372036854775808.0) return INT64_MIN;
+    return (int64_t)x;
+}
+
+Key clamp(int64_t ix, int64_t iy, int64_t iz, int64_t n) {
+    auto c = [n](int64_t i) { return i < 0 ? int64_t(0) : (i >= n ? n - 1 : i); };
+    return Key{c(ix), c(iy), c(iz)};
+}
+
+// an insertion-ordered map (the reference's dicts)
+template <class V>
+struct Ordered {
+    std::vector<std::pair<int64_t, V>> items;
+    V* find(int64_t k) {
+        for (auto& kv : items)
+            if (kv.first == k) return &kv.second;
+        return nullptr;
+    }
+    V& add(int64_t k, V v) {
+        items.emplace_back(k, std::move(v));
+        return items.back().second;
+    }
+    void erase(int64_t k) {
+        for (size_t i = 0; i < items.size(); ++i)
+            if (items[i].first == k) {
+                items.erase(items.begin() + i);
+                return;
+            }
+    }
+};
+
+struct Ball;
+
+struct Box {
+    int level;
+    Key key;
+    double lo[3], hi[3];
+    Box* parent = nullptr;
+    std::map<Key, Box*> children;
+    std::map<int64_t, Ball*> balls;
+    int64_t bubble = -1;
+    bool released = false, deleted = false;
+};
+
+struct Ball {
+    int64_t id;
+    double mass = 0.0, radius = 0.0, max_vel = 0.0, agility = 1.0, speed_fraction = 1.0, time_factor = 1.0;
+    double pos[3] = {1e10, 1e10, 1e10}, vel[3] = {0.0, 0.0, 0.0};
+    bool free = false, interactive = false;
+    int64_t bubble = -1, old_bubble = -1;
+    std::map<Key, Box*> boxes;
+    Box* my_box = nullptr;
+    int mod[3] = {-2, -2, -2};
+    bool active[27] = {};
+};
+
+float f32(double x) { return (float)x; }
+
+struct World {
+    double friction, dt;
+    std::map<Key, Box*> levels[NUM_LEVELS];                // the live boxes
+    std::vector<std::unique_ptr<Box>> made;                // every box ever made (stale reads)
+    int free_boxes = 0;
+    Ordered<std::unique_ptr<Ball>> balls;                  // mBalls, in the order of their first filing
+    Ordered<Ordered<int>> bubbles;                         // bubble -> {ball: +1, 0, -1}
+    std::map<int64_t, std::set<int64_t>> interactives, keep_alives;
+    std::set<int64_t> keep_alive_balls;
+    int64_t bubble_id = 0;
+    bool undefined = false;
+
+    Ball* ball(int64_t id) {
+        auto* p = balls.find(id);
+        return p ? p->get() : nullptr;
+    }
+
+    // ---- the partition ----
+    Box* get_box(int64_t ix, int64_t iy, int64_t iz, int level) {
+        if (level < 0 || level >= NUM_LEVELS) return nullptr;
+        const Key k = clamp(ix, iy, iz, level_grid(level));
+        auto it = levels[level].find(k);
+        if (it != levels[level].end()) return it->second;
+        if (free_boxes > 0) --free_boxes;
+        made.emplace_back(new Box());
+        Box* b = made.back().get();
+        b->level = level;
+        b->key = k;
+        const double w = level_width(level), n = (double)level_grid(level), center = w * n * 0.5;
+        for (int i = 0; i < 3; ++i) {
+            b->lo[i] = (double)k[i] * w - center;
+            b->hi[i] = (double)(k[i] + 1) * w - center;
+        }
+        if (level != 0) {
+            b->parent = get_box(k[0] >> 2, k[1] >> 2, k[2] >> 2, level - 1);
+            b->parent->children[k] = b;
+        }
+        levels[level][k] = b;
+        return b;
+    }
+    Box* check_box(int64_t ix, int64_t iy, int64_t iz, int level) {
+        if (level < 0 || level >= NUM_LEVELS) return nullptr;
+        auto it = levels[level].find(clamp(ix, iy, iz, level_grid(level)));
+        return it == levels[level].end() ? nullptr : it->second;
+    }
+    static int level_for(double radius) {
+        int level = 0;
+        for (int i = 0; i < NUM_LEVELS; ++i) {
+            if (3.0 * radius > level_width(i)) break;
+            level = i;
+        }
+        return level;
+    }
+    static Key key_for(int level, const double* pos) {
+        const double w = level_width(level), fac = 1.0 / w, half = 0.5 * w * (double)level_grid(level);
+        return Key{to_int64((pos[0] + half) * fac), to_int64((pos[1] + half) * fac), to_int64((pos[2] + half) * fac)};
+    }
+    Box* get_box_r(double radius, const double* pos) {
+        const int level = level_for(radius);
+        const Key k = key_for(level, pos);
+        return get_box(k[0], k[1], k[2], level);
+    }
+    static Box* topmost(Box* b) {
+        while (b && b->parent) b = b->parent;
+        return b;
+    }
+    void release(Box* box) {
+        const bool keep = free_boxes < BOX_KEEP;
+        if (box->parent) {
+            Box* p = box->parent;
+            p->children.erase(box->key);
+            if (p->children.empty() && p->balls.empty()) release(p);
+        }
+        levels[box->level].erase(box->key);
+        box->released = true;
+        if (keep)
+            ++free_boxes;
+        else
+            box->deleted = true;
+    }
+    Box* stale(Box* b) {
+        if (b->deleted) undefined = true;
+        return b;
+    }
+    void box_remove_ball(Box* box, Ball* b) {
+        box->balls.erase(b->id);
+        if (box->children.empty() && box->balls.empty()) release(box);
+    }
+    static void clear_boxes(Ball* b) {
+        b->boxes.clear();
+        b->my_box = nullptr;
+        std::fill(b->active, b->active + 27, false);
+        b->mod[0] = b->mod[1] = b->mod[2] = -2;
+    }
+    void delete_from_boxes(Ball* b) {
+        std::vector<Box*> order;
+        for (auto& kv : b->boxes) order.push_back(kv.second);    // in key order
+        for (Box* box : order) box_remove_ball(box, b);
+        clear_boxes(b);
+    }
+    static void insert_in_box(Ball* b, Box* box) {
+        if (!box) return;
+        box->balls[b->id] = b;
+        b->boxes[box->key] = box;
+    }
+    double inflated_radius(const Ball* b) const {         // a free ball's radius plus a tick at full thrust
+        if (!b->free) return b->radius;
+        const double m = b->mass * b->agility;
+        const double a = friction * b->speed_fraction * b->max_vel / m;
+        const double v = std::sqrt(b->vel[0] * b->vel[0] + b->vel[1] * b->vel[1] + b->vel[2] * b->vel[2]);
+        const double k = friction;
+        const double max_speed = (m * a - (m * a - v * k) * b->time_factor) / k;
+        return b->radius + dt * max_speed;
+    }
+
+    // ---- bubbles ----
+    int64_t nearby_bubbles(Box* box) {
+        for (int i = -1; i <= 1; ++i)
+            for (int j = -1; j <= 1; ++j)
+                for (int k = -1; k <= 1; ++k) {
+                    if (i == 0 && j == 0 && k == 0) continue;
+                    Box* o = check_box(box->key[0] + i, box->key[1] + j, box->key[2] + k, box->level);
+                    if (o && o->bubble != -1) return o->bubble;
+                }
+        return -1;
+    }
+    void traverse(Box* box, int64_t seed) {
+        if (box->bubble != -1) return;
+        box->bubble = seed;
+        for (int i = -1; i <= 1; ++i)
+            for (int j = -1; j <= 1; ++j)
+                for (int k = -1; k <= 1; ++k) {
+                    if (i == 0 && j == 0 && k == 0) continue;
+                    Box* o = check_box(box->key[0] + i, box->key[1] + j, box->key[2] + k, box->level);
+                    if (o) traverse(o, seed);
+                }
+    }
+    void add_to_bubble(Ball* b) {
+        if (b->bubble != -1) {
+            Ordered<int>* nb = bubbles.find(b->bubble);
+            if (!nb) nb = &bubbles.add(b->bubble, Ordered<int>());
+            int* v = nb->find(b->id);
+            if (!v)
+                nb->add(b->id, 1);
+            else if (*v == -1)
+                *v = 0;
+        }
+        if (b->old_bubble != -1) {
+            Ordered<int>* ob = bubbles.find(b->old_bubble);
+            if (ob) {
+                int* v = ob->find(b->id);
+                if (v) {
+                    if (*v == 0)
+                        *v = -1;
+                    else if (*v == 1)
+                        ob->erase(b->id);
+                }
+            }
+        }
+        if (b->interactive) {
+            increase_interactive(b, b->bubble);
+            decrease_interactive(b, b->old_bubble);
+        }
+        if (keep_alive_balls.count(b->id)) {
+            if (b->bubble != -1) keep_alives[b->bubble].insert(b->id);
+            if (b->old_bubble != -1) {
+                auto it = keep_alives.find(b->old_bubble);
+                if (it != keep_alives.end()) {
+                    it->second.erase(b->id);
+                    if (it->second.empty()) keep_alives.erase(it);
+                }
+            }
+        }
+    }
+    void increase_interactive(const Ball* b, int64_t bubble) {
+        if (b->interactive && bubble != -1) interactives[bubble].insert(b->id);
+    }
+    void decrease_interactive(const Ball* b, int64_t bubble) {
+        if (!b->interactive || bubble == -1) return;
+        auto it = interactives.find(bubble);
+        if (it == interactives.end()) return;
+        it->second.erase(b->id);
+        if (it->second.empty()) interactives.erase(it);
+    }
+    bool in_dead_bubble(const Ball* b) const {
+        auto i = interactives.find(b->bubble);
+        if (i != interactives.end() && !i->second.empty()) return false;
+        auto k = keep_alives.find(b->bubble);
+        if (k != keep_alives.end() && !k->second.empty()) return false;
+        return true;
+    }
+
+    // ---- filing ----
+    void ball_insert_in_boxes(Ball* b, Box* box1, int64_t new_bubble) {
+        const double inflated = inflated_radius(b);
+        if (box1->released) stale(box1);
+        int mod[3] = {0, 0, 0};
+        for (int q = 0; q < 3; ++q) {
+            if (box1->lo[q] + inflated - b->pos[q] > 0.0)
+                mod[q] = -1;
+            else if (box1->hi[q] - inflated - b->pos[q] < 0.0)
+                mod[q] = 1;
+        }
+        if (b->my_box && box1->level == b->my_box->level && box1->key == b->my_box->key && mod[0] == b->mod[0] &&
+            mod[1] == b->mod[1] && mod[2] == b->mod[2])
+            return;
+        delete_from_boxes(b);
+        for (int q = 0; q < 3; ++q) b->mod[q] = mod[q];
+        box1 = get_box_r(inflated, b->pos);
+        const int64_t ix = box1->key[0], iy = box1->key[1], iz = box1->key[2];
+        const int level = box1->level;
+        insert_in_box(b, box1);
+        topmost(box1)->bubble = new_bubble;                 // (the master)
+        b->active[13] = true;
+        b->my_box = box1;
+        if (level == 0 && (double)(f32(b->radius) * 2.0f) > level_width(0)) {   // a huge ball: every neighbour
+            for (int x = -1; x <= 1; ++x)
+                for (int y = -1; y <= 1; ++y)
+                    for (int z = -1; z <= 1; ++z) {
+                        if (x == 0 && y == 0 && z == 0) continue;
+                        insert_in_box(b, get_box(ix + x, iy + y, iz + z, 0));
+                        b->active[13 + x + 3 * y + 9 * z] = true;
+                    }
+            return;
+        }
+        const int mx = mod[0], my = mod[1], mz = mod[2];
+        auto side = [&](int x, int y, int z) {
+            insert_in_box(b, get_box(ix + x, iy + y, iz + z, level));
+            b->active[13 + x + 3 * y + 9 * z] = true;
+        };
+        if (mx) side(mx, 0, 0);
+        if (my) side(0, my, 0);
+        if (mz) side(0, 0, mz);
+        if (mx && my) side(mx, my, 0);
+        if (mx && mz) side(mx, 0, mz);
+        if (my && mz) side(0, my, mz);
+        if (mx && my && mz) side(mx, my, mz);
+    }
+    void insert_in_boxes(Ball* b) {                        // Ballpark::InsertInBoxes on the master
+        const double inflated = inflated_radius(b);
+        Box* box1 = get_box_r(inflated, b->pos);
+        Box* top = topmost(box1);
+        int64_t new_bubble = top->bubble;
+        if (new_bubble == -1) {
+            delete_from_boxes(b);                           // may release box1 and top: both still read
+            b->my_box = nullptr;
+            new_bubble = nearby_bubbles(stale(top));
+            if (new_bubble == -1) new_bubble = bubble_id++;
+            stale(top)->bubble = new_bubble;
+        }
+        if (b->bubble != new_bubble) {
+            b->old_bubble = b->bubble;
+            b->bubble = new_bubble;
+            add_to_bubble(b);
+        }
+        ball_insert_in_boxes(b, box1, new_bubble);
+    }
+    void refresh_time_factor(Ball* b) {
+        const double m = b->mass * b->agility;
+        b->time_factor = (m <= 0.0) ? 0.0 : std::exp(-friction * dt / m);
+    }
+
+    // ---- the operations ----
+    void add_ball(int64_t id, double mass, double radius, double max_vel, bool free, bool interactive, const double* p,
+                  const double* v, double agility, double sf) {
+        const float r = f32(radius), mv = f32(max_vel), ag = f32(agility), s = f32(sf);
+        Ball* b = ball(id);
+        const bool created = b == nullptr;
+        if (created) {
+            std::unique_ptr<Ball> nb(new Ball());
+            nb->id = id;
+            b = nb.get();
+            balls.add(id, std::move(nb));
+        } else {
+            delete_from_boxes(b);
+        }
+        for (int i = 0; i < 3; ++i) {
+            b->pos[i] = p[i];
+            b->vel[i] = v[i];
+        }
+        b->radius = r < 0.0f ? 0.0 : (double)r;
+        b->mass = mass < 0.0 ? 0.0 : mass;
+        b->free = free;
+        b->interactive = interactive;
+        b->max_vel = mv < 0.0f ? 0.0 : (double)mv;
+        b->agility = ag <= 0.0f ? 1.0 : (double)ag;
+        b->speed_fraction = s < 0.0f ? 0.0 : (double)s;
+        refresh_time_factor(b);
+        insert_in_boxes(b);
+    }
+    void set_position(int64_t id, const double* p) {
+        Ball* b = ball(id);
+        if (!b) return;
+        for (int i = 0; i < 3; ++i) b->pos[i] = p[i];
+        insert_in_boxes(b);
+    }
+    void set_radius(int64_t id, double radius) {
+        Ball* b = ball(id);
+        const float r = f32(radius);
+        if (!b || r < 0.0f) return;
+        b->radius = r;
+        insert_in_boxes(b);
+    }
+    void set_max_velocity(int64_t id, double v) {
+        const float mv = f32(v);
+        Ball* b = ball(id);
+        if (mv < 0.0f || !b) return;
+        b->max_vel = mv;
+        insert_in_boxes(b);
+    }
+    void remove_ball(int64_t id) {
+        Ball* b = ball(id);
+        if (!b) return;
+        delete_from_boxes(b);
+        b->old_bubble = b->bubble;
+        b->bubble = -1;
+        add_to_bubble(b);
+        balls.erase(id);
+    }
+    void set_interactive(int64_t id, bool flag) {
+        Ball* b = ball(id);
+        if (!b) return;
+        if (flag && !b->interactive) {
+            b->interactive = true;
+            increase_interactive(b, b->bubble);
+        } else if (!flag && b->interactive) {
+            decrease_interactive(b, b->bubble);
+            b->interactive = false;
+        }
+    }
+    void initialize_bubbles() {
+        for (auto& kv : levels[0]) kv.second->bubble = -1;
+        bubble_id = 0;
+        bubbles.items.clear();
+        interactives.clear();
+        keep_alives.clear();
+        keep_alive_balls.clear();
+        std::vector<Ball*> order;
+        for (auto& kv : balls.items) order.push_back(kv.second.get());
+        for (Ball* b : order) {
+            if (!b->my_box) {
+                b->old_bubble = b->bubble;
+                b->bubble = -1;
+                continue;
+            }
+            Box* top = topmost(b->my_box);
+            if (top->bubble != -1) {
+                b->old_bubble = b->bubble;
+                b->bubble = top->bubble;
+                add_to_bubble(b);
+                continue;
+            }
+            traverse(top, bubble_id);
+            b->old_bubble = b->bubble;
+            b->bubble = bubble_id;
+            add_to_bubble(b);
+            ++bubble_id;
+        }
+    }
+    void copy_bubbles() {
+        std::vector<int64_t> dead;
+        for (auto& kv : bubbles.items) {
+            std::vector<int64_t> gone;
+            for (auto& e : kv.second.items) {
+                if (e.second == 1)
+                    e.second = 0;
+                else if (e.second == -1)
+                    gone.push_back(e.first);
+            }
+            for (int64_t g : gone) kv.second.erase(g);
+            if (kv.second.items.empty()) dead.push_back(kv.first);
+        }
+        for (int64_t d : dead) bubbles.erase(d);
+    }
+
+    // ---- the state, as text ----
+    std::string state() const {
+        std::string out;
+        char buf[256];
+        std::vector<const Ball*> order;
+        for (auto& kv : balls.items) order.push_back(kv.second.get());
+        std::sort(order.begin(), order.end(), [](const Ball* a, const Ball* b) { return a->id < b->id; });
+        for (const Ball* b : order) {
+            int active = 0;
+            for (int i = 0; i < 27; ++i) active |= (b->active[i] ? 1 : 0) << i;
+            if (b->my_box)
+                snprintf(buf, sizeof buf, "B %lld %lld %lld %d %lld %lld %lld %d %d %d %d %d", (long long)b->id,
+                         (long long)b->bubble, (long long)b->old_bubble, b->my_box->level, (long long)b->my_box->key[0],
+                         (long long)b->my_box->key[1], (long long)b->my_box->key[2], b->mod[0], b->mod[1], b->mod[2],
+                         active, in_dead_bubble(b) ? 1 : 0);
+            else
+                snprintf(buf, sizeof buf, "B %lld %lld %lld - %d %d %d %d %d", (long long)b->id, (long long)b->bubble,
+                         (long long)b->old_bubble, b->mod[0], b->mod[1], b->mod[2], active, in_dead_bubble(b) ? 1 : 0);
+            out += buf;
+            for (auto& kv : b->boxes) {
+                snprintf(buf, sizeof buf, " %lld,%lld,%lld", (long long)kv.first[0], (long long)kv.first[1],
+                         (long long)kv.first[2]);
+                out += buf;
+            }
+            out += "\n";
+        }
+        out += "L";
+        for (int i = 0; i < NUM_LEVELS; ++i) {
+            snprintf(buf, sizeof buf, " %zu", levels[i].size());
+            out += buf;
+        }
+        snprintf(buf, sizeof buf, "\nF %d %lld %d\n", free_boxes, (long long)bubble_id, undefined ? 1 : 0);
+        out += buf;
+        std::vector<std::pair<int64_t, const Ordered<int>*>> bs;
+        for (auto& kv : bubbles.items) bs.emplace_back(kv.first, &kv.second);
+        std::sort(bs.begin(), bs.end(), [](auto& a, auto& b) { return a.first < b.first; });
+        for (auto& kv : bs) {
+            snprintf(buf, sizeof buf, "U %lld", (long long)kv.first);
+            out += buf;
+            for (auto& e : kv.second->items) {
+                snprintf(buf, sizeof buf, " %lld:%d", (long long)e.first, e.second);
+                out += buf;
+            }
+            out += "\n";
+        }
+        for (auto* m : {&interactives, &keep_alives}) {
+            for (auto& kv : *m) {
+                snprintf(buf, sizeof buf, "%s %lld", m == &interactives ? "I" : "K", (long long)kv.first);
+                out += buf;
+                for (int64_t id : kv.second) {
+                    snprintf(buf, sizeof buf, " %lld", (long long)id);
+                    out += buf;
+                }
+                out += "\n";
+            }
+        }
+        return out;
+    }
+};
+
+}  // namespace space_oracle
+
+extern "C" {
+
+// Runs n operations of `stride` doubles each on a fresh master world and writes each state after an operation,
+// separated by 0x1e, into out[cap]; returns the bytes needed (the text is whole when that is at most cap). An
+// operation: its code, then its arguments: 1 AddBall (id, mass, radius, max velocity, free, interactive, x, y, z, vx,
+// vy, vz, agility, speed fraction), 2 SetBallPosition (id, x, y, z), 3 SetBallRadius (id, r), 4 SetMaxSpeed (id, v),
+// 5 RemoveBall (id), 6 InitializeBubbles, 7 CopyBubbles, 8 SetBallInteractive (id, flag), 9 a keep-alive ball (id).
+int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double friction, double dt, char* out,
+                         int64_t cap) {
+    space_oracle::World w;
+    w.friction = friction;
+    w.dt = dt;
+    std::string all;
+    for (int64_t i = 0; i < n; ++i) {
+        const double* o = ops + i * stride;
+        const int code = (int)o[0];
+        const int64_t id = (int64_t)o[1];
+        switch (code) {
+            case 1: w.add_ball(id, o[2], o[3], o[4], o[5] != 0.0, o[6] != 0.0, o + 7, o + 10, o[13], o[14]); break;
+            case 2: w.set_position(id, o + 2); break;
+            case 3: w.set_radius(id, o[2]); break;
+            case 4: w.set_max_velocity(id, o[2]); break;
+            case 5: w.remove_ball(id); break;
+            case 6: w.initialize_bubbles(); break;
+            case 7: w.copy_bubbles(); break;
+            case 8: w.set_interactive(id, o[2] != 0.0); break;
+            case 9: w.keep_alive_balls.insert(id); break;
+            default: break;
+        }
+        all += w.state();
+        all += '\x1e';
+    }
+    const int64_t need = (int64_t)all.size();
+    if (need <= cap && out) std::memcpy(out, all.data(), all.size());
+    return need;
+}
+
+}  // extern "C"

@@ -596,10 +596,38 @@ def make_server_collide_more() -> None:
     print(f"  server_collide_ontick: {res['coverage']}, {time.time() - t0:.0f} s", flush=True)
 
 
+def make_space_bubbles() -> None:
+    """space_bubbles: the master's partition and bubble partition of one world (tests/golden/space_trace.py's streams:
+    60 worlds of 60 mixed operations, 6 of 600, 6 sweeps past BoxAllocator's 256 kept boxes), each operation's state
+    digest recorded on the reference's own SpaceBallpark (exact_ballpark.space, is_master). A stream whose reference run
+    reads a deleted box (DestinyUndefined) is left out."""
+    import space_trace as sp
+    from exact_ballpark.space import DestinyUndefined, SpaceBallpark
+    t0 = time.time()
+    scenarios, dropped = [], 0
+    streams = ([("mixed", s, sp.ops_for(s)) for s in range(1, 61)]
+               + [("long", s, sp.ops_for(s, n_ops=600)) for s in range(1000, 1006)]
+               + [("sweep", s, sp.sweep_ops(s)) for s in range(1, 7)])
+    for family, seed, ops in streams:
+        park = SpaceBallpark(1.0e6, 1000, is_master=True)
+        digests = []
+        try:
+            for op in ops:
+                sp.apply(park, op)
+                digests.append(sp.digest(sp.state_text(park)))
+        except DestinyUndefined:
+            dropped += 1
+            continue
+        scenarios.append({"seed": f"{family}-{seed}", "ops": ops, "digests": digests})
+    sp.save(HERE / "space_bubbles", scenarios)
+    print(f"  space_bubbles: {len(scenarios)} worlds, {sum(len(s['ops']) for s in scenarios)} operations, "
+          f"{dropped} left out, {time.time() - t0:.0f} s", flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending", "server_ontick",
-                                       "server_collide", "server_collide_more"),
+                                       "server_collide", "server_collide_more", "space_bubbles"),
                     default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
     a = ap.parse_args()
@@ -627,6 +655,8 @@ def main() -> None:
         make_server_collide()
     if a.only in (None, "server_collide_more"):
         make_server_collide_more()
+    if a.only in (None, "space_bubbles"):
+        make_space_bubbles()
 
 
 if __name__ == "__main__":

@@ -1,0 +1,171 @@
+"""Golden traces of the master's partition and bubble partition of one world (the space layer's first slice): seeded
+streams of operations (AddBall, SetBallPosition, SetBallRadius, SetMaxSpeed, RemoveBall, SetBallInteractive, a
+keep-alive ball, InitializeBubbles, CopyBubbles) and, after each one, the world's state as a text: each ball's bubble,
+old bubble, filing box, sides, active neighbours, dead-bubble flag and boxes; the live boxes per level; the kept
+boxes, the next bubble id; each bubble's dictionary in its order; the interactive and keep-alive sets.
+
+`make_golden.py` records the texts' digests by running the reference's own SpaceBallpark (exact_ballpark.space, the
+master's view; its scalar transcription of Destiny's Partition and Ballpark); the tests run the same operations on the
+CPU oracle (oracle/space.cpp) and compare, operation by operation.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import random
+from pathlib import Path
+
+import numpy as np
+
+GOLDEN = Path(__file__).resolve().parent
+STRIDE = 16
+ADD, POS, RADIUS, MAXVEL, REMOVE, INIT, COPY, INTERACTIVE, KEEPALIVE = range(1, 10)
+TOP = 7864320.0                                           # a top box's width (m)
+
+
+def _op(code: int, bid: int = 0, *args) -> list:
+    row = [float(code), float(bid)] + [float(a) for a in args]
+    return row + [0.0] * (STRIDE - len(row))
+
+
+def ops_for(seed: int, n_ops: int = 60) -> list:
+    """One world's operations: balls added around a few centres near top-box faces and corners, moved within and
+    across top boxes (joining, splitting and re-forming bubbles), resized up to huge, sped up, removed and re-added,
+    made interactive or not, kept alive, and the bubble partition re-initialised and copied now and then."""
+    r = random.Random(f"space-bubbles-{seed}")
+    centres = [[r.choice((-1.0, 0.0, 1.0)) * TOP * r.choice((0.5, 1.0)) + r.uniform(-2e4, 2e4) for _ in range(3)]
+               for _ in range(r.randint(1, 3))]
+    ids, live, ops = list(range(1, 13)), [], []
+
+    def where() -> list:
+        c = r.choice(centres)
+        k = r.random()
+        if k < 0.5:
+            return [x + r.uniform(-3e4, 3e4) for x in c]
+        if k < 0.8:                                        # near a face of a finer box
+            return [x + r.choice((-1.0, 1.0)) * r.uniform(0.0, 2e3) for x in c]
+        return [x + r.uniform(-1.2 * TOP, 1.2 * TOP) for x in c]
+
+    def radius() -> float:
+        return r.choice([r.uniform(5.0, 300.0), r.uniform(300.0, 5e4), r.uniform(5e4, 2e6), r.uniform(4e6, 6e6)])
+
+    for _ in range(n_ops):
+        k = r.random()
+        free = [b for b in ids if b not in live]
+        if (k < 0.3 or not live) and free:
+            b = r.choice(free)
+            vel = [r.uniform(-300.0, 300.0) for _ in range(3)] if r.random() < 0.6 else [0.0, 0.0, 0.0]
+            ops.append(_op(ADD, b, 10 ** r.uniform(5.0, 9.0), radius(), r.uniform(0.0, 3000.0),
+                           1.0 if r.random() < 0.8 else 0.0, 1.0 if r.random() < 0.6 else 0.0, *where(), *vel,
+                           r.uniform(0.05, 3.0), r.choice((0.0, 0.5, 1.0))))
+            live.append(b)
+        elif k < 0.55:
+            ops.append(_op(POS, r.choice(live), *where()))
+        elif k < 0.62:
+            ops.append(_op(RADIUS, r.choice(live), radius() if r.random() < 0.9 else -1.0))
+        elif k < 0.67:
+            ops.append(_op(MAXVEL, r.choice(live), r.uniform(0.0, 1e5)))
+        elif k < 0.74:
+            b = r.choice(live)
+            ops.append(_op(REMOVE, b))
+            live.remove(b)
+        elif k < 0.82:
+            ops.append(_op(INTERACTIVE, r.choice(live), float(r.random() < 0.5)))
+        elif k < 0.86:
+            ops.append(_op(KEEPALIVE, r.choice(ids)))
+        elif k < 0.93:
+            ops.append(_op(COPY))
+        else:
+            ops.append(_op(INIT))
+    return ops
+
+
+def sweep_ops(seed: int) -> list:
+    """A world that releases more boxes than BoxAllocator keeps: a dozen huge balls (27 top boxes each) far apart,
+    a few small ones among them, then every huge ball removed (past 256 kept boxes the released ones are deleted), new
+    balls added (taking kept boxes), the partition re-initialised and copied."""
+    r = random.Random(f"space-sweep-{seed}")
+    ops = []
+    for b in range(1, 13):
+        c = [(b - 6) * 4.0 * TOP, r.uniform(-TOP, TOP), r.uniform(-TOP, TOP)]
+        ops.append(_op(ADD, b, 1e8, r.uniform(4.0e6, 4.5e6), 0.0, 0.0, float(b % 3 == 0), *c, 0.0, 0.0, 0.0, 1.0,
+                       1.0))
+    for b in range(20, 26):
+        c = [r.uniform(-20.0, 20.0) * TOP, r.uniform(-TOP, TOP), r.uniform(-TOP, TOP)]
+        ops.append(_op(ADD, b, 1e7, r.uniform(10.0, 500.0), 200.0, 1.0, 1.0, *c, 50.0, 0.0, 0.0, 1.0, 1.0))
+    ops.append(_op(COPY))
+    for b in r.sample(range(1, 13), 12):
+        ops.append(_op(REMOVE, b))
+    for b in range(30, 36):
+        c = [r.uniform(-20.0, 20.0) * TOP, r.uniform(-TOP, TOP), r.uniform(-TOP, TOP)]
+        ops.append(_op(ADD, b, 1e7, r.choice((100.0, 3e5, 4.2e6)), 200.0, 1.0, 1.0, *c, 0.0, 0.0, 0.0, 1.0, 1.0))
+    ops += [_op(INIT), _op(COPY)]
+    for b in (20, 21, 30):
+        ops.append(_op(POS, b, r.uniform(-20.0, 20.0) * TOP, 0.0, 0.0))
+    return ops
+
+
+def apply(park, op: list) -> None:
+    """One operation on the reference's SpaceBallpark."""
+    code, bid = int(op[0]), int(op[1])
+    a = op[2:]
+    if code == ADD:
+        park.add_ball(bid, a[0], a[1], a[2], is_free=bool(a[3]), is_interactive=bool(a[4]), x=a[5], y=a[6], z=a[7],
+                      vx=a[8], vy=a[9], vz=a[10], agility=a[11], speed_fraction=a[12])
+    elif code == POS:
+        park.set_position(bid, a[0], a[1], a[2])
+    elif code == RADIUS:
+        park.set_radius(bid, a[0])
+    elif code == MAXVEL:
+        park.set_max_velocity(bid, a[0])
+    elif code == REMOVE:
+        park.remove_ball(bid)
+    elif code == INIT:
+        park.initialize_bubbles(0)
+    elif code == COPY:
+        park.copy_bubbles()
+    elif code == INTERACTIVE:
+        park.set_interactive(bid, bool(a[0]))
+    elif code == KEEPALIVE:
+        park.add_keep_alive_ball(bid)
+
+
+def state_text(park) -> str:
+    """The reference world's state in the oracle's text (oracle/space.cpp's `state`)."""
+    out = []
+    for bid in sorted(park.balls):
+        b = park.balls[bid]
+        active = sum(1 << i for i in range(27) if b.active[i])
+        dead = 1 if park.in_dead_bubble(b) else 0
+        if b.my_box is not None:
+            head = (f"B {b.id} {b.bubble} {b.old_bubble} {b.my_box.level} {b.my_box.key[0]} {b.my_box.key[1]} "
+                    f"{b.my_box.key[2]} {b.mod[0]} {b.mod[1]} {b.mod[2]} {active} {dead}")
+        else:
+            head = f"B {b.id} {b.bubble} {b.old_bubble} - {b.mod[0]} {b.mod[1]} {b.mod[2]} {active} {dead}"
+        out.append(head + "".join(f" {k[0]},{k[1]},{k[2]}" for k in sorted(b.boxes)) + "\n")
+    out.append("L" + "".join(f" {len(lv)}" for lv in park.levels) + "\n")
+    out.append(f"F {park.free_boxes} {park.bubble_id} 0\n")
+    for bub in sorted(park.bubbles):
+        out.append(f"U {bub}" + "".join(f" {k}:{v}" for k, v in park.bubbles[bub].items()) + "\n")
+    for tag, m in (("I", park.bubble_interactives), ("K", park.bubble_keep_alives)):
+        for bub in sorted(m):
+            out.append(f"{tag} {bub}" + "".join(f" {i}" for i in sorted(m[bub])) + "\n")
+    return "".join(out)
+
+
+def digest(text: str) -> np.uint64:
+    return np.frombuffer(hashlib.sha256(text.encode()).digest()[:8], dtype=np.uint64)[0]
+
+
+def save(path: Path, scenarios: list) -> None:
+    """scenarios: [{"seed", "ops" [n][STRIDE], "digests" [n] uint64}], as one compressed archive."""
+    arrays = {"names": np.array([s["seed"] for s in scenarios])}
+    for i, sc in enumerate(scenarios):
+        arrays[f"ops{i}"] = np.array(sc["ops"], dtype=np.float64)
+        arrays[f"digests{i}"] = np.array(sc["digests"], dtype=np.uint64)
+    np.savez_compressed(str(path) + ".npz", **arrays)
+
+
+def load(path: Path) -> list:
+    z = np.load(str(path) + ".npz")
+    return [{"seed": str(name), "ops": z[f"ops{i}"], "digests": z[f"digests{i}"]} for i, name in enumerate(z["names"])]

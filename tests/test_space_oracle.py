@@ -1,0 +1,45 @@
+"""The CPU oracle of the master's partition and bubble partition of one world (oracle/space.cpp) against the golden
+digests recorded on the reference's own SpaceBallpark (tests/golden/space_trace.py): 72 worlds, 7,452 operations
+(balls added near top-box faces and corners, moved across top boxes, resized up to huge, removed and re-added, made
+interactive, kept alive; InitializeBubbles and CopyBubbles; sweeps past BoxAllocator's 256 kept boxes), every state
+after every operation. The first slice of the space layer: its kernel is built on this oracle."""
+
+import numpy as np
+
+import space_trace as sp
+from oracle import space_world
+
+
+def _scenarios():
+    return sp.load(sp.GOLDEN / "space_bubbles")
+
+
+def test_the_oracle_matches_the_references_partition_and_bubbles_after_every_operation():
+    bad = []
+    for sc in _scenarios():
+        got = np.array([sp.digest(t) for t in space_world.run(sc["ops"])], dtype=np.uint64)
+        if got.shape != sc["digests"].shape or not (got == sc["digests"]).all():
+            first = int(np.nonzero(got != sc["digests"])[0][0]) if got.shape == sc["digests"].shape else -1
+            bad.append((sc["seed"], first))
+    assert not bad, f"{len(bad)} worlds differ, first {bad[:3]}"
+
+
+def test_the_streams_reach_the_partitions_paths():
+    texts = [t for sc in _scenarios() for t in space_world.run(sc["ops"])]
+    kept = max(int(line.split()[1]) for t in texts for line in t.splitlines() if line.startswith("F "))
+    assert kept == 256                                     # BoxAllocator full: later releases delete
+    huge = sum(1 for t in texts for line in t.splitlines()
+               if line.startswith("B ") and " - " not in line and bin(int(line.split()[11])).count("1") == 27)
+    assert huge > 100                                      # huge balls in their 27 top boxes
+    bubbles = max(int(line.split()[2]) for t in texts for line in t.splitlines() if line.startswith("F "))
+    assert bubbles >= 5
+    assert any(" -1:" in t or ":-1" in t for t in texts)   # a ball leaving a bubble before CopyBubbles
+
+
+def test_a_planted_fault_in_the_operations_is_seen():
+    sc = _scenarios()[0]
+    ops = sc["ops"].copy()
+    k = next(i for i in range(len(ops)) if int(ops[i, 0]) == sp.ADD)
+    ops[k, 7] += sp.TOP                                    # one ball added a top box further along x
+    got = np.array([sp.digest(t) for t in space_world.run(ops)], dtype=np.uint64)
+    assert not (got == sc["digests"]).all()
