@@ -9,7 +9,8 @@
 // boxes, BoxAllocator's free list) or deleted, and Destiny reads a released box in one path (a ball that was its
 // box's only occupant): every box ever made is kept here, so that read sees the stale values, and a read of a deleted
 // box sets `undefined` (Destiny's result is undefined there). Balls, bubbles and the bubble dictionaries keep the
-// reference's insertion orders. Sensors, collisions, queries, modes and the tick are not in this slice.
+// reference's insertion orders; the queries (GetNearbyBalls' walk, CheckVisibility, GetBallIdsInRange,
+// GetBubbleAtCoordinates) read them. Sensors, collisions, modes and the tick are not in this slice.
 
 #include <algorithm>
 #include <array>
@@ -79,14 +80,15 @@ struct Box {
     std::map<Key, Box*> children;
     std::map<int64_t, Ball*> balls;
     int64_t bubble = -1;
-    bool released = false, deleted = false;
+    bool released = false, deleted = false, handled = false;
 };
 
 struct Ball {
     int64_t id;
     double mass = 0.0, radius = 0.0, max_vel = 0.0, agility = 1.0, speed_fraction = 1.0, time_factor = 1.0;
     double pos[3] = {1e10, 1e10, 1e10}, vel[3] = {0.0, 0.0, 0.0};
-    bool free = false, interactive = false;
+    bool free = false, interactive = false, massive = false, handled = false;
+    int64_t cloaked = 0;
     int64_t bubble = -1, old_bubble = -1;
     std::map<Key, Box*> boxes;
     Box* my_box = nullptr;
@@ -360,7 +362,7 @@ struct World {
 
     // ---- the operations ----
     void add_ball(int64_t id, double mass, double radius, double max_vel, bool free, bool interactive, const double* p,
-                  const double* v, double agility, double sf) {
+                  const double* v, double agility, double sf, bool massive) {
         const float r = f32(radius), mv = f32(max_vel), ag = f32(agility), s = f32(sf);
         Ball* b = ball(id);
         const bool created = b == nullptr;
@@ -380,6 +382,7 @@ struct World {
         b->mass = mass < 0.0 ? 0.0 : mass;
         b->free = free;
         b->interactive = interactive;
+        b->massive = massive;
         b->max_vel = mv < 0.0f ? 0.0 : (double)mv;
         b->agility = ag <= 0.0f ? 1.0 : (double)ag;
         b->speed_fraction = s < 0.0f ? 0.0 : (double)s;
@@ -471,6 +474,118 @@ struct World {
         for (int64_t d : dead) bubbles.erase(d);
     }
 
+    // ---- the queries (space.py:819-895, 1057-1061, 1524-1611) ----
+    static double lensq(const double* v) { return v[0] * v[0] + v[1] * v[1] + v[2] * v[2]; }
+    static double dot(const double* u, const double* v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; }
+
+    void explode_children(Box* box, std::vector<Box*>& out) {
+        for (auto& kv : box->children) {
+            explode_children(kv.second, out);
+            if (!kv.second->balls.empty()) out.push_back(kv.second);
+        }
+    }
+    // GetNearbyBalls: the ball's boxes, their ancestors holding balls and their descendants, then the balls in them that
+    // pass the filter, each once, in box order and then id order (no missiles, fields or global balls in this slice)
+    std::vector<Ball*> nearby_balls(Ball* b, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked) {
+        std::vector<Ball*> uni;
+        if (exclude_inert) {
+            auto it = interactives.find(b->bubble);
+            if (it == interactives.end() || it->second.empty()) return uni;
+        }
+        std::vector<Box*> s_boxes;
+        for (auto& kv : b->boxes) {
+            Box* box = kv.second;
+            if (box->handled) continue;
+            Box* p = box;
+            while (p->parent) {
+                p = p->parent;
+                if (p->handled) break;
+                if (!p->balls.empty()) {
+                    s_boxes.push_back(p);
+                    p->handled = true;
+                }
+            }
+            explode_children(box, s_boxes);
+            if (box->balls.size() > 1) {
+                s_boxes.push_back(box);
+                box->handled = true;
+            }
+        }
+        for (Box* box : s_boxes) {
+            box->handled = false;
+            for (auto& kv : box->balls) {
+                Ball* o = kv.second;
+                if (o->handled || o == b) continue;
+                if (exclude_cloaked && (o->cloaked || !o->massive)) continue;
+                if (exclude_inert) {
+                    if (!o->interactive) continue;
+                } else {
+                    if (o->bubble != b->bubble) continue;
+                    if (exclude_fixed && !o->free) continue;
+                }
+                o->handled = true;
+                uni.push_back(o);
+            }
+        }
+        for (Ball* o : uni) o->handled = false;
+        return uni;
+    }
+    int64_t check_visibility(int64_t src_id, int64_t dst_id) {
+        Ball *src = ball(src_id), *dst = ball(dst_id);
+        if (!src || !dst || src->bubble != dst->bubble) return -2;
+        double ray[3] = {dst->pos[0] - src->pos[0], dst->pos[1] - src->pos[1], dst->pos[2] - src->pos[2]};
+        const double distance = std::sqrt(lensq(ray));
+        const double norm = std::sqrt(ray[0] * ray[0] + ray[1] * ray[1] + ray[2] * ray[2]);
+        if (norm != 0.0) {
+            const double inv = 1.0 / norm;
+            for (double& x : ray) x = x * inv;
+        }
+        for (auto& kv : balls.items) {
+            Ball* o = kv.second.get();
+            if (o->bubble != src->bubble || o == src || o == dst || !o->massive || o->cloaked) continue;
+            const double to_center[3] = {o->pos[0] - src->pos[0], o->pos[1] - src->pos[1], o->pos[2] - src->pos[2]};
+            const double v = dot(ray, to_center), r = o->radius;
+            const double dsq = r * r - (dot(to_center, to_center) - v * v);
+            if (dsq < 0.0) continue;
+            const double d = std::sqrt(dsq);
+            if (v - d > 0.0 && v - d < distance) return o->id;
+        }
+        return 0;
+    }
+    int64_t top_bubble_at(const double* p) {               // the existing top box's bubble, or -2 for none
+        const Key k = key_for(level_for(10000000.0), p);
+        Box* top = check_box(k[0], k[1], k[2], level_for(10000000.0));
+        return top ? top->bubble : -2;
+    }
+    // GetBallIdsInRange (and with distances): the balls listed in the bubble's dictionary, in its order
+    std::string in_range(Ball* ref, const double* center, int64_t bubble_id, double range, bool cloaked, bool dist) {
+        std::string out;
+        char buf[96];
+        if (bubble_id == -1) return out;
+        Ordered<int>* dict = bubbles.find(bubble_id);
+        if (!dict) return out;
+        std::vector<int64_t> ids;
+        for (auto& e : dict->items) ids.push_back(e.first);
+        for (int64_t id : ids) {
+            Ball* o = ball(id);
+            if (!o || o == ref) continue;
+            if (o->cloaked && !cloaked) continue;
+            const double d[3] = {o->pos[0] - center[0], o->pos[1] - center[1], o->pos[2] - center[2]};
+            const double d2 = lensq(d), lim = range + o->radius;
+            if (d2 <= lim * lim) {
+                if (dist) {
+                    uint64_t bits;
+                    std::memcpy(&bits, &d2, 8);
+                    snprintf(buf, sizeof buf, " %016llx:%lld", (unsigned long long)bits, (long long)o->id);
+                } else {
+                    snprintf(buf, sizeof buf, " %lld", (long long)o->id);
+                }
+                out += buf;
+            }
+        }
+        return out;
+    }
+
     // ---- the state, as text ----
     std::string state() const {
         std::string out;
@@ -539,19 +654,66 @@ extern "C" {
 // separated by 0x1e, into out[cap]; returns the bytes needed (the text is whole when that is at most cap). An
 // operation: its code, then its arguments: 1 AddBall (id, mass, radius, max velocity, free, interactive, x, y, z, vx,
 // vy, vz, agility, speed fraction), 2 SetBallPosition (id, x, y, z), 3 SetBallRadius (id, r), 4 SetMaxSpeed (id, v),
-// 5 RemoveBall (id), 6 InitializeBubbles, 7 CopyBubbles, 8 SetBallInteractive (id, flag), 9 a keep-alive ball (id).
+// 5 RemoveBall (id), 6 InitializeBubbles, 7 CopyBubbles, 8 SetBallInteractive (id, flag), 9 a keep-alive ball (id),
+// 10 the cloak attribute (id, value); the queries, their answer after the state: 11 CheckVisibility (src, dst),
+// 12 GetBallIdsInRange from a ball (id, range, include cloaked, with distances), 13 the same from a point (x, y, z,
+// range, include cloaked, with distances), 14 GetBubbleAtCoordinates (x, y, z), 15 GetNearbyBalls (id, exclude fixed,
+// exclude inert, exclude cloaked). AddBall's sixteenth value is its massive flag.
 int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double friction, double dt, char* out,
                          int64_t cap) {
     space_oracle::World w;
     w.friction = friction;
     w.dt = dt;
     std::string all;
+    char buf[64];
     for (int64_t i = 0; i < n; ++i) {
         const double* o = ops + i * stride;
         const int code = (int)o[0];
         const int64_t id = (int64_t)o[1];
+        std::string answer;
         switch (code) {
-            case 1: w.add_ball(id, o[2], o[3], o[4], o[5] != 0.0, o[6] != 0.0, o + 7, o + 10, o[13], o[14]); break;
+            case 1:
+                w.add_ball(id, o[2], o[3], o[4], o[5] != 0.0, o[6] != 0.0, o + 7, o + 10, o[13], o[14], o[15] != 0.0);
+                break;
+            case 10:
+                if (space_oracle::Ball* b = w.ball(id)) b->cloaked = (int64_t)o[2] & 0xFF;
+                break;
+            case 11:
+                snprintf(buf, sizeof buf, "Q %lld\n", (long long)w.check_visibility(id, (int64_t)o[2]));
+                answer = buf;
+                break;
+            case 12: {
+                space_oracle::Ball* ref = w.ball(id);
+                answer = ref ? "Q" + w.in_range(ref, ref->pos, ref->bubble, o[2], o[3] != 0.0, o[4] != 0.0) + "\n"
+                             : "Q None\n";
+                break;
+            }
+            case 13: {
+                const int64_t top = w.top_bubble_at(o + 2);
+                answer = "Q" + w.in_range(nullptr, o + 2, top == -2 ? -1 : top, o[5], o[6] != 0.0, o[7] != 0.0) + "\n";
+                break;
+            }
+            case 14: {
+                const int64_t top = w.top_bubble_at(o + 2);
+                if (top == -2)
+                    answer = "Q None\n";
+                else {
+                    snprintf(buf, sizeof buf, "Q %lld\n", (long long)top);
+                    answer = buf;
+                }
+                break;
+            }
+            case 15: {
+                space_oracle::Ball* b = w.ball(id);
+                answer = "Q";
+                if (b)
+                    for (space_oracle::Ball* x : w.nearby_balls(b, o[2] != 0.0, o[3] != 0.0, o[4] != 0.0)) {
+                        snprintf(buf, sizeof buf, " %lld", (long long)x->id);
+                        answer += buf;
+                    }
+                answer += "\n";
+                break;
+            }
             case 2: w.set_position(id, o + 2); break;
             case 3: w.set_radius(id, o[2]); break;
             case 4: w.set_max_velocity(id, o[2]); break;
@@ -563,6 +725,7 @@ int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double fr
             default: break;
         }
         all += w.state();
+        all += answer;
         all += '\x1e';
     }
     const int64_t need = (int64_t)all.size();

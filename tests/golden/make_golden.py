@@ -613,8 +613,8 @@ def make_space_bubbles() -> None:
         digests = []
         try:
             for op in ops:
-                sp.apply(park, op)
-                digests.append(sp.digest(sp.state_text(park)))
+                answer = sp.apply(park, op)
+                digests.append(sp.digest(sp.state_text(park) + answer))
         except DestinyUndefined:
             dropped += 1
             continue

@@ -1,8 +1,10 @@
 """Golden traces of the master's partition and bubble partition of one world (the space layer's first slice): seeded
 streams of operations (AddBall, SetBallPosition, SetBallRadius, SetMaxSpeed, RemoveBall, SetBallInteractive, a
-keep-alive ball, InitializeBubbles, CopyBubbles) and, after each one, the world's state as a text: each ball's bubble,
-old bubble, filing box, sides, active neighbours, dead-bubble flag and boxes; the live boxes per level; the kept
-boxes, the next bubble id; each bubble's dictionary in its order; the interactive and keep-alive sets.
+keep-alive ball, the cloak attribute, InitializeBubbles, CopyBubbles, and the queries GetNearbyBalls, CheckVisibility,
+GetBallIdsInRange from a ball or a point, GetBubbleAtCoordinates) and, after each one, the world's state as a text: each
+ball's bubble, old bubble, filing box, sides, active neighbours, dead-bubble flag and boxes; the live boxes per level;
+the kept boxes, the next bubble id; each bubble's dictionary in its order; the interactive and keep-alive sets; the
+query's answer.
 
 `make_golden.py` records the texts' digests by running the reference's own SpaceBallpark (exact_ballpark.space, the
 master's view; its scalar transcription of Destiny's Partition and Ballpark); the tests run the same operations on the
@@ -13,6 +15,7 @@ from __future__ import annotations
 
 import hashlib
 import random
+import struct
 from pathlib import Path
 
 import numpy as np
@@ -20,6 +23,7 @@ import numpy as np
 GOLDEN = Path(__file__).resolve().parent
 STRIDE = 16
 ADD, POS, RADIUS, MAXVEL, REMOVE, INIT, COPY, INTERACTIVE, KEEPALIVE = range(1, 10)
+CLOAKED, VISIBILITY, RANGE_BALL, RANGE_POINT, BUBBLE_AT, NEARBY = range(10, 16)
 TOP = 7864320.0                                           # a top box's width (m)
 
 
@@ -57,8 +61,25 @@ def ops_for(seed: int, n_ops: int = 60) -> list:
             vel = [r.uniform(-300.0, 300.0) for _ in range(3)] if r.random() < 0.6 else [0.0, 0.0, 0.0]
             ops.append(_op(ADD, b, 10 ** r.uniform(5.0, 9.0), radius(), r.uniform(0.0, 3000.0),
                            1.0 if r.random() < 0.8 else 0.0, 1.0 if r.random() < 0.6 else 0.0, *where(), *vel,
-                           r.uniform(0.05, 3.0), r.choice((0.0, 0.5, 1.0))))
+                           r.uniform(0.05, 3.0), r.choice((0.0, 0.5, 1.0)), 1.0 if r.random() < 0.7 else 0.0))
             live.append(b)
+        elif k < 0.4 and live:                             # a query
+            q = r.random()
+            a, c = r.choice(live), r.choice(ids)
+            if q < 0.3:
+                ops.append(_op(NEARBY, a, float(r.random() < 0.5), float(r.random() < 0.3), float(r.random() < 0.5)))
+            elif q < 0.5:
+                ops.append(_op(VISIBILITY, a, c))
+            elif q < 0.7:
+                ops.append(_op(RANGE_BALL, a, r.choice((1e3, 3e4, 1e6, 1e7)), float(r.random() < 0.5),
+                               float(r.random() < 0.5)))
+            elif q < 0.85:
+                ops.append(_op(RANGE_POINT, 0, *where(), r.choice((1e3, 3e4, 1e6, 1e7)), float(r.random() < 0.5),
+                               float(r.random() < 0.5)))
+            else:
+                ops.append(_op(BUBBLE_AT, 0, *where()))
+        elif k < 0.43 and live:
+            ops.append(_op(CLOAKED, r.choice(live), r.choice((0.0, 1.0, 2.0, 200.0))))
         elif k < 0.55:
             ops.append(_op(POS, r.choice(live), *where()))
         elif k < 0.62:
@@ -105,13 +126,36 @@ def sweep_ops(seed: int) -> list:
     return ops
 
 
-def apply(park, op: list) -> None:
-    """One operation on the reference's SpaceBallpark."""
+def _bits(x: float) -> str:
+    return "%016x" % struct.unpack("<Q", struct.pack("<d", float(x)))[0]
+
+
+def apply(park, op: list) -> str:
+    """One operation on the reference's SpaceBallpark; a query's answer as the oracle writes it ("" for the others)."""
     code, bid = int(op[0]), int(op[1])
-    a = op[2:]
+    a = [float(x) for x in op[2:]]
+    if code == CLOAKED:
+        park.set_cloaked(bid, int(a[0]))
+    elif code == VISIBILITY:
+        return f"Q {park.check_visibility(bid, int(a[0]))}\n"
+    elif code in (RANGE_BALL, RANGE_POINT):
+        if code == RANGE_BALL:
+            got = park.ball_ids_in_range(bid, a[0], int(a[1]), include_dist=bool(a[2]))
+        else:
+            got = park.ball_ids_in_range(a[0], a[1], a[2], a[3], int(a[4]), include_dist=bool(a[5]))
+        if got is None:
+            return "Q None\n"
+        return "Q" + "".join(f" {_bits(x[0])}:{x[1]}" if isinstance(x, tuple) else f" {x}" for x in got) + "\n"
+    elif code == BUBBLE_AT:
+        top = park.bubble_at(a[0], a[1], a[2])
+        return "Q None\n" if top is None else f"Q {top}\n"
+    elif code == NEARBY:
+        b = park.balls.get(bid)
+        got = [] if b is None else park._nearby_balls(b, bool(a[0]), bool(a[1]), False, bool(a[2]), False)
+        return "Q" + "".join(f" {o.id}" for o in got) + "\n"
     if code == ADD:
         park.add_ball(bid, a[0], a[1], a[2], is_free=bool(a[3]), is_interactive=bool(a[4]), x=a[5], y=a[6], z=a[7],
-                      vx=a[8], vy=a[9], vz=a[10], agility=a[11], speed_fraction=a[12])
+                      vx=a[8], vy=a[9], vz=a[10], agility=a[11], speed_fraction=a[12], is_massive=bool(a[13]))
     elif code == POS:
         park.set_position(bid, a[0], a[1], a[2])
     elif code == RADIUS:
@@ -128,6 +172,7 @@ def apply(park, op: list) -> None:
         park.set_interactive(bid, bool(a[0]))
     elif code == KEEPALIVE:
         park.add_keep_alive_ball(bid)
+    return ""
 
 
 def state_text(park) -> str:

@@ -1,8 +1,9 @@
 """The CPU oracle of the master's partition and bubble partition of one world (oracle/space.cpp) against the golden
-digests recorded on the reference's own SpaceBallpark (tests/golden/space_trace.py): 72 worlds, 7,452 operations
-(balls added near top-box faces and corners, moved across top boxes, resized up to huge, removed and re-added, made
-interactive, kept alive; InitializeBubbles and CopyBubbles; sweeps past BoxAllocator's 256 kept boxes), every state
-after every operation. The first slice of the space layer: its kernel is built on this oracle."""
+digests recorded on the reference's own SpaceBallpark (tests/golden/space_trace.py): 72 worlds (balls added near
+top-box faces and corners, moved across top boxes, resized up to huge, removed and re-added, made interactive, kept
+alive, cloaked; InitializeBubbles and CopyBubbles; sweeps past BoxAllocator's 256 kept boxes; the queries
+GetNearbyBalls, CheckVisibility, GetBallIdsInRange from a ball or a point, GetBubbleAtCoordinates), every state and
+every answer after every operation. The first slice of the space layer: its kernel is built on this oracle."""
 
 import numpy as np
 
@@ -34,6 +35,11 @@ def test_the_streams_reach_the_partitions_paths():
     bubbles = max(int(line.split()[2]) for t in texts for line in t.splitlines() if line.startswith("F "))
     assert bubbles >= 5
     assert any(" -1:" in t or ":-1" in t for t in texts)   # a ball leaving a bubble before CopyBubbles
+    answers = [t.splitlines()[-1] for t in texts if t.splitlines()[-1].startswith("Q")]
+    assert len(answers) > 300
+    assert sum(1 for a in answers if len(a.split()) > 2) > 50         # answers listing several balls
+    assert any(":" in a for a in answers) and any(a == "Q None" for a in answers)
+    assert any(a.split()[1:] and a.split()[1].isdigit() and int(a.split()[1]) > 0 for a in answers if len(a.split()) == 2)
 
 
 def test_a_planted_fault_in_the_operations_is_seen():
