@@ -10,7 +10,10 @@
 // box's only occupant): every box ever made is kept here, so that read sees the stale values, and a read of a deleted
 // box sets `undefined` (Destiny's result is undefined there). Balls, bubbles and the bubble dictionaries keep the
 // reference's insertion orders; the queries (GetNearbyBalls' walk, CheckVisibility, GetBallIdsInRange,
-// GetBubbleAtCoordinates) read them. Sensors, collisions, modes and the tick are not in this slice.
+// GetBubbleAtCoordinates) read them; the proximity sensors (AddProximitySensor, HandleProximities: the candidates of
+// GetNearbyBalls with the inflated radius, the ball re-filed twice, enter and leave in the unordered maps' order).
+// Notification ranges, target tracking, a shuffled sensor's first period, collisions, modes and the tick are not in
+// this slice.
 
 #include <algorithm>
 #include <array>
@@ -70,6 +73,33 @@ struct Ordered {
     }
 };
 
+// std::unordered_map<int64_t, ...>'s iteration order under libstdc++'s prime rehash policy, for the maps this slice
+// holds (at most 13 keys): a map's first insertion gives it 13 buckets (its policy asked for 11 keys); a key is linked
+// just before the first key of the order in its bucket (the key modulo the bucket count), else at the front; erasures
+// and clear() keep the rest; a 14th key would grow the table, which is outside the slice (`overflow`).
+struct HashOrder {
+    std::vector<int64_t> order;
+    uint64_t buckets = 1;
+    bool overflow = false;
+    bool contains(int64_t k) const { return std::find(order.begin(), order.end(), k) != order.end(); }
+    void insert(int64_t k) {
+        if (contains(k)) return;
+        if (buckets == 1) buckets = 13;
+        if (order.size() + 1 > 13) overflow = true;
+        const uint64_t b = (uint64_t)k % buckets;
+        for (size_t i = 0; i < order.size(); ++i)
+            if ((uint64_t)order[i] % buckets == b) {
+                order.insert(order.begin() + i, k);
+                return;
+            }
+        order.insert(order.begin(), k);
+    }
+    void erase(int64_t k) {
+        auto it = std::find(order.begin(), order.end(), k);
+        if (it != order.end()) order.erase(it);
+    }
+};
+
 struct Ball;
 
 struct Box {
@@ -89,6 +119,10 @@ struct Ball {
     double pos[3] = {1e10, 1e10, 1e10}, vel[3] = {0.0, 0.0, 0.0};
     bool free = false, interactive = false, massive = false, handled = false;
     int64_t cloaked = 0;
+    bool sensor_active = false, sensor_only_interactives = false, has_proximity = false;
+    float sensor_range = 0.0f;
+    double sensor_period = 2.0, sensor_elapsed = 0.0;
+    HashOrder sensor_balls;
     int64_t bubble = -1, old_bubble = -1;
     std::map<Key, Box*> boxes;
     Box* my_box = nullptr;
@@ -109,6 +143,7 @@ struct World {
     std::set<int64_t> keep_alive_balls;
     int64_t bubble_id = 0;
     bool undefined = false;
+    HashOrder proximity;                                   // mProximityBalls
 
     Ball* ball(int64_t id) {
         auto* p = balls.find(id);
@@ -416,6 +451,7 @@ struct World {
         b->old_bubble = b->bubble;
         b->bubble = -1;
         add_to_bubble(b);
+        if (b->has_proximity) proximity.erase(id);
         balls.erase(id);
     }
     void set_interactive(int64_t id, bool flag) {
@@ -586,6 +622,103 @@ struct World {
         return out;
     }
 
+    // ---- proximity sensors (space.py:1345-1523; SEN-701, SEN-702; no notification range or tracking here) ----
+    void update_proximity_status(Ball* b) {
+        b->has_proximity = b->sensor_active;
+        if (b->has_proximity)
+            proximity.insert(b->id);
+        else
+            proximity.erase(b->id);
+    }
+    void add_sensor(int64_t id, double range, double period, bool only_interactives) {
+        Ball* b = ball(id);
+        if (!b) return;
+        const float r = f32(range);
+        if (f32((double)f32(b->radius) + (double)r) < 0.0f) return;
+        b->sensor_balls.order.clear();
+        b->sensor_range = r;
+        b->sensor_period = period;
+        b->sensor_active = true;
+        b->sensor_only_interactives = only_interactives;
+        update_proximity_status(b);
+    }
+    void remove_sensor(int64_t id) {
+        Ball* b = ball(id);
+        if (!b) return;
+        b->sensor_active = false;
+        update_proximity_status(b);
+    }
+    void set_ball_radius(Ball* b, float r) {
+        if (r < 0.0f) return;
+        b->radius = r;
+        insert_in_boxes(b);
+    }
+    void check_sensor(Ball* b, std::string& events) {
+        char buf[96];
+        b->sensor_elapsed += dt;
+        if (b->sensor_elapsed < b->sensor_period) return;
+        b->sensor_elapsed = 0.0;
+        const double radius = b->radius;
+        const double vel[3] = {b->vel[0], b->vel[1], b->vel[2]};
+        b->vel[0] = b->vel[1] = b->vel[2] = 0.0;
+        set_ball_radius(b, f32((double)f32(b->radius) + (double)b->sensor_range));   // float + float
+        const bool exclude_fixed = b->cloaked == 0;
+        std::vector<Ball*> uni = nearby_balls(b, exclude_fixed, b->sensor_only_interactives, false);
+        for (int i = 0; i < 3; ++i) b->vel[i] = vel[i];
+        set_ball_radius(b, (float)radius);
+        if (!b->sensor_balls.order.empty()) {
+            std::set<int64_t> near;
+            for (Ball* o : uni) near.insert(o->id);
+            const std::vector<int64_t> keys = b->sensor_balls.order;
+            for (int64_t k : keys) {
+                if (k == b->id || near.count(k)) continue;
+                b->sensor_balls.erase(k);
+                snprintf(buf, sizeof buf, " %lld:%lld:0", (long long)b->id, (long long)k);
+                events += buf;
+                if (!b->sensor_active) break;
+            }
+        }
+        for (Ball* o : uni) {
+            if (o->id == b->id) continue;
+            const bool inside = b->sensor_balls.contains(o->id);
+            const double d[3] = {b->pos[0] - o->pos[0], b->pos[1] - o->pos[1], b->pos[2] - o->pos[2]};
+            const double d2 = lensq(d);
+            const double ck = (double)f32((double)f32((double)b->sensor_range + (double)f32(o->radius)) +
+                                          (double)f32(b->radius));
+            if (d2 > ck * ck) {
+                if (inside) {
+                    b->sensor_balls.erase(o->id);
+                    snprintf(buf, sizeof buf, " %lld:%lld:0", (long long)b->id, (long long)o->id);
+                    events += buf;
+                }
+            } else if (!inside) {
+                b->sensor_balls.insert(o->id);
+                snprintf(buf, sizeof buf, " %lld:%lld:1", (long long)b->id, (long long)o->id);
+                events += buf;
+            }
+            if (!b->sensor_active) break;
+        }
+    }
+    std::string handle_proximities() {
+        std::string events;
+        const std::vector<int64_t> keys = proximity.order;
+        for (int64_t id : keys) {
+            Ball* b = ball(id);
+            if (!b) continue;
+            if (in_dead_bubble(b)) {
+                if (!b->sensor_balls.order.empty()) {
+                    b->sensor_elapsed = b->sensor_period;
+                    if (b->sensor_active) check_sensor(b, events);
+                }
+                b->sensor_balls.order.clear();
+                continue;
+            }
+            if (!b->has_proximity) continue;
+            if (b->sensor_active) check_sensor(b, events);
+        }
+        return events;
+    }
+
     // ---- the state, as text ----
     std::string state() const {
         std::string out;
@@ -617,8 +750,31 @@ struct World {
             snprintf(buf, sizeof buf, " %zu", levels[i].size());
             out += buf;
         }
-        snprintf(buf, sizeof buf, "\nF %d %lld %d\n", free_boxes, (long long)bubble_id, undefined ? 1 : 0);
+        bool overflow = proximity.overflow;
+        for (const Ball* b : order) overflow = overflow || b->sensor_balls.overflow;
+        snprintf(buf, sizeof buf, "\nF %d %lld %d\n", free_boxes, (long long)bubble_id, (undefined || overflow) ? 1 : 0);
         out += buf;
+        if (!proximity.order.empty()) {
+            out += "P";
+            for (int64_t id : proximity.order) {
+                snprintf(buf, sizeof buf, " %lld", (long long)id);
+                out += buf;
+            }
+            out += "\n";
+        }
+        for (const Ball* b : order) {
+            if (!b->sensor_active && b->sensor_balls.order.empty()) continue;
+            uint64_t bits;
+            std::memcpy(&bits, &b->sensor_elapsed, 8);
+            snprintf(buf, sizeof buf, "S %lld %d %016llx", (long long)b->id, b->sensor_active ? 1 : 0,
+                     (unsigned long long)bits);
+            out += buf;
+            for (int64_t id : b->sensor_balls.order) {
+                snprintf(buf, sizeof buf, " %lld", (long long)id);
+                out += buf;
+            }
+            out += "\n";
+        }
         std::vector<std::pair<int64_t, const Ordered<int>*>> bs;
         for (auto& kv : bubbles.items) bs.emplace_back(kv.first, &kv.second);
         std::sort(bs.begin(), bs.end(), [](auto& a, auto& b) { return a.first < b.first; });
@@ -658,7 +814,9 @@ extern "C" {
 // 10 the cloak attribute (id, value); the queries, their answer after the state: 11 CheckVisibility (src, dst),
 // 12 GetBallIdsInRange from a ball (id, range, include cloaked, with distances), 13 the same from a point (x, y, z,
 // range, include cloaked, with distances), 14 GetBubbleAtCoordinates (x, y, z), 15 GetNearbyBalls (id, exclude fixed,
-// exclude inert, exclude cloaked). AddBall's sixteenth value is its massive flag.
+// exclude inert, exclude cloaked); 16 AddProximitySensor (id, range, period, only interactives; no shuffle), 17
+// RemoveProximitySensor (id), 18 HandleProximities (the answer: each DoProximity event, ball:other:entered). AddBall's
+// sixteenth value is its massive flag.
 int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double friction, double dt, char* out,
                          int64_t cap) {
     space_oracle::World w;
@@ -703,6 +861,9 @@ int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double fr
                 }
                 break;
             }
+            case 16: w.add_sensor(id, o[2], o[3], o[4] != 0.0); break;
+            case 17: w.remove_sensor(id); break;
+            case 18: answer = "Q" + w.handle_proximities() + "\n"; break;
             case 15: {
                 space_oracle::Ball* b = w.ball(id);
                 answer = "Q";

@@ -24,6 +24,7 @@ GOLDEN = Path(__file__).resolve().parent
 STRIDE = 16
 ADD, POS, RADIUS, MAXVEL, REMOVE, INIT, COPY, INTERACTIVE, KEEPALIVE = range(1, 10)
 CLOAKED, VISIBILITY, RANGE_BALL, RANGE_POINT, BUBBLE_AT, NEARBY = range(10, 16)
+SENSOR, UNSENSOR, PROXIMITIES = range(16, 19)
 TOP = 7864320.0                                           # a top box's width (m)
 
 
@@ -80,6 +81,14 @@ def ops_for(seed: int, n_ops: int = 60) -> list:
                 ops.append(_op(BUBBLE_AT, 0, *where()))
         elif k < 0.43 and live:
             ops.append(_op(CLOAKED, r.choice(live), r.choice((0.0, 1.0, 2.0, 200.0))))
+        elif k < 0.47 and live:                            # a proximity sensor on, or off
+            if r.random() < 0.8:
+                ops.append(_op(SENSOR, r.choice(live), r.choice((100.0, 3e4, 1e6, 5e6, -1e7)), r.choice((0.5, 1.0, 3.0)),
+                               float(r.random() < 0.3)))
+            else:
+                ops.append(_op(UNSENSOR, r.choice(live)))
+        elif k < 0.53:
+            ops.append(_op(PROXIMITIES))
         elif k < 0.55:
             ops.append(_op(POS, r.choice(live), *where()))
         elif k < 0.62:
@@ -153,6 +162,14 @@ def apply(park, op: list) -> str:
         b = park.balls.get(bid)
         got = [] if b is None else park._nearby_balls(b, bool(a[0]), bool(a[1]), False, bool(a[2]), False)
         return "Q" + "".join(f" {o.id}" for o in got) + "\n"
+    elif code == SENSOR:
+        park.add_proximity_sensor(bid, a[0], a[1], 0, bool(a[2]))
+    elif code == UNSENSOR:
+        park.remove_proximity_sensor(bid)
+    elif code == PROXIMITIES:
+        park.events = []
+        park._handle_proximities()
+        return "Q" + "".join(f" {e[2]}:{e[3]}:{e[4]}" for e in park.events if e[1] == "DoProximity") + "\n"
     if code == ADD:
         park.add_ball(bid, a[0], a[1], a[2], is_free=bool(a[3]), is_interactive=bool(a[4]), x=a[5], y=a[6], z=a[7],
                       vx=a[8], vy=a[9], vz=a[10], agility=a[11], speed_fraction=a[12], is_massive=bool(a[13]))
@@ -190,6 +207,14 @@ def state_text(park) -> str:
         out.append(head + "".join(f" {k[0]},{k[1]},{k[2]}" for k in sorted(b.boxes)) + "\n")
     out.append("L" + "".join(f" {len(lv)}" for lv in park.levels) + "\n")
     out.append(f"F {park.free_boxes} {park.bubble_id} 0\n")
+    if len(park.proximity_balls):
+        out.append("P" + "".join(f" {i}" for i in park.proximity_balls.keys()) + "\n")
+    for bid in sorted(park.balls):
+        b = park.balls[bid]
+        if not b.sensor_active and len(b.sensor_balls) == 0:
+            continue
+        out.append(f"S {b.id} {int(b.sensor_active)} {_bits(b.sensor_elapsed)}"
+                   + "".join(f" {i}" for i in b.sensor_balls.keys()) + "\n")
     for bub in sorted(park.bubbles):
         out.append(f"U {bub}" + "".join(f" {k}:{v}" for k, v in park.bubbles[bub].items()) + "\n")
     for tag, m in (("I", park.bubble_interactives), ("K", park.bubble_keep_alives)):

@@ -2,8 +2,9 @@
 digests recorded on the reference's own SpaceBallpark (tests/golden/space_trace.py): 72 worlds (balls added near
 top-box faces and corners, moved across top boxes, resized up to huge, removed and re-added, made interactive, kept
 alive, cloaked; InitializeBubbles and CopyBubbles; sweeps past BoxAllocator's 256 kept boxes; the queries
-GetNearbyBalls, CheckVisibility, GetBallIdsInRange from a ball or a point, GetBubbleAtCoordinates), every state and
-every answer after every operation. The first slice of the space layer: its kernel is built on this oracle."""
+GetNearbyBalls, CheckVisibility, GetBallIdsInRange from a ball or a point, GetBubbleAtCoordinates; proximity sensors
+added and removed, HandleProximities with its DoProximity events in the unordered maps' order), every state and every
+answer after every operation. The first slice of the space layer: its kernel is built on this oracle."""
 
 import numpy as np
 
@@ -40,6 +41,9 @@ def test_the_streams_reach_the_partitions_paths():
     assert sum(1 for a in answers if len(a.split()) > 2) > 50         # answers listing several balls
     assert any(":" in a for a in answers) and any(a == "Q None" for a in answers)
     assert any(a.split()[1:] and a.split()[1].isdigit() and int(a.split()[1]) > 0 for a in answers if len(a.split()) == 2)
+    events = [e for a in answers for e in a.split()[1:] if e.count(":") == 2]
+    assert sum(e.endswith(":1") for e in events) > 100 and sum(e.endswith(":0") for e in events) > 10
+    assert any(line.startswith("S ") and len(line.split()) > 5 for t in texts for line in t.splitlines())
 
 
 def test_a_planted_fault_in_the_operations_is_seen():
