@@ -12,8 +12,8 @@
 // reference's insertion orders; the queries (GetNearbyBalls' walk, CheckVisibility, GetBallIdsInRange,
 // GetBubbleAtCoordinates) read them; the proximity sensors (AddProximitySensor, HandleProximities: the candidates of
 // GetNearbyBalls with the inflated radius, the ball re-filed twice, enter and leave in the unordered maps' order).
-// Notification ranges, target tracking, a shuffled sensor's first period, collisions, modes and the tick are not in
-// this slice.
+// Notification ranges (in GOTO), target tracking and a shuffled sensor's first period (glibc's rand) too. The follow
+// modes, collisions and the tick are not in this slice.
 
 #include <algorithm>
 #include <array>
@@ -100,6 +100,35 @@ struct HashOrder {
     }
 };
 
+// glibc's rand() after srand(seed) (random_r's TYPE_3: degree 31, separation 3; glibc's published algorithm): a
+// shuffled sensor's first period (floatrand, Ball.cpp:19)
+struct GlibcRand {
+    int32_t t[31];
+    int f = 3, r = 0;
+    explicit GlibcRand(uint32_t seed) {
+        int32_t word = (int32_t)(seed == 0 ? 1u : seed);
+        t[0] = word;
+        for (int i = 1; i < 31; ++i) {
+            const int32_t hi = word / 127773, lo = word % 127773;
+            word = 16807 * lo - 2836 * hi;
+            if (word < 0) word += 2147483647;
+            t[i] = word;
+        }
+        for (int i = 0; i < 310; ++i) next();
+    }
+    int32_t next() {
+        const uint32_t val = (uint32_t)t[f] + (uint32_t)t[r];
+        t[f] = (int32_t)val;
+        if (++f >= 31) {
+            f = 0;
+            ++r;
+        } else if (++r >= 31) {
+            r = 0;
+        }
+        return (int32_t)(val >> 1);
+    }
+};
+
 struct Ball;
 
 struct Box {
@@ -123,6 +152,11 @@ struct Ball {
     float sensor_range = 0.0f;
     double sensor_period = 2.0, sensor_elapsed = 0.0;
     HashOrder sensor_balls;
+    int mode = 2;                                          // STOP; GOTO is 0
+    double goto_pt[3] = {0.0, 0.0, 0.0};
+    double notification_range = 0.0, tracking_range = 0.0;
+    bool within_range = false, within_tracking = false;
+    Ball* tracking = nullptr;                              // mTrackingPtr: the ball itself, which may outlive removal
     int64_t bubble = -1, old_bubble = -1;
     std::map<Key, Box*> boxes;
     Box* my_box = nullptr;
@@ -144,6 +178,8 @@ struct World {
     int64_t bubble_id = 0;
     bool undefined = false;
     HashOrder proximity;                                   // mProximityBalls
+    std::vector<std::unique_ptr<Ball>> removed;            // removed balls a tracking pointer may still read
+    GlibcRand rng{1};
 
     Ball* ball(int64_t id) {
         auto* p = balls.find(id);
@@ -452,6 +488,8 @@ struct World {
         b->bubble = -1;
         add_to_bubble(b);
         if (b->has_proximity) proximity.erase(id);
+        for (auto& kv : balls.items)
+            if (kv.first == id) removed.push_back(std::move(kv.second));
         balls.erase(id);
     }
     void set_interactive(int64_t id, bool flag) {
@@ -624,13 +662,13 @@ struct World {
 
     // ---- proximity sensors (space.py:1345-1523; SEN-701, SEN-702; no notification range or tracking here) ----
     void update_proximity_status(Ball* b) {
-        b->has_proximity = b->sensor_active;
+        b->has_proximity = b->tracking_range != 0.0 || b->notification_range != 0.0 || b->sensor_active;
         if (b->has_proximity)
             proximity.insert(b->id);
         else
             proximity.erase(b->id);
     }
-    void add_sensor(int64_t id, double range, double period, bool only_interactives) {
+    void add_sensor(int64_t id, double range, double period, bool only_interactives, bool shuffle) {
         Ball* b = ball(id);
         if (!b) return;
         const float r = f32(range);
@@ -640,7 +678,87 @@ struct World {
         b->sensor_period = period;
         b->sensor_active = true;
         b->sensor_only_interactives = only_interactives;
+        if (shuffle) b->sensor_elapsed = 0.0 + (double)rng.next() / 2147483647.0 * (b->sensor_period - 0.0);
         update_proximity_status(b);
+    }
+    void set_notification_range(int64_t id, double n) {
+        Ball* b = ball(id);
+        if (!b || n < 0.0) return;
+        b->notification_range = n;
+        update_proximity_status(b);
+        b->within_range = false;
+    }
+    void set_target_tracking(int64_t id, int64_t target, double range) {
+        Ball* b = ball(id);
+        if (!b) return;
+        if (range <= 0.0 || target == 0) {
+            b->tracking = nullptr;
+            b->tracking_range = 0.0;
+            return;
+        }
+        Ball* t = ball(target);
+        if (!t) return;
+        b->tracking = t;
+        b->tracking_range = range;
+        update_proximity_status(b);
+        b->within_tracking = false;
+    }
+    void stop(int64_t id) {
+        Ball* b = ball(id);
+        if (b && b->mode != 2) b->mode = 2;
+    }
+    void goto_point(int64_t id, const double* p) {
+        Ball* b = ball(id);
+        if (!b || !std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) return;
+        b->mode = 2;
+        for (int i = 0; i < 3; ++i) b->goto_pt[i] = p[i];
+        if (b->speed_fraction == 0.0) b->speed_fraction = 1.0;
+        b->mode = 0;
+    }
+    void check_notification_range(Ball* b, std::string& events) {
+        char buf[64];
+        bool send = false, inside = false;
+        if (b->notification_range != 0.0) {
+            if (b->mode == 0) {                            // GOTO (the follow modes are not in this slice)
+                const double lim = b->notification_range + b->radius;
+                const double d[3] = {b->pos[0] - b->goto_pt[0], b->pos[1] - b->goto_pt[1], b->pos[2] - b->goto_pt[2]};
+                inside = lensq(d) < lim * lim;
+            }
+            if (inside) {
+                if (!b->within_range) send = b->within_range = true;
+            } else if (b->within_range) {
+                send = true;
+                b->within_range = false;
+            }
+        }
+        if (send) {
+            snprintf(buf, sizeof buf, " R%lld:%d", (long long)b->id, b->within_range ? 1 : 0);
+            events += buf;
+        }
+    }
+    void check_target_tracking(Ball* b, std::string& events) {
+        char buf[64];
+        bool send = false;
+        if (b->tracking_range >= 0.00001 && b->tracking) {
+            const double d[3] = {b->pos[0] - b->tracking->pos[0], b->pos[1] - b->tracking->pos[1],
+                                 b->pos[2] - b->tracking->pos[2]};
+            const double lim = b->tracking_range + b->radius;
+            if (lensq(d) < lim * lim) {
+                if (!b->within_tracking) send = b->within_tracking = true;
+            } else if (b->within_tracking) {
+                send = true;
+                b->within_tracking = false;
+            }
+        }
+        if (send) {
+            snprintf(buf, sizeof buf, " T%lld:%d", (long long)b->id, b->within_tracking ? 1 : 0);
+            events += buf;
+        }
+    }
+    void check_for_proximity(Ball* b, std::string& events) {
+        check_notification_range(b, events);
+        check_target_tracking(b, events);
+        if (b->sensor_active) check_sensor(b, events);
     }
     void remove_sensor(int64_t id) {
         Ball* b = ball(id);
@@ -708,13 +826,13 @@ struct World {
             if (in_dead_bubble(b)) {
                 if (!b->sensor_balls.order.empty()) {
                     b->sensor_elapsed = b->sensor_period;
-                    if (b->sensor_active) check_sensor(b, events);
+                    check_for_proximity(b, events);
                 }
                 b->sensor_balls.order.clear();
                 continue;
             }
             if (!b->has_proximity) continue;
-            if (b->sensor_active) check_sensor(b, events);
+            check_for_proximity(b, events);
         }
         return events;
     }
@@ -763,11 +881,12 @@ struct World {
             out += "\n";
         }
         for (const Ball* b : order) {
-            if (!b->sensor_active && b->sensor_balls.order.empty()) continue;
+            if (!b->sensor_active && b->sensor_balls.order.empty() && !b->has_proximity) continue;
             uint64_t bits;
             std::memcpy(&bits, &b->sensor_elapsed, 8);
-            snprintf(buf, sizeof buf, "S %lld %d %016llx", (long long)b->id, b->sensor_active ? 1 : 0,
-                     (unsigned long long)bits);
+            snprintf(buf, sizeof buf, "S %lld %d %016llx %d %d %d %lld", (long long)b->id, b->sensor_active ? 1 : 0,
+                     (unsigned long long)bits, b->has_proximity ? 1 : 0, b->within_range ? 1 : 0,
+                     b->within_tracking ? 1 : 0, (long long)(b->tracking ? b->tracking->id : 0));
             out += buf;
             for (int64_t id : b->sensor_balls.order) {
                 snprintf(buf, sizeof buf, " %lld", (long long)id);
@@ -814,14 +933,17 @@ extern "C" {
 // 10 the cloak attribute (id, value); the queries, their answer after the state: 11 CheckVisibility (src, dst),
 // 12 GetBallIdsInRange from a ball (id, range, include cloaked, with distances), 13 the same from a point (x, y, z,
 // range, include cloaked, with distances), 14 GetBubbleAtCoordinates (x, y, z), 15 GetNearbyBalls (id, exclude fixed,
-// exclude inert, exclude cloaked); 16 AddProximitySensor (id, range, period, only interactives; no shuffle), 17
-// RemoveProximitySensor (id), 18 HandleProximities (the answer: each DoProximity event, ball:other:entered). AddBall's
-// sixteenth value is its massive flag.
-int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double friction, double dt, char* out,
-                         int64_t cap) {
+// exclude inert, exclude cloaked); 16 AddProximitySensor (id, range, period, only interactives, shuffle), 17
+// RemoveProximitySensor (id), 18 HandleProximities (the answer: each DoProximity event ball:other:entered, DoRange
+// R<ball>:<inside>, DoTargetTracking T<ball>:<inside>), 19 SetNotificationRange (id, range), 20 SetTargetTracking (id,
+// target, range), 21 GotoPoint (id, x, y, z), 22 Stop (id). AddBall's sixteenth value is its massive flag. `seed` is the
+// world's srand seed.
+int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double friction, double dt, int64_t seed,
+                         char* out, int64_t cap) {
     space_oracle::World w;
     w.friction = friction;
     w.dt = dt;
+    w.rng = space_oracle::GlibcRand((uint32_t)seed);
     std::string all;
     char buf[64];
     for (int64_t i = 0; i < n; ++i) {
@@ -861,7 +983,11 @@ int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double fr
                 }
                 break;
             }
-            case 16: w.add_sensor(id, o[2], o[3], o[4] != 0.0); break;
+            case 16: w.add_sensor(id, o[2], o[3], o[4] != 0.0, o[5] != 0.0); break;
+            case 19: w.set_notification_range(id, o[2]); break;
+            case 20: w.set_target_tracking(id, (int64_t)o[2], o[3]); break;
+            case 21: w.goto_point(id, o + 2); break;
+            case 22: w.stop(id); break;
             case 17: w.remove_sensor(id); break;
             case 18: answer = "Q" + w.handle_proximities() + "\n"; break;
             case 15: {

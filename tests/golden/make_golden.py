@@ -609,7 +609,7 @@ def make_space_bubbles() -> None:
                + [("long", s, sp.ops_for(s, n_ops=600)) for s in range(1000, 1006)]
                + [("sweep", s, sp.sweep_ops(s)) for s in range(1, 7)])
     for family, seed, ops in streams:
-        park = SpaceBallpark(1.0e6, 1000, is_master=True)
+        park = SpaceBallpark(1.0e6, 1000, is_master=True, seed=seed)
         digests = []
         try:
             for op in ops:
@@ -618,7 +618,7 @@ def make_space_bubbles() -> None:
         except DestinyUndefined:
             dropped += 1
             continue
-        scenarios.append({"seed": f"{family}-{seed}", "ops": ops, "digests": digests})
+        scenarios.append({"seed": f"{family}-{seed}", "ops": ops, "digests": digests, "rand_seed": seed})
     sp.save(HERE / "space_bubbles", scenarios)
     print(f"  space_bubbles: {len(scenarios)} worlds, {sum(len(s['ops']) for s in scenarios)} operations, "
           f"{dropped} left out, {time.time() - t0:.0f} s", flush=True)

@@ -24,7 +24,7 @@ GOLDEN = Path(__file__).resolve().parent
 STRIDE = 16
 ADD, POS, RADIUS, MAXVEL, REMOVE, INIT, COPY, INTERACTIVE, KEEPALIVE = range(1, 10)
 CLOAKED, VISIBILITY, RANGE_BALL, RANGE_POINT, BUBBLE_AT, NEARBY = range(10, 16)
-SENSOR, UNSENSOR, PROXIMITIES = range(16, 19)
+SENSOR, UNSENSOR, PROXIMITIES, NOTIFY, TRACK, GOTO, STOP = range(16, 23)
 TOP = 7864320.0                                           # a top box's width (m)
 
 
@@ -61,7 +61,7 @@ def ops_for(seed: int, n_ops: int = 60) -> list:
             b = r.choice(free)
             vel = [r.uniform(-300.0, 300.0) for _ in range(3)] if r.random() < 0.6 else [0.0, 0.0, 0.0]
             ops.append(_op(ADD, b, 10 ** r.uniform(5.0, 9.0), radius(), r.uniform(0.0, 3000.0),
-                           1.0 if r.random() < 0.8 else 0.0, 1.0 if r.random() < 0.6 else 0.0, *where(), *vel,
+                           1.0 if r.random() < 0.8 else 0.0, 1.0 if r.random() < 0.75 else 0.0, *where(), *vel,
                            r.uniform(0.05, 3.0), r.choice((0.0, 0.5, 1.0)), 1.0 if r.random() < 0.7 else 0.0))
             live.append(b)
         elif k < 0.4 and live:                             # a query
@@ -84,9 +84,22 @@ def ops_for(seed: int, n_ops: int = 60) -> list:
         elif k < 0.47 and live:                            # a proximity sensor on, or off
             if r.random() < 0.8:
                 ops.append(_op(SENSOR, r.choice(live), r.choice((100.0, 3e4, 1e6, 5e6, -1e7)), r.choice((0.5, 1.0, 3.0)),
-                               float(r.random() < 0.3)))
+                               float(r.random() < 0.3), float(r.random() < 0.3)))
             else:
                 ops.append(_op(UNSENSOR, r.choice(live)))
+        elif k < 0.49 and live:                            # a notification range, a tracked target, a goto, a stop
+            q, a = r.random(), r.choice(live)
+            if q < 0.3:
+                if r.random() < 0.6:
+                    ops.append(_op(GOTO, a, *where()))
+                ops.append(_op(NOTIFY, a, r.choice((0.0, 500.0, 5e4, 1e7, 1e7, -1.0))))
+            elif q < 0.6:
+                target = r.choice(live) if r.random() < 0.85 else r.choice(ids + [0])
+                ops.append(_op(TRACK, a, target, r.choice((0.0, 1e3, 1e5, 1e7, 1e7))))
+            elif q < 0.85:
+                ops.append(_op(GOTO, a, *where()))
+            else:
+                ops.append(_op(STOP, a))
         elif k < 0.53:
             ops.append(_op(PROXIMITIES))
         elif k < 0.55:
@@ -163,13 +176,29 @@ def apply(park, op: list) -> str:
         got = [] if b is None else park._nearby_balls(b, bool(a[0]), bool(a[1]), False, bool(a[2]), False)
         return "Q" + "".join(f" {o.id}" for o in got) + "\n"
     elif code == SENSOR:
-        park.add_proximity_sensor(bid, a[0], a[1], 0, bool(a[2]))
+        park.add_proximity_sensor(bid, a[0], a[1], int(a[3]), bool(a[2]))
+    elif code == NOTIFY:
+        park.set_notification_range(bid, a[0])
+    elif code == TRACK:
+        park.set_target_tracking(bid, int(a[0]), a[1])
+    elif code == GOTO:
+        park.goto_point(bid, a[0], a[1], a[2])
+    elif code == STOP:
+        park.stop(bid)
     elif code == UNSENSOR:
         park.remove_proximity_sensor(bid)
     elif code == PROXIMITIES:
         park.events = []
         park._handle_proximities()
-        return "Q" + "".join(f" {e[2]}:{e[3]}:{e[4]}" for e in park.events if e[1] == "DoProximity") + "\n"
+        out = []
+        for e in park.events:
+            if e[1] == "DoProximity":
+                out.append(f" {e[2]}:{e[3]}:{e[4]}")
+            elif e[1] == "DoRange":
+                out.append(f" R{e[2]}:{e[3]}")
+            elif e[1] == "DoTargetTracking":
+                out.append(f" T{e[2]}:{e[3]}")
+        return "Q" + "".join(out) + "\n"
     if code == ADD:
         park.add_ball(bid, a[0], a[1], a[2], is_free=bool(a[3]), is_interactive=bool(a[4]), x=a[5], y=a[6], z=a[7],
                       vx=a[8], vy=a[9], vz=a[10], agility=a[11], speed_fraction=a[12], is_massive=bool(a[13]))
@@ -211,9 +240,11 @@ def state_text(park) -> str:
         out.append("P" + "".join(f" {i}" for i in park.proximity_balls.keys()) + "\n")
     for bid in sorted(park.balls):
         b = park.balls[bid]
-        if not b.sensor_active and len(b.sensor_balls) == 0:
+        if not b.sensor_active and len(b.sensor_balls) == 0 and not b.has_proximity:
             continue
-        out.append(f"S {b.id} {int(b.sensor_active)} {_bits(b.sensor_elapsed)}"
+        tracked = b.tracking_ptr.id if b.tracking_ptr is not None else 0
+        out.append(f"S {b.id} {int(b.sensor_active)} {_bits(b.sensor_elapsed)} {int(b.has_proximity)} "
+                   f"{int(b.within_range)} {int(b.within_tracking_range)} {tracked}"
                    + "".join(f" {i}" for i in b.sensor_balls.keys()) + "\n")
     for bub in sorted(park.bubbles):
         out.append(f"U {bub}" + "".join(f" {k}:{v}" for k, v in park.bubbles[bub].items()) + "\n")
@@ -229,7 +260,8 @@ def digest(text: str) -> np.uint64:
 
 def save(path: Path, scenarios: list) -> None:
     """scenarios: [{"seed", "ops" [n][STRIDE], "digests" [n] uint64}], as one compressed archive."""
-    arrays = {"names": np.array([s["seed"] for s in scenarios])}
+    arrays = {"names": np.array([s["seed"] for s in scenarios]),
+              "rand_seeds": np.array([s.get("rand_seed", 1) for s in scenarios], dtype=np.int64)}
     for i, sc in enumerate(scenarios):
         arrays[f"ops{i}"] = np.array(sc["ops"], dtype=np.float64)
         arrays[f"digests{i}"] = np.array(sc["digests"], dtype=np.uint64)
@@ -238,4 +270,5 @@ def save(path: Path, scenarios: list) -> None:
 
 def load(path: Path) -> list:
     z = np.load(str(path) + ".npz")
-    return [{"seed": str(name), "ops": z[f"ops{i}"], "digests": z[f"digests{i}"]} for i, name in enumerate(z["names"])]
+    return [{"seed": str(name), "ops": z[f"ops{i}"], "digests": z[f"digests{i}"], "rand_seed": int(z["rand_seeds"][i])}
+            for i, name in enumerate(z["names"])]

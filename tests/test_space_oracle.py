@@ -3,8 +3,9 @@ digests recorded on the reference's own SpaceBallpark (tests/golden/space_trace.
 top-box faces and corners, moved across top boxes, resized up to huge, removed and re-added, made interactive, kept
 alive, cloaked; InitializeBubbles and CopyBubbles; sweeps past BoxAllocator's 256 kept boxes; the queries
 GetNearbyBalls, CheckVisibility, GetBallIdsInRange from a ball or a point, GetBubbleAtCoordinates; proximity sensors
-added and removed, HandleProximities with its DoProximity events in the unordered maps' order), every state and every
-answer after every operation. The first slice of the space layer: its kernel is built on this oracle."""
+added (shuffled ones too, from the world's glibc rand) and removed, notification ranges in GOTO, tracked targets,
+HandleProximities with its DoProximity, DoRange and DoTargetTracking events in the unordered maps' order), every state
+and every answer after every operation. The first slice of the space layer: its kernel is built on this oracle."""
 
 import numpy as np
 
@@ -19,7 +20,7 @@ def _scenarios():
 def test_the_oracle_matches_the_references_partition_and_bubbles_after_every_operation():
     bad = []
     for sc in _scenarios():
-        got = np.array([sp.digest(t) for t in space_world.run(sc["ops"])], dtype=np.uint64)
+        got = np.array([sp.digest(t) for t in space_world.run(sc["ops"], seed=sc["rand_seed"])], dtype=np.uint64)
         if got.shape != sc["digests"].shape or not (got == sc["digests"]).all():
             first = int(np.nonzero(got != sc["digests"])[0][0]) if got.shape == sc["digests"].shape else -1
             bad.append((sc["seed"], first))
@@ -27,7 +28,7 @@ def test_the_oracle_matches_the_references_partition_and_bubbles_after_every_ope
 
 
 def test_the_streams_reach_the_partitions_paths():
-    texts = [t for sc in _scenarios() for t in space_world.run(sc["ops"])]
+    texts = [t for sc in _scenarios() for t in space_world.run(sc["ops"], seed=sc["rand_seed"])]
     kept = max(int(line.split()[1]) for t in texts for line in t.splitlines() if line.startswith("F "))
     assert kept == 256                                     # BoxAllocator full: later releases delete
     huge = sum(1 for t in texts for line in t.splitlines()
@@ -43,7 +44,9 @@ def test_the_streams_reach_the_partitions_paths():
     assert any(a.split()[1:] and a.split()[1].isdigit() and int(a.split()[1]) > 0 for a in answers if len(a.split()) == 2)
     events = [e for a in answers for e in a.split()[1:] if e.count(":") == 2]
     assert sum(e.endswith(":1") for e in events) > 100 and sum(e.endswith(":0") for e in events) > 10
-    assert any(line.startswith("S ") and len(line.split()) > 5 for t in texts for line in t.splitlines())
+    assert any(line.startswith("S ") and len(line.split()) > 9 for t in texts for line in t.splitlines())
+    assert any(e.startswith("R") for a in answers for e in a.split()[1:])
+    assert any(e.startswith("T") for a in answers for e in a.split()[1:])
 
 
 def test_a_planted_fault_in_the_operations_is_seen():
@@ -51,5 +54,5 @@ def test_a_planted_fault_in_the_operations_is_seen():
     ops = sc["ops"].copy()
     k = next(i for i in range(len(ops)) if int(ops[i, 0]) == sp.ADD)
     ops[k, 7] += sp.TOP                                    # one ball added a top box further along x
-    got = np.array([sp.digest(t) for t in space_world.run(ops)], dtype=np.uint64)
+    got = np.array([sp.digest(t) for t in space_world.run(ops, seed=sc["rand_seed"])], dtype=np.uint64)
     assert not (got == sc["digests"]).all()
