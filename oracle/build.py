@@ -10,7 +10,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 SOURCES = ("oracle_libm.cpp", "flight.cpp", "collide.cpp", "space.cpp")
-DEPS = ("../exact_ballpark_b200/csrc/ebb_libm.cuh", "../exact_ballpark_b200/csrc/ebb_arith.cuh",
+DEPS = ("flight_state.h", "../exact_ballpark_b200/csrc/ebb_libm.cuh", "../exact_ballpark_b200/csrc/ebb_arith.cuh",
         "../exact_ballpark_b200/csrc/ebb_libm_tables.h")
 
 

@@ -29,6 +29,8 @@
 
 #include "../exact_ballpark_b200/csrc/ebb_libm.cuh"
 
+#include "flight_state.h"
+
 namespace {
 
 namespace lm = ebb::lm;
@@ -1220,19 +1222,7 @@ struct Tick {
 
 extern "C" {
 
-// The oracle's park, field for field the reference park's tensors (see the file's header for the layout).
-struct OracleFlight {
-    int64_t n;
-    double friction, dt;
-    float ffriction, fdt;
-    int32_t new_orbit, dynamical;
-    double *pos, *vel, *old_pos, *old_vel, *goto_, *last_g;
-    double *mass, *time_factor, *last_collision;
-    double *radius, *max_vel, *agility, *speed_fraction, *follow_range, *max_ang_vel, *rot_agility, *rot_roll;
-    double *rot, *old_rot, *ang_vel, *old_ang_vel, *torque;
-    int64_t *ids, *world, *mode, *effect_stamp, *follow_id, *owner_id, *follow_ptr, *clock;
-    uint8_t *free_, *moribund, *massive, *interactive, *sensor;
-};
+// The oracle's park: oracle/flight_state.h.
 
 // One tick of every world in place, the worlds shared among `threads` host threads. Returns 0.
 // The combat park's extra state (the Combat structure above, field for field).

@@ -13,7 +13,8 @@
 // GetBubbleAtCoordinates) read them; the proximity sensors (AddProximitySensor, HandleProximities: the candidates of
 // GetNearbyBalls with the inflated radius, the ball re-filed twice, enter and leave in the unordered maps' order).
 // Notification ranges (in GOTO), target tracking and a shuffled sensor's first period (glibc's rand) too. The follow
-// modes, collisions and the tick are not in this slice.
+// modes and collisions are not in this slice; the tick is, for GOTO and STOP (the flight oracle's tick, then the
+// re-filings of the balls that moved, then HandleProximities).
 
 #include <algorithm>
 #include <array>
@@ -27,6 +28,8 @@
 #include <string>
 #include <utility>
 #include <vector>
+
+#include "flight_state.h"
 
 namespace space_oracle {
 
@@ -153,6 +156,7 @@ struct Ball {
     double sensor_period = 2.0, sensor_elapsed = 0.0;
     HashOrder sensor_balls;
     int mode = 2;                                          // STOP; GOTO is 0
+    double old_pos[3] = {0.0, 0.0, 0.0}, old_vel[3] = {0.0, 0.0, 0.0}, last_g[3] = {0.0, 0.0, 0.0};
     double goto_pt[3] = {0.0, 0.0, 0.0};
     double notification_range = 0.0, tracking_range = 0.0;
     bool within_range = false, within_tracking = false;
@@ -449,6 +453,12 @@ struct World {
             b->pos[i] = p[i];
             b->vel[i] = v[i];
         }
+        if (created)
+            for (int i = 0; i < 3; ++i) {
+                b->old_pos[i] = b->pos[i] - b->vel[i] * dt;
+                b->old_vel[i] = b->vel[i];
+            }
+        b->mode = 2;
         b->radius = r < 0.0f ? 0.0 : (double)r;
         b->mass = mass < 0.0 ? 0.0 : mass;
         b->free = free;
@@ -463,7 +473,7 @@ struct World {
     void set_position(int64_t id, const double* p) {
         Ball* b = ball(id);
         if (!b) return;
-        for (int i = 0; i < 3; ++i) b->pos[i] = p[i];
+        for (int i = 0; i < 3; ++i) b->pos[i] = b->old_pos[i] = p[i];
         insert_in_boxes(b);
     }
     void set_radius(int64_t id, double radius) {
@@ -837,6 +847,95 @@ struct World {
         return events;
     }
 
+    // ---- the tick (space.py's ModeBallpark.evolve with SpaceBallpark's hooks, modes.py:702-745) ----
+    // The free balls outside a dead bubble (TIME-714: a dead bubble's balls skip the whole tick) run one flight tick
+    // through the flight oracle (GOTO and STOP here, no collisions: the slice's balls are not massive); each that moved
+    // at least sqrt(0.1) m is re-filed, in ascending id; then HandleProximities.
+    std::string tick() {
+        std::vector<Ball*> order;
+        for (auto& kv : balls.items) order.push_back(kv.second.get());
+        std::sort(order.begin(), order.end(), [](const Ball* a, const Ball* b) { return a->id < b->id; });
+        std::vector<Ball*> live;
+        for (Ball* b : order)
+            if (b->free && !in_dead_bubble(b)) live.push_back(b);
+        const size_t n = live.size();
+        if (n) {
+            std::vector<double> v3[9], v1[12], q4[2];
+            for (auto& v : v3) v.assign(3 * n, 0.0);
+            for (auto& v : v1) v.assign(n, 0.0);
+            for (auto& v : q4) v.assign(4 * n, 0.0);
+            std::vector<int64_t> i64[8];
+            for (auto& v : i64) v.assign(n, 0);
+            std::vector<uint8_t> u8[5];
+            for (auto& v : u8) v.assign(n, 0);
+            enum { POS, VEL, OPOS, OVEL, GOTO_, LASTG, ANG, OANG, TORQUE };
+            enum { MASS, TF, LASTC, RAD, MAXV, AGI, SF, FRANGE, MAXW, ROTAG, ROLL };
+            for (size_t i = 0; i < n; ++i) {
+                const Ball* b = live[i];
+                for (int c = 0; c < 3; ++c) {
+                    v3[POS][3 * i + c] = b->pos[c];
+                    v3[VEL][3 * i + c] = b->vel[c];
+                    v3[OPOS][3 * i + c] = b->old_pos[c];
+                    v3[OVEL][3 * i + c] = b->old_vel[c];
+                    v3[GOTO_][3 * i + c] = b->goto_pt[c];
+                    v3[LASTG][3 * i + c] = b->last_g[c];
+                }
+                q4[0][4 * i + 3] = q4[1][4 * i + 3] = 1.0;
+                v1[MASS][i] = b->mass;
+                v1[TF][i] = b->time_factor;
+                v1[LASTC][i] = -1.0;
+                v1[RAD][i] = b->radius;
+                v1[MAXV][i] = b->max_vel;
+                v1[AGI][i] = b->agility;
+                v1[SF][i] = b->speed_fraction;
+                v1[FRANGE][i] = 10.0;
+                v1[MAXW][i] = 1.0;
+                v1[ROTAG][i] = 0.9;
+                i64[0][i] = b->id;                        // ids; world 0; mode; the follow fields 0 and -1
+                i64[2][i] = b->mode;
+                i64[6][i] = -1;
+                u8[0][i] = 1;                              // free
+                u8[3][i] = b->interactive;
+            }
+            OracleFlight s{};
+            s.n = (int64_t)n;
+            s.friction = friction;
+            s.dt = dt;
+            s.ffriction = (float)friction;
+            s.fdt = (float)dt;
+            s.pos = v3[POS].data(); s.vel = v3[VEL].data(); s.old_pos = v3[OPOS].data(); s.old_vel = v3[OVEL].data();
+            s.goto_ = v3[GOTO_].data(); s.last_g = v3[LASTG].data();
+            s.mass = v1[MASS].data(); s.time_factor = v1[TF].data(); s.last_collision = v1[LASTC].data();
+            s.radius = v1[RAD].data(); s.max_vel = v1[MAXV].data(); s.agility = v1[AGI].data();
+            s.speed_fraction = v1[SF].data(); s.follow_range = v1[FRANGE].data(); s.max_ang_vel = v1[MAXW].data();
+            s.rot_agility = v1[ROTAG].data(); s.rot_roll = v1[ROLL].data();
+            s.rot = q4[0].data(); s.old_rot = q4[1].data();
+            s.ang_vel = v3[ANG].data(); s.old_ang_vel = v3[OANG].data(); s.torque = v3[TORQUE].data();
+            s.ids = i64[0].data(); s.world = i64[1].data(); s.mode = i64[2].data(); s.effect_stamp = i64[3].data();
+            s.follow_id = i64[4].data(); s.owner_id = i64[5].data(); s.follow_ptr = i64[6].data(); s.clock = i64[7].data();
+            s.free_ = u8[0].data(); s.moribund = u8[1].data(); s.massive = u8[2].data(); s.interactive = u8[3].data();
+            s.sensor = u8[4].data();
+            oracle_flight_tick_mt(&s, 1);
+            for (size_t i = 0; i < n; ++i) {
+                Ball* b = live[i];
+                for (int c = 0; c < 3; ++c) {
+                    b->pos[c] = v3[POS][3 * i + c];
+                    b->vel[c] = v3[VEL][3 * i + c];
+                    b->old_pos[c] = v3[OPOS][3 * i + c];
+                    b->old_vel[c] = v3[OVEL][3 * i + c];
+                    b->last_g[c] = v3[LASTG][3 * i + c];
+                }
+                b->mode = (int)i64[2][i];
+                b->speed_fraction = v1[SF][i];
+            }
+        }
+        for (Ball* b : live) {
+            const double d[3] = {b->pos[0] - b->old_pos[0], b->pos[1] - b->old_pos[1], b->pos[2] - b->old_pos[2]};
+            if (!(lensq(d) < 0.1)) insert_in_boxes(b);
+        }
+        return handle_proximities();
+    }
+
     // ---- the state, as text ----
     std::string state() const {
         std::string out;
@@ -936,8 +1035,8 @@ extern "C" {
 // exclude inert, exclude cloaked); 16 AddProximitySensor (id, range, period, only interactives, shuffle), 17
 // RemoveProximitySensor (id), 18 HandleProximities (the answer: each DoProximity event ball:other:entered, DoRange
 // R<ball>:<inside>, DoTargetTracking T<ball>:<inside>), 19 SetNotificationRange (id, range), 20 SetTargetTracking (id,
-// target, range), 21 GotoPoint (id, x, y, z), 22 Stop (id). AddBall's sixteenth value is its massive flag. `seed` is the
-// world's srand seed.
+// target, range), 21 GotoPoint (id, x, y, z), 22 Stop (id), 23 a tick (its answer HandleProximities' events). AddBall's
+// sixteenth value is its massive flag. `seed` is the world's srand seed.
 int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double friction, double dt, int64_t seed,
                          char* out, int64_t cap) {
     space_oracle::World w;
@@ -988,6 +1087,7 @@ int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double fr
             case 20: w.set_target_tracking(id, (int64_t)o[2], o[3]); break;
             case 21: w.goto_point(id, o + 2); break;
             case 22: w.stop(id); break;
+            case 23: answer = "Q" + w.tick() + "\n"; break;
             case 17: w.remove_sensor(id); break;
             case 18: answer = "Q" + w.handle_proximities() + "\n"; break;
             case 15: {

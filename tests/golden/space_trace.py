@@ -24,7 +24,7 @@ GOLDEN = Path(__file__).resolve().parent
 STRIDE = 16
 ADD, POS, RADIUS, MAXVEL, REMOVE, INIT, COPY, INTERACTIVE, KEEPALIVE = range(1, 10)
 CLOAKED, VISIBILITY, RANGE_BALL, RANGE_POINT, BUBBLE_AT, NEARBY = range(10, 16)
-SENSOR, UNSENSOR, PROXIMITIES, NOTIFY, TRACK, GOTO, STOP = range(16, 23)
+SENSOR, UNSENSOR, PROXIMITIES, NOTIFY, TRACK, GOTO, STOP, TICK = range(16, 24)
 TOP = 7864320.0                                           # a top box's width (m)
 
 
@@ -152,6 +152,63 @@ def _bits(x: float) -> str:
     return "%016x" % struct.unpack("<Q", struct.pack("<d", float(x)))[0]
 
 
+def tick_ops(seed: int, n_ops: int = 80) -> list:
+    """A world that ticks: up to 10 non-massive ships near top-box faces (so that they cross top boxes within a few
+    ticks), flying GOTO legs at up to 3 km/s across boxes and bubbles, stopped, moved, with sensors, tracked targets
+    and notification ranges, the bubble partition re-initialised and copied, balls made interactive or not and
+    removed; a tick between most operations."""
+    r = random.Random(f"space-tick-{seed}")
+    centres = [[r.choice((-1.0, 0.0, 1.0)) * TOP + r.uniform(-4e3, 4e3) for _ in range(3)] for _ in range(r.randint(1, 3))]
+    ids, live, ops = list(range(1, 11)), [], []
+
+    def near() -> list:
+        return [x + r.uniform(-6e3, 6e3) for x in r.choice(centres)]
+
+    def add(b: int) -> None:
+        vel = [r.uniform(-300.0, 300.0) for _ in range(3)] if r.random() < 0.6 else [0.0, 0.0, 0.0]
+        ops.append(_op(ADD, b, 10 ** r.uniform(5.0, 9.0), r.choice((r.uniform(5.0, 300.0), r.uniform(300.0, 3e4),
+                                                                     r.uniform(3e4, 1e6))),
+                       r.uniform(50.0, 3000.0), 1.0 if r.random() < 0.9 else 0.0, 1.0 if r.random() < 0.75 else 0.0,
+                       *near(), *vel, r.uniform(0.1, 3.0), r.choice((0.5, 1.0)), 0.0))
+        live.append(b)
+    for b in r.sample(ids, r.randint(3, 8)):
+        add(b)
+    for _ in range(n_ops):
+        k = r.random()
+        free = [b for b in ids if b not in live]
+        a = r.choice(live) if live else None
+        if k < 0.45 or a is None:
+            ops.append(_op(TICK))
+        elif k < 0.6:
+            far = [x + r.choice((-1.0, 1.0)) * r.uniform(1e5, 3e7) for x in near()]
+            ops.append(_op(GOTO, a, *far))
+        elif k < 0.63:
+            ops.append(_op(STOP, a))
+        elif k < 0.7:
+            ops.append(_op(SENSOR, a, r.choice((100.0, 3e4, 1e6)), r.choice((0.5, 1.0, 3.0)), float(r.random() < 0.3),
+                           float(r.random() < 0.3)))
+        elif k < 0.74:
+            ops.append(_op(TRACK, a, r.choice(live), r.choice((1e3, 1e5, 1e7))))
+        elif k < 0.78:
+            ops.append(_op(NOTIFY, a, r.choice((500.0, 5e4, 1e7))))
+        elif k < 0.81:
+            ops.append(_op(POS, a, *near()))
+        elif k < 0.84:
+            ops.append(_op(INIT))
+        elif k < 0.88:
+            ops.append(_op(COPY))
+        elif k < 0.92:
+            ops.append(_op(INTERACTIVE, a, float(r.random() < 0.6)))
+        elif k < 0.95 and free:
+            add(r.choice(free))
+        elif k < 0.97:
+            ops.append(_op(REMOVE, a))
+            live.remove(a)
+        else:
+            ops.append(_op(NEARBY, a, 1.0, 0.0, 0.0))
+    return ops
+
+
 def apply(park, op: list) -> str:
     """One operation on the reference's SpaceBallpark; a query's answer as the oracle writes it ("" for the others)."""
     code, bid = int(op[0]), int(op[1])
@@ -187,9 +244,12 @@ def apply(park, op: list) -> str:
         park.stop(bid)
     elif code == UNSENSOR:
         park.remove_proximity_sensor(bid)
-    elif code == PROXIMITIES:
+    elif code in (PROXIMITIES, TICK):
         park.events = []
-        park._handle_proximities()
+        if code == TICK:
+            park.evolve()
+        else:
+            park._handle_proximities()
         out = []
         for e in park.events:
             if e[1] == "DoProximity":

@@ -1,11 +1,12 @@
 """The CPU oracle of the master's partition and bubble partition of one world (oracle/space.cpp) against the golden
-digests recorded on the reference's own SpaceBallpark (tests/golden/space_trace.py): 72 worlds (balls added near
+digests recorded on the reference's own SpaceBallpark (tests/golden/space_trace.py): 112 worlds (balls added near
 top-box faces and corners, moved across top boxes, resized up to huge, removed and re-added, made interactive, kept
 alive, cloaked; InitializeBubbles and CopyBubbles; sweeps past BoxAllocator's 256 kept boxes; the queries
 GetNearbyBalls, CheckVisibility, GetBallIdsInRange from a ball or a point, GetBubbleAtCoordinates; proximity sensors
 added (shuffled ones too, from the world's glibc rand) and removed, notification ranges in GOTO, tracked targets,
-HandleProximities with its DoProximity, DoRange and DoTargetTracking events in the unordered maps' order), every state
-and every answer after every operation. The first slice of the space layer: its kernel is built on this oracle."""
+HandleProximities with its DoProximity, DoRange and DoTargetTracking events in the unordered maps' order; ticking
+worlds whose ships fly GOTO legs across top boxes and bubbles: the flight tick of the free balls outside dead bubbles,
+the re-filings of the balls that moved, HandleProximities), every state and every answer after every operation. The first slice of the space layer: its kernel is built on this oracle."""
 
 import numpy as np
 
@@ -47,6 +48,8 @@ def test_the_streams_reach_the_partitions_paths():
     assert any(line.startswith("S ") and len(line.split()) > 9 for t in texts for line in t.splitlines())
     assert any(e.startswith("R") for a in answers for e in a.split()[1:])
     assert any(e.startswith("T") for a in answers for e in a.split()[1:])
+    ticking = [sc for sc in _scenarios() if sc["seed"].startswith("tick")]
+    assert len(ticking) == 40 and sum(int((sc["ops"][:, 0] == sp.TICK).sum()) for sc in ticking) > 1000
 
 
 def test_a_planted_fault_in_the_operations_is_seen():
