@@ -12,9 +12,11 @@
 // reference's insertion orders; the queries (GetNearbyBalls' walk, CheckVisibility, GetBallIdsInRange,
 // GetBubbleAtCoordinates) read them; the proximity sensors (AddProximitySensor, HandleProximities: the candidates of
 // GetNearbyBalls with the inflated radius, the ball re-filed twice, enter and leave in the unordered maps' order).
-// Notification ranges (in GOTO), target tracking and a shuffled sensor's first period (glibc's rand) too. The follow
-// modes and collisions are not in this slice; the tick is, for GOTO and STOP (the flight oracle's tick, then the
-// re-filings of the balls that moved, then HandleProximities).
+// Notification ranges (of a goto point or a followed ball), target tracking and a shuffled sensor's first period (glibc's rand) too. The follow
+// modes (FOLLOW, ORBIT, WARP, with the targets' follower sets and StopAllFollowers) and the tick are too: the flight
+// oracle's tick of every ball (a dead bubble's balls marked so that it skips them and others still read them), a warp's
+// drop-out re-filed at its drop-out point, the re-filings of the balls that moved, HandleProximities. Collisions are
+// not in this slice.
 
 #include <algorithm>
 #include <array>
@@ -155,8 +157,12 @@ struct Ball {
     float sensor_range = 0.0f;
     double sensor_period = 2.0, sensor_elapsed = 0.0;
     HashOrder sensor_balls;
-    int mode = 2;                                          // STOP; GOTO is 0
+    int mode = 2;                                          // GOTO 0, FOLLOW 1, STOP 2, WARP 3, ORBIT 4
     double old_pos[3] = {0.0, 0.0, 0.0}, old_vel[3] = {0.0, 0.0, 0.0}, last_g[3] = {0.0, 0.0, 0.0};
+    int64_t follow_ptr = 0, follow_id = 0, owner_id = 0, effect_stamp = 0;   // follow_ptr: the target's id, 0 none
+    float follow_range = 10.0f;
+    double last_collision = -1.0;
+    HashOrder followers;
     double goto_pt[3] = {0.0, 0.0, 0.0};
     double notification_range = 0.0, tracking_range = 0.0;
     bool within_range = false, within_tracking = false;
@@ -184,6 +190,7 @@ struct World {
     HashOrder proximity;                                   // mProximityBalls
     std::vector<std::unique_ptr<Ball>> removed;            // removed balls a tracking pointer may still read
     GlibcRand rng{1};
+    int64_t current_time = 0;
 
     Ball* ball(int64_t id) {
         auto* p = balls.find(id);
@@ -358,6 +365,7 @@ struct World {
         if (it->second.empty()) interactives.erase(it);
     }
     bool in_dead_bubble(const Ball* b) const {
+        if (b->mode == 3) return false;                    // a warping (or aligning) ball never is
         auto i = interactives.find(b->bubble);
         if (i != interactives.end() && !i->second.empty()) return false;
         auto k = keep_alives.find(b->bubble);
@@ -453,11 +461,17 @@ struct World {
             b->pos[i] = p[i];
             b->vel[i] = v[i];
         }
-        if (created)
+        if (created) {
             for (int i = 0; i < 3; ++i) {
                 b->old_pos[i] = b->pos[i] - b->vel[i] * dt;
                 b->old_vel[i] = b->vel[i];
             }
+        } else {                                           // a re-added ball keeps its target pointer and set entry
+            b->effect_stamp = 0;
+            b->owner_id = 0;
+            b->follow_id = 0;
+            b->follow_range = 10.0f;
+        }
         b->mode = 2;
         b->radius = r < 0.0f ? 0.0 : (double)r;
         b->mass = mass < 0.0 ? 0.0 : mass;
@@ -468,6 +482,13 @@ struct World {
         b->agility = ag <= 0.0f ? 1.0 : (double)ag;
         b->speed_fraction = s < 0.0f ? 0.0 : (double)s;
         refresh_time_factor(b);
+        if (!created) {                                    // its own set loses the entries that no longer follow it
+            const std::vector<int64_t> ids = b->followers.order;
+            for (int64_t fid : ids) {
+                const Ball* f = ball(fid);
+                if (!f || f->follow_ptr != b->id) b->followers.erase(fid);
+            }
+        }
         insert_in_boxes(b);
     }
     void set_position(int64_t id, const double* p) {
@@ -493,6 +514,8 @@ struct World {
     void remove_ball(int64_t id) {
         Ball* b = ball(id);
         if (!b) return;
+        stop_ball(b);
+        stop_all_followers(b);
         delete_from_boxes(b);
         b->old_bubble = b->bubble;
         b->bubble = -1;
@@ -713,26 +736,112 @@ struct World {
         update_proximity_status(b);
         b->within_tracking = false;
     }
+    // ---- the modes' commands (modes.py:206-330, 391-426): Stop, GotoPoint, GotoDirection, FollowBall, Orbit, WarpTo,
+    // StopAllFollowers, with the targets' follower sets ----
+    void stop_ball(Ball* b) {                              // Stop(Ball*)
+        if (b->mode == 1 || b->mode == 4) {
+            if (Ball* t = ball(b->follow_ptr)) t->followers.erase(b->id);
+            b->effect_stamp = 0;
+            b->follow_ptr = 0;
+            b->follow_id = 0;
+            b->owner_id = 0;
+            b->follow_range = 0.0f;
+        }
+        b->mode = 2;
+    }
     void stop(int64_t id) {
         Ball* b = ball(id);
-        if (b && b->mode != 2) b->mode = 2;
+        if (b && b->mode != 2) stop_ball(b);
     }
-    void goto_point(int64_t id, const double* p) {
-        Ball* b = ball(id);
-        if (!b || !std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) return;
-        b->mode = 2;
+    void goto_ball(Ball* b, const double* p) {
+        if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) return;
+        stop_ball(b);
         for (int i = 0; i < 3; ++i) b->goto_pt[i] = p[i];
         if (b->speed_fraction == 0.0) b->speed_fraction = 1.0;
         b->mode = 0;
+    }
+    void goto_point(int64_t id, const double* p) {
+        if (Ball* b = ball(id)) goto_ball(b, p);
+    }
+    void goto_direction(Ball* b, const double* d) {
+        if (!std::isfinite(d[0]) || !std::isfinite(d[1]) || !std::isfinite(d[2])) return;
+        double u[3] = {d[0], d[1], d[2]};
+        const double norm = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        if (norm != 0.0) {
+            const double inv = 1.0 / norm;
+            for (double& x : u) x = x * inv;
+        }
+        const double p[3] = {b->pos[0] + u[0] * 1.0e17, b->pos[1] + u[1] * 1.0e17, b->pos[2] + u[2] * 1.0e17};
+        goto_ball(b, p);
+    }
+    void follow(int64_t src, int64_t dst, double range, int mode) {
+        const float rng = f32(range);
+        if (!std::isfinite(rng)) return;
+        Ball* b = ball(src);
+        if (!b || src == dst) return;
+        Ball* t = ball(dst);
+        if (!t || b->bubble != t->bubble || t->cloaked) return;
+        stop_ball(b);
+        b->follow_id = dst;
+        b->follow_ptr = dst;
+        b->follow_range = rng;
+        b->mode = mode;
+        t->followers.insert(b->id);
+    }
+    void warp_to(int64_t id, const double* p, double min_range, int64_t factor) {
+        if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) return;
+        if (min_range < 0.0) min_range = 0.0;
+        if (factor <= 0) factor = 1;
+        Ball* b = ball(id);
+        if (!b) return;
+        const double d[3] = {b->pos[0] - p[0], b->pos[1] - p[1], b->pos[2] - p[2]};
+        if (lensq(d) < 10000000000.0) {                    // within 1e5 m: a GotoPoint
+            goto_ball(b, p);
+            return;
+        }
+        if (b->mode == 3 && b->goto_pt[0] == p[0] && b->goto_pt[1] == p[1] && b->goto_pt[2] == p[2]) return;
+        stop_ball(b);
+        for (int i = 0; i < 3; ++i) b->goto_pt[i] = p[i];
+        b->effect_stamp = -1;
+        b->follow_range = 0.0f;
+        std::memcpy(&b->follow_id, &min_range, 8);
+        b->owner_id = factor;
+        b->mode = 3;
+    }
+    void stop_all_followers(Ball* b) {                     // missiles (none here) and interactive orbiters fly on
+        if (b->followers.order.empty()) return;
+        const std::vector<int64_t> ids = b->followers.order;
+        for (int64_t fid : ids) {
+            Ball* f = ball(fid);
+            if (!f || f->follow_id != b->id || f->follow_ptr != b->id) {
+                b->followers.erase(fid);
+                continue;
+            }
+            if (f->interactive && f->mode == 4) {
+                const double v[3] = {f->vel[0], f->vel[1], f->vel[2]};
+                goto_direction(f, v);
+            } else {
+                stop_ball(f);
+            }
+        }
     }
     void check_notification_range(Ball* b, std::string& events) {
         char buf[64];
         bool send = false, inside = false;
         if (b->notification_range != 0.0) {
-            if (b->mode == 0) {                            // GOTO (the follow modes are not in this slice)
-                const double lim = b->notification_range + b->radius;
+            const double n = b->notification_range;
+            if (b->mode == 0) {                            // GOTO: within the range of the goto point
+                const double lim = n + b->radius;
                 const double d[3] = {b->pos[0] - b->goto_pt[0], b->pos[1] - b->goto_pt[1], b->pos[2] - b->goto_pt[2]};
                 inside = lensq(d) < lim * lim;
+            } else if (b->mode == 1 || b->mode == 4) {     // FOLLOW, ORBIT: within a shell of the range's width
+                const Ball* o = ball(b->follow_ptr);
+                const double d[3] = {b->pos[0] - o->pos[0], b->pos[1] - o->pos[1], b->pos[2] - o->pos[2]};
+                const double len2 = lensq(d);
+                const double hi = o->radius + (double)b->follow_range + n + b->radius;
+                double lo = hi - 2.0 * n;
+                if (lo < 0.0) lo = 0.0;
+                inside = len2 < hi * hi && len2 > lo * lo;
             }
             if (inside) {
                 if (!b->within_range) send = b->within_range = true;
@@ -855,10 +964,20 @@ struct World {
         std::vector<Ball*> order;
         for (auto& kv : balls.items) order.push_back(kv.second.get());
         std::sort(order.begin(), order.end(), [](const Ball* a, const Ball* b) { return a->id < b->id; });
-        std::vector<Ball*> live;
-        for (Ball* b : order)
-            if (b->free && !in_dead_bubble(b)) live.push_back(b);
-        const size_t n = live.size();
+        const size_t n = order.size();
+        std::vector<bool> dead(n, false);
+        std::map<int64_t, int64_t> row_of;
+        for (size_t i = 0; i < n; ++i) {
+            row_of[order[i]->id] = (int64_t)i;
+            dead[i] = order[i]->free && in_dead_bubble(order[i]);    // a dead bubble's balls skip the whole tick
+        }
+        std::vector<int> mode_before(n), warping_before(n);
+        std::vector<int64_t> target_before(n);
+        for (size_t i = 0; i < n; ++i) {
+            mode_before[i] = order[i]->mode;
+            warping_before[i] = order[i]->mode == 3 && order[i]->effect_stamp >= 0;
+            target_before[i] = order[i]->follow_ptr;
+        }
         if (n) {
             std::vector<double> v3[9], v1[12], q4[2];
             for (auto& v : v3) v.assign(3 * n, 0.0);
@@ -870,8 +989,10 @@ struct World {
             for (auto& v : u8) v.assign(n, 0);
             enum { POS, VEL, OPOS, OVEL, GOTO_, LASTG, ANG, OANG, TORQUE };
             enum { MASS, TF, LASTC, RAD, MAXV, AGI, SF, FRANGE, MAXW, ROTAG, ROLL };
+            enum { IDS, WORLD, MODE, STAMP, FID, OWNER, FPTR, CLOCK };
+            enum { FREE, MORIBUND, MASSIVE, INTERACTIVE, SENSOR };
             for (size_t i = 0; i < n; ++i) {
-                const Ball* b = live[i];
+                const Ball* b = order[i];
                 for (int c = 0; c < 3; ++c) {
                     v3[POS][3 * i + c] = b->pos[c];
                     v3[VEL][3 * i + c] = b->vel[c];
@@ -883,19 +1004,27 @@ struct World {
                 q4[0][4 * i + 3] = q4[1][4 * i + 3] = 1.0;
                 v1[MASS][i] = b->mass;
                 v1[TF][i] = b->time_factor;
-                v1[LASTC][i] = -1.0;
+                v1[LASTC][i] = b->last_collision;
                 v1[RAD][i] = b->radius;
                 v1[MAXV][i] = b->max_vel;
                 v1[AGI][i] = b->agility;
                 v1[SF][i] = b->speed_fraction;
-                v1[FRANGE][i] = 10.0;
+                v1[FRANGE][i] = b->follow_range;
                 v1[MAXW][i] = 1.0;
                 v1[ROTAG][i] = 0.9;
-                i64[0][i] = b->id;                        // ids; world 0; mode; the follow fields 0 and -1
-                i64[2][i] = b->mode;
-                i64[6][i] = -1;
-                u8[0][i] = 1;                              // free
-                u8[3][i] = b->interactive;
+                i64[IDS][i] = b->id;
+                i64[MODE][i] = b->mode;
+                i64[STAMP][i] = b->effect_stamp;
+                i64[FID][i] = b->follow_id;
+                i64[OWNER][i] = b->owner_id;
+                auto t = row_of.find(b->follow_ptr);
+                i64[FPTR][i] = (b->follow_ptr != 0 && t != row_of.end()) ? t->second : -1;
+                i64[CLOCK][i] = current_time;
+                u8[FREE][i] = b->free;
+                u8[MORIBUND][i] = dead[i];
+                u8[MASSIVE][i] = b->massive;
+                u8[INTERACTIVE][i] = b->interactive;
+                u8[SENSOR][i] = b->sensor_active;
             }
             OracleFlight s{};
             s.n = (int64_t)n;
@@ -911,29 +1040,76 @@ struct World {
             s.rot_agility = v1[ROTAG].data(); s.rot_roll = v1[ROLL].data();
             s.rot = q4[0].data(); s.old_rot = q4[1].data();
             s.ang_vel = v3[ANG].data(); s.old_ang_vel = v3[OANG].data(); s.torque = v3[TORQUE].data();
-            s.ids = i64[0].data(); s.world = i64[1].data(); s.mode = i64[2].data(); s.effect_stamp = i64[3].data();
-            s.follow_id = i64[4].data(); s.owner_id = i64[5].data(); s.follow_ptr = i64[6].data(); s.clock = i64[7].data();
-            s.free_ = u8[0].data(); s.moribund = u8[1].data(); s.massive = u8[2].data(); s.interactive = u8[3].data();
-            s.sensor = u8[4].data();
+            s.ids = i64[IDS].data(); s.world = i64[WORLD].data(); s.mode = i64[MODE].data();
+            s.effect_stamp = i64[STAMP].data(); s.follow_id = i64[FID].data(); s.owner_id = i64[OWNER].data();
+            s.follow_ptr = i64[FPTR].data(); s.clock = i64[CLOCK].data();
+            s.free_ = u8[FREE].data(); s.moribund = u8[MORIBUND].data(); s.massive = u8[MASSIVE].data();
+            s.interactive = u8[INTERACTIVE].data(); s.sensor = u8[SENSOR].data();
             oracle_flight_tick_mt(&s, 1);
             for (size_t i = 0; i < n; ++i) {
-                Ball* b = live[i];
+                Ball* b = order[i];
                 for (int c = 0; c < 3; ++c) {
                     b->pos[c] = v3[POS][3 * i + c];
                     b->vel[c] = v3[VEL][3 * i + c];
                     b->old_pos[c] = v3[OPOS][3 * i + c];
                     b->old_vel[c] = v3[OVEL][3 * i + c];
+                    b->goto_pt[c] = v3[GOTO_][3 * i + c];
                     b->last_g[c] = v3[LASTG][3 * i + c];
                 }
-                b->mode = (int)i64[2][i];
+                b->mode = (int)i64[MODE][i];
+                b->effect_stamp = i64[STAMP][i];
+                b->follow_id = i64[FID][i];
+                b->owner_id = i64[OWNER][i];
+                b->follow_range = (float)v1[FRANGE][i];
+                b->last_collision = v1[LASTC][i];
                 b->speed_fraction = v1[SF][i];
+                b->massive = u8[MASSIVE][i] != 0;
+                b->sensor_active = u8[SENSOR][i] != 0;
+                if (i64[FPTR][i] >= 0)                     // a pointer to a removed ball stays as it was
+                    b->follow_ptr = order[(size_t)i64[FPTR][i]]->id;
+                else if (ball(target_before[i]))
+                    b->follow_ptr = 0;
+            }
+            // a ball that began warp proper released its followers (stale entries too); a follower released in the
+            // tick leaves its target's follower set
+            for (size_t i = 0; i < n; ++i)
+                if (mode_before[i] == 3 && !warping_before[i] && order[i]->mode == 3 && order[i]->effect_stamp >= 0)
+                    order[i]->followers.order.clear();
+            for (size_t i = 0; i < n; ++i) {
+                Ball* b = order[i];
+                const bool was = mode_before[i] == 1 || mode_before[i] == 4;
+                const bool is = (b->mode == 1 || b->mode == 4) && b->follow_ptr == target_before[i];
+                if (was && !is)
+                    if (Ball* t = ball(target_before[i])) t->followers.erase(b->id);
             }
         }
-        for (Ball* b : live) {
+        // a warp's drop-out re-filed at the drop-out point when it is nearly at rest there, then every ball that moved
+        for (size_t i = 0; i < n; ++i) {
+            Ball* b = order[i];
+            if (dead[i] || !b->free || !warping_before[i] || b->mode != 2) continue;
+            if (!(lensq(b->old_vel) < 0.1)) continue;
+            double keep_p[3], keep_v[3];
+            for (int c = 0; c < 3; ++c) {
+                keep_p[c] = b->pos[c];
+                keep_v[c] = b->vel[c];
+                b->pos[c] = b->old_pos[c];
+                b->vel[c] = b->old_vel[c];
+            }
+            insert_in_boxes(b);
+            for (int c = 0; c < 3; ++c) {
+                b->pos[c] = keep_p[c];
+                b->vel[c] = keep_v[c];
+            }
+        }
+        for (size_t i = 0; i < n; ++i) {
+            Ball* b = order[i];
+            if (dead[i] || !b->free) continue;
             const double d[3] = {b->pos[0] - b->old_pos[0], b->pos[1] - b->old_pos[1], b->pos[2] - b->old_pos[2]};
             if (!(lensq(d) < 0.1)) insert_in_boxes(b);
         }
-        return handle_proximities();
+        std::string events = handle_proximities();
+        ++current_time;
+        return events;
     }
 
     // ---- the state, as text ----
@@ -1016,6 +1192,24 @@ struct World {
                 out += "\n";
             }
         }
+        for (const Ball* b : order) {                      // each ball's mode and flight state, its followers in order
+            uint64_t bits[6];
+            std::memcpy(bits, b->pos, 24);
+            std::memcpy(bits + 3, b->vel, 24);
+            snprintf(buf, sizeof buf, "M %lld %d %d %lld", (long long)b->id, b->mode, b->massive ? 1 : 0,
+                     (long long)b->follow_ptr);
+            out += buf;
+            for (uint64_t x : bits) {
+                snprintf(buf, sizeof buf, " %016llx", (unsigned long long)x);
+                out += buf;
+            }
+            out += " :";
+            for (int64_t id : b->followers.order) {
+                snprintf(buf, sizeof buf, " %lld", (long long)id);
+                out += buf;
+            }
+            out += "\n";
+        }
         return out;
     }
 };
@@ -1035,8 +1229,9 @@ extern "C" {
 // exclude inert, exclude cloaked); 16 AddProximitySensor (id, range, period, only interactives, shuffle), 17
 // RemoveProximitySensor (id), 18 HandleProximities (the answer: each DoProximity event ball:other:entered, DoRange
 // R<ball>:<inside>, DoTargetTracking T<ball>:<inside>), 19 SetNotificationRange (id, range), 20 SetTargetTracking (id,
-// target, range), 21 GotoPoint (id, x, y, z), 22 Stop (id), 23 a tick (its answer HandleProximities' events). AddBall's
-// sixteenth value is its massive flag. `seed` is the world's srand seed.
+// target, range), 21 GotoPoint (id, x, y, z), 22 Stop (id), 23 a tick (its answer HandleProximities' events), 24
+// FollowBall (id, target, range), 25 Orbit (id, target, range), 26 WarpTo (id, x, y, z, min range, warp factor).
+// AddBall's sixteenth value is its massive flag. `seed` is the world's srand seed.
 int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double friction, double dt, int64_t seed,
                          char* out, int64_t cap) {
     space_oracle::World w;
@@ -1088,6 +1283,9 @@ int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double fr
             case 21: w.goto_point(id, o + 2); break;
             case 22: w.stop(id); break;
             case 23: answer = "Q" + w.tick() + "\n"; break;
+            case 24: w.follow(id, (int64_t)o[2], o[3], 1); break;
+            case 25: w.follow(id, (int64_t)o[2], o[3], 4); break;
+            case 26: w.warp_to(id, o + 2, o[5], (int64_t)o[6]); break;
             case 17: w.remove_sensor(id); break;
             case 18: answer = "Q" + w.handle_proximities() + "\n"; break;
             case 15: {

@@ -25,6 +25,7 @@ STRIDE = 16
 ADD, POS, RADIUS, MAXVEL, REMOVE, INIT, COPY, INTERACTIVE, KEEPALIVE = range(1, 10)
 CLOAKED, VISIBILITY, RANGE_BALL, RANGE_POINT, BUBBLE_AT, NEARBY = range(10, 16)
 SENSOR, UNSENSOR, PROXIMITIES, NOTIFY, TRACK, GOTO, STOP, TICK = range(16, 24)
+FOLLOW, ORBIT, WARP = range(24, 27)
 TOP = 7864320.0                                           # a top box's width (m)
 
 
@@ -209,6 +210,68 @@ def tick_ops(seed: int, n_ops: int = 80) -> list:
     return ops
 
 
+def mode_ops(seed: int, n_ops: int = 110) -> list:
+    """A world of the follow, orbit and warp modes: up to 10 light non-massive ships (a time constant of 0.01 to 10 s,
+    some with a top speed under 0.6 m/s, so that their warps drop out nearly at rest and are re-filed there) around
+    one or two centres near top-box faces, following and orbiting one another, warping 0.3 to 30 Mm at warp factors
+    of 1,000 to 30,000 (a few tens of ticks a warp), sent along GOTO legs, stopped, re-added (which keeps a follower's
+    target pointer), removed (which releases its followers), with sensors, notification ranges and the bubble partition
+    re-initialised;
+    runs of ticks between the commands."""
+    r = random.Random(f"space-modes-{seed}")
+    centres = [[r.choice((-1.0, 0.0, 1.0)) * TOP + r.uniform(-4e3, 4e3) for _ in range(3)] for _ in range(r.randint(1, 2))]
+    ids, live, ops = list(range(1, 11)), [], []
+
+    def near() -> list:
+        return [x + r.uniform(-5e3, 5e3) for x in r.choice(centres)]
+
+    def add(b: int) -> None:
+        vel = [r.uniform(-100.0, 100.0) for _ in range(3)] if r.random() < 0.5 else [0.0, 0.0, 0.0]
+        max_vel = r.uniform(0.2, 0.6) if r.random() < 0.2 else r.uniform(50.0, 500.0)
+        ops.append(_op(ADD, b, 10 ** r.uniform(5.0, 7.0), r.uniform(5.0, 3e3), max_vel,
+                       1.0 if r.random() < 0.9 else 0.0, 1.0 if r.random() < 0.6 else 0.0, *near(), *vel,
+                       r.uniform(0.1, 1.0), 1.0 if r.random() < 0.8 else 0.5, 0.0))
+        if b not in live:
+            live.append(b)
+    for b in r.sample(ids, r.randint(3, 8)):
+        add(b)
+    for _ in range(n_ops):
+        k = r.random()
+        a = r.choice(live) if live else None
+        if k < 0.4 or a is None:
+            ops.extend(_op(TICK) for _ in range(r.choice((1, 1, 3, 10))))
+        elif k < 0.52:
+            ops.append(_op(FOLLOW, a, r.choice(live), r.choice((0.0, 50.0, 2e3))))
+        elif k < 0.62:
+            ops.append(_op(ORBIT, a, r.choice(live), r.choice((0.0, 500.0, 5e3))))
+        elif k < 0.74:
+            d = [r.gauss(0.0, 1.0) for _ in range(3)]
+            n = sum(x * x for x in d) ** 0.5 or 1.0
+            dist = 10 ** r.uniform(5.5, 7.5)
+            origin = near()
+            ops.append(_op(WARP, a, *[origin[i] + d[i] / n * dist for i in range(3)],
+                           r.choice((0.0, 2e4, 1e5)), r.choice((1000, 3000, 10000, 30000))))
+        elif k < 0.8:
+            far = [x + r.choice((-1.0, 1.0)) * r.uniform(1e4, 1e6) for x in near()]
+            ops.append(_op(GOTO, a, *far))
+        elif k < 0.84:
+            ops.append(_op(STOP, a))
+        elif k < 0.88:
+            add(r.choice(ids))
+        elif k < 0.9:
+            ops.append(_op(REMOVE, a))
+            live.remove(a)
+        elif k < 0.92:
+            ops.append(_op(SENSOR, a, r.choice((1e3, 3e4)), r.choice((1.0, 2.0)), 0.0, float(r.random() < 0.3)))
+        elif k < 0.94:
+            ops.append(_op(NOTIFY, a, r.choice((100.0, 2e3, 1e5))))
+        elif k < 0.96:
+            ops.append(_op(INTERACTIVE, a, float(r.random() < 0.6)))
+        else:
+            ops.append(_op(INIT))
+    return ops
+
+
 def apply(park, op: list) -> str:
     """One operation on the reference's SpaceBallpark; a query's answer as the oracle writes it ("" for the others)."""
     code, bid = int(op[0]), int(op[1])
@@ -242,6 +305,12 @@ def apply(park, op: list) -> str:
         park.goto_point(bid, a[0], a[1], a[2])
     elif code == STOP:
         park.stop(bid)
+    elif code == FOLLOW:
+        park.follow_ball(bid, int(a[0]), a[1])
+    elif code == ORBIT:
+        park.orbit(bid, int(a[0]), a[1])
+    elif code == WARP:
+        park.warp_to(bid, a[0], a[1], a[2], a[3], int(a[4]))
     elif code == UNSENSOR:
         park.remove_proximity_sensor(bid)
     elif code in (PROXIMITIES, TICK):
@@ -311,6 +380,11 @@ def state_text(park) -> str:
     for tag, m in (("I", park.bubble_interactives), ("K", park.bubble_keep_alives)):
         for bub in sorted(m):
             out.append(f"{tag} {bub}" + "".join(f" {i}" for i in sorted(m[bub])) + "\n")
+    for bid in sorted(park.balls):
+        b = park.balls[bid]
+        out.append(f"M {b.id} {b.mode} {int(b.is_massive)} {b.follow_ptr or 0}"
+                   + "".join(f" {_bits(x)}" for x in (*b.pos, *b.vel)) + " :"
+                   + "".join(f" {i}" for i in b.followers.ordered()) + "\n")
     return "".join(out)
 
 

@@ -1,12 +1,16 @@
 """The CPU oracle of the master's partition and bubble partition of one world (oracle/space.cpp) against the golden
-digests recorded on the reference's own SpaceBallpark (tests/golden/space_trace.py): 112 worlds (balls added near
+digests recorded on the reference's own SpaceBallpark (tests/golden/space_trace.py): 152 worlds (balls added near
 top-box faces and corners, moved across top boxes, resized up to huge, removed and re-added, made interactive, kept
 alive, cloaked; InitializeBubbles and CopyBubbles; sweeps past BoxAllocator's 256 kept boxes; the queries
 GetNearbyBalls, CheckVisibility, GetBallIdsInRange from a ball or a point, GetBubbleAtCoordinates; proximity sensors
 added (shuffled ones too, from the world's glibc rand) and removed, notification ranges in GOTO, tracked targets,
 HandleProximities with its DoProximity, DoRange and DoTargetTracking events in the unordered maps' order; ticking
 worlds whose ships fly GOTO legs across top boxes and bubbles: the flight tick of the free balls outside dead bubbles,
-the re-filings of the balls that moved, HandleProximities), every state and every answer after every operation. The first slice of the space layer: its kernel is built on this oracle."""
+the re-filings of the balls that moved, HandleProximities; worlds of the follow, orbit and warp modes: FollowBall and
+Orbit with the targets' follower sets in libstdc++'s order, WarpTo through alignment, warp proper and the drop-out
+(re-filed at its drop-out point when nearly at rest there, massive again), StopAllFollowers when a target warps or is
+removed, a re-added follower's kept target pointer), every state (each ball's mode, flight state and followers too)
+and every answer after every operation. The first slice of the space layer: its kernel is built on this oracle."""
 
 import numpy as np
 
@@ -57,5 +61,27 @@ def test_a_planted_fault_in_the_operations_is_seen():
     ops = sc["ops"].copy()
     k = next(i for i in range(len(ops)) if int(ops[i, 0]) == sp.ADD)
     ops[k, 7] += sp.TOP                                    # one ball added a top box further along x
+    got = np.array([sp.digest(t) for t in space_world.run(ops, seed=sc["rand_seed"])], dtype=np.uint64)
+    assert not (got == sc["digests"]).all()
+
+
+def test_the_mode_worlds_reach_the_modes_paths():
+    scs = [sc for sc in _scenarios() if sc["seed"].startswith("modes")]
+    assert len(scs) == 40
+    modes = [line.split() for sc in scs for t in space_world.run(sc["ops"], seed=sc["rand_seed"])
+             for line in t.splitlines() if line.startswith("M ")]
+    seen = {int(m[2]) for m in modes}
+    assert {0, 1, 2, 3, 4} <= seen                         # GOTO, FOLLOW, STOP, WARP, ORBIT
+    assert sum(1 for m in modes if m[-1] != ":") > 200     # balls with followers
+    assert any(len(m) > 13 for m in modes)                 # a set of several followers, in its order
+    assert any(m[2] == "2" and m[4] != "0" for m in modes)  # a stopped ball still pointing at its old target
+    assert any(m[2] == "2" and m[3] == "1" for m in modes)  # massive again after a warp's drop-out
+
+
+def test_a_planted_fault_in_a_warp_is_seen():
+    sc = next(sc for sc in _scenarios() if sc["seed"].startswith("modes"))
+    ops = sc["ops"].copy()
+    k = next(i for i in range(len(ops)) if int(ops[i, 0]) == sp.WARP)
+    ops[k, 2] += 1.0e6                                     # the warp's destination 1,000 km further along x
     got = np.array([sp.digest(t) for t in space_world.run(ops, seed=sc["rand_seed"])], dtype=np.uint64)
     assert not (got == sc["digests"]).all()
