@@ -68,6 +68,7 @@ struct Composed {
 struct Park {
     Combat* c = nullptr;
     Composed* x = nullptr;
+    const OracleTickHooks* h = nullptr;
     int64_t n;
     double friction, dt;
     float ffriction, fdt;
@@ -1089,10 +1090,11 @@ struct Tick {
                 if (p.massive[i]) gradient(i, rows);
             } else if (p.massive[i]) {
                 p.last_collision[i] = -1.0;
+                if (p.h && p.h->gradient) p.h->gradient(p.h->world, i);
             }
             V pv = ld(p.pos, i), vv = ld(p.vel, i);
             const V lg = ld(p.last_g, i);
-            const V lc = p.x ? ld(p.x->last_c, i) : V{0.0, 0.0, 0.0};
+            const V lc = p.x ? ld(p.x->last_c, i) : (p.h && p.h->last_c) ? ld(p.h->last_c, i) : V{0.0, 0.0, 0.0};
             const V a = V{lg.x + lc.x, lg.y + lc.y, lg.z + lc.z};
             if (warping(i)) {
                 const bool drop = warp_distance(i, &pv, &vv, (double)(p.clock[i] - p.effect_stamp[i]) * p.dt);
@@ -1103,6 +1105,7 @@ struct Tick {
                     st(p.pos, i, pv);           // TRV-714: the drop-out point becomes the old state
                     st(p.vel, i, vv);
                     if (p.x && !(lensq(vv) >= 0.1)) file(i, pv, vv, p.speed_fraction[i]);   // re-filed at rest
+                    if (p.h && p.h->drop_out && !(lensq(vv) >= 0.1)) p.h->drop_out(p.h->world, i);
                     integrate(&pv, &vv, a, p.mass[i] * p.agility[i], p.time_factor[i]);
                 }
             } else {
@@ -1260,6 +1263,13 @@ static Park park_of(const OracleFlight* s);
 int oracle_flight_tick_mt(const OracleFlight* s, int threads) {
     Park p = park_of(s);
     Tick(p).run(threads);
+    return 0;
+}
+
+int oracle_flight_tick_hooked(const OracleFlight* s, const OracleTickHooks* h) {
+    Park p = park_of(s);
+    p.h = h;
+    Tick(p).run(1);
     return 0;
 }
 

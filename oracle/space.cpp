@@ -15,8 +15,9 @@
 // Notification ranges (of a goto point or a followed ball), target tracking and a shuffled sensor's first period (glibc's rand) too. The follow
 // modes (FOLLOW, ORBIT, WARP, with the targets' follower sets and StopAllFollowers) and the tick are too: the flight
 // oracle's tick of every ball (a dead bubble's balls marked so that it skips them and others still read them), a warp's
-// drop-out re-filed at its drop-out point, the re-filings of the balls that moved, HandleProximities. Collisions are
-// not in this slice.
+// drop-out re-filed at its drop-out point and each massive ball's Gradient (Potential with GetNearbyBalls' candidates,
+// space.py:1609-1735) at their turns in phase 3, through the flight oracle's hooks, then the re-filings of the balls
+// that moved, HandleProximities. The iterative collision method is not in this slice.
 
 #include <algorithm>
 #include <array>
@@ -31,6 +32,7 @@
 #include <utility>
 #include <vector>
 
+#include "../exact_ballpark_b200/csrc/ebb_libm.cuh"
 #include "flight_state.h"
 
 namespace space_oracle {
@@ -161,7 +163,7 @@ struct Ball {
     double old_pos[3] = {0.0, 0.0, 0.0}, old_vel[3] = {0.0, 0.0, 0.0}, last_g[3] = {0.0, 0.0, 0.0};
     int64_t follow_ptr = 0, follow_id = 0, owner_id = 0, effect_stamp = 0;   // follow_ptr: the target's id, 0 none
     float follow_range = 10.0f;
-    double last_collision = -1.0;
+    double last_collision = -1.0, last_c[3] = {0.0, 0.0, 0.0};
     HashOrder followers;
     double goto_pt[3] = {0.0, 0.0, 0.0};
     double notification_range = 0.0, tracking_range = 0.0;
@@ -736,6 +738,151 @@ struct World {
         update_proximity_status(b);
         b->within_tracking = false;
     }
+    // ---- collisions inside the tick: Gradient and Potential (space.py:1609-1735) ----
+    // Ballpark::Integrate over t seconds: nothing for t = 0, the ball's cached factor for a whole tick, else glibc's
+    // exp(-k t / m)
+    void integrate(double* p, double* v, const double* a, double m, double tf, double t) const {
+        if (t == 0.0) return;
+        const double k = friction;
+        if (t != dt) tf = ebb::lm::exp((-k / m) * t);
+        const double k2 = k * k, ook2 = 1.0 / k2, ook = 1.0 / k;
+        double pn[3], vn[3];
+        if (k < 1e-10 * m * t) {
+            const double inv_m = 1.0 / m;
+            for (int i = 0; i < 3; ++i)
+                pn[i] = (m * (a[i] * (-k * t) + k * (a[i] * t + v[i] * k * inv_m * t)) + p[i] * k2) * ook2;
+        } else {
+            for (int i = 0; i < 3; ++i)
+                pn[i] = (m * (m * a[i] * (tf - 1.0) + k * (a[i] * t + v[i] - tf * v[i])) + p[i] * k2) * ook2;
+        }
+        for (int i = 0; i < 3; ++i) vn[i] = (m * a[i] - (m * a[i] - v[i] * k) * tf) * ook;
+        for (int i = 0; i < 3; ++i) {
+            p[i] = pn[i];
+            v[i] = vn[i];
+        }
+    }
+    // CollideTwoSpheres: 0 when already touching, else the earlier root of the closing quadratic in [0, 1], or -1
+    static double collide_two_spheres(const double* p0, const double* p1, const double* q0, const double* q1,
+                                      double cr) {
+        const double p0q0[3] = {p0[0] - q0[0], p0[1] - q0[1], p0[2] - q0[2]};
+        const double p0q0_2 = dot(p0q0, p0q0);
+        if (p0q0_2 <= cr * cr) return 0.0;
+        double dpq[3];
+        for (int i = 0; i < 3; ++i) dpq[i] = (p1[i] - p0[i]) - (q1[i] - q0[i]);
+        const double a = dot(dpq, dpq), b = 2.0 * dot(p0q0, dpq), c = p0q0_2 - cr * cr;
+        if (a == 0.0 && b == 0.0) return -1.0;
+        double det = b * b - 4.0 * a * c;
+        if (det < 0.0) return -1.0;
+        det = std::sqrt(det);
+        const double s2 = ((-b - det) * 0.5) / a;
+        return (s2 >= 0.0 && s2 <= 1.0) ? s2 : -1.0;
+    }
+    static void normalize(double* v) {
+        const double n = std::sqrt(lensq(v));
+        if (n == 0.0) return;
+        const double inv = 1.0 / n;
+        for (int i = 0; i < 3; ++i) v[i] = v[i] * inv;
+    }
+    // Potential of `me` with `other`: the response to their first contact within the tick, or to an overlap (the pair
+    // pushed apart by mass and Potential called again on the pushed positions, twice at most); the latest contact's
+    // response kept, the larger of two at the same time
+    void potential(Ball* me, Ball* other, int depth) {
+        const double cr = me->radius + other->radius;
+        const double m1 = me->free ? me->mass * me->agility : 1.0e34;
+        const double m2 = other->free ? other->mass * other->agility : 1.0e34;
+        const double k = friction;
+        double p0[3], q0[3], p1[3], q1[3], vp1[3], vq1[3];
+        std::memcpy(p0, me->pos, 24);
+        std::memcpy(q0, other->pos, 24);
+        std::memcpy(p1, me->pos, 24);
+        std::memcpy(vp1, me->vel, 24);
+        std::memcpy(q1, other->pos, 24);
+        std::memcpy(vq1, other->vel, 24);
+        integrate(p1, vp1, me->last_g, m1, me->time_factor, dt);
+        integrate(q1, vq1, other->last_g, m2, other->time_factor, dt);
+        const double sv = collide_two_spheres(p0, p1, q0, q1, cr);
+        if (sv == -1.0) return;
+        std::memcpy(p1, me->pos, 24);
+        std::memcpy(vp1, me->vel, 24);
+        std::memcpy(q1, other->pos, 24);
+        std::memcpy(vq1, other->vel, 24);
+        const double tf = me->time_factor;
+        double a1[3];
+        if (sv > 0.0) {                                    // a contact within the tick: bounce, then fly on
+            integrate(p1, vp1, me->last_g, m1, tf, sv * dt);
+            integrate(q1, vq1, other->last_g, m2, other->time_factor, sv * dt);
+            double normal[3] = {q1[0] - p1[0], q1[1] - p1[1], q1[2] - p1[2]};
+            normalize(normal);
+            const double v1 = dot(vp1, normal), v2 = dot(vq1, normal);
+            if (!other->free) {                            // a fixed ball reflects
+                const double c = 2.0 * v1;
+                for (int i = 0; i < 3; ++i) vp1[i] = vp1[i] - normal[i] * c;
+            } else {                                       // two free balls exchange momentum along the normal
+                const double mm1 = me->mass, mm2 = other->mass;
+                const double v1p = (mm1 * v1 - mm2 * v1 + 2.0 * mm2 * v2) / (mm1 + mm2);
+                for (int i = 0; i < 3; ++i) vp1[i] = vp1[i] + normal[i] * (v1p - v1);
+            }
+            integrate(p1, vp1, me->last_g, m1, tf, (1.0 - sv) * dt);
+            const double inv_m = 1.0 / m1, inv_t = 1.0 / (tf - 1.0);
+            const double* g = me->last_g;
+            const double* v0 = me->vel;
+            for (int i = 0; i < 3; ++i)
+                a1[i] = -((((g[i] * -m1) + g[i] * (tf * m1)) - (v0[i] * tf) * k) + vp1[i] * k) * inv_m * inv_t;
+        } else {                                           // already overlapping
+            const double p0q0[3] = {q0[0] - p0[0], q0[1] - p0[1], q0[2] - p0[2]};
+            const double p0q0_2 = dot(p0q0, p0q0);
+            double normal[3];
+            if (p0q0_2 == 0.0) {
+                normal[0] = me->id > other->id ? 1.0 : -1.0;
+                normal[1] = normal[2] = 0.0;
+            } else {
+                for (int i = 0; i < 3; ++i) normal[i] = q1[i] - p1[i];
+                normalize(normal);
+            }
+            const double dist = cr - std::sqrt(p0q0_2) + 1;
+            const double d1 = m2 / (m1 + m2) * dist;
+            const double d2 = m1 / (m1 + m2) * dist;
+            if (me->free && other->free && depth < 2) {
+                double keep_me[3], keep_other[3];
+                std::memcpy(keep_me, me->pos, 24);
+                std::memcpy(keep_other, other->pos, 24);
+                for (int i = 0; i < 3; ++i) {
+                    me->pos[i] = me->pos[i] - normal[i] * d1;
+                    other->pos[i] = other->pos[i] + normal[i] * d2;
+                }
+                potential(me, other, depth + 1);
+                std::memcpy(me->pos, keep_me, 24);
+                std::memcpy(other->pos, keep_other, 24);
+                if (m2 / m1 > 25.0) {                      // a light ball: the response scaled to the overlap
+                    normalize(me->last_c);
+                    for (int i = 0; i < 3; ++i) me->last_c[i] = me->last_c[i] * dist;
+                }
+                const double dv[3] = {me->vel[0] - other->vel[0], me->vel[1] - other->vel[1], me->vel[2] - other->vel[2]};
+                if (lensq(dv) > 0.0001) return;
+            }
+            const double normal_comp = dot(me->last_g, normal);
+            const double tmp = 1.0 / (m1 + dt * k);
+            const double c = -d1 / (dt * tmp * m1);
+            const double inv_dt = 1.0 / dt;
+            for (int i = 0; i < 3; ++i) a1[i] = (normal[i] * c - me->vel[i]) * inv_dt - normal[i] * normal_comp;
+        }
+        if (sv >= me->last_collision) {                    // no missiles here
+            double lc[3];
+            for (int i = 0; i < 3; ++i) lc[i] = a1[i] * 0.85;
+            if (sv == me->last_collision) {
+                if (lensq(lc) > lensq(me->last_c)) std::memcpy(me->last_c, lc, 24);
+            } else {
+                std::memcpy(me->last_c, lc, 24);
+                me->last_collision = sv;
+            }
+        }
+    }
+    // Gradient: Potential with each of GetNearbyBalls' candidates (massive, uncloaked, in the ball's bubble), in the
+    // walk's order
+    void gradient(Ball* b) {
+        for (Ball* o : nearby_balls(b, false, false, true)) potential(b, o, 0);
+    }
+
     // ---- the modes' commands (modes.py:206-330, 391-426): Stop, GotoPoint, GotoDirection, FollowBall, Orbit, WarpTo,
     // StopAllFollowers, with the targets' follower sets ----
     void stop_ball(Ball* b) {                              // Stop(Ball*)
@@ -960,6 +1107,44 @@ struct World {
     // The free balls outside a dead bubble (TIME-714: a dead bubble's balls skip the whole tick) run one flight tick
     // through the flight oracle (GOTO and STOP here, no collisions: the slice's balls are not massive); each that moved
     // at least sqrt(0.1) m is re-filed, in ascending id; then HandleProximities.
+    // The flight tick's view of this world: at a hook the balls' flight state is read back from the tick's arrays
+    // (the others as they stand at that turn: before their commit, a drop-out of a lower id at its drop-out point), then
+    // the ball's Gradient runs on the partition, or its drop-out is re-filed
+    struct TickView {
+        World* w;
+        const std::vector<Ball*>* order;
+        const OracleFlight* s;
+        void pull() const {
+            for (size_t i = 0; i < order->size(); ++i) {
+                Ball* b = (*order)[i];
+                for (int c = 0; c < 3; ++c) {
+                    b->pos[c] = s->pos[3 * i + c];
+                    b->vel[c] = s->vel[3 * i + c];
+                    b->last_g[c] = s->last_g[3 * i + c];
+                }
+                b->mode = (int)s->mode[i];
+                b->massive = s->massive[i] != 0;
+            }
+        }
+        static void gradient_at(void* ctx, int64_t row) {
+            TickView* v = static_cast<TickView*>(ctx);
+            v->pull();
+            Ball* b = (*v->order)[(size_t)row];
+            b->last_collision = -1.0;
+            b->last_c[0] = b->last_c[1] = b->last_c[2] = 0.0;
+            v->w->gradient(b);
+            v->s->last_collision[row] = b->last_collision;
+            OracleTickHooks* h = v->hooks;
+            for (int c = 0; c < 3; ++c) h->last_c[3 * row + c] = b->last_c[c];
+        }
+        static void drop_out_at(void* ctx, int64_t row) {
+            TickView* v = static_cast<TickView*>(ctx);
+            v->pull();
+            v->w->insert_in_boxes((*v->order)[(size_t)row]);
+        }
+        OracleTickHooks* hooks = nullptr;
+    };
+
     std::string tick() {
         std::vector<Ball*> order;
         for (auto& kv : balls.items) order.push_back(kv.second.get());
@@ -1045,7 +1230,11 @@ struct World {
             s.follow_ptr = i64[FPTR].data(); s.clock = i64[CLOCK].data();
             s.free_ = u8[FREE].data(); s.moribund = u8[MORIBUND].data(); s.massive = u8[MASSIVE].data();
             s.interactive = u8[INTERACTIVE].data(); s.sensor = u8[SENSOR].data();
-            oracle_flight_tick_mt(&s, 1);
+            std::vector<double> last_c(3 * n, 0.0);      // phase 1 clears every ticked ball's mLastC
+            TickView view{this, &order, &s};
+            OracleTickHooks hooks{last_c.data(), &view, &TickView::gradient_at, &TickView::drop_out_at};
+            view.hooks = &hooks;
+            oracle_flight_tick_hooked(&s, &hooks);
             for (size_t i = 0; i < n; ++i) {
                 Ball* b = order[i];
                 for (int c = 0; c < 3; ++c) {
@@ -1083,24 +1272,7 @@ struct World {
                     if (Ball* t = ball(target_before[i])) t->followers.erase(b->id);
             }
         }
-        // a warp's drop-out re-filed at the drop-out point when it is nearly at rest there, then every ball that moved
-        for (size_t i = 0; i < n; ++i) {
-            Ball* b = order[i];
-            if (dead[i] || !b->free || !warping_before[i] || b->mode != 2) continue;
-            if (!(lensq(b->old_vel) < 0.1)) continue;
-            double keep_p[3], keep_v[3];
-            for (int c = 0; c < 3; ++c) {
-                keep_p[c] = b->pos[c];
-                keep_v[c] = b->vel[c];
-                b->pos[c] = b->old_pos[c];
-                b->vel[c] = b->old_vel[c];
-            }
-            insert_in_boxes(b);
-            for (int c = 0; c < 3; ++c) {
-                b->pos[c] = keep_p[c];
-                b->vel[c] = keep_v[c];
-            }
-        }
+        // every ball that moved re-filed (a warp's drop-out was re-filed at its turn, by the hook)
         for (size_t i = 0; i < n; ++i) {
             Ball* b = order[i];
             if (dead[i] || !b->free) continue;

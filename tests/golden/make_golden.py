@@ -599,7 +599,8 @@ def make_server_collide_more() -> None:
 def make_space_bubbles() -> None:
     """space_bubbles: the master's partition and bubble partition of one world (tests/golden/space_trace.py's streams:
     60 worlds of 60 mixed operations, 6 of 600, 6 sweeps past BoxAllocator's 256 kept boxes, 40 ticking worlds of 80
-    operations with ships flying across top boxes, 40 worlds of the follow, orbit and warp modes), each operation's state
+    operations with ships flying across top boxes, 40 worlds of the follow, orbit and warp modes, 40 worlds of
+    collisions inside the tick), each operation's state
     digest recorded on the reference's own SpaceBallpark (exact_ballpark.space, is_master). A stream whose reference run
     reads a deleted box (DestinyUndefined) is left out."""
     import space_trace as sp
@@ -610,7 +611,8 @@ def make_space_bubbles() -> None:
                + [("long", s, sp.ops_for(s, n_ops=600)) for s in range(1000, 1006)]
                + [("sweep", s, sp.sweep_ops(s)) for s in range(1, 7)]
                + [("tick", s, sp.tick_ops(s)) for s in range(1, 41)]
-               + [("modes", s, sp.mode_ops(s)) for s in range(1, 41)])
+               + [("modes", s, sp.mode_ops(s)) for s in range(1, 41)]
+               + [("collide", s, sp.collide_ops(s)) for s in range(1, 41)])
     for family, seed, ops in streams:
         park = SpaceBallpark(1.0e6, 1000, is_master=True, seed=seed)
         digests = []

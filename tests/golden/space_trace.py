@@ -272,6 +272,67 @@ def mode_ops(seed: int, n_ops: int = 110) -> list:
     return ops
 
 
+def collide_ops(seed: int, n_ops: int = 100) -> list:
+    """A world of collisions inside the tick: up to 10 massive balls packed within a few kilometres of a top-box face,
+    free ships (masses 1e4 to 1e8 kg, so that light balls meet heavy ones) and fixed rocks up to 3 km across, many
+    overlapping from the start, some placed on one another (coincident centres), sent at one another along GOTO legs
+    through the crowd, following one another, cloaked (no longer a candidate), made non-massive by re-adding, warping
+    out (a drop-out is massive again) and re-added; runs of ticks between the commands."""
+    r = random.Random(f"space-collide-{seed}")
+    centre = [r.choice((-1.0, 0.0, 1.0)) * TOP + r.uniform(-2e3, 2e3) for _ in range(3)]
+    ids, live, ops = list(range(1, 11)), [], []
+
+    def near(spread: float = 3e3) -> list:
+        return [x + r.uniform(-spread, spread) for x in centre]
+
+    def add(b: int) -> None:
+        rock = r.random() < 0.25
+        vel = [0.0, 0.0, 0.0] if rock or r.random() < 0.4 else [r.uniform(-200.0, 200.0) for _ in range(3)]
+        ops.append(_op(ADD, b, 10 ** r.uniform(9.0, 11.0) if rock else 10 ** r.uniform(4.0, 8.0),
+                       r.uniform(200.0, 3e3) if rock else r.uniform(20.0, 800.0), 0.0 if rock else r.uniform(50.0, 400.0),
+                       0.0 if rock else 1.0, 1.0 if (not rock and r.random() < 0.8) else 0.0, *near(), *vel,
+                       r.uniform(0.2, 2.0), 1.0, 1.0 if r.random() < 0.9 else 0.0))
+        if b not in live:
+            live.append(b)
+    for b in r.sample(ids, r.randint(4, 9)):
+        add(b)
+    for _ in range(n_ops):
+        k = r.random()
+        a = r.choice(live) if live else None
+        if k < 0.4 or a is None:
+            ops.extend(_op(TICK) for _ in range(r.choice((1, 1, 2, 5))))
+        elif k < 0.56:
+            ops.append(_op(GOTO, a, *near(r.choice((50.0, 3e3, 2e4)))))
+        elif k < 0.64:
+            ops.append(_op(FOLLOW, a, r.choice(live), r.choice((0.0, 100.0))))
+        elif k < 0.7:
+            ops.append(_op(POS, a, *near(r.choice((10.0, 1e3)))))
+        elif k < 0.72 and len(live) > 1:                   # onto where another ball was last placed
+            other = r.choice([b for b in live if b != a])
+            start = next(op for op in reversed(ops) if op[0] in (ADD, POS) and int(op[1]) == other)
+            ops.append(_op(POS, a, *(start[7:10] if start[0] == ADD else start[2:5])))
+        elif k < 0.76:
+            ops.append(_op(CLOAKED, a, float(r.random() < 0.6)))
+        elif k < 0.8:
+            d = [r.gauss(0.0, 1.0) for _ in range(3)]
+            n = sum(x * x for x in d) ** 0.5 or 1.0
+            dist = 10 ** r.uniform(5.5, 6.5)
+            ops.append(_op(WARP, a, *[centre[i] + d[i] / n * dist for i in range(3)], r.choice((0.0, 1e3)),
+                           r.choice((3000, 30000))))
+        elif k < 0.86:
+            add(r.choice(ids))
+        elif k < 0.88:
+            ops.append(_op(STOP, a))
+        elif k < 0.9:
+            ops.append(_op(REMOVE, a))
+            live.remove(a)
+        elif k < 0.95:
+            ops.append(_op(INTERACTIVE, a, float(r.random() < 0.6)))
+        else:
+            ops.append(_op(INIT))
+    return ops
+
+
 def apply(park, op: list) -> str:
     """One operation on the reference's SpaceBallpark; a query's answer as the oracle writes it ("" for the others)."""
     code, bid = int(op[0]), int(op[1])

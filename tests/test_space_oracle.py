@@ -1,5 +1,5 @@
 """The CPU oracle of the master's partition and bubble partition of one world (oracle/space.cpp) against the golden
-digests recorded on the reference's own SpaceBallpark (tests/golden/space_trace.py): 152 worlds (balls added near
+digests recorded on the reference's own SpaceBallpark (tests/golden/space_trace.py): 192 worlds (balls added near
 top-box faces and corners, moved across top boxes, resized up to huge, removed and re-added, made interactive, kept
 alive, cloaked; InitializeBubbles and CopyBubbles; sweeps past BoxAllocator's 256 kept boxes; the queries
 GetNearbyBalls, CheckVisibility, GetBallIdsInRange from a ball or a point, GetBubbleAtCoordinates; proximity sensors
@@ -9,7 +9,9 @@ worlds whose ships fly GOTO legs across top boxes and bubbles: the flight tick o
 the re-filings of the balls that moved, HandleProximities; worlds of the follow, orbit and warp modes: FollowBall and
 Orbit with the targets' follower sets in libstdc++'s order, WarpTo through alignment, warp proper and the drop-out
 (re-filed at its drop-out point when nearly at rest there, massive again), StopAllFollowers when a target warps or is
-removed, a re-added follower's kept target pointer), every state (each ball's mode, flight state and followers too)
+removed, a re-added follower's kept target pointer); worlds of collisions inside the tick (Gradient at each massive
+ball's turn in phase 3 over GetNearbyBalls' candidates, Potential's contacts with free and fixed balls, overlaps pushed
+apart and recursed on, light balls, coincident centres, the latest contact kept), every state (each ball's mode, flight state and followers too)
 and every answer after every operation. The first slice of the space layer: its kernel is built on this oracle."""
 
 import numpy as np
@@ -85,3 +87,15 @@ def test_a_planted_fault_in_a_warp_is_seen():
     ops[k, 2] += 1.0e6                                     # the warp's destination 1,000 km further along x
     got = np.array([sp.digest(t) for t in space_world.run(ops, seed=sc["rand_seed"])], dtype=np.uint64)
     assert not (got == sc["digests"]).all()
+
+
+def test_collisions_inside_the_tick_change_the_worlds():
+    scs = [sc for sc in _scenarios() if sc["seed"].startswith("collide")]
+    assert len(scs) == 40
+    changed = 0
+    for sc in scs[:10]:
+        ops = sc["ops"].copy()
+        ops[ops[:, 0] == sp.ADD, 15] = 0.0                 # every ball added non-massive: no Gradient at all
+        got = np.array([sp.digest(t) for t in space_world.run(ops, seed=sc["rand_seed"])], dtype=np.uint64)
+        changed += not (got == sc["digests"]).all()
+    assert changed >= 8
