@@ -9,9 +9,10 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libebb.so"
-ABI = 5
+ABI = 6
 COLLIDE_MAX_SLOTS = 64          # include/ebb.h: EBB_COLLIDE_MAX_SLOTS
 COLLIDE_MAX_STATICS = 64        # include/ebb.h: EBB_COLLIDE_MAX_STATICS
+SPACE_MAX_SLOTS = 128           # include/ebb.h: EBB_SPACE_MAX_SLOTS
 
 _lib = None
 
@@ -63,6 +64,25 @@ class ServerQueue(ctypes.Structure):
                                                   "gets_bubble")])
 
 
+SPACE_SLOT_FIELDS = ("level", "key", "mod", "active", "bubble", "old_bubble", "seq")
+SPACE_FLAG_FIELDS = ("in_park", "keep_alive", "dead", "dropped")
+SPACE_BOX_FIELDS = ("box_level", "box_key", "box_balls", "box_kids", "box_bubble", "stack", "box_n", "free_boxes")
+SPACE_DICT_FIELDS = ("dict_bubble", "dict_n", "entry_bubble", "entry_id", "entry_value", "entry_n", "inter_bubble",
+                     "inter_id", "inter_n", "keep_bubble", "keep_id", "keep_n", "bubble_id", "seq_next", "flags")
+
+
+class SpaceState(ctypes.Structure):
+    """include/ebb.h's EbbSpaceState, field for field."""
+    _fields_ = ([(k, ctypes.c_int64) for k in ("worlds", "slots", "boxes", "dicts", "entries", "sets")]
+                + [(k, ctypes.c_void_p) for k in ("rows",) + SPACE_SLOT_FIELDS + SPACE_FLAG_FIELDS + SPACE_BOX_FIELDS
+                   + SPACE_DICT_FIELDS])
+
+
+class SpaceTape(ctypes.Structure):
+    """include/ebb.h's EbbSpaceTape, field for field."""
+    _fields_ = [("K", ctypes.c_int64), ("code", ctypes.c_void_p), ("a", ctypes.c_void_p), ("b", ctypes.c_void_p)]
+
+
 def lib() -> ctypes.CDLL:
     """The loaded library (loaded and checked on first use)."""
     global _lib
@@ -92,6 +112,8 @@ def lib() -> ctypes.CDLL:
     L.ebb_composed_tick.argtypes = [ctypes.POINTER(ComposedState), p, i64, p, p, i32]
     L.ebb_composed_file.argtypes = [ctypes.POINTER(ComposedState), p, p, p, p, p]
     L.ebb_server_tick.argtypes = [ctypes.POINTER(ServerState), ctypes.POINTER(ServerQueue), i32, i64, i64, p, i32]
+    L.ebb_space_tape.argtypes = [ctypes.POINTER(FlightState), ctypes.POINTER(SpaceState), ctypes.POINTER(SpaceTape), p,
+                                 i32]
     L.ebb_glibc_srand.argtypes = [p, i64, p, p]
     L.ebb_glibc_rand.argtypes = [p, i64, i64, p, p]
     L.ebb_flight_snap.argtypes = [ctypes.POINTER(FlightState), p, i32, p, i32]

@@ -16,7 +16,8 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libebb.so"
-SOURCES = ("ebb_flight.cu", "ebb_collide.cu", "ebb_combat.cu", "ebb_server.cu", "ebb_rand.cu", "ebb_plan.cpp")
+SOURCES = ("ebb_flight.cu", "ebb_collide.cu", "ebb_combat.cu", "ebb_server.cu", "ebb_space.cu", "ebb_rand.cu",
+           "ebb_plan.cpp")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
               "-prec-div=true", "-prec-sqrt=true", "-ftz=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
               "-Xptxas", "-v", "-shared"]

@@ -1,0 +1,51 @@
+// SPDX-License-Identifier: MIT
+// The space layer's tape on the device: one thread a world runs its K operations in order (ebb_space.cuh), its
+// state [entry][world] so that a warp's 32 worlds read consecutive words.
+#include <cuda_runtime.h>
+
+#include "../../include/ebb.h"
+#include "ebb_space.cuh"
+
+namespace ebb {
+namespace space {
+
+__global__ void __launch_bounds__(128) tape_kernel(const EbbFlightState p, const EbbSpaceState s, const EbbSpaceTape t) {
+    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= s.worlds) return;
+    run_tape(&p, &s, &t, w);
+}
+
+}  // namespace space
+}  // namespace ebb
+
+extern "C" {
+
+int ebb_space_tape(const EbbFlightState* park, const EbbSpaceState* s, const EbbSpaceTape* t, void* stream, int block) {
+    if (park == nullptr || s == nullptr || t == nullptr || block <= 0 || block > 128 || block % 32 != 0)
+        return EBB_EINVAL;
+    if (s->slots < 1 || s->slots > EBB_SPACE_MAX_SLOTS || s->boxes < 1 || s->dicts < 1 || s->entries < 1 ||
+        s->sets < 1 || t->K < 0)
+        return EBB_EINVAL;
+    if (s->worlds <= 0 || t->K == 0) return 0;
+    if (s->rows == nullptr || s->level == nullptr || s->key == nullptr || s->mod == nullptr || s->active == nullptr ||
+        s->bubble == nullptr || s->old_bubble == nullptr || s->seq == nullptr || s->in_park == nullptr ||
+        s->keep_alive == nullptr || s->dead == nullptr || s->dropped == nullptr || s->box_level == nullptr ||
+        s->box_key == nullptr || s->box_balls == nullptr || s->box_kids == nullptr || s->box_bubble == nullptr ||
+        s->stack == nullptr || s->box_n == nullptr || s->free_boxes == nullptr || s->dict_bubble == nullptr ||
+        s->dict_n == nullptr || s->entry_bubble == nullptr || s->entry_id == nullptr || s->entry_value == nullptr ||
+        s->entry_n == nullptr || s->inter_bubble == nullptr || s->inter_id == nullptr || s->inter_n == nullptr ||
+        s->keep_bubble == nullptr || s->keep_id == nullptr || s->keep_n == nullptr || s->bubble_id == nullptr ||
+        s->seq_next == nullptr || s->flags == nullptr || t->code == nullptr || t->a == nullptr || t->b == nullptr)
+        return EBB_EINVAL;
+    if (park->pos == nullptr || park->vel == nullptr || park->old_pos == nullptr || park->old_vel == nullptr ||
+        park->ids == nullptr || park->radius == nullptr || park->max_vel == nullptr || park->agility == nullptr ||
+        park->speed_fraction == nullptr || park->mass == nullptr || park->time_factor == nullptr ||
+        park->free_ == nullptr || park->interactive == nullptr || park->mode == nullptr)
+        return EBB_EINVAL;
+    const unsigned grid = (unsigned)((s->worlds + block - 1) / block);
+    ebb::space::tape_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(*park, *s, *t);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
+}  // extern "C"

@@ -1,0 +1,658 @@
+// SPDX-License-Identifier: MIT
+// The master's partition and bubble partition of one world over a park's rows, as one sequential program a world
+// (exact_ballpark/space.py's SpaceBallpark on the master, the layer exact_ballpark/vec_space.py's VecSpace runs over
+// a batched park): the partition's boxes, made on demand with their parents and released when empty, BoxAllocator's
+// kept count and the reads of a released box (Partition's GetBox, CheckBox and the allocator, space.py:596-676); each
+// ball's filing (Ball::InsertInBoxes and DeleteFromBoxes, space.py:683-818); the top boxes' bubbles, a neighbour's or
+// a new id (Ballpark::InsertInBoxes, NearbyBubbles, Traverse), the bubble dictionaries (+1, 0, -1 in insertion
+// order), the interactive and keep-alive sets (AddToBubble), InitializeBubbles, CopyBubbles, InDeadBubble
+// (space.py:896-1056); AddBall's filing, the setters' re-filings and RemoveBall (space.py:1097-1319); the tick's
+// dead-bubble flags and its re-filings (a warp's drop-out, the commits of the balls that moved).
+//
+// Layout: W worlds of N slots; every per-slot array is [N][W] and every per-entry array [cap][W] (world w's entry e
+// at e W + w), so that the threads of a warp, one world each, touch consecutive words. A world's boxes live in a
+// table of `boxes` entries (level -1 for a free entry), found by scanning it. Exactness: the filing's double
+// arithmetic through ebb_arith.cuh (correctly rounded single operations), compiled with -fmad=false.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/ebb.h"
+#include "ebb_arith.cuh"
+
+namespace ebb {
+namespace space {
+
+constexpr int NUM_LEVELS = 8;
+constexpr int64_t BOX_KEEP = 256;                          // BoxAllocator's kept boxes
+constexpr int64_t F_EDGE = EBB_SPACE_FLAG_EDGE, F_BOXES = EBB_SPACE_FLAG_BOXES, F_DICTS = EBB_SPACE_FLAG_DICTS,
+                  F_ENTRIES = EBB_SPACE_FLAG_ENTRIES, F_BAD_OP = EBB_SPACE_FLAG_BAD_OP,
+                  F_SETS = EBB_SPACE_FLAG_SETS, F_UNDEFINED = EBB_SPACE_FLAG_UNDEFINED;
+constexpr int64_t WARP = 3;
+
+// a box's width at level i (Partition.h's constants: 2^16 grid units of 480 m a quarter at the top)
+EBB_HD double level_width(int i) {
+    return ddiv(dmul(dmul((double)(int64_t(1) << (2 * NUM_LEVELS)), 480.0), 0.25), (double)(int64_t(1) << (2 * i)));
+}
+EBB_HD int64_t level_grid(int i) { return int64_t(1) << (2 * i - 2 * NUM_LEVELS + 39); }
+EBB_HD int64_t clamp_key(int64_t i, int64_t n) { return i < 0 ? int64_t(0) : (i >= n ? n - 1 : i); }
+
+// the filing level of an inflated radius: the deepest level whose width is at least three radii
+EBB_HD int level_for(double radius) {
+    int level = 0;
+    for (int i = 0; i < NUM_LEVELS; ++i) {
+        if (dmul(3.0, radius) > level_width(i)) break;
+        level = i;
+    }
+    return level;
+}
+
+struct World {
+    const EbbFlightState* p;
+    const EbbSpaceState* s;
+    int64_t w, W, N, B;
+
+    // ---- accessors: entry e of a [cap][W] array, component c of a [3][cap][W] array ----
+    EBB_HD int64_t& I(int64_t* a, int64_t e) const { return a[e * W + w]; }
+    EBB_HD int64_t& I3(int64_t* a, int64_t c, int64_t e, int64_t cap) const { return a[(c * cap + e) * W + w]; }
+    EBB_HD uint8_t& U(uint8_t* a, int64_t e) const { return a[e * W + w]; }
+    EBB_HD int64_t& one(int64_t* a) const { return a[w]; }
+    EBB_HD void flag(int64_t f) const { s->flags[w] |= f; }
+
+    // ---- the park's row of a slot ----
+    EBB_HD int64_t row(int64_t j) const { return s->rows[j * W + w]; }
+    EBB_HD double pos(int64_t j, int c) const { return p->pos[c * p->n + row(j)]; }
+    EBB_HD double vel(int64_t j, int c) const { return p->vel[c * p->n + row(j)]; }
+    EBB_HD int64_t id(int64_t j) const { return p->ids[row(j)]; }
+    EBB_HD bool interactive(int64_t j) const { return p->interactive[row(j)] != 0; }
+
+    // ---- the box table ----
+    EBB_HD int64_t box_find(int level, int64_t kx, int64_t ky, int64_t kz) const {
+        const int64_t n = one(s->box_n);
+        for (int64_t e = 0; e < n; ++e) {
+            if (I(s->box_level, e) != level) continue;
+            if (I3(s->box_key, 0, e, B) == kx && I3(s->box_key, 1, e, B) == ky && I3(s->box_key, 2, e, B) == kz)
+                return e;
+        }
+        return -1;
+    }
+    // a key at the grid's edge, where Partition clamps (two neighbours would be one box): outside this layer
+    EBB_HD bool edge(int64_t ix, int64_t iy, int64_t iz, int level) const {
+        const int64_t g = level_grid(level);
+        if (ix >= 0 && ix < g && iy >= 0 && iy < g && iz >= 0 && iz < g) return false;
+        flag(F_EDGE);
+        return true;
+    }
+    EBB_HD int64_t check_box(int64_t ix, int64_t iy, int64_t iz, int level) const {
+        if (edge(ix, iy, iz, level)) return -1;
+        return box_find(level, ix, iy, iz);
+    }
+    // a new box-table entry (a free one, else the next), which takes one of BoxAllocator's kept boxes
+    EBB_HD int64_t new_box(int level, int64_t kx, int64_t ky, int64_t kz) {
+        int64_t e = -1;
+        const int64_t n = one(s->box_n);
+        for (int64_t i = 0; i < n; ++i)
+            if (I(s->box_level, i) < 0) {
+                e = i;
+                break;
+            }
+        if (e < 0) {
+            if (n >= B) {
+                flag(F_BOXES);
+                return -1;
+            }
+            e = n;
+            one(s->box_n) = n + 1;
+        }
+        if (one(s->free_boxes) > 0) --one(s->free_boxes);
+        I(s->box_level, e) = level;
+        I3(s->box_key, 0, e, B) = kx;
+        I3(s->box_key, 1, e, B) = ky;
+        I3(s->box_key, 2, e, B) = kz;
+        I(s->box_balls, e) = 0;
+        I(s->box_kids, e) = 0;
+        I(s->box_bubble, e) = -1;
+        return e;
+    }
+    // GetBox: the box, made with its missing ancestors when missing (a parent's key is its child's over 4)
+    EBB_HD int64_t get_box(int64_t ix, int64_t iy, int64_t iz, int level) {
+        if (edge(ix, iy, iz, level)) return -1;
+        const int64_t found = box_find(level, ix, iy, iz);
+        if (found >= 0) return found;
+        int first = level;                                 // the shallowest missing level of the chain
+        int64_t parent = -1;
+        while (first > 0) {
+            const int sh = 2 * (level - first + 1);
+            parent = box_find(first - 1, ix >> sh, iy >> sh, iz >> sh);
+            if (parent >= 0) break;
+            --first;
+        }
+        for (int L = first; L <= level; ++L) {
+            const int sh = 2 * (level - L);
+            const int64_t e = new_box(L, ix >> sh, iy >> sh, iz >> sh);
+            if (e < 0) return -1;
+            if (parent >= 0) ++I(s->box_kids, parent);
+            parent = e;
+        }
+        return parent;
+    }
+    // Release of an empty box, then of each ancestor it leaves empty: every box of the chain kept while BoxAllocator
+    // held fewer than 256 when the chain began, else deleted. `watch` records the fate of two boxes the caller reads
+    // afterwards (0 live, 1 released and kept, 2 released and deleted).
+    EBB_HD void release(int64_t e, const int64_t* watch, int* fate) {
+        const bool keep = one(s->free_boxes) < BOX_KEEP;
+        int64_t cur = e;
+        for (int guard = 0; guard < NUM_LEVELS && cur >= 0; ++guard) {
+            const int level = (int)I(s->box_level, cur);
+            int64_t parent = -1;
+            if (level > 0) {
+                parent = box_find(level - 1, I3(s->box_key, 0, cur, B) >> 2, I3(s->box_key, 1, cur, B) >> 2,
+                                  I3(s->box_key, 2, cur, B) >> 2);
+                if (parent >= 0) --I(s->box_kids, parent);
+            }
+            I(s->box_level, cur) = -1;
+            for (int k = 0; k < 2; ++k)
+                if (watch[k] == cur) fate[k] = keep ? 1 : 2;
+            if (keep) ++one(s->free_boxes);
+            if (parent >= 0 && I(s->box_kids, parent) == 0 && I(s->box_balls, parent) == 0)
+                cur = parent;
+            else
+                cur = -1;
+        }
+    }
+
+    // ---- a ball's filing: level, key, sides, the active neighbours (bit 13 + x + 3 y + 9 z) ----
+    EBB_HD int64_t& lvl(int64_t j) const { return I(s->level, j); }
+    EBB_HD int64_t& key(int64_t j, int c) const { return I3(s->key, c, j, N); }
+    EBB_HD int64_t& mod(int64_t j, int c) const { return I3(s->mod, c, j, N); }
+    EBB_HD int64_t& active(int64_t j) const { return I(s->active, j); }
+
+    // the ball's boxes in key order (the map DeleteFromBoxes walks), as table entries; returns their count
+    EBB_HD int ball_boxes(int64_t j, int64_t* out) const {
+        if (lvl(j) < 0) return 0;
+        int64_t keys[27][3];
+        int n = 0;
+        const int64_t a = active(j);
+        for (int z = -1; z <= 1; ++z)
+            for (int y = -1; y <= 1; ++y)
+                for (int x = -1; x <= 1; ++x) {
+                    if (!((a >> (13 + x + 3 * y + 9 * z)) & 1)) continue;
+                    const int64_t g = level_grid((int)lvl(j));
+                    keys[n][0] = clamp_key(key(j, 0) + x, g);
+                    keys[n][1] = clamp_key(key(j, 1) + y, g);
+                    keys[n][2] = clamp_key(key(j, 2) + z, g);
+                    ++n;
+                }
+        for (int i = 1; i < n; ++i)                        // insertion sort by (x, y, z)
+            for (int k = i; k > 0; --k) {
+                const bool less = keys[k][0] != keys[k - 1][0] ? keys[k][0] < keys[k - 1][0]
+                                  : keys[k][1] != keys[k - 1][1] ? keys[k][1] < keys[k - 1][1]
+                                                                 : keys[k][2] < keys[k - 1][2];
+                if (!less) break;
+                for (int c = 0; c < 3; ++c) {
+                    const int64_t t = keys[k][c];
+                    keys[k][c] = keys[k - 1][c];
+                    keys[k - 1][c] = t;
+                }
+            }
+        int m = 0;
+        for (int i = 0; i < n; ++i) {
+            if (i > 0 && keys[i][0] == keys[i - 1][0] && keys[i][1] == keys[i - 1][1] && keys[i][2] == keys[i - 1][2])
+                continue;                                  // a clamped duplicate is one map entry
+            out[m++] = box_find((int)lvl(j), keys[i][0], keys[i][1], keys[i][2]);
+        }
+        return m;
+    }
+    EBB_HD void clear_filing(int64_t j) const {
+        lvl(j) = -1;
+        active(j) = 0;
+        for (int c = 0; c < 3; ++c) mod(j, c) = -2;
+    }
+    // DeleteFromBoxes: the ball leaves each of its boxes in key order, each box released when left empty
+    EBB_HD void delete_from_boxes(int64_t j, const int64_t* watch, int* fate) {
+        int64_t boxes[27];
+        const int n = ball_boxes(j, boxes);
+        for (int i = 0; i < n; ++i) {
+            const int64_t e = boxes[i];
+            if (e < 0) continue;
+            --I(s->box_balls, e);
+            if (I(s->box_balls, e) == 0 && I(s->box_kids, e) == 0) release(e, watch, fate);
+        }
+        clear_filing(j);
+    }
+    EBB_HD void delete_from_boxes(int64_t j) {
+        const int64_t watch[2] = {-1, -1};
+        int fate[2] = {0, 0};
+        delete_from_boxes(j, watch, fate);
+    }
+    EBB_HD int64_t topmost_of(int64_t e) const {
+        int level = (int)I(s->box_level, e);
+        int64_t kx = I3(s->box_key, 0, e, B), ky = I3(s->box_key, 1, e, B), kz = I3(s->box_key, 2, e, B);
+        return box_find(0, kx >> (2 * level), ky >> (2 * level), kz >> (2 * level));
+    }
+    // a free ball's radius plus a tick at full thrust (Ball::GetInflatedRadius)
+    EBB_HD double inflated_radius(int64_t j, const double* v) const {
+        const int64_t r = row(j);
+        const double radius = (double)p->radius[r];
+        if (!p->free_[r]) return radius;
+        const double m = dmul(p->mass[r], (double)p->agility[r]);
+        const double k = p->friction;
+        const double a = ddiv(dmul(dmul(k, (double)p->speed_fraction[r]), (double)p->max_vel[r]), m);
+        const double speed = dsqrt(dadd(dadd(dmul(v[0], v[0]), dmul(v[1], v[1])), dmul(v[2], v[2])));
+        const double ma = dmul(m, a);
+        const double max_speed = ddiv(dsub(ma, dmul(dsub(ma, dmul(speed, k)), p->time_factor[r])), k);
+        return dadd(radius, dmul(p->dt, max_speed));
+    }
+    EBB_HD static void key_for(int level, const double* x, int64_t* k) {
+        const double wd = level_width(level), fac = ddiv(1.0, wd);
+        const double half = dmul(dmul(0.5, wd), (double)level_grid(level));
+        for (int c = 0; c < 3; ++c) k[c] = to_i64(dmul(dadd(x[c], half), fac));
+    }
+
+    // ---- bubbles ----
+    EBB_HD int64_t nearby_bubbles(int64_t kx, int64_t ky, int64_t kz) const {
+        for (int i = -1; i <= 1; ++i)
+            for (int j = -1; j <= 1; ++j)
+                for (int k = -1; k <= 1; ++k) {
+                    if (i == 0 && j == 0 && k == 0) continue;
+                    const int64_t o = check_box(kx + i, ky + j, kz + k, 0);
+                    if (o >= 0 && I(s->box_bubble, o) != -1) return I(s->box_bubble, o);
+                }
+        return -1;
+    }
+    // Traverse: the seed given to every top box reachable through neighbours without a bubble (a fill; the stack
+    // holds each box once, marked as it is pushed)
+    EBB_HD void traverse(int64_t top, int64_t seed) {
+        if (I(s->box_bubble, top) != -1) return;
+        I(s->box_bubble, top) = seed;
+        int64_t sp = 0;
+        I(s->stack, sp++) = top;
+        while (sp > 0) {
+            const int64_t e = I(s->stack, --sp);
+            const int64_t kx = I3(s->box_key, 0, e, B), ky = I3(s->box_key, 1, e, B), kz = I3(s->box_key, 2, e, B);
+            for (int i = -1; i <= 1; ++i)
+                for (int j = -1; j <= 1; ++j)
+                    for (int k = -1; k <= 1; ++k) {
+                        if (i == 0 && j == 0 && k == 0) continue;
+                        const int64_t o = check_box(kx + i, ky + j, kz + k, 0);
+                        if (o < 0 || I(s->box_bubble, o) != -1) continue;
+                        I(s->box_bubble, o) = seed;
+                        if (sp >= B) {
+                            flag(F_BOXES);
+                            return;
+                        }
+                        I(s->stack, sp++) = o;
+                    }
+        }
+    }
+    // the dictionary of bubble `bub`: whether it exists; its entry for ball `bid` (-1 none)
+    EBB_HD int64_t dict_index(int64_t bub) const {
+        const int64_t n = one(s->dict_n);
+        for (int64_t d = 0; d < n; ++d)
+            if (I(s->dict_bubble, d) == bub) return d;
+        return -1;
+    }
+    EBB_HD int64_t entry_index(int64_t bub, int64_t bid) const {
+        const int64_t n = one(s->entry_n);
+        for (int64_t e = 0; e < n; ++e)
+            if (I(s->entry_bubble, e) == bub && I(s->entry_id, e) == bid) return e;
+        return -1;
+    }
+    EBB_HD void entry_erase(int64_t e) {
+        const int64_t n = one(s->entry_n);
+        for (int64_t i = e; i + 1 < n; ++i) {
+            I(s->entry_bubble, i) = I(s->entry_bubble, i + 1);
+            I(s->entry_id, i) = I(s->entry_id, i + 1);
+            I(s->entry_value, i) = I(s->entry_value, i + 1);
+        }
+        one(s->entry_n) = n - 1;
+    }
+    // the interactive (which = 0) or keep-alive (1) set of a bubble: membership, insertion, removal
+    EBB_HD int64_t* set_bub(int which) const { return which ? s->keep_bubble : s->inter_bubble; }
+    EBB_HD int64_t* set_id(int which) const { return which ? s->keep_id : s->inter_id; }
+    EBB_HD int64_t* set_n(int which) const { return which ? s->keep_n : s->inter_n; }
+    EBB_HD bool set_any(int which, int64_t bub) const {
+        const int64_t n = one(set_n(which));
+        for (int64_t e = 0; e < n; ++e)
+            if (I(set_bub(which), e) == bub) return true;
+        return false;
+    }
+    EBB_HD void set_insert(int which, int64_t bub, int64_t bid) {
+        const int64_t n = one(set_n(which));
+        for (int64_t e = 0; e < n; ++e)
+            if (I(set_bub(which), e) == bub && I(set_id(which), e) == bid) return;
+        if (n >= s->sets) {
+            flag(F_SETS);
+            return;
+        }
+        I(set_bub(which), n) = bub;
+        I(set_id(which), n) = bid;
+        one(set_n(which)) = n + 1;
+    }
+    EBB_HD void set_erase(int which, int64_t bub, int64_t bid) {
+        const int64_t n = one(set_n(which));
+        for (int64_t e = 0; e < n; ++e)
+            if (I(set_bub(which), e) == bub && I(set_id(which), e) == bid) {
+                I(set_bub(which), e) = I(set_bub(which), n - 1);
+                I(set_id(which), e) = I(set_id(which), n - 1);
+                one(set_n(which)) = n - 1;
+                return;
+            }
+    }
+    // AddToBubble: the ball entered (+1, or 0 again after leaving) its bubble's dictionary and left (-1, or gone if it
+    // had only entered) its old one's; its interactive and keep-alive memberships follow
+    EBB_HD void add_to_bubble(int64_t j) {
+        const int64_t bid = id(j), bub = I(s->bubble, j), old = I(s->old_bubble, j);
+        if (bub != -1) {
+            if (dict_index(bub) < 0) {
+                const int64_t n = one(s->dict_n);
+                if (n >= s->dicts) {
+                    flag(F_DICTS);
+                } else {
+                    I(s->dict_bubble, n) = bub;
+                    one(s->dict_n) = n + 1;
+                }
+            }
+            const int64_t e = entry_index(bub, bid);
+            if (e < 0) {
+                const int64_t n = one(s->entry_n);
+                if (n >= s->entries) {
+                    flag(F_ENTRIES);
+                } else {
+                    I(s->entry_bubble, n) = bub;
+                    I(s->entry_id, n) = bid;
+                    I(s->entry_value, n) = 1;
+                    one(s->entry_n) = n + 1;
+                }
+            } else if (I(s->entry_value, e) == -1) {
+                I(s->entry_value, e) = 0;
+            }
+        }
+        if (old != -1 && dict_index(old) >= 0) {
+            const int64_t e = entry_index(old, bid);
+            if (e >= 0) {
+                if (I(s->entry_value, e) == 0)
+                    I(s->entry_value, e) = -1;
+                else if (I(s->entry_value, e) == 1)
+                    entry_erase(e);
+            }
+        }
+        if (interactive(j)) {
+            if (bub != -1) set_insert(0, bub, bid);
+            if (old != -1) set_erase(0, old, bid);
+        }
+        if (U(s->keep_alive, j)) {
+            if (bub != -1) set_insert(1, bub, bid);
+            if (old != -1) set_erase(1, old, bid);
+        }
+    }
+    // InDeadBubble: no interactive and no keep-alive ball in the ball's bubble, and the ball not in WARP
+    EBB_HD bool in_dead_bubble(int64_t j) const {
+        if (p->mode[row(j)] == WARP) return false;
+        const int64_t bub = I(s->bubble, j);
+        return !set_any(0, bub) && !set_any(1, bub);
+    }
+
+    // ---- filing ----
+    EBB_HD void insert_in_box(int64_t j, int64_t e) const {
+        (void)j;
+        if (e >= 0) ++I(s->box_balls, e);
+    }
+    // Ball::InsertInBoxes: the ball's box at the level of its inflated radius and the neighbours its sphere reaches
+    // (every neighbour for a huge ball), unless box and sides are as they were; the top box takes the bubble
+    EBB_HD void ball_insert_in_boxes(int64_t j, const double* x, const double* v, int level0, const int64_t* key0,
+                                     int fate_box1, int64_t new_bubble) {
+        if (fate_box1 == 2) flag(F_UNDEFINED);             // a deleted box's memory read
+        const double inflated = inflated_radius(j, v);
+        const double wd = level_width(level0);
+        const double center = dmul(dmul(wd, (double)level_grid(level0)), 0.5);
+        int64_t m[3] = {0, 0, 0};
+        for (int q = 0; q < 3; ++q) {
+            const double lo = dsub(dmul((double)key0[q], wd), center);
+            const double hi = dsub(dmul((double)(key0[q] + 1), wd), center);
+            if (dsub(dadd(lo, inflated), x[q]) > 0.0)
+                m[q] = -1;
+            else if (dsub(dsub(hi, inflated), x[q]) < 0.0)
+                m[q] = 1;
+        }
+        if (lvl(j) >= 0 && lvl(j) == level0 && key(j, 0) == key0[0] && key(j, 1) == key0[1] && key(j, 2) == key0[2] &&
+            mod(j, 0) == m[0] && mod(j, 1) == m[1] && mod(j, 2) == m[2])
+            return;
+        delete_from_boxes(j);
+        const int level = level_for(inflated);
+        int64_t k[3];
+        key_for(level, x, k);
+        const int64_t box1 = get_box(k[0], k[1], k[2], level);
+        if (box1 < 0) return;
+        for (int c = 0; c < 3; ++c) {
+            mod(j, c) = m[c];
+            key(j, c) = I3(s->box_key, c, box1, B);
+        }
+        lvl(j) = level;
+        insert_in_box(j, box1);
+        const int64_t top = topmost_of(box1);
+        if (top >= 0) I(s->box_bubble, top) = new_bubble;
+        int64_t act = int64_t(1) << 13;
+        const int64_t ix = key(j, 0), iy = key(j, 1), iz = key(j, 2);
+        const int64_t row_j = row(j);
+        if (level == 0 && (double)fmul(p->radius[row_j], 2.0f) > level_width(0)) {   // a huge ball: every neighbour
+            for (int a = -1; a <= 1; ++a)
+                for (int b = -1; b <= 1; ++b)
+                    for (int c = -1; c <= 1; ++c) {
+                        if (a == 0 && b == 0 && c == 0) continue;
+                        insert_in_box(j, get_box(ix + a, iy + b, iz + c, 0));
+                        act |= int64_t(1) << (13 + a + 3 * b + 9 * c);
+                    }
+            active(j) = act;
+            return;
+        }
+        const int64_t mx = m[0], my = m[1], mz = m[2];
+        auto side = [&](int64_t a, int64_t b, int64_t c) {
+            insert_in_box(j, get_box(ix + a, iy + b, iz + c, level));
+            act |= int64_t(1) << (13 + a + 3 * b + 9 * c);
+        };
+        if (mx) side(mx, 0, 0);
+        if (my) side(0, my, 0);
+        if (mz) side(0, 0, mz);
+        if (mx && my) side(mx, my, 0);
+        if (mx && mz) side(mx, 0, mz);
+        if (my && mz) side(0, my, mz);
+        if (mx && my && mz) side(mx, my, mz);
+        active(j) = act;
+    }
+    // Ballpark::InsertInBoxes on the master: the ball's new top box, its bubble or, for a top without one, a
+    // neighbour's or a new id; AddToBubble when the ball's bubble changes; then its filing
+    EBB_HD void insert_in_boxes(int64_t j, const double* x, const double* v) {
+        const double inflated = inflated_radius(j, v);
+        const int level0 = level_for(inflated);
+        int64_t k[3];
+        key_for(level0, x, k);
+        const int64_t box1 = get_box(k[0], k[1], k[2], level0);
+        if (box1 < 0) return;
+        int64_t key0[3];
+        for (int c = 0; c < 3; ++c) key0[c] = I3(s->box_key, c, box1, B);
+        const int64_t top = topmost_of(box1);
+        int64_t new_bubble = I(s->box_bubble, top);
+        int fate[2] = {0, 0};
+        if (new_bubble == -1) {
+            const int64_t tk[3] = {I3(s->box_key, 0, top, B), I3(s->box_key, 1, top, B), I3(s->box_key, 2, top, B)};
+            const int64_t watch[2] = {box1, top};
+            delete_from_boxes(j, watch, fate);             // may release box1 and its top: both are still read
+            if (fate[1] == 2) flag(F_UNDEFINED);
+            new_bubble = nearby_bubbles(tk[0], tk[1], tk[2]);
+            if (new_bubble == -1) new_bubble = one(s->bubble_id)++;
+            if (fate[1] == 0) I(s->box_bubble, top) = new_bubble;   // (a released top's write is lost)
+        }
+        if (I(s->bubble, j) != new_bubble) {
+            I(s->old_bubble, j) = I(s->bubble, j);
+            I(s->bubble, j) = new_bubble;
+            add_to_bubble(j);
+        }
+        ball_insert_in_boxes(j, x, v, level0, key0, fate[0], new_bubble);
+    }
+    EBB_HD void insert_in_boxes(int64_t j) {
+        const double x[3] = {pos(j, 0), pos(j, 1), pos(j, 2)}, v[3] = {vel(j, 0), vel(j, 1), vel(j, 2)};
+        insert_in_boxes(j, x, v);
+    }
+
+    // ---- the operations ----
+    EBB_HD bool slot_ok(int64_t j) const { return j >= 0 && j < N && row(j) >= 0 && row(j) < p->n; }
+    EBB_HD void add(int64_t j) {                           // AddBall's filing (a ball already in: re-filed)
+        if (U(s->in_park, j)) {
+            delete_from_boxes(j);
+        } else {                                           // a new ball: last in the ball dictionary's order
+            I(s->seq, j) = one(s->seq_next)++;
+            I(s->bubble, j) = -1;
+            I(s->old_bubble, j) = -1;
+            clear_filing(j);
+        }
+        U(s->in_park, j) = 1;
+        insert_in_boxes(j);
+    }
+    EBB_HD void remove(int64_t j) {                        // RemoveBall outside Evolve: its boxes and bubble left
+        if (!U(s->in_park, j)) return;
+        delete_from_boxes(j);
+        I(s->old_bubble, j) = I(s->bubble, j);
+        I(s->bubble, j) = -1;
+        add_to_bubble(j);
+        U(s->in_park, j) = 0;
+    }
+    EBB_HD void set_interactive(int64_t j, bool on) {
+        const int64_t r = row(j);
+        if (on && !p->interactive[r]) {
+            p->interactive[r] = 1;
+            if (I(s->bubble, j) != -1) set_insert(0, I(s->bubble, j), id(j));
+        } else if (!on && p->interactive[r]) {
+            if (I(s->bubble, j) != -1) set_erase(0, I(s->bubble, j), id(j));
+            p->interactive[r] = 0;
+        }
+    }
+    // InitializeBubbles: every top box's bubble cleared, the dictionaries and sets emptied, then each ball's top
+    // given its bubble (a fill from the first ball to reach it) in the ball dictionary's order
+    EBB_HD void init_bubbles() {
+        const int64_t n = one(s->box_n);
+        for (int64_t e = 0; e < n; ++e)
+            if (I(s->box_level, e) == 0) I(s->box_bubble, e) = -1;
+        one(s->bubble_id) = 0;
+        one(s->dict_n) = 0;
+        one(s->entry_n) = 0;
+        one(s->inter_n) = 0;
+        one(s->keep_n) = 0;
+        for (int64_t j = 0; j < N; ++j) U(s->keep_alive, j) = 0;
+        int64_t last = -1;
+        for (int64_t t = 0; t < N; ++t) {                  // the slots in the order their balls were added
+            int64_t j = -1;
+            for (int64_t i = 0; i < N; ++i)
+                if (U(s->in_park, i) && I(s->seq, i) > last && (j < 0 || I(s->seq, i) < I(s->seq, j))) j = i;
+            if (j < 0) break;
+            last = I(s->seq, j);
+            if (lvl(j) < 0) {
+                I(s->old_bubble, j) = I(s->bubble, j);
+                I(s->bubble, j) = -1;
+                continue;
+            }
+            const int64_t g = level_grid((int)lvl(j));
+            const int64_t my_box = box_find((int)lvl(j), clamp_key(key(j, 0), g), clamp_key(key(j, 1), g),
+                                            clamp_key(key(j, 2), g));
+            const int64_t top = my_box >= 0 ? topmost_of(my_box) : -1;
+            if (top < 0) continue;
+            if (I(s->box_bubble, top) != -1) {
+                I(s->old_bubble, j) = I(s->bubble, j);
+                I(s->bubble, j) = I(s->box_bubble, top);
+                add_to_bubble(j);
+                continue;
+            }
+            const int64_t seed = one(s->bubble_id);
+            traverse(top, seed);
+            I(s->old_bubble, j) = I(s->bubble, j);
+            I(s->bubble, j) = seed;
+            add_to_bubble(j);
+            one(s->bubble_id) = seed + 1;
+        }
+    }
+    // CopyBubbles: each dictionary's entries settle (+1 to 0, -1 gone); an emptied dictionary goes
+    EBB_HD void copy_bubbles() {
+        for (int64_t e = 0; e < one(s->entry_n);) {
+            if (I(s->entry_value, e) == -1) {
+                entry_erase(e);
+                continue;
+            }
+            if (I(s->entry_value, e) == 1) I(s->entry_value, e) = 0;
+            ++e;
+        }
+        int64_t m = 0;
+        const int64_t n = one(s->dict_n);
+        for (int64_t d = 0; d < n; ++d) {
+            const int64_t bub = I(s->dict_bubble, d);
+            bool any = false;
+            for (int64_t e = 0; e < one(s->entry_n) && !any; ++e) any = I(s->entry_bubble, e) == bub;
+            if (any) I(s->dict_bubble, m++) = bub;
+        }
+        one(s->dict_n) = m;
+    }
+    // phase 1's dead-bubble flags: a free ball of the park in a dead bubble skips the tick
+    EBB_HD void dead() {
+        for (int64_t j = 0; j < N; ++j) {
+            const bool in = U(s->in_park, j) && slot_ok(j);
+            U(s->dead, j) = (in && p->free_[row(j)] && in_dead_bubble(j)) ? 1 : 0;
+        }
+    }
+    // after the park's tick, in ascending id: each warp drop-out nearly at rest re-filed at its drop-out point (the old
+    // state), then each ball that moved at least sqrt(0.1) m
+    EBB_HD void after_evolve() {
+        int64_t order[EBB_SPACE_MAX_SLOTS];
+        int64_t n = 0;
+        for (int64_t j = 0; j < N; ++j)
+            if (U(s->in_park, j) && slot_ok(j)) order[n++] = j;
+        for (int64_t i = 1; i < n; ++i)
+            for (int64_t k = i; k > 0 && id(order[k]) < id(order[k - 1]); --k) {
+                const int64_t t = order[k];
+                order[k] = order[k - 1];
+                order[k - 1] = t;
+            }
+        for (int64_t i = 0; i < n; ++i) {
+            const int64_t j = order[i], r = row(j);
+            if (!U(s->dropped, j) || U(s->dead, j) || !p->free_[r]) continue;
+            const double ov[3] = {p->old_vel[r], p->old_vel[p->n + r], p->old_vel[2 * p->n + r]};
+            if (!(dadd(dadd(dmul(ov[0], ov[0]), dmul(ov[1], ov[1])), dmul(ov[2], ov[2])) < 0.1)) continue;
+            const double op[3] = {p->old_pos[r], p->old_pos[p->n + r], p->old_pos[2 * p->n + r]};
+            insert_in_boxes(j, op, ov);
+        }
+        for (int64_t i = 0; i < n; ++i) {
+            const int64_t j = order[i], r = row(j);
+            if (U(s->dead, j) || !p->free_[r]) continue;
+            double d[3];
+            for (int c = 0; c < 3; ++c) d[c] = dsub(p->pos[c * p->n + r], p->old_pos[c * p->n + r]);
+            if (!(dadd(dadd(dmul(d[0], d[0]), dmul(d[1], d[1])), dmul(d[2], d[2])) < 0.1)) insert_in_boxes(j);
+        }
+    }
+    EBB_HD void apply(int64_t code, int64_t j, int64_t b) {
+        const bool has_slot = slot_ok(j);
+        switch (code) {
+            case EBB_SPACE_NONE: break;
+            case EBB_SPACE_ADD: if (has_slot) add(j); else flag(F_BAD_OP); break;
+            case EBB_SPACE_REFILE: if (has_slot && U(s->in_park, j)) insert_in_boxes(j); break;
+            case EBB_SPACE_INIT_BUBBLES: init_bubbles(); break;
+            case EBB_SPACE_COPY_BUBBLES: copy_bubbles(); break;
+            case EBB_SPACE_KEEP_ALIVE: if (has_slot) U(s->keep_alive, j) = 1; break;
+            case EBB_SPACE_SET_INTERACTIVE: if (has_slot && U(s->in_park, j)) set_interactive(j, b != 0); break;
+            case EBB_SPACE_REMOVE_BALL: if (has_slot) remove(j); break;
+            case EBB_SPACE_DEAD: dead(); break;
+            case EBB_SPACE_AFTER_EVOLVE: after_evolve(); break;
+            default: flag(F_BAD_OP); break;
+        }
+    }
+};
+
+// world w's K operations of the tape, in order (a flagged world is left alone)
+EBB_HD void run_tape(const EbbFlightState* p, const EbbSpaceState* s, const EbbSpaceTape* t, int64_t w) {
+    World wd{p, s, w, s->worlds, s->slots, s->boxes};
+    for (int64_t k = 0; k < t->K; ++k) {
+        if (s->flags[w] & (F_EDGE | F_BOXES | F_DICTS | F_ENTRIES | F_SETS | F_BAD_OP)) return;
+        const int64_t at = k * s->worlds + w;
+        wd.apply(t->code[at], t->a[at], t->b[at]);
+    }
+}
+
+}  // namespace space
+}  // namespace ebb

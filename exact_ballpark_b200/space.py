@@ -1,0 +1,193 @@
+"""The master's partition and bubble partition over the flight park, on the device: the drop-in for the reference's
+`exact_ballpark.vec_space.VecSpace` layer (vec_space.py:777) over `VecModesPark`, in this build's slice: each ball's
+filing (the level of its inflated radius, the key of its box, the sides its sphere reaches), the partition's boxes
+(made with their parents, released when empty, BoxAllocator's kept count, the reads of a released box), the top boxes'
+bubbles (a neighbour's or a new id), the bubble dictionaries (+1, 0, -1 in insertion order), the interactive and
+keep-alive sets, InitializeBubbles, CopyBubbles, the dead-bubble rows the park's tick skips (TIME-714) and the tick's
+re-filings (a warp's drop-out nearly at rest, at its drop-out point; every ball that moved at least sqrt(0.1) m, in
+ascending id), as the reference's `SpaceBallpark` on the master runs them (space.py:596-1319).
+
+The layer is one sequential program a world, one CUDA thread a world (csrc/ebb_space.cuh): an operation is a tape,
+per world K operations applied in order, one launch for all worlds (`tape`, `ops`, `broadcast`), with the reference's
+operation names (`OP`). Its state is [entry, world] tensors (a warp's 32 worlds read consecutive words). A world that
+leaves the layer's domain (a table full, the grid's edge, an operation outside this slice) is flagged and left alone;
+`check()` raises for it. Not in this slice: the proximity sensors, target tracking, notification ranges,
+HandleProximities, the queries (CheckVisibility, GetBallIdsInRange, GetBubbleAtCoordinates), the collision park's
+view, the delayed removal; their operations flag BAD_OP.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _native
+from .modes import VecModesPark, WARP
+
+I64, U8, BOOL = torch.int64, torch.uint8, torch.bool
+
+OPS = ("NONE", "ADD", "REFILE", "INIT_BUBBLES", "COPY_BUBBLES", "KEEP_ALIVE", "SET_INTERACTIVE", "ADD_SENSOR",
+       "REMOVE_SENSOR", "NOTIFY_RANGE", "TRACK", "REMOVE_BALL", "DEAD", "AFTER_EVOLVE")
+OP = {name: k for k, name in enumerate(OPS)}
+FLAGS = ("EVENTS", "TOPS", "EDGE", "BOXES", "DICTS", "ENTRIES", "PROXIMITY", "SENSOR_LIST", "HUGE", "BAD_OP", "SETS",
+         "UNDEFINED")
+FLAG = {name: 1 << k for k, name in enumerate(FLAGS)}
+BLOCK = 128
+
+
+class VecSpace:
+    """The layer for W worlds of N slots over a flight park's rows. `rows` [W, N]: the park's row of each slot (-1 for
+    none), each world's slots in the order its balls are added. Capacities a world: `boxes` box-table entries,
+    `dicts` bubble dictionaries, `entries` dictionary entries, `sets` members of each of the interactive and keep-alive
+    set families (defaults from N)."""
+
+    def __init__(self, park: VecModesPark, rows, boxes: int | None = None, dicts: int | None = None,
+                 entries: int | None = None, sets: int | None = None, block: int = BLOCK):
+        if not isinstance(park, VecModesPark):
+            raise TypeError("the space layer runs over the flight park (exact_ballpark_b200.VecModesPark)")
+        self.park, self.dev, self.block = park, park.dev, int(block)
+        rows = torch.as_tensor(rows, dtype=I64)
+        if rows.dim() != 2:
+            raise ValueError("rows: [W, N]")
+        self.W, self.N = int(rows.shape[0]), int(rows.shape[1])
+        if not 1 <= self.N <= _native.SPACE_MAX_SLOTS:
+            raise ValueError(f"{self.N} slots a world: from 1 to {_native.SPACE_MAX_SLOTS}")
+        if bool(((rows < -1) | (rows >= park.n)).any()):
+            raise ValueError("rows: a park row or -1 for each slot")
+        N, W, d = self.N, self.W, self.dev
+        self.B = int(boxes) if boxes is not None else 16 * N + 64
+        self.D = int(dicts) if dicts is not None else 8 * N + 16
+        self.E = int(entries) if entries is not None else 4 * N + 8
+        self.S = int(sets) if sets is not None else 2 * N + 8
+        self.rows = rows.t().contiguous().to(d)                       # [N][W]
+        z = lambda *shape, dt=I64: torch.zeros(*shape, dtype=dt, device=d)   # noqa: E731
+        self.st = {
+            "level": z(N, W) - 1, "key": z(3, N, W), "mod": z(3, N, W) - 2, "active": z(N, W), "bubble": z(N, W) - 1,
+            "old_bubble": z(N, W) - 1, "seq": z(N, W),
+            "in_park": z(N, W, dt=U8), "keep_alive": z(N, W, dt=U8), "dead": z(N, W, dt=U8), "dropped": z(N, W, dt=U8),
+            "box_level": z(self.B, W) - 1, "box_key": z(3, self.B, W), "box_balls": z(self.B, W),
+            "box_kids": z(self.B, W), "box_bubble": z(self.B, W) - 1, "stack": z(self.B, W), "box_n": z(W),
+            "free_boxes": z(W),
+            "dict_bubble": z(self.D, W), "dict_n": z(W), "entry_bubble": z(self.E, W), "entry_id": z(self.E, W),
+            "entry_value": z(self.E, W), "entry_n": z(W), "inter_bubble": z(self.S, W), "inter_id": z(self.S, W),
+            "inter_n": z(W), "keep_bubble": z(self.S, W), "keep_id": z(self.S, W), "keep_n": z(W),
+            "bubble_id": z(W), "seq_next": z(W), "flags": z(W)}
+        self._flat = torch.where(self.rows >= 0, self.rows, park.n).t().flatten()   # [W N] slot -> row, n for none
+        self._state = None
+        self.last_dead = None
+
+    # ---- plumbing ----
+
+    def state(self) -> _native.SpaceState:
+        """include/ebb.h's EbbSpaceState over the layer's tensors."""
+        if self._state is None:
+            s = _native.SpaceState()
+            s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets = self.W, self.N, self.B, self.D, self.E, self.S
+            s.rows = self.rows.data_ptr()
+            for name, t in self.st.items():
+                setattr(s, name, t.data_ptr())
+            self._state = s
+        return self._state
+
+    def tape(self, code, a=None, b=None) -> None:
+        """Per world, K operations in order: code [W, K] (OP), a [W, K] (a slot), b [W, K] (an integer)."""
+        code = torch.as_tensor(code, dtype=I64).to(self.dev).reshape(self.W, -1)
+        K = int(code.shape[1])
+        if K == 0:
+            return
+        a = (torch.full_like(code, -1) if a is None else torch.as_tensor(a, dtype=I64).to(self.dev).reshape(self.W, K))
+        b = (torch.zeros_like(code) if b is None else torch.as_tensor(b, dtype=I64).to(self.dev).reshape(self.W, K))
+        code_t, a_t, b_t = (x.t().contiguous() for x in (code, a, b))    # [K][W]
+        t = _native.SpaceTape(K, code_t.data_ptr(), a_t.data_ptr(), b_t.data_ptr())
+        rc = _native.lib().ebb_space_tape(ctypes.byref(self.park.state()), ctypes.byref(self.state()), ctypes.byref(t),
+                                          self.park._stream(), self.block)
+        _native.check(rc, "ebb_space_tape")
+        self._keep = (code_t, a_t, b_t)                     # alive until the stream has run the launch
+
+    def ops(self, per_world: list) -> None:
+        """A tape from per-world lists of (op name, slot, int)."""
+        K = max((len(x) for x in per_world), default=0)
+        if K == 0:
+            return
+        code = torch.zeros(self.W, K, dtype=I64)
+        a = torch.full((self.W, K), -1, dtype=I64)
+        b = torch.zeros(self.W, K, dtype=I64)
+        for w, lst in enumerate(per_world):
+            for k, op in enumerate(lst):
+                code[w, k] = OP[op[0]]
+                a[w, k] = int(op[1]) if len(op) > 1 else -1
+                b[w, k] = int(op[2]) if len(op) > 2 else 0
+        self.tape(code, a, b)
+
+    def broadcast(self, name: str, mask: torch.Tensor | None = None) -> None:
+        """One operation without arguments for every world (or the worlds in mask [W]), on the device."""
+        code = torch.full((self.W, 1), OP[name], dtype=I64, device=self.dev)
+        if mask is not None:
+            code = torch.where(mask.to(self.dev).reshape(self.W, 1), code, torch.zeros_like(code))
+        self.tape(code)
+
+    # ---- the load and the tick ----
+
+    def load(self) -> None:
+        """AddBall's filing of every ball, each world's slots in order: one tape, made on the device."""
+        code = torch.where(self.rows.t() >= 0, OP["ADD"], OP["NONE"]).to(I64)
+        slots = torch.arange(self.N, dtype=I64, device=self.dev).expand(self.W, self.N).contiguous()
+        self.tape(code, slots)
+
+    def dead_rows(self, worlds: torch.Tensor | None = None) -> torch.Tensor:
+        """Phase 1's dead-bubble flags [n] (TIME-714) for the park's tick to skip, no host synchronisation."""
+        self.broadcast("DEAD", worlds)
+        out = torch.zeros(self.park.n + 1, dtype=BOOL, device=self.dev)
+        out.scatter_(0, self._flat, self.st["dead"].t().flatten().to(BOOL))
+        return out[:self.park.n]
+
+    def after_evolve(self, dropped_rows: torch.Tensor | None = None, worlds: torch.Tensor | None = None) -> None:
+        """After the park's tick: the warp drop-outs' re-filings, then the commits' (no host synchronisation)."""
+        dr = self.st["dropped"]
+        if dropped_rows is None:
+            dr.zero_()
+        else:
+            pad = torch.cat([dropped_rows.to(self.dev).to(U8), torch.zeros(1, dtype=U8, device=self.dev)])
+            dr.copy_(pad[self._flat].reshape(self.W, self.N).t())
+        self.broadcast("AFTER_EVOLVE", worlds)
+
+    def tick(self) -> None:
+        """One tick of the park with the layer, as Destiny's Evolve runs it on the master: the dead bubbles' balls left
+        out of the park's tick (flagged moribund for the call, which every phase skips), then the re-filings."""
+        park = self.park
+        dead = self.dead_rows()
+        self.last_dead = dead
+        warp_proper = ((park._mode == WARP) & (park._effect_stamp >= 0) & park._free & ~park._moribund & ~dead)
+        saved = park._moribund.clone()
+        park._moribund.logical_or_(dead)
+        try:
+            park.evolve()
+        finally:
+            park._moribund.copy_(saved)
+        self.after_evolve(warp_proper & (park._mode != WARP))
+
+    def check(self) -> None:
+        """Raise on a world flagged outside this layer's domain (a deleted box read included)."""
+        bad = torch.nonzero(self.st["flags"]).flatten().tolist()
+        if bad:
+            fl = int(self.st["flags"][bad[0]])
+            names = [n for n, bit in FLAG.items() if fl & bit]
+            raise RuntimeError(f"worlds {bad[:8]} left the space layer's domain (world {bad[0]}: {names})")
+
+    # ---- readers (host) ----
+
+    def world(self, w: int) -> dict:
+        """World w's state on the host: each tensor's column for the world."""
+        out = {}
+        for name, t in self.st.items():
+            out[name] = t[..., w].cpu() if t.dim() > 1 else t[w].cpu()
+        return out
+
+    def dicts(self, w: int) -> dict:
+        """World w's bubble dictionaries: {bubble: [(ball id, +1 | 0 | -1), ...] in insertion order}."""
+        st = self.world(w)
+        out = {int(b): [] for b in st["dict_bubble"][:int(st["dict_n"])].tolist()}
+        for e in range(int(st["entry_n"])):
+            out.setdefault(int(st["entry_bubble"][e]), []).append((int(st["entry_id"][e]), int(st["entry_value"][e])))
+        return out

@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define EBB_ABI_VERSION 5
+#define EBB_ABI_VERSION 6
 #define EBB_EINVAL (-1)
 #define EBB_ETOOBIG (-2)
 
@@ -156,6 +156,48 @@ typedef struct EbbServerQueue {
     int64_t *stamp, *clock;
     uint8_t *has_character, *gets_bubble;
 } EbbServerQueue;
+
+/* The master's partition and bubble partition over a flight park's rows (exact_ballpark.vec_space.VecSpace's
+ * layer, vec_space.py:777; this build's slice: each ball's filing, the partition's boxes with BoxAllocator's kept
+ * count, the top boxes' bubbles, the bubble dictionaries, the interactive and keep-alive sets, InitializeBubbles,
+ * CopyBubbles, the tick's dead-bubble flags and re-filings). W worlds of N slots (N at most EBB_SPACE_MAX_SLOTS);
+ * `rows` maps a slot to its park row (-1 for none). Every per-slot array is [N][W], every per-entry array [cap][W]
+ * and every key [3][cap][W] (world w's entry e at e W + w), one thread a world. Capacities a world: `boxes` box-table
+ * entries (and the same for the fill's stack), `dicts` bubble dictionaries, `entries` dictionary entries in insertion
+ * order, `sets` members of the interactive sets and of the keep-alive sets. A world that leaves the layer's domain is
+ * flagged (EBB_SPACE_FLAG_*) and left alone by later operations. Field for field the state the reference's layer keeps
+ * in its `st` tensors (vec_space.py:808-830), with a box table in place of its top-box table. */
+#define EBB_SPACE_MAX_SLOTS 128
+enum {  /* the tape's operations, numbered as the reference's OPS (vec_space.py:159) */
+    EBB_SPACE_NONE = 0, EBB_SPACE_ADD = 1, EBB_SPACE_REFILE = 2, EBB_SPACE_INIT_BUBBLES = 3,
+    EBB_SPACE_COPY_BUBBLES = 4, EBB_SPACE_KEEP_ALIVE = 5, EBB_SPACE_SET_INTERACTIVE = 6, EBB_SPACE_ADD_SENSOR = 7,
+    EBB_SPACE_REMOVE_SENSOR = 8, EBB_SPACE_NOTIFY_RANGE = 9, EBB_SPACE_TRACK = 10, EBB_SPACE_REMOVE_BALL = 11,
+    EBB_SPACE_DEAD = 12, EBB_SPACE_AFTER_EVOLVE = 13
+};
+enum {  /* a world's flags, the reference's FLAG bits (vec_space.py:171) and UNDEFINED (a deleted box read) */
+    EBB_SPACE_FLAG_EVENTS = 1, EBB_SPACE_FLAG_TOPS = 2, EBB_SPACE_FLAG_EDGE = 4, EBB_SPACE_FLAG_BOXES = 8,
+    EBB_SPACE_FLAG_DICTS = 16, EBB_SPACE_FLAG_ENTRIES = 32, EBB_SPACE_FLAG_PROXIMITY = 64,
+    EBB_SPACE_FLAG_SENSOR_LIST = 128, EBB_SPACE_FLAG_HUGE = 256, EBB_SPACE_FLAG_BAD_OP = 512,
+    EBB_SPACE_FLAG_SETS = 1024, EBB_SPACE_FLAG_UNDEFINED = 2048
+};
+typedef struct EbbSpaceState {
+    int64_t worlds, slots, boxes, dicts, entries, sets;
+    const int64_t* rows;                                          /* [N][W] */
+    int64_t *level, *key, *mod, *active, *bubble, *old_bubble, *seq;   /* [N][W]; key, mod [3][N][W] */
+    uint8_t *in_park, *keep_alive, *dead, *dropped;                /* [N][W] */
+    int64_t *box_level, *box_key, *box_balls, *box_kids, *box_bubble, *stack;   /* [boxes][W]; key [3][boxes][W] */
+    int64_t *box_n, *free_boxes;                                   /* [W] */
+    int64_t *dict_bubble, *dict_n;                                 /* [dicts][W], [W] */
+    int64_t *entry_bubble, *entry_id, *entry_value, *entry_n;      /* [entries][W], [W] */
+    int64_t *inter_bubble, *inter_id, *inter_n;                    /* [sets][W], [W] */
+    int64_t *keep_bubble, *keep_id, *keep_n;                       /* [sets][W], [W] */
+    int64_t *bubble_id, *seq_next, *flags;                         /* [W] */
+} EbbSpaceState;
+/* K operations a world, applied in order: code, a (a slot), b (an integer argument), each [K][W]. */
+typedef struct EbbSpaceTape {
+    int64_t K;
+    const int64_t *code, *a, *b;
+} EbbSpaceTape;
 
 /* The ABI version (EBB_ABI_VERSION). Replaces xbpm_abi / xbpo_abi (exact_ballpark/vec_modes_cuda.cu:750,
  * vec_orient_cuda.cu:499). */
@@ -310,6 +352,10 @@ int ebb_flight_decay(const EbbFlightState* s, const uint8_t* mask, double neg_kd
  * 16 atan2f(y, x) (floats held in doubles). Replaces xbpm_dlibm and xbpo_libm (vec_modes_cuda.cu:779,
  * vec_orient_cuda.cu:520). */
 int ebb_libm(int func, int64_t n, const double* x, const double* y, double* out, void* stream, int block);
+
+/* The tape's operations on every world, one thread a world, on `stream` (the park's rows are read and, by
+ * SET_INTERACTIVE, written). Replaces xbps_tape_cuda (exact_ballpark/vec_space.py:896). */
+int ebb_space_tape(const EbbFlightState* park, const EbbSpaceState* s, const EbbSpaceTape* t, void* stream, int block);
 
 /* A kernel's resources as loaded on the current device: which 0 the plain tick, 1 the prepass, 2 the tiled tick,
  * 3 the listed-worlds tick, 4 the row move, 7 the combat tick, 8 the composed tick.

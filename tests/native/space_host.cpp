@@ -1,0 +1,10 @@
+// SPDX-License-Identifier: MIT
+// TEST INFRASTRUCTURE, NOT THE PRODUCT. The space layer's per-world program (exact_ballpark_b200/csrc/ebb_space.cuh,
+// which the device kernel runs, one thread a world) compiled for the host with g++, so that the CPU tests hold the
+// same source to the oracle (oracle/space.cpp) without a GPU; the product has no host path.
+#include "../../exact_ballpark_b200/csrc/ebb_space.cuh"
+
+extern "C" int space_tape_host(const EbbFlightState* p, const EbbSpaceState* s, const EbbSpaceTape* t) {
+    for (int64_t w = 0; w < s->worlds; ++w) ebb::space::run_tape(p, s, t, w);
+    return 0;
+}

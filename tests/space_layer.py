@@ -1,0 +1,267 @@
+"""Test harness of the space layer (exact_ballpark_b200.space, csrc/ebb_space.cuh): the golden streams of
+tests/golden/space_trace.py driven through the layer, one world a stream, and the layer's state written as the
+oracle's state text (oracle/space.cpp's `state`) less what the layer does not hold (the sensors' lines, each ball's
+flight-state line, the queries' answers), so that it compares line for line with the oracle's text of the same
+operations.
+
+Two backends: "host", the layer's per-world program compiled for the host (tests/native/space_host.cpp: the same
+source the device runs), and "cuda", the product's VecSpace over a VecModesPark on the device. A stream's ball ids
+are 1 to N (the largest in the streams) and ball id b sits in slot b - 1 of its world, row w N + b - 1 of the park;
+the streams' setters are applied to the park's rows and their re-filings are the layer's operations."""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import struct
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+import space_trace as sp
+
+ROOT = Path(__file__).resolve().parent.parent
+NATIVE = Path(__file__).resolve().parent / "native"
+HOST_LIB = NATIVE / "_build" / "libspace_host.so"
+FRICTION, DT = 1.0e6, 1.0
+_host = None
+
+
+def host_lib() -> ctypes.CDLL:
+    """The host build of the layer's program (g++, the device build's arithmetic flags)."""
+    global _host
+    if _host is not None:
+        return _host
+    src = NATIVE / "space_host.cpp"
+    deps = [src, ROOT / "exact_ballpark_b200/csrc/ebb_space.cuh", ROOT / "exact_ballpark_b200/csrc/ebb_arith.cuh",
+            ROOT / "include/ebb.h"]
+    if not HOST_LIB.exists() or HOST_LIB.stat().st_mtime < max(d.stat().st_mtime for d in deps):
+        HOST_LIB.parent.mkdir(parents=True, exist_ok=True)
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
+                        "-o", str(HOST_LIB), str(src)], check=True)
+    from exact_ballpark_b200 import _native
+    L = ctypes.CDLL(str(HOST_LIB))
+    L.space_tape_host.argtypes = [ctypes.POINTER(_native.FlightState), ctypes.POINTER(_native.SpaceState),
+                                  ctypes.POINTER(_native.SpaceTape)]
+    _host = L
+    return L
+
+
+def f32(x: float) -> float:
+    return struct.unpack("<f", struct.pack("<f", float(x)))[0]
+
+
+class HostPark:
+    """The park's rows the layer reads, as numpy arrays in include/ebb.h's EbbFlightState layout."""
+
+    def __init__(self, n: int):
+        self.n = n
+        self.pos, self.vel = np.zeros((3, n)), np.zeros((3, n))
+        self.old_pos, self.old_vel = np.zeros((3, n)), np.zeros((3, n))
+        self.mass, self.time_factor = np.zeros(n), np.zeros(n)
+        self.radius, self.max_vel = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        self.agility, self.speed_fraction = np.ones(n, np.float32), np.ones(n, np.float32)
+        self.ids = np.arange(1, n + 1, dtype=np.int64)
+        self.mode = np.full(n, 2, np.int32)
+        self.free, self.interactive = np.zeros(n, np.uint8), np.zeros(n, np.uint8)
+
+    def struct(self):
+        from exact_ballpark_b200 import _native
+        s = _native.FlightState()
+        s.n, s.friction, s.dt = self.n, FRICTION, DT
+        for name in ("pos", "vel", "old_pos", "old_vel", "mass", "time_factor", "radius", "max_vel", "agility",
+                     "speed_fraction", "ids", "mode", "interactive"):
+            setattr(s, name, getattr(self, name).ctypes.data)
+        s.free_ = self.free.ctypes.data
+        return s
+
+    def add(self, r: int, a: list) -> None:
+        """AddBall's values for row r (space.py:1097): float parameters as floats, the clamps, the time factor."""
+        mass, radius, max_vel = a[0], f32(a[1]), f32(a[2])
+        self.free[r], self.interactive[r] = int(bool(a[3])), int(bool(a[4]))
+        self.pos[:, r], self.vel[:, r] = a[5:8], a[8:11]
+        self.old_pos[:, r] = [a[5 + i] - a[8 + i] * DT for i in range(3)]
+        self.old_vel[:, r] = a[8:11]
+        self.radius[r] = 0.0 if radius < 0.0 else radius
+        self.mass[r] = 0.0 if mass < 0.0 else mass
+        self.max_vel[r] = 0.0 if max_vel < 0.0 else max_vel
+        ag, sf = f32(a[11]), f32(a[12])
+        self.agility[r] = 1.0 if ag <= 0.0 else ag
+        self.speed_fraction[r] = 0.0 if sf < 0.0 else sf
+        m = float(self.mass[r]) * float(self.agility[r])
+        self.time_factor[r] = 0.0 if m <= 0.0 else math.exp(-FRICTION * DT / m)
+        self.mode[r] = 2
+
+
+class HostLayer:
+    """The layer's state as numpy arrays (VecSpace's tensors, the same shapes), run by the host build."""
+
+    def __init__(self, W: int, n: int, boxes: int | None = None):
+        self.W, self.N = W, n
+        self.B, self.D, self.E, self.S = (boxes or 16 * n + 64), 8 * n + 16, 4 * n + 8, 2 * n + 8
+        self.rows = np.array([[w * n + j for w in range(W)] for j in range(n)], dtype=np.int64)
+        z = lambda *shape, dt=np.int64: np.zeros(shape, dtype=dt)   # noqa: E731
+        B, D, E, S = self.B, self.D, self.E, self.S
+        self.st = {
+            "level": z(n, W) - 1, "key": z(3, n, W), "mod": z(3, n, W) - 2, "active": z(n, W), "bubble": z(n, W) - 1,
+            "old_bubble": z(n, W) - 1, "seq": z(n, W),
+            "in_park": z(n, W, dt=np.uint8), "keep_alive": z(n, W, dt=np.uint8), "dead": z(n, W, dt=np.uint8),
+            "dropped": z(n, W, dt=np.uint8),
+            "box_level": z(B, W) - 1, "box_key": z(3, B, W), "box_balls": z(B, W), "box_kids": z(B, W),
+            "box_bubble": z(B, W) - 1, "stack": z(B, W), "box_n": z(W), "free_boxes": z(W),
+            "dict_bubble": z(D, W), "dict_n": z(W), "entry_bubble": z(E, W), "entry_id": z(E, W),
+            "entry_value": z(E, W), "entry_n": z(W), "inter_bubble": z(S, W), "inter_id": z(S, W), "inter_n": z(W),
+            "keep_bubble": z(S, W), "keep_id": z(S, W), "keep_n": z(W), "bubble_id": z(W), "seq_next": z(W),
+            "flags": z(W)}
+
+    def tape(self, park: HostPark, code, a, b) -> None:
+        from exact_ballpark_b200 import _native
+        s = _native.SpaceState()
+        s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets = self.W, self.N, self.B, self.D, self.E, self.S
+        s.rows = self.rows.ctypes.data
+        for name, arr in self.st.items():
+            setattr(s, name, arr.ctypes.data)
+        code, a, b = (np.ascontiguousarray(np.asarray(x, dtype=np.int64).reshape(-1, self.W)) for x in (code, a, b))
+        t = _native.SpaceTape(code.shape[0], code.ctypes.data, a.ctypes.data, b.ctypes.data)
+        ps = park.struct()
+        host_lib().space_tape_host(ctypes.byref(ps), ctypes.byref(s), ctypes.byref(t))
+
+
+def translate(park: HostPark, w: int, op, n: int) -> tuple:
+    """One golden operation of world w: its effect on the park's rows, and the layer's operation (code, slot, b)."""
+    from exact_ballpark_b200.space import OP
+    code, bid = int(op[0]), int(op[1])
+    a = [float(x) for x in op[2:]]
+    j = bid - 1
+    r = w * n + j
+    if code == sp.ADD:
+        park.add(r, a)
+        return OP["ADD"], j, 0
+    if code == sp.POS:
+        park.pos[:, r] = a[0:3]
+        park.old_pos[:, r] = a[0:3]
+        return OP["REFILE"], j, 0
+    if code == sp.RADIUS:
+        v = f32(a[0])
+        if v < 0.0:
+            return OP["NONE"], -1, 0
+        park.radius[r] = v
+        return OP["REFILE"], j, 0
+    if code == sp.MAXVEL:
+        v = f32(a[0])
+        if v < 0.0:
+            return OP["NONE"], -1, 0
+        park.max_vel[r] = v
+        return OP["REFILE"], j, 0
+    if code == sp.REMOVE:
+        return OP["REMOVE_BALL"], j, 0
+    if code == sp.INIT:
+        return OP["INIT_BUBBLES"], -1, 0
+    if code == sp.COPY:
+        return OP["COPY_BUBBLES"], -1, 0
+    if code == sp.INTERACTIVE:
+        return OP["SET_INTERACTIVE"], j, int(bool(a[0]))
+    if code == sp.KEEPALIVE:
+        return OP["KEEP_ALIVE"], j, 0
+    if code == sp.GOTO and all(math.isfinite(x) for x in a[0:3]):   # GotoPoint: a speed fraction of 0 becomes 1
+        if park.speed_fraction[r] == 0.0:
+            park.speed_fraction[r] = 1.0
+        park.mode[r] = 0
+        return OP["NONE"], -1, 0
+    if code == sp.STOP:
+        park.mode[r] = 2
+        return OP["NONE"], -1, 0
+    return OP["NONE"], -1, 0                              # the cloak attribute, the queries: not the layer's
+
+
+def text(st: dict, park_ids, park_mode, w: int) -> str:
+    """World w's layer state as the oracle's state text (the lines the layer holds)."""
+    n = st["level"].shape[0]
+    col = lambda name: st[name][..., w]                   # noqa: E731
+    level, key, mod, active = col("level"), col("key"), col("mod"), col("active")
+    bubble, old_bubble, in_park = col("bubble"), col("old_bubble"), col("in_park")
+    inter = {}
+    for e in range(int(st["inter_n"][w])):
+        inter.setdefault(int(st["inter_bubble"][e, w]), set()).add(int(st["inter_id"][e, w]))
+    keep = {}
+    for e in range(int(st["keep_n"][w])):
+        keep.setdefault(int(st["keep_bubble"][e, w]), set()).add(int(st["keep_id"][e, w]))
+    out = []
+    slots = sorted((int(park_ids[w * n + j]), j) for j in range(n) if in_park[j])
+    for bid, j in slots:
+        dead = 0 if int(park_mode[w * n + j]) == 3 else int(not inter.get(int(bubble[j])) and
+                                                             not keep.get(int(bubble[j])))
+        act = int(active[j])
+        if level[j] >= 0:
+            head = (f"B {bid} {bubble[j]} {old_bubble[j]} {level[j]} {key[0, j]} {key[1, j]} {key[2, j]} "
+                    f"{mod[0, j]} {mod[1, j]} {mod[2, j]} {act} {dead}")
+            boxes = sorted((key[0, j] + x, key[1, j] + y, key[2, j] + z) for z in (-1, 0, 1) for y in (-1, 0, 1)
+                           for x in (-1, 0, 1) if (act >> (13 + x + 3 * y + 9 * z)) & 1)
+        else:
+            head = f"B {bid} {bubble[j]} {old_bubble[j]} - {mod[0, j]} {mod[1, j]} {mod[2, j]} {act} {dead}"
+            boxes = []
+        out.append(head + "".join(f" {k[0]},{k[1]},{k[2]}" for k in boxes) + "\n")
+    lv = col("box_level")[:int(st["box_n"][w])]
+    out.append("L" + "".join(f" {int((lv == i).sum())}" for i in range(8)) + "\n")
+    undefined = 1 if int(st["flags"][w]) & (1 << 11) else 0
+    out.append(f"F {int(st['free_boxes'][w])} {int(st['bubble_id'][w])} {undefined}\n")
+    dicts = {int(b): [] for b in col("dict_bubble")[:int(st["dict_n"][w])]}
+    for e in range(int(st["entry_n"][w])):
+        dicts.setdefault(int(st["entry_bubble"][e, w]), []).append((int(st["entry_id"][e, w]),
+                                                                     int(st["entry_value"][e, w])))
+    for bub in sorted(dicts):
+        out.append(f"U {bub}" + "".join(f" {k}:{v}" for k, v in dicts[bub]) + "\n")
+    for tag, m in (("I", inter), ("K", keep)):
+        for bub in sorted(m):
+            out.append(f"{tag} {bub}" + "".join(f" {i}" for i in sorted(m[bub])) + "\n")
+    return "".join(out)
+
+
+def oracle_lines(t: str) -> str:
+    """The oracle's state text less the lines the layer does not hold (the sensors', the flight states', answers)."""
+    return "".join(line + "\n" for line in t.splitlines() if line[:1] in ("B", "L", "F", "U", "I", "K"))
+
+
+def drive(streams: list, kernel: str = "host", device=None) -> tuple:
+    """Every stream through the layer, one world each, one operation a launch: (texts [world][op], flags [W])."""
+    W = len(streams)
+    N = int(max(int(np.max(np.asarray(s)[:, 1])) for s in streams))
+    park = HostPark(W * N)
+    park.ids[:] = np.tile(np.arange(1, N + 1, dtype=np.int64), W)       # world w's ball b at row w N + b - 1
+    K = max(len(s) for s in streams)
+    texts = [[] for _ in range(W)]
+    if kernel == "host":
+        layer = HostLayer(W, N)
+        run = lambda code, a, b: layer.tape(park, code, a, b)                       # noqa: E731
+        read = lambda: layer.st                                                     # noqa: E731
+    else:
+        import torch
+        from exact_ballpark_b200.modes import VecModesPark
+        from exact_ballpark_b200.space import VecSpace
+        dpark = VecModesPark(W * N, friction=FRICTION, tick_interval_ms=1000, device=device or "cuda")
+        layer = VecSpace(dpark, np.arange(W * N, dtype=np.int64).reshape(W, N))
+
+        def run(code, a, b):
+            for name in ("pos", "vel", "old_pos", "old_vel", "mass", "time_factor", "radius", "max_vel", "agility",
+                         "speed_fraction", "ids", "mode"):
+                getattr(dpark, "_" + name).copy_(torch.from_numpy(getattr(park, name)).to(getattr(dpark, "_" + name)))
+            dpark._free.copy_(torch.from_numpy(park.free.astype(bool)).to(dpark.dev))
+            dpark._interactive.copy_(torch.from_numpy(park.interactive.astype(bool)).to(dpark.dev))
+            layer.tape(torch.from_numpy(np.asarray(code, dtype=np.int64).reshape(W, 1)),
+                       torch.from_numpy(np.asarray(a, dtype=np.int64).reshape(W, 1)),
+                       torch.from_numpy(np.asarray(b, dtype=np.int64).reshape(W, 1)))
+            park.interactive[:] = dpark._interactive.cpu().numpy().astype(np.uint8)
+
+        read = lambda: {k: v.cpu().numpy() for k, v in layer.st.items()}            # noqa: E731
+    for k in range(K):
+        code, a, b = np.zeros(W, np.int64), np.full(W, -1, np.int64), np.zeros(W, np.int64)
+        for w, ops in enumerate(streams):
+            if k < len(ops):
+                code[w], a[w], b[w] = translate(park, w, ops[k], N)
+        run(code, a, b)
+        st = read()
+        for w, ops in enumerate(streams):
+            if k < len(ops):
+                texts[w].append(text(st, park.ids, park.mode, w))
+    return texts, read()["flags"].copy()

@@ -26,7 +26,7 @@ def test_the_library_exports_every_declared_entry_point():
 
 def test_abi_version_and_scratch_size():
     lib = _native.lib()
-    assert lib.ebb_abi() == _native.ABI == 5
+    assert lib.ebb_abi() == _native.ABI == 6
     assert lib.ebb_flight_scratch_bytes(0) == 0
     b = lib.ebb_flight_scratch_bytes(1000)
     assert b >= 1000 * (8 * 7 + 1) and b % 256 == 0
@@ -62,3 +62,20 @@ def test_the_server_tick_refuses_bad_arguments_before_launching():
     assert call(0) == -1                                  # no world table
     assert ctypes.sizeof(_native.ServerState) == ctypes.sizeof(_native.FlightState) + 16 + 14 * 8 + 16
     assert ctypes.sizeof(_native.ServerQueue) == 8 + 17 * 8
+
+
+def test_the_space_tape_refuses_bad_arguments_before_launching():
+    lib = _native.lib()
+    p, s, t = _native.FlightState(), _native.SpaceState(), _native.SpaceTape()
+    call = lambda block=128: lib.ebb_space_tape(ctypes.byref(p), ctypes.byref(s), ctypes.byref(t), None, block)  # noqa: E731
+    s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets, t.K = 4, 10, 64, 16, 16, 16, 1
+    assert call(block=100) == -1 and call(block=256) == -1
+    assert call() == -1                                   # no state buffers
+    s.slots = 129
+    assert call() == -1                                   # more than EBB_SPACE_MAX_SLOTS
+    s.slots, s.boxes = 10, 0
+    assert call() == -1                                   # no box table
+    s.boxes, s.worlds = 64, 0
+    assert call() == 0                                    # no worlds: nothing to do
+    s.worlds, t.K = 4, 0
+    assert call() == 0                                    # no operations

@@ -1,0 +1,96 @@
+"""The space layer (exact_ballpark_b200.space over csrc/ebb_space.cuh) against the oracle (oracle/space.cpp, held to
+the reference's own SpaceBallpark by tests/test_space_oracle.py): the golden streams of tests/golden/space_bubbles.npz
+(mixed operations, long streams, the sweeps past BoxAllocator's 256 kept boxes) driven through the layer, one world a
+stream, and after every operation each ball's filing, bubble and old bubble, the dead-bubble flag, the live boxes per
+level, BoxAllocator's kept count, the next bubble id, the bubble dictionaries in their order and the interactive and
+keep-alive sets compared with the oracle's state text of the same operations. The streams' sensor operations are left
+out on both sides (the sensors are not in the layer's slice). On the CPU the layer's per-world program runs as its
+host build (tests/native/space_host.cpp, the same source); on a GPU the product's VecSpace runs it, one CUDA thread a
+world, and must give the same texts and the same state, word for word."""
+
+import numpy as np
+import pytest
+
+import space_layer as sl
+import space_trace as sp
+from oracle import space_world
+
+FAMILIES = ("mixed", "long", "sweep")
+
+
+def _streams(families=FAMILIES):
+    out = []
+    for sc in sp.load(sp.GOLDEN / "space_bubbles"):
+        if sc["seed"].split("-")[0] in families:
+            keep = ~np.isin(sc["ops"][:, 0], (sp.SENSOR, sp.UNSENSOR))
+            out.append(dict(sc, ops=sc["ops"][keep]))
+    return out
+
+
+def _oracle_texts(sc):
+    return [sl.oracle_lines(t) for t in space_world.run(sc["ops"], seed=sc["rand_seed"])]
+
+
+def test_the_layers_program_matches_the_oracle_after_every_operation():
+    scs = _streams()
+    assert len(scs) == 72
+    texts, flags = sl.drive([sc["ops"] for sc in scs], "host")
+    assert not flags.any()
+    bad = []
+    for sc, got in zip(scs, texts):
+        want = _oracle_texts(sc)
+        if got != want:
+            bad.append((sc["seed"], next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
+    assert not bad, f"{len(bad)} worlds differ, first {bad[:3]}"
+
+
+def test_the_streams_reach_the_layers_paths():
+    scs = _streams()
+    texts, _ = sl.drive([sc["ops"] for sc in scs], "host")
+    lines = [line for t in texts for text in t for line in text.splitlines()]
+    assert max(int(x.split()[1]) for x in lines if x.startswith("F ")) == 256   # BoxAllocator full, later deletions
+    assert sum(1 for x in lines if x.startswith("B ") and " - " not in x and int(x.split()[11]) == (1 << 27) - 1) > 100
+    assert max(int(x.split()[2]) for x in lines if x.startswith("F ")) >= 5      # bubbles made and joined
+    assert any(":-1" in x for x in lines if x.startswith("U "))                 # a ball that left, before CopyBubbles
+    assert any(x.startswith("K ") for x in lines) and any(x.startswith("I ") for x in lines)
+
+
+def test_a_planted_fault_in_the_oracle_is_seen():
+    sc = _streams(("mixed",))[0]
+    texts, _ = sl.drive([sc["ops"]], "host")
+    ops = sc["ops"].copy()
+    k = next(i for i in range(len(ops)) if int(ops[i, 0]) == sp.ADD)
+    ops[k, 7] += sp.TOP                                    # the oracle's ball added a top box further along x
+    want = [sl.oracle_lines(t) for t in space_world.run(ops, seed=sc["rand_seed"])]
+    assert texts[0] != want
+
+
+def test_a_full_box_table_flags_the_world_and_leaves_it_alone():
+    sc = _streams(("sweep",))[0]
+    park = sl.HostPark(40)
+    park.ids[:] = np.arange(1, 41)
+    layer = sl.HostLayer(1, 40, boxes=8)
+    flagged_at = None
+    for k, op in enumerate(sc["ops"][:200]):
+        code, a, b = sl.translate(park, 0, op, 40)
+        layer.tape(park, [code], [a], [b])
+        if layer.st["flags"][0] and flagged_at is None:
+            flagged_at = k
+            frozen = {n: v.copy() for n, v in layer.st.items()}
+    assert flagged_at is not None and layer.st["flags"][0] & 8                  # EBB_SPACE_FLAG_BOXES
+    assert all((layer.st[n] == frozen[n]).all() for n in frozen)                # nothing ran after the flag
+
+
+@pytest.mark.gpu
+def test_the_device_layer_matches_its_host_program_word_for_word():
+    import torch
+    assert torch.cuda.is_available()
+    scs = _streams()
+    streams = [sc["ops"] for sc in scs]
+    got, flags = sl.drive(streams, "cuda")
+    want, _ = sl.drive(streams, "host")
+    assert not flags.any()
+    bad = [sc["seed"] for sc, g, w in zip(scs, got, want) if g != w]
+    assert not bad, f"{len(bad)} worlds differ from the host program, first {bad[:3]}"
+    bad = [sc["seed"] for sc, g in zip(scs, got) if g != _oracle_texts(sc)]
+    assert not bad, f"{len(bad)} worlds differ from the oracle, first {bad[:3]}"
