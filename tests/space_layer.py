@@ -265,3 +265,59 @@ def drive(streams: list, kernel: str = "host", device=None) -> tuple:
             if k < len(ops):
                 texts[w].append(text(st, park.ids, park.mode, w))
     return texts, read()["flags"].copy()
+
+
+def drive_ticks(ops, device="cuda") -> list:
+    """One ticking stream (GOTO and STOP ships, tests/golden/space_trace.py's tick_ops) through VecSpace over a
+    VecModesPark on the device, its ticks the layer's `tick` (dead bubbles skipped, the re-filings after): the texts
+    after every operation. The park is the state's owner: AddBall writes its row, GotoPoint and Stop are its commands;
+    the sensors' operations are left out."""
+    import torch
+    from exact_ballpark_b200.modes import VecModesPark
+    from exact_ballpark_b200.space import VecSpace
+    n = int(np.max(np.asarray(ops)[:, 1]))
+    park = VecModesPark(n, friction=FRICTION, tick_interval_ms=1000, device=device)
+    layer = VecSpace(park, np.arange(n, dtype=np.int64).reshape(1, n))
+    host = HostPark(n)
+    out = []
+    for op in ops:
+        code, bid = int(op[0]), int(op[1])
+        a = [float(x) for x in op[2:]]
+        j = bid - 1
+        mask = torch.zeros(n, dtype=torch.bool, device=park.dev)
+        if 0 <= j < n:
+            mask[j] = True
+        if code == sp.TICK:
+            layer.tick()
+        elif code == sp.ADD:
+            host.add(j, a)
+            for name in ("pos", "vel", "old_pos", "old_vel", "mass", "time_factor", "radius", "max_vel", "agility",
+                         "speed_fraction", "mode"):
+                getattr(park, "_" + name)[..., j] = torch.as_tensor(getattr(host, name)[..., j]).to(
+                    getattr(park, "_" + name))
+            park._free[j], park._interactive[j] = bool(host.free[j]), bool(host.interactive[j])
+            park._massive[j] = bool(a[13])
+            park._last_g[:, j] = 0.0
+            layer.ops([[("ADD", j)]])
+        elif code == sp.POS:
+            park._pos[:, j] = torch.tensor(a[0:3], dtype=torch.float64, device=park.dev)
+            park._old_pos[:, j] = torch.tensor(a[0:3], dtype=torch.float64, device=park.dev)
+            layer.ops([[("REFILE", j)]])
+        elif code == sp.GOTO:
+            park.goto_point(mask, torch.tensor([a[0:3]] * n, dtype=torch.float64, device=park.dev))
+        elif code == sp.STOP:
+            park.stop(mask)
+        elif code == sp.REMOVE:
+            park.stop(mask)
+            layer.ops([[("REMOVE_BALL", j)]])
+        elif code == sp.INIT:
+            layer.ops([[("INIT_BUBBLES",)]])
+        elif code == sp.COPY:
+            layer.ops([[("COPY_BUBBLES",)]])
+        elif code == sp.INTERACTIVE:
+            layer.ops([[("SET_INTERACTIVE", j, int(bool(a[0])))]])
+        elif code == sp.KEEPALIVE:
+            layer.ops([[("KEEP_ALIVE", j)]])
+        st = {k: v.cpu().numpy() for k, v in layer.st.items()}
+        out.append(text(st, park._ids.cpu().numpy(), park._mode.cpu().numpy(), 0))
+    return out

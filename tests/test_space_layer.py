@@ -94,3 +94,21 @@ def test_the_device_layer_matches_its_host_program_word_for_word():
     assert not bad, f"{len(bad)} worlds differ from the host program, first {bad[:3]}"
     bad = [sc["seed"] for sc, g in zip(scs, got) if g != _oracle_texts(sc)]
     assert not bad, f"{len(bad)} worlds differ from the oracle, first {bad[:3]}"
+
+
+@pytest.mark.gpu
+def test_the_layers_tick_over_the_flight_park_matches_the_oracle():
+    """The ticking streams (GOTO and STOP ships across top boxes and bubbles): VecSpace.tick over a VecModesPark (the
+    dead bubbles' rows skipped by the park's tick, then the re-filings of the balls that moved, in ascending id)
+    against the oracle's tick, after every operation."""
+    import torch
+    assert torch.cuda.is_available()
+    scs = _streams(("tick",))
+    assert len(scs) == 40
+    bad = []
+    for sc in scs:
+        got = sl.drive_ticks(sc["ops"])
+        want = _oracle_texts(sc)
+        if got != want:
+            bad.append((sc["seed"], next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
+    assert not bad, f"{len(bad)} worlds differ, first {bad[:3]}"
