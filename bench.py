@@ -578,6 +578,63 @@ def server_cpu_sample(worlds: int, warmup: int, steps: int) -> dict:
                       f"C++ oracle's flight park (its tick on {threads} threads over disjoint worlds)"}
 
 
+def space_runs(args, dev) -> dict:
+    """The space layer (exact_ballpark_b200.space: filing, boxes, bubbles, dictionaries, dead rows, the tick's
+    re-filings; one thread a world) over the flight park: --space-worlds worlds of 128 slots with ragged ship counts
+    (log-uniform 1 to 128, the ragged benchmark's draw: ragged_flight_worlds, follow, orbit and warp, positions in a
+    +-50 km cube a world), loaded and filed, then --space-steps ticks of VecSpace.tick after warm-up, each timed with
+    CUDA events: the whole tick (DEAD, the park's tick with the dead rows skipped, AFTER_EVOLVE) and the layer's two
+    launches alone; the worlds a full table flagged are counted. Not a headline line: the sensors are not in the layer
+    yet."""
+    import torch
+
+    from exact_ballpark_b200 import VecModesPark
+    from exact_ballpark_b200.modes import WARP
+    from exact_ballpark_b200.space import VecSpace
+    from exact_ballpark_b200.workloads import ragged_flight_worlds
+    W, N = args.space_worlds, 128
+    fw = ragged_flight_worlds(7, W, N)
+    sizes = fw.sizes
+    n = sum(sizes)
+    park = VecModesPark(n, device=dev)
+    park.load_columns(fw.packed().cols)
+    fw.apply(park)
+    slots = np.full((W, N), -1, dtype=np.int64)
+    start = 0
+    for w, k in enumerate(sizes):
+        slots[w, :k] = np.arange(start, start + k)
+        start += k
+    space = VecSpace(park, slots, boxes=64 * N + 64, entries=16 * N + 64)   # warpers file far from their worlds
+    space.load()
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        space.tick()
+    ev = lambda: torch.cuda.Event(enable_timing=True)     # noqa: E731
+    whole = layer = 0.0
+    for _ in range(args.space_steps):
+        e = [ev() for _ in range(6)]
+        e[0].record(stream)
+        dead = space.dead_rows()
+        e[1].record(stream)
+        warp_proper = ((park._mode == WARP) & (park._effect_stamp >= 0) & park._free & ~park._moribund & ~dead)
+        saved = park._moribund.clone()
+        park._moribund.logical_or_(dead)
+        park.evolve()
+        park._moribund.copy_(saved)
+        dropped = warp_proper & (park._mode != WARP)
+        e[2].record(stream)
+        space.after_evolve(dropped)
+        e[3].record(stream)
+        e[3].synchronize()
+        whole += e[0].elapsed_time(e[3])
+        layer += e[0].elapsed_time(e[1]) + e[2].elapsed_time(e[3])
+    K = args.space_steps
+    return {"worlds": W, "slots": N, "ships": n, "steps": K, "ms_per_tick": whole / K,
+            "layer_ms_per_tick": layer / K, "ship_ticks_per_s": n * K / (whole * 1e-3),
+            "layer_share": layer / whole, "dead_rows_last": int(dead.sum()),
+            "flagged_worlds": int((space.st["flags"] != 0).sum()), "boxes_max": int(space.st["box_n"].max())}
+
+
 def server_runs(args, dev) -> dict:
     """The server layer (exact_ballpark_b200.server) over the flight park at the reference's server benchmark shape
     (benchmarks/server_speed.py): --server-worlds worlds of 4 ships, each flown by a pilot that sends GotoDirection
@@ -709,7 +766,8 @@ def main() -> None:
     ap.add_argument("--collide-worlds", type=int, default=65536)
     ap.add_argument("--collide-steps", type=int, default=50)
     ap.add_argument("--no-combat", action="store_true")
-    ap.add_argument("--only", choices=("ragged", "collide", "collide_statics", "combat", "composed", "serve", "server"),
+    ap.add_argument("--only", choices=("ragged", "collide", "collide_statics", "combat", "composed", "serve", "server",
+                                       "space"),
                     default=None, help="run one section alone on one GPU and print it (for profiling); the default "
                                        "run prints the headline line with every section")
     ap.add_argument("--combat-worlds", type=int, default=65536)
@@ -717,6 +775,8 @@ def main() -> None:
     ap.add_argument("--no-server", action="store_true")
     ap.add_argument("--server-worlds", type=int, default=65536)
     ap.add_argument("--server-steps", type=int, default=100)
+    ap.add_argument("--space-worlds", type=int, default=20000)
+    ap.add_argument("--space-steps", type=int, default=5)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-seconds", type=float, default=6.0)
     ap.add_argument("--serve-budget-gb", type=float, default=80.0)
@@ -752,7 +812,8 @@ def main() -> None:
         run = {"ragged": lambda: ragged_runs(args, dev), "collide": lambda: collide_runs(args, dev),
                "collide_statics": lambda: collide_runs(args, dev, statics=True),
                "combat": lambda: combat_runs(args, dev), "composed": lambda: combat_runs(args, dev, composed=True),
-               "serve": lambda: serve_runs(args, dev), "server": lambda: server_runs(args, dev)}[args.only]
+               "serve": lambda: serve_runs(args, dev), "server": lambda: server_runs(args, dev),
+               "space": lambda: space_runs(args, dev)}[args.only]
         print(json.dumps({"metric": METRIC, "section": args.only, args.only: run()}), flush=True)
         return
     dist = None
