@@ -586,6 +586,7 @@ def space_runs(args, dev) -> dict:
     CUDA events: the whole tick (DEAD, the park's tick with the dead rows skipped, AFTER_EVOLVE) and the layer's two
     launches alone; the worlds a full table flagged are counted. Not a headline line: the sensors are not in the layer
     yet."""
+    import numpy as np
     import torch
 
     from exact_ballpark_b200 import VecModesPark
