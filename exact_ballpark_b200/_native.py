@@ -64,7 +64,7 @@ class ServerQueue(ctypes.Structure):
                                                   "gets_bubble")])
 
 
-SPACE_SLOT_FIELDS = ("level", "key", "mod", "active", "bubble", "old_bubble", "seq")
+SPACE_SLOT_FIELDS = ("level", "key", "mod", "active", "bubble", "old_bubble", "seq", "my_box", "my_top")
 SPACE_FLAG_FIELDS = ("in_park", "keep_alive", "dead", "dropped")
 SPACE_BOX_FIELDS = ("box_level", "box_key", "box_balls", "box_kids", "box_bubble", "stack", "box_n", "free_boxes")
 SPACE_DICT_FIELDS = ("dict_bubble", "dict_n", "entry_bubble", "entry_id", "entry_value", "entry_n", "inter_bubble",

@@ -205,6 +205,8 @@ struct World {
     }
     EBB_HD void clear_filing(int64_t j) const {
         lvl(j) = -1;
+        I(s->my_box, j) = -1;
+        I(s->my_top, j) = -1;
         active(j) = 0;
         for (int c = 0; c < 3; ++c) mod(j, c) = -2;
     }
@@ -432,6 +434,8 @@ struct World {
         insert_in_box(j, box1);
         const int64_t top = topmost_of(box1);
         if (top >= 0) I(s->box_bubble, top) = new_bubble;
+        I(s->my_box, j) = box1;                            // (entries stay put while the ball is filed in them)
+        I(s->my_top, j) = top;
         int64_t act = int64_t(1) << 13;
         const int64_t ix = key(j, 0), iy = key(j, 1), iz = key(j, 2);
         const int64_t row_j = row(j);
@@ -467,11 +471,14 @@ struct World {
         const int level0 = level_for(inflated);
         int64_t k[3];
         key_for(level0, x, k);
-        const int64_t box1 = get_box(k[0], k[1], k[2], level0);
+        // the ball's own box when it stays in it (the common re-filing): its entry and its top's, without a scan
+        const bool same = lvl(j) == level0 && key(j, 0) == k[0] && key(j, 1) == k[1] && key(j, 2) == k[2] &&
+                          I(s->my_box, j) >= 0 && I(s->my_top, j) >= 0;
+        const int64_t box1 = same ? I(s->my_box, j) : get_box(k[0], k[1], k[2], level0);
         if (box1 < 0) return;
         int64_t key0[3];
         for (int c = 0; c < 3; ++c) key0[c] = I3(s->box_key, c, box1, B);
-        const int64_t top = topmost_of(box1);
+        const int64_t top = same ? I(s->my_top, j) : topmost_of(box1);
         int64_t new_bubble = I(s->box_bubble, top);
         int fate[2] = {0, 0};
         if (new_bubble == -1) {
@@ -551,10 +558,7 @@ struct World {
                 I(s->bubble, j) = -1;
                 continue;
             }
-            const int64_t g = level_grid((int)lvl(j));
-            const int64_t my_box = box_find((int)lvl(j), clamp_key(key(j, 0), g), clamp_key(key(j, 1), g),
-                                            clamp_key(key(j, 2), g));
-            const int64_t top = my_box >= 0 ? topmost_of(my_box) : -1;
+            const int64_t top = I(s->my_top, j);
             if (top < 0) continue;
             if (I(s->box_bubble, top) != -1) {
                 I(s->old_bubble, j) = I(s->bubble, j);

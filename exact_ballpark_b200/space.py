@@ -64,7 +64,7 @@ class VecSpace:
         z = lambda *shape, dt=I64: torch.zeros(*shape, dtype=dt, device=d)   # noqa: E731
         self.st = {
             "level": z(N, W) - 1, "key": z(3, N, W), "mod": z(3, N, W) - 2, "active": z(N, W), "bubble": z(N, W) - 1,
-            "old_bubble": z(N, W) - 1, "seq": z(N, W),
+            "old_bubble": z(N, W) - 1, "seq": z(N, W), "my_box": z(N, W) - 1, "my_top": z(N, W) - 1,
             "in_park": z(N, W, dt=U8), "keep_alive": z(N, W, dt=U8), "dead": z(N, W, dt=U8), "dropped": z(N, W, dt=U8),
             "box_level": z(self.B, W) - 1, "box_key": z(3, self.B, W), "box_balls": z(self.B, W),
             "box_kids": z(self.B, W), "box_bubble": z(self.B, W) - 1, "stack": z(self.B, W), "box_n": z(W),

@@ -184,6 +184,7 @@ typedef struct EbbSpaceState {
     int64_t worlds, slots, boxes, dicts, entries, sets;
     const int64_t* rows;                                          /* [N][W] */
     int64_t *level, *key, *mod, *active, *bubble, *old_bubble, *seq;   /* [N][W]; key, mod [3][N][W] */
+    int64_t *my_box, *my_top;          /* [N][W] the box-table entries of a filed ball's box and of its top box */
     uint8_t *in_park, *keep_alive, *dead, *dropped;                /* [N][W] */
     int64_t *box_level, *box_key, *box_balls, *box_kids, *box_bubble, *stack;   /* [boxes][W]; key [3][boxes][W] */
     int64_t *box_n, *free_boxes;                                   /* [W] */

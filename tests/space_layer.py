@@ -105,7 +105,7 @@ class HostLayer:
         B, D, E, S = self.B, self.D, self.E, self.S
         self.st = {
             "level": z(n, W) - 1, "key": z(3, n, W), "mod": z(3, n, W) - 2, "active": z(n, W), "bubble": z(n, W) - 1,
-            "old_bubble": z(n, W) - 1, "seq": z(n, W),
+            "old_bubble": z(n, W) - 1, "seq": z(n, W), "my_box": z(n, W) - 1, "my_top": z(n, W) - 1,
             "in_park": z(n, W, dt=np.uint8), "keep_alive": z(n, W, dt=np.uint8), "dead": z(n, W, dt=np.uint8),
             "dropped": z(n, W, dt=np.uint8),
             "box_level": z(B, W) - 1, "box_key": z(3, B, W), "box_balls": z(B, W), "box_kids": z(B, W),
