@@ -66,7 +66,8 @@ class ServerQueue(ctypes.Structure):
 
 SPACE_SLOT_FIELDS = ("level", "key", "mod", "active", "bubble", "old_bubble", "seq", "my_box", "my_top")
 SPACE_FLAG_FIELDS = ("in_park", "keep_alive", "dead", "dropped")
-SPACE_BOX_FIELDS = ("box_level", "box_key", "box_balls", "box_kids", "box_bubble", "stack", "box_n", "free_boxes")
+SPACE_BOX_FIELDS = ("box_level", "box_key", "box_balls", "box_kids", "box_bubble", "stack", "box_n", "free_boxes",
+                    "box_hash", "box_free", "box_free_n")
 SPACE_DICT_FIELDS = ("dict_bubble", "dict_n", "entry_bubble", "entry_id", "entry_value", "entry_n", "inter_bubble",
                      "inter_id", "inter_n", "keep_bubble", "keep_id", "keep_n", "bubble_id", "seq_next", "flags")
 

@@ -11,7 +11,8 @@
 //
 // Layout: W worlds of N slots; every per-slot array is [N][W] and every per-entry array [cap][W] (world w's entry e
 // at e W + w), so that the threads of a warp, one world each, touch consecutive words. A world's boxes live in a
-// table of `boxes` entries (level -1 for a free entry), found by scanning it. Exactness: the filing's double
+// table of `boxes` entries (level -1 for a free entry, the free ones on a stack), found through a hash index of
+// 2 `boxes` slots (linear probing, deletion by moving the run back). Exactness: the filing's double
 // arithmetic through ebb_arith.cuh (correctly rounded single operations), compiled with -fmad=false.
 #pragma once
 
@@ -66,15 +67,64 @@ struct World {
     EBB_HD int64_t id(int64_t j) const { return p->ids[row(j)]; }
     EBB_HD bool interactive(int64_t j) const { return p->interactive[row(j)] != 0; }
 
-    // ---- the box table ----
+    // ---- the box table and its index (linear probing over 2 B slots, each entry + 1, 0 for an empty slot) ----
+    EBB_HD int64_t home(int level, int64_t kx, int64_t ky, int64_t kz) const {
+        uint64_t h = (uint64_t)kx * 0x9E3779B97F4A7C15ull;
+        h ^= (uint64_t)ky * 0xC2B2AE3D27D4EB4Full + (h << 6) + (h >> 2);
+        h ^= (uint64_t)kz * 0x165667B19E3779F9ull + (h << 6) + (h >> 2);
+        h ^= (uint64_t)level * 0x27D4EB2F165667C5ull;
+        h ^= h >> 29;
+        return (int64_t)(h % (uint64_t)(2 * B));
+    }
+    EBB_HD bool is_box(int64_t e, int level, int64_t kx, int64_t ky, int64_t kz) const {
+        return I(s->box_level, e) == level && I3(s->box_key, 0, e, B) == kx && I3(s->box_key, 1, e, B) == ky &&
+               I3(s->box_key, 2, e, B) == kz;
+    }
     EBB_HD int64_t box_find(int level, int64_t kx, int64_t ky, int64_t kz) const {
-        const int64_t n = one(s->box_n);
-        for (int64_t e = 0; e < n; ++e) {
-            if (I(s->box_level, e) != level) continue;
-            if (I3(s->box_key, 0, e, B) == kx && I3(s->box_key, 1, e, B) == ky && I3(s->box_key, 2, e, B) == kz)
-                return e;
+        const int64_t H = 2 * B;
+        int64_t i = home(level, kx, ky, kz);
+        for (int64_t probe = 0; probe < H; ++probe) {
+            const int64_t v = I(s->box_hash, i);
+            if (v == 0) return -1;
+            if (is_box(v - 1, level, kx, ky, kz)) return v - 1;
+            i = i + 1 == H ? 0 : i + 1;
         }
         return -1;
+    }
+    EBB_HD void hash_insert(int64_t e) {
+        const int64_t H = 2 * B;
+        int64_t i = home((int)I(s->box_level, e), I3(s->box_key, 0, e, B), I3(s->box_key, 1, e, B),
+                         I3(s->box_key, 2, e, B));
+        for (int64_t probe = 0; probe < H; ++probe) {
+            if (I(s->box_hash, i) == 0) {
+                I(s->box_hash, i) = e + 1;
+                return;
+            }
+            i = i + 1 == H ? 0 : i + 1;
+        }
+        flag(F_BOXES);                                     // (never: at most B entries in 2 B slots)
+    }
+    // the entry leaves the index; the entries after it in its run move back so that every probe still finds them
+    EBB_HD void hash_erase(int64_t e) {
+        const int64_t H = 2 * B;
+        int64_t i = home((int)I(s->box_level, e), I3(s->box_key, 0, e, B), I3(s->box_key, 1, e, B),
+                         I3(s->box_key, 2, e, B));
+        int64_t probe = 0;
+        for (; probe < H && I(s->box_hash, i) != e + 1; ++probe) i = i + 1 == H ? 0 : i + 1;
+        if (probe == H) return;
+        int64_t j = i;
+        for (int64_t step = 0; step < H; ++step) {
+            j = j + 1 == H ? 0 : j + 1;
+            const int64_t v = I(s->box_hash, j);
+            if (v == 0) break;
+            const int64_t k = home((int)I(s->box_level, v - 1), I3(s->box_key, 0, v - 1, B),
+                                   I3(s->box_key, 1, v - 1, B), I3(s->box_key, 2, v - 1, B));
+            const bool stays = i <= j ? (i < k && k <= j) : (i < k || k <= j);
+            if (stays) continue;
+            I(s->box_hash, i) = v;
+            i = j;
+        }
+        I(s->box_hash, i) = 0;
     }
     // a key at the grid's edge, where Partition clamps (two neighbours would be one box): outside this layer
     EBB_HD bool edge(int64_t ix, int64_t iy, int64_t iz, int level) const {
@@ -91,11 +141,7 @@ struct World {
     EBB_HD int64_t new_box(int level, int64_t kx, int64_t ky, int64_t kz) {
         int64_t e = -1;
         const int64_t n = one(s->box_n);
-        for (int64_t i = 0; i < n; ++i)
-            if (I(s->box_level, i) < 0) {
-                e = i;
-                break;
-            }
+        if (one(s->box_free_n) > 0) e = I(s->box_free, --one(s->box_free_n));   // a released entry again
         if (e < 0) {
             if (n >= B) {
                 flag(F_BOXES);
@@ -112,6 +158,7 @@ struct World {
         I(s->box_balls, e) = 0;
         I(s->box_kids, e) = 0;
         I(s->box_bubble, e) = -1;
+        hash_insert(e);
         return e;
     }
     // GetBox: the box, made with its missing ancestors when missing (a parent's key is its child's over 4)
@@ -150,7 +197,9 @@ struct World {
                                   I3(s->box_key, 2, cur, B) >> 2);
                 if (parent >= 0) --I(s->box_kids, parent);
             }
+            hash_erase(cur);
             I(s->box_level, cur) = -1;
+            I(s->box_free, one(s->box_free_n)++) = cur;
             for (int k = 0; k < 2; ++k)
                 if (watch[k] == cur) fate[k] = keep ? 1 : 2;
             if (keep) ++one(s->free_boxes);

@@ -68,7 +68,7 @@ class VecSpace:
             "in_park": z(N, W, dt=U8), "keep_alive": z(N, W, dt=U8), "dead": z(N, W, dt=U8), "dropped": z(N, W, dt=U8),
             "box_level": z(self.B, W) - 1, "box_key": z(3, self.B, W), "box_balls": z(self.B, W),
             "box_kids": z(self.B, W), "box_bubble": z(self.B, W) - 1, "stack": z(self.B, W), "box_n": z(W),
-            "free_boxes": z(W),
+            "free_boxes": z(W), "box_hash": z(2 * self.B, W), "box_free": z(self.B, W), "box_free_n": z(W),
             "dict_bubble": z(self.D, W), "dict_n": z(W), "entry_bubble": z(self.E, W), "entry_id": z(self.E, W),
             "entry_value": z(self.E, W), "entry_n": z(W), "inter_bubble": z(self.S, W), "inter_id": z(self.S, W),
             "inter_n": z(W), "keep_bubble": z(self.S, W), "keep_id": z(self.S, W), "keep_n": z(W),

@@ -188,6 +188,8 @@ typedef struct EbbSpaceState {
     uint8_t *in_park, *keep_alive, *dead, *dropped;                /* [N][W] */
     int64_t *box_level, *box_key, *box_balls, *box_kids, *box_bubble, *stack;   /* [boxes][W]; key [3][boxes][W] */
     int64_t *box_n, *free_boxes;                                   /* [W] */
+    int64_t *box_hash;              /* [2 boxes][W] the table's index: entry + 1 by (level, key), linear probing */
+    int64_t *box_free, *box_free_n;                                /* [boxes][W] the free entries, [W] their count */
     int64_t *dict_bubble, *dict_n;                                 /* [dicts][W], [W] */
     int64_t *entry_bubble, *entry_id, *entry_value, *entry_n;      /* [entries][W], [W] */
     int64_t *inter_bubble, *inter_id, *inter_n;                    /* [sets][W], [W] */

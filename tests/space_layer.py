@@ -110,6 +110,7 @@ class HostLayer:
             "dropped": z(n, W, dt=np.uint8),
             "box_level": z(B, W) - 1, "box_key": z(3, B, W), "box_balls": z(B, W), "box_kids": z(B, W),
             "box_bubble": z(B, W) - 1, "stack": z(B, W), "box_n": z(W), "free_boxes": z(W),
+            "box_hash": z(2 * B, W), "box_free": z(B, W), "box_free_n": z(W),
             "dict_bubble": z(D, W), "dict_n": z(W), "entry_bubble": z(E, W), "entry_id": z(E, W),
             "entry_value": z(E, W), "entry_n": z(W), "inter_bubble": z(S, W), "inter_id": z(S, W), "inter_n": z(W),
             "keep_bubble": z(S, W), "keep_id": z(S, W), "keep_n": z(W), "bubble_id": z(W), "seq_next": z(W),
