@@ -322,3 +322,103 @@ def drive_ticks(ops, device="cuda") -> list:
         st = {k: v.cpu().numpy() for k, v in layer.st.items()}
         out.append(text(st, park._ids.cpu().numpy(), park._mode.cpu().numpy(), 0))
     return out
+
+
+def drive_ticks_host(ops) -> list:
+    """drive_ticks on the CPU, for the ticking and the mode streams: the flight oracle's park (oracle/park.py's
+    OraclePark, its tick the C++ oracle) owns the rows (AddBall, GotoPoint, Stop, FollowBall and Orbit with the
+    layer's bubbles for their same-bubble test, WarpTo, RemoveBall's Stop and StopAllFollowers) and ticks them with
+    the dead rows flagged moribund for the call; the layer's host build runs DEAD and AFTER_EVOLVE around the tick (the
+    warp drop-outs among its re-filings), as VecSpace.tick does on the device."""
+    from exact_ballpark_b200.space import OP
+    from oracle.park import OraclePark
+    n = int(np.max(np.asarray(ops)[:, 1]))
+    op = OraclePark(n, friction=FRICTION, tick_interval_ms=1000)
+    host, layer = HostPark(n), HostLayer(1, n)
+
+    def pull() -> None:                                   # the layer's view of the oracle park's rows
+        for name in ("pos", "vel", "old_pos", "old_vel"):
+            getattr(host, name)[:] = getattr(op, name).T
+        for name in ("mass", "time_factor"):
+            getattr(host, name)[:] = getattr(op, name)
+        for name in ("radius", "max_vel", "agility", "speed_fraction"):
+            getattr(host, name)[:] = getattr(op, name).astype(np.float32)
+        host.ids[:] = op.ids
+        host.mode[:] = op.mode.astype(np.int32)
+        host.free[:] = op.free.astype(np.uint8)
+        host.interactive[:] = op.interactive.astype(np.uint8)
+
+    def run(name: str, j: int = -1, b: int = 0) -> None:
+        pull()
+        layer.tape(host, [OP[name]], [j], [b])
+        op.interactive = host.interactive.astype(bool)
+
+    out = []
+    for row in ops:
+        code, bid = int(row[0]), int(row[1])
+        a = [float(x) for x in row[2:]]
+        j = bid - 1
+        mask = np.zeros(n, dtype=bool)
+        if 0 <= j < n:
+            mask[j] = True
+        if code == sp.TICK:
+            run("DEAD")
+            dead = layer.st["dead"][:, 0].astype(bool)
+            warp_proper = (op.mode == 3) & (op.effect_stamp >= 0) & op.free & ~op.moribund & ~dead
+            saved = op.moribund.copy()
+            op.moribund = saved | dead
+            op.evolve()
+            op.moribund = saved
+            layer.st["dropped"][:, 0] = (warp_proper & (op.mode != 3)).astype(np.uint8)
+            run("AFTER_EVOLVE")
+        elif code == sp.ADD:
+            h = HostPark(n)
+            h.add(j, a)
+            again = bool(layer.st["in_park"][j, 0])
+            for name in ("pos", "vel") if again else ("pos", "vel", "old_pos", "old_vel"):
+                getattr(op, name)[j] = getattr(h, name)[:, j]
+            for name in ("mass", "time_factor", "radius", "max_vel", "agility", "speed_fraction"):
+                getattr(op, name)[j] = float(getattr(h, name)[j])
+            op.free[j], op.interactive[j], op.massive[j] = bool(h.free[j]), bool(h.interactive[j]), bool(a[13])
+            op.effect_stamp[j] = op.owner_id[j] = op.follow_id[j] = 0
+            op.follow_range[j], op.mode[j] = 10.0, 2         # a re-added ball keeps its target pointer
+            if not again:
+                op.follow_ptr[j], op.last_g[j], op.last_collision[j] = -1, 0.0, -1.0
+            run("ADD", j)
+        elif not (0 <= j < n and layer.st["in_park"][j, 0]) and code in (sp.GOTO, sp.STOP, sp.REMOVE, sp.FOLLOW,
+                                                                           sp.ORBIT, sp.WARP):
+            pass                                          # a command to a ball not in the world does nothing
+        elif code in (sp.FOLLOW, sp.ORBIT):
+            t = int(a[0]) - 1
+            op.bubble = layer.st["bubble"][:, 0].copy()  # FollowBall's same-bubble test reads the layer's bubbles
+            saved = op.moribund.copy()
+            op.moribund = saved | ~layer.st["in_park"][:, 0].astype(bool)   # a target not in the world is refused
+            (op.follow if code == sp.FOLLOW else op.orbit)(mask, np.full(n, t if 0 <= t < n else -1), np.full(n, a[1]))
+            op.moribund = saved
+        elif code == sp.WARP:
+            op.warp_to(mask, np.array([a[0:3]] * n), np.full(n, a[3]), np.full(n, int(a[4]), dtype=np.int64))
+        elif code == sp.POS:
+            op.pos[j] = a[0:3]
+            op.old_pos[j] = a[0:3]
+            run("REFILE", j)
+        elif code == sp.GOTO:
+            op.goto_point(mask, np.array([a[0:3]] * n))
+        elif code == sp.STOP:
+            op.stop(mask)
+        elif code == sp.REMOVE:                           # RemoveBall: Stop, then StopAllFollowers
+            op.stop(mask)
+            members = op._members(mask)
+            orbiter = members & op.interactive & (op.mode == 4)
+            op._stop_rows(members & ~orbiter)
+            op.goto_direction(orbiter, op.vel.copy())
+            run("REMOVE_BALL", j)
+        elif code == sp.INIT:
+            run("INIT_BUBBLES")
+        elif code == sp.COPY:
+            run("COPY_BUBBLES")
+        elif code == sp.INTERACTIVE:
+            run("SET_INTERACTIVE", j, int(bool(a[0])))
+        elif code == sp.KEEPALIVE:
+            run("KEEP_ALIVE", j)
+        out.append(text(layer.st, op.ids, op.mode, 0))
+    return out

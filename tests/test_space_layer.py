@@ -3,7 +3,8 @@ the reference's own SpaceBallpark by tests/test_space_oracle.py): the golden str
 (mixed operations, long streams, the sweeps past BoxAllocator's 256 kept boxes) driven through the layer, one world a
 stream, and after every operation each ball's filing, bubble and old bubble, the dead-bubble flag, the live boxes per
 level, BoxAllocator's kept count, the next bubble id, the bubble dictionaries in their order and the interactive and
-keep-alive sets compared with the oracle's state text of the same operations. The streams' sensor operations are left
+keep-alive sets compared with the oracle's state text of the same operations; and the ticking and mode streams through
+the layer's tick (the dead rows skipped by the park's tick, the drop-outs' and the commits' re-filings after it). The streams' sensor operations are left
 out on both sides (the sensors are not in the layer's slice). On the CPU the layer's per-world program runs as its
 host build (tests/native/space_host.cpp, the same source); on a GPU the product's VecSpace runs it, one CUDA thread a
 world, and must give the same texts and the same state, word for word."""
@@ -79,6 +80,22 @@ def test_a_full_box_table_flags_the_world_and_leaves_it_alone():
             frozen = {n: v.copy() for n, v in layer.st.items()}
     assert flagged_at is not None and layer.st["flags"][0] & 8                  # EBB_SPACE_FLAG_BOXES
     assert all((layer.st[n] == frozen[n]).all() for n in frozen)                # nothing ran after the flag
+
+
+@pytest.mark.parametrize("family", ["tick", "modes"])
+def test_the_layers_tick_matches_the_oracle_on_the_cpu(family):
+    """The ticking and the mode streams (GOTO and STOP ships; FollowBall, Orbit and WarpTo with drop-outs, releases
+    and re-added followers): the layer's host build around the flight oracle's tick (dead rows skipped), every state
+    after every operation against the space oracle's."""
+    scs = _streams((family,))
+    assert len(scs) == 40
+    bad = []
+    for sc in scs:
+        got = sl.drive_ticks_host(sc["ops"])
+        want = _oracle_texts(sc)
+        if got != want:
+            bad.append((sc["seed"], next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
+    assert not bad, f"{len(bad)} worlds differ, first {bad[:3]}"
 
 
 @pytest.mark.gpu
