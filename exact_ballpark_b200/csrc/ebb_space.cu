@@ -31,6 +31,8 @@ int ebb_space_tape(const EbbFlightState* park, const EbbSpaceState* s, const Ebb
         s->bubble == nullptr || s->old_bubble == nullptr || s->seq == nullptr || s->in_park == nullptr ||
         s->keep_alive == nullptr || s->dead == nullptr || s->dropped == nullptr || s->box_level == nullptr ||
         s->box_key == nullptr || s->box_balls == nullptr || s->box_kids == nullptr || s->box_bubble == nullptr ||
+        s->my_box == nullptr || s->my_top == nullptr || s->box_hash == nullptr || s->box_free == nullptr ||
+        s->box_free_n == nullptr ||
         s->stack == nullptr || s->box_n == nullptr || s->free_boxes == nullptr || s->dict_bubble == nullptr ||
         s->dict_n == nullptr || s->entry_bubble == nullptr || s->entry_id == nullptr || s->entry_value == nullptr ||
         s->entry_n == nullptr || s->inter_bubble == nullptr || s->inter_id == nullptr || s->inter_n == nullptr ||

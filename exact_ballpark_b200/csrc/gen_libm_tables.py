@@ -34,7 +34,9 @@ def _exact_fma(a, b, c):
 
 
 def _load():
-    ref = os.environ.get("EXACT_BALLPARK_REF", "/root/reference")
+    ref = os.environ.get("EXACT_BALLPARK_REF")
+    if not ref:
+        raise SystemExit("set EXACT_BALLPARK_REF to a checkout of exact-ballpark (the tables are read from its modules)")
     sys.path.insert(0, os.path.join(ref, "src"))
     if not hasattr(math, "fma"):
         math.fma = _exact_fma

@@ -215,7 +215,7 @@ int64_t ebb_flight_scratch_bytes(int64_t n);
 /* One tick of every world of the park in place: the prepass (each ship's start-of-tick position and velocity, its
  * vertical velocity after its own turn, whether it starts warp proper) into `scratch`, then each ship's tick (phase 1,
  * phase 3, phase 4, PetrifyTroll, its world's clock), one thread a ship. `scratch` holds at least
- * ebb_flight_scratch_bytes(n) bytes of device memory, 256-byte aligned; block is a multiple of 32 up to 1024.
+ * ebb_flight_scratch_bytes(n) bytes of device memory, 256-byte aligned; block is a multiple of 32 up to 256.
  * Replaces xbpm_tick (exact_ballpark/vec_modes_cuda.cu:754), which exact_ballpark.vec_modes_cuda.tick calls
  * (vec_modes_cuda.py:322). */
 int ebb_flight_tick(const EbbFlightState* s, void* scratch, int64_t scratch_bytes, void* stream, int block);
@@ -226,9 +226,12 @@ int ebb_flight_tick(const EbbFlightState* s, void* scratch, int64_t scratch_byte
  * rows, about 14.4 MB of device memory on every device that loads the library, held until the process exits), so
  * parks of more rows are refused with EBB_ETOOBIG, nothing launched. The same kernels and results as ebb_flight_tick.
  * The first call on a device looks up the buffer's device address (cudaGetSymbolAddress, with that device current);
- * make that first call before any stream capture. All calls on a device share the buffer: calls that may overlap on
- * the GPU (other streams, other threads) race on it and must be ordered by the caller. Each call writes every record
- * it reads, so the buffer needs no clearing. No counterpart in the reference. */
+ * make that first call before any stream capture. The address is kept for the life of the process, so a device reset
+ * (cudaDeviceReset) or a new primary context on that device after the first call is not supported: the kept address
+ * would name the old context's memory. `block` is a multiple of 32 up to 256, as for ebb_flight_tick. All calls on a
+ * device share the buffer: calls that may overlap on the GPU (other streams, other threads) race on it and must be
+ * ordered by the caller. Each call writes every record it reads, so the buffer needs no clearing. No counterpart in
+ * the reference. */
 int ebb_flight_tick_noalloc(const EbbFlightState* s, void* stream, int block);
 
 /* The same tick with the worlds packed into tiles, one thread block a tile, the prepass's records in shared memory

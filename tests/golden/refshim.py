@@ -23,7 +23,9 @@ import os
 import sys
 from fractions import Fraction
 
-REF = os.environ.get("EXACT_BALLPARK_REF", "/root/reference")
+REF = os.environ.get("EXACT_BALLPARK_REF", "")
+if not REF:
+    raise SystemExit("set EXACT_BALLPARK_REF to a checkout of exact-ballpark: the fixtures are made by its own code")
 
 
 def _fma(a: float, b: float, c: float) -> float:

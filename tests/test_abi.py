@@ -79,3 +79,22 @@ def test_the_space_tape_refuses_bad_arguments_before_launching():
     assert call() == 0                                    # no worlds: nothing to do
     s.worlds, t.K = 4, 0
     assert call() == 0                                    # no operations
+
+
+def test_the_space_tape_refuses_a_missing_box_index_before_launching():
+    """Every buffer the tape writes through is checked: with one of the box table's index, free list or filing
+    buffers missing the call is refused with EBB_EINVAL, nothing launched."""
+    lib = _native.lib()
+    p, s, t = _native.FlightState(), _native.SpaceState(), _native.SpaceTape()
+    s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets, t.K = 4, 10, 64, 16, 16, 16, 1
+    fake = 4096
+    for st in (p, s, t):
+        for name, kind in type(st)._fields_:
+            if kind is ctypes.c_void_p:
+                setattr(st, name, fake)
+    for missing in ("box_hash", "box_free", "box_free_n", "my_box", "my_top"):
+        keep = getattr(s, missing)
+        setattr(s, missing, None)
+        rc = lib.ebb_space_tape(ctypes.byref(p), ctypes.byref(s), ctypes.byref(t), None, 128)
+        assert rc == -1, missing
+        setattr(s, missing, keep)

@@ -29,11 +29,15 @@ def _same(a: np.ndarray, b: np.ndarray) -> bool:
     return bool((a == b).all())
 
 
-def test_the_no_alloc_tick_equals_the_scratch_tick_twice():
+@pytest.mark.parametrize("worlds", [2048, 65536], ids=["8192_rows", "max_rows"])
+def test_the_no_alloc_tick_equals_the_scratch_tick_twice(worlds):
+    """Two calls in a row, on a small park and on one of exactly EBB_NOALLOC_MAX_ROWS rows (65,536 worlds of 4 ships),
+    where the records' last plane ends at the buffer's end."""
     from exact_ballpark_b200 import VecModesPark, _native
     from exact_ballpark_b200.workloads import flight_worlds
     lib = _native.lib()
-    w = flight_worlds(55, 2048, 4)
+    w = flight_worlds(55, worlds, 4)
+    assert worlds != 65536 or len(w.rows) == 262144
     parks = []
     for _ in range(2):
         p = VecModesPark(len(w.rows), device="cuda", dynamical_orientation=True, use_new_orbit=True)
