@@ -9,10 +9,11 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libebb.so"
-ABI = 6
+ABI = 7
 COLLIDE_MAX_SLOTS = 64          # include/ebb.h: EBB_COLLIDE_MAX_SLOTS
 COLLIDE_MAX_STATICS = 64        # include/ebb.h: EBB_COLLIDE_MAX_STATICS
 SPACE_MAX_SLOTS = 128           # include/ebb.h: EBB_SPACE_MAX_SLOTS
+RAND_WORDS = 33                 # include/ebb.h: EBB_RAND_WORDS
 
 _lib = None
 
@@ -72,16 +73,23 @@ SPACE_DICT_FIELDS = ("dict_bubble", "dict_n", "entry_bubble", "entry_id", "entry
                      "inter_id", "inter_n", "keep_bubble", "keep_id", "keep_n", "bubble_id", "seq_next", "flags")
 
 
+SPACE_SENSOR_FIELDS = ("srange", "speriod", "selapsed", "ntf_range", "trk_range", "trk", "cloaked", "sonly",
+                       "has_prox", "ntf_in", "trk_in", "slist", "slen", "sbkt", "pmap", "pn", "pbkt", "ev", "evn", "rnd")
+
+
 class SpaceState(ctypes.Structure):
     """include/ebb.h's EbbSpaceState, field for field."""
     _fields_ = ([(k, ctypes.c_int64) for k in ("worlds", "slots", "boxes", "dicts", "entries", "sets")]
                 + [(k, ctypes.c_void_p) for k in ("rows",) + SPACE_SLOT_FIELDS + SPACE_FLAG_FIELDS + SPACE_BOX_FIELDS
-                   + SPACE_DICT_FIELDS])
+                   + SPACE_DICT_FIELDS]
+                + [("umap_cap", ctypes.c_int64), ("events", ctypes.c_int64)]
+                + [(k, ctypes.c_void_p) for k in SPACE_SENSOR_FIELDS])
 
 
 class SpaceTape(ctypes.Structure):
     """include/ebb.h's EbbSpaceTape, field for field."""
-    _fields_ = [("K", ctypes.c_int64), ("code", ctypes.c_void_p), ("a", ctypes.c_void_p), ("b", ctypes.c_void_p)]
+    _fields_ = [("K", ctypes.c_int64), ("code", ctypes.c_void_p), ("a", ctypes.c_void_p), ("b", ctypes.c_void_p),
+                ("f", ctypes.c_void_p)]
 
 
 def lib() -> ctypes.CDLL:

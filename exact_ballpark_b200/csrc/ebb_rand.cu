@@ -8,23 +8,10 @@
 #include <cuda_runtime.h>
 
 #include "../../include/ebb.h"
+#include "ebb_rand.cuh"
 
 namespace ebb {
 namespace grand {
-
-constexpr int DEG = 31, SEP = 3;
-
-__device__ __forceinline__ int32_t draw(int32_t* t, int32_t& f, int32_t& r) {
-    const uint32_t val = (uint32_t)t[f] + (uint32_t)t[r];
-    t[f] = (int32_t)val;
-    if (++f >= DEG) {
-        f = 0;
-        ++r;
-    } else if (++r >= DEG) {
-        r = 0;
-    }
-    return (int32_t)(val >> 1);
-}
 
 // srand(seed) for each world: the table, then the front and rear indices (EBB_RAND_WORDS int32 a world)
 __global__ void srand_kernel(const int64_t* __restrict__ seeds, int64_t worlds, int32_t* __restrict__ state) {

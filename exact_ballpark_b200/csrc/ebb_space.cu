@@ -39,10 +39,18 @@ int ebb_space_tape(const EbbFlightState* park, const EbbSpaceState* s, const Ebb
         s->keep_bubble == nullptr || s->keep_id == nullptr || s->keep_n == nullptr || s->bubble_id == nullptr ||
         s->seq_next == nullptr || s->flags == nullptr || t->code == nullptr || t->a == nullptr || t->b == nullptr)
         return EBB_EINVAL;
+    if (s->umap_cap < 1 || s->umap_cap > EBB_SPACE_MAX_SLOTS || s->events < 0 || s->srange == nullptr ||
+        s->speriod == nullptr || s->selapsed == nullptr || s->ntf_range == nullptr || s->trk_range == nullptr ||
+        s->trk == nullptr || s->cloaked == nullptr || s->sonly == nullptr || s->has_prox == nullptr ||
+        s->ntf_in == nullptr || s->trk_in == nullptr || s->slist == nullptr || s->slen == nullptr ||
+        s->sbkt == nullptr || s->pmap == nullptr || s->pn == nullptr || s->pbkt == nullptr || s->evn == nullptr ||
+        s->rnd == nullptr || (s->events > 0 && s->ev == nullptr))
+        return EBB_EINVAL;
     if (park->pos == nullptr || park->vel == nullptr || park->old_pos == nullptr || park->old_vel == nullptr ||
         park->ids == nullptr || park->radius == nullptr || park->max_vel == nullptr || park->agility == nullptr ||
         park->speed_fraction == nullptr || park->mass == nullptr || park->time_factor == nullptr ||
-        park->free_ == nullptr || park->interactive == nullptr || park->mode == nullptr)
+        park->free_ == nullptr || park->interactive == nullptr || park->mode == nullptr || park->goto_pt == nullptr ||
+        park->follow_ptr == nullptr || park->follow_range == nullptr || park->massive == nullptr || park->sensor == nullptr)
         return EBB_EINVAL;
     const unsigned grid = (unsigned)((s->worlds + block - 1) / block);
     ebb::space::tape_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(*park, *s, *t);

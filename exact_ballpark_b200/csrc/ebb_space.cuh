@@ -20,6 +20,7 @@
 
 #include "../../include/ebb.h"
 #include "ebb_arith.cuh"
+#include "ebb_rand.cuh"   // LGPL-2.1-or-later: the C library's rand(), a shuffled sensor's draw
 
 namespace ebb {
 namespace space {
@@ -28,8 +29,22 @@ constexpr int NUM_LEVELS = 8;
 constexpr int64_t BOX_KEEP = 256;                          // BoxAllocator's kept boxes
 constexpr int64_t F_EDGE = EBB_SPACE_FLAG_EDGE, F_BOXES = EBB_SPACE_FLAG_BOXES, F_DICTS = EBB_SPACE_FLAG_DICTS,
                   F_ENTRIES = EBB_SPACE_FLAG_ENTRIES, F_BAD_OP = EBB_SPACE_FLAG_BAD_OP,
-                  F_SETS = EBB_SPACE_FLAG_SETS, F_UNDEFINED = EBB_SPACE_FLAG_UNDEFINED;
-constexpr int64_t WARP = 3;
+                  F_SETS = EBB_SPACE_FLAG_SETS, F_UNDEFINED = EBB_SPACE_FLAG_UNDEFINED,
+                  F_EVENTS = EBB_SPACE_FLAG_EVENTS, F_PROXIMITY = EBB_SPACE_FLAG_PROXIMITY,
+                  F_SENSOR_LIST = EBB_SPACE_FLAG_SENSOR_LIST, F_HUGE = EBB_SPACE_FLAG_HUGE;
+constexpr int64_t GOTO = 0, FOLLOW = 1, WARP = 3, ORBIT = 4;
+constexpr double TRACKING_MIN = 0.00001;                   // Ball.cpp:598's least tracking range
+constexpr double RAND_MAX_D = 2147483647.0;                // floatrand's RAND_MAX (Ball.cpp:19)
+// GetNearbyBalls' walk as a sort key (the reference's per-pair statement of the walk, vec_collide.py:825): one digit
+// base 65 a level below the sensing ball's (64 children a box, then "past the candidate's level")
+constexpr int64_t CODE_BASE = 65;
+constexpr int64_t NOT_A_CANDIDATE = int64_t(1) << 62;
+// The bucket counts of a std::unordered_map<int64_t, ...> under libstdc++'s prime rehash policy (max load factor 1)
+// as it grows from its first insertion (13 buckets, room asked for 11 keys) past its bucket count each time: the
+// first entry of the library's prime list at or above twice the old count. A map of at most 256 keys reaches 257.
+EBB_HD constexpr int32_t umap_next_buckets(int32_t b) {
+    return b <= 1 ? 13 : b == 13 ? 29 : b == 29 ? 59 : b == 59 ? 127 : b == 127 ? 257 : -1;
+}
 
 // a box's width at level i (Partition.h's constants: 2^16 grid units of 480 m a quarter at the top)
 EBB_HD double level_width(int i) {
@@ -57,6 +72,8 @@ struct World {
     EBB_HD int64_t& I(int64_t* a, int64_t e) const { return a[e * W + w]; }
     EBB_HD int64_t& I3(int64_t* a, int64_t c, int64_t e, int64_t cap) const { return a[(c * cap + e) * W + w]; }
     EBB_HD uint8_t& U(uint8_t* a, int64_t e) const { return a[e * W + w]; }
+    template <class T>
+    EBB_HD T& at(T* a, int64_t e) const { return a[e * W + w]; }
     EBB_HD int64_t& one(int64_t* a) const { return a[w]; }
     EBB_HD void flag(int64_t f) const { s->flags[w] |= f; }
 
@@ -551,6 +568,417 @@ struct World {
         insert_in_boxes(j, x, v);
     }
 
+
+    // ---- GetNearbyBalls' walk (Partition.cpp:344), as a sort key per pair ----
+    // A ball's boxes are a product of one key range an axis: its box's key and the side its sphere reaches (mod), or
+    // for a huge ball the three keys around its own (its 27 top boxes).
+    EBB_HD bool huge(int64_t j) const { return active(j) == int64_t(0x7FFFFFF); }
+    EBB_HD void key_range(int64_t j, int q, int64_t* lo, int64_t* hi) const {
+        const int64_t k = key(j, q), m = mod(j, q);
+        if (huge(j)) {
+            *lo = k - 1;
+            *hi = k + 1;
+        } else {
+            *lo = k + (m < 0 ? m : 0);
+            *hi = k + (m > 0 ? m : 0);
+        }
+    }
+    // The position of slot o's first box in slot b's walk, or NOT_A_CANDIDATE when no box of o is one of b's, an
+    // ancestor of one or below one. b's boxes are walked in key order; at each, its ancestors holding balls bottom-up
+    // (those not met before), its descendants in post-order (children by key), then the box itself. The key: the
+    // index of the first of b's boxes o's box relates to, the part (0 an ancestor, 1 below, 2 the box itself), then
+    // the ancestor's distance or the box's post-order code (path digits below b's level, 64 past o's level).
+    // Relatedness factors over the axes: the finer filing's key range, shifted to the coarser level, meets the
+    // coarser's.
+    EBB_HD int64_t walk_key(int64_t b, int64_t o) const {
+        const int64_t Lb = lvl(b), Ln = lvl(o);
+        int64_t lo_b[3], hi_b[3], lo_n[3], hi_n[3], cb[3];
+        for (int q = 0; q < 3; ++q) {
+            key_range(b, q, &lo_b[q], &hi_b[q]);
+            key_range(o, q, &lo_n[q], &hi_n[q]);
+            cb[q] = hi_b[q] - lo_b[q] + 1;
+        }
+        const bool coarse = Ln <= Lb;
+        const int64_t sh = 2 * (coarse ? Lb - Ln : Ln - Lb);
+        for (int q = 0; q < 3; ++q) {
+            const int64_t xl = (coarse ? lo_b[q] : lo_n[q]) >> sh, xh = (coarse ? hi_b[q] : hi_n[q]) >> sh;
+            const int64_t yl = coarse ? lo_n[q] : lo_b[q], yh = coarse ? hi_n[q] : hi_b[q];
+            if ((xl > yl ? xl : yl) > (xh < yh ? xh : yh)) return NOT_A_CANDIDATE;
+        }
+        int64_t span = 1;
+        for (int l = 0; l < NUM_LEVELS - 1; ++l) span *= CODE_BASE;
+        if (coarse) {                                      // an ancestor or a box of b's level: b's first box under it
+            int64_t idx[3];
+            for (int q = 0; q < 3; ++q) {
+                idx[q] = 0;
+                while (idx[q] + 1 < cb[q]) {
+                    const int64_t v = (lo_b[q] + idx[q]) >> sh;
+                    if (v >= lo_n[q] && v <= hi_n[q]) break;
+                    ++idx[q];
+                }
+            }
+            const int64_t seg = (idx[0] * cb[1] + idx[1]) * cb[2] + idx[2];
+            return Ln < Lb ? (seg * 3) * span + (Lb - Ln) : (seg * 3 + 2) * span;
+        }
+        int64_t best = NOT_A_CANDIDATE;                    // below: the least code over o's boxes under b's
+        for (int64_t bx = lo_n[0]; bx <= hi_n[0]; ++bx)
+            for (int64_t by = lo_n[1]; by <= hi_n[1]; ++by)
+                for (int64_t bz = lo_n[2]; bz <= hi_n[2]; ++bz) {
+                    const int64_t box[3] = {bx, by, bz};
+                    int64_t jx[3];
+                    bool ok = true;
+                    for (int q = 0; q < 3; ++q) {
+                        const int64_t anc = box[q] >> sh;
+                        if (anc < lo_b[q] || anc > hi_b[q]) ok = false;
+                        jx[q] = anc - lo_b[q];
+                    }
+                    if (!ok) continue;
+                    const int64_t seg = (jx[0] * cb[1] + jx[1]) * cb[2] + jx[2];
+                    int64_t code = 0, power = span;
+                    for (int64_t li = 1; li < NUM_LEVELS; ++li) {
+                        power /= CODE_BASE;
+                        const int64_t shift = 2 * (Ln - li) > 0 ? 2 * (Ln - li) : 0;
+                        int64_t digit =
+                            ((box[0] >> shift) & 3) * 16 + ((box[1] >> shift) & 3) * 4 + ((box[2] >> shift) & 3);
+                        if (li > Ln) digit = CODE_BASE - 1;
+                        if (li <= Lb) digit = 0;
+                        code += digit * power;
+                    }
+                    const int64_t k = (seg * 3 + 1) * span + code;
+                    if (k < best) best = k;
+                }
+        return best;
+    }
+    // GetNearbyBalls from slot b (no missiles, fields or global balls here): the balls filed in related boxes that
+    // pass the filter, in the walk's order (its key, then id), into out; returns their count
+    EBB_HD int nearby(int64_t b, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked, uint8_t* out) const {
+        const int64_t bub = I(s->bubble, b);
+        if (exclude_inert && !set_any(0, bub)) return 0;
+        if (lvl(b) < 0) return 0;
+        int64_t keys[EBB_SPACE_MAX_SLOTS], oid[EBB_SPACE_MAX_SLOTS];
+        int n = 0;
+        for (int64_t o = 0; o < N; ++o) {
+            if (o == b || !slot_ok(o) || !U(s->in_park, o) || lvl(o) < 0) continue;
+            const int64_t k = walk_key(b, o);
+            if (k == NOT_A_CANDIDATE) continue;
+            const int64_t r = row(o);
+            if (exclude_cloaked && (at(s->cloaked, o) != 0 || !p->massive[r])) continue;
+            if (exclude_inert) {
+                if (!p->interactive[r]) continue;
+            } else {
+                if (I(s->bubble, o) != bub) continue;
+                if (exclude_fixed && !p->free_[r]) continue;
+            }
+            const int64_t i = p->ids[r];
+            int m = n;
+            for (; m > 0 && (keys[m - 1] > k || (keys[m - 1] == k && oid[m - 1] > i)); --m) {
+                keys[m] = keys[m - 1];
+                oid[m] = oid[m - 1];
+                out[m] = out[m - 1];
+            }
+            keys[m] = k;
+            oid[m] = i;
+            out[m] = (uint8_t)o;
+            ++n;
+        }
+        return n;
+    }
+
+    // ---- std::unordered_map<int64_t, ...> in libstdc++'s iteration order (space.py:193-322) ----
+    // A map's keys are slots (their balls' ids the keys' values): k[e step] for e < len, in iteration order, with
+    // the map's bucket count (1 for a fresh map).
+    struct UMap {
+        uint8_t* k;
+        int64_t step;
+        int32_t* len;
+        int32_t* bkt;
+    };
+    EBB_HD UMap sensor_map(int64_t j) const {
+        return UMap{s->slist + j * W + w, N * W, &at(s->slen, j), &at(s->sbkt, j)};
+    }
+    EBB_HD UMap proximity_map() const { return UMap{s->pmap + w, W, &s->pn[w], &s->pbkt[w]}; }
+    EBB_HD uint64_t bucket_of(int64_t slot, int32_t bkt) const { return (uint64_t)id(slot) % (uint64_t)bkt; }
+    EBB_HD int32_t umap_find(const UMap& m, int64_t slot) const {
+        const int32_t n = *m.len;
+        for (int32_t e = 0; e < n; ++e)
+            if (m.k[e * m.step] == (uint8_t)slot) return e;
+        return -1;
+    }
+    // the linking rule: just before the first key of the order in the key's bucket, else at the front
+    EBB_HD void umap_link(const UMap& m, int64_t slot) const {
+        const int32_t n = *m.len, bkt = *m.bkt;
+        const uint64_t b = bucket_of(slot, bkt);
+        int32_t at0 = 0;
+        for (int32_t e = 0; e < n; ++e)
+            if (bucket_of(m.k[e * m.step], bkt) == b) {
+                at0 = e;
+                break;
+            }
+        for (int32_t e = n; e > at0; --e) m.k[e * m.step] = m.k[(e - 1) * m.step];
+        m.k[at0 * m.step] = (uint8_t)slot;
+        *m.len = n + 1;
+    }
+    // insert(): an absent key linked; before it, a fresh map takes 13 buckets and a key past the bucket count grows
+    // the table, every key re-linked in its old order. A map past umap_cap keys flags the world.
+    EBB_HD bool umap_insert(const UMap& m, int64_t slot, int64_t flag_bit) const {
+        if (umap_find(m, slot) >= 0) return false;
+        const int32_t n = *m.len;
+        if (n >= s->umap_cap) {
+            flag(flag_bit);
+            return false;
+        }
+        if (*m.bkt <= 1 || n + 1 > *m.bkt) {
+            const int32_t nb = umap_next_buckets(*m.bkt);
+            if (nb < 0) {
+                flag(flag_bit);
+                return false;
+            }
+            uint8_t old[EBB_SPACE_MAX_SLOTS];
+            for (int32_t e = 0; e < n; ++e) old[e] = m.k[e * m.step];
+            *m.bkt = nb;
+            *m.len = 0;
+            for (int32_t e = 0; e < n; ++e) umap_link(m, old[e]);
+        }
+        umap_link(m, slot);
+        return true;
+    }
+    EBB_HD void umap_erase_at(const UMap& m, int32_t e0) const {
+        const int32_t n = *m.len;
+        for (int32_t e = e0; e + 1 < n; ++e) m.k[e * m.step] = m.k[(e + 1) * m.step];
+        *m.len = n - 1;
+    }
+    EBB_HD void umap_erase(const UMap& m, int64_t slot) const {
+        const int32_t e = umap_find(m, slot);
+        if (e >= 0) umap_erase_at(m, e);
+    }
+
+    // ---- the proximity sensors, notification ranges and target tracking (space.py:1345-1477) ----
+    EBB_HD void event(int kind, int64_t ball, int64_t other, int value) const {
+        const int64_t n = s->evn[w];
+        if (n < s->events)
+            at(s->ev, n) = (int32_t)(kind | (value << 4) | ((int32_t)ball << 8) | ((int32_t)other << 16));
+        else
+            flag(F_EVENTS);
+        s->evn[w] = n + 1;
+    }
+    EBB_HD double dist2(int64_t a, const double* x) const {
+        const double d0 = dsub(pos(a, 0), x[0]), d1 = dsub(pos(a, 1), x[1]), d2 = dsub(pos(a, 2), x[2]);
+        return dadd(dadd(dmul(d0, d0), dmul(d1, d1)), dmul(d2, d2));
+    }
+    EBB_HD double dist2_slots(int64_t a, int64_t b) const {
+        const double x[3] = {pos(b, 0), pos(b, 1), pos(b, 2)};
+        return dist2(a, x);
+    }
+    // Ball::UpdateProximityStatus: a ball with a tracking range, a notification range or an active sensor is in the
+    // proximity map, else out of it
+    EBB_HD void update_proximity_status(int64_t j) const {
+        const bool on = at(s->trk_range, j) != 0.0 || at(s->ntf_range, j) != 0.0 || p->sensor[row(j)] != 0;
+        at(s->has_prox, j) = on ? 1 : 0;
+        if (on)
+            umap_insert(proximity_map(), j, F_PROXIMITY);
+        else
+            umap_erase(proximity_map(), j);
+    }
+    // a new ball's: no sensor (period 2 s), no notification range, no tracking, not cloaked, a fresh sensor list
+    EBB_HD void reset_sensors(int64_t j) const {
+        at(s->srange, j) = 0.0;
+        at(s->speriod, j) = 2.0;
+        at(s->selapsed, j) = 0.0;
+        at(s->sonly, j) = 0;
+        at(s->has_prox, j) = 0;
+        at(s->ntf_range, j) = 0.0;
+        at(s->ntf_in, j) = 0;
+        at(s->trk, j) = -1;
+        at(s->trk_range, j) = 0.0;
+        at(s->trk_in, j) = 0;
+        at(s->cloaked, j) = 0;
+        at(s->slen, j) = 0;
+        at(s->sbkt, j) = 1;
+        p->sensor[row(j)] = 0;
+    }
+    // AddProximitySensor (Ball.cpp:244; SEN-701): refused when float radius + float range < 0; the list emptied (its
+    // buckets kept); a shuffled sensor starts its period at floatrand(0, period), the world's rand() drawn once
+    EBB_HD void add_sensor(int64_t j, double range, double period, bool only, bool shuffle) const {
+        const int64_t r = row(j);
+        const float rng = (float)range;
+        if (fadd(p->radius[r], rng) < 0.0f) return;
+        at(s->slen, j) = 0;
+        at(s->srange, j) = (double)rng;
+        at(s->speriod, j) = period;
+        p->sensor[r] = 1;
+        at(s->sonly, j) = only ? 1 : 0;
+        if (shuffle) {
+            int32_t* st = s->rnd + w * EBB_RAND_WORDS;
+            int32_t f = st[grand::DEG], rr = st[grand::DEG + 1];
+            const int32_t v = grand::draw(st, f, rr);
+            st[grand::DEG] = f;
+            st[grand::DEG + 1] = rr;
+            at(s->selapsed, j) = dadd(0.0, dmul(ddiv((double)v, RAND_MAX_D), dsub(period, 0.0)));
+        }
+        update_proximity_status(j);
+    }
+    EBB_HD void remove_sensor(int64_t j) const {
+        p->sensor[row(j)] = 0;
+        update_proximity_status(j);
+    }
+    // SetNotificationRange (SEN-704): a negative range ignored; the in-range flag reset
+    EBB_HD void set_notification_range(int64_t j, double n) const {
+        if (n < 0.0) return;
+        at(s->ntf_range, j) = n;
+        update_proximity_status(j);
+        at(s->ntf_in, j) = 0;
+    }
+    // SetTargetTracking (SEN-703): a range <= 0 or a target id of 0 turns it off (the proximity status kept)
+    EBB_HD void set_tracking(int64_t j, int64_t target, double range, bool target_zero) const {
+        if (range <= 0.0 || target_zero) {
+            at(s->trk, j) = -1;
+            at(s->trk_range, j) = 0.0;
+            return;
+        }
+        if (!slot_ok(target) || !U(s->in_park, target)) return;
+        at(s->trk, j) = target;
+        at(s->trk_range, j) = range;
+        update_proximity_status(j);
+        at(s->trk_in, j) = 0;
+    }
+    // CheckForProximity_NotificationRange (Ball.cpp:520): within the range of the goto point, or within a shell of
+    // the range's width around the followed ball's follow range
+    EBB_HD void check_notification_range(int64_t j) const {
+        const double n = at(s->ntf_range, j);
+        if (n == 0.0) return;
+        const int64_t r = row(j);
+        const int32_t mode = p->mode[r];
+        const double rad = (double)p->radius[r];
+        bool inside = false;
+        if (mode == GOTO) {
+            const double lim = dadd(n, rad);
+            const double g[3] = {p->goto_pt[r], p->goto_pt[p->n + r], p->goto_pt[2 * p->n + r]};
+            inside = dist2(j, g) < dmul(lim, lim);
+        } else if (mode == FOLLOW || mode == ORBIT) {
+            const int32_t t = p->follow_ptr[r];
+            if (t >= 0) {
+                const double x[3] = {p->pos[t], p->pos[p->n + t], p->pos[2 * p->n + t]};
+                const double len2 = dist2(j, x);
+                const double hi = dadd(dadd(dadd((double)p->radius[t], (double)p->follow_range[r]), n), rad);
+                double lo = dsub(hi, dmul(2.0, n));
+                if (lo < 0.0) lo = 0.0;
+                inside = len2 < dmul(hi, hi) && len2 > dmul(lo, lo);
+            }
+        }
+        bool send = false;
+        if (inside) {
+            if (!at(s->ntf_in, j)) {
+                send = true;
+                at(s->ntf_in, j) = 1;
+            }
+        } else if (at(s->ntf_in, j)) {
+            send = true;
+            at(s->ntf_in, j) = 0;
+        }
+        if (send) event(EBB_SPACE_EV_RANGE, j, 0, at(s->ntf_in, j));
+    }
+    // CheckForProximity_TargetTracking (Ball.cpp:595)
+    EBB_HD void check_target_tracking(int64_t j) const {
+        const double tr = at(s->trk_range, j);
+        const int64_t t = at(s->trk, j);
+        if (!(tr >= TRACKING_MIN) || t < 0) return;
+        const double lim = dadd(tr, (double)p->radius[row(j)]);
+        bool send = false;
+        if (dist2_slots(j, t) < dmul(lim, lim)) {
+            if (!at(s->trk_in, j)) {
+                send = true;
+                at(s->trk_in, j) = 1;
+            }
+        } else if (at(s->trk_in, j)) {
+            send = true;
+            at(s->trk_in, j) = 0;
+        }
+        if (send) event(EBB_SPACE_EV_TRACKING, j, 0, at(s->trk_in, j));
+    }
+    // CheckForProximity_Sensor (Ball.cpp:642; SEN-701, SEN-702): every period, GetNearbyBalls with the sensor's
+    // radius inflated and the velocity zeroed (the ball re-filed for it and back), the balls no longer near first (in
+    // the list's order), then each candidate in the walk's order entering or leaving (the inside test in float sums)
+    EBB_HD void check_sensor(int64_t j) {
+        at(s->selapsed, j) = dadd(at(s->selapsed, j), p->dt);
+        if (at(s->selapsed, j) < at(s->speriod, j)) return;
+        at(s->selapsed, j) = 0.0;
+        const int64_t r = row(j);
+        const float radius = p->radius[r];
+        const double x[3] = {pos(j, 0), pos(j, 1), pos(j, 2)};
+        const double v[3] = {vel(j, 0), vel(j, 1), vel(j, 2)};
+        const double rest[3] = {0.0, 0.0, 0.0};
+        const float inflated = fadd(radius, (float)at(s->srange, j));
+        if (!(inflated < 0.0f)) {
+            p->radius[r] = inflated;
+            insert_in_boxes(j, x, rest);
+        }
+        uint8_t cand[EBB_SPACE_MAX_SLOTS];
+        const int nc = nearby(j, at(s->cloaked, j) == 0, at(s->sonly, j) != 0, false, cand);
+        if (!(radius < 0.0f)) {
+            p->radius[r] = radius;
+            insert_in_boxes(j, x, v);
+        }
+        const UMap m = sensor_map(j);
+        if (*m.len > 0) {
+            uint64_t near[2] = {0, 0};
+            for (int i = 0; i < nc; ++i) near[cand[i] >> 6] |= uint64_t(1) << (cand[i] & 63);
+            uint8_t keys[EBB_SPACE_MAX_SLOTS];
+            const int32_t n0 = *m.len;
+            for (int32_t e = 0; e < n0; ++e) keys[e] = m.k[e * m.step];
+            for (int32_t e = 0; e < n0; ++e) {
+                const int64_t k = keys[e];
+                if (k == j || ((near[k >> 6] >> (k & 63)) & 1)) continue;
+                umap_erase(m, k);
+                event(EBB_SPACE_EV_PROXIMITY, j, k, 0);
+                if (!p->sensor[r]) break;
+            }
+        }
+        const float range = (float)at(s->srange, j);
+        for (int i = 0; i < nc; ++i) {
+            const int64_t o = cand[i];
+            if (o == j) continue;
+            const bool inside = umap_find(m, o) >= 0;
+            const double ck = (double)fadd(fadd(range, p->radius[row(o)]), p->radius[r]);
+            if (dist2_slots(j, o) > dmul(ck, ck)) {
+                if (inside) {
+                    umap_erase(m, o);
+                    event(EBB_SPACE_EV_PROXIMITY, j, o, 0);
+                }
+            } else if (!inside) {
+                umap_insert(m, o, F_SENSOR_LIST);
+                event(EBB_SPACE_EV_PROXIMITY, j, o, 1);
+            }
+            if (!p->sensor[r]) break;
+        }
+    }
+    EBB_HD void check_for_proximity(int64_t j) {
+        check_notification_range(j);
+        check_target_tracking(j);
+        if (p->sensor[row(j)]) check_sensor(j);
+    }
+    // Ballpark::HandleProximities (Ballpark.cpp:5822): every proximity ball in the map's order (a copy of it); a ball
+    // in a dead bubble gets one forced check when its sensor holds balls, and its list is emptied (TIME-714)
+    EBB_HD void handle_proximities() {
+        const UMap pm = proximity_map();
+        const int32_t n = *pm.len;
+        uint8_t keys[EBB_SPACE_MAX_SLOTS];
+        for (int32_t e = 0; e < n; ++e) keys[e] = pm.k[e * pm.step];
+        for (int32_t e = 0; e < n; ++e) {
+            const int64_t j = keys[e];
+            if (!slot_ok(j) || !U(s->in_park, j)) continue;
+            if (in_dead_bubble(j)) {
+                if (at(s->slen, j) > 0) {
+                    at(s->selapsed, j) = at(s->speriod, j);
+                    check_for_proximity(j);
+                }
+                at(s->slen, j) = 0;
+                continue;
+            }
+            if (!at(s->has_prox, j)) continue;
+            check_for_proximity(j);
+        }
+    }
+
     // ---- the operations ----
     EBB_HD bool slot_ok(int64_t j) const { return j >= 0 && j < N && row(j) >= 0 && row(j) < p->n; }
     EBB_HD void add(int64_t j) {                           // AddBall's filing (a ball already in: re-filed)
@@ -561,6 +989,7 @@ struct World {
             I(s->bubble, j) = -1;
             I(s->old_bubble, j) = -1;
             clear_filing(j);
+            reset_sensors(j);
         }
         U(s->in_park, j) = 1;
         insert_in_boxes(j);
@@ -571,6 +1000,7 @@ struct World {
         I(s->old_bubble, j) = I(s->bubble, j);
         I(s->bubble, j) = -1;
         add_to_bubble(j);
+        if (at(s->has_prox, j)) umap_erase(proximity_map(), j);
         U(s->in_park, j) = 0;
     }
     EBB_HD void set_interactive(int64_t j, bool on) {
@@ -678,9 +1108,11 @@ struct World {
             for (int c = 0; c < 3; ++c) d[c] = dsub(p->pos[c * p->n + r], p->old_pos[c * p->n + r]);
             if (!(dadd(dadd(dmul(d[0], d[0]), dmul(d[1], d[1])), dmul(d[2], d[2])) < 0.1)) insert_in_boxes(j);
         }
+        handle_proximities();
     }
-    EBB_HD void apply(int64_t code, int64_t j, int64_t b) {
+    EBB_HD void apply(int64_t code, int64_t j, int64_t b, const double* f) {
         const bool has_slot = slot_ok(j);
+        const bool live = has_slot && U(s->in_park, j);
         switch (code) {
             case EBB_SPACE_NONE: break;
             case EBB_SPACE_ADD: if (has_slot) add(j); else flag(F_BAD_OP); break;
@@ -692,6 +1124,13 @@ struct World {
             case EBB_SPACE_REMOVE_BALL: if (has_slot) remove(j); break;
             case EBB_SPACE_DEAD: dead(); break;
             case EBB_SPACE_AFTER_EVOLVE: after_evolve(); break;
+            case EBB_SPACE_ADD_SENSOR: if (live) add_sensor(j, f[0], f[1], (b & 1) != 0, (b & 2) != 0); break;
+            case EBB_SPACE_REMOVE_SENSOR: if (live) remove_sensor(j); break;
+            case EBB_SPACE_NOTIFY_RANGE: if (live) set_notification_range(j, f[0]); break;
+            case EBB_SPACE_TRACK: if (live) set_tracking(j, b, f[0], f[1] != 0.0); break;
+            case EBB_SPACE_CLEAR_EVENTS: s->evn[w] = 0; break;
+            case EBB_SPACE_HANDLE_PROXIMITIES: handle_proximities(); break;
+            case EBB_SPACE_SET_CLOAKED: if (live) at(s->cloaked, j) = b; break;
             default: flag(F_BAD_OP); break;
         }
     }
@@ -703,7 +1142,10 @@ EBB_HD void run_tape(const EbbFlightState* p, const EbbSpaceState* s, const EbbS
     for (int64_t k = 0; k < t->K; ++k) {
         if (s->flags[w] & (F_EDGE | F_BOXES | F_DICTS | F_ENTRIES | F_SETS | F_BAD_OP)) return;
         const int64_t at = k * s->worlds + w;
-        wd.apply(t->code[at], t->a[at], t->b[at]);
+        double f[4] = {0.0, 0.0, 0.0, 0.0};
+        if (t->f != nullptr)
+            for (int c = 0; c < 4; ++c) f[c] = t->f[(k * 4 + c) * s->worlds + w];
+        wd.apply(t->code[at], t->a[at], t->b[at], f);
     }
 }
 

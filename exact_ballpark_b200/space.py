@@ -28,8 +28,10 @@ from .modes import VecModesPark, WARP
 I64, U8, BOOL = torch.int64, torch.uint8, torch.bool
 
 OPS = ("NONE", "ADD", "REFILE", "INIT_BUBBLES", "COPY_BUBBLES", "KEEP_ALIVE", "SET_INTERACTIVE", "ADD_SENSOR",
-       "REMOVE_SENSOR", "NOTIFY_RANGE", "TRACK", "REMOVE_BALL", "DEAD", "AFTER_EVOLVE")
+       "REMOVE_SENSOR", "NOTIFY_RANGE", "TRACK", "REMOVE_BALL", "DEAD", "AFTER_EVOLVE", "CLEAR_EVENTS")
 OP = {name: k for k, name in enumerate(OPS)}
+OP.update(HANDLE_PROXIMITIES=18, SET_CLOAKED=19)            # this build's own (no number in the reference's OPS)
+EVENTS = ("", "DoProximity", "DoRange", "DoTargetTracking")
 FLAGS = ("EVENTS", "TOPS", "EDGE", "BOXES", "DICTS", "ENTRIES", "PROXIMITY", "SENSOR_LIST", "HUGE", "BAD_OP", "SETS",
          "UNDEFINED")
 FLAG = {name: 1 << k for k, name in enumerate(FLAGS)}
@@ -43,7 +45,8 @@ class VecSpace:
     set families (defaults from N)."""
 
     def __init__(self, park: VecModesPark, rows, boxes: int | None = None, dicts: int | None = None,
-                 entries: int | None = None, sets: int | None = None, block: int = BLOCK):
+                 entries: int | None = None, sets: int | None = None, block: int = BLOCK, events: int = 256,
+                 umap_cap: int | None = None, seed=1):
         if not isinstance(park, VecModesPark):
             raise TypeError("the space layer runs over the flight park (exact_ballpark_b200.VecModesPark)")
         self.park, self.dev, self.block = park, park.dev, int(block)
@@ -73,6 +76,25 @@ class VecSpace:
             "entry_value": z(self.E, W), "entry_n": z(W), "inter_bubble": z(self.S, W), "inter_id": z(self.S, W),
             "inter_n": z(W), "keep_bubble": z(self.S, W), "keep_id": z(self.S, W), "keep_n": z(W),
             "bubble_id": z(W), "seq_next": z(W), "flags": z(W)}
+        self.M = int(events)
+        self.U = N if umap_cap is None else int(umap_cap)
+        if not 1 <= self.U <= _native.SPACE_MAX_SLOTS or self.M < 0:
+            raise ValueError(f"umap_cap {self.U}: from 1 to {_native.SPACE_MAX_SLOTS}; events >= 0")
+        zf = lambda *shape: torch.zeros(*shape, dtype=torch.float64, device=d)   # noqa: E731
+        zi32 = lambda *shape: torch.zeros(*shape, dtype=torch.int32, device=d)   # noqa: E731
+        self.st.update({
+            "srange": zf(N, W), "speriod": zf(N, W) + 2.0, "selapsed": zf(N, W), "ntf_range": zf(N, W),
+            "trk_range": zf(N, W), "trk": z(N, W) - 1, "cloaked": z(N, W), "sonly": z(N, W, dt=U8),
+            "has_prox": z(N, W, dt=U8), "ntf_in": z(N, W, dt=U8), "trk_in": z(N, W, dt=U8),
+            "slist": z(self.U, N, W, dt=U8), "slen": zi32(N, W), "sbkt": zi32(N, W) + 1, "pmap": z(self.U, W, dt=U8),
+            "pn": zi32(W), "pbkt": zi32(W) + 1, "ev": zi32(max(self.M, 1), W), "evn": z(W),
+            "rnd": zi32(W, _native.RAND_WORDS)})
+        seeds = torch.as_tensor(seed, dtype=I64).reshape(-1)
+        seeds = (seeds.expand(W) if seeds.numel() == 1 else seeds).contiguous().to(d)
+        if seeds.numel() != W:
+            raise ValueError(f"seed: an int or one a world ({W})")
+        _native.check(_native.lib().ebb_glibc_srand(seeds.data_ptr(), W, self.st["rnd"].data_ptr(),
+                                                     park._stream()), "ebb_glibc_srand")
         self._flat = torch.where(self.rows >= 0, self.rows, park.n).t().flatten()   # [W N] slot -> row, n for none
         self._state = None
         self.last_dead = None
@@ -84,14 +106,17 @@ class VecSpace:
         if self._state is None:
             s = _native.SpaceState()
             s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets = self.W, self.N, self.B, self.D, self.E, self.S
+            s.umap_cap, s.events = self.U, self.M
             s.rows = self.rows.data_ptr()
             for name, t in self.st.items():
                 setattr(s, name, t.data_ptr())
             self._state = s
         return self._state
 
-    def tape(self, code, a=None, b=None) -> None:
-        """Per world, K operations in order: code [W, K] (OP), a [W, K] (a slot), b [W, K] (an integer)."""
+    def tape(self, code, a=None, b=None, f=None) -> None:
+        """Per world, K operations in order: code [W, K] (OP), a [W, K] (a slot), b [W, K] (an integer), f [W, K, 4]
+        (floating-point arguments: ADD_SENSOR's range and period, NOTIFY_RANGE's range, TRACK's range and whether
+        the target's id is 0)."""
         code = torch.as_tensor(code, dtype=I64).to(self.dev).reshape(self.W, -1)
         K = int(code.shape[1])
         if K == 0:
@@ -99,26 +124,34 @@ class VecSpace:
         a = (torch.full_like(code, -1) if a is None else torch.as_tensor(a, dtype=I64).to(self.dev).reshape(self.W, K))
         b = (torch.zeros_like(code) if b is None else torch.as_tensor(b, dtype=I64).to(self.dev).reshape(self.W, K))
         code_t, a_t, b_t = (x.t().contiguous() for x in (code, a, b))    # [K][W]
-        t = _native.SpaceTape(K, code_t.data_ptr(), a_t.data_ptr(), b_t.data_ptr())
+        f_t = None
+        if f is not None:
+            f_t = torch.as_tensor(f, dtype=torch.float64).to(self.dev).reshape(self.W, K, 4).permute(1, 2, 0) \
+                .contiguous()                                               # [K][4][W]
+        t = _native.SpaceTape(K, code_t.data_ptr(), a_t.data_ptr(), b_t.data_ptr(),
+                              f_t.data_ptr() if f_t is not None else None)
         rc = _native.lib().ebb_space_tape(ctypes.byref(self.park.state()), ctypes.byref(self.state()), ctypes.byref(t),
                                           self.park._stream(), self.block)
         _native.check(rc, "ebb_space_tape")
-        self._keep = (code_t, a_t, b_t)                     # alive until the stream has run the launch
+        self._keep = (code_t, a_t, b_t, f_t)                # alive until the stream has run the launch
 
     def ops(self, per_world: list) -> None:
-        """A tape from per-world lists of (op name, slot, int)."""
+        """A tape from per-world lists of (op name, slot, int, floats)."""
         K = max((len(x) for x in per_world), default=0)
         if K == 0:
             return
         code = torch.zeros(self.W, K, dtype=I64)
         a = torch.full((self.W, K), -1, dtype=I64)
         b = torch.zeros(self.W, K, dtype=I64)
+        f = torch.zeros(self.W, K, 4, dtype=torch.float64)
         for w, lst in enumerate(per_world):
             for k, op in enumerate(lst):
                 code[w, k] = OP[op[0]]
                 a[w, k] = int(op[1]) if len(op) > 1 else -1
                 b[w, k] = int(op[2]) if len(op) > 2 else 0
-        self.tape(code, a, b)
+                for c, x in enumerate(op[3] if len(op) > 3 else ()):
+                    f[w, k, c] = float(x)
+        self.tape(code, a, b, f)
 
     def broadcast(self, name: str, mask: torch.Tensor | None = None) -> None:
         """One operation without arguments for every world (or the worlds in mask [W]), on the device."""
@@ -183,6 +216,25 @@ class VecSpace:
         for name, t in self.st.items():
             out[name] = t[..., w].cpu() if t.dim() > 1 else t[w].cpu()
         return out
+
+    def events(self, w: int) -> list:
+        """World w's events since the last CLEAR_EVENTS, in order: (name, ball id, other id, value) for DoProximity,
+        (name, ball id, value) for DoRange and DoTargetTracking."""
+        n = min(int(self.st["evn"][w]), self.M)
+        raw = self.st["ev"][:n, w].cpu().tolist()
+        rows = self.rows[:, w].cpu().tolist()
+        ids = self.park._ids.cpu().tolist()
+        out = []
+        for e in raw:
+            kind, value, ball, other = e & 15, (e >> 4) & 15, (e >> 8) & 255, (e >> 16) & 255
+            if kind == 1:
+                out.append((EVENTS[kind], ids[rows[ball]], ids[rows[other]], value))
+            else:
+                out.append((EVENTS[kind], ids[rows[ball]], value))
+        return out
+
+    def clear_events(self) -> None:
+        self.st["evn"].zero_()
 
     def dicts(self, w: int) -> dict:
         """World w's bubble dictionaries: {bubble: [(ball id, +1 | 0 | -1), ...] in insertion order}."""

@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define EBB_ABI_VERSION 6
+#define EBB_ABI_VERSION 7
 #define EBB_EINVAL (-1)
 #define EBB_ETOOBIG (-2)
 
@@ -172,7 +172,13 @@ enum {  /* the tape's operations, numbered as the reference's OPS (vec_space.py:
     EBB_SPACE_NONE = 0, EBB_SPACE_ADD = 1, EBB_SPACE_REFILE = 2, EBB_SPACE_INIT_BUBBLES = 3,
     EBB_SPACE_COPY_BUBBLES = 4, EBB_SPACE_KEEP_ALIVE = 5, EBB_SPACE_SET_INTERACTIVE = 6, EBB_SPACE_ADD_SENSOR = 7,
     EBB_SPACE_REMOVE_SENSOR = 8, EBB_SPACE_NOTIFY_RANGE = 9, EBB_SPACE_TRACK = 10, EBB_SPACE_REMOVE_BALL = 11,
-    EBB_SPACE_DEAD = 12, EBB_SPACE_AFTER_EVOLVE = 13
+    EBB_SPACE_DEAD = 12, EBB_SPACE_AFTER_EVOLVE = 13, EBB_SPACE_CLEAR_EVENTS = 14,
+    /* this build's own, no number in the reference's OPS: HandleProximities alone (the reference runs it inside
+     * AFTER_EVOLVE, as this one does) and the cloak attribute a sensor's candidates and CheckVisibility read */
+    EBB_SPACE_HANDLE_PROXIMITIES = 18, EBB_SPACE_SET_CLOAKED = 19
+};
+enum {  /* an event's kind (the reference's EVENTS, vec_space.py:164) */
+    EBB_SPACE_EV_PROXIMITY = 1, EBB_SPACE_EV_RANGE = 2, EBB_SPACE_EV_TRACKING = 3
 };
 enum {  /* a world's flags, the reference's FLAG bits (vec_space.py:171) and UNDEFINED (a deleted box read) */
     EBB_SPACE_FLAG_EVENTS = 1, EBB_SPACE_FLAG_TOPS = 2, EBB_SPACE_FLAG_EDGE = 4, EBB_SPACE_FLAG_BOXES = 8,
@@ -195,11 +201,36 @@ typedef struct EbbSpaceState {
     int64_t *inter_bubble, *inter_id, *inter_n;                    /* [sets][W], [W] */
     int64_t *keep_bubble, *keep_id, *keep_n;                       /* [sets][W], [W] */
     int64_t *bubble_id, *seq_next, *flags;                         /* [W] */
+    /* The proximity sensors, notification ranges and target tracking (space.py:1345-1523; the reference's layer keeps
+     * them in its srange ... pmap tensors, vec_space.py:825-836). Per slot [N][W]: the sensor's range (a float's
+     * value), period and elapsed time, its only-interactives flag, the ball's proximity flag, its notification range
+     * and in-range flag, its tracked slot (-1 none) with the range and in-range flag, the cloak attribute. A sensor's
+     * balls and the world's proximity balls are std::unordered_maps whose iteration order is kept as libstdc++ keeps
+     * it: their keys (slots) in that order, [cap][N][W] and [cap][W] (cap = `umap_cap` keys, at most
+     * EBB_SPACE_MAX_SLOTS), each with its length and bucket count (1 for a fresh map). Events [events][W], each an
+     * int32: kind | value << 4 | ball slot << 8 | other slot << 16, their count [W] (past `events`, counted, dropped
+     * and the world flagged EVENTS). `rnd` [W][EBB_RAND_WORDS]: each world's glibc rand() state (ebb_glibc_srand),
+     * drawn by a shuffled sensor. */
+    int64_t umap_cap, events;
+    double *srange, *speriod, *selapsed, *ntf_range, *trk_range;   /* [N][W] */
+    int64_t *trk, *cloaked;                                        /* [N][W] */
+    uint8_t *sonly, *has_prox, *ntf_in, *trk_in;                   /* [N][W] */
+    uint8_t* slist;                                                /* [umap_cap][N][W] */
+    int32_t *slen, *sbkt;                                          /* [N][W] */
+    uint8_t* pmap;                                                 /* [umap_cap][W] */
+    int32_t *pn, *pbkt;                                            /* [W] */
+    int32_t* ev;                                                   /* [events][W] */
+    int64_t* evn;                                                  /* [W] */
+    int32_t* rnd;                                                  /* [W][EBB_RAND_WORDS] */
 } EbbSpaceState;
-/* K operations a world, applied in order: code, a (a slot), b (an integer argument), each [K][W]. */
+/* K operations a world, applied in order: code, a (a slot), b (an integer argument), each [K][W], and f, each
+ * operation's floating-point arguments [K][4][W] (ADD_SENSOR: range, period; NOTIFY_RANGE: range; TRACK: range, and
+ * f[1] nonzero when the target's id is 0, which turns tracking off; b: ADD_SENSOR's flags, bit 0 only interactives,
+ * bit 1 shuffled; TRACK's target slot, -1 when the target is not a ball of the world; SET_CLOAKED's value). */
 typedef struct EbbSpaceTape {
     int64_t K;
     const int64_t *code, *a, *b;
+    const double* f;
 } EbbSpaceTape;
 
 /* The ABI version (EBB_ABI_VERSION). Replaces xbpm_abi / xbpo_abi (exact_ballpark/vec_modes_cuda.cu:750,

@@ -80,19 +80,27 @@ struct Ordered {
     }
 };
 
-// std::unordered_map<int64_t, ...>'s iteration order under libstdc++'s prime rehash policy, for the maps this slice
-// holds (at most 13 keys): a map's first insertion gives it 13 buckets (its policy asked for 11 keys); a key is linked
-// just before the first key of the order in its bucket (the key modulo the bucket count), else at the front; erasures
-// and clear() keep the rest; a 14th key would grow the table, which is outside the slice (`overflow`).
+// std::unordered_map<int64_t, ...>'s iteration order under libstdc++'s prime rehash policy (space.py:193-322, the
+// reference's clean-room statement of it; max load factor 1): a fresh map has one bucket and its first insertion asks
+// for room for 11 keys, which gives 13 buckets; a key past the bucket count grows the table to the first bucket count
+// of the library's prime list at or above twice the old count (the policy's want: the larger of the keys plus one and
+// twice the buckets), and the keys are re-linked one at a time in their old order. Up to 257 buckets that list holds
+// every prime (its first gaps come after 257), so the counts a map of up to 257 keys reaches, 13, 29, 59, 127 and 257,
+// are found here by trial division; a 258th key is outside this oracle (`overflow`). A key is linked just before the
+// first key of the order in its bucket (the key modulo the bucket count, as an unsigned 64-bit value), else at the
+// front; erasures and clear() keep the other keys' order and the bucket count.
 struct HashOrder {
     std::vector<int64_t> order;
     uint64_t buckets = 1;
     bool overflow = false;
+    static bool prime(uint64_t n) {
+        if (n < 2) return false;
+        for (uint64_t d = 2; d * d <= n; ++d)
+            if (n % d == 0) return false;
+        return true;
+    }
     bool contains(int64_t k) const { return std::find(order.begin(), order.end(), k) != order.end(); }
-    void insert(int64_t k) {
-        if (contains(k)) return;
-        if (buckets == 1) buckets = 13;
-        if (order.size() + 1 > 13) overflow = true;
+    void link(int64_t k) {
         const uint64_t b = (uint64_t)k % buckets;
         for (size_t i = 0; i < order.size(); ++i)
             if ((uint64_t)order[i] % buckets == b) {
@@ -100,6 +108,21 @@ struct HashOrder {
                 return;
             }
         order.insert(order.begin(), k);
+    }
+    void insert(int64_t k) {
+        if (contains(k)) return;
+        if (buckets == 1) {
+            buckets = 13;
+        } else if (order.size() + 1 > buckets) {
+            if (buckets >= 257) overflow = true;
+            uint64_t n = 2 * buckets;
+            while (!prime(n)) ++n;
+            buckets = n;
+            const std::vector<int64_t> old = order;
+            order.clear();
+            for (int64_t x : old) link(x);
+        }
+        link(k);
     }
     void erase(int64_t k) {
         auto it = std::find(order.begin(), order.end(), k);

@@ -48,6 +48,13 @@ def host_lib() -> ctypes.CDLL:
     return L
 
 
+def srand(seed: int) -> np.ndarray:
+    """A world's rand() state after srand(seed) (EBB_RAND_WORDS int32: the table, then the front and rear indices),
+    from the oracle's statement of glibc's generator (oracle/grand.py)."""
+    from oracle.grand import Rand
+    return np.array(Rand(int(seed)).state(), dtype=np.int32)
+
+
 def f32(x: float) -> float:
     return struct.unpack("<f", struct.pack("<f", float(x)))[0]
 
@@ -65,13 +72,17 @@ class HostPark:
         self.ids = np.arange(1, n + 1, dtype=np.int64)
         self.mode = np.full(n, 2, np.int32)
         self.free, self.interactive = np.zeros(n, np.uint8), np.zeros(n, np.uint8)
+        self.goto_pt, self.follow_ptr = np.zeros((3, n)), np.full(n, -1, np.int32)
+        self.follow_range = np.full(n, 10.0, np.float32)
+        self.massive, self.sensor = np.zeros(n, np.uint8), np.zeros(n, np.uint8)
 
     def struct(self):
         from exact_ballpark_b200 import _native
         s = _native.FlightState()
         s.n, s.friction, s.dt = self.n, FRICTION, DT
         for name in ("pos", "vel", "old_pos", "old_vel", "mass", "time_factor", "radius", "max_vel", "agility",
-                     "speed_fraction", "ids", "mode", "interactive"):
+                     "speed_fraction", "ids", "mode", "interactive", "goto_pt", "follow_ptr", "follow_range",
+                     "massive", "sensor"):
             setattr(s, name, getattr(self, name).ctypes.data)
         s.free_ = self.free.ctypes.data
         return s
@@ -92,13 +103,14 @@ class HostPark:
         m = float(self.mass[r]) * float(self.agility[r])
         self.time_factor[r] = 0.0 if m <= 0.0 else math.exp(-FRICTION * DT / m)
         self.mode[r] = 2
+        self.massive[r] = int(bool(a[13]))
 
 
 class HostLayer:
     """The layer's state as numpy arrays (VecSpace's tensors, the same shapes), run by the host build."""
 
-    def __init__(self, W: int, n: int, boxes: int | None = None):
-        self.W, self.N = W, n
+    def __init__(self, W: int, n: int, boxes: int | None = None, seeds=None, events: int = 4096):
+        self.W, self.N, self.M = W, n, events
         self.B, self.D, self.E, self.S = (boxes or 16 * n + 64), 8 * n + 16, 4 * n + 8, 2 * n + 8
         self.rows = np.array([[w * n + j for w in range(W)] for j in range(n)], dtype=np.int64)
         z = lambda *shape, dt=np.int64: np.zeros(shape, dtype=dt)   # noqa: E731
@@ -114,69 +126,97 @@ class HostLayer:
             "dict_bubble": z(D, W), "dict_n": z(W), "entry_bubble": z(E, W), "entry_id": z(E, W),
             "entry_value": z(E, W), "entry_n": z(W), "inter_bubble": z(S, W), "inter_id": z(S, W), "inter_n": z(W),
             "keep_bubble": z(S, W), "keep_id": z(S, W), "keep_n": z(W), "bubble_id": z(W), "seq_next": z(W),
-            "flags": z(W)}
+            "flags": z(W),
+            "srange": z(n, W, dt=np.float64), "speriod": z(n, W, dt=np.float64) + 2.0,
+            "selapsed": z(n, W, dt=np.float64), "ntf_range": z(n, W, dt=np.float64),
+            "trk_range": z(n, W, dt=np.float64), "trk": z(n, W) - 1, "cloaked": z(n, W),
+            "sonly": z(n, W, dt=np.uint8), "has_prox": z(n, W, dt=np.uint8), "ntf_in": z(n, W, dt=np.uint8),
+            "trk_in": z(n, W, dt=np.uint8), "slist": z(n, n, W, dt=np.uint8), "slen": z(n, W, dt=np.int32),
+            "sbkt": z(n, W, dt=np.int32) + 1, "pmap": z(n, W, dt=np.uint8), "pn": z(W, dt=np.int32),
+            "pbkt": z(W, dt=np.int32) + 1, "ev": z(self.M, W, dt=np.int32), "evn": z(W),
+            "rnd": np.stack([srand(seed) for seed in (seeds if seeds is not None else [1] * W)])}
 
-    def tape(self, park: HostPark, code, a, b) -> None:
+    def tape(self, park: HostPark, code, a, b, f=None) -> None:
         from exact_ballpark_b200 import _native
         s = _native.SpaceState()
         s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets = self.W, self.N, self.B, self.D, self.E, self.S
+        s.umap_cap, s.events = self.N, self.M
         s.rows = self.rows.ctypes.data
         for name, arr in self.st.items():
             setattr(s, name, arr.ctypes.data)
         code, a, b = (np.ascontiguousarray(np.asarray(x, dtype=np.int64).reshape(-1, self.W)) for x in (code, a, b))
-        t = _native.SpaceTape(code.shape[0], code.ctypes.data, a.ctypes.data, b.ctypes.data)
+        K = code.shape[0]
+        f = np.zeros((K, 4, self.W)) if f is None else np.ascontiguousarray(np.asarray(f, np.float64).reshape(K, 4,
+                                                                                                           self.W))
+        t = _native.SpaceTape(K, code.ctypes.data, a.ctypes.data, b.ctypes.data, f.ctypes.data)
         ps = park.struct()
         host_lib().space_tape_host(ctypes.byref(ps), ctypes.byref(s), ctypes.byref(t))
 
 
 def translate(park: HostPark, w: int, op, n: int) -> tuple:
-    """One golden operation of world w: its effect on the park's rows, and the layer's operation (code, slot, b)."""
+    """One golden operation of world w: its effect on the park's rows, and the layer's operation (code, slot, b, f)."""
     from exact_ballpark_b200.space import OP
     code, bid = int(op[0]), int(op[1])
     a = [float(x) for x in op[2:]]
     j = bid - 1
     r = w * n + j
+    none = (OP["NONE"], -1, 0, (0.0, 0.0, 0.0, 0.0))
     if code == sp.ADD:
         park.add(r, a)
-        return OP["ADD"], j, 0
+        return OP["ADD"], j, 0, none[3]
     if code == sp.POS:
         park.pos[:, r] = a[0:3]
         park.old_pos[:, r] = a[0:3]
-        return OP["REFILE"], j, 0
+        return OP["REFILE"], j, 0, none[3]
     if code == sp.RADIUS:
         v = f32(a[0])
         if v < 0.0:
-            return OP["NONE"], -1, 0
+            return none
         park.radius[r] = v
-        return OP["REFILE"], j, 0
+        return OP["REFILE"], j, 0, none[3]
     if code == sp.MAXVEL:
         v = f32(a[0])
         if v < 0.0:
-            return OP["NONE"], -1, 0
+            return none
         park.max_vel[r] = v
-        return OP["REFILE"], j, 0
+        return OP["REFILE"], j, 0, none[3]
     if code == sp.REMOVE:
-        return OP["REMOVE_BALL"], j, 0
+        return OP["REMOVE_BALL"], j, 0, none[3]
     if code == sp.INIT:
-        return OP["INIT_BUBBLES"], -1, 0
+        return OP["INIT_BUBBLES"], -1, 0, none[3]
     if code == sp.COPY:
-        return OP["COPY_BUBBLES"], -1, 0
+        return OP["COPY_BUBBLES"], -1, 0, none[3]
     if code == sp.INTERACTIVE:
-        return OP["SET_INTERACTIVE"], j, int(bool(a[0]))
+        return OP["SET_INTERACTIVE"], j, int(bool(a[0])), none[3]
     if code == sp.KEEPALIVE:
-        return OP["KEEP_ALIVE"], j, 0
+        return OP["KEEP_ALIVE"], j, 0, none[3]
+    if code == sp.CLOAKED:
+        return OP["SET_CLOAKED"], j, int(a[0]), none[3]
+    if code == sp.SENSOR:                                 # range, period, only interactives, shuffled
+        return OP["ADD_SENSOR"], j, int(bool(a[2])) | (2 if a[3] else 0), (a[0], a[1], 0.0, 0.0)
+    if code == sp.UNSENSOR:
+        return OP["REMOVE_SENSOR"], j, 0, none[3]
+    if code == sp.NOTIFY:
+        return OP["NOTIFY_RANGE"], j, 0, (a[0], 0.0, 0.0, 0.0)
+    if code == sp.TRACK:                                  # the target's slot, or -1 when its id is none of the world's
+        t = int(a[0])
+        slot = t - 1 if 1 <= t <= n else -1
+        return OP["TRACK"], j, slot, (a[1], 1.0 if t == 0 else 0.0, 0.0, 0.0)
+    if code == sp.PROXIMITIES:
+        return OP["HANDLE_PROXIMITIES"], -1, 0, none[3]
     if code == sp.GOTO and all(math.isfinite(x) for x in a[0:3]):   # GotoPoint: a speed fraction of 0 becomes 1
         if park.speed_fraction[r] == 0.0:
             park.speed_fraction[r] = 1.0
         park.mode[r] = 0
-        return OP["NONE"], -1, 0
+        park.goto_pt[:, r] = a[0:3]
+        return none
     if code == sp.STOP:
         park.mode[r] = 2
-        return OP["NONE"], -1, 0
-    return OP["NONE"], -1, 0                              # the cloak attribute, the queries: not the layer's
+        return none
+    return none                                           # the queries: not the layer's
 
 
-def text(st: dict, park_ids, park_mode, w: int) -> str:
+def text(st: dict, park_ids, park_mode, w: int, park_sensor=None) -> str:
     """World w's layer state as the oracle's state text (the lines the layer holds)."""
     n = st["level"].shape[0]
     col = lambda name: st[name][..., w]                   # noqa: E731
@@ -207,6 +247,21 @@ def text(st: dict, park_ids, park_mode, w: int) -> str:
     out.append("L" + "".join(f" {int((lv == i).sum())}" for i in range(8)) + "\n")
     undefined = 1 if int(st["flags"][w]) & (1 << 11) else 0
     out.append(f"F {int(st['free_boxes'][w])} {int(st['bubble_id'][w])} {undefined}\n")
+    if "pn" in st:
+        pid = lambda k: int(park_ids[w * n + int(k)])     # noqa: E731
+        pn = int(st["pn"][w])
+        if pn:
+            out.append("P" + "".join(f" {pid(k)}" for k in st["pmap"][:pn, w]) + "\n")
+        for bid, j in slots:
+            on, ln, hp = int(park_sensor[w * n + j]) if park_sensor is not None else 0, int(st["slen"][j, w]), \
+                int(st["has_prox"][j, w])
+            if not on and not ln and not hp:
+                continue
+            trk = int(st["trk"][j, w])
+            bits = "%016x" % struct.unpack("<Q", struct.pack("<d", float(st["selapsed"][j, w])))[0]
+            out.append(f"S {bid} {on} {bits} {hp} {int(st['ntf_in'][j, w])} {int(st['trk_in'][j, w])} "
+                       f"{pid(trk) if trk >= 0 else 0}" + "".join(f" {pid(k)}" for k in st["slist"][:ln, j, w])
+                       + "\n")
     dicts = {int(b): [] for b in col("dict_bubble")[:int(st["dict_n"][w])]}
     for e in range(int(st["entry_n"][w])):
         dicts.setdefault(int(st["entry_bubble"][e, w]), []).append((int(st["entry_id"][e, w]),
@@ -219,97 +274,161 @@ def text(st: dict, park_ids, park_mode, w: int) -> str:
     return "".join(out)
 
 
-def oracle_lines(t: str) -> str:
-    """The oracle's state text less the lines the layer does not hold (the sensors', the flight states', answers)."""
-    return "".join(line + "\n" for line in t.splitlines() if line[:1] in ("B", "L", "F", "U", "I", "K"))
+def oracle_lines(t: str, code: int = 0) -> str:
+    """The oracle's state text less the lines the layer does not hold (the flight states, the queries' answers):
+    the answer kept for HandleProximities and a tick (their events)."""
+    keep = ("B", "L", "F", "P", "S", "U", "I", "K") + (("Q",) if code in (sp.PROXIMITIES, sp.TICK) else ())
+    return "".join(line + "\n" for line in t.splitlines() if line[:1] in keep)
+
+
+def events_text(st: dict, park_ids, w: int, n: int) -> str:
+    """World w's events as the oracle writes a HandleProximities answer."""
+    out = []
+    for e in st["ev"][:int(st["evn"][w]), w]:
+        e = int(e)
+        kind, value, ball, other = e & 15, (e >> 4) & 15, (e >> 8) & 255, (e >> 16) & 255
+        b = int(park_ids[w * n + ball])
+        if kind == 1:
+            out.append(f" {b}:{int(park_ids[w * n + other])}:{value}")
+        else:
+            out.append(f" {'R' if kind == 2 else 'T'}{b}:{value}")
+    return "Q" + "".join(out) + "\n"
 
 
 def drive(streams: list, kernel: str = "host", device=None) -> tuple:
-    """Every stream through the layer, one world each, one operation a launch: (texts [world][op], flags [W])."""
+    """Every stream through the layer, one world each, one operation a launch: (texts [world][op], flags [W]); a
+    HandleProximities operation's text ends with its events."""
     W = len(streams)
+    seeds = [int(s[1]) if isinstance(s, tuple) else 1 for s in streams]
+    streams = [s[0] if isinstance(s, tuple) else s for s in streams]
     N = int(max(int(np.max(np.asarray(s)[:, 1])) for s in streams))
     park = HostPark(W * N)
     park.ids[:] = np.tile(np.arange(1, N + 1, dtype=np.int64), W)       # world w's ball b at row w N + b - 1
     K = max(len(s) for s in streams)
     texts = [[] for _ in range(W)]
     if kernel == "host":
-        layer = HostLayer(W, N)
-        run = lambda code, a, b: layer.tape(park, code, a, b)                       # noqa: E731
+        layer = HostLayer(W, N, seeds=seeds)
+
+        def run(code, a, b, f):
+            layer.st["evn"][:] = 0
+            layer.tape(park, code, a, b, f)
+
         read = lambda: layer.st                                                     # noqa: E731
+        sensor = lambda: park.sensor                                                # noqa: E731
     else:
         import torch
         from exact_ballpark_b200.modes import VecModesPark
         from exact_ballpark_b200.space import VecSpace
         dpark = VecModesPark(W * N, friction=FRICTION, tick_interval_ms=1000, device=device or "cuda")
-        layer = VecSpace(dpark, np.arange(W * N, dtype=np.int64).reshape(W, N))
+        layer = VecSpace(dpark, np.arange(W * N, dtype=np.int64).reshape(W, N), events=4096, seed=seeds)
 
-        def run(code, a, b):
+        def run(code, a, b, f):
             for name in ("pos", "vel", "old_pos", "old_vel", "mass", "time_factor", "radius", "max_vel", "agility",
-                         "speed_fraction", "ids", "mode"):
+                         "speed_fraction", "ids", "mode", "follow_ptr", "follow_range"):
                 getattr(dpark, "_" + name).copy_(torch.from_numpy(getattr(park, name)).to(getattr(dpark, "_" + name)))
-            dpark._free.copy_(torch.from_numpy(park.free.astype(bool)).to(dpark.dev))
-            dpark._interactive.copy_(torch.from_numpy(park.interactive.astype(bool)).to(dpark.dev))
+            dpark._goto.copy_(torch.from_numpy(park.goto_pt).to(dpark._goto))
+            for name in ("free", "interactive", "massive"):
+                getattr(dpark, "_" + name).copy_(torch.from_numpy(getattr(park, name).astype(bool)).to(dpark.dev))
+            layer.clear_events()
             layer.tape(torch.from_numpy(np.asarray(code, dtype=np.int64).reshape(W, 1)),
                        torch.from_numpy(np.asarray(a, dtype=np.int64).reshape(W, 1)),
-                       torch.from_numpy(np.asarray(b, dtype=np.int64).reshape(W, 1)))
+                       torch.from_numpy(np.asarray(b, dtype=np.int64).reshape(W, 1)),
+                       torch.from_numpy(np.asarray(f, dtype=np.float64).reshape(W, 1, 4)))
             park.interactive[:] = dpark._interactive.cpu().numpy().astype(np.uint8)
+            park.radius[:] = dpark._radius.cpu().numpy()
 
         read = lambda: {k: v.cpu().numpy() for k, v in layer.st.items()}            # noqa: E731
+        sensor = lambda: dpark._sensor.cpu().numpy().astype(np.uint8)                # noqa: E731
     for k in range(K):
         code, a, b = np.zeros(W, np.int64), np.full(W, -1, np.int64), np.zeros(W, np.int64)
+        f = np.zeros((W, 4))
         for w, ops in enumerate(streams):
             if k < len(ops):
-                code[w], a[w], b[w] = translate(park, w, ops[k], N)
-        run(code, a, b)
+                code[w], a[w], b[w], f[w] = translate(park, w, ops[k], N)
+        run(code, a, b, f.T.copy() if kernel == "host" else f)
         st = read()
+        sens = sensor()
         for w, ops in enumerate(streams):
             if k < len(ops):
-                texts[w].append(text(st, park.ids, park.mode, w))
+                t = text(st, park.ids, park.mode, w, sens)
+                if int(ops[k][0]) == sp.PROXIMITIES:
+                    t += events_text(st, park.ids, w, N)
+                texts[w].append(t)
     return texts, read()["flags"].copy()
 
 
-def drive_ticks(ops, device="cuda") -> list:
-    """One ticking stream (GOTO and STOP ships, tests/golden/space_trace.py's tick_ops) through VecSpace over a
-    VecModesPark on the device, its ticks the layer's `tick` (dead bubbles skipped, the re-filings after): the texts
-    after every operation. The park is the state's owner: AddBall writes its row, GotoPoint and Stop are its commands;
-    the sensors' operations are left out."""
+def drive_ticks(ops, device="cuda", seed: int = 1) -> list:
+    """One ticking or mode stream (tests/golden/space_trace.py's tick_ops and mode_ops) through VecSpace over a
+    VecModesPark on the device, its ticks the layer's `tick` (dead bubbles skipped, the re-filings and
+    HandleProximities after): the texts after every operation, a tick's and HandleProximities' with their events. The
+    park owns the rows: AddBall writes a row, GotoPoint, Stop, FollowBall and Orbit (their same-bubble test reading
+    the layer's bubbles), WarpTo and RemoveBall's Stop and StopAllFollowers are its commands; the sensors' operations
+    are the layer's."""
     import torch
     from exact_ballpark_b200.modes import VecModesPark
-    from exact_ballpark_b200.space import VecSpace
+    from exact_ballpark_b200.space import OP, VecSpace
     n = int(np.max(np.asarray(ops)[:, 1]))
     park = VecModesPark(n, friction=FRICTION, tick_interval_ms=1000, device=device)
-    layer = VecSpace(park, np.arange(n, dtype=np.int64).reshape(1, n))
-    host = HostPark(n)
+    layer = VecSpace(park, np.arange(n, dtype=np.int64).reshape(1, n), events=4096, seed=seed)
     out = []
+    dev = park.dev
     for op in ops:
         code, bid = int(op[0]), int(op[1])
         a = [float(x) for x in op[2:]]
         j = bid - 1
-        mask = torch.zeros(n, dtype=torch.bool, device=park.dev)
+        mask = torch.zeros(n, dtype=torch.bool, device=dev)
         if 0 <= j < n:
             mask[j] = True
-        if code == sp.TICK:
+        live = 0 <= j < n and bool(layer.st["in_park"][j, 0])
+        layer.clear_events()
+        if code in (sp.SENSOR, sp.UNSENSOR, sp.NOTIFY, sp.TRACK, sp.CLOAKED, sp.PROXIMITIES):
+            h = HostPark(n)
+            lc, la, lb, lf = translate(h, 0, op, n)
+            if lc:
+                name = next(k for k, v in OP.items() if v == lc)
+                layer.ops([[(name, la, lb, lf)]])
+        elif code == sp.TICK:
             layer.tick()
         elif code == sp.ADD:
-            host.add(j, a)
-            for name in ("pos", "vel", "old_pos", "old_vel", "mass", "time_factor", "radius", "max_vel", "agility",
-                         "speed_fraction", "mode"):
-                getattr(park, "_" + name)[..., j] = torch.as_tensor(getattr(host, name)[..., j]).to(
+            h = HostPark(n)
+            h.add(j, a)
+            names = ("pos", "vel", "mass", "time_factor", "radius", "max_vel", "agility", "speed_fraction")
+            for name in names if live else names + ("old_pos", "old_vel"):
+                getattr(park, "_" + name)[..., j] = torch.as_tensor(getattr(h, name)[..., j]).to(
                     getattr(park, "_" + name))
-            park._free[j], park._interactive[j] = bool(host.free[j]), bool(host.interactive[j])
+            park._free[j], park._interactive[j] = bool(h.free[j]), bool(h.interactive[j])
             park._massive[j] = bool(a[13])
-            park._last_g[:, j] = 0.0
+            park._effect_stamp[j] = park._owner_id[j] = park._follow_id[j] = 0
+            park._follow_range[j], park._mode[j] = 10.0, 2          # a re-added ball keeps its target pointer
+            if not live:
+                park._follow_ptr[j], park._last_g[:, j], park._last_collision[j] = -1, 0.0, -1.0
             layer.ops([[("ADD", j)]])
+        elif not live and code in (sp.GOTO, sp.STOP, sp.REMOVE, sp.FOLLOW, sp.ORBIT, sp.WARP):
+            pass                                          # a command to a ball not in the world does nothing
+        elif code in (sp.FOLLOW, sp.ORBIT):
+            t = int(a[0]) - 1
+            park.bubble.copy_(layer.st["bubble"][:, 0].to(park.bubble))   # FollowBall's same-bubble test
+            saved = park._moribund.clone()
+            park._moribund.logical_or_(~layer.st["in_park"][:, 0].to(torch.bool))   # a target not in the world
+            target = torch.full((n,), t if 0 <= t < n else -1, dtype=torch.int64, device=dev)
+            (park.follow if code == sp.FOLLOW else park.orbit)(mask, target, torch.full((n,), a[1], device=dev,
+                                                                                          dtype=torch.float64))
+            park._moribund.copy_(saved)
+        elif code == sp.WARP:
+            park.warp_to(mask, torch.tensor([a[0:3]] * n, dtype=torch.float64, device=dev),
+                         torch.full((n,), a[3], dtype=torch.float64, device=dev),
+                         torch.full((n,), int(a[4]), dtype=torch.int64, device=dev))
         elif code == sp.POS:
-            park._pos[:, j] = torch.tensor(a[0:3], dtype=torch.float64, device=park.dev)
-            park._old_pos[:, j] = torch.tensor(a[0:3], dtype=torch.float64, device=park.dev)
+            park._pos[:, j] = torch.tensor(a[0:3], dtype=torch.float64, device=dev)
+            park._old_pos[:, j] = torch.tensor(a[0:3], dtype=torch.float64, device=dev)
             layer.ops([[("REFILE", j)]])
         elif code == sp.GOTO:
-            park.goto_point(mask, torch.tensor([a[0:3]] * n, dtype=torch.float64, device=park.dev))
+            park.goto_point(mask, torch.tensor([a[0:3]] * n, dtype=torch.float64, device=dev))
         elif code == sp.STOP:
             park.stop(mask)
-        elif code == sp.REMOVE:
+        elif code == sp.REMOVE:                           # RemoveBall: Stop, then StopAllFollowers
             park.stop(mask)
+            park._release_followers(mask)
             layer.ops([[("REMOVE_BALL", j)]])
         elif code == sp.INIT:
             layer.ops([[("INIT_BUBBLES",)]])
@@ -320,11 +439,15 @@ def drive_ticks(ops, device="cuda") -> list:
         elif code == sp.KEEPALIVE:
             layer.ops([[("KEEP_ALIVE", j)]])
         st = {k: v.cpu().numpy() for k, v in layer.st.items()}
-        out.append(text(st, park._ids.cpu().numpy(), park._mode.cpu().numpy(), 0))
+        ids = park._ids.cpu().numpy()
+        t = text(st, ids, park._mode.cpu().numpy(), 0, park._sensor.cpu().numpy().astype(np.uint8))
+        if code in (sp.TICK, sp.PROXIMITIES):
+            t += events_text(st, ids, 0, n)
+        out.append(t)
     return out
 
 
-def drive_ticks_host(ops) -> list:
+def drive_ticks_host(ops, seed: int = 1) -> list:
     """drive_ticks on the CPU, for the ticking and the mode streams: the flight oracle's park (oracle/park.py's
     OraclePark, its tick the C++ oracle) owns the rows (AddBall, GotoPoint, Stop, FollowBall and Orbit with the
     layer's bubbles for their same-bubble test, WarpTo, RemoveBall's Stop and StopAllFollowers) and ticks them with
@@ -334,7 +457,7 @@ def drive_ticks_host(ops) -> list:
     from oracle.park import OraclePark
     n = int(np.max(np.asarray(ops)[:, 1]))
     op = OraclePark(n, friction=FRICTION, tick_interval_ms=1000)
-    host, layer = HostPark(n), HostLayer(1, n)
+    host, layer = HostPark(n), HostLayer(1, n, seeds=[seed])
 
     def pull() -> None:                                   # the layer's view of the oracle park's rows
         for name in ("pos", "vel", "old_pos", "old_vel"):
@@ -347,11 +470,17 @@ def drive_ticks_host(ops) -> list:
         host.mode[:] = op.mode.astype(np.int32)
         host.free[:] = op.free.astype(np.uint8)
         host.interactive[:] = op.interactive.astype(np.uint8)
+        host.massive[:] = op.massive.astype(np.uint8)
+        host.goto_pt[:] = op.goto.T
+        host.follow_ptr[:] = op.follow_ptr.astype(np.int32)
+        host.follow_range[:] = op.follow_range.astype(np.float32)
+        host.sensor[:] = op.sensor.astype(np.uint8)
 
-    def run(name: str, j: int = -1, b: int = 0) -> None:
+    def run(name: str, j: int = -1, b: int = 0, f=(0.0, 0.0, 0.0, 0.0)) -> None:
         pull()
-        layer.tape(host, [OP[name]], [j], [b])
+        layer.tape(host, [OP[name]], [j], [b], np.asarray(f, dtype=np.float64).reshape(1, 4, 1))
         op.interactive = host.interactive.astype(bool)
+        op.sensor = host.sensor.astype(bool)               # the layer's sensor flags (AddProximitySensor's)
 
     out = []
     for row in ops:
@@ -361,7 +490,13 @@ def drive_ticks_host(ops) -> list:
         mask = np.zeros(n, dtype=bool)
         if 0 <= j < n:
             mask[j] = True
-        if code == sp.TICK:
+        layer.st["evn"][:] = 0
+        sensor_op = code in (sp.SENSOR, sp.UNSENSOR, sp.NOTIFY, sp.TRACK, sp.CLOAKED, sp.PROXIMITIES)
+        if sensor_op:
+            lc, la, lb, lf = translate(host, 0, row, n)
+            if lc:
+                run(next(k for k, v in OP.items() if v == lc), la, lb, lf)
+        elif code == sp.TICK:
             run("DEAD")
             dead = layer.st["dead"][:, 0].astype(bool)
             warp_proper = (op.mode == 3) & (op.effect_stamp >= 0) & op.free & ~op.moribund & ~dead
@@ -420,5 +555,8 @@ def drive_ticks_host(ops) -> list:
             run("SET_INTERACTIVE", j, int(bool(a[0])))
         elif code == sp.KEEPALIVE:
             run("KEEP_ALIVE", j)
-        out.append(text(layer.st, op.ids, op.mode, 0))
+        t = text(layer.st, op.ids, op.mode, 0, op.sensor.astype(np.uint8))
+        if code in (sp.TICK, sp.PROXIMITIES):
+            t += events_text(layer.st, op.ids, 0, n)
+        out.append(t)
     return out

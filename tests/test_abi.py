@@ -26,7 +26,7 @@ def test_the_library_exports_every_declared_entry_point():
 
 def test_abi_version_and_scratch_size():
     lib = _native.lib()
-    assert lib.ebb_abi() == _native.ABI == 6
+    assert lib.ebb_abi() == _native.ABI == 7
     assert lib.ebb_flight_scratch_bytes(0) == 0
     b = lib.ebb_flight_scratch_bytes(1000)
     assert b >= 1000 * (8 * 7 + 1) and b % 256 == 0

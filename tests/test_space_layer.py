@@ -17,26 +17,27 @@ import space_trace as sp
 from oracle import space_world
 
 FAMILIES = ("mixed", "long", "sweep")
+HUGE = 256                                                 # EBB_SPACE_FLAG_HUGE: a sensor meeting a huge ball
 
 
 def _streams(families=FAMILIES):
-    out = []
-    for sc in sp.load(sp.GOLDEN / "space_bubbles"):
-        if sc["seed"].split("-")[0] in families:
-            keep = ~np.isin(sc["ops"][:, 0], (sp.SENSOR, sp.UNSENSOR))
-            out.append(dict(sc, ops=sc["ops"][keep]))
-    return out
+    return [sc for sc in sp.load(sp.GOLDEN / "space_bubbles") if sc["seed"].split("-")[0] in families]
 
 
 def _oracle_texts(sc):
-    return [sl.oracle_lines(t) for t in space_world.run(sc["ops"], seed=sc["rand_seed"])]
+    return [sl.oracle_lines(t, int(op[0])) for t, op in zip(space_world.run(sc["ops"], seed=sc["rand_seed"]),
+                                                            sc["ops"])]
+
+
+def _inputs(scs):
+    return [(sc["ops"], sc["rand_seed"]) for sc in scs]
 
 
 def test_the_layers_program_matches_the_oracle_after_every_operation():
     scs = _streams()
     assert len(scs) == 72
-    texts, flags = sl.drive([sc["ops"] for sc in scs], "host")
-    assert not flags.any()
+    texts, flags = sl.drive(_inputs(scs), "host")
+    assert not (flags & ~HUGE).any()
     bad = []
     for sc, got in zip(scs, texts):
         want = _oracle_texts(sc)
@@ -47,7 +48,7 @@ def test_the_layers_program_matches_the_oracle_after_every_operation():
 
 def test_the_streams_reach_the_layers_paths():
     scs = _streams()
-    texts, _ = sl.drive([sc["ops"] for sc in scs], "host")
+    texts, _ = sl.drive(_inputs(scs), "host")
     lines = [line for t in texts for text in t for line in text.splitlines()]
     assert max(int(x.split()[1]) for x in lines if x.startswith("F ")) == 256   # BoxAllocator full, later deletions
     assert sum(1 for x in lines if x.startswith("B ") and " - " not in x and int(x.split()[11]) == (1 << 27) - 1) > 100
@@ -58,11 +59,11 @@ def test_the_streams_reach_the_layers_paths():
 
 def test_a_planted_fault_in_the_oracle_is_seen():
     sc = _streams(("mixed",))[0]
-    texts, _ = sl.drive([sc["ops"]], "host")
+    texts, _ = sl.drive(_inputs([sc]), "host")
     ops = sc["ops"].copy()
     k = next(i for i in range(len(ops)) if int(ops[i, 0]) == sp.ADD)
     ops[k, 7] += sp.TOP                                    # the oracle's ball added a top box further along x
-    want = [sl.oracle_lines(t) for t in space_world.run(ops, seed=sc["rand_seed"])]
+    want = [sl.oracle_lines(t, int(op[0])) for t, op in zip(space_world.run(ops, seed=sc["rand_seed"]), ops)]
     assert texts[0] != want
 
 
@@ -73,8 +74,8 @@ def test_a_full_box_table_flags_the_world_and_leaves_it_alone():
     layer = sl.HostLayer(1, 40, boxes=8)
     flagged_at = None
     for k, op in enumerate(sc["ops"][:200]):
-        code, a, b = sl.translate(park, 0, op, 40)
-        layer.tape(park, [code], [a], [b])
+        code, a, b, f = sl.translate(park, 0, op, 40)
+        layer.tape(park, [code], [a], [b], np.asarray(f).reshape(1, 4, 1))
         if layer.st["flags"][0] and flagged_at is None:
             flagged_at = k
             frozen = {n: v.copy() for n, v in layer.st.items()}
@@ -91,7 +92,7 @@ def test_the_layers_tick_matches_the_oracle_on_the_cpu(family):
     assert len(scs) == 40
     bad = []
     for sc in scs:
-        got = sl.drive_ticks_host(sc["ops"])
+        got = sl.drive_ticks_host(sc["ops"], sc["rand_seed"])
         want = _oracle_texts(sc)
         if got != want:
             bad.append((sc["seed"], next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
@@ -103,10 +104,10 @@ def test_the_device_layer_matches_its_host_program_word_for_word():
     import torch
     assert torch.cuda.is_available()
     scs = _streams()
-    streams = [sc["ops"] for sc in scs]
+    streams = _inputs(scs)
     got, flags = sl.drive(streams, "cuda")
     want, _ = sl.drive(streams, "host")
-    assert not flags.any()
+    assert not (flags & ~HUGE).any()
     bad = [sc["seed"] for sc, g, w in zip(scs, got, want) if g != w]
     assert not bad, f"{len(bad)} worlds differ from the host program, first {bad[:3]}"
     bad = [sc["seed"] for sc, g in zip(scs, got) if g != _oracle_texts(sc)]
@@ -114,17 +115,20 @@ def test_the_device_layer_matches_its_host_program_word_for_word():
 
 
 @pytest.mark.gpu
-def test_the_layers_tick_over_the_flight_park_matches_the_oracle():
-    """The ticking streams (GOTO and STOP ships across top boxes and bubbles): VecSpace.tick over a VecModesPark (the
-    dead bubbles' rows skipped by the park's tick, then the re-filings of the balls that moved, in ascending id)
-    against the oracle's tick, after every operation."""
+@pytest.mark.parametrize("family", ["tick", "modes"])
+def test_the_layers_tick_over_the_flight_park_matches_the_oracle(family):
+    """The ticking streams (GOTO and STOP ships across top boxes and bubbles, with sensors, tracked targets and
+    notification ranges) and the mode streams (FollowBall, Orbit, WarpTo with drop-outs, releases, re-added
+    followers, sensors): VecSpace.tick over a VecModesPark (the dead bubbles' rows skipped by the park's tick, then
+    the re-filings of the balls that moved, in ascending id, then HandleProximities) against the oracle's tick, every
+    state and every tick's events after every operation."""
     import torch
     assert torch.cuda.is_available()
-    scs = _streams(("tick",))
+    scs = _streams((family,))
     assert len(scs) == 40
     bad = []
     for sc in scs:
-        got = sl.drive_ticks(sc["ops"])
+        got = sl.drive_ticks(sc["ops"], seed=sc["rand_seed"])
         want = _oracle_texts(sc)
         if got != want:
             bad.append((sc["seed"], next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
