@@ -629,10 +629,32 @@ def make_space_bubbles() -> None:
           f"{dropped} left out, {time.time() - t0:.0f} s", flush=True)
 
 
+def make_space_crowd() -> None:
+    """space_crowd: crowded worlds of 16 to 128 sensing ships (tests/golden/space_trace.py's crowd_ops: the sensors'
+    lists and the proximity map past the rehash policy's growths), each operation's state digest recorded on the
+    reference's own SpaceBallpark (is_master)."""
+    import space_trace as sp
+    from exact_ballpark.space import SpaceBallpark
+    t0 = time.time()
+    scenarios = []
+    for seed in range(1, 9):
+        ops = sp.crowd_ops(seed)
+        park = SpaceBallpark(1.0e6, 1000, is_master=True, seed=seed)
+        digests = []
+        for op in ops:
+            answer = sp.apply(park, op)
+            digests.append(sp.digest(sp.state_text(park) + answer))
+        scenarios.append({"seed": f"crowd-{seed}", "ops": ops, "digests": digests, "rand_seed": seed})
+        print(f"    crowd-{seed}: {int(max(op[1] for op in ops))} ships, {len(ops)} operations, "
+              f"{time.time() - t0:.0f} s", flush=True)
+    sp.save(HERE / "space_crowd", scenarios)
+    print(f"  space_crowd: {len(scenarios)} worlds, {time.time() - t0:.0f} s", flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending", "server_ontick",
-                                       "server_collide", "server_collide_more", "space_bubbles"),
+                                       "server_collide", "server_collide_more", "space_bubbles", "space_crowd"),
                     default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
     a = ap.parse_args()
@@ -662,6 +684,8 @@ def main() -> None:
         make_server_collide_more()
     if a.only in (None, "space_bubbles"):
         make_space_bubbles()
+    if a.only in (None, "space_crowd"):
+        make_space_crowd()
 
 
 if __name__ == "__main__":

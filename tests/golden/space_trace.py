@@ -14,6 +14,7 @@ CPU oracle (oracle/space.cpp) and compare, operation by operation.
 from __future__ import annotations
 
 import hashlib
+import math
 import random
 import struct
 from pathlib import Path
@@ -330,6 +331,46 @@ def collide_ops(seed: int, n_ops: int = 100) -> list:
             ops.append(_op(INTERACTIVE, a, float(r.random() < 0.6)))
         else:
             ops.append(_op(INIT))
+    return ops
+
+
+def crowd_ops(seed: int, n_ticks: int = 12) -> list:
+    """A crowded world of config 3's shape at a golden's size: 16 to 128 ships (free, interactive, not massive) in 1
+    to 3 Gaussian blobs (sigma 10 km) around centres within +-1,000 km, every ship with a proximity sensor of 1 to
+    250 km (log-uniform; period 1 s, some shuffled), so that the sensors' lists and the proximity map grow past 13,
+    29, 59 and 127 keys (the rehash policy's growths); GOTO legs of up to 3 km/s, a few notification ranges, tracked
+    targets, removals, InitializeBubbles and CopyBubbles between the ticks."""
+    r = random.Random(f"space-crowd-{seed}")
+    n = r.choice((16, 40, 70, 128)) if seed > 4 else (16, 40, 70, 128)[seed - 1]
+    centres = [[r.uniform(-1e6, 1e6) for _ in range(3)] for _ in range(r.randint(1, 3))]
+    ops, live = [], []
+    for b in range(1, n + 1):
+        c = r.choice(centres)
+        p = [x + r.gauss(0.0, 1e4) for x in c]
+        max_vel = 10 ** r.uniform(2.0, math.log10(3000.0))
+        ops.append(_op(ADD, b, 10 ** r.uniform(6.0, 9.0), r.uniform(20.0, 500.0), max_vel, 1.0, 1.0, *p, 0.0, 0.0,
+                       0.0, r.uniform(0.1, 5.0), 1.0, 0.0))
+        live.append(b)
+    for b in live:
+        ops.append(_op(SENSOR, b, 10 ** r.uniform(3.0, math.log10(2.5e5)), 1.0, 0.0, float(r.random() < 0.3)))
+    for t in range(n_ticks):
+        for b in r.sample(live, max(1, len(live) // 4)):
+            c = r.choice(centres)
+            ops.append(_op(GOTO, b, *[x + r.gauss(0.0, 2e4) for x in c]))
+        k = r.random()
+        if k < 0.2:
+            ops.append(_op(NOTIFY, r.choice(live), r.choice((500.0, 5e3, 5e4))))
+        elif k < 0.4:
+            ops.append(_op(TRACK, r.choice(live), r.choice(live), r.choice((1e3, 2e4, 1e5))))
+        elif k < 0.5 and len(live) > 4:
+            b = r.choice(live)
+            ops.append(_op(REMOVE, b))
+            live.remove(b)
+        elif k < 0.55:
+            ops.append(_op(INIT))
+        elif k < 0.6:
+            ops.append(_op(COPY))
+        ops.append(_op(TICK))
     return ops
 
 

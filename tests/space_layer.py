@@ -109,8 +109,9 @@ class HostPark:
 class HostLayer:
     """The layer's state as numpy arrays (VecSpace's tensors, the same shapes), run by the host build."""
 
-    def __init__(self, W: int, n: int, boxes: int | None = None, seeds=None, events: int = 4096):
-        self.W, self.N, self.M = W, n, events
+    def __init__(self, W: int, n: int, boxes: int | None = None, seeds=None, events: int | None = None):
+        self.W, self.N = W, n
+        self.M = n * (n + 2) if events is None else events     # a tick's most: every pair entering, each range
         self.B, self.D, self.E, self.S = (boxes or 16 * n + 64), 8 * n + 16, 4 * n + 8, 2 * n + 8
         self.rows = np.array([[w * n + j for w in range(W)] for j in range(n)], dtype=np.int64)
         z = lambda *shape, dt=np.int64: np.zeros(shape, dtype=dt)   # noqa: E731
@@ -320,7 +321,7 @@ def drive(streams: list, kernel: str = "host", device=None) -> tuple:
         from exact_ballpark_b200.modes import VecModesPark
         from exact_ballpark_b200.space import VecSpace
         dpark = VecModesPark(W * N, friction=FRICTION, tick_interval_ms=1000, device=device or "cuda")
-        layer = VecSpace(dpark, np.arange(W * N, dtype=np.int64).reshape(W, N), events=4096, seed=seeds)
+        layer = VecSpace(dpark, np.arange(W * N, dtype=np.int64).reshape(W, N), events=N * (N + 2), seed=seeds)
 
         def run(code, a, b, f):
             for name in ("pos", "vel", "old_pos", "old_vel", "mass", "time_factor", "radius", "max_vel", "agility",
@@ -369,7 +370,7 @@ def drive_ticks(ops, device="cuda", seed: int = 1) -> list:
     from exact_ballpark_b200.space import OP, VecSpace
     n = int(np.max(np.asarray(ops)[:, 1]))
     park = VecModesPark(n, friction=FRICTION, tick_interval_ms=1000, device=device)
-    layer = VecSpace(park, np.arange(n, dtype=np.int64).reshape(1, n), events=4096, seed=seed)
+    layer = VecSpace(park, np.arange(n, dtype=np.int64).reshape(1, n), events=n * (n + 2), seed=seed)
     out = []
     dev = park.dev
     for op in ops:

@@ -83,6 +83,22 @@ def test_a_full_box_table_flags_the_world_and_leaves_it_alone():
     assert all((layer.st[n] == frozen[n]).all() for n in frozen)                # nothing ran after the flag
 
 
+def _crowd():
+    return sp.load(sp.GOLDEN / "space_crowd")
+
+
+def test_the_layers_tick_matches_the_oracle_in_crowded_sensing_worlds_on_the_cpu():
+    """16 to 128 sensing ships a world: the sensors' lists and the proximity map past every growth of the rehash
+    policy, thousands of DoProximity events a world; the layer's host build around the flight oracle's tick."""
+    bad = []
+    for sc in _crowd():
+        got = sl.drive_ticks_host(sc["ops"], sc["rand_seed"])
+        want = _oracle_texts(sc)
+        if got != want:
+            bad.append((sc["seed"], next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
+    assert not bad, f"{len(bad)} worlds differ, first {bad[:3]}"
+
+
 @pytest.mark.parametrize("family", ["tick", "modes"])
 def test_the_layers_tick_matches_the_oracle_on_the_cpu(family):
     """The ticking and the mode streams (GOTO and STOP ships; FollowBall, Orbit and WarpTo with drop-outs, releases
@@ -128,6 +144,20 @@ def test_the_layers_tick_over_the_flight_park_matches_the_oracle(family):
     assert len(scs) == 40
     bad = []
     for sc in scs:
+        got = sl.drive_ticks(sc["ops"], seed=sc["rand_seed"])
+        want = _oracle_texts(sc)
+        if got != want:
+            bad.append((sc["seed"], next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
+    assert not bad, f"{len(bad)} worlds differ, first {bad[:3]}"
+
+
+@pytest.mark.gpu
+def test_the_layers_tick_matches_the_oracle_in_crowded_sensing_worlds():
+    """The crowded worlds (16 to 128 sensing ships) through VecSpace.tick over a VecModesPark on the device."""
+    import torch
+    assert torch.cuda.is_available()
+    bad = []
+    for sc in _crowd():
         got = sl.drive_ticks(sc["ops"], seed=sc["rand_seed"])
         want = _oracle_texts(sc)
         if got != want:

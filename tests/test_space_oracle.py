@@ -99,3 +99,19 @@ def test_collisions_inside_the_tick_change_the_worlds():
         got = np.array([sp.digest(t) for t in space_world.run(ops, seed=sc["rand_seed"])], dtype=np.uint64)
         changed += not (got == sc["digests"]).all()
     assert changed >= 8
+
+
+def test_the_oracle_matches_the_reference_in_crowded_sensing_worlds():
+    """Worlds of 16 to 128 sensing ships (config 3's shape at a golden's size): each sensor's list and the proximity
+    map grow past 13, 29, 59 and 127 keys, so the unordered maps' order follows the rehash policy's growths (13, 29,
+    59, 127 and 257 buckets), every state and every tick's events digested against the reference's."""
+    scs = sp.load(sp.GOLDEN / "space_crowd")
+    assert len(scs) == 8
+    longest = 0
+    for sc in scs:
+        texts = space_world.run(sc["ops"], seed=sc["rand_seed"])
+        got = np.array([sp.digest(t) for t in texts], dtype=np.uint64)
+        assert (got == sc["digests"]).all(), (sc["seed"], int(np.nonzero(got != sc["digests"])[0][0]))
+        longest = max([longest] + [len(line.split()) - 8 for t in texts for line in t.splitlines()
+                                   if line.startswith("S ")])
+    assert longest == 127                                  # a list past 59 keys: 127 buckets, then 257
