@@ -86,6 +86,11 @@ class SpaceState(ctypes.Structure):
                 + [(k, ctypes.c_void_p) for k in SPACE_SENSOR_FIELDS])
 
 
+class SpaceQuery(ctypes.Structure):
+    """include/ebb.h's EbbSpaceQuery, field for field."""
+    _fields_ = [("kind", ctypes.c_int64)] + [(k, ctypes.c_void_p) for k in ("a", "b", "f", "out", "outd")]
+
+
 class SpaceTape(ctypes.Structure):
     """include/ebb.h's EbbSpaceTape, field for field."""
     _fields_ = [("K", ctypes.c_int64), ("code", ctypes.c_void_p), ("a", ctypes.c_void_p), ("b", ctypes.c_void_p),
@@ -121,6 +126,8 @@ def lib() -> ctypes.CDLL:
     L.ebb_composed_tick.argtypes = [ctypes.POINTER(ComposedState), p, i64, p, p, i32]
     L.ebb_composed_file.argtypes = [ctypes.POINTER(ComposedState), p, p, p, p, p]
     L.ebb_server_tick.argtypes = [ctypes.POINTER(ServerState), ctypes.POINTER(ServerQueue), i32, i64, i64, p, i32]
+    L.ebb_space_query.argtypes = [ctypes.POINTER(FlightState), ctypes.POINTER(SpaceState), ctypes.POINTER(SpaceQuery),
+                                  p, i32]
     L.ebb_space_tape.argtypes = [ctypes.POINTER(FlightState), ctypes.POINTER(SpaceState), ctypes.POINTER(SpaceTape), p,
                                  i32]
     L.ebb_glibc_srand.argtypes = [p, i64, p, p]

@@ -38,18 +38,37 @@ def _stale(target: Path, deps) -> bool:
 
 
 def build_native(force: bool = False, verbose: bool = False) -> Path:
+    """Each source compiled to an object in parallel (no device code crosses files), then linked into the library."""
+    from concurrent.futures import ThreadPoolExecutor
     deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "ebb.h"]
     if not force and not _stale(LIB, deps):
         return LIB
+    objdir = HERE / "_build"
+    objdir.mkdir(exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+
+    def compile_one(src: str):
+        obj = objdir / (src + ".o")
+        r = subprocess.run([nvcc()] + compile_flags + ["-c", "-o", str(obj), str(CSRC / src)], capture_output=True,
+                           text=True)
+        return src, obj, r
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    report = []
+    for src, obj, r in results:
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src} ({r.returncode}):\n{r.stderr[-4000:]}")
+        report.append(r.stderr)
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", str(tmp)] + [str(CSRC / s) for s in SOURCES]
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    r = subprocess.run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(tmp)]
+                       + [str(obj) for _, obj, _ in results], capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({r.returncode}):\n{r.stderr[-4000:]}")
-    (HERE / "ptxas.txt").write_text(r.stderr)
+        raise RuntimeError(f"nvcc link failed ({r.returncode}):\n{r.stderr[-4000:]}")
+    (HERE / "ptxas.txt").write_text("".join(report))
     tmp.replace(LIB)
     if verbose:
-        print(r.stderr)
+        print("".join(report))
     return LIB
 
 

@@ -15,18 +15,27 @@ __global__ void __launch_bounds__(128) tape_kernel(const EbbFlightState p, const
     run_tape(&p, &s, &t, w);
 }
 
+__global__ void __launch_bounds__(128) query_kernel(const EbbFlightState p, const EbbSpaceState s, const EbbSpaceQuery q) {
+    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= s.worlds) return;
+    run_query(&p, &s, &q, w);
+}
+
 }  // namespace space
 }  // namespace ebb
 
 extern "C" {
 
-int ebb_space_tape(const EbbFlightState* park, const EbbSpaceState* s, const EbbSpaceTape* t, void* stream, int block) {
-    if (park == nullptr || s == nullptr || t == nullptr || block <= 0 || block > 128 || block % 32 != 0)
-        return EBB_EINVAL;
+// the sizes and the block (checked first: a call with no worlds then does nothing), then every buffer
+static int space_sizes(const EbbFlightState* park, const EbbSpaceState* s, int block) {
+    if (park == nullptr || s == nullptr || block <= 0 || block > 128 || block % 32 != 0) return EBB_EINVAL;
     if (s->slots < 1 || s->slots > EBB_SPACE_MAX_SLOTS || s->boxes < 1 || s->dicts < 1 || s->entries < 1 ||
-        s->sets < 1 || t->K < 0)
+        s->sets < 1)
         return EBB_EINVAL;
-    if (s->worlds <= 0 || t->K == 0) return 0;
+    return 0;
+}
+
+static int space_buffers(const EbbFlightState* park, const EbbSpaceState* s) {
     if (s->rows == nullptr || s->level == nullptr || s->key == nullptr || s->mod == nullptr || s->active == nullptr ||
         s->bubble == nullptr || s->old_bubble == nullptr || s->seq == nullptr || s->in_park == nullptr ||
         s->keep_alive == nullptr || s->dead == nullptr || s->dropped == nullptr || s->box_level == nullptr ||
@@ -37,7 +46,7 @@ int ebb_space_tape(const EbbFlightState* park, const EbbSpaceState* s, const Ebb
         s->dict_n == nullptr || s->entry_bubble == nullptr || s->entry_id == nullptr || s->entry_value == nullptr ||
         s->entry_n == nullptr || s->inter_bubble == nullptr || s->inter_id == nullptr || s->inter_n == nullptr ||
         s->keep_bubble == nullptr || s->keep_id == nullptr || s->keep_n == nullptr || s->bubble_id == nullptr ||
-        s->seq_next == nullptr || s->flags == nullptr || t->code == nullptr || t->a == nullptr || t->b == nullptr)
+        s->seq_next == nullptr || s->flags == nullptr)
         return EBB_EINVAL;
     if (s->umap_cap < 1 || s->umap_cap > EBB_SPACE_MAX_SLOTS || s->events < 0 || s->srange == nullptr ||
         s->speriod == nullptr || s->selapsed == nullptr || s->ntf_range == nullptr || s->trk_range == nullptr ||
@@ -52,8 +61,35 @@ int ebb_space_tape(const EbbFlightState* park, const EbbSpaceState* s, const Ebb
         park->free_ == nullptr || park->interactive == nullptr || park->mode == nullptr || park->goto_pt == nullptr ||
         park->follow_ptr == nullptr || park->follow_range == nullptr || park->massive == nullptr || park->sensor == nullptr)
         return EBB_EINVAL;
+    return 0;
+}
+
+int ebb_space_tape(const EbbFlightState* park, const EbbSpaceState* s, const EbbSpaceTape* t, void* stream, int block) {
+    if (t == nullptr || t->K < 0) return EBB_EINVAL;
+    int rc = space_sizes(park, s, block);
+    if (rc) return rc;
+    if (s->worlds <= 0 || t->K == 0) return 0;
+    rc = space_buffers(park, s);
+    if (rc) return rc;
+    if (t->code == nullptr || t->a == nullptr || t->b == nullptr) return EBB_EINVAL;
     const unsigned grid = (unsigned)((s->worlds + block - 1) / block);
     ebb::space::tape_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(*park, *s, *t);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
+int ebb_space_query(const EbbFlightState* park, const EbbSpaceState* s, const EbbSpaceQuery* q, void* stream,
+                    int block) {
+    if (q == nullptr || q->kind < EBB_SPACE_Q_VISIBILITY || q->kind > EBB_SPACE_Q_NEARBY) return EBB_EINVAL;
+    int rc = space_sizes(park, s, block);
+    if (rc) return rc;
+    if (s->worlds <= 0) return 0;
+    rc = space_buffers(park, s);
+    if (rc) return rc;
+    if (q->a == nullptr || q->b == nullptr || q->f == nullptr || q->out == nullptr || q->outd == nullptr)
+        return EBB_EINVAL;
+    const unsigned grid = (unsigned)((s->worlds + block - 1) / block);
+    ebb::space::query_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(*park, *s, *q);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : (int)e;
 }

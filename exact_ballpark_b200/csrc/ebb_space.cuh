@@ -179,7 +179,7 @@ struct World {
         return e;
     }
     // GetBox: the box, made with its missing ancestors when missing (a parent's key is its child's over 4)
-    EBB_HD int64_t get_box(int64_t ix, int64_t iy, int64_t iz, int level) {
+    EBB_HDNI int64_t get_box(int64_t ix, int64_t iy, int64_t iz, int level) {
         if (edge(ix, iy, iz, level)) return -1;
         const int64_t found = box_find(level, ix, iy, iz);
         if (found >= 0) return found;
@@ -203,7 +203,7 @@ struct World {
     // Release of an empty box, then of each ancestor it leaves empty: every box of the chain kept while BoxAllocator
     // held fewer than 256 when the chain began, else deleted. `watch` records the fate of two boxes the caller reads
     // afterwards (0 live, 1 released and kept, 2 released and deleted).
-    EBB_HD void release(int64_t e, const int64_t* watch, int* fate) {
+    EBB_HDNI void release(int64_t e, const int64_t* watch, int* fate) {
         const bool keep = one(s->free_boxes) < BOX_KEEP;
         int64_t cur = e;
         for (int guard = 0; guard < NUM_LEVELS && cur >= 0; ++guard) {
@@ -277,7 +277,7 @@ struct World {
         for (int c = 0; c < 3; ++c) mod(j, c) = -2;
     }
     // DeleteFromBoxes: the ball leaves each of its boxes in key order, each box released when left empty
-    EBB_HD void delete_from_boxes(int64_t j, const int64_t* watch, int* fate) {
+    EBB_HDNI void delete_from_boxes(int64_t j, const int64_t* watch, int* fate) {
         int64_t boxes[27];
         const int n = ball_boxes(j, boxes);
         for (int i = 0; i < n; ++i) {
@@ -409,7 +409,7 @@ struct World {
     }
     // AddToBubble: the ball entered (+1, or 0 again after leaving) its bubble's dictionary and left (-1, or gone if it
     // had only entered) its old one's; its interactive and keep-alive memberships follow
-    EBB_HD void add_to_bubble(int64_t j) {
+    EBB_HDNI void add_to_bubble(int64_t j) {
         const int64_t bid = id(j), bub = I(s->bubble, j), old = I(s->old_bubble, j);
         if (bub != -1) {
             if (dict_index(bub) < 0) {
@@ -468,7 +468,7 @@ struct World {
     }
     // Ball::InsertInBoxes: the ball's box at the level of its inflated radius and the neighbours its sphere reaches
     // (every neighbour for a huge ball), unless box and sides are as they were; the top box takes the bubble
-    EBB_HD void ball_insert_in_boxes(int64_t j, const double* x, const double* v, int level0, const int64_t* key0,
+    EBB_HDNI void ball_insert_in_boxes(int64_t j, const double* x, const double* v, int level0, const int64_t* key0,
                                      int fate_box1, int64_t new_bubble) {
         if (fate_box1 == 2) flag(F_UNDEFINED);             // a deleted box's memory read
         const double inflated = inflated_radius(j, v);
@@ -532,7 +532,7 @@ struct World {
     }
     // Ballpark::InsertInBoxes on the master: the ball's new top box, its bubble or, for a top without one, a
     // neighbour's or a new id; AddToBubble when the ball's bubble changes; then its filing
-    EBB_HD void insert_in_boxes(int64_t j, const double* x, const double* v) {
+    EBB_HDNI void insert_in_boxes(int64_t j, const double* x, const double* v) {
         const double inflated = inflated_radius(j, v);
         const int level0 = level_for(inflated);
         int64_t k[3];
@@ -590,7 +590,7 @@ struct World {
     // the ancestor's distance or the box's post-order code (path digits below b's level, 64 past o's level).
     // Relatedness factors over the axes: the finer filing's key range, shifted to the coarser level, meets the
     // coarser's.
-    EBB_HD int64_t walk_key(int64_t b, int64_t o) const {
+    EBB_HDNI int64_t walk_key(int64_t b, int64_t o) const {
         const int64_t Lb = lvl(b), Ln = lvl(o);
         int64_t lo_b[3], hi_b[3], lo_n[3], hi_n[3], cb[3];
         for (int q = 0; q < 3; ++q) {
@@ -651,7 +651,7 @@ struct World {
     }
     // GetNearbyBalls from slot b (no missiles, fields or global balls here): the balls filed in related boxes that
     // pass the filter, in the walk's order (its key, then id), into out; returns their count
-    EBB_HD int nearby(int64_t b, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked, uint8_t* out) const {
+    EBB_HDNI int nearby(int64_t b, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked, uint8_t* out) const {
         const int64_t bub = I(s->bubble, b);
         if (exclude_inert && !set_any(0, bub)) return 0;
         if (lvl(b) < 0) return 0;
@@ -720,7 +720,7 @@ struct World {
     }
     // insert(): an absent key linked; before it, a fresh map takes 13 buckets and a key past the bucket count grows
     // the table, every key re-linked in its old order. A map past umap_cap keys flags the world.
-    EBB_HD bool umap_insert(const UMap& m, int64_t slot, int64_t flag_bit) const {
+    EBB_HDNI bool umap_insert(const UMap& m, int64_t slot, int64_t flag_bit) const {
         if (umap_find(m, slot) >= 0) return false;
         const int32_t n = *m.len;
         if (n >= s->umap_cap) {
@@ -898,7 +898,7 @@ struct World {
     // CheckForProximity_Sensor (Ball.cpp:642; SEN-701, SEN-702): every period, GetNearbyBalls with the sensor's
     // radius inflated and the velocity zeroed (the ball re-filed for it and back), the balls no longer near first (in
     // the list's order), then each candidate in the walk's order entering or leaving (the inside test in float sums)
-    EBB_HD void check_sensor(int64_t j) {
+    EBB_HDNI void check_sensor(int64_t j) {
         at(s->selapsed, j) = dadd(at(s->selapsed, j), p->dt);
         if (at(s->selapsed, j) < at(s->speriod, j)) return;
         at(s->selapsed, j) = 0.0;
@@ -958,7 +958,7 @@ struct World {
     }
     // Ballpark::HandleProximities (Ballpark.cpp:5822): every proximity ball in the map's order (a copy of it); a ball
     // in a dead bubble gets one forced check when its sensor holds balls, and its list is emptied (TIME-714)
-    EBB_HD void handle_proximities() {
+    EBB_HDNI void handle_proximities() {
         const UMap pm = proximity_map();
         const int32_t n = *pm.len;
         uint8_t keys[EBB_SPACE_MAX_SLOTS];
@@ -976,6 +976,114 @@ struct World {
             }
             if (!at(s->has_prox, j)) continue;
             check_for_proximity(j);
+        }
+    }
+
+    // ---- the queries (space.py:1524-1600: CheckVisibility, GetBallIdsInRange, GetBubbleAtCoordinates) ----
+    // the slot of a ball of the world by id, -1 for none
+    EBB_HD int64_t slot_of(int64_t bid) const {
+        for (int64_t j = 0; j < N; ++j)
+            if (slot_ok(j) && U(s->in_park, j) && id(j) == bid) return j;
+        return -1;
+    }
+    // Ballpark::CheckVisibility (Ballpark.cpp:5299; SEN-709): -2 between bubbles (or a ball missing); else the first
+    // massive, uncloaked ball of the bubble, in the ball dictionary's order, whose sphere the segment enters; else 0
+    EBB_HDNI int64_t visibility(int64_t src, int64_t dst) const {
+        if (!slot_ok(src) || !slot_ok(dst) || !U(s->in_park, src) || !U(s->in_park, dst)) return -2;
+        if (I(s->bubble, src) != I(s->bubble, dst)) return -2;
+        const double x0[3] = {pos(src, 0), pos(src, 1), pos(src, 2)};
+        double ray[3] = {dsub(pos(dst, 0), x0[0]), dsub(pos(dst, 1), x0[1]), dsub(pos(dst, 2), x0[2])};
+        const double len2 = dadd(dadd(dmul(ray[0], ray[0]), dmul(ray[1], ray[1])), dmul(ray[2], ray[2]));
+        const double distance = dsqrt(len2), norm = dsqrt(len2);
+        if (norm != 0.0) {
+            const double inv = ddiv(1.0, norm);
+            for (int c = 0; c < 3; ++c) ray[c] = dmul(ray[c], inv);
+        }
+        int64_t last = -1;
+        for (int64_t t = 0; t < N; ++t) {                  // the balls in the order they were added
+            int64_t o = -1;
+            for (int64_t i = 0; i < N; ++i)
+                if (U(s->in_park, i) && slot_ok(i) && I(s->seq, i) > last && (o < 0 || I(s->seq, i) < I(s->seq, o)))
+                    o = i;
+            if (o < 0) break;
+            last = I(s->seq, o);
+            const int64_t r = row(o);
+            if (I(s->bubble, o) != I(s->bubble, src) || o == src || o == dst || !p->massive[r] ||
+                at(s->cloaked, o) != 0)
+                continue;
+            const double tc[3] = {dsub(pos(o, 0), x0[0]), dsub(pos(o, 1), x0[1]), dsub(pos(o, 2), x0[2])};
+            const double v = dadd(dadd(dmul(ray[0], tc[0]), dmul(ray[1], tc[1])), dmul(ray[2], tc[2]));
+            const double rad = (double)p->radius[r];
+            const double tt = dadd(dadd(dmul(tc[0], tc[0]), dmul(tc[1], tc[1])), dmul(tc[2], tc[2]));
+            const double dsq = dsub(dmul(rad, rad), dsub(tt, dmul(v, v)));
+            if (dsq < 0.0) continue;
+            const double d = dsqrt(dsq);
+            const double near = dsub(v, d);
+            if (near > 0.0 && near < distance) return id(o);
+        }
+        return 0;
+    }
+    // GetBubbleAtCoordinates: the bubble of the existing top box holding the point, -2 for none
+    EBB_HD int64_t bubble_at(const double* x) const {
+        int64_t k[3];
+        key_for(0, x, k);
+        const int64_t e = check_box(k[0], k[1], k[2], 0);
+        return e < 0 ? -2 : I(s->box_bubble, e);
+    }
+    // GetBallIdsInRange (with distances): the balls listed in the bubble's dictionary, in its order (those that left
+    // it included until CopyBubbles), within range + radius of the centre; the reference ball itself left out
+    EBB_HDNI int64_t in_range(int64_t ref, const double* c, int64_t bub, double range, bool cloaked, int64_t* out,
+                            double* outd) const {
+        if (bub == -1 || dict_index(bub) < 0) return 0;
+        int64_t n = 0;
+        const int64_t en = one(s->entry_n);
+        for (int64_t e = 0; e < en; ++e) {
+            if (I(s->entry_bubble, e) != bub) continue;
+            const int64_t o = slot_of(I(s->entry_id, e));
+            if (o < 0 || o == ref) continue;
+            if (at(s->cloaked, o) != 0 && !cloaked) continue;
+            const double d2 = dist2(o, c);
+            const double lim = dadd(range, (double)p->radius[row(o)]);
+            if (d2 <= dmul(lim, lim)) {
+                out[n * W + w] = id(o);
+                outd[n * W + w] = d2;
+                ++n;
+            }
+        }
+        return n;
+    }
+    // One query of the world (EbbSpaceQuery): its answer in out[0][w], the balls' ids in out[1 + i][w], their
+    // squared distances in outd[i][w]
+    EBB_HD void query(int64_t kind, int64_t a, int64_t b, const double* f, int64_t* out, double* outd) {
+        int64_t* ids = out + W;
+        switch (kind) {
+            case EBB_SPACE_Q_VISIBILITY: out[w] = visibility(a, b); break;
+            case EBB_SPACE_Q_RANGE_BALL:
+                if (!slot_ok(a) || !U(s->in_park, a)) {
+                    out[w] = -1;
+                } else {
+                    const double c[3] = {pos(a, 0), pos(a, 1), pos(a, 2)};
+                    out[w] = in_range(a, c, I(s->bubble, a), f[0], (b & 1) != 0, ids, outd);
+                }
+                break;
+            case EBB_SPACE_Q_RANGE_POINT: {
+                const int64_t top = bubble_at(f);
+                out[w] = in_range(-1, f, top == -2 ? -1 : top, f[3], (b & 1) != 0, ids, outd);
+                break;
+            }
+            case EBB_SPACE_Q_BUBBLE_AT: out[w] = bubble_at(f); break;
+            case EBB_SPACE_Q_NEARBY: {
+                if (!slot_ok(a) || !U(s->in_park, a)) {
+                    out[w] = 0;
+                    break;
+                }
+                uint8_t cand[EBB_SPACE_MAX_SLOTS];
+                const int n = nearby(a, (b & 1) != 0, (b & 2) != 0, (b & 4) != 0, cand);
+                for (int i = 0; i < n; ++i) ids[(int64_t)i * W + w] = id(cand[i]);
+                out[w] = n;
+                break;
+            }
+            default: flag(F_BAD_OP); break;
         }
     }
 
@@ -1015,7 +1123,7 @@ struct World {
     }
     // InitializeBubbles: every top box's bubble cleared, the dictionaries and sets emptied, then each ball's top
     // given its bubble (a fill from the first ball to reach it) in the ball dictionary's order
-    EBB_HD void init_bubbles() {
+    EBB_HDNI void init_bubbles() {
         const int64_t n = one(s->box_n);
         for (int64_t e = 0; e < n; ++e)
             if (I(s->box_level, e) == 0) I(s->box_bubble, e) = -1;
@@ -1082,7 +1190,7 @@ struct World {
     }
     // after the park's tick, in ascending id: each warp drop-out nearly at rest re-filed at its drop-out point (the old
     // state), then each ball that moved at least sqrt(0.1) m
-    EBB_HD void after_evolve() {
+    EBB_HDNI void after_evolve() {
         int64_t order[EBB_SPACE_MAX_SLOTS];
         int64_t n = 0;
         for (int64_t j = 0; j < N; ++j)
@@ -1135,6 +1243,16 @@ struct World {
         }
     }
 };
+
+// world w's query (its state read, nothing written but the answer; a flagged world answers nothing)
+EBB_HD void run_query(const EbbFlightState* p, const EbbSpaceState* s, const EbbSpaceQuery* q, int64_t w) {
+    World wd{p, s, w, s->worlds, s->slots, s->boxes};
+    q->out[w] = 0;
+    if (s->flags[w] & (F_EDGE | F_BOXES | F_DICTS | F_ENTRIES | F_SETS | F_BAD_OP)) return;
+    double f[5];
+    for (int c = 0; c < 5; ++c) f[c] = q->f[c * s->worlds + w];
+    wd.query(q->kind, q->a[w], q->b[w], f, q->out, q->outd);
+}
 
 // world w's K operations of the tape, in order (a flagged world is left alone)
 EBB_HD void run_tape(const EbbFlightState* p, const EbbSpaceState* s, const EbbSpaceTape* t, int64_t w) {

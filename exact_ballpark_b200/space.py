@@ -32,6 +32,8 @@ OPS = ("NONE", "ADD", "REFILE", "INIT_BUBBLES", "COPY_BUBBLES", "KEEP_ALIVE", "S
 OP = {name: k for k, name in enumerate(OPS)}
 OP.update(HANDLE_PROXIMITIES=18, SET_CLOAKED=19)            # this build's own (no number in the reference's OPS)
 EVENTS = ("", "DoProximity", "DoRange", "DoTargetTracking")
+QUERIES = ("NONE", "VISIBILITY", "RANGE_BALL", "RANGE_POINT", "BUBBLE_AT", "NEARBY")
+Q = {name: k for k, name in enumerate(QUERIES)}
 FLAGS = ("EVENTS", "TOPS", "EDGE", "BOXES", "DICTS", "ENTRIES", "PROXIMITY", "SENSOR_LIST", "HUGE", "BAD_OP", "SETS",
          "UNDEFINED")
 FLAG = {name: 1 << k for k, name in enumerate(FLAGS)}
@@ -152,6 +154,27 @@ class VecSpace:
                 for c, x in enumerate(op[3] if len(op) > 3 else ()):
                     f[w, k, c] = float(x)
         self.tape(code, a, b, f)
+
+    def query(self, kind: str, a=None, b=None, f=None) -> tuple:
+        """One query a world (the reference's VecSpace.query, vec_space.py:938): kind in QUERIES (NEARBY, GetNearbyBalls,
+        is this build's own), a [W] (a slot), b [W] (a slot or flags), f [W, <=5]. Returns (out [W, 1 + N] int64: the
+        answer, then the balls' ids; outd [W, N]: their squared distances). No host synchronisation."""
+        W, N, d = self.W, self.N, self.dev
+        a = torch.full((W,), -1, dtype=I64, device=d) if a is None else torch.as_tensor(a, dtype=I64).to(d).reshape(W)
+        b = torch.zeros(W, dtype=I64, device=d) if b is None else torch.as_tensor(b, dtype=I64).to(d).reshape(W)
+        ff = torch.zeros(5, W, dtype=torch.float64, device=d)
+        if f is not None:
+            f = torch.as_tensor(f, dtype=torch.float64).to(d).reshape(W, -1)
+            ff[:f.shape[1]] = f.t()
+        a, b = a.contiguous(), b.contiguous()
+        out = torch.zeros(1 + N, W, dtype=I64, device=d)
+        outd = torch.zeros(N, W, dtype=torch.float64, device=d)
+        q = _native.SpaceQuery(Q[kind], a.data_ptr(), b.data_ptr(), ff.data_ptr(), out.data_ptr(), outd.data_ptr())
+        rc = _native.lib().ebb_space_query(ctypes.byref(self.park.state()), ctypes.byref(self.state()), ctypes.byref(q),
+                                           self.park._stream(), self.block)
+        _native.check(rc, "ebb_space_query")
+        self._keep_query = (a, b, ff)
+        return out.t(), outd.t()
 
     def broadcast(self, name: str, mask: torch.Tensor | None = None) -> None:
         """One operation without arguments for every world (or the worlds in mask [W]), on the device."""

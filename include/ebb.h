@@ -232,6 +232,23 @@ typedef struct EbbSpaceTape {
     const int64_t *code, *a, *b;
     const double* f;
 } EbbSpaceTape;
+/* One query a world over the layer's state (the reference's QUERIES, vec_space.py:160, and its xbps_query_*): kind,
+ * a [W] (a slot), b [W] (a slot or flags), f [5][W]; out [1 + N][W]: out[0] the answer (VISIBILITY: the occluding
+ * ball's id, 0 none, -2 between bubbles; RANGE_BALL, RANGE_POINT, NEARBY: the count of balls, -1 when the reference
+ * ball is none of the world's; BUBBLE_AT: the bubble, -2 for no top box), out[1 + i] the balls' ids in order; outd
+ * [N][W] their squared distances (RANGE_*). VISIBILITY: a source, b destination (-1: not a ball); RANGE_BALL: a the
+ * ball, f[0] the range, b bit 0 cloaked balls too; RANGE_POINT: f[0..2] the point, f[3] the range, b as RANGE_BALL;
+ * BUBBLE_AT: f[0..2]; NEARBY (GetNearbyBalls): a the ball, b bit 0 exclude fixed, bit 1 exclude inert, bit 2 exclude
+ * cloaked. */
+enum { EBB_SPACE_Q_VISIBILITY = 1, EBB_SPACE_Q_RANGE_BALL = 2, EBB_SPACE_Q_RANGE_POINT = 3, EBB_SPACE_Q_BUBBLE_AT = 4,
+       EBB_SPACE_Q_NEARBY = 5 };
+typedef struct EbbSpaceQuery {
+    int64_t kind;
+    const int64_t *a, *b;
+    const double* f;
+    int64_t* out;
+    double* outd;
+} EbbSpaceQuery;
 
 /* The ABI version (EBB_ABI_VERSION). Replaces xbpm_abi / xbpo_abi (exact_ballpark/vec_modes_cuda.cu:750,
  * vec_orient_cuda.cu:499). */
@@ -390,9 +407,15 @@ int ebb_flight_decay(const EbbFlightState* s, const uint8_t* mask, double neg_kd
  * vec_orient_cuda.cu:520). */
 int ebb_libm(int func, int64_t n, const double* x, const double* y, double* out, void* stream, int block);
 
-/* The tape's operations on every world, one thread a world, on `stream` (the park's rows are read and, by
- * SET_INTERACTIVE, written). Replaces xbps_tape_cuda (exact_ballpark/vec_space.py:896). */
+/* The tape's operations on every world, one thread a world, on `stream` (the park's rows are read and written: the
+ * interactive and sensor flags, and a sensor check's radius, put back after it). Replaces xbps_tape_cuda
+ * (exact_ballpark/vec_space.py:896). */
 int ebb_space_tape(const EbbFlightState* park, const EbbSpaceState* s, const EbbSpaceTape* t, void* stream, int block);
+
+/* One query a world (EbbSpaceQuery), one thread a world, on `stream`; nothing but the answer written. Replaces
+ * xbps_query_cuda (exact_ballpark/vec_space.py:938). */
+int ebb_space_query(const EbbFlightState* park, const EbbSpaceState* s, const EbbSpaceQuery* q, void* stream,
+                    int block);
 
 /* A kernel's resources as loaded on the current device: which 0 the plain tick, 1 the prepass, 2 the tiled tick,
  * 3 the listed-worlds tick, 4 the row move, 7 the combat tick, 8 the composed tick.

@@ -8,3 +8,8 @@ extern "C" int space_tape_host(const EbbFlightState* p, const EbbSpaceState* s, 
     for (int64_t w = 0; w < s->worlds; ++w) ebb::space::run_tape(p, s, t, w);
     return 0;
 }
+
+extern "C" int space_query_host(const EbbFlightState* p, const EbbSpaceState* s, const EbbSpaceQuery* q) {
+    for (int64_t w = 0; w < s->worlds; ++w) ebb::space::run_query(p, s, q, w);
+    return 0;
+}

@@ -44,6 +44,8 @@ def host_lib() -> ctypes.CDLL:
     L = ctypes.CDLL(str(HOST_LIB))
     L.space_tape_host.argtypes = [ctypes.POINTER(_native.FlightState), ctypes.POINTER(_native.SpaceState),
                                   ctypes.POINTER(_native.SpaceTape)]
+    L.space_query_host.argtypes = [ctypes.POINTER(_native.FlightState), ctypes.POINTER(_native.SpaceState),
+                                   ctypes.POINTER(_native.SpaceQuery)]
     _host = L
     return L
 
@@ -137,6 +139,24 @@ class HostLayer:
             "pbkt": z(W, dt=np.int32) + 1, "ev": z(self.M, W, dt=np.int32), "evn": z(W),
             "rnd": np.stack([srand(seed) for seed in (seeds if seeds is not None else [1] * W)])}
 
+    def query(self, park: HostPark, kind: int, a, b, f) -> tuple:
+        """One query a world on the host build: (out [1 + N][W], outd [N][W])."""
+        from exact_ballpark_b200 import _native
+        s = _native.SpaceState()
+        s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets = self.W, self.N, self.B, self.D, self.E, self.S
+        s.umap_cap, s.events = self.N, self.M
+        s.rows = self.rows.ctypes.data
+        for name, arr in self.st.items():
+            setattr(s, name, arr.ctypes.data)
+        a, b = (np.ascontiguousarray(np.asarray(x, dtype=np.int64).reshape(self.W)) for x in (a, b))
+        f = np.ascontiguousarray(np.asarray(f, dtype=np.float64).reshape(5, self.W))
+        out = np.zeros((1 + self.N, self.W), dtype=np.int64)
+        outd = np.zeros((self.N, self.W))
+        q = _native.SpaceQuery(kind, a.ctypes.data, b.ctypes.data, f.ctypes.data, out.ctypes.data, outd.ctypes.data)
+        ps = park.struct()
+        host_lib().space_query_host(ctypes.byref(ps), ctypes.byref(s), ctypes.byref(q))
+        return out, outd
+
     def tape(self, park: HostPark, code, a, b, f=None) -> None:
         from exact_ballpark_b200 import _native
         s = _native.SpaceState()
@@ -217,6 +237,48 @@ def translate(park: HostPark, w: int, op, n: int) -> tuple:
     return none                                           # the queries: not the layer's
 
 
+QUERY_OPS = (sp.VISIBILITY, sp.RANGE_BALL, sp.RANGE_POINT, sp.BUBBLE_AT, sp.NEARBY)
+
+
+def query_of(op, n: int) -> tuple:
+    """A golden query operation as the layer's query: (kind, a, b, f[5]); ids outside 1..n are no ball's."""
+    from exact_ballpark_b200.space import Q
+    code, bid = int(op[0]), int(op[1])
+    a = [float(x) for x in op[2:]]
+    slot = lambda i: int(i) - 1 if 1 <= int(i) <= n else -1      # noqa: E731
+    if code == sp.VISIBILITY:
+        return Q["VISIBILITY"], slot(bid), slot(a[0]), [0.0] * 5
+    if code == sp.RANGE_BALL:
+        return Q["RANGE_BALL"], slot(bid), int(bool(a[1])), [a[0], 0.0, 0.0, 0.0, 0.0]
+    if code == sp.RANGE_POINT:
+        return Q["RANGE_POINT"], -1, int(bool(a[4])), [a[0], a[1], a[2], a[3], 0.0]
+    if code == sp.BUBBLE_AT:
+        return Q["BUBBLE_AT"], -1, 0, [a[0], a[1], a[2], 0.0, 0.0]
+    return Q["NEARBY"], slot(bid), int(bool(a[0])) | (2 if a[1] else 0) | (4 if a[2] else 0), [0.0] * 5
+
+
+def answer_text(op, out, outd, w: int) -> str:
+    """The layer's answer to world w's query as the oracle writes it."""
+    code = int(op[0])
+    v = int(out[0, w])
+    if code == sp.VISIBILITY:
+        return f"Q {v}\n"
+    if code == sp.BUBBLE_AT:
+        return "Q None\n" if v == -2 else f"Q {v}\n"
+    if code == sp.RANGE_BALL and v == -1:
+        return "Q None\n"
+    dist = code in (sp.RANGE_BALL, sp.RANGE_POINT) and bool(op[4] if code == sp.RANGE_BALL else op[7])
+    items = []
+    for i in range(max(v, 0)):
+        bid = int(out[1 + i, w])
+        if dist:
+            bits = "%016x" % struct.unpack("<Q", struct.pack("<d", float(outd[i, w])))[0]
+            items.append(f" {bits}:{bid}")
+        else:
+            items.append(f" {bid}")
+    return "Q" + "".join(items) + "\n"
+
+
 def text(st: dict, park_ids, park_mode, w: int, park_sensor=None) -> str:
     """World w's layer state as the oracle's state text (the lines the layer holds)."""
     n = st["level"].shape[0]
@@ -278,7 +340,8 @@ def text(st: dict, park_ids, park_mode, w: int, park_sensor=None) -> str:
 def oracle_lines(t: str, code: int = 0) -> str:
     """The oracle's state text less the lines the layer does not hold (the flight states, the queries' answers):
     the answer kept for HandleProximities and a tick (their events)."""
-    keep = ("B", "L", "F", "P", "S", "U", "I", "K") + (("Q",) if code in (sp.PROXIMITIES, sp.TICK) else ())
+    keep = ("B", "L", "F", "P", "S", "U", "I", "K") + (("Q",) if code in (sp.PROXIMITIES, sp.TICK) + QUERY_OPS
+                                                         else ())
     return "".join(line + "\n" for line in t.splitlines() if line[:1] in keep)
 
 
@@ -316,6 +379,7 @@ def drive(streams: list, kernel: str = "host", device=None) -> tuple:
 
         read = lambda: layer.st                                                     # noqa: E731
         sensor = lambda: park.sensor                                                # noqa: E731
+        ask = lambda kind, a, b, f: layer.query(park, kind, a, b, f)                # noqa: E731
     else:
         import torch
         from exact_ballpark_b200.modes import VecModesPark
@@ -340,6 +404,12 @@ def drive(streams: list, kernel: str = "host", device=None) -> tuple:
 
         read = lambda: {k: v.cpu().numpy() for k, v in layer.st.items()}            # noqa: E731
         sensor = lambda: dpark._sensor.cpu().numpy().astype(np.uint8)                # noqa: E731
+
+        def ask(kind, a, b, f):
+            from exact_ballpark_b200.space import QUERIES
+            out, outd = layer.query(QUERIES[kind], torch.from_numpy(a), torch.from_numpy(b),
+                                    torch.from_numpy(np.ascontiguousarray(f.T)))
+            return out.t().cpu().numpy(), outd.t().cpu().numpy()
     for k in range(K):
         code, a, b = np.zeros(W, np.int64), np.full(W, -1, np.int64), np.zeros(W, np.int64)
         f = np.zeros((W, 4))
@@ -349,11 +419,23 @@ def drive(streams: list, kernel: str = "host", device=None) -> tuple:
         run(code, a, b, f.T.copy() if kernel == "host" else f)
         st = read()
         sens = sensor()
+        answers, asked = {}, {}
+        for w, ops in enumerate(streams):
+            if k < len(ops) and int(ops[k][0]) in QUERY_OPS:
+                asked.setdefault(query_of(ops[k], N)[0], []).append(w)
+        for kind, worlds in asked.items():                # one query launch a kind, every world asking it
+            qa, qb, qf = np.full(W, -1, np.int64), np.zeros(W, np.int64), np.zeros((5, W))
+            for w in worlds:
+                _, qa[w], qb[w], qf[:, w] = query_of(streams[w][k], N)
+            out, outd = ask(kind, qa, qb, qf)
+            for w in worlds:
+                answers[w] = answer_text(streams[w][k], out, outd, w)
         for w, ops in enumerate(streams):
             if k < len(ops):
                 t = text(st, park.ids, park.mode, w, sens)
                 if int(ops[k][0]) == sp.PROXIMITIES:
                     t += events_text(st, park.ids, w, N)
+                t += answers.get(w, "")
                 texts[w].append(t)
     return texts, read()["flags"].copy()
 
@@ -444,6 +526,11 @@ def drive_ticks(ops, device="cuda", seed: int = 1) -> list:
         t = text(st, ids, park._mode.cpu().numpy(), 0, park._sensor.cpu().numpy().astype(np.uint8))
         if code in (sp.TICK, sp.PROXIMITIES):
             t += events_text(st, ids, 0, n)
+        if code in QUERY_OPS:
+            from exact_ballpark_b200.space import QUERIES
+            kind, qa, qb, qf = query_of(op, n)
+            qo, qd = layer.query(QUERIES[kind], [qa], [qb], torch.tensor([qf], dtype=torch.float64))
+            t += answer_text(op, qo.t().cpu().numpy(), qd.t().cpu().numpy(), 0)
         out.append(t)
     return out
 
@@ -559,5 +646,10 @@ def drive_ticks_host(ops, seed: int = 1) -> list:
         t = text(layer.st, op.ids, op.mode, 0, op.sensor.astype(np.uint8))
         if code in (sp.TICK, sp.PROXIMITIES):
             t += events_text(layer.st, op.ids, 0, n)
+        if code in QUERY_OPS:
+            pull()
+            kind, qa, qb, qf = query_of(row, n)
+            qo, qd = layer.query(host, kind, [qa], [qb], np.asarray(qf).reshape(5, 1))
+            t += answer_text(row, qo, qd, 0)
         out.append(t)
     return out
