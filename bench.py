@@ -636,6 +636,112 @@ def space_runs(args, dev) -> dict:
             "flagged_worlds": int((space.st["flags"] != 0).sum()), "boxes_max": int(space.st["box_n"].max())}
 
 
+def partition_setup(pw, dev, ragged: bool, server_on: bool = True) -> dict:
+    """A flight park of the partition worlds with the partition layer (ragged size classes, or the plain 128-slot
+    layout), every ship's sensor added, and the server layer on top (a pilot a ship, GotoDirection and
+    SetSpeedFraction queued for every ship every tick: a fixed schedule of 2 x 128 pushes, a world's pushes masked to
+    its ships). The first tick runs eagerly; returns the parts and the captured tick."""
+    import torch
+
+    from exact_ballpark_b200 import VecModesPark, server
+    from exact_ballpark_b200.modes import tick_plain, tick_tiled
+    from exact_ballpark_b200.partition import PartitionGraph, PartitionLayer
+    park = VecModesPark(pw.n, device=dev)
+    park.load_columns(pw.cols)
+    part = PartitionLayer(park, pw.sizes, ragged=ragged)
+    part.load()
+    part.add_sensors(pw.sensor_range, 1.0)
+    park_tick = (lambda: tick_tiled(park)) if ragged else (lambda: tick_plain(park, park.block))
+    if not ragged:
+        park.scratch()
+    srv = q = None
+    W = len(pw.sizes)
+    if server_on:
+        srv = server.VecServer(server.ModesAdapter(park), (pw.cols["id"] - 1).tolist(), kernel="cuda")
+        srv.pre_tick()                                      # the first tick (its additions) eagerly
+        part.tick(park_tick)
+        park.current_time += 1
+        srv.post_tick()
+        sched = [k for _ in range(128) for k in ("GotoDirection", "SetSpeedFraction")]
+        q = srv._queue([server.CODE[k] for k in sched])
+        sizes = torch.as_tensor(pw.sizes, device=dev)
+        starts = torch.as_tensor(pw.starts, device=dev)
+        direction = torch.as_tensor(pw.direction, device=dev)
+        speed = torch.as_tensor(pw.speed, device=dev)
+        for k in range(128):
+            on = sizes > k
+            row = torch.where(on, starts + k, 0)
+            for j, f in ((2 * k, direction[row]), (2 * k + 1, speed[row][:, None])):
+                q["mask"][j].copy_(on.to(q["mask"].dtype))
+                q["ball"][j].fill_(k + 1)
+                q["f"][j][:, :f.shape[1]].copy_(f)
+    else:
+        part.tick(park_tick)
+        park.current_time += 1
+    g = PartitionGraph(part, park_tick, srv, q)
+    return {"park": park, "part": part, "server": srv, "q": q, "graph": g, "park_tick": park_tick}
+
+
+def partition_runs(args, dev) -> dict:
+    """The metric's workload: the partition worlds (exact_ballpark_b200.workloads.partition_worlds: --partition-worlds
+    ragged worlds of 1 to 128 ships, log-uniform, in 1 to 5 Gaussian blobs, a sensor of 1 to 250 km on every ship)
+    with bubbles, the partition and the proximity sensors, the server layer on top (every ship piloted: GotoDirection
+    and SetSpeedFraction every tick). Two arrangements of the same worlds on the same GPU, each a captured tick
+    replayed --partition-steps times after warm-up, timed with CUDA events (L2 flushed before each step):
+    the ragged batch (the layer in size classes, worlds ordered by size; the park's tiled schedule) and the plain
+    per-configuration kernels (one 128-slot layout in world order; the park's plain schedule). Both end in the same
+    state, compared here bit for bit (the park's rows, each world's event count)."""
+    import torch
+
+    from exact_ballpark_b200.workloads import partition_worlds
+    W, K = args.partition_worlds, args.partition_steps
+    pw = partition_worlds(11, W)
+    n = pw.n
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    runs = {}
+    for name, ragged in (("ragged", True), ("plain", False)):
+        t0 = time.time()
+        r = partition_setup(pw, dev, ragged)
+        setup_s = time.time() - t0
+        g = r["graph"]
+        for _ in range(args.warmup):
+            g.tick()
+        total = 0.0
+        for _ in range(K):
+            flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            g.tick()
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        per = total / K
+        part = r["part"]
+        ev = part.event_counts()
+        out[name] = {"ms_per_step": per, "ship_ticks_per_s": n / (per / 1e3), "world_ticks_per_s": W / (per / 1e3),
+                     "setup_s": setup_s, "layers": [[layer.N, layer.W] for layer, _ in part.layers],
+                     "events_last_tick": int(ev.sum()), "flagged_worlds": int((part.flags() != 0).sum())}
+        runs[name] = (r["park"], ev)
+        if name == "ragged":
+            keep = r
+        else:
+            del r, g, part
+    pr, er = runs["ragged"]
+    pp, ep = runs["plain"]
+    same = all(torch.equal(getattr(pr, "_" + k), getattr(pp, "_" + k)) for k in ("pos", "vel", "mode", "clock"))
+    out["bit_identical"] = bool(same and torch.equal(er, ep))
+    out["speedup_ragged_vs_plain"] = out["plain"]["ms_per_step"] / out["ragged"]["ms_per_step"]
+    out["workload"] = (f"partition worlds: {W} ragged worlds of 1-128 ships (log-uniform, mean {n / W:.1f}; {n} "
+                       "ships) in 1-5 Gaussian blobs (sigma 10 km) a world, a proximity sensor of 1-250 km on every "
+                       "ship (period 1 s), bubbles and the partition, the server layer on top (GotoDirection and "
+                       "SetSpeedFraction for every ship every tick), dynamical orientation off")
+    out["ships"], out["worlds"], out["steps"], out["warmup"] = n, W, K, args.warmup
+    del keep
+    return out
+
+
 def server_runs(args, dev) -> dict:
     """The server layer (exact_ballpark_b200.server) over the flight park at the reference's server benchmark shape
     (benchmarks/server_speed.py): --server-worlds worlds of 4 ships, each flown by a pilot that sends GotoDirection
@@ -768,7 +874,7 @@ def main() -> None:
     ap.add_argument("--collide-steps", type=int, default=50)
     ap.add_argument("--no-combat", action="store_true")
     ap.add_argument("--only", choices=("ragged", "collide", "collide_statics", "combat", "composed", "serve", "server",
-                                       "space"),
+                                       "space", "partition"),
                     default=None, help="run one section alone on one GPU and print it (for profiling); the default "
                                        "run prints the headline line with every section")
     ap.add_argument("--combat-worlds", type=int, default=65536)
@@ -778,6 +884,8 @@ def main() -> None:
     ap.add_argument("--server-steps", type=int, default=100)
     ap.add_argument("--space-worlds", type=int, default=20000)
     ap.add_argument("--space-steps", type=int, default=5)
+    ap.add_argument("--partition-worlds", type=int, default=100000)
+    ap.add_argument("--partition-steps", type=int, default=10)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-seconds", type=float, default=6.0)
     ap.add_argument("--serve-budget-gb", type=float, default=80.0)
@@ -814,7 +922,7 @@ def main() -> None:
                "collide_statics": lambda: collide_runs(args, dev, statics=True),
                "combat": lambda: combat_runs(args, dev), "composed": lambda: combat_runs(args, dev, composed=True),
                "serve": lambda: serve_runs(args, dev), "server": lambda: server_runs(args, dev),
-               "space": lambda: space_runs(args, dev)}[args.only]
+               "space": lambda: space_runs(args, dev), "partition": lambda: partition_runs(args, dev)}[args.only]
         print(json.dumps({"metric": METRIC, "section": args.only, args.only: run()}), flush=True)
         return
     dist = None

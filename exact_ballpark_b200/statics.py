@@ -13,8 +13,11 @@ its triangle (a, c, d); then kind, id, parent id, level and the number of boxes.
 
 from __future__ import annotations
 
+import itertools
 import math
 import struct
+
+import numpy as np
 
 STATIC_CAPSULE, STATIC_BOX = 0, 1
 G_A, G_B, G_AB, G_RAD = 0, 3, 6, 9
@@ -25,6 +28,10 @@ G_SIZE = 175
 I_KIND, I_ID, I_PARENT, I_LEVEL, I_NBOX = range(5)
 I_SIZE = 5
 SIDE_FRONT, SIDE_BACK, SIDE_LEFT, SIDE_RIGHT, SIDE_TOP, SIDE_BOTTOM = range(6)
+# BoxShape's corners A .. H as the edges (x, y, z) each adds to A, and its sides' rectangles (a, b, c, d) as corner
+# indices, in the side order above (OrientedBox.cpp's SetCorners and its rectangles)
+_CORNER_BITS = ((0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (0, 1, 1), (1, 0, 1), (1, 1, 1))
+_SIDE_CORNERS = ((7, 5, 3, 6), (2, 4, 1, 0), (5, 2, 0, 3), (4, 7, 6, 1), (2, 5, 7, 4), (1, 6, 3, 0))
 
 NUM_LEVELS = 8
 LEVEL_WIDTH = tuple(7864320.0 / (1 << 2 * i) for i in range(NUM_LEVELS))          # 480 m x 4^(7 - level)
@@ -84,13 +91,10 @@ def _int64(x: float) -> int:
 
 
 def level_for(radius: float) -> int:
-    """Partition::GetBox(radius, pos)'s level: the finest whose width is at least three radii."""
-    level = 0
-    for i in range(NUM_LEVELS):
-        if 3.0 * radius > LEVEL_WIDTH[i]:
-            break
-        level = i
-    return level
+    """Partition::GetBox(radius, pos)'s level: the finest whose width is at least three radii. The widths shrink with
+    the level, so the levels whose width three radii do not exceed are a prefix; the level is its last (0 when even
+    the top is exceeded; 7 for a NaN, which exceeds nothing)."""
+    return max(sum(1 for w in LEVEL_WIDTH if not 3.0 * radius > w) - 1, 0)
 
 
 def key_for(level: int, pos) -> tuple:
@@ -108,13 +112,10 @@ def bounds(level: int, key) -> tuple:
 
 
 def with_sides(key, mod) -> set:
-    """The box and the adjacent boxes an InsertInBoxes reaches with these sides (-1, 0, +1 an axis)."""
-    out = set()
-    for c in range(8):
-        bits = ((c >> 2) & 1, (c >> 1) & 1, c & 1)
-        if all(mod[q] or not bits[q] for q in range(3)):
-            out.add(tuple(key[q] + mod[q] * bits[q] for q in range(3)))
-    return out
+    """The box and the adjacent boxes an InsertInBoxes reaches: per axis the key alone, or the key and its neighbour
+    on the side `mod` gives (-1, 0, +1), and every combination of those."""
+    options = [(key[q],) if mod[q] == 0 else (key[q], key[q] + mod[q]) for q in range(3)]
+    return set(itertools.product(*options))
 
 
 def static_record(s: dict) -> tuple:
@@ -157,35 +158,38 @@ def static_record(s: dict) -> tuple:
                 left = shorter
     elif kind == "box":
         ints[I_KIND] = STATIC_BOX
-        A = [float(x) for x in s["corner"]]
-        lx, ly, lz = ([float(x) for x in s[k]] for k in ("lx", "ly", "lz"))
-        B, C, D = _add(A, lx), _add(A, ly), _add(A, lz)
-        E, F, G = _add(B, ly), _add(C, lz), _add(B, lz)
-        H = _add(E, lz)
-        corners = (A, B, C, D, E, F, G, H)
-        rects = [None] * 6
-        rects[SIDE_FRONT], rects[SIDE_BACK], rects[SIDE_LEFT] = (H, F, D, G), (C, E, B, A), (F, C, A, D)
-        rects[SIDE_RIGHT], rects[SIDE_TOP], rects[SIDE_BOTTOM] = (E, H, G, B), (C, F, H, E), (B, G, D, A)
-        center = _add(A, _scale(_sub(H, A), 1.0 / 2.0))
-        low, high = list(A), list(A)
-        for v in corners[1:]:
-            for q in range(3):
-                if v[q] > high[q]:
-                    high[q] = v[q]
-                elif v[q] < low[q]:
-                    low[q] = v[q]
+        A = np.array([float(x) for x in s["corner"]])
+        edges = np.array([[float(x) for x in s[k]] for k in ("lx", "ly", "lz")])
+        # corner i = A plus the edges its bits name, added x, then y, then z (BoxShape's A .. H: A, A+x, A+y, A+z,
+        # A+x+y, A+y+z, A+x+z, A+x+y+z); an absent edge is not added (A + 0 would turn a -0 into +0)
+        corners = np.empty((8, 3))
+        for i, bits in enumerate(_CORNER_BITS):
+            v = A.copy()
+            for e in range(3):
+                if bits[e]:
+                    v = v + edges[e]
+            corners[i] = v
+        center = corners[0] + (corners[7] - corners[0]) * (1.0 / 2.0)
+        # the AABB: on each axis the first corner holding the extreme (the strict-comparison scan's choice)
+        low = corners[np.argmin(corners, axis=0), [0, 1, 2]]
+        high = corners[np.argmax(corners, axis=0), [0, 1, 2]]
         geo[G_CENTER:G_CENTER + 3], geo[G_LO:G_LO + 3], geo[G_HI:G_HI + 3] = center, low, high
-        for i, axis in enumerate((lx, ly, lz)):
-            geo[G_AXES + 3 * i:G_AXES + 3 * i + 3] = axis
-            geo[G_UNIT + 3 * i:G_UNIT + 3 * i + 3] = _normalized(axis)
-            geo[G_HALF + i], geo[G_LENSQ + i] = _length(axis) / 2.0, _lensq(axis)
-        for i, v in enumerate(corners):
-            geo[G_CORNERS + 3 * i:G_CORNERS + 3 * i + 3] = v
-        for i, (ra, rb, rc, rd) in enumerate(rects):
-            for j, v in enumerate((ra, rb, rc, rd)):
-                geo[G_RECT + 12 * i + 3 * j:G_RECT + 12 * i + 3 * j + 3] = v
-            geo[G_RNORM + 3 * i:G_RNORM + 3 * i + 3] = _normalized(_cross(_sub(rb, ra), _sub(rc, ra)))
-            geo[G_TNORM + 3 * i:G_TNORM + 3 * i + 3] = _normalized(_cross(_sub(rc, ra), _sub(rd, ra)))
+        lengths = np.sqrt(edges[:, 0] * edges[:, 0] + edges[:, 1] * edges[:, 1] + edges[:, 2] * edges[:, 2])
+        inv = np.where(lengths == 0.0, 0.0, 1.0 / np.where(lengths == 0.0, 1.0, lengths))
+        units = np.where(lengths[:, None] == 0.0, edges, edges * inv[:, None])
+        geo[G_AXES:G_AXES + 9] = edges.reshape(-1)
+        geo[G_UNIT:G_UNIT + 9] = units.reshape(-1)
+        geo[G_HALF:G_HALF + 3] = lengths / 2.0
+        geo[G_LENSQ:G_LENSQ + 3] = edges[:, 0] * edges[:, 0] + edges[:, 1] * edges[:, 1] + edges[:, 2] * edges[:, 2]
+        geo[G_CORNERS:G_CORNERS + 24] = corners.reshape(-1)
+        quads = corners[np.array(_SIDE_CORNERS)]                                 # [6 sides][4 corners][3]
+        geo[G_RECT:G_RECT + 72] = quads.reshape(-1)
+        ra, rb, rc, rd = (quads[:, k] for k in range(4))
+        geo[G_RNORM:G_RNORM + 18] = np.array([_normalized(_cross(u, v)) for u, v in zip(rb - ra, rc - ra)]).reshape(-1)
+        geo[G_TNORM:G_TNORM + 18] = np.array([_normalized(_cross(u, v)) for u, v in zip(rc - ra, rd - ra)]).reshape(-1)
+        H = corners[7]
+        low, high = [float(x) for x in low], [float(x) for x in high]
+        center = [float(x) for x in center]
         dx, dy, dz = high[0] - low[0], high[1] - low[1], high[2] - low[2]
         inner = dz if dy < dz else dy
         r = (inner if dx < inner else dx) / 2.0

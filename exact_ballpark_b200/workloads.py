@@ -465,3 +465,56 @@ def composed_worlds(seed: int, worlds: int, ships: int = 6, missiles: int = 2, s
     """The composed benchmark's worlds (its shape: 6 ships, 2 missiles and 1 sphere a world): combat_worlds with
     massive ships in a +-5 km cube and fixed massive spheres among them, so ships, spheres and missiles meet."""
     return combat_worlds(seed, worlds, ships, missiles, spheres, massive=True, cube=5e3)
+
+
+# ============================================================================ the partition's ragged worlds
+
+@dataclass
+class PartitionWorlds:
+    """Ragged worlds for the partition layer over the flight park (bubbles, the spatial partition and proximity
+    sensors, a pilot a ship): `cols` the park's load columns (world-major, each world's ships in id order from 1),
+    `sizes` each world's ship count, `sensor_range` each ship's sensor radius (m), `direction` and `speed` each ship's
+    pilot's GotoDirection and SetSpeedFraction (drawn once; a pilot sends them every tick)."""
+    cols: dict
+    sizes: np.ndarray
+    sensor_range: np.ndarray
+    direction: np.ndarray
+    speed: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return int(self.sizes.sum())
+
+    @property
+    def starts(self) -> np.ndarray:
+        return np.concatenate(([0], np.cumsum(self.sizes)[:-1])).astype(np.int64)
+
+
+def partition_worlds(seed: int, worlds: int, max_ships: int = 128) -> PartitionWorlds:
+    """W worlds of ragged size (ship counts floor(10^U(0, log10 max_ships)), clipped to [1, max_ships]; mean about 20
+    for 128) with the ships clustered as 1 to 5 Gaussian blobs (sigma 10 km) a world around centres uniform in
+    +-1,000 km; ship parameters as the flight benchmark draws them (mass log-uniform 1e6-1e9 kg, radius uniform
+    20-500 m, maximum velocity log-uniform 100-3000 m/s, agility uniform 0.1-5), at rest, free, interactive (each has
+    a pilot), not massive; a proximity sensor on every ship with a radius log-uniform in [1 km, 250 km], period 1 s.
+    Numpy draws from one seeded generator, so a million ships take a second."""
+    g = np.random.default_rng(seed)
+    sizes = np.clip(np.floor(10.0 ** g.uniform(0.0, math.log10(max_ships), worlds)), 1, max_ships).astype(np.int64)
+    n = int(sizes.sum())
+    world = np.repeat(np.arange(worlds, dtype=np.int64), sizes)
+    starts = np.concatenate(([0], np.cumsum(sizes)[:-1]))
+    ids = np.arange(n, dtype=np.int64) - np.repeat(starts, sizes) + 1
+    blobs = g.integers(1, 6, worlds)
+    centres = g.uniform(-1e6, 1e6, (worlds, 5, 3))
+    pick = (g.random(n) * blobs[world]).astype(np.int64)
+    pos = centres[world, pick] + g.normal(0.0, 1e4, (n, 3))
+    cols = {"id": ids, "world": world, "time": np.zeros(n, np.int64),
+            "mass": 10.0 ** g.uniform(6.0, 9.0, n), "radius": g.uniform(20.0, 500.0, n),
+            "max_vel": 10.0 ** g.uniform(2.0, math.log10(3000.0), n), "agility": g.uniform(0.1, 5.0, n),
+            "speed_fraction": np.ones(n), "free": np.ones(n, bool), "massive": np.zeros(n, bool),
+            "interactive": np.ones(n, bool), "moribund": np.zeros(n, bool), "cloaked": np.zeros(n, np.int64),
+            "bubble": np.full(n, -1, np.int64), "mode": np.full(n, 2, np.int64),
+            "max_ang_vel": np.ones(n), "rot_agility": np.full(n, 0.9), "pos": pos, "vel": np.zeros((n, 3))}
+    rng = 10.0 ** g.uniform(3.0, math.log10(2.5e5), n)
+    d = g.normal(0.0, 1.0, (n, 3))
+    d /= np.maximum(np.linalg.norm(d, axis=1, keepdims=True), 1e-9)
+    return PartitionWorlds(cols, sizes, rng, d, g.uniform(0.2, 1.0, n))
