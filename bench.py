@@ -636,52 +636,6 @@ def space_runs(args, dev) -> dict:
             "flagged_worlds": int((space.st["flags"] != 0).sum()), "boxes_max": int(space.st["box_n"].max())}
 
 
-def partition_setup(pw, dev, ragged: bool, server_on: bool = True) -> dict:
-    """A flight park of the partition worlds with the partition layer (ragged size classes, or the plain 128-slot
-    layout), every ship's sensor added, and the server layer on top (a pilot a ship, GotoDirection and
-    SetSpeedFraction queued for every ship every tick: a fixed schedule of 2 x 128 pushes, a world's pushes masked to
-    its ships). The first tick runs eagerly; returns the parts and the captured tick."""
-    import torch
-
-    from exact_ballpark_b200 import VecModesPark, server
-    from exact_ballpark_b200.modes import tick_plain, tick_tiled
-    from exact_ballpark_b200.partition import PartitionGraph, PartitionLayer
-    park = VecModesPark(pw.n, device=dev)
-    park.load_columns(pw.cols)
-    part = PartitionLayer(park, pw.sizes, ragged=ragged)
-    part.load()
-    part.add_sensors(pw.sensor_range, 1.0)
-    park_tick = (lambda: tick_tiled(park)) if ragged else (lambda: tick_plain(park, park.block))
-    if not ragged:
-        park.scratch()
-    srv = q = None
-    W = len(pw.sizes)
-    if server_on:
-        srv = server.VecServer(server.ModesAdapter(park), (pw.cols["id"] - 1).tolist(), kernel="cuda")
-        srv.pre_tick()                                      # the first tick (its additions) eagerly
-        part.tick(park_tick)
-        park.current_time += 1
-        srv.post_tick()
-        sched = [k for _ in range(128) for k in ("GotoDirection", "SetSpeedFraction")]
-        q = srv._queue([server.CODE[k] for k in sched])
-        sizes = torch.as_tensor(pw.sizes, device=dev)
-        starts = torch.as_tensor(pw.starts, device=dev)
-        direction = torch.as_tensor(pw.direction, device=dev)
-        speed = torch.as_tensor(pw.speed, device=dev)
-        for k in range(128):
-            on = sizes > k
-            row = torch.where(on, starts + k, 0)
-            for j, f in ((2 * k, direction[row]), (2 * k + 1, speed[row][:, None])):
-                q["mask"][j].copy_(on.to(q["mask"].dtype))
-                q["ball"][j].fill_(k + 1)
-                q["f"][j][:, :f.shape[1]].copy_(f)
-    else:
-        part.tick(park_tick)
-        park.current_time += 1
-    g = PartitionGraph(part, park_tick, srv, q)
-    return {"park": park, "part": part, "server": srv, "q": q, "graph": g, "park_tick": park_tick}
-
-
 def partition_runs(args, dev) -> dict:
     """The metric's workload: the partition worlds (exact_ballpark_b200.workloads.partition_worlds: --partition-worlds
     ragged worlds of 1 to 128 ships, log-uniform, in 1 to 5 Gaussian blobs, a sensor of 1 to 250 km on every ship)
@@ -693,6 +647,7 @@ def partition_runs(args, dev) -> dict:
     state, compared here bit for bit (the park's rows, each world's event count)."""
     import torch
 
+    from exact_ballpark_b200.partition import partition_setup
     from exact_ballpark_b200.workloads import partition_worlds
     W, K = args.partition_worlds, args.partition_steps
     pw = partition_worlds(11, W)
@@ -703,7 +658,7 @@ def partition_runs(args, dev) -> dict:
     runs = {}
     for name, ragged in (("ragged", True), ("plain", False)):
         t0 = time.time()
-        r = partition_setup(pw, dev, ragged)
+        r = partition_setup(pw, dev, ragged)            # exact_ballpark_b200.partition
         setup_s = time.time() - t0
         g = r["graph"]
         for _ in range(args.warmup):

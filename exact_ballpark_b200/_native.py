@@ -5,10 +5,15 @@ raises."""
 from __future__ import annotations
 
 import ctypes
+import os
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libebb.so"
+# the counting build (every IEEE operation counted; measurement only), loaded in place of the library when the process
+# is started with EBB_COUNTING=1
+if os.environ.get("EBB_COUNTING") == "1":
+    LIB_PATH = HERE / "libebb_count.so"
 ABI = 7
 COLLIDE_MAX_SLOTS = 64          # include/ebb.h: EBB_COLLIDE_MAX_SLOTS
 COLLIDE_MAX_STATICS = 64        # include/ebb.h: EBB_COLLIDE_MAX_STATICS
@@ -109,6 +114,9 @@ def lib() -> ctypes.CDLL:
     if L.ebb_abi() != ABI:
         raise RuntimeError(f"{LIB_PATH}: ABI {L.ebb_abi()} is not {ABI}; rebuild it")
     p, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+    if LIB_PATH.name == "libebb_count.so":
+        for unit in ("flight", "space", "collide", "combat", "server"):
+            getattr(L, "ebb_count_ops_" + unit).argtypes = [p, i32]
     L.ebb_error_string.restype = ctypes.c_char_p
     L.ebb_error_string.argtypes = [i32]
     L.ebb_flight_scratch_bytes.restype = i64

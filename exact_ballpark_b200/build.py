@@ -16,6 +16,7 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libebb.so"
+COUNT_LIB = HERE / "libebb_count.so"
 SOURCES = ("ebb_flight.cu", "ebb_collide.cu", "ebb_combat.cu", "ebb_server.cu", "ebb_space.cu", "ebb_rand.cu",
            "ebb_plan.cpp")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
@@ -37,15 +38,17 @@ def _stale(target: Path, deps) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build_native(force: bool = False, verbose: bool = False) -> Path:
-    """Each source compiled to an object in parallel (no device code crosses files), then linked into the library."""
+def build_native(force: bool = False, verbose: bool = False, counting: bool = False) -> Path:
+    """Each source compiled to an object in parallel (no device code crosses files), then linked into the library.
+    `counting`: the measurement build (EBB_COUNT_OPS: every IEEE operation counted) as libebb_count.so beside it."""
     from concurrent.futures import ThreadPoolExecutor
     deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "ebb.h"]
-    if not force and not _stale(LIB, deps):
-        return LIB
-    objdir = HERE / "_build"
+    target = COUNT_LIB if counting else LIB
+    if not force and not _stale(target, deps):
+        return target
+    objdir = HERE / ("_build_count" if counting else "_build")
     objdir.mkdir(exist_ok=True)
-    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"] + (["-DEBB_COUNT_OPS"] if counting else [])
 
     def compile_one(src: str):
         obj = objdir / (src + ".o")
@@ -60,16 +63,17 @@ def build_native(force: bool = False, verbose: bool = False) -> Path:
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src} ({r.returncode}):\n{r.stderr[-4000:]}")
         report.append(r.stderr)
-    tmp = LIB.with_suffix(".so.tmp")
+    tmp = target.with_suffix(".so.tmp")
     r = subprocess.run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(tmp)]
                        + [str(obj) for _, obj, _ in results], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc link failed ({r.returncode}):\n{r.stderr[-4000:]}")
-    (HERE / "ptxas.txt").write_text("".join(report))
-    tmp.replace(LIB)
+    if not counting:
+        (HERE / "ptxas.txt").write_text("".join(report))
+    tmp.replace(target)
     if verbose:
         print("".join(report))
-    return LIB
+    return target
 
 
 if __name__ == "__main__":

@@ -63,9 +63,39 @@ EBB_HD float ffrom(uint32_t u) {
 #endif
 }
 
+// ---- the counting build ----
+// Built with EBB_COUNT_OPS (a measurement build, never the timed library), every IEEE operation a kernel executes is
+// counted by kind into the translation unit's own device array op_count (one atomic add an operation), which the
+// unit's ebb_count_ops_* entry point reads and clears: the FLOPs per ship-tick of the algorithm as it runs.
+enum OpKind { OP_DADD, OP_DSUB, OP_DMUL, OP_DDIV, OP_DSQRT, OP_DFMA, OP_FADD, OP_FSUB, OP_FMUL, OP_FDIV, OP_FSQRT,
+              OP_FFMA, OP_KINDS };
+#if defined(EBB_COUNT_OPS) && defined(__CUDACC__)
+static __device__ unsigned long long op_count[OP_KINDS];
+#endif
+#if defined(EBB_COUNT_OPS) && defined(__CUDA_ARCH__)
+#define EBB_OP(k) atomicAdd(&op_count[k], 1ull)
+#else
+#define EBB_OP(k) ((void)0)
+#endif
+// the unit's reader (the counting build only): its counts into out[OP_KINDS], cleared after when `reset`
+#if defined(EBB_COUNT_OPS) && defined(__CUDACC__)
+#define EBB_OP_COUNTER(name)                                                                                    \
+    extern "C" int name(unsigned long long* out, int reset) {                                                   \
+        cudaError_t e = cudaMemcpyFromSymbol(out, ebb::op_count, sizeof(unsigned long long) * ebb::OP_KINDS);   \
+        if (e == cudaSuccess && reset) {                                                                        \
+            const unsigned long long zero[ebb::OP_KINDS] = {};                                                  \
+            e = cudaMemcpyToSymbol(ebb::op_count, zero, sizeof(zero));                                          \
+        }                                                                                                       \
+        return e == cudaSuccess ? 0 : (int)e;                                                                   \
+    }
+#else
+#define EBB_OP_COUNTER(name)
+#endif
+
 // ---- double ----
 EBB_HD double dadd(double a, double b) {
 #ifdef __CUDA_ARCH__
+    EBB_OP(OP_DADD);
     return __dadd_rn(a, b);
 #else
     return a + b;
@@ -73,6 +103,7 @@ EBB_HD double dadd(double a, double b) {
 }
 EBB_HD double dsub(double a, double b) {
 #ifdef __CUDA_ARCH__
+    EBB_OP(OP_DSUB);
     return __dsub_rn(a, b);
 #else
     return a - b;
@@ -80,6 +111,7 @@ EBB_HD double dsub(double a, double b) {
 }
 EBB_HD double dmul(double a, double b) {
 #ifdef __CUDA_ARCH__
+    EBB_OP(OP_DMUL);
     return __dmul_rn(a, b);
 #else
     return a * b;
@@ -87,6 +119,7 @@ EBB_HD double dmul(double a, double b) {
 }
 EBB_HD double ddiv(double a, double b) {
 #ifdef __CUDA_ARCH__
+    EBB_OP(OP_DDIV);
     return __ddiv_rn(a, b);
 #else
     return a / b;
@@ -94,6 +127,7 @@ EBB_HD double ddiv(double a, double b) {
 }
 EBB_HD double dsqrt(double a) {
 #ifdef __CUDA_ARCH__
+    EBB_OP(OP_DSQRT);
     return __dsqrt_rn(a);
 #else
     return std::sqrt(a);
@@ -101,6 +135,7 @@ EBB_HD double dsqrt(double a) {
 }
 EBB_HD double dfma(double a, double b, double c) {   // a b + c, rounded once
 #ifdef __CUDA_ARCH__
+    EBB_OP(OP_DFMA);
     return __fma_rn(a, b, c);
 #else
     return std::fma(a, b, c);
@@ -161,6 +196,7 @@ EBB_HD double i2d(int64_t v) {
 // ---- float ----
 EBB_HD float fadd(float a, float b) {
 #ifdef __CUDA_ARCH__
+    EBB_OP(OP_FADD);
     return __fadd_rn(a, b);
 #else
     return a + b;
@@ -168,6 +204,7 @@ EBB_HD float fadd(float a, float b) {
 }
 EBB_HD float fsub(float a, float b) {
 #ifdef __CUDA_ARCH__
+    EBB_OP(OP_FSUB);
     return __fsub_rn(a, b);
 #else
     return a - b;
@@ -175,6 +212,7 @@ EBB_HD float fsub(float a, float b) {
 }
 EBB_HD float fmul(float a, float b) {
 #ifdef __CUDA_ARCH__
+    EBB_OP(OP_FMUL);
     return __fmul_rn(a, b);
 #else
     return a * b;
@@ -182,6 +220,7 @@ EBB_HD float fmul(float a, float b) {
 }
 EBB_HD float fdiv(float a, float b) {
 #ifdef __CUDA_ARCH__
+    EBB_OP(OP_FDIV);
     return __fdiv_rn(a, b);
 #else
     return a / b;
@@ -189,6 +228,7 @@ EBB_HD float fdiv(float a, float b) {
 }
 EBB_HD float fsqrt(float a) {
 #ifdef __CUDA_ARCH__
+    EBB_OP(OP_FSQRT);
     return __fsqrt_rn(a);
 #else
     return std::sqrt(a);
@@ -196,6 +236,7 @@ EBB_HD float fsqrt(float a) {
 }
 EBB_HD float ffma(float a, float b, float c) {       // a b + c, rounded once to binary32
 #ifdef __CUDA_ARCH__
+    EBB_OP(OP_FFMA);
     return __fmaf_rn(a, b, c);
 #else
     return std::fma(a, b, c);

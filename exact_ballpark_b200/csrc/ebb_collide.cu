@@ -876,3 +876,5 @@ int ebb_collide_load(const EbbCollideState* s, int32_t* status, void* stream) {
 }
 
 }  // extern "C"
+
+EBB_OP_COUNTER(ebb_count_ops_collide)

@@ -1071,3 +1071,5 @@ int ebb_composed_file(const EbbComposedState* s, const uint8_t* mask, const doub
 }
 
 }  // extern "C"
+
+EBB_OP_COUNTER(ebb_count_ops_combat)

@@ -810,3 +810,5 @@ int ebb_kernel_info(int which, int* regs, int* local_bytes, int* binary_version,
 }
 
 }  // extern "C"
+
+EBB_OP_COUNTER(ebb_count_ops_flight)

@@ -523,3 +523,5 @@ int ebb_server_tick(const EbbServerState* s, const EbbServerQueue* q, int phase,
 }
 
 }  // extern "C"
+
+EBB_OP_COUNTER(ebb_count_ops_server)

@@ -95,3 +95,5 @@ int ebb_space_query(const EbbFlightState* park, const EbbSpaceState* s, const Eb
 }
 
 }  // extern "C"
+
+EBB_OP_COUNTER(ebb_count_ops_space)

@@ -185,3 +185,46 @@ class PartitionGraph:
     def tick(self) -> None:
         self.graph.replay()
         self.part.park.current_time += 1
+
+
+def partition_setup(pw, dev, ragged: bool, server_on: bool = True) -> dict:
+    """A flight park of the partition worlds with the partition layer (ragged size classes, or the plain 128-slot
+    layout), every ship's sensor added, and the server layer on top (a pilot a ship, GotoDirection and
+    SetSpeedFraction queued for every ship every tick: a fixed schedule of 2 x 128 pushes, a world's pushes masked to
+    its ships). The first tick runs eagerly; returns the parts and the captured tick."""
+    from . import server
+    from .modes import tick_plain, tick_tiled
+    park = VecModesPark(pw.n, device=dev)
+    park.load_columns(pw.cols)
+    part = PartitionLayer(park, pw.sizes, ragged=ragged)
+    part.load()
+    part.add_sensors(pw.sensor_range, 1.0)
+    park_tick = (lambda: tick_tiled(park)) if ragged else (lambda: tick_plain(park, park.block))
+    if not ragged:
+        park.scratch()
+    srv = q = None
+    W = len(pw.sizes)
+    if server_on:
+        srv = server.VecServer(server.ModesAdapter(park), (pw.cols["id"] - 1).tolist(), kernel="cuda")
+        srv.pre_tick()                                      # the first tick (its additions) eagerly
+        part.tick(park_tick)
+        park.current_time += 1
+        srv.post_tick()
+        sched = [k for _ in range(128) for k in ("GotoDirection", "SetSpeedFraction")]
+        q = srv._queue([server.CODE[k] for k in sched])
+        sizes = torch.as_tensor(pw.sizes, device=dev)
+        starts = torch.as_tensor(pw.starts, device=dev)
+        direction = torch.as_tensor(pw.direction, device=dev)
+        speed = torch.as_tensor(pw.speed, device=dev)
+        for k in range(128):
+            on = sizes > k
+            row = torch.where(on, starts + k, 0)
+            for j, f in ((2 * k, direction[row]), (2 * k + 1, speed[row][:, None])):
+                q["mask"][j].copy_(on.to(q["mask"].dtype))
+                q["ball"][j].fill_(k + 1)
+                q["f"][j][:, :f.shape[1]].copy_(f)
+    else:
+        part.tick(park_tick)
+        park.current_time += 1
+    g = PartitionGraph(part, park_tick, srv, q)
+    return {"park": park, "part": part, "server": srv, "q": q, "graph": g, "park_tick": park_tick}

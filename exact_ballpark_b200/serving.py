@@ -64,16 +64,17 @@ class Episode:
 
 
 def episode_stream(seed: int, count: int, rate: float = 2000.0, max_ships: int = 256, min_ticks: int = 10,
-                   max_ticks: int = 10000) -> list:
-    """`count` episodes arriving as a Poisson process of `rate` a second: ship counts log-uniform in [1, max_ships],
-    lengths log-uniform in [min_ticks, max_ticks] ticks, each world drawn by workloads.flight_worlds from its own seed
-    (follow / orbit / warp ships)."""
+                   max_ticks: int = 10000, min_ships: int = 1) -> list:
+    """`count` episodes arriving as a Poisson process of `rate` a second: ship counts log-uniform in [1, max_ships]
+    (redrawn up to min_ships when a floor is given: uniform in [min_ships, max_ships]), lengths log-uniform in
+    [min_ticks, max_ticks] ticks, each world drawn by workloads.flight_worlds from its own seed (follow / orbit / warp
+    ships)."""
     r = random.Random(seed)
     t = 0.0
     out = []
     for e in range(count):
         t += r.expovariate(rate) if rate > 0 else 0.0
-        ships = ragged_ships(r, max_ships)
+        ships = ragged_ships(r, max_ships) if min_ships <= 1 else r.randint(min_ships, max_ships)
         ticks = max(min_ticks, min(max_ticks, int(10.0 ** r.uniform(math.log10(min_ticks), math.log10(max_ticks)))))
         world = flight_worlds(seed * 1_000_033 + e, 1, ships)
         world.packed()                           # the request in columns, made by the client before it arrives

@@ -140,6 +140,43 @@ def test_ragged_worlds_match_the_oracle():
     _compare(o, p, "after 40 ticks")
 
 
+@pytest.mark.parametrize("schedule", ["tiled", "tiled_rounds", "worlds", "plain"])
+def test_worlds_of_65_to_128_ships_match_the_oracle(schedule):
+    """The metric's largest worlds, 65 to 128 ships each, against the oracle under every schedule: tiles of whole
+    worlds one a block (a tile up to 256 rows) and the persistent form with several rounds of ships a thread (tiles
+    of up to 512 rows over 128-thread blocks), the listed-worlds kernel, and the plain two launches."""
+    import random
+    from exact_ballpark_b200 import tick_plain, tick_tiled, tick_worlds
+    from exact_ballpark_b200.tiles import plan_tiles
+    from exact_ballpark_b200.workloads import FlightWorlds, flight_worlds
+    from oracle.park import OraclePark
+    r = random.Random(65)
+    w = FlightWorlds.concat([flight_worlds(7000 + k, 1, r.randint(65, 128)) for k in range(36)])
+    assert min(w.sizes) >= 65 and max(w.sizes) > 120
+    o = OraclePark(len(w.rows), dynamical_orientation=True, use_new_orbit=True)
+    p = _park({"n": len(w.rows), "dynamical_orientation": True, "use_new_orbit": True}, "plain")
+    for park in (o, p):
+        park.load(w.rows)
+        w.apply(park)
+    if schedule == "tiled":
+        plan = plan_tiles(p.world, cap=256, block=256)
+        run = lambda: tick_tiled(p, plan)                                      # noqa: E731
+    elif schedule == "tiled_rounds":
+        plan = plan_tiles(p.world, cap=512, block=128, grid=5)
+        run = lambda: tick_tiled(p, plan)                                      # noqa: E731
+    elif schedule == "worlds":
+        plan = plan_tiles(p.world, cap=512, block=128)
+        run = lambda: tick_worlds(p, None, plan)                               # noqa: E731
+    else:
+        run = lambda: tick_plain(p)                                            # noqa: E731
+    for k in range(25):
+        o.evolve()
+        run()
+        if k in (0, 9, 24):
+            _compare(o, p, f"{schedule}, tick {k}")
+    assert int(p._status.item()) == 0
+
+
 def _state(p) -> dict:
     return {f: getattr(p, f).detach().cpu().numpy().copy() for f in COMPARE}
 

@@ -187,6 +187,28 @@ def test_served_episodes_match_the_oracle_alone():
         _same_states(res, want, f"episode {ep.eid} against the oracle")
 
 
+def test_served_episodes_of_129_to_256_ships_match_the_oracle_alone():
+    """Config 4's largest episodes: 129 to 256 ships a world (tiles of up to 1024 rows, several rounds of ships a
+    thread block), each against the oracle run alone."""
+    from exact_ballpark_b200.serving import episode_stream
+    from oracle.park import OraclePark
+    eps = episode_stream(41, 8, rate=0.0, max_ships=256, min_ships=129, min_ticks=5, max_ticks=25)
+    assert min(e.ships for e in eps) >= 129 and max(e.ships for e in eps) > 200
+    srv, summary = _served(eps, rows=1200, tile_cap=1024)
+    assert summary["admitted"] == summary["retired"] == len(eps)
+    for ep in eps:
+        o = OraclePark(ep.ships, dynamical_orientation=True, use_new_orbit=True)
+        o.load(ep.world.rows)
+        ep.world.apply(o)
+        for _ in range(ep.ticks):
+            o.evolve()
+        res = _result_state(srv.results[ep.eid])
+        start = srv.results[ep.eid].start
+        res["follow_ptr"] = np.where(res["follow_ptr"] >= 0, res["follow_ptr"] - start, -1)
+        want = {f: np.asarray(getattr(o, f)) for f in COMPARE}
+        _same_states(res, want, f"episode {ep.eid} ({ep.ships} ships) against the oracle")
+
+
 def test_open_loop_arrivals_are_served_and_timed():
     """Arrivals in wall time (an open loop): every episode is served and each step's latency is recorded."""
     from exact_ballpark_b200.serving import episode_stream
