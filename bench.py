@@ -674,8 +674,35 @@ def partition_runs(args, dev) -> dict:
             total += a.elapsed_time(b)
         per = total / K
         part = r["part"]
+        # one eager tick, each part timed alone: the server's pre-tick, the layers' dead-bubble tests, the park's tick,
+        # each layer's re-filings and HandleProximities, the send flags
+        parts_ms = {}
+        park, srv, q = r["park"], r["server"], r["q"]
+
+        def timed_part(name, fn):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            out_ = fn()
+            b.record(stream)
+            b.synchronize()
+            parts_ms[name] = parts_ms.get(name, 0.0) + a.elapsed_time(b)
+            return out_
+        if srv is not None:
+            timed_part("server_pre_tick", lambda: srv._launch(q, 5))
+        dead = timed_part("dead_bubbles", part.dead_rows)
+        saved = park._moribund.clone()
+        park._moribund.logical_or_(dead)
+        timed_part("park_tick", r["park_tick"])
+        park._moribund.copy_(saved)
+        for layer, _ in part.layers:
+            layer.clear_events()
+            timed_part(f"after_evolve_{layer.N}", lambda: layer.after_evolve(None))
+        if srv is not None:
+            timed_part("server_flags", lambda: srv._launch(q, 3))
+        park.current_time += 1
         ev = part.event_counts()
         out[name] = {"ms_per_step": per, "ship_ticks_per_s": n / (per / 1e3), "world_ticks_per_s": W / (per / 1e3),
+                     "eager_parts_ms": parts_ms,
                      "setup_s": setup_s, "layers": [[layer.N, layer.W] for layer, _ in part.layers],
                      "events_last_tick": int(ev.sum()), "flagged_worlds": int((part.flags() != 0).sum())}
         runs[name] = (r["park"], ev)

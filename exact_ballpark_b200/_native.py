@@ -88,7 +88,8 @@ class SpaceState(ctypes.Structure):
                 + [(k, ctypes.c_void_p) for k in ("rows",) + SPACE_SLOT_FIELDS + SPACE_FLAG_FIELDS + SPACE_BOX_FIELDS
                    + SPACE_DICT_FIELDS]
                 + [("umap_cap", ctypes.c_int64), ("events", ctypes.c_int64)]
-                + [(k, ctypes.c_void_p) for k in SPACE_SENSOR_FIELDS])
+                + [(k, ctypes.c_void_p) for k in SPACE_SENSOR_FIELDS]
+                + [("smask", ctypes.c_void_p), ("pmask", ctypes.c_void_p), ("lanes", ctypes.c_int64)])
 
 
 class SpaceQuery(ctypes.Structure):

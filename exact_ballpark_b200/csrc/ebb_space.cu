@@ -15,6 +15,15 @@ __global__ void __launch_bounds__(128) tape_kernel(const EbbFlightState p, const
     run_tape(&p, &s, &t, w);
 }
 
+// a warp a world: the world's index is the warp's, the lanes run its program together (ebb_space.cuh's World)
+__global__ void __launch_bounds__(128) tape_kernel_warp(const EbbFlightState p, const EbbSpaceState s,
+                                                        const EbbSpaceTape t) {
+    __shared__ Coop scratch[4];
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= s.worlds) return;                            // (the whole warp: w is the warp's)
+    run_tape(&p, &s, &t, w, (int)(threadIdx.x & 31), &scratch[threadIdx.x >> 5]);
+}
+
 __global__ void __launch_bounds__(128) query_kernel(const EbbFlightState p, const EbbSpaceState s, const EbbSpaceQuery q) {
     const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= s.worlds) return;
@@ -53,7 +62,8 @@ static int space_buffers(const EbbFlightState* park, const EbbSpaceState* s) {
         s->trk == nullptr || s->cloaked == nullptr || s->sonly == nullptr || s->has_prox == nullptr ||
         s->ntf_in == nullptr || s->trk_in == nullptr || s->slist == nullptr || s->slen == nullptr ||
         s->sbkt == nullptr || s->pmap == nullptr || s->pn == nullptr || s->pbkt == nullptr || s->evn == nullptr ||
-        s->rnd == nullptr || (s->events > 0 && s->ev == nullptr))
+        s->rnd == nullptr || (s->events > 0 && s->ev == nullptr) || s->smask == nullptr || s->pmask == nullptr ||
+        (s->lanes != 1 && s->lanes != 32))
         return EBB_EINVAL;
     if (park->pos == nullptr || park->vel == nullptr || park->old_pos == nullptr || park->old_vel == nullptr ||
         park->ids == nullptr || park->radius == nullptr || park->max_vel == nullptr || park->agility == nullptr ||
@@ -72,8 +82,13 @@ int ebb_space_tape(const EbbFlightState* park, const EbbSpaceState* s, const Ebb
     rc = space_buffers(park, s);
     if (rc) return rc;
     if (t->code == nullptr || t->a == nullptr || t->b == nullptr) return EBB_EINVAL;
-    const unsigned grid = (unsigned)((s->worlds + block - 1) / block);
-    ebb::space::tape_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(*park, *s, *t);
+    if (s->lanes == 32) {
+        const unsigned grid = (unsigned)((s->worlds * 32 + 127) / 128);
+        ebb::space::tape_kernel_warp<<<grid, 128, 0, (cudaStream_t)stream>>>(*park, *s, *t);
+    } else {
+        const unsigned grid = (unsigned)((s->worlds + block - 1) / block);
+        ebb::space::tape_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(*park, *s, *t);
+    }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : (int)e;
 }

@@ -63,10 +63,23 @@ EBB_HD int level_for(double radius) {
     return level;
 }
 
+// A warp's scratch when a warp runs a world (EbbSpaceState.lanes = 32): the candidates' walk keys and ids by slot, and
+// their slots in the walk's order
+struct Coop {
+    int64_t key[EBB_SPACE_MAX_SLOTS];
+    int64_t id[EBB_SPACE_MAX_SLOTS];
+    uint8_t out[EBB_SPACE_MAX_SLOTS];
+};
+
+// One world's program. A thread runs it alone (lane -1), or the 32 lanes of a warp run it together (lane 0 .. 31):
+// every lane then takes every step on the same data, so they stay converged and write the same values (one
+// transaction a load or store), and GetNearbyBalls' scan and sort are split over the lanes (nearby_warp).
 struct World {
     const EbbFlightState* p;
     const EbbSpaceState* s;
     int64_t w, W, N, B;
+    int lane = -1;
+    Coop* sh = nullptr;
 
     // ---- accessors: entry e of a [cap][W] array, component c of a [3][cap][W] array ----
     EBB_HD int64_t& I(int64_t* a, int64_t e) const { return a[e * W + w]; }
@@ -655,6 +668,9 @@ struct World {
         const int64_t bub = I(s->bubble, b);
         if (exclude_inert && !set_any(0, bub)) return 0;
         if (lvl(b) < 0) return 0;
+#ifdef __CUDA_ARCH__
+        if (lane >= 0) return nearby_warp(b, bub, exclude_fixed, exclude_inert, exclude_cloaked, out);
+#endif
         int64_t keys[EBB_SPACE_MAX_SLOTS], oid[EBB_SPACE_MAX_SLOTS];
         int n = 0;
         for (int64_t o = 0; o < N; ++o) {
@@ -684,19 +700,78 @@ struct World {
         return n;
     }
 
+#ifdef __CUDA_ARCH__
+    // nearby's warp form: each lane takes the slots lane, lane + 32, ...: the filter and the walk key (NOT_A_CANDIDATE
+    // for a ball that is none), then each candidate's place in the walk's order is the number of candidates before it
+    // by (key, id) (ids are distinct, so the places are too); every lane reads the order back
+    __device__ int nearby_warp(int64_t b, int64_t bub, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked,
+                               uint8_t* out) const {
+        for (int64_t o = lane; o < N; o += 32) {
+            int64_t k = NOT_A_CANDIDATE, i = 0;
+            if (o != b && slot_ok(o) && U(s->in_park, o) && lvl(o) >= 0) {
+                k = walk_key(b, o);
+                const int64_t r = row(o);
+                if (k != NOT_A_CANDIDATE) {
+                    bool keep = !(exclude_cloaked && (at(s->cloaked, o) != 0 || !p->massive[r]));
+                    if (exclude_inert)
+                        keep = keep && p->interactive[r];
+                    else
+                        keep = keep && I(s->bubble, o) == bub && !(exclude_fixed && !p->free_[r]);
+                    if (!keep) k = NOT_A_CANDIDATE;
+                    i = p->ids[r];
+                }
+            }
+            sh->key[o] = k;
+            sh->id[o] = i;
+        }
+        __syncwarp();
+        int mine = 0;
+        for (int64_t o = lane; o < N; o += 32) {
+            const int64_t k = sh->key[o];
+            if (k == NOT_A_CANDIDATE) continue;
+            const int64_t i = sh->id[o];
+            int place = 0;
+            for (int64_t c = 0; c < N; ++c) {
+                const int64_t kc = sh->key[c];
+                place += (kc < k || (kc == k && sh->id[c] < i)) ? 1 : 0;
+            }
+            sh->out[place] = (uint8_t)o;
+            ++mine;
+        }
+        const int n = (int)__reduce_add_sync(0xffffffffu, (unsigned)mine);
+        __syncwarp();
+        for (int i = 0; i < n; ++i) out[i] = sh->out[i];
+        __syncwarp();
+        return n;
+    }
+#endif
+
     // ---- std::unordered_map<int64_t, ...> in libstdc++'s iteration order (space.py:193-322) ----
     // A map's keys are slots (their balls' ids the keys' values): k[e step] for e < len, in iteration order, with
     // the map's bucket count (1 for a fresh map).
+    // Beside the order, the keys as a set of slots: 128 bits, word c at m[c mstep] (membership without a scan).
     struct UMap {
         uint8_t* k;
         int64_t step;
         int32_t* len;
         int32_t* bkt;
+        uint64_t* m;
+        int64_t mstep;
     };
     EBB_HD UMap sensor_map(int64_t j) const {
-        return UMap{s->slist + j * W + w, N * W, &at(s->slen, j), &at(s->sbkt, j)};
+        return UMap{s->slist + j * W + w, N * W, &at(s->slen, j), &at(s->sbkt, j), s->smask + j * W + w, N * W};
     }
-    EBB_HD UMap proximity_map() const { return UMap{s->pmap + w, W, &s->pn[w], &s->pbkt[w]}; }
+    EBB_HD UMap proximity_map() const {
+        return UMap{s->pmap + w, W, &s->pn[w], &s->pbkt[w], s->pmask + w, W};
+    }
+    EBB_HD bool umap_has(const UMap& m, int64_t slot) const {
+        return ((m.m[(slot >> 6) * m.mstep] >> (slot & 63)) & 1) != 0;
+    }
+    EBB_HD void umap_clear(const UMap& m) const {
+        *m.len = 0;
+        m.m[0] = 0;
+        m.m[m.mstep] = 0;
+    }
     EBB_HD uint64_t bucket_of(int64_t slot, int32_t bkt) const { return (uint64_t)id(slot) % (uint64_t)bkt; }
     EBB_HD int32_t umap_find(const UMap& m, int64_t slot) const {
         const int32_t n = *m.len;
@@ -717,11 +792,12 @@ struct World {
         for (int32_t e = n; e > at0; --e) m.k[e * m.step] = m.k[(e - 1) * m.step];
         m.k[at0 * m.step] = (uint8_t)slot;
         *m.len = n + 1;
+        m.m[(slot >> 6) * m.mstep] |= uint64_t(1) << (slot & 63);
     }
     // insert(): an absent key linked; before it, a fresh map takes 13 buckets and a key past the bucket count grows
     // the table, every key re-linked in its old order. A map past umap_cap keys flags the world.
     EBB_HDNI bool umap_insert(const UMap& m, int64_t slot, int64_t flag_bit) const {
-        if (umap_find(m, slot) >= 0) return false;
+        if (umap_has(m, slot)) return false;
         const int32_t n = *m.len;
         if (n >= s->umap_cap) {
             flag(flag_bit);
@@ -744,10 +820,13 @@ struct World {
     }
     EBB_HD void umap_erase_at(const UMap& m, int32_t e0) const {
         const int32_t n = *m.len;
+        const int64_t slot = m.k[e0 * m.step];
+        m.m[(slot >> 6) * m.mstep] &= ~(uint64_t(1) << (slot & 63));
         for (int32_t e = e0; e + 1 < n; ++e) m.k[e * m.step] = m.k[(e + 1) * m.step];
         *m.len = n - 1;
     }
     EBB_HD void umap_erase(const UMap& m, int64_t slot) const {
+        if (!umap_has(m, slot)) return;
         const int32_t e = umap_find(m, slot);
         if (e >= 0) umap_erase_at(m, e);
     }
@@ -792,7 +871,7 @@ struct World {
         at(s->trk_range, j) = 0.0;
         at(s->trk_in, j) = 0;
         at(s->cloaked, j) = 0;
-        at(s->slen, j) = 0;
+        umap_clear(sensor_map(j));
         at(s->sbkt, j) = 1;
         p->sensor[row(j)] = 0;
     }
@@ -802,7 +881,7 @@ struct World {
         const int64_t r = row(j);
         const float rng = (float)range;
         if (fadd(p->radius[r], rng) < 0.0f) return;
-        at(s->slen, j) = 0;
+        umap_clear(sensor_map(j));
         at(s->srange, j) = (double)rng;
         at(s->speriod, j) = period;
         p->sensor[r] = 1;
@@ -937,7 +1016,7 @@ struct World {
         for (int i = 0; i < nc; ++i) {
             const int64_t o = cand[i];
             if (o == j) continue;
-            const bool inside = umap_find(m, o) >= 0;
+            const bool inside = umap_has(m, o);
             const double ck = (double)fadd(fadd(range, p->radius[row(o)]), p->radius[r]);
             if (dist2_slots(j, o) > dmul(ck, ck)) {
                 if (inside) {
@@ -971,7 +1050,7 @@ struct World {
                     at(s->selapsed, j) = at(s->speriod, j);
                     check_for_proximity(j);
                 }
-                at(s->slen, j) = 0;
+                umap_clear(sensor_map(j));
                 continue;
             }
             if (!at(s->has_prox, j)) continue;
@@ -1255,8 +1334,9 @@ EBB_HD void run_query(const EbbFlightState* p, const EbbSpaceState* s, const Ebb
 }
 
 // world w's K operations of the tape, in order (a flagged world is left alone)
-EBB_HD void run_tape(const EbbFlightState* p, const EbbSpaceState* s, const EbbSpaceTape* t, int64_t w) {
-    World wd{p, s, w, s->worlds, s->slots, s->boxes};
+EBB_HD void run_tape(const EbbFlightState* p, const EbbSpaceState* s, const EbbSpaceTape* t, int64_t w, int lane = -1,
+                     Coop* sh = nullptr) {
+    World wd{p, s, w, s->worlds, s->slots, s->boxes, lane, sh};
     for (int64_t k = 0; k < t->K; ++k) {
         if (s->flags[w] & (F_EDGE | F_BOXES | F_DICTS | F_ENTRIES | F_SETS | F_BAD_OP)) return;
         const int64_t at = k * s->worlds + w;

@@ -6,9 +6,11 @@ padded to N, one thread a world in world order. Here the same per-world program 
 same worlds, with the same results world by world:
 
 - `ragged=True` (the ragged batch): each world goes to the smallest size class (4, 8, 16, 32, 64 or 128 slots) that
-  holds it, one layer a class, so a world's loops run over its class's slots and not 128, and a class's worlds are
-  ordered by size, largest first, so that the 32 worlds of a warp run programs of about the same length (one thread a
-  world: a warp lasts as long as its longest world) and the longest warps start first;
+  holds it, one layer a class, so a world's loops run over its class's slots and not 128; a class's worlds are
+  ordered by size, largest first (the longest programs start first); the classes of 4 to 16 slots run a thread a
+  world (a warp's 32 worlds of about the same size, so about the same program length), the classes of 32 to 128 slots
+  a warp a world, its lanes splitting GetNearbyBalls' scan and sort (the sensors' O(N^2) part) and running the rest
+  together;
 - `ragged=False` (the plain per-configuration layout): one layer of 128 slots a world, the worlds in their order.
 
 A tick (`tick`) is Destiny's Evolve with the layer on the master: every layer's dead-bubble rows (TIME-714), the
@@ -26,6 +28,7 @@ from .modes import WARP, VecModesPark
 from .space import OP, VecSpace
 
 CLASSES = (4, 8, 16, 32, 64, 128)
+WARP_CLASS = 32                  # the ragged batch's classes from this size up run a warp a world
 BOOL, I64 = torch.bool, torch.int64
 
 
@@ -63,7 +66,7 @@ class PartitionLayer:
             slots[:] = np.where(col < k[:, None], starts[idx][:, None] + col, -1)
             layer = VecSpace(park, slots, boxes=boxes_per_slot * cap + 64,
                              events=cap * (cap + 2) if events is None else int(events), umap_cap=cap,
-                             seed=(idx + seed).tolist())
+                             seed=(idx + seed).tolist(), lanes=32 if ragged and cap >= WARP_CLASS else 1)
             self.layers.append((layer, idx))
         self.last_dead = None
 

@@ -48,7 +48,7 @@ class VecSpace:
 
     def __init__(self, park: VecModesPark, rows, boxes: int | None = None, dicts: int | None = None,
                  entries: int | None = None, sets: int | None = None, block: int = BLOCK, events: int = 256,
-                 umap_cap: int | None = None, seed=1):
+                 umap_cap: int | None = None, seed=1, lanes: int = 1):
         if not isinstance(park, VecModesPark):
             raise TypeError("the space layer runs over the flight park (exact_ballpark_b200.VecModesPark)")
         self.park, self.dev, self.block = park, park.dev, int(block)
@@ -90,7 +90,10 @@ class VecSpace:
             "has_prox": z(N, W, dt=U8), "ntf_in": z(N, W, dt=U8), "trk_in": z(N, W, dt=U8),
             "slist": z(self.U, N, W, dt=U8), "slen": zi32(N, W), "sbkt": zi32(N, W) + 1, "pmap": z(self.U, W, dt=U8),
             "pn": zi32(W), "pbkt": zi32(W) + 1, "ev": zi32(max(self.M, 1), W), "evn": z(W),
-            "rnd": zi32(W, _native.RAND_WORDS)})
+            "rnd": zi32(W, _native.RAND_WORDS), "smask": z(2, N, W), "pmask": z(2, W)})
+        if lanes not in (1, 32):
+            raise ValueError("lanes: 1 (a thread a world) or 32 (a warp a world)")
+        self.lanes = int(lanes)
         seeds = torch.as_tensor(seed, dtype=I64).reshape(-1)
         seeds = (seeds.expand(W) if seeds.numel() == 1 else seeds).contiguous().to(d)
         if seeds.numel() != W:
@@ -108,7 +111,7 @@ class VecSpace:
         if self._state is None:
             s = _native.SpaceState()
             s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets = self.W, self.N, self.B, self.D, self.E, self.S
-            s.umap_cap, s.events = self.U, self.M
+            s.umap_cap, s.events, s.lanes = self.U, self.M, self.lanes
             s.rows = self.rows.data_ptr()
             for name, t in self.st.items():
                 setattr(s, name, t.data_ptr())

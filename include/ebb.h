@@ -222,6 +222,8 @@ typedef struct EbbSpaceState {
     int32_t* ev;                                                   /* [events][W] */
     int64_t* evn;                                                  /* [W] */
     int32_t* rnd;                                                  /* [W][EBB_RAND_WORDS] */
+    uint64_t *smask, *pmask;   /* the same keys as sets of slots (128 bits): [2][N][W] a sensor's, [2][W] the map's */
+    int64_t lanes;             /* 1: a thread runs a world; 32: a warp runs a world (GetNearbyBalls split over it) */
 } EbbSpaceState;
 /* K operations a world, applied in order: code, a (a slot), b (an integer argument), each [K][W], and f, each
  * operation's floating-point arguments [K][4][W] (ADD_SENSOR: range, period; NOTIFY_RANGE: range; TRACK: range, and

@@ -28,3 +28,17 @@ def bit_equal(a, b) -> np.ndarray:
         a, b = a.astype(np.float64), b.astype(np.float64)
         return (a.view(np.uint64) == b.view(np.uint64)) | (np.isnan(a) & np.isnan(b))
     return a == b
+
+
+F32_DIGEST_K = 0x9E3779B97F4A7C15
+
+
+def f32_digest(arg_bits: np.ndarray, results: np.ndarray) -> np.uint64:
+    """A chunk's digest of a float function's results: sum over the arguments, modulo 2^64, of (bits + 1) x (2 i + 1)
+    x K, i the argument's binary32 pattern, bits the result's (every NaN as 0x7fc00000)."""
+    y = np.asarray(results, dtype=np.float64).astype(np.float32)
+    bits = y.view(np.uint32).astype(np.uint64)
+    bits = np.where(np.isnan(y), np.uint64(0x7FC00000), bits)
+    w = (np.asarray(arg_bits, dtype=np.uint64) * np.uint64(2) + np.uint64(1)) * np.uint64(F32_DIGEST_K)
+    with np.errstate(over="ignore"):
+        return np.uint64(np.sum((bits + np.uint64(1)) * w, dtype=np.uint64))

@@ -137,14 +137,15 @@ class HostLayer:
             "trk_in": z(n, W, dt=np.uint8), "slist": z(n, n, W, dt=np.uint8), "slen": z(n, W, dt=np.int32),
             "sbkt": z(n, W, dt=np.int32) + 1, "pmap": z(n, W, dt=np.uint8), "pn": z(W, dt=np.int32),
             "pbkt": z(W, dt=np.int32) + 1, "ev": z(self.M, W, dt=np.int32), "evn": z(W),
-            "rnd": np.stack([srand(seed) for seed in (seeds if seeds is not None else [1] * W)])}
+            "rnd": np.stack([srand(seed) for seed in (seeds if seeds is not None else [1] * W)]),
+            "smask": z(2, n, W, dt=np.uint64), "pmask": z(2, W, dt=np.uint64)}
 
     def query(self, park: HostPark, kind: int, a, b, f) -> tuple:
         """One query a world on the host build: (out [1 + N][W], outd [N][W])."""
         from exact_ballpark_b200 import _native
         s = _native.SpaceState()
         s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets = self.W, self.N, self.B, self.D, self.E, self.S
-        s.umap_cap, s.events = self.N, self.M
+        s.umap_cap, s.events, s.lanes = self.N, self.M, 1
         s.rows = self.rows.ctypes.data
         for name, arr in self.st.items():
             setattr(s, name, arr.ctypes.data)
@@ -161,7 +162,7 @@ class HostLayer:
         from exact_ballpark_b200 import _native
         s = _native.SpaceState()
         s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets = self.W, self.N, self.B, self.D, self.E, self.S
-        s.umap_cap, s.events = self.N, self.M
+        s.umap_cap, s.events, s.lanes = self.N, self.M, 1
         s.rows = self.rows.ctypes.data
         for name, arr in self.st.items():
             setattr(s, name, arr.ctypes.data)
@@ -359,7 +360,7 @@ def events_text(st: dict, park_ids, w: int, n: int) -> str:
     return "Q" + "".join(out) + "\n"
 
 
-def drive(streams: list, kernel: str = "host", device=None) -> tuple:
+def drive(streams: list, kernel: str = "host", device=None, lanes: int = 1) -> tuple:
     """Every stream through the layer, one world each, one operation a launch: (texts [world][op], flags [W]); a
     HandleProximities operation's text ends with its events."""
     W = len(streams)
@@ -385,7 +386,8 @@ def drive(streams: list, kernel: str = "host", device=None) -> tuple:
         from exact_ballpark_b200.modes import VecModesPark
         from exact_ballpark_b200.space import VecSpace
         dpark = VecModesPark(W * N, friction=FRICTION, tick_interval_ms=1000, device=device or "cuda")
-        layer = VecSpace(dpark, np.arange(W * N, dtype=np.int64).reshape(W, N), events=N * (N + 2), seed=seeds)
+        layer = VecSpace(dpark, np.arange(W * N, dtype=np.int64).reshape(W, N), events=N * (N + 2), seed=seeds,
+                         lanes=lanes)
 
         def run(code, a, b, f):
             for name in ("pos", "vel", "old_pos", "old_vel", "mass", "time_factor", "radius", "max_vel", "agility",
@@ -440,7 +442,7 @@ def drive(streams: list, kernel: str = "host", device=None) -> tuple:
     return texts, read()["flags"].copy()
 
 
-def drive_ticks(ops, device="cuda", seed: int = 1) -> list:
+def drive_ticks(ops, device="cuda", seed: int = 1, lanes: int = 1) -> list:
     """One ticking or mode stream (tests/golden/space_trace.py's tick_ops and mode_ops) through VecSpace over a
     VecModesPark on the device, its ticks the layer's `tick` (dead bubbles skipped, the re-filings and
     HandleProximities after): the texts after every operation, a tick's and HandleProximities' with their events. The
@@ -452,7 +454,7 @@ def drive_ticks(ops, device="cuda", seed: int = 1) -> list:
     from exact_ballpark_b200.space import OP, VecSpace
     n = int(np.max(np.asarray(ops)[:, 1]))
     park = VecModesPark(n, friction=FRICTION, tick_interval_ms=1000, device=device)
-    layer = VecSpace(park, np.arange(n, dtype=np.int64).reshape(1, n), events=n * (n + 2), seed=seed)
+    layer = VecSpace(park, np.arange(n, dtype=np.int64).reshape(1, n), events=n * (n + 2), seed=seed, lanes=lanes)
     out = []
     dev = park.dev
     for op in ops:

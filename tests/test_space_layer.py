@@ -116,12 +116,14 @@ def test_the_layers_tick_matches_the_oracle_on_the_cpu(family):
 
 
 @pytest.mark.gpu
-def test_the_device_layer_matches_its_host_program_word_for_word():
+@pytest.mark.parametrize("lanes", [1, 32])
+def test_the_device_layer_matches_its_host_program_word_for_word(lanes):
+    """A thread a world and a warp a world (its lanes splitting GetNearbyBalls' scan and sort)."""
     import torch
     assert torch.cuda.is_available()
     scs = _streams()
     streams = _inputs(scs)
-    got, flags = sl.drive(streams, "cuda")
+    got, flags = sl.drive(streams, "cuda", lanes=lanes)
     want, _ = sl.drive(streams, "host")
     assert not (flags & ~HUGE).any()
     bad = [sc["seed"] for sc, g, w in zip(scs, got, want) if g != w]
@@ -131,8 +133,9 @@ def test_the_device_layer_matches_its_host_program_word_for_word():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("lanes", [1, 32])
 @pytest.mark.parametrize("family", ["tick", "modes"])
-def test_the_layers_tick_over_the_flight_park_matches_the_oracle(family):
+def test_the_layers_tick_over_the_flight_park_matches_the_oracle(family, lanes):
     """The ticking streams (GOTO and STOP ships across top boxes and bubbles, with sensors, tracked targets and
     notification ranges) and the mode streams (FollowBall, Orbit, WarpTo with drop-outs, releases, re-added
     followers, sensors): VecSpace.tick over a VecModesPark (the dead bubbles' rows skipped by the park's tick, then
@@ -144,7 +147,7 @@ def test_the_layers_tick_over_the_flight_park_matches_the_oracle(family):
     assert len(scs) == 40
     bad = []
     for sc in scs:
-        got = sl.drive_ticks(sc["ops"], seed=sc["rand_seed"])
+        got = sl.drive_ticks(sc["ops"], seed=sc["rand_seed"], lanes=lanes)
         want = _oracle_texts(sc)
         if got != want:
             bad.append((sc["seed"], next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
@@ -152,13 +155,15 @@ def test_the_layers_tick_over_the_flight_park_matches_the_oracle(family):
 
 
 @pytest.mark.gpu
-def test_the_layers_tick_matches_the_oracle_in_crowded_sensing_worlds():
-    """The crowded worlds (16 to 128 sensing ships) through VecSpace.tick over a VecModesPark on the device."""
+@pytest.mark.parametrize("lanes", [1, 32])
+def test_the_layers_tick_matches_the_oracle_in_crowded_sensing_worlds(lanes):
+    """The crowded worlds (16 to 128 sensing ships) through VecSpace.tick over a VecModesPark on the device, a thread
+    or a warp a world."""
     import torch
     assert torch.cuda.is_available()
     bad = []
     for sc in _crowd():
-        got = sl.drive_ticks(sc["ops"], seed=sc["rand_seed"])
+        got = sl.drive_ticks(sc["ops"], seed=sc["rand_seed"], lanes=lanes)
         want = _oracle_texts(sc)
         if got != want:
             bad.append((sc["seed"], next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
