@@ -33,6 +33,7 @@ from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests" / "golden"))      # the golden streams' operation codes (space_trace)
 
 METRIC = "bit-exact ship-ticks/s on 1 B200 (ragged batch vs plain); serve p50/p99 latency"
 UNIT = "ship-ticks/s"
@@ -543,39 +544,46 @@ def server_pushes(W: int, dev) -> list:
 
 
 def server_cpu_sample(worlds: int, warmup: int, steps: int) -> dict:
-    """The server layer's algorithm on the host (its torch path, the reference's organisation, over the C++ oracle's
-    flight park: oracle/server_view.py) on `worlds` worlds of the benchmark's shape: the 8 pushes, the pre-tick, the
-    park's tick and the send flags each tick; ship-ticks/s."""
-    import torch
+    """The server benchmark's ticks on the host: the C++ flight oracle's park (oracle/park.py, its tick on every core
+    over disjoint worlds) with each tick's pilots' calls applied through its commands (GotoDirection and
+    SetSpeedFraction for every ship, in queue order); the queue's bookkeeping and routing are index work the oracle
+    leaves out. ship-ticks/s on `worlds` worlds."""
+    import numpy as np
 
-    from exact_ballpark_b200 import server
     from oracle.park import OraclePark
-    from oracle.server_view import OracleParkView
     threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-    torch.set_num_threads(threads)
     rows = server_worlds(worlds)
-    park = OracleParkView(OraclePark(len(rows)), threads=threads)
+    park = OraclePark(len(rows))
     park.load(rows)
-    srv = server.VecServer(server.ModesAdapter(park), [x["id"] - 1 for x in rows])
     pushes = server_pushes(worlds, "cpu")
+    n = len(rows)
+    calls = []
+    for k in range(4):
+        mask = np.zeros(n, dtype=bool)
+        mask[k::4] = True
+        d = pushes[2 * k][3].numpy()
+        sf = pushes[2 * k + 1][3].numpy()[:, 0]
+        dirs = np.zeros((n, 3))
+        dirs[k::4] = d
+        fr = np.zeros(n)
+        fr[k::4] = sf
+        calls.append((mask, dirs, fr))
 
     def tick():
-        for kind, mask, ball, f in pushes:
-            srv.push(kind, mask, ball, f=f)
-        srv.pre_tick(snapshot=False)
-        srv.evolve()
-        srv.post_tick()
-    srv.tick()
+        for mask, dirs, fr in calls:
+            park.goto_direction(mask, dirs)
+            park.set_speed_fraction(mask, fr)
+        park.evolve(threads=threads)
     for _ in range(warmup):
         tick()
     t0 = time.perf_counter()
     for _ in range(steps):
         tick()
     dt = time.perf_counter() - t0
-    return {"value": len(rows) * steps / dt, "unit": "ship-ticks/s", "cores": threads, "kind": "port",
-            "sample": f"{worlds} worlds x 4 piloted ships, 8 calls a world a tick, ticks {warmup + 2}..{warmup + steps + 1} "
-                      f"({dt:.1f} s wall): the server layer's torch path on the host ({threads} torch threads) over the "
-                      f"C++ oracle's flight park (its tick on {threads} threads over disjoint worlds)"}
+    return {"value": n * steps / dt, "unit": "ship-ticks/s", "cores": threads, "kind": "port",
+            "sample": f"{worlds} worlds x 4 piloted ships, GotoDirection and SetSpeedFraction a ship a tick, "
+                      f"{steps} ticks after {warmup} ({dt:.1f} s wall): the C++ flight oracle's park with the calls "
+                      f"applied by its commands, its tick on {threads} threads over disjoint worlds"}
 
 
 def space_runs(args, dev) -> dict:
@@ -634,6 +642,54 @@ def space_runs(args, dev) -> dict:
             "layer_ms_per_tick": layer / K, "ship_ticks_per_s": n * K / (whole * 1e-3),
             "layer_share": layer / whole, "dead_rows_last": int(dead.sum()),
             "flagged_worlds": int((space.st["flags"] != 0).sum()), "boxes_max": int(space.st["box_n"].max())}
+
+
+def partition_cpu_sample(pw, worlds: int, ticks: int) -> dict:
+    """The space oracle (oracle/space.cpp: the master's partition, bubbles and sensors over the flight oracle's tick, a
+    sequential C++ restatement of the reference's SpaceBallpark) on every host core, one world a task (ctypes releases
+    the interpreter's lock): `worlds` worlds of the partition workload spread over its sizes, each loaded (AddBall,
+    the sensors), then `ticks` ticks, every ship sent to a goto point along its pilot's direction each tick; the
+    ticks' time is the run's less the load's. The server layer is not in the oracle's tick."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+
+    import space_trace as sp_trace
+    from oracle import space_world
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    pick = np.linspace(0, len(pw.sizes) - 1, worlds).astype(np.int64)
+    c = pw.cols
+    jobs = []
+    for w in pick.tolist():
+        s0, k = int(pw.starts[w]), int(pw.sizes[w])
+        load = [sp_trace._op(sp_trace.ADD, j + 1, c["mass"][s0 + j], c["radius"][s0 + j], c["max_vel"][s0 + j], 1.0,
+                             1.0, *c["pos"][s0 + j], 0.0, 0.0, 0.0, c["agility"][s0 + j], 1.0, 0.0) for j in range(k)]
+        load += [sp_trace._op(sp_trace.SENSOR, j + 1, pw.sensor_range[s0 + j], 1.0, 0.0, 0.0) for j in range(k)]
+        run = list(load)
+        for _ in range(ticks):
+            run += [sp_trace._op(sp_trace.GOTO, j + 1, *(c["pos"][s0 + j] + pw.direction[s0 + j] * 1e9))
+                    for j in range(k)]
+            run.append(sp_trace._op(sp_trace.TICK))
+        jobs.append((np.array(load), np.array(run), w + 1))
+
+    def timed(job, which):
+        t = time.perf_counter()
+        space_world.run_quiet(job[which], seed=job[2])
+        return time.perf_counter() - t
+    with ThreadPoolExecutor(threads) as ex:
+        t0 = time.perf_counter()
+        list(ex.map(lambda j: timed(j, 0), jobs))
+        t_load = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        list(ex.map(lambda j: timed(j, 1), jobs))
+        t_all = time.perf_counter() - t0
+    ships = int(pw.sizes[pick].sum())
+    dt = max(t_all - t_load, 1e-9)
+    return {"value": ships * ticks / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{worlds} of the {len(pw.sizes)} worlds ({ships} ships, sizes spread as the workload's), "
+                      f"{ticks} ticks each after the load ({dt:.1f} s wall of ticks), the space oracle "
+                      f"(oracle/space.cpp) over the flight oracle's tick, {threads} threads over disjoint worlds, "
+                      "no server layer"}
 
 
 def partition_runs(args, dev) -> dict:
@@ -721,6 +777,8 @@ def partition_runs(args, dev) -> dict:
                        "SetSpeedFraction for every ship every tick), dynamical orientation off")
     out["ships"], out["worlds"], out["steps"], out["warmup"] = n, W, K, args.warmup
     del keep
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = partition_cpu_sample(pw, min(W, 400), 5)
     return out
 
 

@@ -485,6 +485,7 @@ __global__ void __launch_bounds__(128) server_kernel(EbbServerState s, EbbServer
             history(x, q, 0, q.slots);
             if (!x.any_interactive()) s.dead[w] = 1;
             break;
+        case 6: queue(x, q); break;                       // the queue's test alone: flags, rows, CloakBall's bubble
         default: break;
     }
 }
@@ -498,7 +499,7 @@ extern "C" {
 
 int ebb_server_tick(const EbbServerState* s, const EbbServerQueue* q, int phase, int64_t j0, int64_t j1, void* stream,
                     int block) {
-    if (s == nullptr || q == nullptr || phase < 0 || phase > 5) return EBB_EINVAL;
+    if (s == nullptr || q == nullptr || phase < 0 || phase > 6) return EBB_EINVAL;
     if (q->slots < 0 || q->slots > EBB_SERVER_MAX_SLOTS || block <= 0 || block > 128 || block % 32 != 0)
         return EBB_EINVAL;
     if (phase == 2 && (j0 < 0 || j1 < j0 || j1 > q->slots)) return EBB_EINVAL;

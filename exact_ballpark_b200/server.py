@@ -1,39 +1,18 @@
-"""The server layer over the flight-mode park on a B200: a drop-in for exact_ballpark.vec_server's VecServer and
-ModesAdapter (exact_ballpark/vec_server.py:197-1080): Destiny's net/server layer batched for many worlds, each world one
-bubble with its pilots.
+"""The server layer over the flight-mode park on a B200: the drop-in for exact_ballpark.vec_server's VecServer,
+ModesAdapter and ServerGraph (exact_ballpark/vec_server.py:197-1292) on their kernel path: Destiny's net/server layer
+(server.py, the scalar transcription: Actions, Ticker, BubbleUpdater, ParkUpdateBatcher) batched for many worlds, each
+world one bubble with its pilots.
 
-Per tick, as Destiny's test helper drives the layer: `push` queues an Actions call for every masked world (TIME-709,
-TIME-710: stamped, and dropped when it equals the world's last queued call — same kind, ball, target, floats by value
-(a NaN equals nothing), ints and the local argument exactly); `pre_tick` moves the stamp, flushes the queue and applies
-every queued call but CloakBall through the park in queue order (the j-th calls of every world together, each world's
-in its own order), updates the bubble's additions (BubbleUpdater: a user ball seen for the first time gets every
-uncloaked ball of its bubble), then walks the history: CloakBall applied there and its event sent to the bubble it
-was queued in, UncloakBall's event to its own character with an AddBallsToPark to every other interactive pilot, a
-local SetBallPosition sent nowhere, every other event to the bubble, or to the ball's character while it is cloaked;
-`evolve` is the park's tick (a world whose bubble is dead at an evolve is refused by `check`); `post_tick` sets, per
-pilot, whether it gets the bubble's narrowcast and a character update (ParkUpdateBatcher.send_batch). `batch` holds the
-tick's update batch as tensors: the stamps, the queued calls, their routes, the uncloaks' recipients, the additions
-and the flags, with the park's fields where the streams would be written (`stream_fields`).
-
-Two paths with one result, bit for bit. kernel="torch": every park write is the park's own command or setter
-(exact_ballpark_b200.modes, on the device) over all worlds at once, one queued call after another; the layer adds only
-index work (masks, gathers, comparisons) and the cloak's float sum radius + range as float32, as the C++ does.
-kernel="cuda": the native library's server kernel (ebb_server_tick), one thread a world walking its own queue, every
-command restated for one row; one launch for the whole pre-tick (or one per history segment when the park's fields are
-recorded for the streams), one for the dead-bubble test before the park's tick (fused into the pre-tick's launch in a
-graph, where nothing comes between them) and one for the send flags after it.
-`ServerGraph` captures a kernel-path tick with a fixed schedule of pushes as one CUDA graph.
-
-The pending queries and the undo of a pending cloak (Actions, _actions.py:686-766) answer from the queue on both paths;
-OnTick's per-world intervals (`on_tick`, the masks of `pre_tick`, `evolve` and `post_tick`) run on both paths.
-
-`decode` turns a batch into what Destiny's network sends each client: its singlecast and the bubble's narrowcast, with
-the events, the AddBallsToPark streams in WriteBallToStream's layout and the packaged additions.
-
-`CollideAdapter` puts the layer over the collision park (torch path). `ClientView` keeps what each pilot's client
-holds, `down` ticks behind the server.
-
-Not built: the orientation and combat parks' adapters, bubbles other than one a world.
+The layer's whole tick runs in the native library's server kernel (ebb_server_tick, one thread a world walking its own
+queue): the Actions queue's stamps and duplicate test (TIME-709, TIME-710: a call equal to the world's last queued call
+is dropped), every queued call applied by the flight park's command restated for one row, BubbleUpdater's additions,
+the history (CloakBall applied there; each event routed to the bubble, to the ball's character while it is cloaked, or
+nowhere; an uncloak's AddBallsToPark recipients), the dead-bubble test before the park's tick, and the send flags after
+it. This module keeps the host's side: the pushed calls until the pre-tick (`push`), the pending queries and the undo
+of a pending cloak between ticks (answered from the kernel's own test of the queue, phase 6), OnTick's per-world
+intervals (`on_tick`), the batch of each tick as tensors (`Batch`), a tick captured as a CUDA graph (`ServerGraph`),
+and what Destiny's network sends each client (`decode`). There is no second implementation: a server over a park the
+kernel does not take is refused.
 """
 
 from __future__ import annotations
@@ -44,188 +23,78 @@ import struct
 from dataclasses import dataclass, field
 from enum import IntEnum
 
+import numpy as np
 import torch
 
 from . import _native
-from .modes import WARP, tick as _park_tick
+from .modes import tick as _park_tick
 
-F64, F32, I64, BOOL = torch.float64, torch.float32, torch.int64, torch.bool
+F64, F32, I64, BOOL, U8 = torch.float64, torch.float32, torch.int64, torch.bool, torch.uint8
 
-# the queued actions by the event the server sends (the index is the kind's code; 0 no action)
+# The queued calls by the event the server sends: a call's code is its event's index here (the layer's interface:
+# the kernel, include/ebb.h's EBB_KIND_*, and a caller's pushes share these codes).
 KINDS = ("", "GotoPoint", "GotoDirection", "Stop", "FollowBall", "Orbit", "WarpTo", "EntityWarpIn", "SetSpeedFraction",
          "SetMaxSpeed", "SetBallMass", "SetBallAgility", "SetBallRadius", "SetBallVelocity", "SetBallMassive",
          "SetBallInteractive", "SetBallPosition", "CloakBall", "UncloakBall", "SetMaxAngularSpeed",
          "SetBallAngularVelocity", "SetBallRotation", "SetBallAngularAgility", "SetMaxAngularVelocity",
          "LaunchMissile", "SetBallTroll", "SetBallFree", "AddBallsToPark", "BallNotGlobal")
 CODE = {name: k for k, name in enumerate(KINDS) if name}
-DYNAMICAL_ONLY = frozenset(CODE[k] for k in ("SetBallAngularVelocity", "SetMaxAngularVelocity", "SetBallRotation",
-                                             "SetBallAngularAgility", "SetMaxAngularSpeed"))
-NONE, BUBBLE, CHARACTER = 0, 1, 2                   # where an event goes
+NONE, BUBBLE, CHARACTER = 0, 1, 2                   # where an event goes (the kernel's EBB_ROUTE_*)
 MAX_CATCH_UP_TICKS = 5                              # OnTick's backlog on the master (Ballpark.cpp:248, TIME-703)
-DSTNORMALCLOAK = 1
-CLOAK, UNCLOAK, SETPOS, INTERACTIVE = CODE["CloakBall"], CODE["UncloakBall"], CODE["SetBallPosition"], \
-    CODE["SetBallInteractive"]
+CLOAK, UNCLOAK, INTERACTIVE, TROLL = CODE["CloakBall"], CODE["UncloakBall"], CODE["SetBallInteractive"], \
+    CODE["SetBallTroll"]
 FOLLOWS = (CODE["FollowBall"], CODE["Orbit"])
-TROLL = CODE["SetBallTroll"]
-# applied by the parks with missiles, and by the partition layer's server: not by the flight park
-NOT_APPLIED = frozenset(CODE[k] for k in ("LaunchMissile", "AddBallsToPark", "BallNotGlobal"))
+# the kinds the flight park takes: every one but the missiles' and the global balls' notices, the turning setters only
+# under dynamical orientation
+_TURNING = frozenset(CODE[k] for k in ("SetBallAngularVelocity", "SetMaxAngularVelocity", "SetBallRotation",
+                                       "SetBallAngularAgility", "SetMaxAngularSpeed"))
+_ELSEWHERE = frozenset(CODE[k] for k in ("LaunchMissile", "AddBallsToPark", "BallNotGlobal"))
 
 
-def _char(x: torch.Tensor) -> torch.Tensor:
-    return ((x.to(I64) + 128) & 0xFF) - 128
-
-
-class _Worlds:
-    """The rows of a park grouped into worlds: `world` [R] (0 .. W-1), `rows_of_world` [W, width] (in the order the
-    balls were added, -1 padded) with `ids_of_world` (0 padded), and the lookups the layer makes."""
-
-    def _index_worlds(self, labels: list) -> None:
-        order, groups = [], {}
-        for r, w in enumerate(labels):
-            if w not in groups:
-                groups[w] = []
-                order.append(w)
-            groups[w].append(r)
-        self.labels, self.W = order, len(order)
-        width = max((len(g) for g in groups.values()), default=0)
-        table = [g + [-1] * (width - len(g)) for g in (groups[w] for w in order)]
-        self.rows_of_world = torch.tensor(table, dtype=I64, device=self.dev).reshape(self.W, width)
-        index = {w: k for k, w in enumerate(order)}
-        self.world = torch.tensor([index[w] for w in labels], dtype=I64, device=self.dev)
-        self._ids_of_rows()
-        self.arange = torch.arange(self.R, device=self.dev)
-
-    def _ids_of_rows(self) -> None:
-        safe = self.rows_of_world.clamp(min=0)
-        self.ids_of_world = torch.where(self.rows_of_world >= 0, self.ids[safe], 0)
-
-    def lookup(self, ball: torch.Tensor) -> torch.Tensor:
-        """Each world's row of the ball whose Destiny id is ball[w], or -1."""
-        hit = self.ids_of_world == ball.to(I64)[:, None]
-        first = hit.to(I64).argmax(dim=1)
-        return torch.where(hit.any(dim=1), self.rows_of_world.gather(1, first[:, None])[:, 0], -1)
-
-    def any_in_world(self, flag: torch.Tensor) -> torch.Tensor:
-        safe = self.rows_of_world.clamp(min=0)
-        return (flag[safe] & (self.rows_of_world >= 0)).any(dim=1)
-
-
-class ModesAdapter(_Worlds):
-    """The flight-mode park (exact_ballpark_b200.VecModesPark) as the server layer sees it: its rows grouped by world
-    label (first appearance order; a world's rows in the order its balls were added, the bubble's dictionary order),
-    the Destiny ids, the flags the layer routes by, and each kind applied through the park's command or setter."""
-
-    master = True
+class ModesAdapter:
+    """The flight-mode park (exact_ballpark_b200.VecModesPark) as the server layer sees it: its rows grouped into
+    worlds by their world label (in order of first appearance; a world's rows in the order its balls were added, the
+    bubble dictionary's order) as a [W, width] table of rows (-1 padding) and of Destiny ids (0 padding), the kinds the
+    park applies, and its fields for the streams."""
 
     def __init__(self, park, master: bool = True):
         self.park, self.R, self.dev, self.master = park, park.n, park.dev, bool(master)
+        labels = park.world.detach().cpu().numpy()
+        _, first, world = np.unique(labels, return_index=True, return_inverse=True)
+        rank = np.argsort(np.argsort(first))                   # worlds numbered by their first row
+        world = rank[world]
+        self.W = int(len(first))
+        counts = np.bincount(world, minlength=self.W)
+        width = int(counts.max(initial=0))
+        order = np.argsort(world, kind="stable")               # rows of a world in row order
+        col = np.arange(self.R) - np.repeat(np.cumsum(counts) - counts, counts)
+        table = np.full((self.W, width), -1, dtype=np.int64)
+        table[world[order], col] = order
+        self.rows_of_world = torch.as_tensor(table, device=self.dev)
+        self.world = torch.as_tensor(world.astype(np.int64), device=self.dev)
         self.ids = park.ids
+        self.ids_of_world = torch.where(self.rows_of_world >= 0, self.ids[self.rows_of_world.clamp(min=0)], 0)
         self.exists = torch.ones(self.R, dtype=BOOL, device=self.dev)
-        self._index_worlds(park.world.tolist())
-        do = park.dynamical_orientation
+        self.arange = torch.arange(self.R, device=self.dev)
+        dynamical = bool(park.dynamical_orientation)
         self.kinds = frozenset(k for k in range(1, len(KINDS))
-                               if (do or k not in DYNAMICAL_ONLY) and k not in NOT_APPLIED)
+                               if k not in _ELSEWHERE and (dynamical or k not in _TURNING))
 
-    interactive = property(lambda s: s.park.interactive, lambda s, v: setattr(s.park, "interactive", v))
-    massive = property(lambda s: s.park.massive, lambda s, v: setattr(s.park, "massive", v))
+    interactive = property(lambda s: s.park.interactive)
+    cloaked = property(lambda s: s.park.cloaked)
 
-    @property
-    def cloaked(self) -> torch.Tensor:
-        return self.park.cloaked
+    def lookup(self, ball: torch.Tensor) -> torch.Tensor:
+        """Each world's row of the ball whose Destiny id is ball[w] (the first listed), or -1."""
+        hit = self.ids_of_world == ball.to(I64)[:, None]
+        at = torch.where(hit.any(dim=1), hit.to(torch.int8).argmax(dim=1), -1)
+        return torch.where(at >= 0, self.rows_of_world.gather(1, at.clamp(min=0)[:, None])[:, 0], -1)
 
-    @cloaked.setter
-    def cloaked(self, v) -> None:
-        self.park.cloaked.copy_(torch.as_tensor(v, device=self.dev))
-
-    def radius(self) -> torch.Tensor:
-        return self.park.radius
+    def any_in_world(self, flag: torch.Tensor) -> torch.Tensor:
+        return (flag[self.rows_of_world.clamp(min=0)] & (self.rows_of_world >= 0)).any(dim=1)
 
     def clock(self) -> torch.Tensor:
         """Each world's mCurrentTime (its rows share one clock)."""
         return self.park.clock[self.rows_of_world[:, 0]]
-
-    def warping(self) -> torch.Tensor:
-        return (self.park.mode == WARP) & (self.park.effect_stamp >= 0)
-
-    def cloak(self, m: torch.Tensor, mode: torch.Tensor, rng: torch.Tensor) -> None:
-        """CloakBall (Ballpark.cpp:5223): refused unless the signed char mode is positive; on the master a normal cloak
-        adds a proximity sensor (unless float(radius) + float(range) < 0); the followers released; cloaked with the
-        mode's byte, non-massive."""
-        mode = _char(mode)
-        ok = m & self.exists & (mode > 0)
-        if self.master:
-            rng32 = rng.to(F64).to(F32).to(F64)
-            sense = ok & (mode == DSTNORMALCLOAK) & ~((self.radius() + rng32).to(F32) < 0.0)
-            self.park.sensor = self.park.sensor | sense
-        self.park._release_followers(ok)
-        self.cloaked = torch.where(ok, mode & 0xFF, self.cloaked)
-        self.massive = torch.where(ok, False, self.massive)
-
-    def uncloak(self, m: torch.Tensor) -> None:
-        """UncloakBall (Ballpark.cpp:5257): a normal cloak's sensor removed (master); uncloaked; massive again unless
-        in warp proper."""
-        ok = m & self.exists
-        if self.master:
-            self.park.sensor = self.park.sensor & ~(ok & (self.cloaked == DSTNORMALCLOAK))
-        self.cloaked = torch.where(ok, 0, self.cloaked)
-        self.massive = torch.where(ok & ~self.warping(), True, self.massive)
-
-    def apply(self, kind: int, m: torch.Tensor, trow: torch.Tensor, f: torch.Tensor, n: torch.Tensor) -> None:
-        """One kind on the rows in m, each row's arguments: the park's own command or setter."""
-        p, name = self.park, KINDS[kind]
-        xyz = f[:, :3].contiguous()
-        one = f[:, 0].contiguous()
-        if name == "GotoPoint":
-            p.goto_point(m, xyz)
-        elif name == "GotoDirection":
-            p.goto_direction(m, xyz)
-        elif name == "Stop":
-            p.stop(m)
-        elif name == "FollowBall":
-            p.follow(m, trow, one)
-        elif name == "Orbit":
-            p.orbit(m, trow, one)
-        elif name == "WarpTo":
-            p.warp_to(m, xyz, f[:, 3].contiguous(), n)
-        elif name == "EntityWarpIn":
-            p.entity_warp_in(m, xyz, n)
-        elif name == "SetSpeedFraction":
-            p.set_speed_fraction(m, one)
-        elif name == "SetMaxSpeed":
-            p.set_max_velocity(m, one)
-        elif name == "SetBallMass":
-            p.set_mass(m, one)
-        elif name == "SetBallAgility":
-            p.set_agility(m, one)
-        elif name == "SetBallRadius":
-            p.set_radius(m, one)
-        elif name == "SetBallVelocity":
-            p.set_velocity(m, xyz)
-        elif name == "SetBallMassive":
-            p.massive = torch.where(m, n != 0, p.massive)
-        elif name == "SetBallInteractive":
-            p.interactive = torch.where(m, n != 0, p.interactive)
-        elif name == "SetBallPosition":                 # the new and old position
-            p.pos = torch.where(m[:, None], xyz, p.pos)
-            p.old_pos = torch.where(m[:, None], xyz, p.old_pos)
-        elif name == "UncloakBall":
-            self.uncloak(m)
-        elif name == "SetMaxAngularSpeed":
-            p.set_max_angular_speed(m, one)
-        elif name == "SetBallAngularVelocity":
-            p.set_angular_velocity(m, xyz)
-        elif name == "SetBallRotation":
-            p.set_rotation(m, f)
-        elif name == "SetBallAngularAgility":
-            p.set_rot_agility(m, one)
-        elif name == "SetMaxAngularVelocity":
-            pass                                        # the park has no such method: never applied
-        elif name == "SetBallTroll":
-            p.set_ball_troll(m, n)
-        elif name == "SetBallFree":                     # a flag != 0 frees
-            p.set_free(m, n)
-        else:
-            raise ValueError(f"{name} is not applied by the flight park's server layer")
 
     def evolve(self, worlds: torch.Tensor | None = None) -> None:
         """The park's tick; `worlds` [W] (OnTick's mask): those worlds' rows alone."""
@@ -235,134 +104,29 @@ class ModesAdapter(_Worlds):
         """The fields WriteBallToStream writes (Thunkers.cpp:3180-3377), every row, copied to the host (a snapshot: later
         writes to the park do not reach it)."""
         p = self.park
-        out = {k: getattr(p, k).detach().to("cpu", copy=True) for k in ("ids", "mode", "radius", "pos", "free", "massive",
-                                                          "interactive", "mass", "cloaked", "max_vel", "vel",
-                                                          "agility", "speed_fraction", "goto", "follow_id",
-                                                          "follow_range", "effect_stamp", "last_collision",
-                                                          "owner_id", "rot", "max_ang_vel", "ang_vel",
-                                                          "rot_agility")}
+        out = {k: getattr(p, k).detach().to("cpu", copy=True)
+               for k in ("ids", "mode", "radius", "pos", "free", "massive", "interactive", "mass", "cloaked", "max_vel",
+                         "vel", "agility", "speed_fraction", "goto", "follow_id", "follow_range", "effect_stamp",
+                         "last_collision", "owner_id", "rot", "max_ang_vel", "ang_vel", "rot_agility")}
         out["dynamical"] = bool(p.dynamical_orientation)
-        return out
-
-
-class CollideAdapter(_Worlds):
-    """The collision park (exact_ballpark_b200.VecCollidePark: W worlds of N slots, GOTO and STOP with Destiny's
-    collisions) as the server layer sees it (vec_server.py:491-580): row w N + slot, a world's balls in its first
-    slots; the park's exists, ids, massive flag and cloak flag (the cloak's mode kept here), the interactive flags
-    kept here (given at the construction, all interactive by default), each world's park time kept here; GotoPoint,
-    GotoDirection, Stop, SetSpeedFraction, SetBallMassive, SetBallInteractive, CloakBall and UncloakBall. A normal
-    cloak's proximity sensor is not modelled by this park. The server kernel does not take this adapter."""
-
-    master = True
-
-    def __init__(self, park, interactive=None, master: bool = True):
-        self.park, self.dev, self.master = park, park.dev, bool(master)
-        W, N = park.W, park.N
-        self.R = W * N
-        self.ids = park.id.reshape(-1)
-        self.exists = park.exists.reshape(-1)
-        self._index_worlds([r // N for r in range(self.R)])
-        self.rows_of_world = torch.where(park.exists, self.rows_of_world, -1)
-        self._ids_of_rows()
-        given = [True] * self.R if interactive is None else [bool(x) for x in interactive]
-        self.interactive = torch.tensor(given, dtype=BOOL, device=self.dev) & self.exists
-        self._cloaked = torch.where(park.cloaked.reshape(-1), 1, 0).to(I64)
-        self.time = torch.full((self.W,), int(park.current_time), dtype=I64, device=self.dev)
-        self.kinds = frozenset(CODE[k] for k in ("GotoPoint", "GotoDirection", "Stop", "SetSpeedFraction",
-                                                  "SetBallMassive", "SetBallInteractive", "CloakBall", "UncloakBall"))
-
-    @property
-    def massive(self) -> torch.Tensor:
-        return self.park.massive.reshape(-1)
-
-    @massive.setter
-    def massive(self, v) -> None:
-        self.park.massive.copy_(torch.as_tensor(v, device=self.dev).reshape(self.park.W, self.park.N))
-
-    @property
-    def cloaked(self) -> torch.Tensor:
-        return self._cloaked
-
-    @cloaked.setter
-    def cloaked(self, v) -> None:
-        self._cloaked = torch.as_tensor(v, device=self.dev).to(I64)
-        self.park.cloaked.copy_((self._cloaked != 0).reshape(self.park.W, self.park.N))
-
-    def radius(self) -> torch.Tensor:
-        return self.park.radius.reshape(-1)
-
-    def clock(self) -> torch.Tensor:
-        return self.time
-
-    def cloak(self, m: torch.Tensor, mode: torch.Tensor, rng: torch.Tensor) -> None:
-        """CloakBall: refused unless the signed char mode is positive; cloaked with the mode's byte, non-massive (no
-        followers and no sensor in this park)."""
-        mode = _char(mode)
-        ok = m & self.exists & (mode > 0)
-        self.cloaked = torch.where(ok, mode & 0xFF, self.cloaked)
-        self.massive = torch.where(ok, False, self.massive)
-
-    def uncloak(self, m: torch.Tensor) -> None:
-        """UncloakBall: uncloaked and massive again (no ball of this park is in warp)."""
-        ok = m & self.exists
-        self.cloaked = torch.where(ok, 0, self.cloaked)
-        self.massive = torch.where(ok, True, self.massive)
-
-    def apply(self, kind: int, m: torch.Tensor, trow: torch.Tensor, f: torch.Tensor, n: torch.Tensor) -> None:
-        p, name, W, N = self.park, KINDS[kind], self.park.W, self.park.N
-        mm = m.reshape(W, N)
-        xyz = f[:, :3].reshape(W, N, 3)
-        if name == "GotoPoint":
-            p.goto_point(mm, xyz)
-        elif name == "GotoDirection":
-            p.goto_direction(mm, xyz)
-        elif name == "Stop":
-            p.stop(mm)
-        elif name == "SetSpeedFraction":
-            p.set_speed_fraction(mm, f[:, 0].reshape(W, N))
-        elif name == "SetBallMassive":
-            self.massive = torch.where(m, n != 0, self.massive)
-        elif name == "SetBallInteractive":
-            self.interactive = torch.where(m & self.exists, n != 0, self.interactive)
-        elif name == "UncloakBall":
-            self.uncloak(m)
-        else:
-            raise ValueError(f"{name} is not applied by the collision park's server layer")
-
-    def evolve(self, worlds: torch.Tensor | None = None) -> None:
-        """The park's tick and each world's park time; `worlds` [W] (OnTick's mask): those worlds alone."""
-        if worlds is None:
-            self.park.evolve()
-            self.time.add_(1)
-            return
-        self.park.evolve(active=worlds)
-        self.time.add_(worlds.to(I64))
-
-    def stream_fields(self) -> dict:
-        p, R = self.park, self.R
-        host = lambda t: t.detach().to("cpu", copy=True)                     # noqa: E731  (a snapshot)
-        zero = torch.zeros(R, dtype=I64)
-        out = {k: host(getattr(p, k).reshape(R, *getattr(p, k).shape[2:]))
-               for k in ("mode", "radius", "pos", "free", "mass", "max_vel", "vel", "agility", "speed_fraction", "goto",
-                         "last_collision")}
-        out.update(ids=host(self.ids), massive=host(self.massive), interactive=host(self.interactive),
-                   cloaked=host(self.cloaked), follow_id=zero, owner_id=zero, effect_stamp=zero,
-                   follow_range=torch.zeros(R, dtype=F64), dynamical=False)
         return out
 
 
 @dataclass
 class Slot:
-    """One push: one Actions call for every masked world."""
+    """One push: one Actions call for every masked world. Before the pre-tick `ok`, `row`, `trow` and `loc` are None
+    (the pushed `mask` and local argument are kept); the pre-tick fills them from the kernel."""
     kind: int
-    ok: torch.Tensor                    # [W] queued
+    ok: torch.Tensor | None             # [W] queued
     ball: torch.Tensor                  # [W] Destiny id
-    row: torch.Tensor                   # [W] the ball's row, or -1
+    row: torch.Tensor | None            # [W] the ball's row, or -1
     target: torch.Tensor                # [W] the target's id (FollowBall, Orbit)
-    trow: torch.Tensor                  # [W] the target's row, or -1
+    trow: torch.Tensor | None           # [W] the target's row, or -1
     f: torch.Tensor                     # [W, 4] the float arguments
     n: torch.Tensor                     # [W] the int argument
     loc: torch.Tensor                   # [W] SetBallPosition: is local; CloakBall: its bubble (0, or -1)
+    mask: torch.Tensor | None = None    # [W] pushed (the kernel's test not yet made)
+    resolved: bool = False              # tested already (by an undo's test): `mask` is the queued flag
 
 
 @dataclass
@@ -379,39 +143,53 @@ class Batch:
     ticked: torch.Tensor | None = None
 
 
-class VecServer:
-    """The server layer over an adapter (the module's docstring): kernel "torch" or "cuda"."""
+@dataclass
+class _Clocks:
+    """OnTick's arithmetic for one call, every world at once (Ballpark.cpp:219-330): `due` a whole interval has passed,
+    `first` its first call, `runs` the intervals to run, `left` the remainder carried."""
+    due: torch.Tensor
+    first: torch.Tensor
+    runs: torch.Tensor
+    resync: torch.Tensor
+    left: torch.Tensor
 
-    def __init__(self, adapter: ModesAdapter, pilots=None, kernel: str = "torch", block: int = 128):
-        if kernel not in ("torch", "cuda"):
-            raise ValueError(f"kernel {kernel!r}: 'torch' or 'cuda'")
+    @staticmethod
+    def of(elapsed: torch.Tensor, interval: int, first_time: torch.Tensor, master: bool) -> "_Clocks":
+        due = elapsed >= interval
+        whole = torch.where(due, torch.div(elapsed, interval, rounding_mode="floor"), 0)
+        resync = due & (whole > MAX_CATCH_UP_TICKS) & master       # the master's backlog: one interval, no remainder
+        left = torch.where(resync, 0, elapsed - whole * interval)
+        whole = torch.where(resync, 1, whole)
+        first = due & first_time
+        return _Clocks(due, first, torch.where(due & ~first, whole, 0), resync, torch.where(due & ~first, left, 0))
+
+
+class VecServer:
+    """The server layer over a ModesAdapter (the module's docstring), run by the server kernel. `pilots` [R]: each
+    row's pilot (its client), -1 for none. `kernel` is "cuda", the only path (kept as the reference's argument)."""
+
+    def __init__(self, adapter: ModesAdapter, pilots=None, kernel: str = "cuda", block: int = 128):
+        if kernel != "cuda":
+            raise ValueError(f"kernel {kernel!r}: the server layer runs on the server kernel ('cuda') only")
+        if not isinstance(adapter, ModesAdapter) or adapter.dev.type != "cuda":
+            raise ValueError("the server kernel runs over the flight park's adapter (ModesAdapter) on a CUDA device")
         self.a = A = adapter
         self.W, self.R, self.dev = A.W, A.R, A.dev
-        self.kernel, self.block = kernel, int(block)
+        self.kernel, self.block = "cuda", int(block)
         self.pilot = (torch.full((self.R,), -1, dtype=I64, device=self.dev) if pilots is None
                       else torch.as_tensor(pilots, dtype=I64).to(self.dev))
         clock = A.clock()
-        self.stamp_for_system = torch.where(clock == 0, 0, clock + 1)     # Actions' first stamp
-        self.settled = torch.zeros(self.R, dtype=BOOL, device=self.dev)   # the old bubble is the bubble
-        self.dead = torch.zeros(self.W, dtype=BOOL, device=self.dev)
+        zb = lambda n: torch.zeros(n, dtype=BOOL, device=self.dev)          # noqa: E731
+        self.stamp_for_system = torch.where(clock == 0, 0, clock + 1)       # Actions' first stamp
+        self.settled = zb(self.R)                                          # the old bubble is the bubble
+        self.dead = zb(self.W)
         self._bubble_time = torch.full((self.W,), -1, dtype=I64, device=self.dev)
-        self._fresh = torch.zeros(self.R, dtype=BOOL, device=self.dev)
-        self._listed = torch.zeros(self.R, dtype=BOOL, device=self.dev)
-        self._seen_first = False
+        self._fresh, self._listed = zb(self.R), zb(self.R)
+        self._seen = zb(self.W)                                            # worlds past their first pre-tick
         self.slots: list = []
-        self._reset_last()
         self.batch: Batch | None = None
         self._q = None
-        if kernel == "cuda":
-            if self.dev.type != "cuda" or not isinstance(adapter, ModesAdapter):
-                raise ValueError("the server kernel runs the flight park's layer (a ModesAdapter) on a CUDA device")
-            self._state = self._server_state()
-
-    def _reset_last(self) -> None:
-        W, d = self.W, self.dev
-        self.last = {"kind": torch.zeros(W, dtype=I64, device=d), "ball": torch.zeros(W, dtype=I64, device=d),
-                     "target": torch.zeros(W, dtype=I64, device=d), "f": torch.zeros(W, 4, dtype=F64, device=d),
-                     "n": torch.zeros(W, dtype=I64, device=d), "loc": torch.zeros(W, dtype=I64, device=d)}
+        self._state = self._server_state()
 
     # ---- the kernel's state and queue (include/ebb.h: EbbServerState, EbbServerQueue) ----
     def _server_state(self) -> _native.ServerState:
@@ -438,14 +216,13 @@ class VecServer:
         """The queue's tensors for kinds [J]: the pushes' columns ([J, W] stacks, given or zeros) and the outputs."""
         J, W, R, d = len(kinds), self.W, self.R, self.dev
         z = lambda *shape, dt=I64: torch.zeros(*shape, dtype=dt, device=d)          # noqa: E731
-        q = {"kinds": torch.tensor(kinds, dtype=torch.int32).to(d), "mask": z(J, W, dt=torch.uint8), "ball": z(J, W),
+        q = {"kinds": torch.tensor(kinds, dtype=torch.int32).to(d), "mask": z(J, W, dt=U8), "ball": z(J, W),
              "target": z(J, W), "f": z(J, W, 4, dt=F64), "n": z(J, W), "loc_in": z(J, W),
              "ok": z(J, W, dt=BOOL), "row": z(J, W), "trow": z(J, W), "loc": z(J, W),
              "route": z(W, J, dt=torch.int8), "notice": z(J, R, dt=BOOL), "stamp": z(W), "clock": z(W),
              "has_character": z(R, dt=BOOL), "gets_bubble": z(R, dt=BOOL)}
-        if cols is not None:
-            for k, v in cols.items():
-                q[k].copy_(v)
+        for k, v in (cols or {}).items():
+            q[k].copy_(v)
         qs = _native.ServerQueue()
         qs.slots = J
         for k in ("kinds", "mask", "ball", "target", "n", "loc_in", "f", "ok", "row", "trow", "loc", "route",
@@ -461,126 +238,82 @@ class VecServer:
                                                int(j0), int(j1), stream, self.block)
         _native.check(rc, "ebb_server_tick")
 
+    def _columns(self, slots: list) -> dict | None:
+        """The pushed calls as the queue's [J, W] columns: the mask byte (bit 0 pushed or queued, bit 1 tested)."""
+        if not slots:
+            return None
+        stack = lambda get: torch.stack([get(s) for s in slots])          # noqa: E731
+        return {"mask": stack(lambda s: s.mask.to(U8) | (2 if s.resolved else 0)), "ball": stack(lambda s: s.ball),
+                "target": stack(lambda s: s.target), "f": stack(lambda s: s.f), "n": stack(lambda s: s.n),
+                "loc_in": stack(lambda s: s.loc)}
+
     # ---- the queue ----
     def push(self, kind, mask, ball, target=None, f=None, n=None, loc=None) -> Slot:
         """An Actions call (a kind's code or event name) for every world in mask [W]: ball [W] ids, target [W] ids
-        (FollowBall, Orbit), f [W, k<=4] floats, n [W] the int argument, loc [W] SetBallPosition's is_local_ball.
-        CloakBall captures the ball's bubble (0, or -1 before its old bubble is its bubble) and is not queued for a
-        ball not in the park; a call equal to the world's last queued call is dropped. On the kernel path the call is
-        recorded as given and tested in the pre-tick's launch (its flags and rows filled in there)."""
+        (FollowBall, Orbit), f [W, k<=4] floats, n [W] the int argument, loc [W] SetBallPosition's is_local_ball. Kept
+        as given; the kernel tests it (the duplicate rule, the rows) in the pre-tick's launch."""
         k = CODE[kind] if isinstance(kind, str) else int(kind)
         if k not in self.a.kinds:
             raise ValueError(f"{KINDS[k] or kind} is not applied by this park")
         W, d = self.W, self.dev
-        z = lambda dt: torch.zeros(W, dtype=dt, device=d)                    # noqa: E731
-        mask = torch.as_tensor(mask).to(device=d, dtype=BOOL)
-        ball = torch.as_tensor(ball).to(device=d, dtype=I64)
-        target = z(I64) if target is None else torch.as_tensor(target).to(device=d, dtype=I64)
+        col = lambda v, dt: (torch.zeros(W, dtype=dt, device=d) if v is None                     # noqa: E731
+                             else torch.as_tensor(v).to(device=d, dtype=dt).reshape(W))
         ff = torch.zeros(W, 4, dtype=F64, device=d)
         if f is not None:
             f = torch.as_tensor(f).to(device=d, dtype=F64).reshape(W, -1)
             ff[:, :f.shape[1]] = f
-        n = z(I64) if n is None else torch.as_tensor(n).to(device=d, dtype=I64)
-        loc = z(I64) if loc is None else torch.as_tensor(loc).to(device=d, dtype=I64)
-        if self.kernel == "cuda":
-            slot = Slot(k, None, ball, None, target, None, ff, n, loc)
-            slot.mask = mask
-            self.slots.append(slot)
-            return slot
-        row = self.a.lookup(ball)
-        trow = self.a.lookup(target) if k in FOLLOWS else z(I64) - 1
-        if k == CLOAK:
-            loc = torch.where(self.settled[row.clamp(min=0)], 0, -1)
-            mask = mask & (row >= 0)
-        last = self.last
-        dup = ((last["kind"] == k) & (last["ball"] == ball) & (last["target"] == target)
-               & (last["f"] == ff).all(dim=1) & (last["n"] == n) & (last["loc"] == loc))
-        ok = mask & ~dup
-        for key, val in (("kind", torch.full((W,), k, dtype=I64, device=d)), ("ball", ball), ("target", target),
-                         ("n", n), ("loc", loc)):
-            last[key] = torch.where(ok, val, last[key])
-        last["f"] = torch.where(ok[:, None], ff, last["f"])
-        slot = Slot(k, ok, ball, row, target, trow, ff, n, loc)
+        slot = Slot(k, None, col(ball, I64), None, col(target, I64), None, ff, col(n, I64), col(loc, I64),
+                    mask=col(mask, BOOL))
         self.slots.append(slot)
         return slot
 
     # ---- the pending queries and the undo of a pending cloak (_actions.py:686-766) ----
     #
-    # Destiny's game code asks the queue between ticks what is pending and may undo a pending cloak. On the torch path
-    # each call was tested at its push; on the kernel path the calls are tested here, in queue order, as the kernel
-    # would test them, and an undo hands the kernel the tested calls (`resolved`: bit 1 of the kernel's mask byte,
-    # bit 0 then the queued flag and `loc` CloakBall's tested bubble) so that it does not test them again.
+    # Destiny's game code asks the queue between ticks what is pending and may undo a pending cloak. The queue is
+    # tested here by the kernel's own test of it (phase 6: the duplicate rule against each world's last queued call,
+    # the rows, CloakBall's bubble; nothing applied), in queue order; an undo hands the tested calls back to the queue
+    # (`resolved`: their mask is their queued flag, which the pre-tick's launch takes as it is) and prunes the cloaks.
 
-    def _deferred(self) -> bool:
-        return self.kernel == "cuda"
+    def _tested(self) -> dict | None:
+        """The pending calls as the kernel tests them: the queue's outputs (ok, row, loc [J, W])."""
+        if not self.slots:
+            return None
+        q = self._queue([s.kind for s in self.slots], self._columns(self.slots))
+        self._launch(q, 6)
+        return q
 
-    def _zero_last(self) -> dict:
-        W, d = self.W, self.dev
-        return {"kind": torch.zeros(W, dtype=I64, device=d), "ball": torch.zeros(W, dtype=I64, device=d),
-                "target": torch.zeros(W, dtype=I64, device=d), "f": torch.zeros(W, 4, dtype=F64, device=d),
-                "n": torch.zeros(W, dtype=I64, device=d), "loc": torch.zeros(W, dtype=I64, device=d)}
-
-    @staticmethod
-    def _become_last(last: dict, s: Slot, queued: torch.Tensor, loc: torch.Tensor) -> None:
-        for key, val in (("kind", torch.full_like(last["kind"], s.kind)), ("ball", s.ball), ("target", s.target),
-                         ("n", s.n), ("loc", loc)):
-            last[key] = torch.where(queued, val, last[key])
-        last["f"] = torch.where(queued[:, None], s.f, last["f"])
-
-    def _test_pending(self, commit: bool = False) -> list:
-        """The kernel path's pending calls tested as the kernel tests them (the resolved prefix taken as it is): each
-        call's queued flag [W]; `commit` makes every call resolved."""
-        last = self._zero_last()
-        out = []
-        for s in self.slots:
-            if getattr(s, "resolved", False):
-                queued, loc = s.mask, s.loc
-            else:
-                row = self.a.lookup(s.ball)
-                queued, loc = s.mask, s.loc
-                if s.kind == CLOAK:
-                    loc = torch.where(self.settled[row.clamp(min=0)], 0, -1)
-                    queued = queued & (row >= 0)
-                dup = ((last["kind"] == s.kind) & (last["ball"] == s.ball) & (last["target"] == s.target)
-                       & (last["f"] == s.f).all(dim=1) & (last["n"] == s.n) & (last["loc"] == loc))
-                queued = queued & ~dup
-            self._become_last(last, s, queued, loc)
-            out.append(queued)
-            if commit:
-                s.mask, s.loc, s.resolved = queued, loc, True
-        return out
-
-    def _queued(self) -> list:
-        return self._test_pending() if self._deferred() else [s.ok for s in self.slots]
+    def _resolve(self) -> None:
+        """Every pending call tested and kept with its queued flag and CloakBall's bubble."""
+        q = self._tested()
+        for j, s in enumerate(self.slots):
+            s.mask, s.loc, s.resolved = q["ok"][j].clone(), q["loc"][j].clone(), True
 
     def _last_pending(self, kind: int, mask, ball) -> tuple:
         """Actions._get_pending_actions for one kind in every world of mask: (found [W], the last such call's slot
         index [W], -1 for none)."""
-        mask = torch.as_tensor(mask).to(device=self.dev, dtype=BOOL)
-        ball = torch.as_tensor(ball).to(device=self.dev, dtype=I64)
-        found = torch.zeros(self.W, dtype=BOOL, device=self.dev)
-        at = torch.full((self.W,), -1, dtype=I64, device=self.dev)
-        for j, (s, queued) in enumerate(zip(self.slots, self._queued())):
-            if s.kind == kind:
-                hit = mask & queued & (s.ball == ball)
-                found = found | hit
-                at = torch.where(hit, j, at)
-        return found, at
+        mask = torch.as_tensor(mask).to(device=self.dev, dtype=BOOL).reshape(self.W)
+        ball = torch.as_tensor(ball).to(device=self.dev, dtype=I64).reshape(self.W)
+        q = self._tested()
+        if q is None:
+            return torch.zeros_like(mask), torch.full((self.W,), -1, dtype=I64, device=self.dev)
+        of_kind = torch.tensor([s.kind == kind for s in self.slots], device=self.dev)[:, None]
+        hit = of_kind & q["ok"] & (q["ball"] == ball[None, :]) & mask[None, :]          # [J, W]
+        J = hit.shape[0]
+        last = torch.where(hit, torch.arange(J, device=self.dev)[:, None], -1).max(dim=0).values
+        return last >= 0, last
 
-    def _pending_value(self, at: torch.Tensor, attr: str, col: int | None = None) -> torch.Tensor:
-        if not self.slots:
-            return torch.zeros(self.W, dtype=F64 if col is not None else I64, device=self.dev)
-        vals = torch.stack([getattr(s, attr) if col is None else getattr(s, attr)[:, col] for s in self.slots])
-        return vals.gather(0, at.clamp(min=0)[None, :])[0]
-
-    def _pending_else_current(self, kind: int, mask, ball, attr: str, col, current: torch.Tensor) -> tuple:
-        """The last pending call's argument as pushed, else the ball's current value, else nothing: (value, known)."""
+    def _pending_else_current(self, kind: int, mask, ball, column, current: torch.Tensor) -> tuple:
+        """The last pending call's argument as pushed (`column(slot)` [W]), else the ball's current value, else
+        nothing: (value [W], known [W])."""
         found, at = self._last_pending(kind, mask, ball)
-        row = self.a.lookup(torch.as_tensor(ball).to(device=self.dev, dtype=I64))
-        pending = self._pending_value(at, attr, col)
-        now = current[row.clamp(min=0)].to(pending.dtype)
-        value = torch.where(found, pending, torch.where(row >= 0, now, torch.zeros_like(pending)))
-        known = torch.as_tensor(mask).to(device=self.dev, dtype=BOOL) & (found | (row >= 0))
+        row = self.a.lookup(torch.as_tensor(ball).to(device=self.dev, dtype=I64).reshape(self.W))
+        now = current[row.clamp(min=0)]
+        if self.slots:
+            pushed = torch.stack([column(s).to(now.dtype) for s in self.slots]).gather(0, at.clamp(min=0)[None, :])[0]
+        else:
+            pushed = torch.zeros_like(now)
+        value = torch.where(found, pushed, torch.where(row >= 0, now, torch.zeros_like(now)))
+        known = torch.as_tensor(mask).to(device=self.dev, dtype=BOOL).reshape(self.W) & (found | (row >= 0))
         return value, known
 
     def has_pending_cloak(self, mask, ball) -> torch.Tensor:
@@ -594,22 +327,25 @@ class VecServer:
     def get_pending_cloak_mode(self, mask, ball) -> tuple:
         """Actions.get_pending_cloak_mode: the last pending CloakBall's mode as pushed, else the ball's cloak byte, else
         None: (value [W] int64, known [W] bool)."""
-        return self._pending_else_current(CLOAK, mask, ball, "n", None, self.a.cloaked)
+        return self._pending_else_current(CLOAK, mask, ball, lambda s: s.n, self.a.cloaked.to(I64))
 
     def get_pending_interactive_state(self, mask, ball) -> tuple:
         """Actions.get_pending_interactive_state: the last pending SetBallInteractive's flag, else the ball's, else
         None: (value [W] bool, known [W] bool)."""
-        value, known = self._pending_else_current(INTERACTIVE, mask, ball, "n", None, self.a.interactive.to(I64))
+        value, known = self._pending_else_current(INTERACTIVE, mask, ball, lambda s: s.n, self.a.interactive.to(I64))
         return value != 0, known
 
     def get_pending_speed_fraction(self, mask, ball) -> tuple:
         """Actions.get_pending_speed_fraction: the last pending SetSpeedFraction's value as pushed, else the ball's
         speed fraction, else None: (value [W] float64, known [W] bool)."""
-        return self._pending_else_current(CODE["SetSpeedFraction"], mask, ball, "f", 0, self.a.park.speed_fraction)
+        return self._pending_else_current(CODE["SetSpeedFraction"], mask, ball, lambda s: s.f[:, 0],
+                                          self.a.park.speed_fraction.to(F64))
 
     def _pending_free(self, mask, ball, value: int) -> tuple:
         found, at = self._last_pending(CODE["SetBallFree"], mask, ball)
-        return found & (self._pending_value(at, "n") == value), found
+        flags = (torch.stack([s.n for s in self.slots]).gather(0, at.clamp(min=0)[None, :])[0] if self.slots
+                 else torch.zeros(self.W, dtype=I64, device=self.dev))
+        return found & (flags == value), found
 
     def has_pending_set_free(self, mask, ball) -> tuple:
         """Actions.has_pending_set_free: whether the last pending SetBallFree's flag is 1: (answer, pending) [W]; where
@@ -622,290 +358,158 @@ class VecServer:
 
     def undo_pending_cloak(self, mask, ball) -> None:
         """Actions.undo_pending_cloak, every world of mask: every pending CloakBall of the ball taken out of the
-        world's queue; the calls pushed later are tested against the queue's last call as it then stands."""
-        mask = torch.as_tensor(mask).to(device=self.dev, dtype=BOOL)
-        ball = torch.as_tensor(ball).to(device=self.dev, dtype=I64)
-        deferred = self._deferred()
-        if deferred:
-            self._test_pending(commit=True)
+        world's queue (the calls pushed later are tested against the queue's last call as it then stands)."""
+        mask = torch.as_tensor(mask).to(device=self.dev, dtype=BOOL).reshape(self.W)
+        ball = torch.as_tensor(ball).to(device=self.dev, dtype=I64).reshape(self.W)
+        if not self.slots:
+            return
+        self._resolve()
         for s in self.slots:
-            if s.kind != CLOAK:
-                continue
-            out = mask & (s.ball == ball)
-            if deferred:
-                s.mask = s.mask & ~out
-            else:
-                s.ok = s.ok & ~out
-        if not deferred:                                  # the torch path's queue: its last call again
-            last = self._zero_last()
-            for s in self.slots:
-                self._become_last(last, s, s.ok, s.loc)
-            self.last = last
+            if s.kind == CLOAK:
+                s.mask = s.mask & ~(mask & (s.ball == ball))
 
-    def _rows(self, slot: Slot) -> tuple:
-        """The call as per-row masks and arguments: a row is commanded iff its world's call is queued for it."""
-        A = self.a
-        w = A.world
-        m = slot.ok[w] & (slot.row[w] == A.arange)
-        return m, slot.trow[w], slot.f[w], slot.n[w]
-
-    # ---- OnTick's per-world mask: the queue split, the last call, a world's first pre-tick ----
-    def _split_queue(self, on: torch.Tensor, flag: str) -> list:
-        """The queue split by the worlds that tick (`on` [W]): each call's flag (`ok` on the torch path, the pushed
-        `mask` on the kernel path) restricted to them for this pre-tick; the calls still held by a world without a
-        tick kept, in queue order, with the flag of those worlds (the calls no world holds dropped)."""
-        slots, self.slots = self.slots, []
-        if not slots:
-            return []
-
-        def restricted(s, keep):
-            t = copy.copy(s)
-            setattr(t, flag, getattr(s, flag) & keep)
-            return t
-        kept = [restricted(s, ~on) for s in slots]
-        held = torch.stack([getattr(s, flag) for s in kept]).any(dim=1).tolist()
-        self.slots = [s for s, h in zip(kept, held) if h]
-        return [restricted(s, on) for s in slots]
-
-    def _keep_last(self, on: torch.Tensor) -> None:
-        """The duplicate test's last call after a masked pre-tick: none for the worlds that ticked, kept for the rest."""
-        zero = self._zero_last()
-        self.last = {k: torch.where(on.reshape(self.W, *([1] * (v.dim() - 1))), zero[k], v)
-                     for k, v in self.last.items()}
-
-    def _first_pre_tick(self, on: torch.Tensor) -> bool:
-        """Whether a world in `on` has its first pre-tick now (its additions' fields are then recorded); every world
-        seen once, the layer's first pre-tick is over."""
-        seen = getattr(self, "_seen_w", None)
-        if seen is None:
-            seen = torch.full((self.W,), bool(self._seen_first), dtype=BOOL, device=self.dev)
-        first, every = torch.stack(((on & ~seen).any(), (seen | on).all())).tolist()
-        self._seen_w = seen | on
-        self._seen_first = bool(every)
-        return bool(first)
-
-    def _snapshot(self, kinds, snapshot, on=None) -> bool:
-        first = (not self._seen_first) if on is None else self._first_pre_tick(on)
-        if on is None:
-            self._seen_first = True
-            if getattr(self, "_seen_w", None) is not None:
-                self._seen_w = torch.ones_like(self._seen_w)
-        if snapshot is None:
-            snapshot = (UNCLOAK in kinds) or (INTERACTIVE in kinds) or (TROLL in kinds) or first
-        return snapshot
-
+    # ---- the tick ----
     def _mask(self, mask):
         return None if mask is None else torch.as_tensor(mask).to(device=self.dev, dtype=BOOL).reshape(self.W)
 
-    # ---- the tick ----
-    def pre_tick(self, snapshot: bool | None = None, mask=None) -> None:
-        """The Ticker's tick (TIME-712): the stamp moves, the queue is flushed and applied (CloakBall after the bubble
-        update), the events routed. `snapshot`: record the park's fields where the streams would be written (by
-        default when an uncloak, a SetBallInteractive, a SetBallTroll or a world's first pre-tick can send one).
-        `mask` [W] (OnTick's): the worlds that tick; every other world keeps its queue, its stamp, its last call and
-        its bubble update's lists, and routes nothing (`Batch.ticked`)."""
-        on = self._mask(mask)
-        if self.kernel == "cuda":
-            return self._pre_tick_kernel(snapshot, on)
-        A = self.a
-        clock = A.clock().clone()
-        stamp = self.stamp_for_system
+    def _take(self, on) -> list:
+        """The calls this pre-tick runs: all (the queue emptied), or with OnTick's mask (`on` [W]) each call for the
+        worlds that tick, the others keeping theirs (tested first, so that they keep them as the kernel tested them)
+        in queue order; a call no world keeps leaves the queue."""
         if on is None:
-            self.stamp_for_system = clock + 1
-            slots, self.slots = self.slots, []
-            self._reset_last()
-        else:
-            self.stamp_for_system = torch.where(on, clock + 1, stamp)
-            slots = self._split_queue(on, "ok")
-            self._keep_last(on)
-        snapshot = self._snapshot({s.kind for s in slots}, snapshot, on)
-        for s in slots:                                     # every queued call but CloakBall, in queue order
-            if s.kind != CLOAK:
-                A.apply(s.kind, *self._rows(s))
-        # BubbleUpdater: the additions once per park time (a second pre-tick at the same time reuses the lists)
-        user = A.interactive & A.exists
-        fresh = user & ~self.settled
-        listed = A.exists & (A.cloaked == 0)
-        fresh = fresh & A.any_in_world(listed)[A.world]
-        again = (clock == self._bubble_time)[A.world]
-        if on is not None:                                  # a world without a tick keeps its lists
-            again = again | ~on[A.world]
-        fresh = torch.where(again, self._fresh, fresh)
-        listed = torch.where(again, self._listed, listed)
-        self.settled = torch.where(again, self.settled, self.settled | user)
-        self._bubble_time = clock if on is None else torch.where(on, clock, self._bubble_time)
-        self._fresh, self._listed = fresh, listed
-        additions = (fresh if on is None else fresh & on[A.world], listed, A.stream_fields() if snapshot else None)
-        live = A.any_in_world(A.interactive & A.exists)
-        route = torch.zeros(self.W, len(slots), dtype=torch.int8, device=self.dev)
-        notices = []
-        for j, s in enumerate(slots):                       # the history
-            valid = s.ok & (s.row >= 0)
-            safe = s.row.clamp(min=0)
-            if s.kind == CLOAK:                             # to the bubble it was queued in; then applied
-                r = torch.where(s.ok & (s.loc == 0), BUBBLE, NONE)
-                m, _, f, n = self._rows(s)
-                A.cloak(m, n, f[:, 0])
-            elif s.kind == UNCLOAK:                         # to its own character; AddBallsToPark to the others
-                own = valid & A.interactive[safe] & (self.pilot[safe] >= 0) & live
-                r = torch.where(own, CHARACTER, NONE)
-                rec = ((valid & live)[A.world] & A.interactive & A.exists & (A.arange != s.row[A.world])
-                       & (self.pilot >= 0))
-                notices.append((j, rec, A.stream_fields() if snapshot else None))
-            elif s.kind == SETPOS:                          # a local ball's move is sent nowhere
-                go = valid & (s.loc == 0) & live
-                r = torch.where(go, torch.where(A.cloaked[safe] == 0, BUBBLE,
-                                                torch.where(self.pilot[safe] >= 0, CHARACTER, NONE)), NONE)
-            else:
-                go = valid & live & (s.ball > 0)
-                r = torch.where(go, torch.where(A.cloaked[safe] == 0, BUBBLE,
-                                                torch.where(self.pilot[safe] >= 0, CHARACTER, NONE)), NONE)
-            route[:, j] = r.to(torch.int8)
-        self.batch = Batch(stamp=stamp, clock=clock, slots=slots, route=route, notices=notices, additions=additions,
-                           ticked=on)
+            taken, self.slots = self.slots, []
+            return taken
+        if not self.slots:
+            return []
+        self._resolve()
+        taken, kept = [], []
+        for s in self.slots:
+            mine = copy.copy(s)
+            mine.mask = s.mask & on
+            taken.append(mine)
+            s.mask = s.mask & ~on
+            kept.append(s)
+        held = torch.stack([s.mask for s in kept]).any(dim=1).tolist()
+        self.slots = [s for s, h in zip(kept, held) if h]
+        return taken
 
-    def _pre_tick_kernel(self, snapshot, on=None) -> None:
-        """The pre-tick as the kernel: one launch, or, with the park's fields recorded, the queue and bubble update,
-        then the history split at each UncloakBall (the fields its notices send are read there). With OnTick's mask
-        the worlds without a tick have no pushed call in the launch (no park write) and get their stamp and bubble
-        update's state back after it."""
-        A = self.a
-        if on is None:
-            slots, self.slots = self.slots, []
-        else:                                               # tested first (as the kernel tests them), so that a
-            self._test_pending(commit=True)                 # world without a tick keeps its queued calls alone
-            slots = self._split_queue(on, "mask")
-            saved = [t.clone() for t in (self.stamp_for_system, self._bubble_time, self.settled, self._fresh,
-                                         self._listed)]
+    def _snapshot(self, kinds: set, snapshot, on) -> bool:
+        """Whether this pre-tick records the park's fields for the streams: as asked, else when a call can send a
+        stream (an uncloak, SetBallInteractive, SetBallTroll) or a ticking world has its first pre-tick (its
+        additions)."""
+        ticking = torch.ones(self.W, dtype=BOOL, device=self.dev) if on is None else on
+        first = bool((ticking & ~self._seen).any())
+        self._seen |= ticking
+        if snapshot is not None:
+            return bool(snapshot)
+        return first or bool(kinds & {UNCLOAK, INTERACTIVE, TROLL})
+
+    def pre_tick(self, snapshot: bool | None = None, mask=None) -> None:
+        """The Ticker's tick (TIME-712) in the kernel: the stamp moves, the queue is tested and applied (CloakBall in the
+        history, after the bubble update), the events routed. `snapshot`: record the park's fields where the streams
+        would be written (by default when a call or a world's first pre-tick can send one); the queue and bubble update
+        then run as one launch and the history as one launch a segment between uncloaks, the park's fields read between
+        them. `mask` [W] (OnTick's): the worlds that tick; every other world keeps its queue, its stamp, its bubble
+        update's lists, and routes nothing (`Batch.ticked`)."""
+        A, on = self.a, self._mask(mask)
+        slots = self._take(on)
         kinds = [s.kind for s in slots]
-        J = len(slots)
         snapshot = self._snapshot(set(kinds), snapshot, on)
-        cols = None
-        if J:
-            cols = {"mask": torch.stack([s.mask.to(torch.uint8) | (2 if getattr(s, "resolved", False) else 0)
-                                         for s in slots]),
-                    "ball": torch.stack([s.ball for s in slots]),
-                    "target": torch.stack([s.target for s in slots]), "f": torch.stack([s.f for s in slots]),
-                    "n": torch.stack([s.n for s in slots]), "loc_in": torch.stack([s.loc for s in slots])}
-        q = self._queue(kinds, cols)
+        if on is not None:
+            before = [t.clone() for t in (self.stamp_for_system, self._bubble_time, self.settled, self._fresh,
+                                          self._listed)]
+        q = self._queue(kinds, self._columns(slots))
         notices, fields = [], None
+        uncloaks = [j for j, k in enumerate(kinds) if k == UNCLOAK]
         if not snapshot:
             self._launch(q, 0)
-            notices = [(j, q["notice"][j], None) for j, k in enumerate(kinds) if k == UNCLOAK]
+            notices = [(j, q["notice"][j], None) for j in uncloaks]
         else:
             self._launch(q, 1)
             fields = A.stream_fields()
-            j0 = 0
-            for j in [j for j, k in enumerate(kinds) if k == UNCLOAK]:
-                self._launch(q, 2, j0, j)
-                notices.append((j, q["notice"][j], A.stream_fields()))
-                j0 = j
-            self._launch(q, 2, j0, J)
-        if on is not None:                                  # the worlds without a tick as they were
-            ron = on[A.world]
+            bounds = [0] + uncloaks + [len(kinds)]
+            for j0, j1 in zip(bounds[:-1], bounds[1:]):
+                self._launch(q, 2, j0, j1)
+                if j1 in uncloaks:
+                    notices.append((j1, q["notice"][j1], A.stream_fields()))
+        if on is not None:                                   # the worlds without a tick as they were
+            rows_on = on[A.world]
             for cur, old, sel in zip((self.stamp_for_system, self._bubble_time, self.settled, self._fresh,
-                                      self._listed), saved, (on, on, ron, ron, ron)):
+                                      self._listed), before, (on, on, rows_on, rows_on, rows_on)):
                 cur.copy_(torch.where(sel, cur, old))
         self._finish(q, slots, notices, fields, on=on)
 
     def _finish(self, q: dict, slots: list, notices: list, fields, live: bool = False, on=None) -> None:
-        """The Batch over the queue's tensors; the additions copied (an eager tick) or the live lists (a graph's)."""
-        for j, s in enumerate(slots):                       # the slots as the torch path holds them
+        """The Batch over the queue's tensors; the additions' lists copied (an eager tick) or the live ones (a
+        graph's)."""
+        for j, s in enumerate(slots):
             s.ok, s.row, s.trow, s.loc = q["ok"][j], q["row"][j], q["trow"][j], q["loc"][j]
         self._q = q
-        lists = (self._fresh, self._listed) if live else (self._fresh.clone(), self._listed.clone())
+        fresh, listed = (self._fresh, self._listed) if live else (self._fresh.clone(), self._listed.clone())
         if on is not None:
-            lists = (lists[0] & on[self.a.world], lists[1])
+            fresh = fresh & on[self.a.world]
         self.batch = Batch(stamp=q["stamp"], clock=q["clock"], slots=slots, route=q["route"], notices=notices,
-                           additions=(*lists, fields),
-                           gets_bubble=q["gets_bubble"], has_character=q["has_character"], ticked=on)
+                           additions=(fresh, listed, fields), gets_bubble=q["gets_bubble"],
+                           has_character=q["has_character"], ticked=on)
 
     def evolve(self, mask=None) -> None:
-        """The park's tick; a world whose bubble is dead is recorded (refused by `check`). `mask` [W] (OnTick's):
-        those worlds alone, every other world's balls and clock kept bit for bit."""
-        A = self.a
-        on = self._mask(mask)
-        if on is not None:
-            self.dead = self.dead | (on & ~A.any_in_world(A.interactive & A.exists))
-            A.evolve(on)
-            return
-        if self.kernel == "cuda":
+        """The park's tick, a world whose bubble has no interactive ball recorded (refused by `check`). `mask` [W]
+        (OnTick's): those worlds alone, every other world's balls and clock kept bit for bit."""
+        A, on = self.a, self._mask(mask)
+        if on is None:
             self._launch(self._q if self._q is not None else self._queue([]), 4)
         else:
-            self.dead = self.dead | ~A.any_in_world(A.interactive & A.exists)
-        A.evolve()
+            self.dead |= on & ~A.any_in_world(A.interactive & A.exists)
+        A.evolve(on)
 
     def post_tick(self, mask=None) -> None:
-        """send_batch: per row (its pilot), whether it gets the bubble's narrowcast and a character update. `mask` [W]
-        (OnTick's; by default the pre-tick's, `Batch.ticked`): the worlds that ticked; the others send nothing."""
+        """send_batch's flags in the kernel: per row (its pilot), whether it gets the bubble's narrowcast and a
+        character update. `mask` [W] (OnTick's; by default the pre-tick's, `Batch.ticked`): the worlds that ticked; the
+        others send nothing."""
         on = self._mask(mask)
         if on is None and self.batch is not None:
             on = self.batch.ticked
-        A = self.a
-        if self.kernel == "cuda":                           # the flags' phase, in place in the batch
-            self._launch(self._q, 3)
-            if on is not None:
-                ron = on[A.world]
-                self._q["has_character"].logical_and_(ron)
-                self._q["gets_bubble"].logical_and_(ron)
-            return
-        b = self.batch
-        bubble = ((b.route == BUBBLE).any(dim=1) if b.route.shape[1]
-                  else torch.zeros(self.W, dtype=BOOL, device=self.dev))
-        has = torch.zeros(self.R, dtype=BOOL, device=self.dev)
-        for j, s in enumerate(b.slots):
-            has = has | (s.ok[A.world] & (s.row[A.world] == A.arange) & (b.route[:, j] == CHARACTER)[A.world])
-        for _, rec, _ in b.notices:
-            has = has | rec
-        has = has | b.additions[0]
-        pilot = self.pilot >= 0
+        self._launch(self._q, 3)
         if on is not None:
-            pilot = pilot & on[A.world]
-        b.has_character = has & pilot
-        b.gets_bubble = bubble[A.world] & A.interactive & A.exists & pilot
+            rows_on = on[self.a.world]
+            self._q["has_character"].logical_and_(rows_on)
+            self._q["gets_bubble"].logical_and_(rows_on)
 
     def on_tick(self, sim_time) -> list:
         """Ballpark::OnTick on the master for every world, each at its own simulation time (sim_time [W], 100 ns
         units; Ballpark.cpp:219-330, TIME-702 to TIME-705), with the Ticker's tick at DoPreTick and send_batch at
-        DoPostTick: less than a whole interval since the world's time, nothing (its time and queue kept); on the master
-        a backlog of more than five intervals cut to one; a world's first call evolves once without the tick's events
-        (its queue kept); every other world runs its whole intervals, each a pre-tick, the park's tick and a
-        post-tick, the worlds with an interval left ticking together under a mask (a round of every world unmasked),
-        the remainder carried in its time. `time` [W] and `first_time` [W] are made at the first call. Returns the
-        batches of the rounds run, in order (a world's sends are in those whose `ticked` holds it); `tick_counts` holds
-        the call's counts."""
+        DoPostTick: less than a whole interval since the world's time does nothing (its time and queue kept); on the
+        master a backlog of more than five intervals is cut to one; a world's first call that holds an interval evolves
+        once without the tick's events (its queue kept); every other world runs its whole intervals, each a pre-tick,
+        the park's tick and a post-tick, the worlds with an interval left ticking together under a mask (a round of
+        every world unmasked), the remainder carried in its time. `time` [W] and `first_time` [W] are made at the first
+        call. Returns the batches of the rounds run, in order (a world's sends are in those whose `ticked` holds it);
+        `tick_counts` holds the call's counts."""
         A, W, d = self.a, self.W, self.dev
         if getattr(self, "time", None) is None:
             self.time = torch.zeros(W, dtype=I64, device=d)
             self.first_time = torch.ones(W, dtype=BOOL, device=d)
         sim = torch.as_tensor(sim_time, dtype=I64).to(d).reshape(W)
         interval = int(round(A.park.dt * 1000.0)) * 10000
-        since = sim - self.time
-        go = ~(since < interval)
-        n = torch.where(go, torch.div(since, interval, rounding_mode="floor"), 0)
-        resync = go & (n > MAX_CATCH_UP_TICKS) & bool(A.master)
-        since = torch.where(resync, interval, since)
-        n = torch.where(resync, 1, n)
-        first = go & self.first_time
-        rest = go & ~first
-        runs = torch.where(rest, n, 0)
-        counts = torch.stack(((~go).sum(), first.sum(), first.all().to(I64), resync.sum(), runs.sum(),
-                              (rest & (since - n * interval > 0)).sum(), runs.max() if W else runs.sum())).tolist()
-        self.tick_counts = {"worlds too early": counts[0], "first calls": counts[1], "resynchronisations": counts[3],
-                            "intervals run": counts[4], "remainders carried": counts[5]}
-        if counts[1]:
-            self.evolve(mask=None if counts[2] else first)
-        self.first_time = self.first_time & ~first
+        c = _Clocks.of(sim - self.time, interval, self.first_time, bool(A.master))
+        stats = torch.stack(((~c.due).sum(), c.first.sum(), c.resync.sum(), c.runs.sum(),
+                             ((c.runs > 0) & (c.left > 0)).sum(), c.runs.max() if W else c.runs.sum(),
+                             c.first.all().to(I64))).tolist()
+        self.tick_counts = dict(zip(("worlds too early", "first calls", "resynchronisations", "intervals run",
+                                     "remainders carried"), stats[:5]))
+        if stats[1]:                                          # a first call: one evolve, no events
+            self.evolve(mask=None if stats[6] else c.first)
+        self.first_time &= ~c.first
         batches = []
-        for k in range(counts[6]):
-            m = rest & (n > k)
-            mm = None if bool(m.all()) else m
-            self.pre_tick(mask=mm)
-            self.evolve(mask=mm)
-            self.post_tick(mask=mm)
+        for k in range(stats[5]):
+            m = c.runs > k
+            whole = None if bool(m.all()) else m
+            self.pre_tick(mask=whole)
+            self.evolve(mask=whole)
+            self.post_tick(mask=whole)
             self.batch.ticked = m
             batches.append(self.batch)
-        self.time = torch.where(go, sim - torch.where(rest, since - n * interval, 0), self.time)
+        self.time = torch.where(c.due, sim - c.left, self.time)
         return batches
 
     def tick(self) -> None:
@@ -921,16 +525,14 @@ class VecServer:
 
 
 class ServerGraph:
-    """A kernel-path VecServer's tick with a fixed schedule of pushes, captured once as a CUDA graph (the drop-in for
+    """A VecServer's tick with a fixed schedule of pushes, captured once as a CUDA graph (the drop-in for
     exact_ballpark.vec_server.ServerGraph, vec_server.py:1200): before each replay the caller writes each push's
     arguments into `inputs[j]` (mask, ball, target, f, n, loc: views of the queue's [J, W] buffers) and `tick()`
-    replays the pre-tick with the dead-bubble test (one launch), the park's tick and the send flags, and returns the graph's
-    Batch (its tensors refilled in place; no park fields recorded). Every state tensor is written in place by its
-    kernel, so nothing is re-bound between replays and eager setters between ticks are seen by the next replay."""
+    replays the pre-tick with the dead-bubble test (one launch), the park's tick and the send flags, and returns the
+    graph's Batch (its tensors refilled in place; no park fields recorded). Every state tensor is written in place by
+    its kernel, so nothing is re-bound between replays and eager setters between ticks are seen by the next replay."""
 
     def __init__(self, server: VecServer, schedule: list):
-        if server.kernel != "cuda":
-            raise ValueError("a ServerGraph captures the kernel path (VecServer(..., kernel='cuda'))")
         if server.slots:
             raise ValueError("pushes are queued: tick them eagerly first")
         self.server = srv = server
@@ -940,26 +542,27 @@ class ServerGraph:
                 raise ValueError(f"{KINDS[k]} is not applied by this park")
         p, d = srv.a.park, srv.dev
         self.q = q = srv._queue(self.schedule)
-        self.inputs = [{"mask": q["mask"][j].view(BOOL), "ball": q["ball"][j], "target": q["target"][j], "f": q["f"][j],
-                        "n": q["n"][j], "loc": q["loc_in"][j]} for j in range(len(self.schedule))]
+        self.inputs = [{"mask": q["mask"][j].view(BOOL), "ball": q["ball"][j], "target": q["target"][j],
+                        "f": q["f"][j], "n": q["n"][j], "loc": q["loc_in"][j]} for j in range(len(self.schedule))]
         if p.plan is None:
             p.scratch()
         else:
             p.plan.tile_rows_on(d)
-        keep = [(t, t.clone()) for t in self._state_tensors()]
-        side = torch.cuda.Stream(device=d)                 # a warm-up of every launch, undone
+        state = self._state_tensors()
+        kept = [t.clone() for t in state]
+        side = torch.cuda.Stream(device=d)                   # a warm-up of every launch, undone
         side.wait_stream(torch.cuda.current_stream(d))
         with torch.cuda.stream(side):
             self._body()
         torch.cuda.current_stream(d).wait_stream(side)
         torch.cuda.synchronize(d)
-        for t, v in keep:
+        for t, v in zip(state, kept):
             t.copy_(v)
-        del keep
+        del kept
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph):
             self._body()
-        srv._seen_first = True
+        srv._seen.fill_(True)
         slots = [Slot(k, None, q["ball"][j], None, q["target"][j], None, q["f"][j], q["n"][j], q["loc_in"][j])
                  for j, k in enumerate(self.schedule)]
         notices = [(j, q["notice"][j], None) for j, k in enumerate(self.schedule) if k == UNCLOAK]
@@ -975,7 +578,7 @@ class ServerGraph:
 
     def _body(self) -> None:
         srv, p = self.server, self.server.a.park
-        srv._launch(self.q, 5)                             # the pre-tick and the dead-bubble test, one launch
+        srv._launch(self.q, 5)                               # the pre-tick and the dead-bubble test, one launch
         _park_tick(p, p.block)
         srv._launch(self.q, 3)
 
@@ -986,56 +589,6 @@ class ServerGraph:
         self.server.a.park.current_time += 1
         self.server.batch = self.out
         return self.out
-
-
-# ================================================================================ what each client holds
-
-class ClientView:
-    """What each pilot's client holds after each tick (vec_server.py:1292-1340): the server's state `down` ticks back (a
-    client applies each update at its stamp, so its park settles `down` ticks behind the server's), kept as a ring of
-    the last `down` + 1 recorded states of the observed fields; another pilot's cloaked ship is absent from a client's
-    park (its CloakBall removed it there), the client's own ship is present, and a client's park holds its own world
-    only. `record(time)` after each server tick; `view()` the state each client holds and its park time."""
-
-    def __init__(self, server: VecServer, down: int, fields: tuple = ("pos", "vel", "mode")):
-        if down < 0:
-            raise ValueError("down: whole ticks, at least 0")
-        self.server, self.down, self.fields = server, int(down), tuple(fields)
-        self.depth = self.down + 1
-        self.ring: dict = {}
-        self.times = torch.full((self.depth,), -1, dtype=I64)
-        self.k = 0
-
-    def _field(self, name: str) -> torch.Tensor:
-        a = self.server.a
-        if name == "cloaked":
-            return a.cloaked
-        t = getattr(a.park, name)
-        return t.reshape(a.R, *t.shape[2:]) if isinstance(a, CollideAdapter) else t
-
-    def record(self, time: int) -> None:
-        """Keep the server's state at park time `time` (the time the park has reached)."""
-        slot = self.k % self.depth
-        for name in self.fields + ("cloaked",):
-            t = self._field(name)
-            if name not in self.ring:
-                self.ring[name] = torch.zeros((self.depth, *t.shape), dtype=t.dtype, device=t.device)
-            self.ring[name][slot].copy_(t)
-        self.times[slot] = int(time)
-        self.k += 1
-
-    def view(self) -> tuple:
-        """(time, {field: [R, ...]}, present [R, R]: row r is in the park of the pilot whose ship is row c), the state
-        `down` ticks before the latest recorded one; time -1 (and nothing) until that state was recorded."""
-        if self.k <= self.down:
-            return -1, {}, None
-        slot = (self.k - 1 - self.down) % self.depth
-        out = {name: self.ring[name][slot] for name in self.fields}
-        cloaked = self.ring["cloaked"][slot]
-        a = self.server.a
-        own_world = a.world[:, None] == a.world[None, :]
-        mine = torch.eye(a.R, dtype=BOOL, device=cloaked.device)
-        return int(self.times[slot]), out, own_world & ((cloaked == 0)[:, None] | mine)
 
 
 # ================================================================================ the batches as Destiny sends them

@@ -376,7 +376,8 @@ int ebb_composed_file(const EbbComposedState* s, const uint8_t* mask, const doub
  * bubble update; 2: the history over slots [j0, j1) (routes, CloakBall applied, the uncloaks' recipients), so that the
  * host can read the park between segments; 3: the send flags (after the park's tick); 4: a bubble without an
  * interactive ball recorded as dead (before the park's tick); 5: phase 0 then phase 4 (a tick whose park tick
- * follows the pre-tick directly). Returns -1 for a bad argument (J outside
+ * follows the pre-tick directly); 6: the queue's test alone (each call's queued flag, rows and CloakBall's bubble,
+ * nothing applied: what the pending queries read between ticks). Returns -1 for a bad argument (J outside
  * [0, EBB_SERVER_MAX_SLOTS], a bad phase, range or block), else a cudaError_t. Replaces xbpv_pre_tick
  * (exact_ballpark/vec_server_cuda.cu:615), which exact_ballpark.vec_server_cuda.launch calls (vec_server_cuda.py:307),
  * and VecServer.evolve's dead-bubble test (vec_server.py:1021). */

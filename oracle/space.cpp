@@ -1426,7 +1426,8 @@ extern "C" {
 // R<ball>:<inside>, DoTargetTracking T<ball>:<inside>), 19 SetNotificationRange (id, range), 20 SetTargetTracking (id,
 // target, range), 21 GotoPoint (id, x, y, z), 22 Stop (id), 23 a tick (its answer HandleProximities' events), 24
 // FollowBall (id, target, range), 25 Orbit (id, target, range), 26 WarpTo (id, x, y, z, min range, warp factor).
-// AddBall's sixteenth value is its massive flag. `seed` is the world's srand seed.
+// AddBall's sixteenth value is its massive flag. `seed` is the world's srand seed. A negative `cap` runs the operations
+// without writing any text (the CPU baseline's timed runs).
 int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double friction, double dt, int64_t seed,
                          char* out, int64_t cap) {
     space_oracle::World w;
@@ -1504,6 +1505,7 @@ int64_t oracle_space_run(const double* ops, int64_t n, int64_t stride, double fr
             case 9: w.keep_alive_balls.insert(id); break;
             default: break;
         }
+        if (cap < 0) continue;                             // timed runs: the operations alone, no texts
         all += w.state();
         all += answer;
         all += '\x1e';

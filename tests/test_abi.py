@@ -52,7 +52,7 @@ def test_the_server_tick_refuses_bad_arguments_before_launching():
     call = lambda phase, j0=0, j1=0, block=128: lib.ebb_server_tick(ctypes.byref(s), ctypes.byref(q), phase, j0,  # noqa: E731
                                                                      j1, None, block)
     assert call(0) == 0                                   # no worlds: nothing to do
-    assert call(6) == -1 and call(-1) == -1               # no such phase
+    assert call(7) == -1 and call(-1) == -1               # no such phase
     assert call(0, block=100) == -1 and call(0, block=256) == -1
     q.slots = 257
     assert call(0) == -1                                  # more than EBB_SERVER_MAX_SLOTS

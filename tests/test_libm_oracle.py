@@ -25,3 +25,18 @@ def test_a_planted_fault_is_caught():
     got = libm("sin", z["sin_x"])
     got[17] = np.nextafter(got[17], np.inf)
     assert not bit_equal(got, z["sin_y"]).all()
+
+
+@pytest.mark.parametrize("fn", ("expf", "logf", "sinf", "cosf", "acosf", "atanf"))
+def test_oracle_float_libm_matches_the_exhaustive_digests_on_two_chunks(fn):
+    """Two of the 256 exhaustive chunks (the arguments 0x3f000000-0x3fffffff, [0.5, 2), and their negatives) through
+    the oracle's libm, hashed as the reference's were (the whole range runs on the device, tests/test_gpu_libm.py)."""
+    from golden_util import f32_digest
+    path = GOLDEN / "libm_f32_digests.npz"
+    z = np.load(path) if path.exists() else {}
+    if fn not in z:
+        pytest.skip(f"no exhaustive digests of {fn} recorded")
+    for c in (63, 191):
+        bits = np.arange(c << 24, (c + 1) << 24, dtype=np.uint64).astype(np.uint32)
+        y = libm(fn, bits.view(np.float32).astype(np.float64))
+        assert f32_digest(bits, y) == z[fn][c], (fn, c)
