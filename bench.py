@@ -714,7 +714,7 @@ def partition_runs(args, dev) -> dict:
     runs = {}
     for name, ragged in (("ragged", True), ("plain", False)):
         t0 = time.time()
-        r = partition_setup(pw, dev, ragged)            # exact_ballpark_b200.partition
+        r = partition_setup(pw, dev, ragged, warp_class=args.partition_warp_class)   # exact_ballpark_b200.partition
         setup_s = time.time() - t0
         g = r["graph"]
         for _ in range(args.warmup):
@@ -926,6 +926,8 @@ def main() -> None:
     ap.add_argument("--space-steps", type=int, default=5)
     ap.add_argument("--partition-worlds", type=int, default=100000)
     ap.add_argument("--partition-steps", type=int, default=10)
+    ap.add_argument("--partition-warp-class", type=int, default=32,
+                    help="the ragged batch's size classes from this size up run a warp a world (129: none)")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-seconds", type=float, default=6.0)
     ap.add_argument("--serve-budget-gb", type=float, default=80.0)

@@ -997,6 +997,12 @@ struct World {
             p->radius[r] = radius;
             insert_in_boxes(j, x, v);
         }
+#ifdef __CUDA_ARCH__
+        if (lane >= 0) {
+            sensor_events_warp(j, r, cand, nc);
+            return;
+        }
+#endif
         const UMap m = sensor_map(j);
         if (*m.len > 0) {
             uint64_t near[2] = {0, 0};
@@ -1030,6 +1036,71 @@ struct World {
             if (!p->sensor[r]) break;
         }
     }
+#ifdef __CUDA_ARCH__
+    // check_sensor's events in a warp: the lanes read the list's keys and test 32 of them (then 32 candidates) at a
+    // time, a ballot naming the ones that change; those are applied one after another in their order, every lane
+    // together (a candidate's membership is its own: the changes before it leave it as it was)
+    __device__ void sensor_events_warp(int64_t j, int64_t r, const uint8_t* cand, int nc) {
+        const UMap m = sensor_map(j);
+        uint64_t near[2] = {0, 0};
+        for (int i = 0; i < nc; ++i) near[cand[i] >> 6] |= uint64_t(1) << (cand[i] & 63);
+        const int32_t n0 = *m.len;
+        if (n0 > 0) {
+            uint8_t* keys = sh->out;
+            for (int32_t e = lane; e < n0; e += 32) keys[e] = m.k[e * m.step];
+            __syncwarp();
+            for (int32_t base = 0; base < n0; base += 32) {
+                bool gone = false;
+                if (base + lane < n0) {
+                    const int64_t k = keys[base + lane];
+                    gone = k != j && !((near[k >> 6] >> (k & 63)) & 1);
+                }
+                unsigned bits = __ballot_sync(0xffffffffu, gone);
+                while (bits) {
+                    const int b = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    const int64_t k = keys[base + b];
+                    umap_erase(m, k);
+                    event(EBB_SPACE_EV_PROXIMITY, j, k, 0);
+                }
+            }
+            __syncwarp();
+        }
+        const float range = (float)at(s->srange, j), rb = p->radius[r];
+        const double xj[3] = {pos(j, 0), pos(j, 1), pos(j, 2)};
+        for (int base = 0; base < nc; base += 32) {
+            int act = 0;                                  // 1 enters, 2 leaves
+            if (base + lane < nc) {
+                const int64_t o = cand[base + lane];
+                if (o != j) {
+                    const bool inside = umap_has(m, o);
+                    const double ck = (double)fadd(fadd(range, p->radius[row(o)]), rb);
+                    const double d0 = dsub(xj[0], pos(o, 0)), d1 = dsub(xj[1], pos(o, 1)), d2 = dsub(xj[2], pos(o, 2));
+                    const double len2 = dadd(dadd(dmul(d0, d0), dmul(d1, d1)), dmul(d2, d2));
+                    if (len2 > dmul(ck, ck)) {
+                        if (inside) act = 2;
+                    } else if (!inside) {
+                        act = 1;
+                    }
+                }
+            }
+            unsigned bits = __ballot_sync(0xffffffffu, act != 0);
+            const unsigned enter = __ballot_sync(0xffffffffu, act == 1);
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                const int64_t o = cand[base + b];
+                if ((enter >> b) & 1) {
+                    umap_insert(m, o, F_SENSOR_LIST);
+                    event(EBB_SPACE_EV_PROXIMITY, j, o, 1);
+                } else {
+                    umap_erase(m, o);
+                    event(EBB_SPACE_EV_PROXIMITY, j, o, 0);
+                }
+            }
+        }
+    }
+#endif
     EBB_HD void check_for_proximity(int64_t j) {
         check_notification_range(j);
         check_target_tracking(j);

@@ -39,7 +39,7 @@ class PartitionLayer:
     multiple of the class's slots (plus 64)."""
 
     def __init__(self, park: VecModesPark, sizes, ragged: bool = True, events: int | None = None,
-                 boxes_per_slot: int = 16, seed: int = 1):
+                 boxes_per_slot: int = 16, seed: int = 1, warp_class: int = WARP_CLASS):
         self.park = park
         sizes = np.asarray(sizes, dtype=np.int64)
         if sizes.ndim != 1 or (sizes < 1).any() or sizes.max(initial=0) > CLASSES[-1]:
@@ -66,7 +66,7 @@ class PartitionLayer:
             slots[:] = np.where(col < k[:, None], starts[idx][:, None] + col, -1)
             layer = VecSpace(park, slots, boxes=boxes_per_slot * cap + 64,
                              events=cap * (cap + 2) if events is None else int(events), umap_cap=cap,
-                             seed=(idx + seed).tolist(), lanes=32 if ragged and cap >= WARP_CLASS else 1)
+                             seed=(idx + seed).tolist(), lanes=32 if ragged and cap >= warp_class else 1)
             self.layers.append((layer, idx))
         self.last_dead = None
 
@@ -190,7 +190,7 @@ class PartitionGraph:
         self.part.park.current_time += 1
 
 
-def partition_setup(pw, dev, ragged: bool, server_on: bool = True) -> dict:
+def partition_setup(pw, dev, ragged: bool, server_on: bool = True, warp_class: int = WARP_CLASS) -> dict:
     """A flight park of the partition worlds with the partition layer (ragged size classes, or the plain 128-slot
     layout), every ship's sensor added, and the server layer on top (a pilot a ship, GotoDirection and
     SetSpeedFraction queued for every ship every tick: a fixed schedule of 2 x 128 pushes, a world's pushes masked to
@@ -199,7 +199,7 @@ def partition_setup(pw, dev, ragged: bool, server_on: bool = True) -> dict:
     from .modes import tick_plain, tick_tiled
     park = VecModesPark(pw.n, device=dev)
     park.load_columns(pw.cols)
-    part = PartitionLayer(park, pw.sizes, ragged=ragged)
+    part = PartitionLayer(park, pw.sizes, ragged=ragged, warp_class=warp_class)
     part.load()
     part.add_sensors(pw.sensor_range, 1.0)
     park_tick = (lambda: tick_tiled(park)) if ragged else (lambda: tick_plain(park, park.block))
