@@ -158,33 +158,27 @@ def reduce_max(x: float, dist, device) -> float:
 
 
 def run_reference(args, rank: int) -> None:
-    """The reference arm: the CPU port of the reference's algorithm on the whole workload, host cores, rank 0."""
+    """The reference arm: the reference's algorithm on the host's cores (the space oracle, oracle/space.cpp, its
+    compiled restatement; the reference's own implementation is Python), on the headline's workload and metric, rank 0
+    only: a bounded sample of the partition worlds (up to 2,000 worlds spread over the sizes) loaded and ticked W times,
+    then K ticks timed; ship-ticks/s over the sample."""
     if rank != 0:
         return
-    from exact_ballpark_b200.workloads import flight_worlds
-    from oracle.park import OraclePark
-    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-    w = flight_worlds(1, args.worlds, args.ships)
-    p = OraclePark(len(w.rows), dynamical_orientation=True, use_new_orbit=True)
-    p.load(w.rows)
-    w.apply(p)
-    for _ in range(args.warmup):
-        p.evolve(threads=threads)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        p.evolve(threads=threads)
-    dt = time.perf_counter() - t0
-    value = len(w.rows) * args.steps / dt
-    sample = (f"{args.worlds} worlds x {args.ships} ships, {args.steps} ticks after {args.warmup}; the reference's "
-              f"algorithm as the C++ oracle (its implementation is Python), {threads} host threads")
+    from exact_ballpark_b200.workloads import partition_worlds
+    pw = partition_worlds(11, args.partition_worlds)
+    sample = partition_cpu_sample(pw, min(args.partition_worlds, 2000), args.steps, warm=args.warmup)
+    value = sample["value"]
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": pw.n / value * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32",
-            "data": "synthetic (seeded)", "config": _config(args, "CPU port of the reference algorithm"),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic (seeded)",
+            "config": {"workload": (f"partition worlds: {args.partition_worlds} worlds of 1-128 ships, sensors, "
+                                    "bubbles and the partition (the headline's); a bounded sample timed, ms_per_step "
+                                    "the whole workload's at the sample's rate"),
+                       "worlds_per_rank": args.partition_worlds, "parallelism": "host cores"},
+            "cpu_baseline": dict(sample), "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                                  "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
 
 def serve_runs(args, dev) -> dict:
     """The serving loop (exact_ballpark_b200.serving) on this GPU: an open loop of episodes arriving as a Poisson
@@ -644,12 +638,13 @@ def space_runs(args, dev) -> dict:
             "flagged_worlds": int((space.st["flags"] != 0).sum()), "boxes_max": int(space.st["box_n"].max())}
 
 
-def partition_cpu_sample(pw, worlds: int, ticks: int) -> dict:
+def partition_cpu_sample(pw, worlds: int, ticks: int, warm: int = 0) -> dict:
     """The space oracle (oracle/space.cpp: the master's partition, bubbles and sensors over the flight oracle's tick, a
     sequential C++ restatement of the reference's SpaceBallpark) on every host core, one world a task (ctypes releases
     the interpreter's lock): `worlds` worlds of the partition workload spread over its sizes, each loaded (AddBall,
-    the sensors), then `ticks` ticks, every ship sent to a goto point along its pilot's direction each tick; the
-    ticks' time is the run's less the load's. The server layer is not in the oracle's tick."""
+    the sensors) and ticked `warm` times, then `ticks` ticks more, every ship sent to a goto point along its pilot's
+    direction each tick; the timed ticks' time is the longer run's less the shorter's. The server layer is not in the
+    oracle's tick."""
     from concurrent.futures import ThreadPoolExecutor
 
     import numpy as np
@@ -662,34 +657,29 @@ def partition_cpu_sample(pw, worlds: int, ticks: int) -> dict:
     jobs = []
     for w in pick.tolist():
         s0, k = int(pw.starts[w]), int(pw.sizes[w])
-        load = [sp_trace._op(sp_trace.ADD, j + 1, c["mass"][s0 + j], c["radius"][s0 + j], c["max_vel"][s0 + j], 1.0,
-                             1.0, *c["pos"][s0 + j], 0.0, 0.0, 0.0, c["agility"][s0 + j], 1.0, 0.0) for j in range(k)]
-        load += [sp_trace._op(sp_trace.SENSOR, j + 1, pw.sensor_range[s0 + j], 1.0, 0.0, 0.0) for j in range(k)]
-        run = list(load)
-        for _ in range(ticks):
-            run += [sp_trace._op(sp_trace.GOTO, j + 1, *(c["pos"][s0 + j] + pw.direction[s0 + j] * 1e9))
-                    for j in range(k)]
-            run.append(sp_trace._op(sp_trace.TICK))
-        jobs.append((np.array(load), np.array(run), w + 1))
+        ops = [sp_trace._op(sp_trace.ADD, j + 1, c["mass"][s0 + j], c["radius"][s0 + j], c["max_vel"][s0 + j], 1.0,
+                            1.0, *c["pos"][s0 + j], 0.0, 0.0, 0.0, c["agility"][s0 + j], 1.0, 0.0) for j in range(k)]
+        ops += [sp_trace._op(sp_trace.SENSOR, j + 1, pw.sensor_range[s0 + j], 1.0, 0.0, 0.0) for j in range(k)]
+        per_tick = [sp_trace._op(sp_trace.GOTO, j + 1, *(c["pos"][s0 + j] + pw.direction[s0 + j] * 1e9))
+                    for j in range(k)] + [sp_trace._op(sp_trace.TICK)]
+        jobs.append((np.array(ops + per_tick * warm), np.array(ops + per_tick * (warm + ticks)), w + 1))
 
     def timed(job, which):
-        t = time.perf_counter()
         space_world.run_quiet(job[which], seed=job[2])
-        return time.perf_counter() - t
     with ThreadPoolExecutor(threads) as ex:
         t0 = time.perf_counter()
         list(ex.map(lambda j: timed(j, 0), jobs))
-        t_load = time.perf_counter() - t0
+        t_short = time.perf_counter() - t0
         t0 = time.perf_counter()
         list(ex.map(lambda j: timed(j, 1), jobs))
-        t_all = time.perf_counter() - t0
+        t_long = time.perf_counter() - t0
     ships = int(pw.sizes[pick].sum())
-    dt = max(t_all - t_load, 1e-9)
-    return {"value": ships * ticks / dt, "unit": UNIT, "cores": threads, "kind": "port",
+    dt = max(t_long - t_short, 1e-9)
+    return {"value": ships * ticks / dt, "unit": UNIT, "cores": threads, "kind": "port", "seconds": dt,
             "sample": f"{worlds} of the {len(pw.sizes)} worlds ({ships} ships, sizes spread as the workload's), "
-                      f"{ticks} ticks each after the load ({dt:.1f} s wall of ticks), the space oracle "
-                      f"(oracle/space.cpp) over the flight oracle's tick, {threads} threads over disjoint worlds, "
-                      "no server layer"}
+                      f"{ticks} ticks each after the load and {warm} ticks ({dt:.2f} s wall of timed ticks), the "
+                      f"space oracle (oracle/space.cpp) over the flight oracle's tick, {threads} threads over "
+                      "disjoint worlds, no server layer"}
 
 
 def partition_runs(args, dev) -> dict:
@@ -889,6 +879,163 @@ def server_runs(args, dev) -> dict:
             **({} if args.no_cpu_baseline else {"cpu_baseline": server_cpu_sample(16384, 3, 100)})}
 
 
+# Algorithmic bytes of one ship's tick in the partition layer's re-filings and HandleProximities (the layer's
+# dominant launches): the ship's filing read and written (level, key, side, active neighbours, its box and top entries:
+# 10 x 8 B each way), its position, velocity and old position read (72), its bubble and seq (16), its row, id, mode
+# and the park's flags (8 + 8 + 4 + 4), radius and the flight values of the inflated radius (mass, decay factor,
+# agility, speed fraction, max velocity: 8 + 8 + 4 x 4 + 4), its sensor's range, period and elapsed time (24, the
+# elapsed time written back 8), its proximity flags (4), its sensor list's length and bucket count (8), and each
+# candidate a sensing ship meets counted once for the world (its filing, position and radius: 96 + 24 + 4, in the
+# ship's own share).
+PARTITION_BYTES_PER_SHIP_TICK = 2 * 80 + 72 + 16 + 24 + 36 + 24 + 8 + 4 + 8 + 124
+
+
+def partition_headline(args, dev, dist, rank: int, world_size: int, barrier, max_over_ranks) -> dict:
+    """The metric's own line: the partition worlds (workloads.partition_worlds: --partition-worlds ragged worlds of
+    1-128 ships a rank, sensors on every ship, bubbles and the partition, the server layer on top), the ragged batch's
+    captured tick (the layer in size classes ordered by size, the large ones a warp a world; the park's tiled schedule)
+    timed against the plain per-configuration layout's (one 128-slot layout in world order, a thread a world; the
+    park's plain schedule) on the same GPU, both replayed K times after W warm-up ticks, CUDA events on the launching
+    stream, L2 flushed before each step, max over ranks; both must end bit-identical. `e2e` runs the ragged tick
+    through the public API from host buffers: every step each ship's pilot's GotoDirection and SetSpeedFraction
+    arguments copied in from pinned memory and scattered into the server's queue, the tick, and every world's event
+    count and every row's two send flags copied back, double-buffered over a copy stream."""
+    import torch
+
+    from exact_ballpark_b200.partition import partition_setup
+    from exact_ballpark_b200.workloads import partition_worlds
+    W, K = args.partition_worlds, args.steps
+    pw = partition_worlds(11 + rank, W)
+    n = pw.n
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(step, k: int) -> float:
+        total = 0.0
+        for _ in range(k):
+            flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step()
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total
+
+    out = {}
+    plain = partition_setup(pw, dev, ragged=False)
+    for _ in range(args.warmup):
+        plain["graph"].tick()
+    barrier()
+    ms_plain = max_over_ranks(timed(plain["graph"].tick, K))
+    plain_park, plain_ev = plain["park"], plain["part"].event_counts()
+    plain_state = {k: getattr(plain_park, "_" + k).clone() for k in ("pos", "vel", "mode", "clock")}
+    plain_layout = [[layer.N, layer.W, layer.lanes] for layer, _ in plain["part"].layers]
+    del plain, plain_park
+    torch.cuda.empty_cache()
+    r = partition_setup(pw, dev, ragged=True, warp_class=args.partition_warp_class)
+    g, part, park = r["graph"], r["part"], r["park"]
+    for _ in range(args.warmup):
+        g.tick()
+    barrier()
+    with Clocks(dev.index or 0) as clk:
+        barrier()
+        ms_ragged = max_over_ranks(timed(g.tick, K))
+        barrier()
+    clocks = clk.summary()
+    same = all(torch.equal(getattr(park, "_" + k), v) for k, v in plain_state.items())
+    same = same and torch.equal(part.event_counts(), plain_ev)
+    del plain_state
+    # the dominant launches, eager, each timed alone: every layer's re-filings and HandleProximities
+    launch_ms = {}
+    for layer, _ in part.layers:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.fill_(1)
+        a.record(stream)
+        layer.after_evolve(None)
+        b.record(stream)
+        b.synchronize()
+        launch_ms[f"{layer.N}_slots_{'warp' if layer.lanes == 32 else 'thread'}"] = a.elapsed_time(b)
+    layer_ms = sum(launch_ms.values())
+    # e2e: the pilots' arguments in, the events and send flags out
+    q, srv = r["q"], r["server"]
+    sizes = torch.as_tensor(pw.sizes, device=dev)
+    world = torch.repeat_interleave(torch.arange(W, device=dev), sizes)
+    k_in = torch.arange(n, device=dev) - torch.repeat_interleave(torch.as_tensor(pw.starts, device=dev), sizes)
+    at_dir, at_sf = (2 * k_in) * W + world, (2 * k_in + 1) * W + world
+    qf = q["f"].view(-1, 4)
+    cmd_host = torch.empty(n, 4, dtype=torch.float64, pin_memory=True)
+    cmd_host[:, :3] = torch.from_numpy(pw.direction)
+    cmd_host[:, 3] = torch.from_numpy(pw.speed)
+    cmd_slot = [torch.empty(n, 4, dtype=torch.float64, device=dev) for _ in range(2)]
+    res_slot = [torch.empty(W * 8 + 2 * n, dtype=torch.uint8, device=dev) for _ in range(2)]
+    res_host = [torch.empty(W * 8 + 2 * n, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+
+    def send(t, s_):
+        cmd_slot[s_].copy_(cmd_host, non_blocking=True)
+
+    def run(t, s_):
+        qf[at_dir, :3] = cmd_slot[s_][:, :3]
+        qf[at_sf, 0] = cmd_slot[s_][:, 3]
+        g.tick()
+        res_slot[s_][:W * 8].view(torch.int64).copy_(part.event_counts())
+        res_slot[s_][W * 8:W * 8 + n].copy_(q["has_character"].view(torch.uint8))
+        res_slot[s_][W * 8 + n:].copy_(q["gets_bubble"].view(torch.uint8))
+
+    def fetch(t, s_):
+        res_host[s_].copy_(res_slot[s_], non_blocking=True)
+
+    pipelined(dev, 3, send, run, fetch)
+    barrier()
+    ms_e2e = max_over_ranks(pipelined(dev, K, send, run, fetch))
+    total = n * world_size
+    peak, peak_kind = _peaks()
+    achieved = PARTITION_BYTES_PER_SHIP_TICK * n / (layer_ms / 1e3) / 1e9
+    part.check()
+    out.update({
+        "value": total * K / (ms_ragged / 1e3), "ms_per_step": ms_ragged / K,
+        "plain": {"value": total * K / (ms_plain / 1e3), "ms_per_step": ms_plain / K, "layout": plain_layout,
+                  "schedule": "the plain per-configuration layout: one 128-slot layer, worlds in their order, a "
+                              "thread a world; the park's plain schedule; the same server layer; one CUDA graph"},
+        "speedup_ragged_vs_plain": ms_plain / ms_ragged, "bit_identical_ragged_vs_plain": bool(same),
+        "ragged_layout": [[layer.N, layer.W, layer.lanes] for layer, _ in part.layers],
+        "layer_launch_ms": launch_ms, "layer_share": layer_ms / (ms_ragged / K),
+        "roofline": {"bound": "hbm", "kernel": "the space layer's re-filings and HandleProximities (tape kernels, "
+                                                "a launch a size class)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_kind": peak_kind,
+                     "note": f"algorithmic {PARTITION_BYTES_PER_SHIP_TICK} B/ship-tick x {n} ships over the layer "
+                             "launches' summed CUDA-event time (eager, L2 flushed); a sequential program a world "
+                             "(dependent loads through the box table and the unordered maps): latency-bound"},
+        "e2e": {"value": total * K / (ms_e2e / 1e3), "unit": UNIT, "ms_per_step": ms_e2e / K,
+                "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": W * 8 + 2 * n,
+                "pipeline": "double-buffered: step t+1's pilots' arguments in and step t-1's event counts and send "
+                            "flags out on a copy stream during step t's tick; timed over all steps; inputs larger "
+                            "than L2, no flush"},
+        "clocks": clocks, "ships_per_rank": n, "worlds_per_rank": W,
+        "events_last_tick": int(part.event_counts().sum()), "flagged_worlds": int((part.flags() != 0).sum()),
+        "gpu_launches": K * (2 + 3 + 2 * len(part.layers))})
+    del r, g, part, park, q, srv
+    torch.cuda.empty_cache()
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = partition_cpu_sample(pw, min(W, 400), 5, warm=2)
+        out["compute"] = op_counts("partition", 2000, 5)
+    return out
+
+
+def op_counts(workload: str, worlds: int, ticks: int) -> dict | None:
+    """FLOPs per ship-tick of a workload, counted by the counting build in a process of its own
+    (exact_ballpark_b200.opcount with EBB_COUNTING=1), or None when that build is missing."""
+    if not (ROOT / "exact_ballpark_b200" / "libebb_count.so").exists():
+        return None
+    env = dict(os.environ, EBB_COUNTING="1")
+    r = subprocess.run([sys.executable, "-m", "exact_ballpark_b200.opcount", workload, "--worlds", str(worlds),
+                        "--ticks", str(ticks)], capture_output=True, text=True, env=env, cwd=str(ROOT), timeout=600)
+    if r.returncode != 0:
+        return {"error": r.stderr[-300:]}
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
 def _config(args, schedule: str) -> dict:
     return {"workload": (f"flight-mode park, dynamical orientation on, new orbit law: {args.worlds} worlds x "
                          f"{args.ships} ships (follow / orbit / warp), per-rank"),
@@ -896,11 +1043,126 @@ def _config(args, schedule: str) -> dict:
             "parallelism": f"replicas x{args.gpus}", "l2": "flushed between timed steps (256 MiB write, untimed)"}
 
 
+def flight_runs(args, dev, rank: int, world_size: int, barrier, max_over_ranks) -> dict:
+    """The flight-mode park's benchmark shape (config 0's distributions at --worlds worlds x --ships ships a rank,
+    dynamical orientation on): the tiled schedule's CUDA graph (autotuned) against the plain schedule, CUDA events, L2
+    flushed before each step, max over ranks; `e2e` through the public API (speed fractions in, positions out,
+    double-buffered); the HBM roofline of the tiled launch and the FLOPs per ship-tick."""
+    import torch
+
+    from exact_ballpark_b200 import ModesGraph, VecModesPark, tick_plain
+    from exact_ballpark_b200.autotune import autotune
+    from exact_ballpark_b200.workloads import flight_worlds
+    w = flight_worlds(rank + 1, args.worlds, args.ships)
+    n = len(w.rows)
+    park = VecModesPark(n, device=dev, dynamical_orientation=True, use_new_orbit=True)
+    park.load(w.rows)
+    w.apply(park)
+    plain = VecModesPark(n, device=dev, dynamical_orientation=True, use_new_orbit=True)
+    plain.load(w.rows)
+    w.apply(plain)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(step, k: int) -> float:
+        total = 0.0
+        for _ in range(k):
+            flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step()
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total
+
+    for _ in range(args.warmup):                                     # warm-up ticks
+        park.evolve()
+        tick_plain(plain, 256)
+        plain.current_time += 1
+    tuning = autotune(park)                                          # the tiled plan, the park's state unchanged
+    plan = park.plan
+    graph = ModesGraph(park)
+    barrier()
+    with Clocks(dev.index or 0) as clk:
+        barrier()
+        ms_tiled = timed(graph.tick, args.flight_steps)
+        barrier()
+        ms_plain = timed(lambda: tick_plain(plain, 256), args.flight_steps)
+        barrier()
+    clocks = clk.summary()
+    ms_tiled, ms_plain = max_over_ranks(ms_tiled), max_over_ranks(ms_plain)
+    per_tiled, per_plain = ms_tiled / args.flight_steps, ms_plain / args.flight_steps
+
+    # e2e through the public API from host buffers: each step's speed fractions in, each step's positions out,
+    # double-buffered over a copy stream
+    every = torch.ones(n, dtype=torch.bool, device=dev)
+    sf_host = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    sf_host.copy_(park.speed_fraction.cpu())
+    sf_slot = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(2)]
+    pos_slot = [torch.empty(3, n, dtype=torch.float64, device=dev) for _ in range(2)]
+    pos_host = [torch.empty(3, n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+
+    def send(t, s):
+        sf_slot[s].copy_(sf_host, non_blocking=True)
+
+    def run(t, s):
+        park.set_speed_fraction(every, sf_slot[s])
+        graph.tick()
+        pos_slot[s].copy_(park._pos)                                 # the positions as stored: x, y, z planes
+
+    def fetch(t, s):
+        pos_host[s].copy_(pos_slot[s], non_blocking=True)
+
+    pipelined(dev, 3, send, run, fetch)
+    barrier()
+    ms_e2e = max_over_ranks(pipelined(dev, args.flight_steps, send, run, fetch))
+    h2d, d2h = n * 8, n * 24
+
+    total_ships = n * world_size
+    value = total_ships * args.flight_steps / (ms_tiled / 1e3)
+    peak, peak_kind = _peaks()
+    achieved = BYTES_PER_SHIP_TICK * n / (per_tiled / 1e3) / 1e9
+    traffic = None
+    tp = ROOT / "profiles" / "flight_tiled_traffic.json"
+    if tp.exists():
+        try:
+            t = json.loads(tp.read_text())
+            traffic = float(t["dram_bytes_per_ship_tick"]) * n
+        except Exception:
+            traffic = None
+    line = {"value": value, "unit": UNIT, "ms_per_step": per_tiled,
+            "config": dict(_config(args, "tiled: worlds packed in tiles, one block a tile, records in shared memory, "
+                                         "warp-cooperative torque searches, one launch, CUDA graph"),
+                           plan={"tile_rows_max": plan.cap, "block": plan.block, "grid": plan.grid, "tiles": plan.tiles,
+                                 "candidates_timed": len(tuning)}),
+            "plain": {"value": total_ships * args.flight_steps / (ms_plain / 1e3), "ms_per_step": per_plain,
+                      "schedule": "plain: records pass + tick, two launches, records in scratch, 256-thread blocks"},
+            "speedup_tiled_vs_plain": per_plain / per_tiled,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "note": (f"algorithmic {BYTES_PER_SHIP_TICK} B/ship-tick x {n} ships per launch over the "
+                                  "tiled launch's CUDA-event time; the tick is FP64/FP32 issue- and latency-bound "
+                                  "(divides, square roots, libm, divergent torque searches), not HBM-bound")},
+            "e2e": {"value": total_ships * args.flight_steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.flight_steps,
+                    "pipeline": "double-buffered: step t+1's speed fractions in and step t-1's positions out on a "
+                                "copy stream during step t's tick (SetSpeedFraction, the graph's tick); timed over "
+                                "all steps; the park's state (131 MB) larger than L2, no flush"},
+            "gpu_launches": 3 * args.flight_steps, "clocks": clocks}
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(args.worlds, args.ships, args.warmup, args.flight_steps)
+        line["compute"] = op_counts("flight", 4096, 10)
+    del graph
+    return line
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10, help="timed steps of the headline (the partition worlds' tick)")
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--flight-steps", type=int, default=200, help="timed steps of the flight-mode section")
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--worlds", type=int, default=65536)
     ap.add_argument("--ships", type=int, default=4)
@@ -953,9 +1215,6 @@ def main() -> None:
 
     import torch
 
-    from exact_ballpark_b200 import ModesGraph, VecModesPark, tick_plain
-    from exact_ballpark_b200.autotune import autotune
-    from exact_ballpark_b200.workloads import flight_worlds
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -977,29 +1236,6 @@ def main() -> None:
         dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300),
                                 device_id=dev)
 
-    w = flight_worlds(rank + 1, args.worlds, args.ships)
-    n = len(w.rows)
-    park = VecModesPark(n, device=dev, dynamical_orientation=True, use_new_orbit=True)
-    park.load(w.rows)
-    w.apply(park)
-    plain = VecModesPark(n, device=dev, dynamical_orientation=True, use_new_orbit=True)
-    plain.load(w.rows)
-    w.apply(plain)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    stream = torch.cuda.current_stream(dev)
-
-    def timed(step, k: int) -> float:
-        total = 0.0
-        for _ in range(k):
-            flush.fill_(1)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            step()
-            b.record(stream)
-            b.synchronize()
-            total += a.elapsed_time(b)
-        return total
-
     def barrier():
         torch.cuda.synchronize(dev)
         if dist is not None:
@@ -1008,82 +1244,26 @@ def main() -> None:
     def max_over_ranks(x: float) -> float:
         return reduce_max(x, dist, dev)
 
-    for _ in range(args.warmup):                                     # warm-up ticks
-        park.evolve()
-        tick_plain(plain, 256)
-        plain.current_time += 1
-    tuning = autotune(park)                                          # the tiled plan, the park's state unchanged
-    plan = park.plan
-    graph = ModesGraph(park)
-    barrier()
-    with Clocks(local) as clk:
-        barrier()
-        ms_tiled = timed(graph.tick, args.steps)
-        barrier()
-        ms_plain = timed(lambda: tick_plain(plain, 256), args.steps)
-        barrier()
-    clocks = clk.summary()
-    ms_tiled, ms_plain = max_over_ranks(ms_tiled), max_over_ranks(ms_plain)
-    per_tiled, per_plain = ms_tiled / args.steps, ms_plain / args.steps
-
-    # e2e through the public API from host buffers: each step's speed fractions in, each step's positions out,
-    # double-buffered over a copy stream
-    every = torch.ones(n, dtype=torch.bool, device=dev)
-    sf_host = torch.empty(n, dtype=torch.float64, pin_memory=True)
-    sf_host.copy_(park.speed_fraction.cpu())
-    sf_slot = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(2)]
-    pos_slot = [torch.empty(3, n, dtype=torch.float64, device=dev) for _ in range(2)]
-    pos_host = [torch.empty(3, n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
-
-    def send(t, s):
-        sf_slot[s].copy_(sf_host, non_blocking=True)
-
-    def run(t, s):
-        park.set_speed_fraction(every, sf_slot[s])
-        graph.tick()
-        pos_slot[s].copy_(park._pos)                                 # the positions as stored: x, y, z planes
-
-    def fetch(t, s):
-        pos_host[s].copy_(pos_slot[s], non_blocking=True)
-
-    pipelined(dev, 3, send, run, fetch)
-    barrier()
-    ms_e2e = max_over_ranks(pipelined(dev, args.steps, send, run, fetch))
-    h2d, d2h = n * 8, n * 24
-
-    total_ships = n * world_size
-    value = total_ships * args.steps / (ms_tiled / 1e3)
-    peak, peak_kind = _peaks()
-    achieved = BYTES_PER_SHIP_TICK * n / (per_tiled / 1e3) / 1e9
-    traffic = None
-    tp = ROOT / "profiles" / "flight_tiled_traffic.json"
-    if tp.exists():
-        try:
-            t = json.loads(tp.read_text())
-            traffic = float(t["dram_bytes_per_ship_tick"]) * n
-        except Exception:
-            traffic = None
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": per_tiled, "higher_is_better": True, "scaling": "weak",
+    head = partition_headline(args, dev, dist, rank, world_size, barrier, max_over_ranks)
+    rest = {k: v for k, v in head.items() if k not in ("value", "ms_per_step", "roofline", "e2e", "clocks",
+                                                      "gpu_launches", "cpu_baseline")}
+    line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64/f32", "data": "synthetic (seeded)",
-            "config": dict(_config(args, "tiled: worlds packed in tiles, one block a tile, records in shared memory, "
-                                         "warp-cooperative torque searches, one launch, CUDA graph"),
-                           plan={"tile_rows_max": plan.cap, "block": plan.block, "grid": plan.grid, "tiles": plan.tiles,
-                                 "candidates_timed": len(tuning)}),
-            "plain": {"value": total_ships * args.steps / (ms_plain / 1e3), "ms_per_step": per_plain,
-                      "schedule": "plain: records pass + tick, two launches, records in scratch, 256-thread blocks"},
-            "speedup_tiled_vs_plain": per_plain / per_tiled,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_kind": peak_kind,
-                         "note": (f"algorithmic {BYTES_PER_SHIP_TICK} B/ship-tick x {n} ships per launch over the "
-                                  "tiled launch's CUDA-event time; the tick is FP64/FP32 issue- and latency-bound "
-                                  "(divides, square roots, libm, divergent torque searches), not HBM-bound")},
-            "e2e": {"value": total_ships * args.steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps,
-                    "pipeline": "double-buffered: step t+1's speed fractions in and step t-1's positions out on a "
-                                "copy stream during step t's tick (SetSpeedFraction, the graph's tick); timed over "
-                                "all steps; the park's state (131 MB) larger than L2, no flush"},
-            "gpu_launches": 3 * args.steps, "clocks": clocks}
+            "config": {"workload": (f"partition worlds (the metric's ragged batch): {args.partition_worlds} worlds a "
+                                    "rank of 1-128 ships (log-uniform) in 1-5 Gaussian blobs (sigma 10 km), a "
+                                    "proximity sensor of 1-250 km on every ship, bubbles and the spatial partition, "
+                                    "the server layer on top (GotoDirection and SetSpeedFraction for every ship every "
+                                    "tick), dynamical orientation off; the ragged persistent graph (size classes, "
+                                    "the large ones a warp a world) against the plain per-configuration layout"),
+                       "worlds_per_rank": args.partition_worlds, "ships_per_rank": head["ships_per_rank"],
+                       "max_ships": 128, "parallelism": f"replicas x{world_size}",
+                       "l2": "flushed between timed steps (256 MiB write, untimed)"},
+            "roofline": head["roofline"], "e2e": head["e2e"], "gpu_launches": head["gpu_launches"],
+            "clocks": head["clocks"], "partition": rest}
+    if "cpu_baseline" in head:
+        line["cpu_baseline"] = head["cpu_baseline"]
+    line["flight"] = flight_runs(args, dev, rank, world_size, barrier, max_over_ranks)
     if not args.no_ragged:
         line["ragged"] = ragged_runs(args, dev)
     if not args.no_collide:
@@ -1096,11 +1276,8 @@ def main() -> None:
         line["server"] = server_runs(args, dev)
     if not args.no_serve:
         line["serve"] = serve_runs(args, dev)
-        line["serve"]["plain_ship_ticks_per_s"] = line["plain"]["value"] / world_size
-    if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_sample(args.worlds, args.ships, args.warmup, args.steps)
+        line["serve"]["plain_ship_ticks_per_s"] = line["flight"]["plain"]["value"] / world_size
     if dist is not None:
-        del graph
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)

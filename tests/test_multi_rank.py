@@ -50,7 +50,7 @@ def test_the_reference_arm_under_torchrun_prints_one_line():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
            "127.0.0.1", "--master-port", str(port), str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2",
-           "--steps", "2", "--warmup", "3", "--worlds", "64"]
+           "--steps", "2", "--warmup", "3", "--partition-worlds", "200"]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=str(ROOT),
                        env=dict(os.environ, OMP_NUM_THREADS="1"))
     assert r.returncode == 0, r.stderr[-2000:]
