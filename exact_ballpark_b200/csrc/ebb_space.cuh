@@ -104,7 +104,12 @@ struct World {
         h ^= (uint64_t)kz * 0x165667B19E3779F9ull + (h << 6) + (h >> 2);
         h ^= (uint64_t)level * 0x27D4EB2F165667C5ull;
         h ^= h >> 29;
-        return (int64_t)(h % (uint64_t)(2 * B));
+        // the slot: the high word of h x 2B (a multiply in place of a 64-bit remainder: the same spread over [0, 2B))
+#ifdef __CUDA_ARCH__
+        return (int64_t)__umul64hi(h, (uint64_t)(2 * B));
+#else
+        return (int64_t)(((unsigned __int128)h * (uint64_t)(2 * B)) >> 64);
+#endif
     }
     EBB_HD bool is_box(int64_t e, int level, int64_t kx, int64_t ky, int64_t kz) const {
         return I(s->box_level, e) == level && I3(s->box_key, 0, e, B) == kx && I3(s->box_key, 1, e, B) == ky &&
@@ -701,14 +706,40 @@ struct World {
     }
 
 #ifdef __CUDA_ARCH__
+    // A bitonic sort of the warp's scratch (sh->key, sh->id, carrying sh->out) by (key, id), every slot of the table
+    // (EBB_SPACE_MAX_SLOTS, a power of two), the lanes taking the pairs of each stage
+    __device__ void warp_sort() const {
+        for (int k = 2; k <= EBB_SPACE_MAX_SLOTS; k <<= 1)
+            for (int jj = k >> 1; jj > 0; jj >>= 1) {
+                for (int i = lane; i < EBB_SPACE_MAX_SLOTS; i += 32) {
+                    const int x = i ^ jj;
+                    if (x <= i) continue;
+                    const int64_t ki = sh->key[i], kx = sh->key[x], ii = sh->id[i], ix = sh->id[x];
+                    const bool x_less = kx < ki || (kx == ki && ix < ii);
+                    const bool x_more = kx > ki || (kx == ki && ix > ii);
+                    if (((i & k) == 0) ? x_less : x_more) {
+                        sh->key[i] = kx;
+                        sh->key[x] = ki;
+                        sh->id[i] = ix;
+                        sh->id[x] = ii;
+                        const uint8_t t = sh->out[i];
+                        sh->out[i] = sh->out[x];
+                        sh->out[x] = t;
+                    }
+                }
+                __syncwarp();
+            }
+    }
+
     // nearby's warp form: each lane takes the slots lane, lane + 32, ...: the filter and the walk key (NOT_A_CANDIDATE
-    // for a ball that is none), then each candidate's place in the walk's order is the number of candidates before it
-    // by (key, id) (ids are distinct, so the places are too); every lane reads the order back
+    // for a ball that is none), then a bitonic sort of the slots by (key, id) over the lanes (ids are distinct, so
+    // the order is the serial insertion's); every lane reads the order back
     __device__ int nearby_warp(int64_t b, int64_t bub, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked,
                                uint8_t* out) const {
-        for (int64_t o = lane; o < N; o += 32) {
-            int64_t k = NOT_A_CANDIDATE, i = 0;
-            if (o != b && slot_ok(o) && U(s->in_park, o) && lvl(o) >= 0) {
+        int mine = 0;
+        for (int64_t o = lane; o < EBB_SPACE_MAX_SLOTS; o += 32) {
+            int64_t k = NOT_A_CANDIDATE, i = INT64_MAX;
+            if (o < N && o != b && slot_ok(o) && U(s->in_park, o) && lvl(o) >= 0) {
                 k = walk_key(b, o);
                 const int64_t r = row(o);
                 if (k != NOT_A_CANDIDATE) {
@@ -718,28 +749,17 @@ struct World {
                     else
                         keep = keep && I(s->bubble, o) == bub && !(exclude_fixed && !p->free_[r]);
                     if (!keep) k = NOT_A_CANDIDATE;
-                    i = p->ids[r];
+                    else i = p->ids[r];
                 }
             }
+            mine += k != NOT_A_CANDIDATE;
             sh->key[o] = k;
             sh->id[o] = i;
-        }
-        __syncwarp();
-        int mine = 0;
-        for (int64_t o = lane; o < N; o += 32) {
-            const int64_t k = sh->key[o];
-            if (k == NOT_A_CANDIDATE) continue;
-            const int64_t i = sh->id[o];
-            int place = 0;
-            for (int64_t c = 0; c < N; ++c) {
-                const int64_t kc = sh->key[c];
-                place += (kc < k || (kc == k && sh->id[c] < i)) ? 1 : 0;
-            }
-            sh->out[place] = (uint8_t)o;
-            ++mine;
+            sh->out[o] = (uint8_t)o;
         }
         const int n = (int)__reduce_add_sync(0xffffffffu, (unsigned)mine);
         __syncwarp();
+        warp_sort();
         for (int i = 0; i < n; ++i) out[i] = sh->out[i];
         __syncwarp();
         return n;
@@ -772,7 +792,10 @@ struct World {
         m.m[0] = 0;
         m.m[m.mstep] = 0;
     }
-    EBB_HD uint64_t bucket_of(int64_t slot, int32_t bkt) const { return (uint64_t)id(slot) % (uint64_t)bkt; }
+    EBB_HD uint64_t bucket_of(int64_t slot, int32_t bkt) const {
+        const uint64_t k = (uint64_t)id(slot);             // (a 32-bit remainder for the ids that fit in one)
+        return (k >> 32) == 0 ? (uint64_t)((uint32_t)k % (uint32_t)bkt) : k % (uint64_t)bkt;
+    }
     EBB_HD int32_t umap_find(const UMap& m, int64_t slot) const {
         const int32_t n = *m.len;
         for (int32_t e = 0; e < n; ++e)
@@ -1343,14 +1366,33 @@ struct World {
     EBB_HDNI void after_evolve() {
         int64_t order[EBB_SPACE_MAX_SLOTS];
         int64_t n = 0;
-        for (int64_t j = 0; j < N; ++j)
-            if (U(s->in_park, j) && slot_ok(j)) order[n++] = j;
-        for (int64_t i = 1; i < n; ++i)
-            for (int64_t k = i; k > 0 && id(order[k]) < id(order[k - 1]); --k) {
-                const int64_t t = order[k];
-                order[k] = order[k - 1];
-                order[k - 1] = t;
+#ifdef __CUDA_ARCH__
+        if (lane >= 0) {                                   // the lanes sort the slots by id together
+            int mine = 0;
+            for (int64_t j = lane; j < EBB_SPACE_MAX_SLOTS; j += 32) {
+                const bool in = j < N && U(s->in_park, j) && slot_ok(j);
+                sh->key[j] = in ? 0 : NOT_A_CANDIDATE;
+                sh->id[j] = in ? id(j) : INT64_MAX;
+                sh->out[j] = (uint8_t)j;
+                mine += in;
             }
+            n = (int64_t)__reduce_add_sync(0xffffffffu, (unsigned)mine);
+            __syncwarp();
+            warp_sort();
+            for (int64_t i = 0; i < n; ++i) order[i] = sh->out[i];
+            __syncwarp();
+        } else
+#endif
+        {
+            for (int64_t j = 0; j < N; ++j)
+                if (U(s->in_park, j) && slot_ok(j)) order[n++] = j;
+            for (int64_t i = 1; i < n; ++i)
+                for (int64_t k = i; k > 0 && id(order[k]) < id(order[k - 1]); --k) {
+                    const int64_t t = order[k];
+                    order[k] = order[k - 1];
+                    order[k - 1] = t;
+                }
+        }
         for (int64_t i = 0; i < n; ++i) {
             const int64_t j = order[i], r = row(j);
             if (!U(s->dropped, j) || U(s->dead, j) || !p->free_[r]) continue;
