@@ -220,6 +220,72 @@ def serve_runs(args, dev) -> dict:
     return out
 
 
+def serve_configurations(dev, episodes: int = 4000, steps: int = 20, warmup: int = 3) -> dict:
+    """The serving loop's episodes (1-256 ships, flight modes, dynamical orientation on) run two ways on the same
+    GPU, every episode resident: the plain per-configuration kernels (the episodes grouped by their ship count, one
+    park a configuration, each ticked by the plain schedule, every park each step) against the ragged batch (every
+    episode in one park, packed with no padding, one tiled launch a step in a CUDA graph). Both tick the same worlds;
+    their rows are compared bit for bit at the end."""
+    import numpy as np
+    import torch
+
+    from exact_ballpark_b200 import ModesGraph, VecModesPark, tick_plain
+    from exact_ballpark_b200.serving import episode_stream
+    from exact_ballpark_b200.workloads import PackedWorlds
+    eps = episode_stream(13, episodes, rate=0.0)
+    by_size = {}
+    for e in eps:
+        by_size.setdefault(e.ships, []).append(e)
+    parks = []
+    for size, group in sorted(by_size.items()):
+        pk = PackedWorlds.concat([e.world.packed() for e in group])
+        p = VecModesPark(pk.n, device=dev, dynamical_orientation=True, use_new_orbit=True)
+        pk.load(p)
+        pk.apply(p)
+        p.scratch()
+        parks.append((size, group, p))
+    order = [e for _, group, _ in parks for e in group]          # the ragged park holds the same worlds in this order
+    pk = PackedWorlds.concat([e.world.packed() for e in order])
+    ragged = VecModesPark(pk.n, device=dev, dynamical_orientation=True, use_new_orbit=True)
+    pk.load(ragged)
+    pk.apply(ragged)
+    graph = ModesGraph(ragged)
+    stream = torch.cuda.current_stream(dev)
+
+    def per_configuration():
+        for _, _, p in parks:
+            tick_plain(p, 256)
+
+    def timed(step, k):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(k):
+            step()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b)
+    for _ in range(warmup):
+        per_configuration()
+        graph.tick()
+    ms_plain = timed(per_configuration, steps)
+    ms_ragged = timed(graph.tick, steps)
+    same = True
+    at = 0
+    for _, _, p in parks:
+        for k in ("pos", "vel", "rot", "mode", "clock"):
+            same = same and torch.equal(getattr(p, "_" + k)[..., :p.n], getattr(ragged, "_" + k)[..., at:at + p.n])
+        at += p.n
+    n = pk.n
+    return {"episodes": episodes, "ships": n, "configurations": len(parks), "steps": steps,
+            "plain_per_configuration": {"ms_per_step": ms_plain / steps, "ship_ticks_per_s": n * steps / (ms_plain / 1e3),
+                                        "launches_per_step": 2 * len(parks)},
+            "ragged_batch": {"ms_per_step": ms_ragged / steps, "ship_ticks_per_s": n * steps / (ms_ragged / 1e3),
+                             "launches_per_step": 1},
+            "speedup_ragged_vs_plain": ms_plain / ms_ragged, "bit_identical": bool(same),
+            "note": "back-to-back steps on the device (no flush): the serving loop's tick without its host loop, "
+                    "against the same episodes grouped by ship count, a plain-schedule park each"}
+
+
 # Algorithmic bytes of one world-tick of the collision park (4 ships, 4 free spheres, 8 fixed spheres): a free ball
 # reads 235 B (position, velocity, goto point 3 x 24; mode, mass, agility, speed fraction, max velocity, decay factor,
 # radius, id, level 8 x 8; key, side 2 x 24; 5 flags) and writes 740 B (mLastG, mLastC, old position and velocity,
@@ -1176,7 +1242,7 @@ def main() -> None:
     ap.add_argument("--collide-steps", type=int, default=50)
     ap.add_argument("--no-combat", action="store_true")
     ap.add_argument("--only", choices=("ragged", "collide", "collide_statics", "combat", "composed", "serve", "server",
-                                       "space", "partition"),
+                                       "space", "partition", "serve_configurations"),
                     default=None, help="run one section alone on one GPU and print it (for profiling); the default "
                                        "run prints the headline line with every section")
     ap.add_argument("--combat-worlds", type=int, default=65536)
@@ -1188,7 +1254,7 @@ def main() -> None:
     ap.add_argument("--space-steps", type=int, default=5)
     ap.add_argument("--partition-worlds", type=int, default=100000)
     ap.add_argument("--partition-steps", type=int, default=10)
-    ap.add_argument("--partition-warp-class", type=int, default=32,
+    ap.add_argument("--partition-warp-class", type=int, default=64,
                     help="the ragged batch's size classes from this size up run a warp a world (129: none)")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-seconds", type=float, default=6.0)
@@ -1223,6 +1289,7 @@ def main() -> None:
                "collide_statics": lambda: collide_runs(args, dev, statics=True),
                "combat": lambda: combat_runs(args, dev), "composed": lambda: combat_runs(args, dev, composed=True),
                "serve": lambda: serve_runs(args, dev), "server": lambda: server_runs(args, dev),
+               "serve_configurations": lambda: serve_configurations(dev),
                "space": lambda: space_runs(args, dev), "partition": lambda: partition_runs(args, dev)}[args.only]
         print(json.dumps({"metric": METRIC, "section": args.only, args.only: run()}), flush=True)
         return
@@ -1277,6 +1344,7 @@ def main() -> None:
     if not args.no_serve:
         line["serve"] = serve_runs(args, dev)
         line["serve"]["plain_ship_ticks_per_s"] = line["flight"]["plain"]["value"] / world_size
+        line["serve"]["configurations"] = serve_configurations(dev)
     if dist is not None:
         dist.destroy_process_group()
     if rank == 0:

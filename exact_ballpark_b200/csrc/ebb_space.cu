@@ -9,14 +9,14 @@
 namespace ebb {
 namespace space {
 
-__global__ void __launch_bounds__(128) tape_kernel(const EbbFlightState p, const EbbSpaceState s, const EbbSpaceTape t) {
+__global__ void __launch_bounds__(128, 6) tape_kernel(const EbbFlightState p, const EbbSpaceState s, const EbbSpaceTape t) {
     const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= s.worlds) return;
     run_tape(&p, &s, &t, w);
 }
 
 // a warp a world: the world's index is the warp's, the lanes run its program together (ebb_space.cuh's World)
-__global__ void __launch_bounds__(128) tape_kernel_warp(const EbbFlightState p, const EbbSpaceState s,
+__global__ void __launch_bounds__(128, 6) tape_kernel_warp(const EbbFlightState p, const EbbSpaceState s,
                                                         const EbbSpaceTape t) {
     __shared__ Coop scratch[4];
     const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;

@@ -47,9 +47,20 @@ EBB_HD constexpr int32_t umap_next_buckets(int32_t b) {
 }
 
 // a box's width at level i (Partition.h's constants: 2^16 grid units of 480 m a quarter at the top)
-EBB_HD double level_width(int i) {
-    return ddiv(dmul(dmul((double)(int64_t(1) << (2 * NUM_LEVELS)), 480.0), 0.25), (double)(int64_t(1) << (2 * i)));
+// The widths are powers of two times 480 m, so each value below is exact; the reciprocal is the correctly rounded
+// 1 / width and the half-span 0.5 width 2^(2 level + 23) is exact, all folded at compile time to the values the
+// formulas give at run time (level_width: 2^16 x 480 x 0.25 / 4^i; key_for's 1 / width and 0.5 width grid).
+constexpr double level_width_c(int i) { return 65536.0 * 480.0 * 0.25 / (double)(int64_t(1) << (2 * i)); }
+constexpr double level_inv_c(int i) { return 1.0 / level_width_c(i); }
+constexpr double level_half_c(int i) {
+    return 0.5 * level_width_c(i) * (double)(int64_t(1) << (2 * i - 2 * NUM_LEVELS + 39));
 }
+#define EBB_LEVEL_TABLE(f, i)                                                                                     \
+    ((i) == 0 ? f(0) : (i) == 1 ? f(1) : (i) == 2 ? f(2) : (i) == 3 ? f(3) : (i) == 4 ? f(4) : (i) == 5 ? f(5)   \
+     : (i) == 6 ? f(6) : f(7))
+EBB_HD double level_width(int i) { return EBB_LEVEL_TABLE(level_width_c, i); }
+EBB_HD double level_inv(int i) { return EBB_LEVEL_TABLE(level_inv_c, i); }
+EBB_HD double level_half(int i) { return EBB_LEVEL_TABLE(level_half_c, i); }
 EBB_HD int64_t level_grid(int i) { return int64_t(1) << (2 * i - 2 * NUM_LEVELS + 39); }
 EBB_HD int64_t clamp_key(int64_t i, int64_t n) { return i < 0 ? int64_t(0) : (i >= n ? n - 1 : i); }
 
@@ -330,8 +341,7 @@ struct World {
         return dadd(radius, dmul(p->dt, max_speed));
     }
     EBB_HD static void key_for(int level, const double* x, int64_t* k) {
-        const double wd = level_width(level), fac = ddiv(1.0, wd);
-        const double half = dmul(dmul(0.5, wd), (double)level_grid(level));
+        const double fac = level_inv(level), half = level_half(level);
         for (int c = 0; c < 3; ++c) k[c] = to_i64(dmul(dadd(x[c], half), fac));
     }
 
