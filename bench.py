@@ -1084,8 +1084,24 @@ def partition_headline(args, dev, dist, rank: int, world_size: int, barrier, max
     del r, g, part, park, q, srv
     torch.cuda.empty_cache()
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = partition_cpu_sample(pw, min(W, 400), 5, warm=2)
-        out["compute"] = op_counts("partition", 2000, 5)
+        out["cpu_baseline"] = partition_cpu_sample(pw, min(W, 20000), K, warm=args.warmup)
+        out["compute"] = compute_roofline(op_counts("partition", 2000, 5), out["value"])
+    return out
+
+
+FP64_PEAK_TFLOPS = 37.0        # B200 FP64 (vector) nominal; no measured FP64 peak on this pool
+FP32_PEAK_TFLOPS = 75.0        # B200 FP32 nominal
+
+
+def compute_roofline(counts: dict | None, ship_ticks_per_s: float) -> dict | None:
+    """The counted FLOPs per ship-tick as achieved rates against the FP64 and FP32 pipes' nominal peaks."""
+    if not counts or "error" in counts:
+        return counts
+    out = dict(counts)
+    for kind, peak in (("fp64", FP64_PEAK_TFLOPS), ("fp32", FP32_PEAK_TFLOPS)):
+        gf = counts[kind + "_flops"] * ship_ticks_per_s / 1e9
+        out[kind] = {"achieved": gf / 1e3, "peak": peak, "unit": "TFLOP/s", "frac": gf / 1e3 / peak,
+                     "peak_kind": "nominal"}
     return out
 
 
@@ -1218,7 +1234,7 @@ def flight_runs(args, dev, rank: int, world_size: int, barrier, max_over_ranks) 
             "gpu_launches": 3 * args.flight_steps, "clocks": clocks}
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(args.worlds, args.ships, args.warmup, args.flight_steps)
-        line["compute"] = op_counts("flight", 4096, 10)
+        line["compute"] = compute_roofline(op_counts("flight", 4096, 10), value)
     del graph
     return line
 
@@ -1313,7 +1329,7 @@ def main() -> None:
 
     head = partition_headline(args, dev, dist, rank, world_size, barrier, max_over_ranks)
     rest = {k: v for k, v in head.items() if k not in ("value", "ms_per_step", "roofline", "e2e", "clocks",
-                                                      "gpu_launches", "cpu_baseline")}
+                                                      "gpu_launches", "cpu_baseline", "compute")}
     line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64/f32", "data": "synthetic (seeded)",
@@ -1330,6 +1346,8 @@ def main() -> None:
             "clocks": head["clocks"], "partition": rest}
     if "cpu_baseline" in head:
         line["cpu_baseline"] = head["cpu_baseline"]
+    if head.get("compute"):
+        line["compute"] = head["compute"]
     line["flight"] = flight_runs(args, dev, rank, world_size, barrier, max_over_ranks)
     if not args.no_ragged:
         line["ragged"] = ragged_runs(args, dev)

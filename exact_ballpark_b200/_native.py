@@ -14,7 +14,7 @@ LIB_PATH = HERE / "libebb.so"
 # is started with EBB_COUNTING=1
 if os.environ.get("EBB_COUNTING") == "1":
     LIB_PATH = HERE / "libebb_count.so"
-ABI = 7
+ABI = 8
 COLLIDE_MAX_SLOTS = 64          # include/ebb.h: EBB_COLLIDE_MAX_SLOTS
 COLLIDE_MAX_STATICS = 64        # include/ebb.h: EBB_COLLIDE_MAX_STATICS
 SPACE_MAX_SLOTS = 128           # include/ebb.h: EBB_SPACE_MAX_SLOTS
@@ -89,7 +89,9 @@ class SpaceState(ctypes.Structure):
                    + SPACE_DICT_FIELDS]
                 + [("umap_cap", ctypes.c_int64), ("events", ctypes.c_int64)]
                 + [(k, ctypes.c_void_p) for k in SPACE_SENSOR_FIELDS]
-                + [("smask", ctypes.c_void_p), ("pmask", ctypes.c_void_p), ("lanes", ctypes.c_int64)])
+                + [("smask", ctypes.c_void_p), ("pmask", ctypes.c_void_p), ("lanes", ctypes.c_int64),
+                   ("pitch", ctypes.c_int64)]
+                + [(k, ctypes.c_void_p) for k in ("box_parent", "box_top", "box_home", "box_slot", "fbox")])
 
 
 class SpaceQuery(ctypes.Structure):

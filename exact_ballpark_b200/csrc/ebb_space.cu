@@ -1,6 +1,6 @@
 // SPDX-License-Identifier: MIT
-// The space layer's tape on the device: one thread a world runs its K operations in order (ebb_space.cuh), its
-// state [entry][world] so that a warp's 32 worlds read consecutive words.
+// The space layer's tape on the device: one thread (or one warp) a world runs its K operations in order
+// (ebb_space.cuh), over the state in either arrangement (interleaved [entry][world], or world-major).
 #include <cuda_runtime.h>
 
 #include "../../include/ebb.h"
@@ -9,25 +9,28 @@
 namespace ebb {
 namespace space {
 
+template <bool WM>
 __global__ void __launch_bounds__(128, 6) tape_kernel(const EbbFlightState p, const EbbSpaceState s, const EbbSpaceTape t) {
     const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= s.worlds) return;
-    run_tape(&p, &s, &t, w);
+    run_tape<WM>(&p, &s, &t, w);
 }
 
 // a warp a world: the world's index is the warp's, the lanes run its program together (ebb_space.cuh's World)
+template <bool WM>
 __global__ void __launch_bounds__(128, 6) tape_kernel_warp(const EbbFlightState p, const EbbSpaceState s,
                                                         const EbbSpaceTape t) {
     __shared__ Coop scratch[4];
     const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (w >= s.worlds) return;                            // (the whole warp: w is the warp's)
-    run_tape(&p, &s, &t, w, (int)(threadIdx.x & 31), &scratch[threadIdx.x >> 5]);
+    run_tape<WM>(&p, &s, &t, w, (int)(threadIdx.x & 31), &scratch[threadIdx.x >> 5]);
 }
 
+template <bool WM>
 __global__ void __launch_bounds__(128) query_kernel(const EbbFlightState p, const EbbSpaceState s, const EbbSpaceQuery q) {
     const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= s.worlds) return;
-    run_query(&p, &s, &q, w);
+    run_query<WM>(&p, &s, &q, w);
 }
 
 }  // namespace space
@@ -63,7 +66,8 @@ static int space_buffers(const EbbFlightState* park, const EbbSpaceState* s) {
         s->ntf_in == nullptr || s->trk_in == nullptr || s->slist == nullptr || s->slen == nullptr ||
         s->sbkt == nullptr || s->pmap == nullptr || s->pn == nullptr || s->pbkt == nullptr || s->evn == nullptr ||
         s->rnd == nullptr || (s->events > 0 && s->ev == nullptr) || s->smask == nullptr || s->pmask == nullptr ||
-        (s->lanes != 1 && s->lanes != 32))
+        (s->lanes != 1 && s->lanes != 32) || s->pitch < 0 || s->pitch % 16 != 0 || s->box_parent == nullptr ||
+        s->box_top == nullptr || s->box_home == nullptr || s->box_slot == nullptr || s->fbox == nullptr)
         return EBB_EINVAL;
     if (park->pos == nullptr || park->vel == nullptr || park->old_pos == nullptr || park->old_vel == nullptr ||
         park->ids == nullptr || park->radius == nullptr || park->max_vel == nullptr || park->agility == nullptr ||
@@ -82,12 +86,19 @@ int ebb_space_tape(const EbbFlightState* park, const EbbSpaceState* s, const Ebb
     rc = space_buffers(park, s);
     if (rc) return rc;
     if (t->code == nullptr || t->a == nullptr || t->b == nullptr) return EBB_EINVAL;
+    const cudaStream_t st = (cudaStream_t)stream;
     if (s->lanes == 32) {
         const unsigned grid = (unsigned)((s->worlds * 32 + 127) / 128);
-        ebb::space::tape_kernel_warp<<<grid, 128, 0, (cudaStream_t)stream>>>(*park, *s, *t);
+        if (s->pitch > 0)
+            ebb::space::tape_kernel_warp<true><<<grid, 128, 0, st>>>(*park, *s, *t);
+        else
+            ebb::space::tape_kernel_warp<false><<<grid, 128, 0, st>>>(*park, *s, *t);
     } else {
         const unsigned grid = (unsigned)((s->worlds + block - 1) / block);
-        ebb::space::tape_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(*park, *s, *t);
+        if (s->pitch > 0)
+            ebb::space::tape_kernel<true><<<grid, block, 0, st>>>(*park, *s, *t);
+        else
+            ebb::space::tape_kernel<false><<<grid, block, 0, st>>>(*park, *s, *t);
     }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : (int)e;
@@ -104,7 +115,10 @@ int ebb_space_query(const EbbFlightState* park, const EbbSpaceState* s, const Eb
     if (q->a == nullptr || q->b == nullptr || q->f == nullptr || q->out == nullptr || q->outd == nullptr)
         return EBB_EINVAL;
     const unsigned grid = (unsigned)((s->worlds + block - 1) / block);
-    ebb::space::query_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(*park, *s, *q);
+    if (s->pitch > 0)
+        ebb::space::query_kernel<true><<<grid, block, 0, (cudaStream_t)stream>>>(*park, *s, *q);
+    else
+        ebb::space::query_kernel<false><<<grid, block, 0, (cudaStream_t)stream>>>(*park, *s, *q);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : (int)e;
 }

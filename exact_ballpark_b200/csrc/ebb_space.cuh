@@ -9,8 +9,11 @@
 // (space.py:896-1056); AddBall's filing, the setters' re-filings and RemoveBall (space.py:1097-1319); the tick's
 // dead-bubble flags and its re-filings (a warp's drop-out, the commits of the balls that moved).
 //
-// Layout: W worlds of N slots; every per-slot array is [N][W] and every per-entry array [cap][W] (world w's entry e
-// at e W + w), so that the threads of a warp, one world each, touch consecutive words. A world's boxes live in a
+// Layout: W worlds of N slots, in one of two arrangements (EbbSpaceState.pitch). Interleaved (pitch 0): every
+// per-slot array is [N][W] and every per-entry array [cap][W] (world w's entry e at e W + w), so that the threads of
+// a warp, one world each, touch consecutive words. World-major (pitch > 0): world w's copy of every array starts
+// w pitch bytes past world 0's and holds its entries consecutively, so that a warp running one world reads its
+// slots in one transaction and the world's state shares cache lines. A world's boxes live in a
 // table of `boxes` entries (level -1 for a free entry, the free ones on a stack), found through a hash index of
 // 2 `boxes` slots (linear probing, deletion by moving the run back). Exactness: the filing's double
 // arithmetic through ebb_arith.cuh (correctly rounded single operations), compiled with -fmad=false.
@@ -85,24 +88,34 @@ struct Coop {
 // One world's program. A thread runs it alone (lane -1), or the 32 lanes of a warp run it together (lane 0 .. 31):
 // every lane then takes every step on the same data, so they stay converged and write the same values (one
 // transaction a load or store), and GetNearbyBalls' scan and sort are split over the lanes (nearby_warp).
+// WM: the world-major arrangement (the state's pitch > 0), else the interleaved one.
+template <bool WM>
 struct World {
     const EbbFlightState* p;
     const EbbSpaceState* s;
     int64_t w, W, N, B;
     int lane = -1;
     Coop* sh = nullptr;
+    static constexpr bool world_major = WM;
 
-    // ---- accessors: entry e of a [cap][W] array, component c of a [3][cap][W] array ----
-    EBB_HD int64_t& I(int64_t* a, int64_t e) const { return a[e * W + w]; }
-    EBB_HD int64_t& I3(int64_t* a, int64_t c, int64_t e, int64_t cap) const { return a[(c * cap + e) * W + w]; }
-    EBB_HD uint8_t& U(uint8_t* a, int64_t e) const { return a[e * W + w]; }
+    // ---- accessors: entry e of a per-world array ([cap][W], or world w's run of cap entries), component c of a
+    // [3][cap] one ----
     template <class T>
-    EBB_HD T& at(T* a, int64_t e) const { return a[e * W + w]; }
-    EBB_HD int64_t& one(int64_t* a) const { return a[w]; }
-    EBB_HD void flag(int64_t f) const { s->flags[w] |= f; }
+    EBB_HD T& at(T* a, int64_t e) const {
+        if constexpr (WM)
+            return ((T*)((const char*)a + w * s->pitch))[e];
+        else
+            return a[e * W + w];
+    }
+    EBB_HD int64_t step() const { return WM ? 1 : W; }     // the distance of consecutive entries, in elements
+    EBB_HD int64_t& I(int64_t* a, int64_t e) const { return at(a, e); }
+    EBB_HD int64_t& I3(int64_t* a, int64_t c, int64_t e, int64_t cap) const { return at(a, c * cap + e); }
+    EBB_HD uint8_t& U(uint8_t* a, int64_t e) const { return at(a, e); }
+    EBB_HD int64_t& one(int64_t* a) const { return at(a, 0); }
+    EBB_HD void flag(int64_t f) const { one(s->flags) |= f; }
 
     // ---- the park's row of a slot ----
-    EBB_HD int64_t row(int64_t j) const { return s->rows[j * W + w]; }
+    EBB_HD int64_t row(int64_t j) const { return at(s->rows, j); }
     EBB_HD double pos(int64_t j, int c) const { return p->pos[c * p->n + row(j)]; }
     EBB_HD double vel(int64_t j, int c) const { return p->vel[c * p->n + row(j)]; }
     EBB_HD int64_t id(int64_t j) const { return p->ids[row(j)]; }
@@ -137,13 +150,16 @@ struct World {
         }
         return -1;
     }
+    // (each entry keeps its home slot and the slot it sits in, so that its removal starts there without a probe)
     EBB_HD void hash_insert(int64_t e) {
         const int64_t H = 2 * B;
         int64_t i = home((int)I(s->box_level, e), I3(s->box_key, 0, e, B), I3(s->box_key, 1, e, B),
                          I3(s->box_key, 2, e, B));
+        I(s->box_home, e) = i;
         for (int64_t probe = 0; probe < H; ++probe) {
             if (I(s->box_hash, i) == 0) {
                 I(s->box_hash, i) = e + 1;
+                I(s->box_slot, e) = i;
                 return;
             }
             i = i + 1 == H ? 0 : i + 1;
@@ -153,21 +169,18 @@ struct World {
     // the entry leaves the index; the entries after it in its run move back so that every probe still finds them
     EBB_HD void hash_erase(int64_t e) {
         const int64_t H = 2 * B;
-        int64_t i = home((int)I(s->box_level, e), I3(s->box_key, 0, e, B), I3(s->box_key, 1, e, B),
-                         I3(s->box_key, 2, e, B));
-        int64_t probe = 0;
-        for (; probe < H && I(s->box_hash, i) != e + 1; ++probe) i = i + 1 == H ? 0 : i + 1;
-        if (probe == H) return;
+        int64_t i = I(s->box_slot, e);
+        if (I(s->box_hash, i) != e + 1) return;            // (never: the slot is kept as entries move)
         int64_t j = i;
         for (int64_t step = 0; step < H; ++step) {
             j = j + 1 == H ? 0 : j + 1;
             const int64_t v = I(s->box_hash, j);
             if (v == 0) break;
-            const int64_t k = home((int)I(s->box_level, v - 1), I3(s->box_key, 0, v - 1, B),
-                                   I3(s->box_key, 1, v - 1, B), I3(s->box_key, 2, v - 1, B));
+            const int64_t k = I(s->box_home, v - 1);
             const bool stays = i <= j ? (i < k && k <= j) : (i < k || k <= j);
             if (stays) continue;
             I(s->box_hash, i) = v;
+            I(s->box_slot, v - 1) = i;
             i = j;
         }
         I(s->box_hash, i) = 0;
@@ -224,6 +237,8 @@ struct World {
             const int sh = 2 * (level - L);
             const int64_t e = new_box(L, ix >> sh, iy >> sh, iz >> sh);
             if (e < 0) return -1;
+            I(s->box_parent, e) = parent;                  // (a box's parent and top box outlive it: kids > 0)
+            I(s->box_top, e) = parent >= 0 ? I(s->box_top, parent) : e;
             if (parent >= 0) ++I(s->box_kids, parent);
             parent = e;
         }
@@ -236,13 +251,8 @@ struct World {
         const bool keep = one(s->free_boxes) < BOX_KEEP;
         int64_t cur = e;
         for (int guard = 0; guard < NUM_LEVELS && cur >= 0; ++guard) {
-            const int level = (int)I(s->box_level, cur);
-            int64_t parent = -1;
-            if (level > 0) {
-                parent = box_find(level - 1, I3(s->box_key, 0, cur, B) >> 2, I3(s->box_key, 1, cur, B) >> 2,
-                                  I3(s->box_key, 2, cur, B) >> 2);
-                if (parent >= 0) --I(s->box_kids, parent);
-            }
+            const int64_t parent = I(s->box_parent, cur);
+            if (parent >= 0) --I(s->box_kids, parent);
             hash_erase(cur);
             I(s->box_level, cur) = -1;
             I(s->box_free, one(s->box_free_n)++) = cur;
@@ -261,6 +271,9 @@ struct World {
     EBB_HD int64_t& key(int64_t j, int c) const { return I3(s->key, c, j, N); }
     EBB_HD int64_t& mod(int64_t j, int c) const { return I3(s->mod, c, j, N); }
     EBB_HD int64_t& active(int64_t j) const { return I(s->active, j); }
+    // a filed ball's box entries by side (bit c set: the box beside its own on axis c), so that leaving them takes no
+    // lookup; a huge ball's 27 boxes are looked up
+    EBB_HD int64_t& fbox(int64_t j, int bits) const { return I3(s->fbox, bits, j, N); }
 
     // the ball's boxes in key order (the map DeleteFromBoxes walks), as table entries; returns their count
     EBB_HD int ball_boxes(int64_t j, int64_t* out) const {
@@ -305,15 +318,35 @@ struct World {
         active(j) = 0;
         for (int c = 0; c < 3; ++c) mod(j, c) = -2;
     }
-    // DeleteFromBoxes: the ball leaves each of its boxes in key order, each box released when left empty
+    EBB_HD void leave_box(int64_t e, const int64_t* watch, int* fate) {
+        if (e < 0) return;
+        --I(s->box_balls, e);
+        if (I(s->box_balls, e) == 0 && I(s->box_kids, e) == 0) release(e, watch, fate);
+    }
+    // DeleteFromBoxes: the ball leaves each of its boxes in key order, each box released when left empty. The
+    // entries come from the ball's record of them (key order: on each axis the lower key first, so the side box first
+    // where the sphere reaches below); a huge ball, or a world past its table or the grid's edge (where keys clamp
+    // and a box may be missing), looks its boxes up.
     EBB_HDNI void delete_from_boxes(int64_t j, const int64_t* watch, int* fate) {
-        int64_t boxes[27];
-        const int n = ball_boxes(j, boxes);
-        for (int i = 0; i < n; ++i) {
-            const int64_t e = boxes[i];
-            if (e < 0) continue;
-            --I(s->box_balls, e);
-            if (I(s->box_balls, e) == 0 && I(s->box_kids, e) == 0) release(e, watch, fate);
+        if (lvl(j) >= 0 && !huge(j) && !(one(s->flags) & (F_EDGE | F_BOXES))) {
+            const int64_t mx = mod(j, 0), my = mod(j, 1), mz = mod(j, 2);
+            for (int ox = 0; ox < 2; ++ox) {
+                const int bx = mx < 0 ? 1 - ox : ox;
+                if (bx && !mx) continue;
+                for (int oy = 0; oy < 2; ++oy) {
+                    const int by = my < 0 ? 1 - oy : oy;
+                    if (by && !my) continue;
+                    for (int oz = 0; oz < 2; ++oz) {
+                        const int bz = mz < 0 ? 1 - oz : oz;
+                        if (bz && !mz) continue;
+                        leave_box(fbox(j, bx | (by << 1) | (bz << 2)), watch, fate);
+                    }
+                }
+            }
+        } else {
+            int64_t boxes[27];
+            const int n = ball_boxes(j, boxes);
+            for (int i = 0; i < n; ++i) leave_box(boxes[i], watch, fate);
         }
         clear_filing(j);
     }
@@ -322,11 +355,7 @@ struct World {
         int fate[2] = {0, 0};
         delete_from_boxes(j, watch, fate);
     }
-    EBB_HD int64_t topmost_of(int64_t e) const {
-        int level = (int)I(s->box_level, e);
-        int64_t kx = I3(s->box_key, 0, e, B), ky = I3(s->box_key, 1, e, B), kz = I3(s->box_key, 2, e, B);
-        return box_find(0, kx >> (2 * level), ky >> (2 * level), kz >> (2 * level));
-    }
+    EBB_HD int64_t topmost_of(int64_t e) const { return I(s->box_top, e); }
     // a free ball's radius plus a tick at full thrust (Ball::GetInflatedRadius)
     EBB_HD double inflated_radius(int64_t j, const double* v) const {
         const int64_t r = row(j);
@@ -496,10 +525,10 @@ struct World {
     }
     // Ball::InsertInBoxes: the ball's box at the level of its inflated radius and the neighbours its sphere reaches
     // (every neighbour for a huge ball), unless box and sides are as they were; the top box takes the bubble
-    EBB_HDNI void ball_insert_in_boxes(int64_t j, const double* x, const double* v, int level0, const int64_t* key0,
-                                     int fate_box1, int64_t new_bubble) {
+    // (`inflated`: the ball's inflated radius; `box0`: its box at level0, live unless fate_box1 says it was released)
+    EBB_HDNI void ball_insert_in_boxes(int64_t j, const double* x, double inflated, int level0, const int64_t* key0,
+                                     int64_t box0, int fate_box1, int64_t new_bubble) {
         if (fate_box1 == 2) flag(F_UNDEFINED);             // a deleted box's memory read
-        const double inflated = inflated_radius(j, v);
         const double wd = level_width(level0);
         const double center = dmul(dmul(wd, (double)level_grid(level0)), 0.5);
         int64_t m[3] = {0, 0, 0};
@@ -514,11 +543,12 @@ struct World {
         if (lvl(j) >= 0 && lvl(j) == level0 && key(j, 0) == key0[0] && key(j, 1) == key0[1] && key(j, 2) == key0[2] &&
             mod(j, 0) == m[0] && mod(j, 1) == m[1] && mod(j, 2) == m[2])
             return;
-        delete_from_boxes(j);
-        const int level = level_for(inflated);
-        int64_t k[3];
-        key_for(level, x, k);
-        const int64_t box1 = get_box(k[0], k[1], k[2], level);
+        const int64_t watch[2] = {fate_box1 == 0 ? box0 : -1, -1};
+        int fate[2] = {0, 0};
+        delete_from_boxes(j, watch, fate);
+        const int level = level0;                          // (level_for(inflated): the same radius)
+        // the box found before, still live, or GetBox again (made anew when the leaving released it)
+        const int64_t box1 = watch[0] >= 0 && fate[0] == 0 ? box0 : get_box(key0[0], key0[1], key0[2], level);
         if (box1 < 0) return;
         for (int c = 0; c < 3; ++c) {
             mod(j, c) = m[c];
@@ -545,8 +575,11 @@ struct World {
             return;
         }
         const int64_t mx = m[0], my = m[1], mz = m[2];
+        fbox(j, 0) = box1;
         auto side = [&](int64_t a, int64_t b, int64_t c) {
-            insert_in_box(j, get_box(ix + a, iy + b, iz + c, level));
+            const int64_t e = get_box(ix + a, iy + b, iz + c, level);
+            insert_in_box(j, e);
+            fbox(j, (a != 0) | ((b != 0) << 1) | ((c != 0) << 2)) = e;
             act |= int64_t(1) << (13 + a + 3 * b + 9 * c);
         };
         if (mx) side(mx, 0, 0);
@@ -589,7 +622,7 @@ struct World {
             I(s->bubble, j) = new_bubble;
             add_to_bubble(j);
         }
-        ball_insert_in_boxes(j, x, v, level0, key0, fate[0], new_bubble);
+        ball_insert_in_boxes(j, x, inflated, level0, key0, box1, fate[0], new_bubble);
     }
     EBB_HD void insert_in_boxes(int64_t j) {
         const double x[3] = {pos(j, 0), pos(j, 1), pos(j, 2)}, v[3] = {vel(j, 0), vel(j, 1), vel(j, 2)};
@@ -716,12 +749,18 @@ struct World {
     }
 
 #ifdef __CUDA_ARCH__
-    // A bitonic sort of the warp's scratch (sh->key, sh->id, carrying sh->out) by (key, id), every slot of the table
-    // (EBB_SPACE_MAX_SLOTS, a power of two), the lanes taking the pairs of each stage
-    __device__ void warp_sort() const {
-        for (int k = 2; k <= EBB_SPACE_MAX_SLOTS; k <<= 1)
+    // The slots the warp's sorts cover: the world's N rounded up to a power of two, 32 at least
+    __device__ int sort_span() const {
+        int S = 32;
+        while (S < N) S <<= 1;
+        return S;
+    }
+    // A bitonic sort of the warp's scratch (sh->key, sh->id, carrying sh->out) by (key, id) over the first S slots
+    // (sort_span: the slots past N hold no candidate and sort last), the lanes taking the pairs of each stage
+    __device__ void warp_sort(int S) const {
+        for (int k = 2; k <= S; k <<= 1)
             for (int jj = k >> 1; jj > 0; jj >>= 1) {
-                for (int i = lane; i < EBB_SPACE_MAX_SLOTS; i += 32) {
+                for (int i = lane; i < S; i += 32) {
                     const int x = i ^ jj;
                     if (x <= i) continue;
                     const int64_t ki = sh->key[i], kx = sh->key[x], ii = sh->id[i], ix = sh->id[x];
@@ -747,7 +786,8 @@ struct World {
     __device__ int nearby_warp(int64_t b, int64_t bub, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked,
                                uint8_t* out) const {
         int mine = 0;
-        for (int64_t o = lane; o < EBB_SPACE_MAX_SLOTS; o += 32) {
+        const int S = sort_span();
+        for (int64_t o = lane; o < S; o += 32) {
             int64_t k = NOT_A_CANDIDATE, i = INT64_MAX;
             if (o < N && o != b && slot_ok(o) && U(s->in_park, o) && lvl(o) >= 0) {
                 k = walk_key(b, o);
@@ -769,7 +809,7 @@ struct World {
         }
         const int n = (int)__reduce_add_sync(0xffffffffu, (unsigned)mine);
         __syncwarp();
-        warp_sort();
+        warp_sort(S);
         for (int i = 0; i < n; ++i) out[i] = sh->out[i];
         __syncwarp();
         return n;
@@ -789,10 +829,10 @@ struct World {
         int64_t mstep;
     };
     EBB_HD UMap sensor_map(int64_t j) const {
-        return UMap{s->slist + j * W + w, N * W, &at(s->slen, j), &at(s->sbkt, j), s->smask + j * W + w, N * W};
+        return UMap{&at(s->slist, j), N * step(), &at(s->slen, j), &at(s->sbkt, j), &at(s->smask, j), N * step()};
     }
     EBB_HD UMap proximity_map() const {
-        return UMap{s->pmap + w, W, &s->pn[w], &s->pbkt[w], s->pmask + w, W};
+        return UMap{&at(s->pmap, 0), step(), &at(s->pn, 0), &at(s->pbkt, 0), &at(s->pmask, 0), step()};
     }
     EBB_HD bool umap_has(const UMap& m, int64_t slot) const {
         return ((m.m[(slot >> 6) * m.mstep] >> (slot & 63)) & 1) != 0;
@@ -866,12 +906,12 @@ struct World {
 
     // ---- the proximity sensors, notification ranges and target tracking (space.py:1345-1477) ----
     EBB_HD void event(int kind, int64_t ball, int64_t other, int value) const {
-        const int64_t n = s->evn[w];
+        const int64_t n = one(s->evn);
         if (n < s->events)
             at(s->ev, n) = (int32_t)(kind | (value << 4) | ((int32_t)ball << 8) | ((int32_t)other << 16));
         else
             flag(F_EVENTS);
-        s->evn[w] = n + 1;
+        one(s->evn) = n + 1;
     }
     EBB_HD double dist2(int64_t a, const double* x) const {
         const double d0 = dsub(pos(a, 0), x[0]), d1 = dsub(pos(a, 1), x[1]), d2 = dsub(pos(a, 2), x[2]);
@@ -1379,7 +1419,8 @@ struct World {
 #ifdef __CUDA_ARCH__
         if (lane >= 0) {                                   // the lanes sort the slots by id together
             int mine = 0;
-            for (int64_t j = lane; j < EBB_SPACE_MAX_SLOTS; j += 32) {
+            const int S = sort_span();
+            for (int64_t j = lane; j < S; j += 32) {
                 const bool in = j < N && U(s->in_park, j) && slot_ok(j);
                 sh->key[j] = in ? 0 : NOT_A_CANDIDATE;
                 sh->id[j] = in ? id(j) : INT64_MAX;
@@ -1388,7 +1429,7 @@ struct World {
             }
             n = (int64_t)__reduce_add_sync(0xffffffffu, (unsigned)mine);
             __syncwarp();
-            warp_sort();
+            warp_sort(S);
             for (int64_t i = 0; i < n; ++i) order[i] = sh->out[i];
             __syncwarp();
         } else
@@ -1438,7 +1479,7 @@ struct World {
             case EBB_SPACE_REMOVE_SENSOR: if (live) remove_sensor(j); break;
             case EBB_SPACE_NOTIFY_RANGE: if (live) set_notification_range(j, f[0]); break;
             case EBB_SPACE_TRACK: if (live) set_tracking(j, b, f[0], f[1] != 0.0); break;
-            case EBB_SPACE_CLEAR_EVENTS: s->evn[w] = 0; break;
+            case EBB_SPACE_CLEAR_EVENTS: one(s->evn) = 0; break;
             case EBB_SPACE_HANDLE_PROXIMITIES: handle_proximities(); break;
             case EBB_SPACE_SET_CLOAKED: if (live) at(s->cloaked, j) = b; break;
             default: flag(F_BAD_OP); break;
@@ -1447,21 +1488,23 @@ struct World {
 };
 
 // world w's query (its state read, nothing written but the answer; a flagged world answers nothing)
+template <bool WM>
 EBB_HD void run_query(const EbbFlightState* p, const EbbSpaceState* s, const EbbSpaceQuery* q, int64_t w) {
-    World wd{p, s, w, s->worlds, s->slots, s->boxes};
+    World<WM> wd{p, s, w, s->worlds, s->slots, s->boxes};
     q->out[w] = 0;
-    if (s->flags[w] & (F_EDGE | F_BOXES | F_DICTS | F_ENTRIES | F_SETS | F_BAD_OP)) return;
+    if (wd.one(s->flags) & (F_EDGE | F_BOXES | F_DICTS | F_ENTRIES | F_SETS | F_BAD_OP)) return;
     double f[5];
     for (int c = 0; c < 5; ++c) f[c] = q->f[c * s->worlds + w];
     wd.query(q->kind, q->a[w], q->b[w], f, q->out, q->outd);
 }
 
 // world w's K operations of the tape, in order (a flagged world is left alone)
+template <bool WM>
 EBB_HD void run_tape(const EbbFlightState* p, const EbbSpaceState* s, const EbbSpaceTape* t, int64_t w, int lane = -1,
                      Coop* sh = nullptr) {
-    World wd{p, s, w, s->worlds, s->slots, s->boxes, lane, sh};
+    World<WM> wd{p, s, w, s->worlds, s->slots, s->boxes, lane, sh};
     for (int64_t k = 0; k < t->K; ++k) {
-        if (s->flags[w] & (F_EDGE | F_BOXES | F_DICTS | F_ENTRIES | F_SETS | F_BAD_OP)) return;
+        if (wd.one(s->flags) & (F_EDGE | F_BOXES | F_DICTS | F_ENTRIES | F_SETS | F_BAD_OP)) return;
         const int64_t at = k * s->worlds + w;
         double f[4] = {0.0, 0.0, 0.0, 0.0};
         if (t->f != nullptr)

@@ -7,18 +7,22 @@ keep-alive sets, InitializeBubbles, CopyBubbles, the dead-bubble rows the park's
 re-filings (a warp's drop-out nearly at rest, at its drop-out point; every ball that moved at least sqrt(0.1) m, in
 ascending id), as the reference's `SpaceBallpark` on the master runs them (space.py:596-1319).
 
-The layer is one sequential program a world, one CUDA thread a world (csrc/ebb_space.cuh): an operation is a tape,
-per world K operations applied in order, one launch for all worlds (`tape`, `ops`, `broadcast`), with the reference's
-operation names (`OP`). Its state is [entry, world] tensors (a warp's 32 worlds read consecutive words). A world that
+Beside the filing: the proximity sensors, notification ranges and target tracking with their events,
+HandleProximities, and the queries (CheckVisibility, GetBallIdsInRange, GetBubbleAtCoordinates, GetNearbyBalls).
+
+The layer is one sequential program a world, one CUDA thread or one warp a world (csrc/ebb_space.cuh): an operation
+is a tape, per world K operations applied in order, one launch for all worlds (`tape`, `ops`, `broadcast`), with the
+reference's operation names (`OP`). Its state is tensors indexed [entry, world]: stored interleaved (a warp's 32
+worlds read consecutive words; a thread a world) or world-major (a world's entries consecutive, every world `pitch`
+bytes apart in one arena; the form for a warp a world, whose lanes then read a world's slots together). A world that
 leaves the layer's domain (a table full, the grid's edge, an operation outside this slice) is flagged and left alone;
-`check()` raises for it. Not in this slice: the proximity sensors, target tracking, notification ranges,
-HandleProximities, the queries (CheckVisibility, GetBallIdsInRange, GetBubbleAtCoordinates), the collision park's
-view, the delayed removal; their operations flag BAD_OP.
+`check()` raises for it. Not in this slice: the collision park's view and the delayed removal.
 """
 
 from __future__ import annotations
 
 import ctypes
+import math
 
 import torch
 
@@ -40,15 +44,67 @@ FLAG = {name: 1 << k for k, name in enumerate(FLAGS)}
 BLOCK = 128
 
 
+def state_spec(N: int, B: int, D: int, E: int, S: int, U: int, M: int) -> list:
+    """The layer's arrays a world (include/ebb.h's EbbSpaceState, `rnd` aside): (name, shape, dtype, initial value)
+    for N slots, B box-table entries, D dictionaries, E entries, S set members, U keys a map and M events."""
+    F64, I32 = torch.float64, torch.int32
+    return [("rows", (N,), I64, 0), ("level", (N,), I64, -1), ("key", (3, N), I64, 0), ("mod", (3, N), I64, -2),
+            ("active", (N,), I64, 0), ("bubble", (N,), I64, -1), ("old_bubble", (N,), I64, -1),
+            ("seq", (N,), I64, 0), ("my_box", (N,), I64, -1), ("my_top", (N,), I64, -1),
+            ("in_park", (N,), U8, 0), ("keep_alive", (N,), U8, 0), ("dead", (N,), U8, 0),
+            ("dropped", (N,), U8, 0), ("box_level", (B,), I64, -1), ("box_key", (3, B), I64, 0),
+            ("box_balls", (B,), I64, 0), ("box_kids", (B,), I64, 0), ("box_bubble", (B,), I64, -1),
+            ("stack", (B,), I64, 0), ("box_n", (), I64, 0), ("free_boxes", (), I64, 0),
+            ("box_hash", (2 * B,), I64, 0), ("box_free", (B,), I64, 0), ("box_free_n", (), I64, 0),
+            ("dict_bubble", (D,), I64, 0), ("dict_n", (), I64, 0), ("entry_bubble", (E,), I64, 0),
+            ("entry_id", (E,), I64, 0), ("entry_value", (E,), I64, 0), ("entry_n", (), I64, 0),
+            ("inter_bubble", (S,), I64, 0), ("inter_id", (S,), I64, 0), ("inter_n", (), I64, 0),
+            ("keep_bubble", (S,), I64, 0), ("keep_id", (S,), I64, 0), ("keep_n", (), I64, 0),
+            ("bubble_id", (), I64, 0), ("seq_next", (), I64, 0), ("flags", (), I64, 0),
+            ("srange", (N,), F64, 0), ("speriod", (N,), F64, 2.0), ("selapsed", (N,), F64, 0),
+            ("ntf_range", (N,), F64, 0), ("trk_range", (N,), F64, 0), ("trk", (N,), I64, -1),
+            ("cloaked", (N,), I64, 0), ("sonly", (N,), U8, 0), ("has_prox", (N,), U8, 0),
+            ("ntf_in", (N,), U8, 0), ("trk_in", (N,), U8, 0), ("slist", (U, N), U8, 0), ("slen", (N,), I32, 0),
+            ("sbkt", (N,), I32, 1), ("pmap", (U,), U8, 0), ("pn", (), I32, 0), ("pbkt", (), I32, 1),
+            ("ev", (max(M, 1),), I32, 0), ("evn", (), I64, 0), ("smask", (2, N), I64, 0),
+            ("pmask", (2,), I64, 0), ("box_parent", (B,), I64, -1), ("box_top", (B,), I64, -1),
+            ("box_home", (B,), I64, 0), ("box_slot", (B,), I64, 0), ("fbox", (8, N), I64, -1)]
+
+
+def allocate_state(spec, W: int, dev, world_major: bool):
+    """The layer's arrays, each a tensor [*shape, W] (its entries, then the world). Interleaved: each its own
+    contiguous tensor. World-major: views into one arena [W][pitch bytes], each array at its own offset a world (16-byte
+    aligned), the world's row of the arena holding its copy of every array. Returns (arrays, pitch; 0 interleaved)."""
+    if not world_major:
+        return {name: torch.full((*shape, W), fill, dtype=dt, device=dev) for name, shape, dt, fill in spec}, 0
+    at, off = [], 0
+    for name, shape, dt, fill in spec:
+        size = math.prod(shape) * torch.empty((), dtype=dt).element_size()
+        at.append(off)
+        off += (size + 15) // 16 * 16
+    pitch = (off + 127) // 128 * 128
+    arena = torch.zeros(W, pitch, dtype=U8, device=dev)
+    out = {}
+    for (name, shape, dt, fill), o in zip(spec, at):
+        n = math.prod(shape)
+        size = n * torch.empty((), dtype=dt).element_size()
+        t = arena[:, o:o + size].view(dt).reshape(W, *shape).movedim(0, -1)
+        if fill:
+            t.fill_(fill)
+        out[name] = t
+    return out, pitch
+
+
 class VecSpace:
     """The layer for W worlds of N slots over a flight park's rows. `rows` [W, N]: the park's row of each slot (-1 for
     none), each world's slots in the order its balls are added. Capacities a world: `boxes` box-table entries,
     `dicts` bubble dictionaries, `entries` dictionary entries, `sets` members of each of the interactive and keep-alive
-    set families (defaults from N)."""
+    set families (defaults from N). `lanes`: 1 (a thread a world) or 32 (a warp a world); `world_major`: the
+    state's arrangement (default: world-major for a warp a world, interleaved for a thread a world)."""
 
     def __init__(self, park: VecModesPark, rows, boxes: int | None = None, dicts: int | None = None,
                  entries: int | None = None, sets: int | None = None, block: int = BLOCK, events: int = 256,
-                 umap_cap: int | None = None, seed=1, lanes: int = 1):
+                 umap_cap: int | None = None, seed=1, lanes: int = 1, world_major: bool | None = None):
         if not isinstance(park, VecModesPark):
             raise TypeError("the space layer runs over the flight park (exact_ballpark_b200.VecModesPark)")
         self.park, self.dev, self.block = park, park.dev, int(block)
@@ -65,35 +121,19 @@ class VecSpace:
         self.D = int(dicts) if dicts is not None else 8 * N + 16
         self.E = int(entries) if entries is not None else 4 * N + 8
         self.S = int(sets) if sets is not None else 2 * N + 8
-        self.rows = rows.t().contiguous().to(d)                       # [N][W]
-        z = lambda *shape, dt=I64: torch.zeros(*shape, dtype=dt, device=d)   # noqa: E731
-        self.st = {
-            "level": z(N, W) - 1, "key": z(3, N, W), "mod": z(3, N, W) - 2, "active": z(N, W), "bubble": z(N, W) - 1,
-            "old_bubble": z(N, W) - 1, "seq": z(N, W), "my_box": z(N, W) - 1, "my_top": z(N, W) - 1,
-            "in_park": z(N, W, dt=U8), "keep_alive": z(N, W, dt=U8), "dead": z(N, W, dt=U8), "dropped": z(N, W, dt=U8),
-            "box_level": z(self.B, W) - 1, "box_key": z(3, self.B, W), "box_balls": z(self.B, W),
-            "box_kids": z(self.B, W), "box_bubble": z(self.B, W) - 1, "stack": z(self.B, W), "box_n": z(W),
-            "free_boxes": z(W), "box_hash": z(2 * self.B, W), "box_free": z(self.B, W), "box_free_n": z(W),
-            "dict_bubble": z(self.D, W), "dict_n": z(W), "entry_bubble": z(self.E, W), "entry_id": z(self.E, W),
-            "entry_value": z(self.E, W), "entry_n": z(W), "inter_bubble": z(self.S, W), "inter_id": z(self.S, W),
-            "inter_n": z(W), "keep_bubble": z(self.S, W), "keep_id": z(self.S, W), "keep_n": z(W),
-            "bubble_id": z(W), "seq_next": z(W), "flags": z(W)}
         self.M = int(events)
         self.U = N if umap_cap is None else int(umap_cap)
         if not 1 <= self.U <= _native.SPACE_MAX_SLOTS or self.M < 0:
             raise ValueError(f"umap_cap {self.U}: from 1 to {_native.SPACE_MAX_SLOTS}; events >= 0")
-        zf = lambda *shape: torch.zeros(*shape, dtype=torch.float64, device=d)   # noqa: E731
-        zi32 = lambda *shape: torch.zeros(*shape, dtype=torch.int32, device=d)   # noqa: E731
-        self.st.update({
-            "srange": zf(N, W), "speriod": zf(N, W) + 2.0, "selapsed": zf(N, W), "ntf_range": zf(N, W),
-            "trk_range": zf(N, W), "trk": z(N, W) - 1, "cloaked": z(N, W), "sonly": z(N, W, dt=U8),
-            "has_prox": z(N, W, dt=U8), "ntf_in": z(N, W, dt=U8), "trk_in": z(N, W, dt=U8),
-            "slist": z(self.U, N, W, dt=U8), "slen": zi32(N, W), "sbkt": zi32(N, W) + 1, "pmap": z(self.U, W, dt=U8),
-            "pn": zi32(W), "pbkt": zi32(W) + 1, "ev": zi32(max(self.M, 1), W), "evn": z(W),
-            "rnd": zi32(W, _native.RAND_WORDS), "smask": z(2, N, W), "pmask": z(2, W)})
         if lanes not in (1, 32):
             raise ValueError("lanes: 1 (a thread a world) or 32 (a warp a world)")
         self.lanes = int(lanes)
+        self.world_major = (self.lanes == 32) if world_major is None else bool(world_major)
+        spec = state_spec(N, self.B, self.D, self.E, self.S, self.U, self.M)
+        self.st, self.pitch = allocate_state(spec, W, d, self.world_major)
+        self.st["rows"].copy_(rows.t())
+        self.rows = self.st.pop("rows")                              # [N][W]
+        self.st["rnd"] = torch.zeros(W, _native.RAND_WORDS, dtype=torch.int32, device=d)
         seeds = torch.as_tensor(seed, dtype=I64).reshape(-1)
         seeds = (seeds.expand(W) if seeds.numel() == 1 else seeds).contiguous().to(d)
         if seeds.numel() != W:
@@ -111,7 +151,7 @@ class VecSpace:
         if self._state is None:
             s = _native.SpaceState()
             s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets = self.W, self.N, self.B, self.D, self.E, self.S
-            s.umap_cap, s.events, s.lanes = self.U, self.M, self.lanes
+            s.umap_cap, s.events, s.lanes, s.pitch = self.U, self.M, self.lanes, self.pitch
             s.rows = self.rows.data_ptr()
             for name, t in self.st.items():
                 setattr(s, name, t.data_ptr())

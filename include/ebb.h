@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define EBB_ABI_VERSION 7
+#define EBB_ABI_VERSION 8
 #define EBB_EINVAL (-1)
 #define EBB_ETOOBIG (-2)
 
@@ -162,7 +162,10 @@ typedef struct EbbServerQueue {
  * count, the top boxes' bubbles, the bubble dictionaries, the interactive and keep-alive sets, InitializeBubbles,
  * CopyBubbles, the tick's dead-bubble flags and re-filings). W worlds of N slots (N at most EBB_SPACE_MAX_SLOTS);
  * `rows` maps a slot to its park row (-1 for none). Every per-slot array is [N][W], every per-entry array [cap][W]
- * and every key [3][cap][W] (world w's entry e at e W + w), one thread a world. Capacities a world: `boxes` box-table
+ * and every key [3][cap][W] (world w's entry e at e W + w), one thread a world; or, with `pitch` > 0, world-major:
+ * each pointer names world 0's copy of its array, entries consecutive in the shapes below without their [W], and world
+ * w's copy of every array starts w `pitch` bytes further on (`rnd` excepted: [W][EBB_RAND_WORDS] in both
+ * arrangements). Capacities a world: `boxes` box-table
  * entries (and the same for the fill's stack), `dicts` bubble dictionaries, `entries` dictionary entries in insertion
  * order, `sets` members of the interactive sets and of the keep-alive sets. A world that leaves the layer's domain is
  * flagged (EBB_SPACE_FLAG_*) and left alone by later operations. Field for field the state the reference's layer keeps
@@ -224,6 +227,10 @@ typedef struct EbbSpaceState {
     int32_t* rnd;                                                  /* [W][EBB_RAND_WORDS] */
     uint64_t *smask, *pmask;   /* the same keys as sets of slots (128 bits): [2][N][W] a sensor's, [2][W] the map's */
     int64_t lanes;             /* 1: a thread runs a world; 32: a warp runs a world (GetNearbyBalls split over it) */
+    int64_t pitch;             /* 0: the [..][W] arrangement; > 0 (a multiple of 16): world-major, bytes a world */
+    int64_t *box_parent, *box_top;   /* [boxes][W] a box's parent entry (-1 for a top box), its top box's entry */
+    int64_t *box_home, *box_slot;    /* [boxes][W] a box's home slot in box_hash, and the slot it sits in */
+    int64_t* fbox;     /* [8][N][W] a filed ball's box entries by side (bit c: the box beside its own on axis c) */
 } EbbSpaceState;
 /* K operations a world, applied in order: code, a (a slot), b (an integer argument), each [K][W], and f, each
  * operation's floating-point arguments [K][4][W] (ADD_SENSOR: range, period; NOTIFY_RANGE: range; TRACK: range, and

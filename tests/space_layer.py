@@ -111,44 +111,34 @@ class HostPark:
 class HostLayer:
     """The layer's state as numpy arrays (VecSpace's tensors, the same shapes), run by the host build."""
 
-    def __init__(self, W: int, n: int, boxes: int | None = None, seeds=None, events: int | None = None):
+    def __init__(self, W: int, n: int, boxes: int | None = None, seeds=None, events: int | None = None,
+                 world_major: bool = False):
+        from exact_ballpark_b200.space import allocate_state, state_spec
         self.W, self.N = W, n
         self.M = n * (n + 2) if events is None else events     # a tick's most: every pair entering, each range
         self.B, self.D, self.E, self.S = (boxes or 16 * n + 64), 8 * n + 16, 4 * n + 8, 2 * n + 8
-        self.rows = np.array([[w * n + j for w in range(W)] for j in range(n)], dtype=np.int64)
-        z = lambda *shape, dt=np.int64: np.zeros(shape, dtype=dt)   # noqa: E731
-        B, D, E, S = self.B, self.D, self.E, self.S
-        self.st = {
-            "level": z(n, W) - 1, "key": z(3, n, W), "mod": z(3, n, W) - 2, "active": z(n, W), "bubble": z(n, W) - 1,
-            "old_bubble": z(n, W) - 1, "seq": z(n, W), "my_box": z(n, W) - 1, "my_top": z(n, W) - 1,
-            "in_park": z(n, W, dt=np.uint8), "keep_alive": z(n, W, dt=np.uint8), "dead": z(n, W, dt=np.uint8),
-            "dropped": z(n, W, dt=np.uint8),
-            "box_level": z(B, W) - 1, "box_key": z(3, B, W), "box_balls": z(B, W), "box_kids": z(B, W),
-            "box_bubble": z(B, W) - 1, "stack": z(B, W), "box_n": z(W), "free_boxes": z(W),
-            "box_hash": z(2 * B, W), "box_free": z(B, W), "box_free_n": z(W),
-            "dict_bubble": z(D, W), "dict_n": z(W), "entry_bubble": z(E, W), "entry_id": z(E, W),
-            "entry_value": z(E, W), "entry_n": z(W), "inter_bubble": z(S, W), "inter_id": z(S, W), "inter_n": z(W),
-            "keep_bubble": z(S, W), "keep_id": z(S, W), "keep_n": z(W), "bubble_id": z(W), "seq_next": z(W),
-            "flags": z(W),
-            "srange": z(n, W, dt=np.float64), "speriod": z(n, W, dt=np.float64) + 2.0,
-            "selapsed": z(n, W, dt=np.float64), "ntf_range": z(n, W, dt=np.float64),
-            "trk_range": z(n, W, dt=np.float64), "trk": z(n, W) - 1, "cloaked": z(n, W),
-            "sonly": z(n, W, dt=np.uint8), "has_prox": z(n, W, dt=np.uint8), "ntf_in": z(n, W, dt=np.uint8),
-            "trk_in": z(n, W, dt=np.uint8), "slist": z(n, n, W, dt=np.uint8), "slen": z(n, W, dt=np.int32),
-            "sbkt": z(n, W, dt=np.int32) + 1, "pmap": z(n, W, dt=np.uint8), "pn": z(W, dt=np.int32),
-            "pbkt": z(W, dt=np.int32) + 1, "ev": z(self.M, W, dt=np.int32), "evn": z(W),
-            "rnd": np.stack([srand(seed) for seed in (seeds if seeds is not None else [1] * W)]),
-            "smask": z(2, n, W, dt=np.uint64), "pmask": z(2, W, dt=np.uint64)}
+        st, self.pitch = allocate_state(state_spec(n, self.B, self.D, self.E, self.S, n, self.M), W, "cpu",
+                                        world_major)
+        self._keep = st                                        # the tensors the numpy views below share memory with
+        self.st = {k: v.numpy() for k, v in st.items()}
+        self.rows = self.st.pop("rows")
+        self.rows[...] = np.array([[w * n + j for w in range(W)] for j in range(n)], dtype=np.int64)
+        self.st["rnd"] = np.stack([srand(seed) for seed in (seeds if seeds is not None else [1] * W)])
+
+    def _state(self):
+        from exact_ballpark_b200 import _native
+        s = _native.SpaceState()
+        s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets = self.W, self.N, self.B, self.D, self.E, self.S
+        s.umap_cap, s.events, s.lanes, s.pitch = self.N, self.M, 1, self.pitch
+        s.rows = self.rows.ctypes.data
+        for name, arr in self.st.items():
+            setattr(s, name, arr.ctypes.data)
+        return s
 
     def query(self, park: HostPark, kind: int, a, b, f) -> tuple:
         """One query a world on the host build: (out [1 + N][W], outd [N][W])."""
         from exact_ballpark_b200 import _native
-        s = _native.SpaceState()
-        s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets = self.W, self.N, self.B, self.D, self.E, self.S
-        s.umap_cap, s.events, s.lanes = self.N, self.M, 1
-        s.rows = self.rows.ctypes.data
-        for name, arr in self.st.items():
-            setattr(s, name, arr.ctypes.data)
+        s = self._state()
         a, b = (np.ascontiguousarray(np.asarray(x, dtype=np.int64).reshape(self.W)) for x in (a, b))
         f = np.ascontiguousarray(np.asarray(f, dtype=np.float64).reshape(5, self.W))
         out = np.zeros((1 + self.N, self.W), dtype=np.int64)
@@ -160,12 +150,7 @@ class HostLayer:
 
     def tape(self, park: HostPark, code, a, b, f=None) -> None:
         from exact_ballpark_b200 import _native
-        s = _native.SpaceState()
-        s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets = self.W, self.N, self.B, self.D, self.E, self.S
-        s.umap_cap, s.events, s.lanes = self.N, self.M, 1
-        s.rows = self.rows.ctypes.data
-        for name, arr in self.st.items():
-            setattr(s, name, arr.ctypes.data)
+        s = self._state()
         code, a, b = (np.ascontiguousarray(np.asarray(x, dtype=np.int64).reshape(-1, self.W)) for x in (code, a, b))
         K = code.shape[0]
         f = np.zeros((K, 4, self.W)) if f is None else np.ascontiguousarray(np.asarray(f, np.float64).reshape(K, 4,
@@ -360,9 +345,10 @@ def events_text(st: dict, park_ids, w: int, n: int) -> str:
     return "Q" + "".join(out) + "\n"
 
 
-def drive(streams: list, kernel: str = "host", device=None, lanes: int = 1) -> tuple:
+def drive(streams: list, kernel: str = "host", device=None, lanes: int = 1, world_major: bool | None = None) -> tuple:
     """Every stream through the layer, one world each, one operation a launch: (texts [world][op], flags [W]); a
-    HandleProximities operation's text ends with its events."""
+    HandleProximities operation's text ends with its events. `world_major`: the state's arrangement (None: the
+    layer's default for `lanes`; interleaved on the host)."""
     W = len(streams)
     seeds = [int(s[1]) if isinstance(s, tuple) else 1 for s in streams]
     streams = [s[0] if isinstance(s, tuple) else s for s in streams]
@@ -372,7 +358,7 @@ def drive(streams: list, kernel: str = "host", device=None, lanes: int = 1) -> t
     K = max(len(s) for s in streams)
     texts = [[] for _ in range(W)]
     if kernel == "host":
-        layer = HostLayer(W, N, seeds=seeds)
+        layer = HostLayer(W, N, seeds=seeds, world_major=bool(world_major))
 
         def run(code, a, b, f):
             layer.st["evn"][:] = 0
@@ -387,7 +373,7 @@ def drive(streams: list, kernel: str = "host", device=None, lanes: int = 1) -> t
         from exact_ballpark_b200.space import VecSpace
         dpark = VecModesPark(W * N, friction=FRICTION, tick_interval_ms=1000, device=device or "cuda")
         layer = VecSpace(dpark, np.arange(W * N, dtype=np.int64).reshape(W, N), events=N * (N + 2), seed=seeds,
-                         lanes=lanes)
+                         lanes=lanes, world_major=world_major)
 
         def run(code, a, b, f):
             for name in ("pos", "vel", "old_pos", "old_vel", "mass", "time_factor", "radius", "max_vel", "agility",
@@ -442,7 +428,7 @@ def drive(streams: list, kernel: str = "host", device=None, lanes: int = 1) -> t
     return texts, read()["flags"].copy()
 
 
-def drive_ticks(ops, device="cuda", seed: int = 1, lanes: int = 1) -> list:
+def drive_ticks(ops, device="cuda", seed: int = 1, lanes: int = 1, world_major: bool | None = None) -> list:
     """One ticking or mode stream (tests/golden/space_trace.py's tick_ops and mode_ops) through VecSpace over a
     VecModesPark on the device, its ticks the layer's `tick` (dead bubbles skipped, the re-filings and
     HandleProximities after): the texts after every operation, a tick's and HandleProximities' with their events. The
@@ -454,7 +440,8 @@ def drive_ticks(ops, device="cuda", seed: int = 1, lanes: int = 1) -> list:
     from exact_ballpark_b200.space import OP, VecSpace
     n = int(np.max(np.asarray(ops)[:, 1]))
     park = VecModesPark(n, friction=FRICTION, tick_interval_ms=1000, device=device)
-    layer = VecSpace(park, np.arange(n, dtype=np.int64).reshape(1, n), events=n * (n + 2), seed=seed, lanes=lanes)
+    layer = VecSpace(park, np.arange(n, dtype=np.int64).reshape(1, n), events=n * (n + 2), seed=seed, lanes=lanes,
+                     world_major=world_major)
     out = []
     dev = park.dev
     for op in ops:
@@ -537,7 +524,7 @@ def drive_ticks(ops, device="cuda", seed: int = 1, lanes: int = 1) -> list:
     return out
 
 
-def drive_ticks_host(ops, seed: int = 1) -> list:
+def drive_ticks_host(ops, seed: int = 1, world_major: bool = False) -> list:
     """drive_ticks on the CPU, for the ticking and the mode streams: the flight oracle's park (oracle/park.py's
     OraclePark, its tick the C++ oracle) owns the rows (AddBall, GotoPoint, Stop, FollowBall and Orbit with the
     layer's bubbles for their same-bubble test, WarpTo, RemoveBall's Stop and StopAllFollowers) and ticks them with
@@ -547,7 +534,7 @@ def drive_ticks_host(ops, seed: int = 1) -> list:
     from oracle.park import OraclePark
     n = int(np.max(np.asarray(ops)[:, 1]))
     op = OraclePark(n, friction=FRICTION, tick_interval_ms=1000)
-    host, layer = HostPark(n), HostLayer(1, n, seeds=[seed])
+    host, layer = HostPark(n), HostLayer(1, n, seeds=[seed], world_major=world_major)
 
     def pull() -> None:                                   # the layer's view of the oracle park's rows
         for name in ("pos", "vel", "old_pos", "old_vel"):

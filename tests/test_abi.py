@@ -26,7 +26,7 @@ def test_the_library_exports_every_declared_entry_point():
 
 def test_abi_version_and_scratch_size():
     lib = _native.lib()
-    assert lib.ebb_abi() == _native.ABI == 7
+    assert lib.ebb_abi() == _native.ABI == 8
     assert lib.ebb_flight_scratch_bytes(0) == 0
     b = lib.ebb_flight_scratch_bytes(1000)
     assert b >= 1000 * (8 * 7 + 1) and b % 256 == 0
@@ -87,12 +87,14 @@ def test_the_space_tape_refuses_a_missing_box_index_before_launching():
     lib = _native.lib()
     p, s, t = _native.FlightState(), _native.SpaceState(), _native.SpaceTape()
     s.worlds, s.slots, s.boxes, s.dicts, s.entries, s.sets, t.K = 4, 10, 64, 16, 16, 16, 1
+    s.umap_cap, s.events, s.lanes, s.pitch = 10, 16, 32, 1024     # valid: only the missing buffer refuses the call
     fake = 4096
     for st in (p, s, t):
         for name, kind in type(st)._fields_:
             if kind is ctypes.c_void_p:
                 setattr(st, name, fake)
-    for missing in ("box_hash", "box_free", "box_free_n", "my_box", "my_top"):
+    for missing in ("box_hash", "box_free", "box_free_n", "my_box", "my_top", "box_parent", "box_top", "box_home",
+                    "box_slot", "fbox"):
         keep = getattr(s, missing)
         setattr(s, missing, None)
         rc = lib.ebb_space_tape(ctypes.byref(p), ctypes.byref(s), ctypes.byref(t), None, 128)

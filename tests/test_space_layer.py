@@ -33,10 +33,12 @@ def _inputs(scs):
     return [(sc["ops"], sc["rand_seed"]) for sc in scs]
 
 
-def test_the_layers_program_matches_the_oracle_after_every_operation():
+@pytest.mark.parametrize("world_major", [False, True])
+def test_the_layers_program_matches_the_oracle_after_every_operation(world_major):
+    """The host build over the interleaved state and over the world-major arena."""
     scs = _streams()
     assert len(scs) == 72
-    texts, flags = sl.drive(_inputs(scs), "host")
+    texts, flags = sl.drive(_inputs(scs), "host", world_major=world_major)
     assert not (flags & ~HUGE).any()
     bad = []
     for sc, got in zip(scs, texts):
@@ -99,31 +101,35 @@ def test_the_layers_tick_matches_the_oracle_in_crowded_sensing_worlds_on_the_cpu
     assert not bad, f"{len(bad)} worlds differ, first {bad[:3]}"
 
 
-@pytest.mark.parametrize("family", ["tick", "modes"])
-def test_the_layers_tick_matches_the_oracle_on_the_cpu(family):
+@pytest.mark.parametrize("family,world_major", [("tick", False), ("modes", False), ("tick", True)])
+def test_the_layers_tick_matches_the_oracle_on_the_cpu(family, world_major):
     """The ticking and the mode streams (GOTO and STOP ships; FollowBall, Orbit and WarpTo with drop-outs, releases
     and re-added followers): the layer's host build around the flight oracle's tick (dead rows skipped), every state
-    after every operation against the space oracle's."""
+    after every operation against the space oracle's; the ticking ones over the world-major arena too."""
     scs = _streams((family,))
     assert len(scs) == 40
     bad = []
     for sc in scs:
-        got = sl.drive_ticks_host(sc["ops"], sc["rand_seed"])
+        got = sl.drive_ticks_host(sc["ops"], sc["rand_seed"], world_major=world_major)
         want = _oracle_texts(sc)
         if got != want:
             bad.append((sc["seed"], next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
     assert not bad, f"{len(bad)} worlds differ, first {bad[:3]}"
 
 
+ARRANGEMENTS = [(1, False), (32, True), (1, True), (32, False)]   # (lanes, world-major): the defaults first
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("lanes", [1, 32])
-def test_the_device_layer_matches_its_host_program_word_for_word(lanes):
-    """A thread a world and a warp a world (its lanes splitting GetNearbyBalls' scan and sort)."""
+@pytest.mark.parametrize("lanes,world_major", ARRANGEMENTS)
+def test_the_device_layer_matches_its_host_program_word_for_word(lanes, world_major):
+    """A thread a world and a warp a world (its lanes splitting GetNearbyBalls' scan and sort), over the interleaved
+    state and the world-major arena."""
     import torch
     assert torch.cuda.is_available()
     scs = _streams()
     streams = _inputs(scs)
-    got, flags = sl.drive(streams, "cuda", lanes=lanes)
+    got, flags = sl.drive(streams, "cuda", lanes=lanes, world_major=world_major)
     want, _ = sl.drive(streams, "host")
     assert not (flags & ~HUGE).any()
     bad = [sc["seed"] for sc, g, w in zip(scs, got, want) if g != w]
@@ -133,9 +139,9 @@ def test_the_device_layer_matches_its_host_program_word_for_word(lanes):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("lanes", [1, 32])
+@pytest.mark.parametrize("lanes,world_major", ARRANGEMENTS[:3])
 @pytest.mark.parametrize("family", ["tick", "modes"])
-def test_the_layers_tick_over_the_flight_park_matches_the_oracle(family, lanes):
+def test_the_layers_tick_over_the_flight_park_matches_the_oracle(family, lanes, world_major):
     """The ticking streams (GOTO and STOP ships across top boxes and bubbles, with sensors, tracked targets and
     notification ranges) and the mode streams (FollowBall, Orbit, WarpTo with drop-outs, releases, re-added
     followers, sensors): VecSpace.tick over a VecModesPark (the dead bubbles' rows skipped by the park's tick, then
@@ -147,7 +153,7 @@ def test_the_layers_tick_over_the_flight_park_matches_the_oracle(family, lanes):
     assert len(scs) == 40
     bad = []
     for sc in scs:
-        got = sl.drive_ticks(sc["ops"], seed=sc["rand_seed"], lanes=lanes)
+        got = sl.drive_ticks(sc["ops"], seed=sc["rand_seed"], lanes=lanes, world_major=world_major)
         want = _oracle_texts(sc)
         if got != want:
             bad.append((sc["seed"], next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
@@ -155,15 +161,15 @@ def test_the_layers_tick_over_the_flight_park_matches_the_oracle(family, lanes):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("lanes", [1, 32])
-def test_the_layers_tick_matches_the_oracle_in_crowded_sensing_worlds(lanes):
+@pytest.mark.parametrize("lanes,world_major", ARRANGEMENTS[:2])
+def test_the_layers_tick_matches_the_oracle_in_crowded_sensing_worlds(lanes, world_major):
     """The crowded worlds (16 to 128 sensing ships) through VecSpace.tick over a VecModesPark on the device, a thread
-    or a warp a world."""
+    a world over the interleaved state or a warp a world over the world-major arena."""
     import torch
     assert torch.cuda.is_available()
     bad = []
     for sc in _crowd():
-        got = sl.drive_ticks(sc["ops"], seed=sc["rand_seed"], lanes=lanes)
+        got = sl.drive_ticks(sc["ops"], seed=sc["rand_seed"], lanes=lanes, world_major=world_major)
         want = _oracle_texts(sc)
         if got != want:
             bad.append((sc["seed"], next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
