@@ -1270,7 +1270,7 @@ def main() -> None:
     ap.add_argument("--space-steps", type=int, default=5)
     ap.add_argument("--partition-worlds", type=int, default=100000)
     ap.add_argument("--partition-steps", type=int, default=10)
-    ap.add_argument("--partition-warp-class", type=int, default=64,
+    ap.add_argument("--partition-warp-class", type=int, default=32,
                     help="the ragged batch's size classes from this size up run a warp a world (129: none)")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-seconds", type=float, default=6.0)

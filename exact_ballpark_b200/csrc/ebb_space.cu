@@ -1,6 +1,8 @@
 // SPDX-License-Identifier: MIT
 // The space layer's tape on the device: one thread (or one warp) a world runs its K operations in order
-// (ebb_space.cuh), over the state in either arrangement (interleaved [entry][world], or world-major).
+// (ebb_space.cuh), over the state in either arrangement (interleaved [entry][world], or world-major). The parameter
+// structs are __grid_constant__: the program reads its state's pointers through their addresses in the parameter
+// space (uniform constant loads) rather than from a per-thread copy in local memory.
 #include <cuda_runtime.h>
 
 #include "../../include/ebb.h"
@@ -10,7 +12,9 @@ namespace ebb {
 namespace space {
 
 template <bool WM>
-__global__ void __launch_bounds__(128, 6) tape_kernel(const EbbFlightState p, const EbbSpaceState s, const EbbSpaceTape t) {
+__global__ void __launch_bounds__(128, 6) tape_kernel(const __grid_constant__ EbbFlightState p,
+                                                   const __grid_constant__ EbbSpaceState s,
+                                                   const __grid_constant__ EbbSpaceTape t) {
     const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= s.worlds) return;
     run_tape<WM>(&p, &s, &t, w);
@@ -18,8 +22,9 @@ __global__ void __launch_bounds__(128, 6) tape_kernel(const EbbFlightState p, co
 
 // a warp a world: the world's index is the warp's, the lanes run its program together (ebb_space.cuh's World)
 template <bool WM>
-__global__ void __launch_bounds__(128, 6) tape_kernel_warp(const EbbFlightState p, const EbbSpaceState s,
-                                                        const EbbSpaceTape t) {
+__global__ void __launch_bounds__(128, 12) tape_kernel_warp(const __grid_constant__ EbbFlightState p,
+                                                         const __grid_constant__ EbbSpaceState s,
+                                                         const __grid_constant__ EbbSpaceTape t) {
     __shared__ Coop scratch[4];
     const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (w >= s.worlds) return;                            // (the whole warp: w is the warp's)
@@ -27,7 +32,9 @@ __global__ void __launch_bounds__(128, 6) tape_kernel_warp(const EbbFlightState 
 }
 
 template <bool WM>
-__global__ void __launch_bounds__(128) query_kernel(const EbbFlightState p, const EbbSpaceState s, const EbbSpaceQuery q) {
+__global__ void __launch_bounds__(128) query_kernel(const __grid_constant__ EbbFlightState p,
+                                                    const __grid_constant__ EbbSpaceState s,
+                                                    const __grid_constant__ EbbSpaceQuery q) {
     const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= s.worlds) return;
     run_query<WM>(&p, &s, &q, w);

@@ -755,8 +755,8 @@ struct World {
         while (S < N) S <<= 1;
         return S;
     }
-    // A bitonic sort of the warp's scratch (sh->key, sh->id, carrying sh->out) by (key, id) over the first S slots
-    // (sort_span: the slots past N hold no candidate and sort last), the lanes taking the pairs of each stage
+    // A bitonic sort of the warp's scratch (sh->key, sh->id, carrying sh->out) by (key, id) over its first S entries
+    // (S a power of two), the lanes taking the pairs of each stage
     __device__ void warp_sort(int S) const {
         for (int k = 2; k <= S; k <<= 1)
             for (int jj = k >> 1; jj > 0; jj >>= 1) {
@@ -781,13 +781,15 @@ struct World {
     }
 
     // nearby's warp form: each lane takes the slots lane, lane + 32, ...: the filter and the walk key (NOT_A_CANDIDATE
-    // for a ball that is none), then a bitonic sort of the slots by (key, id) over the lanes (ids are distinct, so
+    // for a ball that is none); the candidates are packed to the front of the scratch (a ballot a round) and sorted
+    // by (key, id) over the lanes, a bitonic sort of their count rounded up to a power of two (ids are distinct, so
     // the order is the serial insertion's); every lane reads the order back
     __device__ int nearby_warp(int64_t b, int64_t bub, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked,
                                uint8_t* out) const {
-        int mine = 0;
+        int n = 0;
         const int S = sort_span();
-        for (int64_t o = lane; o < S; o += 32) {
+        for (int64_t base = 0; base < S; base += 32) {     // the candidates packed to the front, in slot order
+            const int64_t o = base + lane;
             int64_t k = NOT_A_CANDIDATE, i = INT64_MAX;
             if (o < N && o != b && slot_ok(o) && U(s->in_park, o) && lvl(o) >= 0) {
                 k = walk_key(b, o);
@@ -802,14 +804,24 @@ struct World {
                     else i = p->ids[r];
                 }
             }
-            mine += k != NOT_A_CANDIDATE;
-            sh->key[o] = k;
-            sh->id[o] = i;
-            sh->out[o] = (uint8_t)o;
+            const bool is = k != NOT_A_CANDIDATE;
+            const unsigned in = __ballot_sync(0xffffffffu, is);
+            if (is) {
+                const int at_ = n + __popc(in & ((1u << lane) - 1u));
+                sh->key[at_] = k;
+                sh->id[at_] = i;
+                sh->out[at_] = (uint8_t)o;
+            }
+            n += __popc(in);
         }
-        const int n = (int)__reduce_add_sync(0xffffffffu, (unsigned)mine);
+        int P = 1;                                         // the sort's span: the candidates, to a power of two
+        while (P < n) P <<= 1;
+        for (int e = n + lane; e < P; e += 32) {
+            sh->key[e] = NOT_A_CANDIDATE;
+            sh->id[e] = INT64_MAX;
+        }
         __syncwarp();
-        warp_sort(S);
+        warp_sort(P);
         for (int i = 0; i < n; ++i) out[i] = sh->out[i];
         __syncwarp();
         return n;

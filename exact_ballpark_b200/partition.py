@@ -28,7 +28,7 @@ from .modes import WARP, VecModesPark
 from .space import OP, VecSpace
 
 CLASSES = (4, 8, 16, 32, 64, 128)
-WARP_CLASS = 64                  # the ragged batch's classes from this size up run a warp a world
+WARP_CLASS = 32                  # the ragged batch's classes from this size up run a warp a world
 BOOL, I64 = torch.bool, torch.int64
 
 
