@@ -358,8 +358,12 @@ struct World {
     EBB_HD int64_t topmost_of(int64_t e) const { return I(s->box_top, e); }
     // a free ball's radius plus a tick at full thrust (Ball::GetInflatedRadius)
     EBB_HD double inflated_radius(int64_t j, const double* v) const {
+        return inflated_radius_of(j, p->radius[row(j)], v);
+    }
+    // the same for a radius `rf` in place of the ball's own (a sensor's inflated one)
+    EBB_HD double inflated_radius_of(int64_t j, float rf, const double* v) const {
         const int64_t r = row(j);
-        const double radius = (double)p->radius[r];
+        const double radius = (double)rf;
         if (!p->free_[r]) return radius;
         const double m = dmul(p->mass[r], (double)p->agility[r]);
         const double k = p->friction;
@@ -372,6 +376,20 @@ struct World {
     EBB_HD static void key_for(int level, const double* x, int64_t* k) {
         const double fac = level_inv(level), half = level_half(level);
         for (int c = 0; c < 3; ++c) k[c] = to_i64(dmul(dadd(x[c], half), fac));
+    }
+    // the sides a sphere of radius `inflated` at x reaches out of its box (key `key0` at level0): -1, 0 or 1 an axis
+    EBB_HD static void side_mods(int level0, const int64_t* key0, double inflated, const double* x, int64_t* m) {
+        const double wd = level_width(level0);
+        const double center = dmul(dmul(wd, (double)level_grid(level0)), 0.5);
+        for (int q = 0; q < 3; ++q) {
+            m[q] = 0;
+            const double lo = dsub(dmul((double)key0[q], wd), center);
+            const double hi = dsub(dmul((double)(key0[q] + 1), wd), center);
+            if (dsub(dadd(lo, inflated), x[q]) > 0.0)
+                m[q] = -1;
+            else if (dsub(dsub(hi, inflated), x[q]) < 0.0)
+                m[q] = 1;
+        }
     }
 
     // ---- bubbles ----
@@ -529,17 +547,8 @@ struct World {
     EBB_HDNI void ball_insert_in_boxes(int64_t j, const double* x, double inflated, int level0, const int64_t* key0,
                                      int64_t box0, int fate_box1, int64_t new_bubble) {
         if (fate_box1 == 2) flag(F_UNDEFINED);             // a deleted box's memory read
-        const double wd = level_width(level0);
-        const double center = dmul(dmul(wd, (double)level_grid(level0)), 0.5);
-        int64_t m[3] = {0, 0, 0};
-        for (int q = 0; q < 3; ++q) {
-            const double lo = dsub(dmul((double)key0[q], wd), center);
-            const double hi = dsub(dmul((double)(key0[q] + 1), wd), center);
-            if (dsub(dadd(lo, inflated), x[q]) > 0.0)
-                m[q] = -1;
-            else if (dsub(dsub(hi, inflated), x[q]) < 0.0)
-                m[q] = 1;
-        }
+        int64_t m[3];
+        side_mods(level0, key0, inflated, x, m);
         if (lvl(j) >= 0 && lvl(j) == level0 && key(j, 0) == key0[0] && key(j, 1) == key0[1] && key(j, 2) == key0[2] &&
             mod(j, 0) == m[0] && mod(j, 1) == m[1] && mod(j, 2) == m[2])
             return;
@@ -644,6 +653,17 @@ struct World {
             *hi = k + (m > 0 ? m : 0);
         }
     }
+    // A filing as the walk reads it: the level and each axis's key range
+    struct Filing {
+        int64_t L;
+        int64_t lo[3], hi[3];
+    };
+    EBB_HD Filing filing_of(int64_t j) const {
+        Filing f;
+        f.L = lvl(j);
+        for (int q = 0; q < 3; ++q) key_range(j, q, &f.lo[q], &f.hi[q]);
+        return f;
+    }
     // The position of slot o's first box in slot b's walk, or NOT_A_CANDIDATE when no box of o is one of b's, an
     // ancestor of one or below one. b's boxes are walked in key order; at each, its ancestors holding balls bottom-up
     // (those not met before), its descendants in post-order (children by key), then the box itself. The key: the
@@ -651,19 +671,16 @@ struct World {
     // the ancestor's distance or the box's post-order code (path digits below b's level, 64 past o's level).
     // Relatedness factors over the axes: the finer filing's key range, shifted to the coarser level, meets the
     // coarser's.
-    EBB_HDNI int64_t walk_key(int64_t b, int64_t o) const {
-        const int64_t Lb = lvl(b), Ln = lvl(o);
-        int64_t lo_b[3], hi_b[3], lo_n[3], hi_n[3], cb[3];
-        for (int q = 0; q < 3; ++q) {
-            key_range(b, q, &lo_b[q], &hi_b[q]);
-            key_range(o, q, &lo_n[q], &hi_n[q]);
-            cb[q] = hi_b[q] - lo_b[q] + 1;
-        }
+    EBB_HD int64_t walk_key(const Filing& fb, int64_t o) const {
+        const Filing fo = filing_of(o);
+        const int64_t Lb = fb.L, Ln = fo.L;
+        int64_t cb[3];
+        for (int q = 0; q < 3; ++q) cb[q] = fb.hi[q] - fb.lo[q] + 1;
         const bool coarse = Ln <= Lb;
         const int64_t sh = 2 * (coarse ? Lb - Ln : Ln - Lb);
         for (int q = 0; q < 3; ++q) {
-            const int64_t xl = (coarse ? lo_b[q] : lo_n[q]) >> sh, xh = (coarse ? hi_b[q] : hi_n[q]) >> sh;
-            const int64_t yl = coarse ? lo_n[q] : lo_b[q], yh = coarse ? hi_n[q] : hi_b[q];
+            const int64_t xl = (coarse ? fb.lo[q] : fo.lo[q]) >> sh, xh = (coarse ? fb.hi[q] : fo.hi[q]) >> sh;
+            const int64_t yl = coarse ? fo.lo[q] : fb.lo[q], yh = coarse ? fo.hi[q] : fb.hi[q];
             if ((xl > yl ? xl : yl) > (xh < yh ? xh : yh)) return NOT_A_CANDIDATE;
         }
         int64_t span = 1;
@@ -673,57 +690,58 @@ struct World {
             for (int q = 0; q < 3; ++q) {
                 idx[q] = 0;
                 while (idx[q] + 1 < cb[q]) {
-                    const int64_t v = (lo_b[q] + idx[q]) >> sh;
-                    if (v >= lo_n[q] && v <= hi_n[q]) break;
+                    const int64_t v = (fb.lo[q] + idx[q]) >> sh;
+                    if (v >= fo.lo[q] && v <= fo.hi[q]) break;
                     ++idx[q];
                 }
             }
             const int64_t seg = (idx[0] * cb[1] + idx[1]) * cb[2] + idx[2];
             return Ln < Lb ? (seg * 3) * span + (Lb - Ln) : (seg * 3 + 2) * span;
         }
-        int64_t best = NOT_A_CANDIDATE;                    // below: the least code over o's boxes under b's
-        for (int64_t bx = lo_n[0]; bx <= hi_n[0]; ++bx)
-            for (int64_t by = lo_n[1]; by <= hi_n[1]; ++by)
-                for (int64_t bz = lo_n[2]; bz <= hi_n[2]; ++bz) {
-                    const int64_t box[3] = {bx, by, bz};
-                    int64_t jx[3];
-                    bool ok = true;
-                    for (int q = 0; q < 3; ++q) {
-                        const int64_t anc = box[q] >> sh;
-                        if (anc < lo_b[q] || anc > hi_b[q]) ok = false;
-                        jx[q] = anc - lo_b[q];
-                    }
-                    if (!ok) continue;
-                    const int64_t seg = (jx[0] * cb[1] + jx[1]) * cb[2] + jx[2];
-                    int64_t code = 0, power = span;
-                    for (int64_t li = 1; li < NUM_LEVELS; ++li) {
-                        power /= CODE_BASE;
-                        const int64_t shift = 2 * (Ln - li) > 0 ? 2 * (Ln - li) : 0;
-                        int64_t digit =
-                            ((box[0] >> shift) & 3) * 16 + ((box[1] >> shift) & 3) * 4 + ((box[2] >> shift) & 3);
-                        if (li > Ln) digit = CODE_BASE - 1;
-                        if (li <= Lb) digit = 0;
-                        code += digit * power;
-                    }
-                    const int64_t k = (seg * 3 + 1) * span + code;
-                    if (k < best) best = k;
+        // below: the least key over o's boxes under b's. o's boxes are the product of its axes' keys, and the key is
+        // the index of b's box (lexicographic in the axes' indices), then the post-order code, whose digit at a level
+        // is 16 x + 4 y + z of the box's path (0 above b's level, 64 past o's): a sum of one term an axis. So the least
+        // key takes on each axis the least index, and among the keys with it the least path term.
+        int64_t jmin[3], pmin[3];
+        for (int q = 0; q < 3; ++q) {
+            jmin[q] = INT64_MAX;
+            pmin[q] = INT64_MAX;
+            for (int64_t v = fo.lo[q]; v <= fo.hi[q]; ++v) {
+                const int64_t anc = v >> sh;
+                if (anc < fb.lo[q] || anc > fb.hi[q]) continue;
+                const int64_t jq = anc - fb.lo[q];
+                int64_t path = 0;                          // the path's digits on this axis, base 65, levels Lb+1..Ln
+                for (int64_t li = Lb + 1; li <= Ln; ++li) path = path * CODE_BASE + ((v >> (2 * (Ln - li))) & 3);
+                if (jq < jmin[q] || (jq == jmin[q] && path < pmin[q])) {
+                    jmin[q] = jq;
+                    pmin[q] = path;
                 }
-        return best;
+            }
+            if (jmin[q] == INT64_MAX) return NOT_A_CANDIDATE;
+        }
+        int64_t tail = 1;                                  // 65 ^ (levels past o's)
+        for (int64_t li = Ln + 1; li < NUM_LEVELS; ++li) tail *= CODE_BASE;
+        const int64_t seg = (jmin[0] * cb[1] + jmin[1]) * cb[2] + jmin[2];
+        const int64_t code = tail * (16 * pmin[0] + 4 * pmin[1] + pmin[2] + 1) - 1;   // the 64s past o's level: tail - 1
+        return (seg * 3 + 1) * span + code;
     }
     // GetNearbyBalls from slot b (no missiles, fields or global balls here): the balls filed in related boxes that
     // pass the filter, in the walk's order (its key, then id), into out; returns their count
-    EBB_HDNI int nearby(int64_t b, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked, uint8_t* out) const {
+    // (`as`: b's filing for the walk in place of its own, the sensor's inflated one when it is not re-filed)
+    EBB_HDNI int nearby(int64_t b, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked, uint8_t* out,
+                        const Filing* as = nullptr) const {
         const int64_t bub = I(s->bubble, b);
         if (exclude_inert && !set_any(0, bub)) return 0;
         if (lvl(b) < 0) return 0;
+        const Filing fb = as ? *as : filing_of(b);
 #ifdef __CUDA_ARCH__
-        if (lane >= 0) return nearby_warp(b, bub, exclude_fixed, exclude_inert, exclude_cloaked, out);
+        if (lane >= 0) return nearby_warp(b, bub, exclude_fixed, exclude_inert, exclude_cloaked, out, fb);
 #endif
         int64_t keys[EBB_SPACE_MAX_SLOTS], oid[EBB_SPACE_MAX_SLOTS];
         int n = 0;
         for (int64_t o = 0; o < N; ++o) {
             if (o == b || !slot_ok(o) || !U(s->in_park, o) || lvl(o) < 0) continue;
-            const int64_t k = walk_key(b, o);
+            const int64_t k = walk_key(fb, o);
             if (k == NOT_A_CANDIDATE) continue;
             const int64_t r = row(o);
             if (exclude_cloaked && (at(s->cloaked, o) != 0 || !p->massive[r])) continue;
@@ -785,14 +803,14 @@ struct World {
     // by (key, id) over the lanes, a bitonic sort of their count rounded up to a power of two (ids are distinct, so
     // the order is the serial insertion's); every lane reads the order back
     __device__ int nearby_warp(int64_t b, int64_t bub, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked,
-                               uint8_t* out) const {
+                               uint8_t* out, const Filing& fb) const {
         int n = 0;
         const int S = sort_span();
         for (int64_t base = 0; base < S; base += 32) {     // the candidates packed to the front, in slot order
             const int64_t o = base + lane;
             int64_t k = NOT_A_CANDIDATE, i = INT64_MAX;
             if (o < N && o != b && slot_ok(o) && U(s->in_park, o) && lvl(o) >= 0) {
-                k = walk_key(b, o);
+                k = walk_key(fb, o);
                 const int64_t r = row(o);
                 if (k != NOT_A_CANDIDATE) {
                     bool keep = !(exclude_cloaked && (at(s->cloaked, o) != 0 || !p->massive[r]));
@@ -1062,6 +1080,136 @@ struct World {
     // CheckForProximity_Sensor (Ball.cpp:642; SEN-701, SEN-702): every period, GetNearbyBalls with the sensor's
     // radius inflated and the velocity zeroed (the ball re-filed for it and back), the balls no longer near first (in
     // the list's order), then each candidate in the walk's order entering or leaving (the inside test in float sums)
+    // CheckSensor's two re-filings (the ball at its radius plus the sensor's range, velocity zeroed; then back) when
+    // they leave no trace but BoxAllocator's kept count. That holds when the ball comes back to the filing it has
+    // (the same level, keys and sides) and its top box keeps its bubble, the ball's: the live boxes are then those of
+    // every ball's filing, as before; each box's ball and child counts follow from them; no bubble, dictionary or set
+    // changes; no released box is read. Conditions, each checked (else false, nothing done): the ball filed, neither
+    // filing huge, the world unflagged; the top box's bubble the ball's; the inflated box live and not emptied by the
+    // ball's leaving, no top box emptied; the inflated sides inside the grid; room in the table for every box the
+    // pair makes; the kept count below 256 throughout (every release kept). Then the pair's boxes are counted, not
+    // made: `a` released by the ball's leaving (`a1` of them on its own box's chain, re-made by the second GetBox),
+    // `b` made for the inflated sides (released again by the second leaving), and the kept count moves as the pair
+    // would move it (+a; -b floored at 0; -a1 floored; +b; -(a - a1) floored). `fi`: the inflated filing, for
+    // GetNearbyBalls.
+    EBB_HDNI bool sensor_fast(int64_t j, const double* x, const double* v, float inflated, Filing* fi) {
+        if (lvl(j) < 0 || huge(j) || one(s->flags) != 0) return false;
+        const int64_t r = row(j);
+        const int64_t box0 = I(s->my_box, j), top = I(s->my_top, j);
+        if (box0 < 0 || top < 0) return false;
+        const int64_t bub = I(s->box_bubble, top);
+        if (bub == -1 || bub != I(s->bubble, j)) return false;
+        // the filing it comes back to: its own
+        const double infl1 = inflated_radius(j, v);
+        const int L1 = level_for(infl1);
+        if (L1 != lvl(j) || (L1 == 0 && (double)fmul(p->radius[r], 2.0f) > level_width(0))) return false;
+        int64_t k1[3], m1[3];
+        key_for(L1, x, k1);
+        side_mods(L1, k1, infl1, x, m1);
+        for (int c = 0; c < 3; ++c)
+            if (k1[c] != key(j, c) || m1[c] != mod(j, c)) return false;
+        // the inflated filing
+        const double rest[3] = {0.0, 0.0, 0.0};
+        const double infl = inflated_radius_of(j, inflated, rest);
+        const int Li = level_for(infl);
+        if (Li == 0 && (double)fmul(inflated, 2.0f) > level_width(0)) return false;
+        int64_t ki[3], mi[3];
+        key_for(Li, x, ki);
+        side_mods(Li, ki, infl, x, mi);
+        fi->L = Li;
+        for (int c = 0; c < 3; ++c) {
+            fi->lo[c] = ki[c] + (mi[c] < 0 ? mi[c] : 0);
+            fi->hi[c] = ki[c] + (mi[c] > 0 ? mi[c] : 0);
+        }
+        if (Li == L1 && ki[0] == k1[0] && ki[1] == k1[1] && ki[2] == k1[2] && mi[0] == m1[0] && mi[1] == m1[1] &&
+            mi[2] == m1[2])
+            return true;                                   // both re-filings return at once
+        const int64_t boxi = box_find(Li, ki[0], ki[1], ki[2]);
+        if (boxi < 0) return false;
+        // the boxes the ball's leaving empties: its boxes, then each parent left with nothing
+        constexpr int CAP = 40;
+        int64_t ent[CAP], nb[CAP], nk[CAP];                // entries touched, their ball and child counts after
+        bool gone[CAP];
+        int ne = 0;
+        auto slot_of_entry = [&](int64_t e) -> int {
+            for (int i = 0; i < ne; ++i)
+                if (ent[i] == e) return i;
+            if (ne == CAP) return -1;
+            ent[ne] = e;
+            nb[ne] = I(s->box_balls, e);
+            nk[ne] = I(s->box_kids, e);
+            gone[ne] = false;
+            return ne++;
+        };
+        int64_t a = 0;
+        for (int bits = 0; bits < 8; ++bits) {
+            if (((bits & 1) && !m1[0]) || ((bits & 2) && !m1[1]) || ((bits & 4) && !m1[2])) continue;
+            int64_t e = fbox(j, bits);
+            if (e < 0) return false;
+            int i = slot_of_entry(e);
+            if (i < 0) return false;
+            --nb[i];
+            while (nb[i] == 0 && nk[i] == 0 && !gone[i]) {
+                gone[i] = true;
+                ++a;
+                if (e == boxi || I(s->box_level, e) == 0) return false;   // the inflated box, or a top box, emptied
+                e = I(s->box_parent, e);
+                if (e < 0) break;
+                i = slot_of_entry(e);
+                if (i < 0) return false;
+                --nk[i];
+            }
+        }
+        auto released = [&](int64_t e) -> bool {
+            for (int i = 0; i < ne; ++i)
+                if (ent[i] == e) return gone[i];
+            return false;
+        };
+        int64_t a1 = 0;
+        for (int64_t e = box0; e >= 0 && released(e); e = I(s->box_parent, e)) ++a1;
+        // the boxes the inflated sides make: each side's missing chain, up to a live box or one made before
+        int64_t made_key[CAP][3];
+        int made_lvl[CAP];
+        int nm = 0;
+        const int64_t g = level_grid(Li);
+        int64_t b = 0;
+        for (int side = 1; side < 8; ++side) {
+            const int64_t oa = (side & 1) ? mi[0] : 0, ob = (side & 2) ? mi[1] : 0, oc = (side & 4) ? mi[2] : 0;
+            if (((side & 1) && !mi[0]) || ((side & 2) && !mi[1]) || ((side & 4) && !mi[2])) continue;
+            const int64_t sk[3] = {ki[0] + oa, ki[1] + ob, ki[2] + oc};
+            for (int c = 0; c < 3; ++c)
+                if (sk[c] < 0 || sk[c] >= g) return false;   // the grid's edge
+            for (int L = Li; L >= 0; --L) {
+                const int sh = 2 * (Li - L);
+                const int64_t kx = sk[0] >> sh, ky = sk[1] >> sh, kz = sk[2] >> sh;
+                bool have = false;
+                for (int i = 0; i < nm && !have; ++i)
+                    have = made_lvl[i] == L && made_key[i][0] == kx && made_key[i][1] == ky && made_key[i][2] == kz;
+                if (!have) {
+                    const int64_t e = box_find(L, kx, ky, kz);
+                    have = e >= 0 && !released(e);
+                }
+                if (have) break;
+                if (nm == CAP) return false;
+                made_lvl[nm] = L;
+                made_key[nm][0] = kx;
+                made_key[nm][1] = ky;
+                made_key[nm][2] = kz;
+                ++nm;
+                ++b;
+            }
+        }
+        const int64_t live = one(s->box_n) - one(s->box_free_n);
+        int64_t c = one(s->free_boxes);
+        if (B - live < b + 8 || c + a + b >= BOX_KEEP) return false;
+        c += a;
+        c = c > b ? c - b : 0;
+        c = c > a1 ? c - a1 : 0;
+        c += b;
+        c = c > a - a1 ? c - (a - a1) : 0;
+        one(s->free_boxes) = c;
+        return true;
+    }
     EBB_HDNI void check_sensor(int64_t j) {
         at(s->selapsed, j) = dadd(at(s->selapsed, j), p->dt);
         if (at(s->selapsed, j) < at(s->speriod, j)) return;
@@ -1072,15 +1220,21 @@ struct World {
         const double v[3] = {vel(j, 0), vel(j, 1), vel(j, 2)};
         const double rest[3] = {0.0, 0.0, 0.0};
         const float inflated = fadd(radius, (float)at(s->srange, j));
-        if (!(inflated < 0.0f)) {
-            p->radius[r] = inflated;
-            insert_in_boxes(j, x, rest);
-        }
         uint8_t cand[EBB_SPACE_MAX_SLOTS];
-        const int nc = nearby(j, at(s->cloaked, j) == 0, at(s->sonly, j) != 0, false, cand);
-        if (!(radius < 0.0f)) {
-            p->radius[r] = radius;
-            insert_in_boxes(j, x, v);
+        int nc;
+        Filing fi;
+        if (!(inflated < 0.0f) && !(radius < 0.0f) && sensor_fast(j, x, v, inflated, &fi)) {
+            nc = nearby(j, at(s->cloaked, j) == 0, at(s->sonly, j) != 0, false, cand, &fi);
+        } else {
+            if (!(inflated < 0.0f)) {
+                p->radius[r] = inflated;
+                insert_in_boxes(j, x, rest);
+            }
+            nc = nearby(j, at(s->cloaked, j) == 0, at(s->sonly, j) != 0, false, cand);
+            if (!(radius < 0.0f)) {
+                p->radius[r] = radius;
+                insert_in_boxes(j, x, v);
+            }
         }
 #ifdef __CUDA_ARCH__
         if (lane >= 0) {
