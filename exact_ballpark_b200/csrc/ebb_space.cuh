@@ -1126,10 +1126,24 @@ struct World {
             return true;                                   // both re-filings return at once
         const int64_t boxi = box_find(Li, ki[0], ki[1], ki[2]);
         if (boxi < 0) return false;
-        // the boxes the ball's leaving empties: its boxes, then each parent left with nothing
-        constexpr int CAP = 40;
-        int64_t ent[CAP], nb[CAP], nk[CAP];                // entries touched, their ball and child counts after
-        bool gone[CAP];
+        // the boxes the ball's leaving empties: its boxes, then each parent left with nothing. The entries touched and
+        // their counts after the leaving: a warp keeps them in its shared scratch (every lane the same values), a
+        // thread in its own arrays.
+        constexpr int CAP = 40, MADE = 24;
+        int64_t own_ent[CAP], own_nb[CAP], own_nk[CAP], own_made[3 * MADE];
+        uint8_t own_gone[CAP], own_lvl[MADE];
+        int64_t *ent = own_ent, *nb = own_nb, *nk = own_nk, *made_key = own_made;
+        uint8_t *gone = own_gone, *made_lvl = own_lvl;
+#ifdef __CUDA_ARCH__
+        if (lane >= 0) {                                   // (sh->key, id, out: free until GetNearbyBalls)
+            ent = sh->key;
+            nb = sh->id;
+            nk = sh->id + 64;
+            made_key = sh->key + 48;
+            gone = sh->out;
+            made_lvl = sh->out + 64;
+        }
+#endif
         int ne = 0;
         auto slot_of_entry = [&](int64_t e) -> int {
             for (int i = 0; i < ne; ++i)
@@ -1138,7 +1152,7 @@ struct World {
             ent[ne] = e;
             nb[ne] = I(s->box_balls, e);
             nk[ne] = I(s->box_kids, e);
-            gone[ne] = false;
+            gone[ne] = 0;
             return ne++;
         };
         int64_t a = 0;
@@ -1150,7 +1164,7 @@ struct World {
             if (i < 0) return false;
             --nb[i];
             while (nb[i] == 0 && nk[i] == 0 && !gone[i]) {
-                gone[i] = true;
+                gone[i] = 1;
                 ++a;
                 if (e == boxi || I(s->box_level, e) == 0) return false;   // the inflated box, or a top box, emptied
                 e = I(s->box_parent, e);
@@ -1162,45 +1176,54 @@ struct World {
         }
         auto released = [&](int64_t e) -> bool {
             for (int i = 0; i < ne; ++i)
-                if (ent[i] == e) return gone[i];
+                if (ent[i] == e) return gone[i] != 0;
             return false;
         };
         int64_t a1 = 0;
         for (int64_t e = box0; e >= 0 && released(e); e = I(s->box_parent, e)) ++a1;
-        // the boxes the inflated sides make: each side's missing chain, up to a live box or one made before
-        int64_t made_key[CAP][3];
-        int made_lvl[CAP];
-        int nm = 0;
         const int64_t g = level_grid(Li);
+        for (int side = 1; side < 8; ++side) {             // the inflated sides inside the grid
+            if (((side & 1) && !mi[0]) || ((side & 2) && !mi[1]) || ((side & 4) && !mi[2])) continue;
+            const int64_t sk[3] = {ki[0] + ((side & 1) ? mi[0] : 0), ki[1] + ((side & 2) ? mi[1] : 0),
+                                   ki[2] + ((side & 4) ? mi[2] : 0)};
+            for (int c = 0; c < 3; ++c)
+                if (sk[c] < 0 || sk[c] >= g) return false;
+        }
+        const int64_t live = one(s->box_n) - one(s->box_free_n);
+        const int64_t c0 = one(s->free_boxes);
+        // at most 56 boxes made for the sides (7 chains of 8 levels): with the kept count at least that, and room for
+        // them, every making takes one off it and every release puts one back (kept below 256): it ends as it began
+        if (c0 >= 56 && c0 + a + 56 < BOX_KEEP && B - live >= 64) return true;
+        // else the boxes the inflated sides make, counted: each side's missing chain, up to a live box or one made
+        // before
+        int nm = 0;
         int64_t b = 0;
         for (int side = 1; side < 8; ++side) {
-            const int64_t oa = (side & 1) ? mi[0] : 0, ob = (side & 2) ? mi[1] : 0, oc = (side & 4) ? mi[2] : 0;
             if (((side & 1) && !mi[0]) || ((side & 2) && !mi[1]) || ((side & 4) && !mi[2])) continue;
-            const int64_t sk[3] = {ki[0] + oa, ki[1] + ob, ki[2] + oc};
-            for (int c = 0; c < 3; ++c)
-                if (sk[c] < 0 || sk[c] >= g) return false;   // the grid's edge
+            const int64_t sk[3] = {ki[0] + ((side & 1) ? mi[0] : 0), ki[1] + ((side & 2) ? mi[1] : 0),
+                                   ki[2] + ((side & 4) ? mi[2] : 0)};
             for (int L = Li; L >= 0; --L) {
-                const int sh = 2 * (Li - L);
-                const int64_t kx = sk[0] >> sh, ky = sk[1] >> sh, kz = sk[2] >> sh;
+                const int sh2 = 2 * (Li - L);
+                const int64_t kx = sk[0] >> sh2, ky = sk[1] >> sh2, kz = sk[2] >> sh2;
                 bool have = false;
                 for (int i = 0; i < nm && !have; ++i)
-                    have = made_lvl[i] == L && made_key[i][0] == kx && made_key[i][1] == ky && made_key[i][2] == kz;
+                    have = made_lvl[i] == L && made_key[3 * i] == kx && made_key[3 * i + 1] == ky &&
+                           made_key[3 * i + 2] == kz;
                 if (!have) {
                     const int64_t e = box_find(L, kx, ky, kz);
                     have = e >= 0 && !released(e);
                 }
                 if (have) break;
-                if (nm == CAP) return false;
-                made_lvl[nm] = L;
-                made_key[nm][0] = kx;
-                made_key[nm][1] = ky;
-                made_key[nm][2] = kz;
+                if (nm == MADE) return false;
+                made_lvl[nm] = (uint8_t)L;
+                made_key[3 * nm] = kx;
+                made_key[3 * nm + 1] = ky;
+                made_key[3 * nm + 2] = kz;
                 ++nm;
                 ++b;
             }
         }
-        const int64_t live = one(s->box_n) - one(s->box_free_n);
-        int64_t c = one(s->free_boxes);
+        int64_t c = c0;
         if (B - live < b + 8 || c + a + b >= BOX_KEEP) return false;
         c += a;
         c = c > b ? c - b : 0;
