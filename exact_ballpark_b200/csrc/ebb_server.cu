@@ -43,9 +43,19 @@ struct World {
     const int64_t* ids;
 
     __device__ int64_t lookup(int64_t id) const {        // the first listed ball with this id (a pad's id is 0)
-        for (int64_t k = 0; k < s.width; ++k)
+        return lookup(id, s.width);
+    }
+    // the same over the first `span` positions, past which the world has pads alone (row -1: the same answer)
+    __device__ int64_t lookup(int64_t id, int64_t span) const {
+        for (int64_t k = 0; k < span; ++k)
             if (ids[k] == id) return rows[k];
         return -1;
+    }
+    __device__ int64_t listed_span() const {              // one past the world's last listed ball
+        int64_t span = 0;
+        for (int64_t k = 0; k < s.width; ++k)
+            if (rows[k] >= 0) span = k + 1;
+        return span;
     }
     __device__ bool any_interactive() const {
         for (int64_t k = 0; k < s.width; ++k) {
@@ -311,8 +321,9 @@ __device__ void queue(const World& x, const EbbServerQueue& q) {
         ids[k] = k < s.width ? x.ids[k] : 0;
         rows[k] = k < s.width ? x.rows[k] : -1;
     }
+    const int64_t span = s.width > IDS_IN_REGISTERS ? x.listed_span() : s.width;
     auto lookup = [&](int64_t id) -> int64_t {
-        if (s.width > IDS_IN_REGISTERS) return x.lookup(id);
+        if (s.width > IDS_IN_REGISTERS) return x.lookup(id, span);
         int64_t found = -1;
 #pragma unroll
         for (int k = IDS_IN_REGISTERS - 1; k >= 0; --k)       // the first match wins
@@ -431,7 +442,7 @@ __device__ void flags(const World& x, const EbbServerQueue& q) {
     const EbbServerState& s = x.s;
     const int64_t W = s.worlds, w = x.w, R = x.p.n, J = q.slots;
     bool bubble = false;
-    uint32_t character = 0;                               // the world's rows (by position) routed to their character
+    uint64_t character[2] = {0, 0};                       // the world's rows (by position) routed to their character
     bool uncloaks = false;
     for (int64_t j = 0; j < J; ++j) {
         const int8_t route = q.route[w * J + j];
@@ -441,15 +452,15 @@ __device__ void flags(const World& x, const EbbServerQueue& q) {
         const int64_t a = j * W + w;
         if (!q.ok[a]) continue;
         const int64_t row = q.row[a];
-        for (int64_t k = 0; k < s.width && k < 32; ++k)
-            if (x.rows[k] == row) character |= 1u << k;
+        for (int64_t k = 0; k < s.width && k < 128; ++k)
+            if (x.rows[k] == row) character[k >> 6] |= uint64_t(1) << (k & 63);
     }
     for (int64_t k = 0; k < s.width; ++k) {
         const int64_t r = x.rows[k];
         if (r < 0) continue;
         bool has = s.fresh[r] != 0;
-        if (k < 32) {
-            has = has || ((character >> k) & 1u);
+        if (k < 128) {
+            has = has || ((character[k >> 6] >> (k & 63)) & 1u);
         } else {                                          // a world wider than the mask: the slots again
             for (int64_t j = 0; j < J && !has; ++j) {
                 const int64_t a = j * W + w;
