@@ -629,6 +629,7 @@ __global__ void libm_kernel(int func, int64_t n, const double* __restrict__ x, c
         case 14: out[i] = tod(lm::acosf(tof(a))); break;
         case 15: out[i] = tod(lm::atanf(tof(a))); break;
         case 16: out[i] = tod(lm::atan2f(tof(y[i]), tof(a))); break;
+        case 17: out[i] = tod(lm::powf(tof(a), tof(y[i]))); break;
         default: out[i] = dnan(); break;
     }
 }
@@ -779,8 +780,8 @@ int ebb_flight_decay(const EbbFlightState* s, const uint8_t* mask, double neg_kd
 int ebb_libm(int func, int64_t n, const double* x, const double* y, double* out, void* stream, int block) {
     if (n <= 0) return 0;
     if (!block_ok(block, 1024) || x == nullptr || out == nullptr) return EBB_EINVAL;
-    if (!((func >= 0 && func <= 6) || (func >= 10 && func <= 16))) return EBB_EINVAL;
-    if ((func == 6 || func == 16) && y == nullptr) return EBB_EINVAL;
+    if (!((func >= 0 && func <= 6) || (func >= 10 && func <= 17))) return EBB_EINVAL;
+    if ((func == 6 || func == 16 || func == 17) && y == nullptr) return EBB_EINVAL;
     ebb::flight::libm_kernel<<<grid_of(n, block), block, 0, (cudaStream_t)stream>>>(func, n, x, y, out);
     return launched();
 }

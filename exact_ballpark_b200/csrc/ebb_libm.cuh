@@ -35,6 +35,8 @@ __device__ const uint64_t d_exp2f_tab[] = FL_EXP2F_TAB_INIT;
 __device__ const double d_logf_tab[] = FL_LOGF_TAB_INIT;
 __device__ const uint32_t d_inv_pio4[] = FL_INV_PIO4_INIT;
 __device__ const double d_pow_tab[] = FL_POW_TAB_INIT;
+__device__ const double d_powf_invc[] = FL_POWF_INVC_INIT;
+__device__ const double d_powf_logc[] = FL_POWF_LOGC_INIT;
 #endif
 static const double h_sincostab[] = DL_SINCOSTAB_INIT;
 static const double h_br_toverp[] = DL_BR_TOVERP_INIT;
@@ -44,6 +46,8 @@ static const uint64_t h_exp2f_tab[] = FL_EXP2F_TAB_INIT;
 static const double h_logf_tab[] = FL_LOGF_TAB_INIT;
 static const uint32_t h_inv_pio4[] = FL_INV_PIO4_INIT;
 static const double h_pow_tab[] = FL_POW_TAB_INIT;
+static const double h_powf_invc[] = FL_POWF_INVC_INIT;
+static const double h_powf_logc[] = FL_POWF_LOGC_INIT;
 
 #ifdef __CUDA_ARCH__
 #define EBB_TAB(name, i) (__ldg(&d_##name[(i)]))
@@ -789,6 +793,99 @@ EBB_HDNI double pow(double x, double y) {
     const double elo = dfma(y, lo, dfma(y, hi, dneg(ehi)));
     return pow_exp_inline(ehi, elo, negative);
 }
+
+// ---- powf: glibc 2.34's e_powf.c (ARM's optimized-routines), as the aarch64 build computes it ----
+// x = 2^k z with z within a 16th of an octave of a table point c: log2 x (times 32) is k + log2 c plus a quintic in
+// r = z/c - 1, all in double; y log2 x then goes through exp2's 32-entry table and a cubic, rounded to float once.
+// Six multiply-adds are fused in the logarithm and three in the exponential, the ones the aarch64 build fuses.
+
+// log2(x) x 32 for the bits ix of a positive normal (or normalised) x
+EBB_HD double powf_log2(uint32_t ix) {
+    const uint32_t tmp = ix - 0x3f330000u;                           // ix - OFF: z in [OFF, 2 OFF)
+    const int i = (int)((tmp >> 19) & 15u);
+    const uint32_t top = tmp & 0xff800000u;
+    const uint32_t iz = ix - top;
+    const int32_t k = (int32_t)top >> 18;                             // the exponent, times 32
+    const double a[5] = FL_POWF_A_INIT;
+    const double invc = EBB_TAB(powf_invc, i), logc = EBB_TAB(powf_logc, i);
+    const double z = tod(ffrom(iz));
+    const double r = dfma(invc, z, -1.0);
+    const double y0 = dadd((double)k, logc);
+    const double p = dfma(r, a[2], a[3]);
+    double q = dfma(r, a[4], y0);
+    const double r2 = dmul(r, r);
+    const double yy = dfma(r, a[0], a[1]);
+    const double r4 = dmul(r2, r2);
+    q = dfma(r2, p, q);
+    return dfma(yy, r4, q);
+}
+// 2^(xd / 32) rounded to float, negative when sign_bias says so (expf's table and cubic)
+EBB_HD float powf_exp2(double xd, uint64_t sign_bias) {
+    const double cc[3] = FL_EXPF_C_INIT;
+    const double kd = frinta(xd);
+    const uint64_t ki = (uint64_t)(int64_t)kd;
+    const double r = dsub(xd, kd);
+    double y = dfma(r, cc[2], 1.0);
+    const double zc = dfma(r, cc[0], cc[1]);
+    const double r2 = dmul(r, r);
+    const uint64_t t = EBB_TAB(exp2f_tab, ki & 31) + ((ki + sign_bias) << 47);
+    y = dfma(zc, r2, y);
+    return tof(dmul(y, dfrom(t)));
+}
+// 1 for an odd integer y, 2 for an even one, 0 for none (its bits iy)
+EBB_HD int powf_checkint(uint32_t iy) {
+    const int e = (int)((iy >> 23) & 0xff);
+    if (e < 0x7f) return 0;
+    if (e > 0x7f + 23) return 2;
+    const uint32_t bit = 1u << (0x7f + 23 - e);
+    if (iy & (bit - 1)) return 0;
+    return (iy & bit) ? 1 : 2;
+}
+EBB_HD bool powf_signaling(uint32_t u) { return ((u ^ 0x00400000u) & 0x7fffffffu) > 0x7fc00000u; }
+// __math_oflowf, __math_uflowf, __math_may_uflowf: (sign ? -t : t) t in float
+EBB_HD float powf_xflow(uint64_t sign_bias, uint32_t tbits) {
+    const float t = ffrom(tbits);
+    return fmul(sign_bias ? fneg(t) : t, t);
+}
+EBB_HD float powf(float x, float y) {
+    uint32_t ix = fbits(x);
+    const uint32_t iy = fbits(y);
+    const bool zinf_y = 2u * iy - 1u >= 2u * 0x7f800000u - 1u;       // y zero, infinite or NaN
+    uint64_t sign_bias = 0;
+    if (ix - 0x00800000u >= 0x7f800000u - 0x00800000u || zinf_y) {
+        if (zinf_y) {
+            if (2u * iy == 0) return powf_signaling(ix) ? fadd(x, y) : 1.0f;
+            if (ix == 0x3f800000u) return powf_signaling(iy) ? fadd(x, y) : 1.0f;
+            if (2u * ix > 2u * 0x7f800000u || 2u * iy > 2u * 0x7f800000u) return fadd(x, y);
+            if (2u * ix == 2u * 0x3f800000u) return 1.0f;
+            if ((2u * ix < 2u * 0x3f800000u) == !(iy & 0x80000000u)) return 0.0f;   // |x|<1 to +inf, |x|>1 to -inf
+            return fmul(y, y);
+        }
+        if (2u * ix - 1u >= 2u * 0x7f800000u - 1u) {                 // x zero, infinite or NaN
+            float x2 = fmul(x, x);
+            if ((ix & 0x80000000u) && powf_checkint(iy) == 1) x2 = fneg(x2);
+            return (iy & 0x80000000u) ? fdiv(1.0f, x2) : x2;
+        }
+        if (ix & 0x80000000u) {                                      // a finite x < 0
+            const int yint = powf_checkint(iy);
+            if (yint == 0) return fnan();                            // __math_invalidf
+            if (yint == 1) sign_bias = 0x10000u;
+            ix &= 0x7fffffffu;
+        }
+        if (ix < 0x00800000u) {                                      // a subnormal x normalised by 2^23
+            ix = fbits(fmul(x, 8388608.0f)) & 0x7fffffffu;
+            ix -= 23u << 23;
+        }
+    }
+    const double ylogx = dmul(tod(y), powf_log2(ix));
+    if (((dbits(ylogx) >> 47) & 0xffff) >= (dbits(126.0 * 32.0) >> 47)) {   // |y log2 x| >= 126: over or under
+        if (ylogx > FL_POWF_OFLOW) return powf_xflow(sign_bias, FL_POWF_OFLOWF_X);
+        if (ylogx <= dfrom(FL_POWF_UFLOW_BITS)) return powf_xflow(sign_bias, FL_POWF_UFLOWF_X);
+        if (ylogx < dfrom(FL_POWF_MAY_UFLOW_BITS)) return powf_xflow(sign_bias, FL_POWF_MAY_UFLOWF_X);
+    }
+    return powf_exp2(ylogx, sign_bias);
+}
+
 
 }  // namespace lm
 }  // namespace ebb

@@ -147,6 +147,19 @@ def main() -> None:
     lines.append(f"#define FL_SIGN_BIAS {u64(L.SIGN_BIAS)}")
     table_d("FL_POW_A", L.POW_A)
     table_d("FL_POW_TAB", [v for row in L.POW_TAB for v in row], per=3)
+    # ---- powf (dlibm_powf.py; __powf_log2_data, and __exp2f_data as expf's) ----
+    lines.append("// ---- powf (dlibm_powf.py; __powf_log2_data; its exp2 table and cubic are expf's) ----")
+    P = dlibm_powf
+    if list(P.POWF_EXP2_TAB) != list(L.EXP2F_TAB) or list(P.POWF_EXP2_C) != list(L.EXPF_C):
+        raise SystemExit("powf's exp2 table or cubic differs from expf's")
+    table_d("FL_POWF_INVC", P.POWF_LOG2_INVC)
+    table_d("FL_POWF_LOGC", P.POWF_LOG2_LOGC)
+    table_d("FL_POWF_A", P.POWF_A)
+    scalar_d("FL", P, ["POWF_OFLOW", "POWF_RND"])
+    for n in ("POWF_UFLOW", "POWF_MAY_UFLOW"):
+        lines.append(f"#define FL_{n}_BITS {u64(getattr(P, n))}")
+    for n in ("POWF_TINY_F", "POWF_OFLOWF_X", "POWF_UFLOWF_X", "POWF_MAY_UFLOWF_X"):
+        lines.append(f"#define FL_{n} {u32(getattr(P, n))}")
     OUT.write_text("\n".join(lines) + "\n")
     print(f"wrote {OUT} ({len(lines)} lines)")
 

@@ -652,7 +652,7 @@ def kernel_info(device=None) -> dict:
 
 
 LIBM_FUNCS = {"sin": 0, "cos": 1, "log": 2, "exp": 3, "sincos_sin": 4, "sincos_cos": 5, "pow": 6, "expf": 10,
-              "logf": 11, "sinf": 12, "cosf": 13, "acosf": 14, "atanf": 15, "atan2f": 16}
+              "logf": 11, "sinf": 12, "cosf": 13, "acosf": 14, "atanf": 15, "atan2f": 16, "powf": 17}
 
 
 def libm(name: str, x: torch.Tensor, y: torch.Tensor | None = None, block: int = 128) -> torch.Tensor:

@@ -413,8 +413,8 @@ int ebb_flight_decay(const EbbFlightState* s, const uint8_t* mask, double neg_kd
 
 /* glibc 2.34 aarch64's function `func` elementwise on the device, for the tests: 0 sin, 1 cos, 2 log, 3 exp,
  * 4 sincos's sine, 5 sincos's cosine, 6 pow(x, y); 10 expf, 11 logf, 12 sinf, 13 cosf, 14 acosf, 15 atanf,
- * 16 atan2f(y, x) (floats held in doubles). Replaces xbpm_dlibm and xbpo_libm (vec_modes_cuda.cu:779,
- * vec_orient_cuda.cu:520). */
+ * 16 atan2f(y, x), 17 powf(x, y) (floats held in doubles; powf is glibc_powf.cuh:65's g_powf, the combat
+ * kernel's mushroom growth). Replaces xbpm_dlibm and xbpo_libm (vec_modes_cuda.cu:779, vec_orient_cuda.cu:520). */
 int ebb_libm(int func, int64_t n, const double* x, const double* y, double* out, void* stream, int block);
 
 /* The tape's operations on every world, one thread a world, on `stream` (the park's rows are read and written: the

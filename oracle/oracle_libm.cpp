@@ -8,7 +8,8 @@
 extern "C" {
 
 // func: 0 sin, 1 cos, 2 log, 3 exp, 4 sincos's sine, 5 sincos's cosine, 6 pow(x, y); 10 expf, 11 logf, 12 sinf,
-// 13 cosf, 14 acosf, 15 atanf, 16 atan2f(y, x) (floats held in doubles). Returns -1 for an unknown func.
+// 13 cosf, 14 acosf, 15 atanf, 16 atan2f(y, x), 17 powf(x, y) (floats held in doubles). Returns -1 for an unknown
+// func.
 int oracle_libm(int func, int64_t n, const double* x, const double* y, double* out) {
     using namespace ebb;
     for (int64_t i = 0; i < n; ++i) {
@@ -29,6 +30,7 @@ int oracle_libm(int func, int64_t n, const double* x, const double* y, double* o
             case 14: out[i] = tod(lm::acosf(tof(a))); break;
             case 15: out[i] = tod(lm::atanf(tof(a))); break;
             case 16: out[i] = tod(lm::atan2f(tof(y[i]), tof(a))); break;
+            case 17: out[i] = tod(lm::powf(tof(a), tof(y[i]))); break;
             default: return -1;
         }
     }

@@ -46,7 +46,7 @@ def lib():
 
 
 LIBM_FUNCS = {"sin": 0, "cos": 1, "log": 2, "exp": 3, "sincos_sin": 4, "sincos_cos": 5, "pow": 6, "expf": 10,
-              "logf": 11, "sinf": 12, "cosf": 13, "acosf": 14, "atanf": 15, "atan2f": 16}
+              "logf": 11, "sinf": 12, "cosf": 13, "acosf": 14, "atanf": 15, "atan2f": 16, "powf": 17}
 
 
 def libm(name: str, x, y=None) -> np.ndarray:

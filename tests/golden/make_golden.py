@@ -175,6 +175,31 @@ def _save_parks(prefix: str, parks: list) -> None:
           f"{sum(len(p.trace['digests']) for p in parks)} ticks")
 
 
+def make_powf(rng: np.random.Generator, n: int = 4000) -> None:
+    """powf's vectors (dlibm_powf.powf, glibc 2.34 aarch64's powf as the reference transcribes it), added to libm.npz
+    beside the others (their arrays kept as they are): floats from every range the function branches on (near 1, small,
+    subnormal, large, negative with integer and non-integer exponents, the over- and underflow thresholds, mushroom
+    growth's range ** 0.25) and every pair of special values."""
+    from exact_ballpark import dlibm_powf
+    f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)   # noqa: E731
+    xs = [rng.uniform(0, 2, n), rng.uniform(0.99, 1.01, n), 10.0 ** rng.uniform(-30, 30, n),
+          10.0 ** rng.uniform(-45, -38, 400), -rng.uniform(0, 20, n), rng.uniform(0, 1, n)]
+    ys = [rng.uniform(-10, 10, n), rng.uniform(-3e3, 3e3, n), rng.uniform(-4, 4, n),
+          rng.uniform(-2, 2, 400), rng.integers(-12, 12, n).astype(float) + (rng.random(n) < 0.2) * 0.5,
+          np.full(n, 0.25)]
+    special = np.array([0.0, -0.0, 1.0, -1.0, 2.0, -2.0, 0.5, -0.5, 3.0, -3.0, np.inf, -np.inf, np.nan, 1e-45, -1e-45,
+                        1.17549435e-38, 3.4028235e38, -3.4028235e38, 1.0000001, 0.99999994, 16777216.0, 16777217.0,
+                        -16777216.0, 149.0, -150.0, 128.0, -126.0, 0.25])
+    sx, sy = np.meshgrid(special, special)
+    px = f32(np.concatenate(xs + [sx.ravel()]))
+    py = f32(np.concatenate(ys + [sy.ravel()]))
+    out = np.array([dlibm_powf.powf(float(a), float(b)) for a, b in zip(px, py)])
+    have = dict(np.load(HERE / "libm.npz"))
+    have.update(powf_x=px, powf_y=py, powf_out=out)
+    np.savez_compressed(HERE / "libm.npz", **have)
+    print("libm.npz powf", px.shape)
+
+
 def make_traces(sample: int) -> None:
     import flight_cases as flc
     import mode_cases as mc
@@ -653,13 +678,15 @@ def make_space_crowd() -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=("libm", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending", "server_ontick",
+    ap.add_argument("--only", choices=("libm", "powf", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending", "server_ontick",
                                        "server_collide", "server_collide_more", "space_bubbles", "space_crowd"),
                     default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
     a = ap.parse_args()
     if a.only in (None, "libm"):
         make_libm(np.random.default_rng(20261203))
+    if a.only in (None, "powf"):
+        make_powf(np.random.default_rng(20261204))
     if a.only in (None, "workload"):
         make_workload_traces()
     if a.only in (None, "traces"):

@@ -14,7 +14,8 @@ LIBM_CASES = (  # (function, input key, second input key or None, output key)
     ("sincos_cos", "sin_x", None, "sincos_c"), ("log", "log_x", None, "log_y"), ("exp", "exp_x", None, "exp_y"),
     ("expf", "f_x", None, "expf_y"), ("sinf", "f_x", None, "sinf_y"), ("cosf", "f_x", None, "cosf_y"),
     ("atanf", "f_x", None, "atanf_y"), ("logf", "logf_x", None, "logf_y"), ("acosf", "acosf_x", None, "acosf_y"),
-    ("atan2f", "f_x", "atan2f_y", "atan2f_out"), ("pow", "pow_x", "pow_y", "pow_out"))
+    ("atan2f", "f_x", "atan2f_y", "atan2f_out"), ("pow", "pow_x", "pow_y", "pow_out"),
+    ("powf", "powf_x", "powf_y", "powf_out"))
 
 
 def available_traces() -> list:
