@@ -968,7 +968,7 @@ def partition_headline(args, dev, dist, rank: int, world_size: int, barrier, max
     count and every row's two send flags copied back, double-buffered over a copy stream."""
     import torch
 
-    from exact_ballpark_b200.partition import partition_setup
+    from exact_ballpark_b200.partition import partition_setup, tune_partition
     from exact_ballpark_b200.workloads import partition_worlds
     W, K = args.partition_worlds, args.steps
     pw = partition_worlds(11 + rank, W)
@@ -999,7 +999,10 @@ def partition_headline(args, dev, dist, rank: int, world_size: int, barrier, max
     plain_layout = [[layer.N, layer.W, layer.lanes] for layer, _ in plain["part"].layers]
     del plain, plain_park
     torch.cuda.empty_cache()
-    r = partition_setup(pw, dev, ragged=True, warp_class=args.partition_warp_class)
+    plan, tuning = None, None
+    if not args.no_partition_autotune:                     # each size class's arrangement, measured (untimed)
+        plan, tuning = tune_partition(pw, dev)
+    r = partition_setup(pw, dev, ragged=True, warp_class=args.partition_warp_class, plan=plan)
     g, part, park = r["graph"], r["part"], r["park"]
     for _ in range(args.warmup):
         g.tick()
@@ -1064,7 +1067,13 @@ def partition_headline(args, dev, dist, rank: int, world_size: int, barrier, max
                   "schedule": "the plain per-configuration layout: one 128-slot layer, worlds in their order, a "
                               "thread a world; the park's plain schedule; the same server layer; one CUDA graph"},
         "speedup_ragged_vs_plain": ms_plain / ms_ragged, "bit_identical_ragged_vs_plain": bool(same),
-        "ragged_layout": [[layer.N, layer.W, layer.lanes] for layer, _ in part.layers],
+        "ragged_layout": [[layer.N, layer.W, layer.lanes, layer.block] for layer, _ in part.layers],
+        "autotune": None if tuning is None else {
+            "plan": {str(c): {"lanes": l, "block": b} for c, (l, b) in plan.items()},
+            "ms_a_class_a_tick": {f"lanes{l}_block{b}": {str(c): round(v, 3) for c, v in t.items()}
+                                  for (l, b), t in tuning.items()},
+            "note": "each size class's arrangement (a thread a world in 64- or 128-thread blocks, or a warp a world) "
+                    "timed on the workload itself, eager, untimed in the headline; each class takes its fastest"},
         "layer_launch_ms": launch_ms, "layer_share": layer_ms / (ms_ragged / K),
         "roofline": {"bound": "hbm", "kernel": "the space layer's re-filings and HandleProximities (tape kernels, "
                                                 "a launch a size class)",
@@ -1270,6 +1279,8 @@ def main() -> None:
     ap.add_argument("--space-steps", type=int, default=5)
     ap.add_argument("--partition-worlds", type=int, default=100000)
     ap.add_argument("--partition-steps", type=int, default=10)
+    ap.add_argument("--no-partition-autotune", action="store_true",
+                    help="the ragged batch's arrangement from --partition-warp-class instead of measured per class")
     ap.add_argument("--partition-warp-class", type=int, default=32,
                     help="the ragged batch's size classes from this size up run a warp a world (129: none)")
     ap.add_argument("--serve-rate", type=float, default=2000.0)

@@ -120,6 +120,7 @@ def lib() -> ctypes.CDLL:
     if LIB_PATH.name == "libebb_count.so":
         for unit in ("flight", "space", "collide", "combat", "server"):
             getattr(L, "ebb_count_ops_" + unit).argtypes = [p, i32]
+        L.ebb_count_sensor_paths.argtypes = [p, i32]
     L.ebb_error_string.restype = ctypes.c_char_p
     L.ebb_error_string.argtypes = [i32]
     L.ebb_flight_scratch_bytes.restype = i64

@@ -133,3 +133,15 @@ int ebb_space_query(const EbbFlightState* park, const EbbSpaceState* s, const Eb
 }  // extern "C"
 
 EBB_OP_COUNTER(ebb_count_ops_space)
+
+#ifdef EBB_COUNT_OPS
+// the counting build's tally of CheckSensor's paths: checks, re-filings skipped, filings unchanged
+extern "C" int ebb_count_sensor_paths(unsigned long long* out, int reset) {
+    cudaError_t e = cudaMemcpyFromSymbol(out, ebb::space::sensor_paths, sizeof(unsigned long long) * 3);
+    if (e == cudaSuccess && reset) {
+        const unsigned long long zero[3] = {};
+        e = cudaMemcpyToSymbol(ebb::space::sensor_paths, zero, sizeof(zero));
+    }
+    return e == cudaSuccess ? 0 : (int)e;
+}
+#endif

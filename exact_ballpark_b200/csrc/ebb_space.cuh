@@ -28,6 +28,24 @@
 namespace ebb {
 namespace space {
 
+// The counting build's tally of CheckSensor's paths (EBB_COUNT_OPS, a measurement of the algorithm as it runs): the
+// checks, those whose two re-filings were skipped (sensor_fast), and of those the ones whose filing did not change
+#ifdef EBB_COUNT_OPS
+#ifdef __CUDACC__
+static __device__ unsigned long long sensor_paths[3];
+#endif
+#ifdef __CUDA_ARCH__
+#define EBB_SENSOR_PATH(k)                                        \
+    do {                                                          \
+        if (lane <= 0) atomicAdd(&::ebb::space::sensor_paths[k], 1ull); \
+    } while (0)
+#else
+#define EBB_SENSOR_PATH(k) ((void)0)
+#endif
+#else
+#define EBB_SENSOR_PATH(k) ((void)0)
+#endif
+
 constexpr int NUM_LEVELS = 8;
 constexpr int64_t BOX_KEEP = 256;                          // BoxAllocator's kept boxes
 constexpr int64_t F_EDGE = EBB_SPACE_FLAG_EDGE, F_BOXES = EBB_SPACE_FLAG_BOXES, F_DICTS = EBB_SPACE_FLAG_DICTS,
@@ -97,6 +115,16 @@ struct World {
     int lane = -1;
     Coop* sh = nullptr;
     static constexpr bool world_major = WM;
+    // the slots whose filing this operation made from their current position, velocity and radius (the tick's
+    // re-filings and a sensor's re-filing back): CheckSensor's fast path then knows the ball comes back to it
+    uint64_t fresh[2] = {0, 0};
+    EBB_HD bool is_fresh(int64_t j) const { return (fresh[j >> 6] >> (j & 63)) & 1; }
+    EBB_HD void set_fresh(int64_t j, bool on) {
+        if (on)
+            fresh[j >> 6] |= uint64_t(1) << (j & 63);
+        else
+            fresh[j >> 6] &= ~(uint64_t(1) << (j & 63));
+    }
 
     // ---- accessors: entry e of a per-world array ([cap][W], or world w's run of cap entries), component c of a
     // [3][cap] one ----
@@ -1099,15 +1127,23 @@ struct World {
         if (box0 < 0 || top < 0) return false;
         const int64_t bub = I(s->box_bubble, top);
         if (bub == -1 || bub != I(s->bubble, j)) return false;
-        // the filing it comes back to: its own
-        const double infl1 = inflated_radius(j, v);
-        const int L1 = level_for(infl1);
-        if (L1 != lvl(j) || (L1 == 0 && (double)fmul(p->radius[r], 2.0f) > level_width(0))) return false;
+        // the filing it comes back to: its own (known for a fresh one, else made again and compared)
+        const int L1 = (int)lvl(j);
         int64_t k1[3], m1[3];
-        key_for(L1, x, k1);
-        side_mods(L1, k1, infl1, x, m1);
-        for (int c = 0; c < 3; ++c)
-            if (k1[c] != key(j, c) || m1[c] != mod(j, c)) return false;
+        for (int c = 0; c < 3; ++c) {
+            k1[c] = key(j, c);
+            m1[c] = mod(j, c);
+        }
+        if (!is_fresh(j)) {
+            const double infl1 = inflated_radius(j, v);
+            if (level_for(infl1) != L1 || (L1 == 0 && (double)fmul(p->radius[r], 2.0f) > level_width(0)))
+                return false;
+            int64_t kk[3], mm[3];
+            key_for(L1, x, kk);
+            side_mods(L1, kk, infl1, x, mm);
+            for (int c = 0; c < 3; ++c)
+                if (kk[c] != k1[c] || mm[c] != m1[c]) return false;
+        }
         // the inflated filing
         const double rest[3] = {0.0, 0.0, 0.0};
         const double infl = inflated_radius_of(j, inflated, rest);
@@ -1122,8 +1158,10 @@ struct World {
             fi->hi[c] = ki[c] + (mi[c] > 0 ? mi[c] : 0);
         }
         if (Li == L1 && ki[0] == k1[0] && ki[1] == k1[1] && ki[2] == k1[2] && mi[0] == m1[0] && mi[1] == m1[1] &&
-            mi[2] == m1[2])
+            mi[2] == m1[2]) {
+            EBB_SENSOR_PATH(2);
             return true;                                   // both re-filings return at once
+        }
         const int64_t boxi = box_find(Li, ki[0], ki[1], ki[2]);
         if (boxi < 0) return false;
         // the boxes the ball's leaving empties: its boxes, then each parent left with nothing. The entries touched and
@@ -1246,7 +1284,9 @@ struct World {
         uint8_t cand[EBB_SPACE_MAX_SLOTS];
         int nc;
         Filing fi;
+        EBB_SENSOR_PATH(0);
         if (!(inflated < 0.0f) && !(radius < 0.0f) && sensor_fast(j, x, v, inflated, &fi)) {
+            EBB_SENSOR_PATH(1);
             nc = nearby(j, at(s->cloaked, j) == 0, at(s->sonly, j) != 0, false, cand, &fi);
         } else {
             if (!(inflated < 0.0f)) {
@@ -1254,9 +1294,11 @@ struct World {
                 insert_in_boxes(j, x, rest);
             }
             nc = nearby(j, at(s->cloaked, j) == 0, at(s->sonly, j) != 0, false, cand);
+            set_fresh(j, false);
             if (!(radius < 0.0f)) {
                 p->radius[r] = radius;
                 insert_in_boxes(j, x, v);
+                set_fresh(j, true);
             }
         }
 #ifdef __CUDA_ARCH__
@@ -1646,11 +1688,15 @@ struct World {
             if (U(s->dead, j) || !p->free_[r]) continue;
             double d[3];
             for (int c = 0; c < 3; ++c) d[c] = dsub(p->pos[c * p->n + r], p->old_pos[c * p->n + r]);
-            if (!(dadd(dadd(dmul(d[0], d[0]), dmul(d[1], d[1])), dmul(d[2], d[2])) < 0.1)) insert_in_boxes(j);
+            if (!(dadd(dadd(dmul(d[0], d[0]), dmul(d[1], d[1])), dmul(d[2], d[2])) < 0.1)) {
+                insert_in_boxes(j);
+                set_fresh(j, true);
+            }
         }
         handle_proximities();
     }
     EBB_HD void apply(int64_t code, int64_t j, int64_t b, const double* f) {
+        fresh[0] = fresh[1] = 0;                           // (an operation's own: AFTER_EVOLVE's re-filings)
         const bool has_slot = slot_ok(j);
         const bool live = has_slot && U(s->in_park, j);
         switch (code) {

@@ -65,6 +65,13 @@ def count_flight(worlds: int, ticks: int) -> dict:
     return per_ship_tick(_counts(), p.n * ticks)
 
 
+def _sensor_paths(reset: bool = True) -> list:
+    from . import _native
+    buf = (ctypes.c_ulonglong * 3)()
+    _native.check(_native.lib().ebb_count_sensor_paths(buf, int(reset)), "ebb_count_sensor_paths")
+    return [int(v) for v in buf]
+
+
 def count_partition(worlds: int, ticks: int) -> dict:
     """The partition worlds (ragged 1-128 ships, sensors on every ship) with the space layer and the server on top,
     as the benchmark ticks them (the ragged arrangement), `ticks` ticks after the set-up and one uncounted tick."""
@@ -77,10 +84,16 @@ def count_partition(worlds: int, ticks: int) -> dict:
     r["graph"].tick()
     torch.cuda.synchronize()
     _counts()
+    _sensor_paths()
     for _ in range(ticks):
         r["graph"].tick()
     torch.cuda.synchronize()
-    return per_ship_tick(_counts(), pw.n * ticks)
+    out = per_ship_tick(_counts(), pw.n * ticks)
+    checks, skipped, same = _sensor_paths()
+    out["sensor_checks"] = checks
+    out["sensor_refilings_skipped"] = skipped / max(checks, 1)    # CheckSensor's two re-filings skipped (no trace)
+    out["sensor_filing_unchanged"] = same / max(checks, 1)        # of them: the inflated filing the ball's own
+    return out
 
 
 def main() -> None:

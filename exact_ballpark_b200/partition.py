@@ -36,10 +36,12 @@ class PartitionLayer:
     """The space layer over a flight park of ragged worlds whose rows are contiguous a world (`sizes` [W], world w's
     rows from sum(sizes[:w])). `events`: each world's event capacity a tick, by default N (N + 2) for a class of N
     slots (every pair entering and each ball's range and tracking events); `boxes`: box-table entries a world as a
-    multiple of the class's slots (plus 64)."""
+    multiple of the class's slots (plus 64). `plan` {class: (lanes, block)}: how each size class runs (1 a thread a
+    world, 32 a warp a world; threads a block), by default a warp a world from `warp_class` slots up, 128-thread
+    blocks (`tune_partition` measures the best)."""
 
     def __init__(self, park: VecModesPark, sizes, ragged: bool = True, events: int | None = None,
-                 boxes_per_slot: int = 16, seed: int = 1, warp_class: int = WARP_CLASS):
+                 boxes_per_slot: int = 16, seed: int = 1, warp_class: int = WARP_CLASS, plan: dict | None = None):
         self.park = park
         sizes = np.asarray(sizes, dtype=np.int64)
         if sizes.ndim != 1 or (sizes < 1).any() or sizes.max(initial=0) > CLASSES[-1]:
@@ -64,9 +66,12 @@ class PartitionLayer:
             k = sizes[idx]
             col = np.arange(cap)[None, :]
             slots[:] = np.where(col < k[:, None], starts[idx][:, None] + col, -1)
+            lanes, block = (32 if ragged and cap >= warp_class else 1), 128
+            if ragged and plan is not None and cap in plan:
+                lanes, block = plan[cap]
             layer = VecSpace(park, slots, boxes=boxes_per_slot * cap + 64,
                              events=cap * (cap + 2) if events is None else int(events), umap_cap=cap,
-                             seed=(idx + seed).tolist(), lanes=32 if ragged and cap >= warp_class else 1)
+                             seed=(idx + seed).tolist(), lanes=lanes, block=block)
             self.layers.append((layer, idx))
         self.last_dead = None
 
@@ -190,7 +195,8 @@ class PartitionGraph:
         self.part.park.current_time += 1
 
 
-def partition_setup(pw, dev, ragged: bool, server_on: bool = True, warp_class: int = WARP_CLASS) -> dict:
+def partition_setup(pw, dev, ragged: bool, server_on: bool = True, warp_class: int = WARP_CLASS,
+                    plan: dict | None = None) -> dict:
     """A flight park of the partition worlds with the partition layer (ragged size classes, or the plain 128-slot
     layout), every ship's sensor added, and the server layer on top (a pilot a ship, GotoDirection and
     SetSpeedFraction queued for every ship every tick: a fixed schedule of 2 x 128 pushes, a world's pushes masked to
@@ -199,7 +205,7 @@ def partition_setup(pw, dev, ragged: bool, server_on: bool = True, warp_class: i
     from .modes import tick_plain, tick_tiled
     park = VecModesPark(pw.n, device=dev)
     park.load_columns(pw.cols)
-    part = PartitionLayer(park, pw.sizes, ragged=ragged, warp_class=warp_class)
+    part = PartitionLayer(park, pw.sizes, ragged=ragged, warp_class=warp_class, plan=plan)
     part.load()
     part.add_sensors(pw.sensor_range, 1.0)
     park_tick = (lambda: tick_tiled(park)) if ragged else (lambda: tick_plain(park, park.block))
@@ -231,3 +237,48 @@ def partition_setup(pw, dev, ragged: bool, server_on: bool = True, warp_class: i
         park.current_time += 1
     g = PartitionGraph(part, park_tick, srv, q)
     return {"park": park, "part": part, "server": srv, "q": q, "graph": g, "park_tick": park_tick}
+
+
+ARRANGEMENTS = ((1, 64), (1, 128), (32, 128))      # (lanes, block): a thread a world in 64- or 128-thread blocks; a warp
+
+
+def tune_partition(pw, dev, warm: int = 1, ticks: int = 2, arrangements=ARRANGEMENTS) -> tuple:
+    """The ragged batch's autotuner: each size class's arrangement (a thread a world, 2 or 4 warps of worlds a
+    block; or a warp a world, 4 worlds a block), measured on the workload itself. For each arrangement every class
+    runs it: the worlds are loaded, their sensors added, `warm` ticks run, then `ticks` ticks each with every class's
+    re-filings and HandleProximities timed alone (CUDA events); every arrangement starts from the same state and does
+    the same work (its results are bit-identical). The classes run one after another in a tick, so each takes its
+    fastest arrangement. Returns (plan {class: (lanes, block)}, {arrangement: {class: ms a tick}})."""
+    times = {}
+    for lanes, block in arrangements:
+        plan = {cap: (lanes, block) for cap in CLASSES}
+        r = partition_setup(pw, dev, ragged=True, server_on=False, plan=plan)
+        part, park_tick = r["part"], r["park_tick"]
+        for _ in range(warm):
+            part.tick(park_tick)
+        stream = torch.cuda.current_stream(dev)
+        ms = {layer.N: 0.0 for layer, _ in part.layers}
+        park = part.park
+        for _ in range(ticks):
+            dead = part.dead_rows()
+            saved = park._moribund.clone()
+            park._moribund.logical_or_(dead)
+            park_tick()
+            park._moribund.copy_(saved)
+            for layer, _ in part.layers:
+                layer.clear_events()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                layer.after_evolve(None)
+                b.record(stream)
+                b.synchronize()
+                ms[layer.N] += a.elapsed_time(b) / ticks
+        times[(lanes, block)] = ms
+        del r, part
+        torch.cuda.empty_cache()
+    best = {}
+    for cap in CLASSES:
+        have = [(t[cap], arr) for arr, t in times.items() if cap in t]
+        if have:
+            best[cap] = min(have)[1]
+    return best, times

@@ -50,7 +50,7 @@ def _world_text(part, park, pw, w: int, events: bool) -> str:
     return t + (sl.events_text(st, ids, 0, N) if events else "")
 
 
-def _run(pw, ragged: bool, goto, ticks: int, dev):
+def _run(pw, ragged: bool, goto, ticks: int, dev, plan=None):
     import torch
 
     from exact_ballpark_b200 import VecModesPark
@@ -58,7 +58,7 @@ def _run(pw, ragged: bool, goto, ticks: int, dev):
     from exact_ballpark_b200.partition import PartitionLayer
     park = VecModesPark(pw.n, device=dev)
     park.load_columns(pw.cols)
-    part = PartitionLayer(park, pw.sizes, ragged=ragged)
+    part = PartitionLayer(park, pw.sizes, ragged=ragged, plan=plan)
     part.load()
     part.add_sensors(pw.sensor_range, 1.0)
     park.goto_point(torch.ones(pw.n, dtype=torch.bool, device=dev), torch.as_tensor(goto, device=dev))
@@ -94,3 +94,28 @@ def test_the_ragged_batch_matches_the_plain_layout_and_the_oracle():
     for w in sample:
         want = space_world.run(_world_ops(pw, w, goto, ticks), seed=w + 1)[-1]
         assert _world_text(ragged, pr, pw, w, True) == sl.oracle_lines(want, sp.TICK), (w, int(pw.sizes[w]))
+
+
+def test_every_arrangement_of_the_classes_gives_the_same_worlds():
+    """The autotuner's choices change no result: the classes crossed (the small ones a warp a world, the large ones a
+    thread a world in 64-thread blocks) against the default, and the tuner's own plan, every world bit for bit."""
+    import torch
+    from exact_ballpark_b200.partition import CLASSES, tune_partition
+    from exact_ballpark_b200.workloads import partition_worlds
+    dev = torch.device("cuda")
+    pw = partition_worlds(7, 200)
+    goto = pw.cols["pos"] + np.random.default_rng(4).normal(0.0, 3e4, (pw.n, 3))
+    ticks = 4
+    base_park, base = _run(pw, True, goto, ticks, dev)
+    crossed = {c: ((32, 128) if c <= 16 else (1, 64)) for c in CLASSES}
+    plan, times = tune_partition(pw, dev, warm=1, ticks=1)
+    assert set(plan) == {layer.N for layer, _ in base.layers}
+    assert all(set(t) == set(plan) for t in times.values())
+    for p in (crossed, plan):
+        park, part = _run(pw, True, goto, ticks, dev, plan=p)
+        assert [(layer.lanes, layer.block) for layer, _ in part.layers] == [p[layer.N] for layer, _ in part.layers]
+        for k in ("pos", "vel", "mode", "clock"):
+            assert torch.equal(getattr(park, "_" + k), getattr(base_park, "_" + k)), k
+        assert torch.equal(part.event_counts(), base.event_counts())
+        for w in range(len(pw.sizes)):
+            assert _world_text(part, park, pw, w, True) == _world_text(base, base_park, pw, w, True), w
