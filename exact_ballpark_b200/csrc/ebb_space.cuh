@@ -118,6 +118,7 @@ struct World {
     // the slots whose filing this operation made from their current position, velocity and radius (the tick's
     // re-filings and a sensor's re-filing back): CheckSensor's fast path then knows the ball comes back to it
     uint64_t fresh[2] = {0, 0};
+    int occupied = EBB_SPACE_MAX_SLOTS;                    // one past the last slot in the park (AFTER_EVOLVE's count)
     EBB_HD bool is_fresh(int64_t j) const { return (fresh[j >> 6] >> (j & 63)) & 1; }
     EBB_HD void set_fresh(int64_t j, bool on) {
         if (on)
@@ -833,7 +834,7 @@ struct World {
     __device__ int nearby_warp(int64_t b, int64_t bub, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked,
                                uint8_t* out, const Filing& fb) const {
         int n = 0;
-        const int S = sort_span();
+        const int S = sort_span() < occupied ? sort_span() : occupied;   // (no candidate past the last slot in the park)
         for (int64_t base = 0; base < S; base += 32) {     // the candidates packed to the front, in slot order
             const int64_t o = base + lane;
             int64_t k = NOT_A_CANDIDATE, i = INT64_MAX;
@@ -1649,7 +1650,7 @@ struct World {
         int64_t n = 0;
 #ifdef __CUDA_ARCH__
         if (lane >= 0) {                                   // the lanes sort the slots by id together
-            int mine = 0;
+            int mine = 0, last = -1;
             const int S = sort_span();
             for (int64_t j = lane; j < S; j += 32) {
                 const bool in = j < N && U(s->in_park, j) && slot_ok(j);
@@ -1657,8 +1658,10 @@ struct World {
                 sh->id[j] = in ? id(j) : INT64_MAX;
                 sh->out[j] = (uint8_t)j;
                 mine += in;
+                if (in) last = (int)j;
             }
             n = (int64_t)__reduce_add_sync(0xffffffffu, (unsigned)mine);
+            occupied = (int)__reduce_max_sync(0xffffffffu, (unsigned)(last + 1));
             __syncwarp();
             warp_sort(S);
             for (int64_t i = 0; i < n; ++i) order[i] = sh->out[i];
@@ -1697,6 +1700,7 @@ struct World {
     }
     EBB_HD void apply(int64_t code, int64_t j, int64_t b, const double* f) {
         fresh[0] = fresh[1] = 0;                           // (an operation's own: AFTER_EVOLVE's re-filings)
+        occupied = EBB_SPACE_MAX_SLOTS;
         const bool has_slot = slot_ok(j);
         const bool live = has_slot && U(s->in_park, j);
         switch (code) {
