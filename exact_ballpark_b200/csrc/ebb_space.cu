@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(128, 12) tape_kernel_warp(const __grid_constan
     __shared__ Coop scratch[4];
     const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (w >= s.worlds) return;                            // (the whole warp: w is the warp's)
-    run_tape<WM>(&p, &s, &t, w, (int)(threadIdx.x & 31), &scratch[threadIdx.x >> 5]);
+    run_tape<WM, true>(&p, &s, &t, w, (int)(threadIdx.x & 31), &scratch[threadIdx.x >> 5]);
 }
 
 template <bool WM>

@@ -106,8 +106,9 @@ struct Coop {
 // One world's program. A thread runs it alone (lane -1), or the 32 lanes of a warp run it together (lane 0 .. 31):
 // every lane then takes every step on the same data, so they stay converged and write the same values (one
 // transaction a load or store), and GetNearbyBalls' scan and sort are split over the lanes (nearby_warp).
-// WM: the world-major arrangement (the state's pitch > 0), else the interleaved one.
-template <bool WM>
+// WM: the world-major arrangement (the state's pitch > 0), else the interleaved one. COOP: a warp runs the world
+// (the lanes' paths compiled in, the single thread's left out), else a thread. (WARP is the flight mode.)
+template <bool WM, bool COOP = false>
 struct World {
     const EbbFlightState* p;
     const EbbSpaceState* s;
@@ -764,8 +765,17 @@ struct World {
         if (lvl(b) < 0) return 0;
         const Filing fb = as ? *as : filing_of(b);
 #ifdef __CUDA_ARCH__
-        if (lane >= 0) return nearby_warp(b, bub, exclude_fixed, exclude_inert, exclude_cloaked, out, fb);
+        if constexpr (COOP) {
+            return nearby_warp(b, bub, exclude_fixed, exclude_inert, exclude_cloaked, out, fb);
+        } else
 #endif
+        {
+            return nearby_serial(b, bub, exclude_fixed, exclude_inert, exclude_cloaked, out, fb);
+        }
+    }
+    // nearby's single-thread form: an insertion by (key, id) as each candidate is met
+    EBB_HDNI int nearby_serial(int64_t b, int64_t bub, bool exclude_fixed, bool exclude_inert, bool exclude_cloaked,
+                             uint8_t* out, const Filing& fb) const {
         int64_t keys[EBB_SPACE_MAX_SLOTS], oid[EBB_SPACE_MAX_SLOTS];
         int n = 0;
         for (int64_t o = 0; o < N; ++o) {
@@ -1174,7 +1184,7 @@ struct World {
         int64_t *ent = own_ent, *nb = own_nb, *nk = own_nk, *made_key = own_made;
         uint8_t *gone = own_gone, *made_lvl = own_lvl;
 #ifdef __CUDA_ARCH__
-        if (lane >= 0) {                                   // (sh->key, id, out: free until GetNearbyBalls)
+        if constexpr (COOP) {                              // (sh->key, id, out: free until GetNearbyBalls)
             ent = sh->key;
             nb = sh->id;
             nk = sh->id + 64;
@@ -1303,11 +1313,17 @@ struct World {
             }
         }
 #ifdef __CUDA_ARCH__
-        if (lane >= 0) {
+        if constexpr (COOP) {
             sensor_events_warp(j, r, cand, nc);
-            return;
-        }
+        } else
 #endif
+        {
+            sensor_events_serial(j, r, cand, nc);
+        }
+    }
+    // check_sensor's events by a single thread: the list's balls no longer near leave in its order, then each
+    // candidate enters or leaves in the walk's order
+    EBB_HDNI void sensor_events_serial(int64_t j, int64_t r, const uint8_t* cand, int nc) const {
         const UMap m = sensor_map(j);
         if (*m.len > 0) {
             uint64_t near[2] = {0, 0};
@@ -1649,7 +1665,7 @@ struct World {
         int64_t order[EBB_SPACE_MAX_SLOTS];
         int64_t n = 0;
 #ifdef __CUDA_ARCH__
-        if (lane >= 0) {                                   // the lanes sort the slots by id together
+        if constexpr (COOP) {                              // the lanes sort the slots by id together
             int mine = 0, last = -1;
             const int S = sort_span();
             for (int64_t j = lane; j < S; j += 32) {
@@ -1738,10 +1754,10 @@ EBB_HD void run_query(const EbbFlightState* p, const EbbSpaceState* s, const Ebb
 }
 
 // world w's K operations of the tape, in order (a flagged world is left alone)
-template <bool WM>
+template <bool WM, bool COOP = false>
 EBB_HD void run_tape(const EbbFlightState* p, const EbbSpaceState* s, const EbbSpaceTape* t, int64_t w, int lane = -1,
                      Coop* sh = nullptr) {
-    World<WM> wd{p, s, w, s->worlds, s->slots, s->boxes, lane, sh};
+    World<WM, COOP> wd{p, s, w, s->worlds, s->slots, s->boxes, lane, sh};
     for (int64_t k = 0; k < t->K; ++k) {
         if (wd.one(s->flags) & (F_EDGE | F_BOXES | F_DICTS | F_ENTRIES | F_SETS | F_BAD_OP)) return;
         const int64_t at = k * s->worlds + w;
