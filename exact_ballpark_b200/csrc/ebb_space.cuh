@@ -1132,6 +1132,32 @@ struct World {
     // would move it (+a; -b floored at 0; -a1 floored; +b; -(a - a1) floored). `fi`: the inflated filing, for
     // GetNearbyBalls.
     EBB_HDNI bool sensor_fast(int64_t j, const double* x, const double* v, float inflated, Filing* fi) {
+        int64_t a = 0, a1 = 0, b = 0;
+        bool same = false;
+        if (!sensor_plan(j, x, v, inflated, fi, &a, &a1, &b, &same, COOP, true)) return false;
+        if (same) EBB_SENSOR_PATH(2);
+        return same || sensor_count(a, a1, b);
+    }
+    // The kept count as the pair would move it, when every release is kept and the table has room (else false)
+    EBB_HD bool sensor_count(int64_t a, int64_t a1, int64_t b) {
+        const int64_t live = one(s->box_n) - one(s->box_free_n);
+        int64_t c = one(s->free_boxes);
+        if (b < 0) return true;                            // (counted as unchanged: see sensor_plan)
+        if (B - live < b + 8 || c + a + b >= BOX_KEEP) return false;
+        c += a;
+        c = c > b ? c - b : 0;
+        c = c > a1 ? c - a1 : 0;
+        c += b;
+        c = c > a - a1 ? c - (a - a1) : 0;
+        one(s->free_boxes) = c;
+        return true;
+    }
+    // sensor_fast's conditions and counts, nothing written: a, a1, b (b = -1 when the kept count cannot move: at
+    // least 56 with room, `shortcut`), `same` when the inflated filing is the ball's own. `shared`: the scratch in
+    // the warp's shared memory (every lane on the same ball), else each thread's (or lane's) own.
+    EBB_HDNI bool sensor_plan(int64_t j, const double* x, const double* v, float inflated, Filing* fi, int64_t* a_out,
+                              int64_t* a1_out, int64_t* b_out, bool* same_out, bool shared, bool shortcut) const {
+        *same_out = false;
         if (lvl(j) < 0 || huge(j) || one(s->flags) != 0) return false;
         const int64_t r = row(j);
         const int64_t box0 = I(s->my_box, j), top = I(s->my_top, j);
@@ -1170,7 +1196,7 @@ struct World {
         }
         if (Li == L1 && ki[0] == k1[0] && ki[1] == k1[1] && ki[2] == k1[2] && mi[0] == m1[0] && mi[1] == m1[1] &&
             mi[2] == m1[2]) {
-            EBB_SENSOR_PATH(2);
+            *same_out = true;
             return true;                                   // both re-filings return at once
         }
         const int64_t boxi = box_find(Li, ki[0], ki[1], ki[2]);
@@ -1184,7 +1210,7 @@ struct World {
         int64_t *ent = own_ent, *nb = own_nb, *nk = own_nk, *made_key = own_made;
         uint8_t *gone = own_gone, *made_lvl = own_lvl;
 #ifdef __CUDA_ARCH__
-        if constexpr (COOP) {                              // (sh->key, id, out: free until GetNearbyBalls)
+        if (COOP && shared) {                              // (sh->key, id, out: free until GetNearbyBalls)
             ent = sh->key;
             nb = sh->id;
             nk = sh->id + 64;
@@ -1238,11 +1264,14 @@ struct World {
             for (int c = 0; c < 3; ++c)
                 if (sk[c] < 0 || sk[c] >= g) return false;
         }
+        *a_out = a;
+        *a1_out = a1;
+        *b_out = -1;
         const int64_t live = one(s->box_n) - one(s->box_free_n);
         const int64_t c0 = one(s->free_boxes);
         // at most 56 boxes made for the sides (7 chains of 8 levels): with the kept count at least that, and room for
         // them, every making takes one off it and every release puts one back (kept below 256): it ends as it began
-        if (c0 >= 56 && c0 + a + 56 < BOX_KEEP && B - live >= 64) return true;
+        if (shortcut && c0 >= 56 && c0 + a + 56 < BOX_KEEP && B - live >= 64) return true;
         // else the boxes the inflated sides make, counted: each side's missing chain, up to a live box or one made
         // before
         int nm = 0;
@@ -1272,20 +1301,17 @@ struct World {
                 ++b;
             }
         }
-        int64_t c = c0;
-        if (B - live < b + 8 || c + a + b >= BOX_KEEP) return false;
-        c += a;
-        c = c > b ? c - b : 0;
-        c = c > a1 ? c - a1 : 0;
-        c += b;
-        c = c > a - a1 ? c - (a - a1) : 0;
-        one(s->free_boxes) = c;
+        *b_out = b;
         return true;
     }
     EBB_HDNI void check_sensor(int64_t j) {
         at(s->selapsed, j) = dadd(at(s->selapsed, j), p->dt);
         if (at(s->selapsed, j) < at(s->speriod, j)) return;
         at(s->selapsed, j) = 0.0;
+        check_sensor_body(j);
+    }
+    // the check itself, its period come
+    EBB_HDNI void check_sensor_body(int64_t j) {
         const int64_t r = row(j);
         const float radius = p->radius[r];
         const double x[3] = {pos(j, 0), pos(j, 1), pos(j, 2)};
@@ -1422,6 +1448,187 @@ struct World {
         }
     }
 #endif
+#ifdef __CUDA_ARCH__
+    // HandleProximities in a warp, 32 sensors at a time: each lane computes one sensor's check ahead (the fast path's
+    // plan, without writing, and its candidates with those in range, as slot sets), then the warp takes the map's
+    // balls in order as one ball does, using a sensor's ahead-computed check while nothing it read has changed: the
+    // world unflagged and no ball's filing changed by an earlier check's re-filings (then the rest of the batch is
+    // checked as it runs alone). The kept count moves in the map's order (sensor_count at the ball's turn).
+    struct Pre {
+        int64_t a, a1, b;
+        Filing fi;
+        uint64_t cand[2], in[2];
+        int ok;                                            // 0 none; 1 the fast path's plan; 2 and the filing the ball's own
+    };
+    __device__ void pre_sensor(int64_t j, Pre& pr) const {
+        pr.ok = 0;
+        pr.cand[0] = pr.cand[1] = pr.in[0] = pr.in[1] = 0;
+        const int64_t r = row(j);
+        const float radius = p->radius[r];
+        const float inflated = fadd(radius, (float)at(s->srange, j));
+        if (inflated < 0.0f || radius < 0.0f) return;
+        const double x[3] = {pos(j, 0), pos(j, 1), pos(j, 2)};
+        const double v[3] = {vel(j, 0), vel(j, 1), vel(j, 2)};
+        bool same = false;
+        if (!sensor_plan(j, x, v, inflated, &pr.fi, &pr.a, &pr.a1, &pr.b, &same, false, false)) return;
+        pr.ok = same ? 2 : 1;
+        const int64_t bub = I(s->bubble, j);
+        const bool excl_fixed = at(s->cloaked, j) == 0, excl_inert = at(s->sonly, j) != 0;
+        if (excl_inert && !set_any(0, bub)) return;       // (no candidates)
+        const float range = (float)at(s->srange, j);
+        const int64_t S = occupied < N ? occupied : N;
+        for (int64_t o = 0; o < S; ++o) {
+            if (o == j || !slot_ok(o) || !U(s->in_park, o) || lvl(o) < 0) continue;
+            if (walk_key(pr.fi, o) == NOT_A_CANDIDATE) continue;
+            const int64_t ro = row(o);
+            if (excl_inert) {
+                if (!p->interactive[ro]) continue;
+            } else {
+                if (I(s->bubble, o) != bub) continue;
+                if (excl_fixed && !p->free_[ro]) continue;
+            }
+            const uint64_t bit = uint64_t(1) << (o & 63);
+            pr.cand[o >> 6] |= bit;
+            const double ck = (double)fadd(fadd(range, p->radius[ro]), radius);
+            const double d0 = dsub(x[0], pos(o, 0)), d1 = dsub(x[1], pos(o, 1)), d2 = dsub(x[2], pos(o, 2));
+            const double len2 = dadd(dadd(dmul(d0, d0), dmul(d1, d1)), dmul(d2, d2));
+            if (!(len2 > dmul(ck, ck))) pr.in[o >> 6] |= bit;
+        }
+    }
+    __device__ static Pre pre_of(const Pre& mine, int i) {
+        Pre o;
+        o.a = __shfl_sync(0xffffffffu, mine.a, i);
+        o.a1 = __shfl_sync(0xffffffffu, mine.a1, i);
+        o.b = __shfl_sync(0xffffffffu, mine.b, i);
+        o.fi.L = __shfl_sync(0xffffffffu, mine.fi.L, i);
+        for (int c = 0; c < 3; ++c) {
+            o.fi.lo[c] = __shfl_sync(0xffffffffu, mine.fi.lo[c], i);
+            o.fi.hi[c] = __shfl_sync(0xffffffffu, mine.fi.hi[c], i);
+        }
+        for (int q = 0; q < 2; ++q) {
+            o.cand[q] = __shfl_sync(0xffffffffu, mine.cand[q], i);
+            o.in[q] = __shfl_sync(0xffffffffu, mine.in[q], i);
+        }
+        o.ok = __shfl_sync(0xffffffffu, mine.ok, i);
+        return o;
+    }
+    // a sensor's events from its ahead-computed sets: the list's balls no longer candidates leave in the list's order;
+    // the candidates whose membership changes enter or leave in the walk's order (their keys made and sorted here)
+    __device__ void sensor_events_pre(int64_t j, const Pre& pr) {
+        const UMap m = sensor_map(j);
+        const int32_t n0 = *m.len;
+        if (n0 > 0) {
+            uint8_t* keys = sh->out;
+            for (int32_t e = lane; e < n0; e += 32) keys[e] = m.k[e * m.step];
+            __syncwarp();
+            for (int32_t base = 0; base < n0; base += 32) {
+                bool gone = false;
+                if (base + lane < n0) {
+                    const int64_t k = keys[base + lane];
+                    gone = k != j && !((pr.cand[k >> 6] >> (k & 63)) & 1);
+                }
+                unsigned bits = __ballot_sync(0xffffffffu, gone);
+                while (bits) {
+                    const int b = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    const int64_t k = keys[base + b];
+                    umap_erase(m, k);
+                    event(EBB_SPACE_EV_PROXIMITY, j, k, 0);
+                }
+            }
+            __syncwarp();
+        }
+        const uint64_t ch[2] = {pr.cand[0] & (pr.in[0] ^ m.m[0]), pr.cand[1] & (pr.in[1] ^ m.m[m.mstep])};
+        if ((ch[0] | ch[1]) == 0) return;
+        int n = 0;
+        for (int base = 0; base < EBB_SPACE_MAX_SLOTS; base += 32) {
+            const int o = base + lane;
+            const bool is = ((ch[o >> 6] >> (o & 63)) & 1) != 0;
+            const unsigned in = __ballot_sync(0xffffffffu, is);
+            if (is) {
+                const int at_ = n + __popc(in & ((1u << lane) - 1u));
+                sh->key[at_] = walk_key(pr.fi, o);
+                sh->id[at_] = id(o);
+                sh->out[at_] = (uint8_t)o;
+            }
+            n += __popc(in);
+        }
+        int P = 1;
+        while (P < n) P <<= 1;
+        for (int e = n + lane; e < P; e += 32) {
+            sh->key[e] = NOT_A_CANDIDATE;
+            sh->id[e] = INT64_MAX;
+        }
+        __syncwarp();
+        warp_sort(P);
+        for (int i = 0; i < n; ++i) {
+            const int64_t o = sh->out[i];
+            if ((pr.in[o >> 6] >> (o & 63)) & 1) {
+                umap_insert(m, o, F_SENSOR_LIST);
+                event(EBB_SPACE_EV_PROXIMITY, j, o, 1);
+            } else {
+                umap_erase(m, o);
+                event(EBB_SPACE_EV_PROXIMITY, j, o, 0);
+            }
+        }
+        __syncwarp();
+    }
+    // CheckSensor at the ball's turn with its ahead-computed check (else as it runs alone; `dirty` when that
+    // changed the ball's filing)
+    __device__ void check_sensor_pre(int64_t j, const Pre& pr, bool& dirty) {
+        at(s->selapsed, j) = dadd(at(s->selapsed, j), p->dt);
+        if (at(s->selapsed, j) < at(s->speriod, j)) return;
+        at(s->selapsed, j) = 0.0;
+        if (pr.ok && !dirty && one(s->flags) == 0 && (pr.ok == 2 || sensor_count(pr.a, pr.a1, pr.b))) {
+            EBB_SENSOR_PATH(0);
+            EBB_SENSOR_PATH(1);
+            if (pr.ok == 2) EBB_SENSOR_PATH(2);
+            sensor_events_pre(j, pr);
+            return;
+        }
+        const int64_t l0 = lvl(j), k0 = key(j, 0), k1 = key(j, 1), k2 = key(j, 2), m0 = mod(j, 0), m1 = mod(j, 1),
+                      m2 = mod(j, 2), a0 = active(j);
+        check_sensor_body(j);
+        if (lvl(j) != l0 || key(j, 0) != k0 || key(j, 1) != k1 || key(j, 2) != k2 || mod(j, 0) != m0 ||
+            mod(j, 1) != m1 || mod(j, 2) != m2 || active(j) != a0)
+            dirty = true;
+    }
+    __device__ void handle_proximities_warp(const uint8_t* keys, int32_t n) {
+        for (int32_t batch = 0; batch < n; batch += 32) {
+            Pre mine;
+            mine.ok = 0;
+            mine.a = mine.a1 = mine.b = 0;
+            mine.fi = Filing{};
+            mine.cand[0] = mine.cand[1] = mine.in[0] = mine.in[1] = 0;
+            if (batch + lane < n) {
+                const int64_t j = keys[batch + lane];
+                if (slot_ok(j) && U(s->in_park, j) && p->sensor[row(j)]) pre_sensor(j, mine);
+            }
+            __syncwarp();
+            bool dirty = false;
+            const int32_t end = n < batch + 32 ? n : batch + 32;
+            for (int32_t e = batch; e < end; ++e) {
+                const Pre pr = pre_of(mine, e - batch);
+                const int64_t j = keys[e];
+                if (!slot_ok(j) || !U(s->in_park, j)) continue;
+                if (in_dead_bubble(j)) {
+                    if (at(s->slen, j) > 0) {
+                        at(s->selapsed, j) = at(s->speriod, j);
+                        check_notification_range(j);
+                        check_target_tracking(j);
+                        if (p->sensor[row(j)]) check_sensor_pre(j, pr, dirty);
+                    }
+                    umap_clear(sensor_map(j));
+                    continue;
+                }
+                if (!at(s->has_prox, j)) continue;
+                check_notification_range(j);
+                check_target_tracking(j);
+                if (p->sensor[row(j)]) check_sensor_pre(j, pr, dirty);
+            }
+        }
+    }
+#endif
     EBB_HD void check_for_proximity(int64_t j) {
         check_notification_range(j);
         check_target_tracking(j);
@@ -1434,6 +1641,12 @@ struct World {
         const int32_t n = *pm.len;
         uint8_t keys[EBB_SPACE_MAX_SLOTS];
         for (int32_t e = 0; e < n; ++e) keys[e] = pm.k[e * pm.step];
+#ifdef __CUDA_ARCH__
+        if constexpr (COOP) {
+            handle_proximities_warp(keys, n);
+            return;
+        }
+#endif
         for (int32_t e = 0; e < n; ++e) {
             const int64_t j = keys[e];
             if (!slot_ok(j) || !U(s->in_park, j)) continue;
