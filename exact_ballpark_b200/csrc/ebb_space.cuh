@@ -1132,21 +1132,25 @@ struct World {
     // would move it (+a; -b floored at 0; -a1 floored; +b; -(a - a1) floored). `fi`: the inflated filing, for
     // GetNearbyBalls.
     EBB_HDNI bool sensor_fast(int64_t j, const double* x, const double* v, float inflated, Filing* fi) {
-        int64_t a = 0, a1 = 0, b = 0;
+        int64_t a = 0, a1 = 0, ak = 0, b = 0;
         bool same = false;
-        if (!sensor_plan(j, x, v, inflated, fi, &a, &a1, &b, &same, COOP, true)) return false;
+        if (!sensor_plan(j, x, v, inflated, fi, &a, &a1, &ak, &b, &same, COOP, true)) return false;
         if (same) EBB_SENSOR_PATH(2);
-        return same || sensor_count(a, a1, b);
+        return same || sensor_count(a, a1, ak, b);
     }
-    // The kept count as the pair would move it, when every release is kept and the table has room (else false)
-    EBB_HD bool sensor_count(int64_t a, int64_t a1, int64_t b) {
+    // The kept count as the pair would move it, when every release is kept and the table has room (else false): +a
+    // (the leaving's releases), -ak floored at 0 (the inflated box's chain made again), -b floored (its sides), -(a1
+    // - ak) floored (the ball's own box's chain below it made again), +b (the sides released), -(a - a1) floored (the
+    // ball's own sides made again)
+    EBB_HD bool sensor_count(int64_t a, int64_t a1, int64_t ak, int64_t b) {
         const int64_t live = one(s->box_n) - one(s->box_free_n);
         int64_t c = one(s->free_boxes);
         if (b < 0) return true;                            // (counted as unchanged: see sensor_plan)
-        if (B - live < b + 8 || c + a + b >= BOX_KEEP) return false;
+        if (B - live < b + ak + 8 || c + a + b >= BOX_KEEP) return false;
         c += a;
+        c = c > ak ? c - ak : 0;
         c = c > b ? c - b : 0;
-        c = c > a1 ? c - a1 : 0;
+        c = c > a1 - ak ? c - (a1 - ak) : 0;
         c += b;
         c = c > a - a1 ? c - (a - a1) : 0;
         one(s->free_boxes) = c;
@@ -1156,7 +1160,8 @@ struct World {
     // least 56 with room, `shortcut`), `same` when the inflated filing is the ball's own. `shared`: the scratch in
     // the warp's shared memory (every lane on the same ball), else each thread's (or lane's) own.
     EBB_HDNI bool sensor_plan(int64_t j, const double* x, const double* v, float inflated, Filing* fi, int64_t* a_out,
-                              int64_t* a1_out, int64_t* b_out, bool* same_out, bool shared, bool shortcut) const {
+                              int64_t* a1_out, int64_t* ak_out, int64_t* b_out, bool* same_out, bool shared,
+                              bool shortcut) const {
         *same_out = false;
         if (lvl(j) < 0 || huge(j) || one(s->flags) != 0) return false;
         const int64_t r = row(j);
@@ -1241,7 +1246,7 @@ struct World {
             while (nb[i] == 0 && nk[i] == 0 && !gone[i]) {
                 gone[i] = 1;
                 ++a;
-                if (e == boxi || I(s->box_level, e) == 0) return false;   // the inflated box, or a top box, emptied
+                if (I(s->box_level, e) == 0 && e != top) return false;   // another top box emptied: its bubble lost
                 e = I(s->box_parent, e);
                 if (e < 0) break;
                 i = slot_of_entry(e);
@@ -1249,13 +1254,32 @@ struct World {
                 --nk[i];
             }
         }
+        // (gone: 1 released, 2 released and made again by the inflated filing's GetBox: the inflated box emptied, its
+        // chain up to a live box released and made again at once, before the sides, with the top box's bubble set)
         auto released = [&](int64_t e) -> bool {
             for (int i = 0; i < ne; ++i)
-                if (ent[i] == e) return gone[i] != 0;
+                if (ent[i] == e) return gone[i] == 1;
             return false;
         };
+        auto gone_at = [&](int64_t e) -> int {
+            for (int i = 0; i < ne; ++i)
+                if (ent[i] == e) return i;
+            return -1;
+        };
+        int64_t ak = 0;
+        for (int64_t e = boxi; e >= 0; e = I(s->box_parent, e)) {
+            const int i = gone_at(e);
+            if (i < 0 || !gone[i]) break;
+            gone[i] = 2;
+            ++ak;
+        }
+        if (ak > 0 && Li == L1) return false;             // (the ball's own box emptied, made again, emptied again)
         int64_t a1 = 0;
-        for (int64_t e = box0; e >= 0 && released(e); e = I(s->box_parent, e)) ++a1;
+        for (int64_t e = box0; e >= 0; e = I(s->box_parent, e)) {
+            const int i = gone_at(e);
+            if (i < 0 || !gone[i]) break;
+            ++a1;
+        }
         const int64_t g = level_grid(Li);
         for (int side = 1; side < 8; ++side) {             // the inflated sides inside the grid
             if (((side & 1) && !mi[0]) || ((side & 2) && !mi[1]) || ((side & 4) && !mi[2])) continue;
@@ -1266,12 +1290,13 @@ struct World {
         }
         *a_out = a;
         *a1_out = a1;
+        *ak_out = ak;
         *b_out = -1;
         const int64_t live = one(s->box_n) - one(s->box_free_n);
         const int64_t c0 = one(s->free_boxes);
         // at most 56 boxes made for the sides (7 chains of 8 levels): with the kept count at least that, and room for
         // them, every making takes one off it and every release puts one back (kept below 256): it ends as it began
-        if (shortcut && c0 >= 56 && c0 + a + 56 < BOX_KEEP && B - live >= 64) return true;
+        if (shortcut && ak == 0 && c0 >= 56 && c0 + a + 56 < BOX_KEEP && B - live >= 64) return true;
         // else the boxes the inflated sides make, counted: each side's missing chain, up to a live box or one made
         // before
         int nm = 0;
@@ -1455,7 +1480,7 @@ struct World {
     // world unflagged and no ball's filing changed by an earlier check's re-filings (then the rest of the batch is
     // checked as it runs alone). The kept count moves in the map's order (sensor_count at the ball's turn).
     struct Pre {
-        int64_t a, a1, b;
+        int64_t a, a1, ak, b;
         Filing fi;
         uint64_t cand[2], in[2];
         int ok;                                            // 0 none; 1 the fast path's plan; 2 and the filing the ball's own
@@ -1470,7 +1495,7 @@ struct World {
         const double x[3] = {pos(j, 0), pos(j, 1), pos(j, 2)};
         const double v[3] = {vel(j, 0), vel(j, 1), vel(j, 2)};
         bool same = false;
-        if (!sensor_plan(j, x, v, inflated, &pr.fi, &pr.a, &pr.a1, &pr.b, &same, false, false)) return;
+        if (!sensor_plan(j, x, v, inflated, &pr.fi, &pr.a, &pr.a1, &pr.ak, &pr.b, &same, false, false)) return;
         pr.ok = same ? 2 : 1;
         const int64_t bub = I(s->bubble, j);
         const bool excl_fixed = at(s->cloaked, j) == 0, excl_inert = at(s->sonly, j) != 0;
@@ -1499,6 +1524,7 @@ struct World {
         Pre o;
         o.a = __shfl_sync(0xffffffffu, mine.a, i);
         o.a1 = __shfl_sync(0xffffffffu, mine.a1, i);
+        o.ak = __shfl_sync(0xffffffffu, mine.ak, i);
         o.b = __shfl_sync(0xffffffffu, mine.b, i);
         o.fi.L = __shfl_sync(0xffffffffu, mine.fi.L, i);
         for (int c = 0; c < 3; ++c) {
@@ -1579,7 +1605,7 @@ struct World {
         at(s->selapsed, j) = dadd(at(s->selapsed, j), p->dt);
         if (at(s->selapsed, j) < at(s->speriod, j)) return;
         at(s->selapsed, j) = 0.0;
-        if (pr.ok && !dirty && one(s->flags) == 0 && (pr.ok == 2 || sensor_count(pr.a, pr.a1, pr.b))) {
+        if (pr.ok && !dirty && one(s->flags) == 0 && (pr.ok == 2 || sensor_count(pr.a, pr.a1, pr.ak, pr.b))) {
             EBB_SENSOR_PATH(0);
             EBB_SENSOR_PATH(1);
             if (pr.ok == 2) EBB_SENSOR_PATH(2);
@@ -1597,7 +1623,7 @@ struct World {
         for (int32_t batch = 0; batch < n; batch += 32) {
             Pre mine;
             mine.ok = 0;
-            mine.a = mine.a1 = mine.b = 0;
+            mine.a = mine.a1 = mine.ak = mine.b = 0;
             mine.fi = Filing{};
             mine.cand[0] = mine.cand[1] = mine.in[0] = mine.in[1] = 0;
             if (batch + lane < n) {

@@ -642,3 +642,21 @@ def drive_ticks_host(ops, seed: int = 1, world_major: bool = False) -> list:
             t += answer_text(row, qo, qd, 0)
         out.append(t)
     return out
+
+
+def partition_world_ops(pw, w: int, goto: np.ndarray, ticks: int) -> np.ndarray:
+    """World w of the partition worlds as a golden-style stream: AddBall of each ship, its sensor, its goto point,
+    then the ticks."""
+    c = pw.cols
+    s0, k = int(pw.starts[w]), int(pw.sizes[w])
+    ops = []
+    for j in range(k):
+        r = s0 + j
+        ops.append(sp._op(sp.ADD, j + 1, c["mass"][r], c["radius"][r], c["max_vel"][r], 1.0, 1.0, *c["pos"][r],
+                          0.0, 0.0, 0.0, c["agility"][r], 1.0, 0.0))
+    for j in range(k):
+        ops.append(sp._op(sp.SENSOR, j + 1, pw.sensor_range[s0 + j], 1.0, 0.0, 0.0))
+    for j in range(k):
+        ops.append(sp._op(sp.GOTO, j + 1, *goto[s0 + j]))
+    ops += [sp._op(sp.TICK) for _ in range(ticks)]
+    return np.array(ops)

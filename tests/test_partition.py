@@ -16,24 +16,6 @@ from oracle import space_world
 pytestmark = pytest.mark.gpu
 
 
-def _world_ops(pw, w: int, goto: np.ndarray, ticks: int) -> np.ndarray:
-    """World w of the partition worlds as a golden-style stream: AddBall of each ship, its sensor, its goto point,
-    then the ticks."""
-    c = pw.cols
-    s0, k = int(pw.starts[w]), int(pw.sizes[w])
-    ops = []
-    for j in range(k):
-        r = s0 + j
-        ops.append(sp._op(sp.ADD, j + 1, c["mass"][r], c["radius"][r], c["max_vel"][r], 1.0, 1.0, *c["pos"][r],
-                          0.0, 0.0, 0.0, c["agility"][r], 1.0, 0.0))
-    for j in range(k):
-        ops.append(sp._op(sp.SENSOR, j + 1, pw.sensor_range[s0 + j], 1.0, 0.0, 0.0))
-    for j in range(k):
-        ops.append(sp._op(sp.GOTO, j + 1, *goto[s0 + j]))
-    ops += [sp._op(sp.TICK) for _ in range(ticks)]
-    return np.array(ops)
-
-
 def _world_text(part, park, pw, w: int, events: bool) -> str:
     """World w's layer state as the oracle's state text (and the last tick's events)."""
     layer, col = part.world(w)
@@ -92,7 +74,7 @@ def test_the_ragged_batch_matches_the_plain_layout_and_the_oracle():
     order = np.argsort(pw.sizes)
     sample = sorted(set([int(order[-1]), int(order[-2]), int(order[0])] + [int(x) for x in order[::60]]))
     for w in sample:
-        want = space_world.run(_world_ops(pw, w, goto, ticks), seed=w + 1)[-1]
+        want = space_world.run(sl.partition_world_ops(pw, w, goto, ticks), seed=w + 1)[-1]
         assert _world_text(ragged, pr, pw, w, True) == sl.oracle_lines(want, sp.TICK), (w, int(pw.sizes[w]))
 
 

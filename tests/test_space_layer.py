@@ -101,6 +101,24 @@ def test_the_layers_tick_matches_the_oracle_in_crowded_sensing_worlds_on_the_cpu
     assert not bad, f"{len(bad)} worlds differ, first {bad[:3]}"
 
 
+def test_the_layers_tick_matches_the_oracle_on_partition_worlds_on_the_cpu():
+    """Worlds of the partition benchmark (the largest, one of about 45 ships, one small; sensors of 1-250 km on every
+    ship, each flying its pilot's direction): the layer's host build, whose sensor checks there mostly skip their two
+    re-filings (the inflated box's chain emptied and made again among them), against the oracle's tick."""
+    from exact_ballpark_b200.workloads import partition_worlds
+    pw = partition_worlds(11, 1200)
+    order = np.argsort(-pw.sizes, kind="stable")
+    goto = pw.cols["pos"] + pw.direction * 1e9
+    bad = []
+    for w in (int(order[0]), int(order[1]), int(order[150]), int(order[600])):
+        ops = sl.partition_world_ops(pw, w, goto, 5)
+        got = sl.drive_ticks_host(ops, seed=w + 1)
+        want = [sl.oracle_lines(t, int(op[0])) for t, op in zip(space_world.run(ops, seed=w + 1), ops)]
+        if got != want:
+            bad.append((w, int(pw.sizes[w]), next(i for i, (x, y) in enumerate(zip(want, got)) if x != y)))
+    assert not bad, f"{len(bad)} worlds differ, first {bad[:3]}"
+
+
 @pytest.mark.parametrize("family,world_major", [("tick", False), ("modes", False), ("tick", True)])
 def test_the_layers_tick_matches_the_oracle_on_the_cpu(family, world_major):
     """The ticking and the mode streams (GOTO and STOP ships; FollowBall, Orbit and WarpTo with drop-outs, releases
