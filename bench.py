@@ -759,7 +759,7 @@ def partition_runs(args, dev) -> dict:
     state, compared here bit for bit (the park's rows, each world's event count)."""
     import torch
 
-    from exact_ballpark_b200.partition import partition_setup
+    from exact_ballpark_b200.partition import partition_setup, tune_partition
     from exact_ballpark_b200.workloads import partition_worlds
     W, K = args.partition_worlds, args.partition_steps
     pw = partition_worlds(11, W)
@@ -768,9 +768,10 @@ def partition_runs(args, dev) -> dict:
     stream = torch.cuda.current_stream(dev)
     out = {}
     runs = {}
+    plan = None if args.no_partition_autotune else tune_partition(pw, dev)[0]
     for name, ragged in (("ragged", True), ("plain", False)):
         t0 = time.time()
-        r = partition_setup(pw, dev, ragged, warp_class=args.partition_warp_class)   # exact_ballpark_b200.partition
+        r = partition_setup(pw, dev, ragged, warp_class=args.partition_warp_class, plan=plan)
         setup_s = time.time() - t0
         g = r["graph"]
         for _ in range(args.warmup):

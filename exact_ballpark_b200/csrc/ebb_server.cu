@@ -434,7 +434,7 @@ __device__ void history(const World& x, const EbbServerQueue& q, int64_t j0, int
                                                              : (valid && live && q.ball[a] > 0);
             if (go) route = x.route_of(row);
         }
-        q.route[w * q.slots + j] = route;
+        q.route[j * s.worlds + w] = route;
     }
 }
 
@@ -445,7 +445,7 @@ __device__ void flags(const World& x, const EbbServerQueue& q) {
     uint64_t character[2] = {0, 0};                       // the world's rows (by position) routed to their character
     bool uncloaks = false;
     for (int64_t j = 0; j < J; ++j) {
-        const int8_t route = q.route[w * J + j];
+        const int8_t route = q.route[j * W + w];
         bubble = bubble || route == EBB_ROUTE_BUBBLE;
         uncloaks = uncloaks || q.kinds[j] == EBB_KIND_UNCLOAK;
         if (route != EBB_ROUTE_CHARACTER) continue;
@@ -464,7 +464,7 @@ __device__ void flags(const World& x, const EbbServerQueue& q) {
         } else {                                          // a world wider than the mask: the slots again
             for (int64_t j = 0; j < J && !has; ++j) {
                 const int64_t a = j * W + w;
-                has = q.ok[a] && q.row[a] == r && q.route[w * J + j] == EBB_ROUTE_CHARACTER;
+                has = q.ok[a] && q.row[a] == r && q.route[j * W + w] == EBB_ROUTE_CHARACTER;
             }
         }
         for (int64_t j = 0; j < J && uncloaks && !has; ++j)

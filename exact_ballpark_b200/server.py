@@ -219,7 +219,7 @@ class VecServer:
         q = {"kinds": torch.tensor(kinds, dtype=torch.int32).to(d), "mask": z(J, W, dt=U8), "ball": z(J, W),
              "target": z(J, W), "f": z(J, W, 4, dt=F64), "n": z(J, W), "loc_in": z(J, W),
              "ok": z(J, W, dt=BOOL), "row": z(J, W), "trow": z(J, W), "loc": z(J, W),
-             "route": z(W, J, dt=torch.int8), "notice": z(J, R, dt=BOOL), "stamp": z(W), "clock": z(W),
+             "route": z(J, W, dt=torch.int8).t(), "notice": z(J, R, dt=BOOL), "stamp": z(W), "clock": z(W),
              "has_character": z(R, dt=BOOL), "gets_bubble": z(R, dt=BOOL)}
         for k, v in (cols or {}).items():
             q[k].copy_(v)

@@ -141,7 +141,7 @@ typedef struct EbbServerState {
  * CloakBall's tested bubble: no duplicate test again; the tested calls are a prefix of the queue), ball id, target id,
  * float arguments (4), int argument and SetBallPosition's local flag ([J][W], f [J][W][4]); out: per slot and world the
  * queued flag, the ball's and target's rows (-1 none) and the local argument or CloakBall's bubble (0, or -1 before
- * the ball's old bubble is its bubble) ([J][W]); the routes [W][J]; the uncloaks' AddBallsToPark recipients [J][n]
+ * the ball's old bubble is its bubble) ([J][W]); the routes [J][W]; the uncloaks' AddBallsToPark recipients [J][n]
  * (rows of other slots untouched); the world's stamp and park time [W]; the send flags [n]. */
 typedef struct EbbServerQueue {
     int64_t slots;
