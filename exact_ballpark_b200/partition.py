@@ -245,21 +245,23 @@ ARRANGEMENTS = ((1, 64), (1, 128), (32, 128))      # (lanes, block): a thread a 
 def tune_partition(pw, dev, warm: int = 1, ticks: int = 2, arrangements=ARRANGEMENTS) -> tuple:
     """The ragged batch's autotuner: each size class's arrangement (a thread a world, 2 or 4 warps of worlds a
     block; or a warp a world, 4 worlds a block), measured on the workload itself. For each arrangement every class
-    runs it: the worlds are loaded, their sensors added, `warm` ticks run, then `ticks` ticks each with every class's
-    re-filings and HandleProximities timed alone (CUDA events); every arrangement starts from the same state and does
-    the same work (its results are bit-identical). The classes run one after another in a tick, so each takes its
-    fastest arrangement. Returns (plan {class: (lanes, block)}, {arrangement: {class: ms a tick}})."""
+    runs it: the worlds are loaded, their sensors added, the server layer on top (the pilots' commands every tick, so
+    the ships move as in the benchmark), `warm` ticks run, then `ticks` ticks each with every class's re-filings and
+    HandleProximities timed alone (CUDA events); every arrangement starts from the same state and does the same work
+    (its results are bit-identical). The classes run one after another in a tick, so each takes its fastest
+    arrangement. Returns (plan {class: (lanes, block)}, {arrangement: {class: ms a tick}})."""
     times = {}
     for lanes, block in arrangements:
         plan = {cap: (lanes, block) for cap in CLASSES}
-        r = partition_setup(pw, dev, ragged=True, server_on=False, plan=plan)
-        part, park_tick = r["part"], r["park_tick"]
+        r = partition_setup(pw, dev, ragged=True, server_on=True, plan=plan)
+        part, park_tick, srv, q = r["part"], r["park_tick"], r["server"], r["q"]
         for _ in range(warm):
-            part.tick(park_tick)
+            r["graph"].tick()
         stream = torch.cuda.current_stream(dev)
         ms = {layer.N: 0.0 for layer, _ in part.layers}
         park = part.park
         for _ in range(ticks):
+            srv._launch(q, 5)
             dead = part.dead_rows()
             saved = park._moribund.clone()
             park._moribund.logical_or_(dead)
@@ -273,8 +275,10 @@ def tune_partition(pw, dev, warm: int = 1, ticks: int = 2, arrangements=ARRANGEM
                 b.record(stream)
                 b.synchronize()
                 ms[layer.N] += a.elapsed_time(b) / ticks
+            srv._launch(q, 3)
+            park.current_time += 1
         times[(lanes, block)] = ms
-        del r, part
+        del r, part, srv, q
         torch.cuda.empty_cache()
     best = {}
     for cap in CLASSES:
