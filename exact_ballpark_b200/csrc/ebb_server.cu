@@ -322,7 +322,12 @@ __device__ void queue(const World& x, const EbbServerQueue& q) {
         rows[k] = k < s.width ? x.rows[k] : -1;
     }
     const int64_t span = s.width > IDS_IN_REGISTERS ? x.listed_span() : s.width;
+    // a wide world whose listed balls are ids 1, 2, ... in order (each id once, no pad among them): a ball's row is
+    // then at its id's position, and an id outside them is no ball's (the pads past them have row -1)
+    bool ordered = s.width > IDS_IN_REGISTERS;
+    for (int64_t k = 0; ordered && k < span; ++k) ordered = x.ids[k] == k + 1 && x.rows[k] >= 0;
     auto lookup = [&](int64_t id) -> int64_t {
+        if (ordered) return id >= 1 && id <= span ? x.rows[id - 1] : -1;
         if (s.width > IDS_IN_REGISTERS) return x.lookup(id, span);
         int64_t found = -1;
 #pragma unroll

@@ -615,8 +615,28 @@ struct World {
         }
         const int64_t mx = m[0], my = m[1], mz = m[2];
         fbox(j, 0) = box1;
+        // a warp finds the side boxes that exist at once, a lane a side (no side's making makes another side's box,
+        // and making moves no entry); the others are made in order
+        int64_t found = -1;
+#ifdef __CUDA_ARCH__
+        if constexpr (COOP) {
+            const int bits = lane & 7;
+            const bool on = lane >= 1 && lane <= 7 && !((bits & 1) && !mx) && !((bits & 2) && !my) && !((bits & 4) && !mz);
+            if (on && (mx | my | mz)) {
+                const int64_t kx = ix + ((bits & 1) ? mx : 0), ky = iy + ((bits & 2) ? my : 0),
+                              kz = iz + ((bits & 4) ? mz : 0);
+                const int64_t g = level_grid(level);
+                if (kx >= 0 && kx < g && ky >= 0 && ky < g && kz >= 0 && kz < g) found = box_find(level, kx, ky, kz);
+            }
+        }
+#endif
         auto side = [&](int64_t a, int64_t b, int64_t c) {
-            const int64_t e = get_box(ix + a, iy + b, iz + c, level);
+            const int bits = (a != 0) | ((b != 0) << 1) | ((c != 0) << 2);
+            int64_t e = -1;
+#ifdef __CUDA_ARCH__
+            if constexpr (COOP) e = __shfl_sync(0xffffffffu, found, bits);
+#endif
+            if (e < 0) e = get_box(ix + a, iy + b, iz + c, level);
             insert_in_box(j, e);
             fbox(j, (a != 0) | ((b != 0) << 1) | ((c != 0) << 2)) = e;
             act |= int64_t(1) << (13 + a + 3 * b + 9 * c);
@@ -701,6 +721,18 @@ struct World {
     // the ancestor's distance or the box's post-order code (path digits below b's level, 64 past o's level).
     // Relatedness factors over the axes: the finer filing's key range, shifted to the coarser level, meets the
     // coarser's.
+    // whether slot o's filing meets b's walk (walk_key's first test: it then has a key)
+    EBB_HD bool related(const Filing& fb, int64_t o) const {
+        const Filing fo = filing_of(o);
+        const bool coarse = fo.L <= fb.L;
+        const int64_t sh = 2 * (coarse ? fb.L - fo.L : fo.L - fb.L);
+        for (int q = 0; q < 3; ++q) {
+            const int64_t xl = (coarse ? fb.lo[q] : fo.lo[q]) >> sh, xh = (coarse ? fb.hi[q] : fo.hi[q]) >> sh;
+            const int64_t yl = coarse ? fo.lo[q] : fb.lo[q], yh = coarse ? fo.hi[q] : fb.hi[q];
+            if ((xl > yl ? xl : yl) > (xh < yh ? xh : yh)) return false;
+        }
+        return true;
+    }
     EBB_HD int64_t walk_key(const Filing& fb, int64_t o) const {
         const Filing fo = filing_of(o);
         const int64_t Lb = fb.L, Ln = fo.L;
@@ -1504,7 +1536,7 @@ struct World {
         const int64_t S = occupied < N ? occupied : N;
         for (int64_t o = 0; o < S; ++o) {
             if (o == j || !slot_ok(o) || !U(s->in_park, o) || lvl(o) < 0) continue;
-            if (walk_key(pr.fi, o) == NOT_A_CANDIDATE) continue;
+            if (!related(pr.fi, o)) continue;              // (a candidate's key is made only if its membership changes)
             const int64_t ro = row(o);
             if (excl_inert) {
                 if (!p->interactive[ro]) continue;
@@ -1941,17 +1973,58 @@ struct World {
             const double op[3] = {p->old_pos[r], p->old_pos[p->n + r], p->old_pos[2 * p->n + r]};
             insert_in_boxes(j, op, ov);
         }
+        // the commits' re-filings; a warp first finds, a lane a ball, those whose re-filing leaves everything as it is
+        // (refile_noop: nothing an earlier ball's re-filing writes changes that), and files the others in id order
+        uint64_t noop[2] = {0, 0};
+#ifdef __CUDA_ARCH__
+        if constexpr (COOP) {
+            for (int64_t i0 = 0; i0 < n; i0 += 32) {
+                bool q = false;
+                int64_t jj = -1;
+                if (i0 + lane < n) {
+                    jj = order[i0 + lane];
+                    q = !U(s->dead, jj) && p->free_[row(jj)] && refile_noop(jj);
+                }
+                unsigned bits = __ballot_sync(0xffffffffu, q);
+                while (bits) {
+                    const int b = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    const int64_t k = __shfl_sync(0xffffffffu, jj, b);
+                    noop[k >> 6] |= uint64_t(1) << (k & 63);
+                }
+            }
+        }
+#endif
         for (int64_t i = 0; i < n; ++i) {
             const int64_t j = order[i], r = row(j);
             if (U(s->dead, j) || !p->free_[r]) continue;
             double d[3];
             for (int c = 0; c < 3; ++c) d[c] = dsub(p->pos[c * p->n + r], p->old_pos[c * p->n + r]);
             if (!(dadd(dadd(dmul(d[0], d[0]), dmul(d[1], d[1])), dmul(d[2], d[2])) < 0.1)) {
-                insert_in_boxes(j);
+                if (!((noop[j >> 6] >> (j & 63)) & 1)) insert_in_boxes(j);
                 set_fresh(j, true);
             }
         }
         handle_proximities();
+    }
+    // Whether InsertInBoxes of ball j at its position and velocity changes nothing: the same box (level and keys) with
+    // its entries kept, its top's bubble the ball's, the same sides. Read-only; for the tick's re-filings.
+    EBB_HD bool refile_noop(int64_t j) const {
+        if (lvl(j) < 0 || I(s->my_box, j) < 0 || I(s->my_top, j) < 0) return false;
+        const double x[3] = {pos(j, 0), pos(j, 1), pos(j, 2)}, v[3] = {vel(j, 0), vel(j, 1), vel(j, 2)};
+        const double inflated = inflated_radius(j, v);
+        const int level0 = level_for(inflated);
+        if (level0 != lvl(j)) return false;
+        int64_t k[3], m[3];
+        key_for(level0, x, k);
+        for (int c = 0; c < 3; ++c)
+            if (k[c] != key(j, c)) return false;
+        const int64_t bub = I(s->box_bubble, I(s->my_top, j));
+        if (bub == -1 || bub != I(s->bubble, j)) return false;
+        side_mods(level0, k, inflated, x, m);
+        for (int c = 0; c < 3; ++c)
+            if (m[c] != mod(j, c)) return false;
+        return true;
     }
     EBB_HD void apply(int64_t code, int64_t j, int64_t b, const double* f) {
         fresh[0] = fresh[1] = 0;                           // (an operation's own: AFTER_EVOLVE's re-filings)
