@@ -142,6 +142,20 @@ struct World {
     EBB_HD int64_t& I3(int64_t* a, int64_t c, int64_t e, int64_t cap) const { return at(a, c * cap + e); }
     EBB_HD uint8_t& U(uint8_t* a, int64_t e) const { return at(a, e); }
     EBB_HD int64_t& one(int64_t* a) const { return at(a, 0); }
+    // the box table's per-entry fields: interleaved [cap][W] arrays, or (world-major) records of BOX_RECORD words an
+    // entry, each field's pointer naming it in world 0's entry 0, so that an entry's fields share a cache line
+    EBB_HD int64_t& BX(int64_t* a, int64_t e) const {
+        if constexpr (WM)
+            return ((int64_t*)((const char*)a + w * s->pitch))[e * EBB_SPACE_BOX_RECORD];
+        else
+            return a[e * W + w];
+    }
+    EBB_HD int64_t& BK(int64_t c, int64_t e) const {
+        if constexpr (WM)
+            return ((int64_t*)((const char*)s->box_key + w * s->pitch))[e * EBB_SPACE_BOX_RECORD + c];
+        else
+            return s->box_key[(c * B + e) * W + w];
+    }
     EBB_HD void flag(int64_t f) const { one(s->flags) |= f; }
 
     // ---- the park's row of a slot ----
@@ -166,8 +180,8 @@ struct World {
 #endif
     }
     EBB_HD bool is_box(int64_t e, int level, int64_t kx, int64_t ky, int64_t kz) const {
-        return I(s->box_level, e) == level && I3(s->box_key, 0, e, B) == kx && I3(s->box_key, 1, e, B) == ky &&
-               I3(s->box_key, 2, e, B) == kz;
+        return BX(s->box_level, e) == level && BK(0, e) == kx && BK(1, e) == ky &&
+               BK(2, e) == kz;
     }
     EBB_HD int64_t box_find(int level, int64_t kx, int64_t ky, int64_t kz) const {
         const int64_t H = 2 * B;
@@ -183,13 +197,13 @@ struct World {
     // (each entry keeps its home slot and the slot it sits in, so that its removal starts there without a probe)
     EBB_HD void hash_insert(int64_t e) {
         const int64_t H = 2 * B;
-        int64_t i = home((int)I(s->box_level, e), I3(s->box_key, 0, e, B), I3(s->box_key, 1, e, B),
-                         I3(s->box_key, 2, e, B));
-        I(s->box_home, e) = i;
+        int64_t i = home((int)BX(s->box_level, e), BK(0, e), BK(1, e),
+                         BK(2, e));
+        BX(s->box_home, e) = i;
         for (int64_t probe = 0; probe < H; ++probe) {
             if (I(s->box_hash, i) == 0) {
                 I(s->box_hash, i) = e + 1;
-                I(s->box_slot, e) = i;
+                BX(s->box_slot, e) = i;
                 return;
             }
             i = i + 1 == H ? 0 : i + 1;
@@ -199,18 +213,18 @@ struct World {
     // the entry leaves the index; the entries after it in its run move back so that every probe still finds them
     EBB_HD void hash_erase(int64_t e) {
         const int64_t H = 2 * B;
-        int64_t i = I(s->box_slot, e);
+        int64_t i = BX(s->box_slot, e);
         if (I(s->box_hash, i) != e + 1) return;            // (never: the slot is kept as entries move)
         int64_t j = i;
         for (int64_t step = 0; step < H; ++step) {
             j = j + 1 == H ? 0 : j + 1;
             const int64_t v = I(s->box_hash, j);
             if (v == 0) break;
-            const int64_t k = I(s->box_home, v - 1);
+            const int64_t k = BX(s->box_home, v - 1);
             const bool stays = i <= j ? (i < k && k <= j) : (i < k || k <= j);
             if (stays) continue;
             I(s->box_hash, i) = v;
-            I(s->box_slot, v - 1) = i;
+            BX(s->box_slot, v - 1) = i;
             i = j;
         }
         I(s->box_hash, i) = 0;
@@ -240,13 +254,13 @@ struct World {
             one(s->box_n) = n + 1;
         }
         if (one(s->free_boxes) > 0) --one(s->free_boxes);
-        I(s->box_level, e) = level;
-        I3(s->box_key, 0, e, B) = kx;
-        I3(s->box_key, 1, e, B) = ky;
-        I3(s->box_key, 2, e, B) = kz;
-        I(s->box_balls, e) = 0;
-        I(s->box_kids, e) = 0;
-        I(s->box_bubble, e) = -1;
+        BX(s->box_level, e) = level;
+        BK(0, e) = kx;
+        BK(1, e) = ky;
+        BK(2, e) = kz;
+        BX(s->box_balls, e) = 0;
+        BX(s->box_kids, e) = 0;
+        BX(s->box_bubble, e) = -1;
         hash_insert(e);
         return e;
     }
@@ -267,9 +281,9 @@ struct World {
             const int sh = 2 * (level - L);
             const int64_t e = new_box(L, ix >> sh, iy >> sh, iz >> sh);
             if (e < 0) return -1;
-            I(s->box_parent, e) = parent;                  // (a box's parent and top box outlive it: kids > 0)
-            I(s->box_top, e) = parent >= 0 ? I(s->box_top, parent) : e;
-            if (parent >= 0) ++I(s->box_kids, parent);
+            BX(s->box_parent, e) = parent;                  // (a box's parent and top box outlive it: kids > 0)
+            BX(s->box_top, e) = parent >= 0 ? BX(s->box_top, parent) : e;
+            if (parent >= 0) ++BX(s->box_kids, parent);
             parent = e;
         }
         return parent;
@@ -281,15 +295,15 @@ struct World {
         const bool keep = one(s->free_boxes) < BOX_KEEP;
         int64_t cur = e;
         for (int guard = 0; guard < NUM_LEVELS && cur >= 0; ++guard) {
-            const int64_t parent = I(s->box_parent, cur);
-            if (parent >= 0) --I(s->box_kids, parent);
+            const int64_t parent = BX(s->box_parent, cur);
+            if (parent >= 0) --BX(s->box_kids, parent);
             hash_erase(cur);
-            I(s->box_level, cur) = -1;
+            BX(s->box_level, cur) = -1;
             I(s->box_free, one(s->box_free_n)++) = cur;
             for (int k = 0; k < 2; ++k)
                 if (watch[k] == cur) fate[k] = keep ? 1 : 2;
             if (keep) ++one(s->free_boxes);
-            if (parent >= 0 && I(s->box_kids, parent) == 0 && I(s->box_balls, parent) == 0)
+            if (parent >= 0 && BX(s->box_kids, parent) == 0 && BX(s->box_balls, parent) == 0)
                 cur = parent;
             else
                 cur = -1;
@@ -350,8 +364,8 @@ struct World {
     }
     EBB_HD void leave_box(int64_t e, const int64_t* watch, int* fate) {
         if (e < 0) return;
-        --I(s->box_balls, e);
-        if (I(s->box_balls, e) == 0 && I(s->box_kids, e) == 0) release(e, watch, fate);
+        --BX(s->box_balls, e);
+        if (BX(s->box_balls, e) == 0 && BX(s->box_kids, e) == 0) release(e, watch, fate);
     }
     // DeleteFromBoxes: the ball leaves each of its boxes in key order, each box released when left empty. The
     // entries come from the ball's record of them (key order: on each axis the lower key first, so the side box first
@@ -385,7 +399,7 @@ struct World {
         int fate[2] = {0, 0};
         delete_from_boxes(j, watch, fate);
     }
-    EBB_HD int64_t topmost_of(int64_t e) const { return I(s->box_top, e); }
+    EBB_HD int64_t topmost_of(int64_t e) const { return BX(s->box_top, e); }
     // a free ball's radius plus a tick at full thrust (Ball::GetInflatedRadius)
     EBB_HD double inflated_radius(int64_t j, const double* v) const {
         return inflated_radius_of(j, p->radius[row(j)], v);
@@ -429,27 +443,27 @@ struct World {
                 for (int k = -1; k <= 1; ++k) {
                     if (i == 0 && j == 0 && k == 0) continue;
                     const int64_t o = check_box(kx + i, ky + j, kz + k, 0);
-                    if (o >= 0 && I(s->box_bubble, o) != -1) return I(s->box_bubble, o);
+                    if (o >= 0 && BX(s->box_bubble, o) != -1) return BX(s->box_bubble, o);
                 }
         return -1;
     }
     // Traverse: the seed given to every top box reachable through neighbours without a bubble (a fill; the stack
     // holds each box once, marked as it is pushed)
     EBB_HD void traverse(int64_t top, int64_t seed) {
-        if (I(s->box_bubble, top) != -1) return;
-        I(s->box_bubble, top) = seed;
+        if (BX(s->box_bubble, top) != -1) return;
+        BX(s->box_bubble, top) = seed;
         int64_t sp = 0;
         I(s->stack, sp++) = top;
         while (sp > 0) {
             const int64_t e = I(s->stack, --sp);
-            const int64_t kx = I3(s->box_key, 0, e, B), ky = I3(s->box_key, 1, e, B), kz = I3(s->box_key, 2, e, B);
+            const int64_t kx = BK(0, e), ky = BK(1, e), kz = BK(2, e);
             for (int i = -1; i <= 1; ++i)
                 for (int j = -1; j <= 1; ++j)
                     for (int k = -1; k <= 1; ++k) {
                         if (i == 0 && j == 0 && k == 0) continue;
                         const int64_t o = check_box(kx + i, ky + j, kz + k, 0);
-                        if (o < 0 || I(s->box_bubble, o) != -1) continue;
-                        I(s->box_bubble, o) = seed;
+                        if (o < 0 || BX(s->box_bubble, o) != -1) continue;
+                        BX(s->box_bubble, o) = seed;
                         if (sp >= B) {
                             flag(F_BOXES);
                             return;
@@ -569,7 +583,7 @@ struct World {
     // ---- filing ----
     EBB_HD void insert_in_box(int64_t j, int64_t e) const {
         (void)j;
-        if (e >= 0) ++I(s->box_balls, e);
+        if (e >= 0) ++BX(s->box_balls, e);
     }
     // Ball::InsertInBoxes: the ball's box at the level of its inflated radius and the neighbours its sphere reaches
     // (every neighbour for a huge ball), unless box and sides are as they were; the top box takes the bubble
@@ -591,12 +605,12 @@ struct World {
         if (box1 < 0) return;
         for (int c = 0; c < 3; ++c) {
             mod(j, c) = m[c];
-            key(j, c) = I3(s->box_key, c, box1, B);
+            key(j, c) = BK(c, box1);
         }
         lvl(j) = level;
         insert_in_box(j, box1);
         const int64_t top = topmost_of(box1);
-        if (top >= 0) I(s->box_bubble, top) = new_bubble;
+        if (top >= 0) BX(s->box_bubble, top) = new_bubble;
         I(s->my_box, j) = box1;                            // (entries stay put while the ball is filed in them)
         I(s->my_top, j) = top;
         int64_t act = int64_t(1) << 13;
@@ -663,18 +677,18 @@ struct World {
         const int64_t box1 = same ? I(s->my_box, j) : get_box(k[0], k[1], k[2], level0);
         if (box1 < 0) return;
         int64_t key0[3];
-        for (int c = 0; c < 3; ++c) key0[c] = I3(s->box_key, c, box1, B);
+        for (int c = 0; c < 3; ++c) key0[c] = BK(c, box1);
         const int64_t top = same ? I(s->my_top, j) : topmost_of(box1);
-        int64_t new_bubble = I(s->box_bubble, top);
+        int64_t new_bubble = BX(s->box_bubble, top);
         int fate[2] = {0, 0};
         if (new_bubble == -1) {
-            const int64_t tk[3] = {I3(s->box_key, 0, top, B), I3(s->box_key, 1, top, B), I3(s->box_key, 2, top, B)};
+            const int64_t tk[3] = {BK(0, top), BK(1, top), BK(2, top)};
             const int64_t watch[2] = {box1, top};
             delete_from_boxes(j, watch, fate);             // may release box1 and its top: both are still read
             if (fate[1] == 2) flag(F_UNDEFINED);
             new_bubble = nearby_bubbles(tk[0], tk[1], tk[2]);
             if (new_bubble == -1) new_bubble = one(s->bubble_id)++;
-            if (fate[1] == 0) I(s->box_bubble, top) = new_bubble;   // (a released top's write is lost)
+            if (fate[1] == 0) BX(s->box_bubble, top) = new_bubble;   // (a released top's write is lost)
         }
         if (I(s->bubble, j) != new_bubble) {
             I(s->old_bubble, j) = I(s->bubble, j);
@@ -1199,7 +1213,7 @@ struct World {
         const int64_t r = row(j);
         const int64_t box0 = I(s->my_box, j), top = I(s->my_top, j);
         if (box0 < 0 || top < 0) return false;
-        const int64_t bub = I(s->box_bubble, top);
+        const int64_t bub = BX(s->box_bubble, top);
         if (bub == -1 || bub != I(s->bubble, j)) return false;
         // the filing it comes back to: its own (known for a fresh one, else made again and compared)
         const int L1 = (int)lvl(j);
@@ -1262,8 +1276,8 @@ struct World {
                 if (ent[i] == e) return i;
             if (ne == CAP) return -1;
             ent[ne] = e;
-            nb[ne] = I(s->box_balls, e);
-            nk[ne] = I(s->box_kids, e);
+            nb[ne] = BX(s->box_balls, e);
+            nk[ne] = BX(s->box_kids, e);
             gone[ne] = 0;
             return ne++;
         };
@@ -1278,8 +1292,8 @@ struct World {
             while (nb[i] == 0 && nk[i] == 0 && !gone[i]) {
                 gone[i] = 1;
                 ++a;
-                if (I(s->box_level, e) == 0 && e != top) return false;   // another top box emptied: its bubble lost
-                e = I(s->box_parent, e);
+                if (BX(s->box_level, e) == 0 && e != top) return false;   // another top box emptied: its bubble lost
+                e = BX(s->box_parent, e);
                 if (e < 0) break;
                 i = slot_of_entry(e);
                 if (i < 0) return false;
@@ -1299,7 +1313,7 @@ struct World {
             return -1;
         };
         int64_t ak = 0;
-        for (int64_t e = boxi; e >= 0; e = I(s->box_parent, e)) {
+        for (int64_t e = boxi; e >= 0; e = BX(s->box_parent, e)) {
             const int i = gone_at(e);
             if (i < 0 || !gone[i]) break;
             gone[i] = 2;
@@ -1307,7 +1321,7 @@ struct World {
         }
         if (ak > 0 && Li == L1) return false;             // (the ball's own box emptied, made again, emptied again)
         int64_t a1 = 0;
-        for (int64_t e = box0; e >= 0; e = I(s->box_parent, e)) {
+        for (int64_t e = box0; e >= 0; e = BX(s->box_parent, e)) {
             const int i = gone_at(e);
             if (i < 0 || !gone[i]) break;
             ++a1;
@@ -1770,7 +1784,7 @@ struct World {
         int64_t k[3];
         key_for(0, x, k);
         const int64_t e = check_box(k[0], k[1], k[2], 0);
-        return e < 0 ? -2 : I(s->box_bubble, e);
+        return e < 0 ? -2 : BX(s->box_bubble, e);
     }
     // GetBallIdsInRange (with distances): the balls listed in the bubble's dictionary, in its order (those that left
     // it included until CopyBubbles), within range + radius of the centre; the reference ball itself left out
@@ -1868,7 +1882,7 @@ struct World {
     EBB_HDNI void init_bubbles() {
         const int64_t n = one(s->box_n);
         for (int64_t e = 0; e < n; ++e)
-            if (I(s->box_level, e) == 0) I(s->box_bubble, e) = -1;
+            if (BX(s->box_level, e) == 0) BX(s->box_bubble, e) = -1;
         one(s->bubble_id) = 0;
         one(s->dict_n) = 0;
         one(s->entry_n) = 0;
@@ -1889,9 +1903,9 @@ struct World {
             }
             const int64_t top = I(s->my_top, j);
             if (top < 0) continue;
-            if (I(s->box_bubble, top) != -1) {
+            if (BX(s->box_bubble, top) != -1) {
                 I(s->old_bubble, j) = I(s->bubble, j);
-                I(s->bubble, j) = I(s->box_bubble, top);
+                I(s->bubble, j) = BX(s->box_bubble, top);
                 add_to_bubble(j);
                 continue;
             }
@@ -2019,7 +2033,7 @@ struct World {
         key_for(level0, x, k);
         for (int c = 0; c < 3; ++c)
             if (k[c] != key(j, c)) return false;
-        const int64_t bub = I(s->box_bubble, I(s->my_top, j));
+        const int64_t bub = BX(s->box_bubble, I(s->my_top, j));
         if (bub == -1 || bub != I(s->bubble, j)) return false;
         side_mods(level0, k, inflated, x, m);
         for (int c = 0; c < 3; ++c)

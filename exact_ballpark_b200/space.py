@@ -71,24 +71,47 @@ def state_spec(N: int, B: int, D: int, E: int, S: int, U: int, M: int) -> list:
             ("box_home", (B,), I64, 0), ("box_slot", (B,), I64, 0), ("fbox", (8, N), I64, -1)]
 
 
+# the box table's per-entry fields in a world-major arena: records of BOX_RECORD int64 words an entry (the word of
+# each field; box_key takes three)
+BOX_RECORD = 16
+BOX_WORDS = {"box_level": 0, "box_key": 1, "box_balls": 4, "box_kids": 5, "box_bubble": 6, "box_parent": 7,
+             "box_top": 8, "box_home": 9, "box_slot": 10}
+
+
 def allocate_state(spec, W: int, dev, world_major: bool):
     """The layer's arrays, each a tensor [*shape, W] (its entries, then the world). Interleaved: each its own
     contiguous tensor. World-major: views into one arena [W][pitch bytes], each array at its own offset a world (16-byte
-    aligned), the world's row of the arena holding its copy of every array. Returns (arrays, pitch; 0 interleaved)."""
+    aligned), the world's row of the arena holding its copy of every array, the box table's per-entry fields as
+    records of BOX_RECORD words an entry (one 128-byte line). Returns (arrays, pitch; 0 interleaved)."""
     if not world_major:
         return {name: torch.full((*shape, W), fill, dtype=dt, device=dev) for name, shape, dt, fill in spec}, 0
-    at, off = [], 0
+    at, off, rec, boxes = [], 0, None, None
     for name, shape, dt, fill in spec:
+        if name in BOX_WORDS:
+            at.append(None)
+            boxes = shape[-1]
+            continue
         size = math.prod(shape) * torch.empty((), dtype=dt).element_size()
         at.append(off)
         off += (size + 15) // 16 * 16
+    if boxes is not None:
+        rec = (off + 127) // 128 * 128
+        off = rec + boxes * BOX_RECORD * 8
     pitch = (off + 127) // 128 * 128
     arena = torch.zeros(W, pitch, dtype=U8, device=dev)
+    words = arena.view(torch.int64)                        # [W, pitch / 8]
     out = {}
     for (name, shape, dt, fill), o in zip(spec, at):
-        n = math.prod(shape)
-        size = n * torch.empty((), dtype=dt).element_size()
-        t = arena[:, o:o + size].view(dt).reshape(W, *shape).movedim(0, -1)
+        if o is None:                                      # a record field: its word of each entry's record
+            first = rec // 8 + BOX_WORDS[name]
+            if len(shape) == 1:
+                t = words.as_strided((shape[0], W), (BOX_RECORD, pitch // 8), first)
+            else:
+                t = words.as_strided((shape[0], shape[1], W), (1, BOX_RECORD, pitch // 8), first)
+        else:
+            n = math.prod(shape)
+            size = n * torch.empty((), dtype=dt).element_size()
+            t = arena[:, o:o + size].view(dt).reshape(W, *shape).movedim(0, -1)
         if fill:
             t.fill_(fill)
         out[name] = t

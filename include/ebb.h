@@ -165,12 +165,15 @@ typedef struct EbbServerQueue {
  * and every key [3][cap][W] (world w's entry e at e W + w), one thread a world; or, with `pitch` > 0, world-major:
  * each pointer names world 0's copy of its array, entries consecutive in the shapes below without their [W], and world
  * w's copy of every array starts w `pitch` bytes further on (`rnd` excepted: [W][EBB_RAND_WORDS] in both
- * arrangements). Capacities a world: `boxes` box-table
+ * arrangements); there the box table's per-entry fields (box_level, box_key's three, box_balls, box_kids,
+ * box_bubble, box_parent, box_top, box_home, box_slot) are records of EBB_SPACE_BOX_RECORD words an entry, at words
+ * 0, 1-3, 4, 5, 6, 7, 8, 9 and 10, each field's pointer naming it in world 0's entry 0. Capacities a world: `boxes` box-table
  * entries (and the same for the fill's stack), `dicts` bubble dictionaries, `entries` dictionary entries in insertion
  * order, `sets` members of the interactive sets and of the keep-alive sets. A world that leaves the layer's domain is
  * flagged (EBB_SPACE_FLAG_*) and left alone by later operations. Field for field the state the reference's layer keeps
  * in its `st` tensors (vec_space.py:808-830), with a box table in place of its top-box table. */
 #define EBB_SPACE_MAX_SLOTS 128
+#define EBB_SPACE_BOX_RECORD 16   /* words a box-table entry's record (world-major: one 128-byte line an entry) */
 enum {  /* the tape's operations, numbered as the reference's OPS (vec_space.py:159) */
     EBB_SPACE_NONE = 0, EBB_SPACE_ADD = 1, EBB_SPACE_REFILE = 2, EBB_SPACE_INIT_BUBBLES = 3,
     EBB_SPACE_COPY_BUBBLES = 4, EBB_SPACE_KEEP_ALIVE = 5, EBB_SPACE_SET_INTERACTIVE = 6, EBB_SPACE_ADD_SENSOR = 7,
