@@ -1016,19 +1016,35 @@ def partition_headline(args, dev, dist, rank: int, world_size: int, barrier, max
     same = all(torch.equal(getattr(park, "_" + k), v) for k, v in plain_state.items())
     same = same and torch.equal(part.event_counts(), plain_ev)
     del plain_state
-    # the dominant launches, eager, each timed alone: every layer's re-filings and HandleProximities
-    launch_ms = {}
-    for layer, _ in part.layers:
+    # one more tick, eager, each part timed alone (L2 flushed before each): the server's pre-tick, the dead-bubble
+    # tests, the park's tick, every layer's re-filings and HandleProximities (the dominant launches), the send flags
+    launch_ms, parts_ms = {}, {}
+    q, srv = r["q"], r["server"]
+
+    def timed_part(name, fn):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         flush.fill_(1)
         a.record(stream)
-        layer.after_evolve(None)
+        res = fn()
         b.record(stream)
         b.synchronize()
-        launch_ms[f"{layer.N}_slots_{'warp' if layer.lanes == 32 else 'thread'}"] = a.elapsed_time(b)
+        parts_ms[name] = a.elapsed_time(b)
+        return res
+    timed_part("server_pre_tick", lambda: srv._launch(q, 5))
+    dead = timed_part("dead_bubbles", part.dead_rows)
+    saved = park._moribund.clone()
+    park._moribund.logical_or_(dead)
+    timed_part("park_tick", r["park_tick"])
+    park._moribund.copy_(saved)
+    for layer, _ in part.layers:
+        layer.clear_events()
+        name = f"{layer.N}_slots_{'warp' if layer.lanes == 32 else 'thread'}"
+        timed_part(name, lambda: layer.after_evolve(None))
+        launch_ms[name] = parts_ms[name]
+    timed_part("server_flags", lambda: srv._launch(q, 3))
+    park.current_time += 1
     layer_ms = sum(launch_ms.values())
     # e2e: the pilots' arguments in, the events and send flags out
-    q, srv = r["q"], r["server"]
     sizes = torch.as_tensor(pw.sizes, device=dev)
     world = torch.repeat_interleave(torch.arange(W, device=dev), sizes)
     k_in = torch.arange(n, device=dev) - torch.repeat_interleave(torch.as_tensor(pw.starts, device=dev), sizes)
@@ -1075,7 +1091,7 @@ def partition_headline(args, dev, dist, rank: int, world_size: int, barrier, max
                                   for (l, b), t in tuning.items()},
             "note": "each size class's arrangement (a thread a world in 64- or 128-thread blocks, or a warp a world) "
                     "timed on the workload itself, eager, untimed in the headline; each class takes its fastest"},
-        "layer_launch_ms": launch_ms, "layer_share": layer_ms / (ms_ragged / K),
+        "layer_launch_ms": launch_ms, "layer_share": layer_ms / (ms_ragged / K), "eager_parts_ms": parts_ms,
         "roofline": {"bound": "hbm", "kernel": "the space layer's re-filings and HandleProximities (tape kernels, "
                                                 "a launch a size class)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
