@@ -946,6 +946,217 @@ def server_runs(args, dev) -> dict:
             **({} if args.no_cpu_baseline else {"cpu_baseline": server_cpu_sample(16384, 3, 100)})}
 
 
+def ref_sm100_runs(args, dev) -> dict:
+    """The Blackwell bar: the reference's own kernels, built for sm_100 by baseline/ref_sm100.py (the reference's
+    build with its flags, sm_100 SASS alone, its PTX read-back not made), driven through the reference's own public
+    API on this GPU beside this package's parks, on the same seeded workloads as the sections above: the flight park
+    (ModesGraph), the collision park (its kernel, eager: the reference has no graph for it), the combat and composed
+    parks (CombatGraph, ComposedGraph) and the server layer (ServerGraph). Per park: --warmup ticks, then
+    --ref-steps ticks, this package's tick and the reference's alternating, each timed alone with CUDA events with L2
+    flushed before it; after the same ticks both parks' states are compared bit for bit."""
+    import torch
+
+    sys.path.insert(0, str(ROOT / "baseline"))
+    import ref_sm100
+    why = ref_sm100.unavailable()
+    if why is not None:
+        return {"unavailable": why}
+    ref_sm100.install()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    K = args.ref_steps
+
+    def timed(step) -> float:
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    def bits(t):
+        t = torch.as_tensor(t).detach().contiguous()
+        as_int = {torch.float64: torch.int64, torch.float32: torch.int32}.get(t.dtype)
+        return t.view(as_int) if as_int is not None else t
+
+    def race(ships: int, mine, theirs, names, prep=None) -> dict:
+        """mine, theirs: (park, tick); prep(park, step) before each tick (step from 1)."""
+        (pm, tm), (pr, tr) = mine, theirs
+        ms_m = ms_r = 0.0
+        for step in range(1, args.warmup + K + 1):
+            if prep is not None:
+                prep(pm, step)
+                prep(pr, step)
+            if step <= args.warmup:
+                tm()
+                tr()
+            else:
+                ms_m += timed(tm)
+                ms_r += timed(tr)
+        torch.cuda.synchronize(dev)
+        diff = {}
+        for nm in names:
+            if not (hasattr(pm, nm) and hasattr(pr, nm)):
+                continue
+            a, b = bits(getattr(pm, nm)), bits(getattr(pr, nm))
+            diff[nm] = int((a != b).sum().item()) if a.shape == b.shape else f"{tuple(a.shape)} vs {tuple(b.shape)}"
+        ms_m, ms_r = ms_m / K, ms_r / K
+        return {"ships": ships, "ms_per_step": ms_m, "ref_sm100_ms_per_step": ms_r,
+                "ship_ticks_per_s": ships / (ms_m / 1e3), "ref_sm100_ship_ticks_per_s": ships / (ms_r / 1e3),
+                "speedup": ms_r / ms_m, "ticks_compared": args.warmup + K, "bit_differences": diff,
+                "bit_identical": all(v == 0 for v in diff.values())}
+
+    def flight():
+        from exact_ballpark import vec_modes as RM
+        from exact_ballpark import vec_modes_cuda as RMC
+
+        from exact_ballpark_b200 import ModesGraph, VecModesPark
+        from exact_ballpark_b200.autotune import autotune
+        from exact_ballpark_b200.workloads import flight_worlds
+        w = flight_worlds(1, args.worlds, args.ships)
+        n = len(w.rows)
+        pm, pr = (cls(n, device=dev, dynamical_orientation=True, use_new_orbit=True)
+                  for cls in (VecModesPark, RM.VecModesPark))
+        for p in (pm, pr):
+            p.load(w.rows)
+            w.apply(p)
+        autotune(pm)
+        out = race(n, (pm, ModesGraph(pm).tick), (pr, RMC.ModesGraph(pr).tick),
+                   ("pos", "vel", "rot", "ang_vel", "mode", "effect_stamp"))
+        out["workload"] = f"flight park: {args.worlds} worlds x {args.ships} ships, dynamical orientation, new orbit"
+        return out
+
+    def collide():
+        from exact_ballpark import vec_collide as RC
+
+        from exact_ballpark_b200.collide import CollideGraph, VecCollidePark
+        from exact_ballpark_b200.workloads import collide_worlds
+        W = args.collide_worlds
+        w = collide_worlds(21, W, ticks=args.warmup + K)
+        pm, pr = VecCollidePark(W, 16, device=dev), RC.VecCollidePark(W, 16, device=dev, kernel="cuda")
+        for p in (pm, pr):
+            p.load(w.worlds)
+        out = race(4 * W, (pm, CollideGraph(pm).tick), (pr, pr.evolve), ("pos", "vel"), prep=w.apply)
+        out["workload"] = f"collision park: {W} worlds x (4 ships + 4 free + 8 fixed spheres)"
+        return out
+
+    def combat(composed: bool):
+        from exact_ballpark import vec_combat as RB
+        from exact_ballpark import vec_combat_cuda as RBC
+        from exact_ballpark import vec_composed as RP
+        from exact_ballpark import vec_composed_cuda as RPC
+
+        from exact_ballpark_b200.combat import CombatGraph, VecCombatPark
+        from exact_ballpark_b200.composed import VecComposedPark
+        from exact_ballpark_b200.workloads import combat_worlds, composed_worlds
+        W = args.combat_worlds
+        w = composed_worlds(41, W) if composed else combat_worlds(31, W)
+        n = len(w.rows)
+        mine = (VecComposedPark if composed else VecCombatPark)(n, device=dev, dynamical_orientation=True,
+                                                                 use_new_orbit=True, block=256)
+        theirs = (RP.VecComposedPark if composed else RB.VecCombatPark)(n, device=dev, dynamical_orientation=True,
+                                                                         use_new_orbit=True)
+        for p in (mine, theirs):
+            p.load(w.rows)
+            w.apply(p)
+        graph = (RPC.ComposedGraph if composed else RBC.CombatGraph)(theirs)
+        out = race(w.ships * W, (mine, CombatGraph(mine).tick), (theirs, graph.tick),
+                   ("pos", "vel", "rot", "mode", "exists"))
+        out["workload"] = (f"{'composed' if composed else 'combat'} park: {W} worlds, "
+                           f"{w.ships} ships a world (missiles{' and spheres' if composed else ''} not counted)")
+        return out
+
+    def server_layer():
+        from exact_ballpark import vec_modes as RM
+        from exact_ballpark import vec_server as RS
+
+        from exact_ballpark_b200 import VecModesPark, server
+        W = args.server_worlds
+        rows = server_worlds(W)
+        n = len(rows)
+        sched = [k for _ in range(4) for k in ("GotoDirection", "SetSpeedFraction")]
+        graphs = []
+        for cls, mod in ((VecModesPark, server), (RM.VecModesPark, RS)):
+            park = cls(n, device=dev)
+            park.load(rows)
+            srv = mod.VecServer(mod.ModesAdapter(park), [x["id"] - 1 for x in rows], kernel="cuda")
+            srv.pre_tick()
+            srv.evolve()
+            srv.post_tick()
+            g = mod.ServerGraph(srv, sched)
+            for j, (kind, mask, ball, f) in enumerate(server_pushes(W, dev)):
+                g.inputs[j]["mask"].copy_(mask)
+                g.inputs[j]["ball"].copy_(ball)
+                g.inputs[j]["f"][:, :f.shape[1]].copy_(f)
+            graphs.append((park, g.tick))
+        out = race(n, graphs[0], graphs[1], ("pos", "vel", "bubble"))
+        out["workload"] = f"server layer over the flight park: {W} worlds x 4 pilots, 8 Actions calls a world a tick"
+        return out
+
+    def space_server():
+        from exact_ballpark import vec_modes as RM
+        from exact_ballpark import vec_server_space as RSS
+        from exact_ballpark import vec_server_space_cuda as RSC
+        from exact_ballpark import vec_space as RV
+
+        from exact_ballpark_b200.partition import partition_setup
+        from exact_ballpark_b200.workloads import face_worlds
+        W, N = args.ref_space_worlds, 4
+        fw = face_worlds(1, W)
+        n = fw.n
+        mine = partition_setup(fw, dev, ragged=True, server_on=True)
+        vec = ("pos", "vel")
+        rows = [{k: (v[i].tolist() if k in vec else v[i].item()) for k, v in fw.cols.items()} for i in range(n)]
+        park = RM.VecModesPark(n, device=dev)
+        park.load(rows)
+        del rows
+        srv = RSC.CudaSpaceServer(RSS.SpaceModesAdapter(park), (fw.cols["id"] - 1).tolist())
+        space = srv.space
+        code = torch.full((W, N), RV.OP["ADD_SENSOR"], dtype=torch.int64, device=dev)
+        f = torch.zeros(W, N, 4, dtype=torch.float64, device=dev)
+        f[..., 0] = torch.as_tensor(fw.sensor_range, device=dev).reshape(W, N)
+        f[..., 1] = 1.0
+        space.tape(code, torch.arange(N, device=dev).expand(W, N).contiguous(), torch.zeros_like(code), f)
+        srv.pre_tick()                                               # the first tick (its additions) eagerly
+        srv.evolve()
+        srv.post_tick()
+        g = RSC.SpaceServerGraph(srv, [k for _ in range(N) for k in ("GotoDirection", "SetSpeedFraction")])
+        direction = torch.as_tensor(fw.direction, device=dev).reshape(W, N, 3)
+        speed = torch.as_tensor(fw.speed, device=dev).reshape(W, N)
+        for k in range(N):
+            for j, v in ((2 * k, direction[:, k]), (2 * k + 1, speed[:, k:k + 1])):
+                g.inputs[j]["mask"].fill_(True)
+                g.inputs[j]["ball"].fill_(k + 1)
+                g.inputs[j]["f"][:, :v.shape[1]].copy_(v)
+        out = race(n, (mine["park"], mine["graph"].tick), (park, g.tick), ("pos", "vel", "mode"))
+        ours_ev, theirs_ev = mine["part"].event_counts().to(torch.int64), space.st["evn"].to(torch.int64)
+        out["event_counts_differ"] = int((ours_ev != theirs_ev).sum().item())
+        out["events_last_tick"] = {"ours": int(ours_ev.sum().item()), "reference": int(theirs_ev.sum().item())}
+        out["flagged_worlds_reference"] = int((space.st["flags"] != 0).sum().item())
+        out["workload"] = (f"the reference's space benchmark shape with its server (benchmarks/space_speed.py "
+                           f"build_server): {W} worlds x 4 piloted ships across a top box's face, a 5 km sensor on "
+                           "every ship, GotoDirection and SetSpeedFraction every ship every tick; this package's "
+                           "PartitionGraph against the reference's SpaceServerGraph (CudaSpaceServer)")
+        return out
+
+    out = {"library": "the reference's kernels, its build for sm_100 (baseline/ref_sm100.py)", "steps": K,
+           "warmup": args.warmup, "l2": "flushed before every timed tick",
+           "partition_worlds": "not run: the reference's partition layer takes at most 64 slots a world "
+                               "(vec_space.py:131), and its fixed box table flags BOXES on worlds whose ships spread "
+                               "over 1-5 blobs 1,000 km apart, so the headline's worlds of 1-128 ships are outside "
+                               "its domain; the space_server line is its own benchmark's shape"}
+    for name, fn in (("flight", flight), ("collide", collide), ("combat", lambda: combat(False)),
+                     ("composed", lambda: combat(True)), ("server", server_layer), ("space_server", space_server)):
+        try:
+            out[name] = fn()
+        except Exception as e:                                       # one park's failure is reported, not fatal
+            out[name] = {"error": f"{type(e).__name__}: {e}"[:400]}
+        torch.cuda.synchronize(dev)
+        torch.cuda.empty_cache()
+    return out
+
+
 # Algorithmic bytes of one ship's tick in the partition layer's re-filings and HandleProximities (the layer's
 # dominant launches): the ship's filing read and written (level, key, side, active neighbours, its box and top entries:
 # 10 x 8 B each way), its position, velocity and old position read (72), its bubble and seq (16), its row, id, mode
@@ -1284,12 +1495,17 @@ def main() -> None:
     ap.add_argument("--collide-steps", type=int, default=50)
     ap.add_argument("--no-combat", action="store_true")
     ap.add_argument("--only", choices=("ragged", "collide", "collide_statics", "combat", "composed", "serve", "server",
-                                       "space", "partition", "serve_configurations"),
+                                       "space", "partition", "serve_configurations", "ref_sm100"),
                     default=None, help="run one section alone on one GPU and print it (for profiling); the default "
                                        "run prints the headline line with every section")
     ap.add_argument("--combat-worlds", type=int, default=65536)
     ap.add_argument("--combat-steps", type=int, default=50)
     ap.add_argument("--no-server", action="store_true")
+    ap.add_argument("--no-ref-sm100", action="store_true",
+                    help="skip the reference's own kernels (built for sm_100) timed beside this package's")
+    ap.add_argument("--ref-steps", type=int, default=10, help="timed ticks a park of the ref_sm100 section")
+    ap.add_argument("--ref-space-worlds", type=int, default=65536,
+                    help="worlds of four ships of the ref_sm100 section's space-server line")
     ap.add_argument("--server-worlds", type=int, default=65536)
     ap.add_argument("--server-steps", type=int, default=100)
     ap.add_argument("--space-worlds", type=int, default=20000)
@@ -1334,7 +1550,8 @@ def main() -> None:
                "combat": lambda: combat_runs(args, dev), "composed": lambda: combat_runs(args, dev, composed=True),
                "serve": lambda: serve_runs(args, dev), "server": lambda: server_runs(args, dev),
                "serve_configurations": lambda: serve_configurations(dev),
-               "space": lambda: space_runs(args, dev), "partition": lambda: partition_runs(args, dev)}[args.only]
+               "space": lambda: space_runs(args, dev), "partition": lambda: partition_runs(args, dev),
+               "ref_sm100": lambda: ref_sm100_runs(args, dev)}[args.only]
         print(json.dumps({"metric": METRIC, "section": args.only, args.only: run()}), flush=True)
         return
     dist = None
@@ -1387,6 +1604,8 @@ def main() -> None:
         line["composed"] = combat_runs(args, dev, composed=True)
     if not args.no_server:
         line["server"] = server_runs(args, dev)
+    if not args.no_ref_sm100 and world_size == 1:
+        line["ref_sm100"] = ref_sm100_runs(args, dev)
     if not args.no_serve:
         line["serve"] = serve_runs(args, dev)
         line["serve"]["plain_ship_ticks_per_s"] = line["flight"]["plain"]["value"] / world_size

@@ -199,8 +199,8 @@ def partition_setup(pw, dev, ragged: bool, server_on: bool = True, warp_class: i
                     plan: dict | None = None) -> dict:
     """A flight park of the partition worlds with the partition layer (ragged size classes, or the plain 128-slot
     layout), every ship's sensor added, and the server layer on top (a pilot a ship, GotoDirection and
-    SetSpeedFraction queued for every ship every tick: a fixed schedule of 2 x 128 pushes, a world's pushes masked to
-    its ships). The first tick runs eagerly; returns the parts and the captured tick."""
+    SetSpeedFraction queued for every ship every tick: a fixed schedule of 2 pushes a slot of the largest world, a
+    world's pushes masked to its ships). The first tick runs eagerly; returns the parts and the captured tick."""
     from . import server
     from .modes import tick_plain, tick_tiled
     park = VecModesPark(pw.n, device=dev)
@@ -219,13 +219,14 @@ def partition_setup(pw, dev, ragged: bool, server_on: bool = True, warp_class: i
         part.tick(park_tick)
         park.current_time += 1
         srv.post_tick()
-        sched = [k for _ in range(128) for k in ("GotoDirection", "SetSpeedFraction")]
+        K = int(np.max(pw.sizes))                         # a world's most ships: the schedule's pilots
+        sched = [k for _ in range(K) for k in ("GotoDirection", "SetSpeedFraction")]
         q = srv._queue([server.CODE[k] for k in sched])
         sizes = torch.as_tensor(pw.sizes, device=dev)
         starts = torch.as_tensor(pw.starts, device=dev)
         direction = torch.as_tensor(pw.direction, device=dev)
         speed = torch.as_tensor(pw.speed, device=dev)
-        for k in range(128):
+        for k in range(K):
             on = sizes > k
             row = torch.where(on, starts + k, 0)
             for j, f in ((2 * k, direction[row]), (2 * k + 1, speed[row][:, None])):
