@@ -208,14 +208,24 @@ __device__ __forceinline__ void potential(const World& W, int b, int o, V me_pos
     ++acc.hits_n;
 }
 
+// A slot's filing as the candidate tests read it: the level, the key of the box holding the centre and the side
+// (-1, 0, +1) an axis; the tick stages every slot's in shared memory, the static walk reads the park's
+struct Filing {
+    int64_t level, key[3], mod[3];
+};
+__device__ __forceinline__ Filing filing_of(const EbbCollideState& s, int64_t i) {
+    return Filing{s.level[i], {s.key[3 * i], s.key[3 * i + 1], s.key[3 * i + 2]},
+                  {s.mod[3 * i], s.mod[3 * i + 1], s.mod[3 * i + 2]}};
+}
+
 // Whether a box of ball n is one of ball b's boxes, an ancestor of one or below one (vec_collide.py:809): per axis,
 // some option of the finer ball shifted to the coarser level equals some option of the coarser
-__device__ __forceinline__ bool related(const EbbCollideState& s, int64_t ib, int64_t in) {
-    const int64_t Lb = s.level[ib], Ln = s.level[in];
+__device__ __forceinline__ bool related(const Filing& fb, const Filing& fn) {
+    const int64_t Lb = fb.level, Ln = fn.level;
     const int64_t sh = 2 * (Lb > Ln ? Lb - Ln : Ln - Lb);
     const bool coarse = Ln <= Lb;
     for (int q = 0; q < 3; ++q) {
-        const int64_t kb = s.key[3 * ib + q], mb = s.mod[3 * ib + q], kn = s.key[3 * in + q], mn = s.mod[3 * in + q];
+        const int64_t kb = fb.key[q], mb = fb.mod[q], kn = fn.key[q], mn = fn.mod[q];
         const int64_t lo_b = kb + (mb < 0 ? mb : 0), hi_b = kb + (mb > 0 ? mb : 0);
         const int64_t lo_n = kn + (mn < 0 ? mn : 0), hi_n = kn + (mn > 0 ? mn : 0);
         const int64_t xl = (coarse ? lo_b : lo_n) >> sh, xh = (coarse ? hi_b : hi_n) >> sh;
@@ -228,13 +238,13 @@ __device__ __forceinline__ bool related(const EbbCollideState& s, int64_t ib, in
 // The position of ball n's first box in ball b's GetNearbyBalls walk, as a sort key (vec_collide.py:825): the index of
 // the first of b's boxes (by key) that n's box relates to, the part (0 an ancestor, 1 below, 2 the box itself) and
 // within it the ancestor's distance or the box's post-order code (path digits from b's level; 64 past n's level)
-__device__ __forceinline__ int64_t order_key(const EbbCollideState& s, int64_t ib, int64_t in) {
-    const int64_t Lb = s.level[ib], Ln = s.level[in];
+__device__ __forceinline__ int64_t order_key(const Filing& fb, const Filing& fn) {
+    const int64_t Lb = fb.level, Ln = fn.level;
     int64_t Kn[3], Mn[3], cb[3], lo_b[3], hi_b[3];
     for (int q = 0; q < 3; ++q) {
-        const int64_t kb = s.key[3 * ib + q], mb = s.mod[3 * ib + q];
-        Kn[q] = s.key[3 * in + q];
-        Mn[q] = s.mod[3 * in + q];
+        const int64_t kb = fb.key[q], mb = fb.mod[q];
+        Kn[q] = fn.key[q];
+        Mn[q] = fn.mod[q];
         cb[q] = 1 + (mb != 0);
         lo_b[q] = kb + (mb < 0 ? mb : 0);
         hi_b[q] = kb + (mb > 0 ? mb : 0);
@@ -679,6 +689,51 @@ __device__ __forceinline__ bool static_values(const EbbCollideState& s, int64_t 
 
 constexpr int MAX_SLOTS = EBB_COLLIDE_MAX_SLOTS;
 
+// A block's neighbourhoods in shared memory (T threads, whole worlds of N slots; built by the tick's second phase):
+// each slot's depth-0 end of the tick, start position (x, y, z planes), radius, id, filing and flags, then the
+// candidate table: column o of responder t's row at key[o * (T + 1) + t] (the walk key, or NO_CANDIDATE), so that a
+// responder's scan reads consecutive words across its warp and the candidates' writes fall in distinct banks; the
+// responder sorts its row in place, the slots beside it in slot[o * (T + 1) + t]
+constexpr int64_t NO_CANDIDATE = INT64_MAX;          // (above every walk key, NOT_A_CANDIDATE included)
+constexpr uint8_t F_EXISTS = 1, F_MASSIVE = 2, F_CLOAKED = 4, F_JUNK = 8, F_RESPONDER = 16;
+
+struct Hood {
+    V* ends;
+    double *px, *py, *pz, *rad;
+    int64_t *id, *level, *kx, *ky, *kz, *key;
+    int8_t* mod;                                       // [3][T]
+    uint8_t *flags, *slot;
+    int T, P;                                          // threads, and the candidate table's column pitch (T + 1)
+
+    __device__ __forceinline__ Hood(unsigned char* raw, int T_, int N) : T(T_), P(T_ + 1) {
+        ends = (V*)raw;
+        double* d = (double*)(ends + T);
+        px = d;
+        py = d + T;
+        pz = d + 2 * T;
+        rad = d + 3 * T;
+        int64_t* q = (int64_t*)(d + 4 * T);
+        id = q;
+        level = q + T;
+        kx = q + 2 * T;
+        ky = q + 3 * T;
+        kz = q + 4 * T;
+        key = q + 5 * T;
+        mod = (int8_t*)(key + (size_t)P * N);
+        flags = (uint8_t*)(mod + 3 * T);
+        slot = flags + T;
+    }
+    __device__ __forceinline__ V pos(int t) const { return V{px[t], py[t], pz[t]}; }
+    __device__ __forceinline__ Filing filing(int t) const {
+        return Filing{level[t], {kx[t], ky[t], kz[t]}, {mod[t], mod[T + t], mod[2 * T + t]}};
+    }
+};
+
+__host__ __forceinline__ size_t hood_bytes(int T, int N) {
+    const size_t P = (size_t)T + 1;
+    return (size_t)T * (sizeof(V) + 9 * 8) + P * N * 8 + (size_t)T * 4 + P * N;
+}
+
 // Threads a block (whole worlds of N slots each) and resident blocks a multiprocessor is asked to fit (the register
 // budget the compiler gets). 128 threads and 6 blocks (80 registers, 24 warps a multiprocessor) measured fastest on
 // B200 at 65,536 worlds of 16 slots: 0.37 ms a tick, against 0.77 ms for 256 threads at the compiler's own 228
@@ -693,9 +748,10 @@ constexpr int MAX_SLOTS = EBB_COLLIDE_MAX_SLOTS;
 __global__ void __launch_bounds__(EBB_COLLIDE_THREADS, EBB_COLLIDE_MIN_BLOCKS) tick_kernel(EbbCollideState s, const uint8_t* __restrict__ active,
                                                    int32_t* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    V* ends = (V*)smem_raw;
     const int N = (int)s.slots, wpb = blockDim.x / N;
-    const int lw = threadIdx.x / N, j = threadIdx.x - lw * N;
+    const Hood H(smem_raw, (int)blockDim.x, N);
+    V* ends = H.ends;
+    const int lw = threadIdx.x / N, j = threadIdx.x - lw * N, t = threadIdx.x, w0 = lw * N;
     const int64_t w = (int64_t)blockIdx.x * wpb + lw;
     const bool mine = lw < wpb && w < s.worlds && (active == nullptr || active[w] != 0);
     const int64_t base = w * N, i = base + j;
@@ -731,46 +787,89 @@ __global__ void __launch_bounds__(EBB_COLLIDE_THREADS, EBB_COLLIDE_MIN_BLOCKS) t
         s.imp_n[i] = 0;
     }
     __syncthreads();
-    // (2) every ball's end of the tick as depth 0 of Potential predicts it (a fixed ball with mass 1e34)
-    if (mine && s.exists[i]) {
-        V p = ldv(s.pos, i), v = ldv(s.vel, i);
-        const double m = s.free_[i] ? dmul(s.mass[i], s.agility[i]) : FIXED_MASS;
-        integrate(p, v, ldv(s.last_g, i), m, k, s.time_factor[i], dt, dt);
-        ends[threadIdx.x] = p;
+    // (2) every ball's end of the tick as depth 0 of Potential predicts it (a fixed ball with mass 1e34), and the
+    // slot's neighbourhood fields staged for the world's candidate tests
+    if (mine) {
+        uint8_t f = 0;
+        if (s.exists[i]) {
+            V p = ldv(s.pos, i), v = ldv(s.vel, i);
+            const V p0 = p;
+            const double m = s.free_[i] ? dmul(s.mass[i], s.agility[i]) : FIXED_MASS;
+            integrate(p, v, ldv(s.last_g, i), m, k, s.time_factor[i], dt, dt);
+            ends[t] = p;
+            H.px[t] = p0.x;
+            H.py[t] = p0.y;
+            H.pz[t] = p0.z;
+            H.rad[t] = s.radius[i];
+            H.id[t] = s.id[i];
+            const Filing fi = filing_of(s, i);
+            H.level[t] = fi.level;
+            H.kx[t] = fi.key[0];
+            H.ky[t] = fi.key[1];
+            H.kz[t] = fi.key[2];
+            for (int q = 0; q < 3; ++q) H.mod[q * H.T + t] = (int8_t)fi.mod[q];
+            const bool massive = s.massive[i] != 0;
+            f = F_EXISTS | (massive ? F_MASSIVE : 0) | (s.cloaked[i] ? F_CLOAKED : 0) | (s.junk[i] ? F_JUNK : 0) |
+                (live && massive ? F_RESPONDER : 0);
+        }
+        H.flags[t] = f;
     }
     __syncthreads();
-    // (3) the gradient: each free massive ball against its candidates in GetNearbyBalls' order
-    if (live && s.massive[i]) {
-        const World W{&s, base, ends + lw * N};
-        const double cr0 = s.radius[i];
-        const V pb = ldv(s.pos, i), eb = W.ends[j];
-        int64_t okey[MAX_SLOTS];
-        int8_t oslot[MAX_SLOTS];
+    // (3a) the candidate tests spread over the world's threads: this slot as a candidate of each responder b (a free
+    // massive ball), its walk key written into b's row
+    if (mine) {
+        const uint8_t fo = H.flags[t];
+        const bool can = (fo & (F_EXISTS | F_MASSIVE | F_CLOAKED)) == (F_EXISTS | F_MASSIVE);
+        const V po = H.pos(t), eo = ends[t];
+        const Filing fo_ = H.filing(t);
+        const double ro = H.rad[t];
+        for (int b = 0; b < N; ++b) {
+            const int tb = w0 + b;
+            const uint8_t fb = H.flags[tb];
+            if (!(fb & F_RESPONDER)) continue;
+            int64_t key = NO_CANDIDATE;
+            if (can && b != j && !((fo & F_JUNK) && !(fb & F_JUNK))) {
+                const Filing fb_ = H.filing(tb);
+                if (related(fb_, fo_) &&
+                    collide_two_spheres(H.pos(tb), ends[tb], po, eo, dadd(H.rad[tb], ro)) != -1.0)
+                    key = order_key(fb_, fo_);
+            }
+            H.key[(size_t)j * H.P + tb] = key;
+        }
+    }
+    __syncthreads();
+    // (3b) the gradient: each free massive ball against its candidates in GetNearbyBalls' order (its row sorted in
+    // place by walk key, then id, as the candidates arrive in slot order)
+    if (live && (H.flags[t] & F_RESPONDER)) {
+        const World W{&s, base, ends + w0};
+        const V pb = H.pos(t);
         int nact = 0;
         for (int o = 0; o < N; ++o) {
-            const int64_t io = base + o;
-            if (o == j || !s.exists[io] || !s.massive[io] || s.cloaked[io]) continue;
-            if (s.junk[io] && !s.junk[i]) continue;
-            if (!related(s, i, io)) continue;
-            if (collide_two_spheres(pb, eb, ldv(s.pos, io), W.ends[o], dadd(cr0, s.radius[io])) == -1.0) continue;
-            const int64_t key = order_key(s, i, io), id = s.id[io];
+            const int64_t key = H.key[(size_t)o * H.P + t];
+            if (key == NO_CANDIDATE) continue;
+            const int64_t id = H.id[w0 + o];
             int at = nact++;                                          // insertion by (key, id)
-            while (at > 0 && (okey[at - 1] > key || (okey[at - 1] == key && s.id[base + oslot[at - 1]] > id))) {
-                okey[at] = okey[at - 1];
-                oslot[at] = oslot[at - 1];
+            while (at > 0) {
+                const int64_t kp = H.key[(size_t)(at - 1) * H.P + t];
+                const int sp = H.slot[(size_t)(at - 1) * H.P + t];
+                if (!(kp > key || (kp == key && H.id[w0 + sp] > id))) break;
+                H.key[(size_t)at * H.P + t] = kp;
+                H.slot[(size_t)at * H.P + t] = (uint8_t)sp;
                 --at;
             }
-            okey[at] = key;
-            oslot[at] = (int8_t)o;
+            H.key[(size_t)at * H.P + t] = key;
+            H.slot[(size_t)at * H.P + t] = (uint8_t)o;
         }
         Acc acc{V{0.0, 0.0, 0.0}, -1.0, 0, 0};
         for (int q = 0; q < nact; ++q) {
-            const int o = oslot[q];
-            potential<0>(W, j, o, pb, ldv(s.pos, base + o), acc);
+            const int o = H.slot[(size_t)q * H.P + t];
+            potential<0>(W, j, o, pb, H.pos(w0 + o), acc);
         }
         if (s.statics > 0) {                                          // then the static collidables (COL-712)
             V pe = pb, ve = ldv(s.vel, i);
             integrate(pe, ve, ldv(s.last_g, i), dmul(s.mass[i], s.agility[i]), k, s.time_factor[i], dt, dt);
+            int64_t okey[MAX_SLOTS];
+            int8_t oslot[MAX_SLOTS];
             int nst = 0;                                                  // the reacting ones in the walk's order:
             for (int q = 0; q < s.statics && q < MAX_SLOTS; ++q) {        // first box, parent id, id, slot
                 const int64_t at = w * s.statics + q;
@@ -862,7 +961,12 @@ int ebb_collide_tick(const EbbCollideState* s, const uint8_t* active, int32_t* s
     if (s->worlds == 0) return 0;
     const int N = (int)s->slots, wpb = EBB_COLLIDE_THREADS / N > 0 ? EBB_COLLIDE_THREADS / N : 1, threads = wpb * N;
     const unsigned grid = (unsigned)((s->worlds + wpb - 1) / wpb);
-    const size_t smem = (size_t)threads * sizeof(ebb::collide::V);
+    const size_t smem = ebb::collide::hood_bytes(threads, N);    // 30 KB at 16 slots, 87 KB at 64
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(ebb::collide::tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
     ebb::collide::tick_kernel<<<grid, threads, smem, (cudaStream_t)stream>>>(*s, active, status);
     return launched();
 }

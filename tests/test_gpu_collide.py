@@ -4,7 +4,7 @@
   static_cases scenarios with capsules and oriented boxes, seeds 1 and 2, and the collision benchmark's worlds): every
   field's digest after every tick, bit for bit;
 - against the CPU oracle beyond the fixtures (the benchmark's worlds at other seeds, 1024 worlds, 150 ticks with the
-  ships re-aimed): every field after every 25th tick;
+  ships re-aimed): every field after every 25th tick; and on crowded worlds of 48 and 64 slots;
 - a CUDA graph's replays against eager ticks, and inactive worlds (evolve(active)) keeping their state.
 """
 
@@ -67,6 +67,29 @@ def test_the_gpu_collision_tick_matches_the_oracle(seed):
         p.evolve()
         if step % 25 == 0 or step < 3:
             _compare(o, p, f"tick {step}")
+    assert int(np.asarray(o.hits_n).sum()) > 0
+
+
+@pytest.mark.parametrize("ships,spheres,fixed", [(8, 16, 24), (8, 24, 32)])
+def test_the_gpu_collision_tick_matches_the_oracle_on_crowded_worlds(ships, spheres, fixed):
+    """Worlds of 48 and 64 slots (the largest the park takes): blocks of 96 and 128 threads whose staged
+    neighbourhoods and candidate tables take more than 48 KB of shared memory."""
+    from exact_ballpark_b200 import VecCollidePark
+    from exact_ballpark_b200.workloads import collide_worlds
+    from oracle.collide_park import OracleCollidePark
+    n = ships + spheres + fixed
+    w = collide_worlds(11 + n, 256, ships=ships, spheres=spheres, statics=fixed, ticks=60, reaim=20)
+    o = OracleCollidePark(256, n)
+    p = VecCollidePark(256, n)
+    o.load(w.worlds)
+    p.load(w.worlds)
+    for step in range(1, 61):
+        w.apply(o, step)
+        w.apply(p, step)
+        o.evolve(threads=8)
+        p.evolve()
+        if step % 20 == 0 or step < 3:
+            _compare(o, p, f"{n} slots, tick {step}")
     assert int(np.asarray(o.hits_n).sum()) > 0
 
 
