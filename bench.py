@@ -1100,12 +1100,13 @@ def ref_sm100_runs(args, dev) -> dict:
         from exact_ballpark import vec_server_space_cuda as RSC
         from exact_ballpark import vec_space as RV
 
-        from exact_ballpark_b200.partition import partition_setup
+        from exact_ballpark_b200.partition import partition_setup, tune_partition
         from exact_ballpark_b200.workloads import face_worlds
         W, N = args.ref_space_worlds, 4
         fw = face_worlds(1, W)
         n = fw.n
-        mine = partition_setup(fw, dev, ragged=True, server_on=True)
+        plan, tuning = tune_partition(fw, dev)                        # as the headline: measured on the workload
+        mine = partition_setup(fw, dev, ragged=True, server_on=True, plan=plan)
         vec = ("pos", "vel")
         rows = [{k: (v[i].tolist() if k in vec else v[i].item()) for k, v in fw.cols.items()} for i in range(n)]
         park = RM.VecModesPark(n, device=dev)
@@ -1129,7 +1130,12 @@ def ref_sm100_runs(args, dev) -> dict:
                 g.inputs[j]["mask"].fill_(True)
                 g.inputs[j]["ball"].fill_(k + 1)
                 g.inputs[j]["f"][:, :v.shape[1]].copy_(v)
-        out = race(n, (mine["park"], mine["graph"].tick), (park, g.tick), ("pos", "vel", "mode"))
+        # the reference's event list grows until its consumer clears it (vec_space.py: clear_events); cleared before
+        # each of its ticks here, outside the timed region, so that both counts are the last tick's events
+        out = race(n, (mine["park"], mine["graph"].tick), (park, g.tick), ("pos", "vel", "mode"),
+                   prep=lambda p, step: space.clear_events() if p is park else None)
+        out["plan"] = {str(k): list(v) for k, v in plan.items()}
+        out["tuning_ms"] = {str(k): v for k, v in tuning.items()}
         ours_ev, theirs_ev = mine["part"].event_counts().to(torch.int64), space.st["evn"].to(torch.int64)
         out["event_counts_differ"] = int((ours_ev != theirs_ev).sum().item())
         out["events_last_tick"] = {"ours": int(ours_ev.sum().item()), "reference": int(theirs_ev.sum().item())}

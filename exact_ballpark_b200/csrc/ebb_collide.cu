@@ -691,9 +691,10 @@ constexpr int MAX_SLOTS = EBB_COLLIDE_MAX_SLOTS;
 
 // A block's neighbourhoods in shared memory (T threads, whole worlds of N slots; built by the tick's second phase):
 // each slot's depth-0 end of the tick, start position (x, y, z planes), radius, id, filing and flags, then the
-// candidate table: column o of responder t's row at key[o * (T + 1) + t] (the walk key, or NO_CANDIDATE), so that a
-// responder's scan reads consecutive words across its warp and the candidates' writes fall in distinct banks; the
-// responder sorts its row in place, the slots beside it in slot[o * (T + 1) + t]
+// candidate table of R rows (R = N, or the static collidables' count where that is larger): column o of responder t's
+// row at key[o * (T + 1) + t] (the walk key, or NO_CANDIDATE), so that a responder's scan reads consecutive words
+// across its warp and the candidates' writes fall in distinct banks; the responder sorts its row in place, the slots
+// beside it in slot[o * (T + 1) + t], then reuses the row to order its reacting static collidables
 constexpr int64_t NO_CANDIDATE = INT64_MAX;          // (above every walk key, NOT_A_CANDIDATE included)
 constexpr uint8_t F_EXISTS = 1, F_MASSIVE = 2, F_CLOAKED = 4, F_JUNK = 8, F_RESPONDER = 16;
 
@@ -705,7 +706,7 @@ struct Hood {
     uint8_t *flags, *slot;
     int T, P;                                          // threads, and the candidate table's column pitch (T + 1)
 
-    __device__ __forceinline__ Hood(unsigned char* raw, int T_, int N) : T(T_), P(T_ + 1) {
+    __device__ __forceinline__ Hood(unsigned char* raw, int T_, int R) : T(T_), P(T_ + 1) {
         ends = (V*)raw;
         double* d = (double*)(ends + T);
         px = d;
@@ -719,7 +720,7 @@ struct Hood {
         ky = q + 3 * T;
         kz = q + 4 * T;
         key = q + 5 * T;
-        mod = (int8_t*)(key + (size_t)P * N);
+        mod = (int8_t*)(key + (size_t)P * R);
         flags = (uint8_t*)(mod + 3 * T);
         slot = flags + T;
     }
@@ -729,9 +730,12 @@ struct Hood {
     }
 };
 
-__host__ __forceinline__ size_t hood_bytes(int T, int N) {
+__host__ __device__ __forceinline__ int hood_rows(int N, int64_t statics) {
+    return statics > N ? (int)(statics < MAX_SLOTS ? statics : MAX_SLOTS) : N;
+}
+__host__ __forceinline__ size_t hood_bytes(int T, int R) {
     const size_t P = (size_t)T + 1;
-    return (size_t)T * (sizeof(V) + 9 * 8) + P * N * 8 + (size_t)T * 4 + P * N;
+    return (size_t)T * (sizeof(V) + 9 * 8) + P * R * 8 + (size_t)T * 4 + P * R;
 }
 
 // Threads a block (whole worlds of N slots each) and resident blocks a multiprocessor is asked to fit (the register
@@ -749,7 +753,7 @@ __global__ void __launch_bounds__(EBB_COLLIDE_THREADS, EBB_COLLIDE_MIN_BLOCKS) t
                                                    int32_t* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N = (int)s.slots, wpb = blockDim.x / N;
-    const Hood H(smem_raw, (int)blockDim.x, N);
+    const Hood H(smem_raw, (int)blockDim.x, hood_rows(N, s.statics));
     V* ends = H.ends;
     const int lw = threadIdx.x / N, j = threadIdx.x - lw * N, t = threadIdx.x, w0 = lw * N;
     const int64_t w = (int64_t)blockIdx.x * wpb + lw;
@@ -781,10 +785,27 @@ __global__ void __launch_bounds__(EBB_COLLIDE_THREADS, EBB_COLLIDE_MIN_BLOCKS) t
             s.vel[3 * i + 1] = dmul(dsub(vy, dmul(0.07, vy)), STOP_DAMP);
         }
         stv(s.last_c, i, V{0.0, 0.0, 0.0});
-        for (int64_t q = 0; q < s.hit_cap; ++q) s.hits[i * s.hit_cap + q] = -1;
         s.hits_n[i] = 0;
-        for (int64_t q = 0; q < s.impact_cap; ++q) s.imp_slot[i * s.impact_cap + q] = -1;
         s.imp_n[i] = 0;
+    }
+    {   // the live balls' collision lists and impact slots cleared by their warp, a run of consecutive live slots
+        // (contiguous rows) at a time: consecutive lanes write consecutive entries (a thread clearing its own row
+        // strides the warp's stores a row apart)
+        const int warp0 = t & ~31, lane = t & 31, nl = min(32, (int)blockDim.x - warp0);
+        const unsigned lanes = nl == 32 ? 0xffffffffu : (1u << nl) - 1u;
+        unsigned todo = __ballot_sync(lanes, live);
+        const int64_t first = (int64_t)blockIdx.x * blockDim.x + warp0;      // the warp's first slot in the park
+        const int hc = (int)s.hit_cap, ic = (int)s.impact_cap;
+        while (todo != 0) {
+            const int b = __ffs(todo) - 1;
+            const unsigned gaps = ~(todo >> b);                          // the run's end: the first clear bit from b
+            const int len = gaps == 0u ? 32 - b : __ffs(gaps) - 1;
+            todo &= ~((len == 32 ? 0xffffffffu : (1u << len) - 1u) << b);
+            int64_t* h = s.hits + (first + b) * hc;
+            for (int q = lane; q < len * hc; q += nl) h[q] = -1;
+            int64_t* m = s.imp_slot + (first + b) * ic;
+            for (int q = lane; q < len * ic; q += nl) m[q] = -1;
+        }
     }
     __syncthreads();
     // (2) every ball's end of the tick as depth 0 of Potential predicts it (a fixed ball with mass 1e34), and the
@@ -868,8 +889,8 @@ __global__ void __launch_bounds__(EBB_COLLIDE_THREADS, EBB_COLLIDE_MIN_BLOCKS) t
         if (s.statics > 0) {                                          // then the static collidables (COL-712)
             V pe = pb, ve = ldv(s.vel, i);
             integrate(pe, ve, ldv(s.last_g, i), dmul(s.mass[i], s.agility[i]), k, s.time_factor[i], dt, dt);
-            int64_t okey[MAX_SLOTS];
-            int8_t oslot[MAX_SLOTS];
+            int64_t* okey = H.key + t;                                    // the row again, a stride P apart
+            uint8_t* oslot = H.slot + t;
             int nst = 0;                                                  // the reacting ones in the walk's order:
             for (int q = 0; q < s.statics && q < MAX_SLOTS; ++q) {        // first box, parent id, id, slot
                 const int64_t at = w * s.statics + q;
@@ -882,20 +903,22 @@ __global__ void __launch_bounds__(EBB_COLLIDE_THREADS, EBB_COLLIDE_MIN_BLOCKS) t
                 if (!static_values(s, i, pe, ve, s.s_geo + at * G_SIZE, ints[I_KIND], &toi, &lc)) continue;
                 int pos = nst++;
                 while (pos > 0) {
-                    const int64_t* pi = s.s_int + (w * s.statics + oslot[pos - 1]) * I_SIZE;
-                    const bool after = okey[pos - 1] > key ||
-                                       (okey[pos - 1] == key && (pi[I_PARENT] > ints[I_PARENT] ||
+                    const int64_t kp = okey[(size_t)(pos - 1) * H.P];
+                    const int sp = oslot[(size_t)(pos - 1) * H.P];
+                    const int64_t* pi = s.s_int + (w * s.statics + sp) * I_SIZE;
+                    const bool after = kp > key ||
+                                       (kp == key && (pi[I_PARENT] > ints[I_PARENT] ||
                                                                  (pi[I_PARENT] == ints[I_PARENT] && pi[I_ID] > ints[I_ID])));
                     if (!after) break;
-                    okey[pos] = okey[pos - 1];
-                    oslot[pos] = oslot[pos - 1];
+                    okey[(size_t)pos * H.P] = kp;
+                    oslot[(size_t)pos * H.P] = (uint8_t)sp;
                     --pos;
                 }
-                okey[pos] = key;
-                oslot[pos] = (int8_t)q;
+                okey[(size_t)pos * H.P] = key;
+                oslot[(size_t)pos * H.P] = (uint8_t)q;
             }
             for (int q = 0; q < nst; ++q) {
-                const int64_t at = w * s.statics + oslot[q];
+                const int64_t at = w * s.statics + oslot[(size_t)q * H.P];
                 const int64_t* ints = s.s_int + at * I_SIZE;
                 double toi;
                 V lc;
@@ -961,7 +984,7 @@ int ebb_collide_tick(const EbbCollideState* s, const uint8_t* active, int32_t* s
     if (s->worlds == 0) return 0;
     const int N = (int)s->slots, wpb = EBB_COLLIDE_THREADS / N > 0 ? EBB_COLLIDE_THREADS / N : 1, threads = wpb * N;
     const unsigned grid = (unsigned)((s->worlds + wpb - 1) / wpb);
-    const size_t smem = ebb::collide::hood_bytes(threads, N);    // 30 KB at 16 slots, 87 KB at 64
+    const size_t smem = ebb::collide::hood_bytes(threads, ebb::collide::hood_rows(N, s->statics));  // 30 KB at 16 slots
     if (smem > 48 * 1024) {
         const cudaError_t e = cudaFuncSetAttribute(ebb::collide::tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    (int)smem);

@@ -524,7 +524,7 @@ def face_worlds(seed: int, worlds: int) -> PartitionWorlds:
     """The reference's space benchmark shape (benchmarks/space_speed.py:31-56): worlds of four ships within 4 km
     (each axis uniform in +-4 km) of a point on the face between two top boxes (x at one top box's width, y and z at
     +-0.3 of it), the first ship moved half a box deeper into the first top so that its bubble comes first; mass 1e7
-    kg, radius 50 m, maximum velocity 300 m/s, agility 0.5, at rest, free, interactive, not massive; a 5 km proximity
+    kg, radius 50 m, maximum velocity 300 m/s, agility 0.5, at rest (STOP), free, interactive, not massive; a 5 km proximity
     sensor on every ship (period 1 s); GotoDirection along (1, 0.2, 0.1) for the odd ships and (-1, -0.1, 0.2) for
     the even ones, so every ship re-files every tick and crosses the face. Ids 1-4 in each world (the reference's
     101-104: the order is the same). The offsets come from this module's seeded generator, not the reference's."""
@@ -539,7 +539,7 @@ def face_worlds(seed: int, worlds: int) -> PartitionWorlds:
             "mass": np.full(n, 1e7), "radius": np.full(n, 50.0), "max_vel": np.full(n, 300.0),
             "agility": np.full(n, 0.5), "speed_fraction": np.ones(n), "free": np.ones(n, bool),
             "massive": np.zeros(n, bool), "interactive": np.ones(n, bool), "moribund": np.zeros(n, bool),
-            "cloaked": np.zeros(n, np.int64), "bubble": np.full(n, -1, np.int64), "pos": pos,
-            "vel": np.zeros((n, 3))}
+            "cloaked": np.zeros(n, np.int64), "bubble": np.full(n, -1, np.int64), "mode": np.full(n, 2, np.int64),
+            "max_ang_vel": np.ones(n), "rot_agility": np.full(n, 0.9), "pos": pos, "vel": np.zeros((n, 3))}
     d = np.where((k % 2 == 1)[:, None], np.array([1.0, 0.2, 0.1]), np.array([-1.0, -0.1, 0.2]))
     return PartitionWorlds(cols, np.full(worlds, 4, np.int64), np.full(n, 5000.0), d, np.ones(n))
