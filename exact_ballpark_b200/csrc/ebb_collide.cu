@@ -687,28 +687,27 @@ __device__ __forceinline__ bool static_values(const EbbCollideState& s, int64_t 
     return true;
 }
 
-constexpr int MAX_SLOTS = EBB_COLLIDE_MAX_SLOTS;
-
 // A block's neighbourhoods in shared memory (T threads, whole worlds of N slots; built by the tick's second phase):
-// each slot's depth-0 end of the tick, start position (x, y, z planes), radius, id, filing and flags, then the
-// candidate table of R rows (R = N, or the static collidables' count where that is larger): column o of responder t's
-// row at key[o * (T + 1) + t] (the walk key, or NO_CANDIDATE), so that a responder's scan reads consecutive words
-// across its warp and the candidates' writes fall in distinct banks; the responder sorts its row in place, the slots
-// beside it in slot[o * (T + 1) + t], then reuses the row to order its reacting static collidables
+// each slot's depth-0 end of the tick (position and velocity), start position (x, y, z planes), radius, id, filing and
+// flags, then two candidate tables, the balls' (N rows) and the static collidables' (S rows, S = the park's static
+// slots): column o of responder t's row at key[o * (T + 1) + t] (the walk key, or NO_CANDIDATE), so that a
+// responder's scan reads consecutive words across its warp and the candidates' writes fall in distinct banks; the
+// responder sorts its row in place, the slots beside it in slot[o * (T + 1) + t]
 constexpr int64_t NO_CANDIDATE = INT64_MAX;          // (above every walk key, NOT_A_CANDIDATE included)
 constexpr uint8_t F_EXISTS = 1, F_MASSIVE = 2, F_CLOAKED = 4, F_JUNK = 8, F_RESPONDER = 16;
 
 struct Hood {
-    V* ends;
+    V *ends, *vend;
     double *px, *py, *pz, *rad;
-    int64_t *id, *level, *kx, *ky, *kz, *key;
+    int64_t *id, *level, *kx, *ky, *kz, *key, *skey;
     int8_t* mod;                                       // [3][T]
-    uint8_t *flags, *slot;
-    int T, P;                                          // threads, and the candidate table's column pitch (T + 1)
+    uint8_t *flags, *slot, *sslot;
+    int T, P;                                          // threads, and the candidate tables' column pitch (T + 1)
 
-    __device__ __forceinline__ Hood(unsigned char* raw, int T_, int R) : T(T_), P(T_ + 1) {
+    __device__ __forceinline__ Hood(unsigned char* raw, int T_, int N, int S) : T(T_), P(T_ + 1) {
         ends = (V*)raw;
-        double* d = (double*)(ends + T);
+        vend = ends + T;
+        double* d = (double*)(vend + T);
         px = d;
         py = d + T;
         pz = d + 2 * T;
@@ -720,9 +719,11 @@ struct Hood {
         ky = q + 3 * T;
         kz = q + 4 * T;
         key = q + 5 * T;
-        mod = (int8_t*)(key + (size_t)P * R);
+        skey = key + (size_t)P * N;
+        mod = (int8_t*)(skey + (size_t)P * S);
         flags = (uint8_t*)(mod + 3 * T);
         slot = flags + T;
+        sslot = slot + (size_t)P * N;
     }
     __device__ __forceinline__ V pos(int t) const { return V{px[t], py[t], pz[t]}; }
     __device__ __forceinline__ Filing filing(int t) const {
@@ -730,12 +731,9 @@ struct Hood {
     }
 };
 
-__host__ __device__ __forceinline__ int hood_rows(int N, int64_t statics) {
-    return statics > N ? (int)(statics < MAX_SLOTS ? statics : MAX_SLOTS) : N;
-}
-__host__ __forceinline__ size_t hood_bytes(int T, int R) {
+__host__ __forceinline__ size_t hood_bytes(int T, int N, int S) {
     const size_t P = (size_t)T + 1;
-    return (size_t)T * (sizeof(V) + 9 * 8) + P * R * 8 + (size_t)T * 4 + P * R;
+    return (size_t)T * (2 * sizeof(V) + 9 * 8) + P * (N + S) * 8 + (size_t)T * 4 + P * (N + S);
 }
 
 // Threads a block (whole worlds of N slots each) and resident blocks a multiprocessor is asked to fit (the register
@@ -749,11 +747,14 @@ __host__ __forceinline__ size_t hood_bytes(int T, int R) {
 #define EBB_COLLIDE_MIN_BLOCKS 6
 #endif
 
+// STATICS: the park has static collidables (the balls-only tick is compiled without their steps)
+template <bool STATICS>
 __global__ void __launch_bounds__(EBB_COLLIDE_THREADS, EBB_COLLIDE_MIN_BLOCKS) tick_kernel(EbbCollideState s, const uint8_t* __restrict__ active,
                                                    int32_t* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N = (int)s.slots, wpb = blockDim.x / N;
-    const Hood H(smem_raw, (int)blockDim.x, hood_rows(N, s.statics));
+    const int S = STATICS ? (int)s.statics : 0;                      // (at most EBB_COLLIDE_MAX_STATICS)
+    const Hood H(smem_raw, (int)blockDim.x, N, S);
     V* ends = H.ends;
     const int lw = threadIdx.x / N, j = threadIdx.x - lw * N, t = threadIdx.x, w0 = lw * N;
     const int64_t w = (int64_t)blockIdx.x * wpb + lw;
@@ -818,6 +819,7 @@ __global__ void __launch_bounds__(EBB_COLLIDE_THREADS, EBB_COLLIDE_MIN_BLOCKS) t
             const double m = s.free_[i] ? dmul(s.mass[i], s.agility[i]) : FIXED_MASS;
             integrate(p, v, ldv(s.last_g, i), m, k, s.time_factor[i], dt, dt);
             ends[t] = p;
+            H.vend[t] = v;
             H.px[t] = p0.x;
             H.py[t] = p0.y;
             H.pz[t] = p0.z;
@@ -857,6 +859,27 @@ __global__ void __launch_bounds__(EBB_COLLIDE_THREADS, EBB_COLLIDE_MIN_BLOCKS) t
             }
             H.key[(size_t)j * H.P + tb] = key;
         }
+        // and the world's static collidables, static q by thread q mod N: each one's walk key (its first box) for
+        // every responder it reacts with (CollideWithBall from the responder's depth-0 end of the tick)
+        for (int q = j; STATICS && q < S; q += N) {
+            const int64_t at = w * S + q;
+            const bool ex = s.s_exists[at] != 0;
+            const int64_t* ints = s.s_int + at * I_SIZE;
+            for (int b = 0; b < N; ++b) {
+                const int tb = w0 + b;
+                if (!(H.flags[tb] & F_RESPONDER)) continue;
+                int64_t key = NO_CANDIDATE;
+                if (ex) {
+                    const int64_t kq = static_order_key(s, base + b, ints, s.s_keys + at * s.boxes * 3);
+                    double toi;
+                    V lc;
+                    if (kq < NOT_A_CANDIDATE &&
+                        static_values(s, base + b, ends[tb], H.vend[tb], s.s_geo + at * G_SIZE, ints[I_KIND], &toi, &lc))
+                        key = kq;
+                }
+                H.skey[(size_t)q * H.P + tb] = key;
+            }
+        }
     }
     __syncthreads();
     // (3b) the gradient: each free massive ball against its candidates in GetNearbyBalls' order (its row sorted in
@@ -886,26 +909,21 @@ __global__ void __launch_bounds__(EBB_COLLIDE_THREADS, EBB_COLLIDE_MIN_BLOCKS) t
             const int o = H.slot[(size_t)q * H.P + t];
             potential<0>(W, j, o, pb, H.pos(w0 + o), acc);
         }
-        if (s.statics > 0) {                                          // then the static collidables (COL-712)
+        if (STATICS) {                                                // then the static collidables (COL-712)
             V pe = pb, ve = ldv(s.vel, i);
             integrate(pe, ve, ldv(s.last_g, i), dmul(s.mass[i], s.agility[i]), k, s.time_factor[i], dt, dt);
-            int64_t* okey = H.key + t;                                    // the row again, a stride P apart
-            uint8_t* oslot = H.slot + t;
+            int64_t* okey = H.skey + t;                                   // the row, a stride P apart
+            uint8_t* oslot = H.sslot + t;
             int nst = 0;                                                  // the reacting ones in the walk's order:
-            for (int q = 0; q < s.statics && q < MAX_SLOTS; ++q) {        // first box, parent id, id, slot
-                const int64_t at = w * s.statics + q;
-                if (!s.s_exists[at]) continue;
-                const int64_t* ints = s.s_int + at * I_SIZE;
-                const int64_t key = static_order_key(s, i, ints, s.s_keys + at * s.boxes * 3);
-                if (key >= NOT_A_CANDIDATE) continue;
-                double toi;
-                V lc;
-                if (!static_values(s, i, pe, ve, s.s_geo + at * G_SIZE, ints[I_KIND], &toi, &lc)) continue;
+            for (int q = 0; q < S; ++q) {                                 // first box, parent id, id, slot
+                const int64_t key = okey[(size_t)q * H.P];
+                if (key == NO_CANDIDATE) continue;
+                const int64_t* ints = s.s_int + (w * S + q) * I_SIZE;
                 int pos = nst++;
                 while (pos > 0) {
                     const int64_t kp = okey[(size_t)(pos - 1) * H.P];
                     const int sp = oslot[(size_t)(pos - 1) * H.P];
-                    const int64_t* pi = s.s_int + (w * s.statics + sp) * I_SIZE;
+                    const int64_t* pi = s.s_int + (w * S + sp) * I_SIZE;
                     const bool after = kp > key ||
                                        (kp == key && (pi[I_PARENT] > ints[I_PARENT] ||
                                                                  (pi[I_PARENT] == ints[I_PARENT] && pi[I_ID] > ints[I_ID])));
@@ -984,13 +1002,17 @@ int ebb_collide_tick(const EbbCollideState* s, const uint8_t* active, int32_t* s
     if (s->worlds == 0) return 0;
     const int N = (int)s->slots, wpb = EBB_COLLIDE_THREADS / N > 0 ? EBB_COLLIDE_THREADS / N : 1, threads = wpb * N;
     const unsigned grid = (unsigned)((s->worlds + wpb - 1) / wpb);
-    const size_t smem = ebb::collide::hood_bytes(threads, ebb::collide::hood_rows(N, s->statics));  // 30 KB at 16 slots
+    const size_t smem = ebb::collide::hood_bytes(threads, N, (int)s->statics);   // 34 KB at 16 slots, 164 KB at most
+    const bool st = s->statics > 0;
     if (smem > 48 * 1024) {
-        const cudaError_t e = cudaFuncSetAttribute(ebb::collide::tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)smem);
+        const cudaError_t e = cudaFuncSetAttribute(st ? ebb::collide::tick_kernel<true> : ebb::collide::tick_kernel<false>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
     }
-    ebb::collide::tick_kernel<<<grid, threads, smem, (cudaStream_t)stream>>>(*s, active, status);
+    if (st)
+        ebb::collide::tick_kernel<true><<<grid, threads, smem, (cudaStream_t)stream>>>(*s, active, status);
+    else
+        ebb::collide::tick_kernel<false><<<grid, threads, smem, (cudaStream_t)stream>>>(*s, active, status);
     return launched();
 }
 
