@@ -28,3 +28,20 @@ def test_ranges_and_targets():
             assert 1e8 * 0.99 <= d <= 1e11 * 1.01
     kinds = sum(w.follow_mask), sum(w.orbit_mask), sum(w.warp_mask)
     assert all(k > 150 for k in kinds)
+
+
+def test_partition_workloads_carry_every_column_the_park_loads():
+    """The partition workloads (the ragged headline's worlds and the reference's space benchmark shape) give every
+    column VecModesPark.load_columns takes, each as the same worlds given as rows would load it."""
+    import numpy as np
+
+    from exact_ballpark_b200.modes import ROW_COLUMNS, rows_to_columns
+    from exact_ballpark_b200.workloads import face_worlds, partition_worlds
+    keys = [k for k, _, _ in ROW_COLUMNS] + ["pos", "vel"]
+    for pw in (face_worlds(1, 16), partition_worlds(1, 16)):
+        assert set(keys) <= set(pw.cols), sorted(set(keys) - set(pw.cols))
+        rows = [{k: (pw.cols[k][i].tolist() if k in ("pos", "vel") else pw.cols[k][i].item()) for k in keys}
+                for i in range(pw.n)]
+        back = rows_to_columns(rows)
+        for k in keys:
+            assert np.array_equal(back[k], np.asarray(pw.cols[k]).astype(back[k].dtype)), k
