@@ -1,12 +1,13 @@
 """Generates the golden fixtures under tests/golden/ from the reference itself (run where the reference is checked
 out; nothing on a GPU box runs this):
 
-    EXACT_BALLPARK_REF=<checkout of exact-ballpark> python tests/golden/make_golden.py [--only libm|traces|collide]
+    EXACT_BALLPARK_REF=<checkout of exact-ballpark> python tests/golden/make_golden.py [--only libm|libm_dense|traces|collide]
 
 1. libm.npz: inputs and outputs of glibc 2.34 aarch64's functions as the reference transcribes them (dlibm.sin,
    cos, sincos, log; vec_exp.exp; vec_libm.expf, logf, sinf, cosf, acosf, atanf, atan2f, pow), on seeded random
    arguments over each function's branches plus the edge cases (zeros, infinities, NaN, subnormals, the branch
-   bounds, sincos's odd point +-0x1.ad1fb54442d18p+0).
+   bounds, sincos's odd point +-0x1.ad1fb54442d18p+0); libm_dense.npz: the double functions densely around their
+   branch bounds (make_libm_dense).
 2. trace_*.json.gz / .npz: the flight-mode park's scenarios as golden traces (tests/golden/trace.py), recorded on
    the reference's batched park (VecModesPark, CPU tick):
    - mc{1,2}: the reference's own mode_cases scenarios (tests/mode_cases.py; seed 1 development, 2 held out),
@@ -113,6 +114,66 @@ def make_libm(rng: np.random.Generator, n: int = 3000) -> None:
     out["pow_out"] = L.pow(torch.tensor(px), torch.tensor(py)).numpy()
     np.savez_compressed(HERE / "libm.npz", **out)
     print("libm.npz", {k: v.shape for k, v in out.items()})
+
+
+def _around(points, ulps: int = 24, rel=(1e-15, 1e-12, 1e-9, 1e-6)) -> np.ndarray:
+    """Each point, its neighbours up to `ulps` representable steps either way, and relative nudges either way."""
+    out = []
+    for p in points:
+        p = float(p)
+        lo = hi = p
+        out.append(p)
+        for _ in range(ulps):
+            lo, hi = np.nextafter(lo, -np.inf), np.nextafter(hi, np.inf)
+            out += [lo, hi]
+        out += [p * (1.0 + r) for r in rel] + [p * (1.0 - r) for r in rel]
+    return np.array(out, dtype=np.float64)
+
+
+def make_libm_dense(rng: np.random.Generator) -> None:
+    """libm_dense.npz: the double functions (dlibm.sin, cos, sincos, log; vec_exp.exp; vec_libm.pow) densely around
+    glibc 2.34's branch bounds, as its sources state them: sin and cos at |x| = 2^-26, 0.126 (the Taylor step),
+    0.855469, 2.426265, 105414350 (the reduction's switch) and 2^48, and near multiples of pi/2 (the reduced
+    argument's cancellation) up to 10^8; exp at 2^-54, +-512 (the scaled path), 709.78 (overflow), -708.39 (the
+    subnormal results) and -745.13 (underflow); log near 1 (the 0.9375 and 1.0644531 bounds of its polynomial path),
+    near the smallest normal and through the subnormals; pow at x near 1 with large |y|, at results near the overflow
+    and underflow bounds, at negative x with integer and half-integer y, and at tiny |y|."""
+    from exact_ballpark import dlibm, vec_exp, vec_libm as L
+
+    sc_bounds = [2.0 ** -26, 0.126, 0.855469, 2.426265, 105414350.0, 2.0 ** 48]
+    k = np.concatenate([np.arange(1, 400), rng.integers(400, 10 ** 8, 600)]).astype(np.float64)
+    halfpi = np.pi / 2.0
+    sx = np.concatenate([_around(sc_bounds), -_around(sc_bounds), _around(k * halfpi, ulps=6, rel=()),
+                         -_around(k[:200] * halfpi, ulps=6, rel=())])
+    out = {"sin_x": sx}
+    out["sin_y"] = np.array([dlibm.sin(float(v)) for v in sx])
+    out["cos_y"] = np.array([dlibm.cos(float(v)) for v in sx])
+    pairs = [dlibm.sincos(float(v)) for v in sx]
+    out["sincos_s"] = np.array([a for a, _ in pairs])
+    out["sincos_c"] = np.array([b for _, b in pairs])
+    ex = np.concatenate([_around([2.0 ** -54, -2.0 ** -54, 512.0, -512.0, 709.782712893384, -708.3964185322641,
+                                  -745.1332191019411, -745.1332191019412, 1024.0, -1024.0], ulps=40),
+                         rng.uniform(-746.0, -700.0, 2000), rng.uniform(700.0, 710.0, 1000)])
+    out["exp_x"] = ex
+    out["exp_y"] = vec_exp.exp(__import__("torch").tensor(ex)).numpy()
+    lx = np.concatenate([_around([1.0, 0.9375, 1.0644531250000000, float.fromhex("0x1.0p-1022")], ulps=40),
+                         np.exp(rng.uniform(-745.0, -708.0, 2000)), rng.uniform(0.93, 1.07, 3000)])
+    out["log_x"] = lx
+    out["log_y"] = np.array([dlibm.log(float(v)) for v in lx])
+    n = 1500
+    px = np.concatenate([1.0 + rng.uniform(-1e-9, 1e-9, n), rng.uniform(0.5, 2.0, n), -rng.integers(1, 50, n) * 1.0,
+                         -rng.uniform(0.1, 10.0, n), rng.uniform(0.0, 1e-300, 200), rng.uniform(1.0, 10.0, n)])
+    py = np.concatenate([rng.uniform(-1e12, 1e12, n),
+                         np.log(2.0) * rng.choice([1024.0, -1022.0, -1074.0], n) / np.log(rng.uniform(0.5, 2.0, n))
+                         * (1.0 + rng.uniform(-1e-12, 1e-12, n)),
+                         rng.integers(-60, 60, n).astype(np.float64) + rng.choice([0.0, 0.5], n),
+                         rng.integers(-9, 9, n).astype(np.float64),
+                         rng.uniform(-2.0, 2.0, 200), rng.uniform(-1.0, 1.0, n) * 2.0 ** -rng.uniform(60.0, 70.0, n)])
+    out["pow_x"], out["pow_y"] = px, py
+    torch = __import__("torch")
+    out["pow_out"] = L.pow(torch.tensor(px), torch.tensor(py)).numpy()
+    np.savez_compressed(HERE / "libm_dense.npz", **out)
+    print("libm_dense.npz", {k: v.shape for k, v in out.items()})
 
 
 # ============================================================================================ traces
@@ -678,7 +739,7 @@ def make_space_crowd() -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=("libm", "powf", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending", "server_ontick",
+    ap.add_argument("--only", choices=("libm", "libm_dense", "powf", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending", "server_ontick",
                                        "server_collide", "server_collide_more", "space_bubbles", "space_crowd"),
                     default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
@@ -687,6 +748,8 @@ def main() -> None:
         make_libm(np.random.default_rng(20261203))
     if a.only in (None, "powf"):
         make_powf(np.random.default_rng(20261204))
+    if a.only in (None, "libm_dense"):
+        make_libm_dense(np.random.default_rng(20261205))
     if a.only in (None, "workload"):
         make_workload_traces()
     if a.only in (None, "traces"):

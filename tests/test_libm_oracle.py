@@ -1,5 +1,5 @@
 """The oracle's libm (ebb_libm.cuh's host build, oracle/oracle_libm.cpp) against the reference's transcriptions of
-glibc 2.34 aarch64 (golden vectors tests/golden/libm.npz, made by tests/golden/make_golden.py from
+glibc 2.34 aarch64 (golden vectors tests/golden/libm.npz and libm_dense.npz, made by tests/golden/make_golden.py from
 exact_ballpark/dlibm.py, vec_exp.py and vec_libm.py): bit for bit on every argument, the edge cases included."""
 
 import numpy as np
@@ -40,3 +40,19 @@ def test_oracle_float_libm_matches_the_exhaustive_digests_on_two_chunks(fn):
         bits = np.arange(c << 24, (c + 1) << 24, dtype=np.uint64).astype(np.uint32)
         y = libm(fn, bits.view(np.float32).astype(np.float64))
         assert f32_digest(bits, y) == z[fn][c], (fn, c)
+
+
+DENSE_CASES = [c for c in LIBM_CASES if c[0] in ("sin", "cos", "sincos_sin", "sincos_cos", "log", "exp", "pow")]
+
+
+@pytest.mark.parametrize("fn,xk,yk,ok", DENSE_CASES, ids=[c[0] for c in DENSE_CASES])
+def test_oracle_double_libm_matches_the_reference_around_its_branch_bounds(fn, xk, yk, ok):
+    """The double functions on arguments packed around glibc's branch bounds (representable neighbours and relative
+    nudges either side; near multiples of pi/2 up to 10^8; exp's and pow's overflow, subnormal and underflow edges;
+    log near 1 and through the subnormals): tests/golden/libm_dense.npz, from the reference's transcriptions."""
+    z = np.load(GOLDEN / "libm_dense.npz")
+    x = z[xk]
+    y = z[yk] if yk else None
+    got = libm(fn, x, y)
+    eq = bit_equal(got, z[ok])
+    assert eq.all(), f"{fn}: {(~eq).sum()} of {eq.size} differ, first at x={x[~eq][:3]}"
