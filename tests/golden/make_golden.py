@@ -381,6 +381,30 @@ def make_collide_traces(sample: int) -> None:
     print(f"  collide_s0: 64 worlds x (8 balls + 8 static collidables), 100 ticks, {time.time() - t:.0f} s")
 
 
+def make_collide_crowd() -> None:
+    """collide_crowd: the reference's collision park on crowded worlds of 48 and 64 slots (the park's largest),
+    workloads.collide_worlds with 8 ships and 16 or 24 free and 24 or 32 fixed spheres, 16 worlds each, 60 ticks,
+    the ships re-aimed every 20 ticks: the worlds the GPU tick's largest shared-memory tables serve."""
+    import collide_trace as ct
+    from exact_ballpark.vec_collide import VecCollidePark
+    from exact_ballpark_b200.workloads import collide_worlds
+
+    Rec = ct.recording(VecCollidePark)
+    traces = []
+    for ships, spheres, fixed in ((8, 16, 24), (8, 24, 32)):
+        t = time.time()
+        n = ships + spheres + fixed
+        w = collide_worlds(31 + n, 16, ships=ships, spheres=spheres, statics=fixed, ticks=60, reaim=20)
+        park = Rec(16, n, friction=1.0e6, tick_interval_ms=1000, device="cpu")
+        park.load(w.worlds)
+        for step in range(1, 61):
+            w.apply(park, step)
+            park.evolve()
+        traces.append(park.trace)
+        print(f"  collide_crowd: 16 worlds x {n} balls, 60 ticks, {time.time() - t:.0f} s")
+    ct.save(traces, HERE / "collide_crowd")
+
+
 def make_rand() -> None:
     """rand.npz: glibc's rand() after srand(seed) from the reference's own generator (exact_ballpark.space's
     GlibcRandom, glibc_rand.py), 2000 draws for each of 40 seeds (edge seeds included: 0, 1, 2^31 - 1, 2^31, 2^32 - 1,
@@ -739,7 +763,7 @@ def make_space_crowd() -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=("libm", "libm_dense", "powf", "traces", "workload", "collide", "rand", "combat", "composed", "server", "server_pending", "server_ontick",
+    ap.add_argument("--only", choices=("libm", "libm_dense", "powf", "traces", "workload", "collide", "collide_crowd", "rand", "combat", "composed", "server", "server_pending", "server_ontick",
                                        "server_collide", "server_collide_more", "space_bubbles", "space_crowd"),
                     default=None)
     ap.add_argument("--sample", type=int, default=3, help="scenarios per family checked against the scalar reference")
@@ -756,6 +780,8 @@ def main() -> None:
         make_traces(a.sample)
     if a.only in (None, "collide"):
         make_collide_traces(a.sample)
+    if a.only in (None, "collide_crowd"):
+        make_collide_crowd()
     if a.only in (None, "rand"):
         make_rand()
     if a.only in (None, "combat"):

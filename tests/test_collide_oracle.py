@@ -7,7 +7,7 @@ frictions), its static_cases scenarios (capsules and oriented boxes: ships throu
 at rest beside, backing into them; faces, edges and corners of aligned, rotated, skewed and flat boxes; a box wider than
 a top box; fields and clusters with racers; several static collidables touched in one tick) and the collision
 benchmark's worlds (64 worlds of 4 ships, 4 free and 8 fixed spheres; and 64 worlds of 4 ships, 4 fixed spheres and 8
-capsules and boxes; 100 ticks each). Every field's digest after every
+capsules and boxes; 100 ticks each; and crowded worlds of 48 and 64 slots, 60 ticks). Every field's digest after every
 tick, bit for bit; a planted fault is caught. The static collidables' records (exact_ballpark_b200.statics) against the
 reference park's own records, double for double."""
 
@@ -16,7 +16,7 @@ import pytest
 
 import collide_trace as ct
 
-TRACES = ("collide_cc1", "collide_cc2", "collide_w0", "collide_st1", "collide_st2", "collide_s0")
+TRACES = ("collide_cc1", "collide_cc2", "collide_w0", "collide_st1", "collide_st2", "collide_s0", "collide_crowd")
 
 
 def _replay(g, park, plant=None) -> list:
